@@ -1,0 +1,335 @@
+"""Benchmark: path samples/s of the render hot path on the icosphere workload.
+
+Workload (one "step"): a complete render of the 1,310,720-triangle displaced
+icosphere scene (GGX conductor, diffuse floor, 2048×1024 env map with alias
+sampling) at 1920×1080, 64 spp, max depth 12, 4 hero wavelengths — 132,710,400
+path samples — accumulated on the device (rt_render_accumulate).  Inputs are
+seeded synthetic data (no data set exists for this workload).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+value    : path samples/s with the scene resident in HBM, device time of each
+           step from CUDA events on the library's launching stream, max over
+           ranks; every rank renders its own 64 spp (sample indices offset by
+           rank) → weak scaling, no collective on the data path.
+e2e      : the same metric through the C ABI with HOST output buffers (the
+           accumulated image is read back every step), wall time per step.
+roofline : the closest-hit traversal kernel (extend).  Algorithmic bytes per
+           launch = Σ over that launch's rays of 224 B × 8-wide nodes visited
+           + 36 B × triangle tests + 16 B × sphere tests + 64 B × quad tests, as
+           counted by the CPU oracle's restatement of the reference traversal
+           on rays captured from the GPU's own queues (a subsample per bounce,
+           scaled by the bounce's ray count); divided by the kernel's CUDA-event
+           time; peak = measured HBM copy bandwidth.
+cpu_baseline: the CPU oracle (restatement of the reference's CPU path) on a
+           bounded sample of the same frame (bands of rows, 1 spp each).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SPP = 64
+W, H = 1920, 1080
+DEPTH = 12
+HERO = 4
+METRIC = "path samples/s (1920x1080 icosphere workload)"
+UNIT = "path samples/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-roofline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ── clocks during the timed region ───────────────────────────────────────────
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i - 5] for r in self.rows for i in range(5, 9) if r[i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ── CPU legs (the oracle is the checker and the CPU baseline, never the product) ──
+def cpu_band_rate(sb, st, seconds, threads):
+    """Oracle samples/s on bands of 32 rows × full width × 1 spp until `seconds` pass."""
+    from oracle import oracle as O
+    from rustracer_b200.renderer import pass_params
+    o = O.OracleScene(sb)
+    n = 0
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        row0 = (k * 97) % (H - 32)
+        p = pass_params(W, H, k, 1, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 1000 + k)
+        o.render_pass(st["camera"], p, threads=threads, rows=(row0, row0 + 32))
+        n += 32 * W
+        k += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            return n / el, f"{k} bands of 32 rows x {W} px x 1 spp ({n} path samples, {el:.1f} s)"
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from rustracer_b200 import configs
+    sb, st = configs.icosphere_scene(seed=2)
+    threads = os.cpu_count() or 1
+    from oracle import oracle as O
+    from rustracer_b200.renderer import pass_params
+    o = O.OracleScene(sb)
+
+    def step(k):
+        row0 = (k * 131) % (H - 16)
+        p = pass_params(W, H, k, 1, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 77 + k)
+        o.render_pass(st["camera"], p, threads=threads, rows=(row0, row0 + 16))
+        return 16 * W
+
+    for k in range(args.warmup):
+        step(k)
+    t0 = time.perf_counter()
+    n = sum(step(args.warmup + k) for k in range(args.steps))
+    el = time.perf_counter() - t0
+    v = n / el
+    sample = f"{args.steps} steps of 16 rows x {W} px x 1 spp of the {W}x{H} frame"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el * 1000 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": "icosphere8 1310720 tris 1920x1080 depth12 hero4 (CPU oracle: restatement of the "
+                               "reference's CPU path; the Rust reference cannot be built here)",
+                   "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import ctypes as C
+    from rustracer_b200 import abi, configs
+    from rustracer_b200.renderer import GpuScene, pass_params
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    sb, st = configs.icosphere_scene(seed=2)
+    scene = GpuScene(sb, device=local)
+    cam = st["camera"]
+    per_step = W * H * SPP
+
+    def params(step):
+        return pass_params(W, H, (rank * 100003 + step) * SPP, SPP, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2)
+
+    outs = (torch.zeros((H, W, 3), device=dev), torch.zeros((H, W, 3), device=dev),
+            torch.zeros((H, W), dtype=torch.int32, device=dev))
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)   # 256 MB > 126 MB L2
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for k in range(args.warmup):
+        scene.render_accumulate(cam, params(k), outputs=outs)
+    flush.fill_(1)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    dev_ms = []
+    ext = sh = launches = 0
+    barrier()
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        scene.render_accumulate(cam, params(args.warmup + k), outputs=outs)
+        stt = scene.last_stats()
+        dev_ms.append(stt["ms"])
+        ext += stt["ext_rays"]
+        sh += stt["shadow_rays"]
+        launches += stt["launches"]
+        flush.fill_(k & 0xFF)    # evict L2 between timed steps (not inside the timed region)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    total_ms = sum(dev_ms)
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = ws * per_step * args.steps / (total_ms / 1000.0)
+
+    # e2e: the public C ABI with host output buffers (accumulated image read back every step)
+    host = (torch.empty((H, W, 3), pin_memory=True), torch.empty((H, W, 3), pin_memory=True),
+            torch.empty((H, W), dtype=torch.int32, pin_memory=True))
+    e2e_s = []
+    barrier()
+    for k in range(max(2, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        scene.render_accumulate(cam, params(1000 + k), outputs=host)
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_total = sum(e2e_s)
+    if ws > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = ws * per_step * len(e2e_s) / e2e_total
+    h2d = C.sizeof(abi.RtCamera) + C.sizeof(abi.RtPassParams)
+    d2h = H * W * (3 + 3) * 4 + H * W * 4
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded icosphere, Perlin displacement, procedural sky)",
+        "config": {"workload": "icosphere8 1310720 tris, GGX conductor + diffuse floor, 2048x1024 env, "
+                               "1920x1080, 64 spp, depth 12, hero 4",
+                   "spp_per_step": SPP, "path_samples_per_step_per_gpu": per_step,
+                   "parallelism": f"weak: {ws} rank(s), each its own 64 spp",
+                   "l2": "256 MB buffer written between timed steps; scene (~230 MB) exceeds L2"},
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "rays": {"extension": int(ext), "shadow": int(sh),
+                 "rays_per_s": (ext + sh) / (sum(dev_ms) / 1000.0)},
+    }
+
+    if rank == 0 and not args.no_roofline:
+        line["roofline"] = roofline(scene, sb, cam)
+    if rank == 0 and not args.no_cpu_baseline and ws == 1:
+        threads = os.cpu_count() or 1
+        v, sample = cpu_band_rate(sb, st, args.cpu_seconds, threads)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def roofline(scene, sb, cam):
+    """Roofline of the extend (closest-hit) kernel; see the module docstring."""
+    from oracle import oracle as O
+    from rustracer_b200.renderer import pass_params
+    peak, peak_kind = measured_peak()
+    p1 = pass_params(W, H, 5000, 1, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2)
+    scene.set_profiling(True)
+    p = pass_params(W, H, 6000, SPP, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2)
+    scene.render_accumulate(cam, p)
+    kt = scene.kernel_times()
+    scene.set_profiling(False)
+    o = O.OracleScene(sb)
+    rng = np.random.default_rng(0)
+    total_bytes_pass = 0.0
+    per_depth = []
+    for d in range(DEPTH):
+        r = scene.capture_rays(cam, p1, d, W * H)
+        if len(r) == 0:
+            break
+        sub = r[rng.choice(len(r), size=min(len(r), 20000), replace=False)]
+        stt = o.trace_stats(sub)
+        bpr = (224.0 * stt[:, 0] + 36.0 * stt[:, 1] + 16.0 * stt[:, 2] + 64.0 * stt[:, 3]).mean()
+        total_bytes_pass += bpr * len(r)
+        per_depth.append((d, len(r), float(bpr), float(stt[:, 0].mean()), float(stt[:, 1].mean())))
+    ext_ms, ext_launches = kt["extend"]
+    achieved = total_bytes_pass * SPP / (ext_ms / 1000.0) / 1e9 if ext_ms > 0 else None
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "extend_icosphere_traffic.txt")
+    if os.path.exists(tfile):
+        for ln in open(tfile):
+            if ln.startswith("traffic_bytes_per_launch:"):
+                traffic = float(ln.split(":")[1])
+    return {"kernel": "k_extend (8-wide BVH closest hit)", "bound": "hbm", "achieved": achieved, "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+            "traffic": traffic, "algorithmic_bytes_per_launch": total_bytes_pass / max(1, len(per_depth)),
+            "launches": ext_launches, "kernel_ms": ext_ms,
+            "stage_ms": {k: v[0] for k, v in kt.items()},
+            "per_bounce": [{"depth": d, "rays": n, "bytes_per_ray": b, "nodes_per_ray": nn, "tris_per_ray": tt}
+                           for d, n, b, nn, tt in per_depth]}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

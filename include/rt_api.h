@@ -1,0 +1,240 @@
+/*
+ * rt_api.h — C ABI of the B200 render hot path (librtb200.so).
+ *
+ * This is the drop-in boundary for the reference renderer's sample-pass entry
+ * point.  The reference exposes (src/renderer.rs:655-669)
+ *
+ *     render_tiles(scratch, converged, sample_idx, strata, width, height,
+ *                  camera, world, background, lights, bg_scale, photon_map,
+ *                  frame_time)
+ *
+ * with trait objects (&dyn Hittable, &dyn Material) that cannot cross an FFI.
+ * Here the scene is handed over once as flat structure-of-arrays buffers
+ * (RtSceneDesc), flattened on the host exactly as the reference's loader builds
+ * it (src/scene_file.rs:899-1132), and rendering calls take plain pointers.
+ *
+ * Conventions
+ *  - Every function returns an int32 status: RT_OK (0) or an RT_ERR_* code.
+ *    rt_last_error() returns the message of the last failure on a handle.
+ *  - The caller owns every buffer it passes; the library copies what it keeps.
+ *  - Buffers flagged RT_MEM_DEVICE are CUDA device pointers on the scene's
+ *    device; otherwise they are host pointers (pageable or pinned).
+ *  - One handle per thread; calls on one handle are serialised on its stream.
+ *  - All arithmetic is IEEE-754 binary32 ("f32" in the reference).
+ */
+#ifndef RT_API_H
+#define RT_API_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RT_API_VERSION 1
+
+/* ── status codes ─────────────────────────────────────────────────────────── */
+#define RT_OK            0
+#define RT_ERR_INVALID   1   /* degenerate or malformed input (replaces the reference's asserts, e.g. src/quad.rs:27-28) */
+#define RT_ERR_CAPACITY  2   /* a queue, stack or table limit was exceeded */
+#define RT_ERR_TIMEOUT   3   /* a bounded device loop ran out of iterations */
+#define RT_ERR_CUDA      4   /* a CUDA runtime call failed */
+#define RT_ERR_NOMEM     5   /* a device allocation failed */
+
+#define RT_MEM_HOST      0
+#define RT_MEM_DEVICE    1
+
+/* ── materials (src/material.rs, src/texture.rs) ─────────────────────────── */
+#define RT_MAT_LAMBERTIAN          0  /* material.rs:85-102, texture Solid */
+#define RT_MAT_CHECKER             1  /* Lambertian with texture.rs:32-37 checker */
+#define RT_MAT_DIELECTRIC          2  /* material.rs:323-332 */
+#define RT_MAT_SPECTRAL_DIELECTRIC 3  /* material.rs:357-403 */
+#define RT_MAT_SPECTRAL_METAL      4  /* material.rs:427-554 */
+#define RT_MAT_DIFFUSE_LIGHT       5  /* material.rs:14-25 */
+#define RT_MAT_BLACKBODY_LIGHT     6  /* material.rs:40-83 */
+
+/* conductor n,k tables built into the library (src/spectrum.rs:213-240) */
+#define RT_METAL_GOLD    0
+#define RT_METAL_COPPER  1
+#define RT_METAL_SILVER  2
+#define RT_METAL_CUSTOM  3  /* uses RtMaterial.nk_* (a uniform wavelength grid) */
+#define RT_MAX_NK        16
+
+typedef struct RtMaterial {
+    int32_t type;            /* RT_MAT_* */
+    float   albedo[3];       /* Lambertian colour, checker "even", DiffuseLight colour */
+    float   odd[3];          /* checker "odd" colour */
+    float   checker_scale;   /* checker tile frequency (texture.rs:32-37) */
+    float   cauchy_b;        /* Dielectric: ior; SpectralDielectric: Cauchy B (µm²) */
+    float   cauchy_c;        /* SpectralDielectric: Cauchy C (µm²) */
+    float   absorption[3];   /* SpectralDielectric Beer-Lambert sigma per unit length */
+    float   roughness;       /* SpectralMetal roughness (alpha = max(r², 1e-4)) */
+    int32_t metal;           /* RT_METAL_* */
+    float   temp_k;          /* BlackbodyLight temperature (K) */
+    float   intensity;       /* BlackbodyLight intensity */
+    int32_t nk_count;        /* RT_METAL_CUSTOM: samples on the grid */
+    float   nk_start;        /* RT_METAL_CUSTOM: first wavelength (nm) */
+    float   nk_step;         /* RT_METAL_CUSTOM: grid step (nm) */
+    float   nk_n[RT_MAX_NK];
+    float   nk_k[RT_MAX_NK];
+} RtMaterial;
+
+/* ── background (src/renderer.rs:183-223) ────────────────────────────────── */
+#define RT_BG_SOLID     0
+#define RT_BG_GRADIENT  1
+#define RT_BG_ENVMAP    2   /* EnvMap, or EnvMapSplit when visible_type >= 0 */
+
+typedef struct RtBackground {
+    int32_t      type;            /* RT_BG_* */
+    float        color[3];        /* Solid */
+    float        top[3];          /* Gradient */
+    float        bottom[3];
+    /* env map: equirectangular, row-major H×W×3 float RGB, top row = +Y */
+    int32_t      env_w, env_h;
+    const float* env_rgb;
+    float        env_rot_y_deg;   /* EnvMapData::with_rotation (renderer.rs:78-81) */
+    /* EnvMapSplit visible backdrop: -1 = none, else RT_BG_SOLID / RT_BG_GRADIENT */
+    int32_t      visible_type;
+    float        visible_color[3];
+    float        visible_top[3];
+    float        visible_bottom[3];
+} RtBackground;
+
+/* ── scene description ───────────────────────────────────────────────────── *
+ * Primitives are world-space (object transforms of transform.rs are applied on
+ * the host before the call).  The canonical primitive id used for hit records
+ * and tie-breaking is: triangles [0, n_tris), then quads, then spheres, each in
+ * the order given. */
+#define RT_PRIM_TRI    0
+#define RT_PRIM_QUAD   1
+#define RT_PRIM_SPHERE 2
+
+typedef struct RtSceneDesc {
+    int64_t        n_tris;
+    const float*   tri_v;         /* n_tris × 9  : v0, v1, v2 */
+    const float*   tri_n;         /* n_tris × 9  : per-vertex normals (NULL → face normal) */
+    const int32_t* tri_mat;       /* n_tris      : material index */
+    int64_t        n_quads;
+    const float*   quad_quv;      /* n_quads × 9 : corner Q, edge u, edge v (quad.rs:21-33) */
+    const int32_t* quad_mat;
+    int64_t        n_spheres;
+    const float*   sphere;        /* n_spheres × 4 : centre xyz, radius */
+    const int32_t* sphere_mat;
+    int32_t        n_mats;
+    const RtMaterial* mats;
+    /* NEE light list (hittable.rs:138-225): canonical prim ids of the light
+     * copies (quads or spheres).  The reference inserts each [[lights]] quad in
+     * the world AND in the light list (scene_file.rs:1065-1066). */
+    int32_t        n_lights;
+    const int32_t* light_prims;
+    RtBackground   bg;
+    /* spectral sampling: 0 = reference range 380–700 nm (65-entry CIE table),
+     * 1 = 380–780 nm (table extended past 700 nm) */
+    int32_t        spectral_range;
+} RtSceneDesc;
+
+/* ── camera (src/camera.rs:24-59) ────────────────────────────────────────── */
+typedef struct RtCamera {
+    float   origin[3];
+    float   lower_left[3];
+    float   horizontal[3];
+    float   vertical[3];
+    float   u[3], v[3];
+    float   lens_radius;
+    int32_t aperture_blades;  /* 0 = round lens; polygonal bokeh is not supported */
+} RtCamera;
+
+/* ── one sample pass (render_tiles, renderer.rs:655-730) ─────────────────── */
+typedef struct RtPassParams {
+    uint32_t width, height;
+    uint32_t sample_idx;     /* first sample index of this call */
+    uint32_t n_samples;      /* consecutive sample passes rendered by this call (≥1) */
+    uint32_t strata;         /* ⌊√spp⌋ stratification grid (main.rs:64) */
+    uint32_t max_depth;      /* reference constant MAX_DEPTH = 50 (renderer.rs:16) */
+    uint32_t hero_count;     /* wavelengths per path: 1 (reference) or 4 */
+    uint32_t use_frame_time; /* 0: time ~ U[0,1) (camera.rs:57); 1: t0 + U·(t1-t0) */
+    float    t0, t1;
+    float    bg_scale;       /* multiplies the background on a miss only (renderer.rs:402) */
+    uint64_t seed;           /* per-pixel RNG streams are keyed on (seed, pixel, sample) */
+} RtPassParams;
+
+/* ── hit record for the ray-level test entry points ──────────────────────── */
+typedef struct RtHit {
+    int32_t prim;      /* canonical primitive id, -1 = miss */
+    float   t;
+    float   b1, b2;    /* triangle barycentrics / quad (alpha, beta) / sphere (u, v) */
+} RtHit;
+
+typedef struct RtScene RtScene;
+
+/* Library / device information. */
+int32_t rt_version(void);
+int32_t rt_device_count(int32_t* count);
+
+/* Create a scene on CUDA device `device`: copies the descriptor's arrays,
+ * builds the 8-wide SAH BVH with the cost model of src/bvh.rs:52-174 and the
+ * environment sampling tables (renderer.rs:32-74).  Replaces
+ * scene_file::build (scene_file.rs:899-1132) + BvhTree::from_list (bvh.rs:199). */
+int32_t rt_scene_create(const RtSceneDesc* desc, int32_t device, RtScene** out);
+int32_t rt_scene_destroy(RtScene* scene);
+int32_t rt_last_error(const RtScene* scene, char* buf, size_t len);
+
+/* BVH statistics of the built tree: node count, leaf count, max depth, SAH cost. */
+int32_t rt_scene_bvh_stats(const RtScene* scene, int64_t* n_nodes, int64_t* n_leaves,
+                           int32_t* max_depth, double* sah_cost);
+/* Export the 8-wide node array in the reference layout (bvh.rs:25-32, 224 B per
+ * node: min[3][8], max[3][8], children[8]; leaf = -(leaf_slot+1), INT32_MIN =
+ * empty) and the canonical prim id of every leaf slot.  Pass NULL to query sizes. */
+int32_t rt_scene_bvh_export(const RtScene* scene, float* nodes_224B, int64_t* n_nodes,
+                            int32_t* leaf_prims, int64_t* n_leaves);
+
+/* Closest hit for n rays.  rays: n × 8 floats (origin xyz, dir xyz, t_min, t_max).
+ * Replaces BvhTree::hit_index (bvh.rs:229-288).  Ties on t go to the smaller
+ * canonical prim id. */
+int32_t rt_trace_closest(RtScene* scene, const float* rays, int64_t n, RtHit* hits, int32_t mem);
+/* Any hit for n rays (bvh.rs:487-530); occluded[i] = 1 when a hit exists. */
+int32_t rt_trace_any(RtScene* scene, const float* rays, int64_t n, uint8_t* occluded, int32_t mem);
+
+/* One call = params->n_samples consecutive sample passes of render_tiles.
+ * scratch_rgb receives n_samples × height × width × 3 floats (linear radiance,
+ * row 0 = top image row), the per-pass output of render_tiles.  converged
+ * (nullable, height × width bytes) skips pixels like renderer.rs:695-698. */
+int32_t rt_render_pass(RtScene* scene, const RtCamera* cam, const RtPassParams* params,
+                       float* scratch_rgb, const uint8_t* converged, int32_t mem);
+
+/* Render params->n_samples passes and fold them into device-resident
+ * accumulators in sample order with the semantics of accumulate_sample
+ * (main.rs:603-643): non-finite samples dropped, optional luminance clamp
+ * max(firefly_clamp·mean_lum, firefly_floor) after firefly_min_samples, per-
+ * channel Welford.  With reset != 0 the accumulators are cleared first.
+ * out_sum (h×w×3), out_m2 (h×w×3), out_count (h×w) are written when non-NULL. */
+int32_t rt_render_accumulate(RtScene* scene, const RtCamera* cam, const RtPassParams* params,
+                             float firefly_clamp, uint32_t firefly_min_samples,
+                             float firefly_floor, int32_t reset,
+                             float* out_sum, float* out_m2, uint32_t* out_count, int32_t mem);
+
+/* Device timing of the last render call: total milliseconds and ray counts. */
+int32_t rt_last_render_stats(const RtScene* scene, double* ms, int64_t* ext_rays,
+                             int64_t* shadow_rays, int64_t* kernel_launches);
+
+/* Per-stage device timing (diagnostics, no reference counterpart): with
+ * profiling enabled every launch of the render loop is bracketed by CUDA
+ * events on the launching stream.  ms[4] / launches[4] receive the totals of
+ * the last render call for: 0 generate+finalize, 1 extend (closest hit),
+ * 2 shade, 3 shadow (any hit). */
+int32_t rt_set_profiling(RtScene* scene, int32_t enable);
+int32_t rt_kernel_times(const RtScene* scene, double* ms, int64_t* launches);
+
+/* Extension rays of bounce `depth` of sample pass params->sample_idx (diagnostics,
+ * no reference counterpart): renders one pass and copies up to max_rays of that
+ * bounce's queued rays as n × 8 floats (origin, direction, t_min, t_max) into
+ * host memory.  Used to count the reference traversal's work on the rays the
+ * GPU actually traces. */
+int32_t rt_capture_rays(RtScene* scene, const RtCamera* cam, const RtPassParams* params,
+                        uint32_t depth, float* rays, int64_t max_rays, int64_t* n_rays);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RT_API_H */

@@ -1,0 +1,213 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so).  TEST INFRASTRUCTURE ONLY:
+imported by tests/, __graft_entry__.smoke() and bench.py's CPU legs, never by
+the rustracer_b200 package.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from rustracer_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            from . import build as _b  # noqa
+        if not os.path.exists(path):
+            import importlib.util
+            spec = importlib.util.spec_from_file_location("oracle_build", os.path.join(HERE, "build.py"))
+            m = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(m)
+            m.build()
+        L = C.CDLL(path)
+        vp, f, i32, i64, u32 = C.c_void_p, C.c_float, C.c_int32, C.c_int64, C.c_uint32
+        fp = C.POINTER(C.c_float)
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_scene_create.argtypes = [C.POINTER(abi.RtSceneDesc), C.POINTER(vp)]
+        L.orc_scene_destroy.argtypes = [vp]
+        L.orc_bvh_export.argtypes = [vp, fp, C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]
+        L.orc_trace_closest.argtypes = [vp, fp, i64, C.POINTER(abi.RtHit), i32, i32]
+        L.orc_trace_any.argtypes = [vp, fp, i64, C.POINTER(C.c_uint8), i32]
+        L.orc_trace_stats.argtypes = [vp, fp, i64, C.POINTER(i64), i32]
+        L.orc_render_pass.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), fp,
+                                      C.POINTER(C.c_uint8), i32, u32, u32, C.POINTER(i64)]
+        L.orc_accumulate.argtypes = [fp, fp, C.POINTER(u32), fp, C.POINTER(C.c_uint8), i64, f, u32, f]
+        L.orc_mark_converged.argtypes = [C.POINTER(C.c_uint8), C.POINTER(u32), fp, fp, i64, f]
+        L.orc_mark_converged.restype = i64
+        for name, nargs in [("orc_fresnel_dielectric", 2), ("orc_fresnel_conductor", 3), ("orc_cauchy_ior", 3),
+                            ("orc_planck_raw", 2), ("orc_ggx_ndf", 2), ("orc_smith_g1", 2),
+                            ("orc_smith_lambda", 2), ("orc_e_ss", 2), ("orc_energy_comp", 2)]:
+            fn = getattr(L, name)
+            fn.argtypes = [f] * nargs
+            fn.restype = f
+        L.orc_elut_export.argtypes = [fp]
+        L.orc_spectral_to_rgb.argtypes = [f, i32, fp]
+        L.orc_spectral_fire_rgb.argtypes = [f, i32, fp]
+        L.orc_metal_ior.argtypes = [i32, f, fp, fp]
+        L.orc_vndf_sample.argtypes = [fp, f, f, f, f, fp]
+        L.orc_env_sample.argtypes = [vp, fp, fp]
+        L.orc_env_pdf.argtypes = [vp, fp]
+        L.orc_env_pdf.restype = f
+        L.orc_env_sample_dir.argtypes = [vp, fp, fp, fp]
+        L.orc_bg_eval.argtypes = [vp, fp, fp]
+        L.orc_env_eval.argtypes = [vp, fp, fp]
+        L.orc_lights_pdf_value.argtypes = [vp, fp, fp]
+        L.orc_lights_pdf_value.restype = f
+        L.orc_rng.argtypes = [C.c_uint64, u32, u32, u32, C.POINTER(u32), fp]
+        _lib = L
+    return _lib
+
+
+def _f(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def vec3_call(name, *args, range_mode=0):
+    out = np.zeros(3, np.float32)
+    getattr(lib(), name)(*args, range_mode, _fp(out))
+    return out
+
+
+def spectral_to_rgb(lam, range_mode=0):
+    return vec3_call("orc_spectral_to_rgb", C.c_float(lam), range_mode=range_mode)
+
+
+def spectral_fire_rgb(lam, range_mode=0):
+    return vec3_call("orc_spectral_fire_rgb", C.c_float(lam), range_mode=range_mode)
+
+
+def metal_ior(metal, lam):
+    n, k = C.c_float(), C.c_float()
+    lib().orc_metal_ior(metal, lam, C.byref(n), C.byref(k))
+    return n.value, k.value
+
+
+def scalar(name, *args):
+    return getattr(lib(), "orc_" + name)(*[C.c_float(a) for a in args])
+
+
+def elut():
+    out = np.zeros((64, 64), np.float32)
+    lib().orc_elut_export(_fp(out))
+    return out
+
+
+def rng(seed, pixel, sample, dim):
+    u, f = C.c_uint32(), C.c_float()
+    lib().orc_rng(seed, pixel, sample, dim, C.byref(u), C.byref(f))
+    return u.value, f.value
+
+
+class OracleScene:
+    """Oracle scene built from a SceneBuilder (same RtSceneDesc as the GPU path)."""
+
+    def __init__(self, builder):
+        self._builder = builder
+        self._desc = builder.desc()
+        self.h = C.c_void_p()
+        rc = lib().orc_scene_create(C.byref(self._desc), C.byref(self.h))
+        if rc != 0:
+            raise ValueError(lib().orc_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().orc_scene_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def bvh(self):
+        nn, nl = C.c_int64(), C.c_int64()
+        lib().orc_bvh_export(self.h, None, C.byref(nn), None, C.byref(nl))
+        nodes = np.zeros((nn.value, 56), np.float32)
+        leaves = np.zeros(nl.value, np.int32)
+        lib().orc_bvh_export(self.h, _fp(nodes), C.byref(nn), leaves.ctypes.data_as(C.POINTER(C.c_int32)),
+                             C.byref(nl))
+        return nodes, leaves
+
+    def trace_closest(self, rays, brute=False, threads=os.cpu_count()):
+        rays = _f(rays).reshape(-1, 8)
+        hits = (abi.RtHit * len(rays))()
+        lib().orc_trace_closest(self.h, _fp(rays), len(rays), hits, 1 if brute else 0, threads)
+        a = np.frombuffer(hits, dtype=np.dtype([("prim", np.int32), ("t", np.float32), ("b1", np.float32),
+                                                ("b2", np.float32)]))
+        return a.copy()
+
+    def trace_any(self, rays, threads=os.cpu_count()):
+        rays = _f(rays).reshape(-1, 8)
+        occ = np.zeros(len(rays), np.uint8)
+        lib().orc_trace_any(self.h, _fp(rays), len(rays), occ.ctypes.data_as(C.POINTER(C.c_uint8)), threads)
+        return occ
+
+    def trace_stats(self, rays, threads=os.cpu_count()):
+        rays = _f(rays).reshape(-1, 8)
+        out = np.zeros((len(rays), 4), np.int64)
+        lib().orc_trace_stats(self.h, _fp(rays), len(rays), out.ctypes.data_as(C.POINTER(C.c_int64)), threads)
+        return out
+
+    def render_pass(self, cam, params, threads=os.cpu_count(), rows=None, converged=None):
+        n = max(1, params.n_samples)
+        out = np.zeros((n, params.height, params.width, 3), np.float32)
+        cnt = np.zeros(2, np.int64)
+        rb, re = (0, 0) if rows is None else rows
+        conv = None if converged is None else np.ascontiguousarray(converged, dtype=np.uint8)
+        lib().orc_render_pass(self.h, C.byref(cam), C.byref(params), _fp(out),
+                              None if conv is None else conv.ctypes.data_as(C.POINTER(C.c_uint8)),
+                              threads, rb, re, cnt.ctypes.data_as(C.POINTER(C.c_int64)))
+        self.last_counters = cnt
+        return out
+
+    def env_sample(self, d):
+        out = np.zeros(3, np.float32)
+        lib().orc_env_sample(self.h, _fp(_f(d)), _fp(out))
+        return out
+
+    def env_pdf(self, d):
+        return lib().orc_env_pdf(self.h, _fp(_f(d)))
+
+    def env_sample_dir(self, xi):
+        d = np.zeros(3, np.float32)
+        pdf = C.c_float()
+        lib().orc_env_sample_dir(self.h, _fp(_f(xi)), _fp(d), C.byref(pdf))
+        return d, pdf.value
+
+    def bg_eval(self, d):
+        out = np.zeros(3, np.float32)
+        lib().orc_bg_eval(self.h, _fp(_f(d)), _fp(out))
+        return out
+
+    def env_eval(self, d):
+        out = np.zeros(3, np.float32)
+        lib().orc_env_eval(self.h, _fp(_f(d)), _fp(out))
+        return out
+
+    def lights_pdf_value(self, o, d):
+        return lib().orc_lights_pdf_value(self.h, _fp(_f(o)), _fp(_f(d)))
+
+
+class Accumulator:
+    """accumulate_sample / mark_converged state (main.rs:603-677) on the CPU."""
+
+    def __init__(self, npix):
+        self.acc = np.zeros((npix, 3), np.float32)
+        self.m2 = np.zeros((npix, 3), np.float32)
+        self.n = np.zeros(npix, np.uint32)
+        self.conv = np.zeros(npix, np.uint8)
+
+    def add(self, scratch, clamp=0.0, min_samples=4, floor=5.0):
+        s = _f(scratch).reshape(-1, 3)
+        lib().orc_accumulate(_fp(self.acc), _fp(s), self.n.ctypes.data_as(C.POINTER(C.c_uint32)), _fp(self.m2),
+                             self.conv.ctypes.data_as(C.POINTER(C.c_uint8)), len(s), clamp, min_samples, floor)
+
+    def mark_converged(self, thresh=0.05):
+        return lib().orc_mark_converged(self.conv.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                        self.n.ctypes.data_as(C.POINTER(C.c_uint32)), _fp(self.m2),
+                                        _fp(self.acc), len(self.n), thresh)

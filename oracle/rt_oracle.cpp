@@ -1,0 +1,1527 @@
+// rt_oracle.cpp — CPU ORACLE for the render hot path.  TEST INFRASTRUCTURE ONLY.
+//
+// This file restates, in plain C++ on the host CPU, the reference renderer's
+// hot path (mcrepeau/rustracer, a pure-Rust CPU path tracer).  It is the
+// checker the CUDA library is compared against and the timed CPU baseline.
+// Nothing in the product (rustracer_b200/) links or calls it; only tests/,
+// __graft_entry__.smoke() and bench.py's CPU legs load it.
+//
+// What it follows, by reference file:line:
+//   math/ray ........ src/vec3.rs:14-116, src/ray.rs:25-42, src/aabb.rs:10-35, src/onb.rs:10-20
+//   BVH build ....... src/bvh.rs:52-225   (binned SAH, 12 buckets, 3 binary levels per 8-wide node)
+//   traversal ....... src/bvh.rs:229-288 (closest), :487-575 (any / transmittance), slab test :326-364
+//   primitives ...... src/triangle.rs:75-140, src/quad.rs:21-96, src/sphere.rs:47-118
+//   light list ...... src/hittable.rs:156-225 (linear hit scan, mean pdf, uniform pick)
+//   materials ....... src/material.rs:14-149 (lights, Lambertian, Fresnel, dielectric boundary),
+//                     :161-321 (GGX, Smith, E_ss LUT, VNDF), :323-403 (Dielectric, SpectralDielectric),
+//                     :427-554 (SpectralMetal)
+//   spectrum ........ src/spectrum.rs:64-277
+//   background ...... src/renderer.rs:23-223 (EnvMapData CDF sampling, bilinear lookup, Solid/Gradient/Split)
+//   path loop ....... src/renderer.rs:371-585 (ray_color), :655-730 (render_tiles)
+//   camera .......... src/camera.rs:24-59
+//   accumulation .... src/main.rs:603-677 (accumulate_sample, mark_converged)
+//
+// Deliberate, documented differences from the reference (both this oracle and
+// the CUDA library implement them identically):
+//   * Random numbers: the reference draws from rand 0.8's SmallRng seeded per
+//     image row (renderer.rs:688-691); its stream cannot be consumed in the
+//     same order by a parallel GPU path, so both sides use a counter-based hash
+//     keyed on (seed, pixel, sample, dimension) — pcg3d of Jarzynski & Olano,
+//     "Hash Functions for GPU Rendering", JCGT 2020.  Image-level parity is
+//     statistical; ray-level parity (hit ids, t) is exact.
+//   * Closest-hit ties: equal t goes to the smaller canonical prim id instead of
+//     the last one visited (bvh.rs:250-253), so hit ids do not depend on the BVH
+//     layout.  Box culling is made conservative (ray reciprocal directions are
+//     kept finite and the slab exit is widened by 2^-16 relative) so that the
+//     traversal returns exactly the brute-force minimum.
+//   * Hero wavelengths: hero_count = 1 reproduces the reference's single λ per
+//     path; hero_count = 4 carries 4 rotated wavelengths (Wilkie et al. 2014)
+//     whose per-λ scalar weights generalise the reference's spectral_weighted
+//     throughput; secondaries are terminated at dispersive boundaries.
+//   * Lens sampling draws the unit disk by the polar map instead of rejection.
+//   * Object transforms are applied to the primitives before the call
+//     (world-space triangles), and meshes join the world BVH directly instead
+//     of being nested BVH leaves (mesh.rs:91).
+//
+// Built by oracle/build.py with -O3 -mavx2 -mfma -ffp-contract=off: Rust never
+// contracts a*b+c into an FMA, so the oracle must not either.
+
+#include "../include/rt_api.h"
+#include "../include/rt_spectral_tables.h"
+
+#include <immintrin.h>
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+static const float PI_F = 3.14159265358979323846f;
+
+// ── vec3.rs ──────────────────────────────────────────────────────────────────
+struct V3 { float x, y, z; };
+static inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+static inline V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
+static inline V3 operator*(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline V3 operator*(V3 a, float t) { return v3(a.x * t, a.y * t, a.z * t); }
+static inline V3 operator*(float t, V3 a) { return a * t; }
+static inline V3 operator/(V3 a, float t) { return v3(a.x / t, a.y / t, a.z / t); }   // exact division (vec3.rs:95-97)
+static inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline float len2(V3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+static inline float length(V3 a) { return std::sqrt(len2(a)); }
+static inline V3 cross(V3 a, V3 b) {
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline V3 unit(V3 a) { return a / length(a); }
+static inline float luminance(V3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+static inline float comp(V3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+static inline float rmin(float a, float b) { return std::fmin(a, b); }   // f32::min drops one NaN
+static inline float rmax(float a, float b) { return std::fmax(a, b); }
+static inline float clampf(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static inline V3 reflect(V3 v, V3 n) { return v - 2.0f * dot(v, n) * n; }   // vec3.rs:49
+// vec3.rs:55-61 — returns false when k < 0
+static inline bool refract(V3 v, V3 n, float eta, V3* out) {
+    float cos_t = rmin(dot(-v, n), 1.0f);
+    V3 perp = eta * (v + cos_t * n);
+    float k = 1.0f - len2(perp);
+    if (k < 0.0f) return false;
+    *out = perp + (-std::sqrt(k) * n);
+    return true;
+}
+// vec3.rs:37-42
+static inline void onb_vec(V3 n, V3* u, V3* v) {
+    V3 up = std::fabs(n.y) < 0.9f ? v3(0, 1, 0) : v3(1, 0, 0);
+    *u = unit(cross(n, up));
+    *v = cross(n, *u);
+}
+// onb.rs:10-20
+struct Onb { V3 u, v, w; };
+static inline Onb onb_from_w(V3 n) {
+    Onb o;
+    o.w = unit(n);
+    V3 a = std::fabs(o.w.x) > 0.9f ? v3(0, 1, 0) : v3(1, 0, 0);
+    o.v = unit(cross(o.w, a));
+    o.u = cross(o.w, o.v);
+    return o;
+}
+static inline V3 onb_local(const Onb& o, V3 a) { return a.x * o.u + a.y * o.v + a.z * o.w; }
+
+// ── counter-based RNG (pcg3d) ────────────────────────────────────────────────
+static inline uint32_t mix32(uint32_t x) {
+    x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+    return x;
+}
+static inline uint32_t pcg3d_x(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t x = a * 1664525u + 1013904223u;
+    uint32_t y = b * 1664525u + 1013904223u;
+    uint32_t z = c * 1664525u + 1013904223u;
+    x += y * z; y += z * x; z += x * y;
+    x ^= x >> 16; y ^= y >> 16; z ^= z >> 16;
+    x += y * z; y += z * x; z += x * y;
+    return x;
+}
+struct Rng { uint32_t a, b, c; };
+static inline Rng make_rng(uint64_t seed, uint32_t pixel, uint32_t sample) {
+    Rng r;
+    r.a = pixel;
+    r.b = sample ^ mix32((uint32_t)seed);
+    r.c = mix32((uint32_t)(seed >> 32) + 0x9E3779B9u);
+    return r;
+}
+static inline uint32_t rnd_u32(const Rng& r, uint32_t dim) { return pcg3d_x(r.a, r.b, dim ^ r.c); }
+static inline float rnd(const Rng& r, uint32_t dim) { return (float)(rnd_u32(r, dim) >> 8) * (1.0f / 16777216.0f); }
+
+// dimension layout of one path
+enum {
+    D_JIT_U = 0, D_JIT_V = 1, D_LENS_R = 2, D_LENS_P = 3, D_TIME = 4, D_LAMBDA = 5,
+    D_BOUNCE0 = 8, D_PER_BOUNCE = 16,
+    B_SCATTER0 = 0, B_SCATTER1 = 1, B_LPICK = 2, B_LPT0 = 3, B_LPT1 = 4,
+    B_ENV_ROW = 7, B_ENV_COL = 8, B_ENV_JU = 9, B_ENV_JV = 10, B_COS0 = 11, B_COS1 = 12, B_RR = 13,
+};
+
+// ── spectrum.rs ──────────────────────────────────────────────────────────────
+struct Spectrum {
+    int n = RT_CIE_N;                 // entries on the 5 nm grid from 380 nm
+    float xyz[RT_CIE_N + RT_CIE_EXT_N][3];
+    float norms[3], fire_norms[3];
+    float lam_lo = 380.0f, lam_range = 320.0f;
+};
+static inline void xyz_to_srgb_clamped(float x, float y, float z, float out[3]) {   // spectrum.rs:66-73
+    out[0] = rmax(3.2406f * x - 1.5372f * y - 0.4986f * z, 0.0f);
+    out[1] = rmax(-0.9689f * x + 1.8758f * y + 0.0415f * z, 0.0f);
+    out[2] = rmax(0.0557f * x - 0.2040f * y + 1.0570f * z, 0.0f);
+}
+static const float FIRE_LUMA_POW = 0.5f, FIRE_LUMA_FLOOR = 0.08f, FIRE_DESAT = 0.5f;
+static inline void fire_color(float x, float y, float z, float c[3]) {            // spectrum.rs:148-160
+    float w = rmax(std::pow(y, FIRE_LUMA_POW), FIRE_LUMA_FLOOR);
+    float rgb[3]; xyz_to_srgb_clamped(x, y, z, rgb);
+    c[0] = rgb[0] * w; c[1] = rgb[1] * w; c[2] = rgb[2] * w;
+    float d = FIRE_DESAT;
+    if (d > 0.0f) {
+        float lum = 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2];
+        for (int i = 0; i < 3; i++) c[i] = c[i] * (1.0f - d) + lum * d;
+    }
+}
+static void spectrum_init(Spectrum& s, int range_mode) {
+    s.n = range_mode ? RT_CIE_N + RT_CIE_EXT_N : RT_CIE_N;
+    for (int i = 0; i < s.n; i++)
+        for (int k = 0; k < 3; k++)
+            s.xyz[i][k] = i < RT_CIE_N ? RT_CIE_XYZ[i][k] : RT_CIE_XYZ_EXT[i - RT_CIE_N][k];
+    float sum[3] = {0, 0, 0}, fsum[3] = {0, 0, 0};
+    for (int i = 0; i < s.n; i++) {                                                 // spectrum.rs:80-95
+        float rgb[3]; xyz_to_srgb_clamped(s.xyz[i][0], s.xyz[i][1], s.xyz[i][2], rgb);
+        sum[0] += rgb[0]; sum[1] += rgb[1]; sum[2] += rgb[2];
+        float c[3]; fire_color(s.xyz[i][0], s.xyz[i][1], s.xyz[i][2], c);           // spectrum.rs:162-177
+        fsum[0] += c[0]; fsum[1] += c[1]; fsum[2] += c[2];
+    }
+    for (int k = 0; k < 3; k++) {
+        s.norms[k] = (float)s.n / rmax(sum[k], 1e-6f);
+        s.fire_norms[k] = (float)s.n / rmax(fsum[k], 1e-6f);
+    }
+    s.lam_lo = 380.0f;
+    s.lam_range = range_mode ? 400.0f : 320.0f;
+}
+static inline void cmf_lerp(const Spectrum& s, float lambda, float xyz[3]) {       // spectrum.rs:105-110
+    float t = clampf((lambda - RT_CIE_START) / RT_CIE_STEP, 0.0f, (float)(s.n - 1));
+    int i = std::min((int)t, s.n - 2);
+    float frac = t - (float)i;
+    for (int k = 0; k < 3; k++) xyz[k] = s.xyz[i][k] + frac * (s.xyz[i + 1][k] - s.xyz[i][k]);
+}
+static inline V3 spectral_to_rgb(const Spectrum& s, float lambda) {               // spectrum.rs:104-114
+    float xyz[3]; cmf_lerp(s, lambda, xyz);
+    float rgb[3]; xyz_to_srgb_clamped(xyz[0], xyz[1], xyz[2], rgb);
+    return v3(rgb[0] * s.norms[0], rgb[1] * s.norms[1], rgb[2] * s.norms[2]);
+}
+static inline V3 spectral_fire_rgb(const Spectrum& s, float lambda) {             // spectrum.rs:183-193
+    float xyz[3]; cmf_lerp(s, lambda, xyz);
+    float c[3]; fire_color(xyz[0], xyz[1], xyz[2], c);
+    return v3(c[0] * s.fire_norms[0], c[1] * s.fire_norms[1], c[2] * s.fire_norms[2]);
+}
+static inline float planck_raw(float lambda_nm, float temp_k) {                    // spectrum.rs:204-208
+    const float HC_OVER_K = 14388000.0f;
+    float x = HC_OVER_K / (lambda_nm * temp_k);
+    float l2 = lambda_nm * lambda_nm, l4 = l2 * l2;
+    return 1.0f / (lambda_nm * l4 * rmax(std::exp(x) - 1.0f, 1e-30f));
+}
+static inline void metal_ior(const RtMaterial& m, float lambda, float* n, float* k) {   // spectrum.rs:227-233
+    const float* ns; const float* ks; int cnt; float start, step;
+    if (m.metal >= RT_METAL_GOLD && m.metal <= RT_METAL_SILVER) {
+        ns = RT_METAL_NK[m.metal][0]; ks = RT_METAL_NK[m.metal][1];
+        cnt = RT_METAL_NK_N; start = RT_METAL_NK_START; step = RT_METAL_NK_STEP;
+    } else {
+        ns = m.nk_n; ks = m.nk_k; cnt = m.nk_count; start = m.nk_start; step = m.nk_step;
+    }
+    float t = clampf((lambda - start) / step, 0.0f, (float)(cnt - 1));
+    int i = std::min((int)t, cnt - 2);
+    float f = t - (float)i;
+    *n = ns[i] + f * (ns[i + 1] - ns[i]);
+    *k = ks[i] + f * (ks[i + 1] - ks[i]);
+}
+static inline float fresnel_conductor(float cos_i, float n, float k) {             // spectrum.rs:247-262
+    float cos2 = cos_i * cos_i;
+    float sin2 = rmax(1.0f - cos2, 0.0f);
+    float n2 = n * n, k2 = k * k;
+    float t0 = n2 - k2 - sin2;
+    float a2pb2 = std::sqrt(t0 * t0 + 4.0f * n2 * k2);
+    float t1 = a2pb2 + cos2;
+    float a = std::sqrt(rmax(0.5f * (a2pb2 + t0), 0.0f));
+    float t2 = 2.0f * cos_i * a;
+    float rs = (t1 - t2) / rmax(t1 + t2, 1e-12f);
+    float t3 = cos2 * a2pb2 + sin2 * sin2;
+    float t4 = t2 * sin2;
+    float rp = rs * (t3 - t4) / rmax(t3 + t4, 1e-12f);
+    return clampf(0.5f * (rp + rs), 0.0f, 1.0f);
+}
+static inline float cauchy_ior(float lambda_nm, float b, float c) {                // spectrum.rs:274-277
+    float um = lambda_nm * 1e-3f;
+    return b + c / (um * um);
+}
+
+// ── material.rs helpers ──────────────────────────────────────────────────────
+static inline float fresnel_dielectric(float cos_i, float eta) {                   // material.rs:119-127
+    float sin2_i = rmax(1.0f - cos_i * cos_i, 0.0f);
+    float sin2_t = eta * eta * sin2_i;
+    if (sin2_t >= 1.0f) return 1.0f;
+    float cos_t = std::sqrt(1.0f - sin2_t);
+    float rs = (eta * cos_i - cos_t) / (eta * cos_i + cos_t);
+    float rp = (eta * cos_t - cos_i) / (eta * cos_t + cos_i);
+    return (rs * rs + rp * rp) * 0.5f;
+}
+static inline float smith_g1(float c, float alpha) {                               // material.rs:163-167
+    float a2 = alpha * alpha, c2 = c * c;
+    return 2.0f * c / (c + std::sqrt(a2 + (1.0f - a2) * c2));
+}
+static inline float smith_lambda(float c, float alpha) {                           // material.rs:179-183
+    float a2 = alpha * alpha, c2 = c * c;
+    return (std::sqrt(a2 + (1.0f - a2) * c2) - c) / (2.0f * c);
+}
+static inline float ggx_ndf(float cos_h, float alpha) {                            // material.rs:308-312
+    float a2 = alpha * alpha;
+    float d = 1.0f + cos_h * cos_h * (a2 - 1.0f);
+    return a2 / rmax(PI_F * d * d, 1e-12f);
+}
+static inline V3 vndf_sample(V3 wo, float ax, float ay, float xi1, float xi2) {   // material.rs:273-303
+    V3 wh = unit(v3(ax * wo.x, ay * wo.y, wo.z));
+    float len = std::sqrt(wh.x * wh.x + wh.y * wh.y);
+    V3 t1 = len > 1e-6f ? v3(-wh.y / len, wh.x / len, 0.0f) : v3(1, 0, 0);
+    V3 t2 = cross(wh, t1);
+    float a = 1.0f / (1.0f + wh.z);
+    float r = std::sqrt(xi1);
+    float p1, p2;
+    if (xi2 < a) {
+        float phi = xi2 / a * PI_F;
+        p1 = r * std::cos(phi); p2 = r * std::sin(phi);
+    } else {
+        float phi = PI_F + (xi2 - a) / (1.0f - a) * PI_F;
+        p1 = r * std::cos(phi); p2 = r * std::sin(phi) * wh.z;
+    }
+    float p3 = std::sqrt(rmax(1.0f - p1 * p1 - p2 * p2, 0.0f));
+    V3 nh = t1 * p1 + t2 * p2 + wh * p3;
+    return unit(v3(ax * nh.x, ay * nh.y, rmax(nh.z, 0.0f)));
+}
+
+// E_ss(mu, alpha) LUT (material.rs:206-241): 64×64 texels, 64×64 stratified
+// VNDF samples each.  Jitter comes from the counter hash (texel, sample) instead
+// of SmallRng; the estimator is the reference's.
+static const int E_N = 64;
+static float g_elut[E_N][E_N];
+static std::once_flag g_elut_once;
+static void build_e_lut() {
+    const int G = 64;
+    for (int i = 0; i < E_N; i++) {
+        float mu = ((float)i + 0.5f) / (float)E_N;
+        for (int j = 0; j < E_N; j++) {
+            float alpha = rmax(((float)j + 0.5f) / (float)E_N, 1e-3f);
+            V3 wo = v3(0.0f, 0.0f, mu);
+            float lam_o = smith_lambda(mu, alpha);
+            double sum = 0.0;
+            uint32_t texel = (uint32_t)(i * E_N + j);
+            for (int k = 0; k < G; k++) {
+                for (int l = 0; l < G; l++) {
+                    uint32_t smp = (uint32_t)(k * G + l);
+                    float r1 = (float)(pcg3d_x(texel, smp, 0xE55E0001u) >> 8) * (1.0f / 16777216.0f);
+                    float r2 = (float)(pcg3d_x(texel, smp, 0xE55E0002u) >> 8) * (1.0f / 16777216.0f);
+                    float xi1 = ((float)k + r1) / (float)G;
+                    float xi2 = ((float)l + r2) / (float)G;
+                    V3 m = vndf_sample(wo, alpha, alpha, xi1, xi2);
+                    float vo_h = rmax(dot(wo, m), 0.0f);
+                    V3 wi = 2.0f * vo_h * m - wo;
+                    if (wi.z <= 0.0f) continue;
+                    float lam_i = smith_lambda(wi.z, alpha);
+                    sum += (double)((1.0f + lam_o) / (1.0f + lam_o + lam_i));
+                }
+            }
+            g_elut[i][j] = (float)(sum / (double)(G * G));
+        }
+    }
+}
+static inline float e_ss_lut(float mu, float alpha) {                              // material.rs:246-260
+    std::call_once(g_elut_once, build_e_lut);
+    float x = clampf(clampf(mu, 0.0f, 1.0f) * (float)E_N - 0.5f, 0.0f, (float)(E_N - 1));
+    float y = clampf(clampf(alpha, 0.0f, 1.0f) * (float)E_N - 0.5f, 0.0f, (float)(E_N - 1));
+    int i0 = (int)x, j0 = (int)y;
+    int i1 = std::min(i0 + 1, E_N - 1), j1 = std::min(j0 + 1, E_N - 1);
+    float fx = x - (float)i0, fy = y - (float)j0;
+    float e00 = g_elut[i0][j0], e10 = g_elut[i1][j0], e01 = g_elut[i0][j1], e11 = g_elut[i1][j1];
+    return (e00 * (1.0f - fx) + e10 * fx) * (1.0f - fy) + (e01 * (1.0f - fx) + e11 * fx) * fy;
+}
+static inline float specular_energy_comp(float mu, float alpha) {                  // material.rs:265-267
+    return rmin(1.0f / rmax(e_ss_lut(mu, alpha), 0.05f), 10.0f);
+}
+
+// ── scene ────────────────────────────────────────────────────────────────────
+struct Aabb { V3 mn, mx; };
+static inline Aabb surrounding(const Aabb& a, const Aabb& b) {                     // aabb.rs:10-15
+    return Aabb{v3(rmin(a.mn.x, b.mn.x), rmin(a.mn.y, b.mn.y), rmin(a.mn.z, b.mn.z)),
+                v3(rmax(a.mx.x, b.mx.x), rmax(a.mx.y, b.mx.y), rmax(a.mx.z, b.mx.z))};
+}
+static inline Aabb pad(Aabb b) {                                                    // aabb.rs:18-29
+    const float D = 0.0001f;
+    float px = b.mx.x - b.mn.x < D ? D : 0.0f;
+    float py = b.mx.y - b.mn.y < D ? D : 0.0f;
+    float pz = b.mx.z - b.mn.z < D ? D : 0.0f;
+    return Aabb{v3(b.mn.x - px, b.mn.y - py, b.mn.z - pz), v3(b.mx.x + px, b.mx.y + py, b.mx.z + pz)};
+}
+static inline float surface_area(const Aabb& b) {                                  // bvh.rs:47-50
+    V3 d = b.mx - b.mn;
+    return 2.0f * (d.x * d.y + d.y * d.z + d.z * d.x);
+}
+
+struct Tri { V3 v0, e1, e2; V3 n0, n1, n2; bool has_n; int mat; };
+struct Quad { V3 q, u, v, normal, w; float d, area; int mat; };
+struct Sphere { V3 c; float r; int mat; };
+
+static const int W8 = 8;
+struct Node { float mn[3][W8], mx[3][W8]; int32_t ch[W8]; };
+
+struct EnvMap {
+    int w = 0, h = 0;
+    std::vector<float> img;           // h × w × 3
+    std::vector<float> marginal, cond;
+    float inv_total = 0.0f, rot_y = 0.0f, sin_r = 0.0f, cos_r = 1.0f;
+};
+
+struct Scene {
+    std::vector<Tri> tris;
+    std::vector<Quad> quads;
+    std::vector<Sphere> spheres;
+    std::vector<RtMaterial> mats;
+    std::vector<int32_t> lights;      // canonical prim ids of the NEE light copies
+    RtBackground bg;
+    EnvMap env;
+    bool has_env = false;
+    Spectrum spec;
+    // blackbody constants per material (material.rs:47-62)
+    std::vector<float> bb_norm;
+    std::vector<V3> bb_avg;
+    // BVH
+    std::vector<Node> nodes;
+    std::vector<int32_t> leaf_prims;  // leaf slot → canonical prim id
+    int64_t n_tris = 0, n_quads = 0, n_spheres = 0;
+};
+
+static inline int prim_type(const Scene& s, int64_t gid) {
+    return gid < s.n_tris ? RT_PRIM_TRI : (gid < s.n_tris + s.n_quads ? RT_PRIM_QUAD : RT_PRIM_SPHERE);
+}
+
+static Aabb prim_box(const Scene& s, int64_t gid) {
+    int t = prim_type(s, gid);
+    if (t == RT_PRIM_TRI) {                                                         // triangle.rs:128-140
+        const Tri& tr = s.tris[gid];
+        V3 a = tr.v0, b = tr.v0 + tr.e1, c = tr.v0 + tr.e2;
+        Aabb bb{v3(rmin(rmin(a.x, b.x), c.x), rmin(rmin(a.y, b.y), c.y), rmin(rmin(a.z, b.z), c.z)),
+                v3(rmax(rmax(a.x, b.x), c.x), rmax(rmax(a.y, b.y), c.y), rmax(rmax(a.z, b.z), c.z))};
+        return pad(bb);
+    } else if (t == RT_PRIM_QUAD) {                                                 // quad.rs:71-80
+        const Quad& q = s.quads[gid - s.n_tris];
+        V3 c[4] = {q.q, q.q + q.u, q.q + q.v, q.q + q.u + q.v};
+        V3 mn = c[0], mx = c[0];
+        for (int i = 1; i < 4; i++) {
+            mn = v3(rmin(mn.x, c[i].x), rmin(mn.y, c[i].y), rmin(mn.z, c[i].z));
+            mx = v3(rmax(mx.x, c[i].x), rmax(mx.y, c[i].y), rmax(mx.z, c[i].z));
+        }
+        return pad(Aabb{mn, mx});
+    } else {                                                                        // sphere.rs:111-118
+        const Sphere& sp = s.spheres[gid - s.n_tris - s.n_quads];
+        V3 r = v3(sp.r, sp.r, sp.r);
+        return Aabb{sp.c - r, sp.c + r};
+    }
+}
+
+// ── BVH build (bvh.rs:52-225) ────────────────────────────────────────────────
+static const int NUM_BUCKETS = 12;
+
+struct Builder {
+    const std::vector<Aabb>* boxes;
+    std::vector<Node>* nodes;
+    std::vector<int32_t>* leaf_prims;
+};
+
+// sah_partition (bvh.rs:52-145) on the index list `objs`; returns the split point
+// after reordering objs into (left, right) by a stable sort on bucket id.
+static size_t sah_partition(const std::vector<Aabb>& boxes, std::vector<int32_t>& objs) {
+    size_t span = objs.size();
+    float c_min[3] = {INFINITY, INFINITY, INFINITY}, c_max[3] = {-INFINITY, -INFINITY, -INFINITY};
+    Aabb node_bbox = boxes[objs[0]];
+    for (size_t k = 0; k < span; k++) {
+        const Aabb& b = boxes[objs[k]];
+        for (int a = 0; a < 3; a++) {
+            float c = (comp(b.mn, a) + comp(b.mx, a)) * 0.5f;
+            c_min[a] = rmin(c_min[a], c);
+            c_max[a] = rmax(c_max[a], c);
+        }
+        if (k > 0) node_bbox = surrounding(node_bbox, b);
+    }
+    float node_sa = surface_area(node_bbox);
+    float best_cost = INFINITY;
+    int best_axis = 0, best_split = 0;
+    for (int axis = 0; axis < 3; axis++) {
+        float extent = c_max[axis] - c_min[axis];
+        if (extent < 1e-6f) continue;
+        bool has[NUM_BUCKETS] = {};
+        Aabb bb[NUM_BUCKETS];
+        uint32_t cnt[NUM_BUCKETS] = {};
+        for (size_t k = 0; k < span; k++) {
+            const Aabb& b = boxes[objs[k]];
+            float c = (comp(b.mn, axis) + comp(b.mx, axis)) * 0.5f;
+            float t = (c - c_min[axis]) / extent;
+            int bi = std::min((int)((float)NUM_BUCKETS * t), NUM_BUCKETS - 1);
+            cnt[bi]++;
+            bb[bi] = has[bi] ? surrounding(bb[bi], b) : b;
+            has[bi] = true;
+        }
+        float left_sa[NUM_BUCKETS]; uint32_t left_n[NUM_BUCKETS];
+        bool acc_has = false; Aabb acc; uint32_t acc_n = 0;
+        for (int i = 0; i < NUM_BUCKETS; i++) {
+            acc_n += cnt[i];
+            if (has[i]) { acc = acc_has ? surrounding(acc, bb[i]) : bb[i]; acc_has = true; }
+            left_n[i] = acc_n;
+            left_sa[i] = acc_has ? surface_area(acc) : 0.0f;
+        }
+        acc_has = false; acc_n = 0;
+        for (int split = NUM_BUCKETS - 2; split >= 0; split--) {
+            acc_n += cnt[split + 1];
+            if (has[split + 1]) { acc = acc_has ? surrounding(acc, bb[split + 1]) : bb[split + 1]; acc_has = true; }
+            uint32_t nl = left_n[split], nr = acc_n;
+            if (nl == 0 || nr == 0) continue;
+            float right_sa = acc_has ? surface_area(acc) : 0.0f;
+            float cost = 1.0f + (left_sa[split] * (float)nl + right_sa * (float)nr) / node_sa;
+            if (cost < best_cost) { best_cost = cost; best_axis = axis; best_split = split; }
+        }
+    }
+    float extent = c_max[best_axis] - c_min[best_axis];
+    // stable counting sort by bucket id == order.sort_by_key(bid) (a stable sort)
+    std::vector<int32_t> bucketed[NUM_BUCKETS];
+    for (size_t k = 0; k < span; k++) {
+        int bi = 0;
+        if (!(extent < 1e-6f)) {
+            const Aabb& b = boxes[objs[k]];
+            float c = (comp(b.mn, best_axis) + comp(b.mx, best_axis)) * 0.5f;
+            float t = (c - c_min[best_axis]) / extent;
+            bi = std::min((int)((float)NUM_BUCKETS * t), NUM_BUCKETS - 1);
+        }
+        bucketed[bi].push_back(objs[k]);
+    }
+    size_t pos = 0, mid_off = 0;
+    for (int bkt = 0; bkt < NUM_BUCKETS; bkt++) {
+        for (int32_t o : bucketed[bkt]) objs[pos++] = o;
+        if (bkt == best_split) mid_off = pos;
+    }
+    return (mid_off == 0 || mid_off == span) ? span / 2 : mid_off;
+}
+
+static void split_recursive(const std::vector<Aabb>& boxes, std::vector<int32_t> objs, int depth,
+                            std::vector<std::vector<int32_t>>& out) {              // bvh.rs:148-162
+    if (depth == 3 || objs.size() <= 1) { out.push_back(std::move(objs)); return; }
+    size_t mid = sah_partition(boxes, objs);
+    std::vector<int32_t> l(objs.begin(), objs.begin() + mid), r(objs.begin() + mid, objs.end());
+    split_recursive(boxes, std::move(l), depth + 1, out);
+    split_recursive(boxes, std::move(r), depth + 1, out);
+}
+
+static int32_t build_rec(Builder& B, const std::vector<int32_t>& objs, Aabb* out_box) {   // bvh.rs:290-323
+    const std::vector<Aabb>& boxes = *B.boxes;
+    if (objs.size() == 1) {
+        int32_t idx = (int32_t)B.leaf_prims->size();
+        B.leaf_prims->push_back(objs[0]);
+        *out_box = boxes[objs[0]];
+        return -(idx + 1);
+    }
+    std::vector<std::vector<int32_t>> groups;
+    if (objs.size() <= (size_t)W8) {                                                // split_n, bvh.rs:165-174
+        for (int32_t o : objs) groups.push_back(std::vector<int32_t>{o});
+    } else {
+        split_recursive(boxes, objs, 0, groups);
+    }
+    size_t my = B.nodes->size();
+    Node sentinel;
+    memset(&sentinel, 0, sizeof(sentinel));
+    for (int c = 0; c < W8; c++) sentinel.ch[c] = INT32_MIN;
+    B.nodes->push_back(sentinel);
+    Node node = sentinel;
+    Aabb nb{};
+    for (size_t i = 0; i < groups.size(); i++) {
+        Aabb cb;
+        int32_t child = build_rec(B, groups[i], &cb);
+        node.ch[i] = child;
+        for (int a = 0; a < 3; a++) { node.mn[a][i] = comp(cb.mn, a); node.mx[a][i] = comp(cb.mx, a); }
+        nb = i == 0 ? cb : surrounding(nb, cb);
+    }
+    (*B.nodes)[my] = node;
+    *out_box = nb;
+    return (int32_t)my;
+}
+
+static void build_bvh(Scene& s) {                                                   // bvh.rs:199-225
+    int64_t n = s.n_tris + s.n_quads + s.n_spheres;
+    s.nodes.clear(); s.leaf_prims.clear();
+    if (n == 0) return;
+    std::vector<Aabb> boxes(n);
+    for (int64_t i = 0; i < n; i++) boxes[i] = prim_box(s, i);
+    std::vector<int32_t> objs(n);
+    for (int64_t i = 0; i < n; i++) objs[i] = (int32_t)i;
+    s.nodes.reserve(n / 4 + 1);
+    Builder B{&boxes, &s.nodes, &s.leaf_prims};
+    Aabb root_box;
+    int32_t root = build_rec(B, objs, &root_box);
+    if (root < 0) {
+        Node nd;
+        memset(&nd, 0, sizeof(nd));
+        for (int c = 0; c < W8; c++) nd.ch[c] = INT32_MIN;
+        nd.ch[0] = root;
+        for (int a = 0; a < 3; a++) { nd.mn[a][0] = comp(boxes[0].mn, a); nd.mx[a][0] = comp(boxes[0].mx, a); }
+        s.nodes.push_back(nd);
+    }
+}
+
+// ── primitive tests ──────────────────────────────────────────────────────────
+struct Ray { V3 o, d; };
+
+// triangle.rs:75-89 (hit) — returns t, barycentrics
+static inline bool tri_hit(const Tri& tr, const Ray& r, float tmin, float tmax, float* t_out, float* b1o, float* b2o) {
+    V3 h = cross(r.d, tr.e2);
+    float a = dot(tr.e1, h);
+    if (std::fabs(a) < 1e-8f) return false;
+    float f = 1.0f / a;
+    V3 s = r.o - tr.v0;
+    float b1 = f * dot(s, h);
+    if (!(b1 >= 0.0f && b1 <= 1.0f)) return false;
+    V3 q = cross(s, tr.e1);
+    float b2 = f * dot(r.d, q);
+    if (b2 < 0.0f || b1 + b2 > 1.0f) return false;
+    float t = f * dot(tr.e2, q);
+    if (t < tmin || t > tmax) return false;
+    *t_out = t; *b1o = b1; *b2o = b2;
+    return true;
+}
+// quad.rs:37-57
+static inline bool quad_hit(const Quad& q, const Ray& r, float tmin, float tmax, float* t_out, float* al, float* be) {
+    float denom = dot(q.normal, r.d);
+    if (!(std::fabs(denom) >= 1e-8f)) return false;
+    float t = (q.d - dot(q.normal, r.o)) / denom;
+    if (t < tmin || t > tmax) return false;
+    V3 p = r.o + t * r.d;
+    V3 planar = p - q.q;
+    float alpha = dot(q.w, cross(planar, q.v));
+    float beta = dot(q.w, cross(q.u, planar));
+    if (!(alpha >= 0.0f && alpha <= 1.0f) || !(beta >= 0.0f && beta <= 1.0f)) return false;
+    *t_out = t; *al = alpha; *be = beta;
+    return true;
+}
+// sphere.rs:47-61
+static inline bool sphere_hit(const Sphere& sp, const Ray& r, float tmin, float tmax, float* t_out) {
+    V3 oc = r.o - sp.c;
+    float a = len2(r.d);
+    if (!(a > 0.0f)) return false;
+    float half_b = dot(oc, r.d);
+    float c = len2(oc) - sp.r * sp.r;
+    float disc = half_b * half_b - a * c;
+    if (disc < 0.0f) return false;
+    float sq = std::sqrt(disc);
+    float root = (-half_b - sq) / a;
+    if (root < tmin || root > tmax) {
+        root = (-half_b + sq) / a;
+        if (root < tmin || root > tmax) return false;
+    }
+    *t_out = root;
+    return true;
+}
+static inline bool prim_hit(const Scene& s, int64_t gid, const Ray& r, float tmin, float tmax,
+                            float* t, float* b1, float* b2) {
+    if (gid < s.n_tris) return tri_hit(s.tris[gid], r, tmin, tmax, t, b1, b2);
+    if (gid < s.n_tris + s.n_quads) return quad_hit(s.quads[gid - s.n_tris], r, tmin, tmax, t, b1, b2);
+    *b1 = 0.0f; *b2 = 0.0f;
+    return sphere_hit(s.spheres[gid - s.n_tris - s.n_quads], r, tmin, tmax, t);
+}
+
+// ── traversal (bvh.rs:229-288, slab test :326-364) ───────────────────────────
+static const float SLAB_WIDEN = 1.52587890625e-05f;   // 2^-16
+
+// Reciprocal direction for the slab test.  A zero (or denormal) component gives
+// ±inf and, for a ray lying exactly in a box face plane, (bound − o)·inv = 0·∞
+// = NaN; that slab is then taken as the whole line (the ray is inside the
+// closed slab), so culling stays conservative (the AVX2 path of the reference,
+// bvh.rs:326-364, drops such boxes — bvh.rs:450-456 documents the asymmetry).
+static inline float safe_inv(float d) { return 1.0f / d; }
+
+struct TraceStats { int64_t nodes = 0, tris = 0, quads = 0, spheres = 0; };
+
+// 8-wide AVX2 slab test; returns the hit mask and t_near per child.
+static inline uint32_t slab8(const Node& nd, const float ro[3], const float id[3], float tmin, float tmax, float tnear[8]) {
+    __m256i ch = _mm256_loadu_si256((const __m256i*)nd.ch);
+    __m256i sent = _mm256_set1_epi32(INT32_MIN);
+    uint32_t invalid = (uint32_t)_mm256_movemask_ps(_mm256_castsi256_ps(_mm256_cmpeq_epi32(ch, sent)));
+    __m256 t0 = _mm256_set1_ps(tmin), t1 = _mm256_set1_ps(tmax);
+    const __m256 ninf = _mm256_set1_ps(-INFINITY), pinf = _mm256_set1_ps(INFINITY);
+    for (int a = 0; a < 3; a++) {
+        __m256 o = _mm256_set1_ps(ro[a]), iv = _mm256_set1_ps(id[a]);
+        __m256 da = _mm256_mul_ps(_mm256_sub_ps(_mm256_loadu_ps(nd.mn[a]), o), iv);
+        __m256 db = _mm256_mul_ps(_mm256_sub_ps(_mm256_loadu_ps(nd.mx[a]), o), iv);
+        __m256 nan = _mm256_cmp_ps(da, db, _CMP_UNORD_Q);
+        __m256 lo = _mm256_blendv_ps(_mm256_min_ps(da, db), ninf, nan);
+        __m256 hi = _mm256_blendv_ps(_mm256_max_ps(da, db), pinf, nan);
+        t0 = _mm256_max_ps(t0, lo);
+        t1 = _mm256_min_ps(t1, hi);
+    }
+    // widened exit: t1 + |t1|·2^-16 (conservative culling)
+    __m256 absmask = _mm256_castsi256_ps(_mm256_set1_epi32(0x7fffffff));
+    __m256 t1w = _mm256_add_ps(t1, _mm256_mul_ps(_mm256_and_ps(t1, absmask), _mm256_set1_ps(SLAB_WIDEN)));
+    uint32_t mask = (uint32_t)_mm256_movemask_ps(_mm256_cmp_ps(t0, t1w, _CMP_LE_OQ));
+    _mm256_storeu_ps(tnear, t0);
+    return mask & (~invalid) & 0xffu;
+}
+
+struct HitRes { int32_t gid; float t, b1, b2; };
+
+// A ray with a NaN coordinate or bound hits nothing (the reference would let a
+// NaN sphere root through its range check, sphere.rs:57-61).
+static inline bool ray_has_nan(const Ray& r, float tmin, float tmax) {
+    return std::isnan(r.o.x) || std::isnan(r.o.y) || std::isnan(r.o.z) || std::isnan(r.d.x) || std::isnan(r.d.y) ||
+           std::isnan(r.d.z) || std::isnan(tmin) || std::isnan(tmax);
+}
+
+template <bool STATS>
+static HitRes closest_hit(const Scene& s, const Ray& r, float tmin, float tmax, TraceStats* st) {
+    HitRes best{-1, tmax, 0.0f, 0.0f};
+    if (s.nodes.empty() || ray_has_nan(r, tmin, tmax)) return best;
+    int32_t stack[128];
+    std::vector<int32_t> overflow;
+    int top = 0;
+    stack[top++] = 0;
+    float ro[3] = {r.o.x, r.o.y, r.o.z};
+    float id[3] = {safe_inv(r.d.x), safe_inv(r.d.y), safe_inv(r.d.z)};
+    float closest = tmax;
+    while (top > 0 || !overflow.empty()) {
+        int32_t e;
+        if (top > 0) e = stack[--top]; else { e = overflow.back(); overflow.pop_back(); }
+        if (e < 0) {
+            int32_t gid = s.leaf_prims[-e - 1];
+            if (STATS) {
+                int t = prim_type(s, gid);
+                if (t == RT_PRIM_TRI) st->tris++; else if (t == RT_PRIM_QUAD) st->quads++; else st->spheres++;
+            }
+            float t, b1, b2;
+            if (prim_hit(s, gid, r, tmin, closest, &t, &b1, &b2)) {
+                if (t < closest || best.gid < 0 || gid < best.gid) {
+                    closest = t;
+                    best = HitRes{gid, t, b1, b2};
+                }
+            }
+            continue;
+        }
+        const Node& nd = s.nodes[e];
+        if (STATS) st->nodes++;
+        float tn[8];
+        uint32_t mask = slab8(nd, ro, id, tmin, closest, tn);
+        if (!mask) continue;
+        float ht[8]; int32_t hc[8]; int n = 0;
+        for (int c = 0; c < 8; c++) if (mask & (1u << c)) { ht[n] = tn[c]; hc[n] = nd.ch[c]; n++; }
+        // sort far-to-near so the nearest is popped first (bvh.rs:271-284)
+        for (int i = 1; i < n; i++) {
+            float tv = ht[i]; int32_t cv = hc[i]; int j = i - 1;
+            while (j >= 0 && ht[j] < tv) { ht[j + 1] = ht[j]; hc[j + 1] = hc[j]; j--; }
+            ht[j + 1] = tv; hc[j + 1] = cv;
+        }
+        for (int i = 0; i < n; i++) {
+            if (top < 128) stack[top++] = hc[i]; else overflow.push_back(hc[i]);
+        }
+    }
+    return best;
+}
+
+static HitRes closest_hit_brute(const Scene& s, const Ray& r, float tmin, float tmax) {
+    HitRes best{-1, tmax, 0.0f, 0.0f};
+    if (ray_has_nan(r, tmin, tmax)) return best;
+    int64_t n = s.n_tris + s.n_quads + s.n_spheres;
+    float closest = tmax;
+    for (int64_t g = 0; g < n; g++) {
+        float t, b1, b2;
+        if (prim_hit(s, g, r, tmin, closest, &t, &b1, &b2)) {
+            if (t < closest || best.gid < 0) { closest = t; best = HitRes{(int32_t)g, t, b1, b2}; }
+        }
+    }
+    return best;
+}
+
+// any_hit / opaque transmittance (bvh.rs:487-575)
+static bool any_hit(const Scene& s, const Ray& r, float tmin, float tmax) {
+    if (s.nodes.empty() || ray_has_nan(r, tmin, tmax)) return false;
+    int32_t stack[128];
+    std::vector<int32_t> overflow;
+    int top = 0;
+    stack[top++] = 0;
+    float ro[3] = {r.o.x, r.o.y, r.o.z};
+    float id[3] = {safe_inv(r.d.x), safe_inv(r.d.y), safe_inv(r.d.z)};
+    while (top > 0 || !overflow.empty()) {
+        int32_t e;
+        if (top > 0) e = stack[--top]; else { e = overflow.back(); overflow.pop_back(); }
+        if (e < 0) {
+            float t, b1, b2;
+            if (prim_hit(s, s.leaf_prims[-e - 1], r, tmin, tmax, &t, &b1, &b2)) return true;
+            continue;
+        }
+        float tn[8];
+        uint32_t mask = slab8(s.nodes[e], ro, id, tmin, tmax, tn);
+        for (int c = 0; c < 8; c++)
+            if (mask & (1u << c)) { if (top < 128) stack[top++] = s.nodes[e].ch[c]; else overflow.push_back(s.nodes[e].ch[c]); }
+    }
+    return false;
+}
+
+// ── hit record (hittable.rs:73-94) ───────────────────────────────────────────
+struct Rec { V3 p, normal; float t, u, v; bool front; int mat; int32_t gid; };
+
+static inline V3 sphere_uv_calc(V3 p, float* u, float* v) {                         // sphere.rs:11-15
+    float theta = std::acos(clampf(-p.y, -1.0f, 1.0f));
+    float phi = std::atan2(-p.z, p.x) + PI_F;
+    *u = phi / (2.0f * PI_F); *v = theta / PI_F;
+    return p;
+}
+
+static Rec make_rec(const Scene& s, const Ray& r, const HitRes& h) {
+    Rec rec;
+    rec.gid = h.gid; rec.t = h.t;
+    rec.p = r.o + h.t * r.d;
+    V3 outward;
+    int t = prim_type(s, h.gid);
+    if (t == RT_PRIM_TRI) {                                                         // triangle.rs:91-108
+        const Tri& tr = s.tris[h.gid];
+        float b0 = 1.0f - h.b1 - h.b2;
+        if (tr.has_n) {
+            V3 sn = b0 * tr.n0 + h.b1 * tr.n1 + h.b2 * tr.n2;
+            outward = len2(sn) > 1e-12f ? unit(sn) : unit(cross(tr.e1, tr.e2));
+        } else {
+            outward = unit(cross(tr.e1, tr.e2));
+        }
+        rec.u = h.b1; rec.v = h.b2;   // no UVs in the flat description: barycentrics
+        rec.mat = tr.mat;
+    } else if (t == RT_PRIM_QUAD) {
+        const Quad& q = s.quads[h.gid - s.n_tris];
+        outward = q.normal;
+        rec.u = h.b1; rec.v = h.b2;
+        rec.mat = q.mat;
+    } else {
+        const Sphere& sp = s.spheres[h.gid - s.n_tris - s.n_quads];
+        outward = (rec.p - sp.c) / sp.r;
+        sphere_uv_calc(outward, &rec.u, &rec.v);
+        rec.mat = sp.mat;
+    }
+    rec.front = dot(r.d, outward) < 0.0f;
+    rec.normal = rec.front ? outward : -outward;
+    return rec;
+}
+
+// ── light list (hittable.rs:156-225, quad.rs:82-96, sphere.rs:87-109) ───────
+static bool light_hit(const Scene& s, int32_t gid, const Ray& r, float tmin, float tmax, Rec* rec) {
+    float t, b1, b2;
+    if (!prim_hit(s, gid, r, tmin, tmax, &t, &b1, &b2)) return false;
+    *rec = make_rec(s, r, HitRes{gid, t, b1, b2});
+    return true;
+}
+static bool lights_hit(const Scene& s, const Ray& r, float tmin, float tmax, Rec* out) {
+    float closest = tmax; bool any = false;
+    for (int32_t g : s.lights) {
+        Rec rec;
+        if (light_hit(s, g, r, tmin, closest, &rec)) { closest = rec.t; *out = rec; any = true; }
+    }
+    return any;
+}
+static float prim_pdf_value(const Scene& s, int32_t gid, V3 origin, V3 dir) {
+    int t = prim_type(s, gid);
+    if (t == RT_PRIM_SPHERE) {
+        const Sphere& sp = s.spheres[gid - s.n_tris - s.n_quads];
+        V3 tc = sp.c - origin;
+        float d2 = len2(tc), r2 = sp.r * sp.r;
+        if (d2 <= r2) return 0.0f;
+        float ctm = std::sqrt(1.0f - r2 / d2);
+        return 1.0f / (2.0f * PI_F * (1.0f - ctm));
+    }
+    Ray r{origin, dir};
+    Rec rec;
+    if (!light_hit(s, gid, r, 0.001f, INFINITY, &rec)) return 0.0f;
+    float dist2 = len2(rec.p - origin);
+    float cos_t = std::fabs(dot(unit(dir), rec.normal));
+    if (t == RT_PRIM_QUAD) {
+        if (cos_t < 1e-8f) return 0.0f;
+        return dist2 / (cos_t * s.quads[gid - s.n_tris].area);
+    }
+    const Tri& tr = s.tris[gid];
+    float area = 0.5f * length(cross(tr.e1, tr.e2));
+    if (cos_t < 1e-8f || area <= 0.0f) return 0.0f;
+    return dist2 / (cos_t * area);
+}
+static float lights_pdf_value(const Scene& s, V3 origin, V3 dir) {
+    if (s.lights.empty()) return 0.0f;
+    float w = 1.0f / (float)s.lights.size();
+    float sum = 0.0f;
+    for (int32_t g : s.lights) sum += w * prim_pdf_value(s, g, origin, dir);
+    return sum;
+}
+static V3 prim_pdf_generate(const Scene& s, int32_t gid, V3 origin, float r1, float r2) {
+    int t = prim_type(s, gid);
+    if (t == RT_PRIM_QUAD) {
+        const Quad& q = s.quads[gid - s.n_tris];
+        V3 point = q.q + r1 * q.u + r2 * q.v;
+        return unit(point - origin);
+    }
+    if (t == RT_PRIM_TRI) {
+        const Tri& tr = s.tris[gid];
+        if (r1 + r2 > 1.0f) { r1 = 1.0f - r1; r2 = 1.0f - r2; }
+        V3 p = tr.v0 + r1 * tr.e1 + r2 * tr.e2;
+        return unit(p - origin);
+    }
+    const Sphere& sp = s.spheres[gid - s.n_tris - s.n_quads];
+    V3 tc = sp.c - origin;
+    float d2 = len2(tc), rr = sp.r * sp.r;
+    if (d2 <= rr) return unit(tc);
+    float ctm = std::sqrt(1.0f - rr / d2);
+    float phi = 2.0f * PI_F * r1;
+    float ct = 1.0f - r2 * (1.0f - ctm);
+    float st = std::sqrt(rmax(1.0f - ct * ct, 0.0f));
+    return onb_local(onb_from_w(unit(tc)), v3(std::cos(phi) * st, std::sin(phi) * st, ct));
+}
+
+// ── environment map (renderer.rs:23-180) ─────────────────────────────────────
+static void env_build(EnvMap& e, const RtBackground& bg) {
+    e.w = bg.env_w; e.h = bg.env_h;
+    size_t n = (size_t)e.w * e.h;
+    e.img.assign(bg.env_rgb, bg.env_rgb + n * 3);
+    e.cond.assign(n, 0.0f);
+    e.marginal.assign(e.h, 0.0f);
+    std::vector<float> row_w(e.h, 0.0f);
+    for (int j = 0; j < e.h; j++) {
+        float sin_j = std::sin(PI_F * ((float)j + 0.5f) / (float)e.h);
+        float sum = 0.0f;
+        for (int i = 0; i < e.w; i++) {
+            const float* px = &e.img[((size_t)j * e.w + i) * 3];
+            sum += luminance(v3(px[0], px[1], px[2])) * sin_j;
+            e.cond[(size_t)j * e.w + i] = sum;
+        }
+        if (sum > 0.0f) { for (int i = 0; i < e.w; i++) e.cond[(size_t)j * e.w + i] /= sum; }
+        else { for (int i = 0; i < e.w; i++) e.cond[(size_t)j * e.w + i] = (float)(i + 1) / (float)e.w; }
+        row_w[j] = sum;
+    }
+    float total = 0.0f;
+    for (int j = 0; j < e.h; j++) total += row_w[j];
+    float cum = 0.0f;
+    for (int j = 0; j < e.h; j++) {
+        cum += row_w[j];
+        e.marginal[j] = total > 0.0f ? cum / total : (float)(j + 1) / (float)e.h;
+    }
+    e.inv_total = total > 0.0f ? 1.0f / total : 0.0f;
+    e.rot_y = bg.env_rot_y_deg * (PI_F / 180.0f);
+    e.sin_r = std::sin(e.rot_y); e.cos_r = std::cos(e.rot_y);
+}
+static inline V3 env_rot(const EnvMap& e, V3 d) { return v3(d.x * e.cos_r + d.z * e.sin_r, d.y, -d.x * e.sin_r + d.z * e.cos_r); }
+static inline V3 env_unrot(const EnvMap& e, V3 d) { return v3(d.x * e.cos_r - d.z * e.sin_r, d.y, d.x * e.sin_r + d.z * e.cos_r); }
+static inline float rem_euclid1(float a) { float r = std::fmod(a, 1.0f); return r < 0.0f ? r + 1.0f : r; }
+static inline int rem_euclid_i(int a, int m) { int r = a % m; return r < 0 ? r + m : r; }
+static V3 env_sample(const EnvMap& e, V3 dir) {                                    // renderer.rs:97-121
+    V3 d = env_unrot(e, unit(dir));
+    float u = rem_euclid1(0.5f + std::atan2(d.x, d.z) / (2.0f * PI_F));
+    float v = std::acos(clampf(d.y, -1.0f, 1.0f)) / PI_F;
+    float x = u * (float)e.w - 0.5f, y = v * (float)e.h - 0.5f;
+    int x0 = (int)std::floor(x), y0 = (int)std::floor(y);
+    float fx = x - (float)x0, fy = y - (float)y0;
+    auto get = [&](int ix, int iy) {
+        int xx = rem_euclid_i(ix, e.w), yy = std::min(std::max(iy, 0), e.h - 1);
+        const float* p = &e.img[((size_t)yy * e.w + xx) * 3];
+        return v3(p[0], p[1], p[2]);
+    };
+    V3 c00 = get(x0, y0), c10 = get(x0 + 1, y0), c01 = get(x0, y0 + 1), c11 = get(x0 + 1, y0 + 1);
+    return (c00 * (1.0f - fx) + c10 * fx) * (1.0f - fy) + (c01 * (1.0f - fx) + c11 * fx) * fy;
+}
+static float env_pdf_at(const EnvMap& e, int i, int j) {                            // renderer.rs:169-179
+    const float* p = &e.img[((size_t)j * e.w + i) * 3];
+    float lum = luminance(v3(p[0], p[1], p[2]));
+    return lum * (float)((size_t)e.w * e.h) * e.inv_total / (2.0f * PI_F * PI_F);
+}
+static float env_dir_pdf(const EnvMap& e, V3 dir) {                                  // renderer.rs:157-167
+    V3 d = env_unrot(e, unit(dir));
+    float u = rem_euclid1(0.5f + std::atan2(d.x, d.z) / (2.0f * PI_F));
+    float v = std::acos(clampf(d.y, -1.0f, 1.0f)) / PI_F;
+    int i = std::min((int)(u * (float)e.w), e.w - 1);
+    int j = std::min((int)(v * (float)e.h), e.h - 1);
+    i = std::max(i, 0);
+    j = std::max(j, 0);
+    return env_pdf_at(e, i, j);
+}
+static V3 env_sample_dir(const EnvMap& e, float x1, float x2, float x3, float x4, float* pdf) {   // renderer.rs:126-154
+    int j = (int)(std::lower_bound(e.marginal.begin(), e.marginal.end(), x1) - e.marginal.begin());
+    j = std::min(j, e.h - 1);
+    const float* row = &e.cond[(size_t)j * e.w];
+    int i = (int)(std::lower_bound(row, row + e.w, x2) - row);
+    i = std::min(i, e.w - 1);
+    float u = ((float)i + x3) / (float)e.w;
+    float v = ((float)j + x4) / (float)e.h;
+    float phi = 2.0f * PI_F * (u - 0.5f);
+    float theta = PI_F * v;
+    float st = std::sin(theta);
+    V3 dir = env_rot(e, v3(st * std::sin(phi), std::cos(theta), st * std::cos(phi)));
+    *pdf = env_pdf_at(e, i, j);
+    return dir;
+}
+static V3 bg_eval_type(int type, const float* color, const float* top, const float* bottom, V3 dir) {
+    if (type == RT_BG_SOLID) return v3(color[0], color[1], color[2]);
+    float t = (clampf(dir.y, -1.0f, 1.0f) + 1.0f) * 0.5f;                           // renderer.rs:200-203
+    return v3(bottom[0], bottom[1], bottom[2]) * (1.0f - t) + v3(top[0], top[1], top[2]) * t;
+}
+static V3 bg_eval(const Scene& s, V3 dir) {                                          // renderer.rs:197-208
+    const RtBackground& b = s.bg;
+    if (b.type == RT_BG_ENVMAP) {
+        if (b.visible_type >= 0) return bg_eval_type(b.visible_type, b.visible_color, b.visible_top, b.visible_bottom, dir);
+        return env_sample(s.env, dir);
+    }
+    return bg_eval_type(b.type, b.color, b.top, b.bottom, dir);
+}
+static V3 env_eval(const Scene& s, V3 dir) { return s.has_env ? env_sample(s.env, dir) : v3(0, 0, 0); }
+static float env_pdf_value(const Scene& s, V3 dir) { return s.has_env ? env_dir_pdf(s.env, dir) : 0.0f; }
+
+// ── hero-wavelength state ────────────────────────────────────────────────────
+// The reference path carries an RGB throughput that, after the first spectral
+// event, includes the CMF tint of its single wavelength (material.rs:384-400,
+// :491-497).  Here throughput T holds every achromatic/RGB factor and each of
+// H wavelengths λ_i carries a scalar weight w_i; the path's effective RGB
+// throughput is T ⊙ (1/H) Σ_i w_i · tint(λ_i), tint = (1,1,1) before the first
+// spectral event, spectral_to_rgb (metal) or spectral_fire_rgb (dispersive
+// refraction) after it.  H = 1 is the reference exactly.
+enum { TINT_NONE = 0, TINT_CMF = 1, TINT_FIRE = 2 };
+struct SpecState { int H; float lam[4]; float w[4]; int tint; };
+static inline V3 tint_rgb(const Spectrum& sp, int tint, float lam) {
+    return tint == TINT_CMF ? spectral_to_rgb(sp, lam) : spectral_fire_rgb(sp, lam);
+}
+static V3 spec_factor(const Spectrum& sp, const SpecState& ss) {
+    if (ss.tint == TINT_NONE) {
+        float m = 0.0f;
+        for (int i = 0; i < ss.H; i++) m += ss.w[i];
+        float v = m / (float)ss.H;
+        return v3(v, v, v);
+    }
+    V3 acc = v3(0, 0, 0);
+    for (int i = 0; i < ss.H; i++) if (ss.w[i] != 0.0f) acc = acc + tint_rgb(sp, ss.tint, ss.lam[i]) * ss.w[i];
+    return acc / (float)ss.H;
+}
+// emitted_at (material.rs:64-81) folded with the spectral factor
+static V3 emission(const Scene& s, int mat, const SpecState& ss) {
+    const RtMaterial& m = s.mats[mat];
+    if (m.type == RT_MAT_DIFFUSE_LIGHT) return v3(m.albedo[0], m.albedo[1], m.albedo[2]) * spec_factor(s.spec, ss);
+    if (m.type == RT_MAT_BLACKBODY_LIGHT) {
+        if (ss.tint == TINT_NONE) return s.bb_avg[mat] * spec_factor(s.spec, ss);
+        V3 acc = v3(0, 0, 0);
+        for (int i = 0; i < ss.H; i++) {
+            if (ss.w[i] == 0.0f) continue;
+            float sc = planck_raw(ss.lam[i], m.temp_k) * s.bb_norm[mat] * m.intensity;
+            acc = acc + tint_rgb(s.spec, ss.tint, ss.lam[i]) * (ss.w[i] * sc);
+        }
+        return acc / (float)ss.H;
+    }
+    return v3(0, 0, 0);
+}
+static inline bool is_emissive_mat(const RtMaterial& m) {
+    return m.type == RT_MAT_DIFFUSE_LIGHT || m.type == RT_MAT_BLACKBODY_LIGHT;
+}
+static inline V3 lambert_albedo(const RtMaterial& m, V3 p) {                        // texture.rs:28-37
+    if (m.type == RT_MAT_CHECKER) {
+        int x = (int)std::floor(m.checker_scale * p.x);
+        int y = (int)std::floor(m.checker_scale * p.y);
+        int z = (int)std::floor(m.checker_scale * p.z);
+        if ((x + y + z) % 2 == 0) return v3(m.albedo[0], m.albedo[1], m.albedo[2]);
+        return v3(m.odd[0], m.odd[1], m.odd[2]);
+    }
+    return v3(m.albedo[0], m.albedo[1], m.albedo[2]);
+}
+
+// ── ray_color (renderer.rs:371-585) ──────────────────────────────────────────
+struct PassCtx {
+    const Scene* s;
+    RtPassParams p;
+    RtCamera cam;
+};
+
+static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint32_t max_depth, float bg_scale,
+                    int64_t* n_ext, int64_t* n_shadow) {
+    V3 T = v3(1, 1, 1);
+    V3 color = v3(0, 0, 0);
+    bool prev_specular = true;
+    float prev_mis_w_brdf = 1.0f;
+    float prev_spec_sun_weight = 1.0f;
+    bool have_lights = !s.lights.empty();
+    for (uint32_t depth = 0; depth < max_depth; depth++) {
+        uint32_t base = D_BOUNCE0 + depth * D_PER_BOUNCE;
+        (*n_ext)++;
+        HitRes h = closest_hit<false>(s, ray, 0.001f, INFINITY, nullptr);
+        if (h.gid < 0) {
+            float env_pdf = env_pdf_value(s, ray.d);                                // no sun: sun_pdf = 0
+            float emit_w = (env_pdf == 0.0f) ? 1.0f : (prev_specular ? prev_spec_sun_weight : prev_mis_w_brdf);
+            V3 bg = (depth == 0 || !s.has_env) ? bg_eval(s, ray.d) : env_eval(s, ray.d);
+            color = color + T * (bg * spec_factor(s.spec, ss)) * bg_scale * emit_w;
+            break;
+        }
+        Rec rec = make_rec(s, ray, h);
+        const RtMaterial& m = s.mats[rec.mat];
+        float emit_w = (prev_specular || !have_lights) ? 1.0f : prev_mis_w_brdf;
+        if (is_emissive_mat(m)) {
+            color = color + T * emission(s, rec.mat, ss) * emit_w;
+            break;   // lights do not scatter (material.rs:19,65)
+        }
+        V3 unit_dir = unit(ray.d);
+        if (m.type == RT_MAT_DIELECTRIC || m.type == RT_MAT_SPECTRAL_DIELECTRIC) {
+            // dielectric_boundary (material.rs:133-149) + SpectralDielectric (:369-402)
+            bool spectral = m.type == RT_MAT_SPECTRAL_DIELECTRIC;
+            float ior = spectral ? cauchy_ior(ss.lam[0], m.cauchy_b, m.cauchy_c) : m.cauchy_b;
+            if (spectral && ss.H > 1 && m.cauchy_c != 0.0f && ss.lam[1] != 0.0f) {
+                // dispersion: only the hero wavelength follows this direction;
+                // the secondaries end here (once — lam[1] = 0 marks them gone)
+                float w0 = ss.w[0] * (float)ss.H;
+                for (int i = 0; i < ss.H; i++) { ss.w[i] = 0.0f; if (i) ss.lam[i] = 0.0f; }
+                ss.w[0] = w0;
+            }
+            float ratio = rec.front ? 1.0f / ior : ior;
+            float cos_t = rmin(dot(-unit_dir, rec.normal), 1.0f);
+            float sin_t = std::sqrt(1.0f - cos_t * cos_t);
+            bool reflected = ratio * sin_t > 1.0f || fresnel_dielectric(cos_t, ratio) > rnd(rng, base + B_SCATTER0);
+            V3 dir;
+            if (reflected) dir = reflect(unit_dir, rec.normal);
+            else if (!refract(unit_dir, rec.normal, ratio, &dir)) dir = reflect(unit_dir, rec.normal);
+            V3 att = v3(1, 1, 1);
+            if (spectral) {
+                if (ss.tint == TINT_NONE && !reflected) ss.tint = TINT_FIRE;
+                if (!rec.front) {
+                    float d = rec.t;
+                    att.x *= std::exp(-m.absorption[0] * d);
+                    att.y *= std::exp(-m.absorption[1] * d);
+                    att.z *= std::exp(-m.absorption[2] * d);
+                }
+            }
+            prev_spec_sun_weight = 1.0f;
+            T = T * att;
+            ray = Ray{rec.p, dir};
+            prev_specular = true;
+            prev_mis_w_brdf = 1.0f;
+        } else if (m.type == RT_MAT_SPECTRAL_METAL) {
+            // SpectralMetal::scatter (material.rs:449-500)
+            V3 n = rec.normal;
+            V3 wo = unit(-ray.d);
+            float cos_o = dot(wo, n);
+            if (cos_o <= 0.0f) break;
+            V3 dir; float cos_h;
+            float alpha = rmax(m.roughness * m.roughness, 1e-4f);
+            if (m.roughness == 0.0f) {
+                dir = reflect(unit_dir, n);
+                cos_h = cos_o;
+            } else {
+                V3 t, b;
+                onb_vec(n, &t, &b);
+                V3 wo_ts = v3(dot(wo, t), dot(wo, b), cos_o);
+                V3 m_ts = vndf_sample(wo_ts, alpha, alpha, rnd(rng, base + B_SCATTER0), rnd(rng, base + B_SCATTER1));
+                V3 mm = unit(t * m_ts.x + b * m_ts.y + n * m_ts.z);
+                float vo_h = rmax(dot(wo, mm), 0.0f);
+                V3 wi = unit(2.0f * vo_h * mm - wo);
+                if (dot(wi, n) <= 0.0f) break;
+                dir = wi; cos_h = vo_h;
+            }
+            if (dot(dir, n) <= 0.0f) break;
+            float weight = 1.0f;
+            if (m.roughness != 0.0f) {
+                float lam_o = smith_lambda(cos_o, alpha);
+                float lam_i = smith_lambda(rmax(dot(dir, n), 0.0f), alpha);
+                weight = ((1.0f + lam_o) / (1.0f + lam_o + lam_i)) * specular_energy_comp(cos_o, alpha);
+            }
+            for (int i = 0; i < ss.H; i++) {
+                if (ss.w[i] == 0.0f) continue;
+                float nn, kk;
+                metal_ior(m, ss.lam[i], &nn, &kk);
+                ss.w[i] *= fresnel_conductor(cos_h, nn, kk);
+            }
+            if (ss.tint == TINT_NONE) ss.tint = TINT_CMF;
+            prev_spec_sun_weight = 1.0f;
+            T = T * weight;
+            ray = Ray{rec.p, dir};
+            prev_specular = true;
+            prev_mis_w_brdf = 1.0f;
+        } else {
+            // Lambertian / checker (material.rs:85-102): diffuse branch renderer.rs:457-572
+            V3 att = lambert_albedo(m, rec.p);
+            if (have_lights) {
+                uint32_t pick = rnd_u32(rng, base + B_LPICK) % (uint32_t)s.lights.size();
+                V3 light_dir = prim_pdf_generate(s, s.lights[pick], rec.p, rnd(rng, base + B_LPT0), rnd(rng, base + B_LPT1));
+                Ray shadow{rec.p, light_dir};
+                Rec lrec;
+                if (lights_hit(s, shadow, 0.001f, INFINITY, &lrec)) {
+                    (*n_shadow)++;
+                    bool occl = any_hit(s, shadow, 0.001f, lrec.t * (1.0f - 1e-4f));
+                    if (!occl) {
+                        float l_pdf = lights_pdf_value(s, rec.p, light_dir);
+                        float brdf = rmax(dot(rec.normal, unit(light_dir)) / PI_F, 0.0f);
+                        float env_p = env_pdf_value(s, light_dir);
+                        float mis_d = l_pdf * l_pdf + brdf * brdf + env_p * env_p;
+                        if (mis_d > 0.0f && brdf > 0.0f) {
+                            V3 nee = emission(s, lrec.mat, ss);
+                            color = color + T * att * brdf * l_pdf * nee / mis_d;
+                        }
+                    }
+                }
+            }
+            if (s.has_env) {
+                float env_pdf;
+                V3 env_dir = env_sample_dir(s.env, rnd(rng, base + B_ENV_ROW), rnd(rng, base + B_ENV_COL),
+                                            rnd(rng, base + B_ENV_JU), rnd(rng, base + B_ENV_JV), &env_pdf);
+                if (env_pdf > 0.0f) {
+                    Ray shadow{rec.p, env_dir};
+                    (*n_shadow)++;
+                    bool occl = any_hit(s, shadow, 0.001f, INFINITY);
+                    if (!occl) {
+                        float brdf = rmax(dot(rec.normal, unit(env_dir)) / PI_F, 0.0f);
+                        if (brdf > 0.0f) {
+                            float area_pdf = have_lights ? lights_pdf_value(s, rec.p, env_dir) : 0.0f;
+                            V3 env_color = env_eval(s, env_dir) * spec_factor(s.spec, ss);
+                            float mis_d = env_pdf * env_pdf + brdf * brdf + area_pdf * area_pdf;
+                            color = color + T * att * brdf * env_pdf * env_color / mis_d;
+                        }
+                    }
+                }
+            }
+            // indirect: cosine-weighted sample (pdf.rs:12-41)
+            Onb uvw = onb_from_w(rec.normal);
+            float r1 = rnd(rng, base + B_COS0), r2 = rnd(rng, base + B_COS1);
+            float phi = 2.0f * PI_F * r1;
+            float sq = std::sqrt(r2);
+            V3 ind_dir = onb_local(uvw, v3(std::cos(phi) * sq, std::sin(phi) * sq, std::sqrt(1.0f - r2)));
+            float pdf_val = rmax(dot(unit(ind_dir), uvw.w) / PI_F, 0.0f);
+            if (pdf_val <= 0.0f) break;
+            float scat_pdf = rmax(dot(rec.normal, unit(ind_dir)) / PI_F, 0.0f);
+            if (scat_pdf <= 0.0f) break;
+            if (dot(ind_dir, rec.normal) <= 0.0f) break;
+            float area = have_lights ? lights_pdf_value(s, rec.p, ind_dir) : 0.0f;
+            float env = env_pdf_value(s, ind_dir);
+            float nee_sq = area * area + env * env;
+            prev_mis_w_brdf = (pdf_val * pdf_val) / rmax(pdf_val * pdf_val + nee_sq, 1e-8f);
+            T = T * (att * (scat_pdf / pdf_val));
+            ray = Ray{rec.p, ind_dir};
+            prev_specular = false;
+        }
+        if (depth >= 2) {                                                           // renderer.rs:574-579
+            V3 eff = T * spec_factor(s.spec, ss);
+            float survive = rmax(rmax(eff.x, eff.y), eff.z);
+            float p = rmin(survive, 1.0f);
+            if (survive <= 0.0f || rnd(rng, base + B_RR) >= p) break;
+            T = T / p;
+        }
+    }
+    return color;
+}
+
+// ── camera + render_tiles (camera.rs:47-59, renderer.rs:655-730) ─────────────
+static void render_pixel(const Scene& s, const RtCamera& cam, const RtPassParams& p, uint32_t sample_idx,
+                         uint32_t row, uint32_t col, float out[3], int64_t* n_ext, int64_t* n_sh) {
+    uint32_t w = p.width, h = p.height;
+    uint32_t i = row * w + col;
+    Rng rng = make_rng(p.seed, i, sample_idx);
+    float w_denom = (float)std::max<uint32_t>(w - 1, 1), h_denom = (float)std::max<uint32_t>(h - 1, 1);
+    uint32_t strata = p.strata, strata2 = strata * strata;
+    uint32_t ray_y = h - 1 - row;
+    float uj, vj;
+    if (strata2 > 0) {
+        uint32_t offset = (i * 0x9E3779B9u) % strata2;
+        uint32_t sidx = (sample_idx + offset) % strata2;
+        uint32_t sx = sidx % strata, sy = sidx / strata;
+        uj = ((float)sx + rnd(rng, D_JIT_U)) / (float)strata;
+        vj = ((float)sy + rnd(rng, D_JIT_V)) / (float)strata;
+    } else {
+        uj = rnd(rng, D_JIT_U); vj = rnd(rng, D_JIT_V);
+    }
+    float u = ((float)col + uj) / w_denom;
+    float v = ((float)ray_y + vj) / h_denom;
+    V3 cu = v3(cam.u[0], cam.u[1], cam.u[2]), cv = v3(cam.v[0], cam.v[1], cam.v[2]);
+    V3 origin = v3(cam.origin[0], cam.origin[1], cam.origin[2]);
+    float lr = std::sqrt(rnd(rng, D_LENS_R)), lp = 2.0f * PI_F * rnd(rng, D_LENS_P);
+    V3 rd = cam.lens_radius * v3(lr * std::cos(lp), lr * std::sin(lp), 0.0f);
+    V3 offset = cu * rd.x + cv * rd.y;
+    V3 ll = v3(cam.lower_left[0], cam.lower_left[1], cam.lower_left[2]);
+    V3 hz = v3(cam.horizontal[0], cam.horizontal[1], cam.horizontal[2]);
+    V3 vt = v3(cam.vertical[0], cam.vertical[1], cam.vertical[2]);
+    Ray r{origin + offset, ll + u * hz + v * vt - origin - offset};
+    (void)rnd(rng, D_TIME);   // ray time: no moving geometry in the flat description
+    SpecState ss;
+    ss.H = (int)std::max<uint32_t>(1, std::min<uint32_t>(p.hero_count, 4));
+    float lam0 = s.spec.lam_lo + s.spec.lam_range * rnd(rng, D_LAMBDA);
+    if (lam0 >= s.spec.lam_lo + s.spec.lam_range) lam0 = std::nextafter(s.spec.lam_lo + s.spec.lam_range, 0.0f);
+    for (int k = 0; k < ss.H; k++) {
+        float off = std::fmod(lam0 - s.spec.lam_lo + (float)k * (s.spec.lam_range / (float)ss.H), s.spec.lam_range);
+        ss.lam[k] = s.spec.lam_lo + off;
+        ss.w[k] = 1.0f;
+    }
+    ss.tint = TINT_NONE;
+    V3 c = ray_color(s, r, rng, ss, p.max_depth, p.bg_scale, n_ext, n_sh);
+    out[0] = c.x; out[1] = c.y; out[2] = c.z;
+}
+
+// ── photon-free scene construction ───────────────────────────────────────────
+static std::string g_err;
+
+static int scene_create(const RtSceneDesc* d, Scene** out) {
+    if (!d || !out) { g_err = "null argument"; return RT_ERR_INVALID; }
+    Scene* s = new Scene();
+    s->n_tris = d->n_tris; s->n_quads = d->n_quads; s->n_spheres = d->n_spheres;
+    s->mats.assign(d->mats, d->mats + d->n_mats);
+    s->tris.resize(d->n_tris);
+    for (int64_t i = 0; i < d->n_tris; i++) {
+        const float* v = d->tri_v + i * 9;
+        Tri& t = s->tris[i];
+        t.v0 = v3(v[0], v[1], v[2]);
+        V3 v1 = v3(v[3], v[4], v[5]), v2 = v3(v[6], v[7], v[8]);
+        t.e1 = v1 - t.v0; t.e2 = v2 - t.v0;
+        t.has_n = d->tri_n != nullptr;
+        if (t.has_n) {
+            const float* n = d->tri_n + i * 9;
+            t.n0 = v3(n[0], n[1], n[2]); t.n1 = v3(n[3], n[4], n[5]); t.n2 = v3(n[6], n[7], n[8]);
+        }
+        t.mat = d->tri_mat[i];
+    }
+    s->quads.resize(d->n_quads);
+    for (int64_t i = 0; i < d->n_quads; i++) {                                      // quad.rs:21-33
+        const float* q = d->quad_quv + i * 9;
+        Quad& Q = s->quads[i];
+        Q.q = v3(q[0], q[1], q[2]); Q.u = v3(q[3], q[4], q[5]); Q.v = v3(q[6], q[7], q[8]);
+        V3 n = cross(Q.u, Q.v);
+        Q.area = length(n);
+        if (!(Q.area > 1e-6f * length(Q.u) * length(Q.v))) {
+            delete s; g_err = "degenerate quad " + std::to_string(i); return RT_ERR_INVALID;
+        }
+        Q.normal = n / Q.area;
+        Q.d = dot(Q.normal, Q.q);
+        Q.w = n / dot(n, n);
+        Q.mat = d->quad_mat[i];
+    }
+    s->spheres.resize(d->n_spheres);
+    for (int64_t i = 0; i < d->n_spheres; i++) {
+        const float* p = d->sphere + i * 4;
+        s->spheres[i] = Sphere{v3(p[0], p[1], p[2]), p[3], d->sphere_mat[i]};
+    }
+    s->lights.assign(d->light_prims, d->light_prims + d->n_lights);
+    s->bg = d->bg;
+    s->has_env = d->bg.type == RT_BG_ENVMAP && d->bg.env_rgb && d->bg.env_w > 0 && d->bg.env_h > 0;
+    if (s->has_env) env_build(s->env, d->bg);
+    s->bg.env_rgb = nullptr;
+    spectrum_init(s->spec, d->spectral_range);
+    s->bb_norm.assign(s->mats.size(), 0.0f);
+    s->bb_avg.assign(s->mats.size(), v3(0, 0, 0));
+    for (size_t mi = 0; mi < s->mats.size(); mi++) {                                // material.rs:47-62
+        const RtMaterial& m = s->mats[mi];
+        if (m.type != RT_MAT_BLACKBODY_LIGHT) continue;
+        int N = s->spec.n;
+        std::vector<float> raw(N);
+        float sum = 0.0f;
+        for (int i = 0; i < N; i++) { raw[i] = planck_raw(380.0f + (float)i * 5.0f, m.temp_k); sum += raw[i]; }
+        float mean = sum / (float)N;
+        float norm = 1.0f / rmax(mean, 1e-30f);
+        V3 acc = v3(0, 0, 0);
+        for (int i = 0; i < N; i++) acc = acc + spectral_to_rgb(s->spec, 380.0f + (float)i * 5.0f) * (raw[i] * norm);
+        s->bb_norm[mi] = norm;
+        s->bb_avg[mi] = acc / (float)N * m.intensity;
+    }
+    std::call_once(g_elut_once, build_e_lut);   // build the E_ss LUT outside any timed render
+    build_bvh(*s);
+    *out = s;
+    return RT_OK;
+}
+
+// ── thread pool helper (rows handed out dynamically, like Rayon's row tasks) ──
+template <class F>
+static void parallel_rows(uint32_t n_rows, int n_threads, F f) {
+    if (n_threads <= 1) { for (uint32_t r = 0; r < n_rows; r++) f(r, 0); return; }
+    std::atomic<uint32_t> next{0};
+    std::vector<std::thread> th;
+    for (int t = 0; t < n_threads; t++)
+        th.emplace_back([&, t]() { for (;;) { uint32_t r = next.fetch_add(1); if (r >= n_rows) break; f(r, t); } });
+    for (auto& x : th) x.join();
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+const char* orc_last_error() { return g_err.c_str(); }
+
+int32_t orc_scene_create(const RtSceneDesc* d, void** out) {
+    Scene* s = nullptr;
+    int rc = scene_create(d, &s);
+    *out = s;
+    return rc;
+}
+int32_t orc_scene_destroy(void* s) { delete (Scene*)s; return RT_OK; }
+
+int32_t orc_bvh_export(void* sp, float* nodes, int64_t* n_nodes, int32_t* leaf, int64_t* n_leaves) {
+    Scene* s = (Scene*)sp;
+    if (n_nodes) *n_nodes = (int64_t)s->nodes.size();
+    if (n_leaves) *n_leaves = (int64_t)s->leaf_prims.size();
+    if (nodes) memcpy(nodes, s->nodes.data(), s->nodes.size() * sizeof(Node));
+    if (leaf) memcpy(leaf, s->leaf_prims.data(), s->leaf_prims.size() * sizeof(int32_t));
+    return RT_OK;
+}
+
+// rays: n × 8 (o, d, tmin, tmax); mode 0 = BVH, 1 = brute force
+int32_t orc_trace_closest(void* sp, const float* rays, int64_t n, RtHit* hits, int32_t mode, int32_t threads) {
+    Scene* s = (Scene*)sp;
+    int64_t chunk = 4096, nch = (n + chunk - 1) / chunk;
+    parallel_rows((uint32_t)nch, threads, [&](uint32_t c, int) {
+        for (int64_t i = c * chunk; i < std::min(n, (int64_t)(c + 1) * chunk); i++) {
+            const float* r = rays + i * 8;
+            Ray ray{v3(r[0], r[1], r[2]), v3(r[3], r[4], r[5])};
+            HitRes h = mode == 1 ? closest_hit_brute(*s, ray, r[6], r[7]) : closest_hit<false>(*s, ray, r[6], r[7], nullptr);
+            hits[i].prim = h.gid; hits[i].t = h.gid >= 0 ? h.t : 0.0f;
+            hits[i].b1 = h.gid >= 0 ? h.b1 : 0.0f; hits[i].b2 = h.gid >= 0 ? h.b2 : 0.0f;
+        }
+    });
+    return RT_OK;
+}
+
+int32_t orc_trace_any(void* sp, const float* rays, int64_t n, uint8_t* occ, int32_t threads) {
+    Scene* s = (Scene*)sp;
+    int64_t chunk = 4096, nch = (n + chunk - 1) / chunk;
+    parallel_rows((uint32_t)nch, threads, [&](uint32_t c, int) {
+        for (int64_t i = c * chunk; i < std::min(n, (int64_t)(c + 1) * chunk); i++) {
+            const float* r = rays + i * 8;
+            occ[i] = any_hit(*s, Ray{v3(r[0], r[1], r[2]), v3(r[3], r[4], r[5])}, r[6], r[7]) ? 1 : 0;
+        }
+    });
+    return RT_OK;
+}
+
+// Per-ray traversal counters for the algorithmic-bytes roofline:
+// out[i*4 + {0,1,2,3}] = nodes visited, triangle, sphere, quad tests.
+int32_t orc_trace_stats(void* sp, const float* rays, int64_t n, int64_t* out, int32_t threads) {
+    Scene* s = (Scene*)sp;
+    int64_t chunk = 4096, nch = (n + chunk - 1) / chunk;
+    parallel_rows((uint32_t)nch, threads, [&](uint32_t c, int) {
+        for (int64_t i = c * chunk; i < std::min(n, (int64_t)(c + 1) * chunk); i++) {
+            const float* r = rays + i * 8;
+            TraceStats st;
+            closest_hit<true>(*s, Ray{v3(r[0], r[1], r[2]), v3(r[3], r[4], r[5])}, r[6], r[7], &st);
+            out[i * 4 + 0] = st.nodes; out[i * 4 + 1] = st.tris; out[i * 4 + 2] = st.spheres; out[i * 4 + 3] = st.quads;
+        }
+    });
+    return RT_OK;
+}
+
+// render_tiles for params->n_samples consecutive passes; scratch n_samples×h×w×3.
+// row_begin/row_end bound the rows rendered (a CPU-baseline sample may render a
+// band of rows); rows outside are left untouched.
+int32_t orc_render_pass(void* sp, const RtCamera* cam, const RtPassParams* p, float* scratch,
+                        const uint8_t* converged, int32_t threads, uint32_t row_begin, uint32_t row_end,
+                        int64_t* counters) {
+    Scene* s = (Scene*)sp;
+    uint32_t w = p->width, h = p->height;
+    if (row_end == 0 || row_end > h) row_end = h;
+    std::vector<int64_t> ext(std::max(threads, 1), 0), sh(std::max(threads, 1), 0);
+    for (uint32_t k = 0; k < std::max<uint32_t>(p->n_samples, 1); k++) {
+        uint32_t sidx = p->sample_idx + k;
+        float* out = scratch + (size_t)k * w * h * 3;
+        parallel_rows(row_end - row_begin, threads, [&](uint32_t rr, int tid) {
+            uint32_t row = rr + row_begin;
+            for (uint32_t col = 0; col < w; col++) {
+                size_t i = (size_t)row * w + col;
+                if (converged && converged[i]) { out[i * 3] = out[i * 3 + 1] = out[i * 3 + 2] = 0.0f; continue; }
+                render_pixel(*s, *cam, *p, sidx, row, col, out + i * 3, &ext[tid], &sh[tid]);
+            }
+        });
+    }
+    if (counters) {
+        counters[0] = counters[1] = 0;
+        for (size_t t = 0; t < ext.size(); t++) { counters[0] += ext[t]; counters[1] += sh[t]; }
+    }
+    return RT_OK;
+}
+
+// accumulate_sample (main.rs:603-643) for one pass over npix pixels
+int32_t orc_accumulate(float* acc, const float* scratch, uint32_t* n, float* m2, const uint8_t* conv,
+                       int64_t npix, float clamp, uint32_t min_samples, float floor_) {
+    for (int64_t i = 0; i < npix; i++) {
+        if (conv && conv[i]) continue;
+        V3 sc = v3(scratch[i * 3], scratch[i * 3 + 1], scratch[i * 3 + 2]);
+        if (!std::isfinite(sc.x) || !std::isfinite(sc.y) || !std::isfinite(sc.z)) continue;
+        uint32_t old_n = n[i];
+        V3 a = v3(acc[i * 3], acc[i * 3 + 1], acc[i * 3 + 2]);
+        V3 old_mean = old_n > 0 ? a / (float)old_n : v3(0, 0, 0);
+        float old_lum = luminance(old_mean);
+        if (clamp > 0.0f && old_n >= min_samples) {
+            float l = luminance(sc);
+            float thresh = rmax(clamp * old_lum, floor_);
+            if (l > thresh) sc = sc * (thresh / l);
+        }
+        a = a + sc;
+        n[i] = old_n + 1;
+        V3 new_mean = a / (float)n[i];
+        V3 mm = v3(m2[i * 3], m2[i * 3 + 1], m2[i * 3 + 2]) + (sc - old_mean) * (sc - new_mean);
+        acc[i * 3] = a.x; acc[i * 3 + 1] = a.y; acc[i * 3 + 2] = a.z;
+        m2[i * 3] = mm.x; m2[i * 3 + 1] = mm.y; m2[i * 3 + 2] = mm.z;
+    }
+    return RT_OK;
+}
+
+// mark_converged (main.rs:646-677) with ADAPTIVE_THRESHOLD as a parameter
+int64_t orc_mark_converged(uint8_t* conv, const uint32_t* n, const float* m2, const float* acc, int64_t npix, float thresh) {
+    int64_t cnt = 0;
+    for (int64_t i = 0; i < npix; i++) {
+        if (!conv[i] && n[i] > 0) {
+            bool ok = true;
+            for (int c = 0; c < 3; c++) {
+                float mean = acc[i * 3 + c] / (float)std::max<uint32_t>(n[i], 1);
+                if (mean < 1e-4f) continue;
+                float var = m2[i * 3 + c] / (float)std::max<uint32_t>(n[i] - 1, 1);
+                float se = std::sqrt(var / (float)n[i]);
+                if (se / mean >= thresh) { ok = false; break; }
+            }
+            if (ok) conv[i] = 1;
+        }
+        cnt += conv[i] ? 1 : 0;
+    }
+    return cnt;
+}
+
+// ── scalar functions pinned by the reference's unit tests ────────────────────
+float orc_fresnel_dielectric(float c, float eta) { return fresnel_dielectric(c, eta); }
+float orc_fresnel_conductor(float c, float n, float k) { return fresnel_conductor(c, n, k); }
+float orc_cauchy_ior(float l, float b, float c) { return cauchy_ior(l, b, c); }
+float orc_planck_raw(float l, float t) { return planck_raw(l, t); }
+float orc_ggx_ndf(float c, float a) { return ggx_ndf(c, a); }
+float orc_smith_g1(float c, float a) { return smith_g1(c, a); }
+float orc_smith_lambda(float c, float a) { return smith_lambda(c, a); }
+float orc_e_ss(float mu, float a) { return e_ss_lut(mu, a); }
+float orc_energy_comp(float mu, float a) { return specular_energy_comp(mu, a); }
+void orc_elut_export(float* out) { e_ss_lut(0.5f, 0.5f); memcpy(out, g_elut, sizeof(g_elut)); }
+void orc_spectral_to_rgb(float l, int32_t range_mode, float* out) {
+    static Spectrum sp[2]; static std::once_flag f[2];
+    int m = range_mode ? 1 : 0;
+    std::call_once(f[m], [&]() { spectrum_init(sp[m], m); });
+    V3 c = spectral_to_rgb(sp[m], l); out[0] = c.x; out[1] = c.y; out[2] = c.z;
+}
+void orc_spectral_fire_rgb(float l, int32_t range_mode, float* out) {
+    static Spectrum sp[2]; static std::once_flag f[2];
+    int m = range_mode ? 1 : 0;
+    std::call_once(f[m], [&]() { spectrum_init(sp[m], m); });
+    V3 c = spectral_fire_rgb(sp[m], l); out[0] = c.x; out[1] = c.y; out[2] = c.z;
+}
+void orc_metal_ior(int32_t metal, float l, float* n, float* k) {
+    RtMaterial m; memset(&m, 0, sizeof(m)); m.metal = metal;
+    metal_ior(m, l, n, k);
+}
+void orc_vndf_sample(const float* wo, float ax, float ay, float x1, float x2, float* out) {
+    V3 m = vndf_sample(v3(wo[0], wo[1], wo[2]), ax, ay, x1, x2); out[0] = m.x; out[1] = m.y; out[2] = m.z;
+}
+// quad/triangle/sphere hit against a one-prim scene is covered by orc_trace_closest;
+// env map queries for the renderer.rs env tests:
+void orc_env_sample(void* sp, const float* dir, float* out) {
+    Scene* s = (Scene*)sp; V3 c = env_sample(s->env, v3(dir[0], dir[1], dir[2])); out[0] = c.x; out[1] = c.y; out[2] = c.z;
+}
+float orc_env_pdf(void* sp, const float* dir) { return env_pdf_value(*(Scene*)sp, v3(dir[0], dir[1], dir[2])); }
+void orc_env_sample_dir(void* sp, const float* xi, float* dir, float* pdf) {
+    Scene* s = (Scene*)sp; V3 d = env_sample_dir(s->env, xi[0], xi[1], xi[2], xi[3], pdf); dir[0] = d.x; dir[1] = d.y; dir[2] = d.z;
+}
+void orc_bg_eval(void* sp, const float* dir, float* out) {
+    Scene* s = (Scene*)sp; V3 c = bg_eval(*s, v3(dir[0], dir[1], dir[2])); out[0] = c.x; out[1] = c.y; out[2] = c.z;
+}
+void orc_env_eval(void* sp, const float* dir, float* out) {
+    Scene* s = (Scene*)sp; V3 c = env_eval(*s, v3(dir[0], dir[1], dir[2])); out[0] = c.x; out[1] = c.y; out[2] = c.z;
+}
+float orc_lights_pdf_value(void* sp, const float* o, const float* d) {
+    return lights_pdf_value(*(Scene*)sp, v3(o[0], o[1], o[2]), v3(d[0], d[1], d[2]));
+}
+void orc_rng(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim, uint32_t* u, float* f) {
+    Rng r = make_rng(seed, pixel, sample);
+    *u = rnd_u32(r, dim); *f = rnd(r, dim);
+}
+
+}  // extern "C"

@@ -1,0 +1,130 @@
+"""ctypes mirror of include/rt_api.h (the C ABI of librtb200.so).
+
+Field order and types follow the header exactly; keep them in sync.
+"""
+import ctypes as C
+
+RT_OK, RT_ERR_INVALID, RT_ERR_CAPACITY, RT_ERR_TIMEOUT, RT_ERR_CUDA, RT_ERR_NOMEM = 0, 1, 2, 3, 4, 5
+RT_MEM_HOST, RT_MEM_DEVICE = 0, 1
+
+RT_MAT_LAMBERTIAN = 0
+RT_MAT_CHECKER = 1
+RT_MAT_DIELECTRIC = 2
+RT_MAT_SPECTRAL_DIELECTRIC = 3
+RT_MAT_SPECTRAL_METAL = 4
+RT_MAT_DIFFUSE_LIGHT = 5
+RT_MAT_BLACKBODY_LIGHT = 6
+
+RT_METAL_GOLD, RT_METAL_COPPER, RT_METAL_SILVER, RT_METAL_CUSTOM = 0, 1, 2, 3
+RT_MAX_NK = 16
+
+RT_BG_SOLID, RT_BG_GRADIENT, RT_BG_ENVMAP = 0, 1, 2
+RT_PRIM_TRI, RT_PRIM_QUAD, RT_PRIM_SPHERE = 0, 1, 2
+
+F3 = C.c_float * 3
+
+
+class RtMaterial(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("albedo", F3),
+        ("odd", F3),
+        ("checker_scale", C.c_float),
+        ("cauchy_b", C.c_float),
+        ("cauchy_c", C.c_float),
+        ("absorption", F3),
+        ("roughness", C.c_float),
+        ("metal", C.c_int32),
+        ("temp_k", C.c_float),
+        ("intensity", C.c_float),
+        ("nk_count", C.c_int32),
+        ("nk_start", C.c_float),
+        ("nk_step", C.c_float),
+        ("nk_n", C.c_float * RT_MAX_NK),
+        ("nk_k", C.c_float * RT_MAX_NK),
+    ]
+
+
+class RtBackground(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("color", F3),
+        ("top", F3),
+        ("bottom", F3),
+        ("env_w", C.c_int32),
+        ("env_h", C.c_int32),
+        ("env_rgb", C.POINTER(C.c_float)),
+        ("env_rot_y_deg", C.c_float),
+        ("visible_type", C.c_int32),
+        ("visible_color", F3),
+        ("visible_top", F3),
+        ("visible_bottom", F3),
+    ]
+
+
+class RtSceneDesc(C.Structure):
+    _fields_ = [
+        ("n_tris", C.c_int64),
+        ("tri_v", C.POINTER(C.c_float)),
+        ("tri_n", C.POINTER(C.c_float)),
+        ("tri_mat", C.POINTER(C.c_int32)),
+        ("n_quads", C.c_int64),
+        ("quad_quv", C.POINTER(C.c_float)),
+        ("quad_mat", C.POINTER(C.c_int32)),
+        ("n_spheres", C.c_int64),
+        ("sphere", C.POINTER(C.c_float)),
+        ("sphere_mat", C.POINTER(C.c_int32)),
+        ("n_mats", C.c_int32),
+        ("mats", C.POINTER(RtMaterial)),
+        ("n_lights", C.c_int32),
+        ("light_prims", C.POINTER(C.c_int32)),
+        ("bg", RtBackground),
+        ("spectral_range", C.c_int32),
+    ]
+
+
+class RtCamera(C.Structure):
+    _fields_ = [
+        ("origin", F3),
+        ("lower_left", F3),
+        ("horizontal", F3),
+        ("vertical", F3),
+        ("u", F3),
+        ("v", F3),
+        ("lens_radius", C.c_float),
+        ("aperture_blades", C.c_int32),
+    ]
+
+
+class RtPassParams(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("sample_idx", C.c_uint32),
+        ("n_samples", C.c_uint32),
+        ("strata", C.c_uint32),
+        ("max_depth", C.c_uint32),
+        ("hero_count", C.c_uint32),
+        ("use_frame_time", C.c_uint32),
+        ("t0", C.c_float),
+        ("t1", C.c_float),
+        ("bg_scale", C.c_float),
+        ("seed", C.c_uint64),
+    ]
+
+
+class RtHit(C.Structure):
+    _fields_ = [("prim", C.c_int32), ("t", C.c_float), ("b1", C.c_float), ("b2", C.c_float)]
+
+
+def fptr(a):
+    """Pointer to a contiguous float32 numpy array (None → NULL)."""
+    if a is None:
+        return C.POINTER(C.c_float)()
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def iptr(a):
+    if a is None:
+        return C.POINTER(C.c_int32)()
+    return a.ctypes.data_as(C.POINTER(C.c_int32))

@@ -1,0 +1,193 @@
+"""Seeded synthetic workloads (the reference ships no data set for them).
+
+Each generator returns (SceneBuilder, render settings dict).  Sizes and value
+distributions follow the workload definitions:
+
+  box        256×256 open-front 1×1×1 Lambertian room, diffuse + dispersive glass
+             sphere, 0.25² 6500 K blackbody ceiling light ×15; 16 spp, depth 8,
+             4 hero wavelengths over 380–780 nm.
+  icosphere  icosphere with 8 subdivisions (1,310,720 triangles), radial Perlin
+             displacement (amplitude 0.08, 4 octaves, frequency 3), GGX conductor
+             roughness 0.2 with a gold-like n,k on 8 wavelengths; diffuse floor
+             (albedo 0.5); 2048×1024 float32 sky (gradient 0.2→1.0 plus a 0.5°
+             sun lobe of peak 5e4); 1920×1080, 64 spp, depth 12.
+
+The Perlin noise is the lattice-gradient noise of src/perlin.rs:21-92 (random
+unit gradients, three 256-entry permutations, Hermite-smoothed trilinear
+interpolation), seeded from numpy instead of thread_rng.
+"""
+import math
+
+import numpy as np
+
+from .scene import Material, SceneBuilder, make_camera
+
+F32 = np.float32
+
+
+# ── Perlin (perlin.rs:21-92), vectorised ────────────────────────────────────
+class Perlin:
+    def __init__(self, seed):
+        rng = np.random.default_rng(seed)
+        v = rng.uniform(-1.0, 1.0, size=(256, 3))
+        self.ranvec = v / np.linalg.norm(v, axis=1, keepdims=True)
+        self.perm = [rng.permutation(256) for _ in range(3)]
+
+    def noise(self, p):
+        p = np.asarray(p, dtype=np.float64)
+        fl = np.floor(p)
+        f = p - fl
+        s = f * f * (3.0 - 2.0 * f)
+        ijk = fl.astype(np.int64)
+        acc = np.zeros(len(p))
+        for di in (0, 1):
+            for dj in (0, 1):
+                for dk in (0, 1):
+                    idx = (self.perm[0][(ijk[:, 0] + di) & 255] ^ self.perm[1][(ijk[:, 1] + dj) & 255]
+                           ^ self.perm[2][(ijk[:, 2] + dk) & 255])
+                    g = self.ranvec[idx]
+                    wv = s - np.array([di, dj, dk], dtype=np.float64)
+                    wgt = ((di * s[:, 0] + (1 - di) * (1 - s[:, 0])) * (dj * s[:, 1] + (1 - dj) * (1 - s[:, 1]))
+                           * (dk * s[:, 2] + (1 - dk) * (1 - s[:, 2])))
+                    acc += wgt * (g * wv).sum(1)
+        return acc
+
+    def fbm(self, p, octaves):
+        acc = np.zeros(len(p))
+        w = 1.0
+        q = np.asarray(p, dtype=np.float64)
+        for _ in range(octaves):
+            acc += w * self.noise(q)
+            w *= 0.5
+            q = q * 2.0
+        return acc
+
+
+# ── icosphere ────────────────────────────────────────────────────────────────
+def icosphere(levels):
+    """Unit icosphere: 20·4^levels faces, shared vertices (midpoint cache)."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t),
+             (0, -1, -t), (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    V = np.array(verts, dtype=np.float64)
+    V /= np.linalg.norm(V, axis=1, keepdims=True)
+    Fc = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4],
+                   [11, 10, 2], [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8],
+                   [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], dtype=np.int64)
+    for _ in range(levels):
+        nv = len(V)
+        e = np.concatenate([Fc[:, [0, 1]], Fc[:, [1, 2]], Fc[:, [2, 0]]])
+        e.sort(axis=1)
+        key = e[:, 0] * (nv + 1) + e[:, 1]
+        uniq, inv = np.unique(key, return_inverse=True)
+        a, b = uniq // (nv + 1), uniq % (nv + 1)
+        mid = V[a] + V[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        V = np.concatenate([V, mid])
+        nf = len(Fc)
+        m01, m12, m20 = nv + inv[:nf], nv + inv[nf:2 * nf], nv + inv[2 * nf:]
+        Fc = np.concatenate([
+            np.stack([Fc[:, 0], m01, m20], 1),
+            np.stack([Fc[:, 1], m12, m01], 1),
+            np.stack([Fc[:, 2], m20, m12], 1),
+            np.stack([m01, m12, m20], 1)])
+    return V, Fc
+
+
+def vertex_normals(V, Fc):
+    fn = np.cross(V[Fc[:, 1]] - V[Fc[:, 0]], V[Fc[:, 2]] - V[Fc[:, 0]])
+    N = np.zeros_like(V)
+    for k in range(3):
+        np.add.at(N, Fc[:, k], fn)
+    return N / np.linalg.norm(N, axis=1, keepdims=True)
+
+
+# ── synthetic environment map ────────────────────────────────────────────────
+def sky_env(width=2048, height=1024, sun_dir=None, sun_peak=5e4, sun_fwhm_deg=0.5, seed=7):
+    """Equirect float32 sky: luminance 0.2 at and below the horizon rising to
+    1.0 at the zenith, plus a Gaussian sun lobe (FWHM 0.5°, peak 5e4).  Texel
+    directions follow the reference's mapping (renderer.rs:145-151)."""
+    if sun_dir is None:
+        rng = np.random.default_rng(seed)
+        az = rng.uniform(0, 2 * math.pi)
+        el = math.radians(rng.uniform(25.0, 55.0))
+        sun_dir = (math.cos(el) * math.sin(az), math.sin(el), math.cos(el) * math.cos(az))
+    s = np.asarray(sun_dir, dtype=np.float64)
+    s /= np.linalg.norm(s)
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    theta = math.pi * v[:, None]
+    phi = 2.0 * math.pi * (u[None, :] - 0.5)
+    dx = np.sin(theta) * np.sin(phi)
+    dy = np.cos(theta) * np.ones_like(phi)
+    dz = np.sin(theta) * np.cos(phi)
+    grad = 0.2 + 0.8 * np.clip(dy, 0.0, 1.0)
+    cosg = np.clip(dx * s[0] + dy * s[1] + dz * s[2], -1.0, 1.0)
+    ang = np.degrees(np.arccos(cosg))
+    sigma = sun_fwhm_deg / (2.0 * math.sqrt(2.0 * math.log(2.0)))
+    sun = sun_peak * np.exp(-0.5 * (ang / sigma) ** 2)
+    sky = np.stack([grad * 0.85 + sun, grad * 0.92 + sun * 0.96, grad * 1.0 + sun * 0.88], axis=-1)
+    return sky.astype(F32), tuple(s)
+
+
+def gold_like_nk(n_samples=8, start=380.0, step=50.0):
+    """n,k of gold (src/spectrum.rs:218-219) resampled on a uniform grid."""
+    from . import abi  # noqa: F401
+    gold_n = [1.69, 1.65, 1.54, 1.33, 0.97, 0.54, 0.30, 0.23, 0.20, 0.19, 0.18, 0.16, 0.16]
+    gold_k = [1.91, 1.94, 1.95, 1.92, 1.80, 1.93, 2.41, 3.00, 3.56, 4.07, 4.56, 4.99, 5.41]
+    lam = start + step * np.arange(n_samples)
+    src = 380.0 + 25.0 * np.arange(13)
+    return (np.interp(lam, src, gold_n).tolist(), np.interp(lam, src, gold_k).tolist())
+
+
+# ── workloads ────────────────────────────────────────────────────────────────
+def box_scene(width=256, height=256, spp=16, max_depth=8, hero=4, seed=1):
+    sb = SceneBuilder()
+    sb.name = "box"
+    sb.spectral_range = 1 if hero > 1 else 0
+    white = sb.add_material(Material.lambertian((0.73, 0.73, 0.73)))
+    red = sb.add_material(Material.lambertian((0.65, 0.05, 0.05)))
+    green = sb.add_material(Material.lambertian((0.12, 0.45, 0.15)))
+    sb.add_quad((0, 0, 0), (1, 0, 0), (0, 0, 1), white)      # floor
+    sb.add_quad((0, 1, 0), (1, 0, 0), (0, 0, 1), white)      # ceiling
+    sb.add_quad((0, 0, 1), (1, 0, 0), (0, 1, 0), white)      # back wall
+    sb.add_quad((1, 0, 0), (0, 0, 1), (0, 1, 0), red)        # left wall (image left)
+    sb.add_quad((0, 0, 0), (0, 0, 1), (0, 1, 0), green)      # right wall
+    light = sb.add_material(Material.blackbody(6500.0, 15.0))
+    sb.add_light_quad((0.375, 1.0 - 1e-3, 0.375), (0.25, 0, 0), (0, 0, 0.25), light)
+    diffuse = sb.add_material(Material.lambertian((0.73, 0.73, 0.73)))
+    glass = sb.add_material(Material.spectral_dielectric_cauchy(1.5, 0.0042))
+    sb.add_sphere((0.3, 0.18, 0.6), 0.18, diffuse)
+    sb.add_sphere((0.7, 0.18, 0.35), 0.18, glass)
+    sb.set_solid((0.0, 0.0, 0.0))
+    cam = make_camera((0.5, 0.5, -1.4), (0.5, 0.5, 0.5), vfov=40.0, aspect=width / height)
+    settings = dict(width=width, height=height, spp=spp, max_depth=max_depth, hero=hero, seed=seed, camera=cam,
+                    name="box 256x256 16spp depth8 hero4")
+    return sb, settings
+
+
+def icosphere_scene(width=1920, height=1080, spp=64, max_depth=12, hero=4, seed=2, levels=8,
+                    env_w=2048, env_h=1024):
+    sb = SceneBuilder()
+    sb.name = "icosphere"
+    sb.spectral_range = 1 if hero > 1 else 0
+    V, Fc = icosphere(levels)
+    per = Perlin(seed)
+    disp = per.fbm(V * 3.0, 4)
+    V = V * (1.0 + 0.08 * disp)[:, None]
+    N = vertex_normals(V, Fc)
+    n, k = gold_like_nk()
+    metal = sb.add_material(Material.spectral_metal_nk(380.0, 50.0, n, k, roughness=0.2))
+    sb.add_mesh(V, Fc, metal, N)
+    floor = sb.add_material(Material.lambertian((0.5, 0.5, 0.5)))
+    sb.add_quad((-10.0, -1.1, -10.0), (0.0, 0.0, 20.0), (20.0, 0.0, 0.0), floor)
+    env, sun = sky_env(env_w, env_h, seed=seed)
+    sb.set_env(env)
+    cam = make_camera((0.0, 0.45, 3.6), (0.0, -0.15, 0.0), vfov=40.0, aspect=width / height)
+    settings = dict(width=width, height=height, spp=spp, max_depth=max_depth, hero=hero, seed=seed, camera=cam,
+                    name=f"icosphere{levels} {len(Fc)} tris {width}x{height} {spp}spp depth{max_depth} hero{hero}",
+                    n_tris=len(Fc), sun_dir=sun)
+    return sb, settings
+
+
+CONFIGS = {"box": box_scene, "icosphere": icosphere_scene}

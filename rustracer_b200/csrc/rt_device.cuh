@@ -1,0 +1,201 @@
+// rt_device.cuh — device data layouts and per-thread math shared by the
+// traversal (rt_trace.cu) and shading (rt_shade.cu) kernels.
+//
+// HBM layout (all arrays 16-byte aligned, read through the read-only path):
+//   nodes  : 8-wide BVH nodes, 14 float4 = 224 B each, the reference layout of
+//            src/bvh.rs:25-32 (min[3][8], max[3][8], children[8]) so one node is
+//            fetched with 14 128-bit loads.  child ≥ 0 → inner node, child with
+//            the top bit set → leaf (type in bits 28-30, index in bits 0-27),
+//            0xFFFFFFFF → empty slot.
+//   tri    : 3 float4 per triangle, leaf order: (v0.xyz, e1.x) (e1.yz, e2.xy)
+//            (e2.z, gid, mat, has_normals).  e1 = v1 - v0 and e2 = v2 - v0 are
+//            the exact f32 differences the reference forms per hit
+//            (triangle.rs:76-77), so the hit arithmetic is unchanged.
+//   tri_n  : 3 float4 per triangle: (n0.xyz, n1.x) (n1.yz, n2.xy) (n2.z, -, -, -)
+//   quad   : 5 float4: (normal.xyz, d) (Q.xyz, u.x) (u.yz, v.xy) (v.z, w.xyz) (gid, mat, area, -)
+//   sphere : 2 float4: (centre.xyz, r) (gid, mat, -, -)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define RT_HD __host__ __device__ __forceinline__
+#define RT_D __device__ __forceinline__
+
+#define RT_LEAF_BIT   0x80000000u
+#define RT_EMPTY_REF  0xFFFFFFFFu
+#define RT_MISS_REF   0xFFFFFFFFu
+#define RT_STACK      96
+
+namespace rtd {
+
+static constexpr float PI_F = 3.14159265358979323846f;
+static constexpr float SLAB_WIDEN = 1.52587890625e-05f;   // 2^-16: conservative slab exit
+
+// ── device material record ──────────────────────────────────────────────────
+struct DevMaterial {
+    int   type;
+    int   metal;        // 0-2 builtin tables, 3 custom
+    float albedo[3];
+    float odd[3];
+    float checker_scale;
+    float cauchy_b, cauchy_c;
+    float absorption[3];
+    float roughness;
+    float temp_k, intensity;
+    float bb_norm;      // 1 / mean(planck) over the sampled grid (material.rs:47-52)
+    float bb_avg[3];    // time-averaged RGB of the blackbody (material.rs:53-59)
+    int   nk_count;
+    float nk_start, nk_step;
+    float nk_n[16], nk_k[16];
+};
+
+struct DevLight {        // one entry of the NEE light list (hittable.rs:138-225)
+    int    type;         // RT_PRIM_QUAD / RT_PRIM_SPHERE
+    int    mat;
+    float4 g[5];         // quad record or sphere record (same packing as above)
+};
+
+struct DevScene {
+    const float4* nodes;
+    const float4* tri;
+    const float4* tri_n;
+    const float4* quad;
+    const float4* sphere;
+    const DevLight* lights;
+    const DevMaterial* mats;
+    int n_lights, n_mats;
+    // spectral tables: CIE x̄ȳz̄ on the 5 nm grid from 380 nm and the per-channel
+    // normalisations of spectral_to_rgb / spectral_fire_rgb (spectrum.rs:78-177)
+    const float4* cmf;          // n_spec entries (x, y, z, -)
+    int   n_spec;
+    float norms[3], fire_norms[3];
+    float lam_lo, lam_range;
+    const float* elut;          // 64×64 E_ss(mu, alpha)
+    // environment map
+    int   has_env;
+    int   env_w, env_h;
+    const float4* env;          // rgb + luminance per texel
+    const float2* env_alias;    // (probability, alias index bits) per texel
+    float env_inv_total;
+    float env_sin_r, env_cos_r;
+    // background
+    int   bg_type;
+    float bg_color[3], bg_top[3], bg_bottom[3];
+    int   vis_type;
+    float vis_color[3], vis_top[3], vis_bottom[3];
+};
+
+// ── float3 helpers ──────────────────────────────────────────────────────────
+RT_HD float3 mk(float x, float y, float z) { return make_float3(x, y, z); }
+RT_HD float3 operator+(float3 a, float3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+RT_HD float3 operator-(float3 a, float3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+RT_HD float3 operator-(float3 a) { return mk(-a.x, -a.y, -a.z); }
+RT_HD float3 operator*(float3 a, float3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+RT_HD float3 operator*(float3 a, float t) { return mk(a.x * t, a.y * t, a.z * t); }
+RT_HD float3 operator*(float t, float3 a) { return mk(a.x * t, a.y * t, a.z * t); }
+RT_HD float3 operator/(float3 a, float t) { return mk(a.x / t, a.y / t, a.z / t); }
+RT_HD float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+RT_HD float len2(float3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+RT_HD float3 cross3(float3 a, float3 b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+RT_D float3 unit3(float3 a) { return a / sqrtf(len2(a)); }
+RT_HD float lum3(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+RT_HD float clampf_(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
+RT_D float3 reflect3(float3 v, float3 n) { return v - 2.0f * dot3(v, n) * n; }
+
+// ── counter-based RNG: pcg3d (Jarzynski & Olano, JCGT 2020) ──────────────────
+RT_HD uint32_t mix32(uint32_t x) {
+    x ^= x >> 16; x *= 0x7feb352dU; x ^= x >> 15; x *= 0x846ca68bU; x ^= x >> 16;
+    return x;
+}
+RT_HD uint32_t pcg3d_x(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t x = a * 1664525u + 1013904223u;
+    uint32_t y = b * 1664525u + 1013904223u;
+    uint32_t z = c * 1664525u + 1013904223u;
+    x += y * z; y += z * x; z += x * y;
+    x ^= x >> 16; y ^= y >> 16; z ^= z >> 16;
+    x += y * z; y += z * x; z += x * y;
+    return x;
+}
+struct Rng { uint32_t a, b, c; };
+RT_HD Rng make_rng(uint64_t seed, uint32_t pixel, uint32_t sample) {
+    Rng r;
+    r.a = pixel;
+    r.b = sample ^ mix32((uint32_t)seed);
+    r.c = mix32((uint32_t)(seed >> 32) + 0x9E3779B9u);
+    return r;
+}
+RT_HD uint32_t rnd_u32(const Rng& r, uint32_t dim) { return pcg3d_x(r.a, r.b, dim ^ r.c); }
+RT_HD float rnd(const Rng& r, uint32_t dim) { return (float)(rnd_u32(r, dim) >> 8) * (1.0f / 16777216.0f); }
+
+enum {
+    D_JIT_U = 0, D_JIT_V = 1, D_LENS_R = 2, D_LENS_P = 3, D_TIME = 4, D_LAMBDA = 5,
+    D_BOUNCE0 = 8, D_PER_BOUNCE = 16,
+    B_SCATTER0 = 0, B_SCATTER1 = 1, B_LPICK = 2, B_LPT0 = 3, B_LPT1 = 4,
+    B_ENV_ROW = 7, B_ENV_COL = 8, B_ENV_JU = 9, B_ENV_JV = 10, B_COS0 = 11, B_COS1 = 12, B_RR = 13,
+};
+
+// Slab reciprocal: plain 1/d.  A ray with an infinite reciprocal component can
+// produce (bound − o)·inv = 0·∞ = NaN when it lies exactly in a box face plane;
+// the traversal then takes the NaN-aware slab path, where such a slab spans the
+// whole line (the ray is inside the closed slab) so culling stays conservative.
+
+// ── primitive hit tests: same f32 operation sequence as the reference ────────
+// triangle.rs:75-89
+RT_D bool tri_test(float4 a, float4 b, float4 c, float3 o, float3 d, float tmin, float tmax,
+                   float* t_out, float* b1o, float* b2o) {
+    float3 v0 = mk(a.x, a.y, a.z), e1 = mk(a.w, b.x, b.y), e2 = mk(b.z, b.w, c.x);
+    float3 h = cross3(d, e2);
+    float aa = dot3(e1, h);
+    if (fabsf(aa) < 1e-8f) return false;
+    float f = 1.0f / aa;
+    float3 s = o - v0;
+    float b1 = f * dot3(s, h);
+    if (!(b1 >= 0.0f && b1 <= 1.0f)) return false;
+    float3 q = cross3(s, e1);
+    float b2 = f * dot3(d, q);
+    if (b2 < 0.0f || b1 + b2 > 1.0f) return false;
+    float t = f * dot3(e2, q);
+    if (t < tmin || t > tmax) return false;
+    *t_out = t; *b1o = b1; *b2o = b2;
+    return true;
+}
+// quad.rs:37-57
+RT_D bool quad_test(const float4* g, float3 o, float3 d, float tmin, float tmax, float* t_out, float* al, float* be) {
+    float4 g0 = g[0];
+    float3 n = mk(g0.x, g0.y, g0.z);
+    float denom = dot3(n, d);
+    if (!(fabsf(denom) >= 1e-8f)) return false;
+    float t = (g0.w - dot3(n, o)) / denom;
+    if (t < tmin || t > tmax) return false;
+    float4 g1 = g[1], g2 = g[2], g3 = g[3];
+    float3 Q = mk(g1.x, g1.y, g1.z), u = mk(g1.w, g2.x, g2.y), v = mk(g2.z, g2.w, g3.x), w = mk(g3.y, g3.z, g3.w);
+    float3 p = o + t * d;
+    float3 planar = p - Q;
+    float alpha = dot3(w, cross3(planar, v));
+    float beta = dot3(w, cross3(u, planar));
+    if (!(alpha >= 0.0f && alpha <= 1.0f) || !(beta >= 0.0f && beta <= 1.0f)) return false;
+    *t_out = t; *al = alpha; *be = beta;
+    return true;
+}
+// sphere.rs:47-61
+RT_D bool sphere_test(float4 s0, float3 o, float3 d, float tmin, float tmax, float* t_out) {
+    float3 oc = o - mk(s0.x, s0.y, s0.z);
+    float a = len2(d);
+    if (!(a > 0.0f)) return false;
+    float half_b = dot3(oc, d);
+    float c = len2(oc) - s0.w * s0.w;
+    float disc = half_b * half_b - a * c;
+    if (disc < 0.0f) return false;
+    float sq = sqrtf(disc);
+    float root = (-half_b - sq) / a;
+    if (root < tmin || root > tmax) {
+        root = (-half_b + sq) / a;
+        if (root < tmin || root > tmax) return false;
+    }
+    *t_out = root;
+    return true;
+}
+
+}  // namespace rtd

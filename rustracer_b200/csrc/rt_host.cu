@@ -1,0 +1,1137 @@
+// rt_host.cu — C ABI of librtb200.so (include/rt_api.h): scene upload, BVH
+// build, environment alias tables, spectral tables, and the wavefront render
+// loop that drives the kernels of rt_trace.cu / rt_shade.cu on one stream.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rt_spectral_tables.h"
+#include "rt_internal.h"
+
+using namespace rtd;
+
+namespace {
+
+// ── small host math (f32, no contraction: built with -ffp-contract=off) ─────
+struct H3 { float x, y, z; };
+static inline H3 h3(float x, float y, float z) { return H3{x, y, z}; }
+static inline H3 operator+(H3 a, H3 b) { return h3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline H3 operator-(H3 a, H3 b) { return h3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline H3 operator*(H3 a, float t) { return h3(a.x * t, a.y * t, a.z * t); }
+static inline H3 operator/(H3 a, float t) { return h3(a.x / t, a.y / t, a.z / t); }
+static inline float hdot(H3 a, H3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline H3 hcross(H3 a, H3 b) { return h3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static inline float hlen(H3 a) { return std::sqrt(hdot(a, a)); }
+static inline float hc(H3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+
+struct Box { H3 mn, mx; };
+static inline Box unite(const Box& a, const Box& b) {
+    return Box{h3(std::fmin(a.mn.x, b.mn.x), std::fmin(a.mn.y, b.mn.y), std::fmin(a.mn.z, b.mn.z)),
+               h3(std::fmax(a.mx.x, b.mx.x), std::fmax(a.mx.y, b.mx.y), std::fmax(a.mx.z, b.mx.z))};
+}
+static inline Box pad(Box b) {                                                      // aabb.rs:18-29
+    const float D = 0.0001f;
+    float px = b.mx.x - b.mn.x < D ? D : 0.0f, py = b.mx.y - b.mn.y < D ? D : 0.0f, pz = b.mx.z - b.mn.z < D ? D : 0.0f;
+    return Box{h3(b.mn.x - px, b.mn.y - py, b.mn.z - pz), h3(b.mx.x + px, b.mx.y + py, b.mx.z + pz)};
+}
+static inline float area(const Box& b) {
+    H3 d = b.mx - b.mn;
+    return 2.0f * (d.x * d.y + d.y * d.z + d.z * d.x);
+}
+
+// Reference-layout node (bvh.rs:25-32).
+struct RefNode { float mn[3][8], mx[3][8]; int32_t ch[8]; };
+
+// ── binned-SAH 8-wide builder (cost model of bvh.rs:52-174) ─────────────────
+// In place on an index array: each sah_partition reorders idx[lo, hi) by a
+// stable counting sort on bucket id, which is what the reference's stable
+// `sort_by_key` + `partition_point` does.
+struct SahBuilder {
+    const std::vector<Box>& boxes;
+    std::vector<float> cen[3];
+    std::vector<int32_t> idx, tmp;
+    std::vector<RefNode> nodes;
+    std::vector<int32_t> leaves;
+    int max_depth = 0;
+
+    explicit SahBuilder(const std::vector<Box>& b) : boxes(b) {
+        size_t n = b.size();
+        for (int a = 0; a < 3; a++) {
+            cen[a].resize(n);
+            for (size_t i = 0; i < n; i++) cen[a][i] = (hc(b[i].mn, a) + hc(b[i].mx, a)) * 0.5f;
+        }
+        idx.resize(n);
+        tmp.resize(n);
+        for (size_t i = 0; i < n; i++) idx[i] = (int32_t)i;
+    }
+
+    size_t partition(size_t lo, size_t hi) {
+        const int NB = 12;
+        size_t span = hi - lo;
+        float cmn[3] = {INFINITY, INFINITY, INFINITY}, cmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+        Box nb = boxes[idx[lo]];
+        for (size_t k = lo; k < hi; k++) {
+            int32_t o = idx[k];
+            for (int a = 0; a < 3; a++) { cmn[a] = std::fmin(cmn[a], cen[a][o]); cmx[a] = std::fmax(cmx[a], cen[a][o]); }
+            if (k > lo) nb = unite(nb, boxes[o]);
+        }
+        float nsa = area(nb);
+        float best = INFINITY;
+        int bax = 0, bsp = 0;
+        for (int ax = 0; ax < 3; ax++) {
+            float ext = cmx[ax] - cmn[ax];
+            if (ext < 1e-6f) continue;
+            bool has[NB] = {};
+            Box bb[NB];
+            uint32_t cnt[NB] = {};
+            for (size_t k = lo; k < hi; k++) {
+                int32_t o = idx[k];
+                float t = (cen[ax][o] - cmn[ax]) / ext;
+                int bi = std::min((int)((float)NB * t), NB - 1);
+                cnt[bi]++;
+                bb[bi] = has[bi] ? unite(bb[bi], boxes[o]) : boxes[o];
+                has[bi] = true;
+            }
+            float lsa[NB];
+            uint32_t ln[NB];
+            bool ah = false;
+            Box acc;
+            uint32_t an = 0;
+            for (int i = 0; i < NB; i++) {
+                an += cnt[i];
+                if (has[i]) { acc = ah ? unite(acc, bb[i]) : bb[i]; ah = true; }
+                ln[i] = an;
+                lsa[i] = ah ? area(acc) : 0.0f;
+            }
+            ah = false; an = 0;
+            for (int s = NB - 2; s >= 0; s--) {
+                an += cnt[s + 1];
+                if (has[s + 1]) { acc = ah ? unite(acc, bb[s + 1]) : bb[s + 1]; ah = true; }
+                uint32_t nl = ln[s], nr = an;
+                if (nl == 0 || nr == 0) continue;
+                float rsa = ah ? area(acc) : 0.0f;
+                float cost = 1.0f + (lsa[s] * (float)nl + rsa * (float)nr) / nsa;
+                if (cost < best) { best = cost; bax = ax; bsp = s; }
+            }
+        }
+        float ext = cmx[bax] - cmn[bax];
+        uint32_t cnt[NB] = {};
+        std::vector<uint8_t> bid(span);
+        for (size_t k = lo; k < hi; k++) {
+            int bi = 0;
+            if (!(ext < 1e-6f)) {
+                float t = (cen[bax][idx[k]] - cmn[bax]) / ext;
+                bi = std::min((int)((float)NB * t), NB - 1);
+            }
+            bid[k - lo] = (uint8_t)bi;
+            cnt[bi]++;
+        }
+        uint32_t off[NB];
+        uint32_t run = 0;
+        size_t mid_off = 0;
+        for (int b = 0; b < NB; b++) { off[b] = run; run += cnt[b]; if (b == bsp) mid_off = run; }
+        for (size_t k = lo; k < hi; k++) tmp[lo + off[bid[k - lo]]++] = idx[k];
+        std::copy(tmp.begin() + lo, tmp.begin() + hi, idx.begin() + lo);
+        size_t mid = (mid_off == 0 || mid_off == span) ? span / 2 : mid_off;
+        return lo + mid;
+    }
+
+    void split(size_t lo, size_t hi, int depth, std::vector<std::pair<size_t, size_t>>& out) {
+        if (depth == 3 || hi - lo <= 1) { out.emplace_back(lo, hi); return; }
+        size_t mid = partition(lo, hi);
+        split(lo, mid, depth + 1, out);
+        split(mid, hi, depth + 1, out);
+    }
+
+    int32_t build(size_t lo, size_t hi, Box* out, int depth) {
+        max_depth = std::max(max_depth, depth);
+        if (hi - lo == 1) {
+            int32_t slot = (int32_t)leaves.size();
+            leaves.push_back(idx[lo]);
+            *out = boxes[idx[lo]];
+            return -(slot + 1);
+        }
+        std::vector<std::pair<size_t, size_t>> groups;
+        if (hi - lo <= 8) { for (size_t k = lo; k < hi; k++) groups.emplace_back(k, k + 1); }
+        else split(lo, hi, 0, groups);
+        size_t my = nodes.size();
+        RefNode nd;
+        memset(&nd, 0, sizeof(nd));
+        for (int c = 0; c < 8; c++) nd.ch[c] = INT32_MIN;
+        nodes.push_back(nd);
+        Box nbox{};
+        for (size_t g = 0; g < groups.size(); g++) {
+            Box cb;
+            int32_t c = build(groups[g].first, groups[g].second, &cb, depth + 1);
+            nd.ch[g] = c;
+            for (int a = 0; a < 3; a++) { nd.mn[a][g] = hc(cb.mn, a); nd.mx[a][g] = hc(cb.mx, a); }
+            nbox = g == 0 ? cb : unite(nbox, cb);
+        }
+        nodes[my] = nd;
+        *out = nbox;
+        return (int32_t)my;
+    }
+};
+
+// ── E_ss LUT on the host (material.rs:206-241), once per process ─────────────
+static float g_elut[64 * 64];
+static std::once_flag g_elut_once;
+static void host_vndf(float wx, float wy, float wz, float alpha, float xi1, float xi2, float* m) {
+    const float PI = 3.14159265358979323846f;
+    H3 wh = h3(alpha * wx, alpha * wy, wz);
+    wh = wh / hlen(wh);
+    float len = std::sqrt(wh.x * wh.x + wh.y * wh.y);
+    H3 t1 = len > 1e-6f ? h3(-wh.y / len, wh.x / len, 0.0f) : h3(1, 0, 0);
+    H3 t2 = hcross(wh, t1);
+    float a = 1.0f / (1.0f + wh.z);
+    float r = std::sqrt(xi1);
+    float p1, p2;
+    if (xi2 < a) { float phi = xi2 / a * PI; p1 = r * std::cos(phi); p2 = r * std::sin(phi); }
+    else { float phi = PI + (xi2 - a) / (1.0f - a) * PI; p1 = r * std::cos(phi); p2 = r * std::sin(phi) * wh.z; }
+    float p3 = std::sqrt(std::fmax(1.0f - p1 * p1 - p2 * p2, 0.0f));
+    H3 nh = t1 * p1 + t2 * p2 + wh * p3;
+    H3 mm = h3(alpha * nh.x, alpha * nh.y, std::fmax(nh.z, 0.0f));
+    mm = mm / hlen(mm);
+    m[0] = mm.x; m[1] = mm.y; m[2] = mm.z;
+}
+static float host_lambda(float c, float alpha) {
+    float a2 = alpha * alpha, c2 = c * c;
+    return (std::sqrt(a2 + (1.0f - a2) * c2) - c) / (2.0f * c);
+}
+static void build_elut() {
+    const int N = 64, G = 64;
+    for (int i = 0; i < N; i++) {
+        float mu = ((float)i + 0.5f) / (float)N;
+        for (int j = 0; j < N; j++) {
+            float alpha = std::fmax(((float)j + 0.5f) / (float)N, 1e-3f);
+            float lo = host_lambda(mu, alpha);
+            double sum = 0.0;
+            uint32_t texel = (uint32_t)(i * N + j);
+            for (int k = 0; k < G; k++)
+                for (int l = 0; l < G; l++) {
+                    uint32_t smp = (uint32_t)(k * G + l);
+                    float r1 = (float)(pcg3d_x(texel, smp, 0xE55E0001u) >> 8) * (1.0f / 16777216.0f);
+                    float r2 = (float)(pcg3d_x(texel, smp, 0xE55E0002u) >> 8) * (1.0f / 16777216.0f);
+                    float m[3];
+                    host_vndf(0.0f, 0.0f, mu, alpha, ((float)k + r1) / (float)G, ((float)l + r2) / (float)G, m);
+                    float voh = std::fmax(mu * m[2], 0.0f);
+                    // wi = 2·(wo·m)·m − wo, wo = (0, 0, mu)
+                    float wiz = 2.0f * voh * m[2] - mu;
+                    if (wiz <= 0.0f) continue;
+                    float li = host_lambda(wiz, alpha);
+                    sum += (double)((1.0f + lo) / (1.0f + lo + li));
+                }
+            g_elut[i * N + j] = (float)(sum / (double)(G * G));
+        }
+    }
+}
+
+static void xyz_srgb_h(float x, float y, float z, float o[3]) {
+    o[0] = std::fmax(3.2406f * x - 1.5372f * y - 0.4986f * z, 0.0f);
+    o[1] = std::fmax(-0.9689f * x + 1.8758f * y + 0.0415f * z, 0.0f);
+    o[2] = std::fmax(0.0557f * x - 0.2040f * y + 1.0570f * z, 0.0f);
+}
+static void fire_h(float x, float y, float z, float c[3]) {
+    float w = std::fmax(std::pow(y, 0.5f), 0.08f);
+    float rgb[3];
+    xyz_srgb_h(x, y, z, rgb);
+    for (int k = 0; k < 3; k++) c[k] = rgb[k] * w;
+    float lum = 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2];
+    for (int k = 0; k < 3; k++) c[k] = c[k] * (1.0f - 0.5f) + lum * 0.5f;
+}
+static float planck_h(float l, float tk) {
+    float x = 14388000.0f / (l * tk);
+    float l2 = l * l, l4 = l2 * l2;
+    return 1.0f / (l * l4 * std::fmax(std::exp(x) - 1.0f, 1e-30f));
+}
+
+}  // namespace
+
+// ── the scene handle ────────────────────────────────────────────────────────
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct RtScene {
+    int device = 0, sms = 148;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    DevScene S{};
+    std::vector<DevBuf> owned;
+    int64_t n_nodes = 0, n_leaves = 0;
+    int32_t max_depth = 0;
+    double sah_cost = 0.0;
+    std::vector<RefNode> ref_nodes;   // reference-layout copy for rt_scene_bvh_export
+    std::vector<int32_t> leaf_gids;
+    bool empty = true;
+    // wavefront buffers (grown on demand)
+    uint32_t cap = 0;
+    PathState P{};
+    uint32_t* queue[2] = {nullptr, nullptr};
+    float4* sq = nullptr;
+    uint32_t* counters = nullptr;     // (RT_MAX_DEPTH+2) × RT_CTR_STRIDE
+    int* d_err = nullptr;
+    float* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    uint8_t* d_conv = nullptr;
+    size_t conv_bytes = 0;
+    // accumulators
+    float *acc = nullptr, *m2 = nullptr;
+    uint32_t* cnt = nullptr;
+    uint32_t acc_npix = 0;
+    // api staging
+    void* stage = nullptr;
+    size_t stage_bytes = 0;
+    // per-stage profiling
+    bool profiling = false;
+    std::vector<cudaEvent_t> pev;
+    std::vector<int> pkind;
+    double kms[4] = {0, 0, 0, 0};
+    int64_t kcount[4] = {0, 0, 0, 0};
+    // ray capture (diagnostics)
+    int32_t cap_depth = -1;
+    float* cap_out = nullptr;
+    int64_t cap_max = 0, cap_n = 0;
+    // stats
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    int64_t last_ext = 0, last_shadow = 0, last_launches = 0;
+};
+
+static int fail(RtScene* s, int code, const std::string& msg) {
+    if (s) s->err = msg;
+    return code;
+}
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(s, RT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+static int dalloc(RtScene* s, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+    if (e != cudaSuccess) return fail(s, RT_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    s->owned.push_back(DevBuf{*p, bytes});
+    return RT_OK;
+}
+template <class T>
+static int upload(RtScene* s, const T* src, size_t count, const T** dst) {
+    void* p = nullptr;
+    int rc = dalloc(s, &p, count * sizeof(T));
+    if (rc) return rc;
+    if (count) CK(cudaMemcpy(p, src, count * sizeof(T), cudaMemcpyHostToDevice));
+    *dst = (const T*)p;
+    return RT_OK;
+}
+
+static void free_dev(void*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+extern "C" {
+
+int32_t rt_version(void) { return RT_API_VERSION; }
+
+int32_t rt_device_count(int32_t* count) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+    if (count) *count = n;
+    return RT_OK;
+}
+
+int32_t rt_last_error(const RtScene* s, char* buf, size_t len) {
+    if (!buf || len == 0) return RT_ERR_INVALID;
+    std::string m = s ? s->err : std::string("null scene");
+    size_t n = std::min(len - 1, m.size());
+    memcpy(buf, m.data(), n);
+    buf[n] = 0;
+    return RT_OK;
+}
+
+int32_t rt_scene_destroy(RtScene* s) {
+    if (!s) return RT_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto& b : s->owned) cudaFree(b.p);
+    void* ps[] = {s->P.ray_o, s->P.ray_d, s->P.hit, s->P.thr, s->P.wts, s->P.meta, s->P.L, s->P.pend0, s->P.pend1,
+                  s->queue[0], s->queue[1], s->sq, s->counters, s->d_err, s->scratch, s->d_conv, s->acc, s->m2,
+                  s->cnt, s->stage};
+    for (void* p : ps) if (p) cudaFree(p);
+    for (auto e : s->pev) cudaEventDestroy(e);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return RT_OK;
+}
+
+int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
+    if (!d || !out) return RT_ERR_INVALID;
+    *out = nullptr;
+    RtScene* s = new RtScene();
+    auto bail = [&](int rc) { RtScene* keep = s; *out = keep; return rc; };   // handle kept for rt_last_error
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return bail(fail(s, RT_ERR_CUDA, "no CUDA device"));
+    if (device < 0 || device >= ndev) return bail(fail(s, RT_ERR_INVALID, "device index out of range"));
+    s->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return bail(fail(s, RT_ERR_CUDA, "cudaSetDevice failed"));
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    s->sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(s, RT_ERR_CUDA, "cudaStreamCreate failed"));
+    cudaEventCreate(&s->ev0);
+    cudaEventCreate(&s->ev1);
+
+    // ── validate ────────────────────────────────────────────────────────────
+    if (d->n_tris < 0 || d->n_quads < 0 || d->n_spheres < 0 || d->n_mats < 0 || d->n_lights < 0)
+        return bail(fail(s, RT_ERR_INVALID, "negative count"));
+    int64_t n = d->n_tris + d->n_quads + d->n_spheres;
+    if (n >= (1ll << 28)) return bail(fail(s, RT_ERR_CAPACITY, "more than 2^28 primitives"));
+    if ((d->n_tris && (!d->tri_v || !d->tri_mat)) || (d->n_quads && (!d->quad_quv || !d->quad_mat)) ||
+        (d->n_spheres && (!d->sphere || !d->sphere_mat)) || (d->n_mats && !d->mats) || (d->n_lights && !d->light_prims))
+        return bail(fail(s, RT_ERR_INVALID, "null array with non-zero count"));
+    auto bad_mat = [&](int32_t m) { return m < 0 || m >= d->n_mats; };
+    for (int64_t i = 0; i < d->n_tris; i++) if (bad_mat(d->tri_mat[i])) return bail(fail(s, RT_ERR_INVALID, "triangle material index out of range"));
+    for (int64_t i = 0; i < d->n_quads; i++) if (bad_mat(d->quad_mat[i])) return bail(fail(s, RT_ERR_INVALID, "quad material index out of range"));
+    for (int64_t i = 0; i < d->n_spheres; i++) if (bad_mat(d->sphere_mat[i])) return bail(fail(s, RT_ERR_INVALID, "sphere material index out of range"));
+    for (int32_t i = 0; i < d->n_mats; i++) {
+        const RtMaterial& m = d->mats[i];
+        if (m.type < RT_MAT_LAMBERTIAN || m.type > RT_MAT_BLACKBODY_LIGHT) return bail(fail(s, RT_ERR_INVALID, "unknown material type"));
+        if (m.type == RT_MAT_SPECTRAL_METAL && m.metal == RT_METAL_CUSTOM && (m.nk_count < 2 || m.nk_count > RT_MAX_NK || !(m.nk_step > 0.0f)))
+            return bail(fail(s, RT_ERR_INVALID, "custom conductor table needs 2..16 samples and a positive step"));
+        if (m.type == RT_MAT_SPECTRAL_METAL && (m.metal < RT_METAL_GOLD || m.metal > RT_METAL_CUSTOM))
+            return bail(fail(s, RT_ERR_INVALID, "unknown conductor"));
+    }
+    if (d->n_lights > 4096) return bail(fail(s, RT_ERR_CAPACITY, "more than 4096 NEE lights"));
+    for (int32_t i = 0; i < d->n_lights; i++) {
+        int64_t g = d->light_prims[i];
+        if (g < d->n_tris || g >= n) return bail(fail(s, RT_ERR_INVALID, "light list entries must be quads or spheres"));
+    }
+    if (d->bg.type == RT_BG_ENVMAP && (!d->bg.env_rgb || d->bg.env_w <= 0 || d->bg.env_h <= 0))
+        return bail(fail(s, RT_ERR_INVALID, "env map background without an image"));
+
+    // ── primitive boxes, quad constants (quad.rs:21-33) ─────────────────────
+    std::vector<Box> boxes(n);
+    std::vector<float> qn(d->n_quads * 3), qd(d->n_quads), qw(d->n_quads * 3), qarea(d->n_quads);
+    for (int64_t i = 0; i < d->n_tris; i++) {                                       // triangle.rs:128-140
+        const float* v = d->tri_v + i * 9;
+        H3 a = h3(v[0], v[1], v[2]);
+        H3 e1 = h3(v[3], v[4], v[5]) - a, e2 = h3(v[6], v[7], v[8]) - a;
+        H3 b = a + e1, c = a + e2;
+        Box bb{h3(std::fmin(std::fmin(a.x, b.x), c.x), std::fmin(std::fmin(a.y, b.y), c.y), std::fmin(std::fmin(a.z, b.z), c.z)),
+               h3(std::fmax(std::fmax(a.x, b.x), c.x), std::fmax(std::fmax(a.y, b.y), c.y), std::fmax(std::fmax(a.z, b.z), c.z))};
+        boxes[i] = pad(bb);
+    }
+    for (int64_t i = 0; i < d->n_quads; i++) {
+        const float* q = d->quad_quv + i * 9;
+        H3 Q = h3(q[0], q[1], q[2]), u = h3(q[3], q[4], q[5]), v = h3(q[6], q[7], q[8]);
+        H3 nn = hcross(u, v);
+        float ar = hlen(nn);
+        if (!(ar > 1e-6f * hlen(u) * hlen(v)))
+            return bail(fail(s, RT_ERR_INVALID, "degenerate quad " + std::to_string(i) + ": u and v are parallel or zero"));
+        H3 nrm = nn / ar, w = nn / hdot(nn, nn);
+        qn[i * 3] = nrm.x; qn[i * 3 + 1] = nrm.y; qn[i * 3 + 2] = nrm.z;
+        qd[i] = hdot(nrm, Q);
+        qw[i * 3] = w.x; qw[i * 3 + 1] = w.y; qw[i * 3 + 2] = w.z;
+        qarea[i] = ar;
+        H3 cs[4] = {Q, Q + u, Q + v, Q + u + v};
+        Box bb{cs[0], cs[0]};
+        for (int k = 1; k < 4; k++) bb = unite(bb, Box{cs[k], cs[k]});
+        boxes[d->n_tris + i] = pad(bb);
+    }
+    for (int64_t i = 0; i < d->n_spheres; i++) {
+        const float* p = d->sphere + i * 4;
+        H3 c = h3(p[0], p[1], p[2]), r = h3(p[3], p[3], p[3]);
+        boxes[d->n_tris + d->n_quads + i] = Box{c - r, c + r};
+    }
+
+    // ── BVH ─────────────────────────────────────────────────────────────────
+    std::vector<float4> gnodes;
+    std::vector<float4> gtri, gtri_n, gquad, gsph;
+    if (n > 0) {
+        SahBuilder B(boxes);
+        Box root_box;
+        int32_t root = B.build(0, (size_t)n, &root_box, 0);
+        if (root < 0) {
+            RefNode nd;
+            memset(&nd, 0, sizeof(nd));
+            for (int c = 0; c < 8; c++) nd.ch[c] = INT32_MIN;
+            nd.ch[0] = root;
+            for (int a = 0; a < 3; a++) { nd.mn[a][0] = hc(boxes[0].mn, a); nd.mx[a][0] = hc(boxes[0].mx, a); }
+            B.nodes.push_back(nd);
+        }
+        s->max_depth = B.max_depth;
+        if ((int64_t)B.max_depth * 7 + 8 > RT_STACK)
+            return bail(fail(s, RT_ERR_CAPACITY, "BVH depth " + std::to_string(B.max_depth) + " exceeds the traversal stack"));
+        // SAH cost of the tree: Σ_inner area(node)/area(root) + Σ_leaf area(leaf)/area(root)
+        s->ref_nodes = std::move(B.nodes);
+        s->leaf_gids = std::move(B.leaves);
+        s->n_nodes = (int64_t)s->ref_nodes.size();
+        s->n_leaves = (int64_t)s->leaf_gids.size();
+        // leaf order per type
+        std::vector<int32_t> typed_slot(s->n_leaves);
+        std::vector<int64_t> order_tri, order_quad, order_sph;
+        for (int64_t k = 0; k < s->n_leaves; k++) {
+            int64_t g = s->leaf_gids[k];
+            if (g < d->n_tris) { typed_slot[k] = (int32_t)order_tri.size(); order_tri.push_back(g); }
+            else if (g < d->n_tris + d->n_quads) { typed_slot[k] = (int32_t)order_quad.size(); order_quad.push_back(g - d->n_tris); }
+            else { typed_slot[k] = (int32_t)order_sph.size(); order_sph.push_back(g - d->n_tris - d->n_quads); }
+        }
+        double root_sa = 0.0;
+        gnodes.resize((size_t)s->n_nodes * 14);
+        for (int64_t k = 0; k < s->n_nodes; k++) {
+            const RefNode& r = s->ref_nodes[k];
+            float* f = reinterpret_cast<float*>(&gnodes[(size_t)k * 14]);
+            for (int a = 0; a < 3; a++)
+                for (int c = 0; c < 8; c++) { f[a * 8 + c] = r.mn[a][c]; f[24 + a * 8 + c] = r.mx[a][c]; }
+            uint32_t* ch = reinterpret_cast<uint32_t*>(f + 48);
+            for (int c = 0; c < 8; c++) {
+                int32_t v = r.ch[c];
+                if (v == INT32_MIN) ch[c] = RT_EMPTY_REF;
+                else if (v >= 0) ch[c] = (uint32_t)v;
+                else {
+                    int64_t slot = -(int64_t)v - 1;
+                    int64_t g = s->leaf_gids[slot];
+                    uint32_t type = g < d->n_tris ? RT_PRIM_TRI : (g < d->n_tris + d->n_quads ? RT_PRIM_QUAD : RT_PRIM_SPHERE);
+                    ch[c] = RT_LEAF_BIT | (type << 28) | (uint32_t)typed_slot[slot];
+                }
+            }
+        }
+        {   // SAH cost (for statistics): inner nodes cost 1 per traversal, leaves 1 per test
+            Box rb{h3(INFINITY, INFINITY, INFINITY), h3(-INFINITY, -INFINITY, -INFINITY)};
+            const RefNode& r0 = s->ref_nodes[0];
+            for (int c = 0; c < 8; c++) if (r0.ch[c] != INT32_MIN)
+                rb = unite(rb, Box{h3(r0.mn[0][c], r0.mn[1][c], r0.mn[2][c]), h3(r0.mx[0][c], r0.mx[1][c], r0.mx[2][c])});
+            root_sa = area(rb);
+            double cost = 0.0;
+            for (int64_t k = 0; k < s->n_nodes; k++) {
+                const RefNode& r = s->ref_nodes[k];
+                Box nb{h3(INFINITY, INFINITY, INFINITY), h3(-INFINITY, -INFINITY, -INFINITY)};
+                for (int c = 0; c < 8; c++) if (r.ch[c] != INT32_MIN) {
+                    Box cb{h3(r.mn[0][c], r.mn[1][c], r.mn[2][c]), h3(r.mx[0][c], r.mx[1][c], r.mx[2][c])};
+                    nb = unite(nb, cb);
+                    if (r.ch[c] < 0) cost += (double)area(cb) / root_sa;
+                }
+                cost += (double)area(nb) / root_sa;
+            }
+            s->sah_cost = cost;
+        }
+        // primitive records in leaf order
+        gtri.resize(order_tri.size() * 3);
+        bool has_n = d->tri_n != nullptr;
+        if (has_n) gtri_n.resize(order_tri.size() * 3);
+        for (size_t k = 0; k < order_tri.size(); k++) {
+            int64_t g = order_tri[k];
+            const float* v = d->tri_v + g * 9;
+            H3 a = h3(v[0], v[1], v[2]);
+            H3 e1 = h3(v[3], v[4], v[5]) - a, e2 = h3(v[6], v[7], v[8]) - a;
+            gtri[k * 3] = make_float4(a.x, a.y, a.z, e1.x);
+            gtri[k * 3 + 1] = make_float4(e1.y, e1.z, e2.x, e2.y);
+            int32_t gi = (int32_t)g, mi = d->tri_mat[g], hn = has_n ? 1 : 0;
+            float fg, fm, fh;
+            memcpy(&fg, &gi, 4); memcpy(&fm, &mi, 4); memcpy(&fh, &hn, 4);
+            gtri[k * 3 + 2] = make_float4(e2.z, fg, fm, fh);
+            if (has_n) {
+                const float* nn = d->tri_n + g * 9;
+                gtri_n[k * 3] = make_float4(nn[0], nn[1], nn[2], nn[3]);
+                gtri_n[k * 3 + 1] = make_float4(nn[4], nn[5], nn[6], nn[7]);
+                gtri_n[k * 3 + 2] = make_float4(nn[8], 0.f, 0.f, 0.f);
+            }
+        }
+        auto quad_rec = [&](int64_t qi, float4* out5, int32_t gid) {
+            const float* q = d->quad_quv + qi * 9;
+            out5[0] = make_float4(qn[qi * 3], qn[qi * 3 + 1], qn[qi * 3 + 2], qd[qi]);
+            out5[1] = make_float4(q[0], q[1], q[2], q[3]);
+            out5[2] = make_float4(q[4], q[5], q[6], q[7]);
+            out5[3] = make_float4(q[8], qw[qi * 3], qw[qi * 3 + 1], qw[qi * 3 + 2]);
+            int32_t mi = d->quad_mat[qi];
+            float fg, fm;
+            memcpy(&fg, &gid, 4); memcpy(&fm, &mi, 4);
+            out5[4] = make_float4(fg, fm, qarea[qi], 0.f);
+        };
+        gquad.resize(order_quad.size() * 5);
+        for (size_t k = 0; k < order_quad.size(); k++)
+            quad_rec(order_quad[k], &gquad[k * 5], (int32_t)(d->n_tris + order_quad[k]));
+        gsph.resize(order_sph.size() * 2);
+        for (size_t k = 0; k < order_sph.size(); k++) {
+            int64_t si = order_sph[k];
+            const float* p = d->sphere + si * 4;
+            int32_t gi = (int32_t)(d->n_tris + d->n_quads + si), mi = d->sphere_mat[si];
+            float fg, fm;
+            memcpy(&fg, &gi, 4); memcpy(&fm, &mi, 4);
+            gsph[k * 2] = make_float4(p[0], p[1], p[2], p[3]);
+            gsph[k * 2 + 1] = make_float4(fg, fm, 0.f, 0.f);
+        }
+        // lights
+        std::vector<DevLight> lights(d->n_lights);
+        for (int32_t i = 0; i < d->n_lights; i++) {
+            int64_t g = d->light_prims[i];
+            DevLight& L = lights[i];
+            memset(&L, 0, sizeof(L));
+            if (g < d->n_tris + d->n_quads) {
+                int64_t qi = g - d->n_tris;
+                L.type = RT_PRIM_QUAD;
+                L.mat = d->quad_mat[qi];
+                quad_rec(qi, L.g, (int32_t)g);
+            } else {
+                int64_t si = g - d->n_tris - d->n_quads;
+                const float* p = d->sphere + si * 4;
+                L.type = RT_PRIM_SPHERE;
+                L.mat = d->sphere_mat[si];
+                L.g[0] = make_float4(p[0], p[1], p[2], p[3]);
+            }
+        }
+        int rc;
+        if ((rc = upload(s, gnodes.data(), gnodes.size(), &s->S.nodes))) return bail(rc);
+        if ((rc = upload(s, gtri.data(), gtri.size(), &s->S.tri))) return bail(rc);
+        if ((rc = upload(s, gtri_n.data(), gtri_n.size(), &s->S.tri_n))) return bail(rc);
+        if ((rc = upload(s, gquad.data(), gquad.size(), &s->S.quad))) return bail(rc);
+        if ((rc = upload(s, gsph.data(), gsph.size(), &s->S.sphere))) return bail(rc);
+        if ((rc = upload(s, lights.data(), lights.size(), &s->S.lights))) return bail(rc);
+        s->S.n_lights = d->n_lights;
+        s->empty = false;
+    }
+
+    // ── spectral tables (spectrum.rs:78-177) ────────────────────────────────
+    int nspec = d->spectral_range ? RT_CIE_N + RT_CIE_EXT_N : RT_CIE_N;
+    std::vector<float4> cmf(nspec);
+    float sum[3] = {0, 0, 0}, fsum[3] = {0, 0, 0};
+    for (int i = 0; i < nspec; i++) {
+        const float* x = i < RT_CIE_N ? RT_CIE_XYZ[i] : RT_CIE_XYZ_EXT[i - RT_CIE_N];
+        cmf[i] = make_float4(x[0], x[1], x[2], 0.f);
+        float rgb[3], fc[3];
+        xyz_srgb_h(x[0], x[1], x[2], rgb);
+        fire_h(x[0], x[1], x[2], fc);
+        for (int k = 0; k < 3; k++) { sum[k] += rgb[k]; fsum[k] += fc[k]; }
+    }
+    for (int k = 0; k < 3; k++) {
+        s->S.norms[k] = (float)nspec / std::fmax(sum[k], 1e-6f);
+        s->S.fire_norms[k] = (float)nspec / std::fmax(fsum[k], 1e-6f);
+    }
+    s->S.n_spec = nspec;
+    s->S.lam_lo = 380.0f;
+    s->S.lam_range = d->spectral_range ? 400.0f : 320.0f;
+    int rc;
+    if ((rc = upload(s, cmf.data(), cmf.size(), &s->S.cmf))) return bail(rc);
+
+    // ── materials (+ blackbody constants, material.rs:47-62) ─────────────────
+    std::vector<DevMaterial> mats(std::max(d->n_mats, 1));
+    for (int32_t i = 0; i < d->n_mats; i++) {
+        const RtMaterial& m = d->mats[i];
+        DevMaterial& g = mats[i];
+        memset(&g, 0, sizeof(g));
+        g.type = m.type;
+        g.metal = m.metal;
+        for (int k = 0; k < 3; k++) { g.albedo[k] = m.albedo[k]; g.odd[k] = m.odd[k]; g.absorption[k] = m.absorption[k]; }
+        g.checker_scale = m.checker_scale;
+        g.cauchy_b = m.cauchy_b;
+        g.cauchy_c = m.cauchy_c;
+        g.roughness = m.roughness;
+        g.temp_k = m.temp_k;
+        g.intensity = m.intensity;
+        if (m.type == RT_MAT_SPECTRAL_METAL) {
+            if (m.metal == RT_METAL_CUSTOM) {
+                g.nk_count = m.nk_count; g.nk_start = m.nk_start; g.nk_step = m.nk_step;
+                for (int k = 0; k < m.nk_count; k++) { g.nk_n[k] = m.nk_n[k]; g.nk_k[k] = m.nk_k[k]; }
+            } else {
+                g.nk_count = RT_METAL_NK_N; g.nk_start = RT_METAL_NK_START; g.nk_step = RT_METAL_NK_STEP;
+                for (int k = 0; k < RT_METAL_NK_N; k++) { g.nk_n[k] = RT_METAL_NK[m.metal][0][k]; g.nk_k[k] = RT_METAL_NK[m.metal][1][k]; }
+            }
+        }
+        if (m.type == RT_MAT_BLACKBODY_LIGHT) {
+            std::vector<float> raw(nspec);
+            float su = 0.0f;
+            for (int k = 0; k < nspec; k++) { raw[k] = planck_h(380.0f + (float)k * 5.0f, m.temp_k); su += raw[k]; }
+            float norm = 1.0f / std::fmax(su / (float)nspec, 1e-30f);
+            float acc[3] = {0, 0, 0};
+            for (int k = 0; k < nspec; k++) {
+                // spectral_to_rgb at the grid wavelength: t is exact, frac = 0
+                int kk = std::min(k, nspec - 2);
+                float frac = (float)k - (float)kk;
+                float xyz[3];
+                const float4 a = cmf[kk], b = cmf[kk + 1];
+                xyz[0] = a.x + frac * (b.x - a.x);
+                xyz[1] = a.y + frac * (b.y - a.y);
+                xyz[2] = a.z + frac * (b.z - a.z);
+                float rgb[3];
+                xyz_srgb_h(xyz[0], xyz[1], xyz[2], rgb);
+                for (int c = 0; c < 3; c++) acc[c] = acc[c] + (rgb[c] * s->S.norms[c]) * (raw[k] * norm);
+            }
+            g.bb_norm = norm;
+            for (int c = 0; c < 3; c++) g.bb_avg[c] = acc[c] / (float)nspec * m.intensity;
+        }
+    }
+    if ((rc = upload(s, mats.data(), mats.size(), &s->S.mats))) return bail(rc);
+    s->S.n_mats = d->n_mats;
+
+    std::call_once(g_elut_once, build_elut);
+    if ((rc = upload(s, g_elut, (size_t)64 * 64, &s->S.elut))) return bail(rc);
+
+    // ── background + env alias table (renderer.rs:32-74) ────────────────────
+    const RtBackground& bg = d->bg;
+    s->S.bg_type = bg.type;
+    s->S.vis_type = bg.type == RT_BG_ENVMAP ? bg.visible_type : -1;
+    for (int k = 0; k < 3; k++) {
+        s->S.bg_color[k] = bg.color[k]; s->S.bg_top[k] = bg.top[k]; s->S.bg_bottom[k] = bg.bottom[k];
+        s->S.vis_color[k] = bg.visible_color[k]; s->S.vis_top[k] = bg.visible_top[k]; s->S.vis_bottom[k] = bg.visible_bottom[k];
+    }
+    if (bg.type == RT_BG_ENVMAP) {
+        int W = bg.env_w, Hh = bg.env_h;
+        size_t N = (size_t)W * Hh;
+        std::vector<float4> env(N);
+        std::vector<double> wgt(N);
+        const float PI = 3.14159265358979323846f;
+        float total = 0.0f;
+        for (int j = 0; j < Hh; j++) {
+            float sin_j = std::sin(PI * ((float)j + 0.5f) / (float)Hh);
+            float rs = 0.0f;
+            for (int i = 0; i < W; i++) {
+                const float* p = bg.env_rgb + ((size_t)j * W + i) * 3;
+                float lum = 0.2126f * p[0] + 0.7152f * p[1] + 0.0722f * p[2];
+                env[(size_t)j * W + i] = make_float4(p[0], p[1], p[2], lum);
+                rs += lum * sin_j;
+                wgt[(size_t)j * W + i] = (double)lum * (double)sin_j;
+            }
+            total += rs;
+        }
+        // Vose's alias method over the texel weights lum·sinθ.
+        std::vector<float2> alias(N);
+        double wsum = 0.0;
+        for (double x : wgt) wsum += x;
+        if (!(wsum > 0.0)) { for (auto& x : wgt) x = 1.0; wsum = (double)N; }
+        std::vector<double> q(N);
+        std::vector<uint32_t> small, large;
+        small.reserve(N); large.reserve(N);
+        for (size_t k = 0; k < N; k++) {
+            q[k] = wgt[k] * (double)N / wsum;
+            (q[k] < 1.0 ? small : large).push_back((uint32_t)k);
+        }
+        std::vector<uint32_t> al(N);
+        for (size_t k = 0; k < N; k++) al[k] = (uint32_t)k;
+        while (!small.empty() && !large.empty()) {
+            uint32_t sm = small.back(); small.pop_back();
+            uint32_t lg = large.back();
+            al[sm] = lg;
+            q[lg] = (q[lg] + q[sm]) - 1.0;
+            if (q[lg] < 1.0) { large.pop_back(); small.push_back(lg); }
+        }
+        for (uint32_t k : large) q[k] = 1.0;
+        for (uint32_t k : small) q[k] = 1.0;
+        for (size_t k = 0; k < N; k++) {
+            float fa;
+            uint32_t a = al[k];
+            memcpy(&fa, &a, 4);
+            alias[k] = make_float2((float)q[k], fa);
+        }
+        if ((rc = upload(s, env.data(), env.size(), &s->S.env))) return bail(rc);
+        if ((rc = upload(s, alias.data(), alias.size(), &s->S.env_alias))) return bail(rc);
+        s->S.has_env = 1;
+        s->S.env_w = W;
+        s->S.env_h = Hh;
+        s->S.env_inv_total = total > 0.0f ? 1.0f / total : 0.0f;
+        float rot = bg.env_rot_y_deg * (PI / 180.0f);
+        s->S.env_sin_r = std::sin(rot);
+        s->S.env_cos_r = std::cos(rot);
+    }
+    if (cudaMalloc(&s->d_err, sizeof(int)) != cudaSuccess) return bail(fail(s, RT_ERR_NOMEM, "cudaMalloc"));
+    cudaMemset(s->d_err, 0, sizeof(int));
+    *out = s;
+    return RT_OK;
+}
+
+int32_t rt_scene_bvh_stats(const RtScene* s, int64_t* n_nodes, int64_t* n_leaves, int32_t* max_depth, double* sah) {
+    if (!s) return RT_ERR_INVALID;
+    if (n_nodes) *n_nodes = s->n_nodes;
+    if (n_leaves) *n_leaves = s->n_leaves;
+    if (max_depth) *max_depth = s->max_depth;
+    if (sah) *sah = s->sah_cost;
+    return RT_OK;
+}
+
+int32_t rt_scene_bvh_export(const RtScene* s, float* nodes, int64_t* n_nodes, int32_t* leaf, int64_t* n_leaves) {
+    if (!s) return RT_ERR_INVALID;
+    if (n_nodes) *n_nodes = s->n_nodes;
+    if (n_leaves) *n_leaves = s->n_leaves;
+    if (nodes) memcpy(nodes, s->ref_nodes.data(), s->ref_nodes.size() * sizeof(RefNode));
+    if (leaf) memcpy(leaf, s->leaf_gids.data(), s->leaf_gids.size() * sizeof(int32_t));
+    return RT_OK;
+}
+
+}  // extern "C"
+
+// ── helpers for the API calls ───────────────────────────────────────────────
+static int ensure_stage(RtScene* s, size_t bytes) {
+    if (s->stage_bytes >= bytes) return RT_OK;
+    free_dev(s->stage);
+    s->stage_bytes = 0;
+    if (cudaMalloc(&s->stage, bytes) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc staging");
+    s->stage_bytes = bytes;
+    return RT_OK;
+}
+static int check_err(RtScene* s) {
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (h) {
+        cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream);
+        return fail(s, h, h == RT_ERR_CAPACITY ? "traversal stack overflow" : "device error");
+    }
+    return RT_OK;
+}
+
+extern "C" int32_t rt_trace_closest(RtScene* s, const float* rays, int64_t n, RtHit* hits, int32_t mem) {
+    if (!s || (n > 0 && (!rays || !hits))) return RT_ERR_INVALID;
+    if (n <= 0) return RT_OK;
+    if (n > 0xFFFFFFF0ll) return fail(s, RT_ERR_CAPACITY, "too many rays");
+    CK(cudaSetDevice(s->device));
+    if (s->empty) {
+        if (mem == RT_MEM_DEVICE) { CK(cudaMemsetAsync(hits, 0xFF, n * sizeof(RtHit), s->stream)); return RT_OK; }
+        for (int64_t i = 0; i < n; i++) hits[i] = RtHit{-1, 0.f, 0.f, 0.f};
+        return RT_OK;
+    }
+    const float* drays = rays;
+    int4* dout = reinterpret_cast<int4*>(hits);
+    size_t rb = (size_t)n * 8 * sizeof(float), hb = (size_t)n * sizeof(RtHit);
+    if (mem != RT_MEM_DEVICE) {
+        int rc = ensure_stage(s, rb + hb + 256);
+        if (rc) return rc;
+        drays = (const float*)s->stage;
+        dout = (int4*)((char*)s->stage + ((rb + 255) & ~(size_t)255));
+        CK(cudaMemcpyAsync((void*)drays, rays, rb, cudaMemcpyHostToDevice, s->stream));
+    }
+    uint32_t* next;
+    if (!s->counters) {
+        if (cudaMalloc(&s->counters, sizeof(uint32_t) * (RT_MAX_DEPTH + 2) * RT_CTR_STRIDE) != cudaSuccess)
+            return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
+    }
+    next = s->counters;
+    CK(cudaMemsetAsync(next, 0, sizeof(uint32_t), s->stream));
+    rth::launch_trace_closest_api(s->S, drays, (uint32_t)n, dout, next, s->d_err, s->sms, s->stream);
+    CK(cudaGetLastError());
+    if (mem != RT_MEM_DEVICE) CK(cudaMemcpyAsync(hits, dout, hb, cudaMemcpyDeviceToHost, s->stream));
+    return check_err(s);
+}
+
+extern "C" int32_t rt_trace_any(RtScene* s, const float* rays, int64_t n, uint8_t* occ, int32_t mem) {
+    if (!s || (n > 0 && (!rays || !occ))) return RT_ERR_INVALID;
+    if (n <= 0) return RT_OK;
+    CK(cudaSetDevice(s->device));
+    if (s->empty) {
+        if (mem == RT_MEM_DEVICE) { CK(cudaMemsetAsync(occ, 0, n, s->stream)); return RT_OK; }
+        memset(occ, 0, n);
+        return RT_OK;
+    }
+    const float* drays = rays;
+    uint8_t* dout = occ;
+    size_t rb = (size_t)n * 8 * sizeof(float);
+    if (mem != RT_MEM_DEVICE) {
+        int rc = ensure_stage(s, rb + n + 256);
+        if (rc) return rc;
+        drays = (const float*)s->stage;
+        dout = (uint8_t*)((char*)s->stage + ((rb + 255) & ~(size_t)255));
+        CK(cudaMemcpyAsync((void*)drays, rays, rb, cudaMemcpyHostToDevice, s->stream));
+    }
+    if (!s->counters) {
+        if (cudaMalloc(&s->counters, sizeof(uint32_t) * (RT_MAX_DEPTH + 2) * RT_CTR_STRIDE) != cudaSuccess)
+            return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
+    }
+    CK(cudaMemsetAsync(s->counters, 0, sizeof(uint32_t), s->stream));
+    rth::launch_trace_any_api(s->S, drays, (uint32_t)n, dout, s->counters, s->d_err, s->sms, s->stream);
+    CK(cudaGetLastError());
+    if (mem != RT_MEM_DEVICE) CK(cudaMemcpyAsync(occ, dout, n, cudaMemcpyDeviceToHost, s->stream));
+    return check_err(s);
+}
+
+// ── render loop ─────────────────────────────────────────────────────────────
+static const uint32_t MAX_PATHS = 1u << 22;   // 4M paths in flight per chunk
+
+static int ensure_paths(RtScene* s, uint32_t cap) {
+    if (s->cap >= cap) return RT_OK;
+    void* ps[] = {s->P.ray_o, s->P.ray_d, s->P.hit, s->P.thr, s->P.wts, s->P.meta, s->P.L, s->P.pend0, s->P.pend1,
+                  s->queue[0], s->queue[1], s->sq};
+    for (void* p : ps) if (p) cudaFree(p);
+    s->P = PathState{};
+    s->queue[0] = s->queue[1] = nullptr;
+    s->sq = nullptr;
+    s->cap = 0;
+    size_t f4 = (size_t)cap * sizeof(float4);
+    void** slots[] = {(void**)&s->P.ray_o, (void**)&s->P.ray_d, (void**)&s->P.hit, (void**)&s->P.thr, (void**)&s->P.wts,
+                      (void**)&s->P.meta, (void**)&s->P.L, (void**)&s->P.pend0, (void**)&s->P.pend1};
+    for (void** sl : slots)
+        if (cudaMalloc(sl, f4) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc path state");
+    if (cudaMalloc(&s->queue[0], (size_t)cap * 4) != cudaSuccess || cudaMalloc(&s->queue[1], (size_t)cap * 4) != cudaSuccess ||
+        cudaMalloc(&s->sq, (size_t)cap * 2 * 2 * sizeof(float4)) != cudaSuccess)
+        return fail(s, RT_ERR_NOMEM, "cudaMalloc queues");
+    if (!s->counters && cudaMalloc(&s->counters, sizeof(uint32_t) * (RT_MAX_DEPTH + 2) * RT_CTR_STRIDE) != cudaSuccess)
+        return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
+    s->cap = cap;
+    return RT_OK;
+}
+
+// Renders params->n_samples passes into the device buffer `dscratch`
+// (n_samples × npix × 3), in chunks of as many samples as fit MAX_PATHS.
+static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p, float* dscratch, const uint8_t* dconv,
+                         int64_t* ext_rays, int64_t* sh_rays, int64_t* launches) {
+    uint32_t npix = p->width * p->height;
+    uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
+    uint32_t per = std::max<uint32_t>(1, std::min<uint32_t>(nsamp, MAX_PATHS / std::max<uint32_t>(npix, 1)));
+    uint32_t cap = (uint32_t)std::min<uint64_t>((uint64_t)per * npix, (uint64_t)std::max<uint32_t>(npix, 1) * per);
+    int rc = ensure_paths(s, cap);
+    if (rc) return rc;
+    uint32_t maxd = std::min<uint32_t>(p->max_depth, RT_MAX_DEPTH);
+    std::vector<uint32_t> hc((size_t)(RT_MAX_DEPTH + 2) * RT_CTR_STRIDE);
+    for (int k = 0; k < 4; k++) { s->kms[k] = 0.0; s->kcount[k] = 0; }
+    int64_t ext = 0, sh = 0, nl = 0;
+    for (uint32_t k0 = 0; k0 < nsamp; k0 += per) {
+        RenderLaunch R{};
+        R.width = p->width; R.height = p->height; R.npix = npix;
+        R.nsamp = std::min(per, nsamp - k0);
+        R.sample_idx = p->sample_idx + k0;
+        R.strata = p->strata;
+        R.max_depth = maxd;
+        R.hero = std::max<uint32_t>(1, std::min<uint32_t>(p->hero_count, 4));
+        R.bg_scale = p->bg_scale;
+        R.seed = p->seed;
+        R.cam = *cam;
+        R.converged = dconv;
+        R.scratch = dscratch + (size_t)k0 * npix * 3;
+        CK(cudaMemsetAsync(s->counters, 0, sizeof(uint32_t) * (maxd + 2) * RT_CTR_STRIDE, s->stream));
+        uint32_t* C = s->counters;
+        size_t ev_used = 0;
+        auto mark = [&](int kind) {
+            if (!s->profiling) return;
+            if (ev_used >= s->pev.size()) { cudaEvent_t e; cudaEventCreate(&e); s->pev.push_back(e); s->pkind.push_back(0); }
+            s->pkind[ev_used] = kind;
+            cudaEventRecord(s->pev[ev_used++], s->stream);
+        };
+        mark(0);
+        rth::launch_generate(s->S, s->P, R, s->queue[0], C + 0, s->stream);
+        nl++;
+        for (uint32_t dpt = 0; dpt < maxd; dpt++) {
+            uint32_t* c = C + dpt * RT_CTR_STRIDE;
+            uint32_t* cn = C + (dpt + 1) * RT_CTR_STRIDE;
+            uint32_t* qin = s->queue[dpt & 1];
+            uint32_t* qout = s->queue[(dpt + 1) & 1];
+            mark(1);
+            rth::launch_extend(s->S, s->P, qin, c + 0, c + 1, s->d_err, s->sms, s->stream);
+            if ((int32_t)dpt == s->cap_depth && s->cap_out) {
+                // diagnostics: copy this bounce's rays out (origin, direction) before shade moves them
+                CK(cudaStreamSynchronize(s->stream));
+                uint32_t cnt = 0;
+                CK(cudaMemcpy(&cnt, c + 0, 4, cudaMemcpyDeviceToHost));
+                int64_t m = std::min<int64_t>(cnt, s->cap_max);
+                std::vector<uint32_t> q(m);
+                std::vector<float4> ro(cap), rd(cap);
+                CK(cudaMemcpy(q.data(), qin, m * 4, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(ro.data(), s->P.ray_o, (size_t)cap * 16, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(rd.data(), s->P.ray_d, (size_t)cap * 16, cudaMemcpyDeviceToHost));
+                for (int64_t i = 0; i < m; i++) {
+                    float* r = s->cap_out + i * 8;
+                    float4 a = ro[q[i]], b = rd[q[i]];
+                    r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = b.x; r[4] = b.y; r[5] = b.z; r[6] = 0.001f; r[7] = INFINITY;
+                }
+                s->cap_n = m;
+            }
+            mark(2);
+            rth::launch_shade(s->S, s->P, R, dpt, qin, c + 0, c + 2, qout, cn + 0, s->sq, c + 3, s->sms, s->stream);
+            mark(3);
+            rth::launch_shadow(s->S, s->P, s->sq, c + 3, c + 4, s->d_err, s->sms, s->stream);
+            nl += 3;
+        }
+        mark(0);
+        rth::launch_finalize(s->P, R, s->stream);
+        mark(0);
+        nl++;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hc.data(), s->counters, sizeof(uint32_t) * (maxd + 2) * RT_CTR_STRIDE, cudaMemcpyDeviceToHost,
+                           s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        for (uint32_t dpt = 0; dpt < maxd; dpt++) { ext += hc[dpt * RT_CTR_STRIDE]; sh += hc[dpt * RT_CTR_STRIDE + 3]; }
+        if (s->profiling) {
+            for (size_t e = 0; e + 1 < ev_used; e++) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, s->pev[e], s->pev[e + 1]);
+                int kind = s->pkind[e];
+                s->kms[kind] += ms;
+                if (!(kind == 0 && e > 0 && s->pkind[e - 1] == 0)) s->kcount[kind]++;
+            }
+        }
+    }
+    if (ext_rays) *ext_rays = ext;
+    if (sh_rays) *sh_rays = sh;
+    if (launches) *launches = nl;
+    return RT_OK;
+}
+
+static int validate_pass(RtScene* s, const RtCamera* cam, const RtPassParams* p) {
+    if (!s || !cam || !p) return RT_ERR_INVALID;
+    if (p->width == 0 || p->height == 0) return fail(s, RT_ERR_INVALID, "zero image size");
+    if ((uint64_t)p->width * p->height > (1ull << 26)) return fail(s, RT_ERR_CAPACITY, "image larger than 2^26 pixels");
+    if (p->max_depth == 0 || p->max_depth > RT_MAX_DEPTH) return fail(s, RT_ERR_INVALID, "max_depth must be in 1..256");
+    if (s->empty) return fail(s, RT_ERR_INVALID, "scene has no primitives");
+    return RT_OK;
+}
+
+static int stage_conv(RtScene* s, const uint8_t* conv, size_t npix, int32_t mem, const uint8_t** dconv) {
+    *dconv = nullptr;
+    if (!conv) return RT_OK;
+    if (mem == RT_MEM_DEVICE) { *dconv = conv; return RT_OK; }
+    if (s->conv_bytes < npix) {
+        free_dev((void*&)s->d_conv);
+        if (cudaMalloc(&s->d_conv, npix) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc converged mask");
+        s->conv_bytes = npix;
+    }
+    CK(cudaMemcpyAsync(s->d_conv, conv, npix, cudaMemcpyHostToDevice, s->stream));
+    *dconv = s->d_conv;
+    return RT_OK;
+}
+
+extern "C" int32_t rt_render_pass(RtScene* s, const RtCamera* cam, const RtPassParams* p, float* scratch,
+                                  const uint8_t* converged, int32_t mem) {
+    int rc = validate_pass(s, cam, p);
+    if (rc) return rc;
+    if (!scratch) return fail(s, RT_ERR_INVALID, "null scratch");
+    CK(cudaSetDevice(s->device));
+    size_t npix = (size_t)p->width * p->height;
+    uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
+    size_t bytes = (size_t)nsamp * npix * 3 * sizeof(float);
+    float* dst = scratch;
+    if (mem != RT_MEM_DEVICE) {
+        if (s->scratch_bytes < bytes) {
+            free_dev((void*&)s->scratch);
+            s->scratch_bytes = 0;
+            if (cudaMalloc(&s->scratch, bytes) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc scratch");
+            s->scratch_bytes = bytes;
+        }
+        dst = s->scratch;
+    }
+    const uint8_t* dconv;
+    if ((rc = stage_conv(s, converged, npix, mem, &dconv))) return rc;
+    CK(cudaEventRecord(s->ev0, s->stream));
+    rc = render_device(s, cam, p, dst, dconv, &s->last_ext, &s->last_shadow, &s->last_launches);
+    if (rc) return rc;
+    CK(cudaEventRecord(s->ev1, s->stream));
+    if (mem != RT_MEM_DEVICE) CK(cudaMemcpyAsync(scratch, dst, bytes, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaEventSynchronize(s->ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    s->last_ms = ms;
+    return check_err(s);
+}
+
+extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const RtPassParams* p, float clamp,
+                                        uint32_t min_samples, float floor_, int32_t reset, float* out_sum,
+                                        float* out_m2, uint32_t* out_count, int32_t mem) {
+    int rc = validate_pass(s, cam, p);
+    if (rc) return rc;
+    CK(cudaSetDevice(s->device));
+    uint32_t npix = p->width * p->height;
+    if (s->acc_npix != npix) {
+        free_dev((void*&)s->acc); free_dev((void*&)s->m2); free_dev((void*&)s->cnt);
+        if (cudaMalloc(&s->acc, (size_t)npix * 12) != cudaSuccess || cudaMalloc(&s->m2, (size_t)npix * 12) != cudaSuccess ||
+            cudaMalloc(&s->cnt, (size_t)npix * 4) != cudaSuccess)
+            return fail(s, RT_ERR_NOMEM, "cudaMalloc accumulators");
+        s->acc_npix = npix;
+        reset = 1;
+    }
+    if (reset) {
+        CK(cudaMemsetAsync(s->acc, 0, (size_t)npix * 12, s->stream));
+        CK(cudaMemsetAsync(s->m2, 0, (size_t)npix * 12, s->stream));
+        CK(cudaMemsetAsync(s->cnt, 0, (size_t)npix * 4, s->stream));
+    }
+    uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
+    uint32_t per = std::max<uint32_t>(1, std::min<uint32_t>(nsamp, MAX_PATHS / npix));
+    size_t bytes = (size_t)per * npix * 3 * sizeof(float);
+    if (s->scratch_bytes < bytes) {
+        free_dev((void*&)s->scratch);
+        s->scratch_bytes = 0;
+        if (cudaMalloc(&s->scratch, bytes) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc scratch");
+        s->scratch_bytes = bytes;
+    }
+    CK(cudaEventRecord(s->ev0, s->stream));
+    int64_t ext = 0, sh = 0, nl = 0;
+    for (uint32_t k0 = 0; k0 < nsamp; k0 += per) {
+        RtPassParams q = *p;
+        q.sample_idx = p->sample_idx + k0;
+        q.n_samples = std::min(per, nsamp - k0);
+        int64_t e1, s1, l1;
+        rc = render_device(s, cam, &q, s->scratch, nullptr, &e1, &s1, &l1);
+        if (rc) return rc;
+        rth::launch_accumulate(s->scratch, q.n_samples, npix, s->acc, s->m2, s->cnt, nullptr, clamp, min_samples, floor_,
+                               s->stream);
+        ext += e1; sh += s1; nl += l1 + 1;
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(s->ev1, s->stream));
+    auto kind = mem == RT_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (out_sum) CK(cudaMemcpyAsync(out_sum, s->acc, (size_t)npix * 12, kind, s->stream));
+    if (out_m2) CK(cudaMemcpyAsync(out_m2, s->m2, (size_t)npix * 12, kind, s->stream));
+    if (out_count) CK(cudaMemcpyAsync(out_count, s->cnt, (size_t)npix * 4, kind, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    s->last_ms = ms;
+    s->last_ext = ext;
+    s->last_shadow = sh;
+    s->last_launches = nl;
+    return check_err(s);
+}
+
+extern "C" int32_t rt_last_render_stats(const RtScene* s, double* ms, int64_t* ext, int64_t* sh, int64_t* launches) {
+    if (!s) return RT_ERR_INVALID;
+    if (ms) *ms = s->last_ms;
+    if (ext) *ext = s->last_ext;
+    if (sh) *sh = s->last_shadow;
+    if (launches) *launches = s->last_launches;
+    return RT_OK;
+}
+
+extern "C" int32_t rt_set_profiling(RtScene* s, int32_t enable) {
+    if (!s) return RT_ERR_INVALID;
+    s->profiling = enable != 0;
+    return RT_OK;
+}
+
+extern "C" int32_t rt_kernel_times(const RtScene* s, double* ms, int64_t* launches) {
+    if (!s) return RT_ERR_INVALID;
+    for (int k = 0; k < 4; k++) {
+        if (ms) ms[k] = s->kms[k];
+        if (launches) launches[k] = s->kcount[k];
+    }
+    return RT_OK;
+}
+
+extern "C" int32_t rt_capture_rays(RtScene* s, const RtCamera* cam, const RtPassParams* p, uint32_t depth, float* rays,
+                                   int64_t max_rays, int64_t* n_rays) {
+    int rc = validate_pass(s, cam, p);
+    if (rc) return rc;
+    if (!rays || max_rays < 0) return fail(s, RT_ERR_INVALID, "null ray buffer");
+    CK(cudaSetDevice(s->device));
+    RtPassParams q = *p;
+    q.n_samples = 1;
+    size_t bytes = (size_t)q.width * q.height * 3 * sizeof(float);
+    if (s->scratch_bytes < bytes) {
+        free_dev((void*&)s->scratch);
+        s->scratch_bytes = 0;
+        if (cudaMalloc(&s->scratch, bytes) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc scratch");
+        s->scratch_bytes = bytes;
+    }
+    s->cap_depth = (int32_t)depth;
+    s->cap_out = rays;
+    s->cap_max = max_rays;
+    s->cap_n = 0;
+    int64_t e, sh, l;
+    rc = render_device(s, cam, &q, s->scratch, nullptr, &e, &sh, &l);
+    s->cap_depth = -1;
+    s->cap_out = nullptr;
+    if (n_rays) *n_rays = s->cap_n;
+    if (rc) return rc;
+    return check_err(s);
+}

@@ -1,0 +1,65 @@
+// rt_internal.h — declarations shared by the CUDA translation units of
+// librtb200.so (not part of the public ABI; that is include/rt_api.h).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/rt_api.h"
+#include "rt_device.cuh"
+
+#define RT_TRACE_BLOCK 128
+#define RT_TRACE_BLOCKS_PER_SM 8
+#define RT_SHADE_BLOCK 128
+#define RT_SHADE_BLOCKS_PER_SM 8
+#define RT_MAX_DEPTH 256
+#define RT_CTR_STRIDE 8    // counters per bounce
+
+// Per-path wavefront state, structure of arrays, indexed by path id.
+struct PathState {
+    float4* ray_o;     // origin xyz
+    float4* ray_d;     // direction xyz
+    float4* hit;       // (leaf ref bits, t, b1, b2) written by extend
+    float4* thr;       // throughput T.rgb, prev_mis_w_brdf
+    float4* wts;       // per-wavelength weights w0..w3
+    uint4*  meta;      // pixel, sample slot, flags, lam0 bits
+    float4* L;         // accumulated radiance rgb
+    float4* pend0;     // parked area-light NEE contribution (cancelled if occluded)
+    float4* pend1;     // parked env-map NEE contribution
+};
+
+// meta.z flag layout
+#define PF_DEPTH_MASK   0xFFu
+#define PF_PREV_SPEC    (1u << 8)
+#define PF_TINT_SHIFT   9
+#define PF_TINT_MASK    (3u << 9)
+#define PF_SEC_ALIVE    (1u << 11)
+
+struct RenderLaunch {
+    uint32_t width, height, npix, nsamp;   // this chunk: nsamp consecutive samples
+    uint32_t sample_idx, strata, max_depth, hero;
+    float    bg_scale;
+    uint64_t seed;
+    RtCamera cam;
+    const uint8_t* converged;              // device, nullable
+    float*   scratch;                      // nsamp × npix × 3 (device)
+};
+
+namespace rth {
+void launch_trace_closest_api(const rtd::DevScene& S, const float* rays, uint32_t n, int4* out, uint32_t* next,
+                              int* err, int sms, cudaStream_t st);
+void launch_trace_any_api(const rtd::DevScene& S, const float* rays, uint32_t n, uint8_t* out, uint32_t* next,
+                          int* err, int sms, cudaStream_t st);
+void launch_extend(const rtd::DevScene& S, const PathState& P, const uint32_t* queue, const uint32_t* count,
+                   uint32_t* next, int* err, int sms, cudaStream_t st);
+void launch_shadow(const rtd::DevScene& S, const PathState& P, const float4* sq, const uint32_t* count,
+                   uint32_t* next, int* err, int sms, cudaStream_t st);
+
+void launch_generate(const rtd::DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t* queue0,
+                     uint32_t* count0, cudaStream_t st);
+void launch_shade(const rtd::DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t depth,
+                  const uint32_t* qin, const uint32_t* cin, uint32_t* next, uint32_t* qout, uint32_t* cout,
+                  float4* sq, uint32_t* scount, int sms, cudaStream_t st);
+void launch_finalize(const PathState& P, const RenderLaunch& R, cudaStream_t st);
+void launch_accumulate(const float* scratch, uint32_t nsamp, uint32_t npix, float* acc, float* m2, uint32_t* cnt,
+                       const uint8_t* conv, float clamp, uint32_t min_samples, float floor_, cudaStream_t st);
+}  // namespace rth

@@ -1,0 +1,684 @@
+// rt_shade.cu — wavefront stages around the traversal kernels:
+//   generate  : camera rays for every (pixel, sample) of the chunk
+//               (render_tiles body, src/renderer.rs:692-726; Camera::get_ray, src/camera.rs:47-59)
+//   shade     : one bounce of ray_color (src/renderer.rs:379-580) for every
+//               path in the queue — emission with its MIS weight, material
+//               scattering, next-event estimation (the shadow ray is queued and
+//               its contribution parked in the path), Russian roulette — and
+//               warp-aggregated compaction of the surviving paths
+//   finalize  : fold the last parked contributions, write the pass output
+//   accumulate: accumulate_sample (src/main.rs:603-643) over the passes in order
+#include "rt_internal.h"
+
+using namespace rtd;
+
+namespace {
+
+// ── spectrum (src/spectrum.rs) ──────────────────────────────────────────────
+RT_D void cmf_lerp(const DevScene& S, float lambda, float xyz[3]) {
+    float t = clampf_((lambda - 380.0f) / 5.0f, 0.0f, (float)(S.n_spec - 1));
+    int i = min((int)t, S.n_spec - 2);
+    float frac = t - (float)i;
+    float4 a = __ldg(S.cmf + i), b = __ldg(S.cmf + i + 1);
+    xyz[0] = a.x + frac * (b.x - a.x);
+    xyz[1] = a.y + frac * (b.y - a.y);
+    xyz[2] = a.z + frac * (b.z - a.z);
+}
+RT_D void xyz_srgb(float x, float y, float z, float o[3]) {
+    o[0] = fmaxf(3.2406f * x - 1.5372f * y - 0.4986f * z, 0.0f);
+    o[1] = fmaxf(-0.9689f * x + 1.8758f * y + 0.0415f * z, 0.0f);
+    o[2] = fmaxf(0.0557f * x - 0.2040f * y + 1.0570f * z, 0.0f);
+}
+RT_D float3 spectral_to_rgb(const DevScene& S, float lambda) {
+    float xyz[3], c[3];
+    cmf_lerp(S, lambda, xyz);
+    xyz_srgb(xyz[0], xyz[1], xyz[2], c);
+    return mk(c[0] * S.norms[0], c[1] * S.norms[1], c[2] * S.norms[2]);
+}
+RT_D float3 spectral_fire_rgb(const DevScene& S, float lambda) {
+    float xyz[3], c[3];
+    cmf_lerp(S, lambda, xyz);
+    float w = fmaxf(powf(xyz[1], 0.5f), 0.08f);
+    xyz_srgb(xyz[0], xyz[1], xyz[2], c);
+    c[0] *= w; c[1] *= w; c[2] *= w;
+    float lum = 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2];
+    for (int k = 0; k < 3; k++) c[k] = c[k] * 0.5f + lum * 0.5f;
+    return mk(c[0] * S.fire_norms[0], c[1] * S.fire_norms[1], c[2] * S.fire_norms[2]);
+}
+RT_D float planck_raw(float l, float tk) {
+    float x = 14388000.0f / (l * tk);
+    float l2 = l * l, l4 = l2 * l2;
+    return 1.0f / (l * l4 * fmaxf(expf(x) - 1.0f, 1e-30f));
+}
+RT_D void metal_ior(const DevMaterial& m, float lambda, float* n, float* k) {
+    float t = clampf_((lambda - m.nk_start) / m.nk_step, 0.0f, (float)(m.nk_count - 1));
+    int i = min((int)t, m.nk_count - 2);
+    float f = t - (float)i;
+    *n = m.nk_n[i] + f * (m.nk_n[i + 1] - m.nk_n[i]);
+    *k = m.nk_k[i] + f * (m.nk_k[i + 1] - m.nk_k[i]);
+}
+RT_D float fresnel_conductor(float ci, float n, float k) {
+    float cos2 = ci * ci, sin2 = fmaxf(1.0f - cos2, 0.0f);
+    float n2 = n * n, k2 = k * k;
+    float t0 = n2 - k2 - sin2;
+    float ab = sqrtf(t0 * t0 + 4.0f * n2 * k2);
+    float t1 = ab + cos2;
+    float a = sqrtf(fmaxf(0.5f * (ab + t0), 0.0f));
+    float t2 = 2.0f * ci * a;
+    float rs = (t1 - t2) / fmaxf(t1 + t2, 1e-12f);
+    float t3 = cos2 * ab + sin2 * sin2;
+    float t4 = t2 * sin2;
+    float rp = rs * (t3 - t4) / fmaxf(t3 + t4, 1e-12f);
+    return clampf_(0.5f * (rp + rs), 0.0f, 1.0f);
+}
+RT_D float fresnel_dielectric(float ci, float eta) {
+    float sin2_i = fmaxf(1.0f - ci * ci, 0.0f);
+    float sin2_t = eta * eta * sin2_i;
+    if (sin2_t >= 1.0f) return 1.0f;
+    float ct = sqrtf(1.0f - sin2_t);
+    float rs = (eta * ci - ct) / (eta * ci + ct);
+    float rp = (eta * ct - ci) / (eta * ct + ci);
+    return (rs * rs + rp * rp) * 0.5f;
+}
+RT_D float smith_lambda(float c, float alpha) {
+    float a2 = alpha * alpha, c2 = c * c;
+    return (sqrtf(a2 + (1.0f - a2) * c2) - c) / (2.0f * c);
+}
+RT_D float3 vndf_sample(float3 wo, float ax, float ay, float xi1, float xi2) {
+    float3 wh = unit3(mk(ax * wo.x, ay * wo.y, wo.z));
+    float len = sqrtf(wh.x * wh.x + wh.y * wh.y);
+    float3 t1 = len > 1e-6f ? mk(-wh.y / len, wh.x / len, 0.0f) : mk(1.0f, 0.0f, 0.0f);
+    float3 t2 = cross3(wh, t1);
+    float a = 1.0f / (1.0f + wh.z);
+    float r = sqrtf(xi1);
+    float p1, p2, sphi, cphi;
+    if (xi2 < a) {
+        sincosf(xi2 / a * PI_F, &sphi, &cphi);
+        p1 = r * cphi; p2 = r * sphi;
+    } else {
+        sincosf(PI_F + (xi2 - a) / (1.0f - a) * PI_F, &sphi, &cphi);
+        p1 = r * cphi; p2 = r * sphi * wh.z;
+    }
+    float p3 = sqrtf(fmaxf(1.0f - p1 * p1 - p2 * p2, 0.0f));
+    float3 nh = t1 * p1 + t2 * p2 + wh * p3;
+    return unit3(mk(ax * nh.x, ay * nh.y, fmaxf(nh.z, 0.0f)));
+}
+RT_D float e_ss_lut(const DevScene& S, float mu, float alpha) {
+    float x = clampf_(clampf_(mu, 0.0f, 1.0f) * 64.0f - 0.5f, 0.0f, 63.0f);
+    float y = clampf_(clampf_(alpha, 0.0f, 1.0f) * 64.0f - 0.5f, 0.0f, 63.0f);
+    int i0 = (int)x, j0 = (int)y, i1 = min(i0 + 1, 63), j1 = min(j0 + 1, 63);
+    float fx = x - (float)i0, fy = y - (float)j0;
+    float e00 = __ldg(S.elut + i0 * 64 + j0), e10 = __ldg(S.elut + i1 * 64 + j0);
+    float e01 = __ldg(S.elut + i0 * 64 + j1), e11 = __ldg(S.elut + i1 * 64 + j1);
+    return (e00 * (1.0f - fx) + e10 * fx) * (1.0f - fy) + (e01 * (1.0f - fx) + e11 * fx) * fy;
+}
+
+// ── environment (renderer.rs:84-179) ────────────────────────────────────────
+RT_D float3 env_unrot(const DevScene& S, float3 d) {
+    return mk(d.x * S.env_cos_r - d.z * S.env_sin_r, d.y, d.x * S.env_sin_r + d.z * S.env_cos_r);
+}
+RT_D float3 env_rot(const DevScene& S, float3 d) {
+    return mk(d.x * S.env_cos_r + d.z * S.env_sin_r, d.y, -d.x * S.env_sin_r + d.z * S.env_cos_r);
+}
+RT_D float rem1(float a) { float r = fmodf(a, 1.0f); return r < 0.0f ? r + 1.0f : r; }
+RT_D void env_uv(const DevScene& S, float3 dir, float* u, float* v) {
+    float3 d = env_unrot(S, unit3(dir));
+    *u = rem1(0.5f + atan2f(d.x, d.z) / (2.0f * PI_F));
+    *v = acosf(clampf_(d.y, -1.0f, 1.0f)) / PI_F;
+}
+RT_D float3 env_lookup(const DevScene& S, float3 dir) {
+    float u, v;
+    env_uv(S, dir, &u, &v);
+    float x = u * (float)S.env_w - 0.5f, y = v * (float)S.env_h - 0.5f;
+    float fx0 = floorf(x), fy0 = floorf(y);
+    int x0 = (int)fx0, y0 = (int)fy0;
+    float fx = x - fx0, fy = y - fy0;
+    int xa = x0 % S.env_w; if (xa < 0) xa += S.env_w;
+    int xb = (x0 + 1) % S.env_w; if (xb < 0) xb += S.env_w;
+    int ya = min(max(y0, 0), S.env_h - 1), yb = min(max(y0 + 1, 0), S.env_h - 1);
+    float4 c00 = __ldg(S.env + (size_t)ya * S.env_w + xa), c10 = __ldg(S.env + (size_t)ya * S.env_w + xb);
+    float4 c01 = __ldg(S.env + (size_t)yb * S.env_w + xa), c11 = __ldg(S.env + (size_t)yb * S.env_w + xb);
+    float3 a = mk(c00.x, c00.y, c00.z) * (1.0f - fx) + mk(c10.x, c10.y, c10.z) * fx;
+    float3 b = mk(c01.x, c01.y, c01.z) * (1.0f - fx) + mk(c11.x, c11.y, c11.z) * fx;
+    return a * (1.0f - fy) + b * fy;
+}
+RT_D float env_pdf_at(const DevScene& S, uint32_t k) {
+    return __ldg(S.env + k).w * (float)((uint32_t)S.env_w * (uint32_t)S.env_h) * S.env_inv_total
+           / (2.0f * PI_F * PI_F);
+}
+RT_D float env_dir_pdf(const DevScene& S, float3 dir) {
+    if (!S.has_env) return 0.0f;
+    float u, v;
+    env_uv(S, dir, &u, &v);
+    int i = min((int)(u * (float)S.env_w), S.env_w - 1);
+    int j = min((int)(v * (float)S.env_h), S.env_h - 1);
+    i = max(i, 0); j = max(j, 0);
+    return env_pdf_at(S, (uint32_t)j * S.env_w + i);
+}
+// Alias-table draw with the same discrete texel distribution (lum·sinθ / Σ)
+// as the reference's two-level CDF inversion, then the same sub-texel jitter.
+RT_D float3 env_sample_dir(const DevScene& S, float x1, float x2, float x3, float x4, float* pdf) {
+    uint32_t N = (uint32_t)S.env_w * (uint32_t)S.env_h;
+    uint32_t k = min((uint32_t)(x1 * (float)N), N - 1);
+    float2 pa = __ldg(S.env_alias + k);
+    if (!(x2 < pa.x)) k = __float_as_uint(pa.y);
+    uint32_t i = k % (uint32_t)S.env_w, j = k / (uint32_t)S.env_w;
+    float u = ((float)i + x3) / (float)S.env_w;
+    float v = ((float)j + x4) / (float)S.env_h;
+    float sp, cp, st, ct;
+    sincosf(2.0f * PI_F * (u - 0.5f), &sp, &cp);
+    sincosf(PI_F * v, &st, &ct);
+    *pdf = env_pdf_at(S, k);
+    return env_rot(S, mk(st * sp, ct, st * cp));
+}
+RT_D float3 bg_type_eval(int type, const float* color, const float* top, const float* bottom, float3 dir) {
+    if (type == RT_BG_SOLID) return mk(color[0], color[1], color[2]);
+    float t = (clampf_(dir.y, -1.0f, 1.0f) + 1.0f) * 0.5f;
+    return mk(bottom[0], bottom[1], bottom[2]) * (1.0f - t) + mk(top[0], top[1], top[2]) * t;
+}
+RT_D float3 bg_eval(const DevScene& S, float3 dir) {
+    if (S.bg_type == RT_BG_ENVMAP) {
+        if (S.vis_type >= 0) return bg_type_eval(S.vis_type, S.vis_color, S.vis_top, S.vis_bottom, dir);
+        return env_lookup(S, dir);
+    }
+    return bg_type_eval(S.bg_type, S.bg_color, S.bg_top, S.bg_bottom, dir);
+}
+
+// ── light list (hittable.rs:156-225, quad.rs:82-96, sphere.rs:87-109) ───────
+struct LRec { float t; float3 p, normal; int mat; };
+RT_D bool light_hit(const DevLight& L, float3 o, float3 d, float tmin, float tmax, LRec* rec) {
+    float t, a, b;
+    float3 outward;
+    if (L.type == RT_PRIM_QUAD) {
+        if (!quad_test(L.g, o, d, tmin, tmax, &t, &a, &b)) return false;
+        outward = mk(L.g[0].x, L.g[0].y, L.g[0].z);
+    } else {
+        if (!sphere_test(L.g[0], o, d, tmin, tmax, &t)) return false;
+        outward = ((o + t * d) - mk(L.g[0].x, L.g[0].y, L.g[0].z)) / L.g[0].w;
+    }
+    rec->t = t;
+    rec->p = o + t * d;
+    rec->normal = dot3(d, outward) < 0.0f ? outward : -outward;
+    rec->mat = L.mat;
+    return true;
+}
+RT_D bool lights_hit(const DevScene& S, float3 o, float3 d, LRec* out) {
+    float closest = INFINITY;
+    bool any = false;
+    for (int i = 0; i < S.n_lights; i++) {
+        LRec r;
+        if (light_hit(S.lights[i], o, d, 0.001f, closest, &r)) { closest = r.t; *out = r; any = true; }
+    }
+    return any;
+}
+RT_D float light_pdf_value(const DevLight& L, float3 o, float3 d) {
+    if (L.type == RT_PRIM_SPHERE) {
+        float3 tc = mk(L.g[0].x, L.g[0].y, L.g[0].z) - o;
+        float d2 = len2(tc), r2 = L.g[0].w * L.g[0].w;
+        if (d2 <= r2) return 0.0f;
+        float ctm = sqrtf(1.0f - r2 / d2);
+        return 1.0f / (2.0f * PI_F * (1.0f - ctm));
+    }
+    LRec r;
+    if (!light_hit(L, o, d, 0.001f, INFINITY, &r)) return 0.0f;
+    float dist2 = len2(r.p - o);
+    float ct = fabsf(dot3(unit3(d), r.normal));
+    if (ct < 1e-8f) return 0.0f;
+    return dist2 / (ct * L.g[4].z);
+}
+RT_D float lights_pdf_value(const DevScene& S, float3 o, float3 d) {
+    if (S.n_lights == 0) return 0.0f;
+    float w = 1.0f / (float)S.n_lights, sum = 0.0f;
+    for (int i = 0; i < S.n_lights; i++) sum += w * light_pdf_value(S.lights[i], o, d);
+    return sum;
+}
+RT_D float3 onb_local_w(float3 n, float3 a) {                                      // onb.rs:10-20
+    float3 w = unit3(n);
+    float3 h = fabsf(w.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+    float3 v = unit3(cross3(w, h));
+    float3 u = cross3(w, v);
+    return a.x * u + a.y * v + a.z * w;
+}
+RT_D float3 light_generate(const DevLight& L, float3 o, float r1, float r2) {
+    if (L.type == RT_PRIM_QUAD) {
+        float3 Q = mk(L.g[1].x, L.g[1].y, L.g[1].z), u = mk(L.g[1].w, L.g[2].x, L.g[2].y);
+        float3 v = mk(L.g[2].z, L.g[2].w, L.g[3].x);
+        return unit3((Q + r1 * u + r2 * v) - o);
+    }
+    float3 tc = mk(L.g[0].x, L.g[0].y, L.g[0].z) - o;
+    float d2 = len2(tc), rr = L.g[0].w * L.g[0].w;
+    if (d2 <= rr) return unit3(tc);
+    float ctm = sqrtf(1.0f - rr / d2);
+    float sphi, cphi;
+    sincosf(2.0f * PI_F * r1, &sphi, &cphi);
+    float ct = 1.0f - r2 * (1.0f - ctm);
+    float st = sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
+    return onb_local_w(unit3(tc), mk(cphi * st, sphi * st, ct));
+}
+
+// ── hero-wavelength bookkeeping (see the header of the CPU checker) ─────────
+enum { TINT_NONE = 0, TINT_CMF = 1, TINT_FIRE = 2 };
+RT_D float3 tint_rgb(const DevScene& S, int tint, float lam) {
+    return tint == TINT_CMF ? spectral_to_rgb(S, lam) : spectral_fire_rgb(S, lam);
+}
+RT_D float lam_k(const DevScene& S, float lam0, int k, int H) {
+    return S.lam_lo + fmodf(lam0 - S.lam_lo + (float)k * (S.lam_range / (float)H), S.lam_range);
+}
+RT_D float3 spec_factor(const DevScene& S, int tint, float4 w, float lam0, int H) {
+    float ws[4] = {w.x, w.y, w.z, w.w};
+    if (tint == TINT_NONE) {
+        float m = 0.0f;
+        for (int i = 0; i < H; i++) m += ws[i];
+        float v = m / (float)H;
+        return mk(v, v, v);
+    }
+    float3 acc = mk(0.f, 0.f, 0.f);
+    for (int i = 0; i < H; i++) if (ws[i] != 0.0f) acc = acc + tint_rgb(S, tint, lam_k(S, lam0, i, H)) * ws[i];
+    return acc / (float)H;
+}
+RT_D float3 emission(const DevScene& S, const DevMaterial& m, int tint, float4 w, float lam0, int H) {
+    if (m.type == RT_MAT_DIFFUSE_LIGHT) return mk(m.albedo[0], m.albedo[1], m.albedo[2]) * spec_factor(S, tint, w, lam0, H);
+    if (m.type == RT_MAT_BLACKBODY_LIGHT) {
+        if (tint == TINT_NONE) return mk(m.bb_avg[0], m.bb_avg[1], m.bb_avg[2]) * spec_factor(S, tint, w, lam0, H);
+        float ws[4] = {w.x, w.y, w.z, w.w};
+        float3 acc = mk(0.f, 0.f, 0.f);
+        for (int i = 0; i < H; i++) {
+            if (ws[i] == 0.0f) continue;
+            float l = lam_k(S, lam0, i, H);
+            float sc = planck_raw(l, m.temp_k) * m.bb_norm * m.intensity;
+            acc = acc + tint_rgb(S, tint, l) * (ws[i] * sc);
+        }
+        return acc / (float)H;
+    }
+    return mk(0.f, 0.f, 0.f);
+}
+
+RT_D uint32_t warp_append(uint32_t* counter, bool pred) {
+    uint32_t m = __ballot_sync(__activemask(), pred);
+    uint32_t lane = threadIdx.x & 31u;
+    int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (m && (int)lane == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(__activemask(), base, leader < 0 ? 0 : leader);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
+}  // namespace
+
+// ── generate ────────────────────────────────────────────────────────────────
+__global__ void k_generate(DevScene S, PathState P, RenderLaunch R, uint32_t* queue0, uint32_t* count0) {
+    uint32_t total = R.npix * R.nsamp;
+    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < total; pid += gridDim.x * blockDim.x) {
+        uint32_t k = pid / R.npix, i = pid - k * R.npix;
+        uint32_t row = i / R.width, col = i - row * R.width;
+        uint32_t sample = R.sample_idx + k;
+        P.L[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+        P.pend0[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+        P.pend1[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+        bool conv = R.converged && R.converged[i];
+        Rng rng = make_rng(R.seed, i, sample);
+        float wd = (float)max(R.width - 1u, 1u), hd = (float)max(R.height - 1u, 1u);
+        uint32_t strata = R.strata, s2 = strata * strata, ray_y = R.height - 1u - row;
+        float uj, vj;
+        if (s2 > 0) {
+            uint32_t off = (i * 0x9E3779B9u) % s2;
+            uint32_t si = (sample + off) % s2;
+            uj = ((float)(si % strata) + rnd(rng, D_JIT_U)) / (float)strata;
+            vj = ((float)(si / strata) + rnd(rng, D_JIT_V)) / (float)strata;
+        } else {
+            uj = rnd(rng, D_JIT_U); vj = rnd(rng, D_JIT_V);
+        }
+        float u = ((float)col + uj) / wd, v = ((float)ray_y + vj) / hd;
+        const RtCamera& c = R.cam;
+        float3 cu = mk(c.u[0], c.u[1], c.u[2]), cv = mk(c.v[0], c.v[1], c.v[2]);
+        float3 org = mk(c.origin[0], c.origin[1], c.origin[2]);
+        float lr = sqrtf(rnd(rng, D_LENS_R));
+        float ls, lc;
+        sincosf(2.0f * PI_F * rnd(rng, D_LENS_P), &ls, &lc);
+        float3 rd = c.lens_radius * mk(lr * lc, lr * ls, 0.0f);
+        float3 off = cu * rd.x + cv * rd.y;
+        float3 ll = mk(c.lower_left[0], c.lower_left[1], c.lower_left[2]);
+        float3 hz = mk(c.horizontal[0], c.horizontal[1], c.horizontal[2]);
+        float3 vt = mk(c.vertical[0], c.vertical[1], c.vertical[2]);
+        float3 o = org + off;
+        float3 d = ll + u * hz + v * vt - org - off;
+        int H = (int)R.hero;
+        float lam0 = S.lam_lo + S.lam_range * rnd(rng, D_LAMBDA);
+        if (lam0 >= S.lam_lo + S.lam_range) lam0 = nextafterf(S.lam_lo + S.lam_range, 0.0f);
+        P.ray_o[pid] = make_float4(o.x, o.y, o.z, 0.f);
+        P.ray_d[pid] = make_float4(d.x, d.y, d.z, 0.f);
+        P.thr[pid] = make_float4(1.f, 1.f, 1.f, 1.f);
+        P.wts[pid] = make_float4(1.f, H > 1 ? 1.f : 0.f, H > 2 ? 1.f : 0.f, H > 3 ? 1.f : 0.f);
+        P.meta[pid] = make_uint4(i, k, PF_PREV_SPEC | (H > 1 ? PF_SEC_ALIVE : 0u), __float_as_uint(lam0));
+        if (!conv) {
+            uint32_t slot = warp_append(count0, true);
+            queue0[slot] = pid;
+        }
+    }
+}
+
+// ── shade: one bounce of ray_color for every queued path ─────────────────────
+__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState P, RenderLaunch R, uint32_t depth,
+                                                          const uint32_t* __restrict__ qin, const uint32_t* cin,
+                                                          uint32_t* next, uint32_t* qout, uint32_t* cout,
+                                                          float4* __restrict__ sq, uint32_t* scount) {
+    uint32_t n = *cin;
+    int H = (int)R.hero;
+    bool have_lights = S.n_lights > 0;
+    while (true) {
+        uint32_t base;
+        if ((threadIdx.x & 31u) == 0) base = atomicAdd(next, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= n) break;
+        uint32_t qi = base + (threadIdx.x & 31u);
+        bool active = qi < n;
+        uint32_t pid = active ? qin[qi] : 0u;
+        bool cont = false, sh0 = false, sh1 = false;
+        float4 sh0a, sh0b, sh1a, sh1b;
+        if (active) {
+            uint4 meta = P.meta[pid];
+            float4 thr = P.thr[pid], w = P.wts[pid], L = P.L[pid];
+            float4 p0 = P.pend0[pid], p1 = P.pend1[pid];
+            // fold the previous bounce's surviving NEE contributions, in order
+            L.x += p0.x; L.y += p0.y; L.z += p0.z;
+            L.x += p1.x; L.y += p1.y; L.z += p1.z;
+            P.pend0[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+            P.pend1[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 ro = P.ray_o[pid], rdv = P.ray_d[pid], hv = P.hit[pid];
+            float3 o = mk(ro.x, ro.y, ro.z), d = mk(rdv.x, rdv.y, rdv.z);
+            float3 T = mk(thr.x, thr.y, thr.z);
+            float prev_mis = thr.w;
+            uint32_t flags = meta.z;
+            bool prev_spec = flags & PF_PREV_SPEC;
+            int tint = (flags & PF_TINT_MASK) >> PF_TINT_SHIFT;
+            float lam0 = __uint_as_float(meta.w);
+            Rng rng = make_rng(R.seed, meta.x, R.sample_idx + meta.y);
+            uint32_t b = D_BOUNCE0 + depth * D_PER_BOUNCE;
+            uint32_t ref = __float_as_uint(hv.x);
+            float3 Lc = mk(L.x, L.y, L.z);
+            if (ref == RT_MISS_REF) {
+                float env_pdf = env_dir_pdf(S, d);
+                float emit_w = env_pdf == 0.0f ? 1.0f : (prev_spec ? 1.0f : prev_mis);
+                float3 bg = (depth == 0 || !S.has_env) ? bg_eval(S, d) : env_lookup(S, d);
+                Lc = Lc + T * (bg * spec_factor(S, tint, w, lam0, H)) * R.bg_scale * emit_w;
+            } else {
+                // hit record (hittable.rs:89-93) from the leaf-ordered primitive
+                float t = hv.y;
+                float3 p = o + t * d;
+                uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
+                float3 outward;
+                int mat;
+                if (type == RT_PRIM_TRI) {
+                    const float4* g = S.tri + (size_t)idx * 3;
+                    float4 ga = __ldg(g), gb = __ldg(g + 1), gc = __ldg(g + 2);
+                    float3 e1 = mk(ga.w, gb.x, gb.y), e2 = mk(gb.z, gb.w, gc.x);
+                    mat = __float_as_int(gc.z);
+                    if (__float_as_int(gc.w)) {
+                        const float4* gn = S.tri_n + (size_t)idx * 3;
+                        float4 na = __ldg(gn), nb = __ldg(gn + 1), nc = __ldg(gn + 2);
+                        float b1 = hv.z, b2 = hv.w, b0 = 1.0f - b1 - b2;
+                        float3 sn = b0 * mk(na.x, na.y, na.z) + b1 * mk(na.w, nb.x, nb.y) + b2 * mk(nb.z, nb.w, nc.x);
+                        outward = len2(sn) > 1e-12f ? unit3(sn) : unit3(cross3(e1, e2));
+                    } else {
+                        outward = unit3(cross3(e1, e2));
+                    }
+                } else if (type == RT_PRIM_QUAD) {
+                    const float4* g = S.quad + (size_t)idx * 5;
+                    float4 g0 = __ldg(g);
+                    outward = mk(g0.x, g0.y, g0.z);
+                    mat = __float_as_int(__ldg(g + 4).y);
+                } else {
+                    const float4* g = S.sphere + (size_t)idx * 2;
+                    float4 s0 = __ldg(g);
+                    outward = (p - mk(s0.x, s0.y, s0.z)) / s0.w;
+                    mat = __float_as_int(__ldg(g + 1).y);
+                }
+                bool front = dot3(d, outward) < 0.0f;
+                float3 nrm = front ? outward : -outward;
+                const DevMaterial& m = S.mats[mat];
+                float emit_w = (prev_spec || !have_lights) ? 1.0f : prev_mis;
+                float3 udir = unit3(d);
+                bool alive = true;
+                if (m.type == RT_MAT_DIFFUSE_LIGHT || m.type == RT_MAT_BLACKBODY_LIGHT) {
+                    Lc = Lc + T * emission(S, m, tint, w, lam0, H) * emit_w;
+                    alive = false;
+                } else if (m.type == RT_MAT_DIELECTRIC || m.type == RT_MAT_SPECTRAL_DIELECTRIC) {
+                    bool spectral = m.type == RT_MAT_SPECTRAL_DIELECTRIC;
+                    float ior = spectral ? m.cauchy_b + m.cauchy_c / ((lam0 * 1e-3f) * (lam0 * 1e-3f)) : m.cauchy_b;
+                    if (spectral && H > 1 && m.cauchy_c != 0.0f && (flags & PF_SEC_ALIVE)) {
+                        w = make_float4(w.x * (float)H, 0.f, 0.f, 0.f);
+                        flags &= ~PF_SEC_ALIVE;
+                    }
+                    float ratio = front ? 1.0f / ior : ior;
+                    float ct = fminf(dot3(-udir, nrm), 1.0f);
+                    float st = sqrtf(1.0f - ct * ct);
+                    bool refl = ratio * st > 1.0f || fresnel_dielectric(ct, ratio) > rnd(rng, b + B_SCATTER0);
+                    float3 dir;
+                    if (refl) {
+                        dir = reflect3(udir, nrm);
+                    } else {
+                        float c2 = fminf(dot3(-udir, nrm), 1.0f);
+                        float3 perp = ratio * (udir + c2 * nrm);
+                        float kk = 1.0f - len2(perp);
+                        dir = kk < 0.0f ? reflect3(udir, nrm) : perp + (-sqrtf(kk) * nrm);
+                    }
+                    float3 att = mk(1.f, 1.f, 1.f);
+                    if (spectral) {
+                        if (tint == TINT_NONE && !refl) tint = TINT_FIRE;
+                        if (!front) {
+                            att.x *= expf(-m.absorption[0] * t);
+                            att.y *= expf(-m.absorption[1] * t);
+                            att.z *= expf(-m.absorption[2] * t);
+                        }
+                    }
+                    T = T * att;
+                    o = p; d = dir;
+                    prev_spec = true; prev_mis = 1.0f;
+                } else if (m.type == RT_MAT_SPECTRAL_METAL) {
+                    float3 wo = unit3(-d);
+                    float cos_o = dot3(wo, nrm);
+                    float alpha = fmaxf(m.roughness * m.roughness, 1e-4f);
+                    float3 dir;
+                    float cos_h;
+                    if (cos_o <= 0.0f) {
+                        alive = false;
+                    } else if (m.roughness == 0.0f) {
+                        dir = reflect3(udir, nrm);
+                        cos_h = cos_o;
+                    } else {
+                        float3 up = fabsf(nrm.y) < 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+                        float3 tt = unit3(cross3(nrm, up));
+                        float3 bb = cross3(nrm, tt);
+                        float3 wo_ts = mk(dot3(wo, tt), dot3(wo, bb), cos_o);
+                        float3 mts = vndf_sample(wo_ts, alpha, alpha, rnd(rng, b + B_SCATTER0), rnd(rng, b + B_SCATTER1));
+                        float3 mm = unit3(tt * mts.x + bb * mts.y + nrm * mts.z);
+                        float vo_h = fmaxf(dot3(wo, mm), 0.0f);
+                        dir = unit3(2.0f * vo_h * mm - wo);
+                        cos_h = vo_h;
+                        if (dot3(dir, nrm) <= 0.0f) alive = false;
+                    }
+                    if (alive && dot3(dir, nrm) <= 0.0f) alive = false;
+                    if (alive) {
+                        float weight = 1.0f;
+                        if (m.roughness != 0.0f) {
+                            float lo = smith_lambda(cos_o, alpha);
+                            float li = smith_lambda(fmaxf(dot3(dir, nrm), 0.0f), alpha);
+                            float ec = fminf(1.0f / fmaxf(e_ss_lut(S, cos_o, alpha), 0.05f), 10.0f);
+                            weight = ((1.0f + lo) / (1.0f + lo + li)) * ec;
+                        }
+                        float ws[4] = {w.x, w.y, w.z, w.w};
+                        for (int i = 0; i < H; i++) {
+                            if (ws[i] == 0.0f) continue;
+                            float nn, kk;
+                            metal_ior(m, lam_k(S, lam0, i, H), &nn, &kk);
+                            ws[i] *= fresnel_conductor(cos_h, nn, kk);
+                        }
+                        w = make_float4(ws[0], ws[1], ws[2], ws[3]);
+                        if (tint == TINT_NONE) tint = TINT_CMF;
+                        T = T * weight;
+                        o = p; d = dir;
+                        prev_spec = true; prev_mis = 1.0f;
+                    }
+                } else {
+                    // Lambertian / checker: diffuse branch (renderer.rs:457-572)
+                    float3 att = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
+                    if (m.type == RT_MAT_CHECKER) {
+                        int xi = (int)floorf(m.checker_scale * p.x), yi = (int)floorf(m.checker_scale * p.y);
+                        int zi = (int)floorf(m.checker_scale * p.z);
+                        if ((xi + yi + zi) % 2 != 0) att = mk(m.odd[0], m.odd[1], m.odd[2]);
+                    }
+                    if (have_lights) {
+                        uint32_t pick = rnd_u32(rng, b + B_LPICK) % (uint32_t)S.n_lights;
+                        float3 ldir = light_generate(S.lights[pick], p, rnd(rng, b + B_LPT0), rnd(rng, b + B_LPT1));
+                        LRec lr;
+                        if (lights_hit(S, p, ldir, &lr)) {
+                            float l_pdf = lights_pdf_value(S, p, ldir);
+                            float brdf = fmaxf(dot3(nrm, unit3(ldir)) / PI_F, 0.0f);
+                            float env_p = env_dir_pdf(S, ldir);
+                            float mis_d = l_pdf * l_pdf + brdf * brdf + env_p * env_p;
+                            if (mis_d > 0.0f && brdf > 0.0f) {
+                                float3 nee = emission(S, S.mats[lr.mat], tint, w, lam0, H);
+                                float3 c = T * att * brdf * l_pdf * nee / mis_d;
+                                P.pend0[pid] = make_float4(c.x, c.y, c.z, 0.f);
+                                sh0 = true;
+                                sh0a = make_float4(p.x, p.y, p.z, lr.t * (1.0f - 1e-4f));
+                                sh0b = make_float4(ldir.x, ldir.y, ldir.z, __uint_as_float(pid << 1));
+                            }
+                        }
+                    }
+                    if (S.has_env) {
+                        float epdf;
+                        float3 edir = env_sample_dir(S, rnd(rng, b + B_ENV_ROW), rnd(rng, b + B_ENV_COL),
+                                                     rnd(rng, b + B_ENV_JU), rnd(rng, b + B_ENV_JV), &epdf);
+                        if (epdf > 0.0f) {
+                            float brdf = fmaxf(dot3(nrm, unit3(edir)) / PI_F, 0.0f);
+                            if (brdf > 0.0f) {
+                                float area_pdf = have_lights ? lights_pdf_value(S, p, edir) : 0.0f;
+                                float3 ec = env_lookup(S, edir) * spec_factor(S, tint, w, lam0, H);
+                                float mis_d = epdf * epdf + brdf * brdf + area_pdf * area_pdf;
+                                float3 c = T * att * brdf * epdf * ec / mis_d;
+                                P.pend1[pid] = make_float4(c.x, c.y, c.z, 0.f);
+                                sh1 = true;
+                                sh1a = make_float4(p.x, p.y, p.z, INFINITY);
+                                sh1b = make_float4(edir.x, edir.y, edir.z, __uint_as_float((pid << 1) | 1u));
+                            }
+                        }
+                    }
+                    // cosine-weighted bounce (pdf.rs:12-41)
+                    float r1 = rnd(rng, b + B_COS0), r2 = rnd(rng, b + B_COS1);
+                    float sp_, cp_;
+                    sincosf(2.0f * PI_F * r1, &sp_, &cp_);
+                    float sq = sqrtf(r2);
+                    float3 wn = unit3(nrm);
+                    float3 hh = fabsf(wn.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+                    float3 vv = unit3(cross3(wn, hh));
+                    float3 uu = cross3(wn, vv);
+                    float3 idir = (cp_ * sq) * uu + (sp_ * sq) * vv + sqrtf(1.0f - r2) * wn;
+                    float3 iu = unit3(idir);
+                    float pdf_val = fmaxf(dot3(iu, wn) / PI_F, 0.0f);
+                    float scat = fmaxf(dot3(nrm, iu) / PI_F, 0.0f);
+                    if (pdf_val <= 0.0f || scat <= 0.0f || dot3(idir, nrm) <= 0.0f) {
+                        alive = false;
+                    } else {
+                        float area = have_lights ? lights_pdf_value(S, p, idir) : 0.0f;
+                        float env = env_dir_pdf(S, idir);
+                        prev_mis = (pdf_val * pdf_val) / fmaxf(pdf_val * pdf_val + area * area + env * env, 1e-8f);
+                        T = T * (att * (scat / pdf_val));
+                        o = p; d = idir;
+                        prev_spec = false;
+                    }
+                }
+                if (alive && depth >= 2) {                                          // renderer.rs:574-579
+                    float3 eff = T * spec_factor(S, tint, w, lam0, H);
+                    float survive = fmaxf(fmaxf(eff.x, eff.y), eff.z);
+                    float pr = fminf(survive, 1.0f);
+                    if (survive <= 0.0f || rnd(rng, b + B_RR) >= pr) alive = false;
+                    else T = T / pr;
+                }
+                cont = alive && depth + 1 < R.max_depth;
+            }
+            P.L[pid] = make_float4(Lc.x, Lc.y, Lc.z, 0.f);
+            if (cont) {
+                flags = (flags & ~(PF_DEPTH_MASK | PF_PREV_SPEC | PF_TINT_MASK)) | ((depth + 1) & PF_DEPTH_MASK)
+                        | (prev_spec ? PF_PREV_SPEC : 0u) | ((uint32_t)tint << PF_TINT_SHIFT);
+                P.ray_o[pid] = make_float4(o.x, o.y, o.z, 0.f);
+                P.ray_d[pid] = make_float4(d.x, d.y, d.z, 0.f);
+                P.thr[pid] = make_float4(T.x, T.y, T.z, prev_mis);
+                P.wts[pid] = w;
+                P.meta[pid] = make_uint4(meta.x, meta.y, flags, meta.w);
+            }
+        }
+        // warp-aggregated compaction of survivors and shadow rays
+        uint32_t slot = warp_append(cout, cont);
+        if (cont) qout[slot] = pid;
+        uint32_t s0 = warp_append(scount, sh0);
+        if (sh0) { sq[(size_t)s0 * 2] = sh0a; sq[(size_t)s0 * 2 + 1] = sh0b; }
+        uint32_t s1 = warp_append(scount, sh1);
+        if (sh1) { sq[(size_t)s1 * 2] = sh1a; sq[(size_t)s1 * 2 + 1] = sh1b; }
+    }
+}
+
+// ── finalize: fold parked contributions, write the pass output ──────────────
+__global__ void k_finalize(PathState P, RenderLaunch R) {
+    uint32_t total = R.npix * R.nsamp;
+    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < total; pid += gridDim.x * blockDim.x) {
+        float4 L = P.L[pid], a = P.pend0[pid], b = P.pend1[pid];
+        L.x += a.x; L.y += a.y; L.z += a.z;
+        L.x += b.x; L.y += b.y; L.z += b.z;
+        uint4 meta = P.meta[pid];
+        float* out = R.scratch + ((size_t)meta.y * R.npix + meta.x) * 3;
+        out[0] = L.x; out[1] = L.y; out[2] = L.z;
+    }
+}
+
+// ── accumulate_sample over the passes of one call, in sample order ──────────
+__global__ void k_accumulate(const float* __restrict__ scratch, uint32_t nsamp, uint32_t npix, float* acc, float* m2,
+                             uint32_t* cnt, const uint8_t* conv, float clamp, uint32_t min_samples, float floor_) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+        if (conv && conv[i]) continue;
+        float3 a = mk(acc[i * 3], acc[i * 3 + 1], acc[i * 3 + 2]);
+        float3 q = mk(m2[i * 3], m2[i * 3 + 1], m2[i * 3 + 2]);
+        uint32_t n = cnt[i];
+        for (uint32_t k = 0; k < nsamp; k++) {
+            const float* s = scratch + ((size_t)k * npix + i) * 3;
+            float3 sc = mk(s[0], s[1], s[2]);
+            if (!isfinite(sc.x) || !isfinite(sc.y) || !isfinite(sc.z)) continue;
+            float3 old_mean = n > 0 ? a / (float)n : mk(0.f, 0.f, 0.f);
+            if (clamp > 0.0f && n >= min_samples) {
+                float l = lum3(sc), th = fmaxf(clamp * lum3(old_mean), floor_);
+                if (l > th) sc = sc * (th / l);
+            }
+            a = a + sc;
+            n += 1;
+            float3 nm = a / (float)n;
+            q = q + (sc - old_mean) * (sc - nm);
+        }
+        acc[i * 3] = a.x; acc[i * 3 + 1] = a.y; acc[i * 3 + 2] = a.z;
+        m2[i * 3] = q.x; m2[i * 3 + 1] = q.y; m2[i * 3 + 2] = q.z;
+        cnt[i] = n;
+    }
+}
+
+namespace rth {
+void launch_generate(const DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t* queue0, uint32_t* count0,
+                     cudaStream_t st) {
+    uint32_t total = R.npix * R.nsamp;
+    int grid = (int)std::min<uint32_t>((total + 255) / 256, 148u * 16u);
+    k_generate<<<grid, 256, 0, st>>>(S, P, R, queue0, count0);
+}
+void launch_shade(const DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t depth, const uint32_t* qin,
+                  const uint32_t* cin, uint32_t* next, uint32_t* qout, uint32_t* cout, float4* sq, uint32_t* scount,
+                  int sms, cudaStream_t st) {
+    k_shade<<<sms * RT_SHADE_BLOCKS_PER_SM, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, qin, cin, next, qout, cout, sq, scount);
+}
+void launch_finalize(const PathState& P, const RenderLaunch& R, cudaStream_t st) {
+    uint32_t total = R.npix * R.nsamp;
+    int grid = (int)std::min<uint32_t>((total + 255) / 256, 148u * 16u);
+    k_finalize<<<grid, 256, 0, st>>>(P, R);
+}
+void launch_accumulate(const float* scratch, uint32_t nsamp, uint32_t npix, float* acc, float* m2, uint32_t* cnt,
+                       const uint8_t* conv, float clamp, uint32_t min_samples, float floor_, cudaStream_t st) {
+    int grid = (int)std::min<uint32_t>((npix + 255) / 256, 148u * 16u);
+    k_accumulate<<<grid, 256, 0, st>>>(scratch, nsamp, npix, acc, m2, cnt, conv, clamp, min_samples, floor_);
+}
+}  // namespace rth

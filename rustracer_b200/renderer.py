@@ -1,0 +1,235 @@
+"""Host-side mirror of the reference's render entry points over librtb200.so.
+
+    render_tiles(scratch, converged, sample_idx, strata, width, height, camera,
+                 world, background, lights, bg_scale, photon_map, frame_time)
+    (src/renderer.rs:655-669)
+
+becomes GpuScene(builder).render_tiles(...): the world/background/lights are the
+scene handle, created once (scene_file::build + BvhTree::from_list); every call
+renders sample passes on the GPU.  There is no CPU fallback: without the CUDA
+library or a GPU every call raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librtb200.so")
+_lib = None
+
+
+class RtError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rt error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load librtb200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m rustracer_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, i64, u32, f = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32, C.c_float
+        L.rt_version.restype = i32
+        L.rt_device_count.argtypes = [C.POINTER(i32)]
+        L.rt_scene_create.argtypes = [C.POINTER(abi.RtSceneDesc), i32, C.POINTER(vp)]
+        L.rt_scene_destroy.argtypes = [vp]
+        L.rt_last_error.argtypes = [vp, C.c_char_p, C.c_size_t]
+        L.rt_scene_bvh_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32), C.POINTER(C.c_double)]
+        L.rt_scene_bvh_export.argtypes = [vp, C.POINTER(f), C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]
+        L.rt_trace_closest.argtypes = [vp, vp, i64, vp, i32]
+        L.rt_trace_any.argtypes = [vp, vp, i64, vp, i32]
+        L.rt_render_pass.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), vp, vp, i32]
+        L.rt_render_accumulate.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), f, u32, f, i32,
+                                           vp, vp, vp, i32]
+        L.rt_last_render_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
+        L.rt_set_profiling.argtypes = [vp, i32]
+        L.rt_kernel_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
+        L.rt_capture_rays.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), u32, vp, i64,
+                                      C.POINTER(i64)]
+        _lib = L
+    return _lib
+
+
+def device_count():
+    n = C.c_int32(0)
+    lib().rt_device_count(C.byref(n))
+    return n.value
+
+
+def _ptr(a):
+    """(pointer, mem flag) for a numpy array or a CUDA torch tensor."""
+    if isinstance(a, np.ndarray):
+        return C.c_void_p(a.ctypes.data), abi.RT_MEM_HOST
+    try:
+        import torch
+        if isinstance(a, torch.Tensor):
+            if a.is_cuda:
+                return C.c_void_p(a.data_ptr()), abi.RT_MEM_DEVICE
+            return C.c_void_p(a.data_ptr()), abi.RT_MEM_HOST
+    except ImportError:
+        pass
+    raise TypeError("expected a numpy array or a torch tensor")
+
+
+def pass_params(width, height, sample_idx=0, n_samples=1, strata=None, max_depth=50, hero=1, bg_scale=1.0,
+                seed=0, spp_total=None, frame_time=None):
+    """RtPassParams; strata defaults to ⌊√spp⌋ of the whole render (main.rs:64)."""
+    p = abi.RtPassParams()
+    p.width, p.height = int(width), int(height)
+    p.sample_idx, p.n_samples = int(sample_idx), int(n_samples)
+    if strata is None:
+        strata = int(np.sqrt(np.float32(spp_total if spp_total else n_samples)))
+    p.strata = int(strata)
+    p.max_depth = int(max_depth)
+    p.hero_count = int(hero)
+    p.bg_scale = float(bg_scale)
+    p.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    if frame_time is not None:
+        p.use_frame_time = 1
+        p.t0, p.t1 = float(frame_time[0]), float(frame_time[1])
+    return p
+
+
+class GpuScene:
+    """A scene resident on one GPU (RtScene handle)."""
+
+    def __init__(self, builder, device=0):
+        self._builder = builder
+        self._desc = builder.desc()
+        self.h = C.c_void_p()
+        rc = lib().rt_scene_create(C.byref(self._desc), int(device), C.byref(self.h))
+        if rc != 0:
+            msg = self.last_error()
+            if self.h.value:
+                lib().rt_scene_destroy(self.h)
+                self.h = C.c_void_p()
+            raise RtError(rc, msg)
+
+    def last_error(self):
+        buf = C.create_string_buffer(512)
+        lib().rt_last_error(self.h, buf, 512)
+        return buf.value.decode()
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RtError(rc, self.last_error())
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().rt_scene_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ── BVH ──────────────────────────────────────────────────────────────
+    def bvh_stats(self):
+        nn, nl, md, sah = C.c_int64(), C.c_int64(), C.c_int32(), C.c_double()
+        lib().rt_scene_bvh_stats(self.h, C.byref(nn), C.byref(nl), C.byref(md), C.byref(sah))
+        return dict(nodes=nn.value, leaves=nl.value, max_depth=md.value, sah_cost=sah.value)
+
+    def bvh(self):
+        nn, nl = C.c_int64(), C.c_int64()
+        lib().rt_scene_bvh_export(self.h, None, C.byref(nn), None, C.byref(nl))
+        nodes = np.zeros((nn.value, 56), np.float32)
+        leaves = np.zeros(nl.value, np.int32)
+        lib().rt_scene_bvh_export(self.h, nodes.ctypes.data_as(C.POINTER(C.c_float)), C.byref(nn),
+                                  leaves.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(nl))
+        return nodes, leaves
+
+    # ── ray-level entry points ───────────────────────────────────────────
+    def trace_closest(self, rays, out=None):
+        """rays: (n, 8) float32 (origin, direction, t_min, t_max) numpy or CUDA tensor.
+        Returns a structured array (prim, t, b1, b2) or fills `out` (n, 4) int32 tensor."""
+        n = int(rays.shape[0])
+        if isinstance(rays, np.ndarray):
+            rays = np.ascontiguousarray(rays, dtype=np.float32)
+            hits = np.zeros(n, dtype=np.dtype([("prim", np.int32), ("t", np.float32), ("b1", np.float32),
+                                               ("b2", np.float32)]))
+            self._check(lib().rt_trace_closest(self.h, C.c_void_p(rays.ctypes.data), n,
+                                               C.c_void_p(hits.ctypes.data), abi.RT_MEM_HOST))
+            return hits
+        rp, mem = _ptr(rays)
+        op, _ = _ptr(out)
+        self._check(lib().rt_trace_closest(self.h, rp, n, op, mem))
+        return out
+
+    def trace_any(self, rays):
+        rays = np.ascontiguousarray(rays, dtype=np.float32)
+        occ = np.zeros(len(rays), np.uint8)
+        self._check(lib().rt_trace_any(self.h, C.c_void_p(rays.ctypes.data), len(rays), C.c_void_p(occ.ctypes.data),
+                                       abi.RT_MEM_HOST))
+        return occ
+
+    # ── sample passes ────────────────────────────────────────────────────
+    def render_pass(self, cam, params, out=None, converged=None):
+        """params.n_samples passes; returns (n_samples, height, width, 3) float32."""
+        n = max(1, params.n_samples)
+        if out is None:
+            out = np.zeros((n, params.height, params.width, 3), np.float32)
+        op, mem = _ptr(out)
+        cp = None
+        if converged is not None:
+            cp, _ = _ptr(converged)
+        self._check(lib().rt_render_pass(self.h, C.byref(cam), C.byref(params), op, cp, mem))
+        return out
+
+    def render_tiles(self, scratch, converged, sample_idx, strata, width, height, camera, bg_scale=1.0,
+                     max_depth=50, hero=1, seed=0):
+        """The reference's render_tiles signature (renderer.rs:655-669): one pass into scratch (H, W, 3)."""
+        p = pass_params(width, height, sample_idx, 1, strata, max_depth, hero, bg_scale, seed)
+        out = scratch.reshape(1, height, width, 3)
+        self.render_pass(camera, p, out=out, converged=converged)
+        return scratch
+
+    def render_accumulate(self, cam, params, firefly_clamp=0.0, firefly_min_samples=4, firefly_floor=5.0,
+                          reset=True, outputs=None):
+        """Render params.n_samples passes and accumulate on the device (main.rs:603-643).
+        Returns (sum (H,W,3), m2 (H,W,3), count (H,W)) as numpy, or fills `outputs` tensors."""
+        H, W = params.height, params.width
+        if outputs is None:
+            s = np.zeros((H, W, 3), np.float32)
+            m = np.zeros((H, W, 3), np.float32)
+            c = np.zeros((H, W), np.uint32)
+        else:
+            s, m, c = outputs
+        sp, mem = _ptr(s)
+        mp, _ = _ptr(m)
+        cp, _ = _ptr(c)
+        self._check(lib().rt_render_accumulate(self.h, C.byref(cam), C.byref(params), float(firefly_clamp),
+                                               int(firefly_min_samples), float(firefly_floor), 1 if reset else 0,
+                                               sp, mp, cp, mem))
+        return s, m, c
+
+    def last_stats(self):
+        ms, e, s, l = C.c_double(), C.c_int64(), C.c_int64(), C.c_int64()
+        lib().rt_last_render_stats(self.h, C.byref(ms), C.byref(e), C.byref(s), C.byref(l))
+        return dict(ms=ms.value, ext_rays=e.value, shadow_rays=s.value, launches=l.value)
+
+    # ── diagnostics ──────────────────────────────────────────────────────
+    def set_profiling(self, enable=True):
+        self._check(lib().rt_set_profiling(self.h, 1 if enable else 0))
+
+    def kernel_times(self):
+        """{stage: (ms, launches)} of the last render call (profiling on)."""
+        ms = (C.c_double * 4)()
+        n = (C.c_int64 * 4)()
+        self._check(lib().rt_kernel_times(self.h, ms, n))
+        names = ("generate", "extend", "shade", "shadow")
+        return {k: (ms[i], n[i]) for i, k in enumerate(names)}
+
+    def capture_rays(self, cam, params, depth, max_rays):
+        out = np.zeros((max_rays, 8), np.float32)
+        n = C.c_int64()
+        self._check(lib().rt_capture_rays(self.h, C.byref(cam), C.byref(params), int(depth),
+                                          C.c_void_p(out.ctypes.data), int(max_rays), C.byref(n)))
+        return out[: n.value]

@@ -1,0 +1,553 @@
+"""Host-side scene model: the flat structure-of-arrays description handed to
+librtb200.so through rt_scene_create (include/rt_api.h).
+
+It mirrors what the reference's loader builds (src/scene_file.rs:899-1132):
+objects with materials and scale → rotate → translate transforms, NEE light
+quads inserted into the world AND the light list (scene_file.rs:1056-1067),
+backgrounds, and the spectral_dielectric (ior, dispersion) → Cauchy (B, C)
+conversion (scene_file.rs:1161-1174).  Transforms (src/transform.rs) are applied
+here to the primitives — the GPU path traces world-space primitives only — and
+meshes join the world BVH directly instead of nesting a per-mesh BVH
+(src/mesh.rs:91).
+
+Canonical primitive ids (used for hit records and for tie-breaking) are:
+triangles first, then quads, then spheres, each in insertion order.
+"""
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+from . import abi
+
+F32 = np.float32
+
+
+def _f3(v):
+    return (C.c_float * 3)(*[float(x) for x in v])
+
+
+class Material:
+    """Constructors for RtMaterial records (material.rs / texture.rs)."""
+
+    @staticmethod
+    def _new(t):
+        m = abi.RtMaterial()
+        m.type = t
+        m.checker_scale = 1.0
+        m.intensity = 1.0
+        return m
+
+    @staticmethod
+    def lambertian(color):                                   # material.rs:85-102
+        m = Material._new(abi.RT_MAT_LAMBERTIAN)
+        m.albedo = _f3(color)
+        return m
+
+    @staticmethod
+    def checker(even, odd, scale=1.0):                       # texture.rs:32-37
+        m = Material._new(abi.RT_MAT_CHECKER)
+        m.albedo = _f3(even)
+        m.odd = _f3(odd)
+        m.checker_scale = float(scale)
+        return m
+
+    @staticmethod
+    def dielectric(ior):                                     # material.rs:323-332
+        m = Material._new(abi.RT_MAT_DIELECTRIC)
+        m.cauchy_b = float(ior)
+        return m
+
+    @staticmethod
+    def spectral_dielectric_cauchy(b, c, absorption=(0.0, 0.0, 0.0)):   # material.rs:357-403
+        m = Material._new(abi.RT_MAT_SPECTRAL_DIELECTRIC)
+        m.cauchy_b = float(b)
+        m.cauchy_c = float(c)
+        m.absorption = _f3(absorption)
+        return m
+
+    @staticmethod
+    def spectral_dielectric(ior, dispersion=0.0, absorption=(0.0, 0.0, 0.0)):
+        """TOML form: (ior at the d-line, nF-nC-style spread) → Cauchy B, C
+        exactly as scene_file.rs:1161-1174 computes them in f32."""
+        c = F32(dispersion) / F32(3.250)
+        b = F32(ior) - c / (F32(0.58756) * F32(0.58756))
+        return Material.spectral_dielectric_cauchy(float(b), float(c), absorption)
+
+    @staticmethod
+    def spectral_metal(variant="gold", roughness=0.0):       # material.rs:427-554
+        m = Material._new(abi.RT_MAT_SPECTRAL_METAL)
+        m.metal = {"gold": abi.RT_METAL_GOLD, "copper": abi.RT_METAL_COPPER,
+                   "silver": abi.RT_METAL_SILVER}.get(str(variant).lower(), abi.RT_METAL_GOLD)
+        m.roughness = float(roughness)
+        return m
+
+    @staticmethod
+    def spectral_metal_nk(start_nm, step_nm, n, k, roughness=0.0):
+        """Conductor with a custom n,k table on a uniform wavelength grid."""
+        if len(n) != len(k) or not (2 <= len(n) <= abi.RT_MAX_NK):
+            raise ValueError("custom n,k table needs 2..16 samples")
+        m = Material._new(abi.RT_MAT_SPECTRAL_METAL)
+        m.metal = abi.RT_METAL_CUSTOM
+        m.roughness = float(roughness)
+        m.nk_count = len(n)
+        m.nk_start = float(start_nm)
+        m.nk_step = float(step_nm)
+        for i, (a, b) in enumerate(zip(n, k)):
+            m.nk_n[i] = float(a)
+            m.nk_k[i] = float(b)
+        return m
+
+    @staticmethod
+    def diffuse_light(color):                                # material.rs:14-25
+        m = Material._new(abi.RT_MAT_DIFFUSE_LIGHT)
+        m.albedo = _f3(color)
+        return m
+
+    @staticmethod
+    def blackbody(temp_k, intensity=1.0):                    # material.rs:40-83
+        m = Material._new(abi.RT_MAT_BLACKBODY_LIGHT)
+        m.temp_k = float(temp_k)
+        m.intensity = float(intensity)
+        return m
+
+
+def _euler_fwd(angles_deg):
+    """Rotate::euler (transform.rs:204-213): fwd = Ry · Rx · Rz, degrees."""
+    rx, ry, rz = [math.radians(a) for a in angles_deg]
+    sx, cx = math.sin(rx), math.cos(rx)
+    sy, cy = math.sin(ry), math.cos(ry)
+    sz, cz = math.sin(rz), math.cos(rz)
+    Rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]], dtype=np.float64)
+    Ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]], dtype=np.float64)
+    Rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]], dtype=np.float64)
+    return Ry @ (Rx @ Rz)
+
+
+class Transform:
+    """scale → rotate (Euler about the local origin) → translate (scene_file.rs:1036-1042)."""
+
+    def __init__(self, scale=None, rotate=None, rotate_y=None, spin=None, translate=None):
+        self.scale = 1.0 if scale is None else float(scale)
+        ang = list(rotate) if rotate is not None else [0.0, 0.0, 0.0]
+        if rotate_y is not None:
+            ang[1] += float(rotate_y)
+        if spin is not None:
+            ang[1] += float(spin)
+        self.R = _euler_fwd(ang) if any(a != 0.0 for a in ang) else np.eye(3)
+        self.t = np.zeros(3) if translate is None else np.asarray(translate, dtype=np.float64)
+
+    @property
+    def identity(self):
+        return self.scale == 1.0 and np.array_equal(self.R, np.eye(3)) and not self.t.any()
+
+    def point(self, p):
+        return (np.asarray(p, dtype=np.float64) * self.scale) @ self.R.T + self.t
+
+    def vector(self, v):
+        return (np.asarray(v, dtype=np.float64) * self.scale) @ self.R.T
+
+    def normal(self, n):
+        return np.asarray(n, dtype=np.float64) @ self.R.T
+
+
+class SceneBuilder:
+    """Collects primitives, materials, lights and the background, then emits an
+    RtSceneDesc whose pointers stay valid while this object lives."""
+
+    def __init__(self):
+        self.materials = []
+        self.tri_v = []          # list of (n,9) float32
+        self.tri_n = []          # list of (n,9) float32 or None
+        self.tri_mat = []
+        self.quads = []          # (Q, u, v, mat)
+        self.spheres = []        # (c, r, mat)
+        self._lights = []        # ("quad"|"sphere", local index)
+        self.bg = {"type": abi.RT_BG_SOLID, "color": (0.0, 0.0, 0.0)}
+        self.env = None          # (h, w, 3) float32
+        self.spectral_range = 0
+        self.name = "scene"
+        self.camera = None       # dict(look_from, look_at, vfov, aperture, focus_dist)
+        self.caustics = None
+
+    # materials ---------------------------------------------------------
+    def add_material(self, m):
+        self.materials.append(m)
+        return len(self.materials) - 1
+
+    # primitives --------------------------------------------------------
+    def add_sphere(self, center, radius, mat, xf=None):
+        c = np.asarray(center, dtype=np.float64)
+        r = float(radius)
+        if xf is not None and not xf.identity:
+            c = xf.point(c)
+            r = r * xf.scale
+        self.spheres.append((c.astype(F32), F32(r), mat))
+        return len(self.spheres) - 1
+
+    def add_quad(self, corner, u, v, mat, xf=None):
+        q, uu, vv = (np.asarray(a, dtype=np.float64) for a in (corner, u, v))
+        if xf is not None and not xf.identity:
+            q, uu, vv = xf.point(q), xf.vector(uu), xf.vector(vv)
+        self.quads.append((q.astype(F32), uu.astype(F32), vv.astype(F32), mat))
+        return len(self.quads) - 1
+
+    def add_box(self, p0, p1, mat, xf=None):
+        """make_box (quad.rs:201-215): six quads."""
+        p0, p1 = np.asarray(p0, dtype=F32), np.asarray(p1, dtype=F32)
+        mn, mx = np.minimum(p0, p1), np.maximum(p0, p1)
+        dx = np.array([mx[0] - mn[0], 0, 0], dtype=F32)
+        dy = np.array([0, mx[1] - mn[1], 0], dtype=F32)
+        dz = np.array([0, 0, mx[2] - mn[2]], dtype=F32)
+        self.add_quad([mn[0], mn[1], mx[2]], dx, dy, mat, xf)
+        self.add_quad([mx[0], mn[1], mx[2]], -dz, dy, mat, xf)
+        self.add_quad([mx[0], mn[1], mn[2]], -dx, dy, mat, xf)
+        self.add_quad([mn[0], mn[1], mn[2]], dz, dy, mat, xf)
+        self.add_quad([mn[0], mx[1], mx[2]], dx, -dz, mat, xf)
+        self.add_quad([mn[0], mn[1], mn[2]], dx, dz, mat, xf)
+
+    def add_mesh(self, verts, faces, mat, vnormals=None, xf=None):
+        """Indexed triangle mesh; vertex normals are normalised at load with a
+        face-normal fallback (mesh.rs:68-73); zero-area faces are skipped."""
+        V = np.asarray(verts, dtype=np.float64)
+        Fi = np.asarray(faces, dtype=np.int64).reshape(-1, 3)
+        if xf is not None and not xf.identity:
+            V = xf.point(V)
+        Vf = V.astype(F32)
+        v0, v1, v2 = Vf[Fi[:, 0]], Vf[Fi[:, 1]], Vf[Fi[:, 2]]
+        fn_raw = np.cross((v1 - v0).astype(F32), (v2 - v0).astype(F32))
+        l2 = (fn_raw.astype(np.float64) ** 2).sum(1)
+        keep = l2 >= 1e-16
+        Fi, v0, v1, v2, fn_raw, l2 = Fi[keep], v0[keep], v1[keep], v2[keep], fn_raw[keep], l2[keep]
+        tv = np.concatenate([v0, v1, v2], axis=1).astype(F32)
+        tn = None
+        if vnormals is not None:
+            N = np.asarray(vnormals, dtype=np.float64)
+            if xf is not None and not xf.identity:
+                N = xf.normal(N)
+            face_n = fn_raw / np.sqrt(l2)[:, None]
+            cols = []
+            for k in range(3):
+                nk = N[Fi[:, k]]
+                ln = (nk ** 2).sum(1)
+                ok = ln > 1e-12
+                nk = np.where(ok[:, None], nk / np.sqrt(np.where(ok, ln, 1.0))[:, None], face_n)
+                cols.append(nk)
+            tn = np.concatenate(cols, axis=1).astype(F32)
+        self.tri_v.append(np.ascontiguousarray(tv))
+        self.tri_n.append(tn)
+        self.tri_mat.append(np.full(len(tv), mat, dtype=np.int32))
+        return len(tv)
+
+    def add_light_quad(self, corner, u, v, mat):
+        """[[lights]] entry: the quad joins the world and the NEE list."""
+        qi = self.add_quad(corner, u, v, mat)
+        self._lights.append(("quad", qi))
+        return qi
+
+    def add_light_sphere(self, center, radius, mat):
+        si = self.add_sphere(center, radius, mat)
+        self._lights.append(("sphere", si))
+        return si
+
+    # background --------------------------------------------------------
+    def set_solid(self, color):
+        self.bg = {"type": abi.RT_BG_SOLID, "color": tuple(color)}
+
+    def set_gradient(self, top, bottom):
+        self.bg = {"type": abi.RT_BG_GRADIENT, "top": tuple(top), "bottom": tuple(bottom)}
+
+    def set_env(self, rgb, rotate_y=0.0, visible=None):
+        """rgb: (H, W, 3) float32 equirect, row 0 = +Y.  visible: None or a dict
+        {'type': 'solid', 'color': ...} / {'type': 'gradient', 'top':..., 'bottom':...}."""
+        self.env = np.ascontiguousarray(np.asarray(rgb, dtype=F32))
+        self.bg = {"type": abi.RT_BG_ENVMAP, "rot": float(rotate_y), "visible": visible}
+
+    # emission ----------------------------------------------------------
+    @property
+    def n_tris(self):
+        return int(sum(len(t) for t in self.tri_v))
+
+    def light_prim_ids(self):
+        nt, nq = self.n_tris, len(self.quads)
+        out = []
+        for kind, i in self._lights:
+            out.append(nt + i if kind == "quad" else nt + nq + i)
+        return np.asarray(out, dtype=np.int32)
+
+    def desc(self):
+        """Build the RtSceneDesc; the arrays are cached on self to keep them alive."""
+        nt = self.n_tris
+        if nt:
+            self._tv = np.ascontiguousarray(np.concatenate(self.tri_v).astype(F32))
+            if all(n is not None for n in self.tri_n):
+                self._tn = np.ascontiguousarray(np.concatenate(self.tri_n).astype(F32))
+            elif any(n is not None for n in self.tri_n):
+                parts = []
+                for v, n in zip(self.tri_v, self.tri_n):
+                    if n is None:
+                        e1 = v[:, 3:6] - v[:, 0:3]
+                        e2 = v[:, 6:9] - v[:, 0:3]
+                        fn = np.cross(e1, e2)
+                        fn = fn / np.linalg.norm(fn, axis=1, keepdims=True)
+                        n = np.concatenate([fn, fn, fn], axis=1)
+                    parts.append(n.astype(F32))
+                self._tn = np.ascontiguousarray(np.concatenate(parts))
+            else:
+                self._tn = None
+            self._tm = np.ascontiguousarray(np.concatenate(self.tri_mat).astype(np.int32))
+        else:
+            self._tv = np.zeros((0, 9), F32)
+            self._tn = None
+            self._tm = np.zeros(0, np.int32)
+        if self.quads:
+            self._qv = np.ascontiguousarray(np.array([np.concatenate([q, u, v]) for q, u, v, _ in self.quads], dtype=F32))
+            self._qm = np.array([m for *_, m in self.quads], dtype=np.int32)
+        else:
+            self._qv = np.zeros((0, 9), F32)
+            self._qm = np.zeros(0, np.int32)
+        if self.spheres:
+            self._sv = np.ascontiguousarray(np.array([[c[0], c[1], c[2], r] for c, r, _ in self.spheres], dtype=F32))
+            self._sm = np.array([m for *_, m in self.spheres], dtype=np.int32)
+        else:
+            self._sv = np.zeros((0, 4), F32)
+            self._sm = np.zeros(0, np.int32)
+        self._mats = (abi.RtMaterial * max(1, len(self.materials)))(*self.materials)
+        self._lp = self.light_prim_ids()
+        d = abi.RtSceneDesc()
+        d.n_tris = nt
+        d.tri_v = abi.fptr(self._tv)
+        d.tri_n = abi.fptr(self._tn)
+        d.tri_mat = abi.iptr(self._tm)
+        d.n_quads = len(self.quads)
+        d.quad_quv = abi.fptr(self._qv)
+        d.quad_mat = abi.iptr(self._qm)
+        d.n_spheres = len(self.spheres)
+        d.sphere = abi.fptr(self._sv)
+        d.sphere_mat = abi.iptr(self._sm)
+        d.n_mats = len(self.materials)
+        d.mats = C.cast(self._mats, C.POINTER(abi.RtMaterial))
+        d.n_lights = len(self._lp)
+        d.light_prims = abi.iptr(self._lp)
+        bg = abi.RtBackground()
+        bg.type = self.bg["type"]
+        bg.visible_type = -1
+        if bg.type == abi.RT_BG_SOLID:
+            bg.color = _f3(self.bg["color"])
+        elif bg.type == abi.RT_BG_GRADIENT:
+            bg.top = _f3(self.bg["top"])
+            bg.bottom = _f3(self.bg["bottom"])
+        else:
+            h, w, _ = self.env.shape
+            bg.env_w, bg.env_h = w, h
+            bg.env_rgb = abi.fptr(self.env)
+            bg.env_rot_y_deg = self.bg["rot"]
+            vis = self.bg.get("visible")
+            if vis:
+                if vis["type"] == "solid":
+                    bg.visible_type = abi.RT_BG_SOLID
+                    bg.visible_color = _f3(vis["color"])
+                else:
+                    bg.visible_type = abi.RT_BG_GRADIENT
+                    bg.visible_top = _f3(vis["top"])
+                    bg.visible_bottom = _f3(vis["bottom"])
+        d.bg = bg
+        d.spectral_range = int(self.spectral_range)
+        self._desc = d
+        return d
+
+
+# ── camera (camera.rs:24-45) ────────────────────────────────────────────────
+def make_camera(look_from, look_at, vup=(0.0, 1.0, 0.0), vfov=40.0, aspect=1.0,
+                aperture=0.0, focus_dist=None):
+    """Camera::new in f32 arithmetic; returns an RtCamera."""
+    f = lambda x: np.asarray(x, dtype=F32)
+    lf, la, up = f(look_from), f(look_at), f(vup)
+    if focus_dist is None:
+        focus_dist = max(float(np.linalg.norm((lf - la).astype(np.float64))), 0.01)
+    fd = F32(focus_dist)
+    h = F32(math.tan(float(F32(vfov) * F32(math.pi / 180.0)) / 2.0))
+    vh = F32(2.0) * h
+    vw = F32(aspect) * vh
+
+    def unit(a):
+        return (a / F32(np.sqrt(F32((a * a).sum())))).astype(F32)
+
+    w = unit((lf - la).astype(F32))
+    u = unit(np.cross(up, w).astype(F32))
+    v = np.cross(w, u).astype(F32)
+    horizontal = (fd * vw * u).astype(F32)
+    vertical = (fd * vh * v).astype(F32)
+    lower_left = (lf - horizontal / F32(2) - vertical / F32(2) - fd * w).astype(F32)
+    cam = abi.RtCamera()
+    cam.origin = _f3(lf)
+    cam.lower_left = _f3(lower_left)
+    cam.horizontal = _f3(horizontal)
+    cam.vertical = _f3(vertical)
+    cam.u = _f3(u)
+    cam.v = _f3(v)
+    cam.lens_radius = float(F32(aperture) / F32(2))
+    cam.aperture_blades = 0
+    return cam
+
+
+# ── OBJ + HDR readers ────────────────────────────────────────────────────────
+def load_obj(path):
+    """Minimal Wavefront OBJ reader: positions, optional normals, polygon faces
+    fan-triangulated with a single index per corner (the effect of tobj's
+    GPU_LOAD_OPTIONS in mesh.rs:14).  Returns (verts, faces, vnormals|None)."""
+    vs, vn, faces, fnorm = [], [], [], []
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith("v "):
+                vs.append([float(x) for x in line.split()[1:4]])
+            elif line.startswith("vn "):
+                vn.append([float(x) for x in line.split()[1:4]])
+            elif line.startswith("f "):
+                idx = []
+                nidx = []
+                for tok in line.split()[1:]:
+                    parts = tok.split("/")
+                    i = int(parts[0])
+                    idx.append(i - 1 if i > 0 else len(vs) + i)
+                    if len(parts) >= 3 and parts[2]:
+                        j = int(parts[2])
+                        nidx.append(j - 1 if j > 0 else len(vn) + j)
+                for k in range(1, len(idx) - 1):
+                    faces.append([idx[0], idx[k], idx[k + 1]])
+                    if len(nidx) == len(idx):
+                        fnorm.append([nidx[0], nidx[k], nidx[k + 1]])
+    V = np.asarray(vs, dtype=np.float64)
+    Fa = np.asarray(faces, dtype=np.int64)
+    if vn and len(fnorm) == len(faces):
+        # expand to per-corner vertices so each corner carries its own normal
+        N = np.asarray(vn, dtype=np.float64)
+        Fn = np.asarray(fnorm, dtype=np.int64)
+        V2 = V[Fa.reshape(-1)]
+        N2 = N[Fn.reshape(-1)]
+        return V2, np.arange(len(V2)).reshape(-1, 3), N2
+    return V, Fa, None
+
+
+def load_hdr(path):
+    """Radiance RGBE (.hdr) reader with new-style RLE; returns (H, W, 3) float32."""
+    with open(path, "rb") as fh:
+        data = fh.read()
+    pos = 0
+    while True:
+        end = data.index(b"\n", pos)
+        line = data[pos:end]
+        pos = end + 1
+        if line.strip() == b"":
+            break
+    end = data.index(b"\n", pos)
+    dims = data[pos:end].split()
+    pos = end + 1
+    H, W = int(dims[1]), int(dims[3])
+    out = np.zeros((H, W, 4), dtype=np.uint8)
+    buf = np.frombuffer(data, dtype=np.uint8)
+    for y in range(H):
+        if buf[pos] == 2 and buf[pos + 1] == 2 and (buf[pos + 2] << 8 | buf[pos + 3]) == W:
+            pos += 4
+            for c in range(4):
+                x = 0
+                while x < W:
+                    cnt = int(buf[pos]); pos += 1
+                    if cnt > 128:
+                        cnt -= 128
+                        out[y, x:x + cnt, c] = buf[pos]; pos += 1
+                    else:
+                        out[y, x:x + cnt, c] = buf[pos:pos + cnt]; pos += cnt
+                    x += cnt
+        else:
+            out[y] = buf[pos:pos + W * 4].reshape(W, 4)
+            pos += W * 4
+    e = out[..., 3].astype(np.int32)
+    scale = np.where(e > 0, np.ldexp(1.0, e - 136), 0.0)
+    return (out[..., :3].astype(np.float64) * scale[..., None]).astype(F32)
+
+
+# ── TOML loader (scene_file.rs:621-1216, the subset the GPU path supports) ───
+def _material_from_toml(m, base):
+    t = m["type"]
+    if t == "lambertian":
+        return Material.lambertian(m["color"])
+    if t == "checker":
+        return Material.checker(m["even"], m["odd"], m.get("scale", 1.0))
+    if t == "dielectric":
+        return Material.dielectric(m["ior"])
+    if t == "spectral_dielectric":
+        return Material.spectral_dielectric(m["ior"], m.get("dispersion", 0.0), m.get("absorption", (0, 0, 0)))
+    if t == "spectral_metal":
+        if "n" in m and "k" in m:
+            return Material.spectral_metal_nk(m.get("lambda_start", 380.0), m.get("lambda_step", 25.0),
+                                              m["n"], m["k"], m.get("roughness", 0.0))
+        return Material.spectral_metal(m.get("variant", "gold"), m.get("roughness", 0.0))
+    if t == "diffuse_light":
+        return Material.diffuse_light(m["color"])
+    raise ValueError(f"material type '{t}' is not supported by the GPU path")
+
+
+def load_toml(path):
+    """Parse a scene TOML (the reference's schema, scene_file.rs:31-601) into a
+    SceneBuilder.  Raises ValueError for fields the GPU path does not support."""
+    import tomllib
+    with open(path, "rb") as fh:
+        doc = tomllib.load(fh)
+    return scene_from_toml_dict(doc, os.path.dirname(os.path.abspath(path)))
+
+
+def _resolve(base, p):
+    cand = os.path.join(base, p)
+    return cand if os.path.exists(cand) else p
+
+
+def scene_from_toml_dict(doc, base="."):
+    sb = SceneBuilder()
+    sb.name = doc.get("name", "Custom Scene")
+    cam = doc["camera"]
+    lf, la = cam["look_from"], cam["look_at"]
+    sb.camera = dict(look_from=lf, look_at=la, vfov=cam.get("vfov", 40.0), aperture=cam.get("aperture", 0.0),
+                     focus_dist=cam.get("focus_dist"))
+    bg = doc.get("background", {"type": "solid", "color": [0, 0, 0]})
+    if bg["type"] == "solid":
+        sb.set_solid(bg["color"])
+    elif bg["type"] == "env_map":
+        img = load_hdr(_resolve(base, bg["path"]))
+        sb.set_env(img, bg.get("rotate_y", 0.0) or 0.0, bg.get("visible"))
+    else:
+        raise ValueError(f"background type '{bg['type']}' is not supported by the GPU path")
+    for i, obj in enumerate(doc.get("objects", [])):
+        sh = obj["shape"]
+        if "material" not in obj:
+            raise ValueError(f"objects[{i}]: material is required for this shape type")
+        mat = sb.add_material(_material_from_toml(obj["material"], base))
+        xf = Transform(obj.get("scale"), obj.get("rotate"), obj.get("rotate_y"), obj.get("spin"), obj.get("translate"))
+        st = sh["type"]
+        emissive = obj["material"]["type"] == "diffuse_light" and any(c > 0 for c in obj["material"]["color"])
+        if st == "sphere":
+            si = sb.add_sphere(sh["center"], sh["radius"], mat, xf)
+            if emissive:
+                sb._lights.append(("sphere", si))
+        elif st == "quad":
+            qi = sb.add_quad(sh["corner"], sh["u"], sh["v"], mat, xf)
+            if emissive:
+                sb._lights.append(("quad", qi))
+        elif st == "box":
+            sb.add_box(sh["p_min"], sh["p_max"], mat, xf)
+        elif st == "mesh":
+            V, Fa, N = load_obj(_resolve(base, sh["path"]))
+            sb.add_mesh(V, Fa, mat, N, xf)
+        else:
+            raise ValueError(f"objects[{i}]: shape '{st}' is not supported by the GPU path")
+    for lc in doc.get("lights", []):
+        if "temp_k" in lc:
+            m = Material.blackbody(lc["temp_k"], lc.get("intensity", 1.0))
+        else:
+            m = Material.diffuse_light(lc["color"])
+        sb.add_light_quad(lc["corner"], lc["u"], lc["v"], sb.add_material(m))
+    if doc.get("gems"):
+        raise ValueError("[[gems]] analytic solids are not supported by the GPU path")
+    sb.caustics = doc.get("caustics")
+    return sb
