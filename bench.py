@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--mode", choices=["bench", "pass"], default="bench",
+                    help="pass: one warm-up pass + one 1-spp pass of the workload, no JSON (profiler driver)")
     return ap.parse_args()
 
 
@@ -307,6 +309,7 @@ def roofline(scene, sb, cam):
         total_bytes_pass += bpr * len(r)
         per_depth.append((d, len(r), float(bpr), float(stt[:, 0].mean()), float(stt[:, 1].mean())))
     ext_ms, ext_launches = kt["extend"]
+    # total algorithmic bytes of all extend launches of the 64-spp render ÷ their total device time
     achieved = total_bytes_pass * SPP / (ext_ms / 1000.0) / 1e9 if ext_ms > 0 else None
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "extend_icosphere_traffic.txt")
@@ -316,15 +319,33 @@ def roofline(scene, sb, cam):
                 traffic = float(ln.split(":")[1])
     return {"kernel": "k_extend (8-wide BVH closest hit)", "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
-            "traffic": traffic, "algorithmic_bytes_per_launch": total_bytes_pass / max(1, len(per_depth)),
+            "traffic": traffic, "algorithmic_bytes_per_launch": total_bytes_pass * SPP / max(1, ext_launches),
             "launches": ext_launches, "kernel_ms": ext_ms,
             "stage_ms": {k: v[0] for k, v in kt.items()},
             "per_bounce": [{"depth": d, "rays": n, "bytes_per_ray": b, "nodes_per_ray": nn, "tris_per_ray": tt}
                            for d, n, b, nn, tt in per_depth]}
 
 
+def one_pass():
+    """Profiler driver: one warm-up pass and one measured 1-spp pass of the
+    1920×1080 workload (76 kernel launches)."""
+    import torch
+    from rustracer_b200 import configs
+    from rustracer_b200.renderer import GpuScene, pass_params
+    sb, st = configs.icosphere_scene(seed=2)
+    scene = GpuScene(sb, device=0)
+    out = torch.zeros((1, H, W, 3), device="cuda")
+    for k in range(2):
+        scene.render_pass(st["camera"], pass_params(W, H, k, 1, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2), out=out)
+    torch.cuda.synchronize()
+    print("pass ok", scene.last_stats(), flush=True)
+
+
 def main():
     args = parse()
+    if args.mode == "pass":
+        one_pass()
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/rt_spectral_tables.h"
@@ -48,9 +49,9 @@ static inline float area(const Box& b) {
 struct RefNode { float mn[3][8], mx[3][8]; int32_t ch[8]; };
 
 // ── binned-SAH 8-wide builder (cost model of bvh.rs:52-174) ─────────────────
-// In place on an index array: each sah_partition reorders idx[lo, hi) by a
-// stable counting sort on bucket id, which is what the reference's stable
-// `sort_by_key` + `partition_point` does.
+// In place on an index array: each partition reorders idx[lo, hi) by a stable
+// counting sort on bucket id, which is what the reference's stable
+// `sort_by_key` + `partition_point` does (bvh.rs:132-137).
 struct SahBuilder {
     const std::vector<Box>& boxes;
     std::vector<float> cen[3];
@@ -141,41 +142,93 @@ struct SahBuilder {
         return lo + mid;
     }
 
-    void split(size_t lo, size_t hi, int depth, std::vector<std::pair<size_t, size_t>>& out) {
-        if (depth == 3 || hi - lo <= 1) { out.emplace_back(lo, hi); return; }
+    // ── binary SAH tree + greedy collapse to 8-wide nodes ───────────────────
+    // The binary tree applies the reference's sah_partition recursively (the
+    // same tree its fixed 3-level split walks), down to one primitive per
+    // leaf.  The internal node that splits [lo, hi) at `mid` gets id mid − 1, a
+    // bijection onto [0, n−1), so subtrees can be built by threads and the
+    // result is still deterministic.  Children: ≥ 0 internal id, < 0 leaf
+    // −(position in idx + 1).
+    struct BinNode { int32_t l, r; Box box; };
+    std::vector<BinNode> bin;
+
+    void build_binary(size_t lo, size_t hi, int32_t* ref, Box* box, int depth) {
+        if (hi - lo == 1) { *ref = -(int32_t)lo - 1; *box = boxes[idx[lo]]; return; }
         size_t mid = partition(lo, hi);
-        split(lo, mid, depth + 1, out);
-        split(mid, hi, depth + 1, out);
+        int32_t id = (int32_t)mid - 1;
+        BinNode& b = bin[id];
+        Box lb, rb;
+        if (depth < 4 && hi - lo > 65536) {
+            std::thread t([&]() { build_binary(lo, mid, &b.l, &lb, depth + 1); });
+            build_binary(mid, hi, &b.r, &rb, depth + 1);
+            t.join();
+        } else {
+            build_binary(lo, mid, &b.l, &lb, depth + 1);
+            build_binary(mid, hi, &b.r, &rb, depth + 1);
+        }
+        b.box = unite(lb, rb);
+        *ref = id;
+        *box = b.box;
     }
 
-    int32_t build(size_t lo, size_t hi, Box* out, int depth) {
+    const Box& bbox_of(int32_t ref) const { return ref >= 0 ? bin[ref].box : boxes[idx[-ref - 1]]; }
+
+    // Wide node from binary node `b`: open the inner child of largest surface
+    // area until 8 children (or only leaves) remain; preorder node numbering.
+    int32_t collapse(int32_t b, int depth) {
         max_depth = std::max(max_depth, depth);
-        if (hi - lo == 1) {
-            int32_t slot = (int32_t)leaves.size();
-            leaves.push_back(idx[lo]);
-            *out = boxes[idx[lo]];
-            return -(slot + 1);
+        int32_t kids[8];
+        int nk = 2;
+        kids[0] = bin[b].l; kids[1] = bin[b].r;
+        while (nk < 8) {
+            int best = -1;
+            float ba = -1.0f;
+            for (int i = 0; i < nk; i++)
+                if (kids[i] >= 0) { float a = area(bin[kids[i]].box); if (a > ba) { ba = a; best = i; } }
+            if (best < 0) break;
+            int32_t o = kids[best];
+            kids[best] = bin[o].l;
+            kids[nk++] = bin[o].r;
         }
-        std::vector<std::pair<size_t, size_t>> groups;
-        if (hi - lo <= 8) { for (size_t k = lo; k < hi; k++) groups.emplace_back(k, k + 1); }
-        else split(lo, hi, 0, groups);
         size_t my = nodes.size();
         RefNode nd;
         memset(&nd, 0, sizeof(nd));
         for (int c = 0; c < 8; c++) nd.ch[c] = INT32_MIN;
         nodes.push_back(nd);
-        Box nbox{};
-        for (size_t g = 0; g < groups.size(); g++) {
-            Box cb;
-            int32_t c = build(groups[g].first, groups[g].second, &cb, depth + 1);
-            nd.ch[g] = c;
-            for (int a = 0; a < 3; a++) { nd.mn[a][g] = hc(cb.mn, a); nd.mx[a][g] = hc(cb.mx, a); }
-            nbox = g == 0 ? cb : unite(nbox, cb);
+        for (int c = 0; c < nk; c++) {
+            const Box cb = bbox_of(kids[c]);
+            for (int a = 0; a < 3; a++) { nd.mn[a][c] = hc(cb.mn, a); nd.mx[a][c] = hc(cb.mx, a); }
+            if (kids[c] < 0) {
+                int32_t slot = (int32_t)leaves.size();
+                leaves.push_back(idx[-kids[c] - 1]);
+                nd.ch[c] = -(slot + 1);
+            } else {
+                nd.ch[c] = collapse(kids[c], depth + 1);
+            }
         }
         nodes[my] = nd;
-        *out = nbox;
         return (int32_t)my;
     }
+
+    void build_wide() {
+        size_t n = boxes.size();
+        bin.assign(n > 1 ? n - 1 : 1, BinNode{});
+        int32_t root;
+        Box rb;
+        build_binary(0, n, &root, &rb, 0);
+        if (root < 0) {                       // single primitive: one node with one leaf
+            RefNode nd;
+            memset(&nd, 0, sizeof(nd));
+            for (int c = 0; c < 8; c++) nd.ch[c] = INT32_MIN;
+            nd.ch[0] = -1;
+            leaves.push_back(idx[0]);
+            for (int a = 0; a < 3; a++) { nd.mn[a][0] = hc(rb.mn, a); nd.mx[a][0] = hc(rb.mx, a); }
+            nodes.push_back(nd);
+            return;
+        }
+        collapse(root, 0);
+    }
+
 };
 
 // ── E_ss LUT on the host (material.rs:206-241), once per process ─────────────
@@ -457,16 +510,7 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     std::vector<float4> gtri, gtri_n, gquad, gsph;
     if (n > 0) {
         SahBuilder B(boxes);
-        Box root_box;
-        int32_t root = B.build(0, (size_t)n, &root_box, 0);
-        if (root < 0) {
-            RefNode nd;
-            memset(&nd, 0, sizeof(nd));
-            for (int c = 0; c < 8; c++) nd.ch[c] = INT32_MIN;
-            nd.ch[0] = root;
-            for (int a = 0; a < 3; a++) { nd.mn[a][0] = hc(boxes[0].mn, a); nd.mx[a][0] = hc(boxes[0].mx, a); }
-            B.nodes.push_back(nd);
-        }
+        B.build_wide();
         s->max_depth = B.max_depth;
         if ((int64_t)B.max_depth * 7 + 8 > RT_STACK)
             return bail(fail(s, RT_ERR_CAPACITY, "BVH depth " + std::to_string(B.max_depth) + " exceeds the traversal stack"));
@@ -887,7 +931,6 @@ static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p,
     if (rc) return rc;
     uint32_t maxd = std::min<uint32_t>(p->max_depth, RT_MAX_DEPTH);
     std::vector<uint32_t> hc((size_t)(RT_MAX_DEPTH + 2) * RT_CTR_STRIDE);
-    for (int k = 0; k < 4; k++) { s->kms[k] = 0.0; s->kcount[k] = 0; }
     int64_t ext = 0, sh = 0, nl = 0;
     for (uint32_t k0 = 0; k0 < nsamp; k0 += per) {
         RenderLaunch R{};
@@ -1014,6 +1057,7 @@ extern "C" int32_t rt_render_pass(RtScene* s, const RtCamera* cam, const RtPassP
     }
     const uint8_t* dconv;
     if ((rc = stage_conv(s, converged, npix, mem, &dconv))) return rc;
+    for (int k = 0; k < 4; k++) { s->kms[k] = 0.0; s->kcount[k] = 0; }
     CK(cudaEventRecord(s->ev0, s->stream));
     rc = render_device(s, cam, p, dst, dconv, &s->last_ext, &s->last_shadow, &s->last_launches);
     if (rc) return rc;
@@ -1055,6 +1099,7 @@ extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const R
         if (cudaMalloc(&s->scratch, bytes) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc scratch");
         s->scratch_bytes = bytes;
     }
+    for (int k = 0; k < 4; k++) { s->kms[k] = 0.0; s->kcount[k] = 0; }
     CK(cudaEventRecord(s->ev0, s->stream));
     int64_t ext = 0, sh = 0, nl = 0;
     for (uint32_t k0 = 0; k0 < nsamp; k0 += per) {

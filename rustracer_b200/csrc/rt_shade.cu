@@ -358,7 +358,7 @@ __global__ void k_generate(DevScene S, PathState P, RenderLaunch R, uint32_t* qu
 }
 
 // ── shade: one bounce of ray_color for every queued path ─────────────────────
-__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState P, RenderLaunch R, uint32_t depth,
+__global__ void __launch_bounds__(RT_SHADE_BLOCK, 6) k_shade(DevScene S, PathState P, RenderLaunch R, uint32_t depth,
                                                           const uint32_t* __restrict__ qin, const uint32_t* cin,
                                                           uint32_t* next, uint32_t* qout, uint32_t* cout,
                                                           float4* __restrict__ sq, uint32_t* scount) {
@@ -438,7 +438,8 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                 const DevMaterial& m = S.mats[mat];
                 float emit_w = (prev_spec || !have_lights) ? 1.0f : prev_mis;
                 float3 udir = unit3(d);
-                bool alive = true;
+                bool alive = true, diffuse = false;
+                float3 sf = mk(1.f, 1.f, 1.f);
                 if (m.type == RT_MAT_DIFFUSE_LIGHT || m.type == RT_MAT_BLACKBODY_LIGHT) {
                     Lc = Lc + T * emission(S, m, tint, w, lam0, H) * emit_w;
                     alive = false;
@@ -521,6 +522,8 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                     }
                 } else {
                     // Lambertian / checker: diffuse branch (renderer.rs:457-572)
+                    diffuse = true;
+                    sf = spec_factor(S, tint, w, lam0, H);
                     float3 att = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
                     if (m.type == RT_MAT_CHECKER) {
                         int xi = (int)floorf(m.checker_scale * p.x), yi = (int)floorf(m.checker_scale * p.y);
@@ -554,7 +557,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                             float brdf = fmaxf(dot3(nrm, unit3(edir)) / PI_F, 0.0f);
                             if (brdf > 0.0f) {
                                 float area_pdf = have_lights ? lights_pdf_value(S, p, edir) : 0.0f;
-                                float3 ec = env_lookup(S, edir) * spec_factor(S, tint, w, lam0, H);
+                                float3 ec = env_lookup(S, edir) * sf;
                                 float mis_d = epdf * epdf + brdf * brdf + area_pdf * area_pdf;
                                 float3 c = T * att * brdf * epdf * ec / mis_d;
                                 P.pend1[pid] = make_float4(c.x, c.y, c.z, 0.f);
@@ -589,7 +592,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                     }
                 }
                 if (alive && depth >= 2) {                                          // renderer.rs:574-579
-                    float3 eff = T * spec_factor(S, tint, w, lam0, H);
+                    float3 eff = T * (diffuse ? sf : spec_factor(S, tint, w, lam0, H));
                     float survive = fmaxf(fmaxf(eff.x, eff.y), eff.z);
                     float pr = fminf(survive, 1.0f);
                     if (survive <= 0.0f || rnd(rng, b + B_RR) >= pr) alive = false;

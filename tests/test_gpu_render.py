@@ -28,12 +28,18 @@ def tile_stats(samples, tile=16):
     return m, se
 
 
-def assert_tiles_agree(a, b, k=3.0, max_frac=0.0):
+def assert_tiles_agree(a, b, k=3.0):
+    """Tile means agree within k standard errors.  Under the null hypothesis a
+    tile exceeds 3 SE with probability ~0.3 %, so with tens of tiles a single
+    exceedance is routine: allow max(1, 2 %) tiles beyond 3 SE, none beyond
+    5 SE, and require mean z² < 2 (it is ~1 when the two estimators agree)."""
     ma, sa = tile_stats(a)
     mb, sb = tile_stats(b)
     z = np.abs(ma - mb) / np.sqrt(sa ** 2 + sb ** 2 + 1e-30)
-    bad = z > k
-    assert bad.mean() <= max_frac, f"{bad.sum()} of {bad.size} tiles beyond {k} SE (max z {z.max():.2f})"
+    bad = int((z > k).sum())
+    assert bad <= max(1, int(0.02 * z.size)), f"{bad} of {z.size} tiles beyond {k} SE (max z {z.max():.2f})"
+    assert z.max() <= 5.0, f"tile beyond 5 SE (z {z.max():.2f})"
+    assert (z ** 2).mean() < 2.0, f"mean z^2 {(z ** 2).mean():.2f}"
     return z
 
 
@@ -63,7 +69,7 @@ def test_box_scene_same_seed_matches_pixelwise():
 
 def test_icosphere_env_tiles_match_oracle():
     sb, st = configs.icosphere_scene(width=128, height=72, levels=5, env_w=512, env_h=256)
-    gi, oi, _ = render_both(sb, st, 128, 64, 32, 3, 4)
+    gi, oi, _ = render_both(sb, st, 128, 64, 64, 3, 4)
     assert np.isfinite(gi).all()
     assert_tiles_agree(gi, oi)
 
@@ -78,7 +84,7 @@ def test_full_config_band_matches_oracle():
     """The benchmark workload at 1920×1080: a 32-row band rendered by both."""
     sb, st = configs.icosphere_scene()
     g, o = GpuScene(sb), O.OracleScene(sb)
-    p = pass_params(1920, 1080, 0, 4, 8, 12, 4, 1.0, 11)
+    p = pass_params(1920, 1080, 0, 16, 8, 12, 4, 1.0, 11)
     gi = g.render_pass(st["camera"], p)
     p.seed = 12
     oi = o.render_pass(st["camera"], p, rows=(512, 544))
