@@ -234,6 +234,26 @@ int32_t rt_kernel_times(const RtScene* scene, double* ms, int64_t* launches);
 int32_t rt_capture_rays(RtScene* scene, const RtCamera* cam, const RtPassParams* params,
                         uint32_t depth, float* rays, int64_t max_rays, int64_t* n_rays);
 
+/* rt_render_pass without any device allocation (no counterpart in the
+ * reference).  For hosts that may not allocate device memory while they run —
+ * a real-time loop that must not stall on cudaMalloc, a process whose device
+ * memory is already owned by its framework's caching allocator, a plugin host
+ * that hands over only its own buffers — the wavefront scratch comes from a
+ * fixed device array inside the library (RT_NOALLOC_SCRATCH_BYTES, held on
+ * every GPU that loads the library until exit) instead of cudaMalloc.
+ *  - scratch_rgb must be DEVICE memory: n_samples × height × width × 3 floats.
+ *  - width × height must not exceed RT_NOALLOC_MAX_PIXELS (RT_ERR_CAPACITY).
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - All calls share the one array: calls that overlap on the GPU (two
+ *    streams, two threads, two scenes on one device) race and must be
+ *    serialised by the caller.
+ *  - No converged mask (every pixel is rendered). */
+#define RT_NOALLOC_MAX_PIXELS     65536
+#define RT_NOALLOC_SCRATCH_BYTES  (15u << 20)
+int32_t rt_render_pass_noalloc(RtScene* scene, const RtCamera* cam, const RtPassParams* params,
+                               float* scratch_rgb);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1180,3 +1180,108 @@ extern "C" int32_t rt_capture_rays(RtScene* s, const RtCamera* cam, const RtPass
     if (rc) return rc;
     return check_err(s);
 }
+
+// ── allocation-free sample pass ─────────────────────────────────────────────
+// Some hosts cannot let a library allocate device memory once they are
+// running: a render loop that must not stall on cudaMalloc (it synchronises
+// the device), a process whose device memory is already handed out by its
+// framework's caching allocator so a direct cudaMalloc would fail or fragment
+// the pool, or a plugin host that passes only buffers it allocated itself.
+// rt_render_pass_noalloc serves them: its wavefront scratch (path state, ray
+// and shadow queues, counters, error word) lives in the file-scope device array
+// below instead of memory obtained at call time.  Every GPU that loads the
+// library holds this array (RT_NOALLOC_SCRATCH_BYTES = 15 MB) until the
+// process exits.
+#define RT_NOALLOC_PATHS RT_NOALLOC_MAX_PIXELS
+static constexpr size_t kNaF4 = (size_t)RT_NOALLOC_PATHS * sizeof(float4);
+static constexpr size_t kNaQueue = (size_t)RT_NOALLOC_PATHS * sizeof(uint32_t);
+static constexpr size_t kNaShadow = (size_t)RT_NOALLOC_PATHS * 2 * 2 * sizeof(float4);
+static constexpr size_t kNaCounters = (size_t)(RT_MAX_DEPTH + 2) * RT_CTR_STRIDE * sizeof(uint32_t);
+static constexpr size_t kNaBytes = 9 * kNaF4 + 2 * kNaQueue + kNaShadow + kNaCounters + 256;
+static_assert(kNaBytes <= RT_NOALLOC_SCRATCH_BYTES, "no-alloc scratch size");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[RT_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[64] = {};
+
+// Device address of g_noalloc_scratch on `device` (the current device).  The
+// symbol's host-side name is only a stand-in, so its address must come from
+// cudaGetSymbolAddress, once per device.
+static int noalloc_base(RtScene* s, void** out) {
+    if (s->device < 0 || s->device >= 64) return fail(s, RT_ERR_INVALID, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[s->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(s, RT_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_addr[s->device] = p;
+    }
+    *out = g_noalloc_addr[s->device];
+    return RT_OK;
+}
+
+extern "C" int32_t rt_render_pass_noalloc(RtScene* s, const RtCamera* cam, const RtPassParams* p,
+                                          float* scratch_rgb) {
+    int rc = validate_pass(s, cam, p);
+    if (rc) return rc;
+    if (!scratch_rgb) return fail(s, RT_ERR_INVALID, "null output buffer");
+    uint64_t npix = (uint64_t)p->width * p->height;
+    if (npix > RT_NOALLOC_MAX_PIXELS)
+        return fail(s, RT_ERR_CAPACITY, "rt_render_pass_noalloc: width*height = " + std::to_string(npix) +
+                                            " exceeds the fixed scratch limit of " +
+                                            std::to_string(RT_NOALLOC_MAX_PIXELS) + " pixels");
+    CK(cudaSetDevice(s->device));
+    void* base = nullptr;
+    if ((rc = noalloc_base(s, &base))) return rc;
+    unsigned char* b = (unsigned char*)base;
+    PathState P;
+    float4** f4[] = {&P.ray_o, &P.ray_d, &P.hit, &P.thr, &P.wts, (float4**)&P.meta, &P.L, &P.pend0, &P.pend1};
+    for (int i = 0; i < 9; i++) *f4[i] = (float4*)(b + i * kNaF4);
+    size_t off = 9 * kNaF4;
+    uint32_t* queue[2] = {(uint32_t*)(b + off), (uint32_t*)(b + off + kNaQueue)};
+    off += 2 * kNaQueue;
+    float4* sq = (float4*)(b + off);
+    off += kNaShadow;
+    uint32_t* C = (uint32_t*)(b + off);
+    off += kNaCounters;
+    int* derr = (int*)(b + ((off + 255) & ~(size_t)255));
+    CK(cudaMemsetAsync(derr, 0, sizeof(int), s->stream));
+
+    uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
+    uint32_t per = std::max<uint32_t>(1, std::min<uint32_t>(nsamp, (uint32_t)(RT_NOALLOC_PATHS / npix)));
+    uint32_t maxd = std::min<uint32_t>(p->max_depth, RT_MAX_DEPTH);
+    for (uint32_t k0 = 0; k0 < nsamp; k0 += per) {
+        RenderLaunch R{};
+        R.width = p->width; R.height = p->height; R.npix = (uint32_t)npix;
+        R.nsamp = std::min(per, nsamp - k0);
+        R.sample_idx = p->sample_idx + k0;
+        R.strata = p->strata;
+        R.max_depth = maxd;
+        R.hero = std::max<uint32_t>(1, std::min<uint32_t>(p->hero_count, 4));
+        R.bg_scale = p->bg_scale;
+        R.seed = p->seed;
+        R.cam = *cam;
+        R.converged = nullptr;
+        R.scratch = scratch_rgb + (size_t)k0 * npix * 3;
+        // counters start at zero on every chunk: the array keeps the last call's contents
+        CK(cudaMemsetAsync(C, 0, kNaCounters, s->stream));
+        rth::launch_generate(s->S, P, R, queue[0], C + 0, s->stream);
+        for (uint32_t dpt = 0; dpt < maxd; dpt++) {
+            uint32_t* c = C + dpt * RT_CTR_STRIDE;
+            uint32_t* cn = C + (dpt + 1) * RT_CTR_STRIDE;
+            rth::launch_extend(s->S, P, queue[dpt & 1], c + 0, c + 1, derr, s->sms, s->stream);
+            rth::launch_shade(s->S, P, R, dpt, queue[dpt & 1], c + 0, c + 2, queue[(dpt + 1) & 1], cn + 0, sq, c + 3,
+                              s->sms, s->stream);
+            rth::launch_shadow(s->S, P, sq, c + 3, c + 4, derr, s->sms, s->stream);
+        }
+        rth::launch_finalize(P, R, s->stream);
+        CK(cudaGetLastError());
+    }
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, derr, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (h) return fail(s, h, "traversal stack overflow");
+    return RT_OK;
+}

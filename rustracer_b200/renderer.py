@@ -48,6 +48,7 @@ def lib():
         L.rt_render_accumulate.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), f, u32, f, i32,
                                            vp, vp, vp, i32]
         L.rt_last_render_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
+        L.rt_render_pass_noalloc.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), vp]
         L.rt_set_profiling.argtypes = [vp, i32]
         L.rt_kernel_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
         L.rt_capture_rays.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), u32, vp, i64,
@@ -181,6 +182,16 @@ class GpuScene:
         if converged is not None:
             cp, _ = _ptr(converged)
         self._check(lib().rt_render_pass(self.h, C.byref(cam), C.byref(params), op, cp, mem))
+        return out
+
+    def render_pass_noalloc(self, cam, params, out):
+        """rt_render_pass without device allocation: `out` is a CUDA tensor of
+        (n_samples, height, width, 3) float32; width·height ≤ 65536.  For hosts
+        that must not allocate device memory while running (see rt_api.h)."""
+        op, mem = _ptr(out)
+        if mem != abi.RT_MEM_DEVICE:
+            raise TypeError("render_pass_noalloc writes device memory: pass a CUDA tensor")
+        self._check(lib().rt_render_pass_noalloc(self.h, C.byref(cam), C.byref(params), op))
         return out
 
     def render_tiles(self, scratch, converged, sample_idx, strata, width, height, camera, bg_scale=1.0,
