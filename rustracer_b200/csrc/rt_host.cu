@@ -327,6 +327,7 @@ struct RtScene {
     uint32_t cap = 0;
     PathState P{};
     uint32_t* queue[2] = {nullptr, nullptr};
+    ClassQueues cq{};
     float4* sq = nullptr;
     uint32_t* counters = nullptr;     // (RT_MAX_DEPTH+2) × RT_CTR_STRIDE
     int* d_err = nullptr;
@@ -416,6 +417,7 @@ int32_t rt_scene_destroy(RtScene* s) {
                   s->queue[0], s->queue[1], s->sq, s->counters, s->d_err, s->scratch, s->d_conv, s->acc, s->m2,
                   s->cnt, s->stage};
     for (void* p : ps) if (p) cudaFree(p);
+    for (int c = 0; c < CLS_N; c++) if (s->cq.q[c]) cudaFree(s->cq.q[c]);
     for (auto e : s->pev) cudaEventDestroy(e);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
@@ -894,13 +896,15 @@ extern "C" int32_t rt_trace_any(RtScene* s, const float* rays, int64_t n, uint8_
 }
 
 // ── render loop ─────────────────────────────────────────────────────────────
-static const uint32_t MAX_PATHS = 1u << 22;   // 4M paths in flight per chunk
+static const uint32_t MAX_PATHS = 1u << 23;   // 8M paths in flight per chunk
 
 static int ensure_paths(RtScene* s, uint32_t cap) {
     if (s->cap >= cap) return RT_OK;
     void* ps[] = {s->P.ray_o, s->P.ray_d, s->P.hit, s->P.thr, s->P.wts, s->P.meta, s->P.L, s->P.pend0, s->P.pend1,
                   s->queue[0], s->queue[1], s->sq};
     for (void* p : ps) if (p) cudaFree(p);
+    for (int c = 0; c < CLS_N; c++) if (s->cq.q[c]) cudaFree(s->cq.q[c]);
+    s->cq = ClassQueues{};
     s->P = PathState{};
     s->queue[0] = s->queue[1] = nullptr;
     s->sq = nullptr;
@@ -913,6 +917,8 @@ static int ensure_paths(RtScene* s, uint32_t cap) {
     if (cudaMalloc(&s->queue[0], (size_t)cap * 4) != cudaSuccess || cudaMalloc(&s->queue[1], (size_t)cap * 4) != cudaSuccess ||
         cudaMalloc(&s->sq, (size_t)cap * 2 * 2 * sizeof(float4)) != cudaSuccess)
         return fail(s, RT_ERR_NOMEM, "cudaMalloc queues");
+    for (int c = 0; c < CLS_N; c++)
+        if (cudaMalloc(&s->cq.q[c], (size_t)cap * 4) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc class queues");
     if (!s->counters && cudaMalloc(&s->counters, sizeof(uint32_t) * (RT_MAX_DEPTH + 2) * RT_CTR_STRIDE) != cudaSuccess)
         return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
     s->cap = cap;
@@ -963,7 +969,7 @@ static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p,
             uint32_t* qin = s->queue[dpt & 1];
             uint32_t* qout = s->queue[(dpt + 1) & 1];
             mark(1);
-            rth::launch_extend(s->S, s->P, qin, c + 0, c + 1, s->d_err, s->sms, s->stream);
+            rth::launch_extend(s->S, s->P, qin, c + CTR_COUNT, c + CTR_EXTEND_NEXT, s->d_err, s->sms, s->stream);
             if ((int32_t)dpt == s->cap_depth && s->cap_out) {
                 // diagnostics: copy this bounce's rays out (origin, direction) before shade moves them
                 CK(cudaStreamSynchronize(s->stream));
@@ -983,10 +989,12 @@ static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p,
                 s->cap_n = m;
             }
             mark(2);
-            rth::launch_shade(s->S, s->P, R, dpt, qin, c + 0, c + 2, qout, cn + 0, s->sq, c + 3, s->sms, s->stream);
+            rth::launch_shade(s->S, s->P, R, dpt, qin, c + CTR_COUNT, c, s->cq, qout, cn + CTR_COUNT, s->sq,
+                              c + CTR_SHADOW_COUNT, s->sms, s->stream);
             mark(3);
-            rth::launch_shadow(s->S, s->P, s->sq, c + 3, c + 4, s->d_err, s->sms, s->stream);
-            nl += 3;
+            rth::launch_shadow(s->S, s->P, s->sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, s->d_err, s->sms,
+                               s->stream);
+            nl += 3 + CLS_N;
         }
         mark(0);
         rth::launch_finalize(s->P, R, s->stream);
@@ -996,7 +1004,10 @@ static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p,
         CK(cudaMemcpyAsync(hc.data(), s->counters, sizeof(uint32_t) * (maxd + 2) * RT_CTR_STRIDE, cudaMemcpyDeviceToHost,
                            s->stream));
         CK(cudaStreamSynchronize(s->stream));
-        for (uint32_t dpt = 0; dpt < maxd; dpt++) { ext += hc[dpt * RT_CTR_STRIDE]; sh += hc[dpt * RT_CTR_STRIDE + 3]; }
+        for (uint32_t dpt = 0; dpt < maxd; dpt++) {
+            ext += hc[dpt * RT_CTR_STRIDE + CTR_COUNT];
+            sh += hc[dpt * RT_CTR_STRIDE + CTR_SHADOW_COUNT];
+        }
         if (s->profiling) {
             for (size_t e = 0; e + 1 < ev_used; e++) {
                 float ms = 0.f;
@@ -1197,7 +1208,7 @@ static constexpr size_t kNaF4 = (size_t)RT_NOALLOC_PATHS * sizeof(float4);
 static constexpr size_t kNaQueue = (size_t)RT_NOALLOC_PATHS * sizeof(uint32_t);
 static constexpr size_t kNaShadow = (size_t)RT_NOALLOC_PATHS * 2 * 2 * sizeof(float4);
 static constexpr size_t kNaCounters = (size_t)(RT_MAX_DEPTH + 2) * RT_CTR_STRIDE * sizeof(uint32_t);
-static constexpr size_t kNaBytes = 9 * kNaF4 + 2 * kNaQueue + kNaShadow + kNaCounters + 256;
+static constexpr size_t kNaBytes = 9 * kNaF4 + (2 + CLS_N) * kNaQueue + kNaShadow + kNaCounters + 256;
 static_assert(kNaBytes <= RT_NOALLOC_SCRATCH_BYTES, "no-alloc scratch size");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[RT_NOALLOC_SCRATCH_BYTES];
@@ -1242,6 +1253,9 @@ extern "C" int32_t rt_render_pass_noalloc(RtScene* s, const RtCamera* cam, const
     size_t off = 9 * kNaF4;
     uint32_t* queue[2] = {(uint32_t*)(b + off), (uint32_t*)(b + off + kNaQueue)};
     off += 2 * kNaQueue;
+    ClassQueues cq;
+    for (int c = 0; c < CLS_N; c++) cq.q[c] = (uint32_t*)(b + off + c * kNaQueue);
+    off += CLS_N * kNaQueue;
     float4* sq = (float4*)(b + off);
     off += kNaShadow;
     uint32_t* C = (uint32_t*)(b + off);
@@ -1271,10 +1285,10 @@ extern "C" int32_t rt_render_pass_noalloc(RtScene* s, const RtCamera* cam, const
         for (uint32_t dpt = 0; dpt < maxd; dpt++) {
             uint32_t* c = C + dpt * RT_CTR_STRIDE;
             uint32_t* cn = C + (dpt + 1) * RT_CTR_STRIDE;
-            rth::launch_extend(s->S, P, queue[dpt & 1], c + 0, c + 1, derr, s->sms, s->stream);
-            rth::launch_shade(s->S, P, R, dpt, queue[dpt & 1], c + 0, c + 2, queue[(dpt + 1) & 1], cn + 0, sq, c + 3,
-                              s->sms, s->stream);
-            rth::launch_shadow(s->S, P, sq, c + 3, c + 4, derr, s->sms, s->stream);
+            rth::launch_extend(s->S, P, queue[dpt & 1], c + CTR_COUNT, c + CTR_EXTEND_NEXT, derr, s->sms, s->stream);
+            rth::launch_shade(s->S, P, R, dpt, queue[dpt & 1], c + CTR_COUNT, c, cq, queue[(dpt + 1) & 1],
+                              cn + CTR_COUNT, sq, c + CTR_SHADOW_COUNT, s->sms, s->stream);
+            rth::launch_shadow(s->S, P, sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, derr, s->sms, s->stream);
         }
         rth::launch_finalize(P, R, s->stream);
         CK(cudaGetLastError());

@@ -12,7 +12,22 @@
 #define RT_SHADE_BLOCK 128
 #define RT_SHADE_BLOCKS_PER_SM 8
 #define RT_MAX_DEPTH 256
-#define RT_CTR_STRIDE 8    // counters per bounce
+
+// Counter block of one bounce (RT_CTR_STRIDE uint32 per bounce): ray count,
+// fetch cursors of the persistent kernels, shadow-ray count, and per-material-
+// class path counts and cursors.
+#define RT_CTR_STRIDE 16
+#define CTR_COUNT          0
+#define CTR_EXTEND_NEXT    1
+#define CTR_CLASSIFY_NEXT  2
+#define CTR_SHADOW_COUNT   3
+#define CTR_SHADOW_NEXT    4
+#define CTR_CLS_COUNT      5   // 5 entries
+#define CTR_CLS_NEXT       10  // 5 entries
+
+// material classes shaded by separate kernels
+enum { CLS_MISS = 0, CLS_EMIT = 1, CLS_DIFFUSE = 2, CLS_METAL = 3, CLS_DIELEC = 4, CLS_N = 5 };
+struct ClassQueues { uint32_t* q[CLS_N]; };
 
 // Per-path wavefront state, structure of arrays, indexed by path id.
 struct PathState {
@@ -57,8 +72,8 @@ void launch_shadow(const rtd::DevScene& S, const PathState& P, const float4* sq,
 void launch_generate(const rtd::DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t* queue0,
                      uint32_t* count0, cudaStream_t st);
 void launch_shade(const rtd::DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t depth,
-                  const uint32_t* qin, const uint32_t* cin, uint32_t* next, uint32_t* qout, uint32_t* cout,
-                  float4* sq, uint32_t* scount, int sms, cudaStream_t st);
+                  const uint32_t* qin, const uint32_t* cin, uint32_t* ctr, const ClassQueues& Q, uint32_t* qout,
+                  uint32_t* cout, float4* sq, uint32_t* scount, int sms, cudaStream_t st);
 void launch_finalize(const PathState& P, const RenderLaunch& R, cudaStream_t st);
 void launch_accumulate(const float* scratch, uint32_t nsamp, uint32_t npix, float* acc, float* m2, uint32_t* cnt,
                        const uint8_t* conv, float clamp, uint32_t min_samples, float floor_, cudaStream_t st);

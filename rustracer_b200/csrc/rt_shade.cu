@@ -357,8 +357,90 @@ __global__ void k_generate(DevScene S, PathState P, RenderLaunch R, uint32_t* qu
     }
 }
 
-// ── shade: one bounce of ray_color for every queued path ─────────────────────
-__global__ void __launch_bounds__(RT_SHADE_BLOCK, 6) k_shade(DevScene S, PathState P, RenderLaunch R, uint32_t depth,
+// ── classify: bin the paths of this bounce by material class ────────────────
+// Warp-aggregated appends (ballot + popc + one atomic per class per warp) into
+// one queue per class, so each shading kernel below runs one material's code:
+// no divergence between materials and a much smaller instruction footprint.
+RT_D int material_class(const DevScene& S, uint32_t ref) {
+    if (ref == RT_MISS_REF) return CLS_MISS;
+    uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
+    int mat;
+    if (type == RT_PRIM_TRI) mat = __float_as_int(__ldg(S.tri + (size_t)idx * 3 + 2).z);
+    else if (type == RT_PRIM_QUAD) mat = __float_as_int(__ldg(S.quad + (size_t)idx * 5 + 4).y);
+    else mat = __float_as_int(__ldg(S.sphere + (size_t)idx * 2 + 1).y);
+    int t = S.mats[mat].type;
+    if (t == RT_MAT_DIFFUSE_LIGHT || t == RT_MAT_BLACKBODY_LIGHT) return CLS_EMIT;
+    if (t == RT_MAT_SPECTRAL_METAL) return CLS_METAL;
+    if (t == RT_MAT_DIELECTRIC || t == RT_MAT_SPECTRAL_DIELECTRIC) return CLS_DIELEC;
+    return CLS_DIFFUSE;
+}
+
+__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_classify(DevScene S, PathState P, const uint32_t* __restrict__ qin,
+                                                             const uint32_t* cin, uint32_t* next, ClassQueues Q,
+                                                             uint32_t* cls_count) {
+    uint32_t n = *cin;
+    while (true) {
+        uint32_t base;
+        if ((threadIdx.x & 31u) == 0) base = atomicAdd(next, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= n) break;
+        uint32_t qi = base + (threadIdx.x & 31u);
+        int cls = -1;
+        uint32_t pid = 0;
+        if (qi < n) {
+            pid = qin[qi];
+            cls = material_class(S, __float_as_uint(P.hit[pid].x));
+        }
+#pragma unroll
+        for (int c = 0; c < CLS_N; c++) {
+            uint32_t slot = warp_append(cls_count + c, cls == c);
+            if (cls == c) Q.q[c][slot] = pid;
+        }
+    }
+}
+
+// ── shade: one bounce of ray_color for the paths of one material class ───────
+struct Surf { float3 p, nrm; float t; bool front; int mat; };
+
+RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
+    Surf r;
+    uint32_t ref = __float_as_uint(hv.x);
+    r.t = hv.y;
+    r.p = o + r.t * d;
+    uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
+    float3 outward;
+    if (type == RT_PRIM_TRI) {                                                      // triangle.rs:91-108
+        const float4* g = S.tri + (size_t)idx * 3;
+        float4 ga = __ldg(g), gb = __ldg(g + 1), gc = __ldg(g + 2);
+        float3 e1 = mk(ga.w, gb.x, gb.y), e2 = mk(gb.z, gb.w, gc.x);
+        r.mat = __float_as_int(gc.z);
+        if (__float_as_int(gc.w)) {
+            const float4* gn = S.tri_n + (size_t)idx * 3;
+            float4 na = __ldg(gn), nb = __ldg(gn + 1), nc = __ldg(gn + 2);
+            float b1 = hv.z, b2 = hv.w, b0 = 1.0f - b1 - b2;
+            float3 sn = b0 * mk(na.x, na.y, na.z) + b1 * mk(na.w, nb.x, nb.y) + b2 * mk(nb.z, nb.w, nc.x);
+            outward = len2(sn) > 1e-12f ? unit3(sn) : unit3(cross3(e1, e2));
+        } else {
+            outward = unit3(cross3(e1, e2));
+        }
+    } else if (type == RT_PRIM_QUAD) {                                              // quad.rs:53-56
+        const float4* g = S.quad + (size_t)idx * 5;
+        float4 g0 = __ldg(g);
+        outward = mk(g0.x, g0.y, g0.z);
+        r.mat = __float_as_int(__ldg(g + 4).y);
+    } else {                                                                        // sphere.rs:62-68
+        const float4* g = S.sphere + (size_t)idx * 2;
+        float4 s0 = __ldg(g);
+        outward = (r.p - mk(s0.x, s0.y, s0.z)) / s0.w;
+        r.mat = __float_as_int(__ldg(g + 1).y);
+    }
+    r.front = dot3(d, outward) < 0.0f;                                              // hittable.rs:89-93
+    r.nrm = r.front ? outward : -outward;
+    return r;
+}
+
+template <int CLS>
+__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState P, RenderLaunch R, uint32_t depth,
                                                           const uint32_t* __restrict__ qin, const uint32_t* cin,
                                                           uint32_t* next, uint32_t* qout, uint32_t* cout,
                                                           float4* __restrict__ sq, uint32_t* scount) {
@@ -382,9 +464,9 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK, 6) k_shade(DevScene S, PathSta
             // fold the previous bounce's surviving NEE contributions, in order
             L.x += p0.x; L.y += p0.y; L.z += p0.z;
             L.x += p1.x; L.y += p1.y; L.z += p1.z;
-            P.pend0[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
-            P.pend1[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
-            float4 ro = P.ray_o[pid], rdv = P.ray_d[pid], hv = P.hit[pid];
+            if (p0.x != 0.f || p0.y != 0.f || p0.z != 0.f) P.pend0[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (p1.x != 0.f || p1.y != 0.f || p1.z != 0.f) P.pend1[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 ro = P.ray_o[pid], rdv = P.ray_d[pid];
             float3 o = mk(ro.x, ro.y, ro.z), d = mk(rdv.x, rdv.y, rdv.z);
             float3 T = mk(thr.x, thr.y, thr.z);
             float prev_mis = thr.w;
@@ -394,56 +476,30 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK, 6) k_shade(DevScene S, PathSta
             float lam0 = __uint_as_float(meta.w);
             Rng rng = make_rng(R.seed, meta.x, R.sample_idx + meta.y);
             uint32_t b = D_BOUNCE0 + depth * D_PER_BOUNCE;
-            uint32_t ref = __float_as_uint(hv.x);
             float3 Lc = mk(L.x, L.y, L.z);
-            if (ref == RT_MISS_REF) {
+            if (CLS == CLS_MISS) {                                                  // renderer.rs:381-403
                 float env_pdf = env_dir_pdf(S, d);
                 float emit_w = env_pdf == 0.0f ? 1.0f : (prev_spec ? 1.0f : prev_mis);
                 float3 bg = (depth == 0 || !S.has_env) ? bg_eval(S, d) : env_lookup(S, d);
                 Lc = Lc + T * (bg * spec_factor(S, tint, w, lam0, H)) * R.bg_scale * emit_w;
-            } else {
-                // hit record (hittable.rs:89-93) from the leaf-ordered primitive
-                float t = hv.y;
-                float3 p = o + t * d;
-                uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
-                float3 outward;
-                int mat;
-                if (type == RT_PRIM_TRI) {
-                    const float4* g = S.tri + (size_t)idx * 3;
-                    float4 ga = __ldg(g), gb = __ldg(g + 1), gc = __ldg(g + 2);
-                    float3 e1 = mk(ga.w, gb.x, gb.y), e2 = mk(gb.z, gb.w, gc.x);
-                    mat = __float_as_int(gc.z);
-                    if (__float_as_int(gc.w)) {
-                        const float4* gn = S.tri_n + (size_t)idx * 3;
-                        float4 na = __ldg(gn), nb = __ldg(gn + 1), nc = __ldg(gn + 2);
-                        float b1 = hv.z, b2 = hv.w, b0 = 1.0f - b1 - b2;
-                        float3 sn = b0 * mk(na.x, na.y, na.z) + b1 * mk(na.w, nb.x, nb.y) + b2 * mk(nb.z, nb.w, nc.x);
-                        outward = len2(sn) > 1e-12f ? unit3(sn) : unit3(cross3(e1, e2));
-                    } else {
-                        outward = unit3(cross3(e1, e2));
-                    }
-                } else if (type == RT_PRIM_QUAD) {
-                    const float4* g = S.quad + (size_t)idx * 5;
-                    float4 g0 = __ldg(g);
-                    outward = mk(g0.x, g0.y, g0.z);
-                    mat = __float_as_int(__ldg(g + 4).y);
-                } else {
-                    const float4* g = S.sphere + (size_t)idx * 2;
-                    float4 s0 = __ldg(g);
-                    outward = (p - mk(s0.x, s0.y, s0.z)) / s0.w;
-                    mat = __float_as_int(__ldg(g + 1).y);
-                }
-                bool front = dot3(d, outward) < 0.0f;
-                float3 nrm = front ? outward : -outward;
-                const DevMaterial& m = S.mats[mat];
+            } else if (CLS == CLS_EMIT) {                                           // renderer.rs:415-419
+                float4 hv = P.hit[pid];
+                uint32_t ref = __float_as_uint(hv.x), type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
+                int mat = type == RT_PRIM_TRI ? __float_as_int(__ldg(S.tri + (size_t)idx * 3 + 2).z)
+                        : type == RT_PRIM_QUAD ? __float_as_int(__ldg(S.quad + (size_t)idx * 5 + 4).y)
+                                               : __float_as_int(__ldg(S.sphere + (size_t)idx * 2 + 1).y);
                 float emit_w = (prev_spec || !have_lights) ? 1.0f : prev_mis;
+                Lc = Lc + T * emission(S, S.mats[mat], tint, w, lam0, H) * emit_w;
+            } else {
+                Surf sf_ = surface(S, P.hit[pid], o, d);
+                float3 p = sf_.p, nrm = sf_.nrm;
+                float t = sf_.t;
+                bool front = sf_.front;
+                const DevMaterial& m = S.mats[sf_.mat];
                 float3 udir = unit3(d);
-                bool alive = true, diffuse = false;
+                bool alive = true;
                 float3 sf = mk(1.f, 1.f, 1.f);
-                if (m.type == RT_MAT_DIFFUSE_LIGHT || m.type == RT_MAT_BLACKBODY_LIGHT) {
-                    Lc = Lc + T * emission(S, m, tint, w, lam0, H) * emit_w;
-                    alive = false;
-                } else if (m.type == RT_MAT_DIELECTRIC || m.type == RT_MAT_SPECTRAL_DIELECTRIC) {
+                if (CLS == CLS_DIELEC) {                                            // material.rs:133-149, 369-402
                     bool spectral = m.type == RT_MAT_SPECTRAL_DIELECTRIC;
                     float ior = spectral ? m.cauchy_b + m.cauchy_c / ((lam0 * 1e-3f) * (lam0 * 1e-3f)) : m.cauchy_b;
                     if (spectral && H > 1 && m.cauchy_c != 0.0f && (flags & PF_SEC_ALIVE)) {
@@ -475,7 +531,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK, 6) k_shade(DevScene S, PathSta
                     T = T * att;
                     o = p; d = dir;
                     prev_spec = true; prev_mis = 1.0f;
-                } else if (m.type == RT_MAT_SPECTRAL_METAL) {
+                } else if (CLS == CLS_METAL) {                                      // material.rs:449-500
                     float3 wo = unit3(-d);
                     float cos_o = dot3(wo, nrm);
                     float alpha = fmaxf(m.roughness * m.roughness, 1e-4f);
@@ -520,9 +576,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK, 6) k_shade(DevScene S, PathSta
                         o = p; d = dir;
                         prev_spec = true; prev_mis = 1.0f;
                     }
-                } else {
-                    // Lambertian / checker: diffuse branch (renderer.rs:457-572)
-                    diffuse = true;
+                } else {                                                            // renderer.rs:457-572
                     sf = spec_factor(S, tint, w, lam0, H);
                     float3 att = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
                     if (m.type == RT_MAT_CHECKER) {
@@ -571,12 +625,12 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK, 6) k_shade(DevScene S, PathSta
                     float r1 = rnd(rng, b + B_COS0), r2 = rnd(rng, b + B_COS1);
                     float sp_, cp_;
                     sincosf(2.0f * PI_F * r1, &sp_, &cp_);
-                    float sq = sqrtf(r2);
+                    float sq_ = sqrtf(r2);
                     float3 wn = unit3(nrm);
                     float3 hh = fabsf(wn.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
                     float3 vv = unit3(cross3(wn, hh));
                     float3 uu = cross3(wn, vv);
-                    float3 idir = (cp_ * sq) * uu + (sp_ * sq) * vv + sqrtf(1.0f - r2) * wn;
+                    float3 idir = (cp_ * sq_) * uu + (sp_ * sq_) * vv + sqrtf(1.0f - r2) * wn;
                     float3 iu = unit3(idir);
                     float pdf_val = fmaxf(dot3(iu, wn) / PI_F, 0.0f);
                     float scat = fmaxf(dot3(nrm, iu) / PI_F, 0.0f);
@@ -592,7 +646,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK, 6) k_shade(DevScene S, PathSta
                     }
                 }
                 if (alive && depth >= 2) {                                          // renderer.rs:574-579
-                    float3 eff = T * (diffuse ? sf : spec_factor(S, tint, w, lam0, H));
+                    float3 eff = T * (CLS == CLS_DIFFUSE ? sf : spec_factor(S, tint, w, lam0, H));
                     float survive = fmaxf(fmaxf(eff.x, eff.y), eff.z);
                     float pr = fminf(survive, 1.0f);
                     if (survive <= 0.0f || rnd(rng, b + B_RR) >= pr) alive = false;
@@ -611,13 +665,17 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK, 6) k_shade(DevScene S, PathSta
                 P.meta[pid] = make_uint4(meta.x, meta.y, flags, meta.w);
             }
         }
-        // warp-aggregated compaction of survivors and shadow rays
-        uint32_t slot = warp_append(cout, cont);
-        if (cont) qout[slot] = pid;
-        uint32_t s0 = warp_append(scount, sh0);
-        if (sh0) { sq[(size_t)s0 * 2] = sh0a; sq[(size_t)s0 * 2 + 1] = sh0b; }
-        uint32_t s1 = warp_append(scount, sh1);
-        if (sh1) { sq[(size_t)s1 * 2] = sh1a; sq[(size_t)s1 * 2 + 1] = sh1b; }
+        if (CLS != CLS_MISS && CLS != CLS_EMIT) {
+            // warp-aggregated compaction of survivors and shadow rays
+            uint32_t slot = warp_append(cout, cont);
+            if (cont) qout[slot] = pid;
+        }
+        if (CLS == CLS_DIFFUSE) {
+            uint32_t s0 = warp_append(scount, sh0);
+            if (sh0) { sq[(size_t)s0 * 2] = sh0a; sq[(size_t)s0 * 2 + 1] = sh0b; }
+            uint32_t s1 = warp_append(scount, sh1);
+            if (sh1) { sq[(size_t)s1 * 2] = sh1a; sq[(size_t)s1 * 2 + 1] = sh1b; }
+        }
     }
 }
 
@@ -670,9 +728,23 @@ void launch_generate(const DevScene& S, const PathState& P, const RenderLaunch& 
     k_generate<<<grid, 256, 0, st>>>(S, P, R, queue0, count0);
 }
 void launch_shade(const DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t depth, const uint32_t* qin,
-                  const uint32_t* cin, uint32_t* next, uint32_t* qout, uint32_t* cout, float4* sq, uint32_t* scount,
-                  int sms, cudaStream_t st) {
-    k_shade<<<sms * RT_SHADE_BLOCKS_PER_SM, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, qin, cin, next, qout, cout, sq, scount);
+                  const uint32_t* cin, uint32_t* ctr, const ClassQueues& Q, uint32_t* qout, uint32_t* cout,
+                  float4* sq, uint32_t* scount, int sms, cudaStream_t st) {
+    // ctr: this bounce's counter block (see rt_internal.h for the slots)
+    int grid = sms * RT_SHADE_BLOCKS_PER_SM;
+    k_classify<<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, qin, cin, ctr + CTR_CLASSIFY_NEXT, Q, ctr + CTR_CLS_COUNT);
+    k_shade<CLS_MISS><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, Q.q[CLS_MISS], ctr + CTR_CLS_COUNT + CLS_MISS,
+                                                       ctr + CTR_CLS_NEXT + CLS_MISS, qout, cout, sq, scount);
+    k_shade<CLS_EMIT><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, Q.q[CLS_EMIT], ctr + CTR_CLS_COUNT + CLS_EMIT,
+                                                       ctr + CTR_CLS_NEXT + CLS_EMIT, qout, cout, sq, scount);
+    k_shade<CLS_DIFFUSE><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, Q.q[CLS_DIFFUSE],
+                                                          ctr + CTR_CLS_COUNT + CLS_DIFFUSE,
+                                                          ctr + CTR_CLS_NEXT + CLS_DIFFUSE, qout, cout, sq, scount);
+    k_shade<CLS_METAL><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, Q.q[CLS_METAL], ctr + CTR_CLS_COUNT + CLS_METAL,
+                                                        ctr + CTR_CLS_NEXT + CLS_METAL, qout, cout, sq, scount);
+    k_shade<CLS_DIELEC><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, Q.q[CLS_DIELEC],
+                                                         ctr + CTR_CLS_COUNT + CLS_DIELEC,
+                                                         ctr + CTR_CLS_NEXT + CLS_DIELEC, qout, cout, sq, scount);
 }
 void launch_finalize(const PathState& P, const RenderLaunch& R, cudaStream_t st) {
     uint32_t total = R.npix * R.nsamp;

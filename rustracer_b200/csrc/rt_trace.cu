@@ -66,31 +66,96 @@ RT_D bool leaf_any(const DevScene& S, uint32_t ref, float3 o, float3 d, float tm
 
 #define CAS(a, b) { uint32_t lo_ = min(k[a], k[b]); uint32_t hi_ = max(k[a], k[b]); k[a] = lo_; k[b] = hi_; }
 
-// Slab test of the 8 children of node `ni`; returns the hit mask and the entry
-// distances.  Bit-identical to the CPU checker's AVX2 slab test.
-template <bool NANSAFE>
-RT_D uint32_t node_test(const DevScene& S, uint32_t ni, float3 o, float3 inv, float tmin, float tmax,
-                        float tn[8], uint32_t ch[8]) {
+// Per-ray slab constants.  Fast path (every direction component non-zero and
+// t_min ≥ 0): the near and far planes of each axis are chosen once per ray from
+// the sign of the direction, so a child costs 6 FSUB + 6 FMUL + 6 FMNMX.  The
+// far-plane reciprocal is widened by 2^-15, which after the two roundings of
+// (b − o)·inv still exceeds the exact exit distance by ≥ 2^-16 relative — the
+// culling stays conservative, so any layout returns the brute-force answer.
+// General path (a zero or denormal component, or t_min < 0): both planes with
+// min/max, a NaN slab (ray lying in a face plane) spanning the whole line, and
+// the exit widened explicitly.
+struct RayC {
+    float3 o, inv, invf;
+    int nx, ny, nz;          // float4 offsets of the near-plane arrays in a node
+    bool general;
+};
+
+RT_D RayC make_rayc(float3 o, float3 d, float tmin) {
+    RayC r;
+    r.o = o;
+    r.inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    const float W = 1.000030517578125f;   // 1 + 2^-15
+    r.invf = mk(r.inv.x * W, r.inv.y * W, r.inv.z * W);
+    r.general = isinf(r.inv.x) || isinf(r.inv.y) || isinf(r.inv.z) || !(tmin >= 0.0f);
+    r.nx = signbit(r.inv.x) ? 6 : 0;
+    r.ny = signbit(r.inv.y) ? 8 : 2;
+    r.nz = signbit(r.inv.z) ? 10 : 4;
+    return r;
+}
+
+__device__ __noinline__ uint32_t node_test_general(const DevScene& S, uint32_t ni, const RayC& R, float tmin,
+                                                   float tmax, float* tn);
+
+// Slab test of the 8 children of node `ni` against [tmin, tmax]; returns the
+// hit mask and the entry distances.
+RT_D uint32_t node_test(const DevScene& S, uint32_t ni, const RayC& R, float tmin, float tmax, float tn[8],
+                        uint32_t ch[8]) {
     const float4* N = S.nodes + (size_t)ni * 14;
+    uint32_t mask = 0;
+    float4 c0 = __ldg(N + 12), c1 = __ldg(N + 13);
+    const uint32_t cc[8] = {__float_as_uint(c0.x), __float_as_uint(c0.y), __float_as_uint(c0.z), __float_as_uint(c0.w),
+                            __float_as_uint(c1.x), __float_as_uint(c1.y), __float_as_uint(c1.z), __float_as_uint(c1.w)};
+#pragma unroll
+    for (int c = 0; c < 8; c++) ch[c] = cc[c];
+    if (!R.general) {
+        float4 q[12];
+        q[0] = __ldg(N + R.nx); q[1] = __ldg(N + R.nx + 1);
+        q[2] = __ldg(N + R.ny); q[3] = __ldg(N + R.ny + 1);
+        q[4] = __ldg(N + R.nz); q[5] = __ldg(N + R.nz + 1);
+        q[6] = __ldg(N + 6 - R.nx); q[7] = __ldg(N + 7 - R.nx);
+        q[8] = __ldg(N + 10 - R.ny); q[9] = __ldg(N + 11 - R.ny);
+        q[10] = __ldg(N + 14 - R.nz); q[11] = __ldg(N + 15 - R.nz);
+        const float* f = reinterpret_cast<const float*>(q);
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            float nx = (f[0 + c] - R.o.x) * R.inv.x, fx = (f[24 + c] - R.o.x) * R.invf.x;
+            float ny = (f[8 + c] - R.o.y) * R.inv.y, fy = (f[32 + c] - R.o.y) * R.invf.y;
+            float nz = (f[16 + c] - R.o.z) * R.inv.z, fz = (f[40 + c] - R.o.z) * R.invf.z;
+            float t0 = fmaxf(fmaxf(fmaxf(tmin, nx), ny), nz);
+            float t1 = fminf(fminf(fminf(tmax, fx), fy), fz);
+            tn[c] = t0;
+            if (t0 <= t1 && ch[c] != RT_EMPTY_REF) mask |= 1u << c;
+        }
+        return mask;
+    }
+    float tg[8];
+    mask = node_test_general(S, ni, R, tmin, tmax, tg);
+#pragma unroll
+    for (int c = 0; c < 8; c++) tn[c] = tg[c];
+    return mask;
+}
+
+__device__ __noinline__ uint32_t node_test_general(const DevScene& S, uint32_t ni, const RayC& R, float tmin,
+                                                   float tmax, float* tn) {
+    const float4* N = S.nodes + (size_t)ni * 14;
+    uint32_t mask = 0;
     float4 q[14];
 #pragma unroll
     for (int i = 0; i < 14; i++) q[i] = __ldg(N + i);
     const float* f = reinterpret_cast<const float*>(q);
-    uint32_t mask = 0;
+    const uint32_t* ch = reinterpret_cast<const uint32_t*>(f + 48);
 #pragma unroll
     for (int c = 0; c < 8; c++) {
-        ch[c] = __float_as_uint(f[48 + c]);
-        float dax = (f[0 + c] - o.x) * inv.x, dbx = (f[24 + c] - o.x) * inv.x;
-        float day = (f[8 + c] - o.y) * inv.y, dby = (f[32 + c] - o.y) * inv.y;
-        float daz = (f[16 + c] - o.z) * inv.z, dbz = (f[40 + c] - o.z) * inv.z;
+        float dax = (f[0 + c] - R.o.x) * R.inv.x, dbx = (f[24 + c] - R.o.x) * R.inv.x;
+        float day = (f[8 + c] - R.o.y) * R.inv.y, dby = (f[32 + c] - R.o.y) * R.inv.y;
+        float daz = (f[16 + c] - R.o.z) * R.inv.z, dbz = (f[40 + c] - R.o.z) * R.inv.z;
         float lx = fminf(dax, dbx), hx = fmaxf(dax, dbx);
         float ly = fminf(day, dby), hy = fmaxf(day, dby);
         float lz = fminf(daz, dbz), hz = fmaxf(daz, dbz);
-        if (NANSAFE) {
-            if (isnan(dax) || isnan(dbx)) { lx = -INFINITY; hx = INFINITY; }
-            if (isnan(day) || isnan(dby)) { ly = -INFINITY; hy = INFINITY; }
-            if (isnan(daz) || isnan(dbz)) { lz = -INFINITY; hz = INFINITY; }
-        }
+        if (isnan(dax) || isnan(dbx)) { lx = -INFINITY; hx = INFINITY; }
+        if (isnan(day) || isnan(dby)) { ly = -INFINITY; hy = INFINITY; }
+        if (isnan(daz) || isnan(dbz)) { lz = -INFINITY; hz = INFINITY; }
         float t0 = fmaxf(fmaxf(fmaxf(tmin, lx), ly), lz);
         float t1 = fminf(fminf(fminf(tmax, hx), hy), hz);
         float t1w = t1 + fabsf(t1) * SLAB_WIDEN;
@@ -108,15 +173,26 @@ namespace rtk {
 // intersects hit leaves in slot order, then continues with the nearest hit inner
 // child (sorted by a 19-comparator network on packed (t | slot) keys) and pushes
 // the others far → near.  Returns false when the traversal is finished.
-RT_D bool closest_step(const DevScene& S, float3 o, float3 d, float3 inv, bool nansafe, float tmin, Best& best,
+RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, Best& best,
                        uint32_t& node, int& sp, uint32_t* stack, bool& ok) {
     float tn[8];
     uint32_t ch[8];
-    uint32_t mask = nansafe ? node_test<true>(S, node, o, inv, tmin, best.t, tn, ch)
-                            : node_test<false>(S, node, o, inv, tmin, best.t, tn, ch);
+    // the closest hit so far bounds the boxes; widened like every exit distance
+    float cwin = best.t + fabsf(best.t) * SLAB_WIDEN;
+    uint32_t mask = node_test(S, node, R, tmin, R.general ? best.t : cwin, tn, ch);
+    uint32_t leaves = 0;
 #pragma unroll
-    for (int c = 0; c < 8; c++)
-        if ((mask >> c) & 1u && (ch[c] & RT_LEAF_BIT)) leaf_closest(S, ch[c], o, d, tmin, best);
+    for (int c = 0; c < 8; c++) leaves |= ((ch[c] & RT_LEAF_BIT) ? 1u : 0u) << c;
+    leaves &= mask;
+    if (leaves) {
+        const uint32_t* refs = reinterpret_cast<const uint32_t*>(S.nodes + (size_t)node * 14 + 12);
+#pragma unroll 1
+        while (leaves) {
+            int c = __ffs(leaves) - 1;
+            leaves &= leaves - 1;
+            leaf_closest(S, __ldg(refs + c), R.o, d, tmin, best);
+        }
+    }
     float cw = best.t + fabsf(best.t) * SLAB_WIDEN;
     uint32_t k[8];
     int n = 0;
@@ -131,7 +207,20 @@ RT_D bool closest_step(const DevScene& S, float3 o, float3 d, float3 inv, bool n
         node = stack[--sp];
         return true;
     }
-    if (n > 1) {
+    if (n == 2) {
+        // two inner children: continue with the nearer, push the farther
+        uint32_t a = 0xFFFFFFFFu, b = 0xFFFFFFFFu;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            if (k[c] == 0xFFFFFFFFu) continue;
+            if (a == 0xFFFFFFFFu) a = k[c]; else b = k[c];
+        }
+        uint32_t lo = min(a, b), hi = max(a, b);
+        if (sp + 1 > RT_STACK) { ok = false; return false; }
+        const uint32_t* refs = reinterpret_cast<const uint32_t*>(S.nodes + (size_t)node * 14 + 12);
+        stack[sp++] = __ldg(refs + (hi & 7u));
+        node = __ldg(refs + (lo & 7u));
+    } else if (n > 2) {
         CAS(0, 1) CAS(2, 3) CAS(4, 5) CAS(6, 7)
         CAS(0, 2) CAS(1, 3) CAS(4, 6) CAS(5, 7)
         CAS(1, 2) CAS(5, 6) CAS(0, 4) CAS(3, 7)
@@ -156,23 +245,30 @@ RT_D bool closest_step(const DevScene& S, float3 o, float3 d, float3 inv, bool n
 
 // One node visit of the any-hit traversal (bvh.rs:487-530).  Returns false when
 // finished; *hit is set when a primitive was hit.
-RT_D bool any_step(const DevScene& S, float3 o, float3 d, float3 inv, bool nansafe, float tmin, float tmax,
+RT_D bool any_step(const DevScene& S, const RayC& R, float3 d, float tmin, float tmax,
                    uint32_t& node, int& sp, uint32_t* stack, bool& hit, bool& ok) {
     float tn[8];
     uint32_t ch[8];
-    uint32_t mask = nansafe ? node_test<true>(S, node, o, inv, tmin, tmax, tn, ch)
-                            : node_test<false>(S, node, o, inv, tmin, tmax, tn, ch);
-    uint32_t inner = 0;
+    float tw = tmax + fabsf(tmax) * SLAB_WIDEN;
+    uint32_t mask = node_test(S, node, R, tmin, R.general ? tmax : tw, tn, ch);
+    uint32_t inner = 0, leaves = 0;
 #pragma unroll
     for (int c = 0; c < 8; c++) {
-        if (!((mask >> c) & 1u)) continue;
-        if (ch[c] & RT_LEAF_BIT) {
-            if (!hit && leaf_any(S, ch[c], o, d, tmin, tmax)) hit = true;
-        } else {
-            inner |= 1u << c;
+        bool lf = ch[c] & RT_LEAF_BIT;
+        leaves |= (lf ? 1u : 0u) << c;
+        inner |= (lf ? 0u : 1u) << c;
+    }
+    leaves &= mask;
+    inner &= mask;
+    if (leaves) {
+        const uint32_t* refs = reinterpret_cast<const uint32_t*>(S.nodes + (size_t)node * 14 + 12);
+#pragma unroll 1
+        while (leaves) {
+            int c = __ffs(leaves) - 1;
+            leaves &= leaves - 1;
+            if (leaf_any(S, __ldg(refs + c), R.o, d, tmin, tmax)) { hit = true; return false; }
         }
     }
-    if (hit) return false;
     if (inner == 0) {
         if (sp == 0) return false;
         node = stack[--sp];
@@ -216,8 +312,8 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_closest(DevScene S, PathStat
     bool active = false, exhausted = false, ok = true;
     uint32_t item = 0, node = 0, pid = 0;
     int sp = 0;
-    float3 o = mk(0.f, 0.f, 0.f), d = o, inv = o;
-    bool nansafe = false;
+    float3 o = mk(0.f, 0.f, 0.f), d = o;
+    RayC R = make_rayc(o, mk(1.f, 1.f, 1.f), 0.0f);
     float tmin = 0.0f;
     Best best{0.0f, 0.0f, 0.0f, RT_MISS_REF, 0xFFFFFFFFu};
     while (true) {
@@ -242,8 +338,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_closest(DevScene S, PathStat
                         o = mk(r[0], r[1], r[2]); d = mk(r[3], r[4], r[5]);
                         tmin = r[6]; tmax = r[7];
                     }
-                    inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-                    nansafe = isinf(inv.x) || isinf(inv.y) || isinf(inv.z);
+                    R = make_rayc(o, d, tmin);
                     best = Best{tmax, 0.0f, 0.0f, RT_MISS_REF, 0xFFFFFFFFu};
                     node = 0; sp = 0;
                     active = !rtk::nan_ray(o, d, tmin, tmax);
@@ -257,7 +352,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_closest(DevScene S, PathStat
         if (exhausted && __ballot_sync(FULLMASK, active) == 0) break;
         if (active) {
             bool lok = true;
-            bool more = rtk::closest_step(S, o, d, inv, nansafe, tmin, best, node, sp, stack, lok);
+            bool more = rtk::closest_step(S, R, d, tmin, best, node, sp, stack, lok);
             if (!lok) ok = false;
             if (!more) {
                 active = false;
@@ -287,8 +382,8 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_any(DevScene S, PathState P,
     bool active = false, exhausted = false, ok = true;
     uint32_t item = 0, node = 0, tag = 0;
     int sp = 0;
-    float3 o = mk(0.f, 0.f, 0.f), d = o, inv = o;
-    bool nansafe = false;
+    float3 o = mk(0.f, 0.f, 0.f), d = o;
+    RayC R = make_rayc(o, mk(1.f, 1.f, 1.f), 0.0f);
     float tmin = 0.0f, tmax = 0.0f;
     bool hit = false;
     while (true) {
@@ -312,8 +407,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_any(DevScene S, PathState P,
                         o = mk(r[0], r[1], r[2]); d = mk(r[3], r[4], r[5]);
                         tmin = r[6]; tmax = r[7];
                     }
-                    inv = mk(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-                    nansafe = isinf(inv.x) || isinf(inv.y) || isinf(inv.z);
+                    R = make_rayc(o, d, tmin);
                     node = 0; sp = 0; hit = false;
                     active = !rtk::nan_ray(o, d, tmin, tmax);
                     if (!active && MODE == 1) out[i] = 0;
@@ -323,7 +417,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_any(DevScene S, PathState P,
         if (exhausted && __ballot_sync(FULLMASK, active) == 0) break;
         if (active) {
             bool lok = true;
-            bool more = rtk::any_step(S, o, d, inv, nansafe, tmin, tmax, node, sp, stack, hit, lok);
+            bool more = rtk::any_step(S, R, d, tmin, tmax, node, sp, stack, hit, lok);
             if (!lok) ok = false;
             if (!more) {
                 active = false;
