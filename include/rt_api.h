@@ -214,6 +214,50 @@ int32_t rt_render_accumulate(RtScene* scene, const RtCamera* cam, const RtPassPa
                              float firefly_floor, int32_t reset,
                              float* out_sum, float* out_m2, uint32_t* out_count, int32_t mem);
 
+/* ── caustic photon map (src/photon.rs, src/scene.rs:35-74) ──────────────── */
+#define RT_EMIT_DISK     0   /* directional disk facing `dir` (PhotonMap::build, photon.rs:41-94) */
+#define RT_EMIT_QUAD     1   /* cosine-weighted quad (PhotonMap::build_from_quad, photon.rs:97-135) */
+#define RT_MAX_EMITTERS  8
+
+typedef struct RtPhotonEmitter {
+    int32_t  type;          /* RT_EMIT_* */
+    float    dir[3];        /* DISK: direction toward the source (sun_dir) */
+    float    color[3];      /* DISK: sun colour (radiance · π); QUAD: emission colour */
+    float    corner[3];     /* QUAD corner, edges u and v */
+    float    u[3], v[3];
+    uint32_t n_photons;     /* photons emitted by this source */
+} RtPhotonEmitter;
+
+typedef struct RtPhotonParams {
+    int32_t  n_emitters;
+    RtPhotonEmitter emitters[RT_MAX_EMITTERS];
+    float    gather_radius; /* Epanechnikov radius (photon.rs:137-157), or the k-NN maximum radius */
+    uint32_t knn_k;         /* 0: fixed-radius gather (the reference); k > 0: k nearest within the radius */
+    uint64_t seed;
+} RtPhotonParams;
+
+/* Emit, trace and store photons on the device, then build the gather
+ * structure (Morton-sorted photons under an implicit box tree).  Replaces
+ * SceneData::rebuild_caustics → PhotonMap::build/_from_quad (scene.rs:35-74,
+ * photon.rs:41-135, trace_photon :232-277, kd_build :165-191).  The map then
+ * feeds every diffuse vertex of later render calls (renderer.rs:461-467). */
+int32_t rt_photon_build(RtScene* scene, const RtPhotonParams* params, int64_t* n_stored);
+/* Replace the map with caller-given photons (n × 3 positions, powers, normals;
+ * indices = emission index used to break distance ties). */
+int32_t rt_photon_set(RtScene* scene, const float* pos, const float* power, const float* nor,
+                      const int32_t* index, int64_t n, float gather_radius, uint32_t knn_k);
+int32_t rt_photon_clear(RtScene* scene);
+/* Stored photons in emission order (NULL arrays query the count). */
+int32_t rt_photon_export(const RtScene* scene, float* pos, float* power, float* nor, int32_t* index,
+                         int64_t* n);
+/* Irradiance estimate at n queries (n × 6: position, surface normal) → n × 3
+ * (PhotonMap::irradiance, photon.rs:148-157, or the k-NN estimate). */
+int32_t rt_photon_gather(RtScene* scene, const float* queries, int64_t n, float* irr, int32_t mem);
+/* k nearest photons of n query points with d² ≤ rmax²: emission indices and
+ * d², sorted by (d², index); -1 / INFINITY pad when fewer exist. */
+int32_t rt_knn(RtScene* scene, const float* queries, int64_t n, int32_t k, float rmax,
+               int32_t* idx, float* d2, int32_t mem);
+
 /* Device timing of the last render call: total milliseconds and ray counts. */
 int32_t rt_last_render_stats(const RtScene* scene, double* ms, int64_t* ext_rays,
                              int64_t* shadow_rays, int64_t* kernel_launches);

@@ -60,6 +60,12 @@ def lib():
         L.orc_lights_pdf_value.argtypes = [vp, fp, fp]
         L.orc_lights_pdf_value.restype = f
         L.orc_rng.argtypes = [C.c_uint64, u32, u32, u32, C.POINTER(u32), fp]
+        ip = C.POINTER(C.c_int32)
+        L.orc_photon_build.argtypes = [vp, C.POINTER(abi.RtPhotonParams), C.POINTER(i64), i32]
+        L.orc_photon_set.argtypes = [vp, fp, fp, fp, ip, i64, f, u32]
+        L.orc_photon_export.argtypes = [vp, fp, fp, fp, ip, C.POINTER(i64)]
+        L.orc_photon_gather.argtypes = [vp, fp, i64, fp, i32]
+        L.orc_knn.argtypes = [vp, fp, i64, i32, f, ip, fp, i32]
         _lib = L
     return _lib
 
@@ -164,6 +170,42 @@ class OracleScene:
                               threads, rb, re, cnt.ctypes.data_as(C.POINTER(C.c_int64)))
         self.last_counters = cnt
         return out
+
+    # ── caustic photon map ─────────────────────────────────────────────────
+    def photon_build(self, params, threads=os.cpu_count()):
+        n = C.c_int64()
+        rc = lib().orc_photon_build(self.h, C.byref(params), C.byref(n), threads)
+        if rc != 0:
+            raise ValueError(f"photon build failed ({rc})")
+        return n.value
+
+    def photon_set(self, pos, power, nor, index=None, radius=0.1, knn_k=0):
+        pos, power, nor = _f(pos).reshape(-1, 3), _f(power).reshape(-1, 3), _f(nor).reshape(-1, 3)
+        idx = None if index is None else np.ascontiguousarray(index, dtype=np.int32)
+        lib().orc_photon_set(self.h, _fp(pos), _fp(power), _fp(nor),
+                             None if idx is None else idx.ctypes.data_as(C.POINTER(C.c_int32)), len(pos), radius, knn_k)
+
+    def photon_export(self):
+        n = C.c_int64()
+        lib().orc_photon_export(self.h, None, None, None, None, C.byref(n))
+        pos, power, nor = (np.zeros((n.value, 3), np.float32) for _ in range(3))
+        idx = np.zeros(n.value, np.int32)
+        lib().orc_photon_export(self.h, _fp(pos), _fp(power), _fp(nor), idx.ctypes.data_as(C.POINTER(C.c_int32)),
+                                C.byref(n))
+        return pos, power, nor, idx
+
+    def photon_gather(self, queries, threads=os.cpu_count()):
+        q = _f(queries).reshape(-1, 6)
+        out = np.zeros((len(q), 3), np.float32)
+        lib().orc_photon_gather(self.h, _fp(q), len(q), _fp(out), threads)
+        return out
+
+    def knn(self, queries, k, rmax, threads=os.cpu_count()):
+        q = _f(queries).reshape(-1, 3)
+        idx = np.zeros((len(q), k), np.int32)
+        d2 = np.zeros((len(q), k), np.float32)
+        lib().orc_knn(self.h, _fp(q), len(q), k, rmax, idx.ctypes.data_as(C.POINTER(C.c_int32)), _fp(d2), threads)
+        return idx, d2
 
     def env_sample(self, d):
         out = np.zeros(3, np.float32)

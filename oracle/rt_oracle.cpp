@@ -388,6 +388,13 @@ struct Scene {
     std::vector<Node> nodes;
     std::vector<int32_t> leaf_prims;  // leaf slot → canonical prim id
     int64_t n_tris = 0, n_quads = 0, n_spheres = 0;
+    // caustic photon map (photon.rs:31-36): implicit kd-tree, kept in emission order too
+    struct KdPhoton { float pos[3], power[3], nor[3]; uint8_t axis; int32_t idx; };
+    std::vector<KdPhoton> photons;    // kd order
+    std::vector<KdPhoton> photons_by_index;
+    bool has_photons = false;
+    float gather_r2 = 0.0f, gather_norm = 0.0f;
+    uint32_t knn_k = 0;
 };
 
 static inline int prim_type(const Scene& s, int64_t gid) {
@@ -967,6 +974,258 @@ static V3 bg_eval(const Scene& s, V3 dir) {                                     
 static V3 env_eval(const Scene& s, V3 dir) { return s.has_env ? env_sample(s.env, dir) : v3(0, 0, 0); }
 static float env_pdf_value(const Scene& s, V3 dir) { return s.has_env ? env_dir_pdf(s.env, dir) : 0.0f; }
 
+// ── caustic photon map (photon.rs) ───────────────────────────────────────────
+typedef Scene::KdPhoton KdPhoton;
+
+// kd_build (photon.rs:165-191): median on the widest axis, implicit tree whose
+// root is the middle element of the slice.
+static void kd_build(KdPhoton* nodes, size_t n) {
+    if (n == 0) return;
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) { mn[k] = std::min(mn[k], nodes[i].pos[k]); mx[k] = std::max(mx[k], nodes[i].pos[k]); }
+    int axis = 0;
+    for (int k = 1; k < 3; k++) if (mx[k] - mn[k] > mx[axis] - mn[axis]) axis = k;
+    size_t mid = n / 2;
+    std::nth_element(nodes, nodes + mid, nodes + n,
+                     [axis](const KdPhoton& a, const KdPhoton& b) { return a.pos[axis] < b.pos[axis]; });
+    nodes[mid].axis = (uint8_t)axis;
+    kd_build(nodes, mid);
+    kd_build(nodes + mid + 1, n - mid - 1);
+}
+
+// kd_gather (photon.rs:195-228): Σ power·(1 − d²/r²) over d² < r², n_p·n > 0.
+static void kd_gather(const KdPhoton* nodes, size_t n, const float p[3], float r2, const float nrm[3], V3& acc) {
+    if (n == 0) return;
+    size_t mid = n / 2;
+    const KdPhoton& nd = nodes[mid];
+    float dx = nd.pos[0] - p[0], dy = nd.pos[1] - p[1], dz = nd.pos[2] - p[2];
+    float d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 < r2) {
+        float dt = nd.nor[0] * nrm[0] + nd.nor[1] * nrm[1] + nd.nor[2] * nrm[2];
+        if (dt > 0.0f) acc = acc + v3(nd.power[0], nd.power[1], nd.power[2]) * (1.0f - d2 / r2);
+    }
+    int axis = nd.axis;
+    float sq = p[axis] - nd.pos[axis];
+    if (sq <= 0.0f) {
+        kd_gather(nodes, mid, p, r2, nrm, acc);
+        if (sq * sq < r2) kd_gather(nodes + mid + 1, n - mid - 1, p, r2, nrm, acc);
+    } else {
+        kd_gather(nodes + mid + 1, n - mid - 1, p, r2, nrm, acc);
+        if (sq * sq < r2) kd_gather(nodes, mid, p, r2, nrm, acc);
+    }
+}
+
+// every photon with d² ≤ r2 (or < r2 when `strict`), optionally on the normal's side
+static void kd_collect(const KdPhoton* nodes, size_t n, const float p[3], float r2, bool strict, const float* nrm,
+                       std::vector<std::pair<float, const KdPhoton*>>& out) {
+    if (n == 0) return;
+    size_t mid = n / 2;
+    const KdPhoton& nd = nodes[mid];
+    float dx = nd.pos[0] - p[0], dy = nd.pos[1] - p[1], dz = nd.pos[2] - p[2];
+    float d2 = dx * dx + dy * dy + dz * dz;
+    if (strict ? d2 < r2 : d2 <= r2) {
+        bool ok = true;
+        if (nrm) ok = nd.nor[0] * nrm[0] + nd.nor[1] * nrm[1] + nd.nor[2] * nrm[2] > 0.0f;
+        if (ok) out.emplace_back(d2, &nd);
+    }
+    int axis = nd.axis;
+    float sq = p[axis] - nd.pos[axis];
+    if (sq <= 0.0f) {
+        kd_collect(nodes, mid, p, r2, strict, nrm, out);
+        if (sq * sq <= r2) kd_collect(nodes + mid + 1, n - mid - 1, p, r2, strict, nrm, out);
+    } else {
+        kd_collect(nodes + mid + 1, n - mid - 1, p, r2, strict, nrm, out);
+        if (sq * sq <= r2) kd_collect(nodes, mid, p, r2, strict, nrm, out);
+    }
+}
+
+// Irradiance estimate at (p, n).  knn_k = 0: the reference's fixed-radius
+// Epanechnikov estimate × 2/(π² r²) (photon.rs:137-157).  knn_k > 0: the same
+// kernel with the radius r_k = distance of the k-th nearest photon on the
+// normal's side within the maximum radius (the maximum radius when fewer than
+// k exist); the k-th photon itself gets weight 0, so the estimate equals the
+// fixed-radius gather at r_k.
+static V3 photon_irradiance(const Scene& s, V3 p, V3 n) {
+    V3 acc = v3(0, 0, 0);
+    if (!s.has_photons || s.photons.empty()) return acc;
+    float pp[3] = {p.x, p.y, p.z}, nn[3] = {n.x, n.y, n.z};
+    float r2 = s.gather_r2;
+    if (s.knn_k > 0) {
+        std::vector<std::pair<float, const KdPhoton*>> c;
+        kd_collect(s.photons.data(), s.photons.size(), pp, r2, true, nn, c);
+        if (c.size() >= s.knn_k) {
+            std::nth_element(c.begin(), c.begin() + (s.knn_k - 1), c.end(),
+                             [](const std::pair<float, const KdPhoton*>& a, const std::pair<float, const KdPhoton*>& b) {
+                                 return a.first < b.first;
+                             });
+            r2 = c[s.knn_k - 1].first;
+        }
+        if (!(r2 > 0.0f)) return acc;
+    }
+    kd_gather(s.photons.data(), s.photons.size(), pp, r2, nn, acc);
+    return acc * (2.0f / (PI_F * PI_F * r2));
+}
+
+// trace_photon (photon.rs:232-277): one wavelength per photon, at most 12
+// bounces; stored at the first diffuse hit after ≥ 1 specular bounce.  Each new
+// segment is a fresh ray (spectral_weighted = false), so every refraction of a
+// spectral dielectric and every conductor bounce applies its colour tint.
+enum { P_EMIT0 = 0, P_EMIT1 = 1, P_EMIT2 = 2, P_EMIT3 = 3, P_LAMBDA = 4, P_BOUNCE0 = 8, P_PER_BOUNCE = 4 };
+static const int PHOTON_MAX_DEPTH = 12;
+
+static bool trace_photon(const Scene& s, V3 pos, V3 dir, float lum_clamp, V3 power, const Rng& rng, KdPhoton* out) {
+    float lam = s.spec.lam_lo + s.spec.lam_range * rnd(rng, P_LAMBDA);
+    if (lam >= s.spec.lam_lo + s.spec.lam_range) lam = std::nextafter(s.spec.lam_lo + s.spec.lam_range, 0.0f);
+    uint32_t spec_depth = 0;
+    for (int bounce = 0; bounce < PHOTON_MAX_DEPTH; bounce++) {
+        uint32_t base = P_BOUNCE0 + bounce * P_PER_BOUNCE;
+        Ray ray{pos, dir};
+        HitRes h = closest_hit<false>(s, ray, 0.001f, INFINITY, nullptr);
+        if (h.gid < 0) return false;
+        Rec rec = make_rec(s, ray, h);
+        const RtMaterial& m = s.mats[rec.mat];
+        if (m.type == RT_MAT_DIFFUSE_LIGHT || m.type == RT_MAT_BLACKBODY_LIGHT) return false;   // scatter → None
+        V3 unit_dir = unit(ray.d);
+        if (m.type == RT_MAT_DIELECTRIC || m.type == RT_MAT_SPECTRAL_DIELECTRIC) {
+            bool spectral = m.type == RT_MAT_SPECTRAL_DIELECTRIC;
+            float ior = spectral ? cauchy_ior(lam, m.cauchy_b, m.cauchy_c) : m.cauchy_b;
+            float ratio = rec.front ? 1.0f / ior : ior;
+            float cos_t = rmin(dot(-unit_dir, rec.normal), 1.0f);
+            float sin_t = std::sqrt(1.0f - cos_t * cos_t);
+            bool reflected = ratio * sin_t > 1.0f || fresnel_dielectric(cos_t, ratio) > rnd(rng, base + 0);
+            V3 nd;
+            if (reflected) nd = reflect(unit_dir, rec.normal);
+            else if (!refract(unit_dir, rec.normal, ratio, &nd)) nd = reflect(unit_dir, rec.normal);
+            V3 att = v3(1, 1, 1);
+            if (spectral) {
+                if (!reflected) att = spectral_fire_rgb(s.spec, lam);
+                if (!rec.front) {
+                    att.x *= std::exp(-m.absorption[0] * rec.t);
+                    att.y *= std::exp(-m.absorption[1] * rec.t);
+                    att.z *= std::exp(-m.absorption[2] * rec.t);
+                }
+            }
+            power = power * att;
+            pos = rec.p; dir = nd;
+            spec_depth++;
+        } else if (m.type == RT_MAT_SPECTRAL_METAL) {
+            V3 n = rec.normal;
+            V3 wo = unit(-ray.d);
+            float cos_o = dot(wo, n);
+            if (cos_o <= 0.0f) return false;
+            float alpha = rmax(m.roughness * m.roughness, 1e-4f);
+            V3 nd; float cos_h;
+            if (m.roughness == 0.0f) { nd = reflect(unit_dir, n); cos_h = cos_o; }
+            else {
+                V3 t, b;
+                onb_vec(n, &t, &b);
+                V3 wo_ts = v3(dot(wo, t), dot(wo, b), cos_o);
+                V3 m_ts = vndf_sample(wo_ts, alpha, alpha, rnd(rng, base + 0), rnd(rng, base + 1));
+                V3 mm = unit(t * m_ts.x + b * m_ts.y + n * m_ts.z);
+                float vo_h = rmax(dot(wo, mm), 0.0f);
+                V3 wi = unit(2.0f * vo_h * mm - wo);
+                if (dot(wi, n) <= 0.0f) return false;
+                nd = wi; cos_h = vo_h;
+            }
+            if (dot(nd, n) <= 0.0f) return false;
+            float weight = 1.0f;
+            if (m.roughness != 0.0f) {
+                float lam_o = smith_lambda(cos_o, alpha);
+                float lam_i = smith_lambda(rmax(dot(nd, n), 0.0f), alpha);
+                weight = ((1.0f + lam_o) / (1.0f + lam_o + lam_i)) * specular_energy_comp(cos_o, alpha);
+            }
+            float nn, kk;
+            metal_ior(m, lam, &nn, &kk);
+            power = power * (spectral_to_rgb(s.spec, lam) * (fresnel_conductor(cos_h, nn, kk) * weight));
+            pos = rec.p; dir = nd;
+            spec_depth++;
+        } else {
+            // diffuse (Lambertian / checker): can_receive_caustics (material.rs:101)
+            if (spec_depth == 0) return false;
+            float lum = luminance(power);
+            if (lum > lum_clamp) power = power * (lum_clamp / lum);
+            KdPhoton k;
+            k.pos[0] = rec.p.x; k.pos[1] = rec.p.y; k.pos[2] = rec.p.z;
+            k.power[0] = power.x; k.power[1] = power.y; k.power[2] = power.z;
+            k.nor[0] = rec.normal.x; k.nor[1] = rec.normal.y; k.nor[2] = rec.normal.z;
+            k.axis = 0;
+            *out = k;
+            return true;
+        }
+    }
+    return false;
+}
+
+static inline Rng photon_rng(uint64_t seed, uint32_t gid) {
+    Rng r;
+    r.a = gid;
+    r.b = mix32((uint32_t)seed) ^ 0x50484F54u;
+    r.c = mix32((uint32_t)(seed >> 32) + 0x9E3779B9u);
+    return r;
+}
+
+// photon_bounds of the world (hittable.rs:199-212): union of the primitive boxes
+static Aabb world_bounds(const Scene& s) {
+    int64_t n = s.n_tris + s.n_quads + s.n_spheres;
+    Aabb b = prim_box(s, 0);
+    for (int64_t i = 1; i < n; i++) b = surrounding(b, prim_box(s, i));
+    return b;
+}
+
+// Emitter geometry for photon `i` of emitter `e` (photon.rs:41-94, 97-135).
+struct EmitterSetup { V3 t, b, center, dir, power, normal, corner, u, v, ta, ba; float radius, lum_clamp; int type; };
+static EmitterSetup setup_emitter(const Scene& s, const RtPhotonEmitter& e) {
+    EmitterSetup E{};
+    E.type = e.type;
+    if (e.type == RT_EMIT_DISK) {
+        V3 sun = v3(e.dir[0], e.dir[1], e.dir[2]);
+        V3 sun_down = unit(-sun);
+        V3 up = std::fabs(sun_down.x) < 0.999f ? v3(1, 0, 0) : v3(0, 1, 0);
+        E.t = unit(cross(sun_down, up));
+        E.b = cross(sun_down, E.t);
+        const float CLIP = 1.0e3f;
+        Aabb bb = world_bounds(s);
+        auto clip = [&](float x) { return clampf(x, -CLIP, CLIP); };
+        V3 mn = v3(clip(bb.mn.x), clip(bb.mn.y), clip(bb.mn.z)), mx = v3(clip(bb.mx.x), clip(bb.mx.y), clip(bb.mx.z));
+        V3 c = (mn + mx) * 0.5f;
+        float r = rmax(length(mx - mn) * 0.5f, 1.0e-3f);
+        E.center = c + unit(sun) * r;
+        E.radius = r;
+        float disk_area = PI_F * r * r;
+        E.power = v3(e.color[0], e.color[1], e.color[2]) * (disk_area / ((float)e.n_photons * PI_F));
+        E.lum_clamp = 15.0f * disk_area / (PI_F * 20.0f * 20.0f);
+        E.dir = sun_down;
+    } else {
+        E.corner = v3(e.corner[0], e.corner[1], e.corner[2]);
+        E.u = v3(e.u[0], e.u[1], e.u[2]);
+        E.v = v3(e.v[0], e.v[1], e.v[2]);
+        V3 cr = cross(E.u, E.v);
+        float area = length(cr);
+        E.normal = cr / area;
+        onb_vec(E.normal, &E.ta, &E.ba);
+        E.power = v3(e.color[0], e.color[1], e.color[2]) * (area * PI_F / (float)e.n_photons);
+        E.lum_clamp = 15.0f;
+    }
+    return E;
+}
+
+static void emit_photon(const EmitterSetup& E, const Rng& rng, V3* pos, V3* dir) {
+    if (E.type == RT_EMIT_DISK) {
+        float r = E.radius * std::sqrt(rnd(rng, P_EMIT0));
+        float phi = 2.0f * PI_F * rnd(rng, P_EMIT1);
+        *pos = E.center + E.t * (r * std::cos(phi)) + E.b * (r * std::sin(phi));
+        *dir = E.dir;
+    } else {
+        float ss = rnd(rng, P_EMIT0), tt = rnd(rng, P_EMIT1);
+        *pos = E.corner + E.u * ss + E.v * tt;
+        float ct = std::sqrt(rnd(rng, P_EMIT2));
+        float st = std::sqrt(1.0f - ct * ct);
+        float phi = 2.0f * PI_F * rnd(rng, P_EMIT3);
+        *dir = st * std::cos(phi) * E.ta + st * std::sin(phi) * E.ba + ct * E.normal;
+    }
+}
+
 // ── hero-wavelength state ────────────────────────────────────────────────────
 // The reference path carries an RGB throughput that, after the first spectral
 // event, includes the CMF tint of its single wavelength (material.rs:384-400,
@@ -1132,6 +1391,11 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
         } else {
             // Lambertian / checker (material.rs:85-102): diffuse branch renderer.rs:457-572
             V3 att = lambert_albedo(m, rec.p);
+            if (s.has_photons) {                                                    // renderer.rs:461-467
+                V3 irr = photon_irradiance(s, rec.p, rec.normal);
+                if (irr.x > 0.0f || irr.y > 0.0f || irr.z > 0.0f)
+                    color = color + (T * spec_factor(s.spec, ss)) * att * irr;
+            }
             if (have_lights) {
                 uint32_t pick = rnd_u32(rng, base + B_LPICK) % (uint32_t)s.lights.size();
                 V3 light_dir = prim_pdf_generate(s, s.lights[pick], rec.p, rnd(rng, base + B_LPT0), rnd(rng, base + B_LPT1));
@@ -1522,6 +1786,119 @@ float orc_lights_pdf_value(void* sp, const float* o, const float* d) {
 void orc_rng(uint64_t seed, uint32_t pixel, uint32_t sample, uint32_t dim, uint32_t* u, float* f) {
     Rng r = make_rng(seed, pixel, sample);
     *u = rnd_u32(r, dim); *f = rnd(r, dim);
+}
+
+}  // extern "C"
+
+// ── photon map entry points ───────────────────────────────────────────────────
+extern "C" {
+
+static void photon_finish(Scene* s, std::vector<KdPhoton>&& ph, float radius, uint32_t k) {
+    s->photons_by_index = ph;
+    s->photons = std::move(ph);
+    kd_build(s->photons.data(), s->photons.size());
+    s->has_photons = true;
+    s->gather_r2 = radius * radius;
+    s->gather_norm = 2.0f / (PI_F * PI_F * radius * radius);
+    s->knn_k = k;
+}
+
+int32_t orc_photon_build(void* sp, const RtPhotonParams* p, int64_t* n_stored, int32_t threads) {
+    Scene* s = (Scene*)sp;
+    if (!p || p->n_emitters < 0 || p->n_emitters > RT_MAX_EMITTERS || !(p->gather_radius > 0.0f)) return RT_ERR_INVALID;
+    uint32_t total = 0;
+    for (int e = 0; e < p->n_emitters; e++) total += p->emitters[e].n_photons;
+    std::vector<KdPhoton> slot(total);
+    std::vector<uint8_t> ok(total, 0);
+    uint32_t off = 0;
+    for (int e = 0; e < p->n_emitters; e++) {
+        const RtPhotonEmitter& em = p->emitters[e];
+        if (em.n_photons == 0) continue;
+        EmitterSetup E = setup_emitter(*s, em);
+        uint32_t n = em.n_photons, base = off;
+        uint32_t chunk = 4096, nch = (n + chunk - 1) / chunk;
+        parallel_rows(nch, threads, [&](uint32_t c, int) {
+            for (uint32_t i = c * chunk; i < std::min(n, (c + 1) * chunk); i++) {
+                uint32_t gid = base + i;
+                Rng rng = photon_rng(p->seed, gid);
+                V3 pos, dir;
+                emit_photon(E, rng, &pos, &dir);
+                KdPhoton k;
+                if (trace_photon(*s, pos, dir, E.lum_clamp, E.power, rng, &k)) {
+                    k.idx = (int32_t)gid;
+                    slot[gid] = k;
+                    ok[gid] = 1;
+                }
+            }
+        });
+        off += n;
+    }
+    std::vector<KdPhoton> ph;
+    for (uint32_t i = 0; i < total; i++) if (ok[i]) ph.push_back(slot[i]);
+    if (n_stored) *n_stored = (int64_t)ph.size();
+    photon_finish(s, std::move(ph), p->gather_radius, p->knn_k);
+    return RT_OK;
+}
+
+int32_t orc_photon_set(void* sp, const float* pos, const float* power, const float* nor, const int32_t* idx, int64_t n,
+                       float radius, uint32_t k) {
+    Scene* s = (Scene*)sp;
+    std::vector<KdPhoton> ph(n);
+    for (int64_t i = 0; i < n; i++) {
+        for (int c = 0; c < 3; c++) { ph[i].pos[c] = pos[i * 3 + c]; ph[i].power[c] = power[i * 3 + c]; ph[i].nor[c] = nor[i * 3 + c]; }
+        ph[i].axis = 0;
+        ph[i].idx = idx ? idx[i] : (int32_t)i;
+    }
+    photon_finish(s, std::move(ph), radius, k);
+    return RT_OK;
+}
+
+int32_t orc_photon_export(void* sp, float* pos, float* power, float* nor, int32_t* idx, int64_t* n) {
+    Scene* s = (Scene*)sp;
+    if (n) *n = (int64_t)s->photons_by_index.size();
+    for (size_t i = 0; pos && i < s->photons_by_index.size(); i++) {
+        const KdPhoton& k = s->photons_by_index[i];
+        for (int c = 0; c < 3; c++) { pos[i * 3 + c] = k.pos[c]; power[i * 3 + c] = k.power[c]; nor[i * 3 + c] = k.nor[c]; }
+        idx[i] = k.idx;
+    }
+    return RT_OK;
+}
+
+// queries n × 6 (p, n) → irradiance n × 3
+int32_t orc_photon_gather(void* sp, const float* q, int64_t n, float* irr, int32_t threads) {
+    Scene* s = (Scene*)sp;
+    int64_t chunk = 1024, nch = (n + chunk - 1) / chunk;
+    parallel_rows((uint32_t)nch, threads, [&](uint32_t c, int) {
+        for (int64_t i = c * chunk; i < std::min(n, (int64_t)(c + 1) * chunk); i++) {
+            V3 r = photon_irradiance(*s, v3(q[i * 6], q[i * 6 + 1], q[i * 6 + 2]), v3(q[i * 6 + 3], q[i * 6 + 4], q[i * 6 + 5]));
+            irr[i * 3] = r.x; irr[i * 3 + 1] = r.y; irr[i * 3 + 2] = r.z;
+        }
+    });
+    return RT_OK;
+}
+
+// k nearest photons with d² ≤ rmax², sorted by (d², emission index)
+int32_t orc_knn(void* sp, const float* q, int64_t n, int32_t k, float rmax, int32_t* out_idx, float* out_d2, int32_t threads) {
+    Scene* s = (Scene*)sp;
+    float r2 = rmax * rmax;
+    int64_t chunk = 256, nch = (n + chunk - 1) / chunk;
+    parallel_rows((uint32_t)nch, threads, [&](uint32_t c, int) {
+        std::vector<std::pair<float, const KdPhoton*>> cand;
+        for (int64_t i = c * chunk; i < std::min(n, (int64_t)(c + 1) * chunk); i++) {
+            cand.clear();
+            kd_collect(s->photons.data(), s->photons.size(), q + i * 3, r2, false, nullptr, cand);
+            std::sort(cand.begin(), cand.end(), [](const std::pair<float, const KdPhoton*>& a,
+                                                   const std::pair<float, const KdPhoton*>& b) {
+                return a.first < b.first || (a.first == b.first && a.second->idx < b.second->idx);
+            });
+            for (int j = 0; j < k; j++) {
+                bool have = j < (int)cand.size();
+                out_idx[i * k + j] = have ? cand[j].second->idx : -1;
+                out_d2[i * k + j] = have ? cand[j].first : INFINITY;
+            }
+        }
+    });
+    return RT_OK;
 }
 
 }  // extern "C"

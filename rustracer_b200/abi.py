@@ -128,3 +128,29 @@ def iptr(a):
     if a is None:
         return C.POINTER(C.c_int32)()
     return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+RT_EMIT_DISK, RT_EMIT_QUAD = 0, 1
+RT_MAX_EMITTERS = 8
+
+
+class RtPhotonEmitter(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("dir", F3),
+        ("color", F3),
+        ("corner", F3),
+        ("u", F3),
+        ("v", F3),
+        ("n_photons", C.c_uint32),
+    ]
+
+
+class RtPhotonParams(C.Structure):
+    _fields_ = [
+        ("n_emitters", C.c_int32),
+        ("emitters", RtPhotonEmitter * RT_MAX_EMITTERS),
+        ("gather_radius", C.c_float),
+        ("knn_k", C.c_uint32),
+        ("seed", C.c_uint64),
+    ]

@@ -22,6 +22,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 UNITS = [
     ("rt_trace.cu", ["--fmad=false"]),
     ("rt_shade.cu", []),
+    ("rt_photon.cu", []),
     ("rt_host.cu", []),
 ]
 

@@ -342,6 +342,9 @@ struct RtScene {
     // api staging
     void* stage = nullptr;
     size_t stage_bytes = 0;
+    // caustic photon map and the union of the primitive boxes (photon_bounds)
+    PhotonMapDev photons;
+    float world_lo[3] = {0, 0, 0}, world_hi[3] = {0, 0, 0};
     // per-stage profiling
     bool profiling = false;
     std::vector<cudaEvent_t> pev;
@@ -414,8 +417,9 @@ int32_t rt_scene_destroy(RtScene* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto& b : s->owned) cudaFree(b.p);
     void* ps[] = {s->P.ray_o, s->P.ray_d, s->P.hit, s->P.thr, s->P.wts, s->P.meta, s->P.L, s->P.pend0, s->P.pend1,
-                  s->queue[0], s->queue[1], s->sq, s->counters, s->d_err, s->scratch, s->d_conv, s->acc, s->m2,
-                  s->cnt, s->stage};
+                  s->P.pendC, s->P.gq, s->queue[0], s->queue[1], s->sq, s->counters, s->d_err, s->scratch,
+                  s->d_conv, s->acc, s->m2, s->cnt, s->stage};
+    s->photons.release();
     for (void* p : ps) if (p) cudaFree(p);
     for (int c = 0; c < CLS_N; c++) if (s->cq.q[c]) cudaFree(s->cq.q[c]);
     for (auto e : s->pev) cudaEventDestroy(e);
@@ -505,6 +509,12 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         const float* p = d->sphere + i * 4;
         H3 c = h3(p[0], p[1], p[2]), r = h3(p[3], p[3], p[3]);
         boxes[d->n_tris + d->n_quads + i] = Box{c - r, c + r};
+    }
+
+    if (n > 0) {
+        Box wb = boxes[0];
+        for (int64_t i = 1; i < n; i++) wb = unite(wb, boxes[i]);
+        for (int a = 0; a < 3; a++) { s->world_lo[a] = hc(wb.mn, a); s->world_hi[a] = hc(wb.mx, a); }
     }
 
     // ── BVH ─────────────────────────────────────────────────────────────────
@@ -901,7 +911,7 @@ static const uint32_t MAX_PATHS = 1u << 23;   // 8M paths in flight per chunk
 static int ensure_paths(RtScene* s, uint32_t cap) {
     if (s->cap >= cap) return RT_OK;
     void* ps[] = {s->P.ray_o, s->P.ray_d, s->P.hit, s->P.thr, s->P.wts, s->P.meta, s->P.L, s->P.pend0, s->P.pend1,
-                  s->queue[0], s->queue[1], s->sq};
+                  s->P.pendC, s->P.gq, s->queue[0], s->queue[1], s->sq};
     for (void* p : ps) if (p) cudaFree(p);
     for (int c = 0; c < CLS_N; c++) if (s->cq.q[c]) cudaFree(s->cq.q[c]);
     s->cq = ClassQueues{};
@@ -911,7 +921,8 @@ static int ensure_paths(RtScene* s, uint32_t cap) {
     s->cap = 0;
     size_t f4 = (size_t)cap * sizeof(float4);
     void** slots[] = {(void**)&s->P.ray_o, (void**)&s->P.ray_d, (void**)&s->P.hit, (void**)&s->P.thr, (void**)&s->P.wts,
-                      (void**)&s->P.meta, (void**)&s->P.L, (void**)&s->P.pend0, (void**)&s->P.pend1};
+                      (void**)&s->P.meta, (void**)&s->P.L, (void**)&s->P.pend0, (void**)&s->P.pend1,
+                      (void**)&s->P.pendC};
     for (void** sl : slots)
         if (cudaMalloc(sl, f4) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc path state");
     if (cudaMalloc(&s->queue[0], (size_t)cap * 4) != cudaSuccess || cudaMalloc(&s->queue[1], (size_t)cap * 4) != cudaSuccess ||
@@ -919,6 +930,8 @@ static int ensure_paths(RtScene* s, uint32_t cap) {
         return fail(s, RT_ERR_NOMEM, "cudaMalloc queues");
     for (int c = 0; c < CLS_N; c++)
         if (cudaMalloc(&s->cq.q[c], (size_t)cap * 4) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc class queues");
+    if (cudaMalloc(&s->P.gq, (size_t)cap * 2 * sizeof(float4)) != cudaSuccess)
+        return fail(s, RT_ERR_NOMEM, "cudaMalloc gather queue");
     if (!s->counters && cudaMalloc(&s->counters, sizeof(uint32_t) * (RT_MAX_DEPTH + 2) * RT_CTR_STRIDE) != cudaSuccess)
         return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
     s->cap = cap;
@@ -951,6 +964,7 @@ static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p,
         R.cam = *cam;
         R.converged = dconv;
         R.scratch = dscratch + (size_t)k0 * npix * 3;
+        R.photons = s->photons.present && s->photons.n > 0;
         CK(cudaMemsetAsync(s->counters, 0, sizeof(uint32_t) * (maxd + 2) * RT_CTR_STRIDE, s->stream));
         uint32_t* C = s->counters;
         size_t ev_used = 0;
@@ -991,6 +1005,8 @@ static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p,
             mark(2);
             rth::launch_shade(s->S, s->P, R, dpt, qin, c + CTR_COUNT, c, s->cq, qout, cn + CTR_COUNT, s->sq,
                               c + CTR_SHADOW_COUNT, s->sms, s->stream);
+            if (R.photons) rth::launch_photon_gather_paths(s->photons, s->P, s->P.gq, c + CTR_GATHER_COUNT, s->sms,
+                                                           s->stream);
             mark(3);
             rth::launch_shadow(s->S, s->P, s->sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, s->d_err, s->sms,
                                s->stream);
@@ -1243,6 +1259,8 @@ extern "C" int32_t rt_render_pass_noalloc(RtScene* s, const RtCamera* cam, const
         return fail(s, RT_ERR_CAPACITY, "rt_render_pass_noalloc: width*height = " + std::to_string(npix) +
                                             " exceeds the fixed scratch limit of " +
                                             std::to_string(RT_NOALLOC_MAX_PIXELS) + " pixels");
+    if (s->photons.present && s->photons.n > 0)
+        return fail(s, RT_ERR_INVALID, "rt_render_pass_noalloc does not render scenes with a photon map");
     CK(cudaSetDevice(s->device));
     void* base = nullptr;
     if ((rc = noalloc_base(s, &base))) return rc;
@@ -1298,4 +1316,180 @@ extern "C" int32_t rt_render_pass_noalloc(RtScene* s, const RtCamera* cam, const
     CK(cudaStreamSynchronize(s->stream));
     if (h) return fail(s, h, "traversal stack overflow");
     return RT_OK;
+}
+
+// ── photon map entry points ──────────────────────────────────────────────────
+// Emitter set-up of PhotonMap::build / build_from_quad (photon.rs:41-135):
+// 40 floats per emitter, consumed by the emission kernel.
+static void emitter_setup(const RtScene* s, const RtPhotonEmitter& e, float* f) {
+    const float PI = 3.14159265358979323846f;
+    memset(f, 0, 40 * sizeof(float));
+    auto put = [&](int at, H3 v) { f[at] = v.x; f[at + 1] = v.y; f[at + 2] = v.z; };
+    if (e.type == RT_EMIT_DISK) {
+        H3 sun = h3(e.dir[0], e.dir[1], e.dir[2]);
+        H3 ms = h3(-sun.x, -sun.y, -sun.z);
+        H3 sd = ms / hlen(ms);
+        H3 up = std::fabs(sd.x) < 0.999f ? h3(1, 0, 0) : h3(0, 1, 0);
+        H3 t = hcross(sd, up);
+        t = t / hlen(t);
+        H3 b = hcross(sd, t);
+        const float CLIP = 1.0e3f;
+        auto clip = [&](float x) { return std::min(std::max(x, -CLIP), CLIP); };
+        H3 mn = h3(clip(s->world_lo[0]), clip(s->world_lo[1]), clip(s->world_lo[2]));
+        H3 mx = h3(clip(s->world_hi[0]), clip(s->world_hi[1]), clip(s->world_hi[2]));
+        H3 c = (mn + mx) * 0.5f;
+        float r = std::fmax(hlen(mx - mn) * 0.5f, 1.0e-3f);
+        H3 su = sun / hlen(sun);
+        float area = PI * r * r;
+        put(0, t); put(3, b); put(6, c + su * r); put(9, sd);
+        put(30, h3(e.color[0], e.color[1], e.color[2]) * (area / ((float)e.n_photons * PI)));
+        f[33] = r;
+        f[34] = 15.0f * area / (PI * 20.0f * 20.0f);
+    } else {
+        H3 u = h3(e.u[0], e.u[1], e.u[2]), v = h3(e.v[0], e.v[1], e.v[2]);
+        H3 cr = hcross(u, v);
+        float area = hlen(cr);
+        H3 nrm = cr / area;
+        H3 up = std::fabs(nrm.y) < 0.9f ? h3(0, 1, 0) : h3(1, 0, 0);
+        H3 ta = hcross(nrm, up);
+        ta = ta / hlen(ta);
+        H3 ba = hcross(nrm, ta);
+        put(12, nrm); put(15, h3(e.corner[0], e.corner[1], e.corner[2])); put(18, u); put(21, v);
+        put(24, ta); put(27, ba);
+        put(30, h3(e.color[0], e.color[1], e.color[2]) * (area * PI / (float)e.n_photons));
+        f[34] = 15.0f;
+    }
+}
+
+extern "C" int32_t rt_photon_build(RtScene* s, const RtPhotonParams* p, int64_t* n_stored) {
+    if (!s || !p) return RT_ERR_INVALID;
+    if (p->n_emitters < 1 || p->n_emitters > RT_MAX_EMITTERS) return fail(s, RT_ERR_INVALID, "1..8 photon emitters");
+    if (!(p->gather_radius > 0.0f)) return fail(s, RT_ERR_INVALID, "gather radius must be positive");
+    if (p->knn_k > 4096) return fail(s, RT_ERR_INVALID, "knn_k must be ≤ 4096");
+    if (s->empty) return fail(s, RT_ERR_INVALID, "scene has no primitives");
+    uint64_t total = 0;
+    for (int i = 0; i < p->n_emitters; i++) {
+        const RtPhotonEmitter& e = p->emitters[i];
+        if (e.type != RT_EMIT_DISK && e.type != RT_EMIT_QUAD) return fail(s, RT_ERR_INVALID, "unknown emitter type");
+        if (e.n_photons == 0) return fail(s, RT_ERR_INVALID, "emitter with zero photons");
+        total += e.n_photons;
+    }
+    if (total > MAX_PATHS) return fail(s, RT_ERR_CAPACITY, "more than 8M photons per build");
+    CK(cudaSetDevice(s->device));
+    int rc = ensure_paths(s, (uint32_t)std::max<uint64_t>(total, s->cap));
+    if (rc) return rc;
+    std::vector<float> setup((size_t)p->n_emitters * 40);
+    for (int i = 0; i < p->n_emitters; i++) emitter_setup(s, p->emitters[i], &setup[(size_t)i * 40]);
+    cudaError_t e = rth::photon_build(s->S, s->photons, s->P, s->queue[0], s->queue[1], s->counters, *p, setup.data(),
+                                      s->sms, s->stream, n_stored);
+    if (e != cudaSuccess) return fail(s, RT_ERR_CUDA, std::string("photon build: ") + cudaGetErrorString(e));
+    return check_err(s);
+}
+
+extern "C" int32_t rt_photon_set(RtScene* s, const float* pos, const float* power, const float* nor,
+                                 const int32_t* index, int64_t n, float radius, uint32_t k) {
+    if (!s || n < 0 || (n > 0 && (!pos || !power || !nor))) return RT_ERR_INVALID;
+    if (!(radius > 0.0f)) return fail(s, RT_ERR_INVALID, "gather radius must be positive");
+    if (n > (int64_t)MAX_PATHS) return fail(s, RT_ERR_CAPACITY, "more than 8M photons");
+    CK(cudaSetDevice(s->device));
+    std::vector<float4> a(n), b(n), c(n);
+    for (int64_t i = 0; i < n; i++) {
+        int32_t id = index ? index[i] : (int32_t)i;
+        float fid;
+        memcpy(&fid, &id, 4);
+        a[i] = make_float4(pos[i * 3], pos[i * 3 + 1], pos[i * 3 + 2], fid);
+        b[i] = make_float4(power[i * 3], power[i * 3 + 1], power[i * 3 + 2], 0.f);
+        c[i] = make_float4(nor[i * 3], nor[i * 3 + 1], nor[i * 3 + 2], 0.f);
+    }
+    cudaError_t e = rth::photon_set(s->photons, a.data(), b.data(), c.data(), (uint32_t)n, radius, k, s->stream);
+    if (e != cudaSuccess) return fail(s, RT_ERR_CUDA, std::string("photon set: ") + cudaGetErrorString(e));
+    return RT_OK;
+}
+
+extern "C" int32_t rt_photon_clear(RtScene* s) {
+    if (!s) return RT_ERR_INVALID;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    s->photons.release();
+    return RT_OK;
+}
+
+extern "C" int32_t rt_photon_export(const RtScene* s, float* pos, float* power, float* nor, int32_t* index, int64_t* n) {
+    if (!s) return RT_ERR_INVALID;
+    uint32_t m = s->photons.present ? s->photons.n : 0;
+    if (n) *n = m;
+    if (!pos || m == 0) return RT_OK;
+    cudaSetDevice(s->device);
+    std::vector<float4> a(m), b(m), c(m);
+    cudaMemcpy(a.data(), s->photons.exp_pos, (size_t)m * 16, cudaMemcpyDeviceToHost);
+    cudaMemcpy(b.data(), s->photons.exp_pow, (size_t)m * 16, cudaMemcpyDeviceToHost);
+    cudaMemcpy(c.data(), s->photons.exp_nor, (size_t)m * 16, cudaMemcpyDeviceToHost);
+    for (uint32_t i = 0; i < m; i++) {
+        pos[i * 3] = a[i].x; pos[i * 3 + 1] = a[i].y; pos[i * 3 + 2] = a[i].z;
+        power[i * 3] = b[i].x; power[i * 3 + 1] = b[i].y; power[i * 3 + 2] = b[i].z;
+        nor[i * 3] = c[i].x; nor[i * 3 + 1] = c[i].y; nor[i * 3 + 2] = c[i].z;
+        if (index) memcpy(&index[i], &a[i].w, 4);
+    }
+    return RT_OK;
+}
+
+extern "C" int32_t rt_photon_gather(RtScene* s, const float* q, int64_t n, float* irr, int32_t mem) {
+    if (!s || n < 0 || (n > 0 && (!q || !irr))) return RT_ERR_INVALID;
+    if (n == 0) return RT_OK;
+    CK(cudaSetDevice(s->device));
+    if (!s->photons.present || s->photons.n == 0) {
+        if (mem == RT_MEM_DEVICE) { CK(cudaMemsetAsync(irr, 0, n * 12, s->stream)); return RT_OK; }
+        memset(irr, 0, n * 12);
+        return RT_OK;
+    }
+    const float* dq = q;
+    float* dout = irr;
+    size_t qb = (size_t)n * 24, ob = (size_t)n * 12;
+    if (mem != RT_MEM_DEVICE) {
+        int rc = ensure_stage(s, qb + ob + 256);
+        if (rc) return rc;
+        dq = (const float*)s->stage;
+        dout = (float*)((char*)s->stage + ((qb + 255) & ~(size_t)255));
+        CK(cudaMemcpyAsync((void*)dq, q, qb, cudaMemcpyHostToDevice, s->stream));
+    }
+    rth::launch_photon_gather_api(s->photons, dq, (uint32_t)n, dout, s->sms, s->stream);
+    CK(cudaGetLastError());
+    if (mem != RT_MEM_DEVICE) CK(cudaMemcpyAsync(irr, dout, ob, cudaMemcpyDeviceToHost, s->stream));
+    return check_err(s);
+}
+
+extern "C" int32_t rt_knn(RtScene* s, const float* q, int64_t n, int32_t k, float rmax, int32_t* idx, float* d2,
+                          int32_t mem) {
+    if (!s || n < 0 || k <= 0 || (n > 0 && (!q || !idx || !d2))) return RT_ERR_INVALID;
+    if (k > 256) return fail(s, RT_ERR_INVALID, "k must be ≤ 256");
+    if (n == 0) return RT_OK;
+    CK(cudaSetDevice(s->device));
+    if (!s->photons.present || s->photons.n == 0) {
+        std::vector<int32_t> mi((size_t)n * k, -1);
+        std::vector<float> md((size_t)n * k, INFINITY);
+        auto kind = mem == RT_MEM_DEVICE ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost;
+        CK(cudaMemcpy(idx, mi.data(), mi.size() * 4, kind));
+        CK(cudaMemcpy(d2, md.data(), md.size() * 4, kind));
+        return RT_OK;
+    }
+    const float* dq = q;
+    int32_t* di = idx;
+    float* dd = d2;
+    size_t qb = (size_t)n * 12, ob = (size_t)n * k * 4;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    if (mem != RT_MEM_DEVICE) {
+        int rc = ensure_stage(s, al(qb) + 2 * al(ob) + 256);
+        if (rc) return rc;
+        dq = (const float*)s->stage;
+        di = (int32_t*)((char*)s->stage + al(qb));
+        dd = (float*)((char*)s->stage + al(qb) + al(ob));
+        CK(cudaMemcpyAsync((void*)dq, q, qb, cudaMemcpyHostToDevice, s->stream));
+    }
+    rth::launch_knn_api(s->photons, dq, (uint32_t)n, k, rmax * rmax, di, dd, s->d_err, s->sms, s->stream);
+    CK(cudaGetLastError());
+    if (mem != RT_MEM_DEVICE) {
+        CK(cudaMemcpyAsync(idx, di, ob, cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaMemcpyAsync(d2, dd, ob, cudaMemcpyDeviceToHost, s->stream));
+    }
+    return check_err(s);
 }

@@ -24,6 +24,7 @@
 #define CTR_SHADOW_NEXT    4
 #define CTR_CLS_COUNT      5   // 5 entries
 #define CTR_CLS_NEXT       10  // 5 entries
+#define CTR_GATHER_COUNT   15  // photon-gather requests of the bounce
 
 // material classes shaded by separate kernels
 enum { CLS_MISS = 0, CLS_EMIT = 1, CLS_DIFFUSE = 2, CLS_METAL = 3, CLS_DIELEC = 4, CLS_N = 5 };
@@ -40,6 +41,8 @@ struct PathState {
     float4* L;         // accumulated radiance rgb
     float4* pend0;     // parked area-light NEE contribution (cancelled if occluded)
     float4* pend1;     // parked env-map NEE contribution
+    float4* pendC;     // parked caustic (photon-map) contribution, folded before pend0/pend1
+    float4* gq;        // photon-gather requests of the bounce: (p, pid) (n, -)
 };
 
 // meta.z flag layout
@@ -49,6 +52,20 @@ struct PathState {
 #define PF_TINT_MASK    (3u << 9)
 #define PF_SEC_ALIVE    (1u << 11)
 
+namespace rtph { struct Map; }
+
+// Device photon map: Morton-ordered photons, box heap, and an emission-order copy.
+struct PhotonMapDev {
+    float4 *pos = nullptr, *pow = nullptr, *nor = nullptr, *blo = nullptr, *bhi = nullptr;
+    float4 *exp_pos = nullptr, *exp_pow = nullptr, *exp_nor = nullptr;
+    uint32_t n = 0, nleaf_pow2 = 1, knn_k = 0;
+    float r2 = 0.0f;
+    bool present = false;
+    ~PhotonMapDev();
+    void release();
+    rtph::Map view() const;
+};
+
 struct RenderLaunch {
     uint32_t width, height, npix, nsamp;   // this chunk: nsamp consecutive samples
     uint32_t sample_idx, strata, max_depth, hero;
@@ -57,6 +74,7 @@ struct RenderLaunch {
     RtCamera cam;
     const uint8_t* converged;              // device, nullable
     float*   scratch;                      // nsamp × npix × 3 (device)
+    int      photons;                      // a photon map feeds the diffuse vertices
 };
 
 namespace rth {
@@ -75,6 +93,17 @@ void launch_shade(const rtd::DevScene& S, const PathState& P, const RenderLaunch
                   const uint32_t* qin, const uint32_t* cin, uint32_t* ctr, const ClassQueues& Q, uint32_t* qout,
                   uint32_t* cout, float4* sq, uint32_t* scount, int sms, cudaStream_t st);
 void launch_finalize(const PathState& P, const RenderLaunch& R, cudaStream_t st);
+
+cudaError_t photon_build(const rtd::DevScene& S, PhotonMapDev& map, const PathState& P, uint32_t* qa, uint32_t* qb,
+                         uint32_t* counters, const RtPhotonParams& prm, const float* emit_setup, int sms,
+                         cudaStream_t st, int64_t* n_stored);
+cudaError_t photon_set(PhotonMapDev& map, const float4* pos, const float4* pow, const float4* nor, uint32_t n,
+                       float radius, uint32_t k, cudaStream_t st);
+void launch_photon_gather_api(const PhotonMapDev& map, const float* q, uint32_t n, float* out, int sms, cudaStream_t st);
+void launch_knn_api(const PhotonMapDev& map, const float* q, uint32_t n, int k, float rmax2, int* idx, float* d2,
+                    int* err, int sms, cudaStream_t st);
+void launch_photon_gather_paths(const PhotonMapDev& map, const PathState& P, const float4* gq, const uint32_t* count,
+                                int sms, cudaStream_t st);
 void launch_accumulate(const float* scratch, uint32_t nsamp, uint32_t npix, float* acc, float* m2, uint32_t* cnt,
                        const uint8_t* conv, float clamp, uint32_t min_samples, float floor_, cudaStream_t st);
 }  // namespace rth

@@ -1,0 +1,815 @@
+// rt_photon.cu — caustic photon map on the device (src/photon.rs).
+//
+// Build (rt_photon_build):
+//   emit      one thread per photon: disk or cosine quad source (photon.rs:41-135)
+//   trace     ≤ 12 bounces, reusing the closest-hit traversal kernel; k_photon_shade
+//             continues specular photons and stores the first diffuse hit after a
+//             specular bounce (trace_photon, photon.rs:232-277) into its emission slot
+//   compact   stored photons in emission order (exclusive scan of the flags)
+//   sort      30-bit Morton codes of the positions, stable radix sort
+//   tree      implicit complete binary tree of boxes over 32-photon leaves of the
+//             Morton order (node i has children 2i+1, 2i+2)
+// Gather (warp per query; lane j of the warp tests photon j of a leaf):
+//   radius    Σ power·(1 − d²/r²) over d² < r², n_p·n > 0, × 2/(π²r²) (photon.rs:195-228)
+//   k-NN      the k-th smallest d² among those photons within the maximum radius,
+//             found by histogram refinement, then the radius gather at that distance
+//   rt_knn    exact k nearest (d² ≤ rmax²) sorted by (d², emission index)
+#include <cub/cub.cuh>
+
+#include "rt_internal.h"
+
+using namespace rtd;
+
+#define PH_LEAF 32
+#define PH_STACK 64
+#define PH_SEL_CAP 256
+
+namespace {
+
+RT_D float box_d2(float4 lo, float4 hi, float3 p) {
+    float dx = fmaxf(fmaxf(lo.x - p.x, 0.0f), p.x - hi.x);
+    float dy = fmaxf(fmaxf(lo.y - p.y, 0.0f), p.y - hi.y);
+    float dz = fmaxf(fmaxf(lo.z - p.z, 0.0f), p.z - hi.z);
+    // rounded like the photon distances (no fused multiply-add), so a box is
+    // never farther than a photon on its boundary
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+// ── emission ────────────────────────────────────────────────────────────────
+struct EmitSetup {
+    int type;
+    float3 t, b, center, dir, normal, corner, u, v, ta, ba, power;
+    float radius, lum_clamp;
+    uint32_t first, count;
+};
+struct EmitSet { EmitSetup e[RT_MAX_EMITTERS]; int n; float lam_lo, lam_range; uint64_t seed; };
+
+RT_D Rng photon_rng(uint64_t seed, uint32_t gid) {
+    Rng r;
+    r.a = gid;
+    r.b = mix32((uint32_t)seed) ^ 0x50484F54u;
+    r.c = mix32((uint32_t)(seed >> 32) + 0x9E3779B9u);
+    return r;
+}
+enum { P_EMIT0 = 0, P_EMIT1 = 1, P_EMIT2 = 2, P_EMIT3 = 3, P_LAMBDA = 4, P_BOUNCE0 = 8, P_PER_BOUNCE = 4 };
+
+__global__ void k_photon_emit(PathState P, EmitSet E, uint32_t total, uint32_t* queue0, uint32_t* count0,
+                              uint8_t* flags) {
+    for (uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x; gid < total; gid += gridDim.x * blockDim.x) {
+        int ei = 0;
+        for (int k = 1; k < E.n; k++) if (gid >= E.e[k].first) ei = k;
+        const EmitSetup& em = E.e[ei];
+        Rng rng = photon_rng(E.seed, gid);
+        float3 o, d;
+        if (em.type == RT_EMIT_DISK) {
+            float r = em.radius * sqrtf(rnd(rng, P_EMIT0));
+            float sp, cp;
+            sincosf(2.0f * PI_F * rnd(rng, P_EMIT1), &sp, &cp);
+            o = em.center + em.t * (r * cp) + em.b * (r * sp);
+            d = em.dir;
+        } else {
+            float ss = rnd(rng, P_EMIT0), tt = rnd(rng, P_EMIT1);
+            o = em.corner + em.u * ss + em.v * tt;
+            float ct = sqrtf(rnd(rng, P_EMIT2));
+            float st = sqrtf(1.0f - ct * ct);
+            float sp, cp;
+            sincosf(2.0f * PI_F * rnd(rng, P_EMIT3), &sp, &cp);
+            d = st * cp * em.ta + st * sp * em.ba + ct * em.normal;
+        }
+        float lam = E.lam_lo + E.lam_range * rnd(rng, P_LAMBDA);
+        if (lam >= E.lam_lo + E.lam_range) lam = nextafterf(E.lam_lo + E.lam_range, 0.0f);
+        P.ray_o[gid] = make_float4(o.x, o.y, o.z, em.lum_clamp);
+        P.ray_d[gid] = make_float4(d.x, d.y, d.z, lam);
+        P.thr[gid] = make_float4(em.power.x, em.power.y, em.power.z, 0.0f);
+        P.meta[gid] = make_uint4(gid, 0u, 0u, 0u);
+        flags[gid] = 0;
+        queue0[gid] = gid;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *count0 = total;
+}
+
+// spectrum helpers (spectrum.rs); duplicated from the shading TU as device
+// functions local to this file
+RT_D float3 cmf_rgb(const DevScene& S, float lambda, bool fire) {
+    float t = clampf_((lambda - 380.0f) / 5.0f, 0.0f, (float)(S.n_spec - 1));
+    int i = min((int)t, S.n_spec - 2);
+    float frac = t - (float)i;
+    float4 a = __ldg(S.cmf + i), bb = __ldg(S.cmf + i + 1);
+    float x = a.x + frac * (bb.x - a.x), y = a.y + frac * (bb.y - a.y), z = a.z + frac * (bb.z - a.z);
+    float c[3] = {fmaxf(3.2406f * x - 1.5372f * y - 0.4986f * z, 0.0f),
+                  fmaxf(-0.9689f * x + 1.8758f * y + 0.0415f * z, 0.0f),
+                  fmaxf(0.0557f * x - 0.2040f * y + 1.0570f * z, 0.0f)};
+    if (!fire) return mk(c[0] * S.norms[0], c[1] * S.norms[1], c[2] * S.norms[2]);
+    float w = fmaxf(powf(y, 0.5f), 0.08f);
+    for (int k = 0; k < 3; k++) c[k] *= w;
+    float lum = 0.2126f * c[0] + 0.7152f * c[1] + 0.0722f * c[2];
+    for (int k = 0; k < 3; k++) c[k] = c[k] * 0.5f + lum * 0.5f;
+    return mk(c[0] * S.fire_norms[0], c[1] * S.fire_norms[1], c[2] * S.fire_norms[2]);
+}
+RT_D float fresnel_diel(float ci, float eta) {
+    float sin2_i = fmaxf(1.0f - ci * ci, 0.0f), sin2_t = eta * eta * sin2_i;
+    if (sin2_t >= 1.0f) return 1.0f;
+    float ct = sqrtf(1.0f - sin2_t);
+    float rs = (eta * ci - ct) / (eta * ci + ct), rp = (eta * ct - ci) / (eta * ct + ci);
+    return (rs * rs + rp * rp) * 0.5f;
+}
+RT_D float fresnel_cond(float ci, float n, float k) {
+    float cos2 = ci * ci, sin2 = fmaxf(1.0f - cos2, 0.0f), n2 = n * n, k2 = k * k;
+    float t0 = n2 - k2 - sin2, ab = sqrtf(t0 * t0 + 4.0f * n2 * k2), t1 = ab + cos2;
+    float a = sqrtf(fmaxf(0.5f * (ab + t0), 0.0f)), t2 = 2.0f * ci * a;
+    float rs = (t1 - t2) / fmaxf(t1 + t2, 1e-12f);
+    float t3 = cos2 * ab + sin2 * sin2, t4 = t2 * sin2;
+    float rp = rs * (t3 - t4) / fmaxf(t3 + t4, 1e-12f);
+    return clampf_(0.5f * (rp + rs), 0.0f, 1.0f);
+}
+RT_D float smith_lam(float c, float alpha) {
+    float a2 = alpha * alpha, c2 = c * c;
+    return (sqrtf(a2 + (1.0f - a2) * c2) - c) / (2.0f * c);
+}
+RT_D float3 vndf(float3 wo, float al, float xi1, float xi2) {
+    float3 wh = unit3(mk(al * wo.x, al * wo.y, wo.z));
+    float len = sqrtf(wh.x * wh.x + wh.y * wh.y);
+    float3 t1 = len > 1e-6f ? mk(-wh.y / len, wh.x / len, 0.0f) : mk(1.0f, 0.0f, 0.0f);
+    float3 t2 = cross3(wh, t1);
+    float a = 1.0f / (1.0f + wh.z), r = sqrtf(xi1), p1, p2, sp, cp;
+    if (xi2 < a) { sincosf(xi2 / a * PI_F, &sp, &cp); p1 = r * cp; p2 = r * sp; }
+    else { sincosf(PI_F + (xi2 - a) / (1.0f - a) * PI_F, &sp, &cp); p1 = r * cp; p2 = r * sp * wh.z; }
+    float p3 = sqrtf(fmaxf(1.0f - p1 * p1 - p2 * p2, 0.0f));
+    float3 nh = t1 * p1 + t2 * p2 + wh * p3;
+    return unit3(mk(al * nh.x, al * nh.y, fmaxf(nh.z, 0.0f)));
+}
+RT_D float elut(const DevScene& S, float mu, float alpha) {
+    float x = clampf_(clampf_(mu, 0.0f, 1.0f) * 64.0f - 0.5f, 0.0f, 63.0f);
+    float y = clampf_(clampf_(alpha, 0.0f, 1.0f) * 64.0f - 0.5f, 0.0f, 63.0f);
+    int i0 = (int)x, j0 = (int)y, i1 = min(i0 + 1, 63), j1 = min(j0 + 1, 63);
+    float fx = x - (float)i0, fy = y - (float)j0;
+    return (__ldg(S.elut + i0 * 64 + j0) * (1.0f - fx) + __ldg(S.elut + i1 * 64 + j0) * fx) * (1.0f - fy) +
+           (__ldg(S.elut + i0 * 64 + j1) * (1.0f - fx) + __ldg(S.elut + i1 * 64 + j1) * fx) * fy;
+}
+
+// One bounce of trace_photon for every queued photon.
+__global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const uint32_t* __restrict__ qin,
+                               const uint32_t* cin, uint32_t* qout, uint32_t* cout, float4* st_pos, float4* st_pow,
+                               float4* st_nor, uint8_t* flags, uint64_t seed) {
+    uint32_t n = *cin;
+    for (uint32_t qi0 = blockIdx.x * blockDim.x; qi0 < n; qi0 += gridDim.x * blockDim.x) {
+        uint32_t qi = qi0 + threadIdx.x;
+        bool cont = false;
+        uint32_t gid = 0;
+        if (qi < n) {
+            gid = qin[qi];
+            float4 hv = P.hit[gid], ro = P.ray_o[gid], rdv = P.ray_d[gid], th = P.thr[gid];
+            uint32_t ref = __float_as_uint(hv.x);
+            if (ref != RT_MISS_REF) {
+                float3 o = mk(ro.x, ro.y, ro.z), d = mk(rdv.x, rdv.y, rdv.z), power = mk(th.x, th.y, th.z);
+                float lam = rdv.w, lum_clamp = ro.w;
+                uint32_t spec_depth = __float_as_uint(th.w);
+                float t = hv.y;
+                float3 p = o + t * d;
+                uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
+                float3 outward;
+                int mat;
+                if (type == RT_PRIM_TRI) {
+                    const float4* g = S.tri + (size_t)idx * 3;
+                    float4 ga = __ldg(g), gb = __ldg(g + 1), gc = __ldg(g + 2);
+                    float3 e1 = mk(ga.w, gb.x, gb.y), e2 = mk(gb.z, gb.w, gc.x);
+                    mat = __float_as_int(gc.z);
+                    if (__float_as_int(gc.w)) {
+                        const float4* gn = S.tri_n + (size_t)idx * 3;
+                        float4 na = __ldg(gn), nb = __ldg(gn + 1), nc = __ldg(gn + 2);
+                        float b1 = hv.z, b2 = hv.w, b0 = 1.0f - b1 - b2;
+                        float3 sn = b0 * mk(na.x, na.y, na.z) + b1 * mk(na.w, nb.x, nb.y) + b2 * mk(nb.z, nb.w, nc.x);
+                        outward = len2(sn) > 1e-12f ? unit3(sn) : unit3(cross3(e1, e2));
+                    } else {
+                        outward = unit3(cross3(e1, e2));
+                    }
+                } else if (type == RT_PRIM_QUAD) {
+                    const float4* g = S.quad + (size_t)idx * 5;
+                    float4 g0 = __ldg(g);
+                    outward = mk(g0.x, g0.y, g0.z);
+                    mat = __float_as_int(__ldg(g + 4).y);
+                } else {
+                    const float4* g = S.sphere + (size_t)idx * 2;
+                    float4 s0 = __ldg(g);
+                    outward = (p - mk(s0.x, s0.y, s0.z)) / s0.w;
+                    mat = __float_as_int(__ldg(g + 1).y);
+                }
+                bool front = dot3(d, outward) < 0.0f;
+                float3 nrm = front ? outward : -outward;
+                const DevMaterial& m = S.mats[mat];
+                Rng rng = photon_rng(seed, gid);
+                uint32_t base = P_BOUNCE0 + bounce * P_PER_BOUNCE;
+                float3 udir = unit3(d);
+                if (m.type == RT_MAT_DIELECTRIC || m.type == RT_MAT_SPECTRAL_DIELECTRIC) {
+                    bool spectral = m.type == RT_MAT_SPECTRAL_DIELECTRIC;
+                    float ior = spectral ? m.cauchy_b + m.cauchy_c / ((lam * 1e-3f) * (lam * 1e-3f)) : m.cauchy_b;
+                    float ratio = front ? 1.0f / ior : ior;
+                    float ct = fminf(dot3(-udir, nrm), 1.0f), st = sqrtf(1.0f - ct * ct);
+                    bool refl = ratio * st > 1.0f || fresnel_diel(ct, ratio) > rnd(rng, base + 0);
+                    float3 nd;
+                    if (refl) nd = reflect3(udir, nrm);
+                    else {
+                        float3 perp = ratio * (udir + ct * nrm);
+                        float kk = 1.0f - len2(perp);
+                        nd = kk < 0.0f ? reflect3(udir, nrm) : perp + (-sqrtf(kk) * nrm);
+                    }
+                    float3 att = mk(1.f, 1.f, 1.f);
+                    if (spectral) {
+                        if (!refl) att = cmf_rgb(S, lam, true);
+                        if (!front) {
+                            att.x *= expf(-m.absorption[0] * t);
+                            att.y *= expf(-m.absorption[1] * t);
+                            att.z *= expf(-m.absorption[2] * t);
+                        }
+                    }
+                    power = power * att;
+                    o = p; d = nd; spec_depth++; cont = true;
+                } else if (m.type == RT_MAT_SPECTRAL_METAL) {
+                    float3 wo = unit3(-d);
+                    float cos_o = dot3(wo, nrm);
+                    if (cos_o > 0.0f) {
+                        float alpha = fmaxf(m.roughness * m.roughness, 1e-4f);
+                        float3 nd;
+                        float cos_h;
+                        bool ok = true;
+                        if (m.roughness == 0.0f) { nd = reflect3(udir, nrm); cos_h = cos_o; }
+                        else {
+                            float3 up = fabsf(nrm.y) < 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+                            float3 tt = unit3(cross3(nrm, up)), bb = cross3(nrm, tt);
+                            float3 mts = vndf(mk(dot3(wo, tt), dot3(wo, bb), cos_o), alpha, rnd(rng, base + 0),
+                                              rnd(rng, base + 1));
+                            float3 mm = unit3(tt * mts.x + bb * mts.y + nrm * mts.z);
+                            float voh = fmaxf(dot3(wo, mm), 0.0f);
+                            nd = unit3(2.0f * voh * mm - wo);
+                            cos_h = voh;
+                            ok = dot3(nd, nrm) > 0.0f;
+                        }
+                        if (ok && dot3(nd, nrm) > 0.0f) {
+                            float weight = 1.0f;
+                            if (m.roughness != 0.0f) {
+                                float lo = smith_lam(cos_o, alpha), li = smith_lam(fmaxf(dot3(nd, nrm), 0.0f), alpha);
+                                weight = ((1.0f + lo) / (1.0f + lo + li)) * fminf(1.0f / fmaxf(elut(S, cos_o, alpha), 0.05f), 10.0f);
+                            }
+                            float tn = clampf_((lam - m.nk_start) / m.nk_step, 0.0f, (float)(m.nk_count - 1));
+                            int i = min((int)tn, m.nk_count - 2);
+                            float f = tn - (float)i;
+                            float nn = m.nk_n[i] + f * (m.nk_n[i + 1] - m.nk_n[i]);
+                            float kk = m.nk_k[i] + f * (m.nk_k[i + 1] - m.nk_k[i]);
+                            power = power * (cmf_rgb(S, lam, false) * (fresnel_cond(cos_h, nn, kk) * weight));
+                            o = p; d = nd; spec_depth++; cont = true;
+                        }
+                    }
+                } else if (m.type == RT_MAT_LAMBERTIAN || m.type == RT_MAT_CHECKER) {
+                    if (spec_depth > 0) {
+                        float lum = lum3(power);
+                        if (lum > lum_clamp) power = power * (lum_clamp / lum);
+                        st_pos[gid] = make_float4(p.x, p.y, p.z, __uint_as_float(gid));
+                        st_pow[gid] = make_float4(power.x, power.y, power.z, 0.f);
+                        st_nor[gid] = make_float4(nrm.x, nrm.y, nrm.z, 0.f);
+                        flags[gid] = 1;
+                    }
+                }
+                if (cont) {
+                    P.ray_o[gid] = make_float4(o.x, o.y, o.z, lum_clamp);
+                    P.ray_d[gid] = make_float4(d.x, d.y, d.z, lam);
+                    P.thr[gid] = make_float4(power.x, power.y, power.z, __uint_as_float(spec_depth));
+                }
+            }
+        }
+        uint32_t m = __ballot_sync(__activemask(), cont);
+        if (m) {
+            uint32_t lane = threadIdx.x & 31u;
+            int leader = __ffs(m) - 1;
+            uint32_t b = 0;
+            if ((int)lane == leader) b = atomicAdd(cout, __popc(m));
+            b = __shfl_sync(__activemask(), b, leader);
+            if (cont) qout[b + __popc(m & ((1u << lane) - 1u))] = gid;
+        }
+    }
+}
+
+__global__ void k_flags_to_u32(const uint8_t* f, uint32_t* o, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) o[i] = f[i];
+}
+__global__ void k_compact(const uint8_t* f, const uint32_t* scan, uint32_t n, const float4* sp, const float4* sw,
+                          const float4* sn, float4* dp, float4* dw, float4* dn) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (!f[i]) continue;
+        uint32_t j = scan[i];
+        dp[j] = sp[i]; dw[j] = sw[i]; dn[j] = sn[i];
+    }
+}
+
+// ── Morton codes over the stored photons' box ────────────────────────────────
+__global__ void k_bounds(const float4* p, uint32_t n, float* lo, float* hi) {
+    float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 q = p[i];
+        l[0] = fminf(l[0], q.x); l[1] = fminf(l[1], q.y); l[2] = fminf(l[2], q.z);
+        h[0] = fmaxf(h[0], q.x); h[1] = fmaxf(h[1], q.y); h[2] = fmaxf(h[2], q.z);
+    }
+    for (int k = 0; k < 3; k++) {
+        for (int o = 16; o > 0; o >>= 1) {
+            l[k] = fminf(l[k], __shfl_xor_sync(0xFFFFFFFFu, l[k], o));
+            h[k] = fmaxf(h[k], __shfl_xor_sync(0xFFFFFFFFu, h[k], o));
+        }
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        // float min/max through ordered integer atomics (values are finite)
+        for (int k = 0; k < 3; k++) {
+            int li = __float_as_int(l[k]), hi_ = __float_as_int(h[k]);
+            if (li >= 0) atomicMin((int*)&lo[k], li); else atomicMax((unsigned*)&lo[k], (unsigned)li);
+            if (hi_ >= 0) atomicMax((int*)&hi[k], hi_); else atomicMin((unsigned*)&hi[k], (unsigned)hi_);
+        }
+    }
+}
+RT_D uint32_t expand10(uint32_t v) {
+    v &= 1023u;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__global__ void k_morton(const float4* p, uint32_t n, const float* lo, const float* hi, uint32_t* key, uint32_t* val) {
+    float3 l = mk(lo[0], lo[1], lo[2]);
+    float3 e = mk(fmaxf(hi[0] - lo[0], 1e-30f), fmaxf(hi[1] - lo[1], 1e-30f), fmaxf(hi[2] - lo[2], 1e-30f));
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 q = p[i];
+        uint32_t x = (uint32_t)fminf(fmaxf((q.x - l.x) / e.x * 1024.0f, 0.0f), 1023.0f);
+        uint32_t y = (uint32_t)fminf(fmaxf((q.y - l.y) / e.y * 1024.0f, 0.0f), 1023.0f);
+        uint32_t z = (uint32_t)fminf(fmaxf((q.z - l.z) / e.z * 1024.0f, 0.0f), 1023.0f);
+        key[i] = (expand10(x) << 2) | (expand10(y) << 1) | expand10(z);
+        val[i] = i;
+    }
+}
+__global__ void k_gather_sorted(const uint32_t* order, uint32_t n, const float4* sp, const float4* sw, const float4* sn,
+                                float4* dp, float4* dw, float4* dn) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t j = order[i];
+        dp[i] = sp[j]; dw[i] = sw[j]; dn[i] = sn[j];
+    }
+}
+// leaf boxes (level `leaves` of the heap), then each internal level bottom-up
+__global__ void k_leaf_boxes(const float4* p, uint32_t n, uint32_t nleaf_pow2, float4* blo, float4* bhi) {
+    uint32_t first = nleaf_pow2 - 1;
+    for (uint32_t L = blockIdx.x * blockDim.x + threadIdx.x; L < nleaf_pow2; L += gridDim.x * blockDim.x) {
+        float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+        for (uint32_t k = L * PH_LEAF; k < min(n, (L + 1) * PH_LEAF); k++) {
+            float4 q = p[k];
+            lo.x = fminf(lo.x, q.x); lo.y = fminf(lo.y, q.y); lo.z = fminf(lo.z, q.z);
+            hi.x = fmaxf(hi.x, q.x); hi.y = fmaxf(hi.y, q.y); hi.z = fmaxf(hi.z, q.z);
+        }
+        blo[first + L] = lo;
+        bhi[first + L] = hi;
+    }
+}
+__global__ void k_level_boxes(uint32_t first, uint32_t count, float4* blo, float4* bhi) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        uint32_t nd = first + i, a = 2 * nd + 1, b = 2 * nd + 2;
+        float4 la = blo[a], lb = blo[b], ha = bhi[a], hb = bhi[b];
+        blo[nd] = make_float4(fminf(la.x, lb.x), fminf(la.y, lb.y), fminf(la.z, lb.z), 0.f);
+        bhi[nd] = make_float4(fmaxf(ha.x, hb.x), fmaxf(ha.y, hb.y), fmaxf(ha.z, hb.z), 0.f);
+    }
+}
+
+}  // namespace
+
+// ── warp-cooperative queries (used by the render path and the API) ─────────
+namespace rtph {
+
+struct Map {
+    const float4 *pos, *pow, *nor;   // Morton order; pos.w = emission index bits
+    const float4 *blo, *bhi;         // heap of boxes
+    uint32_t n, nleaf_pow2;
+    float r2;                        // radius (or k-NN maximum radius) squared
+    uint32_t knn_k;
+};
+
+// Visit every leaf whose box is within r2 of p; for each, lane j gets photon j
+// of the leaf (or nothing).  `f(lane_photon_index_or_-1)` is called warp-wide.
+template <class F>
+RT_D void for_leaves(const Map& M, float3 p, float r2, F f) {
+    uint32_t stack[PH_STACK];
+    int sp = 0;
+    uint32_t node = 0;
+    uint32_t lane = threadIdx.x & 31u;
+    uint32_t first_leaf = M.nleaf_pow2 - 1;
+    while (true) {
+        float4 lo = __ldg(M.blo + node), hi = __ldg(M.bhi + node);
+        bool near = box_d2(lo, hi, p) <= r2 && lo.x <= hi.x;
+        if (near) {
+            if (node >= first_leaf) {
+                uint32_t k = (node - first_leaf) * PH_LEAF + lane;
+                f(k < M.n ? (int)k : -1);
+            } else if (sp + 2 <= PH_STACK) {
+                stack[sp++] = 2 * node + 2;
+                stack[sp++] = 2 * node + 1;
+            }
+        }
+        if (sp == 0) break;
+        node = stack[--sp];
+    }
+}
+
+RT_D float warp_sum(float v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
+}
+
+// Squared distance and dot product with separately rounded products and sums
+// (no fused multiply-add), so the values equal the oracle's bit for bit.
+RT_D float pdist2(float4 q, float3 p) {
+    float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+RT_D float pdot(float4 a, float3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+
+// Candidate test shared by every pass: d² in [lo, hi) (or [lo, hi]) and, when
+// a normal is given, the photon faces it.
+struct KthRange {
+    float lo, hi;
+    bool hi_inclusive;
+    RT_D bool in(float d2) const { return d2 >= lo && (hi_inclusive ? d2 <= hi : d2 < hi); }
+};
+
+RT_D bool kth_candidate(const Map& M, int i, float3 p, const float3* nrm, const KthRange& R, float& d2) {
+    if (i < 0) return false;
+    d2 = pdist2(__ldg(M.pos + i), p);
+    if (!R.in(d2)) return false;
+    return !nrm || pdot(__ldg(M.nor + i), *nrm) > 0.0f;
+}
+
+// k-th smallest d² among photons with d² < r2max (strict) or ≤ r2max, [and
+// n_p·n > 0 when `nrm` is given]; returns r2max when fewer than k exist.
+// Histogram refinement: 32 bins per pass over the current range; a bin's
+// edges are the same floats in the counting pass and the next pass's range
+// test, so no candidate is lost or counted twice.  Once the bin holding the
+// k-th has at most PH_SEL_CAP candidates they are selected exactly in shared
+// memory; if the range stops shrinking (many equal distances) the remaining
+// distinct values are peeled off smallest first.
+RT_D float warp_kth_d2(const Map& M, float3 p, const float3* nrm, float r2max, uint32_t k, bool strict,
+                       uint32_t* hist /*32*/, float* sel /*PH_SEL_CAP*/) {
+    uint32_t lane = threadIdx.x & 31u;
+    KthRange R{0.0f, r2max, !strict};
+    uint32_t need = k;        // rank of the k-th within the range
+    for (int pass = 0; pass < 8; pass++) {
+        hist[lane] = 0;
+        __syncwarp();
+        float w = (R.hi - R.lo) / 32.0f;
+        if (!(w > 0.0f)) break;
+        // edge j = lo + w·j for j < 32, edge 32 = hi; bin = last edge ≤ d2
+        float my_edge = R.lo + w * (float)lane;
+        uint32_t total = 0;
+        for_leaves(M, p, R.hi, [&](int i) {
+            float d2 = 0.0f;
+            bool c = kth_candidate(M, i, p, nrm, R, d2);
+            if (c) {
+                int bin = w > 0.0f ? min(max((int)((d2 - R.lo) / w), 0), 31) : 0;
+                while (bin > 0 && d2 < R.lo + w * (float)bin) bin--;
+                while (bin < 31 && d2 >= R.lo + w * (float)(bin + 1)) bin++;
+                atomicAdd(&hist[bin], 1u);
+            }
+            total += __popc(__ballot_sync(0xFFFFFFFFu, c));
+        });
+        __syncwarp();
+        if (total < need) return pass == 0 ? r2max : R.hi;   // fewer than k in the whole range
+        if (total <= PH_SEL_CAP) {
+            // exact select: collect the candidates of the range and rank them
+            uint32_t cnt = 0;
+            for_leaves(M, p, R.hi, [&](int i) {
+                float d2 = 0.0f;
+                bool c = kth_candidate(M, i, p, nrm, R, d2);
+                uint32_t m = __ballot_sync(0xFFFFFFFFu, c);
+                if (c) sel[cnt + __popc(m & ((1u << lane) - 1u))] = d2;
+                cnt += __popc(m);
+            });
+            __syncwarp();
+            float found = R.hi;
+            for (uint32_t j = lane; j < cnt; j += 32) {
+                float v = sel[j];
+                uint32_t less = 0, eq_before = 0;
+                for (uint32_t t = 0; t < cnt; t++) {
+                    float u = sel[t];
+                    less += u < v;
+                    eq_before += (u == v && t < j);
+                }
+                if (less + eq_before == need - 1) found = v;
+            }
+            for (int o = 16; o > 0; o >>= 1) found = fminf(found, __shfl_xor_sync(0xFFFFFFFFu, found, o));
+            __syncwarp();
+            return found;
+        }
+        // narrow to the bin that holds the need-th candidate
+        uint32_t cum = 0, b = 31;
+        for (int j = 0; j < 32; j++) {
+            uint32_t h = hist[j];
+            if (cum + h >= need) { b = j; break; }
+            cum += h;
+        }
+        __syncwarp();
+        float nlo = __shfl_sync(0xFFFFFFFFu, my_edge, b);
+        float nhi = b == 31 ? R.hi : __shfl_sync(0xFFFFFFFFu, my_edge, (b + 1) & 31);
+        if (b == 0) nlo = R.lo;
+        bool same = nlo == R.lo && nhi == R.hi;
+        need -= cum;
+        R.hi_inclusive = b == 31 ? R.hi_inclusive : false;
+        R.lo = nlo;
+        R.hi = nhi;
+        if (same) break;
+    }
+    // peel distinct values, smallest first (bounded)
+    for (int it = 0; it < 64; it++) {
+        float mn = INFINITY;
+        for_leaves(M, p, R.hi, [&](int i) {
+            float d2 = 0.0f;
+            if (kth_candidate(M, i, p, nrm, R, d2)) mn = fminf(mn, d2);
+        });
+        for (int o = 16; o > 0; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
+        if (!(mn < INFINITY)) return R.hi;
+        uint32_t eq = 0;
+        for_leaves(M, p, R.hi, [&](int i) {
+            float d2 = 0.0f;
+            bool c = kth_candidate(M, i, p, nrm, R, d2) && d2 == mn;
+            eq += __popc(__ballot_sync(0xFFFFFFFFu, c));
+        });
+        if (eq >= need) return mn;
+        need -= eq;
+        R.lo = nextafterf(mn, INFINITY);
+    }
+    return R.hi;
+}
+
+// Irradiance estimate at (p, n) by one warp (all lanes call with the same query).
+RT_D float3 warp_irradiance(const Map& M, float3 p, float3 n, uint32_t* hist, float* sel) {
+    float r2 = M.r2;
+    if (M.knn_k > 0) {
+        r2 = warp_kth_d2(M, p, &n, M.r2, M.knn_k, true, hist, sel);
+        if (!(r2 > 0.0f)) return mk(0.f, 0.f, 0.f);
+    }
+    float3 acc = mk(0.f, 0.f, 0.f);
+    for_leaves(M, p, r2, [&](int i) {
+        if (i < 0) return;
+        float d2 = pdist2(__ldg(M.pos + i), p);
+        if (d2 < r2) {
+            if (pdot(__ldg(M.nor + i), n) > 0.0f) {
+                float4 pw = __ldg(M.pow + i);
+                float wgt = 1.0f - d2 / r2;
+                acc = acc + mk(pw.x, pw.y, pw.z) * wgt;
+            }
+        }
+    });
+    float s = 2.0f / (PI_F * PI_F * r2);
+    return mk(warp_sum(acc.x) * s, warp_sum(acc.y) * s, warp_sum(acc.z) * s);
+}
+
+}  // namespace rtph
+
+// queries n × 6 → irradiance n × 3; one warp per query
+__global__ void k_photon_gather_api(rtph::Map M, const float* q, uint32_t n, float* out) {
+    __shared__ uint32_t hist[RT_SHADE_BLOCK / 32][32];
+    __shared__ float sel[RT_SHADE_BLOCK / 32][PH_SEL_CAP];
+    uint32_t w = threadIdx.x >> 5, gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = gw; i < n; i += nw) {
+        float3 p = mk(q[i * 6], q[i * 6 + 1], q[i * 6 + 2]), nn = mk(q[i * 6 + 3], q[i * 6 + 4], q[i * 6 + 5]);
+        float3 r = rtph::warp_irradiance(M, p, nn, hist[w], sel[w]);
+        if ((threadIdx.x & 31u) == 0) { out[i * 3] = r.x; out[i * 3 + 1] = r.y; out[i * 3 + 2] = r.z; }
+    }
+}
+
+// exact k nearest with d² ≤ rmax², sorted by (d², emission index)
+__global__ void k_knn_api(rtph::Map M, const float* q, uint32_t n, int k, float rmax2, int* out_idx, float* out_d2,
+                          int* err) {
+    __shared__ uint32_t hist[RT_SHADE_BLOCK / 32][32];
+    __shared__ float sel[RT_SHADE_BLOCK / 32][PH_SEL_CAP];
+    __shared__ uint32_t cid[RT_SHADE_BLOCK / 32][PH_SEL_CAP];
+    __shared__ float cd2[RT_SHADE_BLOCK / 32][PH_SEL_CAP];
+    uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = gw; i < n; i += nw) {
+        float3 p = mk(q[i * 3], q[i * 3 + 1], q[i * 3 + 2]);
+        float rk = rtph::warp_kth_d2(M, p, nullptr, rmax2, (uint32_t)k, false, hist[w], sel[w]);
+        // every photon with d² ≤ r_k² (k plus ties at r_k)
+        uint32_t cnt = 0;
+        rtph::for_leaves(M, p, rk, [&](int j) {
+            bool c = false;
+            float d2 = 0.0f;
+            uint32_t id = 0;
+            if (j >= 0) {
+                float4 qq = __ldg(M.pos + j);
+                d2 = rtph::pdist2(qq, p);
+                c = d2 <= rk;
+                id = __float_as_uint(qq.w);
+            }
+            uint32_t m = __ballot_sync(0xFFFFFFFFu, c);
+            uint32_t slot = cnt + __popc(m & ((1u << lane) - 1u));
+            if (c && slot < PH_SEL_CAP) { cid[w][slot] = id; cd2[w][slot] = d2; }
+            cnt += __popc(m);
+        });
+        __syncwarp();
+        if (cnt > PH_SEL_CAP) { if (lane == 0) atomicExch(err, RT_ERR_CAPACITY); cnt = PH_SEL_CAP; }
+        // rank sort by (d², index)
+        for (uint32_t j = lane; j < cnt; j += 32) {
+            float v = cd2[w][j];
+            uint32_t id = cid[w][j], r = 0;
+            for (uint32_t t = 0; t < cnt; t++) {
+                float u = cd2[w][t];
+                r += (u < v) || (u == v && cid[w][t] < id);
+            }
+            if (r < (uint32_t)k) { out_idx[(size_t)i * k + r] = (int)id; out_d2[(size_t)i * k + r] = v; }
+        }
+        for (uint32_t r = cnt + lane; r < (uint32_t)k; r += 32) {
+            out_idx[(size_t)i * k + r] = -1;
+            out_d2[(size_t)i * k + r] = INFINITY;
+        }
+        __syncwarp();
+    }
+}
+
+// render path: caustic injection at queued diffuse vertices (renderer.rs:461-467);
+// pendC[pid] holds T·tint·albedo and becomes that × irradiance
+__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Map M, PathState P,
+                                                                        const float4* __restrict__ gq,
+                                                                        const uint32_t* count) {
+    __shared__ uint32_t hist[RT_SHADE_BLOCK / 32][32];
+    __shared__ float sel[RT_SHADE_BLOCK / 32][PH_SEL_CAP];
+    uint32_t n = *count;
+    uint32_t w = threadIdx.x >> 5, gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = gw; i < n; i += nw) {
+        float4 a = gq[(size_t)i * 2], b = gq[(size_t)i * 2 + 1];
+        uint32_t pid = __float_as_uint(a.w);
+        float3 r = rtph::warp_irradiance(M, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), hist[w], sel[w]);
+        if ((threadIdx.x & 31u) == 0) {
+            float4 f = P.pendC[pid];
+            bool any = r.x > 0.0f || r.y > 0.0f || r.z > 0.0f;
+            P.pendC[pid] = any ? make_float4(f.x * r.x, f.y * r.y, f.z * r.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
+}
+
+// ── host side ───────────────────────────────────────────────────────────────
+PhotonMapDev::~PhotonMapDev() { release(); }
+void PhotonMapDev::release() {
+    void* ps[] = {pos, pow, nor, blo, bhi, exp_pos, exp_pow, exp_nor};
+    for (void* p : ps) if (p) cudaFree(p);
+    pos = pow = nor = blo = bhi = exp_pos = exp_pow = exp_nor = nullptr;
+    n = 0;
+    present = false;
+}
+
+rtph::Map PhotonMapDev::view() const {
+    rtph::Map M;
+    M.pos = pos; M.pow = pow; M.nor = nor; M.blo = blo; M.bhi = bhi;
+    M.n = n; M.nleaf_pow2 = nleaf_pow2; M.r2 = r2; M.knn_k = knn_k;
+    return M;
+}
+
+
+namespace rth {
+
+static cudaError_t build_tree(PhotonMapDev& map, const float4* cp, const float4* cw, const float4* cn, uint32_t n,
+                              cudaStream_t st) {
+    // Morton sort (stable radix sort keeps emission order among equal codes)
+    cudaError_t e;
+    float* bounds;
+    if ((e = cudaMalloc(&bounds, 6 * sizeof(float)))) return e;
+    float init[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st);
+    k_bounds<<<std::min<uint32_t>((n + 255) / 256, 2048), 256, 0, st>>>(cp, n, bounds, bounds + 3);
+    uint32_t *key, *val, *key2, *val2;
+    cudaMalloc(&key, (size_t)n * 4); cudaMalloc(&val, (size_t)n * 4);
+    cudaMalloc(&key2, (size_t)n * 4); cudaMalloc(&val2, (size_t)n * 4);
+    k_morton<<<std::min<uint32_t>((n + 255) / 256, 4096), 256, 0, st>>>(cp, n, bounds, bounds + 3, key, val);
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, key, key2, val, val2, (int)n, 0, 30, st);
+    void* tmp;
+    cudaMalloc(&tmp, std::max<size_t>(tb, 16));
+    cub::DeviceRadixSort::SortPairs(tmp, tb, key, key2, val, val2, (int)n, 0, 30, st);
+    uint32_t nleaf = (n + PH_LEAF - 1) / PH_LEAF, p2 = 1;
+    while (p2 < nleaf) p2 <<= 1;
+    map.nleaf_pow2 = p2;
+    cudaMalloc(&map.pos, (size_t)std::max(n, 1u) * 16);
+    cudaMalloc(&map.pow, (size_t)std::max(n, 1u) * 16);
+    cudaMalloc(&map.nor, (size_t)std::max(n, 1u) * 16);
+    cudaMalloc(&map.blo, (size_t)(2 * p2 - 1) * 16);
+    cudaMalloc(&map.bhi, (size_t)(2 * p2 - 1) * 16);
+    k_gather_sorted<<<std::min<uint32_t>((n + 255) / 256, 4096), 256, 0, st>>>(val2, n, cp, cw, cn, map.pos, map.pow,
+                                                                               map.nor);
+    k_leaf_boxes<<<std::min<uint32_t>((p2 + 255) / 256, 4096), 256, 0, st>>>(map.pos, n, p2, map.blo, map.bhi);
+    for (uint32_t cnt = p2 / 2; cnt >= 1; cnt /= 2)
+        k_level_boxes<<<std::min<uint32_t>((cnt + 255) / 256, 4096), 256, 0, st>>>(cnt - 1, cnt, map.blo, map.bhi);
+    e = cudaStreamSynchronize(st);
+    cudaFree(bounds); cudaFree(key); cudaFree(val); cudaFree(key2); cudaFree(val2); cudaFree(tmp);
+    return e ? e : cudaGetLastError();
+}
+
+cudaError_t photon_build(const DevScene& S, PhotonMapDev& map, const PathState& P, uint32_t* qa, uint32_t* qb,
+                         uint32_t* counters, const RtPhotonParams& prm, const float* emit_setup, int sms,
+                         cudaStream_t st, int64_t* n_stored) {
+    map.release();
+    EmitSet E{};
+    E.n = prm.n_emitters;
+    E.lam_lo = S.lam_lo;
+    E.lam_range = S.lam_range;
+    E.seed = prm.seed;
+    uint32_t total = 0;
+    for (int i = 0; i < prm.n_emitters; i++) {
+        const float* f = emit_setup + i * 40;
+        EmitSetup& x = E.e[i];
+        x.type = prm.emitters[i].type;
+        x.t = mk(f[0], f[1], f[2]); x.b = mk(f[3], f[4], f[5]); x.center = mk(f[6], f[7], f[8]);
+        x.dir = mk(f[9], f[10], f[11]); x.normal = mk(f[12], f[13], f[14]); x.corner = mk(f[15], f[16], f[17]);
+        x.u = mk(f[18], f[19], f[20]); x.v = mk(f[21], f[22], f[23]); x.ta = mk(f[24], f[25], f[26]);
+        x.ba = mk(f[27], f[28], f[29]); x.power = mk(f[30], f[31], f[32]);
+        x.radius = f[33]; x.lum_clamp = f[34];
+        x.first = total; x.count = prm.emitters[i].n_photons;
+        total += x.count;
+    }
+    cudaError_t e;
+    uint8_t* flags;
+    float4 *sp, *sw, *sn;
+    if ((e = cudaMalloc(&flags, std::max(total, 1u)))) return e;
+    cudaMalloc(&sp, (size_t)std::max(total, 1u) * 16);
+    cudaMalloc(&sw, (size_t)std::max(total, 1u) * 16);
+    cudaMalloc(&sn, (size_t)std::max(total, 1u) * 16);
+    cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 14 * RT_CTR_STRIDE, st);
+    int grid = std::min<uint32_t>((total + 255) / 256, 148u * 16u);
+    k_photon_emit<<<std::max(grid, 1), 256, 0, st>>>(P, E, total, qa, counters, flags);
+    uint32_t* q[2] = {qa, qb};
+    for (uint32_t b = 0; b < 12; b++) {
+        uint32_t* c = counters + b * RT_CTR_STRIDE;
+        uint32_t* cn = counters + (b + 1) * RT_CTR_STRIDE;
+        launch_extend(S, P, q[b & 1], c + CTR_COUNT, c + CTR_EXTEND_NEXT, (int*)(counters + 13 * RT_CTR_STRIDE), sms, st);
+        k_photon_shade<<<sms * 8, 128, 0, st>>>(S, P, b, q[b & 1], c + CTR_COUNT, q[(b + 1) & 1], cn + CTR_COUNT, sp, sw,
+                                                sn, flags, prm.seed);
+    }
+    // compact in emission order
+    uint32_t *fl32, *scan;
+    cudaMalloc(&fl32, (size_t)std::max(total, 1u) * 4);
+    cudaMalloc(&scan, (size_t)std::max(total, 1u) * 4);
+    k_flags_to_u32<<<std::max(grid, 1), 256, 0, st>>>(flags, fl32, total);
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, fl32, scan, (int)total, st);
+    void* tmp;
+    cudaMalloc(&tmp, std::max<size_t>(tb, 16));
+    cub::DeviceScan::ExclusiveSum(tmp, tb, fl32, scan, (int)total, st);
+    uint32_t last_scan = 0, last_flag = 0;
+    if (total) {
+        cudaMemcpyAsync(&last_scan, scan + total - 1, 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&last_flag, fl32 + total - 1, 4, cudaMemcpyDeviceToHost, st);
+    }
+    if ((e = cudaStreamSynchronize(st))) return e;
+    uint32_t n = total ? last_scan + last_flag : 0;
+    float4 *cp, *cw, *cn;
+    cudaMalloc(&cp, (size_t)std::max(n, 1u) * 16);
+    cudaMalloc(&cw, (size_t)std::max(n, 1u) * 16);
+    cudaMalloc(&cn, (size_t)std::max(n, 1u) * 16);
+    k_compact<<<std::max(grid, 1), 256, 0, st>>>(flags, scan, total, sp, sw, sn, cp, cw, cn);
+    e = cudaStreamSynchronize(st);
+    cudaFree(flags); cudaFree(sp); cudaFree(sw); cudaFree(sn); cudaFree(fl32); cudaFree(scan); cudaFree(tmp);
+    if (e) return e;
+    map.exp_pos = cp; map.exp_pow = cw; map.exp_nor = cn;   // emission-order copy for export
+    map.n = n;
+    map.r2 = prm.gather_radius * prm.gather_radius;
+    map.knn_k = prm.knn_k;
+    if (n_stored) *n_stored = n;
+    if (n == 0) { map.present = true; return cudaSuccess; }
+    e = build_tree(map, cp, cw, cn, n, st);
+    map.present = e == cudaSuccess;
+    return e;
+}
+
+cudaError_t photon_set(PhotonMapDev& map, const float4* cp, const float4* cw, const float4* cn, uint32_t n, float radius,
+                       uint32_t k, cudaStream_t st) {
+    map.release();
+    cudaMalloc(&map.exp_pos, (size_t)std::max(n, 1u) * 16);
+    cudaMalloc(&map.exp_pow, (size_t)std::max(n, 1u) * 16);
+    cudaMalloc(&map.exp_nor, (size_t)std::max(n, 1u) * 16);
+    cudaMemcpyAsync(map.exp_pos, cp, (size_t)n * 16, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(map.exp_pow, cw, (size_t)n * 16, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(map.exp_nor, cn, (size_t)n * 16, cudaMemcpyHostToDevice, st);
+    map.n = n;
+    map.r2 = radius * radius;
+    map.knn_k = k;
+    cudaError_t e = n ? build_tree(map, map.exp_pos, map.exp_pow, map.exp_nor, n, st) : cudaStreamSynchronize(st);
+    map.present = e == cudaSuccess;
+    return e;
+}
+
+void launch_photon_gather_api(const PhotonMapDev& map, const float* q, uint32_t n, float* out, int sms, cudaStream_t st) {
+    k_photon_gather_api<<<sms * 4, RT_SHADE_BLOCK, 0, st>>>(map.view(), q, n, out);
+}
+void launch_knn_api(const PhotonMapDev& map, const float* q, uint32_t n, int k, float rmax2, int* idx, float* d2,
+                    int* err, int sms, cudaStream_t st) {
+    k_knn_api<<<sms * 4, RT_SHADE_BLOCK, 0, st>>>(map.view(), q, n, k, rmax2, idx, d2, err);
+}
+void launch_photon_gather_paths(const PhotonMapDev& map, const PathState& P, const float4* gq, const uint32_t* count,
+                                int sms, cudaStream_t st) {
+    k_photon_gather_paths<<<sms * 4, RT_SHADE_BLOCK, 0, st>>>(map.view(), P, gq, count);
+}
+
+}  // namespace rth

@@ -315,6 +315,7 @@ __global__ void k_generate(DevScene S, PathState P, RenderLaunch R, uint32_t* qu
         P.L[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
         P.pend0[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
         P.pend1[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (R.photons) P.pendC[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
         bool conv = R.converged && R.converged[i];
         Rng rng = make_rng(R.seed, i, sample);
         float wd = (float)max(R.width - 1u, 1u), hd = (float)max(R.height - 1u, 1u);
@@ -455,13 +456,19 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
         uint32_t qi = base + (threadIdx.x & 31u);
         bool active = qi < n;
         uint32_t pid = active ? qin[qi] : 0u;
-        bool cont = false, sh0 = false, sh1 = false;
-        float4 sh0a, sh0b, sh1a, sh1b;
+        bool cont = false, sh0 = false, sh1 = false, gath = false;
+        float4 sh0a, sh0b, sh1a, sh1b, ga, gb;
         if (active) {
             uint4 meta = P.meta[pid];
             float4 thr = P.thr[pid], w = P.wts[pid], L = P.L[pid];
             float4 p0 = P.pend0[pid], p1 = P.pend1[pid];
-            // fold the previous bounce's surviving NEE contributions, in order
+            // fold the previous bounce's parked contributions in the reference's
+            // order: caustic injection, area-light NEE, env NEE (renderer.rs:461-540)
+            if (R.photons) {
+                float4 pc = P.pendC[pid];
+                L.x += pc.x; L.y += pc.y; L.z += pc.z;
+                if (pc.x != 0.f || pc.y != 0.f || pc.z != 0.f) P.pendC[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
             L.x += p0.x; L.y += p0.y; L.z += p0.z;
             L.x += p1.x; L.y += p1.y; L.z += p1.z;
             if (p0.x != 0.f || p0.y != 0.f || p0.z != 0.f) P.pend0[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -584,6 +591,14 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         int zi = (int)floorf(m.checker_scale * p.z);
                         if ((xi + yi + zi) % 2 != 0) att = mk(m.odd[0], m.odd[1], m.odd[2]);
                     }
+                    if (R.photons) {
+                        // caustic injection: the gather kernel turns T·tint·albedo into × irradiance
+                        float3 f = T * sf * att;
+                        P.pendC[pid] = make_float4(f.x, f.y, f.z, 0.f);
+                        gath = true;
+                        ga = make_float4(p.x, p.y, p.z, __uint_as_float(pid));
+                        gb = make_float4(nrm.x, nrm.y, nrm.z, 0.f);
+                    }
                     if (have_lights) {
                         uint32_t pick = rnd_u32(rng, b + B_LPICK) % (uint32_t)S.n_lights;
                         float3 ldir = light_generate(S.lights[pick], p, rnd(rng, b + B_LPT0), rnd(rng, b + B_LPT1));
@@ -671,6 +686,10 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
             if (cont) qout[slot] = pid;
         }
         if (CLS == CLS_DIFFUSE) {
+            if (R.photons) {
+                uint32_t g = warp_append(scount + (CTR_GATHER_COUNT - CTR_SHADOW_COUNT), gath);
+                if (gath) { P.gq[(size_t)g * 2] = ga; P.gq[(size_t)g * 2 + 1] = gb; }
+            }
             uint32_t s0 = warp_append(scount, sh0);
             if (sh0) { sq[(size_t)s0 * 2] = sh0a; sq[(size_t)s0 * 2 + 1] = sh0b; }
             uint32_t s1 = warp_append(scount, sh1);
@@ -684,6 +703,7 @@ __global__ void k_finalize(PathState P, RenderLaunch R) {
     uint32_t total = R.npix * R.nsamp;
     for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < total; pid += gridDim.x * blockDim.x) {
         float4 L = P.L[pid], a = P.pend0[pid], b = P.pend1[pid];
+        if (R.photons) { float4 c = P.pendC[pid]; L.x += c.x; L.y += c.y; L.z += c.z; }
         L.x += a.x; L.y += a.y; L.z += a.z;
         L.x += b.x; L.y += b.y; L.z += b.z;
         uint4 meta = P.meta[pid];

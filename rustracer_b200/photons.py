@@ -1,0 +1,60 @@
+"""Photon-map emitter set-up: the host side of SceneData::rebuild_caustics
+(src/scene.rs:35-74) producing RtPhotonParams for rt_photon_build."""
+import math
+
+import numpy as np
+
+import ctypes as C
+
+from . import abi
+
+
+def _f3(v):
+    return (C.c_float * 3)(*[float(x) for x in v])
+
+
+def disk_emitter(sun_dir, sun_color, n_photons):
+    """PhotonMap::build (photon.rs:41-94): a disk facing sun_dir sized to the scene."""
+    e = abi.RtPhotonEmitter()
+    e.type = abi.RT_EMIT_DISK
+    e.dir = (C.c_float * 3)(*[float(x) for x in sun_dir])
+    e.color = (C.c_float * 3)(*[float(x) for x in sun_color])
+    e.n_photons = int(n_photons)
+    return e
+
+
+def quad_emitter(corner, u, v, color, n_photons):
+    """PhotonMap::build_from_quad (photon.rs:97-135): cosine-weighted quad source."""
+    e = abi.RtPhotonEmitter()
+    e.type = abi.RT_EMIT_QUAD
+    fl = lambda x: (C.c_float * 3)(*[float(y) for y in x])
+    e.corner, e.u, e.v, e.color = fl(corner), fl(u), fl(v), fl(color)
+    e.n_photons = int(n_photons)
+    return e
+
+
+def photon_params(emitters, gather_radius, knn_k=0, seed=0):
+    if not (1 <= len(emitters) <= abi.RT_MAX_EMITTERS):
+        raise ValueError("1..8 emitters")
+    p = abi.RtPhotonParams()
+    p.n_emitters = len(emitters)
+    for i, e in enumerate(emitters):
+        p.emitters[i] = e
+    p.gather_radius = float(gather_radius)
+    p.knn_k = int(knn_k)
+    p.seed = int(seed)
+    return p
+
+
+def caustic_params(builder, n_photons, gather_radius, knn_k=0, seed=0, env_dir=None, env_color=None):
+    """rebuild_caustics emitter choice (scene.rs:40-73): an env map → disk facing a
+    bright env direction (computed by the caller as the reference does from 8
+    CDF samples), otherwise the first [[lights]] quad with its `color`."""
+    if env_dir is not None:
+        return photon_params([disk_emitter(env_dir, env_color, n_photons)], gather_radius, knn_k, seed)
+    quads = [builder.quads[i] for kind, i in builder._lights if kind == "quad"]
+    if not quads:
+        raise ValueError("no caustic emitter: the scene has neither an env map nor a light quad")
+    q, u, v, mat = quads[0]
+    color = list(builder.materials[mat].albedo)
+    return photon_params([quad_emitter(q, u, v, color, n_photons)], gather_radius, knn_k, seed)

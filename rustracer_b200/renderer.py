@@ -49,6 +49,12 @@ def lib():
                                            vp, vp, vp, i32]
         L.rt_last_render_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
         L.rt_render_pass_noalloc.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), vp]
+        L.rt_photon_build.argtypes = [vp, C.POINTER(abi.RtPhotonParams), C.POINTER(i64)]
+        L.rt_photon_set.argtypes = [vp, vp, vp, vp, vp, i64, f, u32]
+        L.rt_photon_clear.argtypes = [vp]
+        L.rt_photon_export.argtypes = [vp, vp, vp, vp, vp, C.POINTER(i64)]
+        L.rt_photon_gather.argtypes = [vp, vp, i64, vp, i32]
+        L.rt_knn.argtypes = [vp, vp, i64, i32, f, vp, vp, i32]
         L.rt_set_profiling.argtypes = [vp, i32]
         L.rt_kernel_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
         L.rt_capture_rays.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), u32, vp, i64,
@@ -225,6 +231,48 @@ class GpuScene:
         ms, e, s, l = C.c_double(), C.c_int64(), C.c_int64(), C.c_int64()
         lib().rt_last_render_stats(self.h, C.byref(ms), C.byref(e), C.byref(s), C.byref(l))
         return dict(ms=ms.value, ext_rays=e.value, shadow_rays=s.value, launches=l.value)
+
+    # ── caustic photon map (photon.rs, scene.rs:35-74) ────────────────────
+    def photon_build(self, params):
+        """rebuild_caustics on the GPU; returns the number of stored photons."""
+        n = C.c_int64()
+        self._check(lib().rt_photon_build(self.h, C.byref(params), C.byref(n)))
+        return n.value
+
+    def photon_set(self, pos, power, nor, index=None, radius=0.1, knn_k=0):
+        pos, power, nor = (np.ascontiguousarray(np.asarray(a, np.float32).reshape(-1, 3)) for a in (pos, power, nor))
+        idx = None if index is None else np.ascontiguousarray(index, dtype=np.int32)
+        self._check(lib().rt_photon_set(self.h, C.c_void_p(pos.ctypes.data), C.c_void_p(power.ctypes.data),
+                                        C.c_void_p(nor.ctypes.data),
+                                        None if idx is None else C.c_void_p(idx.ctypes.data), len(pos), float(radius),
+                                        int(knn_k)))
+
+    def photon_clear(self):
+        self._check(lib().rt_photon_clear(self.h))
+
+    def photon_export(self):
+        n = C.c_int64()
+        self._check(lib().rt_photon_export(self.h, None, None, None, None, C.byref(n)))
+        pos, power, nor = (np.zeros((n.value, 3), np.float32) for _ in range(3))
+        idx = np.zeros(n.value, np.int32)
+        self._check(lib().rt_photon_export(self.h, C.c_void_p(pos.ctypes.data), C.c_void_p(power.ctypes.data),
+                                           C.c_void_p(nor.ctypes.data), C.c_void_p(idx.ctypes.data), C.byref(n)))
+        return pos, power, nor, idx
+
+    def photon_gather(self, queries):
+        q = np.ascontiguousarray(np.asarray(queries, np.float32).reshape(-1, 6))
+        out = np.zeros((len(q), 3), np.float32)
+        self._check(lib().rt_photon_gather(self.h, C.c_void_p(q.ctypes.data), len(q), C.c_void_p(out.ctypes.data),
+                                           abi.RT_MEM_HOST))
+        return out
+
+    def knn(self, queries, k, rmax):
+        q = np.ascontiguousarray(np.asarray(queries, np.float32).reshape(-1, 3))
+        idx = np.zeros((len(q), k), np.int32)
+        d2 = np.zeros((len(q), k), np.float32)
+        self._check(lib().rt_knn(self.h, C.c_void_p(q.ctypes.data), len(q), int(k), float(rmax),
+                                 C.c_void_p(idx.ctypes.data), C.c_void_p(d2.ctypes.data), abi.RT_MEM_HOST))
+        return idx, d2
 
     # ── diagnostics ──────────────────────────────────────────────────────
     def set_profiling(self, enable=True):

@@ -1,0 +1,75 @@
+"""CPU oracle of the caustic photon map (src/photon.rs) against the reference's
+photon tests, plus the k-NN rule; no GPU needed."""
+import numpy as np
+
+from oracle import oracle as O
+from rustracer_b200 import photons
+from rustracer_b200.scene import Material, SceneBuilder
+
+
+def glass_over_floor(floor_half=0.6):
+    """photon.rs:345-364 with the infinite plane replaced by a finite floor quad
+    (infinite planes are not in the GPU path; the reference excludes them from
+    the photon bounds, a finite floor around the sphere plays the same role)."""
+    sb = SceneBuilder()
+    white = sb.add_material(Material.lambertian((0.7, 0.7, 0.7)))
+    glass = sb.add_material(Material.dielectric(1.5))
+    h = floor_half
+    sb.add_quad((-h, 0.0, -h), (0, 0, 2 * h), (2 * h, 0, 0), white)
+    sb.add_sphere((0.0, 1.0, 0.0), 0.5, glass)
+    return sb
+
+
+def test_photon_disk_hugs_geometry_and_stores_caustics():
+    s = O.OracleScene(glass_over_floor())
+    p = photons.photon_params([photons.disk_emitter((0, 1, 0), (10, 10, 10), 20000)], 0.5, seed=1)
+    n = s.photon_build(p)
+    assert n > 2000, n                                        # photon.rs:362-363
+    pos, power, nor, idx = s.photon_export()
+    assert np.isfinite(pos).all() and np.isfinite(power).all()
+    assert (np.diff(idx) > 0).all()                           # emission order
+    assert np.allclose(pos[:, 1], 0.0, atol=1e-4)             # all on the floor
+    assert (nor[:, 1] > 0.99).all()
+    # caustic under the sphere: positive, finite irradiance
+    irr = s.photon_gather(np.array([[0, 0, 0, 0, 1, 0]], np.float32))[0]
+    assert np.isfinite(irr).all() and irr[0] > 0
+
+
+def test_photon_gather_matches_brute_force():
+    rng = np.random.default_rng(3)
+    n = 4000
+    pos = rng.uniform(-1, 1, size=(n, 3)).astype(np.float32)
+    pos[:, 1] = 0
+    power = rng.uniform(0, 1, size=(n, 3)).astype(np.float32)
+    nor = np.tile(np.array([0, 1, 0], np.float32), (n, 1))
+    nor[::7] = (0, -1, 0)                                     # some on the opposite side
+    s = O.OracleScene(glass_over_floor())
+    s.photon_set(pos, power, nor, np.arange(n), radius=0.2)
+    q = np.zeros((50, 6), np.float32)
+    q[:, 0] = rng.uniform(-0.8, 0.8, 50)
+    q[:, 2] = rng.uniform(-0.8, 0.8, 50)
+    q[:, 4] = 1.0
+    got = s.photon_gather(q)
+    r2 = np.float32(0.04)
+    for i in range(50):
+        d2 = ((pos - q[i, :3]) ** 2).sum(1)
+        m = (d2 < r2) & (nor[:, 1] > 0)
+        want = (power[m] * (1 - d2[m] / r2)[:, None]).sum(0) * 2 / (np.pi ** 2 * r2)
+        np.testing.assert_allclose(got[i], want, rtol=1e-4, atol=1e-6)
+
+
+def test_knn_rule_sorted_with_index_ties():
+    rng = np.random.default_rng(4)
+    n = 3000
+    pos = np.round(rng.uniform(-1, 1, size=(n, 3)) * 8) / 8            # many exact distance ties
+    pos = pos.astype(np.float32)
+    s = O.OracleScene(glass_over_floor())
+    s.photon_set(pos, np.ones((n, 3), np.float32), np.tile([0, 1, 0], (n, 1)), np.arange(n), radius=0.3)
+    q = rng.uniform(-1, 1, size=(40, 3)).astype(np.float32)
+    idx, d2 = s.knn(q, 16, 0.5)
+    for i in range(40):
+        dd = ((pos - q[i]) ** 2).sum(1).astype(np.float32)
+        order = np.lexsort((np.arange(n), dd))
+        order = order[dd[order] <= np.float32(0.25)][:16]
+        assert list(idx[i][: len(order)]) == list(order)
+        assert (idx[i][len(order):] == -1).all()
