@@ -327,16 +327,17 @@ def roofline(scene, sb, cam):
 
 
 def one_pass():
-    """Profiler driver: one warm-up pass and one measured 1-spp pass of the
-    1920×1080 workload (76 kernel launches)."""
+    """Profiler driver: one warm-up pass and one measured pass of the
+    1920×1080 icosphere workload, 4 samples per pixel per pass — the same
+    8.3M-path chunk that each wavefront launch of the timed render processes."""
     import torch
     from rustracer_b200 import configs
     from rustracer_b200.renderer import GpuScene, pass_params
     sb, st = configs.icosphere_scene(seed=2)
     scene = GpuScene(sb, device=0)
-    out = torch.zeros((1, H, W, 3), device="cuda")
+    out = torch.zeros((4, H, W, 3), device="cuda")
     for k in range(2):
-        scene.render_pass(st["camera"], pass_params(W, H, k, 1, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2), out=out)
+        scene.render_pass(st["camera"], pass_params(W, H, 4 * k, 4, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2), out=out)
     torch.cuda.synchronize()
     print("pass ok", scene.last_stats(), flush=True)
 
