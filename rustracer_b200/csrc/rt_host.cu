@@ -325,12 +325,19 @@ struct RtScene {
     bool empty = true;
     // wavefront buffers (grown on demand)
     uint32_t cap = 0;
-    PathState P{};
-    uint32_t* queue[2] = {nullptr, nullptr};
+    PathState P{};                    // set 0 (also the photon tracer's state)
+    PathState P2{};                   // set 1 (shares hit and gq with set 0)
+    PathState Rt{};                   // retire records: L, pend0, pend1, pendC, meta
+    uint32_t* queue[2] = {nullptr, nullptr};   // photon tracer queues
     ClassQueues cq{};
     float4* sq = nullptr;
-    uint32_t* counters = nullptr;     // (RT_MAX_DEPTH+2) × RT_CTR_STRIDE
+    uint32_t* counters = nullptr;     // RT_CTR_WORDS (header + ring of iteration blocks)
     int* d_err = nullptr;
+    uint32_t* d_active = nullptr;     // active-pixel list of a converged mask
+    uint32_t active_cap = 0;
+    // lagged end-of-work check: next-iteration ray counts copied to pinned memory
+    uint32_t* h_status = nullptr;
+    cudaEvent_t st_ev[8] = {};
     float* scratch = nullptr;
     size_t scratch_bytes = 0;
     uint8_t* d_conv = nullptr;
@@ -360,6 +367,8 @@ struct RtScene {
     double last_ms = 0.0;
     int64_t last_ext = 0, last_shadow = 0, last_launches = 0;
 };
+
+static void free_paths(RtScene* s);
 
 static int fail(RtScene* s, int code, const std::string& msg) {
     if (s) s->err = msg;
@@ -416,13 +425,13 @@ int32_t rt_scene_destroy(RtScene* s) {
     if (!s) return RT_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto& b : s->owned) cudaFree(b.p);
-    void* ps[] = {s->P.ray_o, s->P.ray_d, s->P.hit, s->P.thr, s->P.wts, s->P.meta, s->P.L, s->P.pend0, s->P.pend1,
-                  s->P.pendC, s->P.gq, s->queue[0], s->queue[1], s->sq, s->counters, s->d_err, s->scratch,
-                  s->d_conv, s->acc, s->m2, s->cnt, s->stage};
+    void* ps[] = {s->counters, s->d_err, s->scratch, s->d_conv, s->acc, s->m2, s->cnt, s->stage, s->d_active};
+    free_paths(s);
     s->photons.release();
     for (void* p : ps) if (p) cudaFree(p);
-    for (int c = 0; c < CLS_N; c++) if (s->cq.q[c]) cudaFree(s->cq.q[c]);
     for (auto e : s->pev) cudaEventDestroy(e);
+    for (auto e : s->st_ev) if (e) cudaEventDestroy(e);
+    if (s->h_status) cudaFreeHost(s->h_status);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -447,6 +456,11 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         return bail(fail(s, RT_ERR_CUDA, "cudaStreamCreate failed"));
     cudaEventCreate(&s->ev0);
     cudaEventCreate(&s->ev1);
+    for (auto& e : s->st_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(s, RT_ERR_CUDA, "cudaEventCreate failed"));
+    if (cudaHostAlloc((void**)&s->h_status, 8 * sizeof(uint32_t), cudaHostAllocDefault) != cudaSuccess)
+        return bail(fail(s, RT_ERR_NOMEM, "cudaHostAlloc status words"));
 
     // ── validate ────────────────────────────────────────────────────────────
     if (d->n_tris < 0 || d->n_quads < 0 || d->n_spheres < 0 || d->n_mats < 0 || d->n_lights < 0)
@@ -864,7 +878,7 @@ extern "C" int32_t rt_trace_closest(RtScene* s, const float* rays, int64_t n, Rt
     }
     uint32_t* next;
     if (!s->counters) {
-        if (cudaMalloc(&s->counters, sizeof(uint32_t) * (RT_MAX_DEPTH + 2) * RT_CTR_STRIDE) != cudaSuccess)
+        if (cudaMalloc(&s->counters, sizeof(uint32_t) * RT_CTR_WORDS) != cudaSuccess)
             return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
     }
     next = s->counters;
@@ -895,7 +909,7 @@ extern "C" int32_t rt_trace_any(RtScene* s, const float* rays, int64_t n, uint8_
         CK(cudaMemcpyAsync((void*)drays, rays, rb, cudaMemcpyHostToDevice, s->stream));
     }
     if (!s->counters) {
-        if (cudaMalloc(&s->counters, sizeof(uint32_t) * (RT_MAX_DEPTH + 2) * RT_CTR_STRIDE) != cudaSuccess)
+        if (cudaMalloc(&s->counters, sizeof(uint32_t) * RT_CTR_WORDS) != cudaSuccess)
             return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
     }
     CK(cudaMemsetAsync(s->counters, 0, sizeof(uint32_t), s->stream));
@@ -906,138 +920,227 @@ extern "C" int32_t rt_trace_any(RtScene* s, const float* rays, int64_t n, uint8_
 }
 
 // ── render loop ─────────────────────────────────────────────────────────────
-static const uint32_t MAX_PATHS = 1u << 23;   // 8M paths in flight per chunk
+static const uint32_t MAX_PATHS = 1u << 23;   // 8M paths in flight
+
+// every path buffer of the scene, for allocation and release
+template <class F>
+static void for_path_buffers(RtScene* s, F f) {
+    PathState* sets[3] = {&s->P, &s->P2, &s->Rt};
+    for (PathState* P : sets) {
+        float4** f4[] = {&P->ray_o, &P->ray_d, &P->thr, &P->wts, (float4**)&P->meta, &P->L, &P->pend0, &P->pend1,
+                         &P->pendC};
+        for (int i = 0; i < 9; i++)
+            if (P != &s->Rt || i >= 4) f((void**)f4[i], sizeof(float4));
+    }
+    f((void**)&s->P.hit, sizeof(float4));
+    f((void**)&s->P.gq, 2 * sizeof(float4));
+    f((void**)&s->queue[0], sizeof(uint32_t));
+    f((void**)&s->queue[1], sizeof(uint32_t));
+    f((void**)&s->sq, 2 * 2 * sizeof(float4));
+    for (int c = 0; c < CLS_N; c++) f((void**)&s->cq.q[c], sizeof(uint32_t));
+}
+
+static void free_paths(RtScene* s) {
+    s->P2.hit = s->P2.gq = nullptr;
+    for_path_buffers(s, [](void** p, size_t) { if (*p) cudaFree(*p); *p = nullptr; });
+    s->cap = 0;
+}
 
 static int ensure_paths(RtScene* s, uint32_t cap) {
     if (s->cap >= cap) return RT_OK;
-    void* ps[] = {s->P.ray_o, s->P.ray_d, s->P.hit, s->P.thr, s->P.wts, s->P.meta, s->P.L, s->P.pend0, s->P.pend1,
-                  s->P.pendC, s->P.gq, s->queue[0], s->queue[1], s->sq};
-    for (void* p : ps) if (p) cudaFree(p);
-    for (int c = 0; c < CLS_N; c++) if (s->cq.q[c]) cudaFree(s->cq.q[c]);
-    s->cq = ClassQueues{};
-    s->P = PathState{};
-    s->queue[0] = s->queue[1] = nullptr;
-    s->sq = nullptr;
-    s->cap = 0;
-    size_t f4 = (size_t)cap * sizeof(float4);
-    void** slots[] = {(void**)&s->P.ray_o, (void**)&s->P.ray_d, (void**)&s->P.hit, (void**)&s->P.thr, (void**)&s->P.wts,
-                      (void**)&s->P.meta, (void**)&s->P.L, (void**)&s->P.pend0, (void**)&s->P.pend1,
-                      (void**)&s->P.pendC};
-    for (void** sl : slots)
-        if (cudaMalloc(sl, f4) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc path state");
-    if (cudaMalloc(&s->queue[0], (size_t)cap * 4) != cudaSuccess || cudaMalloc(&s->queue[1], (size_t)cap * 4) != cudaSuccess ||
-        cudaMalloc(&s->sq, (size_t)cap * 2 * 2 * sizeof(float4)) != cudaSuccess)
-        return fail(s, RT_ERR_NOMEM, "cudaMalloc queues");
-    for (int c = 0; c < CLS_N; c++)
-        if (cudaMalloc(&s->cq.q[c], (size_t)cap * 4) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc class queues");
-    if (cudaMalloc(&s->P.gq, (size_t)cap * 2 * sizeof(float4)) != cudaSuccess)
-        return fail(s, RT_ERR_NOMEM, "cudaMalloc gather queue");
-    if (!s->counters && cudaMalloc(&s->counters, sizeof(uint32_t) * (RT_MAX_DEPTH + 2) * RT_CTR_STRIDE) != cudaSuccess)
+    free_paths(s);
+    bool ok = true;
+    for_path_buffers(s, [&](void** p, size_t per) {
+        if (ok && cudaMalloc(p, (size_t)cap * per) != cudaSuccess) ok = false;
+    });
+    if (!ok) { free_paths(s); return fail(s, RT_ERR_NOMEM, "cudaMalloc path state"); }
+    s->P2.hit = s->P.hit;
+    s->P2.gq = s->P.gq;
+    if (!s->counters && cudaMalloc(&s->counters, sizeof(uint32_t) * RT_CTR_WORDS) != cudaSuccess)
         return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
     s->cap = cap;
     return RT_OK;
 }
 
-// Renders params->n_samples passes into the device buffer `dscratch`
-// (n_samples × npix × 3), in chunks of as many samples as fit MAX_PATHS.
+// Device buffers of one wavefront run: the scene's own (grown on demand) or
+// the fixed array of rt_render_pass_noalloc.
+struct WaveBufs {
+    PathState set[2]{};
+    PathState Rt{};
+    ClassQueues cq{};
+    float4* sq = nullptr;
+    uint32_t* counters = nullptr;
+    int* derr = nullptr;
+    uint32_t cap = 0;
+};
+
+static WaveBufs scene_bufs(const RtScene* s) {
+    WaveBufs W;
+    W.set[0] = s->P; W.set[1] = s->P2; W.Rt = s->Rt;
+    W.cq = s->cq; W.sq = s->sq; W.counters = s->counters; W.derr = s->d_err; W.cap = s->cap;
+    return W;
+}
+
+// Samples sample_idx .. sample_idx+nsamp−1 of the `nactive` active pixels
+// (`active` = null: all pixels) into dscratch (nsamp × npix × 3).
+//
+// The path pool (min(samples, W.cap) slots) is filled once; then each
+// iteration runs extend → classify/shade → photon gather → shadow → retire,
+// and the retire kernel hands every slot whose path ended to the next
+// ungenerated sample.  While samples remain, the pool stays full, so every
+// launch but those of the final drain works on a full wavefront.  The host
+// does not wait per iteration: it reads the next-iteration ray count of the
+// iteration launched STATUS_LAG iterations earlier (copied to pinned memory)
+// and stops at the first zero; the at most STATUS_LAG iterations launched
+// after it find empty queues.
+static const uint32_t STATUS_RING = 8, STATUS_LAG = 2;
+
+static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, const RtPassParams* p, uint32_t sample_idx,
+                         uint32_t nsamp, float* dscratch, const uint32_t* active, uint32_t nactive, int64_t* ext_rays,
+                         int64_t* sh_rays, int64_t* launches) {
+    uint64_t total = (uint64_t)nsamp * nactive;
+    if (total == 0) return RT_OK;
+    uint32_t pool = (uint32_t)std::min<uint64_t>(total, W.cap);
+    uint32_t maxd = std::min<uint32_t>(p->max_depth, RT_MAX_DEPTH);
+    RenderLaunch R{};
+    R.width = p->width; R.height = p->height; R.npix = p->width * p->height;
+    R.nsamp = nsamp;
+    R.sample_idx = sample_idx;
+    R.strata = p->strata;
+    R.max_depth = maxd;
+    R.hero = std::max<uint32_t>(1, std::min<uint32_t>(p->hero_count, 4));
+    R.bg_scale = p->bg_scale;
+    R.seed = p->seed;
+    R.cam = *cam;
+    R.active = active;
+    R.nactive = nactive;
+    R.total = total;
+    R.gen_next = (unsigned long long*)(W.counters + HDR_GEN);
+    R.scratch = dscratch;
+    R.photons = s->photons.present && s->photons.n > 0;
+    uint32_t* hdr = W.counters;
+    auto blk = [&](uint64_t it) { return W.counters + CTR_HDR_WORDS + (it % RT_CTR_RING) * RT_CTR_STRIDE; };
+    size_t ev_used = 0;
+    auto mark = [&](int kind) {
+        if (!s->profiling) return;
+        if (ev_used >= s->pev.size()) { cudaEvent_t e; cudaEventCreate(&e); s->pev.push_back(e); s->pkind.push_back(0); }
+        s->pkind[ev_used] = kind;
+        cudaEventRecord(s->pev[ev_used++], s->stream);
+    };
+    int64_t nl = 0;
+    CK(cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * RT_CTR_WORDS, s->stream));
+    mark(0);
+    rth::launch_generate(s->S, W.set[0], R, pool, blk(0) + CTR_COUNT, s->stream);
+    nl++;
+    // every iteration with samples left advances `pool` path segments, and a
+    // sample has at most maxd segments; the drain takes at most maxd more
+    uint64_t max_it = total * maxd / pool + maxd + 2;
+    bool done = false;
+    uint64_t it = 0;
+    for (; it < max_it && !done; it++) {
+        uint32_t* c = blk(it);
+        uint32_t* cn = blk(it + 1);
+        const PathState& A = W.set[it & 1];
+        const PathState& B = W.set[(it + 1) & 1];
+        PendTargets T{{B.pend0, B.pend1, W.Rt.pend0, W.Rt.pend1}, {B.pendC, W.Rt.pendC}};
+        mark(1);
+        rth::launch_extend(s->S, A, nullptr, c + CTR_COUNT, c + CTR_EXTEND_NEXT, W.derr, s->sms, s->stream);
+        if ((int64_t)it == s->cap_depth && s->cap_out) {
+            // diagnostics: copy this iteration's rays out (origin, direction)
+            CK(cudaStreamSynchronize(s->stream));
+            uint32_t cnt = 0;
+            CK(cudaMemcpy(&cnt, c + CTR_COUNT, 4, cudaMemcpyDeviceToHost));
+            int64_t m = std::min<int64_t>(cnt, s->cap_max);
+            std::vector<float4> ro(m), rd(m);
+            CK(cudaMemcpy(ro.data(), A.ray_o, (size_t)m * 16, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(rd.data(), A.ray_d, (size_t)m * 16, cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < m; i++) {
+                float* r = s->cap_out + i * 8;
+                float4 a = ro[i], b = rd[i];
+                r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = b.x; r[4] = b.y; r[5] = b.z; r[6] = 0.001f; r[7] = INFINITY;
+            }
+            s->cap_n = m;
+        }
+        mark(2);
+        rth::launch_shade(s->S, A, B, W.Rt, R, c, W.cq, cn + CTR_COUNT, W.sq, s->sms, s->stream);
+        if (R.photons) {
+            rth::launch_photon_gather_paths(s->photons, T, A.gq, c + CTR_GATHER_COUNT, s->sms, s->stream);
+            nl++;
+        }
+        mark(3);
+        rth::launch_shadow(s->S, T, W.sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, W.derr, s->sms, s->stream);
+        mark(0);
+        rth::launch_retire(s->S, B, W.Rt, R, c, hdr, blk(it + 2), cn + CTR_COUNT, s->sms, s->stream);
+        nl += 4 + CLS_N;
+        uint32_t slot = (uint32_t)(it % STATUS_RING);
+        CK(cudaMemcpyAsync(s->h_status + slot, cn + CTR_COUNT, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaEventRecord(s->st_ev[slot], s->stream));
+        if (it >= STATUS_LAG) {
+            uint32_t js = (uint32_t)((it - STATUS_LAG) % STATUS_RING);
+            CK(cudaEventSynchronize(s->st_ev[js]));
+            if (((volatile uint32_t*)s->h_status)[js] == 0) done = true;
+        }
+    }
+    mark(0);
+    CK(cudaGetLastError());
+    uint64_t tot[3] = {0, 0, 0};
+    CK(cudaMemcpyAsync(tot, W.counters, sizeof(tot), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (!done) {
+        // the bound was reached: the last iterations' counts must be zero
+        for (uint32_t k = 0; k < std::min<uint64_t>(it, STATUS_LAG); k++)
+            if (s->h_status[(uint32_t)((it - 1 - k) % STATUS_RING)] != 0)
+                return fail(s, RT_ERR_CAPACITY, "wavefront did not drain within its iteration bound");
+    }
+    if (ext_rays) *ext_rays += (int64_t)tot[HDR_EXT / 2];
+    if (sh_rays) *sh_rays += (int64_t)tot[HDR_SHADOW / 2];
+    if (launches) *launches += nl;
+    if (s->profiling) {
+        for (size_t e = 0; e + 1 < ev_used; e++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, s->pev[e], s->pev[e + 1]);
+            int kind = s->pkind[e];
+            s->kms[kind] += ms;
+            if (!(kind == 0 && e > 0 && s->pkind[e - 1] == 0)) s->kcount[kind]++;
+        }
+    }
+    return RT_OK;
+}
+
+// Renders params->n_samples samples of every pixel into the device buffer
+// `dscratch` (n_samples × npix × 3).  Pixels set in the converged mask are
+// not traced and get zero.
 static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p, float* dscratch, const uint8_t* dconv,
                          int64_t* ext_rays, int64_t* sh_rays, int64_t* launches) {
     uint32_t npix = p->width * p->height;
     uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
-    uint32_t per = std::max<uint32_t>(1, std::min<uint32_t>(nsamp, MAX_PATHS / std::max<uint32_t>(npix, 1)));
-    uint32_t cap = (uint32_t)std::min<uint64_t>((uint64_t)per * npix, (uint64_t)std::max<uint32_t>(npix, 1) * per);
-    int rc = ensure_paths(s, cap);
+    uint64_t total = (uint64_t)nsamp * npix;
+    int rc = ensure_paths(s, (uint32_t)std::min<uint64_t>(total, MAX_PATHS));
     if (rc) return rc;
-    uint32_t maxd = std::min<uint32_t>(p->max_depth, RT_MAX_DEPTH);
-    std::vector<uint32_t> hc((size_t)(RT_MAX_DEPTH + 2) * RT_CTR_STRIDE);
-    int64_t ext = 0, sh = 0, nl = 0;
-    for (uint32_t k0 = 0; k0 < nsamp; k0 += per) {
-        RenderLaunch R{};
-        R.width = p->width; R.height = p->height; R.npix = npix;
-        R.nsamp = std::min(per, nsamp - k0);
-        R.sample_idx = p->sample_idx + k0;
-        R.strata = p->strata;
-        R.max_depth = maxd;
-        R.hero = std::max<uint32_t>(1, std::min<uint32_t>(p->hero_count, 4));
-        R.bg_scale = p->bg_scale;
-        R.seed = p->seed;
-        R.cam = *cam;
-        R.converged = dconv;
-        R.scratch = dscratch + (size_t)k0 * npix * 3;
-        R.photons = s->photons.present && s->photons.n > 0;
-        CK(cudaMemsetAsync(s->counters, 0, sizeof(uint32_t) * (maxd + 2) * RT_CTR_STRIDE, s->stream));
-        uint32_t* C = s->counters;
-        size_t ev_used = 0;
-        auto mark = [&](int kind) {
-            if (!s->profiling) return;
-            if (ev_used >= s->pev.size()) { cudaEvent_t e; cudaEventCreate(&e); s->pev.push_back(e); s->pkind.push_back(0); }
-            s->pkind[ev_used] = kind;
-            cudaEventRecord(s->pev[ev_used++], s->stream);
-        };
-        mark(0);
-        rth::launch_generate(s->S, s->P, R, s->queue[0], C + 0, s->stream);
-        nl++;
-        for (uint32_t dpt = 0; dpt < maxd; dpt++) {
-            uint32_t* c = C + dpt * RT_CTR_STRIDE;
-            uint32_t* cn = C + (dpt + 1) * RT_CTR_STRIDE;
-            uint32_t* qin = s->queue[dpt & 1];
-            uint32_t* qout = s->queue[(dpt + 1) & 1];
-            mark(1);
-            rth::launch_extend(s->S, s->P, qin, c + CTR_COUNT, c + CTR_EXTEND_NEXT, s->d_err, s->sms, s->stream);
-            if ((int32_t)dpt == s->cap_depth && s->cap_out) {
-                // diagnostics: copy this bounce's rays out (origin, direction) before shade moves them
-                CK(cudaStreamSynchronize(s->stream));
-                uint32_t cnt = 0;
-                CK(cudaMemcpy(&cnt, c + 0, 4, cudaMemcpyDeviceToHost));
-                int64_t m = std::min<int64_t>(cnt, s->cap_max);
-                std::vector<uint32_t> q(m);
-                std::vector<float4> ro(cap), rd(cap);
-                CK(cudaMemcpy(q.data(), qin, m * 4, cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(ro.data(), s->P.ray_o, (size_t)cap * 16, cudaMemcpyDeviceToHost));
-                CK(cudaMemcpy(rd.data(), s->P.ray_d, (size_t)cap * 16, cudaMemcpyDeviceToHost));
-                for (int64_t i = 0; i < m; i++) {
-                    float* r = s->cap_out + i * 8;
-                    float4 a = ro[q[i]], b = rd[q[i]];
-                    r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = b.x; r[4] = b.y; r[5] = b.z; r[6] = 0.001f; r[7] = INFINITY;
-                }
-                s->cap_n = m;
-            }
-            mark(2);
-            rth::launch_shade(s->S, s->P, R, dpt, qin, c + CTR_COUNT, c, s->cq, qout, cn + CTR_COUNT, s->sq,
-                              c + CTR_SHADOW_COUNT, s->sms, s->stream);
-            if (R.photons) rth::launch_photon_gather_paths(s->photons, s->P, s->P.gq, c + CTR_GATHER_COUNT, s->sms,
-                                                           s->stream);
-            mark(3);
-            rth::launch_shadow(s->S, s->P, s->sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, s->d_err, s->sms,
-                               s->stream);
-            nl += 3 + CLS_N;
+    if (ext_rays) *ext_rays = 0;
+    if (sh_rays) *sh_rays = 0;
+    if (launches) *launches = 0;
+    const uint32_t* active = nullptr;
+    uint32_t nactive = npix;
+    if (dconv) {
+        if (s->active_cap < npix + 1) {
+            free_dev((void*&)s->d_active);
+            s->active_cap = 0;
+            if (cudaMalloc(&s->d_active, ((size_t)npix + 1) * 4) != cudaSuccess)
+                return fail(s, RT_ERR_NOMEM, "cudaMalloc active pixel list");
+            s->active_cap = npix + 1;
         }
-        mark(0);
-        rth::launch_finalize(s->P, R, s->stream);
-        mark(0);
-        nl++;
-        CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(hc.data(), s->counters, sizeof(uint32_t) * (maxd + 2) * RT_CTR_STRIDE, cudaMemcpyDeviceToHost,
-                           s->stream));
+        uint32_t* dcount = s->d_active + npix;
+        CK(cudaMemsetAsync(dcount, 0, 4, s->stream));
+        rth::launch_active_list(dconv, npix, s->d_active, dcount, s->stream);
+        rth::launch_zero_converged(dconv, npix, nsamp, dscratch, s->stream);
+        CK(cudaMemcpyAsync(&nactive, dcount, 4, cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
-        for (uint32_t dpt = 0; dpt < maxd; dpt++) {
-            ext += hc[dpt * RT_CTR_STRIDE + CTR_COUNT];
-            sh += hc[dpt * RT_CTR_STRIDE + CTR_SHADOW_COUNT];
-        }
-        if (s->profiling) {
-            for (size_t e = 0; e + 1 < ev_used; e++) {
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, s->pev[e], s->pev[e + 1]);
-                int kind = s->pkind[e];
-                s->kms[kind] += ms;
-                if (!(kind == 0 && e > 0 && s->pkind[e - 1] == 0)) s->kcount[kind]++;
-            }
-        }
+        active = s->d_active;
+        if (launches) *launches += 2;
     }
-    if (ext_rays) *ext_rays = ext;
-    if (sh_rays) *sh_rays = sh;
-    if (launches) *launches = nl;
-    return RT_OK;
+    return run_wavefront(s, scene_bufs(s), cam, p, p->sample_idx, nsamp, dscratch, active, nactive, ext_rays, sh_rays,
+                         launches);
 }
 
 static int validate_pass(RtScene* s, const RtCamera* cam, const RtPassParams* p) {
@@ -1118,7 +1221,8 @@ extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const R
         CK(cudaMemsetAsync(s->cnt, 0, (size_t)npix * 4, s->stream));
     }
     uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
-    uint32_t per = std::max<uint32_t>(1, std::min<uint32_t>(nsamp, MAX_PATHS / npix));
+    // samples per wavefront run: as many as fit a 2 GiB sample buffer
+    uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nsamp, (2ull << 30) / ((uint64_t)npix * 12)));
     size_t bytes = (size_t)per * npix * 3 * sizeof(float);
     if (s->scratch_bytes < bytes) {
         free_dev((void*&)s->scratch);
@@ -1219,12 +1323,15 @@ extern "C" int32_t rt_capture_rays(RtScene* s, const RtCamera* cam, const RtPass
 // below instead of memory obtained at call time.  Every GPU that loads the
 // library holds this array (RT_NOALLOC_SCRATCH_BYTES = 15 MB) until the
 // process exits.
-#define RT_NOALLOC_PATHS RT_NOALLOC_MAX_PIXELS
+// path pool of the fixed array (positions are refilled with new samples as paths end):
+// two path sets of 8 float4 fields, hit, retire records (4 float4), class
+// queues and shadow rays
+#define RT_NOALLOC_PATHS 32768u
 static constexpr size_t kNaF4 = (size_t)RT_NOALLOC_PATHS * sizeof(float4);
 static constexpr size_t kNaQueue = (size_t)RT_NOALLOC_PATHS * sizeof(uint32_t);
 static constexpr size_t kNaShadow = (size_t)RT_NOALLOC_PATHS * 2 * 2 * sizeof(float4);
-static constexpr size_t kNaCounters = (size_t)(RT_MAX_DEPTH + 2) * RT_CTR_STRIDE * sizeof(uint32_t);
-static constexpr size_t kNaBytes = 9 * kNaF4 + (2 + CLS_N) * kNaQueue + kNaShadow + kNaCounters + 256;
+static constexpr size_t kNaCounters = (size_t)RT_CTR_WORDS * sizeof(uint32_t);
+static constexpr size_t kNaBytes = 21 * kNaF4 + CLS_N * kNaQueue + kNaShadow + kNaCounters + 256;
 static_assert(kNaBytes <= RT_NOALLOC_SCRATCH_BYTES, "no-alloc scratch size");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[RT_NOALLOC_SCRATCH_BYTES];
@@ -1265,54 +1372,32 @@ extern "C" int32_t rt_render_pass_noalloc(RtScene* s, const RtCamera* cam, const
     void* base = nullptr;
     if ((rc = noalloc_base(s, &base))) return rc;
     unsigned char* b = (unsigned char*)base;
-    PathState P;
-    float4** f4[] = {&P.ray_o, &P.ray_d, &P.hit, &P.thr, &P.wts, (float4**)&P.meta, &P.L, &P.pend0, &P.pend1};
-    for (int i = 0; i < 9; i++) *f4[i] = (float4*)(b + i * kNaF4);
-    size_t off = 9 * kNaF4;
-    uint32_t* queue[2] = {(uint32_t*)(b + off), (uint32_t*)(b + off + kNaQueue)};
-    off += 2 * kNaQueue;
-    ClassQueues cq;
-    for (int c = 0; c < CLS_N; c++) cq.q[c] = (uint32_t*)(b + off + c * kNaQueue);
-    off += CLS_N * kNaQueue;
-    float4* sq = (float4*)(b + off);
-    off += kNaShadow;
-    uint32_t* C = (uint32_t*)(b + off);
-    off += kNaCounters;
-    int* derr = (int*)(b + ((off + 255) & ~(size_t)255));
-    CK(cudaMemsetAsync(derr, 0, sizeof(int), s->stream));
-
-    uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
-    uint32_t per = std::max<uint32_t>(1, std::min<uint32_t>(nsamp, (uint32_t)(RT_NOALLOC_PATHS / npix)));
-    uint32_t maxd = std::min<uint32_t>(p->max_depth, RT_MAX_DEPTH);
-    for (uint32_t k0 = 0; k0 < nsamp; k0 += per) {
-        RenderLaunch R{};
-        R.width = p->width; R.height = p->height; R.npix = (uint32_t)npix;
-        R.nsamp = std::min(per, nsamp - k0);
-        R.sample_idx = p->sample_idx + k0;
-        R.strata = p->strata;
-        R.max_depth = maxd;
-        R.hero = std::max<uint32_t>(1, std::min<uint32_t>(p->hero_count, 4));
-        R.bg_scale = p->bg_scale;
-        R.seed = p->seed;
-        R.cam = *cam;
-        R.converged = nullptr;
-        R.scratch = scratch_rgb + (size_t)k0 * npix * 3;
-        // counters start at zero on every chunk: the array keeps the last call's contents
-        CK(cudaMemsetAsync(C, 0, kNaCounters, s->stream));
-        rth::launch_generate(s->S, P, R, queue[0], C + 0, s->stream);
-        for (uint32_t dpt = 0; dpt < maxd; dpt++) {
-            uint32_t* c = C + dpt * RT_CTR_STRIDE;
-            uint32_t* cn = C + (dpt + 1) * RT_CTR_STRIDE;
-            rth::launch_extend(s->S, P, queue[dpt & 1], c + CTR_COUNT, c + CTR_EXTEND_NEXT, derr, s->sms, s->stream);
-            rth::launch_shade(s->S, P, R, dpt, queue[dpt & 1], c + CTR_COUNT, c, cq, queue[(dpt + 1) & 1],
-                              cn + CTR_COUNT, sq, c + CTR_SHADOW_COUNT, s->sms, s->stream);
-            rth::launch_shadow(s->S, P, sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, derr, s->sms, s->stream);
-        }
-        rth::launch_finalize(P, R, s->stream);
-        CK(cudaGetLastError());
+    WaveBufs W;
+    size_t off = 0;
+    auto take_f4 = [&]() { float4* q = (float4*)(b + off); off += kNaF4; return q; };
+    for (int k = 0; k < 2; k++) {
+        PathState& P = W.set[k];
+        P.ray_o = take_f4(); P.ray_d = take_f4(); P.thr = take_f4(); P.wts = take_f4();
+        P.meta = (uint4*)take_f4(); P.L = take_f4(); P.pend0 = take_f4(); P.pend1 = take_f4();
     }
+    W.set[0].hit = W.set[1].hit = take_f4();
+    W.Rt.meta = (uint4*)take_f4(); W.Rt.L = take_f4(); W.Rt.pend0 = take_f4(); W.Rt.pend1 = take_f4();
+    for (int c = 0; c < CLS_N; c++) W.cq.q[c] = (uint32_t*)(b + off + c * kNaQueue);
+    off += CLS_N * kNaQueue;
+    W.sq = (float4*)(b + off);
+    off += kNaShadow;
+    W.counters = (uint32_t*)(b + off);
+    off += kNaCounters;
+    W.derr = (int*)(b + ((off + 255) & ~(size_t)255));
+    W.cap = RT_NOALLOC_PATHS;
+    CK(cudaMemsetAsync(W.derr, 0, sizeof(int), s->stream));
+    uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
+    // the run clears the counters it uses: the array keeps the last call's contents
+    rc = run_wavefront(s, W, cam, p, p->sample_idx, nsamp, scratch_rgb, nullptr, (uint32_t)npix, nullptr, nullptr,
+                       nullptr);
+    if (rc) return rc;
     int h = 0;
-    CK(cudaMemcpyAsync(&h, derr, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(&h, W.derr, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     if (h) return fail(s, h, "traversal stack overflow");
     return RT_OK;

@@ -13,10 +13,10 @@
 #define RT_SHADE_BLOCKS_PER_SM 8
 #define RT_MAX_DEPTH 256
 
-// Counter block of one bounce (RT_CTR_STRIDE uint32 per bounce): ray count,
-// fetch cursors of the persistent kernels, shadow-ray count, and per-material-
-// class path counts and cursors.
-#define RT_CTR_STRIDE 16
+// Counter block of one wavefront iteration (RT_CTR_STRIDE uint32): ray count,
+// fetch cursors of the persistent kernels, shadow-ray count, per-material-class
+// path counts and cursors, photon-gather requests and retired paths.
+#define RT_CTR_STRIDE 32
 #define CTR_COUNT          0
 #define CTR_EXTEND_NEXT    1
 #define CTR_CLASSIFY_NEXT  2
@@ -24,13 +24,30 @@
 #define CTR_SHADOW_NEXT    4
 #define CTR_CLS_COUNT      5   // 5 entries
 #define CTR_CLS_NEXT       10  // 5 entries
-#define CTR_GATHER_COUNT   15  // photon-gather requests of the bounce
+#define CTR_GATHER_COUNT   15  // photon-gather requests of the iteration
+#define CTR_RETIRE_COUNT   16  // paths that ended in the iteration
+
+// Render counters: a header of 64-bit totals, then a ring of RT_CTR_RING
+// iteration blocks (iteration it uses block it % RT_CTR_RING; the retire
+// kernel of iteration it clears block it + 2, whose last user, it − 2, is done).
+#define RT_CTR_RING        4
+#define CTR_HDR_WORDS      32
+#define HDR_GEN            0   // u64: next sample index to generate
+#define HDR_EXT            2   // u64: extension rays traced
+#define HDR_SHADOW         4   // u64: shadow rays traced
+#define RT_CTR_WORDS       512 // allocation (the photon build uses 14 blocks)
+static_assert(CTR_HDR_WORDS + RT_CTR_RING * RT_CTR_STRIDE <= RT_CTR_WORDS, "counter layout");
+static_assert(14 * RT_CTR_STRIDE <= RT_CTR_WORDS, "photon counter layout");
 
 // material classes shaded by separate kernels
 enum { CLS_MISS = 0, CLS_EMIT = 1, CLS_DIFFUSE = 2, CLS_METAL = 3, CLS_DIELEC = 4, CLS_N = 5 };
 struct ClassQueues { uint32_t* q[CLS_N]; };
 
-// Per-path wavefront state, structure of arrays, indexed by path id.
+// Per-path wavefront state, structure of arrays.  The render loop keeps two
+// dense sets (iteration it reads set it&1 at positions 0..count−1 and writes
+// the paths that go on, compacted, into the other set), plus a set of
+// retire records for the paths that ended (L, pend*, meta only).  `hit` and
+// `gq` are shared by the sets.
 struct PathState {
     float4* ray_o;     // origin xyz
     float4* ray_d;     // direction xyz
@@ -44,6 +61,14 @@ struct PathState {
     float4* pendC;     // parked caustic (photon-map) contribution, folded before pend0/pend1
     float4* gq;        // photon-gather requests of the bounce: (p, pid) (n, -)
 };
+
+// Where a contribution parked this iteration lives, for the shadow and gather
+// kernels: target tag = index << 2 | retired << 1 | (1 for the env-NEE slot).
+struct PendTargets {
+    float4* pend[4];    // [retired * 2 + which]: pend0 / pend1 of the next set, then of the retire records
+    float4* pendC[2];   // [retired]
+};
+#define PT_RETIRED 2u
 
 // meta.z flag layout
 #define PF_DEPTH_MASK   0xFFu
@@ -66,14 +91,20 @@ struct PhotonMapDev {
     rtph::Map view() const;
 };
 
+// One sample group of a render call: samples sample_idx .. sample_idx+nsamp−1
+// of every active pixel, traced by a pool of paths that is refilled with new
+// samples as paths end (sample g ↦ slot k = g / nactive, pixel active[g % nactive]).
 struct RenderLaunch {
-    uint32_t width, height, npix, nsamp;   // this chunk: nsamp consecutive samples
+    uint32_t width, height, npix, nsamp;
     uint32_t sample_idx, strata, max_depth, hero;
     float    bg_scale;
     uint64_t seed;
     RtCamera cam;
-    const uint8_t* converged;              // device, nullable
-    float*   scratch;                      // nsamp × npix × 3 (device)
+    const uint32_t* active;                // active pixel list (device), or null: every pixel
+    uint32_t nactive;
+    uint64_t total;                        // nsamp × nactive samples to trace
+    unsigned long long* gen_next;          // device cursor over [0, total)
+    float*   scratch;                      // nsamp × npix × 3 (device), slot-major
     int      photons;                      // a photon map feeds the diffuse vertices
 };
 
@@ -84,15 +115,25 @@ void launch_trace_any_api(const rtd::DevScene& S, const float* rays, uint32_t n,
                           int* err, int sms, cudaStream_t st);
 void launch_extend(const rtd::DevScene& S, const PathState& P, const uint32_t* queue, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st);
-void launch_shadow(const rtd::DevScene& S, const PathState& P, const float4* sq, const uint32_t* count,
+void launch_shadow(const rtd::DevScene& S, const PendTargets& T, const float4* sq, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st);
 
-void launch_generate(const rtd::DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t* queue0,
+// first fill of the path pool: samples 0 .. pool−1 into positions 0 .. pool−1 of set A
+void launch_generate(const rtd::DevScene& S, const PathState& A, const RenderLaunch& R, uint32_t pool,
                      uint32_t* count0, cudaStream_t st);
-void launch_shade(const rtd::DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t depth,
-                  const uint32_t* qin, const uint32_t* cin, uint32_t* ctr, const ClassQueues& Q, uint32_t* qout,
-                  uint32_t* cout, float4* sq, uint32_t* scount, int sms, cudaStream_t st);
-void launch_finalize(const PathState& P, const RenderLaunch& R, cudaStream_t st);
+// classify + one shading kernel per material class: paths that go on are
+// compacted into B (count `cout`), ended paths into the retire records Rt
+void launch_shade(const rtd::DevScene& S, const PathState& A, const PathState& B, const PathState& Rt,
+                  const RenderLaunch& R, uint32_t* ctr, const ClassQueues& Q, uint32_t* cout, float4* sq, int sms,
+                  cudaStream_t st);
+// write the ended paths' samples and append new samples, one per ended path
+// while samples remain, to B; add the iteration's ray counts to the header;
+// clear the counter block of iteration it + 2
+void launch_retire(const rtd::DevScene& S, const PathState& B, const PathState& Rt, const RenderLaunch& R,
+                   uint32_t* ctr, uint32_t* hdr, uint32_t* clear_block, uint32_t* cout, int sms, cudaStream_t st);
+// active-pixel list of a converged mask, and zero output for converged pixels
+void launch_active_list(const uint8_t* conv, uint32_t npix, uint32_t* list, uint32_t* count, cudaStream_t st);
+void launch_zero_converged(const uint8_t* conv, uint32_t npix, uint32_t nsamp, float* scratch, cudaStream_t st);
 
 cudaError_t photon_build(const rtd::DevScene& S, PhotonMapDev& map, const PathState& P, uint32_t* qa, uint32_t* qb,
                          uint32_t* counters, const RtPhotonParams& prm, const float* emit_setup, int sms,
@@ -102,7 +143,7 @@ cudaError_t photon_set(PhotonMapDev& map, const float4* pos, const float4* pow, 
 void launch_photon_gather_api(const PhotonMapDev& map, const float* q, uint32_t n, float* out, int sms, cudaStream_t st);
 void launch_knn_api(const PhotonMapDev& map, const float* q, uint32_t n, int k, float rmax2, int* idx, float* d2,
                     int* err, int sms, cudaStream_t st);
-void launch_photon_gather_paths(const PhotonMapDev& map, const PathState& P, const float4* gq, const uint32_t* count,
+void launch_photon_gather_paths(const PhotonMapDev& map, const PendTargets& T, const float4* gq, const uint32_t* count,
                                 int sms, cudaStream_t st);
 void launch_accumulate(const float* scratch, uint32_t nsamp, uint32_t npix, float* acc, float* m2, uint32_t* cnt,
                        const uint8_t* conv, float clamp, uint32_t min_samples, float floor_, cudaStream_t st);

@@ -631,7 +631,7 @@ __global__ void k_knn_api(rtph::Map M, const float* q, uint32_t n, int k, float 
 
 // render path: caustic injection at queued diffuse vertices (renderer.rs:461-467);
 // pendC[pid] holds T·tint·albedo and becomes that × irradiance
-__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Map M, PathState P,
+__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Map M, PendTargets T,
                                                                         const float4* __restrict__ gq,
                                                                         const uint32_t* count) {
     __shared__ uint32_t hist[RT_SHADE_BLOCK / 32][32];
@@ -641,12 +641,13 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Ma
     uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t i = gw; i < n; i += nw) {
         float4 a = gq[(size_t)i * 2], b = gq[(size_t)i * 2 + 1];
-        uint32_t pid = __float_as_uint(a.w);
+        uint32_t tag = __float_as_uint(a.w);
         float3 r = rtph::warp_irradiance(M, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), hist[w], sel[w]);
         if ((threadIdx.x & 31u) == 0) {
-            float4 f = P.pendC[pid];
+            float4* pc = T.pendC[(tag >> 1) & 1u] + (tag >> 2);
+            float4 f = *pc;
             bool any = r.x > 0.0f || r.y > 0.0f || r.z > 0.0f;
-            P.pendC[pid] = any ? make_float4(f.x * r.x, f.y * r.y, f.z * r.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+            *pc = any ? make_float4(f.x * r.x, f.y * r.y, f.z * r.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
     }
 }
@@ -807,9 +808,9 @@ void launch_knn_api(const PhotonMapDev& map, const float* q, uint32_t n, int k, 
                     int* err, int sms, cudaStream_t st) {
     k_knn_api<<<sms * 4, RT_SHADE_BLOCK, 0, st>>>(map.view(), q, n, k, rmax2, idx, d2, err);
 }
-void launch_photon_gather_paths(const PhotonMapDev& map, const PathState& P, const float4* gq, const uint32_t* count,
+void launch_photon_gather_paths(const PhotonMapDev& map, const PendTargets& T, const float4* gq, const uint32_t* count,
                                 int sms, cudaStream_t st) {
-    k_photon_gather_paths<<<sms * 4, RT_SHADE_BLOCK, 0, st>>>(map.view(), P, gq, count);
+    k_photon_gather_paths<<<sms * 4, RT_SHADE_BLOCK, 0, st>>>(map.view(), T, gq, count);
 }
 
 }  // namespace rth

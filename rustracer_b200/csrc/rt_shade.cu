@@ -306,55 +306,113 @@ RT_D uint32_t warp_append(uint32_t* counter, bool pred) {
 }  // namespace
 
 // ── generate ────────────────────────────────────────────────────────────────
-__global__ void k_generate(DevScene S, PathState P, RenderLaunch R, uint32_t* queue0, uint32_t* count0) {
-    uint32_t total = R.npix * R.nsamp;
-    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < total; pid += gridDim.x * blockDim.x) {
-        uint32_t k = pid / R.npix, i = pid - k * R.npix;
-        uint32_t row = i / R.width, col = i - row * R.width;
-        uint32_t sample = R.sample_idx + k;
-        P.L[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
-        P.pend0[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
-        P.pend1[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (R.photons) P.pendC[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
-        bool conv = R.converged && R.converged[i];
-        Rng rng = make_rng(R.seed, i, sample);
-        float wd = (float)max(R.width - 1u, 1u), hd = (float)max(R.height - 1u, 1u);
-        uint32_t strata = R.strata, s2 = strata * strata, ray_y = R.height - 1u - row;
-        float uj, vj;
-        if (s2 > 0) {
-            uint32_t off = (i * 0x9E3779B9u) % s2;
-            uint32_t si = (sample + off) % s2;
-            uj = ((float)(si % strata) + rnd(rng, D_JIT_U)) / (float)strata;
-            vj = ((float)(si / strata) + rnd(rng, D_JIT_V)) / (float)strata;
-        } else {
-            uj = rnd(rng, D_JIT_U); vj = rnd(rng, D_JIT_V);
+// Camera ray of sample g of the group into path slot `pid` (Camera::get_ray,
+// camera.rs:93-127, with the stratified jitter of renderer.rs:262-283).
+RT_D void init_path(const DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t pid, uint64_t g) {
+    uint32_t k = (uint32_t)(g / R.nactive), j = (uint32_t)(g - (uint64_t)k * R.nactive);
+    uint32_t i = R.active ? __ldg(R.active + j) : j;
+    uint32_t row = i / R.width, col = i - row * R.width;
+    uint32_t sample = R.sample_idx + k;
+    P.L[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+    P.pend0[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+    P.pend1[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (R.photons) P.pendC[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
+    Rng rng = make_rng(R.seed, i, sample);
+    float wd = (float)max(R.width - 1u, 1u), hd = (float)max(R.height - 1u, 1u);
+    uint32_t strata = R.strata, s2 = strata * strata, ray_y = R.height - 1u - row;
+    float uj, vj;
+    if (s2 > 0) {
+        uint32_t off = (i * 0x9E3779B9u) % s2;
+        uint32_t si = (sample + off) % s2;
+        uj = ((float)(si % strata) + rnd(rng, D_JIT_U)) / (float)strata;
+        vj = ((float)(si / strata) + rnd(rng, D_JIT_V)) / (float)strata;
+    } else {
+        uj = rnd(rng, D_JIT_U); vj = rnd(rng, D_JIT_V);
+    }
+    float u = ((float)col + uj) / wd, v = ((float)ray_y + vj) / hd;
+    const RtCamera& c = R.cam;
+    float3 cu = mk(c.u[0], c.u[1], c.u[2]), cv = mk(c.v[0], c.v[1], c.v[2]);
+    float3 org = mk(c.origin[0], c.origin[1], c.origin[2]);
+    float lr = sqrtf(rnd(rng, D_LENS_R));
+    float ls, lc;
+    sincosf(2.0f * PI_F * rnd(rng, D_LENS_P), &ls, &lc);
+    float3 rd = c.lens_radius * mk(lr * lc, lr * ls, 0.0f);
+    float3 off = cu * rd.x + cv * rd.y;
+    float3 ll = mk(c.lower_left[0], c.lower_left[1], c.lower_left[2]);
+    float3 hz = mk(c.horizontal[0], c.horizontal[1], c.horizontal[2]);
+    float3 vt = mk(c.vertical[0], c.vertical[1], c.vertical[2]);
+    float3 o = org + off;
+    float3 d = ll + u * hz + v * vt - org - off;
+    int H = (int)R.hero;
+    float lam0 = S.lam_lo + S.lam_range * rnd(rng, D_LAMBDA);
+    if (lam0 >= S.lam_lo + S.lam_range) lam0 = nextafterf(S.lam_lo + S.lam_range, 0.0f);
+    P.ray_o[pid] = make_float4(o.x, o.y, o.z, 0.f);
+    P.ray_d[pid] = make_float4(d.x, d.y, d.z, 0.f);
+    P.thr[pid] = make_float4(1.f, 1.f, 1.f, 1.f);
+    P.wts[pid] = make_float4(1.f, H > 1 ? 1.f : 0.f, H > 2 ? 1.f : 0.f, H > 3 ? 1.f : 0.f);
+    P.meta[pid] = make_uint4(i, k, PF_PREV_SPEC | (H > 1 ? PF_SEC_ALIVE : 0u), __float_as_uint(lam0));
+}
+
+__global__ void k_generate(DevScene S, PathState A, RenderLaunch R, uint32_t pool, uint32_t* count0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) { *R.gen_next = pool; *count0 = pool; }
+    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < pool; pid += gridDim.x * blockDim.x)
+        init_path(S, A, R, pid, pid);
+}
+
+// ── retire + refill ─────────────────────────────────────────────────────────
+// An ended path folds its last parked contributions (caustic, area-light NEE,
+// env NEE — the order of renderer.rs:461-540) and writes its sample; for each
+// ended path the next ungenerated sample, if any, is appended to the next set.
+__global__ void k_retire(DevScene S, PathState B, PathState Rt, RenderLaunch R, uint32_t* ctr, uint32_t* hdr,
+                         uint32_t* clear_block, uint32_t* cout) {
+    uint32_t n = ctr[CTR_RETIRE_COUNT];
+    if (blockIdx.x == 0) {
+        if (threadIdx.x == 0) {
+            atomicAdd((unsigned long long*)(hdr + HDR_EXT), (unsigned long long)ctr[CTR_COUNT]);
+            atomicAdd((unsigned long long*)(hdr + HDR_SHADOW), (unsigned long long)ctr[CTR_SHADOW_COUNT]);
         }
-        float u = ((float)col + uj) / wd, v = ((float)ray_y + vj) / hd;
-        const RtCamera& c = R.cam;
-        float3 cu = mk(c.u[0], c.u[1], c.u[2]), cv = mk(c.v[0], c.v[1], c.v[2]);
-        float3 org = mk(c.origin[0], c.origin[1], c.origin[2]);
-        float lr = sqrtf(rnd(rng, D_LENS_R));
-        float ls, lc;
-        sincosf(2.0f * PI_F * rnd(rng, D_LENS_P), &ls, &lc);
-        float3 rd = c.lens_radius * mk(lr * lc, lr * ls, 0.0f);
-        float3 off = cu * rd.x + cv * rd.y;
-        float3 ll = mk(c.lower_left[0], c.lower_left[1], c.lower_left[2]);
-        float3 hz = mk(c.horizontal[0], c.horizontal[1], c.horizontal[2]);
-        float3 vt = mk(c.vertical[0], c.vertical[1], c.vertical[2]);
-        float3 o = org + off;
-        float3 d = ll + u * hz + v * vt - org - off;
-        int H = (int)R.hero;
-        float lam0 = S.lam_lo + S.lam_range * rnd(rng, D_LAMBDA);
-        if (lam0 >= S.lam_lo + S.lam_range) lam0 = nextafterf(S.lam_lo + S.lam_range, 0.0f);
-        P.ray_o[pid] = make_float4(o.x, o.y, o.z, 0.f);
-        P.ray_d[pid] = make_float4(d.x, d.y, d.z, 0.f);
-        P.thr[pid] = make_float4(1.f, 1.f, 1.f, 1.f);
-        P.wts[pid] = make_float4(1.f, H > 1 ? 1.f : 0.f, H > 2 ? 1.f : 0.f, H > 3 ? 1.f : 0.f);
-        P.meta[pid] = make_uint4(i, k, PF_PREV_SPEC | (H > 1 ? PF_SEC_ALIVE : 0u), __float_as_uint(lam0));
-        if (!conv) {
-            uint32_t slot = warp_append(count0, true);
-            queue0[slot] = pid;
+        if (threadIdx.x < RT_CTR_STRIDE) clear_block[threadIdx.x] = 0u;
+    }
+    uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        uint32_t j = base + threadIdx.x;
+        bool act = j < n;
+        if (act) {
+            float4 L = Rt.L[j], a = Rt.pend0[j], b = Rt.pend1[j];
+            if (R.photons) { float4 c = Rt.pendC[j]; L.x += c.x; L.y += c.y; L.z += c.z; }
+            L.x += a.x; L.y += a.y; L.z += a.z;
+            L.x += b.x; L.y += b.y; L.z += b.z;
+            uint4 meta = Rt.meta[j];
+            float* out = R.scratch + ((size_t)meta.y * R.npix + meta.x) * 3;
+            out[0] = L.x; out[1] = L.y; out[2] = L.z;
         }
+        // warp-aggregated claim of new samples
+        uint32_t m = __ballot_sync(0xFFFFFFFFu, act);
+        unsigned long long g0 = 0;
+        if (m && lane == 0) g0 = atomicAdd(R.gen_next, (unsigned long long)__popc(m));
+        g0 = __shfl_sync(0xFFFFFFFFu, g0, 0);
+        uint64_t g = g0 + __popc(m & ((1u << lane) - 1u));
+        bool fresh = act && g < R.total;
+        uint32_t slot = warp_append(cout, fresh);
+        if (fresh) init_path(S, B, R, slot, g);
+    }
+}
+
+// ── converged pixels ─────────────────────────────────────────────────────────
+__global__ void k_active_list(const uint8_t* __restrict__ conv, uint32_t npix, uint32_t* list, uint32_t* count) {
+    for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < npix; b0 += gridDim.x * blockDim.x) {
+        uint32_t i = b0 + threadIdx.x;
+        bool a = i < npix && !conv[i];
+        uint32_t slot = warp_append(count, a);
+        if (a) list[slot] = i;
+    }
+}
+
+__global__ void k_zero_converged(const uint8_t* __restrict__ conv, uint32_t npix, uint32_t nsamp, float* scratch) {
+    uint64_t total = (uint64_t)npix * nsamp;
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t i = (uint32_t)(e % npix);
+        if (conv[i]) { float* o = scratch + e * 3; o[0] = 0.f; o[1] = 0.f; o[2] = 0.f; }
     }
 }
 
@@ -376,7 +434,7 @@ RT_D int material_class(const DevScene& S, uint32_t ref) {
     return CLS_DIFFUSE;
 }
 
-__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_classify(DevScene S, PathState P, const uint32_t* __restrict__ qin,
+__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_classify(DevScene S, const float4* __restrict__ hit,
                                                              const uint32_t* cin, uint32_t* next, ClassQueues Q,
                                                              uint32_t* cls_count) {
     uint32_t n = *cin;
@@ -389,8 +447,8 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_classify(DevScene S, PathSta
         int cls = -1;
         uint32_t pid = 0;
         if (qi < n) {
-            pid = qin[qi];
-            cls = material_class(S, __float_as_uint(P.hit[pid].x));
+            pid = qi;
+            cls = material_class(S, __float_as_uint(hit[pid].x));
         }
 #pragma unroll
         for (int c = 0; c < CLS_N; c++) {
@@ -441,10 +499,10 @@ RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
 }
 
 template <int CLS>
-__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState P, RenderLaunch R, uint32_t depth,
-                                                          const uint32_t* __restrict__ qin, const uint32_t* cin,
-                                                          uint32_t* next, uint32_t* qout, uint32_t* cout,
-                                                          float4* __restrict__ sq, uint32_t* scount) {
+__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState A, PathState B, PathState Rt,
+                                                          RenderLaunch R, const uint32_t* __restrict__ qin,
+                                                          const uint32_t* cin, uint32_t* next, uint32_t* cout,
+                                                          float4* __restrict__ sq, uint32_t* ctr) {
     uint32_t n = *cin;
     int H = (int)R.hero;
     bool have_lights = S.n_lights > 0;
@@ -458,26 +516,28 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
         uint32_t pid = active ? qin[qi] : 0u;
         bool cont = false, sh0 = false, sh1 = false, gath = false;
         float4 sh0a, sh0b, sh1a, sh1b, ga, gb;
+        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 np0 = zero4, np1 = zero4, npc = zero4;     // contributions parked this bounce
+        float4 Lout = zero4, o_out = zero4, d_out = zero4, thr_out = zero4, w_out = zero4;
+        uint4 meta = make_uint4(0u, 0u, 0u, 0u);
         if (active) {
-            uint4 meta = P.meta[pid];
-            float4 thr = P.thr[pid], w = P.wts[pid], L = P.L[pid];
-            float4 p0 = P.pend0[pid], p1 = P.pend1[pid];
+            meta = A.meta[pid];
+            float4 thr = A.thr[pid], w = A.wts[pid], L = A.L[pid];
+            float4 p0 = A.pend0[pid], p1 = A.pend1[pid];
             // fold the previous bounce's parked contributions in the reference's
             // order: caustic injection, area-light NEE, env NEE (renderer.rs:461-540)
             if (R.photons) {
-                float4 pc = P.pendC[pid];
+                float4 pc = A.pendC[pid];
                 L.x += pc.x; L.y += pc.y; L.z += pc.z;
-                if (pc.x != 0.f || pc.y != 0.f || pc.z != 0.f) P.pendC[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
             L.x += p0.x; L.y += p0.y; L.z += p0.z;
             L.x += p1.x; L.y += p1.y; L.z += p1.z;
-            if (p0.x != 0.f || p0.y != 0.f || p0.z != 0.f) P.pend0[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (p1.x != 0.f || p1.y != 0.f || p1.z != 0.f) P.pend1[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
-            float4 ro = P.ray_o[pid], rdv = P.ray_d[pid];
+            float4 ro = A.ray_o[pid], rdv = A.ray_d[pid];
             float3 o = mk(ro.x, ro.y, ro.z), d = mk(rdv.x, rdv.y, rdv.z);
             float3 T = mk(thr.x, thr.y, thr.z);
             float prev_mis = thr.w;
             uint32_t flags = meta.z;
+            uint32_t depth = flags & PF_DEPTH_MASK;
             bool prev_spec = flags & PF_PREV_SPEC;
             int tint = (flags & PF_TINT_MASK) >> PF_TINT_SHIFT;
             float lam0 = __uint_as_float(meta.w);
@@ -490,7 +550,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                 float3 bg = (depth == 0 || !S.has_env) ? bg_eval(S, d) : env_lookup(S, d);
                 Lc = Lc + T * (bg * spec_factor(S, tint, w, lam0, H)) * R.bg_scale * emit_w;
             } else if (CLS == CLS_EMIT) {                                           // renderer.rs:415-419
-                float4 hv = P.hit[pid];
+                float4 hv = A.hit[pid];
                 uint32_t ref = __float_as_uint(hv.x), type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
                 int mat = type == RT_PRIM_TRI ? __float_as_int(__ldg(S.tri + (size_t)idx * 3 + 2).z)
                         : type == RT_PRIM_QUAD ? __float_as_int(__ldg(S.quad + (size_t)idx * 5 + 4).y)
@@ -498,7 +558,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                 float emit_w = (prev_spec || !have_lights) ? 1.0f : prev_mis;
                 Lc = Lc + T * emission(S, S.mats[mat], tint, w, lam0, H) * emit_w;
             } else {
-                Surf sf_ = surface(S, P.hit[pid], o, d);
+                Surf sf_ = surface(S, A.hit[pid], o, d);
                 float3 p = sf_.p, nrm = sf_.nrm;
                 float t = sf_.t;
                 bool front = sf_.front;
@@ -594,9 +654,9 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                     if (R.photons) {
                         // caustic injection: the gather kernel turns T·tint·albedo into × irradiance
                         float3 f = T * sf * att;
-                        P.pendC[pid] = make_float4(f.x, f.y, f.z, 0.f);
+                        npc = make_float4(f.x, f.y, f.z, 0.f);
                         gath = true;
-                        ga = make_float4(p.x, p.y, p.z, __uint_as_float(pid));
+                        ga = make_float4(p.x, p.y, p.z, 0.f);
                         gb = make_float4(nrm.x, nrm.y, nrm.z, 0.f);
                     }
                     if (have_lights) {
@@ -611,10 +671,10 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                             if (mis_d > 0.0f && brdf > 0.0f) {
                                 float3 nee = emission(S, S.mats[lr.mat], tint, w, lam0, H);
                                 float3 c = T * att * brdf * l_pdf * nee / mis_d;
-                                P.pend0[pid] = make_float4(c.x, c.y, c.z, 0.f);
+                                np0 = make_float4(c.x, c.y, c.z, 0.f);
                                 sh0 = true;
                                 sh0a = make_float4(p.x, p.y, p.z, lr.t * (1.0f - 1e-4f));
-                                sh0b = make_float4(ldir.x, ldir.y, ldir.z, __uint_as_float(pid << 1));
+                                sh0b = make_float4(ldir.x, ldir.y, ldir.z, 0.f);
                             }
                         }
                     }
@@ -629,10 +689,10 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                                 float3 ec = env_lookup(S, edir) * sf;
                                 float mis_d = epdf * epdf + brdf * brdf + area_pdf * area_pdf;
                                 float3 c = T * att * brdf * epdf * ec / mis_d;
-                                P.pend1[pid] = make_float4(c.x, c.y, c.z, 0.f);
+                                np1 = make_float4(c.x, c.y, c.z, 0.f);
                                 sh1 = true;
                                 sh1a = make_float4(p.x, p.y, p.z, INFINITY);
-                                sh1b = make_float4(edir.x, edir.y, edir.z, __uint_as_float((pid << 1) | 1u));
+                                sh1b = make_float4(edir.x, edir.y, edir.z, 0.f);
                             }
                         }
                     }
@@ -669,46 +729,41 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                 }
                 cont = alive && depth + 1 < R.max_depth;
             }
-            P.L[pid] = make_float4(Lc.x, Lc.y, Lc.z, 0.f);
+            Lout = make_float4(Lc.x, Lc.y, Lc.z, 0.f);
             if (cont) {
-                flags = (flags & ~(PF_DEPTH_MASK | PF_PREV_SPEC | PF_TINT_MASK)) | ((depth + 1) & PF_DEPTH_MASK)
-                        | (prev_spec ? PF_PREV_SPEC : 0u) | ((uint32_t)tint << PF_TINT_SHIFT);
-                P.ray_o[pid] = make_float4(o.x, o.y, o.z, 0.f);
-                P.ray_d[pid] = make_float4(d.x, d.y, d.z, 0.f);
-                P.thr[pid] = make_float4(T.x, T.y, T.z, prev_mis);
-                P.wts[pid] = w;
-                P.meta[pid] = make_uint4(meta.x, meta.y, flags, meta.w);
+                meta.z = (flags & ~(PF_DEPTH_MASK | PF_PREV_SPEC | PF_TINT_MASK)) | ((depth + 1) & PF_DEPTH_MASK)
+                         | (prev_spec ? PF_PREV_SPEC : 0u) | ((uint32_t)tint << PF_TINT_SHIFT);
+                o_out = make_float4(o.x, o.y, o.z, 0.f);
+                d_out = make_float4(d.x, d.y, d.z, 0.f);
+                thr_out = make_float4(T.x, T.y, T.z, prev_mis);
+                w_out = w;
             }
         }
-        if (CLS != CLS_MISS && CLS != CLS_EMIT) {
-            // warp-aggregated compaction of survivors and shadow rays
-            uint32_t slot = warp_append(cout, cont);
-            if (cont) qout[slot] = pid;
+        // warp-aggregated compaction: paths that go on into B, ended paths into
+        // the retire records; parked contributions and shadow rays follow them
+        uint32_t slot = 0;
+        if (CLS != CLS_MISS && CLS != CLS_EMIT) slot = warp_append(cout, cont);
+        bool ended = active && !cont;
+        uint32_t rs = warp_append(ctr + CTR_RETIRE_COUNT, ended);
+        if (cont) {
+            B.ray_o[slot] = o_out; B.ray_d[slot] = d_out; B.thr[slot] = thr_out; B.wts[slot] = w_out;
+            B.meta[slot] = meta; B.L[slot] = Lout; B.pend0[slot] = np0; B.pend1[slot] = np1;
+            if (R.photons) B.pendC[slot] = npc;
+        } else if (ended) {
+            Rt.meta[rs] = meta; Rt.L[rs] = Lout; Rt.pend0[rs] = np0; Rt.pend1[rs] = np1;
+            if (R.photons) Rt.pendC[rs] = npc;
         }
+        uint32_t tag = cont ? slot << 2 : (rs << 2) | PT_RETIRED;
         if (CLS == CLS_DIFFUSE) {
             if (R.photons) {
-                uint32_t g = warp_append(scount + (CTR_GATHER_COUNT - CTR_SHADOW_COUNT), gath);
-                if (gath) { P.gq[(size_t)g * 2] = ga; P.gq[(size_t)g * 2 + 1] = gb; }
+                uint32_t g = warp_append(ctr + CTR_GATHER_COUNT, gath);
+                if (gath) { ga.w = __uint_as_float(tag); A.gq[(size_t)g * 2] = ga; A.gq[(size_t)g * 2 + 1] = gb; }
             }
-            uint32_t s0 = warp_append(scount, sh0);
-            if (sh0) { sq[(size_t)s0 * 2] = sh0a; sq[(size_t)s0 * 2 + 1] = sh0b; }
-            uint32_t s1 = warp_append(scount, sh1);
-            if (sh1) { sq[(size_t)s1 * 2] = sh1a; sq[(size_t)s1 * 2 + 1] = sh1b; }
+            uint32_t s0 = warp_append(ctr + CTR_SHADOW_COUNT, sh0);
+            if (sh0) { sh0b.w = __uint_as_float(tag); sq[(size_t)s0 * 2] = sh0a; sq[(size_t)s0 * 2 + 1] = sh0b; }
+            uint32_t s1 = warp_append(ctr + CTR_SHADOW_COUNT, sh1);
+            if (sh1) { sh1b.w = __uint_as_float(tag | 1u); sq[(size_t)s1 * 2] = sh1a; sq[(size_t)s1 * 2 + 1] = sh1b; }
         }
-    }
-}
-
-// ── finalize: fold parked contributions, write the pass output ──────────────
-__global__ void k_finalize(PathState P, RenderLaunch R) {
-    uint32_t total = R.npix * R.nsamp;
-    for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < total; pid += gridDim.x * blockDim.x) {
-        float4 L = P.L[pid], a = P.pend0[pid], b = P.pend1[pid];
-        if (R.photons) { float4 c = P.pendC[pid]; L.x += c.x; L.y += c.y; L.z += c.z; }
-        L.x += a.x; L.y += a.y; L.z += a.z;
-        L.x += b.x; L.y += b.y; L.z += b.z;
-        uint4 meta = P.meta[pid];
-        float* out = R.scratch + ((size_t)meta.y * R.npix + meta.x) * 3;
-        out[0] = L.x; out[1] = L.y; out[2] = L.z;
     }
 }
 
@@ -741,35 +796,37 @@ __global__ void k_accumulate(const float* __restrict__ scratch, uint32_t nsamp, 
 }
 
 namespace rth {
-void launch_generate(const DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t* queue0, uint32_t* count0,
+void launch_generate(const DevScene& S, const PathState& A, const RenderLaunch& R, uint32_t pool, uint32_t* count0,
                      cudaStream_t st) {
-    uint32_t total = R.npix * R.nsamp;
-    int grid = (int)std::min<uint32_t>((total + 255) / 256, 148u * 16u);
-    k_generate<<<grid, 256, 0, st>>>(S, P, R, queue0, count0);
+    int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>((pool + 255) / 256, 148u * 16u));
+    k_generate<<<grid, 256, 0, st>>>(S, A, R, pool, count0);
 }
-void launch_shade(const DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t depth, const uint32_t* qin,
-                  const uint32_t* cin, uint32_t* ctr, const ClassQueues& Q, uint32_t* qout, uint32_t* cout,
-                  float4* sq, uint32_t* scount, int sms, cudaStream_t st) {
-    // ctr: this bounce's counter block (see rt_internal.h for the slots)
+void launch_shade(const DevScene& S, const PathState& A, const PathState& B, const PathState& Rt, const RenderLaunch& R,
+                  uint32_t* ctr, const ClassQueues& Q, uint32_t* cout, float4* sq, int sms, cudaStream_t st) {
+    // ctr: this iteration's counter block (see rt_internal.h for the slots)
     int grid = sms * RT_SHADE_BLOCKS_PER_SM;
-    k_classify<<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, qin, cin, ctr + CTR_CLASSIFY_NEXT, Q, ctr + CTR_CLS_COUNT);
-    k_shade<CLS_MISS><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, Q.q[CLS_MISS], ctr + CTR_CLS_COUNT + CLS_MISS,
-                                                       ctr + CTR_CLS_NEXT + CLS_MISS, qout, cout, sq, scount);
-    k_shade<CLS_EMIT><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, Q.q[CLS_EMIT], ctr + CTR_CLS_COUNT + CLS_EMIT,
-                                                       ctr + CTR_CLS_NEXT + CLS_EMIT, qout, cout, sq, scount);
-    k_shade<CLS_DIFFUSE><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, Q.q[CLS_DIFFUSE],
-                                                          ctr + CTR_CLS_COUNT + CLS_DIFFUSE,
-                                                          ctr + CTR_CLS_NEXT + CLS_DIFFUSE, qout, cout, sq, scount);
-    k_shade<CLS_METAL><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, Q.q[CLS_METAL], ctr + CTR_CLS_COUNT + CLS_METAL,
-                                                        ctr + CTR_CLS_NEXT + CLS_METAL, qout, cout, sq, scount);
-    k_shade<CLS_DIELEC><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, P, R, depth, Q.q[CLS_DIELEC],
-                                                         ctr + CTR_CLS_COUNT + CLS_DIELEC,
-                                                         ctr + CTR_CLS_NEXT + CLS_DIELEC, qout, cout, sq, scount);
+    k_classify<<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A.hit, ctr + CTR_COUNT, ctr + CTR_CLASSIFY_NEXT, Q,
+                                                ctr + CTR_CLS_COUNT);
+#define RT_SHADE_CLASS(C)                                                                                   \
+    k_shade<C><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C,            \
+                                                ctr + CTR_CLS_NEXT + C, cout, sq, ctr)
+    RT_SHADE_CLASS(CLS_MISS);
+    RT_SHADE_CLASS(CLS_EMIT);
+    RT_SHADE_CLASS(CLS_DIFFUSE);
+    RT_SHADE_CLASS(CLS_METAL);
+    RT_SHADE_CLASS(CLS_DIELEC);
+#undef RT_SHADE_CLASS
 }
-void launch_finalize(const PathState& P, const RenderLaunch& R, cudaStream_t st) {
-    uint32_t total = R.npix * R.nsamp;
-    int grid = (int)std::min<uint32_t>((total + 255) / 256, 148u * 16u);
-    k_finalize<<<grid, 256, 0, st>>>(P, R);
+void launch_retire(const DevScene& S, const PathState& B, const PathState& Rt, const RenderLaunch& R, uint32_t* ctr,
+                   uint32_t* hdr, uint32_t* clear_block, uint32_t* cout, int sms, cudaStream_t st) {
+    k_retire<<<sms * 8, 256, 0, st>>>(S, B, Rt, R, ctr, hdr, clear_block, cout);
+}
+void launch_active_list(const uint8_t* conv, uint32_t npix, uint32_t* list, uint32_t* count, cudaStream_t st) {
+    int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>((npix + 255) / 256, 148u * 16u));
+    k_active_list<<<grid, 256, 0, st>>>(conv, npix, list, count);
+}
+void launch_zero_converged(const uint8_t* conv, uint32_t npix, uint32_t nsamp, float* scratch, cudaStream_t st) {
+    k_zero_converged<<<148 * 16, 256, 0, st>>>(conv, npix, nsamp, scratch);
 }
 void launch_accumulate(const float* scratch, uint32_t nsamp, uint32_t npix, float* acc, float* m2, uint32_t* cnt,
                        const uint8_t* conv, float clamp, uint32_t min_samples, float floor_, cudaStream_t st) {

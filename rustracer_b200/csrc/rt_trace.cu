@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_closest(DevScene S, PathStat
                     item = i;
                     float tmax;
                     if (MODE == 0) {
-                        pid = queue[i];
+                        pid = queue ? queue[i] : i;
                         float4 ro = P.ray_o[pid], rd = P.ray_d[pid];
                         o = mk(ro.x, ro.y, ro.z); d = mk(rd.x, rd.y, rd.z);
                         tmin = 0.001f; tmax = INFINITY;
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_closest(DevScene S, PathStat
 // MODE 0: wavefront shadow rays (an occluded ray cancels its parked contribution)
 // MODE 1: API any-hit (occluded flags)
 template <int MODE>
-__global__ void __launch_bounds__(RT_TRACE_BLOCK) k_any(DevScene S, PathState P, const float4* __restrict__ sq,
+__global__ void __launch_bounds__(RT_TRACE_BLOCK) k_any(DevScene S, PendTargets T, const float4* __restrict__ sq,
                                                         const float* __restrict__ rays, uint32_t n_api,
                                                         const uint32_t* count, uint32_t* next,
                                                         uint8_t* __restrict__ out, int* err) {
@@ -422,11 +422,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_any(DevScene S, PathState P,
             if (!more) {
                 active = false;
                 if (MODE == 0) {
-                    if (hit) {
-                        uint32_t p = tag >> 1;
-                        if (tag & 1u) P.pend1[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-                        else          P.pend0[p] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    }
+                    if (hit) T.pend[tag & 3u][tag >> 2] = make_float4(0.f, 0.f, 0.f, 0.f);
                 } else {
                     out[item] = hit ? 1 : 0;
                 }
@@ -446,14 +442,14 @@ void launch_trace_closest_api(const DevScene& S, const float* rays, uint32_t n, 
 }
 void launch_trace_any_api(const DevScene& S, const float* rays, uint32_t n, uint8_t* out, uint32_t* next, int* err,
                           int sms, cudaStream_t st) {
-    k_any<1><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, PathState{}, nullptr, rays, n, nullptr, next, out, err);
+    k_any<1><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, PendTargets{}, nullptr, rays, n, nullptr, next, out, err);
 }
 void launch_extend(const DevScene& S, const PathState& P, const uint32_t* queue, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st) {
     k_closest<0><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, P, queue, nullptr, 0, count, next, nullptr, err);
 }
-void launch_shadow(const DevScene& S, const PathState& P, const float4* sq, const uint32_t* count,
+void launch_shadow(const DevScene& S, const PendTargets& T, const float4* sq, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st) {
-    k_any<0><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, P, sq, nullptr, 0, count, next, nullptr, err);
+    k_any<0><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, T, sq, nullptr, 0, count, next, nullptr, err);
 }
 }  // namespace rth
