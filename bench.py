@@ -327,17 +327,18 @@ def roofline(scene, sb, cam):
 
 
 def one_pass():
-    """Profiler driver: one warm-up pass and one measured pass of the
-    1920×1080 icosphere workload, 4 samples per pixel per pass — the same
-    8.3M-path chunk that each wavefront launch of the timed render processes."""
+    """Profiler driver: one warm-up call and one measured call of the 1920×1080
+    icosphere workload, 16 samples per pixel per call: 33.2M path samples
+    through the 8.4M-path pool, so most launches run on a full, refilled pool
+    as in the timed 64-spp render."""
     import torch
     from rustracer_b200 import configs
     from rustracer_b200.renderer import GpuScene, pass_params
     sb, st = configs.icosphere_scene(seed=2)
     scene = GpuScene(sb, device=0)
-    out = torch.zeros((4, H, W, 3), device="cuda")
+    out = torch.zeros((16, H, W, 3), device="cuda")
     for k in range(2):
-        scene.render_pass(st["camera"], pass_params(W, H, 4 * k, 4, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2), out=out)
+        scene.render_pass(st["camera"], pass_params(W, H, 16 * k, 16, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2), out=out)
     torch.cuda.synchronize()
     print("pass ok", scene.last_stats(), flush=True)
 

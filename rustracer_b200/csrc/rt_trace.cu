@@ -296,13 +296,21 @@ RT_D bool nan_ray(float3 o, float3 d, float tmin, float tmax) {
 // active lane.  When at least RT_REFILL lanes of a warp are idle, they pull
 // new rays from the queue together (one atomic per warp), so a warp is not held
 // by its slowest ray (persistent threads with dynamic fetch, Aila & Laine 2009).
+#ifndef RT_REFILL
 #define RT_REFILL 12
+#endif
 #define FULLMASK 0xFFFFFFFFu
 
 // MODE 0: wavefront extend (queue of path ids, rays in PathState, hits to PathState)
 // MODE 1: API (rays n×8 in memory, hits as int4)
+// 6 resident blocks of 128 threads per SM: caps the kernels at 80 registers
+// (measured faster than 5 blocks at 96 registers and than 8 blocks at 64)
+#ifndef RT_TRACE_MINB
+#define RT_TRACE_MINB 6
+#endif
+
 template <int MODE>
-__global__ void __launch_bounds__(RT_TRACE_BLOCK) k_closest(DevScene S, PathState P, const uint32_t* __restrict__ queue,
+__global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevScene S, PathState P, const uint32_t* __restrict__ queue,
                                                             const float* __restrict__ rays, uint32_t n_api,
                                                             const uint32_t* count, uint32_t* next,
                                                             int4* __restrict__ out, int* err) {
@@ -372,7 +380,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_closest(DevScene S, PathStat
 // MODE 0: wavefront shadow rays (an occluded ray cancels its parked contribution)
 // MODE 1: API any-hit (occluded flags)
 template <int MODE>
-__global__ void __launch_bounds__(RT_TRACE_BLOCK) k_any(DevScene S, PendTargets T, const float4* __restrict__ sq,
+__global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene S, PendTargets T, const float4* __restrict__ sq,
                                                         const float* __restrict__ rays, uint32_t n_api,
                                                         const uint32_t* count, uint32_t* next,
                                                         uint8_t* __restrict__ out, int* err) {
@@ -434,7 +442,11 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK) k_any(DevScene S, PendTargets 
 
 // ── host launchers ──────────────────────────────────────────────────────────
 namespace rth {
-int trace_grid(int dev_sms) { return dev_sms * RT_TRACE_BLOCKS_PER_SM; }
+#ifndef RT_TRACE_GRID_PER_SM
+#define RT_TRACE_GRID_PER_SM RT_TRACE_MINB
+#endif
+// persistent kernels: one wave of resident blocks
+int trace_grid(int dev_sms) { return dev_sms * RT_TRACE_GRID_PER_SM; }
 
 void launch_trace_closest_api(const DevScene& S, const float* rays, uint32_t n, int4* out, uint32_t* next, int* err,
                               int sms, cudaStream_t st) {
