@@ -24,6 +24,13 @@
 #define RT_LEAF_BIT   0x80000000u
 #define RT_EMPTY_REF  0xFFFFFFFFu
 #define RT_MISS_REF   0xFFFFFFFFu
+// Hit records written by the extend kernel carry the primitive reference with
+// its leaf bit replaced by the material class: bits 31:30 = class code
+// (0 emitter, 1 diffuse, 2 conductor, 3 dielectric), 29:28 = primitive type,
+// 27:0 = typed index.  RT_MISS_REF (type 3) is never a hit.
+#define RT_HIT_TYPE(ref)  (((ref) >> 28) & 3u)
+#define RT_HIT_INDEX(ref) ((ref) & 0x0FFFFFFFu)
+#define RT_HIT_CODE(ref)  ((ref) >> 30)
 #define RT_STACK      96
 
 namespace rtd {
@@ -63,6 +70,7 @@ struct DevScene {
     const float4* sphere;
     const DevLight* lights;
     const DevMaterial* mats;
+    const uint8_t* mat_code;    // class code per material (see RT_HIT_CODE)
     int n_lights, n_mats;
     // spectral tables: CIE x̄ȳz̄ on the 5 nm grid from 380 nm and the per-channel
     // normalisations of spectral_to_rgb / spectral_fire_rgb (spectrum.rs:78-177)

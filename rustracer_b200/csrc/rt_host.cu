@@ -740,6 +740,14 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     }
     if ((rc = upload(s, mats.data(), mats.size(), &s->S.mats))) return bail(rc);
     s->S.n_mats = d->n_mats;
+    std::vector<uint8_t> codes(mats.size(), 1);
+    for (int32_t i = 0; i < d->n_mats; i++) {
+        int t = d->mats[i].type;
+        codes[i] = (t == RT_MAT_DIFFUSE_LIGHT || t == RT_MAT_BLACKBODY_LIGHT) ? 0
+                 : t == RT_MAT_SPECTRAL_METAL ? 2
+                 : (t == RT_MAT_DIELECTRIC || t == RT_MAT_SPECTRAL_DIELECTRIC) ? 3 : 1;
+    }
+    if ((rc = upload(s, codes.data(), codes.size(), &s->S.mat_code))) return bail(rc);
 
     std::call_once(g_elut_once, build_elut);
     if ((rc = upload(s, g_elut, (size_t)64 * 64, &s->S.elut))) return bail(rc);

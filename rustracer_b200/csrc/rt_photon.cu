@@ -166,7 +166,7 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                 uint32_t spec_depth = __float_as_uint(th.w);
                 float t = hv.y;
                 float3 p = o + t * d;
-                uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
+                uint32_t type = RT_HIT_TYPE(ref), idx = RT_HIT_INDEX(ref);
                 float3 outward;
                 int mat;
                 if (type == RT_PRIM_TRI) {

@@ -120,15 +120,14 @@ RT_D float3 env_unrot(const DevScene& S, float3 d) {
 RT_D float3 env_rot(const DevScene& S, float3 d) {
     return mk(d.x * S.env_cos_r + d.z * S.env_sin_r, d.y, -d.x * S.env_sin_r + d.z * S.env_cos_r);
 }
-RT_D float rem1(float a) { float r = fmodf(a, 1.0f); return r < 0.0f ? r + 1.0f : r; }
+// rem_euclid(1.0): a − ⌊a⌋ is exact, so this equals the fmod form
+RT_D float rem1(float a) { return a - floorf(a); }
 RT_D void env_uv(const DevScene& S, float3 dir, float* u, float* v) {
     float3 d = env_unrot(S, unit3(dir));
     *u = rem1(0.5f + atan2f(d.x, d.z) / (2.0f * PI_F));
     *v = acosf(clampf_(d.y, -1.0f, 1.0f)) / PI_F;
 }
-RT_D float3 env_lookup(const DevScene& S, float3 dir) {
-    float u, v;
-    env_uv(S, dir, &u, &v);
+RT_D float3 env_lookup_uv(const DevScene& S, float u, float v) {
     float x = u * (float)S.env_w - 0.5f, y = v * (float)S.env_h - 0.5f;
     float fx0 = floorf(x), fy0 = floorf(y);
     int x0 = (int)fx0, y0 = (int)fy0;
@@ -146,14 +145,22 @@ RT_D float env_pdf_at(const DevScene& S, uint32_t k) {
     return __ldg(S.env + k).w * (float)((uint32_t)S.env_w * (uint32_t)S.env_h) * S.env_inv_total
            / (2.0f * PI_F * PI_F);
 }
-RT_D float env_dir_pdf(const DevScene& S, float3 dir) {
-    if (!S.has_env) return 0.0f;
+RT_D float3 env_lookup(const DevScene& S, float3 dir) {
     float u, v;
     env_uv(S, dir, &u, &v);
+    return env_lookup_uv(S, u, v);
+}
+RT_D float env_pdf_uv(const DevScene& S, float u, float v) {
     int i = min((int)(u * (float)S.env_w), S.env_w - 1);
     int j = min((int)(v * (float)S.env_h), S.env_h - 1);
     i = max(i, 0); j = max(j, 0);
     return env_pdf_at(S, (uint32_t)j * S.env_w + i);
+}
+RT_D float env_dir_pdf(const DevScene& S, float3 dir) {
+    if (!S.has_env) return 0.0f;
+    float u, v;
+    env_uv(S, dir, &u, &v);
+    return env_pdf_uv(S, u, v);
 }
 // Alias-table draw with the same discrete texel distribution (lum·sinθ / Σ)
 // as the reference's two-level CDF inversion, then the same sub-texel jitter.
@@ -262,7 +269,10 @@ RT_D float3 tint_rgb(const DevScene& S, int tint, float lam) {
     return tint == TINT_CMF ? spectral_to_rgb(S, lam) : spectral_fire_rgb(S, lam);
 }
 RT_D float lam_k(const DevScene& S, float lam0, int k, int H) {
-    return S.lam_lo + fmodf(lam0 - S.lam_lo + (float)k * (S.lam_range / (float)H), S.lam_range);
+    // the offset lies in [0, 2·range): one conditional subtraction (exact by
+    // Sterbenz's lemma) equals fmod
+    float x = lam0 - S.lam_lo + (float)k * (S.lam_range / (float)H);
+    return S.lam_lo + (x >= S.lam_range ? x - S.lam_range : x);
 }
 RT_D float3 spec_factor(const DevScene& S, int tint, float4 w, float lam0, int H) {
     float ws[4] = {w.x, w.y, w.z, w.w};
@@ -420,19 +430,7 @@ __global__ void k_zero_converged(const uint8_t* __restrict__ conv, uint32_t npix
 // Warp-aggregated appends (ballot + popc + one atomic per class per warp) into
 // one queue per class, so each shading kernel below runs one material's code:
 // no divergence between materials and a much smaller instruction footprint.
-RT_D int material_class(const DevScene& S, uint32_t ref) {
-    if (ref == RT_MISS_REF) return CLS_MISS;
-    uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
-    int mat;
-    if (type == RT_PRIM_TRI) mat = __float_as_int(__ldg(S.tri + (size_t)idx * 3 + 2).z);
-    else if (type == RT_PRIM_QUAD) mat = __float_as_int(__ldg(S.quad + (size_t)idx * 5 + 4).y);
-    else mat = __float_as_int(__ldg(S.sphere + (size_t)idx * 2 + 1).y);
-    int t = S.mats[mat].type;
-    if (t == RT_MAT_DIFFUSE_LIGHT || t == RT_MAT_BLACKBODY_LIGHT) return CLS_EMIT;
-    if (t == RT_MAT_SPECTRAL_METAL) return CLS_METAL;
-    if (t == RT_MAT_DIELECTRIC || t == RT_MAT_SPECTRAL_DIELECTRIC) return CLS_DIELEC;
-    return CLS_DIFFUSE;
-}
+RT_D int material_class(uint32_t ref) { return ref == RT_MISS_REF ? CLS_MISS : CLS_EMIT + (int)RT_HIT_CODE(ref); }
 
 __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_classify(DevScene S, const float4* __restrict__ hit,
                                                              const uint32_t* cin, uint32_t* next, ClassQueues Q,
@@ -448,7 +446,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_classify(DevScene S, const f
         uint32_t pid = 0;
         if (qi < n) {
             pid = qi;
-            cls = material_class(S, __float_as_uint(hit[pid].x));
+            cls = material_class(__float_as_uint(__ldg(reinterpret_cast<const float*>(hit + pid))));
         }
 #pragma unroll
         for (int c = 0; c < CLS_N; c++) {
@@ -466,7 +464,7 @@ RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
     uint32_t ref = __float_as_uint(hv.x);
     r.t = hv.y;
     r.p = o + r.t * d;
-    uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
+    uint32_t type = RT_HIT_TYPE(ref), idx = RT_HIT_INDEX(ref);
     float3 outward;
     if (type == RT_PRIM_TRI) {                                                      // triangle.rs:91-108
         const float4* g = S.tri + (size_t)idx * 3;
@@ -545,13 +543,23 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
             uint32_t b = D_BOUNCE0 + depth * D_PER_BOUNCE;
             float3 Lc = mk(L.x, L.y, L.z);
             if (CLS == CLS_MISS) {                                                  // renderer.rs:381-403
-                float env_pdf = env_dir_pdf(S, d);
+                float env_pdf = 0.0f;
+                float3 bg;
+                if (S.has_env) {
+                    float u, v;
+                    env_uv(S, d, &u, &v);
+                    env_pdf = env_pdf_uv(S, u, v);
+                    bg = (depth == 0 && S.vis_type >= 0) ? bg_type_eval(S.vis_type, S.vis_color, S.vis_top,
+                                                                        S.vis_bottom, d)
+                                                         : env_lookup_uv(S, u, v);
+                } else {
+                    bg = bg_eval(S, d);
+                }
                 float emit_w = env_pdf == 0.0f ? 1.0f : (prev_spec ? 1.0f : prev_mis);
-                float3 bg = (depth == 0 || !S.has_env) ? bg_eval(S, d) : env_lookup(S, d);
                 Lc = Lc + T * (bg * spec_factor(S, tint, w, lam0, H)) * R.bg_scale * emit_w;
             } else if (CLS == CLS_EMIT) {                                           // renderer.rs:415-419
                 float4 hv = A.hit[pid];
-                uint32_t ref = __float_as_uint(hv.x), type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
+                uint32_t ref = __float_as_uint(hv.x), type = RT_HIT_TYPE(ref), idx = RT_HIT_INDEX(ref);
                 int mat = type == RT_PRIM_TRI ? __float_as_int(__ldg(S.tri + (size_t)idx * 3 + 2).z)
                         : type == RT_PRIM_QUAD ? __float_as_int(__ldg(S.quad + (size_t)idx * 5 + 4).y)
                                                : __float_as_int(__ldg(S.sphere + (size_t)idx * 2 + 1).y);

@@ -19,7 +19,7 @@ using namespace rtd;
 
 namespace {
 
-struct Best { float t, b1, b2; uint32_t ref, gid; };
+struct Best { float t, b1, b2; uint32_t ref, gid, mat; };
 
 RT_D uint32_t f2u(float f) { return __float_as_uint(f); }
 
@@ -27,26 +27,31 @@ RT_D uint32_t f2u(float f) { return __float_as_uint(f); }
 RT_D void leaf_closest(const DevScene& S, uint32_t ref, float3 o, float3 d, float tmin, Best& best) {
     uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
     float t, b1, b2;
-    uint32_t gid;
+    uint32_t gid, mat;
     bool h;
     if (type == RT_PRIM_TRI) {
         const float4* g = S.tri + (size_t)idx * 3;
         float4 a = __ldg(g), b = __ldg(g + 1), c = __ldg(g + 2);
         h = tri_test(a, b, c, o, d, tmin, best.t, &t, &b1, &b2);
         gid = f2u(c.y);
+        mat = f2u(c.z);
     } else if (type == RT_PRIM_QUAD) {
         const float4* g = S.quad + (size_t)idx * 5;
         float4 gg[4] = {__ldg(g), __ldg(g + 1), __ldg(g + 2), __ldg(g + 3)};
         h = quad_test(gg, o, d, tmin, best.t, &t, &b1, &b2);
-        gid = h ? f2u(__ldg(g + 4).x) : 0u;
+        float4 gm = h ? __ldg(g + 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+        gid = f2u(gm.x);
+        mat = f2u(gm.y);
     } else {
         const float4* g = S.sphere + (size_t)idx * 2;
         h = sphere_test(__ldg(g), o, d, tmin, best.t, &t);
         b1 = b2 = 0.0f;
-        gid = h ? f2u(__ldg(g + 1).x) : 0u;
+        float4 gm = h ? __ldg(g + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
+        gid = f2u(gm.x);
+        mat = f2u(gm.y);
     }
     if (h && (t < best.t || best.ref == RT_MISS_REF || gid < best.gid)) {
-        best.t = t; best.b1 = b1; best.b2 = b2; best.ref = ref; best.gid = gid;
+        best.t = t; best.b1 = b1; best.b2 = b2; best.ref = ref; best.gid = gid; best.mat = mat;
     }
 }
 
@@ -323,7 +328,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
     float3 o = mk(0.f, 0.f, 0.f), d = o;
     RayC R = make_rayc(o, mk(1.f, 1.f, 1.f), 0.0f);
     float tmin = 0.0f;
-    Best best{0.0f, 0.0f, 0.0f, RT_MISS_REF, 0xFFFFFFFFu};
+    Best best{0.0f, 0.0f, 0.0f, RT_MISS_REF, 0xFFFFFFFFu, 0u};
     while (true) {
         uint32_t idle = __ballot_sync(FULLMASK, !active);
         if (!exhausted && __popc(idle) >= RT_REFILL) {
@@ -347,7 +352,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
                         tmin = r[6]; tmax = r[7];
                     }
                     R = make_rayc(o, d, tmin);
-                    best = Best{tmax, 0.0f, 0.0f, RT_MISS_REF, 0xFFFFFFFFu};
+                    best = Best{tmax, 0.0f, 0.0f, RT_MISS_REF, 0xFFFFFFFFu, 0u};
                     node = 0; sp = 0;
                     active = !rtk::nan_ray(o, d, tmin, tmax);
                     if (!active) {
@@ -366,7 +371,9 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
                 active = false;
                 bool hit = best.ref != RT_MISS_REF;
                 if (MODE == 0) {
-                    P.hit[pid] = make_float4(__uint_as_float(best.ref), best.t, best.b1, best.b2);
+                    uint32_t href = hit ? (best.ref & 0x3FFFFFFFu) | ((uint32_t)__ldg(S.mat_code + best.mat) << 30)
+                                        : RT_MISS_REF;
+                    P.hit[pid] = make_float4(__uint_as_float(href), best.t, best.b1, best.b2);
                 } else {
                     out[item] = make_int4(hit ? (int)best.gid : -1, __float_as_int(hit ? best.t : 0.0f),
                                           __float_as_int(hit ? best.b1 : 0.0f), __float_as_int(hit ? best.b2 : 0.0f));
