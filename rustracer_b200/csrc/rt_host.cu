@@ -867,7 +867,7 @@ static int check_err(RtScene* s) {
 extern "C" int32_t rt_trace_closest(RtScene* s, const float* rays, int64_t n, RtHit* hits, int32_t mem) {
     if (!s || (n > 0 && (!rays || !hits))) return RT_ERR_INVALID;
     if (n <= 0) return RT_OK;
-    if (n > 0xFFFFFFF0ll) return fail(s, RT_ERR_CAPACITY, "too many rays");
+    if (n > (1ll << 31)) return fail(s, RT_ERR_CAPACITY, "more than 2^31 rays per call");
     CK(cudaSetDevice(s->device));
     if (s->empty) {
         if (mem == RT_MEM_DEVICE) { CK(cudaMemsetAsync(hits, 0xFF, n * sizeof(RtHit), s->stream)); return RT_OK; }
@@ -900,6 +900,7 @@ extern "C" int32_t rt_trace_closest(RtScene* s, const float* rays, int64_t n, Rt
 extern "C" int32_t rt_trace_any(RtScene* s, const float* rays, int64_t n, uint8_t* occ, int32_t mem) {
     if (!s || (n > 0 && (!rays || !occ))) return RT_ERR_INVALID;
     if (n <= 0) return RT_OK;
+    if (n > (1ll << 31)) return fail(s, RT_ERR_CAPACITY, "more than 2^31 rays per call");
     CK(cudaSetDevice(s->device));
     if (s->empty) {
         if (mem == RT_MEM_DEVICE) { CK(cudaMemsetAsync(occ, 0, n, s->stream)); return RT_OK; }

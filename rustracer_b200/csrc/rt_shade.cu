@@ -313,6 +313,48 @@ RT_D uint32_t warp_append(uint32_t* counter, bool pred) {
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
+// Block-wide reservation in NC append-only queues: each thread asks for
+// cnt[c] entries of queue c and gets its first position in off[c].  One global
+// atomic per queue per call (warp scans, then a scan over the warps in shared
+// memory), instead of one per warp.  Every thread of the block must call it.
+template <int NC, int NW>
+struct BlockQ {
+    uint32_t wsum[NC][NW];
+    uint32_t base[NC];
+};
+template <int NC, int NW>
+RT_D void block_reserve(BlockQ<NC, NW>& sh, uint32_t* const (&ctr)[NC], const uint32_t (&cnt)[NC],
+                        uint32_t (&off)[NC]) {
+    uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t incl[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+        uint32_t v = cnt[c];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t t = __shfl_up_sync(0xFFFFFFFFu, v, d);
+            if (lane >= (uint32_t)d) v += t;
+        }
+        incl[c] = v;
+        if (lane == 31) sh.wsum[c][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NC) {
+        int c = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < NW; w++) { uint32_t t = sh.wsum[c][w]; sh.wsum[c][w] = run; run += t; }
+        uint32_t* q = ctr[0];
+#pragma unroll
+        for (int k = 1; k < NC; k++) if (c == k) q = ctr[k];
+        sh.base[c] = run ? atomicAdd(q, run) : 0u;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < NC; c++) off[c] = sh.base[c] + sh.wsum[c][warp] + incl[c] - cnt[c];
+    __syncthreads();
+}
+
 }  // namespace
 
 // ── generate ────────────────────────────────────────────────────────────────
@@ -373,8 +415,12 @@ __global__ void k_generate(DevScene S, PathState A, RenderLaunch R, uint32_t poo
 // An ended path folds its last parked contributions (caustic, area-light NEE,
 // env NEE — the order of renderer.rs:461-540) and writes its sample; for each
 // ended path the next ungenerated sample, if any, is appended to the next set.
-__global__ void k_retire(DevScene S, PathState B, PathState Rt, RenderLaunch R, uint32_t* ctr, uint32_t* hdr,
-                         uint32_t* clear_block, uint32_t* cout) {
+#define RETIRE_BLOCK 256
+__global__ void __launch_bounds__(RETIRE_BLOCK) k_retire(DevScene S, PathState B, PathState Rt, RenderLaunch R,
+                                                         uint32_t* ctr, uint32_t* hdr, uint32_t* clear_block,
+                                                         uint32_t* cout) {
+    __shared__ BlockQ<1, RETIRE_BLOCK / 32> shq;
+    __shared__ unsigned long long gbase;
     uint32_t n = ctr[CTR_RETIRE_COUNT];
     if (blockIdx.x == 0) {
         if (threadIdx.x == 0) {
@@ -383,9 +429,9 @@ __global__ void k_retire(DevScene S, PathState B, PathState Rt, RenderLaunch R, 
         }
         if (threadIdx.x < RT_CTR_STRIDE) clear_block[threadIdx.x] = 0u;
     }
-    uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        uint32_t j = base + threadIdx.x;
+    uint32_t* qctr[1] = {cout};
+    for (uint32_t t0 = blockIdx.x * RETIRE_BLOCK; t0 < n; t0 += gridDim.x * RETIRE_BLOCK) {
+        uint32_t j = t0 + threadIdx.x;
         bool act = j < n;
         if (act) {
             float4 L = Rt.L[j], a = Rt.pend0[j], b = Rt.pend1[j];
@@ -396,15 +442,16 @@ __global__ void k_retire(DevScene S, PathState B, PathState Rt, RenderLaunch R, 
             float* out = R.scratch + ((size_t)meta.y * R.npix + meta.x) * 3;
             out[0] = L.x; out[1] = L.y; out[2] = L.z;
         }
-        // warp-aggregated claim of new samples
-        uint32_t m = __ballot_sync(0xFFFFFFFFu, act);
-        unsigned long long g0 = 0;
-        if (m && lane == 0) g0 = atomicAdd(R.gen_next, (unsigned long long)__popc(m));
-        g0 = __shfl_sync(0xFFFFFFFFu, g0, 0);
-        uint64_t g = g0 + __popc(m & ((1u << lane) - 1u));
+        // one claim of new samples per block: the tile's ended paths are
+        // t0 .. t0 + min(n − t0, RETIRE_BLOCK) − 1, in thread order
+        uint32_t tile_n = min(n - t0, (uint32_t)RETIRE_BLOCK);
+        if (threadIdx.x == 0) gbase = atomicAdd(R.gen_next, (unsigned long long)tile_n);
+        __syncthreads();
+        uint64_t g = gbase + threadIdx.x;
         bool fresh = act && g < R.total;
-        uint32_t slot = warp_append(cout, fresh);
-        if (fresh) init_path(S, B, R, slot, g);
+        uint32_t cnt[1] = {fresh}, off[1];
+        block_reserve(shq, qctr, cnt, off);
+        if (fresh) init_path(S, B, R, off[0], g);
     }
 }
 
@@ -432,26 +479,37 @@ __global__ void k_zero_converged(const uint8_t* __restrict__ conv, uint32_t npix
 // no divergence between materials and a much smaller instruction footprint.
 RT_D int material_class(uint32_t ref) { return ref == RT_MISS_REF ? CLS_MISS : CLS_EMIT + (int)RT_HIT_CODE(ref); }
 
-__global__ void __launch_bounds__(RT_SHADE_BLOCK) k_classify(DevScene S, const float4* __restrict__ hit,
-                                                             const uint32_t* cin, uint32_t* next, ClassQueues Q,
-                                                             uint32_t* cls_count) {
-    uint32_t n = *cin;
-    while (true) {
-        uint32_t base;
-        if ((threadIdx.x & 31u) == 0) base = atomicAdd(next, 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= n) break;
-        uint32_t qi = base + (threadIdx.x & 31u);
-        int cls = -1;
-        uint32_t pid = 0;
-        if (qi < n) {
-            pid = qi;
-            cls = material_class(__float_as_uint(__ldg(reinterpret_cast<const float*>(hit + pid))));
-        }
+#define CLS_BLOCK 256
+#define CLS_ITEMS 4
+__global__ void __launch_bounds__(CLS_BLOCK) k_classify(const float4* __restrict__ hit, const uint32_t* cin,
+                                                        ClassQueues Q, uint32_t* cls_count) {
+    __shared__ BlockQ<CLS_N, CLS_BLOCK / 32> shq;
+    uint32_t* qctr[CLS_N];
 #pragma unroll
-        for (int c = 0; c < CLS_N; c++) {
-            uint32_t slot = warp_append(cls_count + c, cls == c);
-            if (cls == c) Q.q[c][slot] = pid;
+    for (int c = 0; c < CLS_N; c++) qctr[c] = cls_count + c;
+    uint32_t n = *cin;
+    const uint32_t tile = CLS_BLOCK * CLS_ITEMS;
+    for (uint32_t t0 = blockIdx.x * tile; t0 < n; t0 += gridDim.x * tile) {
+        // CLS_ITEMS consecutive paths per thread, so each class queue lists
+        // neighbouring paths next to each other
+        uint32_t i0 = t0 + threadIdx.x * CLS_ITEMS;
+        int cls[CLS_ITEMS];
+        uint32_t cnt[CLS_N], off[CLS_N];
+#pragma unroll
+        for (int c = 0; c < CLS_N; c++) cnt[c] = 0;
+#pragma unroll
+        for (int k = 0; k < CLS_ITEMS; k++) {
+            uint32_t i = i0 + k;
+            cls[k] = i < n ? material_class(__float_as_uint(__ldg(reinterpret_cast<const float*>(hit + i)))) : -1;
+#pragma unroll
+            for (int c = 0; c < CLS_N; c++) cnt[c] += cls[k] == c;
+        }
+        block_reserve(shq, qctr, cnt, off);
+#pragma unroll
+        for (int k = 0; k < CLS_ITEMS; k++) {
+#pragma unroll
+            for (int c = 0; c < CLS_N; c++)
+                if (cls[k] == c) Q.q[c][off[c]++] = i0 + k;
         }
     }
 }
@@ -499,17 +557,25 @@ RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
 template <int CLS>
 __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState A, PathState B, PathState Rt,
                                                           RenderLaunch R, const uint32_t* __restrict__ qin,
-                                                          const uint32_t* cin, uint32_t* next, uint32_t* cout,
+                                                          const uint32_t* cin, uint32_t* cout,
                                                           float4* __restrict__ sq, uint32_t* ctr) {
+    // queues appended to: [next set, retire records, gather requests, shadow rays]
+    constexpr int NQ = CLS == CLS_DIFFUSE ? 4 : (CLS == CLS_MISS || CLS == CLS_EMIT) ? 1 : 2;
+    __shared__ BlockQ<NQ, RT_SHADE_BLOCK / 32> shq;
+    uint32_t* qctr[NQ];
+    if constexpr (NQ == 1) {
+        qctr[0] = ctr + CTR_RETIRE_COUNT;
+    } else {
+        qctr[0] = cout;
+        qctr[1] = ctr + CTR_RETIRE_COUNT;
+        if constexpr (NQ == 4) { qctr[2] = ctr + CTR_GATHER_COUNT; qctr[3] = ctr + CTR_SHADOW_COUNT; }
+    }
     uint32_t n = *cin;
     int H = (int)R.hero;
     bool have_lights = S.n_lights > 0;
-    while (true) {
-        uint32_t base;
-        if ((threadIdx.x & 31u) == 0) base = atomicAdd(next, 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= n) break;
-        uint32_t qi = base + (threadIdx.x & 31u);
+    // static tiles of one path per thread (the cost per path of one class is even)
+    for (uint32_t t0 = blockIdx.x * RT_SHADE_BLOCK; t0 < n; t0 += gridDim.x * RT_SHADE_BLOCK) {
+        uint32_t qi = t0 + threadIdx.x;
         bool active = qi < n;
         uint32_t pid = active ? qin[qi] : 0u;
         bool cont = false, sh0 = false, sh1 = false, gath = false;
@@ -747,12 +813,23 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                 w_out = w;
             }
         }
-        // warp-aggregated compaction: paths that go on into B, ended paths into
+        // block-aggregated compaction: paths that go on into B, ended paths into
         // the retire records; parked contributions and shadow rays follow them
-        uint32_t slot = 0;
-        if (CLS != CLS_MISS && CLS != CLS_EMIT) slot = warp_append(cout, cont);
         bool ended = active && !cont;
-        uint32_t rs = warp_append(ctr + CTR_RETIRE_COUNT, ended);
+        uint32_t cnt[NQ], off[NQ];
+        uint32_t slot = 0, rs = 0;
+        if constexpr (NQ == 1) {
+            cnt[0] = ended;
+            block_reserve(shq, qctr, cnt, off);
+            rs = off[0];
+        } else {
+            cnt[0] = cont;
+            cnt[1] = ended;
+            if constexpr (NQ == 4) { cnt[2] = gath; cnt[3] = (uint32_t)sh0 + (uint32_t)sh1; }
+            block_reserve(shq, qctr, cnt, off);
+            slot = off[0];
+            rs = off[1];
+        }
         if (cont) {
             B.ray_o[slot] = o_out; B.ray_d[slot] = d_out; B.thr[slot] = thr_out; B.wts[slot] = w_out;
             B.meta[slot] = meta; B.L[slot] = Lout; B.pend0[slot] = np0; B.pend1[slot] = np1;
@@ -761,16 +838,16 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
             Rt.meta[rs] = meta; Rt.L[rs] = Lout; Rt.pend0[rs] = np0; Rt.pend1[rs] = np1;
             if (R.photons) Rt.pendC[rs] = npc;
         }
-        uint32_t tag = cont ? slot << 2 : (rs << 2) | PT_RETIRED;
-        if (CLS == CLS_DIFFUSE) {
-            if (R.photons) {
-                uint32_t g = warp_append(ctr + CTR_GATHER_COUNT, gath);
-                if (gath) { ga.w = __uint_as_float(tag); A.gq[(size_t)g * 2] = ga; A.gq[(size_t)g * 2 + 1] = gb; }
+        if constexpr (NQ == 4) {
+            uint32_t tag = cont ? slot << 2 : (rs << 2) | PT_RETIRED;
+            if (gath) {
+                uint32_t g = off[2];
+                ga.w = __uint_as_float(tag);
+                A.gq[(size_t)g * 2] = ga; A.gq[(size_t)g * 2 + 1] = gb;
             }
-            uint32_t s0 = warp_append(ctr + CTR_SHADOW_COUNT, sh0);
-            if (sh0) { sh0b.w = __uint_as_float(tag); sq[(size_t)s0 * 2] = sh0a; sq[(size_t)s0 * 2 + 1] = sh0b; }
-            uint32_t s1 = warp_append(ctr + CTR_SHADOW_COUNT, sh1);
-            if (sh1) { sh1b.w = __uint_as_float(tag | 1u); sq[(size_t)s1 * 2] = sh1a; sq[(size_t)s1 * 2 + 1] = sh1b; }
+            uint32_t s0 = off[3];
+            if (sh0) { sh0b.w = __uint_as_float(tag); sq[(size_t)s0 * 2] = sh0a; sq[(size_t)s0 * 2 + 1] = sh0b; s0++; }
+            if (sh1) { sh1b.w = __uint_as_float(tag | 1u); sq[(size_t)s0 * 2] = sh1a; sq[(size_t)s0 * 2 + 1] = sh1b; }
         }
     }
 }
@@ -813,11 +890,9 @@ void launch_shade(const DevScene& S, const PathState& A, const PathState& B, con
                   uint32_t* ctr, const ClassQueues& Q, uint32_t* cout, float4* sq, int sms, cudaStream_t st) {
     // ctr: this iteration's counter block (see rt_internal.h for the slots)
     int grid = sms * RT_SHADE_BLOCKS_PER_SM;
-    k_classify<<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A.hit, ctr + CTR_COUNT, ctr + CTR_CLASSIFY_NEXT, Q,
-                                                ctr + CTR_CLS_COUNT);
+    k_classify<<<sms * 4, CLS_BLOCK, 0, st>>>(A.hit, ctr + CTR_COUNT, Q, ctr + CTR_CLS_COUNT);
 #define RT_SHADE_CLASS(C)                                                                                   \
-    k_shade<C><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C,            \
-                                                ctr + CTR_CLS_NEXT + C, cout, sq, ctr)
+    k_shade<C><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr)
     RT_SHADE_CLASS(CLS_MISS);
     RT_SHADE_CLASS(CLS_EMIT);
     RT_SHADE_CLASS(CLS_DIFFUSE);
@@ -827,7 +902,7 @@ void launch_shade(const DevScene& S, const PathState& A, const PathState& B, con
 }
 void launch_retire(const DevScene& S, const PathState& B, const PathState& Rt, const RenderLaunch& R, uint32_t* ctr,
                    uint32_t* hdr, uint32_t* clear_block, uint32_t* cout, int sms, cudaStream_t st) {
-    k_retire<<<sms * 8, 256, 0, st>>>(S, B, Rt, R, ctr, hdr, clear_block, cout);
+    k_retire<<<sms * 8, RETIRE_BLOCK, 0, st>>>(S, B, Rt, R, ctr, hdr, clear_block, cout);
 }
 void launch_active_list(const uint8_t* conv, uint32_t npix, uint32_t* list, uint32_t* count, cudaStream_t st) {
     int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>((npix + 255) / 256, 148u * 16u));
