@@ -559,8 +559,14 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         for (int64_t k = 0; k < s->n_nodes; k++) {
             const RefNode& r = s->ref_nodes[k];
             float* f = reinterpret_cast<float*>(&gnodes[(size_t)k * 14]);
+            // an empty slot gets an inverted box (+inf, −inf): its slab test fails
+            // by itself on the traversal's fast path
             for (int a = 0; a < 3; a++)
-                for (int c = 0; c < 8; c++) { f[a * 8 + c] = r.mn[a][c]; f[24 + a * 8 + c] = r.mx[a][c]; }
+                for (int c = 0; c < 8; c++) {
+                    bool empty = r.ch[c] == INT32_MIN;
+                    f[a * 8 + c] = empty ? INFINITY : r.mn[a][c];
+                    f[24 + a * 8 + c] = empty ? -INFINITY : r.mx[a][c];
+                }
             uint32_t* ch = reinterpret_cast<uint32_t*>(f + 48);
             for (int c = 0; c < 8; c++) {
                 int32_t v = r.ch[c];
@@ -1141,7 +1147,7 @@ static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p,
         }
         uint32_t* dcount = s->d_active + npix;
         CK(cudaMemsetAsync(dcount, 0, 4, s->stream));
-        rth::launch_active_list(dconv, npix, s->d_active, dcount, s->stream);
+        rth::launch_active_list(dconv, p->width, p->height, s->d_active, dcount, s->stream);
         rth::launch_zero_converged(dconv, npix, nsamp, dscratch, s->stream);
         CK(cudaMemcpyAsync(&nactive, dcount, 4, cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));

@@ -132,7 +132,8 @@ void launch_shade(const rtd::DevScene& S, const PathState& A, const PathState& B
 void launch_retire(const rtd::DevScene& S, const PathState& B, const PathState& Rt, const RenderLaunch& R,
                    uint32_t* ctr, uint32_t* hdr, uint32_t* clear_block, uint32_t* cout, int sms, cudaStream_t st);
 // active-pixel list of a converged mask, and zero output for converged pixels
-void launch_active_list(const uint8_t* conv, uint32_t npix, uint32_t* list, uint32_t* count, cudaStream_t st);
+void launch_active_list(const uint8_t* conv, uint32_t width, uint32_t height, uint32_t* list, uint32_t* count,
+                        cudaStream_t st);
 void launch_zero_converged(const uint8_t* conv, uint32_t npix, uint32_t nsamp, float* scratch, cudaStream_t st);
 
 cudaError_t photon_build(const rtd::DevScene& S, PhotonMapDev& map, const PathState& P, uint32_t* qa, uint32_t* qb,

@@ -360,9 +360,31 @@ RT_D void block_reserve(BlockQ<NC, NW>& sh, uint32_t* const (&ctr)[NC], const ui
 // ── generate ────────────────────────────────────────────────────────────────
 // Camera ray of sample g of the group into path slot `pid` (Camera::get_ray,
 // camera.rs:93-127, with the stratified jitter of renderer.rs:262-283).
+#ifndef RT_TILE_SWIZZLE
+#define RT_TILE_SWIZZLE 1
+#endif
+// Generation order of the pixels: 8×4 tiles, tiles row by row, so a warp's 32
+// camera rays cover a compact tile (coherent traversal) rather than a 32-pixel
+// strip.  A bijection of 0 .. W·H−1 for any W, H (edge tiles are smaller).
+RT_D uint32_t tile_order_pixel(uint32_t j, uint32_t W, uint32_t H) {
+#if RT_TILE_SWIZZLE
+    uint32_t band = j / (W * 4u);
+    uint32_t hb = min(4u, H - band * 4u);
+    uint32_t idx = j - band * W * 4u;
+    uint32_t chunk = idx / (8u * hb);
+    uint32_t wc = min(8u, W - chunk * 8u);
+    uint32_t rem = idx - chunk * 8u * hb;
+    uint32_t row = rem / wc, col = rem - row * wc;
+    return (band * 4u + row) * W + chunk * 8u + col;
+#else
+    (void)W; (void)H;
+    return j;
+#endif
+}
+
 RT_D void init_path(const DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t pid, uint64_t g) {
     uint32_t k = (uint32_t)(g / R.nactive), j = (uint32_t)(g - (uint64_t)k * R.nactive);
-    uint32_t i = R.active ? __ldg(R.active + j) : j;
+    uint32_t i = R.active ? __ldg(R.active + j) : tile_order_pixel(j, R.width, R.height);
     uint32_t row = i / R.width, col = i - row * R.width;
     uint32_t sample = R.sample_idx + k;
     P.L[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -456,10 +478,13 @@ __global__ void __launch_bounds__(RETIRE_BLOCK) k_retire(DevScene S, PathState B
 }
 
 // ── converged pixels ─────────────────────────────────────────────────────────
-__global__ void k_active_list(const uint8_t* __restrict__ conv, uint32_t npix, uint32_t* list, uint32_t* count) {
+__global__ void k_active_list(const uint8_t* __restrict__ conv, uint32_t W, uint32_t H, uint32_t* list,
+                              uint32_t* count) {
+    uint32_t npix = W * H;
     for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < npix; b0 += gridDim.x * blockDim.x) {
-        uint32_t i = b0 + threadIdx.x;
-        bool a = i < npix && !conv[i];
+        uint32_t j = b0 + threadIdx.x;
+        uint32_t i = j < npix ? tile_order_pixel(j, W, H) : 0u;
+        bool a = j < npix && !conv[i];
         uint32_t slot = warp_append(count, a);
         if (a) list[slot] = i;
     }
@@ -904,9 +929,11 @@ void launch_retire(const DevScene& S, const PathState& B, const PathState& Rt, c
                    uint32_t* hdr, uint32_t* clear_block, uint32_t* cout, int sms, cudaStream_t st) {
     k_retire<<<sms * 8, RETIRE_BLOCK, 0, st>>>(S, B, Rt, R, ctr, hdr, clear_block, cout);
 }
-void launch_active_list(const uint8_t* conv, uint32_t npix, uint32_t* list, uint32_t* count, cudaStream_t st) {
+void launch_active_list(const uint8_t* conv, uint32_t width, uint32_t height, uint32_t* list, uint32_t* count,
+                        cudaStream_t st) {
+    uint32_t npix = width * height;
     int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>((npix + 255) / 256, 148u * 16u));
-    k_active_list<<<grid, 256, 0, st>>>(conv, npix, list, count);
+    k_active_list<<<grid, 256, 0, st>>>(conv, width, height, list, count);
 }
 void launch_zero_converged(const uint8_t* conv, uint32_t npix, uint32_t nsamp, float* scratch, cudaStream_t st) {
     k_zero_converged<<<148 * 16, 256, 0, st>>>(conv, npix, nsamp, scratch);

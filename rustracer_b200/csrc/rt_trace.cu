@@ -69,6 +69,32 @@ RT_D bool leaf_any(const DevScene& S, uint32_t ref, float3 o, float3 d, float tm
     return sphere_test(__ldg(S.sphere + (size_t)idx * 2), o, d, tmin, tmax, &t);
 }
 
+#ifndef RT_MNMX3
+#define RT_MNMX3 1
+#endif
+#ifndef RT_EMPTY_INVERTED
+#define RT_EMPTY_INVERTED 1
+#endif
+// three-input min / max (sm_100)
+RT_D float fmax3f(float a, float b, float c) {
+#if RT_MNMX3
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+#else
+    return fmaxf(fmaxf(a, b), c);
+#endif
+}
+RT_D float fmin3f(float a, float b, float c) {
+#if RT_MNMX3
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+#else
+    return fminf(fminf(a, b), c);
+#endif
+}
+
 #define CAS(a, b) { uint32_t lo_ = min(k[a], k[b]); uint32_t hi_ = max(k[a], k[b]); k[a] = lo_; k[b] = hi_; }
 
 // Per-ray slab constants.  Fast path (every direction component non-zero and
@@ -127,10 +153,14 @@ RT_D uint32_t node_test(const DevScene& S, uint32_t ni, const RayC& R, float tmi
             float nx = (f[0 + c] - R.o.x) * R.inv.x, fx = (f[24 + c] - R.o.x) * R.invf.x;
             float ny = (f[8 + c] - R.o.y) * R.inv.y, fy = (f[32 + c] - R.o.y) * R.invf.y;
             float nz = (f[16 + c] - R.o.z) * R.inv.z, fz = (f[40 + c] - R.o.z) * R.invf.z;
-            float t0 = fmaxf(fmaxf(fmaxf(tmin, nx), ny), nz);
-            float t1 = fminf(fminf(fminf(tmax, fx), fy), fz);
+            float t0 = fmax3f(fmaxf(tmin, nx), ny, nz);
+            float t1 = fmin3f(fminf(tmax, fx), fy, fz);
             tn[c] = t0;
+#if RT_EMPTY_INVERTED
+            if (t0 <= t1) mask |= 1u << c;     // empty slots hold inverted boxes
+#else
             if (t0 <= t1 && ch[c] != RT_EMPTY_REF) mask |= 1u << c;
+#endif
         }
         return mask;
     }
