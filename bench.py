@@ -294,6 +294,7 @@ def roofline(scene, sb, cam):
     p = pass_params(W, H, 6000, SPP, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2)
     scene.render_accumulate(cam, p)
     kt = scene.kernel_times()
+    ext_rays = scene.last_stats()["ext_rays"]
     scene.set_profiling(False)
     o = O.OracleScene(sb)
     rng = np.random.default_rng(0)
@@ -311,12 +312,14 @@ def roofline(scene, sb, cam):
     ext_ms, ext_launches = kt["extend"]
     # total algorithmic bytes of all extend launches of the 64-spp render ÷ their total device time
     achieved = total_bytes_pass * SPP / (ext_ms / 1000.0) / 1e9 if ext_ms > 0 else None
+    # DRAM traffic: ncu's bytes per extension ray on this kernel and scene (profiles/)
+    # times this render's extension rays per launch
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "extend_icosphere_traffic.txt")
     if os.path.exists(tfile):
         for ln in open(tfile):
-            if ln.startswith("traffic_bytes_per_launch:"):
-                traffic = float(ln.split(":")[1])
+            if ln.startswith("traffic_bytes_per_ray:"):
+                traffic = float(ln.split(":")[1]) * ext_rays / max(1, ext_launches)
     return {"kernel": "k_extend (8-wide BVH closest hit)", "bound": "hbm", "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
             "traffic": traffic, "algorithmic_bytes_per_launch": total_bytes_pass * SPP / max(1, ext_launches),
