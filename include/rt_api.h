@@ -110,6 +110,33 @@ typedef struct RtBackground {
 #define RT_PRIM_QUAD   1
 #define RT_PRIM_SPHERE 2
 
+/* ── participating media (volume.rs:39-263, scene_file.rs:297-336, 962-983) ─
+ * A medium is not a BVH primitive: its scatter distance depends only on the
+ * ray (the reference seeds the medium's random stream from the ray's bits,
+ * volume.rs:114-120), so each ray's medium candidates are computed next to the
+ * BVH traversal and the nearer event wins (medium ids follow the primitives'
+ * canonical ids; an exact tie goes to the surface). */
+#define RT_MEDIUM_CONSTANT 0   /* ConstantMedium: exponential free flight, Beer–Lambert shadows */
+#define RT_MEDIUM_NOISE    1   /* NoiseMedium: delta tracking against density·max, 16-point shadow quadrature */
+#define RT_BOUND_SPHERE    0
+#define RT_BOUND_BOX       1   /* axis-aligned box of 6 quads (quad.rs:201-215) */
+
+typedef struct RtMedium {
+    int32_t type;               /* RT_MEDIUM_* */
+    int32_t boundary;           /* RT_BOUND_* */
+    float   center[3], radius;  /* sphere boundary */
+    float   p_min[3], p_max[3]; /* box boundary */
+    float   density;            /* σ (constant) or density scale = majorant (noise) */
+    float   color[3];           /* single-scattering albedo of the HG phase function */
+    float   g;                  /* Henyey–Greenstein asymmetry */
+    float   noise_scale;        /* noise: turbulence frequency */
+    float   threshold;          /* noise: density = max(turb(7)·0.5 − threshold, 0)·density */
+    /* noise: the Perlin tables of this medium (perlin.rs:4-33): 256 unit
+     * vectors and three permutations of 0..255 */
+    float   perlin_vec[256 * 3];
+    int32_t perlin_perm[3 * 256];
+} RtMedium;
+
 typedef struct RtSceneDesc {
     int64_t        n_tris;
     const float*   tri_v;         /* n_tris × 9  : v0, v1, v2 */
@@ -132,6 +159,9 @@ typedef struct RtSceneDesc {
     /* spectral sampling: 0 = reference range 380–700 nm (65-entry CIE table),
      * 1 = 380–780 nm (table extended past 700 nm) */
     int32_t        spectral_range;
+    /* participating media (may be 0 / NULL) */
+    int32_t        n_media;
+    const RtMedium* media;
 } RtSceneDesc;
 
 /* ── camera (src/camera.rs:24-59) ────────────────────────────────────────── */
@@ -191,10 +221,17 @@ int32_t rt_scene_bvh_export(const RtScene* scene, float* nodes_224B, int64_t* n_
 
 /* Closest hit for n rays.  rays: n × 8 floats (origin xyz, dir xyz, t_min, t_max).
  * Replaces BvhTree::hit_index (bvh.rs:229-288).  Ties on t go to the smaller
- * canonical prim id. */
+ * canonical prim id.  With media, a medium scatter event nearer than the
+ * surface hit is returned as prim = n_prims + medium index (b1 = b2 = 0); the
+ * ray's wavelength, which keys the medium's random stream, is 550 nm. */
 int32_t rt_trace_closest(RtScene* scene, const float* rays, int64_t n, RtHit* hits, int32_t mem);
-/* Any hit for n rays (bvh.rs:487-530); occluded[i] = 1 when a hit exists. */
+/* Any hit for n rays (bvh.rs:487-530); occluded[i] = 1 when an opaque hit
+ * exists (media never occlude). */
 int32_t rt_trace_any(RtScene* scene, const float* rays, int64_t n, uint8_t* occluded, int32_t mem);
+/* Transmittance for n rays over [t_min, t_max] (bvh.rs:532-575 with
+ * volume.rs:140-146, 239-252): 0 if an opaque primitive is hit, else the
+ * product of the media's transmittances. */
+int32_t rt_trace_transmittance(RtScene* scene, const float* rays, int64_t n, float* tr, int32_t mem);
 
 /* One call = params->n_samples consecutive sample passes of render_tiles.
  * scratch_rgb receives n_samples × height × width × 3 floats (linear radiance,

@@ -35,6 +35,8 @@ def lib():
         L.orc_trace_closest.argtypes = [vp, fp, i64, C.POINTER(abi.RtHit), i32, i32]
         L.orc_trace_any.argtypes = [vp, fp, i64, C.POINTER(C.c_uint8), i32]
         L.orc_trace_stats.argtypes = [vp, fp, i64, C.POINTER(i64), i32]
+        L.orc_trace_transmittance.argtypes = [vp, fp, i64, fp, i32]
+        L.orc_hg_sample.argtypes = [fp, i64, fp]
         L.orc_render_pass.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), fp,
                                       C.POINTER(C.c_uint8), i32, u32, u32, C.POINTER(i64)]
         L.orc_accumulate.argtypes = [fp, fp, C.POINTER(u32), fp, C.POINTER(C.c_uint8), i64, f, u32, f]
@@ -108,6 +110,20 @@ def elut():
     return out
 
 
+def hg_sample(w, g, xi1, xi2):
+    """hg_sample (volume.rs:39-62) for arrays of incident directions and numbers."""
+    w = np.asarray(w, np.float32).reshape(-1, 3)
+    n = len(w)
+    a = np.zeros((n, 6), np.float32)
+    a[:, :3] = w
+    a[:, 3] = g
+    a[:, 4] = xi1
+    a[:, 5] = xi2
+    out = np.zeros((n, 3), np.float32)
+    lib().orc_hg_sample(_fp(a), n, _fp(out))
+    return out
+
+
 def rng(seed, pixel, sample, dim):
     u, f = C.c_uint32(), C.c_float()
     lib().orc_rng(seed, pixel, sample, dim, C.byref(u), C.byref(f))
@@ -152,6 +168,13 @@ class OracleScene:
         occ = np.zeros(len(rays), np.uint8)
         lib().orc_trace_any(self.h, _fp(rays), len(rays), occ.ctypes.data_as(C.POINTER(C.c_uint8)), threads)
         return occ
+
+    def trace_transmittance(self, rays, threads=os.cpu_count()):
+        """world.transmittance (bvh.rs:532-575) per ray: 0 if occluded, else Π media."""
+        rays = _f(rays).reshape(-1, 8)
+        out = np.zeros(len(rays), np.float32)
+        lib().orc_trace_transmittance(self.h, _fp(rays), len(rays), _fp(out), threads)
+        return out
 
     def trace_stats(self, rays, threads=os.cpu_count()):
         rays = _f(rays).reshape(-1, 8)

@@ -395,6 +395,9 @@ struct Scene {
     bool has_photons = false;
     float gather_r2 = 0.0f, gather_norm = 0.0f;
     uint32_t knn_k = 0;
+    // participating media (volume.rs:78-263); a box boundary is its 6 quads
+    std::vector<RtMedium> media;
+    std::vector<std::vector<Quad>> media_quads;
 };
 
 static inline int prim_type(const Scene& s, int64_t gid) {
@@ -765,6 +768,172 @@ static bool any_hit(const Scene& s, const Ray& r, float tmin, float tmax) {
     return false;
 }
 
+// ── participating media (volume.rs:39-263, perlin.rs:35-91) ──────────────────
+// A medium's random stream is keyed on the ray's bits, as the reference seeds
+// a SmallRng from origin xyz, direction x and wavelength (volume.rs:114-120):
+// here a pcg3d stream of those bits, identical on the CPU and the GPU.
+struct MedRng { uint32_t a, b, c; };
+static inline uint32_t fbits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+static inline MedRng medium_rng(V3 o, V3 d, float lam) {
+    MedRng r;
+    r.a = fbits(o.x) ^ mix32(fbits(d.x) + 0x9E3779B9u);
+    r.b = fbits(o.y) ^ mix32(fbits(lam) + 0x7F4A7C15u);
+    r.c = mix32(fbits(o.z) + 0x4D454449u);
+    return r;
+}
+static inline float medium_rnd(const MedRng& r, uint32_t i) {
+    return (float)(pcg3d_x(r.a, r.b, r.c ^ (i * 0x9E3779B9u)) >> 8) * (1.0f / 16777216.0f);
+}
+
+// Perlin::noise / turb (perlin.rs:35-91)
+static float perlin_noise(const RtMedium& m, V3 p) {
+    float fx = std::floor(p.x), fy = std::floor(p.y), fz = std::floor(p.z);
+    float u = p.x - fx, v = p.y - fy, w = p.z - fz;
+    u = u * u * (3.0f - 2.0f * u);
+    v = v * v * (3.0f - 2.0f * v);
+    w = w * w * (3.0f - 2.0f * w);
+    int i = (int)fx, j = (int)fy, k = (int)fz;
+    float accum = 0.0f;
+    for (int di = 0; di < 2; di++)
+        for (int dj = 0; dj < 2; dj++)
+            for (int dk = 0; dk < 2; dk++) {
+                int idx = m.perlin_perm[(i + di) & 255] ^ m.perlin_perm[256 + ((j + dj) & 255)] ^
+                          m.perlin_perm[512 + ((k + dk) & 255)];
+                V3 c = v3(m.perlin_vec[idx * 3], m.perlin_vec[idx * 3 + 1], m.perlin_vec[idx * 3 + 2]);
+                float fi = (float)di, fj = (float)dj, fk = (float)dk;
+                V3 wt = v3(u - fi, v - fj, w - fk);
+                accum += (fi * u + (1.0f - fi) * (1.0f - u)) * (fj * v + (1.0f - fj) * (1.0f - v)) *
+                         (fk * w + (1.0f - fk) * (1.0f - w)) * dot(c, wt);
+            }
+    return accum;
+}
+static float perlin_turb(const RtMedium& m, V3 p, int depth) {
+    float accum = 0.0f, weight = 1.0f;
+    for (int i = 0; i < depth; i++) {
+        accum += weight * perlin_noise(m, p);
+        weight *= 0.5f;
+        p = v3(p.x * 2.0f, p.y * 2.0f, p.z * 2.0f);
+    }
+    return std::fabs(accum);
+}
+// NoiseMedium::density_at (volume.rs:188-191); density holds max(density, ε)
+// and threshold is clamped to [0, 0.99] at scene creation (volume.rs:180-184)
+static float medium_density_at(const RtMedium& m, V3 p) {
+    float n = perlin_turb(m, p * m.noise_scale, 7) * 0.5f;
+    return rmax(n - m.threshold, 0.0f) * m.density;
+}
+
+// First boundary hit in [tmin, tmax]: the sphere's near-then-far root, or the
+// nearest of the box's 6 quads (the BvhTree over make_box, quad.rs:201-215).
+static bool bound_hit(const Scene& s, int mi, const Ray& r, float tmin, float tmax, float* t) {
+    const RtMedium& m = s.media[mi];
+    if (m.boundary == RT_BOUND_SPHERE)
+        return sphere_hit(Sphere{v3(m.center[0], m.center[1], m.center[2]), m.radius, 0}, r, tmin, tmax, t);
+    bool any = false;
+    float closest = tmax;
+    for (const Quad& q : s.media_quads[mi]) {
+        float tq, a, b;
+        if (quad_hit(q, r, tmin, closest, &tq, &a, &b)) { closest = tq; any = true; }
+    }
+    *t = closest;
+    return any;
+}
+
+// Scatter distance of ConstantMedium::hit (volume.rs:97-138) / NoiseMedium::hit
+// (:195-235) for t_max = ∞; INFINITY when the ray leaves the medium first.  The
+// candidate depends on the ray alone, so "nearest of surface and medium" gives
+// the reference's closest hit for any traversal order.  Delta tracking is
+// bounded at 4096 steps (the reference loops until exit).
+static float medium_sample(const Scene& s, int mi, const Ray& r, float lam, float tmin) {
+    const RtMedium& m = s.media[mi];
+    float t1, t2;
+    if (!bound_hit(s, mi, r, -INFINITY, INFINITY, &t1)) return INFINITY;
+    if (!bound_hit(s, mi, r, t1 + 0.0001f, INFINITY, &t2)) return INFINITY;
+    if (t1 < tmin) t1 = tmin;
+    if (t1 >= t2) return INFINITY;
+    if (t1 < 0.0f) t1 = 0.0f;
+    float len = length(r.d);
+    MedRng g = medium_rng(r.o, r.d, lam);
+    if (m.type == RT_MEDIUM_CONSTANT) {
+        float dist_inside = (t2 - t1) * len;
+        float xi = rmax(medium_rnd(g, 0), FLT_EPSILON);
+        float hit_dist = (-1.0f / m.density) * std::log(xi);
+        if (hit_dist > dist_inside) return INFINITY;
+        return t1 + hit_dist / len;
+    }
+    float inv_maj = 1.0f / (m.density * len);
+    float t = t1;
+    for (uint32_t k = 0; k < 4096; k++) {
+        t -= inv_maj * std::log(rmax(medium_rnd(g, 2 * k), FLT_EPSILON));
+        if (t >= t2) return INFINITY;
+        float dens = medium_density_at(m, r.o + t * r.d);
+        if (medium_rnd(g, 2 * k + 1) < dens / m.density) return t;
+    }
+    return INFINITY;
+}
+
+// Nearest medium event before `tsurf` (medium ids follow all primitives, so an
+// exact tie goes to the surface); returns the medium index or -1.
+static int media_event(const Scene& s, const Ray& r, float lam, float tmin, float tsurf, float* t_out) {
+    int best = -1;
+    float bt = tsurf;
+    for (int mi = 0; mi < (int)s.media.size(); mi++) {
+        float t = medium_sample(s, mi, r, lam, tmin);
+        if (t < bt) { bt = t; best = mi; }
+    }
+    *t_out = bt;
+    return best;
+}
+
+// Medium::transmittance (volume.rs:68-76, 140-146, 237-252)
+static float medium_transmittance(const Scene& s, int mi, const Ray& r, float tmin, float tmax) {
+    const RtMedium& m = s.media[mi];
+    float t1, t2;
+    if (!bound_hit(s, mi, r, -INFINITY, INFINITY, &t1)) return 1.0f;
+    if (!bound_hit(s, mi, r, t1 + 0.0001f, INFINITY, &t2)) return 1.0f;
+    float a = rmax(rmax(t1, 0.0f), tmin), b = rmin(t2, tmax);
+    if (a >= b) return 1.0f;
+    float len = length(r.d);
+    float l = (b - a) * len;
+    if (m.type == RT_MEDIUM_CONSTANT) return std::exp(-m.density * l);
+    const int K = 16;
+    float seg_t = l / len, sum = 0.0f;
+    for (int i = 0; i < K; i++) {
+        float t = a + seg_t * ((float)i + 0.5f) / (float)K;
+        sum += medium_density_at(m, r.o + t * r.d);
+    }
+    return std::exp(-sum / (float)K * l);
+}
+
+// world.transmittance (bvh.rs:532-575): 0 behind an opaque primitive, else
+// the product of the media's transmittances
+static float scene_transmittance(const Scene& s, const Ray& r, float tmin, float tmax) {
+    if (any_hit(s, r, tmin, tmax)) return 0.0f;
+    float tr = 1.0f;
+    for (int mi = 0; mi < (int)s.media.size(); mi++) {
+        tr *= medium_transmittance(s, mi, r, tmin, tmax);
+        if (tr <= 0.0f) return 0.0f;
+    }
+    return tr;
+}
+
+// hg_sample (volume.rs:39-62)
+static V3 hg_sample(V3 w, float g, float xi1, float xi2) {
+    float cos_t;
+    if (std::fabs(g) < 1e-3f) {
+        cos_t = 1.0f - 2.0f * xi1;
+    } else {
+        float sq = (1.0f - g * g) / rmax(1.0f - g + 2.0f * g * xi1, 1e-12f);
+        cos_t = (1.0f + g * g - sq * sq) / (2.0f * g);
+    }
+    float sin_t = std::sqrt(rmax(1.0f - cos_t * cos_t, 0.0f));
+    float phi = 2.0f * PI_F * xi2;
+    V3 helper = std::fabs(w.x) > 0.9f ? v3(0, 1, 0) : v3(1, 0, 0);
+    V3 u = unit(cross(w, helper));
+    V3 v = cross(w, u);
+    return u * (sin_t * std::cos(phi)) + v * (sin_t * std::sin(phi)) + w * cos_t;
+}
+
 // ── hit record (hittable.rs:73-94) ───────────────────────────────────────────
 struct Rec { V3 p, normal; float t, u, v; bool front; int mat; int32_t gid; };
 
@@ -1082,6 +1251,18 @@ static bool trace_photon(const Scene& s, V3 pos, V3 dir, float lum_clamp, V3 pow
         uint32_t base = P_BOUNCE0 + bounce * P_PER_BOUNCE;
         Ray ray{pos, dir};
         HitRes h = closest_hit<false>(s, ray, 0.001f, INFINITY, nullptr);
+        float tmed;
+        int med = s.media.empty() ? -1 : media_event(s, ray, lam, 0.001f, h.gid < 0 ? INFINITY : h.t, &tmed);
+        if (med >= 0) {
+            // a medium scatter is a skip_pdf bounce of the caustic path (photon.rs:252-260)
+            const RtMedium& M = s.media[med];
+            power = power * v3(M.color[0], M.color[1], M.color[2]);
+            V3 np = ray.o + tmed * ray.d;
+            dir = hg_sample(unit(ray.d), M.g, rnd(rng, base + 0), rnd(rng, base + 1));
+            pos = np;
+            spec_depth++;
+            continue;
+        }
         if (h.gid < 0) return false;
         Rec rec = make_rec(s, ray, h);
         const RtMaterial& m = s.mats[rec.mat];
@@ -1299,13 +1480,26 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
         uint32_t base = D_BOUNCE0 + depth * D_PER_BOUNCE;
         (*n_ext)++;
         HitRes h = closest_hit<false>(s, ray, 0.001f, INFINITY, nullptr);
-        if (h.gid < 0) {
+        float tmed;
+        int med = s.media.empty() ? -1 : media_event(s, ray, ss.lam[0], 0.001f, h.gid < 0 ? INFINITY : h.t, &tmed);
+        if (med >= 0) {
+            // medium scatter: HenyeyGreenstein::scatter (volume.rs:29-35), skip_pdf →
+            // the specular branch (renderer.rs:421-456) with no emission
+            const RtMedium& M = s.media[med];
+            V3 p = ray.o + tmed * ray.d;
+            V3 dir = hg_sample(unit(ray.d), M.g, rnd(rng, base + B_SCATTER0), rnd(rng, base + B_SCATTER1));
+            prev_spec_sun_weight = 1.0f;
+            T = T * v3(M.color[0], M.color[1], M.color[2]);
+            ray = Ray{p, dir};
+            prev_specular = true;
+            prev_mis_w_brdf = 1.0f;
+        } else if (h.gid < 0) {
             float env_pdf = env_pdf_value(s, ray.d);                                // no sun: sun_pdf = 0
             float emit_w = (env_pdf == 0.0f) ? 1.0f : (prev_specular ? prev_spec_sun_weight : prev_mis_w_brdf);
             V3 bg = (depth == 0 || !s.has_env) ? bg_eval(s, ray.d) : env_eval(s, ray.d);
             color = color + T * (bg * spec_factor(s.spec, ss)) * bg_scale * emit_w;
             break;
-        }
+        } else {
         Rec rec = make_rec(s, ray, h);
         const RtMaterial& m = s.mats[rec.mat];
         float emit_w = (prev_specular || !have_lights) ? 1.0f : prev_mis_w_brdf;
@@ -1403,15 +1597,15 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                 Rec lrec;
                 if (lights_hit(s, shadow, 0.001f, INFINITY, &lrec)) {
                     (*n_shadow)++;
-                    bool occl = any_hit(s, shadow, 0.001f, lrec.t * (1.0f - 1e-4f));
-                    if (!occl) {
+                    float tr = scene_transmittance(s, shadow, 0.001f, lrec.t * (1.0f - 1e-4f));
+                    if (tr > 0.0f) {
                         float l_pdf = lights_pdf_value(s, rec.p, light_dir);
                         float brdf = rmax(dot(rec.normal, unit(light_dir)) / PI_F, 0.0f);
                         float env_p = env_pdf_value(s, light_dir);
                         float mis_d = l_pdf * l_pdf + brdf * brdf + env_p * env_p;
                         if (mis_d > 0.0f && brdf > 0.0f) {
                             V3 nee = emission(s, lrec.mat, ss);
-                            color = color + T * att * brdf * l_pdf * nee / mis_d;
+                            color = color + T * tr * att * brdf * l_pdf * nee / mis_d;
                         }
                     }
                 }
@@ -1423,14 +1617,14 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                 if (env_pdf > 0.0f) {
                     Ray shadow{rec.p, env_dir};
                     (*n_shadow)++;
-                    bool occl = any_hit(s, shadow, 0.001f, INFINITY);
-                    if (!occl) {
+                    float tr = scene_transmittance(s, shadow, 0.001f, INFINITY);
+                    if (tr > 0.0f) {
                         float brdf = rmax(dot(rec.normal, unit(env_dir)) / PI_F, 0.0f);
                         if (brdf > 0.0f) {
                             float area_pdf = have_lights ? lights_pdf_value(s, rec.p, env_dir) : 0.0f;
                             V3 env_color = env_eval(s, env_dir) * spec_factor(s.spec, ss);
                             float mis_d = env_pdf * env_pdf + brdf * brdf + area_pdf * area_pdf;
-                            color = color + T * att * brdf * env_pdf * env_color / mis_d;
+                            color = color + T * tr * att * brdf * env_pdf * env_color / mis_d;
                         }
                     }
                 }
@@ -1454,6 +1648,7 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
             ray = Ray{rec.p, ind_dir};
             prev_specular = false;
         }
+        }   // surface hit
         if (depth >= 2) {                                                           // renderer.rs:574-579
             V3 eff = T * spec_factor(s.spec, ss);
             float survive = rmax(rmax(eff.x, eff.y), eff.z);
@@ -1552,6 +1747,43 @@ static int scene_create(const RtSceneDesc* d, Scene** out) {
         const float* p = d->sphere + i * 4;
         s->spheres[i] = Sphere{v3(p[0], p[1], p[2]), p[3], d->sphere_mat[i]};
     }
+    // participating media (scene_file.rs:962-983, volume.rs:88-97, 170-186)
+    if (d->n_media < 0 || (d->n_media > 0 && !d->media)) { delete s; g_err = "bad media list"; return RT_ERR_INVALID; }
+    for (int32_t i = 0; i < d->n_media; i++) {
+        RtMedium m = d->media[i];
+        bool ok = (m.type == RT_MEDIUM_CONSTANT || m.type == RT_MEDIUM_NOISE) &&
+                  (m.boundary == RT_BOUND_SPHERE || m.boundary == RT_BOUND_BOX) && std::isfinite(m.density) &&
+                  m.density >= 0.0f;
+        if (m.boundary == RT_BOUND_SPHERE) ok = ok && m.radius > 0.0f;
+        if (!ok) { delete s; g_err = "invalid medium " + std::to_string(i); return RT_ERR_INVALID; }
+        if (m.type == RT_MEDIUM_NOISE) {
+            m.density = rmax(m.density, FLT_EPSILON);
+            m.threshold = rmin(rmax(m.threshold, 0.0f), 0.99f);
+        }
+        std::vector<Quad> qs;
+        if (m.boundary == RT_BOUND_BOX) {                                            // quad.rs:201-215
+            V3 mn = v3(rmin(m.p_min[0], m.p_max[0]), rmin(m.p_min[1], m.p_max[1]), rmin(m.p_min[2], m.p_max[2]));
+            V3 mx = v3(rmax(m.p_min[0], m.p_max[0]), rmax(m.p_min[1], m.p_max[1]), rmax(m.p_min[2], m.p_max[2]));
+            V3 dx = v3(mx.x - mn.x, 0, 0), dy = v3(0, mx.y - mn.y, 0), dz = v3(0, 0, mx.z - mn.z);
+            V3 qq[6][3] = {{v3(mn.x, mn.y, mx.z), dx, dy}, {v3(mx.x, mn.y, mx.z), -dz, dy},
+                           {v3(mx.x, mn.y, mn.z), -dx, dy}, {v3(mn.x, mn.y, mn.z), dz, dy},
+                           {v3(mn.x, mx.y, mx.z), dx, -dz}, {v3(mn.x, mn.y, mn.z), dx, dz}};
+            for (auto& f : qq) {
+                Quad Q;
+                Q.q = f[0]; Q.u = f[1]; Q.v = f[2];
+                V3 n = cross(Q.u, Q.v);
+                Q.area = length(n);
+                if (!(Q.area > 0.0f)) { delete s; g_err = "degenerate medium box " + std::to_string(i); return RT_ERR_INVALID; }
+                Q.normal = n / Q.area;
+                Q.d = dot(Q.normal, Q.q);
+                Q.w = n / dot(n, n);
+                Q.mat = 0;
+                qs.push_back(Q);
+            }
+        }
+        s->media.push_back(m);
+        s->media_quads.push_back(qs);
+    }
     s->lights.assign(d->light_prims, d->light_prims + d->n_lights);
     s->bg = d->bg;
     s->has_env = d->bg.type == RT_BG_ENVMAP && d->bg.env_rgb && d->bg.env_w > 0 && d->bg.env_h > 0;
@@ -1625,6 +1857,9 @@ int32_t orc_trace_closest(void* sp, const float* rays, int64_t n, RtHit* hits, i
             const float* r = rays + i * 8;
             Ray ray{v3(r[0], r[1], r[2]), v3(r[3], r[4], r[5])};
             HitRes h = mode == 1 ? closest_hit_brute(*s, ray, r[6], r[7]) : closest_hit<false>(*s, ray, r[6], r[7], nullptr);
+            float tm;
+            int med = s->media.empty() ? -1 : media_event(*s, ray, 550.0f, r[6], h.gid < 0 ? r[7] : h.t, &tm);
+            if (med >= 0) h = HitRes{(int32_t)(s->n_tris + s->n_quads + s->n_spheres + med), tm, 0.0f, 0.0f};
             hits[i].prim = h.gid; hits[i].t = h.gid >= 0 ? h.t : 0.0f;
             hits[i].b1 = h.gid >= 0 ? h.b1 : 0.0f; hits[i].b2 = h.gid >= 0 ? h.b2 : 0.0f;
         }
@@ -1641,6 +1876,28 @@ int32_t orc_trace_any(void* sp, const float* rays, int64_t n, uint8_t* occ, int3
             occ[i] = any_hit(*s, Ray{v3(r[0], r[1], r[2]), v3(r[3], r[4], r[5])}, r[6], r[7]) ? 1 : 0;
         }
     });
+    return RT_OK;
+}
+
+int32_t orc_trace_transmittance(void* sp, const float* rays, int64_t n, float* tr, int32_t threads) {
+    Scene* s = (Scene*)sp;
+    int64_t chunk = 1024, nch = (n + chunk - 1) / chunk;
+    parallel_rows((uint32_t)nch, threads, [&](uint32_t c, int) {
+        for (int64_t i = c * chunk; i < std::min(n, (int64_t)(c + 1) * chunk); i++) {
+            const float* r = rays + i * 8;
+            tr[i] = scene_transmittance(*s, Ray{v3(r[0], r[1], r[2]), v3(r[3], r[4], r[5])}, r[6], r[7]);
+        }
+    });
+    return RT_OK;
+}
+
+// hg_sample for n (w, g, xi1, xi2) rows of 6 floats → n × 3 directions
+int32_t orc_hg_sample(const float* in, int64_t n, float* out) {
+    for (int64_t i = 0; i < n; i++) {
+        const float* a = in + i * 6;
+        V3 d = hg_sample(v3(a[0], a[1], a[2]), a[3], a[4], a[5]);
+        out[i * 3] = d.x; out[i * 3 + 1] = d.y; out[i * 3 + 2] = d.z;
+    }
     return RT_OK;
 }
 

@@ -62,6 +62,28 @@ class RtBackground(C.Structure):
     ]
 
 
+RT_MEDIUM_CONSTANT, RT_MEDIUM_NOISE = 0, 1
+RT_BOUND_SPHERE, RT_BOUND_BOX = 0, 1
+
+
+class RtMedium(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("boundary", C.c_int32),
+        ("center", F3),
+        ("radius", C.c_float),
+        ("p_min", F3),
+        ("p_max", F3),
+        ("density", C.c_float),
+        ("color", F3),
+        ("g", C.c_float),
+        ("noise_scale", C.c_float),
+        ("threshold", C.c_float),
+        ("perlin_vec", C.c_float * (256 * 3)),
+        ("perlin_perm", C.c_int32 * (3 * 256)),
+    ]
+
+
 class RtSceneDesc(C.Structure):
     _fields_ = [
         ("n_tris", C.c_int64),
@@ -80,6 +102,8 @@ class RtSceneDesc(C.Structure):
         ("light_prims", C.POINTER(C.c_int32)),
         ("bg", RtBackground),
         ("spectral_range", C.c_int32),
+        ("n_media", C.c_int32),
+        ("media", C.POINTER(RtMedium)),
     ]
 
 

@@ -190,4 +190,18 @@ def icosphere_scene(width=1920, height=1080, spp=64, max_depth=12, hero=4, seed=
     return sb, settings
 
 
-CONFIGS = {"box": box_scene, "icosphere": icosphere_scene}
+def media_box_scene(width=256, height=256, spp=16, max_depth=24, hero=4, seed=5, density=4.0):
+    """The box room with participating media (volume.rs): a Perlin-noise medium
+    filling the lower half (density scale `density`, albedo 0.9, g = 0.3) and a
+    constant-density sphere (σ = 2, albedo 0.8, g = −0.2) above it."""
+    sb, st = box_scene(width, height, spp, max_depth, hero, seed)
+    sb.name = "media box"
+    sb.spheres.clear()                                   # keep the room and the light
+    sb.add_medium("noise", "box", density, (0.9, 0.9, 0.9), g=0.3, noise_scale=4.0, threshold=0.05,
+                  p_min=(0.0, 0.0, 0.0), p_max=(1.0, 0.5, 1.0), seed=seed)
+    sb.add_medium("constant", "sphere", 2.0, (0.8, 0.8, 0.8), g=-0.2, center=(0.5, 0.7, 0.55), radius=0.15)
+    st["name"] = f"media box {width}x{height} {spp}spp depth{max_depth} hero{hero}"
+    return sb, st
+
+
+CONFIGS = {"box": box_scene, "icosphere": icosphere_scene, "media_box": media_box_scene}

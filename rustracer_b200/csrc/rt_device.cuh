@@ -62,6 +62,21 @@ struct DevLight {        // one entry of the NEE light list (hittable.rs:138-225
     float4 g[5];         // quad record or sphere record (same packing as above)
 };
 
+// A participating medium (volume.rs:78-263): boundary sphere or box faces (the
+// quad record of make_box, quad.rs:201-215, without the id row), HG albedo and
+// asymmetry, and for the noise medium its Perlin tables (perlin.rs:4-33).
+struct DevFace { float4 g[4]; };
+struct DevMedium {
+    int type, boundary;          // RT_MEDIUM_*, RT_BOUND_*
+    float4 sphere;               // centre, radius
+    DevFace face[6];
+    float density;               // σ, or the noise medium's density scale max(density, ε)
+    float g, noise_scale, threshold;
+    float3 color;
+    const float4* vec;           // 256 Perlin vectors
+    const int32_t* perm;         // 3 × 256 permutations
+};
+
 struct DevScene {
     const float4* nodes;
     const float4* tri;
@@ -72,6 +87,8 @@ struct DevScene {
     const DevMaterial* mats;
     const uint8_t* mat_code;    // class code per material (see RT_HIT_CODE)
     int n_lights, n_mats;
+    const DevMedium* media;
+    int n_media;
     // spectral tables: CIE x̄ȳz̄ on the 5 nm grid from 380 nm and the per-channel
     // normalisations of spectral_to_rgb / spectral_fire_rgb (spectrum.rs:78-177)
     const float4* cmf;          // n_spec entries (x, y, z, -)

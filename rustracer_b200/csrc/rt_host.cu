@@ -3,6 +3,7 @@
 // loop that drives the kernels of rt_trace.cu / rt_shade.cu on one stream.
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -317,7 +318,7 @@ struct RtScene {
     std::string err;
     DevScene S{};
     std::vector<DevBuf> owned;
-    int64_t n_nodes = 0, n_leaves = 0;
+    int64_t n_nodes = 0, n_leaves = 0, n_prims = 0;
     int32_t max_depth = 0;
     double sah_cost = 0.0;
     std::vector<RefNode> ref_nodes;   // reference-layout copy for rt_scene_bvh_export
@@ -467,6 +468,7 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         return bail(fail(s, RT_ERR_INVALID, "negative count"));
     int64_t n = d->n_tris + d->n_quads + d->n_spheres;
     if (n >= (1ll << 28)) return bail(fail(s, RT_ERR_CAPACITY, "more than 2^28 primitives"));
+    s->n_prims = n;
     if ((d->n_tris && (!d->tri_v || !d->tri_mat)) || (d->n_quads && (!d->quad_quv || !d->quad_mat)) ||
         (d->n_spheres && (!d->sphere || !d->sphere_mat)) || (d->n_mats && !d->mats) || (d->n_lights && !d->light_prims))
         return bail(fail(s, RT_ERR_INVALID, "null array with non-zero count"));
@@ -755,6 +757,72 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     }
     if ((rc = upload(s, codes.data(), codes.size(), &s->S.mat_code))) return bail(rc);
 
+    // ── participating media (scene_file.rs:962-983, volume.rs:88-97, 170-186) ─
+    if (d->n_media < 0 || (d->n_media > 0 && !d->media)) return bail(fail(s, RT_ERR_INVALID, "bad media list"));
+    if (d->n_media > 0) {
+        std::vector<DevMedium> dm(d->n_media);
+        for (int32_t i = 0; i < d->n_media; i++) {
+            const RtMedium& m = d->media[i];
+            bool ok = (m.type == RT_MEDIUM_CONSTANT || m.type == RT_MEDIUM_NOISE) &&
+                      (m.boundary == RT_BOUND_SPHERE || m.boundary == RT_BOUND_BOX) && std::isfinite(m.density) &&
+                      m.density >= 0.0f && (m.boundary != RT_BOUND_SPHERE || m.radius > 0.0f);
+            if (!ok) return bail(fail(s, RT_ERR_INVALID, "invalid medium " + std::to_string(i)));
+            DevMedium& g = dm[i];
+            memset(&g, 0, sizeof(g));
+            g.type = m.type;
+            g.boundary = m.boundary;
+            g.sphere = make_float4(m.center[0], m.center[1], m.center[2], m.radius);
+            g.density = m.type == RT_MEDIUM_NOISE ? std::fmax(m.density, FLT_EPSILON) : m.density;
+            g.g = m.g;
+            g.noise_scale = m.noise_scale;
+            g.threshold = std::fmin(std::fmax(m.threshold, 0.0f), 0.99f);
+            g.color = make_float3(m.color[0], m.color[1], m.color[2]);
+            Box mb;
+            if (m.boundary == RT_BOUND_BOX) {                                        // quad.rs:201-215
+                H3 mn = h3(std::fmin(m.p_min[0], m.p_max[0]), std::fmin(m.p_min[1], m.p_max[1]), std::fmin(m.p_min[2], m.p_max[2]));
+                H3 mx = h3(std::fmax(m.p_min[0], m.p_max[0]), std::fmax(m.p_min[1], m.p_max[1]), std::fmax(m.p_min[2], m.p_max[2]));
+                H3 dx = h3(mx.x - mn.x, 0, 0), dy = h3(0, mx.y - mn.y, 0), dz = h3(0, 0, mx.z - mn.z);
+                H3 nz = h3(-dz.x, -dz.y, -dz.z), nx = h3(-dx.x, -dx.y, -dx.z);
+                H3 faces[6][3] = {{h3(mn.x, mn.y, mx.z), dx, dy}, {h3(mx.x, mn.y, mx.z), nz, dy},
+                                  {h3(mx.x, mn.y, mn.z), nx, dy}, {h3(mn.x, mn.y, mn.z), dz, dy},
+                                  {h3(mn.x, mx.y, mx.z), dx, nz}, {h3(mn.x, mn.y, mn.z), dx, dz}};
+                for (int f = 0; f < 6; f++) {
+                    H3 Q = faces[f][0], u = faces[f][1], v = faces[f][2];
+                    H3 nn = hcross(u, v);
+                    float ar = hlen(nn);
+                    if (!(ar > 0.0f)) return bail(fail(s, RT_ERR_INVALID, "degenerate medium box " + std::to_string(i)));
+                    H3 nrm = nn / ar, w = nn / hdot(nn, nn);
+                    g.face[f].g[0] = make_float4(nrm.x, nrm.y, nrm.z, hdot(nrm, Q));
+                    g.face[f].g[1] = make_float4(Q.x, Q.y, Q.z, u.x);
+                    g.face[f].g[2] = make_float4(u.y, u.z, v.x, v.y);
+                    g.face[f].g[3] = make_float4(v.z, w.x, w.y, w.z);
+                }
+                mb = Box{mn, mx};
+            } else {
+                H3 c = h3(m.center[0], m.center[1], m.center[2]), r = h3(m.radius, m.radius, m.radius);
+                mb = Box{c - r, c + r};
+            }
+            std::vector<float4> vec(256);
+            for (int k = 0; k < 256; k++) vec[k] = make_float4(m.perlin_vec[k * 3], m.perlin_vec[k * 3 + 1], m.perlin_vec[k * 3 + 2], 0.f);
+            std::vector<int32_t> perm(768);
+            for (int k = 0; k < 768; k++) {
+                if (m.type == RT_MEDIUM_NOISE && (m.perlin_perm[k] < 0 || m.perlin_perm[k] > 255))
+                    return bail(fail(s, RT_ERR_INVALID, "Perlin permutation entry out of 0..255 in medium " + std::to_string(i)));
+                perm[k] = m.perlin_perm[k] & 255;
+            }
+            if ((rc = upload(s, vec.data(), vec.size(), &g.vec))) return bail(rc);
+            if ((rc = upload(s, perm.data(), perm.size(), &g.perm))) return bail(rc);
+            // media join the photon bounds (volume.rs:152-154)
+            for (int a = 0; a < 3; a++) {
+                bool first = s->empty && i == 0;
+                s->world_lo[a] = first ? hc(mb.mn, a) : std::fmin(s->world_lo[a], hc(mb.mn, a));
+                s->world_hi[a] = first ? hc(mb.mx, a) : std::fmax(s->world_hi[a], hc(mb.mx, a));
+            }
+        }
+        if ((rc = upload(s, dm.data(), dm.size(), &s->S.media))) return bail(rc);
+        s->S.n_media = d->n_media;
+    }
+
     std::call_once(g_elut_once, build_elut);
     if ((rc = upload(s, g_elut, (size_t)64 * 64, &s->S.elut))) return bail(rc);
 
@@ -875,7 +943,8 @@ extern "C" int32_t rt_trace_closest(RtScene* s, const float* rays, int64_t n, Rt
     if (n <= 0) return RT_OK;
     if (n > (1ll << 31)) return fail(s, RT_ERR_CAPACITY, "more than 2^31 rays per call");
     CK(cudaSetDevice(s->device));
-    if (s->empty) {
+    bool media = s->S.n_media > 0;
+    if (s->empty && !media) {
         if (mem == RT_MEM_DEVICE) { CK(cudaMemsetAsync(hits, 0xFF, n * sizeof(RtHit), s->stream)); return RT_OK; }
         for (int64_t i = 0; i < n; i++) hits[i] = RtHit{-1, 0.f, 0.f, 0.f};
         return RT_OK;
@@ -890,17 +959,31 @@ extern "C" int32_t rt_trace_closest(RtScene* s, const float* rays, int64_t n, Rt
         dout = (int4*)((char*)s->stage + ((rb + 255) & ~(size_t)255));
         CK(cudaMemcpyAsync((void*)drays, rays, rb, cudaMemcpyHostToDevice, s->stream));
     }
-    uint32_t* next;
     if (!s->counters) {
         if (cudaMalloc(&s->counters, sizeof(uint32_t) * RT_CTR_WORDS) != cudaSuccess)
             return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
     }
-    next = s->counters;
-    CK(cudaMemsetAsync(next, 0, sizeof(uint32_t), s->stream));
-    rth::launch_trace_closest_api(s->S, drays, (uint32_t)n, dout, next, s->d_err, s->sms, s->stream);
+    if (!s->empty) {
+        CK(cudaMemsetAsync(s->counters, 0, sizeof(uint32_t), s->stream));
+        rth::launch_trace_closest_api(s->S, drays, (uint32_t)n, dout, s->counters, s->d_err, s->sms, s->stream);
+    }
+    if (media)
+        rth::launch_media_api(s->S, drays, (uint32_t)n, dout, (int32_t)s->n_prims, s->empty ? 1 : 0, s->sms, s->stream);
     CK(cudaGetLastError());
     if (mem != RT_MEM_DEVICE) CK(cudaMemcpyAsync(hits, dout, hb, cudaMemcpyDeviceToHost, s->stream));
     return check_err(s);
+}
+
+// any-hit flags into `dout` (device); no primitives → all clear
+static int any_hit_device(RtScene* s, const float* drays, int64_t n, uint8_t* dout) {
+    if (s->empty) { CK(cudaMemsetAsync(dout, 0, n, s->stream)); return RT_OK; }
+    if (!s->counters) {
+        if (cudaMalloc(&s->counters, sizeof(uint32_t) * RT_CTR_WORDS) != cudaSuccess)
+            return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
+    }
+    CK(cudaMemsetAsync(s->counters, 0, sizeof(uint32_t), s->stream));
+    rth::launch_trace_any_api(s->S, drays, (uint32_t)n, dout, s->counters, s->d_err, s->sms, s->stream);
+    return RT_OK;
 }
 
 extern "C" int32_t rt_trace_any(RtScene* s, const float* rays, int64_t n, uint8_t* occ, int32_t mem) {
@@ -908,11 +991,6 @@ extern "C" int32_t rt_trace_any(RtScene* s, const float* rays, int64_t n, uint8_
     if (n <= 0) return RT_OK;
     if (n > (1ll << 31)) return fail(s, RT_ERR_CAPACITY, "more than 2^31 rays per call");
     CK(cudaSetDevice(s->device));
-    if (s->empty) {
-        if (mem == RT_MEM_DEVICE) { CK(cudaMemsetAsync(occ, 0, n, s->stream)); return RT_OK; }
-        memset(occ, 0, n);
-        return RT_OK;
-    }
     const float* drays = rays;
     uint8_t* dout = occ;
     size_t rb = (size_t)n * 8 * sizeof(float);
@@ -923,14 +1001,34 @@ extern "C" int32_t rt_trace_any(RtScene* s, const float* rays, int64_t n, uint8_
         dout = (uint8_t*)((char*)s->stage + ((rb + 255) & ~(size_t)255));
         CK(cudaMemcpyAsync((void*)drays, rays, rb, cudaMemcpyHostToDevice, s->stream));
     }
-    if (!s->counters) {
-        if (cudaMalloc(&s->counters, sizeof(uint32_t) * RT_CTR_WORDS) != cudaSuccess)
-            return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
-    }
-    CK(cudaMemsetAsync(s->counters, 0, sizeof(uint32_t), s->stream));
-    rth::launch_trace_any_api(s->S, drays, (uint32_t)n, dout, s->counters, s->d_err, s->sms, s->stream);
+    int rc = any_hit_device(s, drays, n, dout);
+    if (rc) return rc;
     CK(cudaGetLastError());
     if (mem != RT_MEM_DEVICE) CK(cudaMemcpyAsync(occ, dout, n, cudaMemcpyDeviceToHost, s->stream));
+    return check_err(s);
+}
+
+extern "C" int32_t rt_trace_transmittance(RtScene* s, const float* rays, int64_t n, float* tr, int32_t mem) {
+    if (!s || (n > 0 && (!rays || !tr))) return RT_ERR_INVALID;
+    if (n <= 0) return RT_OK;
+    if (n > (1ll << 31)) return fail(s, RT_ERR_CAPACITY, "more than 2^31 rays per call");
+    CK(cudaSetDevice(s->device));
+    size_t rb = (size_t)n * 8 * sizeof(float), ob = (size_t)n * sizeof(float);
+    size_t off_out = (rb + 255) & ~(size_t)255, off_occ = (off_out + ob + 255) & ~(size_t)255;
+    int rc = ensure_stage(s, off_occ + n + 256);
+    if (rc) return rc;
+    const float* drays = rays;
+    float* dout = tr;
+    uint8_t* docc = (uint8_t*)s->stage + off_occ;
+    if (mem != RT_MEM_DEVICE) {
+        drays = (const float*)s->stage;
+        dout = (float*)((char*)s->stage + off_out);
+        CK(cudaMemcpyAsync((void*)drays, rays, rb, cudaMemcpyHostToDevice, s->stream));
+    }
+    if ((rc = any_hit_device(s, drays, n, docc))) return rc;
+    rth::launch_transmittance_api(s->S, drays, (uint32_t)n, docc, dout, s->sms, s->stream);
+    CK(cudaGetLastError());
+    if (mem != RT_MEM_DEVICE) CK(cudaMemcpyAsync(tr, dout, ob, cudaMemcpyDeviceToHost, s->stream));
     return check_err(s);
 }
 
@@ -1060,6 +1158,10 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         PendTargets T{{B.pend0, B.pend1, W.Rt.pend0, W.Rt.pend1}, {B.pendC, W.Rt.pendC}};
         mark(1);
         rth::launch_extend(s->S, A, nullptr, c + CTR_COUNT, c + CTR_EXTEND_NEXT, W.derr, s->sms, s->stream);
+        if (s->S.n_media > 0) {
+            rth::launch_media(s->S, A, nullptr, c + CTR_COUNT, s->sms, s->stream);
+            nl += 2;   // media events, medium shading
+        }
         if ((int64_t)it == s->cap_depth && s->cap_out) {
             // diagnostics: copy this iteration's rays out (origin, direction)
             CK(cudaStreamSynchronize(s->stream));

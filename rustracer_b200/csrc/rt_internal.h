@@ -19,11 +19,9 @@
 #define RT_CTR_STRIDE 32
 #define CTR_COUNT          0
 #define CTR_EXTEND_NEXT    1
-#define CTR_CLASSIFY_NEXT  2
 #define CTR_SHADOW_COUNT   3
 #define CTR_SHADOW_NEXT    4
-#define CTR_CLS_COUNT      5   // 5 entries
-#define CTR_CLS_NEXT       10  // 5 entries
+#define CTR_CLS_COUNT      5   // CLS_N entries
 #define CTR_GATHER_COUNT   15  // photon-gather requests of the iteration
 #define CTR_RETIRE_COUNT   16  // paths that ended in the iteration
 
@@ -40,8 +38,9 @@ static_assert(CTR_HDR_WORDS + RT_CTR_RING * RT_CTR_STRIDE <= RT_CTR_WORDS, "coun
 static_assert(14 * RT_CTR_STRIDE <= RT_CTR_WORDS, "photon counter layout");
 
 // material classes shaded by separate kernels
-enum { CLS_MISS = 0, CLS_EMIT = 1, CLS_DIFFUSE = 2, CLS_METAL = 3, CLS_DIELEC = 4, CLS_N = 5 };
+enum { CLS_MISS = 0, CLS_EMIT = 1, CLS_DIFFUSE = 2, CLS_METAL = 3, CLS_DIELEC = 4, CLS_MEDIUM = 5, CLS_N = 6 };
 struct ClassQueues { uint32_t* q[CLS_N]; };
+static_assert(CTR_CLS_COUNT + CLS_N <= CTR_GATHER_COUNT, "counter slots");
 
 // Per-path wavefront state, structure of arrays.  The render loop keeps two
 // dense sets (iteration it reads set it&1 at positions 0..count−1 and writes
@@ -113,6 +112,14 @@ void launch_trace_closest_api(const rtd::DevScene& S, const float* rays, uint32_
                               int* err, int sms, cudaStream_t st);
 void launch_trace_any_api(const rtd::DevScene& S, const float* rays, uint32_t n, uint8_t* out, uint32_t* next,
                           int* err, int sms, cudaStream_t st);
+// media events after the closest hit: queue = NULL for the dense path set
+// (wavelength in meta.w), else queued photons (wavelength in ray_d.w)
+void launch_media(const rtd::DevScene& S, const PathState& P, const uint32_t* queue, const uint32_t* count, int sms,
+                  cudaStream_t st);
+void launch_media_api(const rtd::DevScene& S, const float* rays, uint32_t n, int4* out, int32_t n_prims,
+                      int fill_miss, int sms, cudaStream_t st);
+void launch_transmittance_api(const rtd::DevScene& S, const float* rays, uint32_t n, const uint8_t* occ, float* out,
+                              int sms, cudaStream_t st);
 void launch_extend(const rtd::DevScene& S, const PathState& P, const uint32_t* queue, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st);
 void launch_shadow(const rtd::DevScene& S, const PendTargets& T, const float4* sq, const uint32_t* count,

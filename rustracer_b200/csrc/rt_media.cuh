@@ -1,0 +1,163 @@
+// rt_media.cuh — participating media on the device (volume.rs:39-263,
+// perlin.rs:35-91): the ray-keyed random stream, Perlin turbulence, boundary
+// intervals, free-flight sampling (constant: exponential; noise: delta
+// tracking to the density scale), shadow transmittance and the HG phase
+// function.  The CPU oracle restates the same functions (oracle/rt_oracle.cpp).
+#pragma once
+#include "../../include/rt_api.h"
+#include "rt_device.cuh"
+
+namespace rtd {
+
+// A hit record of a medium event: type bits 29:28 = 3 (no primitive type), the
+// medium index in bits 27:0; RT_MISS_REF also has type 3 but all code bits set.
+#define RT_HIT_MEDIUM_BASE 0x30000000u
+RT_HD bool hit_is_medium(uint32_t ref) { return ref != RT_MISS_REF && ((ref >> 28) & 3u) == 3u; }
+
+// random stream keyed on the ray's bits (origin xyz, direction x, wavelength;
+// the reference seeds its medium RNG from these, volume.rs:114-120)
+struct MedRng { uint32_t a, b, c; };
+RT_D MedRng medium_rng(float3 o, float3 d, float lam) {
+    MedRng r;
+    r.a = __float_as_uint(o.x) ^ mix32(__float_as_uint(d.x) + 0x9E3779B9u);
+    r.b = __float_as_uint(o.y) ^ mix32(__float_as_uint(lam) + 0x7F4A7C15u);
+    r.c = mix32(__float_as_uint(o.z) + 0x4D454449u);
+    return r;
+}
+RT_D float medium_rnd(const MedRng& r, uint32_t i) {
+    return (float)(pcg3d_x(r.a, r.b, r.c ^ (i * 0x9E3779B9u)) >> 8) * (1.0f / 16777216.0f);
+}
+
+RT_D float perlin_noise(const DevMedium& m, float3 p) {
+    float fx = floorf(p.x), fy = floorf(p.y), fz = floorf(p.z);
+    float u = p.x - fx, v = p.y - fy, w = p.z - fz;
+    u = u * u * (3.0f - 2.0f * u);
+    v = v * v * (3.0f - 2.0f * v);
+    w = w * w * (3.0f - 2.0f * w);
+    int i = (int)fx, j = (int)fy, k = (int)fz;
+    float accum = 0.0f;
+#pragma unroll
+    for (int di = 0; di < 2; di++)
+#pragma unroll
+        for (int dj = 0; dj < 2; dj++)
+#pragma unroll
+            for (int dk = 0; dk < 2; dk++) {
+                int idx = (int)__ldg(m.perm + ((i + di) & 255)) ^ (int)__ldg(m.perm + 256 + ((j + dj) & 255)) ^
+                          (int)__ldg(m.perm + 512 + ((k + dk) & 255));
+                float4 c = __ldg(m.vec + idx);
+                float fi = (float)di, fj = (float)dj, fk = (float)dk;
+                float dt = c.x * (u - fi) + c.y * (v - fj) + c.z * (w - fk);
+                accum += (fi * u + (1.0f - fi) * (1.0f - u)) * (fj * v + (1.0f - fj) * (1.0f - v)) *
+                         (fk * w + (1.0f - fk) * (1.0f - w)) * dt;
+            }
+    return accum;
+}
+RT_D float medium_density_at(const DevMedium& m, float3 p) {
+    float accum = 0.0f, weight = 1.0f;
+    float3 q = p * m.noise_scale;
+    for (int i = 0; i < 7; i++) {
+        accum += weight * perlin_noise(m, q);
+        weight *= 0.5f;
+        q = mk(q.x * 2.0f, q.y * 2.0f, q.z * 2.0f);
+    }
+    float n = fabsf(accum) * 0.5f;
+    return fmaxf(n - m.threshold, 0.0f) * m.density;
+}
+
+// first boundary hit in [tmin, tmax]
+RT_D bool bound_hit(const DevMedium& m, float3 o, float3 d, float tmin, float tmax, float* t) {
+    if (m.boundary == RT_BOUND_SPHERE) return sphere_test(m.sphere, o, d, tmin, tmax, t);
+    bool any = false;
+    float closest = tmax;
+    for (int f = 0; f < 6; f++) {
+        float tq, a, b;
+        if (quad_test(m.face[f].g, o, d, tmin, closest, &tq, &a, &b)) { closest = tq; any = true; }
+    }
+    *t = closest;
+    return any;
+}
+
+// scatter distance for t_max = ∞ (INFINITY when the ray leaves first);
+// delta tracking is bounded at 4096 steps
+RT_D float medium_sample(const DevMedium& m, float3 o, float3 d, float lam, float tmin) {
+    float t1, t2;
+    if (!bound_hit(m, o, d, -INFINITY, INFINITY, &t1)) return INFINITY;
+    if (!bound_hit(m, o, d, t1 + 0.0001f, INFINITY, &t2)) return INFINITY;
+    if (t1 < tmin) t1 = tmin;
+    if (t1 >= t2) return INFINITY;
+    if (t1 < 0.0f) t1 = 0.0f;
+    float len = sqrtf(dot3(d, d));
+    MedRng g = medium_rng(o, d, lam);
+    if (m.type == RT_MEDIUM_CONSTANT) {
+        float dist_inside = (t2 - t1) * len;
+        float hit_dist = (-1.0f / m.density) * logf(fmaxf(medium_rnd(g, 0), 1.1920928955078125e-07f));
+        if (hit_dist > dist_inside) return INFINITY;
+        return t1 + hit_dist / len;
+    }
+    float inv_maj = 1.0f / (m.density * len);
+    float t = t1;
+    for (uint32_t k = 0; k < 4096u; k++) {
+        t -= inv_maj * logf(fmaxf(medium_rnd(g, 2u * k), 1.1920928955078125e-07f));
+        if (t >= t2) return INFINITY;
+        float dens = medium_density_at(m, o + t * d);
+        if (medium_rnd(g, 2u * k + 1u) < dens / m.density) return t;
+    }
+    return INFINITY;
+}
+
+// nearest medium event before tsurf: medium index or -1
+RT_D int media_event(const DevScene& S, float3 o, float3 d, float lam, float tmin, float tsurf, float* t_out) {
+    int best = -1;
+    float bt = tsurf;
+    for (int mi = 0; mi < S.n_media; mi++) {
+        float t = medium_sample(S.media[mi], o, d, lam, tmin);
+        if (t < bt) { bt = t; best = mi; }
+    }
+    *t_out = bt;
+    return best;
+}
+
+RT_D float medium_transmittance(const DevMedium& m, float3 o, float3 d, float tmin, float tmax) {
+    float t1, t2;
+    if (!bound_hit(m, o, d, -INFINITY, INFINITY, &t1)) return 1.0f;
+    if (!bound_hit(m, o, d, t1 + 0.0001f, INFINITY, &t2)) return 1.0f;
+    float a = fmaxf(fmaxf(t1, 0.0f), tmin), b = fminf(t2, tmax);
+    if (a >= b) return 1.0f;
+    float len = sqrtf(dot3(d, d));
+    float l = (b - a) * len;
+    if (m.type == RT_MEDIUM_CONSTANT) return expf(-m.density * l);
+    float seg_t = l / len, sum = 0.0f;
+    for (int i = 0; i < 16; i++) {
+        float t = a + seg_t * ((float)i + 0.5f) / 16.0f;
+        sum += medium_density_at(m, o + t * d);
+    }
+    return expf(-sum / 16.0f * l);
+}
+
+RT_D float media_transmittance(const DevScene& S, float3 o, float3 d, float tmin, float tmax) {
+    float tr = 1.0f;
+    for (int mi = 0; mi < S.n_media; mi++) {
+        tr *= medium_transmittance(S.media[mi], o, d, tmin, tmax);
+        if (tr <= 0.0f) return 0.0f;
+    }
+    return tr;
+}
+
+RT_D float3 hg_sample(float3 w, float g, float xi1, float xi2) {
+    float cos_t;
+    if (fabsf(g) < 1e-3f) {
+        cos_t = 1.0f - 2.0f * xi1;
+    } else {
+        float sq = (1.0f - g * g) / fmaxf(1.0f - g + 2.0f * g * xi1, 1e-12f);
+        cos_t = (1.0f + g * g - sq * sq) / (2.0f * g);
+    }
+    float sin_t = sqrtf(fmaxf(1.0f - cos_t * cos_t, 0.0f));
+    float sp, cp;
+    sincosf(2.0f * PI_F * xi2, &sp, &cp);
+    float3 helper = fabsf(w.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+    float3 u = unit3(cross3(w, helper));
+    float3 v = cross3(w, u);
+    return u * (sin_t * cp) + v * (sin_t * sp) + w * cos_t;
+}
+
+}  // namespace rtd

@@ -17,6 +17,7 @@
 #include <cub/cub.cuh>
 
 #include "rt_internal.h"
+#include "rt_media.cuh"
 
 using namespace rtd;
 
@@ -160,7 +161,20 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
             gid = qin[qi];
             float4 hv = P.hit[gid], ro = P.ray_o[gid], rdv = P.ray_d[gid], th = P.thr[gid];
             uint32_t ref = __float_as_uint(hv.x);
-            if (ref != RT_MISS_REF) {
+            if (hit_is_medium(ref)) {
+                // a medium scatter is a skip_pdf bounce of the caustic path (photon.rs:252-260)
+                float3 o = mk(ro.x, ro.y, ro.z), d = mk(rdv.x, rdv.y, rdv.z);
+                const DevMedium& M = S.media[RT_HIT_INDEX(ref)];
+                Rng rng = photon_rng(seed, gid);
+                uint32_t base = P_BOUNCE0 + bounce * P_PER_BOUNCE;
+                float3 p = o + hv.y * d;
+                float3 nd = hg_sample(unit3(d), M.g, rnd(rng, base + 0), rnd(rng, base + 1));
+                P.ray_o[gid] = make_float4(p.x, p.y, p.z, ro.w);
+                P.ray_d[gid] = make_float4(nd.x, nd.y, nd.z, rdv.w);
+                P.thr[gid] = make_float4(th.x * M.color.x, th.y * M.color.y, th.z * M.color.z,
+                                         __uint_as_float(__float_as_uint(th.w) + 1u));
+                cont = true;
+            } else if (ref != RT_MISS_REF) {
                 float3 o = mk(ro.x, ro.y, ro.z), d = mk(rdv.x, rdv.y, rdv.z), power = mk(th.x, th.y, th.z);
                 float lam = rdv.w, lum_clamp = ro.w;
                 uint32_t spec_depth = __float_as_uint(th.w);
@@ -745,6 +759,7 @@ cudaError_t photon_build(const DevScene& S, PhotonMapDev& map, const PathState& 
         uint32_t* c = counters + b * RT_CTR_STRIDE;
         uint32_t* cn = counters + (b + 1) * RT_CTR_STRIDE;
         launch_extend(S, P, q[b & 1], c + CTR_COUNT, c + CTR_EXTEND_NEXT, (int*)(counters + 13 * RT_CTR_STRIDE), sms, st);
+        if (S.n_media > 0) launch_media(S, P, q[b & 1], c + CTR_COUNT, sms, st);
         k_photon_shade<<<sms * 8, 128, 0, st>>>(S, P, b, q[b & 1], c + CTR_COUNT, q[(b + 1) & 1], cn + CTR_COUNT, sp, sw,
                                                 sn, flags, prm.seed);
     }

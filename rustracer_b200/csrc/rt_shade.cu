@@ -9,6 +9,7 @@
 //   finalize  : fold the last parked contributions, write the pass output
 //   accumulate: accumulate_sample (src/main.rs:603-643) over the passes in order
 #include "rt_internal.h"
+#include "rt_media.cuh"
 
 using namespace rtd;
 
@@ -502,7 +503,10 @@ __global__ void k_zero_converged(const uint8_t* __restrict__ conv, uint32_t npix
 // Warp-aggregated appends (ballot + popc + one atomic per class per warp) into
 // one queue per class, so each shading kernel below runs one material's code:
 // no divergence between materials and a much smaller instruction footprint.
-RT_D int material_class(uint32_t ref) { return ref == RT_MISS_REF ? CLS_MISS : CLS_EMIT + (int)RT_HIT_CODE(ref); }
+RT_D int material_class(uint32_t ref) {
+    if (ref == RT_MISS_REF) return CLS_MISS;
+    return hit_is_medium(ref) ? CLS_MEDIUM : CLS_EMIT + (int)RT_HIT_CODE(ref);
+}
 
 #define CLS_BLOCK 256
 #define CLS_ITEMS 4
@@ -657,14 +661,25 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                 float emit_w = (prev_spec || !have_lights) ? 1.0f : prev_mis;
                 Lc = Lc + T * emission(S, S.mats[mat], tint, w, lam0, H) * emit_w;
             } else {
+                bool alive = true;
+                float3 sf = mk(1.f, 1.f, 1.f);
+                if constexpr (CLS == CLS_MEDIUM) {
+                    // medium scatter: HenyeyGreenstein::scatter (volume.rs:29-35), a
+                    // skip_pdf bounce of the specular branch (renderer.rs:421-456)
+                    float4 hv = A.hit[pid];
+                    const DevMedium& M = S.media[RT_HIT_INDEX(__float_as_uint(hv.x))];
+                    float3 p = o + hv.y * d;
+                    float3 dir = hg_sample(unit3(d), M.g, rnd(rng, b + B_SCATTER0), rnd(rng, b + B_SCATTER1));
+                    T = T * M.color;
+                    o = p; d = dir;
+                    prev_spec = true; prev_mis = 1.0f;
+                } else {
                 Surf sf_ = surface(S, A.hit[pid], o, d);
                 float3 p = sf_.p, nrm = sf_.nrm;
                 float t = sf_.t;
                 bool front = sf_.front;
                 const DevMaterial& m = S.mats[sf_.mat];
                 float3 udir = unit3(d);
-                bool alive = true;
-                float3 sf = mk(1.f, 1.f, 1.f);
                 if (CLS == CLS_DIELEC) {                                            // material.rs:133-149, 369-402
                     bool spectral = m.type == RT_MAT_SPECTRAL_DIELECTRIC;
                     float ior = spectral ? m.cauchy_b + m.cauchy_c / ((lam0 * 1e-3f) * (lam0 * 1e-3f)) : m.cauchy_b;
@@ -819,6 +834,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         prev_spec = false;
                     }
                 }
+                }   // surface
                 if (alive && depth >= 2) {                                          // renderer.rs:574-579
                     float3 eff = T * (CLS == CLS_DIFFUSE ? sf : spec_factor(S, tint, w, lam0, H));
                     float survive = fmaxf(fmaxf(eff.x, eff.y), eff.z);
@@ -923,6 +939,7 @@ void launch_shade(const DevScene& S, const PathState& A, const PathState& B, con
     RT_SHADE_CLASS(CLS_DIFFUSE);
     RT_SHADE_CLASS(CLS_METAL);
     RT_SHADE_CLASS(CLS_DIELEC);
+    if (S.n_media > 0) RT_SHADE_CLASS(CLS_MEDIUM);
 #undef RT_SHADE_CLASS
 }
 void launch_retire(const DevScene& S, const PathState& B, const PathState& Rt, const RenderLaunch& R, uint32_t* ctr,

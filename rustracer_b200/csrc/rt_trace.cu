@@ -14,6 +14,7 @@
 // by entry distance with a 19-comparator network on packed (t | slot) keys and
 // continues with the nearest while the others go on a per-thread stack.
 #include "rt_internal.h"
+#include "rt_media.cuh"
 
 using namespace rtd;
 
@@ -467,7 +468,17 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
             if (!more) {
                 active = false;
                 if (MODE == 0) {
-                    if (hit) T.pend[tag & 3u][tag >> 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (hit) {
+                        T.pend[tag & 3u][tag >> 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    } else if (S.n_media > 0) {
+                        // world.transmittance (bvh.rs:532-575): the media scale what got through
+                        float tr = media_transmittance(S, o, d, tmin, tmax);
+                        if (tr < 1.0f) {
+                            float4* pp = T.pend[tag & 3u] + (tag >> 2);
+                            float4 v = *pp;
+                            *pp = make_float4(v.x * tr, v.y * tr, v.z * tr, v.w);
+                        }
+                    }
                 } else {
                     out[item] = hit ? 1 : 0;
                 }
@@ -475,6 +486,57 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
         }
     }
     if (!ok) atomicExch(err, RT_ERR_CAPACITY);
+}
+
+// ── participating media next to the traversal ───────────────────────────────
+// A medium's scatter distance depends on the ray alone, so after the closest
+// hit each ray takes the nearest medium event before its surface hit (media
+// ids follow the primitives: a tie goes to the surface).
+// MODE 0: wavefront paths (dense set, wavelength in meta.w)
+// MODE 1: photons (queued, wavelength in ray_d.w)
+template <int MODE>
+__global__ void k_media(DevScene S, PathState P, const uint32_t* __restrict__ queue, const uint32_t* count) {
+    uint32_t n = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t pid = MODE == 1 ? queue[i] : i;
+        float4 ro = P.ray_o[pid], rd = P.ray_d[pid], hv = P.hit[pid];
+        float lam = MODE == 1 ? rd.w : __uint_as_float(P.meta[pid].w);
+        float3 o = mk(ro.x, ro.y, ro.z), d = mk(rd.x, rd.y, rd.z);
+        if (rtk::nan_ray(o, d, 0.001f, INFINITY)) continue;
+        float tsurf = __float_as_uint(hv.x) == RT_MISS_REF ? INFINITY : hv.y;
+        float tm;
+        int med = media_event(S, o, d, lam, 0.001f, tsurf, &tm);
+        if (med >= 0) P.hit[pid] = make_float4(__uint_as_float(RT_HIT_MEDIUM_BASE | (uint32_t)med), tm, 0.f, 0.f);
+    }
+}
+
+// API: rays n × 8 (o, d, t_min, t_max) with closest hits already in `out`
+// (fill_miss: there is no BVH, every ray starts as a miss)
+__global__ void k_media_api(DevScene S, const float* __restrict__ rays, uint32_t n, int4* out, int32_t n_prims,
+                            int fill_miss) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* r = rays + (size_t)i * 8;
+        float3 o = mk(r[0], r[1], r[2]), d = mk(r[3], r[4], r[5]);
+        if (fill_miss) out[i] = make_int4(-1, 0, 0, 0);
+        if (rtk::nan_ray(o, d, r[6], r[7])) continue;
+        int4 h = out[i];
+        float tsurf = h.x < 0 ? r[7] : __int_as_float(h.y);
+        float tm;
+        int med = media_event(S, o, d, 550.0f, r[6], tsurf, &tm);
+        if (med >= 0) out[i] = make_int4(n_prims + med, __float_as_int(tm), 0, 0);
+    }
+}
+
+// API: world.transmittance per ray, from the any-hit flags (NULL: no primitives)
+__global__ void k_transmittance_api(DevScene S, const float* __restrict__ rays, uint32_t n,
+                                    const uint8_t* __restrict__ occ, float* out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* r = rays + (size_t)i * 8;
+        float3 o = mk(r[0], r[1], r[2]), d = mk(r[3], r[4], r[5]);
+        float tr = (occ && occ[i]) ? 0.0f : 1.0f;
+        if (tr > 0.0f && S.n_media > 0 && !rtk::nan_ray(o, d, r[6], r[7])) tr = media_transmittance(S, o, d, r[6], r[7]);
+        out[i] = tr;
+    }
 }
 
 // ── host launchers ──────────────────────────────────────────────────────────
@@ -500,5 +562,18 @@ void launch_extend(const DevScene& S, const PathState& P, const uint32_t* queue,
 void launch_shadow(const DevScene& S, const PendTargets& T, const float4* sq, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st) {
     k_any<0><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, T, sq, nullptr, 0, count, next, nullptr, err);
+}
+void launch_media(const DevScene& S, const PathState& P, const uint32_t* queue, const uint32_t* count, int sms,
+                  cudaStream_t st) {
+    if (queue) k_media<1><<<sms * 8, 128, 0, st>>>(S, P, queue, count);
+    else       k_media<0><<<sms * 8, 128, 0, st>>>(S, P, nullptr, count);
+}
+void launch_media_api(const DevScene& S, const float* rays, uint32_t n, int4* out, int32_t n_prims, int fill_miss,
+                      int sms, cudaStream_t st) {
+    k_media_api<<<sms * 8, 128, 0, st>>>(S, rays, n, out, n_prims, fill_miss);
+}
+void launch_transmittance_api(const DevScene& S, const float* rays, uint32_t n, const uint8_t* occ, float* out,
+                              int sms, cudaStream_t st) {
+    k_transmittance_api<<<sms * 8, 128, 0, st>>>(S, rays, n, occ, out);
 }
 }  // namespace rth

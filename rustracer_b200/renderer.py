@@ -44,6 +44,7 @@ def lib():
         L.rt_scene_bvh_export.argtypes = [vp, C.POINTER(f), C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]
         L.rt_trace_closest.argtypes = [vp, vp, i64, vp, i32]
         L.rt_trace_any.argtypes = [vp, vp, i64, vp, i32]
+        L.rt_trace_transmittance.argtypes = [vp, vp, i64, vp, i32]
         L.rt_render_pass.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), vp, vp, i32]
         L.rt_render_accumulate.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), f, u32, f, i32,
                                            vp, vp, vp, i32]
@@ -176,6 +177,15 @@ class GpuScene:
         self._check(lib().rt_trace_any(self.h, C.c_void_p(rays.ctypes.data), len(rays), C.c_void_p(occ.ctypes.data),
                                        abi.RT_MEM_HOST))
         return occ
+
+    def trace_transmittance(self, rays):
+        """world.transmittance (bvh.rs:532-575) per ray: 0 behind an opaque
+        primitive, else the product of the media's transmittances."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32)
+        tr = np.zeros(len(rays), np.float32)
+        self._check(lib().rt_trace_transmittance(self.h, C.c_void_p(rays.ctypes.data), len(rays),
+                                                 C.c_void_p(tr.ctypes.data), abi.RT_MEM_HOST))
+        return tr
 
     # ── sample passes ────────────────────────────────────────────────────
     def render_pass(self, cam, params, out=None, converged=None):

@@ -170,6 +170,7 @@ class SceneBuilder:
         self.name = "scene"
         self.camera = None       # dict(look_from, look_at, vfov, aperture, focus_dist)
         self.caustics = None
+        self.media = []          # abi.RtMedium
 
     # materials ---------------------------------------------------------
     def add_material(self, m):
@@ -185,6 +186,33 @@ class SceneBuilder:
             r = r * xf.scale
         self.spheres.append((c.astype(F32), F32(r), mat))
         return len(self.spheres) - 1
+
+    # participating media (volume.rs:78-263, scene_file.rs:297-336) ------
+    def add_medium(self, kind, boundary, density, color, g=0.0, noise_scale=1.0, threshold=0.0, center=None,
+                   radius=None, p_min=None, p_max=None, seed=0):
+        """A constant ("constant") or Perlin-noise ("noise") medium inside a
+        sphere (center, radius) or an axis-aligned box (p_min, p_max).  The
+        noise medium's Perlin tables are drawn from `seed` (the reference draws
+        them from the thread RNG, perlin.rs:22-33)."""
+        m = abi.RtMedium()
+        m.type = {"constant": abi.RT_MEDIUM_CONSTANT, "noise": abi.RT_MEDIUM_NOISE}[kind]
+        m.boundary = {"sphere": abi.RT_BOUND_SPHERE, "box": abi.RT_BOUND_BOX}[boundary]
+        if boundary == "sphere":
+            m.center = _f3(center)
+            m.radius = float(radius)
+        else:
+            m.p_min = _f3(p_min)
+            m.p_max = _f3(p_max)
+        m.density = float(density)
+        m.color = _f3(color)
+        m.g = float(g)
+        m.noise_scale = float(noise_scale)
+        m.threshold = float(threshold)
+        vec, perm = perlin_tables(seed)
+        m.perlin_vec[:] = [float(x) for x in vec.reshape(-1)]
+        m.perlin_perm[:] = [int(x) for x in perm.reshape(-1)]
+        self.media.append(m)
+        return len(self.media) - 1
 
     def add_quad(self, corner, u, v, mat, xf=None):
         q, uu, vv = (np.asarray(a, dtype=np.float64) for a in (corner, u, v))
@@ -354,6 +382,9 @@ class SceneBuilder:
                     bg.visible_bottom = _f3(vis["bottom"])
         d.bg = bg
         d.spectral_range = int(self.spectral_range)
+        self._media = (abi.RtMedium * max(1, len(self.media)))(*self.media)
+        d.n_media = len(self.media)
+        d.media = C.cast(self._media, C.POINTER(abi.RtMedium)) if self.media else None
         self._desc = d
         return d
 
@@ -503,6 +534,27 @@ def _resolve(base, p):
     return cand if os.path.exists(cand) else p
 
 
+def perlin_tables(seed):
+    """Perlin::new (perlin.rs:22-33) from a seeded generator: 256 random unit
+    vectors (components uniform in [-1, 1), normalised) and three Fisher–Yates
+    permutations of 0..255."""
+    rng = np.random.default_rng(seed)
+    vec = rng.uniform(-1.0, 1.0, size=(256, 3)).astype(F32)
+    vec = (vec / np.linalg.norm(vec, axis=1, keepdims=True)).astype(F32)
+    perm = np.zeros((3, 256), np.int32)
+    for a in range(3):
+        p = np.arange(256)
+        for i in range(255, 0, -1):
+            j = int(rng.integers(0, i + 1))
+            p[i], p[j] = p[j], p[i]
+        perm[a] = p
+    return vec, perm
+
+
+_VOLUMES = {"constant_volume_sphere": ("constant", "sphere"), "constant_volume_box": ("constant", "box"),
+            "noise_volume_sphere": ("noise", "sphere"), "noise_volume_box": ("noise", "box")}
+
+
 def scene_from_toml_dict(doc, base="."):
     sb = SceneBuilder()
     sb.name = doc.get("name", "Custom Scene")
@@ -520,6 +572,16 @@ def scene_from_toml_dict(doc, base="."):
         raise ValueError(f"background type '{bg['type']}' is not supported by the GPU path")
     for i, obj in enumerate(doc.get("objects", [])):
         sh = obj["shape"]
+        if sh["type"] in _VOLUMES:                                  # scene_file.rs:962-983
+            kind, bound = _VOLUMES[sh["type"]]
+            xf = Transform(obj.get("scale"), obj.get("rotate"), obj.get("rotate_y"), obj.get("spin"), obj.get("translate"))
+            if not xf.identity:
+                raise ValueError(f"objects[{i}]: transformed volumes are not supported by the GPU path")
+            sb.add_medium(kind, bound, sh["density"], sh["color"], g=sh.get("g", 0.0),
+                          noise_scale=sh.get("noise_scale", 1.0), threshold=sh.get("threshold", 0.0),
+                          center=sh.get("center"), radius=sh.get("radius"), p_min=sh.get("p_min"),
+                          p_max=sh.get("p_max"), seed=i)
+            continue
         if "material" not in obj:
             raise ValueError(f"objects[{i}]: material is required for this shape type")
         mat = sb.add_material(_material_from_toml(obj["material"], base))

@@ -66,3 +66,14 @@ def tile_means(img, tile=16):
     """Per-tile mean over (H, W, 3) → (H/tile, W/tile, 3)."""
     h, w, _ = img.shape
     return img[: h // tile * tile, : w // tile * tile].reshape(h // tile, tile, w // tile, tile, 3).mean(axis=(1, 3))
+
+
+def medium_sphere_scene(density=1.0, blocker=False, kind="constant"):
+    """volume.rs:281-325: a medium in the unit sphere at the origin, optionally
+    with an opaque sphere (-2, 0, 0) r 0.5 in front of it."""
+    sb = SceneBuilder()
+    m = sb.add_material(Material.lambertian((0.5, 0.5, 0.5)))
+    sb.add_medium(kind, "sphere", density, (1, 1, 1), center=(0, 0, 0), radius=1.0)
+    if blocker:
+        sb.add_sphere((-2.0, 0.0, 0.0), 0.5, m)
+    return sb

@@ -1,0 +1,80 @@
+"""Participating media on the GPU against the CPU oracle: Beer–Lambert and
+noise transmittance through the shadow-ray API, medium scatter events in the
+closest hit, rendering through media, and photon tracing through media."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rustracer_b200 import configs, photons
+from rustracer_b200.renderer import GpuScene
+from tests.helpers import medium_sphere_scene, ray, rays
+from tests.test_gpu_render import assert_tiles_agree, render_both
+
+pytestmark = pytest.mark.gpu
+
+
+def test_gpu_beer_lambert_known_answers():
+    # volume.rs:280-325
+    g = GpuScene(medium_sphere_scene())
+    tr = g.trace_transmittance(rays(ray((-5, 0, 0), (1, 0, 0)), ray((-5, 5, 0), (1, 0, 0)),
+                                    ray((0, 0, 0), (1, 0, 0)), ray((0, 0, 0), (1, 0, 0), tmax=0.5)))
+    assert abs(tr[0] - math.exp(-2.0)) < 1e-6
+    assert tr[1] == 1.0
+    assert abs(tr[2] - math.exp(-0.999)) < 1e-6
+    assert abs(tr[3] - math.exp(-(0.5 - 0.001))) < 1e-5
+    assert g.trace_any(rays(ray((-5, 0, 0), (1, 0, 0))))[0] == 0
+    gb = GpuScene(medium_sphere_scene(blocker=True))
+    tr = gb.trace_transmittance(rays(ray((-5, 0, 0), (1, 0, 0)), ray((-5, 0.9, 0), (1, 0, 0))))
+    assert tr[0] == 0.0
+    assert abs(tr[1] - math.exp(-2.0 * math.sqrt(1.0 - 0.81))) < 1e-5
+
+
+def _media_rays(n, seed):
+    rng = np.random.default_rng(seed)
+    o = np.column_stack([rng.uniform(0.02, 0.98, n), rng.uniform(0.02, 0.98, n), np.full(n, -0.5)])
+    tgt = np.column_stack([rng.uniform(0, 1, n), rng.uniform(0, 1, n), np.full(n, 1.0)])
+    d = tgt - o
+    tmax = np.where(rng.random(n) < 0.5, np.inf, rng.uniform(0.3, 1.2, n))
+    return np.concatenate([o, d, np.full((n, 1), 0.001), tmax[:, None]], 1).astype(np.float32)
+
+
+def test_gpu_transmittance_matches_oracle():
+    sb, _ = configs.media_box_scene()
+    g, o = GpuScene(sb), O.OracleScene(sb)
+    r = _media_rays(20000, 1)
+    r[:, 2] = 0.999          # start inside the room, towards the back wall or the tmax cut
+    r[:, 5] = np.abs(r[:, 5]) * -1.0
+    a, b = g.trace_transmittance(r), o.trace_transmittance(r)
+    np.testing.assert_allclose(a, b, rtol=2e-4, atol=1e-6)
+    assert (b > 0).mean() > 0.3 and (b[b > 0] < 0.999).mean() > 0.3
+
+
+def test_gpu_medium_events_match_oracle():
+    sb, _ = configs.media_box_scene()
+    g, o = GpuScene(sb), O.OracleScene(sb)
+    r = _media_rays(20000, 2)
+    a, b = g.trace_closest(r), o.trace_closest(r)
+    n_prims = len(sb.quads) + len(sb.spheres)
+    assert (b["prim"] >= n_prims).mean() > 0.03                # a fair share scatters in a medium
+    same = a["prim"] == b["prim"]
+    assert same.mean() > 0.999
+    np.testing.assert_allclose(a["t"][same], b["t"][same], rtol=1e-4, atol=1e-6)
+
+
+def test_gpu_media_render_matches_oracle():
+    sb, st = configs.media_box_scene(width=64, height=64)
+    gi, oi, _ = render_both(sb, st, 64, 64, 64, 11, 12)
+    assert np.isfinite(gi).all()
+    assert_tiles_agree(gi, oi)
+
+
+def test_gpu_photons_through_media():
+    sb, st = configs.media_box_scene(width=64, height=64)
+    glass = sb.add_material(configs.Material.spectral_dielectric_cauchy(1.5, 0.0042))
+    sb.add_sphere((0.5, 0.75, 0.5), 0.12, glass)
+    g, o = GpuScene(sb), O.OracleScene(sb)
+    p = photons.caustic_params(sb, 200000, 0.05, seed=4)
+    ng, no = g.photon_build(p), o.photon_build(p)
+    assert ng > 100 and abs(ng - no) <= max(30, no // 20), (ng, no)
