@@ -417,12 +417,14 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
 
 // MODE 0: wavefront shadow rays (an occluded ray cancels its parked contribution)
 // MODE 1: API any-hit (occluded flags)
+// MODE 2: wavefront shadow rays in a scene with media (an unoccluded ray scales
+//         its parked contribution by the media's transmittance)
 template <int MODE>
 __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene S, PendTargets T, const float4* __restrict__ sq,
                                                         const float* __restrict__ rays, uint32_t n_api,
                                                         const uint32_t* count, uint32_t* next,
                                                         uint8_t* __restrict__ out, int* err) {
-    const uint32_t n = MODE == 0 ? *count : n_api;
+    const uint32_t n = MODE != 1 ? *count : n_api;
     const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
     uint32_t stack[RT_STACK];
     bool active = false, exhausted = false, ok = true;
@@ -443,7 +445,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
                 uint32_t i = base + __popc(idle & lt);
                 if (i < n) {
                     item = i;
-                    if (MODE == 0) {
+                    if (MODE != 1) {
                         float4 a = sq[(size_t)i * 2], b = sq[(size_t)i * 2 + 1];
                         o = mk(a.x, a.y, a.z); d = mk(b.x, b.y, b.z);
                         tmin = 0.001f; tmax = a.w;
@@ -467,10 +469,10 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
             if (!lok) ok = false;
             if (!more) {
                 active = false;
-                if (MODE == 0) {
+                if (MODE != 1) {
                     if (hit) {
                         T.pend[tag & 3u][tag >> 2] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    } else if (S.n_media > 0) {
+                    } else if (MODE == 2) {
                         // world.transmittance (bvh.rs:532-575): the media scale what got through
                         float tr = media_transmittance(S, o, d, tmin, tmax);
                         if (tr < 1.0f) {
@@ -561,7 +563,8 @@ void launch_extend(const DevScene& S, const PathState& P, const uint32_t* queue,
 }
 void launch_shadow(const DevScene& S, const PendTargets& T, const float4* sq, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st) {
-    k_any<0><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, T, sq, nullptr, 0, count, next, nullptr, err);
+    if (S.n_media > 0) k_any<2><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, T, sq, nullptr, 0, count, next, nullptr, err);
+    else               k_any<0><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, T, sq, nullptr, 0, count, next, nullptr, err);
 }
 void launch_media(const DevScene& S, const PathState& P, const uint32_t* queue, const uint32_t* count, int sms,
                   cudaStream_t st) {
