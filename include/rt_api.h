@@ -84,6 +84,8 @@ typedef struct RtMaterial {
 #define RT_BG_SOLID     0
 #define RT_BG_GRADIENT  1
 #define RT_BG_ENVMAP    2   /* EnvMap, or EnvMapSplit when visible_type >= 0 */
+#define RT_BG_PHYSICAL  3   /* Preetham sky with a sun disc (renderer.rs:231-337): sun NEE at
+                               diffuse and rough-conductor vertices (renderer.rs:421-456, 495-518) */
 
 typedef struct RtBackground {
     int32_t      type;            /* RT_BG_* */
@@ -99,6 +101,10 @@ typedef struct RtBackground {
     float        visible_color[3];
     float        visible_top[3];
     float        visible_bottom[3];
+    /* RT_BG_PHYSICAL: unit direction towards the sun and the turbidity
+     * (scene_file.rs:917-927 builds sun_dir from azimuth and elevation) */
+    float        sun_dir[3];
+    float        turbidity;
 } RtBackground;
 
 /* ── scene description ───────────────────────────────────────────────────── *
@@ -254,6 +260,8 @@ int32_t rt_render_accumulate(RtScene* scene, const RtCamera* cam, const RtPassPa
 /* ── caustic photon map (src/photon.rs, src/scene.rs:35-74) ──────────────── */
 #define RT_EMIT_DISK     0   /* directional disk facing `dir` (PhotonMap::build, photon.rs:41-94) */
 #define RT_EMIT_QUAD     1   /* cosine-weighted quad (PhotonMap::build_from_quad, photon.rs:97-135) */
+#define RT_EMIT_SUN      2   /* the Physical sky's sun: a disk facing sun_dir with the sky radiance at
+                                the sun direction nudged by 0.04, ×π (scene.rs:40-52); dir/color unused */
 #define RT_MAX_EMITTERS  8
 
 typedef struct RtPhotonEmitter {

@@ -37,6 +37,8 @@ def lib():
         L.orc_trace_stats.argtypes = [vp, fp, i64, C.POINTER(i64), i32]
         L.orc_trace_transmittance.argtypes = [vp, fp, i64, fp, i32]
         L.orc_hg_sample.argtypes = [fp, i64, fp]
+        L.orc_bg_eval_n.argtypes = [vp, fp, i64, fp, fp]
+        L.orc_sun_sample.argtypes = [vp, fp, i64, fp]
         L.orc_render_pass.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), fp,
                                       C.POINTER(C.c_uint8), i32, u32, u32, C.POINTER(i64)]
         L.orc_accumulate.argtypes = [fp, fp, C.POINTER(u32), fp, C.POINTER(C.c_uint8), i64, f, u32, f]
@@ -174,6 +176,20 @@ class OracleScene:
         rays = _f(rays).reshape(-1, 8)
         out = np.zeros(len(rays), np.float32)
         lib().orc_trace_transmittance(self.h, _fp(rays), len(rays), _fp(out), threads)
+        return out
+
+    def bg_eval_n(self, dirs):
+        """Background::eval (renderer.rs:196-208) and the sun pdf per direction."""
+        dirs = _f(dirs).reshape(-1, 3)
+        rgb = np.zeros((len(dirs), 3), np.float32)
+        pdf = np.zeros(len(dirs), np.float32)
+        lib().orc_bg_eval_n(self.h, _fp(dirs), len(dirs), _fp(rgb), _fp(pdf))
+        return rgb, pdf
+
+    def sun_sample(self, r):
+        r = _f(r).reshape(-1, 2)
+        out = np.zeros((len(r), 3), np.float32)
+        lib().orc_sun_sample(self.h, _fp(r), len(r), _fp(out))
         return out
 
     def trace_stats(self, rays, threads=os.cpu_count()):

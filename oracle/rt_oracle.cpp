@@ -146,6 +146,7 @@ enum {
     D_JIT_U = 0, D_JIT_V = 1, D_LENS_R = 2, D_LENS_P = 3, D_TIME = 4, D_LAMBDA = 5,
     D_BOUNCE0 = 8, D_PER_BOUNCE = 16,
     B_SCATTER0 = 0, B_SCATTER1 = 1, B_LPICK = 2, B_LPT0 = 3, B_LPT1 = 4,
+    B_SUN0 = 5, B_SUN1 = 6,
     B_ENV_ROW = 7, B_ENV_COL = 8, B_ENV_JU = 9, B_ENV_JV = 10, B_COS0 = 11, B_COS1 = 12, B_RR = 13,
 };
 
@@ -1127,6 +1128,78 @@ static V3 env_sample_dir(const EnvMap& e, float x1, float x2, float x3, float x4
     *pdf = env_pdf_at(e, i, j);
     return dir;
 }
+// ── Physical sky (renderer.rs:18, 231-362) ──────────────────────────────────
+static const float COS_SUN_MAX = 0.9999892f;
+static inline float perez(float a, float b, float c, float dp, float e, float ct, float g, float cg) {
+    return (1.0f + a * std::exp(b / ct)) * (1.0f + c * std::exp(dp * g) + e * cg * cg);
+}
+// preetham_sky (renderer.rs:231-337)
+static V3 preetham_sky(V3 dir, V3 sun_dir, float turbidity) {
+    V3 d = unit(dir), sun = unit(sun_dir);
+    float cos_gamma = clampf(dot(d, sun), -1.0f, 1.0f);
+    float gamma = std::acos(cos_gamma);
+    float t = clampf(turbidity, 1.7f, 20.0f);
+    float cos_theta_s = rmax(sun.y, 0.0175f);
+    float theta_s = std::acos(cos_theta_s);
+    float ay = 0.1787f * t - 1.4630f, by = -0.3554f * t + 0.4275f, cy = 0.0227f * t + 5.3251f,
+          dy = 0.1206f * t - 2.5771f, ey = -0.0670f * t + 0.3703f;
+    float ax = -0.0193f * t - 0.2592f, bx = -0.0665f * t + 0.0008f, cx = -0.0004f * t + 0.2125f,
+          dx = -0.0641f * t - 0.8989f, ex = -0.0033f * t + 0.0452f;
+    float acy = -0.0167f * t - 0.2608f, bcy = -0.0950f * t + 0.0092f, ccy = -0.0079f * t + 0.2102f,
+          dcy = -0.0441f * t - 1.6537f, ecy = -0.0109f * t + 0.0529f;
+    float fn_y = perez(ay, by, cy, dy, ey, 1.0f, theta_s, cos_theta_s);
+    float fn_x = perez(ax, bx, cx, dx, ex, 1.0f, theta_s, cos_theta_s);
+    float fn_cy = perez(acy, bcy, ccy, dcy, ecy, 1.0f, theta_s, cos_theta_s);
+    float yz = rmax((4.0453f * t - 4.9710f) * std::tan((4.0f / 9.0f - t / 120.0f) * (PI_F - 2.0f * theta_s))
+                    - 0.2155f * t + 2.4192f, 0.0f);
+    if (cos_gamma > COS_SUN_MAX && sun.y > 0.0f && d.y > 0.0f) {
+        float disc = yz * 111.0f;
+        return v3(disc, disc * 0.95f, disc * 0.85f);
+    }
+    float ts = theta_s, ts2 = ts * ts, ts3 = ts2 * ts;
+    float xz = t * t * (0.00166f * ts3 - 0.00375f * ts2 + 0.00209f * ts)
+             + t * (-0.02903f * ts3 + 0.06377f * ts2 - 0.03202f * ts + 0.00394f)
+             + (0.11693f * ts3 - 0.21196f * ts2 + 0.06052f * ts + 0.25886f);
+    float yzc = t * t * (0.00275f * ts3 - 0.00610f * ts2 + 0.00317f * ts)
+              + t * (-0.04214f * ts3 + 0.08970f * ts2 - 0.04153f * ts + 0.00516f)
+              + (0.15346f * ts3 - 0.26756f * ts2 + 0.06670f * ts + 0.26688f);
+    float ct = rmax(d.y, 0.001f);
+    float fy = perez(ay, by, cy, dy, ey, ct, gamma, cos_gamma);
+    float fx = perez(ax, bx, cx, dx, ex, ct, gamma, cos_gamma);
+    float fcy = perez(acy, bcy, ccy, dcy, ecy, ct, gamma, cos_gamma);
+    float cap_y = rmax(yz * fy / fn_y, 0.0f);
+    float cap_x = clampf(xz * fx / fn_x, 0.001f, 0.998f);
+    float cap_yc = clampf(yzc * fcy / fn_cy, 0.001f, 0.998f);
+    float lum = cap_y * 0.05f;
+    float big_x = cap_x / cap_yc * lum, big_y = lum;
+    float big_z = rmax((1.0f - cap_x - cap_yc) / cap_yc * lum, 0.0f);
+    V3 sky = v3(rmax(3.2406f * big_x - 1.5372f * big_y - 0.4986f * big_z, 0.0f),
+                rmax(-0.9689f * big_x + 1.8758f * big_y + 0.0415f * big_z, 0.0f),
+                rmax(0.0557f * big_x - 0.2040f * big_y + 1.0570f * big_z, 0.0f));
+    if (d.y < 0.0f) {
+        float tt = rmin(-d.y * 8.0f, 1.0f);
+        return sky * (1.0f - tt) + v3(0.07f, 0.06f, 0.05f) * tt;
+    }
+    return sky;
+}
+static inline bool has_sun(const Scene& s) { return s.bg.type == RT_BG_PHYSICAL && s.bg.sun_dir[1] > 0.0f; }
+static inline V3 sun_vec(const Scene& s) { return v3(s.bg.sun_dir[0], s.bg.sun_dir[1], s.bg.sun_dir[2]); }
+// sun_pdf_value (renderer.rs:340-348)
+static float sun_pdf_value(const Scene& s, V3 dir) {
+    if (has_sun(s) && dot(unit(dir), unit(sun_vec(s))) > COS_SUN_MAX) return 1.0f / (2.0f * PI_F * (1.0f - COS_SUN_MAX));
+    return 0.0f;
+}
+// sample_sun_cone (renderer.rs:351-362)
+static V3 sample_sun_cone(V3 axis, float cos_max, float r1, float r2) {
+    float cos_t = 1.0f - r1 * (1.0f - cos_max);
+    float sin_t = std::sqrt(rmax(1.0f - cos_t * cos_t, 0.0f));
+    float phi = 2.0f * PI_F * r2;
+    V3 up = std::fabs(axis.x) < 0.999f ? v3(1, 0, 0) : v3(0, 1, 0);
+    V3 t = unit(cross(axis, up));
+    V3 b = cross(axis, t);
+    return t * (sin_t * std::cos(phi)) + b * (sin_t * std::sin(phi)) + axis * cos_t;
+}
+
 static V3 bg_eval_type(int type, const float* color, const float* top, const float* bottom, V3 dir) {
     if (type == RT_BG_SOLID) return v3(color[0], color[1], color[2]);
     float t = (clampf(dir.y, -1.0f, 1.0f) + 1.0f) * 0.5f;                           // renderer.rs:200-203
@@ -1138,6 +1211,7 @@ static V3 bg_eval(const Scene& s, V3 dir) {                                     
         if (b.visible_type >= 0) return bg_eval_type(b.visible_type, b.visible_color, b.visible_top, b.visible_bottom, dir);
         return env_sample(s.env, dir);
     }
+    if (b.type == RT_BG_PHYSICAL) return preetham_sky(dir, v3(b.sun_dir[0], b.sun_dir[1], b.sun_dir[2]), b.turbidity);
     return bg_eval_type(b.type, b.color, b.top, b.bottom, dir);
 }
 static V3 env_eval(const Scene& s, V3 dir) { return s.has_env ? env_sample(s.env, dir) : v3(0, 0, 0); }
@@ -1349,14 +1423,38 @@ static inline Rng photon_rng(uint64_t seed, uint32_t gid) {
 // photon_bounds of the world (hittable.rs:199-212): union of the primitive boxes
 static Aabb world_bounds(const Scene& s) {
     int64_t n = s.n_tris + s.n_quads + s.n_spheres;
-    Aabb b = prim_box(s, 0);
+    bool any = n > 0;
+    Aabb b = any ? prim_box(s, 0) : Aabb{v3(0, 0, 0), v3(0, 0, 0)};
     for (int64_t i = 1; i < n; i++) b = surrounding(b, prim_box(s, i));
+    for (const RtMedium& m : s.media) {                                            // volume.rs:152-154
+        Aabb mb;
+        if (m.boundary == RT_BOUND_BOX)
+            mb = Aabb{v3(rmin(m.p_min[0], m.p_max[0]), rmin(m.p_min[1], m.p_max[1]), rmin(m.p_min[2], m.p_max[2])),
+                      v3(rmax(m.p_min[0], m.p_max[0]), rmax(m.p_min[1], m.p_max[1]), rmax(m.p_min[2], m.p_max[2]))};
+        else
+            mb = Aabb{v3(m.center[0] - m.radius, m.center[1] - m.radius, m.center[2] - m.radius),
+                      v3(m.center[0] + m.radius, m.center[1] + m.radius, m.center[2] + m.radius)};
+        b = any ? surrounding(b, mb) : mb;
+        any = true;
+    }
     return b;
 }
 
 // Emitter geometry for photon `i` of emitter `e` (photon.rs:41-94, 97-135).
 struct EmitterSetup { V3 t, b, center, dir, power, normal, corner, u, v, ta, ba; float radius, lum_clamp; int type; };
-static EmitterSetup setup_emitter(const Scene& s, const RtPhotonEmitter& e) {
+static EmitterSetup setup_emitter(const Scene& s, const RtPhotonEmitter& e0) {
+    RtPhotonEmitter e = e0;
+    if (e.type == RT_EMIT_SUN) {
+        // rebuild_caustics with a Physical sky (scene.rs:40-52): the sun as a disk
+        // emitter, coloured by the sky radiance 0.04 off the sun direction, ×π
+        V3 sun = sun_vec(s);
+        V3 perp = std::fabs(sun.x) < 0.9f ? unit(v3(0.0f, -sun.z, sun.y)) : unit(v3(-sun.z, 0.0f, sun.x));
+        V3 power_dir = unit(sun + perp * 0.04f);
+        V3 col = bg_eval(s, power_dir) * PI_F;
+        e.type = RT_EMIT_DISK;
+        e.dir[0] = sun.x; e.dir[1] = sun.y; e.dir[2] = sun.z;
+        e.color[0] = col.x; e.color[1] = col.y; e.color[2] = col.z;
+    }
     EmitterSetup E{};
     E.type = e.type;
     if (e.type == RT_EMIT_DISK) {
@@ -1494,8 +1592,9 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
             prev_specular = true;
             prev_mis_w_brdf = 1.0f;
         } else if (h.gid < 0) {
-            float env_pdf = env_pdf_value(s, ray.d);                                // no sun: sun_pdf = 0
-            float emit_w = (env_pdf == 0.0f) ? 1.0f : (prev_specular ? prev_spec_sun_weight : prev_mis_w_brdf);
+            float sun_pdf = sun_pdf_value(s, ray.d);
+            float env_pdf = env_pdf_value(s, ray.d);
+            float emit_w = (sun_pdf + env_pdf == 0.0f) ? 1.0f : (prev_specular ? prev_spec_sun_weight : prev_mis_w_brdf);
             V3 bg = (depth == 0 || !s.has_env) ? bg_eval(s, ray.d) : env_eval(s, ray.d);
             color = color + T * (bg * spec_factor(s.spec, ss)) * bg_scale * emit_w;
             break;
@@ -1570,6 +1669,41 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                 float lam_i = smith_lambda(rmax(dot(dir, n), 0.0f), alpha);
                 weight = ((1.0f + lam_o) / (1.0f + lam_o + lam_i)) * specular_energy_comp(cos_o, alpha);
             }
+            // specular sun NEE (renderer.rs:421-456) with SpectralMetal::specular_brdf_cos /
+            // specular_sampling_pdf (material.rs:504-551); zero for a smooth conductor
+            prev_spec_sun_weight = 1.0f;
+            if (has_sun(s) && m.roughness != 0.0f) {
+                const float p_sun = 1.0f / (2.0f * PI_F * (1.0f - COS_SUN_MAX));
+                V3 sun_s = sample_sun_cone(unit(sun_vec(s)), COS_SUN_MAX, rnd(rng, base + B_SUN0), rnd(rng, base + B_SUN1));
+                float cos_i = dot(sun_s, n);
+                if (cos_o > 0.0f && cos_i > 0.0f) {
+                    V3 hh = unit(wo + sun_s);
+                    float wo_h = rmax(dot(wo, hh), 0.0f), h_n = rmax(dot(hh, n), 0.0f);
+                    float D = ggx_ndf(h_n, alpha);
+                    float g2 = 1.0f / (1.0f + smith_lambda(cos_o, alpha) + smith_lambda(cos_i, alpha));
+                    float comp = specular_energy_comp(cos_o, alpha);
+                    SpecState sv = ss;
+                    for (int i = 0; i < ss.H; i++) {
+                        if (ss.w[i] == 0.0f) continue;
+                        float nn, kk;
+                        metal_ior(m, ss.lam[i], &nn, &kk);
+                        sv.w[i] = ss.w[i] * (D * fresnel_conductor(wo_h, nn, kk) * g2 / (4.0f * cos_o) * comp);
+                    }
+                    if (sv.tint == TINT_NONE) sv.tint = TINT_CMF;
+                    V3 brdf_cos = spec_factor(s.spec, sv);
+                    (*n_shadow)++;
+                    float tr = scene_transmittance(s, Ray{rec.p, sun_s}, 0.001f, INFINITY);
+                    if (tr > 0.0f && (brdf_cos.x > 0.0f || brdf_cos.y > 0.0f || brdf_cos.z > 0.0f)) {
+                        float p_mat = ggx_ndf(h_n, alpha) * smith_g1(cos_o, alpha) / (4.0f * cos_o);
+                        V3 sun_color = bg_eval(s, sun_s);
+                        float mis_d = p_sun * p_sun + p_mat * p_mat;
+                        if (mis_d > 0.0f) color = color + T * tr * brdf_cos * sun_color * p_sun / mis_d;
+                    }
+                }
+                V3 hb = unit(wo + dir);
+                float p_b = (dot(dir, n) > 0.0f) ? ggx_ndf(rmax(dot(hb, n), 0.0f), alpha) * smith_g1(cos_o, alpha) / (4.0f * cos_o) : 0.0f;
+                if (p_b > 0.0f) prev_spec_sun_weight = (p_b * p_b) / rmax(p_b * p_b + p_sun * p_sun, 1e-8f);
+            }
             for (int i = 0; i < ss.H; i++) {
                 if (ss.w[i] == 0.0f) continue;
                 float nn, kk;
@@ -1577,7 +1711,6 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                 ss.w[i] *= fresnel_conductor(cos_h, nn, kk);
             }
             if (ss.tint == TINT_NONE) ss.tint = TINT_CMF;
-            prev_spec_sun_weight = 1.0f;
             T = T * weight;
             ray = Ray{rec.p, dir};
             prev_specular = true;
@@ -1601,12 +1734,28 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                     if (tr > 0.0f) {
                         float l_pdf = lights_pdf_value(s, rec.p, light_dir);
                         float brdf = rmax(dot(rec.normal, unit(light_dir)) / PI_F, 0.0f);
+                        float sun_p = sun_pdf_value(s, light_dir);
                         float env_p = env_pdf_value(s, light_dir);
-                        float mis_d = l_pdf * l_pdf + brdf * brdf + env_p * env_p;
+                        float mis_d = l_pdf * l_pdf + brdf * brdf + sun_p * sun_p + env_p * env_p;
                         if (mis_d > 0.0f && brdf > 0.0f) {
                             V3 nee = emission(s, lrec.mat, ss);
                             color = color + T * tr * att * brdf * l_pdf * nee / mis_d;
                         }
+                    }
+                }
+            }
+            if (has_sun(s)) {                                                       // renderer.rs:495-518
+                V3 sun_s = sample_sun_cone(unit(sun_vec(s)), COS_SUN_MAX, rnd(rng, base + B_SUN0), rnd(rng, base + B_SUN1));
+                (*n_shadow)++;
+                float tr = scene_transmittance(s, Ray{rec.p, sun_s}, 0.001f, INFINITY);
+                if (tr > 0.0f) {
+                    float brdf = rmax(dot(rec.normal, unit(sun_s)) / PI_F, 0.0f);
+                    if (brdf > 0.0f) {
+                        float sun_pdf = 1.0f / (2.0f * PI_F * (1.0f - COS_SUN_MAX));
+                        V3 sun_color = bg_eval(s, sun_s) * spec_factor(s.spec, ss);
+                        float area_pdf = have_lights ? lights_pdf_value(s, rec.p, sun_s) : 0.0f;
+                        float mis_d = sun_pdf * sun_pdf + brdf * brdf + area_pdf * area_pdf;
+                        color = color + T * tr * att * brdf * sun_pdf * sun_color / mis_d;
                     }
                 }
             }
@@ -1641,8 +1790,9 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
             if (scat_pdf <= 0.0f) break;
             if (dot(ind_dir, rec.normal) <= 0.0f) break;
             float area = have_lights ? lights_pdf_value(s, rec.p, ind_dir) : 0.0f;
+            float sun = sun_pdf_value(s, ind_dir);
             float env = env_pdf_value(s, ind_dir);
-            float nee_sq = area * area + env * env;
+            float nee_sq = area * area + sun * sun + env * env;
             prev_mis_w_brdf = (pdf_val * pdf_val) / rmax(pdf_val * pdf_val + nee_sq, 1e-8f);
             T = T * (att * (scat_pdf / pdf_val));
             ray = Ray{rec.p, ind_dir};
@@ -1891,6 +2041,27 @@ int32_t orc_trace_transmittance(void* sp, const float* rays, int64_t n, float* t
     return RT_OK;
 }
 
+// Background::eval for n directions (renderer.rs:196-208), and the sun pdf
+int32_t orc_bg_eval_n(void* sp, const float* dirs, int64_t n, float* rgb, float* sun_pdf) {
+    Scene* s = (Scene*)sp;
+    for (int64_t i = 0; i < n; i++) {
+        V3 d = v3(dirs[i * 3], dirs[i * 3 + 1], dirs[i * 3 + 2]);
+        V3 c = bg_eval(*s, d);
+        rgb[i * 3] = c.x; rgb[i * 3 + 1] = c.y; rgb[i * 3 + 2] = c.z;
+        if (sun_pdf) sun_pdf[i] = sun_pdf_value(*s, d);
+    }
+    return RT_OK;
+}
+// sample_sun_cone around the scene's sun for n (r1, r2) pairs
+int32_t orc_sun_sample(void* sp, const float* r, int64_t n, float* dirs) {
+    Scene* s = (Scene*)sp;
+    for (int64_t i = 0; i < n; i++) {
+        V3 d = sample_sun_cone(unit(sun_vec(*s)), COS_SUN_MAX, r[i * 2], r[i * 2 + 1]);
+        dirs[i * 3] = d.x; dirs[i * 3 + 1] = d.y; dirs[i * 3 + 2] = d.z;
+    }
+    return RT_OK;
+}
+
 // hg_sample for n (w, g, xi1, xi2) rows of 6 floats → n × 3 directions
 int32_t orc_hg_sample(const float* in, int64_t n, float* out) {
     for (int64_t i = 0; i < n; i++) {
@@ -2064,7 +2235,10 @@ int32_t orc_photon_build(void* sp, const RtPhotonParams* p, int64_t* n_stored, i
     Scene* s = (Scene*)sp;
     if (!p || p->n_emitters < 0 || p->n_emitters > RT_MAX_EMITTERS || !(p->gather_radius > 0.0f)) return RT_ERR_INVALID;
     uint32_t total = 0;
-    for (int e = 0; e < p->n_emitters; e++) total += p->emitters[e].n_photons;
+    for (int e = 0; e < p->n_emitters; e++) {
+        if (p->emitters[e].type == RT_EMIT_SUN && s->bg.type != RT_BG_PHYSICAL) return RT_ERR_INVALID;
+        total += p->emitters[e].n_photons;
+    }
     std::vector<KdPhoton> slot(total);
     std::vector<uint8_t> ok(total, 0);
     uint32_t off = 0;

@@ -18,7 +18,7 @@ RT_MAT_BLACKBODY_LIGHT = 6
 RT_METAL_GOLD, RT_METAL_COPPER, RT_METAL_SILVER, RT_METAL_CUSTOM = 0, 1, 2, 3
 RT_MAX_NK = 16
 
-RT_BG_SOLID, RT_BG_GRADIENT, RT_BG_ENVMAP = 0, 1, 2
+RT_BG_SOLID, RT_BG_GRADIENT, RT_BG_ENVMAP, RT_BG_PHYSICAL = 0, 1, 2, 3
 RT_PRIM_TRI, RT_PRIM_QUAD, RT_PRIM_SPHERE = 0, 1, 2
 
 F3 = C.c_float * 3
@@ -59,6 +59,8 @@ class RtBackground(C.Structure):
         ("visible_color", F3),
         ("visible_top", F3),
         ("visible_bottom", F3),
+        ("sun_dir", F3),
+        ("turbidity", C.c_float),
     ]
 
 
@@ -154,7 +156,7 @@ def iptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_int32))
 
 
-RT_EMIT_DISK, RT_EMIT_QUAD = 0, 1
+RT_EMIT_DISK, RT_EMIT_QUAD, RT_EMIT_SUN = 0, 1, 2
 RT_MAX_EMITTERS = 8
 
 

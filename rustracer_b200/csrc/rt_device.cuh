@@ -108,6 +108,11 @@ struct DevScene {
     float bg_color[3], bg_top[3], bg_bottom[3];
     int   vis_type;
     float vis_color[3], vis_top[3], vis_bottom[3];
+    // Physical sky (renderer.rs:231-362): unit sun direction, turbidity, and
+    // whether the sun is above the horizon (sun NEE and the sun pdf need it)
+    float3 sun_dir;
+    float  turbidity;
+    int    has_sun;
 };
 
 // ── float3 helpers ──────────────────────────────────────────────────────────
@@ -158,6 +163,7 @@ enum {
     D_JIT_U = 0, D_JIT_V = 1, D_LENS_R = 2, D_LENS_P = 3, D_TIME = 4, D_LAMBDA = 5,
     D_BOUNCE0 = 8, D_PER_BOUNCE = 16,
     B_SCATTER0 = 0, B_SCATTER1 = 1, B_LPICK = 2, B_LPT0 = 3, B_LPT1 = 4,
+    B_SUN0 = 5, B_SUN1 = 6,
     B_ENV_ROW = 7, B_ENV_COL = 8, B_ENV_JU = 9, B_ENV_JV = 10, B_COS0 = 11, B_COS1 = 12, B_RR = 13,
 };
 

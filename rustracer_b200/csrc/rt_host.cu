@@ -14,6 +14,7 @@
 
 #include "../../include/rt_spectral_tables.h"
 #include "rt_internal.h"
+#include "rt_sky.cuh"
 
 using namespace rtd;
 
@@ -828,8 +829,19 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
 
     // ── background + env alias table (renderer.rs:32-74) ────────────────────
     const RtBackground& bg = d->bg;
+    if (bg.type < RT_BG_SOLID || bg.type > RT_BG_PHYSICAL) return bail(fail(s, RT_ERR_INVALID, "unknown background type"));
     s->S.bg_type = bg.type;
     s->S.vis_type = bg.type == RT_BG_ENVMAP ? bg.visible_type : -1;
+    if (bg.type == RT_BG_PHYSICAL) {
+        float3 sd = make_float3(bg.sun_dir[0], bg.sun_dir[1], bg.sun_dir[2]);
+        float l2 = sd.x * sd.x + sd.y * sd.y + sd.z * sd.z;
+        if (!(l2 > 0.0f) || !std::isfinite(l2) || !std::isfinite(bg.turbidity))
+            return bail(fail(s, RT_ERR_INVALID, "Physical sky needs a finite non-zero sun direction and turbidity"));
+        float l = std::sqrt(l2);
+        s->S.sun_dir = make_float3(sd.x / l, sd.y / l, sd.z / l);
+        s->S.turbidity = bg.turbidity;
+        s->S.has_sun = bg.sun_dir[1] > 0.0f;
+    }
     for (int k = 0; k < 3; k++) {
         s->S.bg_color[k] = bg.color[k]; s->S.bg_top[k] = bg.top[k]; s->S.bg_bottom[k] = bg.bottom[k];
         s->S.vis_color[k] = bg.visible_color[k]; s->S.vis_top[k] = bg.visible_top[k]; s->S.vis_bottom[k] = bg.visible_bottom[k];
@@ -1523,8 +1535,21 @@ extern "C" int32_t rt_render_pass_noalloc(RtScene* s, const RtCamera* cam, const
 // ── photon map entry points ──────────────────────────────────────────────────
 // Emitter set-up of PhotonMap::build / build_from_quad (photon.rs:41-135):
 // 40 floats per emitter, consumed by the emission kernel.
-static void emitter_setup(const RtScene* s, const RtPhotonEmitter& e, float* f) {
+static void emitter_setup(const RtScene* s, const RtPhotonEmitter& e0, float* f) {
     const float PI = 3.14159265358979323846f;
+    RtPhotonEmitter e = e0;
+    if (e.type == RT_EMIT_SUN) {
+        // rebuild_caustics with a Physical sky (scene.rs:40-52): a disk facing the
+        // sun, coloured by the sky radiance 0.04 off the sun direction, ×π
+        float3 sun = s->S.sun_dir;
+        float3 perp = std::fabs(sun.x) < 0.9f ? rtd::sky_unit(make_float3(0.0f, -sun.z, sun.y))
+                                              : rtd::sky_unit(make_float3(-sun.z, 0.0f, sun.x));
+        float3 pd = rtd::sky_unit(make_float3(sun.x + perp.x * 0.04f, sun.y + perp.y * 0.04f, sun.z + perp.z * 0.04f));
+        float3 col = rtd::preetham_sky(pd, sun, s->S.turbidity);
+        e.type = RT_EMIT_DISK;
+        e.dir[0] = sun.x; e.dir[1] = sun.y; e.dir[2] = sun.z;
+        e.color[0] = col.x * PI; e.color[1] = col.y * PI; e.color[2] = col.z * PI;
+    }
     memset(f, 0, 40 * sizeof(float));
     auto put = [&](int at, H3 v) { f[at] = v.x; f[at + 1] = v.y; f[at + 2] = v.z; };
     if (e.type == RT_EMIT_DISK) {
@@ -1572,7 +1597,10 @@ extern "C" int32_t rt_photon_build(RtScene* s, const RtPhotonParams* p, int64_t*
     uint64_t total = 0;
     for (int i = 0; i < p->n_emitters; i++) {
         const RtPhotonEmitter& e = p->emitters[i];
-        if (e.type != RT_EMIT_DISK && e.type != RT_EMIT_QUAD) return fail(s, RT_ERR_INVALID, "unknown emitter type");
+        if (e.type != RT_EMIT_DISK && e.type != RT_EMIT_QUAD && e.type != RT_EMIT_SUN)
+            return fail(s, RT_ERR_INVALID, "unknown emitter type");
+        if (e.type == RT_EMIT_SUN && s->S.bg_type != RT_BG_PHYSICAL)
+            return fail(s, RT_ERR_INVALID, "a sun emitter needs a Physical sky background");
         if (e.n_photons == 0) return fail(s, RT_ERR_INVALID, "emitter with zero photons");
         total += e.n_photons;
     }

@@ -735,7 +735,7 @@ cudaError_t photon_build(const DevScene& S, PhotonMapDev& map, const PathState& 
     for (int i = 0; i < prm.n_emitters; i++) {
         const float* f = emit_setup + i * 40;
         EmitSetup& x = E.e[i];
-        x.type = prm.emitters[i].type;
+        x.type = prm.emitters[i].type == RT_EMIT_QUAD ? RT_EMIT_QUAD : RT_EMIT_DISK;   // the sun is a disk source
         x.t = mk(f[0], f[1], f[2]); x.b = mk(f[3], f[4], f[5]); x.center = mk(f[6], f[7], f[8]);
         x.dir = mk(f[9], f[10], f[11]); x.normal = mk(f[12], f[13], f[14]); x.corner = mk(f[15], f[16], f[17]);
         x.u = mk(f[18], f[19], f[20]); x.v = mk(f[21], f[22], f[23]); x.ta = mk(f[24], f[25], f[26]);

@@ -10,6 +10,7 @@
 //   accumulate: accumulate_sample (src/main.rs:603-643) over the passes in order
 #include "rt_internal.h"
 #include "rt_media.cuh"
+#include "rt_sky.cuh"
 
 using namespace rtd;
 
@@ -84,6 +85,15 @@ RT_D float fresnel_dielectric(float ci, float eta) {
 RT_D float smith_lambda(float c, float alpha) {
     float a2 = alpha * alpha, c2 = c * c;
     return (sqrtf(a2 + (1.0f - a2) * c2) - c) / (2.0f * c);
+}
+RT_D float smith_g1(float c, float alpha) {                                         // material.rs:163-167
+    float a2 = alpha * alpha, c2 = c * c;
+    return 2.0f * c / (c + sqrtf(a2 + (1.0f - a2) * c2));
+}
+RT_D float ggx_ndf(float cos_h, float alpha) {                                      // material.rs:308-312
+    float a2 = alpha * alpha;
+    float dd = 1.0f + cos_h * cos_h * (a2 - 1.0f);
+    return a2 / fmaxf(PI_F * dd * dd, 1e-12f);
 }
 RT_D float3 vndf_sample(float3 wo, float ax, float ay, float xi1, float xi2) {
     float3 wh = unit3(mk(ax * wo.x, ay * wo.y, wo.z));
@@ -185,6 +195,7 @@ RT_D float3 bg_type_eval(int type, const float* color, const float* top, const f
     return mk(bottom[0], bottom[1], bottom[2]) * (1.0f - t) + mk(top[0], top[1], top[2]) * t;
 }
 RT_D float3 bg_eval(const DevScene& S, float3 dir) {
+    if (S.bg_type == RT_BG_PHYSICAL) return preetham_sky(dir, S.sun_dir, S.turbidity);
     if (S.bg_type == RT_BG_ENVMAP) {
         if (S.vis_type >= 0) return bg_type_eval(S.vis_type, S.vis_color, S.vis_top, S.vis_bottom, dir);
         return env_lookup(S, dir);
@@ -589,7 +600,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                                                           const uint32_t* cin, uint32_t* cout,
                                                           float4* __restrict__ sq, uint32_t* ctr) {
     // queues appended to: [next set, retire records, gather requests, shadow rays]
-    constexpr int NQ = CLS == CLS_DIFFUSE ? 4 : (CLS == CLS_MISS || CLS == CLS_EMIT) ? 1 : 2;
+    constexpr int NQ = (CLS == CLS_DIFFUSE || CLS == CLS_METAL) ? 4 : (CLS == CLS_MISS || CLS == CLS_EMIT) ? 1 : 2;
     __shared__ BlockQ<NQ, RT_SHADE_BLOCK / 32> shq;
     uint32_t* qctr[NQ];
     if constexpr (NQ == 1) {
@@ -650,7 +661,8 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                 } else {
                     bg = bg_eval(S, d);
                 }
-                float emit_w = env_pdf == 0.0f ? 1.0f : (prev_spec ? 1.0f : prev_mis);
+                // prev_mis holds the specular-bounce sun weight after a specular vertex
+                float emit_w = (sun_pdf_value(S, d) + env_pdf == 0.0f) ? 1.0f : prev_mis;
                 Lc = Lc + T * (bg * spec_factor(S, tint, w, lam0, H)) * R.bg_scale * emit_w;
             } else if (CLS == CLS_EMIT) {                                           // renderer.rs:415-419
                 float4 hv = A.hit[pid];
@@ -751,11 +763,48 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                             metal_ior(m, lam_k(S, lam0, i, H), &nn, &kk);
                             ws[i] *= fresnel_conductor(cos_h, nn, kk);
                         }
+                        // specular sun NEE (renderer.rs:421-456) with the conductor's
+                        // specular_brdf_cos / specular_sampling_pdf (material.rs:504-551)
+                        float sun_w = 1.0f;
+                        if (S.has_sun && m.roughness != 0.0f) {
+                            float3 sun_s = sample_sun_cone(S.sun_dir, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1));
+                            float cos_i = dot3(sun_s, nrm);
+                            if (cos_i > 0.0f) {
+                                float3 hh = unit3(wo + sun_s);
+                                float wo_h = fmaxf(dot3(wo, hh), 0.0f), h_n = fmaxf(dot3(hh, nrm), 0.0f);
+                                float base = ggx_ndf(h_n, alpha) * (1.0f / (1.0f + smith_lambda(cos_o, alpha) +
+                                                                            smith_lambda(cos_i, alpha)));
+                                float comp = fminf(1.0f / fmaxf(e_ss_lut(S, cos_o, alpha), 0.05f), 10.0f);
+                                float wv[4] = {w.x, w.y, w.z, w.w};
+                                for (int i = 0; i < H; i++) {
+                                    if (wv[i] == 0.0f) continue;
+                                    float nn, kk;
+                                    metal_ior(m, lam_k(S, lam0, i, H), &nn, &kk);
+                                    wv[i] *= base * fresnel_conductor(wo_h, nn, kk) / (4.0f * cos_o) * comp;
+                                }
+                                float3 brdf_cos = spec_factor(S, tint == TINT_NONE ? TINT_CMF : tint,
+                                                              make_float4(wv[0], wv[1], wv[2], wv[3]), lam0, H);
+                                if (brdf_cos.x > 0.0f || brdf_cos.y > 0.0f || brdf_cos.z > 0.0f) {
+                                    float p_mat = ggx_ndf(h_n, alpha) * smith_g1(cos_o, alpha) / (4.0f * cos_o);
+                                    float mis_d = SUN_PDF * SUN_PDF + p_mat * p_mat;
+                                    if (mis_d > 0.0f) {
+                                        float3 c = T * brdf_cos * preetham_sky(sun_s, S.sun_dir, S.turbidity) * SUN_PDF / mis_d;
+                                        np0 = make_float4(c.x, c.y, c.z, 0.f);
+                                        sh0 = true;
+                                        sh0a = make_float4(p.x, p.y, p.z, INFINITY);
+                                        sh0b = make_float4(sun_s.x, sun_s.y, sun_s.z, 0.f);
+                                    }
+                                }
+                            }
+                            float3 hb = unit3(wo + dir);
+                            float p_b = ggx_ndf(fmaxf(dot3(hb, nrm), 0.0f), alpha) * smith_g1(cos_o, alpha) / (4.0f * cos_o);
+                            if (p_b > 0.0f) sun_w = (p_b * p_b) / fmaxf(p_b * p_b + SUN_PDF * SUN_PDF, 1e-8f);
+                        }
                         w = make_float4(ws[0], ws[1], ws[2], ws[3]);
                         if (tint == TINT_NONE) tint = TINT_CMF;
                         T = T * weight;
                         o = p; d = dir;
-                        prev_spec = true; prev_mis = 1.0f;
+                        prev_spec = true; prev_mis = sun_w;
                     }
                 } else {                                                            // renderer.rs:457-572
                     sf = spec_factor(S, tint, w, lam0, H);
@@ -780,8 +829,9 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         if (lights_hit(S, p, ldir, &lr)) {
                             float l_pdf = lights_pdf_value(S, p, ldir);
                             float brdf = fmaxf(dot3(nrm, unit3(ldir)) / PI_F, 0.0f);
+                            float sun_p = sun_pdf_value(S, ldir);
                             float env_p = env_dir_pdf(S, ldir);
-                            float mis_d = l_pdf * l_pdf + brdf * brdf + env_p * env_p;
+                            float mis_d = l_pdf * l_pdf + brdf * brdf + sun_p * sun_p + env_p * env_p;
                             if (mis_d > 0.0f && brdf > 0.0f) {
                                 float3 nee = emission(S, S.mats[lr.mat], tint, w, lam0, H);
                                 float3 c = T * att * brdf * l_pdf * nee / mis_d;
@@ -790,6 +840,21 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                                 sh0a = make_float4(p.x, p.y, p.z, lr.t * (1.0f - 1e-4f));
                                 sh0b = make_float4(ldir.x, ldir.y, ldir.z, 0.f);
                             }
+                        }
+                    }
+                    if (S.has_sun) {                                                // renderer.rs:495-518
+                        // the sun shares the env-NEE slot: a Physical sky has no env map
+                        float3 sun_s = sample_sun_cone(S.sun_dir, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1));
+                        float brdf = fmaxf(dot3(nrm, unit3(sun_s)) / PI_F, 0.0f);
+                        if (brdf > 0.0f) {
+                            float3 sun_color = preetham_sky(sun_s, S.sun_dir, S.turbidity) * sf;
+                            float area_pdf = have_lights ? lights_pdf_value(S, p, sun_s) : 0.0f;
+                            float mis_d = SUN_PDF * SUN_PDF + brdf * brdf + area_pdf * area_pdf;
+                            float3 c = T * att * brdf * SUN_PDF * sun_color / mis_d;
+                            np1 = make_float4(c.x, c.y, c.z, 0.f);
+                            sh1 = true;
+                            sh1a = make_float4(p.x, p.y, p.z, INFINITY);
+                            sh1b = make_float4(sun_s.x, sun_s.y, sun_s.z, 0.f);
                         }
                     }
                     if (S.has_env) {
@@ -827,8 +892,9 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         alive = false;
                     } else {
                         float area = have_lights ? lights_pdf_value(S, p, idir) : 0.0f;
+                        float sun = sun_pdf_value(S, idir);
                         float env = env_dir_pdf(S, idir);
-                        prev_mis = (pdf_val * pdf_val) / fmaxf(pdf_val * pdf_val + area * area + env * env, 1e-8f);
+                        prev_mis = (pdf_val * pdf_val) / fmaxf(pdf_val * pdf_val + (area * area + sun * sun + env * env), 1e-8f);
                         T = T * (att * (scat / pdf_val));
                         o = p; d = idir;
                         prev_spec = false;

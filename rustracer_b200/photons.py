@@ -33,6 +33,15 @@ def quad_emitter(corner, u, v, color, n_photons):
     return e
 
 
+def sun_emitter(n_photons):
+    """The Physical sky's sun as the caustic source (scene.rs:40-52); the library
+    derives the direction and colour from the scene's background."""
+    e = abi.RtPhotonEmitter()
+    e.type = abi.RT_EMIT_SUN
+    e.n_photons = int(n_photons)
+    return e
+
+
 def photon_params(emitters, gather_radius, knn_k=0, seed=0):
     if not (1 <= len(emitters) <= abi.RT_MAX_EMITTERS):
         raise ValueError("1..8 emitters")
@@ -47,9 +56,11 @@ def photon_params(emitters, gather_radius, knn_k=0, seed=0):
 
 
 def caustic_params(builder, n_photons, gather_radius, knn_k=0, seed=0, env_dir=None, env_color=None):
-    """rebuild_caustics emitter choice (scene.rs:40-73): an env map → disk facing a
-    bright env direction (computed by the caller as the reference does from 8
+    """rebuild_caustics emitter choice (scene.rs:40-73): a Physical sky → its sun;
+    an env map → disk facing a bright env direction (computed by the caller as the reference does from 8
     CDF samples), otherwise the first [[lights]] quad with its `color`."""
+    if builder.bg.get("type") == abi.RT_BG_PHYSICAL:
+        return photon_params([sun_emitter(n_photons)], gather_radius, knn_k, seed)
     if env_dir is not None:
         return photon_params([disk_emitter(env_dir, env_color, n_photons)], gather_radius, knn_k, seed)
     quads = [builder.quads[i] for kind, i in builder._lights if kind == "quad"]

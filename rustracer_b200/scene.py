@@ -280,6 +280,14 @@ class SceneBuilder:
         return si
 
     # background --------------------------------------------------------
+    def set_physical(self, sun_azimuth=0.0, sun_elevation=30.0, turbidity=3.0):
+        """Background::Physical from the TOML angles (scene_file.rs:917-927): the sun
+        direction (cos el · sin az, sin el, cos el · cos az), normalised."""
+        el, az = math.radians(sun_elevation), math.radians(sun_azimuth)
+        d = np.array([math.cos(el) * math.sin(az), math.sin(el), math.cos(el) * math.cos(az)], np.float32)
+        d = d / np.float32(np.linalg.norm(d))
+        self.bg = {"type": abi.RT_BG_PHYSICAL, "sun_dir": tuple(float(x) for x in d), "turbidity": float(turbidity)}
+
     def set_solid(self, color):
         self.bg = {"type": abi.RT_BG_SOLID, "color": tuple(color)}
 
@@ -363,6 +371,9 @@ class SceneBuilder:
         bg.visible_type = -1
         if bg.type == abi.RT_BG_SOLID:
             bg.color = _f3(self.bg["color"])
+        elif bg.type == abi.RT_BG_PHYSICAL:
+            bg.sun_dir = _f3(self.bg["sun_dir"])
+            bg.turbidity = self.bg["turbidity"]
         elif bg.type == abi.RT_BG_GRADIENT:
             bg.top = _f3(self.bg["top"])
             bg.bottom = _f3(self.bg["bottom"])
@@ -565,6 +576,8 @@ def scene_from_toml_dict(doc, base="."):
     bg = doc.get("background", {"type": "solid", "color": [0, 0, 0]})
     if bg["type"] == "solid":
         sb.set_solid(bg["color"])
+    elif bg["type"] == "physical":
+        sb.set_physical(bg.get("sun_azimuth", 0.0), bg.get("sun_elevation", 30.0), bg.get("turbidity", 3.0))
     elif bg["type"] == "env_map":
         img = load_hdr(_resolve(base, bg["path"]))
         sb.set_env(img, bg.get("rotate_y", 0.0) or 0.0, bg.get("visible"))

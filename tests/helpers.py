@@ -77,3 +77,19 @@ def medium_sphere_scene(density=1.0, blocker=False, kind="constant"):
     if blocker:
         sb.add_sphere((-2.0, 0.0, 0.0), 0.5, m)
     return sb
+
+
+def physical_sky_scene(elevation=35.0, azimuth=30.0, turbidity=3.0, roughness=0.3):
+    """An open scene under the Physical sky: a diffuse floor, a rough conductor
+    sphere and a diffuse sphere (sun NEE at diffuse and conductor vertices)."""
+    from rustracer_b200.configs import gold_like_nk
+    sb = SceneBuilder()
+    sb.set_physical(azimuth, elevation, turbidity)
+    floor = sb.add_material(Material.lambertian((0.5, 0.5, 0.5)))
+    n, k = gold_like_nk()
+    metal = sb.add_material(Material.spectral_metal_nk(380.0, 50.0, n, k, roughness=roughness))
+    white = sb.add_material(Material.lambertian((0.8, 0.8, 0.8)))
+    sb.add_quad((-5.0, 0.0, -5.0), (0.0, 0.0, 10.0), (10.0, 0.0, 0.0), floor)
+    sb.add_sphere((-0.6, 0.5, 0.0), 0.5, metal)
+    sb.add_sphere((0.6, 0.4, 0.2), 0.4, white)
+    return sb
