@@ -143,7 +143,7 @@ static inline float rnd(const Rng& r, uint32_t dim) { return (float)(rnd_u32(r, 
 
 // dimension layout of one path
 enum {
-    D_JIT_U = 0, D_JIT_V = 1, D_LENS_R = 2, D_LENS_P = 3, D_TIME = 4, D_LAMBDA = 5,
+    D_JIT_U = 0, D_JIT_V = 1, D_LENS_R = 2, D_LENS_P = 3, D_TIME = 4, D_LAMBDA = 5, D_LENS_K = 6,
     D_BOUNCE0 = 8, D_PER_BOUNCE = 16,
     B_SCATTER0 = 0, B_SCATTER1 = 1, B_LPICK = 2, B_LPT0 = 3, B_LPT1 = 4,
     B_SUN0 = 5, B_SUN1 = 6,
@@ -1833,8 +1833,20 @@ static void render_pixel(const Scene& s, const RtCamera& cam, const RtPassParams
     float v = ((float)ray_y + vj) / h_denom;
     V3 cu = v3(cam.u[0], cam.u[1], cam.u[2]), cv = v3(cam.v[0], cam.v[1], cam.v[2]);
     V3 origin = v3(cam.origin[0], cam.origin[1], cam.origin[2]);
-    float lr = std::sqrt(rnd(rng, D_LENS_R)), lp = 2.0f * PI_F * rnd(rng, D_LENS_P);
-    V3 rd = cam.lens_radius * v3(lr * std::cos(lp), lr * std::sin(lp), 0.0f);
+    V3 rd;
+    if (cam.aperture_blades >= 3) {
+        // sample_polygon (camera.rs:66-79): a fan wedge of the N-gon, then a folded
+        // uniform triangle sample
+        float nb = (float)cam.aperture_blades, rot = PI_F / nb;
+        float k = (float)(rnd_u32(rng, D_LENS_K) % (uint32_t)cam.aperture_blades);
+        float a1 = 2.0f * PI_F * k / nb + rot, a2 = 2.0f * PI_F * (k + 1.0f) / nb + rot;
+        float r1 = rnd(rng, D_LENS_R), r2 = rnd(rng, D_LENS_P);
+        if (r1 + r2 > 1.0f) { r1 = 1.0f - r1; r2 = 1.0f - r2; }
+        rd = cam.lens_radius * (v3(std::cos(a1), std::sin(a1), 0.0f) * r1 + v3(std::cos(a2), std::sin(a2), 0.0f) * r2);
+    } else {
+        float lr = std::sqrt(rnd(rng, D_LENS_R)), lp = 2.0f * PI_F * rnd(rng, D_LENS_P);
+        rd = cam.lens_radius * v3(lr * std::cos(lp), lr * std::sin(lp), 0.0f);
+    }
     V3 offset = cu * rd.x + cv * rd.y;
     V3 ll = v3(cam.lower_left[0], cam.lower_left[1], cam.lower_left[2]);
     V3 hz = v3(cam.horizontal[0], cam.horizontal[1], cam.horizontal[2]);

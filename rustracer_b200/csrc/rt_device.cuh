@@ -160,7 +160,7 @@ RT_HD uint32_t rnd_u32(const Rng& r, uint32_t dim) { return pcg3d_x(r.a, r.b, di
 RT_HD float rnd(const Rng& r, uint32_t dim) { return (float)(rnd_u32(r, dim) >> 8) * (1.0f / 16777216.0f); }
 
 enum {
-    D_JIT_U = 0, D_JIT_V = 1, D_LENS_R = 2, D_LENS_P = 3, D_TIME = 4, D_LAMBDA = 5,
+    D_JIT_U = 0, D_JIT_V = 1, D_LENS_R = 2, D_LENS_P = 3, D_TIME = 4, D_LAMBDA = 5, D_LENS_K = 6,
     D_BOUNCE0 = 8, D_PER_BOUNCE = 16,
     B_SCATTER0 = 0, B_SCATTER1 = 1, B_LPICK = 2, B_LPT0 = 3, B_LPT1 = 4,
     B_SUN0 = 5, B_SUN1 = 6,

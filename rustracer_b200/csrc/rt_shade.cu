@@ -419,10 +419,24 @@ RT_D void init_path(const DevScene& S, const PathState& P, const RenderLaunch& R
     const RtCamera& c = R.cam;
     float3 cu = mk(c.u[0], c.u[1], c.u[2]), cv = mk(c.v[0], c.v[1], c.v[2]);
     float3 org = mk(c.origin[0], c.origin[1], c.origin[2]);
-    float lr = sqrtf(rnd(rng, D_LENS_R));
-    float ls, lc;
-    sincosf(2.0f * PI_F * rnd(rng, D_LENS_P), &ls, &lc);
-    float3 rd = c.lens_radius * mk(lr * lc, lr * ls, 0.0f);
+    float3 rd;
+    if (c.aperture_blades >= 3) {
+        // sample_polygon (camera.rs:66-79): a fan wedge of the N-gon, then a folded
+        // uniform triangle sample
+        float nb = (float)c.aperture_blades, rot = PI_F / nb;
+        float k = (float)(rnd_u32(rng, D_LENS_K) % (uint32_t)c.aperture_blades);
+        float s1, c1, s2, c2;
+        sincosf(2.0f * PI_F * k / nb + rot, &s1, &c1);
+        sincosf(2.0f * PI_F * (k + 1.0f) / nb + rot, &s2, &c2);
+        float r1 = rnd(rng, D_LENS_R), r2 = rnd(rng, D_LENS_P);
+        if (r1 + r2 > 1.0f) { r1 = 1.0f - r1; r2 = 1.0f - r2; }
+        rd = c.lens_radius * (mk(c1, s1, 0.0f) * r1 + mk(c2, s2, 0.0f) * r2);
+    } else {
+        float lr = sqrtf(rnd(rng, D_LENS_R));
+        float ls, lc;
+        sincosf(2.0f * PI_F * rnd(rng, D_LENS_P), &ls, &lc);
+        rd = c.lens_radius * mk(lr * lc, lr * ls, 0.0f);
+    }
     float3 off = cu * rd.x + cv * rd.y;
     float3 ll = mk(c.lower_left[0], c.lower_left[1], c.lower_left[2]);
     float3 hz = mk(c.horizontal[0], c.horizontal[1], c.horizontal[2]);

@@ -402,7 +402,7 @@ class SceneBuilder:
 
 # ── camera (camera.rs:24-45) ────────────────────────────────────────────────
 def make_camera(look_from, look_at, vup=(0.0, 1.0, 0.0), vfov=40.0, aspect=1.0,
-                aperture=0.0, focus_dist=None):
+                aperture=0.0, focus_dist=None, aperture_blades=0):
     """Camera::new in f32 arithmetic; returns an RtCamera."""
     f = lambda x: np.asarray(x, dtype=F32)
     lf, la, up = f(look_from), f(look_at), f(vup)
@@ -430,7 +430,7 @@ def make_camera(look_from, look_at, vup=(0.0, 1.0, 0.0), vfov=40.0, aspect=1.0,
     cam.u = _f3(u)
     cam.v = _f3(v)
     cam.lens_radius = float(F32(aperture) / F32(2))
-    cam.aperture_blades = 0
+    cam.aperture_blades = int(aperture_blades)         # ≥ 3: polygonal aperture (camera.rs:48-50)
     return cam
 
 
@@ -572,7 +572,7 @@ def scene_from_toml_dict(doc, base="."):
     cam = doc["camera"]
     lf, la = cam["look_from"], cam["look_at"]
     sb.camera = dict(look_from=lf, look_at=la, vfov=cam.get("vfov", 40.0), aperture=cam.get("aperture", 0.0),
-                     focus_dist=cam.get("focus_dist"))
+                     focus_dist=cam.get("focus_dist"), aperture_blades=cam.get("aperture_blades", 0))
     bg = doc.get("background", {"type": "solid", "color": [0, 0, 0]})
     if bg["type"] == "solid":
         sb.set_solid(bg["color"])

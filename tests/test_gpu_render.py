@@ -128,3 +128,18 @@ def test_multi_call_sample_indices_are_consistent():
     a = g.render_pass(st["camera"], p)
     b = np.concatenate([g.render_pass(st["camera"], pass_params(32, 32, k, 1, 2, 8, 4, 1.0, 5)) for k in range(4)])
     np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-7)
+
+
+def test_polygonal_aperture_depth_of_field_matches_oracle():
+    # Camera::get_ray with aperture_blades ≥ 3 (camera.rs:47-79)
+    from rustracer_b200.scene import make_camera
+    sb, st = configs.box_scene(width=64, height=64)
+    cam = make_camera((0.5, 0.5, -1.4), (0.5, 0.5, 0.5), vfov=40.0, aspect=1.0, aperture=0.15, focus_dist=1.8,
+                      aperture_blades=6)
+    g, o = GpuScene(sb), O.OracleScene(sb)
+    p = pass_params(64, 64, 0, 64, 8, 8, 4, 1.0, 31)
+    gi = g.render_pass(cam, p)
+    p.seed = 32
+    oi = o.render_pass(cam, p)
+    assert np.isfinite(gi).all()
+    assert_tiles_agree(gi, oi)
