@@ -1545,7 +1545,7 @@ static void emitter_setup(const RtScene* s, const RtPhotonEmitter& e0, float* f)
         float3 perp = std::fabs(sun.x) < 0.9f ? rtd::sky_unit(make_float3(0.0f, -sun.z, sun.y))
                                               : rtd::sky_unit(make_float3(-sun.z, 0.0f, sun.x));
         float3 pd = rtd::sky_unit(make_float3(sun.x + perp.x * 0.04f, sun.y + perp.y * 0.04f, sun.z + perp.z * 0.04f));
-        float3 col = rtd::preetham_sky(pd, sun, s->S.turbidity);
+        float3 col = rtd::preetham_sky_eval(pd, sun, s->S.turbidity);
         e.type = RT_EMIT_DISK;
         e.dir[0] = sun.x; e.dir[1] = sun.y; e.dir[2] = sun.z;
         e.color[0] = col.x * PI; e.color[1] = col.y * PI; e.color[2] = col.z * PI;

@@ -195,7 +195,6 @@ RT_D float3 bg_type_eval(int type, const float* color, const float* top, const f
     return mk(bottom[0], bottom[1], bottom[2]) * (1.0f - t) + mk(top[0], top[1], top[2]) * t;
 }
 RT_D float3 bg_eval(const DevScene& S, float3 dir) {
-    if (S.bg_type == RT_BG_PHYSICAL) return preetham_sky(dir, S.sun_dir, S.turbidity);
     if (S.bg_type == RT_BG_ENVMAP) {
         if (S.vis_type >= 0) return bg_type_eval(S.vis_type, S.vis_color, S.vis_top, S.vis_bottom, dir);
         return env_lookup(S, dir);
@@ -528,6 +527,61 @@ __global__ void k_zero_converged(const uint8_t* __restrict__ conv, uint32_t npix
 // Warp-aggregated appends (ballot + popc + one atomic per class per warp) into
 // one queue per class, so each shading kernel below runs one material's code:
 // no divergence between materials and a much smaller instruction footprint.
+// Sun NEE at a diffuse vertex (renderer.rs:495-518): the parked contribution
+// with the occlusion test still to do.
+RT_D bool sun_nee_diffuse(const DevScene& S, float3 p, float3 nrm, float3 T_att, float3 sf,
+                                             float r1, float r2, float3* dir, float3* c) {
+    float3 sun_s = sample_sun_cone(S.sun_dir, r1, r2);
+    float brdf = fmaxf(dot3(nrm, unit3(sun_s)) / PI_F, 0.0f);
+    if (!(brdf > 0.0f)) return false;
+    float3 sun_color = preetham_sky(sun_s, S.sun_dir, S.turbidity) * sf;
+    float area_pdf = S.n_lights > 0 ? lights_pdf_value(S, p, sun_s) : 0.0f;
+    float mis_d = SUN_PDF * SUN_PDF + brdf * brdf + area_pdf * area_pdf;
+    *c = T_att * brdf * SUN_PDF * sun_color / mis_d;
+    *dir = sun_s;
+    return true;
+}
+
+// Specular sun NEE at a rough conductor (renderer.rs:421-456) with the
+// conductor's specular_brdf_cos / specular_sampling_pdf (material.rs:504-551),
+// per hero wavelength; also the MIS weight of the sampled bounce against the sun.
+RT_D bool sun_nee_conductor(const DevScene& S, const DevMaterial& m, float3 p, float3 nrm,
+                                               float3 wo, float3 dir, float cos_o, float alpha, float3 T, float4 w,
+                                               int tint, float lam0, int H, float r1, float r2, float3* sdir,
+                                               float3* c, float* sun_w) {
+    bool park = false;
+    float3 sun_s = sample_sun_cone(S.sun_dir, r1, r2);
+    float cos_i = dot3(sun_s, nrm);
+    if (cos_i > 0.0f) {
+        float3 hh = unit3(wo + sun_s);
+        float wo_h = fmaxf(dot3(wo, hh), 0.0f), h_n = fmaxf(dot3(hh, nrm), 0.0f);
+        float base = ggx_ndf(h_n, alpha) * (1.0f / (1.0f + smith_lambda(cos_o, alpha) + smith_lambda(cos_i, alpha)));
+        float comp = fminf(1.0f / fmaxf(e_ss_lut(S, cos_o, alpha), 0.05f), 10.0f);
+        float wv[4] = {w.x, w.y, w.z, w.w};
+        for (int i = 0; i < H; i++) {
+            if (wv[i] == 0.0f) continue;
+            float nn, kk;
+            metal_ior(m, lam_k(S, lam0, i, H), &nn, &kk);
+            wv[i] *= base * fresnel_conductor(wo_h, nn, kk) / (4.0f * cos_o) * comp;
+        }
+        float3 brdf_cos = spec_factor(S, tint == TINT_NONE ? TINT_CMF : tint,
+                                      make_float4(wv[0], wv[1], wv[2], wv[3]), lam0, H);
+        if (brdf_cos.x > 0.0f || brdf_cos.y > 0.0f || brdf_cos.z > 0.0f) {
+            float p_mat = ggx_ndf(h_n, alpha) * smith_g1(cos_o, alpha) / (4.0f * cos_o);
+            float mis_d = SUN_PDF * SUN_PDF + p_mat * p_mat;
+            if (mis_d > 0.0f) {
+                *c = T * brdf_cos * preetham_sky(sun_s, S.sun_dir, S.turbidity) * SUN_PDF / mis_d;
+                *sdir = sun_s;
+                park = true;
+            }
+        }
+    }
+    float3 hb = unit3(wo + dir);
+    float p_b = ggx_ndf(fmaxf(dot3(hb, nrm), 0.0f), alpha) * smith_g1(cos_o, alpha) / (4.0f * cos_o);
+    *sun_w = p_b > 0.0f ? (p_b * p_b) / fmaxf(p_b * p_b + SUN_PDF * SUN_PDF, 1e-8f) : 1.0f;
+    return park;
+}
+
 RT_D int material_class(uint32_t ref) {
     if (ref == RT_MISS_REF) return CLS_MISS;
     return hit_is_medium(ref) ? CLS_MEDIUM : CLS_EMIT + (int)RT_HIT_CODE(ref);
@@ -608,7 +662,10 @@ RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
     return r;
 }
 
-template <int CLS>
+// SKY: the scene has a Physical sky (Preetham background, sun NEE); the other
+// instantiation leaves that code out so env-map and plain scenes keep their
+// registers.
+template <int CLS, bool SKY>
 __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState A, PathState B, PathState Rt,
                                                           RenderLaunch R, const uint32_t* __restrict__ qin,
                                                           const uint32_t* cin, uint32_t* cout,
@@ -676,7 +733,12 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                     bg = bg_eval(S, d);
                 }
                 // prev_mis holds the specular-bounce sun weight after a specular vertex
-                float emit_w = (sun_pdf_value(S, d) + env_pdf == 0.0f) ? 1.0f : prev_mis;
+                float sun_pdf = 0.0f;
+                if constexpr (SKY) {
+                    sun_pdf = sun_pdf_value(S, d);
+                    bg = preetham_sky(d, S.sun_dir, S.turbidity);
+                }
+                float emit_w = (sun_pdf + env_pdf == 0.0f) ? 1.0f : prev_mis;
                 Lc = Lc + T * (bg * spec_factor(S, tint, w, lam0, H)) * R.bg_scale * emit_w;
             } else if (CLS == CLS_EMIT) {                                           // renderer.rs:415-419
                 float4 hv = A.hit[pid];
@@ -780,39 +842,15 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         // specular sun NEE (renderer.rs:421-456) with the conductor's
                         // specular_brdf_cos / specular_sampling_pdf (material.rs:504-551)
                         float sun_w = 1.0f;
-                        if (S.has_sun && m.roughness != 0.0f) {
-                            float3 sun_s = sample_sun_cone(S.sun_dir, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1));
-                            float cos_i = dot3(sun_s, nrm);
-                            if (cos_i > 0.0f) {
-                                float3 hh = unit3(wo + sun_s);
-                                float wo_h = fmaxf(dot3(wo, hh), 0.0f), h_n = fmaxf(dot3(hh, nrm), 0.0f);
-                                float base = ggx_ndf(h_n, alpha) * (1.0f / (1.0f + smith_lambda(cos_o, alpha) +
-                                                                            smith_lambda(cos_i, alpha)));
-                                float comp = fminf(1.0f / fmaxf(e_ss_lut(S, cos_o, alpha), 0.05f), 10.0f);
-                                float wv[4] = {w.x, w.y, w.z, w.w};
-                                for (int i = 0; i < H; i++) {
-                                    if (wv[i] == 0.0f) continue;
-                                    float nn, kk;
-                                    metal_ior(m, lam_k(S, lam0, i, H), &nn, &kk);
-                                    wv[i] *= base * fresnel_conductor(wo_h, nn, kk) / (4.0f * cos_o) * comp;
-                                }
-                                float3 brdf_cos = spec_factor(S, tint == TINT_NONE ? TINT_CMF : tint,
-                                                              make_float4(wv[0], wv[1], wv[2], wv[3]), lam0, H);
-                                if (brdf_cos.x > 0.0f || brdf_cos.y > 0.0f || brdf_cos.z > 0.0f) {
-                                    float p_mat = ggx_ndf(h_n, alpha) * smith_g1(cos_o, alpha) / (4.0f * cos_o);
-                                    float mis_d = SUN_PDF * SUN_PDF + p_mat * p_mat;
-                                    if (mis_d > 0.0f) {
-                                        float3 c = T * brdf_cos * preetham_sky(sun_s, S.sun_dir, S.turbidity) * SUN_PDF / mis_d;
-                                        np0 = make_float4(c.x, c.y, c.z, 0.f);
-                                        sh0 = true;
-                                        sh0a = make_float4(p.x, p.y, p.z, INFINITY);
-                                        sh0b = make_float4(sun_s.x, sun_s.y, sun_s.z, 0.f);
-                                    }
-                                }
+                        if (SKY && S.has_sun && m.roughness != 0.0f) {
+                            float3 sun_s, c;
+                            if (sun_nee_conductor(S, m, p, nrm, wo, dir, cos_o, alpha, T, w, tint, lam0, H,
+                                                  rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1), &sun_s, &c, &sun_w)) {
+                                np0 = make_float4(c.x, c.y, c.z, 0.f);
+                                sh0 = true;
+                                sh0a = make_float4(p.x, p.y, p.z, INFINITY);
+                                sh0b = make_float4(sun_s.x, sun_s.y, sun_s.z, 0.f);
                             }
-                            float3 hb = unit3(wo + dir);
-                            float p_b = ggx_ndf(fmaxf(dot3(hb, nrm), 0.0f), alpha) * smith_g1(cos_o, alpha) / (4.0f * cos_o);
-                            if (p_b > 0.0f) sun_w = (p_b * p_b) / fmaxf(p_b * p_b + SUN_PDF * SUN_PDF, 1e-8f);
                         }
                         w = make_float4(ws[0], ws[1], ws[2], ws[3]);
                         if (tint == TINT_NONE) tint = TINT_CMF;
@@ -843,7 +881,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         if (lights_hit(S, p, ldir, &lr)) {
                             float l_pdf = lights_pdf_value(S, p, ldir);
                             float brdf = fmaxf(dot3(nrm, unit3(ldir)) / PI_F, 0.0f);
-                            float sun_p = sun_pdf_value(S, ldir);
+                            float sun_p = SKY ? sun_pdf_value(S, ldir) : 0.0f;
                             float env_p = env_dir_pdf(S, ldir);
                             float mis_d = l_pdf * l_pdf + brdf * brdf + sun_p * sun_p + env_p * env_p;
                             if (mis_d > 0.0f && brdf > 0.0f) {
@@ -856,15 +894,11 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                             }
                         }
                     }
-                    if (S.has_sun) {                                                // renderer.rs:495-518
+                    if (SKY && S.has_sun) {                                         // renderer.rs:495-518
                         // the sun shares the env-NEE slot: a Physical sky has no env map
-                        float3 sun_s = sample_sun_cone(S.sun_dir, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1));
-                        float brdf = fmaxf(dot3(nrm, unit3(sun_s)) / PI_F, 0.0f);
-                        if (brdf > 0.0f) {
-                            float3 sun_color = preetham_sky(sun_s, S.sun_dir, S.turbidity) * sf;
-                            float area_pdf = have_lights ? lights_pdf_value(S, p, sun_s) : 0.0f;
-                            float mis_d = SUN_PDF * SUN_PDF + brdf * brdf + area_pdf * area_pdf;
-                            float3 c = T * att * brdf * SUN_PDF * sun_color / mis_d;
+                        float3 sun_s, c;
+                        if (sun_nee_diffuse(S, p, nrm, T * att, sf, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1),
+                                            &sun_s, &c)) {
                             np1 = make_float4(c.x, c.y, c.z, 0.f);
                             sh1 = true;
                             sh1a = make_float4(p.x, p.y, p.z, INFINITY);
@@ -906,7 +940,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         alive = false;
                     } else {
                         float area = have_lights ? lights_pdf_value(S, p, idir) : 0.0f;
-                        float sun = sun_pdf_value(S, idir);
+                        float sun = SKY ? sun_pdf_value(S, idir) : 0.0f;
                         float env = env_dir_pdf(S, idir);
                         prev_mis = (pdf_val * pdf_val) / fmaxf(pdf_val * pdf_val + (area * area + sun * sun + env * env), 1e-8f);
                         T = T * (att * (scat / pdf_val));
@@ -1013,13 +1047,16 @@ void launch_shade(const DevScene& S, const PathState& A, const PathState& B, con
     int grid = sms * RT_SHADE_BLOCKS_PER_SM;
     k_classify<<<sms * 4, CLS_BLOCK, 0, st>>>(A.hit, ctr + CTR_COUNT, Q, ctr + CTR_CLS_COUNT);
 #define RT_SHADE_CLASS(C)                                                                                   \
-    k_shade<C><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr)
+    if (S.bg_type == RT_BG_PHYSICAL)                                                                        \
+        k_shade<C, true><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr); \
+    else                                                                                                    \
+        k_shade<C, false><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr)
     RT_SHADE_CLASS(CLS_MISS);
     RT_SHADE_CLASS(CLS_EMIT);
     RT_SHADE_CLASS(CLS_DIFFUSE);
     RT_SHADE_CLASS(CLS_METAL);
     RT_SHADE_CLASS(CLS_DIELEC);
-    if (S.n_media > 0) RT_SHADE_CLASS(CLS_MEDIUM);
+    if (S.n_media > 0) { RT_SHADE_CLASS(CLS_MEDIUM); }
 #undef RT_SHADE_CLASS
 }
 void launch_retire(const DevScene& S, const PathState& B, const PathState& Rt, const RenderLaunch& R, uint32_t* ctr,

@@ -16,7 +16,7 @@ RT_HD float perez(float a, float b, float c, float dp, float e, float ct, float 
     return (1.0f + a * expf(b / ct)) * (1.0f + c * expf(dp * g) + e * cg * cg);
 }
 
-RT_HD float3 preetham_sky(float3 dir, float3 sun_dir, float turbidity) {
+RT_HD float3 preetham_sky_eval(float3 dir, float3 sun_dir, float turbidity) {
     float3 d = sky_unit(dir), sun = sky_unit(sun_dir);
     float cos_gamma = sky_clamp(dot3(d, sun), -1.0f, 1.0f);
     float gamma = acosf(cos_gamma);
@@ -63,6 +63,10 @@ RT_HD float3 preetham_sky(float3 dir, float3 sun_dir, float turbidity) {
         return sky * (1.0f - tt) + mk(0.07f, 0.06f, 0.05f) * tt;
     }
     return sky;
+}
+
+RT_HD float3 preetham_sky(float3 dir, float3 sun_dir, float turbidity) {
+    return preetham_sky_eval(dir, sun_dir, turbidity);
 }
 
 RT_HD float sun_pdf_value(const DevScene& S, float3 dir) {
