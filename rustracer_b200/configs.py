@@ -204,4 +204,118 @@ def media_box_scene(width=256, height=256, spp=16, max_depth=24, hero=4, seed=5,
     return sb, st
 
 
-CONFIGS = {"box": box_scene, "icosphere": icosphere_scene, "media_box": media_box_scene}
+def round_brilliant(radius=0.5, table_pct=57.0, crown_angle=34.5, pavilion_angle=40.75, girdle_pct=3.0,
+                    girdle_facets=16, band_facets=64, subdiv=1, center=(0.0, 0.0, 0.0)):
+    """A round brilliant as a triangle mesh: the half-spaces of Diamond::new
+    (diamond.rs:93-195 — table, N crown and N pavilion facets through the girdle
+    band edges, and a ground-round band of vertical planes), intersected with
+    scipy's half-space intersection and triangulated by the convex hull; each
+    triangle is split 4-way `subdiv` times (the solid is unchanged).  Returns
+    (vertices (n,3), faces (m,3))."""
+    from scipy.spatial import ConvexHull, HalfspaceIntersection
+    r = radius
+    table_r = table_pct / 100.0 * r
+    crown_h = (r - table_r) * math.tan(math.radians(crown_angle))
+    pav_h = r * math.tan(math.radians(pavilion_angle))
+    girdle_h = min(max(girdle_pct / 100.0 * 2.0 * r, 0.0), 0.3 * r)
+    n = max(girdle_facets, 4) // 2 * 2
+    planes = [((0.0, 1.0, 0.0), (0.0, 0.5 * girdle_h + crown_h, 0.0))]
+    for k in range(n):
+        th = k * 2.0 * math.pi / n
+        sn, c = math.sin(th), math.cos(th)
+        planes.append(((c * crown_h, r - table_r, sn * crown_h), (c * r, 0.5 * girdle_h, sn * r)))
+    for k in range(n):
+        ph = k * 2.0 * math.pi / n
+        sn, c = math.sin(ph), math.cos(ph)
+        planes.append(((c * pav_h, -r, sn * pav_h), (c * r, -0.5 * girdle_h, sn * r)))
+    for j in range(band_facets):
+        a = j * 2.0 * math.pi / band_facets
+        planes.append(((math.cos(a), 0.0, math.sin(a)), (math.cos(a) * r, 0.0, math.sin(a) * r)))
+    hs = []
+    for nv, g in planes:
+        nv = np.asarray(nv, np.float64)
+        nv = nv / np.linalg.norm(nv)
+        hs.append(list(nv) + [-float(nv @ np.asarray(g, np.float64))])      # n·x − d ≤ 0
+    hi = HalfspaceIntersection(np.array(hs), np.zeros(3))
+    V = hi.intersections
+    hull = ConvexHull(V)
+    F = hull.simplices.copy()
+    # orient every triangle outward
+    ctr = V.mean(axis=0)
+    for i, (a, b, c) in enumerate(F):
+        nrm = np.cross(V[b] - V[a], V[c] - V[a])
+        if nrm @ (V[a] - ctr) < 0:
+            F[i] = (a, c, b)
+    for _ in range(subdiv):
+        V, F = _split4(V, F)
+    return V + np.asarray(center, np.float64), F
+
+
+def _split4(V, F):
+    V = list(map(tuple, V))
+    mid = {}
+    def m(a, b):
+        key = (min(a, b), max(a, b))
+        if key not in mid:
+            mid[key] = len(V)
+            V.append(tuple((np.asarray(V[a]) + np.asarray(V[b])) * 0.5))
+        return mid[key]
+    out = []
+    for a, b, c in F:
+        ab, bc, ca = m(a, b), m(b, c), m(c, a)
+        out += [(a, ab, ca), (ab, b, bc), (ca, bc, c), (ab, bc, ca)]
+    return np.array(V, np.float64), np.array(out, np.int64)
+
+
+def env_caustic_dir(env, seed=0xC0FFEE, n=8):
+    """The env-map caustic source of rebuild_caustics (scene.rs:53-66): the unit sum
+    of (0, 1, 0) and n directions drawn ∝ luminance·sinθ (a seeded stream standing
+    in for the reference's SmallRng), and the map's radiance there × π."""
+    h, w, _ = env.shape
+    lum = 0.2126 * env[..., 0] + 0.7152 * env[..., 1] + 0.0722 * env[..., 2]
+    wgt = (lum * np.sin(math.pi * (np.arange(h) + 0.5) / h)[:, None]).ravel().astype(np.float64)
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(wgt.size, size=n, p=wgt / wgt.sum())
+    d = np.array([0.0, 1.0, 0.0])
+    for k in idx:
+        j, i = divmod(int(k), w)
+        theta = math.pi * (j + rng.random()) / h
+        phi = 2.0 * math.pi * ((i + rng.random()) / w - 0.5)
+        d = d + np.array([math.sin(theta) * math.sin(phi), math.cos(theta), math.sin(theta) * math.cos(phi)])
+    d = d / np.linalg.norm(d)
+    v = math.acos(max(-1.0, min(1.0, d[1]))) / math.pi
+    u = (0.5 + math.atan2(d[0], d[2]) / (2 * math.pi)) % 1.0
+    col = env[min(int(v * h), h - 1), min(int(u * w), w - 1)] * math.pi
+    return tuple(d), tuple(float(c) for c in col)
+
+
+def gem_scene(width=1280, height=720, spp=256, max_depth=32, hero=4, seed=3, env_w=1024, env_h=512,
+              photons=2_000_000, knn_k=64, radius_max=0.01):
+    """The gem workload: a round brilliant (girdle Ø1, table 57 %, crown 34.5°,
+    pavilion 40.75°, girdle 3 %) in the diamond preset's Cauchy dispersion
+    (B 2.351, C 0.0230: n_D 2.417, n_F − n_C 0.044; scene_file.rs:686) on an
+    albedo-0.8 plane, two 0.3² blackbody lights at 5500 K, the sky env at 0.1,
+    and a caustic photon map (2M photons, k-NN 64 within r ≤ 0.01)."""
+    sb = SceneBuilder()
+    sb.name = "gem"
+    sb.spectral_range = 1 if hero > 1 else 0
+    V, Fc = round_brilliant(center=(0.0, 0.45, 0.0))
+    diamond = sb.add_material(Material.spectral_dielectric_cauchy(2.351, 0.0230))
+    sb.add_mesh(V, Fc, diamond)
+    plane = sb.add_material(Material.lambertian((0.8, 0.8, 0.8)))
+    sb.add_quad((-2.0, 0.0, -2.0), (0.0, 0.0, 4.0), (4.0, 0.0, 0.0), plane)
+    light = sb.add_material(Material.blackbody(5500.0, 25.0))
+    sb.add_light_quad((-1.35, 2.2, -0.65), (0.3, 0, 0), (0, 0, 0.3), light)
+    sb.add_light_quad((0.95, 1.9, 0.45), (0.3, 0, 0), (0, 0, 0.3), light)
+    env, _ = sky_env(env_w, env_h, seed=seed)
+    env = (env * 0.1).astype(F32)
+    sb.set_env(env)
+    cam = make_camera((0.0, 1.55, 2.2), (0.0, 0.35, 0.0), vfov=32.0, aspect=width / height)
+    d, col = env_caustic_dir(env)
+    st = dict(width=width, height=height, spp=spp, max_depth=max_depth, hero=hero, seed=seed, camera=cam,
+              name=f"gem {len(Fc)} tris {width}x{height} {spp}spp depth{max_depth} hero{hero}",
+              n_tris=len(Fc), photons=photons, knn_k=knn_k, radius_max=radius_max, env_dir=d, env_color=col)
+    return sb, st
+
+
+CONFIGS = {"box": box_scene, "icosphere": icosphere_scene, "media_box": media_box_scene, "gem": gem_scene}
