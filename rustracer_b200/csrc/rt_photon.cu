@@ -557,6 +557,29 @@ RT_D float warp_kth_d2(const Map& M, float3 p, const float3* nrm, float r2max, u
 }
 
 // Irradiance estimate at (p, n) by one warp (all lanes call with the same query).
+// Lane-level test: is any leaf box of the heap within r2 of p?  When none is,
+// no photon can be inside the gather radius and the irradiance is zero, so the
+// warp-cooperative gather is skipped (most diffuse vertices of a scene lie far
+// from its caustics).
+RT_D bool any_leaf_near(const Map& M, float3 p, float r2) {
+    uint32_t stack[PH_STACK];
+    int sp = 0;
+    uint32_t node = 0;
+    uint32_t first_leaf = M.nleaf_pow2 - 1;
+    while (true) {
+        float4 lo = __ldg(M.blo + node), hi = __ldg(M.bhi + node);
+        if (lo.x <= hi.x && box_d2(lo, hi, p) <= r2) {
+            if (node >= first_leaf) return true;
+            if (sp + 2 <= PH_STACK) {
+                stack[sp++] = 2 * node + 2;
+                stack[sp++] = 2 * node + 1;
+            }
+        }
+        if (sp == 0) return false;
+        node = stack[--sp];
+    }
+}
+
 RT_D float3 warp_irradiance(const Map& M, float3 p, float3 n, uint32_t* hist, float* sel) {
     float r2 = M.r2;
     if (M.knn_k > 0) {
@@ -651,17 +674,39 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Ma
     __shared__ uint32_t hist[RT_SHADE_BLOCK / 32][32];
     __shared__ float sel[RT_SHADE_BLOCK / 32][PH_SEL_CAP];
     uint32_t n = *count;
-    uint32_t w = threadIdx.x >> 5, gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t i = gw; i < n; i += nw) {
-        float4 a = gq[(size_t)i * 2], b = gq[(size_t)i * 2 + 1];
-        uint32_t tag = __float_as_uint(a.w);
-        float3 r = rtph::warp_irradiance(M, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), hist[w], sel[w]);
-        if ((threadIdx.x & 31u) == 0) {
-            float4* pc = T.pendC[(tag >> 1) & 1u] + (tag >> 2);
-            float4 f = *pc;
-            bool any = r.x > 0.0f || r.y > 0.0f || r.z > 0.0f;
-            *pc = any ? make_float4(f.x * r.x, f.y * r.y, f.z * r.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    // each lane takes one request and drops it when no leaf is in reach; the
+    // warp then gathers the remaining requests one after the other
+    for (uint32_t base = gw * 32u; base < n; base += nw * 32u) {
+        uint32_t i = base + lane;
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+        bool cand = false;
+        if (i < n) {
+            a = gq[(size_t)i * 2];
+            b = gq[(size_t)i * 2 + 1];
+            cand = rtph::any_leaf_near(M, mk(a.x, a.y, a.z), M.r2);
+            if (!cand) {
+                uint32_t tag = __float_as_uint(a.w);
+                T.pendC[(tag >> 1) & 1u][tag >> 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+        uint32_t m = __ballot_sync(0xFFFFFFFFu, cand);
+        while (m) {
+            int src = __ffs(m) - 1;
+            m &= m - 1;
+            float4 qa = make_float4(__shfl_sync(0xFFFFFFFFu, a.x, src), __shfl_sync(0xFFFFFFFFu, a.y, src),
+                                    __shfl_sync(0xFFFFFFFFu, a.z, src), __shfl_sync(0xFFFFFFFFu, a.w, src));
+            float3 qn = mk(__shfl_sync(0xFFFFFFFFu, b.x, src), __shfl_sync(0xFFFFFFFFu, b.y, src),
+                           __shfl_sync(0xFFFFFFFFu, b.z, src));
+            float3 r = rtph::warp_irradiance(M, mk(qa.x, qa.y, qa.z), qn, hist[w], sel[w]);
+            if (lane == 0) {
+                uint32_t tag = __float_as_uint(qa.w);
+                float4* pc = T.pendC[(tag >> 1) & 1u] + (tag >> 2);
+                float4 f = *pc;
+                bool any = r.x > 0.0f || r.y > 0.0f || r.z > 0.0f;
+                *pc = any ? make_float4(f.x * r.x, f.y * r.y, f.z * r.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
         }
     }
 }
@@ -825,7 +870,7 @@ void launch_knn_api(const PhotonMapDev& map, const float* q, uint32_t n, int k, 
 }
 void launch_photon_gather_paths(const PhotonMapDev& map, const PendTargets& T, const float4* gq, const uint32_t* count,
                                 int sms, cudaStream_t st) {
-    k_photon_gather_paths<<<sms * 4, RT_SHADE_BLOCK, 0, st>>>(map.view(), T, gq, count);
+    k_photon_gather_paths<<<sms * 8, RT_SHADE_BLOCK, 0, st>>>(map.view(), T, gq, count);
 }
 
 }  // namespace rth
