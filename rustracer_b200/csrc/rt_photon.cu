@@ -557,27 +557,41 @@ RT_D float warp_kth_d2(const Map& M, float3 p, const float3* nrm, float r2max, u
 }
 
 // Irradiance estimate at (p, n) by one warp (all lanes call with the same query).
-// Lane-level test: is any leaf box of the heap within r2 of p?  When none is,
-// no photon can be inside the gather radius and the irradiance is zero, so the
-// warp-cooperative gather is skipped (most diffuse vertices of a scene lie far
-// from its caustics).
-RT_D bool any_leaf_near(const Map& M, float3 p, float r2) {
+// Lane-level gather for sparse neighbourhoods: the radius-r2 estimate of one
+// query by one lane, counting the photons it takes.  Gives up (returns false)
+// once `limit` photons are in range — then the k-th-distance search or the
+// warp-cooperative gather is needed.  With fewer than k photons in range the
+// k-NN estimate is exactly this radius-r2 estimate.
+RT_D bool lane_gather(const Map& M, float3 p, float3 n, float r2, uint32_t limit, float3* out) {
     uint32_t stack[PH_STACK];
     int sp = 0;
-    uint32_t node = 0;
+    uint32_t node = 0, count = 0;
     uint32_t first_leaf = M.nleaf_pow2 - 1;
+    float3 acc = mk(0.f, 0.f, 0.f);
     while (true) {
         float4 lo = __ldg(M.blo + node), hi = __ldg(M.bhi + node);
         if (lo.x <= hi.x && box_d2(lo, hi, p) <= r2) {
-            if (node >= first_leaf) return true;
-            if (sp + 2 <= PH_STACK) {
+            if (node >= first_leaf) {
+                uint32_t k0 = (node - first_leaf) * PH_LEAF, k1 = min(k0 + PH_LEAF, M.n);
+                for (uint32_t k = k0; k < k1; k++) {
+                    float d2 = pdist2(__ldg(M.pos + k), p);
+                    if (d2 < r2 && pdot(__ldg(M.nor + k), n) > 0.0f) {
+                        if (++count >= limit) return false;
+                        float4 pw = __ldg(M.pow + k);
+                        acc = acc + mk(pw.x, pw.y, pw.z) * (1.0f - d2 / r2);
+                    }
+                }
+            } else if (sp + 2 <= PH_STACK) {
                 stack[sp++] = 2 * node + 2;
                 stack[sp++] = 2 * node + 1;
             }
         }
-        if (sp == 0) return false;
+        if (sp == 0) break;
         node = stack[--sp];
     }
+    float s = 2.0f / (PI_F * PI_F * r2);
+    *out = count ? acc * s : mk(0.f, 0.f, 0.f);
+    return true;
 }
 
 RT_D float3 warp_irradiance(const Map& M, float3 p, float3 n, uint32_t* hist, float* sel) {
@@ -676,8 +690,9 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Ma
     uint32_t n = *count;
     uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    // each lane takes one request and drops it when no leaf is in reach; the
-    // warp then gathers the remaining requests one after the other
+    // each lane gathers one request on its own while the neighbourhood is sparse
+    // (fewer photons in range than k, or than 64 for the radius estimate); the
+    // warp then gathers the dense remaining requests together, one at a time
     for (uint32_t base = gw * 32u; base < n; base += nw * 32u) {
         uint32_t i = base + lane;
         float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
@@ -685,10 +700,16 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Ma
         if (i < n) {
             a = gq[(size_t)i * 2];
             b = gq[(size_t)i * 2 + 1];
-            cand = rtph::any_leaf_near(M, mk(a.x, a.y, a.z), M.r2);
-            if (!cand) {
+            float3 r;
+            uint32_t limit = M.knn_k > 0 ? M.knn_k : 64u;
+            if (rtph::lane_gather(M, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), M.r2, limit, &r)) {
                 uint32_t tag = __float_as_uint(a.w);
-                T.pendC[(tag >> 1) & 1u][tag >> 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+                float4* pc = T.pendC[(tag >> 1) & 1u] + (tag >> 2);
+                float4 f = *pc;
+                bool any = r.x > 0.0f || r.y > 0.0f || r.z > 0.0f;
+                *pc = any ? make_float4(f.x * r.x, f.y * r.y, f.z * r.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                cand = true;
             }
         }
         uint32_t m = __ballot_sync(0xFFFFFFFFu, cand);
