@@ -219,10 +219,21 @@ def run_ours(args):
     ext = sh = launches = 0
     barrier()
     torch.cuda.synchronize()
+    merge_ms = 0.0
     for k in range(args.steps):
         scene.render_accumulate(cam, params(args.warmup + k), outputs=outs)
         stt = scene.last_stats()
         dev_ms.append(stt["ms"])
+        if ws > 1:
+            # one frame across the ranks: combine the accumulators (sum, M2, count)
+            from rustracer_b200.multigpu import merge_accumulators
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            merge_accumulators(*outs)
+            e1.record()
+            e1.synchronize()
+            dev_ms[-1] += e0.elapsed_time(e1)
+            merge_ms += e0.elapsed_time(e1)
         ext += stt["ext_rays"]
         sh += stt["shadow_rays"]
         launches += stt["launches"]
@@ -264,10 +275,12 @@ def run_ours(args):
         "config": {"workload": "icosphere8 1310720 tris, GGX conductor + diffuse floor, 2048x1024 env, "
                                "1920x1080, 64 spp, depth 12, hero 4",
                    "spp_per_step": SPP, "path_samples_per_step_per_gpu": per_step,
-                   "parallelism": f"weak: {ws} rank(s), each its own 64 spp",
+                   "parallelism": f"weak: {ws} rank(s), each its own 64 spp"
+                                  + (", accumulators all-reduced every frame (NCCL)" if ws > 1 else ""),
                    "l2": "256 MB buffer written between timed steps; scene (~230 MB) exceeds L2"},
         "clocks": clk,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "merge_ms_per_step": merge_ms / args.steps if ws > 1 else None,
         "gpu_launches": int(launches),
         "rays": {"extension": int(ext), "shadow": int(sh),
                  "rays_per_s": (ext + sh) / (sum(dev_ms) / 1000.0)},

@@ -1,0 +1,79 @@
+"""Multi-rank frame rendering host logic on CPU (gloo, world size 2): sample
+sharding and the accumulator merge, against one sequential Welford
+accumulation (main.rs:603-643) of all samples."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.multiprocessing as mp
+
+from rustracer_b200.multigpu import merge_accumulators, shard
+
+
+def test_shard_covers_every_sample_once():
+    for total in (1, 7, 64, 257):
+        for world in (1, 2, 3, 8):
+            got = []
+            for r in range(world):
+                s, n = shard(total, world, r)
+                got.extend(range(s, s + n))
+            assert got == list(range(total))
+
+
+def welford(samples):
+    """Sequential accumulate_sample without clamping: samples (N, P, 3)."""
+    mean = np.zeros(samples.shape[1:], np.float64)
+    m2 = np.zeros_like(mean)
+    s = np.zeros_like(mean)
+    for k, x in enumerate(samples.astype(np.float64), 1):
+        s += x
+        d = x - mean
+        mean += d / k
+        m2 += d * (x - mean)
+    return s, m2, len(samples)
+
+
+def _free_port():
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def _worker(rank, world, port, samples, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        start, n = shard(len(samples), world, rank)
+        s, m2, c = welford(samples[start:start + n])
+        npix = samples.shape[1]
+        ms, mm, mc = merge_accumulators(torch.tensor(s, dtype=torch.float32).reshape(1, npix, 3),
+                                        torch.tensor(m2, dtype=torch.float32).reshape(1, npix, 3),
+                                        torch.full((1, npix), c, dtype=torch.int32))
+        out[rank] = (ms.numpy(), mm.numpy(), mc.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_merge_matches_sequential_welford():
+    rng = np.random.default_rng(0)
+    samples = rng.gamma(2.0, 1.5, size=(37, 50, 3)).astype(np.float32)
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, samples, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    s, m2, n = welford(samples)
+    for r in range(2):
+        ms, mm, mc = out[r]
+        np.testing.assert_allclose(ms[0], s, rtol=1e-5)
+        np.testing.assert_allclose(mm[0], m2, rtol=1e-4, atol=1e-4)
+        assert (mc[0] == n).all()
