@@ -57,8 +57,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--mode", choices=["bench", "pass"], default="bench",
                     help="pass: one warm-up call + one measured 16-spp call of the workload, no JSON (profiler driver)")
-    ap.add_argument("--config", choices=["icosphere", "gem"], default="icosphere",
-                    help="gem: the 1280x720 gem workload with its caustic photon map (a secondary line; "
+    ap.add_argument("--config", choices=["icosphere", "gem", "batch"], default="icosphere",
+                    help="gem: the 1280x720 gem workload with its caustic photon map; batch: 64 jobs of "
+                         "the box/icosphere/gem scenes on 4 concurrent handles vs one (secondary lines; "
                          "the headline is the icosphere workload)")
     return ap.parse_args()
 
@@ -408,6 +409,30 @@ def run_gem(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args):
+    """Secondary workload: 64 frames (scene, size, aspect, spp and camera orbit
+    drawn from a seed) rendered on 4 concurrent scene handles, then on one
+    (sequential).  Wall clock from submission of the batch to the last frame;
+    per-frame latency from submission to that frame's completion."""
+    from rustracer_b200 import batch
+    jobs = batch.make_jobs(seed=0, n=64)
+    builders = {k: batch.build_scene(k) for k in batch.SCENES}
+    conc = batch.run_batch(jobs, workers=4, builders=builders)
+    seq = batch.run_batch(jobs, workers=1, builders=builders)
+    line = {
+        "metric": "path samples/s (64-job batch)", "value": conc["rate"], "unit": UNIT, "n_gpus": 1, "steps": 1,
+        "warmup": 1, "ms_per_step": conc["wall_s"] * 1000.0, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (box, icosphere, gem scenes; seeded job list)",
+        "config": {"workload": "64 jobs: scene in {box, icosphere, gem}, width log-U[128,1920], aspect "
+                               "{1:1, 4:3, 16:9}, spp log-U[4,256], orbiting camera",
+                   "path_samples": conc["path_samples"], "workers": 4},
+        "latency_s": {"p50": conc["p50_s"], "p99": conc["p99_s"]},
+        "sequential": {"value": seq["rate"], "wall_s": seq["wall_s"], "p50": seq["p50_s"], "p99": seq["p99_s"]},
+        "timing": "host wall clock around the whole batch (the frames run on several streams)",
+    }
+    print(json.dumps(line), flush=True)
+
+
 def one_pass():
     """Profiler driver: one warm-up call and one measured call of the 1920×1080
     icosphere workload, 16 samples per pixel per call: 33.2M path samples
@@ -434,6 +459,8 @@ def main():
         run_reference(args)
     elif args.config == "gem":
         run_gem(args)
+    elif args.config == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

@@ -1,0 +1,112 @@
+"""Batched rendering: many independent frames of several scenes on one GPU.
+
+Each worker thread owns one scene handle per scene kind (each handle has its
+own CUDA stream and buffers); the library's calls release the GIL, so the
+workers' frames run concurrently and small frames fill the GPU together.  Jobs
+are taken in submission order from one queue.  `run_batch` reports, per job,
+the latency from the batch's start to the job's completion, and the aggregate
+path-sample rate; with one worker it is the sequential baseline.
+"""
+import math
+import queue
+import threading
+import time
+
+import numpy as np
+
+from . import configs
+from .renderer import GpuScene, pass_params
+from .scene import make_camera
+
+SCENES = ("box", "icosphere", "gem")
+
+
+def make_jobs(seed=0, n=64, scenes=SCENES, min_width=128, max_width=1920, min_spp=4, max_spp=256):
+    """The batch workload: scene uniform over `scenes`, width log-uniform in
+    [min_width, max_width], aspect 1:1 / 4:3 / 16:9, spp log-uniform in
+    [min_spp, max_spp], camera orbiting the scene (azimuth U[0, 360), elevation U[10, 40])."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(n):
+        scene = scenes[int(rng.integers(len(scenes)))]
+        w = int(round(math.exp(rng.uniform(math.log(min_width), math.log(max_width)))))
+        aspect = (1.0, 4.0 / 3.0, 16.0 / 9.0)[int(rng.integers(3))]
+        h = max(16, int(round(w / aspect)))
+        spp = int(round(math.exp(rng.uniform(math.log(min_spp), math.log(max_spp)))))
+        jobs.append(dict(id=k, scene=scene, width=w, height=h, spp=spp, azimuth=float(rng.uniform(0.0, 360.0)),
+                         elevation=float(rng.uniform(10.0, 40.0)), seed=int(rng.integers(1 << 30))))
+    return jobs
+
+
+_ORBIT = {"box": ((0.5, 0.5, 0.5), 1.9), "icosphere": ((0.0, -0.15, 0.0), 3.7), "gem": ((0.0, 0.35, 0.0), 2.7)}
+_DEPTH = {"box": 8, "icosphere": 12, "gem": 32}
+
+
+def job_camera(job):
+    look_at, dist = _ORBIT[job["scene"]]
+    az, el = math.radians(job["azimuth"]), math.radians(job["elevation"])
+    la = np.asarray(look_at, np.float64)
+    lf = la + dist * np.array([math.cos(el) * math.sin(az), math.sin(el), -math.cos(el) * math.cos(az)])
+    return make_camera(tuple(lf), tuple(la), vfov=40.0, aspect=job["width"] / job["height"])
+
+
+def build_scene(kind):
+    if kind == "box":
+        return configs.box_scene()[0]
+    if kind == "icosphere":
+        return configs.icosphere_scene(env_w=1024, env_h=512)[0]
+    if kind == "gem":
+        return configs.gem_scene(env_w=512, env_h=256)[0]
+    raise ValueError(kind)
+
+
+def render_job(handles, job):
+    """One frame into host accumulators (sum, M2, count)."""
+    g = handles[job["scene"]]
+    p = pass_params(job["width"], job["height"], 0, job["spp"], int(math.sqrt(job["spp"])), _DEPTH[job["scene"]], 4,
+                    1.0, job["seed"])
+    return g.render_accumulate(job_camera(job), p)
+
+
+def run_batch(jobs, workers=4, device=0, builders=None, keep_outputs=False):
+    """Render `jobs` with `workers` concurrent threads; returns dict with the
+    wall time, per-job latencies (s) and the outputs when asked."""
+    builders = builders or {}
+    kinds = sorted({j["scene"] for j in jobs})
+    descs = {k: builders[k] if k in builders else build_scene(k) for k in kinds}
+    handles = [{k: GpuScene(descs[k], device=device) for k in kinds} for _ in range(workers)]
+    for h in handles:                                    # warm the buffers of every handle
+        for k in kinds:
+            render_job(h, dict(scene=k, width=64, height=64, spp=1, azimuth=0.0, elevation=20.0, seed=0))
+    q = queue.Queue()
+    for j in jobs:
+        q.put(j)
+    lat, outs, errors = {}, {}, []
+    t0 = time.perf_counter()
+
+    def worker(h):
+        while True:
+            try:
+                j = q.get_nowait()
+            except queue.Empty:
+                return
+            try:
+                out = render_job(h, j)
+                lat[j["id"]] = time.perf_counter() - t0
+                if keep_outputs:
+                    outs[j["id"]] = out
+            except Exception as e:   # surfaced after the batch
+                errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(h,)) for h in handles]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    wall = time.perf_counter() - t0
+    if errors:
+        raise errors[0]
+    samples = sum(j["width"] * j["height"] * j["spp"] for j in jobs)
+    ls = np.array([lat[j["id"]] for j in jobs])
+    return dict(wall_s=wall, path_samples=samples, rate=samples / wall, p50_s=float(np.percentile(ls, 50)),
+                p99_s=float(np.percentile(ls, 99)), latencies=lat, outputs=outs)
