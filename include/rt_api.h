@@ -143,6 +143,29 @@ typedef struct RtMedium {
     int32_t perlin_perm[3 * 256];
 } RtMedium;
 
+/* ── analytic convex solids (diamond.rs:198-253) ─────────────────────────────
+ * A gem is a convex polyhedron: the intersection of outward half-spaces
+ * n·x ≤ d (`convex_planes`, 4 floats per plane, in the solid's OBJECT space).
+ * Each solid carries the placement the reference wraps around a gem
+ * (scene_file.rs:924-930): a uniform scale about the origin
+ * (transform.rs:15-27), a rotation about `pivot` (transform.rs:218-224) and a
+ * translation, i.e. x_world = rot·(scale·x − pivot) + pivot + translate.
+ * Identity: scale 1, rot = I, pivot = translate = 0.  Several solids may share
+ * one run of planes.  Canonical ids follow the spheres.  Materials must not
+ * be emissive. */
+#define RT_PRIM_CONVEX 3
+typedef struct RtConvex {
+    int32_t plane_offset;       /* first plane in convex_planes */
+    int32_t n_planes;           /* 4 .. 256 */
+    int32_t mat;
+    float   polish;             /* per-facet micro-tilt amplitude in radians (hittable.rs:261-270), 0 .. 0.25 */
+    float   box_lo[3], box_hi[3]; /* object-space box that contains the solid */
+    float   scale;              /* > 0 */
+    float   rot[9];             /* row-major world-from-object rotation */
+    float   pivot[3];
+    float   translate[3];
+} RtConvex;
+
 typedef struct RtSceneDesc {
     int64_t        n_tris;
     const float*   tri_v;         /* n_tris × 9  : v0, v1, v2 */
@@ -168,6 +191,10 @@ typedef struct RtSceneDesc {
     /* participating media (may be 0 / NULL) */
     int32_t        n_media;
     const RtMedium* media;
+    /* analytic convex solids (may be 0 / NULL); ids follow the spheres, media ids follow them */
+    int64_t        n_convex;
+    const RtConvex* convex;
+    const float*   convex_planes;  /* planes × 4: outward unit normal xyz, offset d (object space) */
 } RtSceneDesc;
 
 /* ── camera (src/camera.rs:24-59) ────────────────────────────────────────── */

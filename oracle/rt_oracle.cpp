@@ -388,7 +388,13 @@ struct Scene {
     // BVH
     std::vector<Node> nodes;
     std::vector<int32_t> leaf_prims;  // leaf slot → canonical prim id
-    int64_t n_tris = 0, n_quads = 0, n_spheres = 0;
+    int64_t n_tris = 0, n_quads = 0, n_spheres = 0, n_convex = 0;
+    // analytic convex solids (diamond.rs:198-253): outward half-spaces n·x ≤ d
+    // placed in world space; `off` indexes the solid's own run of world planes
+    struct Convex { int32_t off, n, mat; float polish; Aabb box; };
+    std::vector<Convex> convex;
+    std::vector<float> convex_planes;   // 4 floats per world plane
+    std::vector<V3> convex_shade;       // per world plane: front-face and back-face shading normal
     // caustic photon map (photon.rs:31-36): implicit kd-tree, kept in emission order too
     struct KdPhoton { float pos[3], power[3], nor[3]; uint8_t axis; int32_t idx; };
     std::vector<KdPhoton> photons;    // kd order
@@ -401,9 +407,13 @@ struct Scene {
     std::vector<std::vector<Quad>> media_quads;
 };
 
+static inline bool is_emissive_type(int t) { return t == RT_MAT_DIFFUSE_LIGHT || t == RT_MAT_BLACKBODY_LIGHT; }
 static inline int prim_type(const Scene& s, int64_t gid) {
-    return gid < s.n_tris ? RT_PRIM_TRI : (gid < s.n_tris + s.n_quads ? RT_PRIM_QUAD : RT_PRIM_SPHERE);
+    if (gid < s.n_tris) return RT_PRIM_TRI;
+    if (gid < s.n_tris + s.n_quads) return RT_PRIM_QUAD;
+    return gid < s.n_tris + s.n_quads + s.n_spheres ? RT_PRIM_SPHERE : RT_PRIM_CONVEX;
 }
+static inline int64_t n_prims(const Scene& s) { return s.n_tris + s.n_quads + s.n_spheres + s.n_convex; }
 
 static Aabb prim_box(const Scene& s, int64_t gid) {
     int t = prim_type(s, gid);
@@ -422,11 +432,12 @@ static Aabb prim_box(const Scene& s, int64_t gid) {
             mx = v3(rmax(mx.x, c[i].x), rmax(mx.y, c[i].y), rmax(mx.z, c[i].z));
         }
         return pad(Aabb{mn, mx});
-    } else {                                                                        // sphere.rs:111-118
+    } else if (t == RT_PRIM_SPHERE) {                                               // sphere.rs:111-118
         const Sphere& sp = s.spheres[gid - s.n_tris - s.n_quads];
         V3 r = v3(sp.r, sp.r, sp.r);
         return Aabb{sp.c - r, sp.c + r};
     }
+    return s.convex[gid - s.n_tris - s.n_quads - s.n_spheres].box;                  // diamond.rs:172-186
 }
 
 // ── BVH build (bvh.rs:52-225) ────────────────────────────────────────────────
@@ -554,7 +565,7 @@ static int32_t build_rec(Builder& B, const std::vector<int32_t>& objs, Aabb* out
 }
 
 static void build_bvh(Scene& s) {                                                   // bvh.rs:199-225
-    int64_t n = s.n_tris + s.n_quads + s.n_spheres;
+    int64_t n = n_prims(s);
     s.nodes.clear(); s.leaf_prims.clear();
     if (n == 0) return;
     std::vector<Aabb> boxes(n);
@@ -627,12 +638,51 @@ static inline bool sphere_hit(const Sphere& sp, const Ray& r, float tmin, float 
     *t_out = root;
     return true;
 }
+// convex_hit (diamond.rs:202-253): the interval inside every half-space; the
+// entry for outside rays, the exit for rays inside the solid.  *plane is the
+// index of the crossing plane.
+static bool convex_hit(const float* planes, int32_t n, const Ray& r, float tmin, float tmax, float* t_out,
+                       int32_t* plane) {
+    float t_enter = tmin, t_exit = tmax;
+    int32_t enter_i = -1, exit_i = -1;
+    bool entry_found = false;
+    for (int32_t i = 0; i < n; i++) {
+        V3 nv = v3(planes[i * 4], planes[i * 4 + 1], planes[i * 4 + 2]);
+        float d = planes[i * 4 + 3];
+        float nd = dot(nv, r.d);
+        float t_face = (d - dot(nv, r.o)) / nd;
+        if (std::fabs(nd) < 1e-8f) {
+            if (dot(nv, r.o) > d) return false;
+            continue;
+        }
+        if (nd < 0.0f) {
+            if (t_face > t_enter) { t_enter = t_face; enter_i = i; entry_found = true; }
+        } else {
+            if (t_face < t_exit) { t_exit = t_face; exit_i = i; }
+        }
+        if (t_enter > t_exit) return false;
+    }
+    if (t_enter > t_exit) return false;
+    if (t_enter == t_exit && t_enter < tmax) return false;
+    if (entry_found) { *t_out = t_enter; *plane = enter_i; return true; }
+    if (t_exit > tmax) return false;
+    *t_out = t_exit; *plane = exit_i;
+    return true;
+}
+
 static inline bool prim_hit(const Scene& s, int64_t gid, const Ray& r, float tmin, float tmax,
                             float* t, float* b1, float* b2) {
     if (gid < s.n_tris) return tri_hit(s.tris[gid], r, tmin, tmax, t, b1, b2);
     if (gid < s.n_tris + s.n_quads) return quad_hit(s.quads[gid - s.n_tris], r, tmin, tmax, t, b1, b2);
     *b1 = 0.0f; *b2 = 0.0f;
-    return sphere_hit(s.spheres[gid - s.n_tris - s.n_quads], r, tmin, tmax, t);
+    if (gid < s.n_tris + s.n_quads + s.n_spheres) return sphere_hit(s.spheres[gid - s.n_tris - s.n_quads], r, tmin, tmax, t);
+    const Scene::Convex& c = s.convex[gid - s.n_tris - s.n_quads - s.n_spheres];
+    int32_t pi = -1;
+    if (!convex_hit(s.convex_planes.data() + (size_t)c.off * 4, c.n, r, tmin, tmax, t, &pi)) return false;
+    // the crossing plane's index rides in b1 (an exit with no exit plane keeps -1)
+    int32_t bits = pi;
+    memcpy(b1, &bits, 4);
+    return true;
 }
 
 // ── traversal (bvh.rs:229-288, slab test :326-364) ───────────────────────────
@@ -733,7 +783,7 @@ static HitRes closest_hit(const Scene& s, const Ray& r, float tmin, float tmax, 
 static HitRes closest_hit_brute(const Scene& s, const Ray& r, float tmin, float tmax) {
     HitRes best{-1, tmax, 0.0f, 0.0f};
     if (ray_has_nan(r, tmin, tmax)) return best;
-    int64_t n = s.n_tris + s.n_quads + s.n_spheres;
+    int64_t n = n_prims(s);
     float closest = tmax;
     for (int64_t g = 0; g < n; g++) {
         float t, b1, b2;
@@ -945,6 +995,58 @@ static inline V3 sphere_uv_calc(V3 p, float* u, float* v) {                     
     return p;
 }
 
+// micro_tilt (hittable.rs:261-270): a fixed per-facet tilt of the normal
+static V3 micro_tilt(uint64_t idx, float amp, V3 n) {
+    if (amp <= 0.0f) return n;
+    uint64_t h = (idx * 0x9E3779B97F4A7C15ull) ^ 0xD1B54A32D192ED03ull;
+    float a = (float)(uint32_t)(h >> 32) / (float)UINT32_MAX * 2.0f - 1.0f;
+    float b = (float)(uint32_t)h / (float)UINT32_MAX * 2.0f - 1.0f;
+    V3 up = std::fabs(n.x) < 0.9f ? v3(1, 0, 0) : v3(0, 1, 0);
+    V3 t = unit(cross(n, up));
+    V3 b2 = cross(n, t);
+    return unit(n + t * (a * amp) + b2 * (b * amp));
+}
+
+// Gem placement (scene_file.rs:924-930): UniformScale about the origin
+// (transform.rs:15-27), Rotate::euler_about the gem's center
+// (transform.rs:218-224), Translate.  The reference moves the ray into object
+// space; here the planes move to world space instead (the same half-spaces):
+// x_w = R(s x − p) + p + t, so n·x ≤ d becomes (R n)·x_w ≤ (R n)·(p + t) + s d − n·p.
+static V3 rot_apply(const float* R, V3 v) {                                         // transform.rs:150-156
+    return v3(R[0] * v.x + R[1] * v.y + R[2] * v.z, R[3] * v.x + R[4] * v.y + R[5] * v.z,
+              R[6] * v.x + R[7] * v.y + R[8] * v.z);
+}
+static void place_planes(const RtConvex& c, const float* pl, std::vector<float>& out, std::vector<V3>& shade) {
+    V3 p = v3(c.pivot[0], c.pivot[1], c.pivot[2]);
+    V3 pt = v3(c.pivot[0] + c.translate[0], c.pivot[1] + c.translate[1], c.pivot[2] + c.translate[2]);
+    for (int j = 0; j < c.n_planes; j++) {
+        V3 n = v3(pl[j * 4], pl[j * 4 + 1], pl[j * 4 + 2]);
+        V3 nw = rot_apply(c.rot, n);
+        float dw = dot(nw, pt) + (c.scale * pl[j * 4 + 3] - dot(n, p));
+        out.insert(out.end(), {nw.x, nw.y, nw.z, dw});
+        // Diamond::hit tilts the object-space face normal of the first plane
+        // whose normal matches (diamond.rs:266-270); Rotate then turns it.
+        int f = 0;
+        while (f < j && !(std::fabs(pl[f * 4] - n.x) < 1e-6f && std::fabs(pl[f * 4 + 1] - n.y) < 1e-6f &&
+                          std::fabs(pl[f * 4 + 2] - n.z) < 1e-6f)) f++;
+        shade.push_back(rot_apply(c.rot, micro_tilt((uint64_t)f, c.polish, n)));
+        shade.push_back(rot_apply(c.rot, micro_tilt((uint64_t)f, c.polish, -n)));
+    }
+}
+static Aabb placed_box(const RtConvex& c) {                                         // transform.rs:180-200
+    V3 mn = v3(INFINITY, INFINITY, INFINITY), mx = v3(-INFINITY, -INFINITY, -INFINITY);
+    V3 p = v3(c.pivot[0], c.pivot[1], c.pivot[2]), t = v3(c.translate[0], c.translate[1], c.translate[2]);
+    for (int k = 0; k < 8; k++) {
+        V3 x = v3(k & 1 ? c.box_hi[0] : c.box_lo[0], k & 2 ? c.box_hi[1] : c.box_lo[1], k & 4 ? c.box_hi[2] : c.box_lo[2]);
+        V3 w = rot_apply(c.rot, x * c.scale - p) + p + t;
+        mn = v3(std::fmin(mn.x, w.x), std::fmin(mn.y, w.y), std::fmin(mn.z, w.z));
+        mx = v3(std::fmax(mx.x, w.x), std::fmax(mx.y, w.y), std::fmax(mx.z, w.z));
+    }
+    float e = 1e-5f * std::fmax(std::fmax(std::fmax(std::fabs(mn.x), std::fabs(mx.x)), std::fmax(std::fabs(mn.y), std::fabs(mx.y))),
+                                std::fmax(std::fabs(mn.z), std::fabs(mx.z))) + 1e-6f;
+    return Aabb{mn - v3(e, e, e), mx + v3(e, e, e)};
+}
+
 static Rec make_rec(const Scene& s, const Ray& r, const HitRes& h) {
     Rec rec;
     rec.gid = h.gid; rec.t = h.t;
@@ -967,11 +1069,23 @@ static Rec make_rec(const Scene& s, const Ray& r, const HitRes& h) {
         outward = q.normal;
         rec.u = h.b1; rec.v = h.b2;
         rec.mat = q.mat;
-    } else {
+    } else if (t == RT_PRIM_SPHERE) {
         const Sphere& sp = s.spheres[h.gid - s.n_tris - s.n_quads];
         outward = (rec.p - sp.c) / sp.r;
         sphere_uv_calc(outward, &rec.u, &rec.v);
         rec.mat = sp.mat;
+    } else {                                                                        // diamond.rs:257-275
+        const Scene::Convex& c = s.convex[h.gid - s.n_tris - s.n_quads - s.n_spheres];
+        int32_t pi;
+        memcpy(&pi, &h.b1, 4);
+        if (pi < 0) pi = 0;                         // (1,0,0)·… fallback of an unbounded exit: plane 0's normal
+        const float* pl = s.convex_planes.data() + (size_t)(c.off + pi) * 4;
+        outward = v3(pl[0], pl[1], pl[2]);
+        rec.u = 0.0f; rec.v = 0.0f;
+        rec.mat = c.mat;
+        rec.front = dot(r.d, outward) < 0.0f;
+        rec.normal = s.convex_shade[(size_t)(c.off + pi) * 2 + (rec.front ? 0 : 1)];
+        return rec;
     }
     rec.front = dot(r.d, outward) < 0.0f;
     rec.normal = rec.front ? outward : -outward;
@@ -1422,7 +1536,7 @@ static inline Rng photon_rng(uint64_t seed, uint32_t gid) {
 
 // photon_bounds of the world (hittable.rs:199-212): union of the primitive boxes
 static Aabb world_bounds(const Scene& s) {
-    int64_t n = s.n_tris + s.n_quads + s.n_spheres;
+    int64_t n = n_prims(s);
     bool any = n > 0;
     Aabb b = any ? prim_box(s, 0) : Aabb{v3(0, 0, 0), v3(0, 0, 0)};
     for (int64_t i = 1; i < n; i++) b = surrounding(b, prim_box(s, i));
@@ -1946,6 +2060,20 @@ static int scene_create(const RtSceneDesc* d, Scene** out) {
         s->media.push_back(m);
         s->media_quads.push_back(qs);
     }
+    // analytic convex solids (diamond.rs:93-195)
+    if (d->n_convex < 0 || (d->n_convex > 0 && (!d->convex || !d->convex_planes))) {
+        delete s; g_err = "bad convex list"; return RT_ERR_INVALID;
+    }
+    s->n_convex = d->n_convex;
+    for (int64_t i = 0; i < d->n_convex; i++) {
+        const RtConvex& c = d->convex[i];
+        bool ok = c.n_planes >= 4 && c.n_planes <= 256 && c.plane_offset >= 0 && c.mat >= 0 && c.mat < d->n_mats &&
+                  !is_emissive_type(d->mats[c.mat].type) && c.scale > 0.0f && c.polish >= 0.0f && c.polish <= 0.25f;
+        if (!ok) { delete s; g_err = "invalid convex solid " + std::to_string(i); return RT_ERR_INVALID; }
+        int32_t off = (int32_t)(s->convex_planes.size() / 4);
+        place_planes(c, d->convex_planes + (size_t)c.plane_offset * 4, s->convex_planes, s->convex_shade);
+        s->convex.push_back(Scene::Convex{off, c.n_planes, c.mat, c.polish, placed_box(c)});
+    }
     s->lights.assign(d->light_prims, d->light_prims + d->n_lights);
     s->bg = d->bg;
     s->has_env = d->bg.type == RT_BG_ENVMAP && d->bg.env_rgb && d->bg.env_w > 0 && d->bg.env_h > 0;
@@ -2021,7 +2149,7 @@ int32_t orc_trace_closest(void* sp, const float* rays, int64_t n, RtHit* hits, i
             HitRes h = mode == 1 ? closest_hit_brute(*s, ray, r[6], r[7]) : closest_hit<false>(*s, ray, r[6], r[7], nullptr);
             float tm;
             int med = s->media.empty() ? -1 : media_event(*s, ray, 550.0f, r[6], h.gid < 0 ? r[7] : h.t, &tm);
-            if (med >= 0) h = HitRes{(int32_t)(s->n_tris + s->n_quads + s->n_spheres + med), tm, 0.0f, 0.0f};
+            if (med >= 0) h = HitRes{(int32_t)(n_prims(*s) + med), tm, 0.0f, 0.0f};
             hits[i].prim = h.gid; hits[i].t = h.gid >= 0 ? h.t : 0.0f;
             hits[i].b1 = h.gid >= 0 ? h.b1 : 0.0f; hits[i].b2 = h.gid >= 0 ? h.b2 : 0.0f;
         }

@@ -19,7 +19,7 @@ RT_METAL_GOLD, RT_METAL_COPPER, RT_METAL_SILVER, RT_METAL_CUSTOM = 0, 1, 2, 3
 RT_MAX_NK = 16
 
 RT_BG_SOLID, RT_BG_GRADIENT, RT_BG_ENVMAP, RT_BG_PHYSICAL = 0, 1, 2, 3
-RT_PRIM_TRI, RT_PRIM_QUAD, RT_PRIM_SPHERE = 0, 1, 2
+RT_PRIM_TRI, RT_PRIM_QUAD, RT_PRIM_SPHERE, RT_PRIM_CONVEX = 0, 1, 2, 3
 
 F3 = C.c_float * 3
 
@@ -86,6 +86,21 @@ class RtMedium(C.Structure):
     ]
 
 
+class RtConvex(C.Structure):
+    _fields_ = [
+        ("plane_offset", C.c_int32),
+        ("n_planes", C.c_int32),
+        ("mat", C.c_int32),
+        ("polish", C.c_float),
+        ("box_lo", F3),
+        ("box_hi", F3),
+        ("scale", C.c_float),
+        ("rot", C.c_float * 9),
+        ("pivot", F3),
+        ("translate", F3),
+    ]
+
+
 class RtSceneDesc(C.Structure):
     _fields_ = [
         ("n_tris", C.c_int64),
@@ -106,6 +121,9 @@ class RtSceneDesc(C.Structure):
         ("spectral_range", C.c_int32),
         ("n_media", C.c_int32),
         ("media", C.POINTER(RtMedium)),
+        ("n_convex", C.c_int64),
+        ("convex", C.POINTER(RtConvex)),
+        ("convex_planes", C.POINTER(C.c_float)),
     ]
 
 

@@ -89,6 +89,13 @@ struct DevScene {
     int n_lights, n_mats;
     const DevMedium* media;
     int n_media;
+    // analytic convex solids in leaf order: 2 float4 each, (plane offset, count,
+    // material, polish) (canonical id, -, -, -); their world-space planes
+    // (n.xyz, d); per plane the world-space shading normals of a front-face and
+    // a back-face hit, micro-tilted in object space (diamond.rs:267-270)
+    const float4* cvx;
+    const float4* cvx_planes;
+    const float4* cvx_shade;
     // spectral tables: CIE x̄ȳz̄ on the 5 nm grid from 380 nm and the per-channel
     // normalisations of spectral_to_rgb / spectral_fire_rgb (spectrum.rs:78-177)
     const float4* cmf;          // n_spec entries (x, y, z, -)
@@ -173,6 +180,38 @@ enum {
 // whole line (the ray is inside the closed slab) so culling stays conservative.
 
 // ── primitive hit tests: same f32 operation sequence as the reference ────────
+// convex_hit (diamond.rs:202-253): the interval inside every half-space; the
+// entry for outside rays, the exit for rays inside; *plane = crossing plane.
+RT_D bool convex_test(const float4* pl, int n, float3 o, float3 d, float tmin, float tmax, float* t_out,
+                      int* plane) {
+    float t_enter = tmin, t_exit = tmax;
+    int enter_i = -1, exit_i = -1;
+    bool entry_found = false;
+    for (int i = 0; i < n; i++) {
+        float4 q = __ldg(pl + i);
+        float3 nv = make_float3(q.x, q.y, q.z);
+        float nd = nv.x * d.x + nv.y * d.y + nv.z * d.z;
+        float no = nv.x * o.x + nv.y * o.y + nv.z * o.z;
+        float t_face = (q.w - no) / nd;
+        if (fabsf(nd) < 1e-8f) {
+            if (no > q.w) return false;
+            continue;
+        }
+        if (nd < 0.0f) {
+            if (t_face > t_enter) { t_enter = t_face; enter_i = i; entry_found = true; }
+        } else {
+            if (t_face < t_exit) { t_exit = t_face; exit_i = i; }
+        }
+        if (t_enter > t_exit) return false;
+    }
+    if (t_enter > t_exit) return false;
+    if (t_enter == t_exit && t_enter < tmax) return false;
+    if (entry_found) { *t_out = t_enter; *plane = enter_i; return true; }
+    if (t_exit > tmax) return false;
+    *t_out = t_exit; *plane = exit_i;
+    return true;
+}
+
 // triangle.rs:75-89
 RT_D bool tri_test(float4 a, float4 b, float4 c, float3 o, float3 d, float tmin, float tmax,
                    float* t_out, float* b1o, float* b2o) {

@@ -42,6 +42,68 @@ static inline Box pad(Box b) {                                                  
     float px = b.mx.x - b.mn.x < D ? D : 0.0f, py = b.mx.y - b.mn.y < D ? D : 0.0f, pz = b.mx.z - b.mn.z < D ? D : 0.0f;
     return Box{h3(b.mn.x - px, b.mn.y - py, b.mn.z - pz), h3(b.mx.x + px, b.mx.y + py, b.mx.z + pz)};
 }
+// ── convex placement (transform.rs:15-27, 140-224; scene_file.rs:924-930) ──
+// x_world = R·(s·x − pivot) + pivot + t.  A plane n·x ≤ d maps to n'·x ≤ d'
+// with n' = R·n and d' = n'·(pivot + t) + (s·d − n·pivot).
+static bool rotation_ok(const float* R) {
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            double dot = 0.0;
+            for (int k = 0; k < 3; k++) dot += (double)R[a * 3 + k] * R[b * 3 + k];
+            if (!(std::fabs(dot - (a == b ? 1.0 : 0.0)) < 1e-3)) return false;
+        }
+    return true;
+}
+static inline H3 rot_apply(const float* R, H3 v) {                                  // transform.rs:150-156
+    return h3(R[0] * v.x + R[1] * v.y + R[2] * v.z, R[3] * v.x + R[4] * v.y + R[5] * v.z,
+              R[6] * v.x + R[7] * v.y + R[8] * v.z);
+}
+// micro_tilt (hittable.rs:261-270) on the host
+static H3 micro_tilt_h(uint64_t idx, float amp, H3 n) {
+    if (!(amp > 0.0f)) return n;
+    uint64_t h = idx * 0x9E3779B97F4A7C15ull ^ 0xD1B54A32D192ED03ull;
+    float a = (float)(uint32_t)(h >> 32) / 4294967295.0f * 2.0f - 1.0f;
+    float b = (float)(uint32_t)h / 4294967295.0f * 2.0f - 1.0f;
+    H3 up = std::fabs(n.x) < 0.9f ? h3(1.f, 0.f, 0.f) : h3(0.f, 1.f, 0.f);
+    H3 t = hcross(n, up);
+    t = t / hlen(t);
+    H3 b2 = hcross(n, t);
+    H3 m = n + t * (a * amp) + b2 * (b * amp);
+    return m / hlen(m);
+}
+static void place_convex(const RtConvex& c, const float* pl, float4* out, float4* shade) {
+    H3 pv = h3(c.pivot[0], c.pivot[1], c.pivot[2]);
+    H3 pt = h3(c.pivot[0] + c.translate[0], c.pivot[1] + c.translate[1], c.pivot[2] + c.translate[2]);
+    for (int j = 0; j < c.n_planes; j++) {
+        H3 n = h3(pl[j * 4], pl[j * 4 + 1], pl[j * 4 + 2]);
+        H3 nw = rot_apply(c.rot, n);
+        float dw = hdot(nw, pt) + (c.scale * pl[j * 4 + 3] - hdot(n, pv));
+        out[j] = make_float4(nw.x, nw.y, nw.z, dw);
+        // the facet a polished normal is keyed on: the first plane with this normal (diamond.rs:267-269)
+        int f = 0;
+        while (f < j && !(std::fabs(pl[f * 4] - n.x) < 1e-6f && std::fabs(pl[f * 4 + 1] - n.y) < 1e-6f &&
+                          std::fabs(pl[f * 4 + 2] - n.z) < 1e-6f)) f++;
+        H3 sf = rot_apply(c.rot, micro_tilt_h((uint64_t)f, c.polish, n));
+        H3 sb = rot_apply(c.rot, micro_tilt_h((uint64_t)f, c.polish, h3(-n.x, -n.y, -n.z)));
+        shade[j * 2] = make_float4(sf.x, sf.y, sf.z, 0.f);
+        shade[j * 2 + 1] = make_float4(sb.x, sb.y, sb.z, 0.f);
+    }
+}
+static Box placed_box(const RtConvex& c) {                                          // transform.rs:180-200
+    Box b{h3(INFINITY, INFINITY, INFINITY), h3(-INFINITY, -INFINITY, -INFINITY)};
+    H3 pv = h3(c.pivot[0], c.pivot[1], c.pivot[2]), t = h3(c.translate[0], c.translate[1], c.translate[2]);
+    for (int k = 0; k < 8; k++) {
+        H3 x = h3(k & 1 ? c.box_hi[0] : c.box_lo[0], k & 2 ? c.box_hi[1] : c.box_lo[1], k & 4 ? c.box_hi[2] : c.box_lo[2]);
+        H3 w = rot_apply(c.rot, x * c.scale - pv) + pv + t;
+        b = unite(b, Box{w, w});
+    }
+    // the corners' rounding must not cut into the solid
+    float e = 1e-5f * std::max(std::max(std::fabs(b.mn.x), std::fabs(b.mx.x)),
+                               std::max(std::max(std::fabs(b.mn.y), std::fabs(b.mx.y)),
+                                        std::max(std::fabs(b.mn.z), std::fabs(b.mx.z)))) + 1e-6f;
+    return Box{b.mn - h3(e, e, e), b.mx + h3(e, e, e)};
+}
+
 static inline float area(const Box& b) {
     H3 d = b.mx - b.mn;
     return 2.0f * (d.x * d.y + d.y * d.z + d.z * d.x);
@@ -371,6 +433,7 @@ struct RtScene {
 };
 
 static void free_paths(RtScene* s);
+static inline float __int_as_float_h(int32_t v) { float f; memcpy(&f, &v, 4); return f; }
 
 static int fail(RtScene* s, int code, const std::string& msg) {
     if (s) s->err = msg;
@@ -467,8 +530,11 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     // ── validate ────────────────────────────────────────────────────────────
     if (d->n_tris < 0 || d->n_quads < 0 || d->n_spheres < 0 || d->n_mats < 0 || d->n_lights < 0)
         return bail(fail(s, RT_ERR_INVALID, "negative count"));
-    int64_t n = d->n_tris + d->n_quads + d->n_spheres;
-    if (n >= (1ll << 28)) return bail(fail(s, RT_ERR_CAPACITY, "more than 2^28 primitives"));
+    if (d->n_convex < 0 || (d->n_convex > 0 && (!d->convex || !d->convex_planes)))
+        return bail(fail(s, RT_ERR_INVALID, "convex solids without their arrays"));
+    const int64_t n_sph_end = d->n_tris + d->n_quads + d->n_spheres;   // canonical ids of the convex solids start here
+    int64_t n = n_sph_end + d->n_convex;
+    if (n >= (1ll << 28) - 1) return bail(fail(s, RT_ERR_CAPACITY, "more than 2^28 - 2 primitives"));
     s->n_prims = n;
     if ((d->n_tris && (!d->tri_v || !d->tri_mat)) || (d->n_quads && (!d->quad_quv || !d->quad_mat)) ||
         (d->n_spheres && (!d->sphere || !d->sphere_mat)) || (d->n_mats && !d->mats) || (d->n_lights && !d->light_prims))
@@ -488,8 +554,29 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     if (d->n_lights > 4096) return bail(fail(s, RT_ERR_CAPACITY, "more than 4096 NEE lights"));
     for (int32_t i = 0; i < d->n_lights; i++) {
         int64_t g = d->light_prims[i];
-        if (g < d->n_tris || g >= n) return bail(fail(s, RT_ERR_INVALID, "light list entries must be quads or spheres"));
+        if (g < d->n_tris || g >= n_sph_end) return bail(fail(s, RT_ERR_INVALID, "light list entries must be quads or spheres"));
     }
+    int64_t n_planes_total = 0, n_world_planes = 0;
+    for (int64_t i = 0; i < d->n_convex; i++) {
+        const RtConvex& c = d->convex[i];
+        if (c.n_planes < 4 || c.n_planes > 256 || c.plane_offset < 0 || bad_mat(c.mat))
+            return bail(fail(s, RT_ERR_INVALID, "convex solid " + std::to_string(i) + ": 4..256 planes and a valid material"));
+        int mt = d->mats[c.mat].type;
+        if (mt == RT_MAT_DIFFUSE_LIGHT || mt == RT_MAT_BLACKBODY_LIGHT)
+            return bail(fail(s, RT_ERR_INVALID, "convex solid " + std::to_string(i) + ": emissive materials are not supported"));
+        for (int a = 0; a < 3; a++)
+            if (!(c.box_lo[a] <= c.box_hi[a]) || !std::isfinite(c.box_lo[a]) || !std::isfinite(c.box_hi[a]))
+                return bail(fail(s, RT_ERR_INVALID, "convex solid " + std::to_string(i) + ": invalid box"));
+        if (!(c.polish >= 0.0f && c.polish <= 0.25f) || !(c.scale > 0.0f) || !std::isfinite(c.scale) ||
+            !rotation_ok(c.rot) || !std::isfinite(c.pivot[0] + c.pivot[1] + c.pivot[2]) ||
+            !std::isfinite(c.translate[0] + c.translate[1] + c.translate[2]))
+            return bail(fail(s, RT_ERR_INVALID, "convex solid " + std::to_string(i) +
+                                                    ": polish in [0, 0.25], a positive scale, a rotation matrix"));
+        n_planes_total = std::max<int64_t>(n_planes_total, (int64_t)c.plane_offset + c.n_planes);
+        n_world_planes += c.n_planes;
+    }
+    for (int64_t k = 0; k < n_planes_total * 4; k++)
+        if (!std::isfinite(d->convex_planes[k])) return bail(fail(s, RT_ERR_INVALID, "non-finite convex plane"));
     if (d->bg.type == RT_BG_ENVMAP && (!d->bg.env_rgb || d->bg.env_w <= 0 || d->bg.env_h <= 0))
         return bail(fail(s, RT_ERR_INVALID, "env map background without an image"));
 
@@ -527,6 +614,16 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         H3 c = h3(p[0], p[1], p[2]), r = h3(p[3], p[3], p[3]);
         boxes[d->n_tris + d->n_quads + i] = Box{c - r, c + r};
     }
+    // convex solids: planes, shading normals and boxes in world space
+    std::vector<float4> wpl(std::max<int64_t>(n_world_planes, 1)), wsh(std::max<int64_t>(n_world_planes * 2, 2));
+    std::vector<int32_t> wofs(d->n_convex);
+    for (int64_t i = 0, o = 0; i < d->n_convex; i++) {
+        const RtConvex& c = d->convex[i];
+        wofs[i] = (int32_t)o;
+        place_convex(c, d->convex_planes + (size_t)c.plane_offset * 4, wpl.data() + o, wsh.data() + o * 2);
+        boxes[n_sph_end + i] = placed_box(c);
+        o += c.n_planes;
+    }
 
     if (n > 0) {
         Box wb = boxes[0];
@@ -550,12 +647,13 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         s->n_leaves = (int64_t)s->leaf_gids.size();
         // leaf order per type
         std::vector<int32_t> typed_slot(s->n_leaves);
-        std::vector<int64_t> order_tri, order_quad, order_sph;
+        std::vector<int64_t> order_tri, order_quad, order_sph, order_cvx;
         for (int64_t k = 0; k < s->n_leaves; k++) {
             int64_t g = s->leaf_gids[k];
             if (g < d->n_tris) { typed_slot[k] = (int32_t)order_tri.size(); order_tri.push_back(g); }
             else if (g < d->n_tris + d->n_quads) { typed_slot[k] = (int32_t)order_quad.size(); order_quad.push_back(g - d->n_tris); }
-            else { typed_slot[k] = (int32_t)order_sph.size(); order_sph.push_back(g - d->n_tris - d->n_quads); }
+            else if (g < n_sph_end) { typed_slot[k] = (int32_t)order_sph.size(); order_sph.push_back(g - d->n_tris - d->n_quads); }
+            else { typed_slot[k] = (int32_t)order_cvx.size(); order_cvx.push_back(g - n_sph_end); }
         }
         double root_sa = 0.0;
         gnodes.resize((size_t)s->n_nodes * 14);
@@ -578,7 +676,8 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
                 else {
                     int64_t slot = -(int64_t)v - 1;
                     int64_t g = s->leaf_gids[slot];
-                    uint32_t type = g < d->n_tris ? RT_PRIM_TRI : (g < d->n_tris + d->n_quads ? RT_PRIM_QUAD : RT_PRIM_SPHERE);
+                    uint32_t type = g < d->n_tris ? RT_PRIM_TRI : (g < d->n_tris + d->n_quads ? RT_PRIM_QUAD
+                                                                  : (g < n_sph_end ? RT_PRIM_SPHERE : RT_PRIM_CONVEX));
                     ch[c] = RT_LEAF_BIT | (type << 28) | (uint32_t)typed_slot[slot];
                 }
             }
@@ -667,7 +766,19 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
                 L.g[0] = make_float4(p[0], p[1], p[2], p[3]);
             }
         }
+        // convex solids in leaf order, pointing at their world-space planes
+        std::vector<float4> gcvx(std::max<size_t>(order_cvx.size() * 2, 2));
+        for (size_t k = 0; k < order_cvx.size(); k++) {
+            const RtConvex& c = d->convex[order_cvx[k]];
+            int32_t gi = (int32_t)(n_sph_end + order_cvx[k]);
+            gcvx[k * 2] = make_float4(__int_as_float_h(wofs[order_cvx[k]]), __int_as_float_h(c.n_planes),
+                                      __int_as_float_h(c.mat), c.polish);
+            gcvx[k * 2 + 1] = make_float4(__int_as_float_h(gi), 0.f, 0.f, 0.f);
+        }
         int rc;
+        if ((rc = upload(s, gcvx.data(), gcvx.size(), &s->S.cvx))) return bail(rc);
+        if ((rc = upload(s, wpl.data(), wpl.size(), &s->S.cvx_planes))) return bail(rc);
+        if ((rc = upload(s, wsh.data(), wsh.size(), &s->S.cvx_shade))) return bail(rc);
         if ((rc = upload(s, gnodes.data(), gnodes.size(), &s->S.nodes))) return bail(rc);
         if ((rc = upload(s, gtri.data(), gtri.size(), &s->S.tri))) return bail(rc);
         if ((rc = upload(s, gtri_n.data(), gtri_n.size(), &s->S.tri_n))) return bail(rc);

@@ -182,7 +182,7 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                 float3 p = o + t * d;
                 uint32_t type = RT_HIT_TYPE(ref), idx = RT_HIT_INDEX(ref);
                 float3 outward;
-                int mat;
+                int mat, cvx_wp = 0;
                 if (type == RT_PRIM_TRI) {
                     const float4* g = S.tri + (size_t)idx * 3;
                     float4 ga = __ldg(g), gb = __ldg(g + 1), gc = __ldg(g + 2);
@@ -202,14 +202,24 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                     float4 g0 = __ldg(g);
                     outward = mk(g0.x, g0.y, g0.z);
                     mat = __float_as_int(__ldg(g + 4).y);
-                } else {
+                } else if (type == RT_PRIM_SPHERE) {
                     const float4* g = S.sphere + (size_t)idx * 2;
                     float4 s0 = __ldg(g);
                     outward = (p - mk(s0.x, s0.y, s0.z)) / s0.w;
                     mat = __float_as_int(__ldg(g + 1).y);
+                } else {                                    // convex solid: the crossing plane's normal
+                    float4 c0 = __ldg(S.cvx + (size_t)idx * 2);
+                    cvx_wp = __float_as_int(c0.x) + max(__float_as_int(hv.z), 0);
+                    float4 q = __ldg(S.cvx_planes + cvx_wp);
+                    outward = mk(q.x, q.y, q.z);
+                    mat = __float_as_int(c0.z);
                 }
                 bool front = dot3(d, outward) < 0.0f;
                 float3 nrm = front ? outward : -outward;
+                if (type == RT_PRIM_CONVEX) {               // polished facet normal, world space
+                    float4 sn = __ldg(S.cvx_shade + (size_t)cvx_wp * 2 + (front ? 0 : 1));
+                    nrm = mk(sn.x, sn.y, sn.z);
+                }
                 const DevMaterial& m = S.mats[mat];
                 Rng rng = photon_rng(seed, gid);
                 uint32_t base = P_BOUNCE0 + bounce * P_PER_BOUNCE;

@@ -651,11 +651,22 @@ RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
         float4 g0 = __ldg(g);
         outward = mk(g0.x, g0.y, g0.z);
         r.mat = __float_as_int(__ldg(g + 4).y);
-    } else {                                                                        // sphere.rs:62-68
+    } else if (type == RT_PRIM_SPHERE) {                                            // sphere.rs:62-68
         const float4* g = S.sphere + (size_t)idx * 2;
         float4 s0 = __ldg(g);
         outward = (r.p - mk(s0.x, s0.y, s0.z)) / s0.w;
         r.mat = __float_as_int(__ldg(g + 1).y);
+    } else {                                                                        // diamond.rs:257-275
+        float4 c0 = __ldg(S.cvx + (size_t)idx * 2);
+        int pi = max(__float_as_int(hv.z), 0);
+        int wp = __float_as_int(c0.x) + pi;
+        float4 q = __ldg(S.cvx_planes + wp);
+        outward = mk(q.x, q.y, q.z);
+        r.mat = __float_as_int(c0.z);
+        r.front = dot3(d, outward) < 0.0f;
+        float4 sn = __ldg(S.cvx_shade + (size_t)wp * 2 + (r.front ? 0 : 1));   // polished facet normal, world space
+        r.nrm = mk(sn.x, sn.y, sn.z);
+        return r;
     }
     r.front = dot3(d, outward) < 0.0f;                                              // hittable.rs:89-93
     r.nrm = r.front ? outward : -outward;

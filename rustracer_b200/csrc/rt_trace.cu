@@ -43,13 +43,21 @@ RT_D void leaf_closest(const DevScene& S, uint32_t ref, float3 o, float3 d, floa
         float4 gm = h ? __ldg(g + 4) : make_float4(0.f, 0.f, 0.f, 0.f);
         gid = f2u(gm.x);
         mat = f2u(gm.y);
-    } else {
+    } else if (type == RT_PRIM_SPHERE) {
         const float4* g = S.sphere + (size_t)idx * 2;
         h = sphere_test(__ldg(g), o, d, tmin, best.t, &t);
         b1 = b2 = 0.0f;
         float4 gm = h ? __ldg(g + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
         gid = f2u(gm.x);
         mat = f2u(gm.y);
+    } else {                                        // convex solid; b1 carries the crossing plane
+        float4 c0 = __ldg(S.cvx + (size_t)idx * 2);
+        int pi = -1;
+        h = convex_test(S.cvx_planes + __float_as_int(c0.x), __float_as_int(c0.y), o, d, tmin, best.t, &t, &pi);
+        b1 = __int_as_float(pi);
+        b2 = 0.0f;
+        gid = h ? f2u(__ldg(S.cvx + (size_t)idx * 2 + 1).x) : 0u;
+        mat = f2u(c0.z);
     }
     if (h && (t < best.t || best.ref == RT_MISS_REF || gid < best.gid)) {
         best.t = t; best.b1 = b1; best.b2 = b2; best.ref = ref; best.gid = gid; best.mat = mat;
@@ -67,7 +75,10 @@ RT_D bool leaf_any(const DevScene& S, uint32_t ref, float3 o, float3 d, float tm
         float4 gg[4] = {__ldg(g), __ldg(g + 1), __ldg(g + 2), __ldg(g + 3)};
         return quad_test(gg, o, d, tmin, tmax, &t, &b1, &b2);
     }
-    return sphere_test(__ldg(S.sphere + (size_t)idx * 2), o, d, tmin, tmax, &t);
+    if (type == RT_PRIM_SPHERE) return sphere_test(__ldg(S.sphere + (size_t)idx * 2), o, d, tmin, tmax, &t);
+    float4 c0 = __ldg(S.cvx + (size_t)idx * 2);
+    int pi;
+    return convex_test(S.cvx_planes + __float_as_int(c0.x), __float_as_int(c0.y), o, d, tmin, tmax, &t, &pi);
 }
 
 #ifndef RT_MNMX3

@@ -171,6 +171,7 @@ class SceneBuilder:
         self.camera = None       # dict(look_from, look_at, vfov, aperture, focus_dist)
         self.caustics = None
         self.media = []          # abi.RtMedium
+        self.convex = []         # dicts: object-space planes (k,4) float32, mat, polish, box, placement
 
     # materials ---------------------------------------------------------
     def add_material(self, m):
@@ -213,6 +214,35 @@ class SceneBuilder:
         m.perlin_perm[:] = [int(x) for x in perm.reshape(-1)]
         self.media.append(m)
         return len(self.media) - 1
+
+    # analytic convex solids (diamond.rs:198-253) ----------------------
+    def add_convex(self, planes, mat, box_lo, box_hi, polish=0.0, scale=1.0, rot=None, pivot=(0.0, 0.0, 0.0),
+                   translate=(0.0, 0.0, 0.0)):
+        """A convex polyhedron given by object-space outward half-spaces
+        (n.xyz, d), interior n·x ≤ d, and an object-space box that contains it,
+        placed at x_world = rot·(scale·x − pivot) + pivot + translate."""
+        pl = np.ascontiguousarray(np.asarray(planes, dtype=F32).reshape(-1, 4))
+        R = np.eye(3) if rot is None else np.asarray(rot, dtype=np.float64).reshape(3, 3)
+        self.convex.append(dict(planes=pl, mat=mat, polish=float(polish), lo=tuple(map(float, box_lo)),
+                                hi=tuple(map(float, box_hi)), scale=float(scale), rot=R,
+                                pivot=tuple(map(float, pivot)), translate=tuple(map(float, translate))))
+        return len(self.convex) - 1
+
+    def add_diamond(self, center, radius, mat, table_pct=53.0, crown_angle=34.5, pavilion_angle=40.75, polish=0.0,
+                    oval_ratio=1.0, girdle_facets=16, girdle_finish="uniform", girdle_pct=2.0, scale=1.0,
+                    rotate=None, pivot=None, translate=(0.0, 0.0, 0.0)):
+        """Diamond::new (diamond.rs:93-195): the round/oval brilliant's
+        half-spaces, placed as the scene file does (scene_file.rs:924-930,
+        1036-1042): a uniform scale about the origin, an Euler rotation in
+        degrees about `pivot` (the gem's own center when None), then a
+        translation."""
+        planes, lo, hi = diamond_planes(center, radius, table_pct, crown_angle, pavilion_angle, oval_ratio,
+                                        girdle_facets, girdle_finish, girdle_pct)
+        pol = min(max(polish, 0.0), 0.25) if math.isfinite(polish) else 0.0       # diamond.rs:193
+        ang = [0.0, 0.0, 0.0] if rotate is None else [float(a) for a in rotate]
+        R = _euler_fwd(ang) if any(a != 0.0 for a in ang) else np.eye(3)
+        return self.add_convex(planes, mat, lo, hi, polish=pol, scale=scale, rot=R,
+                               pivot=center if pivot is None else pivot, translate=translate)
 
     def add_quad(self, corner, u, v, mat, xf=None):
         q, uu, vv = (np.asarray(a, dtype=np.float64) for a in (corner, u, v))
@@ -393,6 +423,22 @@ class SceneBuilder:
                     bg.visible_bottom = _f3(vis["bottom"])
         d.bg = bg
         d.spectral_range = int(self.spectral_range)
+        if self.convex:
+            offs, recs = 0, []
+            for c in self.convex:
+                r = abi.RtConvex()
+                r.plane_offset, r.n_planes, r.mat, r.polish = offs, len(c["planes"]), c["mat"], c["polish"]
+                r.box_lo, r.box_hi = _f3(c["lo"]), _f3(c["hi"])
+                r.scale = c["scale"]
+                r.rot = (C.c_float * 9)(*[float(v) for v in c["rot"].reshape(-1)])
+                r.pivot, r.translate = _f3(c["pivot"]), _f3(c["translate"])
+                recs.append(r)
+                offs += len(c["planes"])
+            self._cvx = (abi.RtConvex * len(recs))(*recs)
+            self._cvp = np.ascontiguousarray(np.concatenate([c["planes"] for c in self.convex]).astype(F32))
+            d.n_convex = len(recs)
+            d.convex = C.cast(self._cvx, C.POINTER(abi.RtConvex))
+            d.convex_planes = abi.fptr(self._cvp)
         self._media = (abi.RtMedium * max(1, len(self.media)))(*self.media)
         d.n_media = len(self.media)
         d.media = C.cast(self._media, C.POINTER(abi.RtMedium)) if self.media else None
@@ -545,6 +591,194 @@ def _resolve(base, p):
     return cand if os.path.exists(cand) else p
 
 
+def diamond_planes(center, radius, table_pct=53.0, crown_angle=34.5, pavilion_angle=40.75, oval_ratio=1.0,
+                   girdle_facets=16, girdle_finish="uniform", girdle_pct=2.0):
+    """The half-spaces and bounding box of Diamond::new (diamond.rs:93-195), in
+    f32: the table, a crown and a pavilion facet through every girdle edge
+    (every other one with a knife-edge girdle), and the band's vertical planes
+    (the girdle n-gon when faceted, a 64-gon shell otherwise)."""
+    f = np.float32
+    cx, cy, cz = (f(c) for c in center)
+    r, q = f(radius), f(max(oval_ratio, 0.05))
+    table_r = f(table_pct / 100.0) * r
+    crown_h = (r - table_r) * f(math.tan(math.radians(crown_angle)))
+    pav_h = r * f(math.tan(math.radians(pavilion_angle)))
+    girdle_h = f(min(max(girdle_pct / 100.0 * 2.0 * float(r), 0.0), 0.3 * float(r)))
+    n = (max(int(girdle_facets), 4) // 2) * 2
+    m = n // 2
+    band_m = n if girdle_finish == "faceted" else 64
+    planes = []
+
+    def unit(v):
+        v = np.asarray(v, f)
+        return (v / f(math.sqrt(float(v @ v)))).astype(f)
+
+    def push(nv, g):
+        # the oval is the round stone stretched by q along x ABOUT ITS CENTER;
+        # the reference stretches about the origin (q·g.x), which moves an
+        # off-axis oval away from its own bounding box — the one deliberate
+        # difference; round stones (q = 1) and ovals at x = 0 are unchanged
+        nw = unit([f(nv[0]) / q, f(nv[1]), f(nv[2])])
+        gx = f(g[0]) if q == f(1.0) else cx + q * (f(g[0]) - cx)
+        gw = np.array([gx, f(g[1]), f(g[2])], f)
+        planes.append([nw[0], nw[1], nw[2], f(nw @ gw)])
+
+    push((0.0, 1.0, 0.0), (cx, cy + f(0.5) * girdle_h + crown_h, cz))
+    wavy = girdle_h > 0 and girdle_finish == "faceted"
+    band_h = lambda k: f(0.0) if (wavy and k % 2 == 1) else girdle_h
+    crown_n = n if girdle_h > 0 else m
+    for k in range(crown_n):
+        th = f(k) * f(2.0 * math.pi) / f(crown_n)
+        sn, c = f(math.sin(th)), f(math.cos(th))
+        push(unit([c * crown_h, r - table_r, sn * crown_h]), (cx + c * r, cy + f(0.5) * band_h(k), cz + sn * r))
+    pav_n = n if girdle_h > 0 else m
+    for k in range(pav_n):
+        ph = f(k) * f(2.0 * math.pi) / f(n) if girdle_h > 0 else f(k) * f(2.0 * math.pi) / f(m) + f(math.pi) / f(m)
+        sn, c = f(math.sin(ph)), f(math.cos(ph))
+        push(unit([c * pav_h, -r, sn * pav_h]), (cx + c * r, cy - f(0.5) * band_h(k), cz + sn * r))
+    if girdle_h > 0:
+        for j in range(band_m):
+            a = f(j) * f(2.0 * math.pi) / f(band_m)
+            sn, c = f(math.sin(a)), f(math.cos(a))
+            push((c, 0.0, sn), (cx + c * r, cy, cz + sn * r))
+    P = np.array(planes, f)
+    if girdle_h > 0:
+        circ_r = r / f(math.cos(math.pi / band_m))
+        lo = (cx - circ_r * q, cy - (f(0.5) * girdle_h + pav_h), cz - circ_r)
+        hi = (cx + circ_r * q, cy + (f(0.5) * girdle_h + crown_h), cz + circ_r)
+    else:
+        from scipy.spatial import HalfspaceIntersection
+        hs = np.concatenate([P[:, :3].astype(np.float64), -P[:, 3:4].astype(np.float64)], 1)
+        V = HalfspaceIntersection(hs, np.array([cx, cy, cz], np.float64)).intersections
+        lo, hi = tuple(V.min(0) - 1e-4), tuple(V.max(0) + 1e-4)
+    return P, lo, hi
+
+
+def validate_diamond_params(radius, table_pct, crown_angle, pavilion_angle, girdle_pct, what):
+    """validate_diamond_params (scene_file.rs:772-791): NaN/inf and
+    out-of-range cut parameters are errors."""
+    ok = lambda v: isinstance(v, (int, float)) and math.isfinite(v)
+    if not (ok(radius) and radius > 0.0):
+        raise ValueError(f"{what}: radius must be positive and finite, got {radius}")
+    if not (ok(table_pct) and 0.0 < table_pct < 100.0):
+        raise ValueError(f"{what}: table_pct must be in (0, 100), got {table_pct}")
+    if not (ok(crown_angle) and 0.0 < crown_angle < 90.0):
+        raise ValueError(f"{what}: crown angle must be in (0, 90) deg, got {crown_angle}")
+    if not (ok(pavilion_angle) and 0.0 < pavilion_angle < 90.0):
+        raise ValueError(f"{what}: pavilion angle must be in (0, 90) deg, got {pavilion_angle}")
+    if not (ok(girdle_pct) and 0.0 <= girdle_pct < 100.0):
+        raise ValueError(f"{what}: girdle_pct must be in [0, 100), got {girdle_pct}")
+
+
+def parse_girdle_finish(s, what):
+    """parse_girdle_finish (scene_file.rs:651-658)."""
+    v = None if s is None else str(s).lower()
+    if v in (None, ""):
+        return "uniform"
+    if v == "faceted":
+        return "faceted"
+    if v in ("polished", "bruted"):
+        return "polished"
+    raise ValueError(f"{what}: girdle_finish must be faceted|polished|bruted, got '{v}'")
+
+
+# gem material presets (scene_file.rs:681-697): Cauchy B, C (µm²) and the body
+# absorption per scene unit at scale_mm = 0.001
+GEM_PRESETS = {
+    "diamond": (2.351, 0.0230, (0.0, 0.0, 0.0)),
+    "sapphire": (1.741, 0.0094, (650.0, 320.0, 25.0)),
+    "ruby": (1.741, 0.0094, (25.0, 550.0, 450.0)),
+    "emerald": (1.556, 0.0073, (480.0, 25.0, 380.0)),
+}
+
+
+def gem_preset(name):
+    if name not in GEM_PRESETS:
+        raise ValueError(f"unknown gem material '{name}' (expected diamond, sapphire, ruby or emerald)")
+    return GEM_PRESETS[name]
+
+
+def gem_absorption(g, preset_abs):
+    """gem_absorption (scene_file.rs:721-736): preset body colour plus the D..Z
+    grade tint, both rescaled by 0.001/scale_mm, plus an explicit absorption
+    (per scene unit, not rescaled); f32 like the reference."""
+    f = np.float32
+    grade = str(g.get("color_grade", "D")).strip().upper()[:1]
+    sigma = {"D": 0.0, "E": 0.0, "F": 0.0, "G": 50.0, "H": 80.0, "I": 120.0, "J": 170.0, "K": 230.0,
+             "L": 300.0, "M": 300.0}.get(grade, 400.0)
+    tint = np.array([1.0, 0.75, 0.35], f) * f(sigma)
+    unit_fix = f(0.001) / f(g.get("scale_mm", 0.001))
+    extra = np.asarray(g.get("absorption", (0.0, 0.0, 0.0)), f)
+    return (np.asarray(preset_abs, f) + tint) * unit_fix + extra
+
+
+def gem_geometry(g):
+    """The size and cut of a [[gems]] entry (build_gem, scene_file.rs:793-850):
+    radius, oval ratio, crown/pavilion angles, girdle facets/finish/pct."""
+    f = np.float32
+    scale_mm = g.get("scale_mm", 0.001)
+    if g.get("measurements_mm") is not None:
+        m = [f(v) for v in g["measurements_mm"]]
+        if m[0] <= 0 or m[1] <= 0:
+            raise ValueError("measurements_mm must be positive")
+        L, W = (m[0], m[1]) if m[0] >= m[1] else (m[1], m[0])
+        w_mm, ratio = W, (L / W if (L - W) / W > f(0.02) else f(1.0))
+    elif g.get("carat") is not None:
+        ct = f(g["carat"])
+        if ct <= 0:
+            raise ValueError("carat must be positive")
+        w_mm, ratio = f(np.cbrt(ct / f(0.00355))), f(1.0)           # ct ≈ 0.00355 · d_mm³
+    else:
+        raise ValueError("provide either carat or measurements_mm")
+    if not scale_mm > 0:
+        raise ValueError("scale_mm must be positive")
+    radius = f(0.5) * w_mm * f(scale_mm)
+    table_pct = g.get("table_pct", 53.0)
+    if not 0.0 < table_pct < 100.0:
+        raise ValueError(f"table_pct must be in (0, 100), got {table_pct}")
+    girdle_pct = g.get("girdle_pct", 2.0)
+    table_r = f(table_pct / 100.0) * radius
+    crown_angle = g.get("crown_angle", 34.5)
+    if g.get("crown_pct") is not None:           # IGI: % of the minor axis → facet angle
+        crown_angle = math.degrees(math.atan(float(f(g["crown_pct"]) / f(100.0) * w_mm * f(scale_mm) / (radius - table_r))))
+    pavilion_angle = g.get("pavilion_angle", 40.75)
+    if g.get("pavilion_pct") is not None:
+        pavilion_angle = math.degrees(math.atan(float(f(g["pavilion_pct"]) / f(100.0) * w_mm * f(scale_mm) / radius)))
+    validate_diamond_params(float(radius), table_pct, crown_angle, pavilion_angle, girdle_pct, f"gem '{g.get('report', '')}'")
+    finish = parse_girdle_finish(g.get("girdle_finish"), f"gem '{g.get('report', '')}'")
+    facets = g.get("girdle_facets") or (64 if ratio > 1.05 else 16)
+    return dict(radius=float(radius), oval_ratio=float(ratio), table_pct=table_pct, crown_angle=crown_angle,
+                pavilion_angle=pavilion_angle, girdle_facets=int(facets), girdle_finish=finish, girdle_pct=girdle_pct)
+
+
+def add_gem(sb, g):
+    """A [[gems]] entry from a grading report (build_gem, scene_file.rs:793-931):
+    a round/oval brilliant in a preset or overridden spectral dielectric, placed
+    by scale → rotate about its center → translate.  Step-family cuts are not
+    supported by the GPU path."""
+    cut = g.get("cut", "brilliant")
+    geo = gem_geometry(g)
+    name = g.get("material", "diamond")
+    if name == "checker":                       # debug materials (scene_file.rs:862-868)
+        mat = Material.checker((0.9, 0.9, 0.9), (0.05, 0.05, 0.05), 12.0)
+    elif name == "opaque":
+        mat = Material.lambertian((0.8, 0.8, 0.8))
+    else:
+        b, c, pabs = gem_preset(name)
+        b = g["cauchy_b"] if g.get("cauchy_b") is not None else b
+        c = g["cauchy_c"] if g.get("cauchy_c") is not None else c
+        mat = Material.spectral_dielectric_cauchy(b, c, tuple(float(v) for v in gem_absorption(g, pabs)))
+    if cut != "brilliant":
+        raise ValueError(f"gem cut '{cut}' is not supported by the GPU path (brilliant only)")
+    ang = [0.0, 0.0, 0.0] if g.get("rotate") is None else [float(a) for a in g["rotate"]]
+    ang[1] += float(g.get("rotate_y") or 0.0) + float(g.get("spin") or 0.0)
+    return sb.add_diamond(g["center"], geo["radius"], sb.add_material(mat), geo["table_pct"], geo["crown_angle"],
+                          geo["pavilion_angle"], polish=g.get("polish", 0.02), oval_ratio=geo["oval_ratio"],
+                          girdle_facets=geo["girdle_facets"], girdle_finish=geo["girdle_finish"],
+                          girdle_pct=geo["girdle_pct"], scale=g.get("scale") or 1.0, rotate=ang,
+                          translate=g.get("translate") or (0.0, 0.0, 0.0))
+
+
 def perlin_tables(seed):
     """Perlin::new (perlin.rs:22-33) from a seeded generator: 256 random unit
     vectors (components uniform in [-1, 1), normalised) and three Fisher–Yates
@@ -614,6 +848,17 @@ def scene_from_toml_dict(doc, base="."):
         elif st == "mesh":
             V, Fa, N = load_obj(_resolve(base, sh["path"]))
             sb.add_mesh(V, Fa, mat, N, xf)
+        elif st == "diamond":                                       # scene_file.rs:1003-1011
+            validate_diamond_params(sh["radius"], sh.get("table_pct", 53.0), sh.get("crown_angle", 34.5),
+                                    sh.get("pavilion_angle", 40.75), sh.get("girdle_pct", 2.0), f"objects[{i}]")
+            ang = [0.0, 0.0, 0.0] if obj.get("rotate") is None else [float(a) for a in obj["rotate"]]
+            ang[1] += float(obj.get("rotate_y") or 0.0) + float(obj.get("spin") or 0.0)
+            sb.add_diamond(sh["center"], sh["radius"], mat, sh.get("table_pct", 53.0), sh.get("crown_angle", 34.5),
+                           sh.get("pavilion_angle", 40.75), polish=sh.get("polish", 0.02),
+                           oval_ratio=sh.get("oval_ratio", 1.0), girdle_facets=sh.get("girdle_facets", 16),
+                           girdle_finish=parse_girdle_finish(sh.get("girdle_finish"), f"objects[{i}]"),
+                           girdle_pct=sh.get("girdle_pct", 2.0), scale=obj.get("scale") or 1.0, rotate=ang,
+                           pivot=(0.0, 0.0, 0.0), translate=obj.get("translate") or (0.0, 0.0, 0.0))
         else:
             raise ValueError(f"objects[{i}]: shape '{st}' is not supported by the GPU path")
     for lc in doc.get("lights", []):
@@ -622,7 +867,10 @@ def scene_from_toml_dict(doc, base="."):
         else:
             m = Material.diffuse_light(lc["color"])
         sb.add_light_quad(lc["corner"], lc["u"], lc["v"], sb.add_material(m))
-    if doc.get("gems"):
-        raise ValueError("[[gems]] analytic solids are not supported by the GPU path")
+    for i, g in enumerate(doc.get("gems", [])):                     # scene_file.rs:1048-1052
+        try:
+            add_gem(sb, g)
+        except ValueError as e:
+            raise ValueError(f"gems[{i}]: {e}") from None
     sb.caustics = doc.get("caustics")
     return sb
