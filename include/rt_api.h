@@ -156,7 +156,7 @@ typedef struct RtMedium {
 #define RT_PRIM_CONVEX 3
 typedef struct RtConvex {
     int32_t plane_offset;       /* first plane in convex_planes */
-    int32_t n_planes;           /* 4 .. 256 */
+    int32_t n_planes;           /* 4 .. 1024 */
     int32_t mat;
     float   polish;             /* per-facet micro-tilt amplitude in radians (hittable.rs:261-270), 0 .. 0.25 */
     float   box_lo[3], box_hi[3]; /* object-space box that contains the solid */

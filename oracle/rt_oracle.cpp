@@ -658,14 +658,19 @@ static bool convex_hit(const float* planes, int32_t n, const Ray& r, float tmin,
         if (nd < 0.0f) {
             if (t_face > t_enter) { t_enter = t_face; enter_i = i; entry_found = true; }
         } else {
-            if (t_face < t_exit) { t_exit = t_face; exit_i = i; }
+            // an exit exactly at tmax still names its plane
+            if (t_face < t_exit || (exit_i < 0 && t_face == t_exit)) { t_exit = t_face; exit_i = i; }
         }
         if (t_enter > t_exit) return false;
     }
     if (t_enter > t_exit) return false;
     if (t_enter == t_exit && t_enter < tmax) return false;
     if (entry_found) { *t_out = t_enter; *plane = enter_i; return true; }
-    if (t_exit > tmax) return false;
+    // An interior ray whose exit lies beyond tmax crosses no surface in
+    // [tmin, tmax].  The reference returns t_max with a default normal here,
+    // a phantom that its last-visited tie rule lets win against a real hit at
+    // the same t, so the answer would depend on the traversal order.
+    if (exit_i < 0 || t_exit > tmax) return false;
     *t_out = t_exit; *plane = exit_i;
     return true;
 }
@@ -2067,7 +2072,7 @@ static int scene_create(const RtSceneDesc* d, Scene** out) {
     s->n_convex = d->n_convex;
     for (int64_t i = 0; i < d->n_convex; i++) {
         const RtConvex& c = d->convex[i];
-        bool ok = c.n_planes >= 4 && c.n_planes <= 256 && c.plane_offset >= 0 && c.mat >= 0 && c.mat < d->n_mats &&
+        bool ok = c.n_planes >= 4 && c.n_planes <= 1024 && c.plane_offset >= 0 && c.mat >= 0 && c.mat < d->n_mats &&
                   !is_emissive_type(d->mats[c.mat].type) && c.scale > 0.0f && c.polish >= 0.0f && c.polish <= 0.25f;
         if (!ok) { delete s; g_err = "invalid convex solid " + std::to_string(i); return RT_ERR_INVALID; }
         int32_t off = (int32_t)(s->convex_planes.size() / 4);

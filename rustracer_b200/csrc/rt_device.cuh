@@ -130,6 +130,16 @@ RT_HD float3 operator-(float3 a) { return mk(-a.x, -a.y, -a.z); }
 RT_HD float3 operator*(float3 a, float3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
 RT_HD float3 operator*(float3 a, float t) { return mk(a.x * t, a.y * t, a.z * t); }
 RT_HD float3 operator*(float t, float3 a) { return mk(a.x * t, a.y * t, a.z * t); }
+// r.at(t) (ray.rs): o + t·d with the product rounded before the sum, as on the
+// CPU; a fused multiply-add would move points off a plane by a different
+// rounding, which flips floor-based lookups (the checker) at y = 0
+RT_HD float3 ray_at(float3 o, float3 d, float t) {
+#ifdef __CUDA_ARCH__
+    return mk(__fadd_rn(o.x, __fmul_rn(t, d.x)), __fadd_rn(o.y, __fmul_rn(t, d.y)), __fadd_rn(o.z, __fmul_rn(t, d.z)));
+#else
+    return mk(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+#endif
+}
 RT_HD float3 operator/(float3 a, float t) { return mk(a.x / t, a.y / t, a.z / t); }
 RT_HD float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 RT_HD float len2(float3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
@@ -200,14 +210,15 @@ RT_D bool convex_test(const float4* pl, int n, float3 o, float3 d, float tmin, f
         if (nd < 0.0f) {
             if (t_face > t_enter) { t_enter = t_face; enter_i = i; entry_found = true; }
         } else {
-            if (t_face < t_exit) { t_exit = t_face; exit_i = i; }
+            if (t_face < t_exit || (exit_i < 0 && t_face == t_exit)) { t_exit = t_face; exit_i = i; }
         }
         if (t_enter > t_exit) return false;
     }
     if (t_enter > t_exit) return false;
     if (t_enter == t_exit && t_enter < tmax) return false;
     if (entry_found) { *t_out = t_enter; *plane = enter_i; return true; }
-    if (t_exit > tmax) return false;
+    // an interior ray whose exit lies beyond tmax crosses nothing in [tmin, tmax]
+    if (exit_i < 0 || t_exit > tmax) return false;
     *t_out = t_exit; *plane = exit_i;
     return true;
 }
@@ -241,7 +252,7 @@ RT_D bool quad_test(const float4* g, float3 o, float3 d, float tmin, float tmax,
     if (t < tmin || t > tmax) return false;
     float4 g1 = g[1], g2 = g[2], g3 = g[3];
     float3 Q = mk(g1.x, g1.y, g1.z), u = mk(g1.w, g2.x, g2.y), v = mk(g2.z, g2.w, g3.x), w = mk(g3.y, g3.z, g3.w);
-    float3 p = o + t * d;
+    float3 p = ray_at(o, d, t);
     float3 planar = p - Q;
     float alpha = dot3(w, cross3(planar, v));
     float beta = dot3(w, cross3(u, planar));

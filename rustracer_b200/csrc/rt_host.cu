@@ -559,8 +559,8 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     int64_t n_planes_total = 0, n_world_planes = 0;
     for (int64_t i = 0; i < d->n_convex; i++) {
         const RtConvex& c = d->convex[i];
-        if (c.n_planes < 4 || c.n_planes > 256 || c.plane_offset < 0 || bad_mat(c.mat))
-            return bail(fail(s, RT_ERR_INVALID, "convex solid " + std::to_string(i) + ": 4..256 planes and a valid material"));
+        if (c.n_planes < 4 || c.n_planes > 1024 || c.plane_offset < 0 || bad_mat(c.mat))
+            return bail(fail(s, RT_ERR_INVALID, "convex solid " + std::to_string(i) + ": 4..1024 planes and a valid material"));
         int mt = d->mats[c.mat].type;
         if (mt == RT_MAT_DIFFUSE_LIGHT || mt == RT_MAT_BLACKBODY_LIGHT)
             return bail(fail(s, RT_ERR_INVALID, "convex solid " + std::to_string(i) + ": emissive materials are not supported"));

@@ -101,7 +101,7 @@ RT_D float medium_sample(const DevMedium& m, float3 o, float3 d, float lam, floa
     for (uint32_t k = 0; k < 4096u; k++) {
         t -= inv_maj * logf(fmaxf(medium_rnd(g, 2u * k), 1.1920928955078125e-07f));
         if (t >= t2) return INFINITY;
-        float dens = medium_density_at(m, o + t * d);
+        float dens = medium_density_at(m, ray_at(o, d, t));
         if (medium_rnd(g, 2u * k + 1u) < dens / m.density) return t;
     }
     return INFINITY;
@@ -131,7 +131,7 @@ RT_D float medium_transmittance(const DevMedium& m, float3 o, float3 d, float tm
     float seg_t = l / len, sum = 0.0f;
     for (int i = 0; i < 16; i++) {
         float t = a + seg_t * ((float)i + 0.5f) / 16.0f;
-        sum += medium_density_at(m, o + t * d);
+        sum += medium_density_at(m, ray_at(o, d, t));
     }
     return expf(-sum / 16.0f * l);
 }

@@ -167,7 +167,7 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                 const DevMedium& M = S.media[RT_HIT_INDEX(ref)];
                 Rng rng = photon_rng(seed, gid);
                 uint32_t base = P_BOUNCE0 + bounce * P_PER_BOUNCE;
-                float3 p = o + hv.y * d;
+                float3 p = ray_at(o, d, hv.y);
                 float3 nd = hg_sample(unit3(d), M.g, rnd(rng, base + 0), rnd(rng, base + 1));
                 P.ray_o[gid] = make_float4(p.x, p.y, p.z, ro.w);
                 P.ray_d[gid] = make_float4(nd.x, nd.y, nd.z, rdv.w);
@@ -179,7 +179,7 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                 float lam = rdv.w, lum_clamp = ro.w;
                 uint32_t spec_depth = __float_as_uint(th.w);
                 float t = hv.y;
-                float3 p = o + t * d;
+                float3 p = ray_at(o, d, t);
                 uint32_t type = RT_HIT_TYPE(ref), idx = RT_HIT_INDEX(ref);
                 float3 outward;
                 int mat, cvx_wp = 0;

@@ -212,10 +212,10 @@ RT_D bool light_hit(const DevLight& L, float3 o, float3 d, float tmin, float tma
         outward = mk(L.g[0].x, L.g[0].y, L.g[0].z);
     } else {
         if (!sphere_test(L.g[0], o, d, tmin, tmax, &t)) return false;
-        outward = ((o + t * d) - mk(L.g[0].x, L.g[0].y, L.g[0].z)) / L.g[0].w;
+        outward = (ray_at(o, d, t) - mk(L.g[0].x, L.g[0].y, L.g[0].z)) / L.g[0].w;
     }
     rec->t = t;
-    rec->p = o + t * d;
+    rec->p = ray_at(o, d, t);
     rec->normal = dot3(d, outward) < 0.0f ? outward : -outward;
     rec->mat = L.mat;
     return true;
@@ -629,7 +629,7 @@ RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
     Surf r;
     uint32_t ref = __float_as_uint(hv.x);
     r.t = hv.y;
-    r.p = o + r.t * d;
+    r.p = ray_at(o, d, r.t);
     uint32_t type = RT_HIT_TYPE(ref), idx = RT_HIT_INDEX(ref);
     float3 outward;
     if (type == RT_PRIM_TRI) {                                                      // triangle.rs:91-108
@@ -767,7 +767,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                     // skip_pdf bounce of the specular branch (renderer.rs:421-456)
                     float4 hv = A.hit[pid];
                     const DevMedium& M = S.media[RT_HIT_INDEX(__float_as_uint(hv.x))];
-                    float3 p = o + hv.y * d;
+                    float3 p = ray_at(o, d, hv.y);
                     float3 dir = hg_sample(unit3(d), M.g, rnd(rng, b + B_SCATTER0), rnd(rng, b + B_SCATTER1));
                     T = T * M.color;
                     o = p; d = dir;

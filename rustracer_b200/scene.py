@@ -244,6 +244,18 @@ class SceneBuilder:
         return self.add_convex(planes, mat, lo, hi, polish=pol, scale=scale, rot=R,
                                pivot=center if pivot is None else pivot, translate=translate)
 
+    def add_step_cut(self, center, half_a, half_b, mat, polish=0.0, scale=1.0, rotate=None, pivot=None,
+                     translate=(0.0, 0.0, 0.0), **params):
+        """StepCut::new (step_cut.rs:232-392): a step-family cut with semi-length
+        `half_a` along x and semi-width `half_b` along z, placed like
+        `add_diamond`; `params` are step_cut_planes' proportions."""
+        planes, lo, hi = step_cut_planes(center, half_a, half_b, **params)
+        pol = min(max(polish, 0.0), 0.25) if math.isfinite(polish) else 0.0       # step_cut.rs:390
+        ang = [0.0, 0.0, 0.0] if rotate is None else [float(a) for a in rotate]
+        R = _euler_fwd(ang) if any(a != 0.0 for a in ang) else np.eye(3)
+        return self.add_convex(planes, mat, lo, hi, polish=pol, scale=scale, rot=R,
+                               pivot=center if pivot is None else pivot, translate=translate)
+
     def add_quad(self, corner, u, v, mat, xf=None):
         q, uu, vv = (np.asarray(a, dtype=np.float64) for a in (corner, u, v))
         if xf is not None and not xf.identity:
@@ -654,6 +666,245 @@ def diamond_planes(center, radius, table_pct=53.0, crown_angle=34.5, pavilion_an
     return P, lo, hi
 
 
+def _f32_rad(deg):
+    return np.float32(deg) * np.float32(np.float32(math.pi) / np.float32(180.0))
+
+
+def step_outline_vertices(outline, a, b):
+    """StepOutline::vertices (step_cut.rs:38-108): the girdle outline in XZ
+    relative to the centre, sorted by angle about the vertex centroid.
+    `outline` is ("rect", corner_pct) | ("rounded_rect", corner_pct, segs) |
+    ("triangle",) | ("hexagon",) | ("pointed_oval", segs, pear) |
+    ("polygon", [[x, z], ...])."""
+    f = np.float32
+    a, b = f(a), f(b)
+    kind = outline[0]
+    if kind == "rect":
+        c = min(f(outline[1]) / f(100.0) * min(a, b), f(0.45) * min(a, b))
+        if c <= f(1e-6):
+            v = [(a, b), (a, -b), (-a, -b), (-a, b)]
+        else:
+            v = [(a - c, b), (a, b - c), (a, -(b - c)), (a - c, -b), (-(a - c), -b), (-a, -(b - c)), (-a, b - c),
+                 (-(a - c), b)]
+    elif kind == "rounded_rect":
+        r = min(f(outline[1]) / f(100.0) * min(a, b), f(0.45) * min(a, b))
+        segs = max(int(outline[2]), 1)
+        v = []
+        for sx in (f(1.0), f(-1.0)):
+            for sz in (f(1.0), f(-1.0)):
+                ccx, ccz = sx * (a - r), sz * (b - r)
+                for j in range(segs + 1):
+                    ang = f(j) / f(segs) * f(math.pi / 2)
+                    v.append((ccx + sx * r * f(math.cos(ang)), ccz + sz * r * f(math.sin(ang))))
+    elif kind == "triangle":
+        v = []
+        for k in range(3):
+            th = f(math.pi / 2) + f(k) * f(2.0) * f(math.pi) / f(3.0)
+            v.append((a * f(math.cos(th)), b * f(math.sin(th))))
+    elif kind == "hexagon":
+        v = []
+        for k in range(6):
+            th = f(k) * f(math.pi) / f(3.0)
+            v.append((a * f(math.cos(th)), b * f(math.sin(th))))
+    elif kind == "pointed_oval":
+        segs, pear = int(outline[1]), bool(outline[2])
+        n = max(segs, 4) * 2
+        v = []
+        for i in range(n):
+            th = f(2.0) * f(math.pi) * f(i) / f(n)
+            c, sn = f(math.cos(th)), f(math.sin(th))
+            pw = (f(0.6) if c >= 0 else f(1.0)) if pear else f(0.65)
+            sg = f(1.0) if c > 0 or (c == 0 and math.copysign(1.0, c) > 0) else f(-1.0)
+            v.append((a * sg * f(abs(float(c)) ** float(pw)), b * sn))
+    elif kind == "polygon":
+        v = [(f(x), f(z)) for x, z in outline[1]]
+    else:
+        raise ValueError(f"unknown step outline '{kind}'")
+    n = f(len(v))
+    cx = f(0.0)
+    for p in v:
+        cx = cx + p[0]
+    cz = f(0.0)
+    for p in v:
+        cz = cz + p[1]
+    cx, cz = cx / n, cz / n
+    return sorted(v, key=lambda p: f(math.atan2(float(p[1] - cz), float(p[0] - cx))))
+
+
+def _validate_outline(v, scale):
+    """validate_outline (step_cut.rs:183-225): dedupe adjacent vertices, then
+    at least 3 distinct vertices, no zero edge, non-zero area, convex."""
+    f = np.float32
+    eps = f(1e-6) * f(scale)
+    hyp = lambda p, q: f(math.hypot(float(p[0] - q[0]), float(p[1] - q[1])))
+    out = []
+    for p in v:
+        if out and hyp(p, out[-1]) < eps:
+            continue
+        out.append(p)
+    if len(out) > 1 and hyp(out[0], out[-1]) < eps:
+        out.pop()
+    n = len(out)
+    if n < 3:
+        raise ValueError("outline needs at least 3 distinct vertices")
+    for i in range(n):
+        if hyp(out[i], out[(i + 1) % n]) < eps:
+            raise ValueError("outline has a zero-length edge")
+    area2 = f(0.0)
+    for i in range(n):
+        p, q = out[i], out[(i + 1) % n]
+        area2 = area2 + (p[0] * q[1] - q[0] * p[1])
+    if abs(area2) < eps * eps:
+        raise ValueError("outline has zero area")
+    for i in range(n):
+        p, q, r = out[i], out[(i + 1) % n], out[(i + 2) % n]
+        cross = (q[0] - p[0]) * (r[1] - q[1]) - (q[1] - p[1]) * (r[0] - q[0])
+        if cross * area2 < 0:
+            raise ValueError("polygon outline must be convex")
+    return out
+
+
+def step_cut_planes(center, half_a, half_b, table_pct=65.0, crown_angle=35.0, pavilion_angle=42.0,
+                    outline=("rect", 12.0), crown_steps=3, pavilion_steps=3, culet_pct=8.0, step_spread=0.25,
+                    chevrons=0, girdle_pct=0.0):
+    """The half-spaces and bounding box of StepCut::new (step_cut.rs:232-392),
+    in f32: per outline edge an optional vertical girdle face, crown and
+    pavilion rows whose runs are normalised so the table and culet insets are
+    exact, chevron planes at the outline vertices, and the table/culet caps.
+    Defaults are StepCutParams::default (step_cut.rs:147-163)."""
+    f = np.float32
+    if not (half_a > 0 and half_b > 0 and math.isfinite(half_a) and math.isfinite(half_b)):
+        raise ValueError("StepCut: half extents must be positive and finite")
+    cx, cy, cz = (f(c) for c in center)
+    a, b = f(half_a), f(half_b)
+    k = min(max(f(table_pct) / f(100.0), f(0.05)), f(0.95))
+    kc = min(max(f(culet_pct) / f(100.0), f(0.0)), f(0.5))
+    s_in, sp = b * (f(1.0) - k), b * (f(1.0) - kc)
+    tan_c, tan_p = f(math.tan(float(_f32_rad(crown_angle)))), f(math.tan(float(_f32_rad(pavilion_angle))))
+    crown_h, pav_h = s_in * tan_c, sp * tan_p
+    gp = f(girdle_pct)
+    girdle_h = min(max(gp / f(100.0) * f(2.0) * b, f(0.0)), f(0.3) * b)
+    if not (math.isfinite(girdle_pct) and 0.0 <= girdle_pct < 100.0):
+        raise ValueError(f"StepCut: girdle_pct must be in [0, 100), got {girdle_pct}")
+    if not (crown_h > 0 and pav_h > 0):
+        raise ValueError(f"StepCut: crown/pavilion angles must be in (0, 90) degrees, got {crown_angle} / {pavilion_angle}")
+    verts = _validate_outline(step_outline_vertices(outline, a, b), max(a, b))
+    nv = len(verts)
+    gcx, gcz = f(0.0), f(0.0)
+    for p in verts:
+        gcx = gcx + p[0]
+    for p in verts:
+        gcz = gcz + p[1]
+    gcx, gcz = gcx / f(nv), gcz / f(nv)
+
+    def norm2(x, z):
+        l = f(math.sqrt(float(x * x + z * z)))
+        return (x / l, z / l) if l > f(1e-12) else (f(0.0), f(0.0))
+
+    def unit(x, y, z):
+        l = f(math.sqrt(float(x * x + y * y + z * z)))
+        return (x / l, y / l, z / l)
+
+    dot = lambda u, w: u[0] * w[0] + u[1] * w[1] + u[2] * w[2]
+    edges = []
+    for i in range(nv):
+        p, q = verts[i], verts[(i + 1) % nv]
+        m = norm2(q[1] - p[1], -(q[0] - p[0]))
+        if m[0] * (p[0] - gcx) + m[1] * (p[1] - gcz) < 0:
+            m = (-m[0], -m[1])
+        edges.append((m, m[0] * p[0] + m[1] * p[1]))
+    cs, ps = max(int(crown_steps), 1), max(int(pavilion_steps), 1)
+    spread = min(max(f(step_spread), f(0.0)), f(0.9))
+    factor = lambda i, rows: f(1.0) if rows <= 1 else f(1.0) + spread * (f(1.0) - f(2.0) * f(i) / f(rows - 1))
+    dv, dvp = crown_h / f(cs), pav_h / f(ps)
+    sum_c = f(0.0)
+    for i in range(cs):
+        sum_c = sum_c + dv / (tan_c * factor(i, cs))
+    sum_p = f(0.0)
+    for i in range(ps):
+        sum_p = sum_p + dvp / (tan_p * factor(i, ps))
+    norm_c, norm_p = s_in / sum_c, sp / sum_p
+    planes = []
+    for m, h in edges:
+        if girdle_h > 0:
+            planes.append((m[0], f(0.0), m[1], m[0] * cx + m[1] * cz + h))
+        dist, y = h, f(0.5) * girdle_h
+        for i in range(cs):
+            dh = dv / (tan_c * factor(i, cs)) * norm_c
+            n = unit(m[0] * dv, dh, m[1] * dv)
+            planes.append(n + (dot(n, (cx + m[0] * dist, cy + y, cz + m[1] * dist)),))
+            dist, y = dist - dh, y + dv
+        dist, y = h, f(-0.5) * girdle_h
+        for i in range(ps):
+            dh = dvp / (tan_p * factor(i, ps)) * norm_p
+            n = unit(m[0] * dvp, -dh, m[1] * dvp)
+            planes.append(n + (dot(n, (cx + m[0] * dist, cy + y, cz + m[1] * dist)),))
+            dist, y = dist - dh, y - dvp
+    ctr = (cx, cy, cz)
+    for i in range(nv):
+        v, vp, vn = verts[i], verts[(i + nv - 1) % nv], verts[(i + 1) % nv]
+        u1, u2 = norm2(vp[0] - v[0], vp[1] - v[1]), norm2(vn[0] - v[0], vn[1] - v[1])
+        bis = (u1[0] + u2[0], u1[1] + u2[1])
+        if bis[0] * bis[0] + bis[1] * bis[1] < f(1e-12):
+            continue
+        t = (-bis[1], bis[0])
+        c3 = (cx + v[0], cy, cz + v[1])
+        tc = (cx + v[0] * k, cy + f(0.5) * girdle_h + crown_h, cz + v[1] * k)
+        cc = (cx + v[0] * kc, cy - f(0.5) * girdle_h - pav_h, cz + v[1] * kc)
+        for j in range(int(chevrons)):
+            fr = f(j + 1) / f(chevrons)
+            for tgt in (tc, cc):
+                pp = tuple(c3[a_] + (tgt[a_] - c3[a_]) * fr for a_ in range(3))
+                w = (pp[0] - c3[0], pp[1] - c3[1], pp[2] - c3[2])
+                # d3 × w with d3 = (t.x, 0, t.z)
+                n = unit(f(0.0) * w[2] - t[1] * w[1], t[1] * w[0] - t[0] * w[2], t[0] * w[1] - f(0.0) * w[0])
+                if dot(n, ctr) > dot(n, c3):
+                    n = (-n[0], -n[1], -n[2])
+                planes.append(n + (dot(n, c3),))
+    planes.append((f(0.0), f(1.0), f(0.0), cy + f(0.5) * girdle_h + crown_h))
+    planes.append((f(0.0), f(-1.0), f(0.0), -(cy - f(0.5) * girdle_h - pav_h)))
+    xs, zs = [p[0] for p in verts], [p[1] for p in verts]
+    top, bottom = f(0.5) * girdle_h + s_in * tan_c, f(0.5) * girdle_h + sp * tan_p
+    lo = (float(cx + min(xs)), float(cy - bottom), float(cz + min(zs)))
+    hi = (float(cx + max(xs)), float(cy + top), float(cz + max(zs)))
+    return np.array(planes, f), lo, hi
+
+
+# step-family presets for [[gems]] cut = "..." (scene_file.rs:738-766):
+# outline, culet_pct, crown steps, pavilion steps, step spread, default chevrons
+STEP_CUT_PRESETS = {
+    "step": (("rect", 12.0), 8.0, 3, 3, 0.25, 0),
+    "princess": (("rect", 0.0), 0.0, 4, 4, 0.15, 3),
+    "asscher": (("rect", 22.0), 8.0, 3, 3, 0.20, 0),
+    "radiant": (("rect", 12.0), 0.0, 4, 4, 0.15, 2),
+    "baguette": (("rect", 4.0), 8.0, 2, 2, 0.10, 0),
+    "cushion": (("rounded_rect", 30.0, 4), 8.0, 3, 3, 0.15, 0),
+    "trillion": (("triangle",), 0.0, 4, 4, 0.15, 2),
+    "marquise": (("pointed_oval", 24, False), 0.0, 4, 4, 0.15, 2),
+    "pear": (("pointed_oval", 24, True), 0.0, 4, 4, 0.15, 2),
+}
+
+
+def step_outline_from_toml(name, corner_pct, corner_segs, oval_segs, pear, points):
+    """step_outline_name (scene_file.rs:700-715)."""
+    if name == "rect":
+        return ("rect", corner_pct)
+    if name == "rounded_rect":
+        return ("rounded_rect", corner_pct, corner_segs)
+    if name in ("triangle", "hexagon"):
+        return (name,)
+    if name == "marquise":
+        return ("pointed_oval", oval_segs, False)
+    if name == "pear":
+        return ("pointed_oval", oval_segs, pear)
+    if name == "polygon":
+        if points is None:
+            raise ValueError('outline = "polygon" requires `points`')
+        return ("polygon", points)
+    raise ValueError(f"unknown step_cut outline '{name}' (expected rect, rounded_rect, triangle, hexagon, "
+                     "marquise, pear, polygon)")
+
+
 def validate_diamond_params(radius, table_pct, crown_angle, pavilion_angle, girdle_pct, what):
     """validate_diamond_params (scene_file.rs:772-791): NaN/inf and
     out-of-range cut parameters are errors."""
@@ -753,9 +1004,9 @@ def gem_geometry(g):
 
 def add_gem(sb, g):
     """A [[gems]] entry from a grading report (build_gem, scene_file.rs:793-931):
-    a round/oval brilliant in a preset or overridden spectral dielectric, placed
-    by scale → rotate about its center → translate.  Step-family cuts are not
-    supported by the GPU path."""
+    a round/oval brilliant or a step-family preset cut in a preset or
+    overridden spectral dielectric, placed by scale → rotate about its center
+    → translate."""
     cut = g.get("cut", "brilliant")
     geo = gem_geometry(g)
     name = g.get("material", "diamond")
@@ -768,15 +1019,27 @@ def add_gem(sb, g):
         b = g["cauchy_b"] if g.get("cauchy_b") is not None else b
         c = g["cauchy_c"] if g.get("cauchy_c") is not None else c
         mat = Material.spectral_dielectric_cauchy(b, c, tuple(float(v) for v in gem_absorption(g, pabs)))
-    if cut != "brilliant":
-        raise ValueError(f"gem cut '{cut}' is not supported by the GPU path (brilliant only)")
     ang = [0.0, 0.0, 0.0] if g.get("rotate") is None else [float(a) for a in g["rotate"]]
     ang[1] += float(g.get("rotate_y") or 0.0) + float(g.get("spin") or 0.0)
-    return sb.add_diamond(g["center"], geo["radius"], sb.add_material(mat), geo["table_pct"], geo["crown_angle"],
-                          geo["pavilion_angle"], polish=g.get("polish", 0.02), oval_ratio=geo["oval_ratio"],
-                          girdle_facets=geo["girdle_facets"], girdle_finish=geo["girdle_finish"],
-                          girdle_pct=geo["girdle_pct"], scale=g.get("scale") or 1.0, rotate=ang,
-                          translate=g.get("translate") or (0.0, 0.0, 0.0))
+    place = dict(polish=g.get("polish", 0.02), scale=g.get("scale") or 1.0, rotate=ang,
+                 translate=g.get("translate") or (0.0, 0.0, 0.0))
+    if cut == "brilliant":
+        return sb.add_diamond(g["center"], geo["radius"], sb.add_material(mat), geo["table_pct"], geo["crown_angle"],
+                              geo["pavilion_angle"], oval_ratio=geo["oval_ratio"], girdle_facets=geo["girdle_facets"],
+                              girdle_finish=geo["girdle_finish"], girdle_pct=geo["girdle_pct"], **place)
+    if cut not in STEP_CUT_PRESETS:                 # step_cut_preset (scene_file.rs:741-766)
+        raise ValueError(f"unknown gem cut '{cut}' (expected brilliant, step, princess, asscher, radiant, baguette, "
+                         "cushion, trillion, marquise or pear)")
+    outline, culet, cs, ps, spread, chev = STEP_CUT_PRESETS[cut]
+    try:
+        return sb.add_step_cut(g["center"], geo["radius"] * geo["oval_ratio"], geo["radius"], sb.add_material(mat),
+                               table_pct=geo["table_pct"], crown_angle=geo["crown_angle"],
+                               pavilion_angle=geo["pavilion_angle"], outline=outline, crown_steps=cs,
+                               pavilion_steps=ps, culet_pct=culet, step_spread=spread,
+                               chevrons=g["chevrons"] if g.get("chevrons") is not None else chev,
+                               girdle_pct=geo["girdle_pct"], **place)
+    except ValueError as e:
+        raise ValueError(f"gem '{g.get('report', '')}': {e}") from None
 
 
 def perlin_tables(seed):
@@ -848,6 +1111,24 @@ def scene_from_toml_dict(doc, base="."):
         elif st == "mesh":
             V, Fa, N = load_obj(_resolve(base, sh["path"]))
             sb.add_mesh(V, Fa, mat, N, xf)
+        elif st == "step_cut":                                      # scene_file.rs:1013-1021
+            ol = step_outline_from_toml(sh.get("outline") or "rect", sh.get("corner_pct", 12.0),
+                                        sh.get("corner_segs", 4), sh.get("oval_segs", 24), sh.get("pear", False),
+                                        sh.get("points"))
+            ang = [0.0, 0.0, 0.0] if obj.get("rotate") is None else [float(a) for a in obj["rotate"]]
+            ang[1] += float(obj.get("rotate_y") or 0.0) + float(obj.get("spin") or 0.0)
+            try:
+                sb.add_step_cut(sh["center"], np.float32(0.5) * np.float32(sh["length"]),
+                                np.float32(0.5) * np.float32(sh["width"]), mat, polish=sh.get("polish", 0.02),
+                                scale=obj.get("scale") or 1.0, rotate=ang, pivot=(0.0, 0.0, 0.0),
+                                translate=obj.get("translate") or (0.0, 0.0, 0.0),
+                                table_pct=sh.get("table_pct", 53.0), crown_angle=sh.get("crown_angle", 34.5),
+                                pavilion_angle=sh.get("pavilion_angle", 40.75), outline=ol,
+                                crown_steps=sh.get("crown_steps", 3), pavilion_steps=sh.get("pavilion_steps", 3),
+                                culet_pct=sh.get("culet_pct", 8.0), step_spread=sh.get("step_spread", 0.25),
+                                chevrons=sh.get("chevrons", 0), girdle_pct=sh.get("girdle_pct", 2.0))
+            except ValueError as e:
+                raise ValueError(f"objects[{i}].shape: {e}") from None
         elif st == "diamond":                                       # scene_file.rs:1003-1011
             validate_diamond_params(sh["radius"], sh.get("table_pct", 53.0), sh.get("crown_angle", 34.5),
                                     sh.get("pavilion_angle", 40.75), sh.get("girdle_pct", 2.0), f"objects[{i}]")

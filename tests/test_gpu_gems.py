@@ -97,3 +97,73 @@ def test_gpu_toml_gem_sun_caustics_match_oracle():
     common, ga, oa = np.intersect1d(gi, oi, return_indices=True)
     assert len(common) > 0.95 * min(ng, no)
     np.testing.assert_allclose(gw[ga], ow[oa], rtol=1e-3, atol=1e-7)
+
+
+def step_field():
+    """Step-family cuts (princess with chevrons, cushion, trillion, a 626-plane
+    marquise, an emerald step cut) and a round brilliant, as [[gems]] entries."""
+    gems = [dict(measurements_mm=[6.0, 5.9, 4.2], table_pct=65.0, crown_pct=12.0, pavilion_pct=50.0, cut="princess",
+                 material="sapphire", rotate_y=25.0, center=[-1.2, 0.45, 0.3], scale_mm=0.3),
+            dict(measurements_mm=[6.0, 6.0, 3.7], cut="brilliant", material="diamond", center=[0.0, 0.45, 0.0],
+                 scale_mm=0.3),
+            dict(measurements_mm=[6.0, 5.0, 3.5], cut="cushion", material="ruby", center=[1.2, 0.45, 0.3],
+                 scale_mm=0.3, rotate=[0.0, 0.0, 15.0]),
+            dict(measurements_mm=[6.0, 6.0, 3.5], cut="trillion", material="emerald", center=[-0.6, 0.35, -1.0],
+                 scale_mm=0.3),
+            dict(measurements_mm=[9.0, 4.0, 3.0], cut="marquise", center=[0.7, 0.3, -1.0], scale_mm=0.3,
+                 spin=40.0),
+            dict(measurements_mm=[8.0, 6.0, 4.0], cut="step", material="emerald", center=[0.0, 0.4, 1.2],
+                 scale_mm=0.3, polish=0.05)]
+    doc = {"camera": {"look_from": [0.0, 2.0, 4.0], "look_at": [0.0, 0.3, 0.0]},
+           "background": {"type": "physical", "sun_elevation": 25.0, "sun_azimuth": 30.0},
+           "objects": [{"shape": {"type": "quad", "corner": [-4, 0, -4], "u": [8, 0, 0], "v": [0, 0, 8]},
+                        "material": {"type": "checker", "even": [0.1, 0.1, 0.1], "odd": [0.8, 0.8, 0.8],
+                                     "scale": 0.5}}],
+           "lights": [{"corner": [-0.75, 3.0, -0.75], "u": [1.5, 0, 0], "v": [0, 0, 1.5], "temp_k": 6500.0,
+                       "intensity": 8.0}],
+           "gems": gems}
+    return scene_from_toml_dict(doc)
+
+
+def test_gpu_step_cut_trace_matches_oracle():
+    sb = step_field()
+    assert max(len(c["planes"]) for c in sb.convex) == 626
+    g, o = GpuScene(sb), O.OracleScene(sb)
+    rs = np.concatenate([random_rays(60000, 11, center=(0, 0.4, 0), radius=3.0, spread=0.8),
+                         camera_rays(make_camera((0.0, 2.0, 4.0), (0.0, 0.3, 0.0), vfov=35.0, aspect=1.0), 128, 128)])
+    gh, oh = g.trace_closest(rs), o.trace_closest(rs)
+    assert (oh["prim"] >= 2).sum() > 2000
+    assert_same_hits(gh, oh)
+    assert np.array_equal(g.trace_any(rs), o.trace_any(rs))
+
+
+def test_gpu_step_cut_render_matches_oracle():
+    sb = step_field()
+    sb.spectral_range = 1
+    cam = make_camera((0.0, 2.0, 4.0), (0.0, 0.3, 0.0), vfov=35.0, aspect=1.0)
+    g, o = GpuScene(sb), O.OracleScene(sb)
+    p = pass_params(64, 64, 0, 64, 8, 12, 4, 1.0, 41)
+    gi = g.render_pass(cam, p)
+    p.seed = 42
+    oi = o.render_pass(cam, p)
+    assert np.isfinite(gi).all()
+    assert_tiles_agree(gi, oi)
+
+
+def test_gpu_interior_rays_in_overlapping_gems_match_oracle():
+    """Rays that start inside two overlapping stones (as refracted and
+    internally reflected rays do) end on the nearer exit on both paths."""
+    sb = step_field()
+    rng = np.random.default_rng(8)
+    lo = np.array([min(c["pivot"][a] for c in sb.convex) - 0.6 for a in range(3)])
+    hi = np.array([max(c["pivot"][a] for c in sb.convex) + 0.6 for a in range(3)])
+    n = 100000
+    o = lo + (hi - lo) * rng.random((n, 3))
+    d = rng.normal(0, 1, (n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rs = np.concatenate([o, d, np.full((n, 1), 0.001), np.full((n, 1), np.inf)], 1).astype(np.float32)
+    g, orc = GpuScene(sb), O.OracleScene(sb)
+    gh, oh = g.trace_closest(rs), orc.trace_closest(rs)
+    assert (oh["prim"] >= 2).sum() > n // 4
+    assert_same_hits(gh, oh)
+    assert np.array_equal(g.trace_any(rs), orc.trace_any(rs))

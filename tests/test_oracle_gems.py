@@ -308,11 +308,11 @@ def test_gem_girdle_finish_parses_and_validates():
         scene_from_toml_dict(_gem_doc(measurements_mm=[5.0, 5.0, 3.0], girdle_finish="rough"))
 
 
-def test_gem_unknown_material_or_unsupported_cut_errors():
-    with pytest.raises(ValueError, match="unknown gem material"):
+def test_gem_unknown_cut_or_material_errors():
+    with pytest.raises(ValueError, match="material"):
         scene_from_toml_dict(_gem_doc(carat=1.0, material="topaz"))
-    with pytest.raises(ValueError, match="not supported"):
-        scene_from_toml_dict(_gem_doc(carat=1.0, cut="princess"))
+    with pytest.raises(ValueError, match="cut"):
+        scene_from_toml_dict(_gem_doc(carat=1.0, cut="heart"))
 
 
 def test_gem_spin_and_rotate_pivot_on_the_center():
@@ -350,3 +350,43 @@ def test_polish_tilts_the_shading_normal_only():
     _, ha = _hits(a, rs)
     _, hb = _hits(b, rs)
     assert np.array_equal(ha, hb)
+
+
+def test_interior_rays_in_overlapping_gems_are_order_independent():
+    """A ray inside two overlapping stones crosses the nearer exit.  The
+    reference's slab test also reports a phantom crossing at t_max for a solid
+    whose exit lies beyond it; here a solid with no crossing in [tmin, tmax]
+    is no hit, so the BVH and the brute-force scan agree on every ray."""
+    sb = SceneBuilder()
+    m = sb.add_material(Material.dielectric(1.5))
+    sb.add_diamond((-0.3, 0.0, 0.0), 1.0, m)
+    sb.add_diamond((0.3, 0.0, 0.0), 1.0, m, rotate=(0.0, 20.0, 0.0))
+    rng = np.random.default_rng(4)
+    o = np.stack([rng.uniform(-0.4, 0.4, 8000), rng.uniform(-0.3, 0.2, 8000), rng.uniform(-0.4, 0.4, 8000)], 1)
+    for c in sb.convex:                            # keep origins strictly inside both stones
+        P = c["planes"].astype(np.float64)
+        nw = P[:, :3] @ c["rot"].T
+        dw = (nw * (np.array(c["pivot"]) + np.array(c["translate"]))).sum(1) + c["scale"] * P[:, 3] - \
+            (P[:, :3] * np.array(c["pivot"])).sum(1)
+        o = o[((o @ nw.T) < dw[None, :] - 1e-3).all(1)]
+    n = len(o)
+    assert n > 2000
+    d = rng.normal(0, 1, (n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rs = np.concatenate([o, d, np.full((n, 1), 0.001), np.full((n, 1), np.inf)], 1).astype(np.float32)
+    s = O.OracleScene(sb)
+    h, hb = s.trace_closest(rs), s.trace_closest(rs, brute=True)
+    assert (h["prim"] >= 0).all() and np.array_equal(h, hb)
+    assert (_plane_idx(h) >= 0).all()
+    # the nearer of the two exits, from the planes directly (float64)
+    t_exit = []
+    for c in sb.convex:
+        P = c["planes"].astype(np.float64) @ np.eye(4)
+        R = c["rot"]
+        nw = P[:, :3] @ R.T
+        dw = (nw * (np.array(c["pivot"]) + np.array(c["translate"]))).sum(1) + c["scale"] * P[:, 3] - \
+            (P[:, :3] * np.array(c["pivot"])).sum(1)
+        nd = d @ nw.T
+        tf = (dw[None, :] - o @ nw.T) / nd
+        t_exit.append(np.where(nd > 0, tf, np.inf).min(1))
+    np.testing.assert_allclose(h["t"], np.minimum(*t_exit), rtol=1e-4, atol=1e-5)
