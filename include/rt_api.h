@@ -53,6 +53,7 @@ extern "C" {
 #define RT_MAT_SPECTRAL_METAL      4  /* material.rs:427-554 */
 #define RT_MAT_DIFFUSE_LIGHT       5  /* material.rs:14-25 */
 #define RT_MAT_BLACKBODY_LIGHT     6  /* material.rs:40-83 */
+#define RT_MAT_PBR                 7  /* PbrMaterial with scalar parameters, material.rs:680-1050 */
 
 /* conductor n,k tables built into the library (src/spectrum.rs:213-240) */
 #define RT_METAL_GOLD    0
@@ -78,6 +79,20 @@ typedef struct RtMaterial {
     float   nk_step;         /* RT_METAL_CUSTOM: grid step (nm) */
     float   nk_n[RT_MAX_NK];
     float   nk_k[RT_MAX_NK];
+    /* RT_MAT_PBR (albedo, roughness above): metallic workflow GGX with an
+     * anisotropic base lobe, a clearcoat with optional thin film, a sheen lobe
+     * and an emission (material.rs:680-1050) */
+    float   metallic;            /* 0 dielectric .. 1 conductor */
+    float   anisotropy;          /* 0 .. 1 */
+    float   anisotropy_angle;    /* radians, in the tangent plane */
+    float   clearcoat;           /* coat weight 0 .. 1 */
+    float   clearcoat_roughness;
+    float   film_thickness;      /* nm; 0 = no thin film on the coat */
+    float   film_ior;
+    float   sheen;               /* 0 .. 1 */
+    float   sheen_tint;          /* 0 white .. 1 albedo */
+    float   emission[3];         /* linear RGB, times emission_strength */
+    float   emission_strength;
 } RtMaterial;
 
 /* ── background (src/renderer.rs:183-223) ────────────────────────────────── */

@@ -31,6 +31,7 @@ def lib():
         L.orc_last_error.restype = C.c_char_p
         L.orc_scene_create.argtypes = [C.POINTER(abi.RtSceneDesc), C.POINTER(vp)]
         L.orc_scene_destroy.argtypes = [vp]
+        L.orc_pbr_scatter.argtypes = [C.POINTER(abi.RtMaterial), fp, i64, C.POINTER(i32), fp, fp, fp, fp, fp]
         L.orc_bvh_export.argtypes = [vp, fp, C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]
         L.orc_trace_closest.argtypes = [vp, fp, i64, C.POINTER(abi.RtHit), i32, i32]
         L.orc_trace_any.argtypes = [vp, fp, i64, C.POINTER(C.c_uint8), i32]
@@ -110,6 +111,26 @@ def elut():
     out = np.zeros((64, 64), np.float32)
     lib().orc_elut_export(_fp(out))
     return out
+
+
+def pbr_scatter(mat, wo, n, xi, spec_wi=None):
+    """PbrMaterial::scatter (material.rs:790-920) for rows of (wo, n, 4 random
+    numbers): lobe (0 none, 1 specular, 2 diffuse), attenuation, direction, and
+    specular_brdf_cos / specular_sampling_pdf at spec_wi (else the sampled
+    direction)."""
+    wo = np.asarray(wo, np.float32).reshape(-1, 3)
+    k = len(wo)
+    a = np.zeros((k, 10), np.float32)
+    a[:, :3] = wo
+    a[:, 3:6] = np.broadcast_to(np.asarray(n, np.float32), (k, 3))
+    a[:, 6:10] = np.asarray(xi, np.float32).reshape(k, 4)
+    lobe = np.zeros(k, np.int32)
+    att, d, bc = (np.zeros((k, 3), np.float32) for _ in range(3))
+    pdf = np.zeros(k, np.float32)
+    swi = None if spec_wi is None else np.ascontiguousarray(np.asarray(spec_wi, np.float32).reshape(k, 3))
+    lib().orc_pbr_scatter(C.byref(mat), _fp(a), k, lobe.ctypes.data_as(C.POINTER(C.c_int32)), _fp(att), _fp(d),
+                          None if swi is None else _fp(swi), _fp(bc), _fp(pdf))
+    return lobe, att, d, bc, pdf
 
 
 def hg_sample(w, g, xi1, xi2):

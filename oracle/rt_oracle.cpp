@@ -148,6 +148,7 @@ enum {
     B_SCATTER0 = 0, B_SCATTER1 = 1, B_LPICK = 2, B_LPT0 = 3, B_LPT1 = 4,
     B_SUN0 = 5, B_SUN1 = 6,
     B_ENV_ROW = 7, B_ENV_COL = 8, B_ENV_JU = 9, B_ENV_JV = 10, B_COS0 = 11, B_COS1 = 12, B_RR = 13,
+    B_LOBE0 = 14, B_LOBE1 = 15,   // PBR lobe choice: clearcoat, then base specular
 };
 
 // ── spectrum.rs ──────────────────────────────────────────────────────────────
@@ -338,6 +339,187 @@ static inline float e_ss_lut(float mu, float alpha) {                           
 }
 static inline float specular_energy_comp(float mu, float alpha) {                  // material.rs:265-267
     return rmin(1.0f / rmax(e_ss_lut(mu, alpha), 0.05f), 10.0f);
+}
+
+// ── PbrMaterial (material.rs:680-1050) ──────────────────────────────────────
+static inline float smith_lambda_aniso(float c, float tx, float ty, float ax, float ay) {   // material.rs:187-190
+    return (std::sqrt(c * c + ax * ax * tx * tx + ay * ay * ty * ty) - c) / (2.0f * c);
+}
+static inline float smith_g1_aniso(float c, float tx, float ty, float ax, float ay) {       // material.rs:172-175
+    float denom = c + std::sqrt(c * c + ax * ax * tx * tx + ay * ay * ty * ty);
+    return rmin(rmax(2.0f * c / rmax(denom, 1e-6f), 0.0f), 1.0f);
+}
+static inline float ggx_ndf_aniso(V3 h, float ax, float ay) {                      // material.rs:316-321
+    float hx = h.x / ax, hy = h.y / ay;
+    float d = hx * hx + hy * hy + h.z * h.z;
+    return 1.0f / rmax(PI_F * ax * ay * d * d, 1e-12f);
+}
+static inline float schlick(float cosine, float ref_idx) {                         // material.rs:106-111
+    float b = (1.0f - ref_idx) / (1.0f + ref_idx);
+    float r0 = b * b, u = 1.0f - cosine;
+    return r0 + (1.0f - r0) * (u * u * u * u * u);
+}
+static inline V3 schlick_color(float ct, V3 f0) {                                  // material.rs:155-160
+    float u = rmax(1.0f - ct, 0.0f), t = u * u * u * u * u;
+    return f0 + (v3(1, 1, 1) - f0) * t;
+}
+// NACRE_LUT (material.rs:1096-1118) from spectral_to_rgb over 380..700 nm
+static V3 g_nacre[256];
+static std::once_flag g_nacre_once;
+static void nacre_init() {
+    float sum[3] = {0, 0, 0};
+    for (int i = 0; i < RT_CIE_N; i++) {
+        float rgb[3];
+        xyz_to_srgb_clamped(RT_CIE_XYZ[i][0], RT_CIE_XYZ[i][1], RT_CIE_XYZ[i][2], rgb);
+        for (int k = 0; k < 3; k++) sum[k] += rgb[k];
+    }
+    float norm[3];
+    for (int k = 0; k < 3; k++) norm[k] = (float)RT_CIE_N / rmax(sum[k], 1e-6f);
+    for (int i = 0; i < 256; i++) {
+        float opd = (float)i / 255.0f * 2500.0f;
+        V3 c = v3(0, 0, 0);
+        for (float lambda = 380.0f; lambda <= 700.01f; lambda += 5.0f) {
+            float t = rmin(rmax((lambda - 380.0f) / 5.0f, 0.0f), (float)(RT_CIE_N - 1));
+            int k = std::min((int)t, RT_CIE_N - 2);
+            float f = t - (float)k, xyz[3], rgb[3];
+            for (int q = 0; q < 3; q++) xyz[q] = RT_CIE_XYZ[k][q] + f * (RT_CIE_XYZ[k + 1][q] - RT_CIE_XYZ[k][q]);
+            xyz_to_srgb_clamped(xyz[0], xyz[1], xyz[2], rgb);
+            float irid = 0.5f * (1.0f + std::cos(2.0f * PI_F * opd / lambda));
+            c = c + v3(rgb[0] * norm[0], rgb[1] * norm[1], rgb[2] * norm[2]) * irid;
+        }
+        g_nacre[i] = c / 65.0f;
+    }
+}
+static V3 nacre_color(float ct, float film_ior, float thick) {                     // material.rs:1130-1146
+    std::call_once(g_nacre_once, nacre_init);
+    float sin_sq = rmax(1.0f - ct * ct, 0.0f);
+    float cos_t = std::sqrt(rmax(1.0f - sin_sq / (film_ior * film_ior), 0.0f));
+    float opd = 2.0f * film_ior * thick * cos_t;
+    float t = rmin(rmax(opd / 2500.0f, 0.0f), 1.0f) * 255.0f;
+    int lo = (int)t, hi = std::min(lo + 1, 255);
+    V3 raw = g_nacre[lo] * (1.0f - (t - (float)lo)) + g_nacre[hi] * (t - (float)lo);
+    float blend = std::pow(ct, 0.5f);
+    return raw * blend + v3(0.5f, 0.5f, 0.5f) * (1.0f - blend);
+}
+struct PbrCommon { V3 albedo, f0; float alpha, p_coat, p_spec, ax, ay; };
+static PbrCommon pbr_common(const RtMaterial& m, float cos_o) {
+    PbrCommon c;
+    c.albedo = v3(m.albedo[0], m.albedo[1], m.albedo[2]);
+    c.alpha = rmax(m.roughness * m.roughness, 1e-4f);
+    c.f0 = v3(0.04f, 0.04f, 0.04f) * (1.0f - m.metallic) + c.albedo * m.metallic;
+    c.p_coat = m.clearcoat > 1e-3f ? rmax(schlick(cos_o, 1.0f / 1.5f) * m.clearcoat, 0.12f * m.clearcoat) : 0.0f;
+    c.p_spec = m.metallic > 0.999f ? 1.0f : rmin(rmax(luminance(schlick_color(cos_o, c.f0)), 0.04f), 0.9f);
+    // Disney aspect: ax (tangent) = α/aspect, ay (bitangent) = α·aspect
+    float aspect = std::sqrt(rmax(1.0f - 0.9f * rmin(rmax(m.anisotropy, 0.0f), 1.0f), 0.001f));
+    c.ax = c.alpha / aspect;
+    c.ay = c.alpha * aspect;
+    return c;
+}
+static void pbr_frame(const RtMaterial& m, V3 n, V3* t, V3* b) {
+    V3 t0, b0;
+    onb_vec(n, &t0, &b0);
+    float ca = std::cos(m.anisotropy_angle), sa = std::sin(m.anisotropy_angle);
+    *t = t0 * ca + b0 * sa;
+    *b = b0 * ca - t0 * sa;
+}
+enum { PBR_NONE = 0, PBR_SPECULAR = 1, PBR_DIFFUSE = 2 };
+// PbrMaterial::scatter (material.rs:790-920)
+static int pbr_scatter(const RtMaterial& m, V3 wo, V3 n, float xi_coat, float xi_spec, float xi1, float xi2,
+                       V3* att, V3* dir) {
+    float cos_o = dot(wo, n);
+    if (cos_o <= 0.0f) return PBR_NONE;
+    PbrCommon c = pbr_common(m, cos_o);
+    if (xi_coat < c.p_coat) {
+        float ac = rmax(m.clearcoat_roughness * m.clearcoat_roughness, 1e-4f);
+        V3 t, b;
+        onb_vec(n, &t, &b);
+        V3 ms = vndf_sample(v3(dot(wo, t), dot(wo, b), cos_o), ac, ac, xi1, xi2);
+        V3 mm = unit(t * ms.x + b * ms.y + n * ms.z);
+        float vo_h = rmax(dot(wo, mm), 0.0f);
+        V3 wi = unit(2.0f * vo_h * mm - wo);
+        float cos_i = dot(wi, n);
+        if (cos_i <= 0.0f) return PBR_NONE;
+        float f_coat = schlick(vo_h, 1.0f / 1.5f) * m.clearcoat;
+        float lo = smith_lambda(cos_o, ac), li = smith_lambda(cos_i, ac);
+        float w = ((1.0f + lo) / (1.0f + lo + li)) * specular_energy_comp(cos_o, ac);
+        V3 film = m.film_thickness > 0.0f ? nacre_color(vo_h, m.film_ior, m.film_thickness) : v3(1, 1, 1);
+        *att = film * (f_coat * w / c.p_coat);
+        *dir = wi;
+        return PBR_SPECULAR;
+    }
+    if (xi_spec < c.p_spec) {
+        V3 t, b;
+        pbr_frame(m, n, &t, &b);
+        V3 wo_ts = v3(dot(wo, t), dot(wo, b), cos_o);
+        V3 ms = vndf_sample(wo_ts, c.ax, c.ay, xi1, xi2);
+        V3 mm = unit(t * ms.x + b * ms.y + n * ms.z);
+        float vo_h = rmax(dot(wo, mm), 0.0f);
+        V3 wi = unit(2.0f * vo_h * mm - wo);
+        float cos_i = dot(wi, n);
+        if (cos_i <= 0.0f) return PBR_NONE;
+        V3 wi_ts = v3(dot(wi, t), dot(wi, b), cos_i);
+        float lo = smith_lambda_aniso(cos_o, wo_ts.x, wo_ts.y, c.ax, c.ay);
+        float li = smith_lambda_aniso(cos_i, wi_ts.x, wi_ts.y, c.ax, c.ay);
+        float w = ((1.0f + lo) / (1.0f + lo + li)) * specular_energy_comp(cos_o, c.alpha);
+        *att = schlick_color(vo_h, c.f0) * w / (c.p_spec * (1.0f - c.p_coat));
+        *dir = wi;
+        return PBR_SPECULAR;
+    }
+    V3 sheen = v3(0, 0, 0);
+    if (m.sheen > 0.0f && m.metallic < 0.999f) {
+        float luma = luminance(c.albedo);
+        V3 c_tint = luma > 1e-6f ? c.albedo / luma : v3(1, 1, 1);
+        V3 sc = v3(1, 1, 1) * (1.0f - m.sheen_tint) + c_tint * m.sheen_tint;
+        float u = 1.0f - cos_o, f_h = u * u * u * u * u;
+        sheen = sc * (m.sheen * (1.0f - m.metallic) * f_h * PI_F);
+    }
+    *att = (c.albedo * (1.0f - m.metallic) + sheen) / ((1.0f - c.p_spec) * (1.0f - c.p_coat));
+    return PBR_DIFFUSE;
+}
+// PbrMaterial::specular_brdf_cos (material.rs:935-992)
+static V3 pbr_specular_brdf_cos(const RtMaterial& m, V3 wo, V3 n, V3 wi) {
+    float cos_o = dot(wo, n), cos_i = dot(wi, n);
+    if (cos_o <= 0.0f || cos_i <= 0.0f) return v3(0, 0, 0);
+    PbrCommon c = pbr_common(m, cos_o);
+    V3 h = unit(wo + wi);
+    float wo_h = rmax(dot(wo, h), 0.0f), h_n = rmax(dot(h, n), 0.0f);
+    V3 res = v3(0, 0, 0);
+    if (m.clearcoat > 1e-3f) {
+        float ac = rmax(m.clearcoat_roughness * m.clearcoat_roughness, 1e-4f);
+        float d = ggx_ndf(h_n, ac);
+        float g2 = 1.0f / (1.0f + smith_lambda(cos_o, ac) + smith_lambda(cos_i, ac));
+        float f_c = schlick(wo_h, 1.0f / 1.5f) * m.clearcoat;
+        V3 film = m.film_thickness > 0.0f ? nacre_color(wo_h, m.film_ior, m.film_thickness) : v3(1, 1, 1);
+        res = res + film * (d * f_c * g2 / (4.0f * cos_o) * specular_energy_comp(cos_o, ac));
+    }
+    V3 t, b;
+    pbr_frame(m, n, &t, &b);
+    V3 h_ts = v3(dot(h, t), dot(h, b), h_n);
+    float d = ggx_ndf_aniso(h_ts, c.ax, c.ay);
+    float g2 = 1.0f / (1.0f + smith_lambda_aniso(cos_o, dot(wo, t), dot(wo, b), c.ax, c.ay) +
+                       smith_lambda_aniso(cos_i, dot(wi, t), dot(wi, b), c.ax, c.ay));
+    return res + schlick_color(wo_h, c.f0) * (d * g2 / (4.0f * cos_o) * specular_energy_comp(cos_o, c.alpha));
+}
+// PbrMaterial::specular_sampling_pdf (material.rs:994-1045)
+static float pbr_specular_pdf(const RtMaterial& m, V3 wo, V3 n, V3 wi) {
+    float cos_o = dot(wo, n), cos_i = dot(wi, n);
+    if (cos_o <= 0.0f || cos_i <= 0.0f) return 0.0f;
+    PbrCommon c = pbr_common(m, cos_o);
+    V3 h = unit(wo + wi);
+    float h_n = rmax(dot(h, n), 0.0f);
+    float pdf = 0.0f;
+    if (m.clearcoat > 1e-3f) {
+        float ac = rmax(m.clearcoat_roughness * m.clearcoat_roughness, 1e-4f);
+        pdf += c.p_coat * ggx_ndf(h_n, ac) * smith_g1(cos_o, ac) / (4.0f * cos_o);
+    }
+    if ((1.0f - c.p_coat) * c.p_spec > 1e-6f) {
+        V3 t, b;
+        pbr_frame(m, n, &t, &b);
+        float d = ggx_ndf_aniso(v3(dot(h, t), dot(h, b), h_n), c.ax, c.ay);
+        pdf += (1.0f - c.p_coat) * c.p_spec * d * smith_g1_aniso(cos_o, dot(wo, t), dot(wo, b), c.ax, c.ay) /
+               (4.0f * cos_o);
+    }
+    return pdf;
 }
 
 // ── scene ────────────────────────────────────────────────────────────────────
@@ -1440,6 +1622,18 @@ static bool trace_photon(const Scene& s, V3 pos, V3 dir, float lum_clamp, V3 pow
     float lam = s.spec.lam_lo + s.spec.lam_range * rnd(rng, P_LAMBDA);
     if (lam >= s.spec.lam_lo + s.spec.lam_range) lam = std::nextafter(s.spec.lam_lo + s.spec.lam_range, 0.0f);
     uint32_t spec_depth = 0;
+    // storage at a diffuse surface, spectral spikes clamped once (photon.rs:260-271)
+    auto store = [&](const Rec& rec) {
+        float lum = luminance(power);
+        if (lum > lum_clamp) power = power * (lum_clamp / lum);
+        KdPhoton k;
+        k.pos[0] = rec.p.x; k.pos[1] = rec.p.y; k.pos[2] = rec.p.z;
+        k.power[0] = power.x; k.power[1] = power.y; k.power[2] = power.z;
+        k.nor[0] = rec.normal.x; k.nor[1] = rec.normal.y; k.nor[2] = rec.normal.z;
+        k.axis = 0;
+        *out = k;
+        return true;
+    };
     for (int bounce = 0; bounce < PHOTON_MAX_DEPTH; bounce++) {
         uint32_t base = P_BOUNCE0 + bounce * P_PER_BOUNCE;
         Ray ray{pos, dir};
@@ -1514,18 +1708,25 @@ static bool trace_photon(const Scene& s, V3 pos, V3 dir, float lum_clamp, V3 pow
             power = power * (spectral_to_rgb(s.spec, lam) * (fresnel_conductor(cos_h, nn, kk) * weight));
             pos = rec.p; dir = nd;
             spec_depth++;
+        } else if (m.type == RT_MAT_PBR) {
+            // PbrMaterial::scatter: a specular lobe carries the photon on, the
+            // diffuse lobe stores it where can_receive_caustics (material.rs:1049)
+            V3 att, nd;
+            int lobe = pbr_scatter(m, unit(-ray.d), rec.normal, rnd(rng, base + 2), rnd(rng, base + 3),
+                                   rnd(rng, base + 0), rnd(rng, base + 1), &att, &nd);
+            if (lobe == PBR_NONE) return false;
+            if (lobe == PBR_SPECULAR) {
+                power = power * att;
+                pos = rec.p; dir = nd;
+                spec_depth++;
+                continue;
+            }
+            if (!(m.metallic < 0.999f) || spec_depth == 0) return false;
+            return store(rec);
         } else {
             // diffuse (Lambertian / checker): can_receive_caustics (material.rs:101)
             if (spec_depth == 0) return false;
-            float lum = luminance(power);
-            if (lum > lum_clamp) power = power * (lum_clamp / lum);
-            KdPhoton k;
-            k.pos[0] = rec.p.x; k.pos[1] = rec.p.y; k.pos[2] = rec.p.z;
-            k.power[0] = power.x; k.power[1] = power.y; k.power[2] = power.z;
-            k.nor[0] = rec.normal.x; k.nor[1] = rec.normal.y; k.nor[2] = rec.normal.z;
-            k.axis = 0;
-            *out = k;
-            return true;
+            return store(rec);
         }
     }
     return false;
@@ -1652,6 +1853,8 @@ static V3 spec_factor(const Spectrum& sp, const SpecState& ss) {
 static V3 emission(const Scene& s, int mat, const SpecState& ss) {
     const RtMaterial& m = s.mats[mat];
     if (m.type == RT_MAT_DIFFUSE_LIGHT) return v3(m.albedo[0], m.albedo[1], m.albedo[2]) * spec_factor(s.spec, ss);
+    if (m.type == RT_MAT_PBR)                                                       // material.rs:922-924
+        return v3(m.emission[0], m.emission[1], m.emission[2]) * m.emission_strength * spec_factor(s.spec, ss);
     if (m.type == RT_MAT_BLACKBODY_LIGHT) {
         if (ss.tint == TINT_NONE) return s.bb_avg[mat] * spec_factor(s.spec, ss);
         V3 acc = v3(0, 0, 0);
@@ -1835,87 +2038,130 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
             prev_specular = true;
             prev_mis_w_brdf = 1.0f;
         } else {
-            // Lambertian / checker (material.rs:85-102): diffuse branch renderer.rs:457-572
-            V3 att = lambert_albedo(m, rec.p);
-            if (s.has_photons) {                                                    // renderer.rs:461-467
-                V3 irr = photon_irradiance(s, rec.p, rec.normal);
-                if (irr.x > 0.0f || irr.y > 0.0f || irr.z > 0.0f)
-                    color = color + (T * spec_factor(s.spec, ss)) * att * irr;
+            // Lambertian / checker (material.rs:85-102) or PbrMaterial
+            // (material.rs:790-920): diffuse branch renderer.rs:457-572
+            V3 att, hint;   // scatter attenuation; albedo_hint for the caustic term
+            bool diffuse = true;
+            if (m.type == RT_MAT_PBR) {
+                // the emission adds at the hit (renderer.rs:415-417), then one lobe scatters
+                color = color + T * emission(s, rec.mat, ss) * emit_w;
+                V3 wo = unit(-ray.d), dir;
+                int lobe = pbr_scatter(m, wo, rec.normal, rnd(rng, base + B_LOBE0), rnd(rng, base + B_LOBE1),
+                                       rnd(rng, base + B_SCATTER0), rnd(rng, base + B_SCATTER1), &att, &dir);
+                if (lobe == PBR_NONE) break;
+                hint = v3(m.albedo[0], m.albedo[1], m.albedo[2]);
+                if (lobe == PBR_SPECULAR) {
+                    // specular sun NEE (renderer.rs:421-456)
+                    prev_spec_sun_weight = 1.0f;
+                    if (has_sun(s)) {
+                        const float p_sun = 1.0f / (2.0f * PI_F * (1.0f - COS_SUN_MAX));
+                        V3 sun_s = sample_sun_cone(unit(sun_vec(s)), COS_SUN_MAX, rnd(rng, base + B_SUN0),
+                                                   rnd(rng, base + B_SUN1));
+                        (*n_shadow)++;
+                        float tr = scene_transmittance(s, Ray{rec.p, sun_s}, 0.001f, INFINITY);
+                        if (tr > 0.0f) {
+                            V3 bc = pbr_specular_brdf_cos(m, wo, rec.normal, sun_s);
+                            if (bc.x > 0.0f || bc.y > 0.0f || bc.z > 0.0f) {
+                                float p_mat = pbr_specular_pdf(m, wo, rec.normal, sun_s);
+                                V3 sun_color = bg_eval(s, sun_s) * spec_factor(s.spec, ss);
+                                float mis_d = p_sun * p_sun + p_mat * p_mat;
+                                if (mis_d > 0.0f) color = color + T * tr * bc * sun_color * p_sun / mis_d;
+                            }
+                        }
+                        float p_b = pbr_specular_pdf(m, wo, rec.normal, dir);
+                        if (p_b > 0.0f) prev_spec_sun_weight = (p_b * p_b) / rmax(p_b * p_b + p_sun * p_sun, 1e-8f);
+                    }
+                    T = T * att;
+                    ray = Ray{rec.p, dir};
+                    prev_specular = true;
+                    prev_mis_w_brdf = 1.0f;
+                    diffuse = false;
+                }
+            } else {
+                att = lambert_albedo(m, rec.p);
+                hint = att;
             }
-            if (have_lights) {
-                uint32_t pick = rnd_u32(rng, base + B_LPICK) % (uint32_t)s.lights.size();
-                V3 light_dir = prim_pdf_generate(s, s.lights[pick], rec.p, rnd(rng, base + B_LPT0), rnd(rng, base + B_LPT1));
-                Ray shadow{rec.p, light_dir};
-                Rec lrec;
-                if (lights_hit(s, shadow, 0.001f, INFINITY, &lrec)) {
-                    (*n_shadow)++;
-                    float tr = scene_transmittance(s, shadow, 0.001f, lrec.t * (1.0f - 1e-4f));
-                    if (tr > 0.0f) {
-                        float l_pdf = lights_pdf_value(s, rec.p, light_dir);
-                        float brdf = rmax(dot(rec.normal, unit(light_dir)) / PI_F, 0.0f);
-                        float sun_p = sun_pdf_value(s, light_dir);
-                        float env_p = env_pdf_value(s, light_dir);
-                        float mis_d = l_pdf * l_pdf + brdf * brdf + sun_p * sun_p + env_p * env_p;
-                        if (mis_d > 0.0f && brdf > 0.0f) {
-                            V3 nee = emission(s, lrec.mat, ss);
-                            color = color + T * tr * att * brdf * l_pdf * nee / mis_d;
+            if (diffuse) {
+                if (s.has_photons) {                                                    // renderer.rs:461-467
+                    V3 irr = photon_irradiance(s, rec.p, rec.normal);
+                    if (irr.x > 0.0f || irr.y > 0.0f || irr.z > 0.0f)
+                        color = color + (T * spec_factor(s.spec, ss)) * hint * irr;
+                }
+                if (have_lights) {
+                    uint32_t pick = rnd_u32(rng, base + B_LPICK) % (uint32_t)s.lights.size();
+                    V3 light_dir = prim_pdf_generate(s, s.lights[pick], rec.p, rnd(rng, base + B_LPT0), rnd(rng, base + B_LPT1));
+                    Ray shadow{rec.p, light_dir};
+                    Rec lrec;
+                    if (lights_hit(s, shadow, 0.001f, INFINITY, &lrec)) {
+                        (*n_shadow)++;
+                        float tr = scene_transmittance(s, shadow, 0.001f, lrec.t * (1.0f - 1e-4f));
+                        if (tr > 0.0f) {
+                            float l_pdf = lights_pdf_value(s, rec.p, light_dir);
+                            float brdf = rmax(dot(rec.normal, unit(light_dir)) / PI_F, 0.0f);
+                            float sun_p = sun_pdf_value(s, light_dir);
+                            float env_p = env_pdf_value(s, light_dir);
+                            float mis_d = l_pdf * l_pdf + brdf * brdf + sun_p * sun_p + env_p * env_p;
+                            if (mis_d > 0.0f && brdf > 0.0f) {
+                                V3 nee = emission(s, lrec.mat, ss);
+                                color = color + T * tr * att * brdf * l_pdf * nee / mis_d;
+                            }
                         }
                     }
                 }
-            }
-            if (has_sun(s)) {                                                       // renderer.rs:495-518
-                V3 sun_s = sample_sun_cone(unit(sun_vec(s)), COS_SUN_MAX, rnd(rng, base + B_SUN0), rnd(rng, base + B_SUN1));
-                (*n_shadow)++;
-                float tr = scene_transmittance(s, Ray{rec.p, sun_s}, 0.001f, INFINITY);
-                if (tr > 0.0f) {
-                    float brdf = rmax(dot(rec.normal, unit(sun_s)) / PI_F, 0.0f);
-                    if (brdf > 0.0f) {
-                        float sun_pdf = 1.0f / (2.0f * PI_F * (1.0f - COS_SUN_MAX));
-                        V3 sun_color = bg_eval(s, sun_s) * spec_factor(s.spec, ss);
-                        float area_pdf = have_lights ? lights_pdf_value(s, rec.p, sun_s) : 0.0f;
-                        float mis_d = sun_pdf * sun_pdf + brdf * brdf + area_pdf * area_pdf;
-                        color = color + T * tr * att * brdf * sun_pdf * sun_color / mis_d;
-                    }
-                }
-            }
-            if (s.has_env) {
-                float env_pdf;
-                V3 env_dir = env_sample_dir(s.env, rnd(rng, base + B_ENV_ROW), rnd(rng, base + B_ENV_COL),
-                                            rnd(rng, base + B_ENV_JU), rnd(rng, base + B_ENV_JV), &env_pdf);
-                if (env_pdf > 0.0f) {
-                    Ray shadow{rec.p, env_dir};
+                if (has_sun(s)) {                                                       // renderer.rs:495-518
+                    V3 sun_s = sample_sun_cone(unit(sun_vec(s)), COS_SUN_MAX, rnd(rng, base + B_SUN0), rnd(rng, base + B_SUN1));
                     (*n_shadow)++;
-                    float tr = scene_transmittance(s, shadow, 0.001f, INFINITY);
+                    float tr = scene_transmittance(s, Ray{rec.p, sun_s}, 0.001f, INFINITY);
                     if (tr > 0.0f) {
-                        float brdf = rmax(dot(rec.normal, unit(env_dir)) / PI_F, 0.0f);
+                        float brdf = rmax(dot(rec.normal, unit(sun_s)) / PI_F, 0.0f);
                         if (brdf > 0.0f) {
-                            float area_pdf = have_lights ? lights_pdf_value(s, rec.p, env_dir) : 0.0f;
-                            V3 env_color = env_eval(s, env_dir) * spec_factor(s.spec, ss);
-                            float mis_d = env_pdf * env_pdf + brdf * brdf + area_pdf * area_pdf;
-                            color = color + T * tr * att * brdf * env_pdf * env_color / mis_d;
+                            float sun_pdf = 1.0f / (2.0f * PI_F * (1.0f - COS_SUN_MAX));
+                            V3 sun_color = bg_eval(s, sun_s) * spec_factor(s.spec, ss);
+                            float area_pdf = have_lights ? lights_pdf_value(s, rec.p, sun_s) : 0.0f;
+                            float mis_d = sun_pdf * sun_pdf + brdf * brdf + area_pdf * area_pdf;
+                            color = color + T * tr * att * brdf * sun_pdf * sun_color / mis_d;
                         }
                     }
                 }
-            }
-            // indirect: cosine-weighted sample (pdf.rs:12-41)
-            Onb uvw = onb_from_w(rec.normal);
-            float r1 = rnd(rng, base + B_COS0), r2 = rnd(rng, base + B_COS1);
-            float phi = 2.0f * PI_F * r1;
-            float sq = std::sqrt(r2);
-            V3 ind_dir = onb_local(uvw, v3(std::cos(phi) * sq, std::sin(phi) * sq, std::sqrt(1.0f - r2)));
-            float pdf_val = rmax(dot(unit(ind_dir), uvw.w) / PI_F, 0.0f);
-            if (pdf_val <= 0.0f) break;
-            float scat_pdf = rmax(dot(rec.normal, unit(ind_dir)) / PI_F, 0.0f);
-            if (scat_pdf <= 0.0f) break;
-            if (dot(ind_dir, rec.normal) <= 0.0f) break;
-            float area = have_lights ? lights_pdf_value(s, rec.p, ind_dir) : 0.0f;
-            float sun = sun_pdf_value(s, ind_dir);
-            float env = env_pdf_value(s, ind_dir);
-            float nee_sq = area * area + sun * sun + env * env;
-            prev_mis_w_brdf = (pdf_val * pdf_val) / rmax(pdf_val * pdf_val + nee_sq, 1e-8f);
-            T = T * (att * (scat_pdf / pdf_val));
-            ray = Ray{rec.p, ind_dir};
-            prev_specular = false;
+                if (s.has_env) {
+                    float env_pdf;
+                    V3 env_dir = env_sample_dir(s.env, rnd(rng, base + B_ENV_ROW), rnd(rng, base + B_ENV_COL),
+                                                rnd(rng, base + B_ENV_JU), rnd(rng, base + B_ENV_JV), &env_pdf);
+                    if (env_pdf > 0.0f) {
+                        Ray shadow{rec.p, env_dir};
+                        (*n_shadow)++;
+                        float tr = scene_transmittance(s, shadow, 0.001f, INFINITY);
+                        if (tr > 0.0f) {
+                            float brdf = rmax(dot(rec.normal, unit(env_dir)) / PI_F, 0.0f);
+                            if (brdf > 0.0f) {
+                                float area_pdf = have_lights ? lights_pdf_value(s, rec.p, env_dir) : 0.0f;
+                                V3 env_color = env_eval(s, env_dir) * spec_factor(s.spec, ss);
+                                float mis_d = env_pdf * env_pdf + brdf * brdf + area_pdf * area_pdf;
+                                color = color + T * tr * att * brdf * env_pdf * env_color / mis_d;
+                            }
+                        }
+                    }
+                }
+                // indirect: cosine-weighted sample (pdf.rs:12-41)
+                Onb uvw = onb_from_w(rec.normal);
+                float r1 = rnd(rng, base + B_COS0), r2 = rnd(rng, base + B_COS1);
+                float phi = 2.0f * PI_F * r1;
+                float sq = std::sqrt(r2);
+                V3 ind_dir = onb_local(uvw, v3(std::cos(phi) * sq, std::sin(phi) * sq, std::sqrt(1.0f - r2)));
+                float pdf_val = rmax(dot(unit(ind_dir), uvw.w) / PI_F, 0.0f);
+                if (pdf_val <= 0.0f) break;
+                float scat_pdf = rmax(dot(rec.normal, unit(ind_dir)) / PI_F, 0.0f);
+                if (scat_pdf <= 0.0f) break;
+                if (dot(ind_dir, rec.normal) <= 0.0f) break;
+                float area = have_lights ? lights_pdf_value(s, rec.p, ind_dir) : 0.0f;
+                float sun = sun_pdf_value(s, ind_dir);
+                float env = env_pdf_value(s, ind_dir);
+                float nee_sq = area * area + sun * sun + env * env;
+                prev_mis_w_brdf = (pdf_val * pdf_val) / rmax(pdf_val * pdf_val + nee_sq, 1e-8f);
+                T = T * (att * (scat_pdf / pdf_val));
+                ray = Ray{rec.p, ind_dir};
+                prev_specular = false;
+            }   // diffuse
         }
         }   // surface hit
         if (depth >= 2) {                                                           // renderer.rs:574-579
@@ -2213,6 +2459,28 @@ int32_t orc_hg_sample(const float* in, int64_t n, float* out) {
         const float* a = in + i * 6;
         V3 d = hg_sample(v3(a[0], a[1], a[2]), a[3], a[4], a[5]);
         out[i * 3] = d.x; out[i * 3 + 1] = d.y; out[i * 3 + 2] = d.z;
+    }
+    return RT_OK;
+}
+
+// PbrMaterial::scatter for n rows of 10 floats (wo xyz, n xyz, xi_coat, xi_spec,
+// xi1, xi2) → per row lobe (PBR_NONE / PBR_SPECULAR / PBR_DIFFUSE), attenuation
+// and direction; plus specular_brdf_cos and specular_sampling_pdf at an
+// explicit wi (the row's direction when spec_wi is NULL)
+int32_t orc_pbr_scatter(const RtMaterial* m, const float* in, int64_t n, int32_t* lobe, float* att, float* dir,
+                        const float* spec_wi, float* brdf_cos, float* pdf) {
+    for (int64_t i = 0; i < n; i++) {
+        const float* a = in + i * 10;
+        V3 wo = v3(a[0], a[1], a[2]), nn = v3(a[3], a[4], a[5]), at = v3(0, 0, 0), d = v3(0, 0, 0);
+        lobe[i] = pbr_scatter(*m, wo, nn, a[6], a[7], a[8], a[9], &at, &d);
+        att[i * 3] = at.x; att[i * 3 + 1] = at.y; att[i * 3 + 2] = at.z;
+        dir[i * 3] = d.x; dir[i * 3 + 1] = d.y; dir[i * 3 + 2] = d.z;
+        if (brdf_cos && pdf) {
+            V3 wi = spec_wi ? v3(spec_wi[i * 3], spec_wi[i * 3 + 1], spec_wi[i * 3 + 2]) : d;
+            V3 bc = pbr_specular_brdf_cos(*m, wo, nn, wi);
+            brdf_cos[i * 3] = bc.x; brdf_cos[i * 3 + 1] = bc.y; brdf_cos[i * 3 + 2] = bc.z;
+            pdf[i] = pbr_specular_pdf(*m, wo, nn, wi);
+        }
     }
     return RT_OK;
 }

@@ -14,6 +14,7 @@ RT_MAT_SPECTRAL_DIELECTRIC = 3
 RT_MAT_SPECTRAL_METAL = 4
 RT_MAT_DIFFUSE_LIGHT = 5
 RT_MAT_BLACKBODY_LIGHT = 6
+RT_MAT_PBR = 7
 
 RT_METAL_GOLD, RT_METAL_COPPER, RT_METAL_SILVER, RT_METAL_CUSTOM = 0, 1, 2, 3
 RT_MAX_NK = 16
@@ -42,6 +43,17 @@ class RtMaterial(C.Structure):
         ("nk_step", C.c_float),
         ("nk_n", C.c_float * RT_MAX_NK),
         ("nk_k", C.c_float * RT_MAX_NK),
+        ("metallic", C.c_float),
+        ("anisotropy", C.c_float),
+        ("anisotropy_angle", C.c_float),
+        ("clearcoat", C.c_float),
+        ("clearcoat_roughness", C.c_float),
+        ("film_thickness", C.c_float),
+        ("film_ior", C.c_float),
+        ("sheen", C.c_float),
+        ("sheen_tint", C.c_float),
+        ("emission", F3),
+        ("emission_strength", C.c_float),
     ]
 
 

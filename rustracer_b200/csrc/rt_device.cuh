@@ -24,13 +24,16 @@
 #define RT_LEAF_BIT   0x80000000u
 #define RT_EMPTY_REF  0xFFFFFFFFu
 #define RT_MISS_REF   0xFFFFFFFFu
-// Hit records written by the extend kernel carry the primitive reference with
-// its leaf bit replaced by the material class: bits 31:30 = class code
-// (0 emitter, 1 diffuse, 2 conductor, 3 dielectric), 29:28 = primitive type,
-// 27:0 = typed index.  RT_MISS_REF (type 3) is never a hit.
-#define RT_HIT_TYPE(ref)  (((ref) >> 28) & 3u)
-#define RT_HIT_INDEX(ref) ((ref) & 0x0FFFFFFFu)
-#define RT_HIT_CODE(ref)  ((ref) >> 30)
+// Hit records written by the extend kernel: bits 31:29 = material class code
+// (0 emitter, 1 diffuse, 2 conductor, 3 dielectric, 4 PBR), 28:27 = primitive
+// type, 26:0 = typed index (so at most 2^27 primitives of one type).
+// RT_MISS_REF (code 7) is never a hit.
+#define RT_HIT_TYPE(ref)  (((ref) >> 27) & 3u)
+#define RT_HIT_INDEX(ref) ((ref) & 0x07FFFFFFu)
+#define RT_HIT_CODE(ref)  ((ref) >> 29)
+#define RT_HIT_MAX_INDEX  0x07FFFFFFu
+// the hit record of a leaf reference (type in 30:28, index in 27:0) and a class code
+#define RT_HIT_MAKE(leaf_ref, code) (((uint32_t)(code) << 29) | ((((leaf_ref) >> 28) & 3u) << 27) | ((leaf_ref) & 0x07FFFFFFu))
 #define RT_STACK      96
 
 namespace rtd {
@@ -54,6 +57,11 @@ struct DevMaterial {
     int   nk_count;
     float nk_start, nk_step;
     float nk_n[16], nk_k[16];
+    // PBR (material.rs:680-1050); the anisotropy frame rotation and aspect are
+    // precomputed: aniso_c/s = cos/sin(anisotropy_angle), aspect = sqrt(max(1 − 0.9·a, 0.001))
+    float metallic, aniso_c, aniso_s, aspect;
+    float clearcoat, clearcoat_roughness, film_thickness, film_ior, sheen, sheen_tint;
+    float emission[3];   // emission × emission_strength
 };
 
 struct DevLight {        // one entry of the NEE light list (hittable.rs:138-225)
@@ -89,6 +97,7 @@ struct DevScene {
     int n_lights, n_mats;
     const DevMedium* media;
     int n_media;
+    int n_pbr;                  // PBR materials in the scene (their shading kernel runs only if > 0)
     // analytic convex solids in leaf order: 2 float4 each, (plane offset, count,
     // material, polish) (canonical id, -, -, -); their world-space planes
     // (n.xyz, d); per plane the world-space shading normals of a front-face and
@@ -103,6 +112,7 @@ struct DevScene {
     float norms[3], fire_norms[3];
     float lam_lo, lam_range;
     const float* elut;          // 64×64 E_ss(mu, alpha)
+    const float4* nacre;        // 256 thin-film colours over OPD 0..2500 nm (material.rs:1096-1118)
     // environment map
     int   has_env;
     int   env_w, env_h;
@@ -182,6 +192,7 @@ enum {
     B_SCATTER0 = 0, B_SCATTER1 = 1, B_LPICK = 2, B_LPT0 = 3, B_LPT1 = 4,
     B_SUN0 = 5, B_SUN1 = 6,
     B_ENV_ROW = 7, B_ENV_COL = 8, B_ENV_JU = 9, B_ENV_JV = 10, B_COS0 = 11, B_COS1 = 12, B_RR = 13,
+    B_LOBE0 = 14, B_LOBE1 = 15,   // PBR lobe choice: clearcoat, then base specular
 };
 
 // Slab reciprocal: plain 1/d.  A ray with an infinite reciprocal component can

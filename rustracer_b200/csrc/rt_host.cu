@@ -353,6 +353,36 @@ static void xyz_srgb_h(float x, float y, float z, float o[3]) {
     o[1] = std::fmax(-0.9689f * x + 1.8758f * y + 0.0415f * z, 0.0f);
     o[2] = std::fmax(0.0557f * x - 0.2040f * y + 1.0570f * z, 0.0f);
 }
+// NACRE_LUT (material.rs:1096-1118): the thin-film colour over OPD 0..2500 nm
+// in 256 steps, the mean over 380..700 nm of spectral_to_rgb(λ)·½(1 + cos 2π·OPD/λ);
+// spectral_to_rgb uses the 380..700 nm table and its per-channel normalisation
+static float4 g_nacre[256];
+static std::once_flag g_nacre_once;
+static void build_nacre() {
+    float sum[3] = {0, 0, 0};
+    for (int i = 0; i < RT_CIE_N; i++) {
+        float rgb[3];
+        xyz_srgb_h(RT_CIE_XYZ[i][0], RT_CIE_XYZ[i][1], RT_CIE_XYZ[i][2], rgb);
+        for (int k = 0; k < 3; k++) sum[k] += rgb[k];
+    }
+    float norm[3];
+    for (int k = 0; k < 3; k++) norm[k] = (float)RT_CIE_N / std::fmax(sum[k], 1e-6f);
+    for (int i = 0; i < 256; i++) {
+        float opd = (float)i / 255.0f * 2500.0f;
+        float c[3] = {0, 0, 0};
+        for (float lambda = 380.0f; lambda <= 700.01f; lambda += 5.0f) {
+            float t = std::fmin(std::fmax((lambda - 380.0f) / 5.0f, 0.0f), (float)(RT_CIE_N - 1));
+            int k = std::min((int)t, RT_CIE_N - 2);
+            float f = t - (float)k, xyz[3];
+            for (int q = 0; q < 3; q++) xyz[q] = RT_CIE_XYZ[k][q] + f * (RT_CIE_XYZ[k + 1][q] - RT_CIE_XYZ[k][q]);
+            float rgb[3];
+            xyz_srgb_h(xyz[0], xyz[1], xyz[2], rgb);
+            float irid = 0.5f * (1.0f + std::cos(2.0f * 3.14159265358979f * opd / lambda));
+            for (int q = 0; q < 3; q++) c[q] = c[q] + rgb[q] * norm[q] * irid;
+        }
+        g_nacre[i] = make_float4(c[0] / 65.0f, c[1] / 65.0f, c[2] / 65.0f, 0.0f);
+    }
+}
 static void fire_h(float x, float y, float z, float c[3]) {
     float w = std::fmax(std::pow(y, 0.5f), 0.08f);
     float rgb[3];
@@ -532,6 +562,11 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         return bail(fail(s, RT_ERR_INVALID, "negative count"));
     if (d->n_convex < 0 || (d->n_convex > 0 && (!d->convex || !d->convex_planes)))
         return bail(fail(s, RT_ERR_INVALID, "convex solids without their arrays"));
+    // hit records carry a 27-bit index per primitive type
+    if (d->n_tris > (int64_t)RT_HIT_MAX_INDEX + 1 || d->n_quads > (int64_t)RT_HIT_MAX_INDEX + 1 ||
+        d->n_spheres > (int64_t)RT_HIT_MAX_INDEX + 1 || d->n_convex > (int64_t)RT_HIT_MAX_INDEX + 1 ||
+        d->n_media > (int64_t)RT_HIT_MAX_INDEX + 1)
+        return bail(fail(s, RT_ERR_CAPACITY, "more than 2^27 primitives of one type"));
     const int64_t n_sph_end = d->n_tris + d->n_quads + d->n_spheres;   // canonical ids of the convex solids start here
     int64_t n = n_sph_end + d->n_convex;
     if (n >= (1ll << 28) - 1) return bail(fail(s, RT_ERR_CAPACITY, "more than 2^28 - 2 primitives"));
@@ -545,7 +580,16 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     for (int64_t i = 0; i < d->n_spheres; i++) if (bad_mat(d->sphere_mat[i])) return bail(fail(s, RT_ERR_INVALID, "sphere material index out of range"));
     for (int32_t i = 0; i < d->n_mats; i++) {
         const RtMaterial& m = d->mats[i];
-        if (m.type < RT_MAT_LAMBERTIAN || m.type > RT_MAT_BLACKBODY_LIGHT) return bail(fail(s, RT_ERR_INVALID, "unknown material type"));
+        if (m.type < RT_MAT_LAMBERTIAN || m.type > RT_MAT_PBR) return bail(fail(s, RT_ERR_INVALID, "unknown material type"));
+        if (m.type == RT_MAT_PBR) {
+            const float v[] = {m.albedo[0], m.albedo[1], m.albedo[2], m.roughness, m.metallic, m.anisotropy,
+                               m.anisotropy_angle, m.clearcoat, m.clearcoat_roughness, m.film_thickness, m.film_ior,
+                               m.sheen, m.sheen_tint, m.emission[0], m.emission[1], m.emission[2], m.emission_strength};
+            for (float x : v)
+                if (!std::isfinite(x)) return bail(fail(s, RT_ERR_INVALID, "non-finite PBR parameter"));
+            if (m.film_thickness > 0.0f && !(m.film_ior > 0.0f))
+                return bail(fail(s, RT_ERR_INVALID, "a PBR thin film needs a positive film_ior"));
+        }
         if (m.type == RT_MAT_SPECTRAL_METAL && m.metal == RT_METAL_CUSTOM && (m.nk_count < 2 || m.nk_count > RT_MAX_NK || !(m.nk_step > 0.0f)))
             return bail(fail(s, RT_ERR_INVALID, "custom conductor table needs 2..16 samples and a positive step"));
         if (m.type == RT_MAT_SPECTRAL_METAL && (m.metal < RT_METAL_GOLD || m.metal > RT_METAL_CUSTOM))
@@ -813,6 +857,7 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
 
     // ── materials (+ blackbody constants, material.rs:47-62) ─────────────────
     std::vector<DevMaterial> mats(std::max(d->n_mats, 1));
+    int n_pbr = 0;
     for (int32_t i = 0; i < d->n_mats; i++) {
         const RtMaterial& m = d->mats[i];
         DevMaterial& g = mats[i];
@@ -834,6 +879,20 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
                 g.nk_count = RT_METAL_NK_N; g.nk_start = RT_METAL_NK_START; g.nk_step = RT_METAL_NK_STEP;
                 for (int k = 0; k < RT_METAL_NK_N; k++) { g.nk_n[k] = RT_METAL_NK[m.metal][0][k]; g.nk_k[k] = RT_METAL_NK[m.metal][1][k]; }
             }
+        }
+        if (m.type == RT_MAT_PBR) {                                                 // material.rs:790-800
+            g.metallic = m.metallic;
+            g.aniso_c = std::cos(m.anisotropy_angle);
+            g.aniso_s = std::sin(m.anisotropy_angle);
+            g.aspect = std::sqrt(std::fmax(1.0f - 0.9f * std::fmin(std::fmax(m.anisotropy, 0.0f), 1.0f), 0.001f));
+            g.clearcoat = m.clearcoat;
+            g.clearcoat_roughness = m.clearcoat_roughness;
+            g.film_thickness = m.film_thickness;
+            g.film_ior = m.film_ior;
+            g.sheen = m.sheen;
+            g.sheen_tint = m.sheen_tint;
+            for (int c = 0; c < 3; c++) g.emission[c] = m.emission[c] * m.emission_strength;
+            n_pbr++;
         }
         if (m.type == RT_MAT_BLACKBODY_LIGHT) {
             std::vector<float> raw(nspec);
@@ -859,13 +918,15 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         }
     }
     if ((rc = upload(s, mats.data(), mats.size(), &s->S.mats))) return bail(rc);
+    s->S.n_pbr = n_pbr;
     s->S.n_mats = d->n_mats;
     std::vector<uint8_t> codes(mats.size(), 1);
     for (int32_t i = 0; i < d->n_mats; i++) {
         int t = d->mats[i].type;
         codes[i] = (t == RT_MAT_DIFFUSE_LIGHT || t == RT_MAT_BLACKBODY_LIGHT) ? 0
                  : t == RT_MAT_SPECTRAL_METAL ? 2
-                 : (t == RT_MAT_DIELECTRIC || t == RT_MAT_SPECTRAL_DIELECTRIC) ? 3 : 1;
+                 : (t == RT_MAT_DIELECTRIC || t == RT_MAT_SPECTRAL_DIELECTRIC) ? 3
+                 : t == RT_MAT_PBR ? 4 : 1;
     }
     if ((rc = upload(s, codes.data(), codes.size(), &s->S.mat_code))) return bail(rc);
 
@@ -937,6 +998,8 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
 
     std::call_once(g_elut_once, build_elut);
     if ((rc = upload(s, g_elut, (size_t)64 * 64, &s->S.elut))) return bail(rc);
+    std::call_once(g_nacre_once, build_nacre);
+    if ((rc = upload(s, g_nacre, (size_t)256, &s->S.nacre))) return bail(rc);
 
     // ── background + env alias table (renderer.rs:32-74) ────────────────────
     const RtBackground& bg = d->bg;
@@ -1311,7 +1374,9 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         rth::launch_shadow(s->S, T, W.sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, W.derr, s->sms, s->stream);
         mark(0);
         rth::launch_retire(s->S, B, W.Rt, R, c, hdr, blk(it + 2), cn + CTR_COUNT, s->sms, s->stream);
-        nl += 4 + CLS_N;
+        // extend, classify, shadow, retire, the shading classes other than media
+        // and PBR, and the PBR class when the scene has PBR materials
+        nl += 4 + (CLS_N - 2) + (s->S.n_pbr > 0 ? 1 : 0);
         uint32_t slot = (uint32_t)(it % STATUS_RING);
         CK(cudaMemcpyAsync(s->h_status + slot, cn + CTR_COUNT, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
         CK(cudaEventRecord(s->st_ev[slot], s->stream));

@@ -38,7 +38,7 @@ static_assert(CTR_HDR_WORDS + RT_CTR_RING * RT_CTR_STRIDE <= RT_CTR_WORDS, "coun
 static_assert(14 * RT_CTR_STRIDE <= RT_CTR_WORDS, "photon counter layout");
 
 // material classes shaded by separate kernels
-enum { CLS_MISS = 0, CLS_EMIT = 1, CLS_DIFFUSE = 2, CLS_METAL = 3, CLS_DIELEC = 4, CLS_MEDIUM = 5, CLS_N = 6 };
+enum { CLS_MISS = 0, CLS_EMIT = 1, CLS_DIFFUSE = 2, CLS_METAL = 3, CLS_DIELEC = 4, CLS_PBR = 5, CLS_MEDIUM = 6, CLS_N = 7 };
 struct ClassQueues { uint32_t* q[CLS_N]; };
 static_assert(CTR_CLS_COUNT + CLS_N <= CTR_GATHER_COUNT, "counter slots");
 

@@ -9,12 +9,11 @@
 
 namespace rtd {
 
-// A hit record of a medium event: type bits 29:28 = 3 (no primitive type), the
-// medium index in bits 27:0; RT_MISS_REF also has type 3 but all code bits set.
-#define RT_HIT_MEDIUM_BASE 0x30000000u
-// type 3 with class code 0: convex solids share type 3 but are never emissive,
-// so their code is non-zero
-RT_HD bool hit_is_medium(uint32_t ref) { return (ref >> 28) == 3u; }
+// A hit record of a medium event: class code 0 with type 3, the medium index
+// in the index bits.  Convex solids share type 3 but are never emissive, so
+// their code is non-zero; RT_MISS_REF has code 7.
+#define RT_HIT_MEDIUM_BASE (3u << 27)
+RT_HD bool hit_is_medium(uint32_t ref) { return (ref >> 27) == 3u; }
 
 // random stream keyed on the ray's bits (origin xyz, direction x, wavelength;
 // the reference seeds its medium RNG from these, volume.rs:114-120)

@@ -18,6 +18,7 @@
 
 #include "rt_internal.h"
 #include "rt_media.cuh"
+#include "rt_ggx.cuh"
 
 using namespace rtd;
 
@@ -123,31 +124,6 @@ RT_D float fresnel_cond(float ci, float n, float k) {
     float rp = rs * (t3 - t4) / fmaxf(t3 + t4, 1e-12f);
     return clampf_(0.5f * (rp + rs), 0.0f, 1.0f);
 }
-RT_D float smith_lam(float c, float alpha) {
-    float a2 = alpha * alpha, c2 = c * c;
-    return (sqrtf(a2 + (1.0f - a2) * c2) - c) / (2.0f * c);
-}
-RT_D float3 vndf(float3 wo, float al, float xi1, float xi2) {
-    float3 wh = unit3(mk(al * wo.x, al * wo.y, wo.z));
-    float len = sqrtf(wh.x * wh.x + wh.y * wh.y);
-    float3 t1 = len > 1e-6f ? mk(-wh.y / len, wh.x / len, 0.0f) : mk(1.0f, 0.0f, 0.0f);
-    float3 t2 = cross3(wh, t1);
-    float a = 1.0f / (1.0f + wh.z), r = sqrtf(xi1), p1, p2, sp, cp;
-    if (xi2 < a) { sincosf(xi2 / a * PI_F, &sp, &cp); p1 = r * cp; p2 = r * sp; }
-    else { sincosf(PI_F + (xi2 - a) / (1.0f - a) * PI_F, &sp, &cp); p1 = r * cp; p2 = r * sp * wh.z; }
-    float p3 = sqrtf(fmaxf(1.0f - p1 * p1 - p2 * p2, 0.0f));
-    float3 nh = t1 * p1 + t2 * p2 + wh * p3;
-    return unit3(mk(al * nh.x, al * nh.y, fmaxf(nh.z, 0.0f)));
-}
-RT_D float elut(const DevScene& S, float mu, float alpha) {
-    float x = clampf_(clampf_(mu, 0.0f, 1.0f) * 64.0f - 0.5f, 0.0f, 63.0f);
-    float y = clampf_(clampf_(alpha, 0.0f, 1.0f) * 64.0f - 0.5f, 0.0f, 63.0f);
-    int i0 = (int)x, j0 = (int)y, i1 = min(i0 + 1, 63), j1 = min(j0 + 1, 63);
-    float fx = x - (float)i0, fy = y - (float)j0;
-    return (__ldg(S.elut + i0 * 64 + j0) * (1.0f - fx) + __ldg(S.elut + i1 * 64 + j0) * fx) * (1.0f - fy) +
-           (__ldg(S.elut + i0 * 64 + j1) * (1.0f - fx) + __ldg(S.elut + i1 * 64 + j1) * fx) * fy;
-}
-
 // One bounce of trace_photon for every queued photon.
 __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const uint32_t* __restrict__ qin,
                                const uint32_t* cin, uint32_t* qout, uint32_t* cout, float4* st_pos, float4* st_pow,
@@ -221,6 +197,7 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                     nrm = mk(sn.x, sn.y, sn.z);
                 }
                 const DevMaterial& m = S.mats[mat];
+                bool store = false;
                 Rng rng = photon_rng(seed, gid);
                 uint32_t base = P_BOUNCE0 + bounce * P_PER_BOUNCE;
                 float3 udir = unit3(d);
@@ -260,7 +237,7 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                         else {
                             float3 up = fabsf(nrm.y) < 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
                             float3 tt = unit3(cross3(nrm, up)), bb = cross3(nrm, tt);
-                            float3 mts = vndf(mk(dot3(wo, tt), dot3(wo, bb), cos_o), alpha, rnd(rng, base + 0),
+                            float3 mts = vndf_sample(mk(dot3(wo, tt), dot3(wo, bb), cos_o), alpha, alpha, rnd(rng, base + 0),
                                               rnd(rng, base + 1));
                             float3 mm = unit3(tt * mts.x + bb * mts.y + nrm * mts.z);
                             float voh = fmaxf(dot3(wo, mm), 0.0f);
@@ -271,8 +248,8 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                         if (ok && dot3(nd, nrm) > 0.0f) {
                             float weight = 1.0f;
                             if (m.roughness != 0.0f) {
-                                float lo = smith_lam(cos_o, alpha), li = smith_lam(fmaxf(dot3(nd, nrm), 0.0f), alpha);
-                                weight = ((1.0f + lo) / (1.0f + lo + li)) * fminf(1.0f / fmaxf(elut(S, cos_o, alpha), 0.05f), 10.0f);
+                                float lo = smith_lambda(cos_o, alpha), li = smith_lambda(fmaxf(dot3(nd, nrm), 0.0f), alpha);
+                                weight = ((1.0f + lo) / (1.0f + lo + li)) * fminf(1.0f / fmaxf(e_ss_lut(S, cos_o, alpha), 0.05f), 10.0f);
                             }
                             float tn = clampf_((lam - m.nk_start) / m.nk_step, 0.0f, (float)(m.nk_count - 1));
                             int i = min((int)tn, m.nk_count - 2);
@@ -283,7 +260,21 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                             o = p; d = nd; spec_depth++; cont = true;
                         }
                     }
+                } else if (m.type == RT_MAT_PBR) {
+                    // PbrMaterial::scatter: a specular lobe carries the photon on, the
+                    // diffuse lobe stores it where can_receive_caustics (material.rs:1049)
+                    float3 att, nd;
+                    int lobe = pbr_scatter(S, m, unit3(-d), nrm, rnd(rng, base + 2), rnd(rng, base + 3),
+                                           rnd(rng, base + 0), rnd(rng, base + 1), &att, &nd);
+                    if (lobe == PBR_SPECULAR) {
+                        power = power * att;
+                        o = p; d = nd; spec_depth++; cont = true;
+                    }
+                    store = lobe == PBR_DIFFUSE && m.metallic < 0.999f;
                 } else if (m.type == RT_MAT_LAMBERTIAN || m.type == RT_MAT_CHECKER) {
+                    store = true;
+                }
+                if (store) {                                // photon.rs:260-271
                     if (spec_depth > 0) {
                         float lum = lum3(power);
                         if (lum > lum_clamp) power = power * (lum_clamp / lum);

@@ -11,6 +11,7 @@
 #include "rt_internal.h"
 #include "rt_media.cuh"
 #include "rt_sky.cuh"
+#include "rt_ggx.cuh"
 
 using namespace rtd;
 
@@ -82,48 +83,6 @@ RT_D float fresnel_dielectric(float ci, float eta) {
     float rp = (eta * ct - ci) / (eta * ct + ci);
     return (rs * rs + rp * rp) * 0.5f;
 }
-RT_D float smith_lambda(float c, float alpha) {
-    float a2 = alpha * alpha, c2 = c * c;
-    return (sqrtf(a2 + (1.0f - a2) * c2) - c) / (2.0f * c);
-}
-RT_D float smith_g1(float c, float alpha) {                                         // material.rs:163-167
-    float a2 = alpha * alpha, c2 = c * c;
-    return 2.0f * c / (c + sqrtf(a2 + (1.0f - a2) * c2));
-}
-RT_D float ggx_ndf(float cos_h, float alpha) {                                      // material.rs:308-312
-    float a2 = alpha * alpha;
-    float dd = 1.0f + cos_h * cos_h * (a2 - 1.0f);
-    return a2 / fmaxf(PI_F * dd * dd, 1e-12f);
-}
-RT_D float3 vndf_sample(float3 wo, float ax, float ay, float xi1, float xi2) {
-    float3 wh = unit3(mk(ax * wo.x, ay * wo.y, wo.z));
-    float len = sqrtf(wh.x * wh.x + wh.y * wh.y);
-    float3 t1 = len > 1e-6f ? mk(-wh.y / len, wh.x / len, 0.0f) : mk(1.0f, 0.0f, 0.0f);
-    float3 t2 = cross3(wh, t1);
-    float a = 1.0f / (1.0f + wh.z);
-    float r = sqrtf(xi1);
-    float p1, p2, sphi, cphi;
-    if (xi2 < a) {
-        sincosf(xi2 / a * PI_F, &sphi, &cphi);
-        p1 = r * cphi; p2 = r * sphi;
-    } else {
-        sincosf(PI_F + (xi2 - a) / (1.0f - a) * PI_F, &sphi, &cphi);
-        p1 = r * cphi; p2 = r * sphi * wh.z;
-    }
-    float p3 = sqrtf(fmaxf(1.0f - p1 * p1 - p2 * p2, 0.0f));
-    float3 nh = t1 * p1 + t2 * p2 + wh * p3;
-    return unit3(mk(ax * nh.x, ay * nh.y, fmaxf(nh.z, 0.0f)));
-}
-RT_D float e_ss_lut(const DevScene& S, float mu, float alpha) {
-    float x = clampf_(clampf_(mu, 0.0f, 1.0f) * 64.0f - 0.5f, 0.0f, 63.0f);
-    float y = clampf_(clampf_(alpha, 0.0f, 1.0f) * 64.0f - 0.5f, 0.0f, 63.0f);
-    int i0 = (int)x, j0 = (int)y, i1 = min(i0 + 1, 63), j1 = min(j0 + 1, 63);
-    float fx = x - (float)i0, fy = y - (float)j0;
-    float e00 = __ldg(S.elut + i0 * 64 + j0), e10 = __ldg(S.elut + i1 * 64 + j0);
-    float e01 = __ldg(S.elut + i0 * 64 + j1), e11 = __ldg(S.elut + i1 * 64 + j1);
-    return (e00 * (1.0f - fx) + e10 * fx) * (1.0f - fy) + (e01 * (1.0f - fx) + e11 * fx) * fy;
-}
-
 // ── environment (renderer.rs:84-179) ────────────────────────────────────────
 RT_D float3 env_unrot(const DevScene& S, float3 d) {
     return mk(d.x * S.env_cos_r - d.z * S.env_sin_r, d.y, d.x * S.env_sin_r + d.z * S.env_cos_r);
@@ -299,6 +258,7 @@ RT_D float3 spec_factor(const DevScene& S, int tint, float4 w, float lam0, int H
 }
 RT_D float3 emission(const DevScene& S, const DevMaterial& m, int tint, float4 w, float lam0, int H) {
     if (m.type == RT_MAT_DIFFUSE_LIGHT) return mk(m.albedo[0], m.albedo[1], m.albedo[2]) * spec_factor(S, tint, w, lam0, H);
+    if (m.type == RT_MAT_PBR) return mk(m.emission[0], m.emission[1], m.emission[2]) * spec_factor(S, tint, w, lam0, H);
     if (m.type == RT_MAT_BLACKBODY_LIGHT) {
         if (tint == TINT_NONE) return mk(m.bb_avg[0], m.bb_avg[1], m.bb_avg[2]) * spec_factor(S, tint, w, lam0, H);
         float ws[4] = {w.x, w.y, w.z, w.w};
@@ -682,7 +642,8 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                                                           const uint32_t* cin, uint32_t* cout,
                                                           float4* __restrict__ sq, uint32_t* ctr) {
     // queues appended to: [next set, retire records, gather requests, shadow rays]
-    constexpr int NQ = (CLS == CLS_DIFFUSE || CLS == CLS_METAL) ? 4 : (CLS == CLS_MISS || CLS == CLS_EMIT) ? 1 : 2;
+    constexpr int NQ = (CLS == CLS_DIFFUSE || CLS == CLS_METAL || CLS == CLS_PBR) ? 4
+                     : (CLS == CLS_MISS || CLS == CLS_EMIT) ? 1 : 2;
     __shared__ BlockQ<NQ, RT_SHADE_BLOCK / 32> shq;
     uint32_t* qctr[NQ];
     if constexpr (NQ == 1) {
@@ -869,99 +830,143 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         o = p; d = dir;
                         prev_spec = true; prev_mis = sun_w;
                     }
-                } else {                                                            // renderer.rs:457-572
+                } else {                                                            // renderer.rs:405-572
                     sf = spec_factor(S, tint, w, lam0, H);
-                    float3 att = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
-                    if (m.type == RT_MAT_CHECKER) {
-                        int xi = (int)floorf(m.checker_scale * p.x), yi = (int)floorf(m.checker_scale * p.y);
-                        int zi = (int)floorf(m.checker_scale * p.z);
-                        if ((xi + yi + zi) % 2 != 0) att = mk(m.odd[0], m.odd[1], m.odd[2]);
+                    float3 att, hint;       // the scatter attenuation and the caustic albedo hint
+                    bool diffuse = true;
+                    if constexpr (CLS == CLS_PBR) {
+                        // PbrMaterial: its emission adds at the hit (renderer.rs:415-417),
+                        // then one lobe scatters (material.rs:790-920)
+                        float emit_w = (prev_spec || !have_lights) ? 1.0f : prev_mis;
+                        Lc = Lc + T * (mk(m.emission[0], m.emission[1], m.emission[2]) * sf) * emit_w;
+                        float3 wo = unit3(-d), dir;
+                        int lobe = pbr_scatter(S, m, wo, nrm, rnd(rng, b + B_LOBE0), rnd(rng, b + B_LOBE1),
+                                               rnd(rng, b + B_SCATTER0), rnd(rng, b + B_SCATTER1), &att, &dir);
+                        hint = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
+                        if (lobe != PBR_DIFFUSE) diffuse = false;
+                        if (lobe == PBR_NONE) alive = false;
+                        if (lobe == PBR_SPECULAR) {
+                            // specular sun NEE (renderer.rs:421-456) with the PBR lobes'
+                            // specular_brdf_cos / specular_sampling_pdf
+                            float sun_w = 1.0f;
+                            if (SKY && S.has_sun) {
+                                float3 sun_s = sample_sun_cone(S.sun_dir, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1));
+                                float p_mat;
+                                float3 bc = pbr_spec_brdf_cos(S, m, wo, nrm, sun_s, &p_mat);
+                                if (bc.x > 0.0f || bc.y > 0.0f || bc.z > 0.0f) {
+                                    float mis_d = SUN_PDF * SUN_PDF + p_mat * p_mat;
+                                    if (mis_d > 0.0f) {
+                                        float3 c = T * bc * (preetham_sky(sun_s, S.sun_dir, S.turbidity) * sf) *
+                                                   SUN_PDF / mis_d;
+                                        np0 = make_float4(c.x, c.y, c.z, 0.f);
+                                        sh0 = true;
+                                        sh0a = make_float4(p.x, p.y, p.z, INFINITY);
+                                        sh0b = make_float4(sun_s.x, sun_s.y, sun_s.z, 0.f);
+                                    }
+                                }
+                                float p_b = pbr_spec_pdf(S, m, wo, nrm, dir);
+                                if (p_b > 0.0f) sun_w = (p_b * p_b) / fmaxf(p_b * p_b + SUN_PDF * SUN_PDF, 1e-8f);
+                            }
+                            T = T * att;
+                            o = p; d = dir;
+                            prev_spec = true; prev_mis = sun_w;
+                        }
+                    } else {
+                        att = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
+                        if (m.type == RT_MAT_CHECKER) {
+                            int xi = (int)floorf(m.checker_scale * p.x), yi = (int)floorf(m.checker_scale * p.y);
+                            int zi = (int)floorf(m.checker_scale * p.z);
+                            if ((xi + yi + zi) % 2 != 0) att = mk(m.odd[0], m.odd[1], m.odd[2]);
+                        }
+                        hint = att;
                     }
-                    if (R.photons) {
-                        // caustic injection: the gather kernel turns T·tint·albedo into × irradiance
-                        float3 f = T * sf * att;
-                        npc = make_float4(f.x, f.y, f.z, 0.f);
-                        gath = true;
-                        ga = make_float4(p.x, p.y, p.z, 0.f);
-                        gb = make_float4(nrm.x, nrm.y, nrm.z, 0.f);
-                    }
-                    if (have_lights) {
-                        uint32_t pick = rnd_u32(rng, b + B_LPICK) % (uint32_t)S.n_lights;
-                        float3 ldir = light_generate(S.lights[pick], p, rnd(rng, b + B_LPT0), rnd(rng, b + B_LPT1));
-                        LRec lr;
-                        if (lights_hit(S, p, ldir, &lr)) {
-                            float l_pdf = lights_pdf_value(S, p, ldir);
-                            float brdf = fmaxf(dot3(nrm, unit3(ldir)) / PI_F, 0.0f);
-                            float sun_p = SKY ? sun_pdf_value(S, ldir) : 0.0f;
-                            float env_p = env_dir_pdf(S, ldir);
-                            float mis_d = l_pdf * l_pdf + brdf * brdf + sun_p * sun_p + env_p * env_p;
-                            if (mis_d > 0.0f && brdf > 0.0f) {
-                                float3 nee = emission(S, S.mats[lr.mat], tint, w, lam0, H);
-                                float3 c = T * att * brdf * l_pdf * nee / mis_d;
-                                np0 = make_float4(c.x, c.y, c.z, 0.f);
-                                sh0 = true;
-                                sh0a = make_float4(p.x, p.y, p.z, lr.t * (1.0f - 1e-4f));
-                                sh0b = make_float4(ldir.x, ldir.y, ldir.z, 0.f);
+                    if (diffuse) {
+                        if (R.photons) {
+                            // caustic injection: the gather kernel turns T·tint·albedo into × irradiance
+                            float3 f = T * sf * hint;
+                            npc = make_float4(f.x, f.y, f.z, 0.f);
+                            gath = true;
+                            ga = make_float4(p.x, p.y, p.z, 0.f);
+                            gb = make_float4(nrm.x, nrm.y, nrm.z, 0.f);
+                        }
+                        if (have_lights) {
+                            uint32_t pick = rnd_u32(rng, b + B_LPICK) % (uint32_t)S.n_lights;
+                            float3 ldir = light_generate(S.lights[pick], p, rnd(rng, b + B_LPT0), rnd(rng, b + B_LPT1));
+                            LRec lr;
+                            if (lights_hit(S, p, ldir, &lr)) {
+                                float l_pdf = lights_pdf_value(S, p, ldir);
+                                float brdf = fmaxf(dot3(nrm, unit3(ldir)) / PI_F, 0.0f);
+                                float sun_p = SKY ? sun_pdf_value(S, ldir) : 0.0f;
+                                float env_p = env_dir_pdf(S, ldir);
+                                float mis_d = l_pdf * l_pdf + brdf * brdf + sun_p * sun_p + env_p * env_p;
+                                if (mis_d > 0.0f && brdf > 0.0f) {
+                                    float3 nee = emission(S, S.mats[lr.mat], tint, w, lam0, H);
+                                    float3 c = T * att * brdf * l_pdf * nee / mis_d;
+                                    np0 = make_float4(c.x, c.y, c.z, 0.f);
+                                    sh0 = true;
+                                    sh0a = make_float4(p.x, p.y, p.z, lr.t * (1.0f - 1e-4f));
+                                    sh0b = make_float4(ldir.x, ldir.y, ldir.z, 0.f);
+                                }
                             }
                         }
-                    }
-                    if (SKY && S.has_sun) {                                         // renderer.rs:495-518
-                        // the sun shares the env-NEE slot: a Physical sky has no env map
-                        float3 sun_s, c;
-                        if (sun_nee_diffuse(S, p, nrm, T * att, sf, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1),
-                                            &sun_s, &c)) {
-                            np1 = make_float4(c.x, c.y, c.z, 0.f);
-                            sh1 = true;
-                            sh1a = make_float4(p.x, p.y, p.z, INFINITY);
-                            sh1b = make_float4(sun_s.x, sun_s.y, sun_s.z, 0.f);
-                        }
-                    }
-                    if (S.has_env) {
-                        float epdf;
-                        float3 edir = env_sample_dir(S, rnd(rng, b + B_ENV_ROW), rnd(rng, b + B_ENV_COL),
-                                                     rnd(rng, b + B_ENV_JU), rnd(rng, b + B_ENV_JV), &epdf);
-                        if (epdf > 0.0f) {
-                            float brdf = fmaxf(dot3(nrm, unit3(edir)) / PI_F, 0.0f);
-                            if (brdf > 0.0f) {
-                                float area_pdf = have_lights ? lights_pdf_value(S, p, edir) : 0.0f;
-                                float3 ec = env_lookup(S, edir) * sf;
-                                float mis_d = epdf * epdf + brdf * brdf + area_pdf * area_pdf;
-                                float3 c = T * att * brdf * epdf * ec / mis_d;
+                        if (SKY && S.has_sun) {                                         // renderer.rs:495-518
+                            // the sun shares the env-NEE slot: a Physical sky has no env map
+                            float3 sun_s, c;
+                            if (sun_nee_diffuse(S, p, nrm, T * att, sf, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1),
+                                                &sun_s, &c)) {
                                 np1 = make_float4(c.x, c.y, c.z, 0.f);
                                 sh1 = true;
                                 sh1a = make_float4(p.x, p.y, p.z, INFINITY);
-                                sh1b = make_float4(edir.x, edir.y, edir.z, 0.f);
+                                sh1b = make_float4(sun_s.x, sun_s.y, sun_s.z, 0.f);
                             }
                         }
-                    }
-                    // cosine-weighted bounce (pdf.rs:12-41)
-                    float r1 = rnd(rng, b + B_COS0), r2 = rnd(rng, b + B_COS1);
-                    float sp_, cp_;
-                    sincosf(2.0f * PI_F * r1, &sp_, &cp_);
-                    float sq_ = sqrtf(r2);
-                    float3 wn = unit3(nrm);
-                    float3 hh = fabsf(wn.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
-                    float3 vv = unit3(cross3(wn, hh));
-                    float3 uu = cross3(wn, vv);
-                    float3 idir = (cp_ * sq_) * uu + (sp_ * sq_) * vv + sqrtf(1.0f - r2) * wn;
-                    float3 iu = unit3(idir);
-                    float pdf_val = fmaxf(dot3(iu, wn) / PI_F, 0.0f);
-                    float scat = fmaxf(dot3(nrm, iu) / PI_F, 0.0f);
-                    if (pdf_val <= 0.0f || scat <= 0.0f || dot3(idir, nrm) <= 0.0f) {
-                        alive = false;
-                    } else {
-                        float area = have_lights ? lights_pdf_value(S, p, idir) : 0.0f;
-                        float sun = SKY ? sun_pdf_value(S, idir) : 0.0f;
-                        float env = env_dir_pdf(S, idir);
-                        prev_mis = (pdf_val * pdf_val) / fmaxf(pdf_val * pdf_val + (area * area + sun * sun + env * env), 1e-8f);
-                        T = T * (att * (scat / pdf_val));
-                        o = p; d = idir;
-                        prev_spec = false;
-                    }
+                        if (S.has_env) {
+                            float epdf;
+                            float3 edir = env_sample_dir(S, rnd(rng, b + B_ENV_ROW), rnd(rng, b + B_ENV_COL),
+                                                         rnd(rng, b + B_ENV_JU), rnd(rng, b + B_ENV_JV), &epdf);
+                            if (epdf > 0.0f) {
+                                float brdf = fmaxf(dot3(nrm, unit3(edir)) / PI_F, 0.0f);
+                                if (brdf > 0.0f) {
+                                    float area_pdf = have_lights ? lights_pdf_value(S, p, edir) : 0.0f;
+                                    float3 ec = env_lookup(S, edir) * sf;
+                                    float mis_d = epdf * epdf + brdf * brdf + area_pdf * area_pdf;
+                                    float3 c = T * att * brdf * epdf * ec / mis_d;
+                                    np1 = make_float4(c.x, c.y, c.z, 0.f);
+                                    sh1 = true;
+                                    sh1a = make_float4(p.x, p.y, p.z, INFINITY);
+                                    sh1b = make_float4(edir.x, edir.y, edir.z, 0.f);
+                                }
+                            }
+                        }
+                        // cosine-weighted bounce (pdf.rs:12-41)
+                        float r1 = rnd(rng, b + B_COS0), r2 = rnd(rng, b + B_COS1);
+                        float sp_, cp_;
+                        sincosf(2.0f * PI_F * r1, &sp_, &cp_);
+                        float sq_ = sqrtf(r2);
+                        float3 wn = unit3(nrm);
+                        float3 hh = fabsf(wn.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+                        float3 vv = unit3(cross3(wn, hh));
+                        float3 uu = cross3(wn, vv);
+                        float3 idir = (cp_ * sq_) * uu + (sp_ * sq_) * vv + sqrtf(1.0f - r2) * wn;
+                        float3 iu = unit3(idir);
+                        float pdf_val = fmaxf(dot3(iu, wn) / PI_F, 0.0f);
+                        float scat = fmaxf(dot3(nrm, iu) / PI_F, 0.0f);
+                        if (pdf_val <= 0.0f || scat <= 0.0f || dot3(idir, nrm) <= 0.0f) {
+                            alive = false;
+                        } else {
+                            float area = have_lights ? lights_pdf_value(S, p, idir) : 0.0f;
+                            float sun = SKY ? sun_pdf_value(S, idir) : 0.0f;
+                            float env = env_dir_pdf(S, idir);
+                            prev_mis = (pdf_val * pdf_val) / fmaxf(pdf_val * pdf_val + (area * area + sun * sun + env * env), 1e-8f);
+                            T = T * (att * (scat / pdf_val));
+                            o = p; d = idir;
+                            prev_spec = false;
+                        }
+                    }   // diffuse
                 }
                 }   // surface
                 if (alive && depth >= 2) {                                          // renderer.rs:574-579
-                    float3 eff = T * (CLS == CLS_DIFFUSE ? sf : spec_factor(S, tint, w, lam0, H));
+                    float3 eff = T * ((CLS == CLS_DIFFUSE || CLS == CLS_PBR) ? sf : spec_factor(S, tint, w, lam0, H));
                     float survive = fmaxf(fmaxf(eff.x, eff.y), eff.z);
                     float pr = fminf(survive, 1.0f);
                     if (survive <= 0.0f || rnd(rng, b + B_RR) >= pr) alive = false;
@@ -1067,6 +1072,7 @@ void launch_shade(const DevScene& S, const PathState& A, const PathState& B, con
     RT_SHADE_CLASS(CLS_DIFFUSE);
     RT_SHADE_CLASS(CLS_METAL);
     RT_SHADE_CLASS(CLS_DIELEC);
+    if (S.n_pbr > 0) { RT_SHADE_CLASS(CLS_PBR); }
     if (S.n_media > 0) { RT_SHADE_CLASS(CLS_MEDIUM); }
 #undef RT_SHADE_CLASS
 }

@@ -413,8 +413,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
                 active = false;
                 bool hit = best.ref != RT_MISS_REF;
                 if (MODE == 0) {
-                    uint32_t href = hit ? (best.ref & 0x3FFFFFFFu) | ((uint32_t)__ldg(S.mat_code + best.mat) << 30)
-                                        : RT_MISS_REF;
+                    uint32_t href = hit ? RT_HIT_MAKE(best.ref, __ldg(S.mat_code + best.mat)) : RT_MISS_REF;
                     P.hit[pid] = make_float4(__uint_as_float(href), best.t, best.b1, best.b2);
                 } else {
                     out[item] = make_int4(hit ? (int)best.gid : -1, __float_as_int(hit ? best.t : 0.0f),

@@ -112,6 +112,28 @@ class Material:
         m.intensity = float(intensity)
         return m
 
+    @staticmethod
+    def pbr(albedo=(0.8, 0.8, 0.8), roughness=0.5, metallic=0.0, anisotropy=0.0, anisotropy_angle=0.0,
+            clearcoat=0.0, clearcoat_roughness=0.03, film_thickness=0.0, film_ior=1.5, sheen=0.0, sheen_tint=0.5,
+            emission=(0.0, 0.0, 0.0), emission_strength=0.0):
+        """PbrMaterial with scalar parameters (material.rs:680-1050); the
+        defaults are PbrMaterial::default and the TOML `pbr` defaults."""
+        m = Material._new(abi.RT_MAT_PBR)
+        m.albedo = _f3(albedo)
+        m.roughness = float(roughness)
+        m.metallic = float(metallic)
+        m.anisotropy = float(anisotropy)
+        m.anisotropy_angle = float(anisotropy_angle)
+        m.clearcoat = float(clearcoat)
+        m.clearcoat_roughness = float(clearcoat_roughness)
+        m.film_thickness = float(film_thickness)
+        m.film_ior = float(film_ior)
+        m.sheen = float(sheen)
+        m.sheen_tint = float(sheen_tint)
+        m.emission = _f3(emission)
+        m.emission_strength = float(emission_strength)
+        return m
+
 
 def _euler_fwd(angles_deg):
     """Rotate::euler (transform.rs:204-213): fwd = Ry · Rx · Rz, degrees."""
@@ -586,6 +608,12 @@ def _material_from_toml(m, base):
         return Material.spectral_metal(m.get("variant", "gold"), m.get("roughness", 0.0))
     if t == "diffuse_light":
         return Material.diffuse_light(m["color"])
+    if t == "pbr":                                                   # scene_file.rs:380-406, 1179-1187
+        return Material.pbr(m["albedo"], m.get("roughness", 0.5), m.get("metallic", 0.0), m.get("anisotropy", 0.0),
+                            m.get("anisotropy_angle", 0.0), m.get("clearcoat", 0.0),
+                            m.get("clearcoat_roughness", 0.03), m.get("film_thickness", 0.0),
+                            m.get("film_ior", 1.5), m.get("sheen", 0.0), m.get("sheen_tint", 0.5),
+                            m.get("emission", (0.0, 0.0, 0.0)), m.get("emission_strength", 0.0))
     raise ValueError(f"material type '{t}' is not supported by the GPU path")
 
 
@@ -1097,7 +1125,11 @@ def scene_from_toml_dict(doc, base="."):
         mat = sb.add_material(_material_from_toml(obj["material"], base))
         xf = Transform(obj.get("scale"), obj.get("rotate"), obj.get("rotate_y"), obj.get("spin"), obj.get("translate"))
         st = sh["type"]
-        emissive = obj["material"]["type"] == "diffuse_light" and any(c > 0 for c in obj["material"]["color"])
+        mt = obj["material"]
+        # light_area > 0 for an emissive material (quad.rs:98-100, PbrMaterial::is_emissive)
+        emissive = (mt["type"] == "diffuse_light" and any(c > 0 for c in mt["color"])) or \
+            (mt["type"] == "pbr" and mt.get("emission_strength", 0.0) > 0 and
+             float(np.dot(mt.get("emission", (0, 0, 0)), (0.2126, 0.7152, 0.0722))) > 0)
         if st == "sphere":
             si = sb.add_sphere(sh["center"], sh["radius"], mat, xf)
             if emissive:
