@@ -299,6 +299,28 @@ int32_t rt_render_accumulate(RtScene* scene, const RtCamera* cam, const RtPassPa
                              float firefly_floor, int32_t reset,
                              float* out_sum, float* out_m2, uint32_t* out_count, int32_t mem);
 
+/* ── output (src/output.rs, src/main.rs:571-583) ─────────────────────────── */
+#define RT_TONEMAP_AGX   0   /* Blender AgX with the "Punchy" look (output.rs:34-80), the default */
+#define RT_TONEMAP_ACES  1   /* Narkowicz ACES fit in AP1 (output.rs:7-31) */
+
+typedef struct RtDevelopParams {
+    uint32_t width, height;
+    float    exposure;       /* linear multiplier (default 1) */
+    int32_t  tonemapper;     /* RT_TONEMAP_* */
+    float    vignette;       /* 0 .. 1: corners × (1 − vignette) */
+    float    distortion;     /* 0 .. 1: barrel coefficient k */
+} RtDevelopParams;
+
+/* Develop linear radiance into 8-bit sRGB, replacing apply_optics + save_png's
+ * tone_map (output.rs:84-190): optics in linear light (vignette, barrel
+ * distortion with bilinear resampling), exposure, AgX or ACES, the sRGB
+ * curve and the quantisation (x.clamp(0, 0.999)·256 truncated).  linear_rgb
+ * (height × width × 3 per-sample means, row 0 = top) may be NULL: the scene's
+ * accumulators are developed (sum / max(count, 1), main.rs:571-583).
+ * rgb8 receives height × width × 3 bytes.  mem applies to both buffers. */
+int32_t rt_develop(RtScene* scene, const float* linear_rgb, const RtDevelopParams* params, uint8_t* rgb8,
+                   int32_t mem);
+
 /* ── caustic photon map (src/photon.rs, src/scene.rs:35-74) ──────────────── */
 #define RT_EMIT_DISK     0   /* directional disk facing `dir` (PhotonMap::build, photon.rs:41-94) */
 #define RT_EMIT_QUAD     1   /* cosine-weighted quad (PhotonMap::build_from_quad, photon.rs:97-135) */

@@ -31,6 +31,8 @@ def lib():
         L.orc_last_error.restype = C.c_char_p
         L.orc_scene_create.argtypes = [C.POINTER(abi.RtSceneDesc), C.POINTER(vp)]
         L.orc_scene_destroy.argtypes = [vp]
+        L.orc_develop.argtypes = [fp, fp, C.POINTER(C.c_uint32), C.POINTER(abi.RtDevelopParams), C.POINTER(C.c_uint8)]
+        L.orc_apply_optics.argtypes = [fp, C.c_uint32, C.c_uint32, C.c_float, C.c_float, fp]
         L.orc_pbr_scatter.argtypes = [C.POINTER(abi.RtMaterial), fp, i64, C.POINTER(i32), fp, fp, fp, fp, fp]
         L.orc_bvh_export.argtypes = [vp, fp, C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]
         L.orc_trace_closest.argtypes = [vp, fp, i64, C.POINTER(abi.RtHit), i32, i32]
@@ -131,6 +133,27 @@ def pbr_scatter(mat, wo, n, xi, spec_wi=None):
     lib().orc_pbr_scatter(C.byref(mat), _fp(a), k, lobe.ctypes.data_as(C.POINTER(C.c_int32)), _fp(att), _fp(d),
                           None if swi is None else _fp(swi), _fp(bc), _fp(pdf))
     return lobe, att, d, bc, pdf
+
+
+def develop(params, linear=None, sum_=None, count=None):
+    """apply_optics + tone_map (output.rs:84-190): a linear (H, W, 3) image of
+    per-sample means, or accumulators sum (H, W, 3) / max(count, 1)."""
+    h, w = params.height, params.width
+    out = np.zeros((h, w, 3), np.uint8)
+    lp = None if linear is None else _fp(np.ascontiguousarray(linear, np.float32))
+    sp = None if sum_ is None else _fp(np.ascontiguousarray(sum_, np.float32))
+    cp = None if count is None else np.ascontiguousarray(count, np.uint32).ctypes.data_as(C.POINTER(C.c_uint32))
+    lib().orc_develop(lp, sp, cp, C.byref(params), out.ctypes.data_as(C.POINTER(C.c_uint8)))
+    return out
+
+
+def apply_optics(img, vignette, distortion):
+    """apply_optics (output.rs:159-190) on a linear (H, W, 3) image."""
+    img = np.ascontiguousarray(img, np.float32)
+    h, w = img.shape[:2]
+    out = np.zeros_like(img)
+    lib().orc_apply_optics(_fp(img), w, h, float(vignette), float(distortion), _fp(out))
+    return out
 
 
 def hg_sample(w, g, xi1, xi2):

@@ -2485,6 +2485,106 @@ int32_t orc_pbr_scatter(const RtMaterial* m, const float* in, int64_t n, int32_t
     return RT_OK;
 }
 
+// ── output (output.rs:7-190, main.rs:571-583) ──────────────────────────────
+static inline float aces_curve(float x) {                                          // output.rs:12-15
+    x = rmax(x, 0.0f);
+    return (x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f);
+}
+static V3 aces_tonemap(V3 c) {                                                     // output.rs:17-31
+    float r = aces_curve(c.x * 0.59719f + c.y * 0.35458f + c.z * 0.04823f);
+    float g = aces_curve(c.x * 0.07600f + c.y * 0.90834f + c.z * 0.01566f);
+    float b = aces_curve(c.x * 0.02840f + c.y * 0.13383f + c.z * 0.83777f);
+    return v3(r * 1.60475f + g * -0.53108f + b * -0.07367f, r * -0.10208f + g * 1.10813f + b * -0.00605f,
+              r * -0.00327f + g * -0.07276f + b * 1.07602f);
+}
+static inline float agx_curve(float x) {                                           // output.rs:39-43
+    float x2 = x * x, x4 = x2 * x2;
+    return 15.5f * x4 * x2 - 40.14f * x4 * x + 31.96f * x4 - 6.868f * x2 * x + 0.4298f * x2 + 0.1191f * x - 0.00232f;
+}
+static V3 agx_tonemap(V3 c) {                                                      // output.rs:45-80
+    float in[3] = {c.x * 0.842479062253094f + c.y * 0.0784335999999992f + c.z * 0.0792237451477643f,
+                   c.x * 0.0423282422610123f + c.y * 0.878468636469772f + c.z * 0.0791661274605434f,
+                   c.x * 0.0423756549057051f + c.y * 0.0784336f + c.z * 0.879142973793104f};
+    float k[3];
+    for (int i = 0; i < 3; i++) {
+        float e = (std::log2(rmax(in[i], 1e-10f)) - -12.47393f) / 16.5f;
+        k[i] = agx_curve(rmin(rmax(e, 0.0f), 1.0f));
+    }
+    float luma = luminance(v3(k[0], k[1], k[2]));
+    for (int i = 0; i < 3; i++) k[i] = luma + 1.4f * (std::pow(k[i], 1.35f) - luma);
+    return v3(k[0] * 1.19687900512017f + k[1] * -0.0980208811401368f + k[2] * -0.0990297440797205f,
+              k[0] * -0.0528968517574562f + k[1] * 1.15190312990417f + k[2] * -0.0989611768448433f,
+              k[0] * -0.0529716355144234f + k[1] * -0.0980434501171241f + k[2] * 1.15107567775604f);
+}
+static inline uint8_t encode8(float x) {                                           // output.rs:84-86, 104
+    x = rmax(x, 0.0f);
+    float e = x <= 0.0031308f ? 12.92f * x : 1.055f * std::pow(x, 1.0f / 2.4f) - 0.055f;
+    return (uint8_t)(rmin(rmax(e, 0.0f), 0.999f) * 256.0f);
+}
+// apply_optics + tone_map over an image: `lin` per-sample means, or sum / max(count, 1)
+int32_t orc_develop(const float* lin, const float* sum, const uint32_t* cnt, const RtDevelopParams* p,
+                    uint8_t* out) {
+    uint32_t w = p->width, h = p->height;
+    auto fetch = [&](size_t i) {
+        if (lin) return v3(lin[i * 3], lin[i * 3 + 1], lin[i * 3 + 2]);
+        float n = (float)std::max<uint32_t>(cnt[i], 1u);
+        return v3(sum[i * 3] / n, sum[i * 3 + 1] / n, sum[i * 3 + 2] / n);
+    };
+    float cx = ((float)w - 1.0f) * 0.5f, cy = ((float)h - 1.0f) * 0.5f;
+    float rcorner = rmax(std::sqrt(cx * cx + cy * cy), 1e-6f);
+    for (uint32_t y = 0; y < h; y++)
+        for (uint32_t x = 0; x < w; x++) {
+            size_t i = (size_t)y * w + x;
+            V3 c;
+            if (p->vignette == 0.0f && p->distortion == 0.0f) {
+                c = fetch(i);
+            } else {                                                                // output.rs:159-190
+                float dx = ((float)x - cx) / rcorner, dy = ((float)y - cy) / rcorner;
+                float r2 = dx * dx + dy * dy;
+                float s = 1.0f - p->distortion * r2;
+                float sx = rmin(rmax(cx + dx * rcorner * s, 0.0f), (float)w - 1.0f);
+                float sy = rmin(rmax(cy + dy * rcorner * s, 0.0f), (float)h - 1.0f);
+                size_t x0 = (size_t)sx, y0 = (size_t)sy;
+                size_t x1 = std::min<size_t>(x0 + 1, w - 1), y1 = std::min<size_t>(y0 + 1, h - 1);
+                float fx = sx - (float)x0, fy = sy - (float)y0;
+                V3 c00 = fetch(y0 * w + x0), c10 = fetch(y0 * w + x1), c01 = fetch(y1 * w + x0), c11 = fetch(y1 * w + x1);
+                c = (c00 * (1.0f - fx) + c10 * fx) * (1.0f - fy) + (c01 * (1.0f - fx) + c11 * fx) * fy;
+                c = c * rmax(1.0f - p->vignette * r2, 0.0f);
+            }
+            c = c * p->exposure;
+            V3 m = p->tonemapper == RT_TONEMAP_ACES ? aces_tonemap(c) : agx_tonemap(c);
+            out[i * 3] = encode8(m.x);
+            out[i * 3 + 1] = encode8(m.y);
+            out[i * 3 + 2] = encode8(m.z);
+        }
+    return RT_OK;
+}
+// apply_optics alone (output.rs:159-190) on a linear image, for its tests
+int32_t orc_apply_optics(const float* img, uint32_t w, uint32_t h, float vignette, float distortion, float* out) {
+    float cx = ((float)w - 1.0f) * 0.5f, cy = ((float)h - 1.0f) * 0.5f;
+    float rcorner = rmax(std::sqrt(cx * cx + cy * cy), 1e-6f);
+    auto at = [&](size_t i) { return v3(img[i * 3], img[i * 3 + 1], img[i * 3 + 2]); };
+    for (uint32_t y = 0; y < h; y++)
+        for (uint32_t x = 0; x < w; x++) {
+            size_t i = (size_t)y * w + x;
+            V3 c = at(i);
+            if (vignette != 0.0f || distortion != 0.0f) {
+                float dx = ((float)x - cx) / rcorner, dy = ((float)y - cy) / rcorner;
+                float r2 = dx * dx + dy * dy, s = 1.0f - distortion * r2;
+                float sx = rmin(rmax(cx + dx * rcorner * s, 0.0f), (float)w - 1.0f);
+                float sy = rmin(rmax(cy + dy * rcorner * s, 0.0f), (float)h - 1.0f);
+                size_t x0 = (size_t)sx, y0 = (size_t)sy;
+                size_t x1 = std::min<size_t>(x0 + 1, w - 1), y1 = std::min<size_t>(y0 + 1, h - 1);
+                float fx = sx - (float)x0, fy = sy - (float)y0;
+                c = (at(y0 * w + x0) * (1.0f - fx) + at(y0 * w + x1) * fx) * (1.0f - fy) +
+                    (at(y1 * w + x0) * (1.0f - fx) + at(y1 * w + x1) * fx) * fy;
+                c = c * rmax(1.0f - vignette * r2, 0.0f);
+            }
+            out[i * 3] = c.x; out[i * 3 + 1] = c.y; out[i * 3 + 2] = c.z;
+        }
+    return RT_OK;
+}
+
 // Per-ray traversal counters for the algorithmic-bytes roofline:
 // out[i*4 + {0,1,2,3}] = nodes visited, triangle, sphere, quad tests.
 int32_t orc_trace_stats(void* sp, const float* rays, int64_t n, int64_t* out, int32_t threads) {

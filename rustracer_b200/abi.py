@@ -152,6 +152,21 @@ class RtCamera(C.Structure):
     ]
 
 
+RT_TONEMAP_AGX = 0
+RT_TONEMAP_ACES = 1
+
+
+class RtDevelopParams(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("exposure", C.c_float),
+        ("tonemapper", C.c_int32),
+        ("vignette", C.c_float),
+        ("distortion", C.c_float),
+    ]
+
+
 class RtPassParams(C.Structure):
     _fields_ = [
         ("width", C.c_uint32),

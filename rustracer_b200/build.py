@@ -23,6 +23,7 @@ UNITS = [
     ("rt_trace.cu", ["--fmad=false"]),
     ("rt_shade.cu", []),
     ("rt_photon.cu", []),
+    ("rt_output.cu", ["--fmad=false"]),
     ("rt_host.cu", []),
 ]
 

@@ -1565,6 +1565,38 @@ extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const R
     return check_err(s);
 }
 
+extern "C" int32_t rt_develop(RtScene* s, const float* lin, const RtDevelopParams* p, uint8_t* rgb8, int32_t mem) {
+    if (!s || !p || !rgb8) return RT_ERR_INVALID;
+    if (mem != RT_MEM_HOST && mem != RT_MEM_DEVICE) return fail(s, RT_ERR_INVALID, "mem must be RT_MEM_HOST or RT_MEM_DEVICE");
+    if (p->width == 0 || p->height == 0 || (uint64_t)p->width * p->height > (1ull << 31))
+        return fail(s, RT_ERR_INVALID, "develop: bad image size");
+    if (p->tonemapper != RT_TONEMAP_AGX && p->tonemapper != RT_TONEMAP_ACES)
+        return fail(s, RT_ERR_INVALID, "develop: unknown tone mapper");
+    if (!(p->vignette >= 0.0f && p->vignette <= 1.0f) || !(p->distortion >= 0.0f && p->distortion <= 1.0f) ||
+        !std::isfinite(p->exposure))
+        return fail(s, RT_ERR_INVALID, "develop: vignette and distortion in [0, 1], a finite exposure");
+    uint32_t npix = p->width * p->height;
+    if (!lin && s->acc_npix != npix) return fail(s, RT_ERR_INVALID, "develop: no accumulators of this size");
+    CK(cudaSetDevice(s->device));
+    size_t in_bytes = lin && mem == RT_MEM_HOST ? (size_t)npix * 12 : 0;
+    size_t out_bytes = mem == RT_MEM_HOST ? ((size_t)npix * 3 + 15) / 16 * 16 : 0;
+    int rc = ensure_stage(s, in_bytes + out_bytes);
+    if (rc) return rc;
+    const float* d_lin = lin;
+    uint8_t* d_out = rgb8;
+    if (in_bytes) {
+        CK(cudaMemcpyAsync(s->stage, lin, in_bytes, cudaMemcpyHostToDevice, s->stream));
+        d_lin = (const float*)s->stage;
+    }
+    if (out_bytes) d_out = (uint8_t*)s->stage + in_bytes;
+    rth::launch_develop(d_lin, s->acc, s->cnt, p->width, p->height, p->exposure, p->tonemapper, p->vignette,
+                        p->distortion, d_out, s->sms, s->stream);
+    CK(cudaGetLastError());
+    if (out_bytes) CK(cudaMemcpyAsync(rgb8, d_out, (size_t)npix * 3, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return RT_OK;
+}
+
 extern "C" int32_t rt_last_render_stats(const RtScene* s, double* ms, int64_t* ext, int64_t* sh, int64_t* launches) {
     if (!s) return RT_ERR_INVALID;
     if (ms) *ms = s->last_ms;

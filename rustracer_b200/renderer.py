@@ -48,6 +48,7 @@ def lib():
         L.rt_render_pass.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), vp, vp, i32]
         L.rt_render_accumulate.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), f, u32, f, i32,
                                            vp, vp, vp, i32]
+        L.rt_develop.argtypes = [vp, vp, C.POINTER(abi.RtDevelopParams), vp, i32]
         L.rt_last_render_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
         L.rt_render_pass_noalloc.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), vp]
         L.rt_photon_build.argtypes = [vp, C.POINTER(abi.RtPhotonParams), C.POINTER(i64)]
@@ -83,6 +84,17 @@ def _ptr(a):
     except ImportError:
         pass
     raise TypeError("expected a numpy array or a torch tensor")
+
+
+def develop_params(width, height, exposure=1.0, tonemapper="agx", vignette=0.0, distortion=0.0):
+    """RtDevelopParams; tonemapper "agx" (the reference's default) or "aces"."""
+    tm = {"agx": abi.RT_TONEMAP_AGX, "aces": abi.RT_TONEMAP_ACES}
+    if tonemapper not in tm:
+        raise ValueError(f"unknown tonemapper '{tonemapper}' (agx or aces)")
+    p = abi.RtDevelopParams()
+    p.width, p.height, p.exposure, p.tonemapper = int(width), int(height), float(exposure), tm[tonemapper]
+    p.vignette, p.distortion = float(vignette), float(distortion)
+    return p
 
 
 def pass_params(width, height, sample_idx=0, n_samples=1, strata=None, max_depth=50, hero=1, bg_scale=1.0,
@@ -236,6 +248,28 @@ class GpuScene:
                                                int(firefly_min_samples), float(firefly_floor), 1 if reset else 0,
                                                sp, mp, cp, mem))
         return s, m, c
+
+    def develop(self, width, height, linear=None, exposure=1.0, tonemapper="agx", vignette=0.0, distortion=0.0,
+                out=None):
+        """apply_optics + tone_map (output.rs:84-190) on the device: the scene's
+        accumulators (linear=None) or a linear (H, W, 3) image → uint8 (H, W, 3)."""
+        p = develop_params(width, height, exposure, tonemapper, vignette, distortion)
+        if linear is not None and isinstance(linear, np.ndarray):
+            linear = np.ascontiguousarray(linear, np.float32)
+        if out is None:
+            if linear is not None and not isinstance(linear, np.ndarray):
+                import torch
+                out = torch.empty((height, width, 3), dtype=torch.uint8, device=linear.device)
+            else:
+                out = np.zeros((height, width, 3), np.uint8)
+        op, mem = _ptr(out)
+        lp = None
+        if linear is not None:
+            lp, lmem = _ptr(linear)
+            if lmem != mem:
+                raise ValueError("linear and out must both be host arrays or both device tensors")
+        self._check(lib().rt_develop(self.h, lp, C.byref(p), op, mem))
+        return out
 
     def last_stats(self):
         ms, e, s, l = C.c_double(), C.c_int64(), C.c_int64(), C.c_int64()
