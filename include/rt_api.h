@@ -181,6 +181,34 @@ typedef struct RtConvex {
     float   translate[3];
 } RtConvex;
 
+/* ── other analytic shapes (cylinder.rs, cone.rs, disk.rs, plane.rs) ─────────
+ * In object space: the cylinder and the cone stand on the y axis with their
+ * base centre at `center` (cylinder: closed caps at y = 0 and height; cone: a
+ * base disk at y = 0 and the apex at height); the disk and the infinite plane
+ * (with its optional two-sine wave bump of the shading normal) are given by
+ * a point and a normal.  The placement is the objects' SRT wrapper
+ * (scene_file.rs:1036-1042): x_world = rot·(scale·x) + translate.  Canonical
+ * ids follow the convex solids.  Shapes are not NEE lights; an infinite
+ * plane is bounded by the reference's ±1e5 proxy box and stays out of the
+ * photon-emitter bounds. */
+#define RT_SHAPE_CYLINDER 0
+#define RT_SHAPE_CONE     1
+#define RT_SHAPE_DISK     2
+#define RT_SHAPE_PLANE    3
+typedef struct RtShape {
+    int32_t type;               /* RT_SHAPE_* */
+    int32_t mat;
+    float   center[3];          /* base centre (cylinder, cone), centre (disk), point (plane) */
+    float   normal[3];          /* disk / plane normal, any length > 0 */
+    float   radius;             /* cylinder, cone, disk */
+    float   height;             /* cylinder, cone */
+    float   wave_amplitude;     /* plane: 0 = flat */
+    float   wave_scale;
+    float   scale;              /* > 0 */
+    float   rot[9];             /* row-major rotation */
+    float   translate[3];
+} RtShape;
+
 typedef struct RtSceneDesc {
     int64_t        n_tris;
     const float*   tri_v;         /* n_tris × 9  : v0, v1, v2 */
@@ -210,6 +238,9 @@ typedef struct RtSceneDesc {
     int64_t        n_convex;
     const RtConvex* convex;
     const float*   convex_planes;  /* planes × 4: outward unit normal xyz, offset d (object space) */
+    /* cylinders, cones, disks, infinite planes (may be 0 / NULL); ids follow the convex solids */
+    int64_t        n_shapes;
+    const RtShape* shapes;
 } RtSceneDesc;
 
 /* ── camera (src/camera.rs:24-59) ────────────────────────────────────────── */

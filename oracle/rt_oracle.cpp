@@ -577,6 +577,19 @@ struct Scene {
     std::vector<Convex> convex;
     std::vector<float> convex_planes;   // 4 floats per world plane
     std::vector<V3> convex_shade;       // per world plane: front-face and back-face shading normal
+    // cylinders, cones, disks, infinite planes (cylinder.rs, cone.rs, disk.rs, plane.rs) in
+    // object space with the objects' SRT placement; ids follow the convex solids
+    struct Shape {
+        int32_t type, mat;
+        V3 c, n, u, v;          // centre / point; unit normal and its onb (disk, plane)
+        float radius, height, wave_a, wave_s;
+        bool placed;            // a non-identity placement
+        float R[9], inv_scale;
+        V3 t;
+        Aabb box;
+    };
+    int64_t n_shapes = 0;
+    std::vector<Shape> shapes;
     // caustic photon map (photon.rs:31-36): implicit kd-tree, kept in emission order too
     struct KdPhoton { float pos[3], power[3], nor[3]; uint8_t axis; int32_t idx; };
     std::vector<KdPhoton> photons;    // kd order
@@ -590,12 +603,17 @@ struct Scene {
 };
 
 static inline bool is_emissive_type(int t) { return t == RT_MAT_DIFFUSE_LIGHT || t == RT_MAT_BLACKBODY_LIGHT; }
+static const int PRIM_SHAPE = 4;   // oracle-internal type of the other analytic shapes
 static inline int prim_type(const Scene& s, int64_t gid) {
     if (gid < s.n_tris) return RT_PRIM_TRI;
     if (gid < s.n_tris + s.n_quads) return RT_PRIM_QUAD;
-    return gid < s.n_tris + s.n_quads + s.n_spheres ? RT_PRIM_SPHERE : RT_PRIM_CONVEX;
+    if (gid < s.n_tris + s.n_quads + s.n_spheres) return RT_PRIM_SPHERE;
+    return gid < s.n_tris + s.n_quads + s.n_spheres + s.n_convex ? RT_PRIM_CONVEX : PRIM_SHAPE;
 }
-static inline int64_t n_prims(const Scene& s) { return s.n_tris + s.n_quads + s.n_spheres + s.n_convex; }
+static inline int64_t n_prims(const Scene& s) { return s.n_tris + s.n_quads + s.n_spheres + s.n_convex + s.n_shapes; }
+static inline const Scene::Shape& shape_of(const Scene& s, int64_t gid) {
+    return s.shapes[gid - s.n_tris - s.n_quads - s.n_spheres - s.n_convex];
+}
 
 static Aabb prim_box(const Scene& s, int64_t gid) {
     int t = prim_type(s, gid);
@@ -619,6 +637,7 @@ static Aabb prim_box(const Scene& s, int64_t gid) {
         V3 r = v3(sp.r, sp.r, sp.r);
         return Aabb{sp.c - r, sp.c + r};
     }
+    if (t == PRIM_SHAPE) return shape_of(s, gid).box;
     return s.convex[gid - s.n_tris - s.n_quads - s.n_spheres].box;                  // diamond.rs:172-186
 }
 
@@ -857,12 +876,117 @@ static bool convex_hit(const float* planes, int32_t n, const Ray& r, float tmin,
     return true;
 }
 
+// ── cylinder, cone, disk, infinite plane ──────────────────────────────────────
+// The ray in the shape's object space through the SRT wrappers, outermost
+// first: Translate, Rotate (mat_apply_t), UniformScale (transform.rs:29-45,
+// 158-164, 228-242).
+static inline Ray shape_local(const Scene::Shape& sh, const Ray& r) {
+    if (!sh.placed) return r;
+    V3 o1 = r.o - sh.t;
+    const float* m = sh.R;
+    V3 o2 = v3(m[0] * o1.x + m[3] * o1.y + m[6] * o1.z, m[1] * o1.x + m[4] * o1.y + m[7] * o1.z,
+               m[2] * o1.x + m[5] * o1.y + m[8] * o1.z);
+    V3 d2 = v3(m[0] * r.d.x + m[3] * r.d.y + m[6] * r.d.z, m[1] * r.d.x + m[4] * r.d.y + m[7] * r.d.z,
+               m[2] * r.d.x + m[5] * r.d.y + m[8] * r.d.z);
+    return Ray{sh.inv_scale * o2, sh.inv_scale * d2};
+}
+// the closest crossing in [tmin, tmax] and which surface: 0 lateral (or the
+// disk / plane), 1 bottom cap or cone base, 2 top cap
+static bool shape_hit(const Scene::Shape& sh, const Ray& r, float tmin, float tmax, float* t_out, int32_t* part) {
+    if (sh.type == RT_SHAPE_CYLINDER || sh.type == RT_SHAPE_CONE) {
+        bool cone = sh.type == RT_SHAPE_CONE;
+        V3 oc = r.o - sh.c;
+        float dx = r.d.x, dy = r.d.y, dz = r.d.z, h = sh.height;
+        float best_t = tmax;
+        bool found = false;
+        float a, half_b, c;
+        if (cone) {                                                                  // cone.rs:19-63
+            float k = (sh.radius / h) * (sh.radius / h), hy = h - oc.y;
+            a = dx * dx + dz * dz - k * dy * dy;
+            half_b = oc.x * dx + oc.z * dz + k * hy * dy;
+            c = oc.x * oc.x + oc.z * oc.z - k * hy * hy;
+        } else {                                                                     // cylinder.rs:132-167
+            a = dx * dx + dz * dz;
+            half_b = oc.x * dx + oc.z * dz;
+            c = oc.x * oc.x + oc.z * oc.z - sh.radius * sh.radius;
+        }
+        if (cone ? std::fabs(a) > 1e-8f : a > 1e-8f) {
+            float disc = half_b * half_b - a * c;
+            if (disc >= 0.0f) {
+                float sq = std::sqrt(disc);
+                float roots[2] = {(-half_b - sq) / a, (-half_b + sq) / a};
+                for (float root : roots) {
+                    if (root < tmin || root > best_t) continue;
+                    float ly = (r.o + root * r.d).y - sh.c.y;
+                    if (ly < 0.0f || ly > h) continue;
+                    best_t = root; *part = 0; found = true;
+                }
+            }
+        }
+        if (std::fabs(dy) > 1e-8f) {                                                // caps / base disk
+            int ncap = cone ? 1 : 2;
+            for (int k = 0; k < ncap; k++) {
+                float cap_y = k == 0 ? 0.0f : h;
+                float t = cone ? -oc.y / dy : (cap_y - oc.y) / dy;
+                if (cone ? !(t >= tmin && t <= best_t) : (t < tmin || t > best_t)) continue;
+                V3 p = r.o + t * r.d;
+                float lx = p.x - sh.c.x, lz = p.z - sh.c.z;
+                if (lx * lx + lz * lz > sh.radius * sh.radius) continue;
+                best_t = t; *part = 1 + k; found = true;
+            }
+        }
+        if (found) *t_out = best_t;
+        return found;
+    }
+    float denom = dot(sh.n, r.d);                                                   // disk.rs:146-157, plane.rs:37-42
+    if (!(std::fabs(denom) >= 1e-8f)) return false;
+    float t = dot(sh.n, sh.c - r.o) / denom;
+    if (t < tmin || t > tmax) return false;
+    if (sh.type == RT_SHAPE_DISK) {
+        V3 off = (r.o + t * r.d) - sh.c;
+        if (len2(off) > sh.radius * sh.radius) return false;
+    }
+    *t_out = t; *part = 0;
+    return true;
+}
+// object-space outward normal of a crossing (cylinder.rs:155-159, cone.rs:50-54,
+// the caps, disk.rs:153, plane.rs:46-66 with the wave bump)
+static V3 shape_outward(const Scene::Shape& sh, V3 p, int32_t part) {
+    if (sh.type == RT_SHAPE_CYLINDER) {
+        if (part == 0) return v3((p.x - sh.c.x) / sh.radius, 0.0f, (p.z - sh.c.z) / sh.radius);
+        return v3(0.0f, part == 1 ? -1.0f : 1.0f, 0.0f);
+    }
+    if (sh.type == RT_SHAPE_CONE) {
+        if (part != 0) return v3(0.0f, -1.0f, 0.0f);
+        float h = sh.height, k = (sh.radius / h) * (sh.radius / h);
+        float ly = p.y - sh.c.y;
+        V3 g = v3(p.x - sh.c.x, k * (h - ly), p.z - sh.c.z);
+        return len2(g) > 1e-12f ? unit(g) : v3(0.0f, 1.0f, 0.0f);
+    }
+    if (sh.type == RT_SHAPE_PLANE && sh.wave_a > 1e-6f) {
+        V3 off = p - sh.c;
+        float u = dot(off, sh.u), v = dot(off, sh.v), sc = sh.wave_s, a = sh.wave_a;
+        float phi1 = sc * u + 0.7f * sc * v, phi2 = 1.3f * sc * v - 0.5f * sc * u;
+        float dh_du = a * sc * std::cos(phi1) - 0.25f * a * sc * std::cos(phi2);
+        float dh_dv = 0.7f * a * sc * std::cos(phi1) + 0.65f * a * sc * std::cos(phi2);
+        return unit(sh.n - dh_du * sh.u - dh_dv * sh.v);
+    }
+    return sh.n;
+}
+
 static inline bool prim_hit(const Scene& s, int64_t gid, const Ray& r, float tmin, float tmax,
                             float* t, float* b1, float* b2) {
     if (gid < s.n_tris) return tri_hit(s.tris[gid], r, tmin, tmax, t, b1, b2);
     if (gid < s.n_tris + s.n_quads) return quad_hit(s.quads[gid - s.n_tris], r, tmin, tmax, t, b1, b2);
     *b1 = 0.0f; *b2 = 0.0f;
     if (gid < s.n_tris + s.n_quads + s.n_spheres) return sphere_hit(s.spheres[gid - s.n_tris - s.n_quads], r, tmin, tmax, t);
+    if (prim_type(s, gid) == PRIM_SHAPE) {
+        const Scene::Shape& sh = shape_of(s, gid);
+        int32_t part = 0;
+        if (!shape_hit(sh, shape_local(sh, r), tmin, tmax, t, &part)) return false;
+        memcpy(b1, &part, 4);
+        return true;
+    }
     const Scene::Convex& c = s.convex[gid - s.n_tris - s.n_quads - s.n_spheres];
     int32_t pi = -1;
     if (!convex_hit(s.convex_planes.data() + (size_t)c.off * 4, c.n, r, tmin, tmax, t, &pi)) return false;
@@ -1261,6 +1385,24 @@ static Rec make_rec(const Scene& s, const Ray& r, const HitRes& h) {
         outward = (rec.p - sp.c) / sp.r;
         sphere_uv_calc(outward, &rec.u, &rec.v);
         rec.mat = sp.mat;
+    } else if (t == PRIM_SHAPE) {
+        const Scene::Shape& sh = shape_of(s, h.gid);
+        int32_t part;
+        memcpy(&part, &h.b1, 4);
+        Ray lr = shape_local(sh, r);
+        V3 ow = shape_outward(sh, lr.o + h.t * lr.d, part);
+        rec.u = 0.0f; rec.v = 0.0f;
+        rec.mat = sh.mat;
+        // HitRecord::new in object space, then Rotate turns the normal (transform.rs:236-241)
+        rec.front = dot(lr.d, ow) < 0.0f;
+        V3 nn = rec.front ? ow : -ow;
+        if (sh.placed) {
+            const float* m = sh.R;
+            nn = v3(m[0] * nn.x + m[1] * nn.y + m[2] * nn.z, m[3] * nn.x + m[4] * nn.y + m[5] * nn.z,
+                    m[6] * nn.x + m[7] * nn.y + m[8] * nn.z);
+        }
+        rec.normal = nn;
+        return rec;
     } else {                                                                        // diamond.rs:257-275
         const Scene::Convex& c = s.convex[h.gid - s.n_tris - s.n_quads - s.n_spheres];
         int32_t pi;
@@ -1742,10 +1884,14 @@ static inline Rng photon_rng(uint64_t seed, uint32_t gid) {
 
 // photon_bounds of the world (hittable.rs:199-212): union of the primitive boxes
 static Aabb world_bounds(const Scene& s) {
-    int64_t n = n_prims(s);
-    bool any = n > 0;
-    Aabb b = any ? prim_box(s, 0) : Aabb{v3(0, 0, 0), v3(0, 0, 0)};
-    for (int64_t i = 1; i < n; i++) b = surrounding(b, prim_box(s, i));
+    // photon_bounds: infinite planes stay out (plane.rs:97-102)
+    bool any = false;
+    Aabb b{v3(0, 0, 0), v3(0, 0, 0)};
+    for (int64_t i = 0; i < n_prims(s); i++) {
+        if (prim_type(s, i) == PRIM_SHAPE && shape_of(s, i).type == RT_SHAPE_PLANE) continue;
+        b = any ? surrounding(b, prim_box(s, i)) : prim_box(s, i);
+        any = true;
+    }
     for (const RtMedium& m : s.media) {                                            // volume.rs:152-154
         Aabb mb;
         if (m.boundary == RT_BOUND_BOX)
@@ -2324,6 +2470,65 @@ static int scene_create(const RtSceneDesc* d, Scene** out) {
         int32_t off = (int32_t)(s->convex_planes.size() / 4);
         place_planes(c, d->convex_planes + (size_t)c.plane_offset * 4, s->convex_planes, s->convex_shade);
         s->convex.push_back(Scene::Convex{off, c.n_planes, c.mat, c.polish, placed_box(c)});
+    }
+    // cylinders, cones, disks, infinite planes
+    if (d->n_shapes < 0 || (d->n_shapes > 0 && !d->shapes)) { delete s; g_err = "bad shape list"; return RT_ERR_INVALID; }
+    s->n_shapes = d->n_shapes;
+    for (int64_t i = 0; i < d->n_shapes; i++) {
+        const RtShape& q = d->shapes[i];
+        Scene::Shape sh;
+        sh.type = q.type; sh.mat = q.mat;
+        sh.c = v3(q.center[0], q.center[1], q.center[2]);
+        V3 nraw = v3(q.normal[0], q.normal[1], q.normal[2]);
+        bool planar = q.type == RT_SHAPE_DISK || q.type == RT_SHAPE_PLANE;
+        bool ok = q.type >= RT_SHAPE_CYLINDER && q.type <= RT_SHAPE_PLANE && q.mat >= 0 && q.mat < d->n_mats &&
+                  q.scale > 0.0f && !(planar && !(len2(nraw) > 1e-12f)) &&
+                  !(q.type != RT_SHAPE_PLANE && !(q.radius > 0.0f)) &&
+                  !((q.type == RT_SHAPE_CYLINDER || q.type == RT_SHAPE_CONE) && !(q.height > 0.0f));
+        if (!ok) { delete s; g_err = "invalid shape " + std::to_string(i); return RT_ERR_INVALID; }
+        sh.n = planar ? unit(nraw) : v3(0, 1, 0);
+        onb_vec(sh.n, &sh.u, &sh.v);                                               // disk.rs:118-119, plane.rs:31-32
+        sh.radius = q.radius; sh.height = q.height; sh.wave_a = q.wave_amplitude; sh.wave_s = q.wave_scale;
+        memcpy(sh.R, q.rot, sizeof(sh.R));
+        sh.inv_scale = 1.0f / q.scale;
+        sh.t = v3(q.translate[0], q.translate[1], q.translate[2]);
+        bool ident_r = q.rot[0] == 1.0f && q.rot[4] == 1.0f && q.rot[8] == 1.0f && q.rot[1] == 0.0f && q.rot[2] == 0.0f &&
+                       q.rot[3] == 0.0f && q.rot[5] == 0.0f && q.rot[6] == 0.0f && q.rot[7] == 0.0f;
+        sh.placed = !(ident_r && q.scale == 1.0f && sh.t.x == 0.0f && sh.t.y == 0.0f && sh.t.z == 0.0f);
+        // object-space box (cylinder.rs:226-232, cone.rs:126-132, disk.rs:166-175, plane.rs:80-95)
+        Aabb ob;
+        if (q.type == RT_SHAPE_CYLINDER || q.type == RT_SHAPE_CONE) {
+            V3 rr = v3(sh.radius, 0.0f, sh.radius);
+            ob = Aabb{sh.c - rr, sh.c + rr + v3(0.0f, sh.height, 0.0f)};
+        } else if (q.type == RT_SHAPE_DISK) {
+            V3 ext = v3(sh.radius * std::sqrt(rmax(1.0f - sh.n.x * sh.n.x, 0.0f)),
+                        sh.radius * std::sqrt(rmax(1.0f - sh.n.y * sh.n.y, 0.0f)),
+                        sh.radius * std::sqrt(rmax(1.0f - sh.n.z * sh.n.z, 0.0f)));
+            ob = pad(Aabb{sh.c - ext, sh.c + ext});
+        } else {
+            const float B = 1e5f, E = 1e-3f;
+            float lo[3], hi[3], nn[3] = {sh.n.x, sh.n.y, sh.n.z}, pp[3] = {sh.c.x, sh.c.y, sh.c.z};
+            for (int a = 0; a < 3; a++) {
+                if (std::fabs(nn[a]) > 0.999f) { lo[a] = pp[a] - E; hi[a] = pp[a] + E; }
+                else { lo[a] = -B; hi[a] = B; }
+            }
+            ob = Aabb{v3(lo[0], lo[1], lo[2]), v3(hi[0], hi[1], hi[2])};
+        }
+        if (sh.placed) {                                                            // the corners, placed
+            V3 mn = v3(INFINITY, INFINITY, INFINITY), mx = v3(-INFINITY, -INFINITY, -INFINITY);
+            for (int k = 0; k < 8; k++) {
+                V3 x = v3(k & 1 ? ob.mx.x : ob.mn.x, k & 2 ? ob.mx.y : ob.mn.y, k & 4 ? ob.mx.z : ob.mn.z) * q.scale;
+                V3 w = v3(q.rot[0] * x.x + q.rot[1] * x.y + q.rot[2] * x.z, q.rot[3] * x.x + q.rot[4] * x.y + q.rot[5] * x.z,
+                          q.rot[6] * x.x + q.rot[7] * x.y + q.rot[8] * x.z) + sh.t;
+                mn = v3(rmin(mn.x, w.x), rmin(mn.y, w.y), rmin(mn.z, w.z));
+                mx = v3(rmax(mx.x, w.x), rmax(mx.y, w.y), rmax(mx.z, w.z));
+            }
+            float e = 1e-5f * rmax(rmax(rmax(std::fabs(mn.x), std::fabs(mx.x)), rmax(std::fabs(mn.y), std::fabs(mx.y))),
+                                   rmax(std::fabs(mn.z), std::fabs(mx.z))) + 1e-6f;
+            ob = Aabb{mn - v3(e, e, e), mx + v3(e, e, e)};
+        }
+        sh.box = ob;
+        s->shapes.push_back(sh);
     }
     s->lights.assign(d->light_prims, d->light_prims + d->n_lights);
     s->bg = d->bg;

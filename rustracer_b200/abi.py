@@ -113,6 +113,28 @@ class RtConvex(C.Structure):
     ]
 
 
+RT_SHAPE_CYLINDER = 0
+RT_SHAPE_CONE = 1
+RT_SHAPE_DISK = 2
+RT_SHAPE_PLANE = 3
+
+
+class RtShape(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("mat", C.c_int32),
+        ("center", F3),
+        ("normal", F3),
+        ("radius", C.c_float),
+        ("height", C.c_float),
+        ("wave_amplitude", C.c_float),
+        ("wave_scale", C.c_float),
+        ("scale", C.c_float),
+        ("rot", C.c_float * 9),
+        ("translate", F3),
+    ]
+
+
 class RtSceneDesc(C.Structure):
     _fields_ = [
         ("n_tris", C.c_int64),
@@ -136,6 +158,8 @@ class RtSceneDesc(C.Structure):
         ("n_convex", C.c_int64),
         ("convex", C.POINTER(RtConvex)),
         ("convex_planes", C.POINTER(C.c_float)),
+        ("n_shapes", C.c_int64),
+        ("shapes", C.POINTER(RtShape)),
     ]
 
 

@@ -105,6 +105,11 @@ struct DevScene {
     const float4* cvx;
     const float4* cvx_planes;
     const float4* cvx_shade;
+    // cylinders, cones, disks and infinite planes share the convex leaf type:
+    // their count field is −1 − RT_SHAPE_*, their offset indexes 8 float4 here
+    // (see shape_test)
+    const float4* shape_par;
+    int n_analytic;             // convex solids + shapes (the traversal compiles their tests in only if > 0)
     // spectral tables: CIE x̄ȳz̄ on the 5 nm grid from 380 nm and the per-channel
     // normalisations of spectral_to_rgb / spectral_fire_rgb (spectrum.rs:78-177)
     const float4* cmf;          // n_spec entries (x, y, z, -)
@@ -232,6 +237,126 @@ RT_D bool convex_test(const float4* pl, int n, float3 o, float3 d, float tmin, f
     if (exit_i < 0 || t_exit > tmax) return false;
     *t_out = t_exit; *plane = exit_i;
     return true;
+}
+
+// ── cylinder, cone, disk, infinite plane (cylinder.rs, cone.rs, disk.rs, plane.rs)
+// Record P[0..7]: (centre, radius) (unit normal, height) (u axis, wave amplitude)
+// (v axis, wave scale) (rotation row 0, scale) (row 1, 1/scale) (row 2, placed)
+// (translation, 0).  The ray goes to object space through the SRT wrappers,
+// outermost first: Translate, Rotate (transpose), UniformScale (transform.rs).
+RT_D void shape_local(const float4* P, float3 o, float3 d, float3* lo, float3* ld) {
+    float4 r0 = __ldg(P + 4), r1 = __ldg(P + 5), r2 = __ldg(P + 6);
+    if (r2.w == 0.0f) { *lo = o; *ld = d; return; }
+    float4 tr = __ldg(P + 7);
+    float3 o1 = mk(o.x - tr.x, o.y - tr.y, o.z - tr.z);
+    float3 o2 = mk(r0.x * o1.x + r1.x * o1.y + r2.x * o1.z, r0.y * o1.x + r1.y * o1.y + r2.y * o1.z,
+                   r0.z * o1.x + r1.z * o1.y + r2.z * o1.z);
+    float3 d2 = mk(r0.x * d.x + r1.x * d.y + r2.x * d.z, r0.y * d.x + r1.y * d.y + r2.y * d.z,
+                   r0.z * d.x + r1.z * d.y + r2.z * d.z);
+    float inv = r1.w;
+    *lo = mk(inv * o2.x, inv * o2.y, inv * o2.z);
+    *ld = mk(inv * d2.x, inv * d2.y, inv * d2.z);
+}
+// the closest crossing in [tmin, tmax] of an object-space ray; *part = 0 lateral
+// surface (or the disk / plane), 1 bottom cap or cone base, 2 top cap
+RT_D bool shape_test(int type, const float4* P, float3 o, float3 d, float tmin, float tmax, float* t_out, int* part) {
+    float4 p0 = __ldg(P), p1 = __ldg(P + 1);
+    float3 c = mk(p0.x, p0.y, p0.z);
+    float radius = p0.w;
+    if (type == RT_SHAPE_CYLINDER || type == RT_SHAPE_CONE) {                      // cylinder.rs:132-187, cone.rs:19-82
+        bool cone = type == RT_SHAPE_CONE;
+        float h = p1.w;
+        float3 oc = o - c;
+        float a, half_b, cc;
+        if (cone) {
+            float k = (radius / h) * (radius / h), hy = h - oc.y;
+            a = d.x * d.x + d.z * d.z - k * d.y * d.y;
+            half_b = oc.x * d.x + oc.z * d.z + k * hy * d.y;
+            cc = oc.x * oc.x + oc.z * oc.z - k * hy * hy;
+        } else {
+            a = d.x * d.x + d.z * d.z;
+            half_b = oc.x * d.x + oc.z * d.z;
+            cc = oc.x * oc.x + oc.z * oc.z - radius * radius;
+        }
+        float best_t = tmax;
+        bool found = false;
+        if (cone ? fabsf(a) > 1e-8f : a > 1e-8f) {
+            float disc = half_b * half_b - a * cc;
+            if (disc >= 0.0f) {
+                float sq = sqrtf(disc);
+                float roots[2] = {(-half_b - sq) / a, (-half_b + sq) / a};
+                for (int k = 0; k < 2; k++) {
+                    float root = roots[k];
+                    if (root < tmin || root > best_t) continue;
+                    float ly = ray_at(o, d, root).y - c.y;
+                    if (ly < 0.0f || ly > h) continue;
+                    best_t = root; *part = 0; found = true;
+                }
+            }
+        }
+        if (fabsf(d.y) > 1e-8f) {
+            for (int k = 0; k < (cone ? 1 : 2); k++) {
+                float cap_y = k == 0 ? 0.0f : h;
+                float t = cone ? -oc.y / d.y : (cap_y - oc.y) / d.y;
+                if (cone ? !(t >= tmin && t <= best_t) : (t < tmin || t > best_t)) continue;
+                float3 p = ray_at(o, d, t);
+                float lx = p.x - c.x, lz = p.z - c.z;
+                if (lx * lx + lz * lz > radius * radius) continue;
+                best_t = t; *part = 1 + k; found = true;
+            }
+        }
+        if (found) *t_out = best_t;
+        return found;
+    }
+    float3 n = mk(p1.x, p1.y, p1.z);                                                // disk.rs:146-157, plane.rs:37-42
+    float denom = dot3(n, d);
+    if (!(fabsf(denom) >= 1e-8f)) return false;
+    float t = dot3(n, c - o) / denom;
+    if (t < tmin || t > tmax) return false;
+    if (type == RT_SHAPE_DISK && len2(ray_at(o, d, t) - c) > radius * radius) return false;
+    *t_out = t; *part = 0;
+    return true;
+}
+// object-space outward normal of a crossing at p (cylinder.rs:155-159,
+// cone.rs:50-54, the caps, disk.rs:153, plane.rs:46-66 with the wave bump)
+RT_D float3 shape_outward(int type, const float4* P, float3 p, int part) {
+    float4 p0 = __ldg(P), p1 = __ldg(P + 1);
+    float3 c = mk(p0.x, p0.y, p0.z);
+    if (type == RT_SHAPE_CYLINDER) {
+        if (part == 0) return mk((p.x - c.x) / p0.w, 0.0f, (p.z - c.z) / p0.w);
+        return mk(0.0f, part == 1 ? -1.0f : 1.0f, 0.0f);
+    }
+    if (type == RT_SHAPE_CONE) {
+        if (part != 0) return mk(0.0f, -1.0f, 0.0f);
+        float h = p1.w, k = (p0.w / h) * (p0.w / h), ly = p.y - c.y;
+        float3 g = mk(p.x - c.x, k * (h - ly), p.z - c.z);
+        return len2(g) > 1e-12f ? unit3(g) : mk(0.0f, 1.0f, 0.0f);
+    }
+    float3 n = mk(p1.x, p1.y, p1.z);
+    float4 pu = __ldg(P + 2), pv = __ldg(P + 3);
+    if (type == RT_SHAPE_PLANE && pu.w > 1e-6f) {
+        float3 ua = mk(pu.x, pu.y, pu.z), va = mk(pv.x, pv.y, pv.z), off = p - c;
+        float u = dot3(off, ua), v = dot3(off, va), sc = pv.w, a = pu.w;
+        float phi1 = sc * u + 0.7f * sc * v, phi2 = 1.3f * sc * v - 0.5f * sc * u;
+        float c1 = cosf(phi1), c2 = cosf(phi2);
+        float dh_du = a * sc * c1 - 0.25f * a * sc * c2;
+        float dh_dv = 0.7f * a * sc * c1 + 0.65f * a * sc * c2;
+        return unit3(n - dh_du * ua - dh_dv * va);
+    }
+    return n;
+}
+// the world-space shading normal of a shape crossing: face-forward in object
+// space (HitRecord::new), then turned by the rotation (transform.rs:236-241)
+RT_D float3 shape_normal(int type, const float4* P, float3 o, float3 d, float t, int part, bool* front) {
+    float3 lo, ld;
+    shape_local(P, o, d, &lo, &ld);
+    float3 ow = shape_outward(type, P, ray_at(lo, ld, t), part);
+    *front = dot3(ld, ow) < 0.0f;
+    float3 n = *front ? ow : -ow;
+    float4 r0 = __ldg(P + 4), r1 = __ldg(P + 5), r2 = __ldg(P + 6);
+    if (r2.w == 0.0f) return n;
+    return mk(r0.x * n.x + r0.y * n.y + r0.z * n.z, r1.x * n.x + r1.y * n.y + r1.z * n.z,
+              r2.x * n.x + r2.y * n.y + r2.z * n.z);
 }
 
 // triangle.rs:75-89

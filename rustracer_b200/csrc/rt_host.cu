@@ -104,6 +104,66 @@ static Box placed_box(const RtConvex& c) {                                      
     return Box{b.mn - h3(e, e, e), b.mx + h3(e, e, e)};
 }
 
+// Cylinder / cone / disk / plane records (8 float4): (centre, radius),
+// (unit normal, height), (u axis, wave amplitude), (v axis, wave scale), the
+// rotation rows with (scale, 1/scale, placed), (translation, 0); returns the
+// placed box (cylinder.rs:226-232, cone.rs:126-132, disk.rs:166-175,
+// plane.rs:80-95, transform.rs:180-200).
+static Box shape_params(const RtShape& q, float4* P) {
+    H3 c = h3(q.center[0], q.center[1], q.center[2]);
+    bool planar = q.type == RT_SHAPE_DISK || q.type == RT_SHAPE_PLANE;
+    H3 n = h3(0.f, 1.f, 0.f);
+    if (planar) {
+        H3 nr = h3(q.normal[0], q.normal[1], q.normal[2]);
+        n = nr / hlen(nr);
+    }
+    H3 up = std::fabs(n.y) < 0.9f ? h3(0.f, 1.f, 0.f) : h3(1.f, 0.f, 0.f);              // vec3.rs:37-42
+    H3 u = hcross(n, up);
+    u = u / hlen(u);
+    H3 v = hcross(n, u);
+    const float* R = q.rot;
+    bool ident = R[0] == 1.f && R[4] == 1.f && R[8] == 1.f && R[1] == 0.f && R[2] == 0.f && R[3] == 0.f &&
+                 R[5] == 0.f && R[6] == 0.f && R[7] == 0.f && q.scale == 1.f && q.translate[0] == 0.f &&
+                 q.translate[1] == 0.f && q.translate[2] == 0.f;
+    P[0] = make_float4(c.x, c.y, c.z, q.radius);
+    P[1] = make_float4(n.x, n.y, n.z, q.height);
+    P[2] = make_float4(u.x, u.y, u.z, q.wave_amplitude);
+    P[3] = make_float4(v.x, v.y, v.z, q.wave_scale);
+    P[4] = make_float4(R[0], R[1], R[2], q.scale);
+    P[5] = make_float4(R[3], R[4], R[5], 1.0f / q.scale);
+    P[6] = make_float4(R[6], R[7], R[8], ident ? 0.f : 1.f);
+    P[7] = make_float4(q.translate[0], q.translate[1], q.translate[2], 0.f);
+    Box ob;
+    if (!planar) {
+        H3 rr = h3(q.radius, 0.f, q.radius);
+        ob = Box{c - rr, c + rr + h3(0.f, q.height, 0.f)};
+    } else if (q.type == RT_SHAPE_DISK) {
+        H3 ext = h3(q.radius * std::sqrt(std::fmax(1.f - n.x * n.x, 0.f)), q.radius * std::sqrt(std::fmax(1.f - n.y * n.y, 0.f)),
+                    q.radius * std::sqrt(std::fmax(1.f - n.z * n.z, 0.f)));
+        ob = pad(Box{c - ext, c + ext});
+    } else {
+        const float B = 1e5f, E = 1e-3f;
+        float lo[3], hi[3], nn[3] = {n.x, n.y, n.z}, pp[3] = {c.x, c.y, c.z};
+        for (int a = 0; a < 3; a++) {
+            if (std::fabs(nn[a]) > 0.999f) { lo[a] = pp[a] - E; hi[a] = pp[a] + E; }
+            else { lo[a] = -B; hi[a] = B; }
+        }
+        ob = Box{h3(lo[0], lo[1], lo[2]), h3(hi[0], hi[1], hi[2])};
+    }
+    if (ident) return ob;
+    Box b{h3(INFINITY, INFINITY, INFINITY), h3(-INFINITY, -INFINITY, -INFINITY)};
+    H3 t = h3(q.translate[0], q.translate[1], q.translate[2]);
+    for (int k = 0; k < 8; k++) {
+        H3 x = h3(k & 1 ? ob.mx.x : ob.mn.x, k & 2 ? ob.mx.y : ob.mn.y, k & 4 ? ob.mx.z : ob.mn.z) * q.scale;
+        H3 w = rot_apply(R, x) + t;
+        b = unite(b, Box{w, w});
+    }
+    float e = 1e-5f * std::max(std::max(std::fabs(b.mn.x), std::fabs(b.mx.x)),
+                               std::max(std::max(std::fabs(b.mn.y), std::fabs(b.mx.y)),
+                                        std::max(std::fabs(b.mn.z), std::fabs(b.mx.z)))) + 1e-6f;
+    return Box{b.mn - h3(e, e, e), b.mx + h3(e, e, e)};
+}
+
 static inline float area(const Box& b) {
     H3 d = b.mx - b.mn;
     return 2.0f * (d.x * d.y + d.y * d.z + d.z * d.x);
@@ -567,8 +627,12 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         d->n_spheres > (int64_t)RT_HIT_MAX_INDEX + 1 || d->n_convex > (int64_t)RT_HIT_MAX_INDEX + 1 ||
         d->n_media > (int64_t)RT_HIT_MAX_INDEX + 1)
         return bail(fail(s, RT_ERR_CAPACITY, "more than 2^27 primitives of one type"));
+    if (d->n_shapes < 0 || (d->n_shapes > 0 && !d->shapes)) return bail(fail(s, RT_ERR_INVALID, "shapes without their array"));
     const int64_t n_sph_end = d->n_tris + d->n_quads + d->n_spheres;   // canonical ids of the convex solids start here
-    int64_t n = n_sph_end + d->n_convex;
+    const int64_t n_cvx_end = n_sph_end + d->n_convex;                   // ... and of the other shapes here
+    if (d->n_convex + d->n_shapes > (int64_t)RT_HIT_MAX_INDEX + 1)
+        return bail(fail(s, RT_ERR_CAPACITY, "more than 2^27 convex solids and shapes"));
+    int64_t n = n_cvx_end + d->n_shapes;
     if (n >= (1ll << 28) - 1) return bail(fail(s, RT_ERR_CAPACITY, "more than 2^28 - 2 primitives"));
     s->n_prims = n;
     if ((d->n_tris && (!d->tri_v || !d->tri_mat)) || (d->n_quads && (!d->quad_quv || !d->quad_mat)) ||
@@ -621,6 +685,24 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     }
     for (int64_t k = 0; k < n_planes_total * 4; k++)
         if (!std::isfinite(d->convex_planes[k])) return bail(fail(s, RT_ERR_INVALID, "non-finite convex plane"));
+    for (int64_t i = 0; i < d->n_shapes; i++) {
+        const RtShape& q = d->shapes[i];
+        std::string what = "shape " + std::to_string(i);
+        if (q.type < RT_SHAPE_CYLINDER || q.type > RT_SHAPE_PLANE || bad_mat(q.mat))
+            return bail(fail(s, RT_ERR_INVALID, what + ": unknown type or material"));
+        int mt = d->mats[q.mat].type;
+        if (mt == RT_MAT_DIFFUSE_LIGHT || mt == RT_MAT_BLACKBODY_LIGHT)
+            return bail(fail(s, RT_ERR_INVALID, what + ": emissive materials are not supported (shapes are not NEE lights)"));
+        float v[] = {q.center[0], q.center[1], q.center[2], q.normal[0], q.normal[1], q.normal[2], q.radius, q.height,
+                     q.wave_amplitude, q.wave_scale, q.scale, q.translate[0], q.translate[1], q.translate[2]};
+        for (float x : v)
+            if (!std::isfinite(x)) return bail(fail(s, RT_ERR_INVALID, what + ": non-finite parameter"));
+        bool planar = q.type == RT_SHAPE_DISK || q.type == RT_SHAPE_PLANE;
+        float nl2 = q.normal[0] * q.normal[0] + q.normal[1] * q.normal[1] + q.normal[2] * q.normal[2];
+        if (!(q.scale > 0.0f) || !rotation_ok(q.rot) || (planar && !(nl2 > 1e-12f)) ||
+            (q.type != RT_SHAPE_PLANE && !(q.radius > 0.0f)) || (!planar && !(q.height > 0.0f)))
+            return bail(fail(s, RT_ERR_INVALID, what + ": positive scale, radius and height, a non-zero normal, a rotation"));
+    }
     if (d->bg.type == RT_BG_ENVMAP && (!d->bg.env_rgb || d->bg.env_w <= 0 || d->bg.env_h <= 0))
         return bail(fail(s, RT_ERR_INVALID, "env map background without an image"));
 
@@ -669,11 +751,20 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         o += c.n_planes;
     }
 
-    if (n > 0) {
-        Box wb = boxes[0];
-        for (int64_t i = 1; i < n; i++) wb = unite(wb, boxes[i]);
-        for (int a = 0; a < 3; a++) { s->world_lo[a] = hc(wb.mn, a); s->world_hi[a] = hc(wb.mx, a); }
+    // other shapes: 8 float4 each (shape_params) and their boxes
+    std::vector<float4> gshape(std::max<int64_t>(d->n_shapes * 8, 8));
+    for (int64_t i = 0; i < d->n_shapes; i++) boxes[n_cvx_end + i] = shape_params(d->shapes[i], gshape.data() + i * 8);
+
+    // the photon-emitter bounds leave infinite planes out (plane.rs:97-102)
+    bool any = false;
+    Box wb{};
+    for (int64_t i = 0; i < n; i++) {
+        if (i >= n_cvx_end && d->shapes[i - n_cvx_end].type == RT_SHAPE_PLANE) continue;
+        wb = any ? unite(wb, boxes[i]) : boxes[i];
+        any = true;
     }
+    if (any)
+        for (int a = 0; a < 3; a++) { s->world_lo[a] = hc(wb.mn, a); s->world_hi[a] = hc(wb.mx, a); }
 
     // ── BVH ─────────────────────────────────────────────────────────────────
     std::vector<float4> gnodes;
@@ -811,15 +902,26 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
             }
         }
         // convex solids in leaf order, pointing at their world-space planes
+        // (shapes share the leaf type: their count field is −1 − RT_SHAPE_*, the
+        // offset indexes shape_par)
         std::vector<float4> gcvx(std::max<size_t>(order_cvx.size() * 2, 2));
         for (size_t k = 0; k < order_cvx.size(); k++) {
-            const RtConvex& c = d->convex[order_cvx[k]];
-            int32_t gi = (int32_t)(n_sph_end + order_cvx[k]);
-            gcvx[k * 2] = make_float4(__int_as_float_h(wofs[order_cvx[k]]), __int_as_float_h(c.n_planes),
-                                      __int_as_float_h(c.mat), c.polish);
+            int64_t j = order_cvx[k];
+            int32_t gi = (int32_t)(n_sph_end + j);
+            if (j < d->n_convex) {
+                const RtConvex& c = d->convex[j];
+                gcvx[k * 2] = make_float4(__int_as_float_h(wofs[j]), __int_as_float_h(c.n_planes),
+                                          __int_as_float_h(c.mat), c.polish);
+            } else {
+                const RtShape& q = d->shapes[j - d->n_convex];
+                gcvx[k * 2] = make_float4(__int_as_float_h((int32_t)((j - d->n_convex) * 8)),
+                                          __int_as_float_h(-1 - q.type), __int_as_float_h(q.mat), 0.f);
+            }
             gcvx[k * 2 + 1] = make_float4(__int_as_float_h(gi), 0.f, 0.f, 0.f);
         }
         int rc;
+        if ((rc = upload(s, gshape.data(), gshape.size(), &s->S.shape_par))) return bail(rc);
+        s->S.n_analytic = (int)(d->n_convex + d->n_shapes);
         if ((rc = upload(s, gcvx.data(), gcvx.size(), &s->S.cvx))) return bail(rc);
         if ((rc = upload(s, wpl.data(), wpl.size(), &s->S.cvx_planes))) return bail(rc);
         if ((rc = upload(s, wsh.data(), wsh.size(), &s->S.cvx_shade))) return bail(rc);

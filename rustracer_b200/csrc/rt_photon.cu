@@ -158,7 +158,7 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                 float3 p = ray_at(o, d, t);
                 uint32_t type = RT_HIT_TYPE(ref), idx = RT_HIT_INDEX(ref);
                 float3 outward;
-                int mat, cvx_wp = 0;
+                int mat, cvx_wp = 0, shape = -1;
                 if (type == RT_PRIM_TRI) {
                     const float4* g = S.tri + (size_t)idx * 3;
                     float4 ga = __ldg(g), gb = __ldg(g + 1), gc = __ldg(g + 2);
@@ -185,16 +185,25 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                     mat = __float_as_int(__ldg(g + 1).y);
                 } else {                                    // convex solid: the crossing plane's normal
                     float4 c0 = __ldg(S.cvx + (size_t)idx * 2);
-                    cvx_wp = __float_as_int(c0.x) + max(__float_as_int(hv.z), 0);
-                    float4 q = __ldg(S.cvx_planes + cvx_wp);
-                    outward = mk(q.x, q.y, q.z);
+                    shape = __float_as_int(c0.y) < 0 ? -1 - __float_as_int(c0.y) : -1;
+                    cvx_wp = __float_as_int(c0.x) + (shape < 0 ? max(__float_as_int(hv.z), 0) : 0);
+                    if (shape < 0) {
+                        float4 q = __ldg(S.cvx_planes + cvx_wp);
+                        outward = mk(q.x, q.y, q.z);
+                    }
                     mat = __float_as_int(c0.z);
                 }
-                bool front = dot3(d, outward) < 0.0f;
-                float3 nrm = front ? outward : -outward;
-                if (type == RT_PRIM_CONVEX) {               // polished facet normal, world space
-                    float4 sn = __ldg(S.cvx_shade + (size_t)cvx_wp * 2 + (front ? 0 : 1));
-                    nrm = mk(sn.x, sn.y, sn.z);
+                bool front;
+                float3 nrm;
+                if (shape >= 0) {                           // cylinder, cone, disk, plane
+                    nrm = shape_normal(shape, S.shape_par + cvx_wp, o, d, hv.y, __float_as_int(hv.z), &front);
+                } else {
+                    front = dot3(d, outward) < 0.0f;
+                    nrm = front ? outward : -outward;
+                    if (type == RT_PRIM_CONVEX) {           // polished facet normal, world space
+                        float4 sn = __ldg(S.cvx_shade + (size_t)cvx_wp * 2 + (front ? 0 : 1));
+                        nrm = mk(sn.x, sn.y, sn.z);
+                    }
                 }
                 const DevMaterial& m = S.mats[mat];
                 bool store = false;

@@ -618,6 +618,13 @@ RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
         r.mat = __float_as_int(__ldg(g + 1).y);
     } else {                                                                        // diamond.rs:257-275
         float4 c0 = __ldg(S.cvx + (size_t)idx * 2);
+        int cnt = __float_as_int(c0.y);
+        if (cnt < 0) {                                                              // cylinder, cone, disk, plane
+            r.mat = __float_as_int(c0.z);
+            r.nrm = shape_normal(-1 - cnt, S.shape_par + __float_as_int(c0.x), o, d, r.t, __float_as_int(hv.z),
+                                 &r.front);
+            return r;
+        }
         int pi = max(__float_as_int(hv.z), 0);
         int wp = __float_as_int(c0.x) + pi;
         float4 q = __ldg(S.cvx_planes + wp);

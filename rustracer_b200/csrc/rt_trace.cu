@@ -25,6 +25,9 @@ struct Best { float t, b1, b2; uint32_t ref, gid, mat; };
 RT_D uint32_t f2u(float f) { return __float_as_uint(f); }
 
 // Leaf test for one reference; updates `best` and returns nothing.
+// ANA: the scene has convex solids or shapes; without them the type-3 branch
+// is compiled out, so triangle scenes keep a lean traversal kernel.
+template <bool ANA>
 RT_D void leaf_closest(const DevScene& S, uint32_t ref, float3 o, float3 d, float tmin, Best& best) {
     uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
     float t, b1, b2;
@@ -50,10 +53,19 @@ RT_D void leaf_closest(const DevScene& S, uint32_t ref, float3 o, float3 d, floa
         float4 gm = h ? __ldg(g + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
         gid = f2u(gm.x);
         mat = f2u(gm.y);
-    } else {                                        // convex solid; b1 carries the crossing plane
+    } else if (!ANA) {
+        return;
+    } else {                                        // convex solid or shape; b1 carries the plane / surface
         float4 c0 = __ldg(S.cvx + (size_t)idx * 2);
-        int pi = -1;
-        h = convex_test(S.cvx_planes + __float_as_int(c0.x), __float_as_int(c0.y), o, d, tmin, best.t, &t, &pi);
+        int pi = -1, cnt = __float_as_int(c0.y);
+        if (cnt > 0) {
+            h = convex_test(S.cvx_planes + __float_as_int(c0.x), cnt, o, d, tmin, best.t, &t, &pi);
+        } else {
+            const float4* P = S.shape_par + __float_as_int(c0.x);
+            float3 lo, ld;
+            shape_local(P, o, d, &lo, &ld);
+            h = shape_test(-1 - cnt, P, lo, ld, tmin, best.t, &t, &pi);
+        }
         b1 = __int_as_float(pi);
         b2 = 0.0f;
         gid = h ? f2u(__ldg(S.cvx + (size_t)idx * 2 + 1).x) : 0u;
@@ -64,6 +76,7 @@ RT_D void leaf_closest(const DevScene& S, uint32_t ref, float3 o, float3 d, floa
     }
 }
 
+template <bool ANA>
 RT_D bool leaf_any(const DevScene& S, uint32_t ref, float3 o, float3 d, float tmin, float tmax) {
     uint32_t type = (ref >> 28) & 7u, idx = ref & 0x0FFFFFFFu;
     float t, b1, b2;
@@ -76,9 +89,14 @@ RT_D bool leaf_any(const DevScene& S, uint32_t ref, float3 o, float3 d, float tm
         return quad_test(gg, o, d, tmin, tmax, &t, &b1, &b2);
     }
     if (type == RT_PRIM_SPHERE) return sphere_test(__ldg(S.sphere + (size_t)idx * 2), o, d, tmin, tmax, &t);
+    if (!ANA) return false;
     float4 c0 = __ldg(S.cvx + (size_t)idx * 2);
-    int pi;
-    return convex_test(S.cvx_planes + __float_as_int(c0.x), __float_as_int(c0.y), o, d, tmin, tmax, &t, &pi);
+    int pi, cnt = __float_as_int(c0.y);
+    if (cnt > 0) return convex_test(S.cvx_planes + __float_as_int(c0.x), cnt, o, d, tmin, tmax, &t, &pi);
+    const float4* P = S.shape_par + __float_as_int(c0.x);
+    float3 lo, ld;
+    shape_local(P, o, d, &lo, &ld);
+    return shape_test(-1 - cnt, P, lo, ld, tmin, tmax, &t, &pi);
 }
 
 #ifndef RT_MNMX3
@@ -220,6 +238,7 @@ namespace rtk {
 // intersects hit leaves in slot order, then continues with the nearest hit inner
 // child (sorted by a 19-comparator network on packed (t | slot) keys) and pushes
 // the others far → near.  Returns false when the traversal is finished.
+template <bool ANA>
 RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, Best& best,
                        uint32_t& node, int& sp, uint32_t* stack, bool& ok) {
     float tn[8];
@@ -237,7 +256,7 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
         while (leaves) {
             int c = __ffs(leaves) - 1;
             leaves &= leaves - 1;
-            leaf_closest(S, __ldg(refs + c), R.o, d, tmin, best);
+            leaf_closest<ANA>(S, __ldg(refs + c), R.o, d, tmin, best);
         }
     }
     float cw = best.t + fabsf(best.t) * SLAB_WIDEN;
@@ -292,6 +311,7 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
 
 // One node visit of the any-hit traversal (bvh.rs:487-530).  Returns false when
 // finished; *hit is set when a primitive was hit.
+template <bool ANA>
 RT_D bool any_step(const DevScene& S, const RayC& R, float3 d, float tmin, float tmax,
                    uint32_t& node, int& sp, uint32_t* stack, bool& hit, bool& ok) {
     float tn[8];
@@ -313,7 +333,7 @@ RT_D bool any_step(const DevScene& S, const RayC& R, float3 d, float tmin, float
         while (leaves) {
             int c = __ffs(leaves) - 1;
             leaves &= leaves - 1;
-            if (leaf_any(S, __ldg(refs + c), R.o, d, tmin, tmax)) { hit = true; return false; }
+            if (leaf_any<ANA>(S, __ldg(refs + c), R.o, d, tmin, tmax)) { hit = true; return false; }
         }
     }
     if (inner == 0) {
@@ -356,7 +376,7 @@ RT_D bool nan_ray(float3 o, float3 d, float tmin, float tmax) {
 #define RT_TRACE_MINB 6
 #endif
 
-template <int MODE>
+template <int MODE, bool ANA>
 __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevScene S, PathState P, const uint32_t* __restrict__ queue,
                                                             const float* __restrict__ rays, uint32_t n_api,
                                                             const uint32_t* count, uint32_t* next,
@@ -407,7 +427,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
         if (exhausted && __ballot_sync(FULLMASK, active) == 0) break;
         if (active) {
             bool lok = true;
-            bool more = rtk::closest_step(S, R, d, tmin, best, node, sp, stack, lok);
+            bool more = rtk::closest_step<ANA>(S, R, d, tmin, best, node, sp, stack, lok);
             if (!lok) ok = false;
             if (!more) {
                 active = false;
@@ -429,7 +449,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
 // MODE 1: API any-hit (occluded flags)
 // MODE 2: wavefront shadow rays in a scene with media (an unoccluded ray scales
 //         its parked contribution by the media's transmittance)
-template <int MODE>
+template <int MODE, bool ANA>
 __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene S, PendTargets T, const float4* __restrict__ sq,
                                                         const float* __restrict__ rays, uint32_t n_api,
                                                         const uint32_t* count, uint32_t* next,
@@ -475,7 +495,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
         if (exhausted && __ballot_sync(FULLMASK, active) == 0) break;
         if (active) {
             bool lok = true;
-            bool more = rtk::any_step(S, R, d, tmin, tmax, node, sp, stack, hit, lok);
+            bool more = rtk::any_step<ANA>(S, R, d, tmin, tmax, node, sp, stack, hit, lok);
             if (!lok) ok = false;
             if (!more) {
                 active = false;
@@ -559,23 +579,30 @@ namespace rth {
 // persistent kernels: one wave of resident blocks
 int trace_grid(int dev_sms) { return dev_sms * RT_TRACE_GRID_PER_SM; }
 
+// the traversal kernels with (ANA) or without analytic solids
+#define RT_TRACE_LAUNCH(K, MODE, ...)                                                                    \
+    do {                                                                                                 \
+        if (S.n_analytic > 0) K<MODE, true><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);   \
+        else                  K<MODE, false><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);  \
+    } while (0)
 void launch_trace_closest_api(const DevScene& S, const float* rays, uint32_t n, int4* out, uint32_t* next, int* err,
                               int sms, cudaStream_t st) {
-    k_closest<1><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, PathState{}, nullptr, rays, n, nullptr, next, out, err);
+    RT_TRACE_LAUNCH(k_closest, 1, S, PathState{}, nullptr, rays, n, nullptr, next, out, err);
 }
 void launch_trace_any_api(const DevScene& S, const float* rays, uint32_t n, uint8_t* out, uint32_t* next, int* err,
                           int sms, cudaStream_t st) {
-    k_any<1><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, PendTargets{}, nullptr, rays, n, nullptr, next, out, err);
+    RT_TRACE_LAUNCH(k_any, 1, S, PendTargets{}, nullptr, rays, n, nullptr, next, out, err);
 }
 void launch_extend(const DevScene& S, const PathState& P, const uint32_t* queue, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st) {
-    k_closest<0><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, P, queue, nullptr, 0, count, next, nullptr, err);
+    RT_TRACE_LAUNCH(k_closest, 0, S, P, queue, nullptr, 0, count, next, nullptr, err);
 }
 void launch_shadow(const DevScene& S, const PendTargets& T, const float4* sq, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st) {
-    if (S.n_media > 0) k_any<2><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, T, sq, nullptr, 0, count, next, nullptr, err);
-    else               k_any<0><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(S, T, sq, nullptr, 0, count, next, nullptr, err);
+    if (S.n_media > 0) RT_TRACE_LAUNCH(k_any, 2, S, T, sq, nullptr, 0, count, next, nullptr, err);
+    else               RT_TRACE_LAUNCH(k_any, 0, S, T, sq, nullptr, 0, count, next, nullptr, err);
 }
+#undef RT_TRACE_LAUNCH
 void launch_media(const DevScene& S, const PathState& P, const uint32_t* queue, const uint32_t* count, int sms,
                   cudaStream_t st) {
     if (queue) k_media<1><<<sms * 8, 128, 0, st>>>(S, P, queue, count);

@@ -194,6 +194,7 @@ class SceneBuilder:
         self.caustics = None
         self.media = []          # abi.RtMedium
         self.convex = []         # dicts: object-space planes (k,4) float32, mat, polish, box, placement
+        self.shapes = []         # RtShape records
 
     # materials ---------------------------------------------------------
     def add_material(self, m):
@@ -277,6 +278,24 @@ class SceneBuilder:
         R = _euler_fwd(ang) if any(a != 0.0 for a in ang) else np.eye(3)
         return self.add_convex(planes, mat, lo, hi, polish=pol, scale=scale, rot=R,
                                pivot=center if pivot is None else pivot, translate=translate)
+
+    def add_shape(self, kind, mat, center, radius=0.0, height=0.0, normal=(0.0, 1.0, 0.0), wave_amplitude=0.0,
+                  wave_scale=1.0, xf=None):
+        """Cylinder / Cone / Disk / InfinitePlane (cylinder.rs, cone.rs, disk.rs,
+        plane.rs) in object space, placed by the objects' SRT transform."""
+        kinds = {"cylinder": abi.RT_SHAPE_CYLINDER, "cone": abi.RT_SHAPE_CONE, "disk": abi.RT_SHAPE_DISK,
+                 "infinite_plane": abi.RT_SHAPE_PLANE}
+        r = abi.RtShape()
+        r.type, r.mat = kinds[kind], mat
+        r.center, r.normal = _f3(center), _f3(normal)
+        r.radius, r.height = float(radius), float(height)
+        r.wave_amplitude, r.wave_scale = float(wave_amplitude), float(wave_scale)
+        xf = xf or Transform()
+        r.scale = xf.scale
+        r.rot = (C.c_float * 9)(*[float(v) for v in np.asarray(xf.R, np.float64).reshape(-1)])
+        r.translate = _f3(xf.t)
+        self.shapes.append(r)
+        return len(self.shapes) - 1
 
     def add_quad(self, corner, u, v, mat, xf=None):
         q, uu, vv = (np.asarray(a, dtype=np.float64) for a in (corner, u, v))
@@ -473,6 +492,10 @@ class SceneBuilder:
             d.n_convex = len(recs)
             d.convex = C.cast(self._cvx, C.POINTER(abi.RtConvex))
             d.convex_planes = abi.fptr(self._cvp)
+        if self.shapes:
+            self._shapes = (abi.RtShape * len(self.shapes))(*self.shapes)
+            d.n_shapes = len(self.shapes)
+            d.shapes = C.cast(self._shapes, C.POINTER(abi.RtShape))
         self._media = (abi.RtMedium * max(1, len(self.media)))(*self.media)
         d.n_media = len(self.media)
         d.media = C.cast(self._media, C.POINTER(abi.RtMedium)) if self.media else None
@@ -1143,6 +1166,17 @@ def scene_from_toml_dict(doc, base="."):
         elif st == "mesh":
             V, Fa, N = load_obj(_resolve(base, sh["path"]))
             sb.add_mesh(V, Fa, mat, N, xf)
+        elif st in ("cylinder", "cone"):                            # scene_file.rs:997-1000
+            sb.add_shape(st, mat, sh["center"], radius=sh["radius"], height=sh["height"], xf=xf)
+        elif st == "disk":                                          # scene_file.rs:1001-1002
+            if float(np.dot(sh["normal"], sh["normal"])) <= 1e-12:
+                raise ValueError(f"objects[{i}]: disk normal must be non-zero")
+            sb.add_shape("disk", mat, sh["center"], radius=sh["radius"], normal=sh["normal"], xf=xf)
+        elif st == "infinite_plane":                                # scene_file.rs:1023-1024
+            if float(np.dot(sh["normal"], sh["normal"])) <= 1e-12:
+                raise ValueError(f"objects[{i}]: plane normal must be non-zero")
+            sb.add_shape("infinite_plane", mat, sh["point"], normal=sh["normal"],
+                         wave_amplitude=sh.get("wave_amplitude", 0.0), wave_scale=sh.get("wave_scale", 1.0), xf=xf)
         elif st == "step_cut":                                      # scene_file.rs:1013-1021
             ol = step_outline_from_toml(sh.get("outline") or "rect", sh.get("corner_pct", 12.0),
                                         sh.get("corner_segs", 4), sh.get("oval_segs", 24), sh.get("pear", False),
