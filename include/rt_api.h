@@ -93,7 +93,31 @@ typedef struct RtMaterial {
     float   sheen_tint;          /* 0 white .. 1 albedo */
     float   emission[3];         /* linear RGB, times emission_strength */
     float   emission_strength;
+    /* texture maps, 1-based indices into RtSceneDesc.textures (0 = none):
+     * RT_MAT_LAMBERTIAN takes albedo_tex (texture.rs Image / Mottle); RT_MAT_PBR
+     * takes all five (material.rs:758-786) */
+    int32_t albedo_tex, roughness_tex, metallic_tex, ao_tex, normal_tex;
 } RtMaterial;
+
+/* ── textures (src/texture.rs, material.rs:633-671) ──────────────────────────
+ * IMAGE: 8-bit RGB texels, row 0 = top.  A Lambertian albedo samples the
+ * nearest texel and decodes sRGB (texture.rs:34-43); PBR maps sample bilinear
+ * (albedo sRGB-decoded; roughness / metallic / ao the red channel / 255;
+ * normal maps rgb / 255 → 2x − 1).  UVs: triangles carry tri_uv (else the
+ * reference's defaults (0,0) (1,0) (0.5,1)), quads their (α, β), spheres
+ * sphere.rs's (φ, θ) map; convex solids and shapes have (0, 0).
+ * MOTTLE: lerp(lo, hi, clamp(2·turb(p·scale, 7), 0, 1)) (texture.rs:52-55). */
+#define RT_TEX_IMAGE   0
+#define RT_TEX_MOTTLE  1
+typedef struct RtTexture {
+    int32_t        type;          /* RT_TEX_* */
+    int32_t        width, height; /* IMAGE */
+    const uint8_t* rgb8;          /* IMAGE: height × width × 3 */
+    float          scale;         /* MOTTLE */
+    float          lo[3], hi[3];  /* MOTTLE */
+    float          perlin_vec[256 * 3];   /* MOTTLE: the Perlin tables (perlin.rs:4-33) */
+    int32_t        perlin_perm[3 * 256];
+} RtTexture;
 
 /* ── background (src/renderer.rs:183-223) ────────────────────────────────── */
 #define RT_BG_SOLID     0
@@ -241,6 +265,11 @@ typedef struct RtSceneDesc {
     /* cylinders, cones, disks, infinite planes (may be 0 / NULL); ids follow the convex solids */
     int64_t        n_shapes;
     const RtShape* shapes;
+    /* textures and the triangles' texture coordinates and tangents (all may be 0 / NULL) */
+    int32_t          n_textures;
+    const RtTexture* textures;
+    const float*     tri_uv;        /* n_tris × 6: (u, v) at v0, v1, v2 */
+    const float*     tri_tangent;   /* n_tris × 9: per-vertex tangents (mesh.rs:33-54) */
 } RtSceneDesc;
 
 /* ── camera (src/camera.rs:24-59) ────────────────────────────────────────── */

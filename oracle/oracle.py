@@ -33,6 +33,8 @@ def lib():
         L.orc_scene_destroy.argtypes = [vp]
         L.orc_develop.argtypes = [fp, fp, C.POINTER(C.c_uint32), C.POINTER(abi.RtDevelopParams), C.POINTER(C.c_uint8)]
         L.orc_apply_optics.argtypes = [fp, C.c_uint32, C.c_uint32, C.c_float, C.c_float, fp]
+        L.orc_tex_sample.argtypes = [vp, i32, i32, fp, i64, fp]
+        L.orc_hit_uv.argtypes = [vp, fp, i64, fp]
         L.orc_pbr_scatter.argtypes = [C.POINTER(abi.RtMaterial), fp, i64, C.POINTER(i32), fp, fp, fp, fp, fp]
         L.orc_bvh_export.argtypes = [vp, fp, C.POINTER(i64), C.POINTER(i32), C.POINTER(i64)]
         L.orc_trace_closest.argtypes = [vp, fp, i64, C.POINTER(abi.RtHit), i32, i32]
@@ -208,6 +210,27 @@ class OracleScene:
         a = np.frombuffer(hits, dtype=np.dtype([("prim", np.int32), ("t", np.float32), ("b1", np.float32),
                                                 ("b2", np.float32)]))
         return a.copy()
+
+    def tex_sample(self, tex_id, uv, p=None, mode=-1):
+        """Texture::value (mode −1) or the PBR samplers (0 sRGB, 1 raw, 2 red)
+        at rows of (u, v) and points p."""
+        uv = np.asarray(uv, np.float32).reshape(-1, 2)
+        a = np.zeros((len(uv), 5), np.float32)
+        a[:, :2] = uv
+        if p is not None:
+            a[:, 2:] = np.asarray(p, np.float32).reshape(-1, 3)
+        out = np.zeros((len(uv), 3), np.float32)
+        rc = lib().orc_tex_sample(self.h, int(tex_id), int(mode), _fp(a), len(a), _fp(out))
+        if rc:
+            raise ValueError("bad texture id")
+        return out
+
+    def hit_uv(self, rays):
+        """(u, v, tangent xyz) of each ray's closest hit record."""
+        rays = _f(rays).reshape(-1, 8)
+        out = np.zeros((len(rays), 5), np.float32)
+        lib().orc_hit_uv(self.h, _fp(rays), len(rays), _fp(out))
+        return out
 
     def trace_any(self, rays, threads=os.cpu_count()):
         rays = _f(rays).reshape(-1, 8)

@@ -540,7 +540,7 @@ static inline float surface_area(const Aabb& b) {                               
     return 2.0f * (d.x * d.y + d.y * d.z + d.z * d.x);
 }
 
-struct Tri { V3 v0, e1, e2; V3 n0, n1, n2; bool has_n; int mat; };
+struct Tri { V3 v0, e1, e2; V3 n0, n1, n2; bool has_n; int mat; float uv[6]; V3 t0, t1, t2; };
 struct Quad { V3 q, u, v, normal, w; float d, area; int mat; };
 struct Sphere { V3 c; float r; int mat; };
 
@@ -590,6 +590,9 @@ struct Scene {
     };
     int64_t n_shapes = 0;
     std::vector<Shape> shapes;
+    // textures (texture.rs)
+    struct Texture { int32_t type, w, h; std::vector<uint8_t> px; float scale; V3 lo, hi; float vec[768]; int32_t perm[768]; };
+    std::vector<Texture> textures;
     // caustic photon map (photon.rs:31-36): implicit kd-tree, kept in emission order too
     struct KdPhoton { float pos[3], power[3], nor[3]; uint8_t axis; int32_t idx; };
     std::vector<KdPhoton> photons;    // kd order
@@ -1148,7 +1151,7 @@ static inline float medium_rnd(const MedRng& r, uint32_t i) {
 }
 
 // Perlin::noise / turb (perlin.rs:35-91)
-static float perlin_noise(const RtMedium& m, V3 p) {
+static float perlin_noise(const float* perlin_vec, const int32_t* perlin_perm, V3 p) {
     float fx = std::floor(p.x), fy = std::floor(p.y), fz = std::floor(p.z);
     float u = p.x - fx, v = p.y - fy, w = p.z - fz;
     u = u * u * (3.0f - 2.0f * u);
@@ -1159,9 +1162,9 @@ static float perlin_noise(const RtMedium& m, V3 p) {
     for (int di = 0; di < 2; di++)
         for (int dj = 0; dj < 2; dj++)
             for (int dk = 0; dk < 2; dk++) {
-                int idx = m.perlin_perm[(i + di) & 255] ^ m.perlin_perm[256 + ((j + dj) & 255)] ^
-                          m.perlin_perm[512 + ((k + dk) & 255)];
-                V3 c = v3(m.perlin_vec[idx * 3], m.perlin_vec[idx * 3 + 1], m.perlin_vec[idx * 3 + 2]);
+                int idx = perlin_perm[(i + di) & 255] ^ perlin_perm[256 + ((j + dj) & 255)] ^
+                          perlin_perm[512 + ((k + dk) & 255)];
+                V3 c = v3(perlin_vec[idx * 3], perlin_vec[idx * 3 + 1], perlin_vec[idx * 3 + 2]);
                 float fi = (float)di, fj = (float)dj, fk = (float)dk;
                 V3 wt = v3(u - fi, v - fj, w - fk);
                 accum += (fi * u + (1.0f - fi) * (1.0f - u)) * (fj * v + (1.0f - fj) * (1.0f - v)) *
@@ -1169,10 +1172,10 @@ static float perlin_noise(const RtMedium& m, V3 p) {
             }
     return accum;
 }
-static float perlin_turb(const RtMedium& m, V3 p, int depth) {
+static float perlin_turb(const float* perlin_vec, const int32_t* perlin_perm, V3 p, int depth) {
     float accum = 0.0f, weight = 1.0f;
     for (int i = 0; i < depth; i++) {
-        accum += weight * perlin_noise(m, p);
+        accum += weight * perlin_noise(perlin_vec, perlin_perm, p);
         weight *= 0.5f;
         p = v3(p.x * 2.0f, p.y * 2.0f, p.z * 2.0f);
     }
@@ -1181,7 +1184,7 @@ static float perlin_turb(const RtMedium& m, V3 p, int depth) {
 // NoiseMedium::density_at (volume.rs:188-191); density holds max(density, ε)
 // and threshold is clamped to [0, 0.99] at scene creation (volume.rs:180-184)
 static float medium_density_at(const RtMedium& m, V3 p) {
-    float n = perlin_turb(m, p * m.noise_scale, 7) * 0.5f;
+    float n = perlin_turb(m.perlin_vec, m.perlin_perm, p * m.noise_scale, 7) * 0.5f;
     return rmax(n - m.threshold, 0.0f) * m.density;
 }
 
@@ -1297,7 +1300,7 @@ static V3 hg_sample(V3 w, float g, float xi1, float xi2) {
 }
 
 // ── hit record (hittable.rs:73-94) ───────────────────────────────────────────
-struct Rec { V3 p, normal; float t, u, v; bool front; int mat; int32_t gid; };
+struct Rec { V3 p, normal, tangent; float t, u, v; bool front; int mat; int32_t gid; };
 
 static inline V3 sphere_uv_calc(V3 p, float* u, float* v) {                         // sphere.rs:11-15
     float theta = std::acos(clampf(-p.y, -1.0f, 1.0f));
@@ -1360,6 +1363,7 @@ static Aabb placed_box(const RtConvex& c) {                                     
 
 static Rec make_rec(const Scene& s, const Ray& r, const HitRes& h) {
     Rec rec;
+    rec.tangent = v3(0, 0, 0);
     rec.gid = h.gid; rec.t = h.t;
     rec.p = r.o + h.t * r.d;
     V3 outward;
@@ -1373,7 +1377,18 @@ static Rec make_rec(const Scene& s, const Ray& r, const HitRes& h) {
         } else {
             outward = unit(cross(tr.e1, tr.e2));
         }
-        rec.u = h.b1; rec.v = h.b2;   // no UVs in the flat description: barycentrics
+        rec.u = b0 * tr.uv[0] + h.b1 * tr.uv[2] + h.b2 * tr.uv[4];
+        rec.v = b0 * tr.uv[1] + h.b1 * tr.uv[3] + h.b2 * tr.uv[5];
+        // Gram-Schmidt against the shading normal, onb fallback
+        V3 rt = b0 * tr.t0 + h.b1 * tr.t1 + h.b2 * tr.t2;
+        rt = rt - outward * dot(rt, outward);
+        if (len2(rt) > 1e-8f) {
+            rec.tangent = unit(rt);
+        } else {
+            V3 ou, ov;
+            onb_vec(outward, &ou, &ov);
+            rec.tangent = ou;
+        }
         rec.mat = tr.mat;
     } else if (t == RT_PRIM_QUAD) {
         const Quad& q = s.quads[h.gid - s.n_tris];
@@ -1753,6 +1768,64 @@ static V3 photon_irradiance(const Scene& s, V3 p, V3 n) {
     return acc * (2.0f / (PI_F * PI_F * r2));
 }
 
+// ── textures (texture.rs:25-57, material.rs:633-786) ──────────────────────────
+static float srgb_decode(uint8_t c) {                                               // output.rs:90-96
+    float v = (float)c / 255.0f;
+    return v <= 0.04045f ? v / 12.92f : std::pow((v + 0.055f) / 1.055f, 2.4f);
+}
+// Texture::value: the nearest texel sRGB-decoded, or the Perlin mottle
+static V3 tex_value(const Scene& s, int id, float u, float v, V3 p) {
+    const Scene::Texture& t = s.textures[id - 1];
+    if (t.type == RT_TEX_MOTTLE) {
+        float m = clampf(2.0f * perlin_turb(t.vec, t.perm, v3(p.x * t.scale, p.y * t.scale, p.z * t.scale), 7), 0.0f, 1.0f);
+        return t.lo * (1.0f - m) + t.hi * m;
+    }
+    float uu = clampf(u, 0.0f, 1.0f), vv = 1.0f - clampf(v, 0.0f, 1.0f);
+    uint32_t x = std::min((uint32_t)(uu * (float)t.w), (uint32_t)t.w - 1u);
+    uint32_t y = std::min((uint32_t)(vv * (float)t.h), (uint32_t)t.h - 1u);
+    const uint8_t* q = t.px.data() + ((size_t)y * t.w + x) * 3;
+    return v3(srgb_decode(q[0]), srgb_decode(q[1]), srgb_decode(q[2]));
+}
+// bilinear_coords + sample_srgb (mode 0) / sample_rgb (1) / sample_linear (2)
+static V3 tex_bilinear(const Scene& s, int id, float u, float v, int mode) {
+    const Scene::Texture& t = s.textures[id - 1];
+    float uu = clampf(u, 0.0f, 1.0f), vv = 1.0f - clampf(v, 0.0f, 1.0f);
+    float fx = clampf(uu * (float)t.w - 0.5f, 0.0f, (float)(t.w - 1));
+    float fy = clampf(vv * (float)t.h - 0.5f, 0.0f, (float)(t.h - 1));
+    uint32_t x0 = (uint32_t)fx, y0 = (uint32_t)fy;
+    uint32_t x1 = std::min(x0 + 1u, (uint32_t)t.w - 1u), y1 = std::min(y0 + 1u, (uint32_t)t.h - 1u);
+    float tx = fx - (float)x0, ty = fy - (float)y0;
+    auto px = [&](uint32_t x, uint32_t y) {
+        const uint8_t* q = t.px.data() + ((size_t)y * t.w + x) * 3;
+        if (mode == 0) return v3(srgb_decode(q[0]), srgb_decode(q[1]), srgb_decode(q[2]));
+        if (mode == 1) return v3((float)q[0] / 255.0f, (float)q[1] / 255.0f, (float)q[2] / 255.0f);
+        float r = (float)q[0] / 255.0f;
+        return v3(r, r, r);
+    };
+    V3 c0 = px(x0, y0) * (1.0f - tx) + px(x1, y0) * tx;
+    V3 c1 = px(x0, y1) * (1.0f - tx) + px(x1, y1) * tx;
+    return c0 * (1.0f - ty) + c1 * ty;
+}
+// PbrMaterial::params (material.rs:758-786) as a copy of the material with the
+// mapped albedo (× ao), roughness and metallic; *sn the normal-mapped normal
+static RtMaterial pbr_params(const Scene& s, const RtMaterial& m, const Rec& rec, V3* sn) {
+    RtMaterial h = m;
+    *sn = rec.normal;
+    if (m.normal_tex && len2(rec.tangent) > 1e-6f) {                                // tbn_normal
+        V3 raw = tex_bilinear(s, m.normal_tex, rec.u, rec.v, 1);
+        V3 ts = v3(raw.x * 2.0f - 1.0f, raw.y * 2.0f - 1.0f, raw.z * 2.0f - 1.0f);
+        V3 ng = rec.normal, t = rec.tangent, b = cross(ng, t);
+        V3 pert = t * ts.x + b * ts.y + ng * ts.z;
+        if (len2(pert) > 1e-12f) *sn = unit(pert);
+    }
+    V3 a = m.albedo_tex ? tex_bilinear(s, m.albedo_tex, rec.u, rec.v, 0) : v3(m.albedo[0], m.albedo[1], m.albedo[2]);
+    if (m.ao_tex) a = a * tex_bilinear(s, m.ao_tex, rec.u, rec.v, 2).x;
+    h.albedo[0] = a.x; h.albedo[1] = a.y; h.albedo[2] = a.z;
+    if (m.roughness_tex) h.roughness = tex_bilinear(s, m.roughness_tex, rec.u, rec.v, 2).x;
+    if (m.metallic_tex) h.metallic = tex_bilinear(s, m.metallic_tex, rec.u, rec.v, 2).x;
+    return h;
+}
+
 // trace_photon (photon.rs:232-277): one wavelength per photon, at most 12
 // bounces; stored at the first diffuse hit after ≥ 1 specular bounce.  Each new
 // segment is a fresh ray (spectral_weighted = false), so every refraction of a
@@ -1853,8 +1926,9 @@ static bool trace_photon(const Scene& s, V3 pos, V3 dir, float lum_clamp, V3 pow
         } else if (m.type == RT_MAT_PBR) {
             // PbrMaterial::scatter: a specular lobe carries the photon on, the
             // diffuse lobe stores it where can_receive_caustics (material.rs:1049)
-            V3 att, nd;
-            int lobe = pbr_scatter(m, unit(-ray.d), rec.normal, rnd(rng, base + 2), rnd(rng, base + 3),
+            V3 att, nd, sn;
+            RtMaterial mh = pbr_params(s, m, rec, &sn);
+            int lobe = pbr_scatter(mh, unit(-ray.d), sn, rnd(rng, base + 2), rnd(rng, base + 3),
                                    rnd(rng, base + 0), rnd(rng, base + 1), &att, &nd);
             if (lobe == PBR_NONE) return false;
             if (lobe == PBR_SPECULAR) {
@@ -2016,7 +2090,9 @@ static V3 emission(const Scene& s, int mat, const SpecState& ss) {
 static inline bool is_emissive_mat(const RtMaterial& m) {
     return m.type == RT_MAT_DIFFUSE_LIGHT || m.type == RT_MAT_BLACKBODY_LIGHT;
 }
-static inline V3 lambert_albedo(const RtMaterial& m, V3 p) {                        // texture.rs:28-37
+static inline V3 lambert_albedo(const Scene& s, const RtMaterial& m, const Rec& rec) {   // texture.rs:28-57
+    if (m.albedo_tex) return tex_value(s, m.albedo_tex, rec.u, rec.v, rec.p);
+    V3 p = rec.p;
     if (m.type == RT_MAT_CHECKER) {
         int x = (int)std::floor(m.checker_scale * p.x);
         int y = (int)std::floor(m.checker_scale * p.y);
@@ -2187,15 +2263,17 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
             // Lambertian / checker (material.rs:85-102) or PbrMaterial
             // (material.rs:790-920): diffuse branch renderer.rs:457-572
             V3 att, hint;   // scatter attenuation; albedo_hint for the caustic term
+            V3 sn = rec.normal;   // the shading normal (a PBR normal map tilts it)
             bool diffuse = true;
             if (m.type == RT_MAT_PBR) {
                 // the emission adds at the hit (renderer.rs:415-417), then one lobe scatters
                 color = color + T * emission(s, rec.mat, ss) * emit_w;
+                RtMaterial mh = pbr_params(s, m, rec, &sn);
                 V3 wo = unit(-ray.d), dir;
-                int lobe = pbr_scatter(m, wo, rec.normal, rnd(rng, base + B_LOBE0), rnd(rng, base + B_LOBE1),
+                int lobe = pbr_scatter(mh, wo, sn, rnd(rng, base + B_LOBE0), rnd(rng, base + B_LOBE1),
                                        rnd(rng, base + B_SCATTER0), rnd(rng, base + B_SCATTER1), &att, &dir);
                 if (lobe == PBR_NONE) break;
-                hint = v3(m.albedo[0], m.albedo[1], m.albedo[2]);
+                hint = v3(mh.albedo[0], mh.albedo[1], mh.albedo[2]);
                 if (lobe == PBR_SPECULAR) {
                     // specular sun NEE (renderer.rs:421-456)
                     prev_spec_sun_weight = 1.0f;
@@ -2206,15 +2284,15 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                         (*n_shadow)++;
                         float tr = scene_transmittance(s, Ray{rec.p, sun_s}, 0.001f, INFINITY);
                         if (tr > 0.0f) {
-                            V3 bc = pbr_specular_brdf_cos(m, wo, rec.normal, sun_s);
+                            V3 bc = pbr_specular_brdf_cos(mh, wo, sn, sun_s);
                             if (bc.x > 0.0f || bc.y > 0.0f || bc.z > 0.0f) {
-                                float p_mat = pbr_specular_pdf(m, wo, rec.normal, sun_s);
+                                float p_mat = pbr_specular_pdf(mh, wo, sn, sun_s);
                                 V3 sun_color = bg_eval(s, sun_s) * spec_factor(s.spec, ss);
                                 float mis_d = p_sun * p_sun + p_mat * p_mat;
                                 if (mis_d > 0.0f) color = color + T * tr * bc * sun_color * p_sun / mis_d;
                             }
                         }
-                        float p_b = pbr_specular_pdf(m, wo, rec.normal, dir);
+                        float p_b = pbr_specular_pdf(mh, wo, sn, dir);
                         if (p_b > 0.0f) prev_spec_sun_weight = (p_b * p_b) / rmax(p_b * p_b + p_sun * p_sun, 1e-8f);
                     }
                     T = T * att;
@@ -2224,7 +2302,7 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                     diffuse = false;
                 }
             } else {
-                att = lambert_albedo(m, rec.p);
+                att = lambert_albedo(s, m, rec);
                 hint = att;
             }
             if (diffuse) {
@@ -2243,7 +2321,7 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                         float tr = scene_transmittance(s, shadow, 0.001f, lrec.t * (1.0f - 1e-4f));
                         if (tr > 0.0f) {
                             float l_pdf = lights_pdf_value(s, rec.p, light_dir);
-                            float brdf = rmax(dot(rec.normal, unit(light_dir)) / PI_F, 0.0f);
+                            float brdf = rmax(dot(sn, unit(light_dir)) / PI_F, 0.0f);
                             float sun_p = sun_pdf_value(s, light_dir);
                             float env_p = env_pdf_value(s, light_dir);
                             float mis_d = l_pdf * l_pdf + brdf * brdf + sun_p * sun_p + env_p * env_p;
@@ -2259,7 +2337,7 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                     (*n_shadow)++;
                     float tr = scene_transmittance(s, Ray{rec.p, sun_s}, 0.001f, INFINITY);
                     if (tr > 0.0f) {
-                        float brdf = rmax(dot(rec.normal, unit(sun_s)) / PI_F, 0.0f);
+                        float brdf = rmax(dot(sn, unit(sun_s)) / PI_F, 0.0f);
                         if (brdf > 0.0f) {
                             float sun_pdf = 1.0f / (2.0f * PI_F * (1.0f - COS_SUN_MAX));
                             V3 sun_color = bg_eval(s, sun_s) * spec_factor(s.spec, ss);
@@ -2278,7 +2356,7 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                         (*n_shadow)++;
                         float tr = scene_transmittance(s, shadow, 0.001f, INFINITY);
                         if (tr > 0.0f) {
-                            float brdf = rmax(dot(rec.normal, unit(env_dir)) / PI_F, 0.0f);
+                            float brdf = rmax(dot(sn, unit(env_dir)) / PI_F, 0.0f);
                             if (brdf > 0.0f) {
                                 float area_pdf = have_lights ? lights_pdf_value(s, rec.p, env_dir) : 0.0f;
                                 V3 env_color = env_eval(s, env_dir) * spec_factor(s.spec, ss);
@@ -2289,14 +2367,14 @@ static V3 ray_color(const Scene& s, Ray ray, const Rng& rng, SpecState ss, uint3
                     }
                 }
                 // indirect: cosine-weighted sample (pdf.rs:12-41)
-                Onb uvw = onb_from_w(rec.normal);
+                Onb uvw = onb_from_w(sn);
                 float r1 = rnd(rng, base + B_COS0), r2 = rnd(rng, base + B_COS1);
                 float phi = 2.0f * PI_F * r1;
                 float sq = std::sqrt(r2);
                 V3 ind_dir = onb_local(uvw, v3(std::cos(phi) * sq, std::sin(phi) * sq, std::sqrt(1.0f - r2)));
                 float pdf_val = rmax(dot(unit(ind_dir), uvw.w) / PI_F, 0.0f);
                 if (pdf_val <= 0.0f) break;
-                float scat_pdf = rmax(dot(rec.normal, unit(ind_dir)) / PI_F, 0.0f);
+                float scat_pdf = rmax(dot(sn, unit(ind_dir)) / PI_F, 0.0f);
                 if (scat_pdf <= 0.0f) break;
                 if (dot(ind_dir, rec.normal) <= 0.0f) break;
                 float area = have_lights ? lights_pdf_value(s, rec.p, ind_dir) : 0.0f;
@@ -2399,6 +2477,26 @@ static int scene_create(const RtSceneDesc* d, Scene** out) {
             t.n0 = v3(n[0], n[1], n[2]); t.n1 = v3(n[3], n[4], n[5]); t.n2 = v3(n[6], n[7], n[8]);
         }
         t.mat = d->tri_mat[i];
+        // texture coordinates and tangents, or mesh.rs:75-81's defaults
+        static const float duv[6] = {0.0f, 0.0f, 1.0f, 0.0f, 0.5f, 1.0f};
+        const float* uv = d->tri_uv ? d->tri_uv + i * 6 : duv;
+        for (int k = 0; k < 6; k++) t.uv[k] = uv[k];
+        if (d->tri_uv && d->tri_tangent) {
+            const float* g = d->tri_tangent + i * 9;
+            t.t0 = v3(g[0], g[1], g[2]); t.t1 = v3(g[3], g[4], g[5]); t.t2 = v3(g[6], g[7], g[8]);
+        } else {
+            t.t0 = t.t1 = t.t2 = v3(1, 0, 0);
+        }
+    }
+    // textures (texture.rs): image texels, or a mottle's Perlin tables
+    for (int32_t i = 0; i < d->n_textures; i++) {
+        const RtTexture& t = d->textures[i];
+        Scene::Texture x;
+        x.type = t.type; x.w = t.width; x.h = t.height; x.scale = t.scale;
+        x.lo = v3(t.lo[0], t.lo[1], t.lo[2]); x.hi = v3(t.hi[0], t.hi[1], t.hi[2]);
+        if (t.type == RT_TEX_IMAGE) x.px.assign(t.rgb8, t.rgb8 + (size_t)t.width * t.height * 3);
+        else { memcpy(x.vec, t.perlin_vec, sizeof(x.vec)); memcpy(x.perm, t.perlin_perm, sizeof(x.perm)); }
+        s->textures.push_back(std::move(x));
     }
     s->quads.resize(d->n_quads);
     for (int64_t i = 0; i < d->n_quads; i++) {                                      // quad.rs:21-33
@@ -2787,6 +2885,33 @@ int32_t orc_apply_optics(const float* img, uint32_t w, uint32_t h, float vignett
             }
             out[i * 3] = c.x; out[i * 3 + 1] = c.y; out[i * 3 + 2] = c.z;
         }
+    return RT_OK;
+}
+
+// Texture lookups for tests: rows of (u, v, px, py, pz) → RGB; mode −1 is
+// Texture::value, 0/1/2 the PBR bilinear samplers (sRGB, raw, red channel)
+int32_t orc_tex_sample(void* sp, int32_t id, int32_t mode, const float* in, int64_t n, float* out) {
+    Scene* s = (Scene*)sp;
+    if (id < 1 || id > (int32_t)s->textures.size()) return RT_ERR_INVALID;
+    for (int64_t i = 0; i < n; i++) {
+        const float* a = in + i * 5;
+        V3 c = mode < 0 ? tex_value(*s, id, a[0], a[1], v3(a[2], a[3], a[4])) : tex_bilinear(*s, id, a[0], a[1], mode);
+        out[i * 3] = c.x; out[i * 3 + 1] = c.y; out[i * 3 + 2] = c.z;
+    }
+    return RT_OK;
+}
+// The hit record's (u, v) and tangent for rays: n × 8 rays → n × 5 (u, v, tangent)
+int32_t orc_hit_uv(void* sp, const float* rays, int64_t n, float* out) {
+    Scene* s = (Scene*)sp;
+    for (int64_t i = 0; i < n; i++) {
+        const float* r = rays + i * 8;
+        Ray ray{v3(r[0], r[1], r[2]), v3(r[3], r[4], r[5])};
+        HitRes h = closest_hit<false>(*s, ray, r[6], r[7], nullptr);
+        float* o = out + i * 5;
+        if (h.gid < 0) { for (int k = 0; k < 5; k++) o[k] = 0.0f; continue; }
+        Rec rec = make_rec(*s, ray, h);
+        o[0] = rec.u; o[1] = rec.v; o[2] = rec.tangent.x; o[3] = rec.tangent.y; o[4] = rec.tangent.z;
+    }
     return RT_OK;
 }
 

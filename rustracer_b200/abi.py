@@ -54,6 +54,29 @@ class RtMaterial(C.Structure):
         ("sheen_tint", C.c_float),
         ("emission", F3),
         ("emission_strength", C.c_float),
+        ("albedo_tex", C.c_int32),
+        ("roughness_tex", C.c_int32),
+        ("metallic_tex", C.c_int32),
+        ("ao_tex", C.c_int32),
+        ("normal_tex", C.c_int32),
+    ]
+
+
+RT_TEX_IMAGE = 0
+RT_TEX_MOTTLE = 1
+
+
+class RtTexture(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("width", C.c_int32),
+        ("height", C.c_int32),
+        ("rgb8", C.POINTER(C.c_uint8)),
+        ("scale", C.c_float),
+        ("lo", F3),
+        ("hi", F3),
+        ("perlin_vec", C.c_float * 768),
+        ("perlin_perm", C.c_int32 * 768),
     ]
 
 
@@ -160,6 +183,10 @@ class RtSceneDesc(C.Structure):
         ("convex_planes", C.POINTER(C.c_float)),
         ("n_shapes", C.c_int64),
         ("shapes", C.POINTER(RtShape)),
+        ("n_textures", C.c_int32),
+        ("textures", C.POINTER(RtTexture)),
+        ("tri_uv", C.POINTER(C.c_float)),
+        ("tri_tangent", C.POINTER(C.c_float)),
     ]
 
 

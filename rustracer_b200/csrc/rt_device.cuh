@@ -62,6 +62,7 @@ struct DevMaterial {
     float metallic, aniso_c, aniso_s, aspect;
     float clearcoat, clearcoat_roughness, film_thickness, film_ior, sheen, sheen_tint;
     float emission[3];   // emission × emission_strength
+    int albedo_tex, roughness_tex, metallic_tex, ao_tex, normal_tex;   // 1-based, 0 = none
 };
 
 struct DevLight {        // one entry of the NEE light list (hittable.rs:138-225)
@@ -82,6 +83,16 @@ struct DevMedium {
     float g, noise_scale, threshold;
     float3 color;
     const float4* vec;           // 256 Perlin vectors
+    const int32_t* perm;         // 3 × 256 permutations
+};
+
+// A texture (texture.rs): an 8-bit RGB image, or a Perlin mottle between two colours
+struct DevTexture {
+    int type, w, h;              // RT_TEX_*
+    const uint8_t* px;           // IMAGE: h × w × 3
+    float scale;
+    float3 lo, hi;
+    const float4* vec;           // MOTTLE: 256 Perlin vectors
     const int32_t* perm;         // 3 × 256 permutations
 };
 
@@ -110,6 +121,12 @@ struct DevScene {
     // (see shape_test)
     const float4* shape_par;
     int n_analytic;             // convex solids + shapes (the traversal compiles their tests in only if > 0)
+    // textures; per triangle 2 float4 of (u, v) at the corners and 3 float4 of
+    // corner tangents (NULL: the reference's default UVs and (1, 0, 0) tangents)
+    const DevTexture* tex;
+    const float* srgb_lut;      // 256 sRGB → linear values (output.rs:90-96)
+    const float4* tri_uv;
+    const float4* tri_tan;
     // spectral tables: CIE x̄ȳz̄ on the 5 nm grid from 380 nm and the per-channel
     // normalisations of spectral_to_rgb / spectral_fire_rgb (spectrum.rs:78-177)
     const float4* cmf;          // n_spec entries (x, y, z, -)

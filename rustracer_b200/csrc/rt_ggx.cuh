@@ -97,14 +97,24 @@ RT_D float3 nacre_color(const DevScene& S, float ct, float film_ior, float thick
     float blend = powf(ct, 0.5f);
     return raw * blend + mk(0.5f, 0.5f, 0.5f) * (1.0f - blend);
 }
-RT_D float3 pbr_f0(const DevMaterial& m) {
-    return mk(0.04f, 0.04f, 0.04f) * (1.0f - m.metallic) + mk(m.albedo[0], m.albedo[1], m.albedo[2]) * m.metallic;
+// the per-hit PBR parameters (ShadingParams, material.rs:773-786): albedo,
+// roughness and metallic from the scalars or the texture maps
+struct PbrHit { float3 albedo; float roughness, metallic; };
+RT_D PbrHit pbr_scalars(const DevMaterial& m) {
+    PbrHit h;
+    h.albedo = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
+    h.roughness = m.roughness;
+    h.metallic = m.metallic;
+    return h;
+}
+RT_D float3 pbr_f0(const PbrHit& h) {
+    return mk(0.04f, 0.04f, 0.04f) * (1.0f - h.metallic) + h.albedo * h.metallic;
 }
 RT_D float pbr_p_coat(const DevMaterial& m, float cos_o) {
     return m.clearcoat > 1e-3f ? fmaxf(schlick(cos_o, 1.0f / 1.5f) * m.clearcoat, 0.12f * m.clearcoat) : 0.0f;
 }
-RT_D float pbr_p_spec(const DevMaterial& m, float3 f0, float cos_o) {
-    return m.metallic > 0.999f ? 1.0f : clampf_(lum3(schlick_rgb(cos_o, f0)), 0.04f, 0.9f);
+RT_D float pbr_p_spec(const PbrHit& h, float3 f0, float cos_o) {
+    return h.metallic > 0.999f ? 1.0f : clampf_(lum3(schlick_rgb(cos_o, f0)), 0.04f, 0.9f);
 }
 // the anisotropic base-lobe frame: the onb rotated by anisotropy_angle
 RT_D void pbr_frame(const DevMaterial& m, float3 n, float3* t, float3* b) {
@@ -118,15 +128,15 @@ enum { PBR_NONE = 0, PBR_SPECULAR = 1, PBR_DIFFUSE = 2 };
 // PbrMaterial::scatter (material.rs:790-920): the coat, base-specular or
 // diffuse(+sheen) lobe, chosen by xi_coat / xi_spec; xi1, xi2 sample the VNDF.
 // Returns the lobe, its attenuation and (specular lobes) its direction.
-RT_D int pbr_scatter(const DevScene& S, const DevMaterial& m, float3 wo, float3 n, float xi_coat, float xi_spec,
-                     float xi1, float xi2, float3* att, float3* dir) {
+RT_D int pbr_scatter(const DevScene& S, const DevMaterial& m, const PbrHit& ph, float3 wo, float3 n, float xi_coat,
+                     float xi_spec, float xi1, float xi2, float3* att, float3* dir) {
     float cos_o = dot3(wo, n);
     if (cos_o <= 0.0f) return PBR_NONE;
-    float alpha = fmaxf(m.roughness * m.roughness, 1e-4f);
-    float3 albedo = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
-    float3 f0 = pbr_f0(m);
+    float alpha = fmaxf(ph.roughness * ph.roughness, 1e-4f);
+    float3 albedo = ph.albedo;
+    float3 f0 = pbr_f0(ph);
     float p_coat = pbr_p_coat(m, cos_o);
-    float p_spec = pbr_p_spec(m, f0, cos_o);
+    float p_spec = pbr_p_spec(ph, f0, cos_o);
     if (xi_coat < p_coat) {
         float ac = fmaxf(m.clearcoat_roughness * m.clearcoat_roughness, 1e-4f);
         float3 t, b;
@@ -164,25 +174,26 @@ RT_D int pbr_scatter(const DevScene& S, const DevMaterial& m, float3 wo, float3 
         return PBR_SPECULAR;
     }
     float3 sheen = mk(0.f, 0.f, 0.f);
-    if (m.sheen > 0.0f && m.metallic < 0.999f) {
+    if (m.sheen > 0.0f && ph.metallic < 0.999f) {
         float l = lum3(albedo);
         float3 c_tint = l > 1e-6f ? albedo / l : mk(1.f, 1.f, 1.f);
         float3 sc = mk(1.f, 1.f, 1.f) * (1.0f - m.sheen_tint) + c_tint * m.sheen_tint;
         float u = 1.0f - cos_o, f_h = u * u * u * u * u;
-        sheen = sc * (m.sheen * (1.0f - m.metallic) * f_h * PI_F);
+        sheen = sc * (m.sheen * (1.0f - ph.metallic) * f_h * PI_F);
     }
-    *att = (albedo * (1.0f - m.metallic) + sheen) / ((1.0f - p_spec) * (1.0f - p_coat));
+    *att = (albedo * (1.0f - ph.metallic) + sheen) / ((1.0f - p_spec) * (1.0f - p_coat));
     return PBR_DIFFUSE;
 }
 // PbrMaterial::specular_brdf_cos and specular_sampling_pdf (material.rs:935-1047)
-RT_D float3 pbr_spec_brdf_cos(const DevScene& S, const DevMaterial& m, float3 wo, float3 n, float3 wi, float* pdf) {
+RT_D float3 pbr_spec_brdf_cos(const DevScene& S, const DevMaterial& m, const PbrHit& ph, float3 wo, float3 n,
+                              float3 wi, float* pdf) {
     *pdf = 0.0f;
     float cos_o = dot3(wo, n), cos_i = dot3(wi, n);
     if (cos_o <= 0.0f || cos_i <= 0.0f) return mk(0.f, 0.f, 0.f);
     float3 h = unit3(wo + wi);
     float wo_h = fmaxf(dot3(wo, h), 0.0f), h_n = fmaxf(dot3(h, n), 0.0f);
-    float3 f0 = pbr_f0(m);
-    float p_coat = pbr_p_coat(m, cos_o), p_spec = pbr_p_spec(m, f0, cos_o);
+    float3 f0 = pbr_f0(ph);
+    float p_coat = pbr_p_coat(m, cos_o), p_spec = pbr_p_spec(ph, f0, cos_o);
     float3 res = mk(0.f, 0.f, 0.f);
     float pd = 0.0f;
     if (m.clearcoat > 1e-3f) {
@@ -194,7 +205,7 @@ RT_D float3 pbr_spec_brdf_cos(const DevScene& S, const DevMaterial& m, float3 wo
         res = res + film * (d * fc * g2 / (4.0f * cos_o) * energy_comp(S, cos_o, ac));
         pd += p_coat * d * smith_g1(cos_o, ac) / (4.0f * cos_o);
     }
-    float alpha = fmaxf(m.roughness * m.roughness, 1e-4f);
+    float alpha = fmaxf(ph.roughness * ph.roughness, 1e-4f);
     float ax = alpha / m.aspect, ay = alpha * m.aspect;
     float3 t, b;
     pbr_frame(m, n, &t, &b);
@@ -210,9 +221,9 @@ RT_D float3 pbr_spec_brdf_cos(const DevScene& S, const DevMaterial& m, float3 wo
     return res;
 }
 // specular_sampling_pdf alone, for the MIS weight of a sampled specular bounce
-RT_D float pbr_spec_pdf(const DevScene& S, const DevMaterial& m, float3 wo, float3 n, float3 wi) {
+RT_D float pbr_spec_pdf(const DevScene& S, const DevMaterial& m, const PbrHit& ph, float3 wo, float3 n, float3 wi) {
     float pdf;
-    pbr_spec_brdf_cos(S, m, wo, n, wi, &pdf);
+    pbr_spec_brdf_cos(S, m, ph, wo, n, wi, &pdf);
     return pdf;
 }
 

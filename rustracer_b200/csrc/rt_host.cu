@@ -703,6 +703,32 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
             (q.type != RT_SHAPE_PLANE && !(q.radius > 0.0f)) || (!planar && !(q.height > 0.0f)))
             return bail(fail(s, RT_ERR_INVALID, what + ": positive scale, radius and height, a non-zero normal, a rotation"));
     }
+    if (d->tri_uv && !d->tri_tangent) return bail(fail(s, RT_ERR_INVALID, "tri_uv needs tri_tangent"));
+    if (d->n_textures < 0 || (d->n_textures > 0 && !d->textures)) return bail(fail(s, RT_ERR_INVALID, "bad texture list"));
+    for (int32_t i = 0; i < d->n_textures; i++) {
+        const RtTexture& t = d->textures[i];
+        bool ok = t.type == RT_TEX_IMAGE ? (t.width > 0 && t.height > 0 && t.rgb8 && (int64_t)t.width * t.height < (1ll << 31))
+                : t.type == RT_TEX_MOTTLE ? std::isfinite(t.scale) : false;
+        for (int k = 0; ok && t.type == RT_TEX_MOTTLE && k < 768; k++)
+            ok = t.perlin_perm[k] >= 0 && t.perlin_perm[k] < 256 && std::isfinite(t.perlin_vec[k]);
+        if (!ok) return bail(fail(s, RT_ERR_INVALID, "texture " + std::to_string(i) + ": bad image or mottle tables"));
+    }
+    for (int32_t i = 0; i < d->n_mats; i++) {
+        const RtMaterial& m = d->mats[i];
+        const int32_t ids[] = {m.albedo_tex, m.roughness_tex, m.metallic_tex, m.ao_tex, m.normal_tex};
+        for (int32_t id : ids)
+            if (id < 0 || id > d->n_textures) return bail(fail(s, RT_ERR_INVALID, "material texture id out of range"));
+        if ((m.roughness_tex || m.metallic_tex || m.ao_tex || m.normal_tex) && m.type != RT_MAT_PBR)
+            return bail(fail(s, RT_ERR_INVALID, "only PBR materials take roughness / metallic / ao / normal maps"));
+        if (m.albedo_tex && m.type != RT_MAT_PBR && m.type != RT_MAT_LAMBERTIAN)
+            return bail(fail(s, RT_ERR_INVALID, "albedo maps belong to Lambertian or PBR materials"));
+        if (m.type == RT_MAT_PBR && (m.roughness_tex || m.metallic_tex || m.ao_tex || m.normal_tex || m.albedo_tex)) {
+            const int32_t maps[] = {m.albedo_tex, m.roughness_tex, m.metallic_tex, m.ao_tex, m.normal_tex};
+            for (int32_t id : maps)
+                if (id && d->textures[id - 1].type != RT_TEX_IMAGE)
+                    return bail(fail(s, RT_ERR_INVALID, "PBR maps must be image textures"));
+        }
+    }
     if (d->bg.type == RT_BG_ENVMAP && (!d->bg.env_rgb || d->bg.env_w <= 0 || d->bg.env_h <= 0))
         return bail(fail(s, RT_ERR_INVALID, "env map background without an image"));
 
@@ -768,7 +794,7 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
 
     // ── BVH ─────────────────────────────────────────────────────────────────
     std::vector<float4> gnodes;
-    std::vector<float4> gtri, gtri_n, gquad, gsph;
+    std::vector<float4> gtri, gtri_n, gquad, gsph, gtri_uv, gtri_tan;
     if (n > 0) {
         SahBuilder B(boxes);
         B.build_wide();
@@ -840,8 +866,19 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         gtri.resize(order_tri.size() * 3);
         bool has_n = d->tri_n != nullptr;
         if (has_n) gtri_n.resize(order_tri.size() * 3);
+        bool has_uv = d->tri_uv != nullptr;
+        if (has_uv) { gtri_uv.resize(order_tri.size() * 2); gtri_tan.resize(order_tri.size() * 3); }
         for (size_t k = 0; k < order_tri.size(); k++) {
             int64_t g = order_tri[k];
+            if (has_uv) {
+                const float* u = d->tri_uv + g * 6;
+                gtri_uv[k * 2] = make_float4(u[0], u[1], u[2], u[3]);
+                gtri_uv[k * 2 + 1] = make_float4(u[4], u[5], 0.f, 0.f);
+                const float* t = d->tri_tangent + g * 9;
+                gtri_tan[k * 3] = make_float4(t[0], t[1], t[2], t[3]);
+                gtri_tan[k * 3 + 1] = make_float4(t[4], t[5], t[6], t[7]);
+                gtri_tan[k * 3 + 2] = make_float4(t[8], 0.f, 0.f, 0.f);
+            }
             const float* v = d->tri_v + g * 9;
             H3 a = h3(v[0], v[1], v[2]);
             H3 e1 = h3(v[3], v[4], v[5]) - a, e2 = h3(v[6], v[7], v[8]) - a;
@@ -928,6 +965,10 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         if ((rc = upload(s, gnodes.data(), gnodes.size(), &s->S.nodes))) return bail(rc);
         if ((rc = upload(s, gtri.data(), gtri.size(), &s->S.tri))) return bail(rc);
         if ((rc = upload(s, gtri_n.data(), gtri_n.size(), &s->S.tri_n))) return bail(rc);
+        if (!gtri_uv.empty()) {
+            if ((rc = upload(s, gtri_uv.data(), gtri_uv.size(), &s->S.tri_uv))) return bail(rc);
+            if ((rc = upload(s, gtri_tan.data(), gtri_tan.size(), &s->S.tri_tan))) return bail(rc);
+        }
         if ((rc = upload(s, gquad.data(), gquad.size(), &s->S.quad))) return bail(rc);
         if ((rc = upload(s, gsph.data(), gsph.size(), &s->S.sphere))) return bail(rc);
         if ((rc = upload(s, lights.data(), lights.size(), &s->S.lights))) return bail(rc);
@@ -982,6 +1023,8 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
                 for (int k = 0; k < RT_METAL_NK_N; k++) { g.nk_n[k] = RT_METAL_NK[m.metal][0][k]; g.nk_k[k] = RT_METAL_NK[m.metal][1][k]; }
             }
         }
+        g.albedo_tex = m.albedo_tex; g.roughness_tex = m.roughness_tex; g.metallic_tex = m.metallic_tex;
+        g.ao_tex = m.ao_tex; g.normal_tex = m.normal_tex;
         if (m.type == RT_MAT_PBR) {                                                 // material.rs:790-800
             g.metallic = m.metallic;
             g.aniso_c = std::cos(m.anisotropy_angle);
@@ -1102,6 +1145,35 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     if ((rc = upload(s, g_elut, (size_t)64 * 64, &s->S.elut))) return bail(rc);
     std::call_once(g_nacre_once, build_nacre);
     if ((rc = upload(s, g_nacre, (size_t)256, &s->S.nacre))) return bail(rc);
+
+    // ── textures (texture.rs, output.rs:90-96 sRGB decode table) ─────────────
+    {
+        float lut[256];
+        for (int c = 0; c < 256; c++) {
+            float v = (float)c / 255.0f;
+            lut[c] = v <= 0.04045f ? v / 12.92f : std::pow((v + 0.055f) / 1.055f, 2.4f);
+        }
+        if ((rc = upload(s, lut, (size_t)256, &s->S.srgb_lut))) return bail(rc);
+        std::vector<DevTexture> dt(std::max(d->n_textures, 1));
+        for (int32_t i = 0; i < d->n_textures; i++) {
+            const RtTexture& t = d->textures[i];
+            DevTexture& g = dt[i];
+            memset(&g, 0, sizeof(g));
+            g.type = t.type; g.w = t.width; g.h = t.height; g.scale = t.scale;
+            g.lo = make_float3(t.lo[0], t.lo[1], t.lo[2]);
+            g.hi = make_float3(t.hi[0], t.hi[1], t.hi[2]);
+            if (t.type == RT_TEX_IMAGE) {
+                if ((rc = upload(s, t.rgb8, (size_t)t.width * t.height * 3, &g.px))) return bail(rc);
+            } else {
+                std::vector<float4> vec(256);
+                for (int k = 0; k < 256; k++)
+                    vec[k] = make_float4(t.perlin_vec[k * 3], t.perlin_vec[k * 3 + 1], t.perlin_vec[k * 3 + 2], 0.f);
+                if ((rc = upload(s, vec.data(), vec.size(), &g.vec))) return bail(rc);
+                if ((rc = upload(s, t.perlin_perm, (size_t)768, &g.perm))) return bail(rc);
+            }
+        }
+        if ((rc = upload(s, dt.data(), dt.size(), &s->S.tex))) return bail(rc);
+    }
 
     // ── background + env alias table (renderer.rs:32-74) ────────────────────
     const RtBackground& bg = d->bg;

@@ -29,7 +29,7 @@ RT_D float medium_rnd(const MedRng& r, uint32_t i) {
     return (float)(pcg3d_x(r.a, r.b, r.c ^ (i * 0x9E3779B9u)) >> 8) * (1.0f / 16777216.0f);
 }
 
-RT_D float perlin_noise(const DevMedium& m, float3 p) {
+RT_D float perlin_noise(const float4* vec, const int32_t* perm, float3 p) {
     float fx = floorf(p.x), fy = floorf(p.y), fz = floorf(p.z);
     float u = p.x - fx, v = p.y - fy, w = p.z - fz;
     u = u * u * (3.0f - 2.0f * u);
@@ -43,9 +43,9 @@ RT_D float perlin_noise(const DevMedium& m, float3 p) {
         for (int dj = 0; dj < 2; dj++)
 #pragma unroll
             for (int dk = 0; dk < 2; dk++) {
-                int idx = (int)__ldg(m.perm + ((i + di) & 255)) ^ (int)__ldg(m.perm + 256 + ((j + dj) & 255)) ^
-                          (int)__ldg(m.perm + 512 + ((k + dk) & 255));
-                float4 c = __ldg(m.vec + idx);
+                int idx = (int)__ldg(perm + ((i + di) & 255)) ^ (int)__ldg(perm + 256 + ((j + dj) & 255)) ^
+                          (int)__ldg(perm + 512 + ((k + dk) & 255));
+                float4 c = __ldg(vec + idx);
                 float fi = (float)di, fj = (float)dj, fk = (float)dk;
                 float dt = c.x * (u - fi) + c.y * (v - fj) + c.z * (w - fk);
                 accum += (fi * u + (1.0f - fi) * (1.0f - u)) * (fj * v + (1.0f - fj) * (1.0f - v)) *
@@ -57,7 +57,7 @@ RT_D float medium_density_at(const DevMedium& m, float3 p) {
     float accum = 0.0f, weight = 1.0f;
     float3 q = p * m.noise_scale;
     for (int i = 0; i < 7; i++) {
-        accum += weight * perlin_noise(m, q);
+        accum += weight * perlin_noise(m.vec, m.perm, q);
         weight *= 0.5f;
         q = mk(q.x * 2.0f, q.y * 2.0f, q.z * 2.0f);
     }

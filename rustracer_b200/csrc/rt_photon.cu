@@ -19,6 +19,7 @@
 #include "rt_internal.h"
 #include "rt_media.cuh"
 #include "rt_ggx.cuh"
+#include "rt_texture.cuh"
 
 using namespace rtd;
 
@@ -272,14 +273,16 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                 } else if (m.type == RT_MAT_PBR) {
                     // PbrMaterial::scatter: a specular lobe carries the photon on, the
                     // diffuse lobe stores it where can_receive_caustics (material.rs:1049)
-                    float3 att, nd;
-                    int lobe = pbr_scatter(S, m, unit3(-d), nrm, rnd(rng, base + 2), rnd(rng, base + 3),
+                    float3 att, nd, sn = nrm;
+                    PbrHit ph = pbr_scalars(m);
+                    if (pbr_textured(m)) ph = pbr_hit(S, m, hit_uv(S, hv, front ? nrm : -nrm), nrm, &sn);
+                    int lobe = pbr_scatter(S, m, ph, unit3(-d), sn, rnd(rng, base + 2), rnd(rng, base + 3),
                                            rnd(rng, base + 0), rnd(rng, base + 1), &att, &nd);
                     if (lobe == PBR_SPECULAR) {
                         power = power * att;
                         o = p; d = nd; spec_depth++; cont = true;
                     }
-                    store = lobe == PBR_DIFFUSE && m.metallic < 0.999f;
+                    store = lobe == PBR_DIFFUSE && m.metallic < 0.999f;   // can_receive_caustics: the scalar
                 } else if (m.type == RT_MAT_LAMBERTIAN || m.type == RT_MAT_CHECKER) {
                     store = true;
                 }

@@ -12,6 +12,7 @@
 #include "rt_media.cuh"
 #include "rt_sky.cuh"
 #include "rt_ggx.cuh"
+#include "rt_texture.cuh"
 
 using namespace rtd;
 
@@ -741,7 +742,8 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                     o = p; d = dir;
                     prev_spec = true; prev_mis = 1.0f;
                 } else {
-                Surf sf_ = surface(S, A.hit[pid], o, d);
+                float4 hv = A.hit[pid];
+                Surf sf_ = surface(S, hv, o, d);
                 float3 p = sf_.p, nrm = sf_.nrm;
                 float t = sf_.t;
                 bool front = sf_.front;
@@ -840,16 +842,20 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                 } else {                                                            // renderer.rs:405-572
                     sf = spec_factor(S, tint, w, lam0, H);
                     float3 att, hint;       // the scatter attenuation and the caustic albedo hint
+                    float3 sn = nrm;        // the shading normal (a PBR normal map tilts it)
                     bool diffuse = true;
                     if constexpr (CLS == CLS_PBR) {
                         // PbrMaterial: its emission adds at the hit (renderer.rs:415-417),
                         // then one lobe scatters (material.rs:790-920)
                         float emit_w = (prev_spec || !have_lights) ? 1.0f : prev_mis;
                         Lc = Lc + T * (mk(m.emission[0], m.emission[1], m.emission[2]) * sf) * emit_w;
+                        PbrHit ph = pbr_scalars(m);
+                        if (pbr_textured(m))
+                            ph = pbr_hit(S, m, hit_uv(S, hv, front ? nrm : -nrm), nrm, &sn);
                         float3 wo = unit3(-d), dir;
-                        int lobe = pbr_scatter(S, m, wo, nrm, rnd(rng, b + B_LOBE0), rnd(rng, b + B_LOBE1),
+                        int lobe = pbr_scatter(S, m, ph, wo, sn, rnd(rng, b + B_LOBE0), rnd(rng, b + B_LOBE1),
                                                rnd(rng, b + B_SCATTER0), rnd(rng, b + B_SCATTER1), &att, &dir);
-                        hint = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
+                        hint = ph.albedo;
                         if (lobe != PBR_DIFFUSE) diffuse = false;
                         if (lobe == PBR_NONE) alive = false;
                         if (lobe == PBR_SPECULAR) {
@@ -859,7 +865,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                             if (SKY && S.has_sun) {
                                 float3 sun_s = sample_sun_cone(S.sun_dir, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1));
                                 float p_mat;
-                                float3 bc = pbr_spec_brdf_cos(S, m, wo, nrm, sun_s, &p_mat);
+                                float3 bc = pbr_spec_brdf_cos(S, m, ph, wo, sn, sun_s, &p_mat);
                                 if (bc.x > 0.0f || bc.y > 0.0f || bc.z > 0.0f) {
                                     float mis_d = SUN_PDF * SUN_PDF + p_mat * p_mat;
                                     if (mis_d > 0.0f) {
@@ -871,7 +877,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                                         sh0b = make_float4(sun_s.x, sun_s.y, sun_s.z, 0.f);
                                     }
                                 }
-                                float p_b = pbr_spec_pdf(S, m, wo, nrm, dir);
+                                float p_b = pbr_spec_pdf(S, m, ph, wo, sn, dir);
                                 if (p_b > 0.0f) sun_w = (p_b * p_b) / fmaxf(p_b * p_b + SUN_PDF * SUN_PDF, 1e-8f);
                             }
                             T = T * att;
@@ -880,6 +886,10 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         }
                     } else {
                         att = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
+                        if (m.albedo_tex) {                                         // texture.rs Image / Mottle
+                            HitUV uv = hit_uv(S, hv, front ? nrm : -nrm);
+                            att = tex_value(S, m.albedo_tex, uv.u, uv.v, p);
+                        }
                         if (m.type == RT_MAT_CHECKER) {
                             int xi = (int)floorf(m.checker_scale * p.x), yi = (int)floorf(m.checker_scale * p.y);
                             int zi = (int)floorf(m.checker_scale * p.z);
@@ -902,7 +912,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                             LRec lr;
                             if (lights_hit(S, p, ldir, &lr)) {
                                 float l_pdf = lights_pdf_value(S, p, ldir);
-                                float brdf = fmaxf(dot3(nrm, unit3(ldir)) / PI_F, 0.0f);
+                                float brdf = fmaxf(dot3(sn, unit3(ldir)) / PI_F, 0.0f);
                                 float sun_p = SKY ? sun_pdf_value(S, ldir) : 0.0f;
                                 float env_p = env_dir_pdf(S, ldir);
                                 float mis_d = l_pdf * l_pdf + brdf * brdf + sun_p * sun_p + env_p * env_p;
@@ -919,7 +929,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         if (SKY && S.has_sun) {                                         // renderer.rs:495-518
                             // the sun shares the env-NEE slot: a Physical sky has no env map
                             float3 sun_s, c;
-                            if (sun_nee_diffuse(S, p, nrm, T * att, sf, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1),
+                            if (sun_nee_diffuse(S, p, sn, T * att, sf, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1),
                                                 &sun_s, &c)) {
                                 np1 = make_float4(c.x, c.y, c.z, 0.f);
                                 sh1 = true;
@@ -932,7 +942,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                             float3 edir = env_sample_dir(S, rnd(rng, b + B_ENV_ROW), rnd(rng, b + B_ENV_COL),
                                                          rnd(rng, b + B_ENV_JU), rnd(rng, b + B_ENV_JV), &epdf);
                             if (epdf > 0.0f) {
-                                float brdf = fmaxf(dot3(nrm, unit3(edir)) / PI_F, 0.0f);
+                                float brdf = fmaxf(dot3(sn, unit3(edir)) / PI_F, 0.0f);
                                 if (brdf > 0.0f) {
                                     float area_pdf = have_lights ? lights_pdf_value(S, p, edir) : 0.0f;
                                     float3 ec = env_lookup(S, edir) * sf;
@@ -950,14 +960,14 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         float sp_, cp_;
                         sincosf(2.0f * PI_F * r1, &sp_, &cp_);
                         float sq_ = sqrtf(r2);
-                        float3 wn = unit3(nrm);
+                        float3 wn = unit3(sn);
                         float3 hh = fabsf(wn.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
                         float3 vv = unit3(cross3(wn, hh));
                         float3 uu = cross3(wn, vv);
                         float3 idir = (cp_ * sq_) * uu + (sp_ * sq_) * vv + sqrtf(1.0f - r2) * wn;
                         float3 iu = unit3(idir);
                         float pdf_val = fmaxf(dot3(iu, wn) / PI_F, 0.0f);
-                        float scat = fmaxf(dot3(nrm, iu) / PI_F, 0.0f);
+                        float scat = fmaxf(dot3(sn, iu) / PI_F, 0.0f);
                         if (pdf_val <= 0.0f || scat <= 0.0f || dot3(idir, nrm) <= 0.0f) {
                             alive = false;
                         } else {

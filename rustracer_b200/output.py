@@ -28,28 +28,71 @@ def write_png(path, rgb8):
 
 
 def read_png(path):
-    """Read back an 8-bit RGB PNG written by write_png (filter type 0 rows)."""
+    """Decode a non-interlaced PNG (grey, RGB, palette, grey+alpha, RGBA; 8 or
+    16 bits; filter types 0-4) into an (H, W, 3) uint8 RGB image (16-bit
+    samples keep their high byte, alpha is dropped) — what `image::open(..)
+    .into_rgb8()` gives the reference's textures (texture.rs:21-23)."""
     with open(path, "rb") as fh:
         data = fh.read()
     if data[:8] != b"\x89PNG\r\n\x1a\n":
-        raise ValueError("not a PNG file")
-    pos, idat, w, h = 8, b"", 0, 0
+        raise ValueError(f"{path}: not a PNG file")
+    pos, idat, palette, hdr = 8, [], None, None
     while pos < len(data):
         n, tag = struct.unpack(">I4s", data[pos:pos + 8])
         body = data[pos + 8:pos + 8 + n]
         if zlib.crc32(tag + body) & 0xFFFFFFFF != struct.unpack(">I", data[pos + 8 + n:pos + 12 + n])[0]:
-            raise ValueError("bad PNG chunk CRC")
+            raise ValueError(f"{path}: bad PNG chunk CRC")
         if tag == b"IHDR":
-            w, h, depth, ctype = struct.unpack(">IIBB", body[:10])
-            if depth != 8 or ctype != 2:
-                raise ValueError("only 8-bit RGB PNGs")
+            hdr = struct.unpack(">IIBBBBB", body)
+        elif tag == b"PLTE":
+            palette = np.frombuffer(body, np.uint8).reshape(-1, 3)
         elif tag == b"IDAT":
-            idat += body
+            idat.append(body)
+        elif tag == b"IEND":
+            break
         pos += 12 + n
-    rows = np.frombuffer(zlib.decompress(idat), np.uint8).reshape(h, 1 + w * 3)
-    if rows[:, 0].any():
-        raise ValueError("only unfiltered rows")
-    return rows[:, 1:].reshape(h, w, 3).copy()
+    w, h, depth, ctype, _, _, interlace = hdr
+    channels = {0: 1, 2: 3, 3: 1, 4: 2, 6: 4}.get(ctype)
+    if channels is None or depth not in (8, 16) or interlace or (ctype == 3 and depth != 8):
+        raise ValueError(f"{path}: unsupported PNG (colour type {ctype}, depth {depth}, interlace {interlace})")
+    bpp = channels * depth // 8
+    stride = w * bpp
+    raw = np.frombuffer(zlib.decompress(b"".join(idat)), np.uint8).reshape(h, 1 + stride)
+    out = np.zeros((h, stride), np.uint8)
+    prev = np.zeros(stride, np.int32)
+    for y in range(h):
+        ft, line = raw[y, 0], raw[y, 1:].astype(np.int32)
+        cur = np.zeros(stride, np.int32)
+        if ft == 0:
+            cur = line
+        elif ft == 1:
+            for i in range(stride):
+                cur[i] = (line[i] + (cur[i - bpp] if i >= bpp else 0)) & 0xFF
+        elif ft == 2:
+            cur = (line + prev) & 0xFF
+        elif ft == 3:
+            for i in range(stride):
+                cur[i] = (line[i] + ((cur[i - bpp] if i >= bpp else 0) + prev[i]) // 2) & 0xFF
+        elif ft == 4:
+            for i in range(stride):
+                a = cur[i - bpp] if i >= bpp else 0
+                b, c = prev[i], (prev[i - bpp] if i >= bpp else 0)
+                p = a + b - c
+                pa, pb, pc = abs(p - a), abs(p - b), abs(p - c)
+                pred = a if (pa <= pb and pa <= pc) else (b if pb <= pc else c)
+                cur[i] = (line[i] + pred) & 0xFF
+        else:
+            raise ValueError(f"{path}: bad PNG filter {ft}")
+        out[y] = cur
+        prev = cur
+    px = out.reshape(h, w, bpp)
+    if depth == 16:
+        px = px[..., 0::2]                         # high byte of each big-endian sample
+    if ctype == 3:
+        return palette[px[..., 0]].copy()
+    if ctype in (0, 4):
+        return np.repeat(px[..., :1], 3, axis=2).copy()
+    return px[..., :3].copy()
 
 
 def png_name(scene_name, spp):

@@ -183,6 +183,10 @@ class SceneBuilder:
         self.tri_v = []          # list of (n,9) float32
         self.tri_n = []          # list of (n,9) float32 or None
         self.tri_mat = []
+        self.tri_uv = []         # list of (n,6) float32 or None (the reference's default UVs)
+        self.tri_tan = []        # list of (n,9) float32 or None ((1, 0, 0) tangents)
+        self.textures = []       # RtTexture records (materials refer to them 1-based)
+        self._tex_keep = []
         self.quads = []          # (Q, u, v, mat)
         self.spheres = []        # (c, r, mat)
         self._lights = []        # ("quad"|"sphere", local index)
@@ -279,6 +283,27 @@ class SceneBuilder:
         return self.add_convex(planes, mat, lo, hi, polish=pol, scale=scale, rot=R,
                                pivot=center if pivot is None else pivot, translate=translate)
 
+    def add_texture_image(self, rgb8):
+        """An 8-bit RGB image texture (H, W, 3), row 0 = top; returns its 1-based id."""
+        img = np.ascontiguousarray(np.asarray(rgb8, np.uint8)[..., :3])
+        t = abi.RtTexture()
+        t.type, t.height, t.width = abi.RT_TEX_IMAGE, img.shape[0], img.shape[1]
+        t.rgb8 = img.ctypes.data_as(C.POINTER(C.c_uint8))
+        self._tex_keep.append(img)
+        self.textures.append(t)
+        return len(self.textures)
+
+    def add_texture_mottle(self, lo, hi, scale=3.0, seed=0x5EED):
+        """Texture::Mottle (texture.rs:52-55) with seeded Perlin tables; returns its 1-based id."""
+        t = abi.RtTexture()
+        t.type, t.scale = abi.RT_TEX_MOTTLE, float(scale)
+        t.lo, t.hi = _f3(lo), _f3(hi)
+        vec, perm = perlin_tables(seed)
+        t.perlin_vec = (C.c_float * 768)(*vec.reshape(-1).tolist())
+        t.perlin_perm = (C.c_int32 * 768)(*perm.reshape(-1).tolist())
+        self.textures.append(t)
+        return len(self.textures)
+
     def add_shape(self, kind, mat, center, radius=0.0, height=0.0, normal=(0.0, 1.0, 0.0), wave_amplitude=0.0,
                   wave_scale=1.0, xf=None):
         """Cylinder / Cone / Disk / InfinitePlane (cylinder.rs, cone.rs, disk.rs,
@@ -318,11 +343,16 @@ class SceneBuilder:
         self.add_quad([mn[0], mx[1], mx[2]], dx, -dz, mat, xf)
         self.add_quad([mn[0], mn[1], mn[2]], dx, dz, mat, xf)
 
-    def add_mesh(self, verts, faces, mat, vnormals=None, xf=None):
+    def add_mesh(self, verts, faces, mat, vnormals=None, xf=None, uvs=None):
         """Indexed triangle mesh; vertex normals are normalised at load with a
-        face-normal fallback (mesh.rs:68-73); zero-area faces are skipped."""
+        face-normal fallback (mesh.rs:68-73); zero-area faces are skipped.
+        `uvs` (per vertex) also give per-vertex tangents from the UV-space
+        derivatives (mesh.rs:33-54)."""
         V = np.asarray(verts, dtype=np.float64)
         Fi = np.asarray(faces, dtype=np.int64).reshape(-1, 3)
+        tan = None
+        if uvs is not None:
+            tan = mesh_tangents(V.astype(F32), Fi, np.asarray(uvs, F32))
         if xf is not None and not xf.identity:
             V = xf.point(V)
         Vf = V.astype(F32)
@@ -349,6 +379,14 @@ class SceneBuilder:
         self.tri_v.append(np.ascontiguousarray(tv))
         self.tri_n.append(tn)
         self.tri_mat.append(np.full(len(tv), mat, dtype=np.int32))
+        if uvs is not None:
+            UV = np.asarray(uvs, F32)
+            self.tri_uv.append(np.concatenate([UV[Fi[:, k]] for k in range(3)], axis=1).astype(F32))
+            T = tan if xf is None or xf.identity else xf.vector(tan.astype(np.float64)).astype(F32)
+            self.tri_tan.append(np.concatenate([T[Fi[:, k]] for k in range(3)], axis=1).astype(F32))
+        else:
+            self.tri_uv.append(None)
+            self.tri_tan.append(None)
         return len(tv)
 
     def add_light_quad(self, corner, u, v, mat):
@@ -416,7 +454,18 @@ class SceneBuilder:
             else:
                 self._tn = None
             self._tm = np.ascontiguousarray(np.concatenate(self.tri_mat).astype(np.int32))
+            if any(u is not None for u in self.tri_uv):
+                # mesh.rs:75-81: without texcoords the corners get (0,0) (1,0) (0.5,1), tangents (1,0,0)
+                duv = np.array([0, 0, 1, 0, 0.5, 1], F32)
+                dtan = np.array([1, 0, 0] * 3, F32)
+                self._tuv = np.ascontiguousarray(np.concatenate(
+                    [u if u is not None else np.tile(duv, (len(v), 1)) for u, v in zip(self.tri_uv, self.tri_v)]))
+                self._ttan = np.ascontiguousarray(np.concatenate(
+                    [t if t is not None else np.tile(dtan, (len(v), 1)) for t, v in zip(self.tri_tan, self.tri_v)]))
+            else:
+                self._tuv = self._ttan = None
         else:
+            self._tuv = self._ttan = None
             self._tv = np.zeros((0, 9), F32)
             self._tn = None
             self._tm = np.zeros(0, np.int32)
@@ -492,6 +541,13 @@ class SceneBuilder:
             d.n_convex = len(recs)
             d.convex = C.cast(self._cvx, C.POINTER(abi.RtConvex))
             d.convex_planes = abi.fptr(self._cvp)
+        if self._tuv is not None:
+            d.tri_uv = abi.fptr(self._tuv)
+            d.tri_tangent = abi.fptr(self._ttan)
+        if self.textures:
+            self._texs = (abi.RtTexture * len(self.textures))(*self.textures)
+            d.n_textures = len(self.textures)
+            d.textures = C.cast(self._texs, C.POINTER(abi.RtTexture))
         if self.shapes:
             self._shapes = (abi.RtShape * len(self.shapes))(*self.shapes)
             d.n_shapes = len(self.shapes)
@@ -538,24 +594,51 @@ def make_camera(look_from, look_at, vup=(0.0, 1.0, 0.0), vfov=40.0, aspect=1.0,
 
 
 # ── OBJ + HDR readers ────────────────────────────────────────────────────────
-def load_obj(path):
+def mesh_tangents(V, F, UV):
+    """Per-vertex tangents from UV-space derivatives, summed over the faces and
+    normalised with a (1, 0, 0) fallback (mesh.rs:33-54), in f32."""
+    f = np.float32
+    acc = np.zeros((len(V), 3), f)
+    for i0, i1, i2 in F:
+        e1, e2 = (V[i1] - V[i0]).astype(f), (V[i2] - V[i0]).astype(f)
+        du1, dv1 = UV[i1, 0] - UV[i0, 0], UV[i1, 1] - UV[i0, 1]
+        du2, dv2 = UV[i2, 0] - UV[i0, 0], UV[i2, 1] - UV[i0, 1]
+        den = f(du1 * dv2 - dv1 * du2)
+        if abs(den) < f(1e-8):
+            continue
+        t = (e1 * dv2 - e2 * dv1) * (f(1.0) / den)
+        acc[i0] += t
+        acc[i1] += t
+        acc[i2] += t
+    l2 = (acc * acc).sum(1)
+    ok = l2 > f(1e-8)
+    out = np.tile(np.array([1, 0, 0], f), (len(V), 1))
+    out[ok] = acc[ok] / np.sqrt(l2[ok])[:, None]
+    return out
+
+
+def load_obj(path, with_uv=False):
     """Minimal Wavefront OBJ reader: positions, optional normals, polygon faces
     fan-triangulated with a single index per corner (the effect of tobj's
     GPU_LOAD_OPTIONS in mesh.rs:14).  Returns (verts, faces, vnormals|None)."""
-    vs, vn, faces, fnorm = [], [], [], []
+    vs, vn, vt, faces, fnorm, ftex = [], [], [], [], [], []
     with open(path) as fh:
         for line in fh:
             if line.startswith("v "):
                 vs.append([float(x) for x in line.split()[1:4]])
             elif line.startswith("vn "):
                 vn.append([float(x) for x in line.split()[1:4]])
+            elif line.startswith("vt "):
+                vt.append([float(x) for x in line.split()[1:3]])
             elif line.startswith("f "):
-                idx = []
-                nidx = []
+                idx, nidx, tidx = [], [], []
                 for tok in line.split()[1:]:
                     parts = tok.split("/")
                     i = int(parts[0])
                     idx.append(i - 1 if i > 0 else len(vs) + i)
+                    if len(parts) >= 2 and parts[1]:
+                        j = int(parts[1])
+                        tidx.append(j - 1 if j > 0 else len(vt) + j)
                     if len(parts) >= 3 and parts[2]:
                         j = int(parts[2])
                         nidx.append(j - 1 if j > 0 else len(vn) + j)
@@ -563,16 +646,26 @@ def load_obj(path):
                     faces.append([idx[0], idx[k], idx[k + 1]])
                     if len(nidx) == len(idx):
                         fnorm.append([nidx[0], nidx[k], nidx[k + 1]])
+                    if len(tidx) == len(idx):
+                        ftex.append([tidx[0], tidx[k], tidx[k + 1]])
     V = np.asarray(vs, dtype=np.float64)
     Fa = np.asarray(faces, dtype=np.int64)
-    if vn and len(fnorm) == len(faces):
-        # expand to per-corner vertices so each corner carries its own normal
-        N = np.asarray(vn, dtype=np.float64)
-        Fn = np.asarray(fnorm, dtype=np.int64)
-        V2 = V[Fa.reshape(-1)]
-        N2 = N[Fn.reshape(-1)]
-        return V2, np.arange(len(V2)).reshape(-1, 3), N2
-    return V, Fa, None
+    has_n = bool(vn) and len(fnorm) == len(faces)
+    has_t = with_uv and bool(vt) and len(ftex) == len(faces)
+    if has_n or has_t:
+        # single-index vertices: one per distinct (position, uv, normal) triple
+        # of the corners, as tobj's GPU_LOAD_OPTIONS builds them (mesh.rs:14)
+        Fn = np.asarray(fnorm, np.int64) if has_n else np.zeros_like(Fa)
+        Ft = np.asarray(ftex, np.int64) if has_t else np.zeros_like(Fa)
+        key = np.stack([Fa.reshape(-1), Ft.reshape(-1), Fn.reshape(-1)], 1)
+        uniq, inv = np.unique(key, axis=0, return_inverse=True)
+        V2 = V[uniq[:, 0]]
+        N2 = np.asarray(vn, np.float64)[uniq[:, 2]] if has_n else None
+        out = (V2, inv.reshape(-1, 3), N2)
+        if with_uv:
+            return out + ((np.asarray(vt, np.float64)[uniq[:, 1]] if has_t else None),)
+        return out
+    return (V, Fa, None, None) if with_uv else (V, Fa, None)
 
 
 def load_hdr(path):
@@ -614,7 +707,16 @@ def load_hdr(path):
 
 
 # ── TOML loader (scene_file.rs:621-1216, the subset the GPU path supports) ───
-def _material_from_toml(m, base):
+def load_texture(path):
+    """An image file as (H, W, 3) uint8 RGB (texture.rs:21-23): PNG, or a
+    Radiance .hdr clamped to [0, 1] and quantised."""
+    if path.lower().endswith(".hdr"):
+        return (np.clip(load_hdr(path), 0.0, 1.0) * 255.0 + 0.5).astype(np.uint8)
+    from .output import read_png
+    return read_png(path)
+
+
+def _material_from_toml(m, base, sb):
     t = m["type"]
     if t == "lambertian":
         return Material.lambertian(m["color"])
@@ -631,6 +733,24 @@ def _material_from_toml(m, base):
         return Material.spectral_metal(m.get("variant", "gold"), m.get("roughness", 0.0))
     if t == "diffuse_light":
         return Material.diffuse_light(m["color"])
+    if t == "image":                                                 # scene_file.rs:1152-1153
+        mat = Material.lambertian((0.0, 0.0, 0.0))
+        mat.albedo_tex = sb.add_texture_image(load_texture(_resolve(base, m["path"])))
+        return mat
+    if t == "noise":                                                 # scene_file.rs:1149-1150: Texture::Mottle
+        mat = Material.lambertian((0.0, 0.0, 0.0))
+        mat.albedo_tex = sb.add_texture_mottle(m["lo"], m["hi"], m.get("scale", 3.0))
+        return mat
+    if t == "metal":                                                 # scene_file.rs:1155-1156
+        return Material.pbr(m["color"], roughness=m.get("fuzz", 0.0), metallic=1.0)
+    if t == "textured_pbr":                                          # scene_file.rs:1189-1199
+        mat = Material.pbr(roughness=m.get("roughness", 0.5), metallic=m.get("metallic", 0.0))
+        mat.albedo_tex = sb.add_texture_image(load_texture(_resolve(base, m["albedo_path"])))
+        for key, field in (("roughness_path", "roughness_tex"), ("metallic_path", "metallic_tex"),
+                           ("ao_path", "ao_tex"), ("normal_path", "normal_tex")):
+            if m.get(key):
+                setattr(mat, field, sb.add_texture_image(load_texture(_resolve(base, m[key]))))
+        return mat
     if t == "pbr":                                                   # scene_file.rs:380-406, 1179-1187
         return Material.pbr(m["albedo"], m.get("roughness", 0.5), m.get("metallic", 0.0), m.get("anisotropy", 0.0),
                             m.get("anisotropy_angle", 0.0), m.get("clearcoat", 0.0),
@@ -1145,7 +1265,7 @@ def scene_from_toml_dict(doc, base="."):
             continue
         if "material" not in obj:
             raise ValueError(f"objects[{i}]: material is required for this shape type")
-        mat = sb.add_material(_material_from_toml(obj["material"], base))
+        mat = sb.add_material(_material_from_toml(obj["material"], base, sb))
         xf = Transform(obj.get("scale"), obj.get("rotate"), obj.get("rotate_y"), obj.get("spin"), obj.get("translate"))
         st = sh["type"]
         mt = obj["material"]
@@ -1164,8 +1284,8 @@ def scene_from_toml_dict(doc, base="."):
         elif st == "box":
             sb.add_box(sh["p_min"], sh["p_max"], mat, xf)
         elif st == "mesh":
-            V, Fa, N = load_obj(_resolve(base, sh["path"]))
-            sb.add_mesh(V, Fa, mat, N, xf)
+            V, Fa, N, UV = load_obj(_resolve(base, sh["path"]), with_uv=True)
+            sb.add_mesh(V, Fa, mat, N, xf, uvs=UV)
         elif st in ("cylinder", "cone"):                            # scene_file.rs:997-1000
             sb.add_shape(st, mat, sh["center"], radius=sh["radius"], height=sh["height"], xf=xf)
         elif st == "disk":                                          # scene_file.rs:1001-1002

@@ -34,8 +34,8 @@ def test_version_without_gpu():
 
 def test_ctypes_struct_sizes_match_header_layout():
     from rustracer_b200 import abi
-    # RtMaterial: 17 scalars + 2×16 floats + the PBR block (9 scalars, emission[3], strength)
-    assert ctypes.sizeof(abi.RtMaterial) == 4 * (1 + 3 + 3 + 1 + 1 + 1 + 3 + 1 + 1 + 1 + 1 + 1 + 1 + 1 + 16 + 16 + 13)
+    # RtMaterial: 17 scalars + 2×16 floats + the PBR block (9 scalars, emission[3], strength) + 5 texture ids
+    assert ctypes.sizeof(abi.RtMaterial) == 4 * (1 + 3 + 3 + 1 + 1 + 1 + 3 + 1 + 1 + 1 + 1 + 1 + 1 + 1 + 16 + 16 + 13 + 5)
     assert ctypes.sizeof(abi.RtHit) == 16
     assert ctypes.sizeof(abi.RtPassParams) == 4 * 11 + 4 + 8
 
@@ -49,7 +49,8 @@ def test_ctypes_layouts_match_the_c_compiler(tmp_path):
     if shutil.which("gcc") is None:
         pytest.skip("no C compiler")
     inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
-    structs = {n: getattr(abi, n) for n in ("RtMaterial", "RtConvex", "RtMedium", "RtBackground", "RtSceneDesc",
+    structs = {n: getattr(abi, n) for n in ("RtMaterial", "RtConvex", "RtShape", "RtTexture", "RtMedium",
+                                             "RtBackground", "RtSceneDesc", "RtDevelopParams",
                                              "RtCamera", "RtPassParams", "RtHit")}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "rt_api.h"', "int main(void) {"]
     for n, t in structs.items():
