@@ -381,6 +381,12 @@ typedef struct RtDevelopParams {
 int32_t rt_develop(RtScene* scene, const float* linear_rgb, const RtDevelopParams* params, uint8_t* rgb8,
                    int32_t mem);
 
+/* Decode the scanlines of a Radiance RGBE image (flat or new-style RLE rows,
+ * the part of `image`'s HDR decoder the reference's env maps go through,
+ * renderer.rs:32-74) into height × width × 3 linear floats.  Host only; no
+ * device is touched. */
+int32_t rt_rgbe_decode(const uint8_t* scanlines, size_t n_bytes, int32_t width, int32_t height, float* rgb);
+
 /* ── caustic photon map (src/photon.rs, src/scene.rs:35-74) ──────────────── */
 #define RT_EMIT_DISK     0   /* directional disk facing `dir` (PhotonMap::build, photon.rs:41-94) */
 #define RT_EMIT_QUAD     1   /* cosine-weighted quad (PhotonMap::build_from_quad, photon.rs:97-135) */

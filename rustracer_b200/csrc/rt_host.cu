@@ -1771,6 +1771,39 @@ extern "C" int32_t rt_develop(RtScene* s, const float* lin, const RtDevelopParam
     return RT_OK;
 }
 
+extern "C" int32_t rt_rgbe_decode(const uint8_t* d, size_t n, int32_t W, int32_t H, float* rgb) {
+    if (!d || !rgb || W <= 0 || H <= 0) return RT_ERR_INVALID;
+    std::vector<uint8_t> row((size_t)W * 4);
+    size_t pos = 0;
+    for (int32_t y = 0; y < H; y++) {
+        if (pos + 4 <= n && d[pos] == 2 && d[pos + 1] == 2 && ((d[pos + 2] << 8) | d[pos + 3]) == W) {
+            pos += 4;
+            for (int c = 0; c < 4; c++)                      // one run list per channel
+                for (int32_t x = 0; x < W;) {
+                    if (pos >= n) return RT_ERR_INVALID;
+                    int cnt = d[pos++];
+                    bool run = cnt > 128;
+                    if (run) cnt -= 128;
+                    if (cnt == 0 || x + cnt > W || pos + (run ? 1 : (size_t)cnt) > n) return RT_ERR_INVALID;
+                    for (int k = 0; k < cnt; k++) row[(size_t)(x + k) * 4 + c] = run ? d[pos] : d[pos + k];
+                    pos += run ? 1 : cnt;
+                    x += cnt;
+                }
+        } else {
+            if (pos + (size_t)W * 4 > n) return RT_ERR_INVALID;
+            memcpy(row.data(), d + pos, (size_t)W * 4);
+            pos += (size_t)W * 4;
+        }
+        for (int32_t x = 0; x < W; x++) {
+            const uint8_t* q = row.data() + (size_t)x * 4;
+            float sc = q[3] ? std::ldexp(1.0f, (int)q[3] - 136) : 0.0f;
+            float* o = rgb + ((size_t)y * W + x) * 3;
+            o[0] = (float)q[0] * sc; o[1] = (float)q[1] * sc; o[2] = (float)q[2] * sc;
+        }
+    }
+    return RT_OK;
+}
+
 extern "C" int32_t rt_last_render_stats(const RtScene* s, double* ms, int64_t* ext, int64_t* sh, int64_t* launches) {
     if (!s) return RT_ERR_INVALID;
     if (ms) *ms = s->last_ms;

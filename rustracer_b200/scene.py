@@ -683,27 +683,15 @@ def load_hdr(path):
     dims = data[pos:end].split()
     pos = end + 1
     H, W = int(dims[1]), int(dims[3])
-    out = np.zeros((H, W, 4), dtype=np.uint8)
-    buf = np.frombuffer(data, dtype=np.uint8)
-    for y in range(H):
-        if buf[pos] == 2 and buf[pos + 1] == 2 and (buf[pos + 2] << 8 | buf[pos + 3]) == W:
-            pos += 4
-            for c in range(4):
-                x = 0
-                while x < W:
-                    cnt = int(buf[pos]); pos += 1
-                    if cnt > 128:
-                        cnt -= 128
-                        out[y, x:x + cnt, c] = buf[pos]; pos += 1
-                    else:
-                        out[y, x:x + cnt, c] = buf[pos:pos + cnt]; pos += cnt
-                    x += cnt
-        else:
-            out[y] = buf[pos:pos + W * 4].reshape(W, 4)
-            pos += W * 4
-    e = out[..., 3].astype(np.int32)
-    scale = np.where(e > 0, np.ldexp(1.0, e - 136), 0.0)
-    return (out[..., :3].astype(np.float64) * scale[..., None]).astype(F32)
+    # the scanline decoder is native (rt_rgbe_decode in librtb200.so)
+    from .renderer import lib
+    out = np.zeros((H, W, 3), F32)
+    body = np.frombuffer(data, np.uint8)[pos:]
+    rc = lib().rt_rgbe_decode(body.ctypes.data_as(C.POINTER(C.c_uint8)), C.c_size_t(len(body)), W, H,
+                              out.ctypes.data_as(C.POINTER(C.c_float)))
+    if rc != 0:
+        raise ValueError(f"{path}: corrupt RGBE scanlines")
+    return out
 
 
 # ── TOML loader (scene_file.rs:621-1216, the subset the GPU path supports) ───

@@ -122,3 +122,43 @@ def test_texture_materials_from_toml(tmp_path):
     assert mats[3].metallic_tex == 0 and mats[3].ao_tex == 0
     s = O.OracleScene(sb)
     np.testing.assert_allclose(s.tex_sample(1, [[0.01, 0.99]]), [[_srgb(x) for x in img[0, 0]]], rtol=1e-6)
+
+
+def _rgbe(c):
+    """float RGB → RGBE bytes (the Radiance encoding)."""
+    m = max(c)
+    if m < 1e-32:
+        return [0, 0, 0, 0]
+    f, e = math.frexp(m)
+    sc = f * 256.0 / m
+    return [int(c[0] * sc), int(c[1] * sc), int(c[2] * sc), e + 128]
+
+
+def test_radiance_hdr_flat_and_rle_scanlines(tmp_path):
+    """load_hdr's scanline decoder (native rt_rgbe_decode): one flat row and
+    one new-style RLE row with a run and a literal block, width ≥ 256 so the
+    width field needs both bytes."""
+    from rustracer_b200.scene import load_hdr
+    W = 300
+    rng = np.random.default_rng(1)
+    row0 = [_rgbe(rng.random(3) * 4) for _ in range(W)]
+    row1 = [_rgbe((0.5, 0.25, 0.125))] * 200 + [_rgbe(rng.random(3)) for _ in range(W - 200)]
+    body = bytearray(b"".join(bytes(px) for px in row0))
+    body += bytes([2, 2, W >> 8, W & 255])
+    for c in range(4):
+        ch = [px[c] for px in row1]
+        x = 0
+        while x < W:
+            if x < 200:                                  # runs of ≤ 127
+                n = min(127, 200 - x)
+                body += bytes([128 + n, ch[x]])
+            else:                                        # literals of ≤ 128
+                n = min(128, W - x)
+                body += bytes([n] + ch[x:x + n])
+            x += n
+    p = tmp_path / "t.hdr"
+    p.write_bytes(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n-Y 2 +X %d\n" % W + bytes(body))
+    img = load_hdr(str(p))
+    want = np.array([[[q[k] * math.ldexp(1.0, q[3] - 136) if q[3] else 0.0 for k in range(3)] for q in r]
+                     for r in (row0, row1)], np.float32)
+    np.testing.assert_array_equal(img, want)
