@@ -57,10 +57,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--mode", choices=["bench", "pass"], default="bench",
                     help="pass: one warm-up call + one measured 16-spp call of the workload, no JSON (profiler driver)")
-    ap.add_argument("--config", choices=["icosphere", "gem", "batch"], default="icosphere",
-                    help="gem: the 1280x720 gem workload with its caustic photon map; batch: 64 jobs of "
-                         "the box/icosphere/gem scenes on 4 concurrent handles vs one (secondary lines; "
-                         "the headline is the icosphere workload)")
+    ap.add_argument("--config", choices=["icosphere", "gem", "room", "batch"], default="icosphere",
+                    help="gem: the 1280x720 gem workload with its caustic photon map; room: the reference's "
+                         "--bench room (1200x800, 128 spp); batch: 64 jobs of the box/icosphere/gem scenes on 4 "
+                         "concurrent handles vs one (secondary lines; the headline is the icosphere workload)")
     return ap.parse_args()
 
 
@@ -409,6 +409,81 @@ def run_gem(args):
     print(json.dumps(line), flush=True)
 
 
+def run_room(args):
+    """Secondary workload: the reference's own benchmark room (bench.toml's
+    layout; --bench renders it at 1200x800, 128 spp, after building the caustic
+    photon map once, main.rs:84-117).  One step = 128 spp of the frame on the
+    device accumulators, timed by the library's CUDA events; e2e adds the read
+    of the developed 8-bit frame.  The CPU baseline is the oracle on bands of
+    the same frame at 1 spp."""
+    import torch
+    from rustracer_b200 import configs, photons
+    from rustracer_b200.renderer import GpuScene, pass_params
+    from oracle import oracle as O
+    sb, st = configs.gem_room_scene()
+    w, h, spp, depth = st["width"], st["height"], st["spp"], st["max_depth"]
+    strata = int(np.sqrt(np.float32(spp)))
+    scene = GpuScene(sb, device=0)
+    n_stored = scene.photon_build(photons.caustic_params(sb, st["photons"], st["radius"], seed=1))
+    dev = torch.device("cuda", 0)
+    outs = (torch.zeros((h, w, 3), device=dev), torch.zeros((h, w, 3), device=dev),
+            torch.zeros((h, w), dtype=torch.int32, device=dev))
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def step(k, develop=False):
+        scene.render_accumulate(st["camera"], pass_params(w, h, k * spp, spp, strata, depth, st["hero"], 1.0, 5),
+                                outputs=outs)
+        ms = scene.last_stats()["ms"]
+        if develop:
+            scene.develop(w, h)
+        return ms
+
+    for k in range(args.warmup):
+        step(k)
+    flush.fill_(1)
+    clocks = ClockSampler(0)
+    clocks.start()
+    r_ms, e2e_ms = [], []
+    for k in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r_ms.append(step(args.warmup + k, develop=True))
+        e2e_ms.append((time.perf_counter() - t0) * 1000.0)
+        flush.fill_(k & 0xFF)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    per_step = w * h * spp
+    line = {
+        "metric": "path samples/s (1200x800 gem room, the reference's --bench scene)",
+        "value": per_step * args.steps / (sum(r_ms) / 1000.0), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": statistics.mean(r_ms), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (bench.toml layout; the 1,400-face OBJ ball replaced by a generated 1,400-face ball)",
+        "config": {"workload": f"{st['name']}: 2 analytic gems, PBR gold ball, blackbody panel, dusk sky, "
+                               f"{w}x{h}, {spp} spp, depth {depth}, hero 1, photon map {st['photons']} emitted "
+                               f"(r {st['radius']}, {n_stored} stored)",
+                   "l2": "256 MB buffer written between timed steps"},
+        "clocks": clk,
+        "e2e": {"value": per_step * args.steps / (sum(e2e_ms) / 1000.0), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": w * h * 3},
+    }
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        o = O.OracleScene(sb)
+        o.photon_build(photons.caustic_params(sb, st["photons"], st["radius"], seed=1))
+        n, k, t0 = 0, 0, time.perf_counter()
+        while time.perf_counter() - t0 < 10.0:
+            row0 = (k * 61) % (h - 32)
+            o.render_pass(st["camera"], pass_params(w, h, k, 1, strata, depth, st["hero"], 1.0, 900 + k),
+                          threads=threads, rows=(row0, row0 + 32))
+            n += 32 * w
+            k += 1
+        el = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": n / el, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{k} bands of 32 rows x {w} px x 1 spp ({n} path samples, {el:.1f} s)"}
+    print(json.dumps(line), flush=True)
+
+
 def run_batch(args):
     """Secondary workload: 64 frames (scene, size, aspect, spp and camera orbit
     drawn from a seed) rendered on 4 concurrent scene handles, then on one
@@ -459,6 +534,8 @@ def main():
         run_reference(args)
     elif args.config == "gem":
         run_gem(args)
+    elif args.config == "room":
+        run_room(args)
     elif args.config == "batch":
         run_batch(args)
     else:

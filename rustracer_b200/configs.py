@@ -20,7 +20,7 @@ import math
 
 import numpy as np
 
-from .scene import Material, SceneBuilder, make_camera
+from .scene import Material, SceneBuilder, make_camera, scene_from_toml_dict
 
 F32 = np.float32
 
@@ -318,4 +318,83 @@ def gem_scene(width=1280, height=720, spp=256, max_depth=32, hero=4, seed=3, env
     return sb, st
 
 
-CONFIGS = {"box": box_scene, "icosphere": icosphere_scene, "media_box": media_box_scene, "gem": gem_scene}
+def latlong_ball(center, radius, nu=35, nv=21):
+    """A closed latitude-longitude ball mesh: 2·nu·(nv − 2) quad triangles plus
+    two pole fans = 1,400 faces for the defaults."""
+    V = [[center[0], center[1] + radius, center[2]]]
+    for j in range(1, nv):
+        th = math.pi * j / nv
+        for i in range(nu):
+            ph = 2.0 * math.pi * i / nu
+            V.append([center[0] + radius * math.sin(th) * math.cos(ph), center[1] + radius * math.cos(th),
+                      center[2] + radius * math.sin(th) * math.sin(ph)])
+    V.append([center[0], center[1] - radius, center[2]])
+    F = []
+    ring = lambda j, i: 1 + (j - 1) * nu + (i % nu)
+    for i in range(nu):
+        F.append([0, ring(1, i + 1), ring(1, i)])
+    for j in range(1, nv - 1):
+        for i in range(nu):
+            a, b, c, d = ring(j, i), ring(j, i + 1), ring(j + 1, i), ring(j + 1, i + 1)
+            F += [[a, b, c], [b, d, c]]
+    bottom = len(V) - 1
+    for i in range(nu):
+        F.append([bottom, ring(nv - 1, i), ring(nv - 1, i + 1)])
+    return np.array(V), np.array(F)
+
+
+def gem_room_scene(width=1200, height=800, spp=128, max_depth=50, photons=500_000, gather_radius=0.5):
+    """The reference's benchmark room (scenes/bench.toml): a 10 × 5 × 11 room
+    with a checker floor, red and blue side walls, a back wall with a window,
+    a ceiling with an opening around a 6500 K blackbody panel, a dusk
+    Physical sky (sun elevation 10.2°, turbidity 4.5), a round brilliant
+    diamond and a princess-cut sapphire as [[gems]], a brushed-gold PBR ball
+    and a caustic photon map (500k photons, radius 0.5).  The reference's
+    1,400-face OBJ ball is replaced by a generated 1,400-face ball of the
+    same centre and radius."""
+    white = {"type": "lambertian", "color": [0.80, 0.80, 0.80]}
+    quad = lambda c, u, v, m: {"shape": {"type": "quad", "corner": c, "u": u, "v": v}, "material": m}
+    doc = {
+        "name": "Benchmark",
+        "camera": {"look_from": [0.0, 3.4, -9.0], "look_at": [0.0, 2.247, 1.1993], "vfov": 36.0, "aperture": 0.0,
+                   "focus_dist": 10.0},
+        "background": {"type": "physical", "sun_azimuth": 0.0, "sun_elevation": 10.2, "turbidity": 4.5},
+        "objects": [
+            quad([-5.0, 0.0, -2.0], [10.0, 0.0, 0.0], [0.0, 0.0, 11.0],
+                 {"type": "checker", "even": [0.12, 0.12, 0.12], "odd": [0.88, 0.88, 0.88], "scale": 0.8}),
+            quad([-5.0, 0.0, -2.0], [0.0, 0.0, 11.0], [0.0, 5.0, 0.0], {"type": "lambertian", "color": [0.65, 0.10, 0.05]}),
+            quad([5.0, 0.0, -2.0], [0.0, 0.0, 11.0], [0.0, 5.0, 0.0], {"type": "lambertian", "color": [0.05, 0.15, 0.65]}),
+            quad([-5.0, 0.0, 9.0], [10.0, 0.0, 0.0], [0.0, 1.2, 0.0], white),
+            quad([-5.0, 4.2, 9.0], [10.0, 0.0, 0.0], [0.0, 0.8, 0.0], white),
+            quad([-5.0, 1.2, 9.0], [3.0, 0.0, 0.0], [0.0, 3.0, 0.0], white),
+            quad([2.0, 1.2, 9.0], [3.0, 0.0, 0.0], [0.0, 3.0, 0.0], white),
+            quad([-5.0, 5.0, -2.0], [10.0, 0.0, 0.0], [0.0, 0.0, 1.5], white),
+            quad([-5.0, 5.0, 2.5], [10.0, 0.0, 0.0], [0.0, 0.0, 6.5], white),
+            quad([-5.0, 5.0, -0.5], [3.5, 0.0, 0.0], [0.0, 0.0, 3.0], white),
+            quad([1.5, 5.0, -0.5], [3.5, 0.0, 0.0], [0.0, 0.0, 3.0], white),
+        ],
+        "lights": [{"corner": [-1.5, 5.0, -0.5], "u": [3.0, 0.0, 0.0], "v": [0.0, 0.0, 3.0], "color": [8.0, 8.0, 8.0],
+                    "temp_k": 6500.0, "intensity": 8.0}],
+        "gems": [
+            {"report": "round brilliant diamond", "measurements_mm": [9.00, 9.00, 5.60], "table_pct": 57.0,
+             "crown_pct": 14.5, "pavilion_pct": 43.0, "color_grade": "D", "cut": "brilliant", "material": "diamond",
+             "center": [0.0, 1.30, 2.5], "scale_mm": 0.3},
+            {"report": "princess sapphire", "measurements_mm": [6.00, 5.90, 4.20], "table_pct": 65.0,
+             "crown_pct": 12.0, "pavilion_pct": 50.0, "color_grade": "D", "cut": "princess", "material": "sapphire",
+             "rotate_y": 25.0, "center": [-3.0, 0.90, 1.0], "scale_mm": 0.3},
+        ],
+    }
+    sb = scene_from_toml_dict(doc)
+    gold = sb.add_material(Material.pbr((1.0, 0.78, 0.34), roughness=0.25, metallic=1.0))
+    V, F = latlong_ball((3.0, 1.2, 1.0), 1.2)
+    sb.add_mesh(V, F, gold)
+    sb.name = "Benchmark"
+    aspect = width / height
+    # CameraState::autofocus (camera.rs:139-143) does not matter with aperture 0
+    cam = make_camera(doc["camera"]["look_from"], doc["camera"]["look_at"], vfov=36.0, aspect=aspect)
+    return sb, dict(name="gem room", camera=cam, width=width, height=height, spp=spp, max_depth=max_depth, hero=1,
+                    photons=photons, radius=gather_radius)
+
+
+CONFIGS = {"box": box_scene, "icosphere": icosphere_scene, "media_box": media_box_scene, "gem": gem_scene,
+           "gem_room": gem_room_scene}

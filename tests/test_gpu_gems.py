@@ -167,3 +167,20 @@ def test_gpu_interior_rays_in_overlapping_gems_match_oracle():
     assert (oh["prim"] >= 2).sum() > n // 4
     assert_same_hits(gh, oh)
     assert np.array_equal(g.trace_any(rs), orc.trace_any(rs))
+
+
+def test_gpu_gem_room_matches_oracle():
+    """The reference's benchmark room (bench.toml layout: gems, PBR ball,
+    blackbody panel, dusk sky, caustic photon map) at a reduced size."""
+    from rustracer_b200 import configs
+    sb, st = configs.gem_room_scene(width=96, height=64)
+    g, o = GpuScene(sb), O.OracleScene(sb)
+    p = photons.caustic_params(sb, st["photons"], st["radius"], seed=1)
+    ng, no = g.photon_build(p), o.photon_build(p)
+    assert ng > 1000 and abs(ng - no) <= max(30, no // 20), (ng, no)
+    pp = pass_params(96, 64, 0, 64, 8, 16, 1, 1.0, 81)
+    gi = g.render_pass(st["camera"], pp)
+    pp.seed = 82
+    oi = o.render_pass(st["camera"], pp)
+    assert np.isfinite(gi).all()
+    assert_tiles_agree(gi, oi)
