@@ -278,7 +278,8 @@ def run_ours(args):
                    "spp_per_step": SPP, "path_samples_per_step_per_gpu": per_step,
                    "parallelism": f"weak: {ws} rank(s), each its own 64 spp"
                                   + (", accumulators all-reduced every frame (NCCL)" if ws > 1 else ""),
-                   "l2": "256 MB buffer written between timed steps; scene (~230 MB) exceeds L2"},
+                   "l2": "256 MB buffer written between timed steps; scene (~230 MB) exceeds L2",
+                   "bvh_build_ms": scene.build_time_ms()},
         "clocks": clk,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "merge_ms_per_step": merge_ms / args.steps if ws > 1 else None,

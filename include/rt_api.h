@@ -270,7 +270,11 @@ typedef struct RtSceneDesc {
     const RtTexture* textures;
     const float*     tri_uv;        /* n_tris × 6: (u, v) at v0, v1, v2 */
     const float*     tri_tangent;   /* n_tris × 9: per-vertex tangents (mesh.rs:33-54) */
+    int32_t          bvh_builder;   /* RT_BVH_DEVICE (0, default) or RT_BVH_HOST: where the binary SAH tree is built */
 } RtSceneDesc;
+
+#define RT_BVH_DEVICE 0   /* the binary SAH tree on the GPU (same tree as the host builder) */
+#define RT_BVH_HOST   1   /* the binary SAH tree on host threads */
 
 /* ── camera (src/camera.rs:24-59) ────────────────────────────────────────── */
 typedef struct RtCamera {
@@ -319,6 +323,8 @@ int32_t rt_scene_destroy(RtScene* scene);
 int32_t rt_last_error(const RtScene* scene, char* buf, size_t len);
 
 /* BVH statistics of the built tree: node count, leaf count, max depth, SAH cost. */
+/* Wall time of the BVH build at scene creation (binary SAH tree + collapse to 8-wide), ms. */
+int32_t rt_scene_build_time(const RtScene* scene, double* ms);
 int32_t rt_scene_bvh_stats(const RtScene* scene, int64_t* n_nodes, int64_t* n_leaves,
                            int32_t* max_depth, double* sah_cost);
 /* Export the 8-wide node array in the reference layout (bvh.rs:25-32, 224 B per

@@ -187,7 +187,12 @@ class RtSceneDesc(C.Structure):
         ("textures", C.POINTER(RtTexture)),
         ("tri_uv", C.POINTER(C.c_float)),
         ("tri_tangent", C.POINTER(C.c_float)),
+        ("bvh_builder", C.c_int32),
     ]
+
+
+RT_BVH_DEVICE = 0
+RT_BVH_HOST = 1
 
 
 class RtCamera(C.Structure):

@@ -24,6 +24,7 @@ UNITS = [
     ("rt_shade.cu", []),
     ("rt_photon.cu", []),
     ("rt_output.cu", ["--fmad=false"]),
+    ("rt_build.cu", ["--fmad=false"]),
     ("rt_host.cu", []),
 ]
 

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <chrono>
 #include <thread>
 #include <vector>
 
@@ -334,12 +335,36 @@ struct SahBuilder {
         return (int32_t)my;
     }
 
-    void build_wide() {
+    // the binary tree from the device builder (rth::gpu_build_binary): the same
+    // partition, so the same tree; 0 or a CUDA error
+    int build_binary_device(int32_t* root, int sms, cudaStream_t st) {
+        size_t n = boxes.size();
+        std::vector<float> bx(n * 6), nb(n > 1 ? (n - 1) * 6 : 6);
+        for (size_t i = 0; i < n; i++)
+            for (int a = 0; a < 3; a++) { bx[i * 6 + a] = hc(boxes[i].mn, a); bx[i * 6 + 3 + a] = hc(boxes[i].mx, a); }
+        std::vector<int32_t> l(n > 1 ? n - 1 : 1), r(n > 1 ? n - 1 : 1);
+        int rc = rth::gpu_build_binary(bx.data(), (int32_t)n, idx.data(), l.data(), r.data(), nb.data(), root, sms, st);
+        if (rc) return rc;
+        for (size_t i = 0; i + 1 < n; i++) {
+            bin[i].l = l[i]; bin[i].r = r[i];
+            bin[i].box = Box{h3(nb[i * 6], nb[i * 6 + 1], nb[i * 6 + 2]), h3(nb[i * 6 + 3], nb[i * 6 + 4], nb[i * 6 + 5])};
+        }
+        return 0;
+    }
+
+    // device: build the binary tree on the GPU (sms > 0), else on the host threads
+    int build_wide(int sms = 0, cudaStream_t st = 0) {
         size_t n = boxes.size();
         bin.assign(n > 1 ? n - 1 : 1, BinNode{});
         int32_t root;
         Box rb;
-        build_binary(0, n, &root, &rb, 0);
+        if (sms > 0) {
+            int rc = build_binary_device(&root, sms, st);
+            if (rc) return rc;
+            rb = root < 0 ? boxes[idx[-root - 1]] : bin[root].box;
+        } else {
+            build_binary(0, n, &root, &rb, 0);
+        }
         if (root < 0) {                       // single primitive: one node with one leaf
             RefNode nd;
             memset(&nd, 0, sizeof(nd));
@@ -348,9 +373,10 @@ struct SahBuilder {
             leaves.push_back(idx[0]);
             for (int a = 0; a < 3; a++) { nd.mn[a][0] = hc(rb.mn, a); nd.mx[a][0] = hc(rb.mx, a); }
             nodes.push_back(nd);
-            return;
+            return 0;
         }
         collapse(root, 0);
+        return 0;
     }
 
 };
@@ -474,6 +500,7 @@ struct RtScene {
     int64_t n_nodes = 0, n_leaves = 0, n_prims = 0;
     int32_t max_depth = 0;
     double sah_cost = 0.0;
+    double build_ms = 0.0;
     std::vector<RefNode> ref_nodes;   // reference-layout copy for rt_scene_bvh_export
     std::vector<int32_t> leaf_gids;
     bool empty = true;
@@ -797,7 +824,11 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     std::vector<float4> gtri, gtri_n, gquad, gsph, gtri_uv, gtri_tan;
     if (n > 0) {
         SahBuilder B(boxes);
-        B.build_wide();
+        // the binary SAH tree is built on the device unless the description asks for the host
+        auto tb = std::chrono::steady_clock::now();
+        int brc = B.build_wide(d->bvh_builder == RT_BVH_HOST ? 0 : s->sms, s->stream);
+        if (brc) return bail(fail(s, RT_ERR_CUDA, std::string("device BVH build: ") + cudaGetErrorString((cudaError_t)brc)));
+        s->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
         s->max_depth = B.max_depth;
         if ((int64_t)B.max_depth * 7 + 8 > RT_STACK)
             return bail(fail(s, RT_ERR_CAPACITY, "BVH depth " + std::to_string(B.max_depth) + " exceeds the traversal stack"));
@@ -1737,6 +1768,12 @@ extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const R
     s->last_shadow = sh;
     s->last_launches = nl;
     return check_err(s);
+}
+
+extern "C" int32_t rt_scene_build_time(const RtScene* s, double* ms) {
+    if (!s || !ms) return RT_ERR_INVALID;
+    *ms = s->build_ms;
+    return RT_OK;
 }
 
 extern "C" int32_t rt_develop(RtScene* s, const float* lin, const RtDevelopParams* p, uint8_t* rgb8, int32_t mem) {

@@ -155,6 +155,8 @@ void launch_photon_gather_paths(const PhotonMapDev& map, const PendTargets& T, c
                                 int sms, cudaStream_t st);
 void launch_accumulate(const float* scratch, uint32_t nsamp, uint32_t npix, float* acc, float* m2, uint32_t* cnt,
                        const uint8_t* conv, float clamp, uint32_t min_samples, float floor_, cudaStream_t st);
+int gpu_build_binary(const float* boxes_h, int32_t n, int32_t* idx_h, int32_t* bl_h, int32_t* br_h, float* bbox_h,
+                     int32_t* root_h, int sms, cudaStream_t st);
 void launch_develop(const float* lin, const float* sum, const uint32_t* cnt, uint32_t w, uint32_t h, float exposure,
                     int tm, float vignette, float distortion, uint8_t* out, int sms, cudaStream_t st);
 }  // namespace rth

@@ -49,6 +49,8 @@ def lib():
         L.rt_render_accumulate.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), f, u32, f, i32,
                                            vp, vp, vp, i32]
         L.rt_develop.argtypes = [vp, vp, C.POINTER(abi.RtDevelopParams), vp, i32]
+        L.rt_scene_build_time.argtypes = [vp, C.POINTER(C.c_double)]
+        L.rt_rgbe_decode.argtypes = [C.POINTER(C.c_uint8), C.c_size_t, i32, i32, C.POINTER(C.c_float)]
         L.rt_last_render_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
         L.rt_render_pass_noalloc.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), vp]
         L.rt_photon_build.argtypes = [vp, C.POINTER(abi.RtPhotonParams), C.POINTER(i64)]
@@ -156,6 +158,12 @@ class GpuScene:
         nn, nl, md, sah = C.c_int64(), C.c_int64(), C.c_int32(), C.c_double()
         lib().rt_scene_bvh_stats(self.h, C.byref(nn), C.byref(nl), C.byref(md), C.byref(sah))
         return dict(nodes=nn.value, leaves=nl.value, max_depth=md.value, sah_cost=sah.value)
+
+    def build_time_ms(self):
+        """Wall time of the BVH build at scene creation (rt_scene_build_time)."""
+        ms = C.c_double()
+        lib().rt_scene_build_time(self.h, C.byref(ms))
+        return ms.value
 
     def bvh(self):
         nn, nl = C.c_int64(), C.c_int64()

@@ -484,6 +484,7 @@ class SceneBuilder:
         self._mats = (abi.RtMaterial * max(1, len(self.materials)))(*self.materials)
         self._lp = self.light_prim_ids()
         d = abi.RtSceneDesc()
+        d.bvh_builder = getattr(self, "bvh_builder", abi.RT_BVH_DEVICE)
         d.n_tris = nt
         d.tri_v = abi.fptr(self._tv)
         d.tri_n = abi.fptr(self._tn)
