@@ -57,10 +57,14 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--mode", choices=["bench", "pass"], default="bench",
                     help="pass: one warm-up call + one measured 16-spp call of the workload, no JSON (profiler driver)")
-    ap.add_argument("--config", choices=["icosphere", "gem", "room", "batch"], default="icosphere",
+    ap.add_argument("--config", choices=["icosphere", "gem", "room", "batch", "guided"], default="icosphere",
                     help="gem: the 1280x720 gem workload with its caustic photon map; room: the reference's "
                          "--bench room (1200x800, 128 spp); batch: 64 jobs of the box/icosphere/gem scenes on 4 "
-                         "concurrent handles vs one (secondary lines; the headline is the icosphere workload)")
+                         "concurrent handles vs one; guided: equal-time relMSE of the learned proposal against "
+                         "cosine bounces on the slit-light room (secondary lines; the headline is the icosphere "
+                         "workload)")
+    ap.add_argument("--ref-spp", type=int, default=16384, help="guided: samples per pixel of the plain reference")
+    ap.add_argument("--plain-spp", type=int, default=256, help="guided: samples per pixel of the plain render")
     return ap.parse_args()
 
 
@@ -485,6 +489,84 @@ def run_room(args):
     print(json.dumps(line), flush=True)
 
 
+def run_guided(args):
+    """Learned proposal against cosine bounces at equal GPU time on the
+    slit-light room (1280x720, depth 24): a plain render of --plain-spp is
+    timed and scored against a plain --ref-spp reference; a fresh network is
+    trained during the guided render's first 64 spp (one call per sample pass,
+    4 Adam steps of 65,536 records after each) and then frozen, and the guided
+    render's relMSE is read at checkpoints.  `value` is the GPU time the
+    guided render needs to reach the plain render's relMSE over the plain
+    render's time (interpolated in log-log between checkpoints; training
+    included), lower is better."""
+    from rustracer_b200 import configs
+    from rustracer_b200.guiding import relmse
+    from rustracer_b200.renderer import GpuScene, guide_params, pass_params
+    from rustracer_b200 import abi
+    sb, st = configs.guided_box_scene()
+    w, h, depth, hero = st["width"], st["height"], st["max_depth"], st["hero"]
+    scene = GpuScene(sb, device=0)
+    cam = st["camera"]
+
+    def acc(sample_idx, n, seed, reset):
+        s, _, c = scene.render_accumulate(cam, pass_params(w, h, sample_idx, n, 16, depth, hero, 1.0, seed),
+                                          reset=reset)
+        return s / np.maximum(c, 1)[..., None], scene.last_stats()["ms"]
+
+    # reference: plain, --ref-spp in calls of 256
+    ref, ref_ms = None, 0.0
+    for k in range(0, args.ref_spp, 256):
+        ref, ms = acc(k, min(256, args.ref_spp - k), 101, k == 0)
+        ref_ms += ms
+    scene.guide_mode(abi.RT_GUIDE_OFF)
+    acc(0, 4, 7, True)                                    # warm-up
+    img_p, t_p = acc(0, args.plain_spp, 7, True)
+    e_p = relmse(img_p, ref)
+    # guided: train for 64 spp, then frozen; checkpoints of (GPU ms, relMSE)
+    scene.guide_init(guide_params(batch=65536, steps_per_pass=4, seed=3))
+    scene.guide_mode(abi.RT_GUIDE_TRAIN)
+    t_g, done, pts = 0.0, 0, []
+    for _ in range(64):
+        img, ms = acc(done, 1, 9, done == 0)
+        t_g += ms
+        done += 1
+    pts.append((t_g, relmse(img, ref), done))
+    scene.guide_mode(abi.RT_GUIDE_SAMPLE)
+    while done < 4 * args.plain_spp and (pts[-1][1] > e_p or t_g < t_p):
+        n = max(16, done // 4)
+        img, ms = acc(done, n, 9, False)
+        t_g += ms
+        done += n
+        pts.append((t_g, relmse(img, ref), done))
+    gstats = scene.guide_stats()
+    scene.guide_mode(abi.RT_GUIDE_OFF)
+
+    def interp(key_i, key_v, x):
+        # log-log interpolation of column key_v at key_i = x
+        for (a, b) in zip(pts, pts[1:]):
+            if (a[key_i] - x) * (b[key_i] - x) <= 0 and a[key_i] != b[key_i]:
+                f = (np.log(x) - np.log(a[key_i])) / (np.log(b[key_i]) - np.log(a[key_i]))
+                return float(np.exp(np.log(a[key_v]) + f * (np.log(b[key_v]) - np.log(a[key_v]))))
+        return None
+    t_match = interp(1, 0, e_p) if pts[-1][1] <= e_p else None
+    e_eq = interp(0, 1, t_p)
+    line = {
+        "metric": "equal-time relMSE: guided GPU time to reach the plain render's relMSE / plain GPU time "
+                  "(slit-light room)",
+        "value": (t_match / t_p) if t_match else None, "unit": "x", "n_gpus": 1, "steps": 1, "warmup": 1,
+        "ms_per_step": t_p, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
+        "data": "synthetic (box room, slit light, round brilliant, Perlin medium; random-init network trained online)",
+        "config": {"workload": st["name"], "reference": f"plain {args.ref_spp} spp ({ref_ms / 1000:.1f} s)",
+                   "plain": f"{args.plain_spp} spp, {t_p:.0f} ms, relMSE {e_p:.5g}",
+                   "guided_relmse_at_equal_time": e_eq,
+                   "guided_checkpoints": [{"ms": round(a, 1), "relmse": b, "spp": c} for a, b, c in pts],
+                   "training": {"records": gstats["records"], "samples": gstats["samples"],
+                                "adam_steps": gstats["steps"], "train_ms": round(gstats["train_ms"], 1)},
+                   "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_batch(args):
     """Secondary workload: 64 frames (scene, size, aspect, spp and camera orbit
     drawn from a seed) rendered on 4 concurrent scene handles, then on one
@@ -539,6 +621,8 @@ def main():
         run_room(args)
     elif args.config == "batch":
         run_batch(args)
+    elif args.config == "guided":
+        run_guided(args)
     else:
         run_ours(args)
 

@@ -479,6 +479,62 @@ int32_t rt_capture_rays(RtScene* scene, const RtCamera* cam, const RtPassParams*
 int32_t rt_render_pass_noalloc(RtScene* scene, const RtCamera* cam, const RtPassParams* params,
                                float* scratch_rgb);
 
+/* ── path guiding: a learned proposal at diffuse vertices (no counterpart in
+ * the reference, whose diffuse bounce is the cosine lobe of pdf.rs:12-41 and
+ * renderer.rs:545-571).
+ *
+ * A 16-level hash grid of the hit position (2 features per level, 2^19
+ * entries per level) and a one-blob encoding of the shading normal feed a
+ * 64-64-64 ReLU MLP (BF16 weights and activations, FP32 accumulation) whose
+ * 41 outputs are 8 von Mises–Fisher lobes (mean, log κ, mixture logit) and a
+ * guide fraction α ≤ 0.9.  With guiding on, a Lambertian bounce is drawn with
+ * probability α from the lobes and otherwise from the cosine lobe, weighted
+ * by the exact mixture density; NEE and bounce MIS use the same density, so
+ * the estimator stays unbiased.  In training mode every render call records
+ * (position, normal, direction, f·L·cos/p) at its guided vertices and, after
+ * the call, takes `steps_per_pass` Adam steps on minibatches of them,
+ * minimising −w·log p (the KL divergence to the product distribution).
+ * rt_render_pass_noalloc never guides. */
+typedef struct RtGuideParams {
+    float    domain_min[3], domain_max[3]; /* hash-grid box in world space; min == max: the scene bounds */
+    float    learning_rate;                /* Adam step size (1e-2) */
+    float    beta1, beta2, epsilon;        /* Adam moment decays and ε (0.9, 0.99, 1e-8) */
+    uint32_t batch;                        /* training minibatch rows, a multiple of 1024 (65536) */
+    uint32_t steps_per_pass;               /* Adam steps after each training render call */
+    uint32_t record_capacity;              /* training records kept per render call */
+    uint32_t min_resolution;               /* grid resolution of the coarsest level (16) */
+    float    level_scale;                  /* resolution growth per level (1.447: 16 → ≈4096) */
+    uint64_t seed;                         /* initial parameters and minibatch draws */
+} RtGuideParams;
+
+#define RT_GUIDE_OFF    0   /* plain cosine bounces (the reference's estimator) */
+#define RT_GUIDE_SAMPLE 1   /* guided bounces, network frozen */
+#define RT_GUIDE_TRAIN  2   /* guided bounces, records, Adam steps after each render call */
+#define RT_GUIDE_PARAMS 16792576   /* 15360 weights (4 layers, [out][in]; W3 48×64) + 16×2^19×2 table */
+
+/* Create (or re-create) the scene's guide with fresh parameters; mode RT_GUIDE_OFF. */
+int32_t rt_guide_init(RtScene* scene, const RtGuideParams* params);
+int32_t rt_guide_mode(RtScene* scene, int32_t mode);
+/* Copy the RT_GUIDE_PARAMS fp32 parameters out (write = 0) or in (write = 1;
+ * also clears the Adam moments and step count).  Host memory. */
+int32_t rt_guide_params(RtScene* scene, float* params, int32_t write);
+/* Network outputs at q (n × 6: position, unit normal) into raw (n × 41). */
+int32_t rt_guide_eval(RtScene* scene, const float* q, int64_t n, float* raw, int32_t mem);
+/* Mixture density (guide and cosine lobe) at unit directions dirs (n × 3). */
+int32_t rt_guide_pdf(RtScene* scene, const float* q, const float* dirs, int64_t n, float* pdf, int32_t mem);
+/* One-sample draw with u (n × 4: strategy, lobe, two direction numbers) →
+ * out (n × 4: direction, mixture density), the draw the shading kernel makes. */
+int32_t rt_guide_sample(RtScene* scene, const float* q, const float* u, int64_t n, float* out, int32_t mem);
+/* Loss Σ −w·log p over samples (n × 10: position, normal, direction, weight)
+ * and its gradient (RT_GUIDE_PARAMS floats, the loss divided by n) — no
+ * update.  Host memory. */
+int32_t rt_guide_loss_grad(RtScene* scene, const float* samples, int64_t n, float* loss, float* grad);
+/* `steps` Adam steps, each on all n samples; loss of the last step's forward
+ * pass.  Host memory. */
+int32_t rt_guide_train(RtScene* scene, const float* samples, int64_t n, int32_t steps, float* loss);
+/* Training totals: records, weighted samples, Adam steps, GPU time of the training kernels. */
+int32_t rt_guide_stats(const RtScene* scene, int64_t* records, int64_t* samples, int64_t* steps, double* train_ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -223,6 +223,29 @@ class RtDevelopParams(C.Structure):
     ]
 
 
+class RtGuideParams(C.Structure):
+    """RtGuideParams (include/rt_api.h): the path-guiding network's set-up."""
+    _fields_ = [
+        ("domain_min", C.c_float * 3),
+        ("domain_max", C.c_float * 3),
+        ("learning_rate", C.c_float),
+        ("beta1", C.c_float),
+        ("beta2", C.c_float),
+        ("epsilon", C.c_float),
+        ("batch", C.c_uint32),
+        ("steps_per_pass", C.c_uint32),
+        ("record_capacity", C.c_uint32),
+        ("min_resolution", C.c_uint32),
+        ("level_scale", C.c_float),
+        ("seed", C.c_uint64),
+    ]
+
+
+RT_GUIDE_OFF, RT_GUIDE_SAMPLE, RT_GUIDE_TRAIN = 0, 1, 2
+RT_GUIDE_PARAMS = 16792576
+GUIDE_N_MLP = 15360
+
+
 class RtPassParams(C.Structure):
     _fields_ = [
         ("width", C.c_uint32),

@@ -25,6 +25,7 @@ UNITS = [
     ("rt_photon.cu", []),
     ("rt_output.cu", ["--fmad=false"]),
     ("rt_build.cu", ["--fmad=false"]),
+    ("rt_guide.cu", ["--fmad=false"]),
     ("rt_host.cu", []),
 ]
 

@@ -509,6 +509,7 @@ struct RtScene {
     PathState P{};                    // set 0 (also the photon tracer's state)
     PathState P2{};                   // set 1 (shares hit and gq with set 0)
     PathState Rt{};                   // retire records: L, pend0, pend1, pendC, meta
+    rtgh::Guide* guide = nullptr;     // path-guiding network (rt_guide_init)
     uint32_t* queue[2] = {nullptr, nullptr};   // photon tracer queues
     ClassQueues cq{};
     float4* sq = nullptr;
@@ -609,6 +610,7 @@ int32_t rt_scene_destroy(RtScene* s) {
     for (auto& b : s->owned) cudaFree(b.p);
     void* ps[] = {s->counters, s->d_err, s->scratch, s->d_conv, s->acc, s->m2, s->cnt, s->stage, s->d_active};
     free_paths(s);
+    rtgh::destroy(s->guide);
     s->photons.release();
     for (void* p : ps) if (p) cudaFree(p);
     for (auto e : s->pev) cudaEventDestroy(e);
@@ -1435,6 +1437,7 @@ static void for_path_buffers(RtScene* s, F f) {
                          &P->pendC};
         for (int i = 0; i < 9; i++)
             if (P != &s->Rt || i >= 4) f((void**)f4[i], sizeof(float4));
+        f((void**)&P->rec, sizeof(uint32_t));
     }
     f((void**)&s->P.hit, sizeof(float4));
     f((void**)&s->P.gq, 2 * sizeof(float4));
@@ -1476,10 +1479,12 @@ struct WaveBufs {
     uint32_t* counters = nullptr;
     int* derr = nullptr;
     uint32_t cap = 0;
+    bool guide = false;               // the scene's guide may run (not the no-alloc array)
 };
 
 static WaveBufs scene_bufs(const RtScene* s) {
     WaveBufs W;
+    W.guide = true;
     W.set[0] = s->P; W.set[1] = s->P2; W.Rt = s->Rt;
     W.cq = s->cq; W.sq = s->sq; W.counters = s->counters; W.derr = s->d_err; W.cap = s->cap;
     return W;
@@ -1522,6 +1527,7 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
     R.gen_next = (unsigned long long*)(W.counters + HDR_GEN);
     R.scratch = dscratch;
     R.photons = s->photons.present && s->photons.n > 0;
+    if (W.guide && s->guide && rtgh::mode(s->guide) != RT_GUIDE_OFF) R.guide = rtgh::view(s->guide);
     uint32_t* hdr = W.counters;
     auto blk = [&](uint64_t it) { return W.counters + CTR_HDR_WORDS + (it % RT_CTR_RING) * RT_CTR_STRIDE; };
     size_t ev_used = 0;
@@ -1581,7 +1587,7 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         rth::launch_retire(s->S, B, W.Rt, R, c, hdr, blk(it + 2), cn + CTR_COUNT, s->sms, s->stream);
         // extend, classify, shadow, retire, the shading classes other than media
         // and PBR, and the PBR class when the scene has PBR materials
-        nl += 4 + (CLS_N - 2) + (s->S.n_pbr > 0 ? 1 : 0);
+        nl += 4 + (CLS_N - 2) + (s->S.n_pbr > 0 ? 1 : 0) + (R.guide.mode != 0 ? 1 : 0);
         uint32_t slot = (uint32_t)(it % STATUS_RING);
         CK(cudaMemcpyAsync(s->h_status + slot, cn + CTR_COUNT, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
         CK(cudaEventRecord(s->st_ev[slot], s->stream));
@@ -1649,8 +1655,18 @@ static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p,
         active = s->d_active;
         if (launches) *launches += 2;
     }
-    return run_wavefront(s, scene_bufs(s), cam, p, p->sample_idx, nsamp, dscratch, active, nactive, ext_rays, sh_rays,
-                         launches);
+    bool guided = s->guide && rtgh::mode(s->guide) != RT_GUIDE_OFF;
+    if (guided) {
+        if (rtgh::ensure_paths(s->guide, s->cap)) return fail(s, RT_ERR_NOMEM, "cudaMalloc guide mixtures");
+        CK(rtgh::begin_pass(s->guide, s->stream));
+    }
+    rc = run_wavefront(s, scene_bufs(s), cam, p, p->sample_idx, nsamp, dscratch, active, nactive, ext_rays, sh_rays,
+                       launches);
+    if (rc || !guided) return rc;
+    int64_t tl = 0;
+    CK(rtgh::train_pass(s->guide, s->sms, s->stream, &tl));
+    if (launches) *launches += tl;
+    return RT_OK;
 }
 
 static int validate_pass(RtScene* s, const RtCamera* cam, const RtPassParams* p) {
@@ -2174,4 +2190,163 @@ extern "C" int32_t rt_knn(RtScene* s, const float* q, int64_t n, int32_t k, floa
         CK(cudaMemcpyAsync(d2, dd, ob, cudaMemcpyDeviceToHost, s->stream));
     }
     return check_err(s);
+}
+
+// ── path guiding ────────────────────────────────────────────────────────────
+namespace {
+// device copies for the rt_guide_* test entry points (freed on scope exit)
+struct Tmp {
+    void* p = nullptr;
+    ~Tmp() { if (p) cudaFree(p); }
+};
+int guide_ready(RtScene* s) {
+    if (!s) return RT_ERR_INVALID;
+    if (!s->guide) return fail(s, RT_ERR_INVALID, "no guide: call rt_guide_init first");
+    return RT_OK;
+}
+// in: host or device input of `bytes`; returns a device pointer
+int stage_in(RtScene* s, const void* in, size_t bytes, int32_t mem, Tmp& t, const void** d) {
+    if (mem == RT_MEM_DEVICE || bytes == 0) { *d = in; return RT_OK; }
+    if (cudaMalloc(&t.p, bytes) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc guide staging");
+    CK(cudaMemcpyAsync(t.p, in, bytes, cudaMemcpyHostToDevice, s->stream));
+    *d = t.p;
+    return RT_OK;
+}
+int stage_out(RtScene* s, void* out, size_t bytes, int32_t mem, Tmp& t, void** d) {
+    if (mem == RT_MEM_DEVICE || bytes == 0) { *d = out; return RT_OK; }
+    if (cudaMalloc(&t.p, bytes) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc guide staging");
+    *d = t.p;
+    return RT_OK;
+}
+int guide_api(RtScene* s, const float* q, const float* dirs, const float* u, int64_t n, float* raw, float* out,
+              size_t out_per, int32_t mem) {
+    int rc = guide_ready(s);
+    if (rc) return rc;
+    if (n < 0 || n > (1ll << 28) || (n > 0 && !q)) return fail(s, RT_ERR_INVALID, "guide query count or pointer");
+    if (n == 0) return RT_OK;
+    CK(cudaSetDevice(s->device));
+    Tmp tq, td, tu, tr, to;
+    const void *dq = nullptr, *dd = nullptr, *du = nullptr;
+    void *dr = nullptr, *dout = nullptr;
+    if ((rc = stage_in(s, q, (size_t)n * 24, mem, tq, &dq))) return rc;
+    if (dirs && (rc = stage_in(s, dirs, (size_t)n * 12, mem, td, &dd))) return rc;
+    if (u && (rc = stage_in(s, u, (size_t)n * 16, mem, tu, &du))) return rc;
+    if (raw && (rc = stage_out(s, raw, (size_t)n * rtg::NOUT * 4, mem, tr, &dr))) return rc;
+    if (out && (rc = stage_out(s, out, (size_t)n * out_per * 4, mem, to, &dout))) return rc;
+    rtgh::eval(s->guide, (const float*)dq, (uint32_t)n, (const float*)dd, (const float*)du, (float*)dr, (float*)dout,
+               s->sms, s->stream);
+    CK(cudaGetLastError());
+    if (mem != RT_MEM_DEVICE) {
+        if (raw) CK(cudaMemcpyAsync(raw, dr, (size_t)n * rtg::NOUT * 4, cudaMemcpyDeviceToHost, s->stream));
+        if (out) CK(cudaMemcpyAsync(out, dout, (size_t)n * out_per * 4, cudaMemcpyDeviceToHost, s->stream));
+    }
+    CK(cudaStreamSynchronize(s->stream));
+    return check_err(s);
+}
+// host samples (n × 10) → device training samples (3 float4 each)
+int stage_samples(RtScene* s, const float* smp, int64_t n, Tmp& t, const float4** d) {
+    std::vector<float4> h((size_t)n * 3);
+    for (int64_t i = 0; i < n; i++) {
+        const float* r = smp + i * 10;
+        h[i * 3] = make_float4(r[0], r[1], r[2], r[9]);
+        h[i * 3 + 1] = make_float4(r[3], r[4], r[5], 0.f);
+        h[i * 3 + 2] = make_float4(r[6], r[7], r[8], 0.f);
+    }
+    if (cudaMalloc(&t.p, h.size() * sizeof(float4)) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc samples");
+    CK(cudaMemcpy(t.p, h.data(), h.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    *d = (const float4*)t.p;
+    return RT_OK;
+}
+}  // namespace
+
+extern "C" int32_t rt_guide_init(RtScene* s, const RtGuideParams* p) {
+    if (!s || !p) return RT_ERR_INVALID;
+    if (p->batch == 0 || p->batch % 1024 || p->batch > (1u << 22))
+        return fail(s, RT_ERR_INVALID, "guide batch must be a positive multiple of 1024, at most 2^22");
+    if (p->record_capacity == 0 || p->record_capacity > (1u << 27))
+        return fail(s, RT_ERR_INVALID, "guide record capacity must be in 1..2^27");
+    if (!(p->learning_rate > 0.0f) || !(p->beta1 >= 0.0f && p->beta1 < 1.0f) || !(p->beta2 >= 0.0f && p->beta2 < 1.0f) ||
+        !(p->epsilon > 0.0f))
+        return fail(s, RT_ERR_INVALID, "guide Adam parameters");
+    if (p->min_resolution < 2 || !(p->level_scale >= 1.0f) ||
+        (double)p->min_resolution * std::pow((double)p->level_scale, rtg::LEVELS - 1) > (double)(1u << 20))
+        return fail(s, RT_ERR_INVALID, "guide grid resolutions must be in 2..2^20");
+    for (int a = 0; a < 3; a++)
+        if (!std::isfinite(p->domain_min[a]) || !std::isfinite(p->domain_max[a]) || p->domain_max[a] < p->domain_min[a])
+            return fail(s, RT_ERR_INVALID, "guide domain");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    rtgh::destroy(s->guide);
+    s->guide = nullptr;
+    std::string err;
+    s->guide = rtgh::create(*p, s->world_lo, s->world_hi, &err);
+    if (!s->guide) return fail(s, RT_ERR_NOMEM, err);
+    return RT_OK;
+}
+
+extern "C" int32_t rt_guide_mode(RtScene* s, int32_t mode) {
+    if (!s) return RT_ERR_INVALID;
+    if (mode < RT_GUIDE_OFF || mode > RT_GUIDE_TRAIN) return fail(s, RT_ERR_INVALID, "guide mode must be 0, 1 or 2");
+    if (mode != RT_GUIDE_OFF && !s->guide) return fail(s, RT_ERR_INVALID, "no guide: call rt_guide_init first");
+    if (s->guide) rtgh::set_mode(s->guide, mode);
+    return RT_OK;
+}
+
+extern "C" int32_t rt_guide_params(RtScene* s, float* params, int32_t write) {
+    int rc = guide_ready(s);
+    if (rc) return rc;
+    if (!params) return fail(s, RT_ERR_INVALID, "null parameter buffer");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    CK(rtgh::params_io(s->guide, params, write, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return RT_OK;
+}
+
+extern "C" int32_t rt_guide_eval(RtScene* s, const float* q, int64_t n, float* raw, int32_t mem) {
+    if (!raw && n > 0) return s ? fail(s, RT_ERR_INVALID, "null output") : RT_ERR_INVALID;
+    return guide_api(s, q, nullptr, nullptr, n, raw, nullptr, 0, mem);
+}
+
+extern "C" int32_t rt_guide_pdf(RtScene* s, const float* q, const float* dirs, int64_t n, float* pdf, int32_t mem) {
+    if ((!dirs || !pdf) && n > 0) return s ? fail(s, RT_ERR_INVALID, "null direction or output") : RT_ERR_INVALID;
+    return guide_api(s, q, dirs, nullptr, n, nullptr, pdf, 1, mem);
+}
+
+extern "C" int32_t rt_guide_sample(RtScene* s, const float* q, const float* u, int64_t n, float* out, int32_t mem) {
+    if ((!u || !out) && n > 0) return s ? fail(s, RT_ERR_INVALID, "null random numbers or output") : RT_ERR_INVALID;
+    return guide_api(s, q, nullptr, u, n, nullptr, out, 4, mem);
+}
+
+extern "C" int32_t rt_guide_loss_grad(RtScene* s, const float* samples, int64_t n, float* loss, float* grad) {
+    int rc = guide_ready(s);
+    if (rc) return rc;
+    if (n <= 0 || n > (1ll << 22) || !samples) return fail(s, RT_ERR_INVALID, "guide samples: 1..2^22 rows");
+    CK(cudaSetDevice(s->device));
+    Tmp t;
+    const float4* d = nullptr;
+    if ((rc = stage_samples(s, samples, n, t, &d))) return rc;
+    CK(rtgh::train_explicit(s->guide, d, (uint32_t)n, 0, loss, s->sms, s->stream));
+    if (grad) CK(rtgh::grad_out(s->guide, grad, s->stream));
+    return check_err(s);
+}
+
+extern "C" int32_t rt_guide_train(RtScene* s, const float* samples, int64_t n, int32_t steps, float* loss) {
+    int rc = guide_ready(s);
+    if (rc) return rc;
+    if (n <= 0 || n > (1ll << 22) || !samples) return fail(s, RT_ERR_INVALID, "guide samples: 1..2^22 rows");
+    if (steps < 1) return fail(s, RT_ERR_INVALID, "steps must be at least 1");
+    CK(cudaSetDevice(s->device));
+    Tmp t;
+    const float4* d = nullptr;
+    if ((rc = stage_samples(s, samples, n, t, &d))) return rc;
+    CK(rtgh::train_explicit(s->guide, d, (uint32_t)n, steps, loss, s->sms, s->stream));
+    return check_err(s);
+}
+
+extern "C" int32_t rt_guide_stats(const RtScene* s, int64_t* records, int64_t* samples, int64_t* steps,
+                                  double* train_ms) {
+    if (!s || !s->guide) return RT_ERR_INVALID;
+    rtgh::stats(s->guide, records, samples, steps, train_ms);
+    return RT_OK;
 }

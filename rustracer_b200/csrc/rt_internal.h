@@ -6,6 +6,7 @@
 
 #include "../../include/rt_api.h"
 #include "rt_device.cuh"
+#include "rt_guide.cuh"
 
 #define RT_TRACE_BLOCK 128
 #define RT_TRACE_BLOCKS_PER_SM 8
@@ -59,6 +60,7 @@ struct PathState {
     float4* pend1;     // parked env-map NEE contribution
     float4* pendC;     // parked caustic (photon-map) contribution, folded before pend0/pend1
     float4* gq;        // photon-gather requests of the bounce: (p, pid) (n, -)
+    uint32_t* rec;     // newest guide training record of the path (guide training only)
 };
 
 // Where a contribution parked this iteration lives, for the shadow and gather
@@ -75,6 +77,7 @@ struct PendTargets {
 #define PF_TINT_SHIFT   9
 #define PF_TINT_MASK    (3u << 9)
 #define PF_SEC_ALIVE    (1u << 11)
+#define PF_REC_OPEN     (1u << 12)   // the newest guide record waits for its base radiance
 
 namespace rtph { struct Map; }
 
@@ -105,6 +108,7 @@ struct RenderLaunch {
     unsigned long long* gen_next;          // device cursor over [0, total)
     float*   scratch;                      // nsamp × npix × 3 (device), slot-major
     int      photons;                      // a photon map feeds the diffuse vertices
+    rtg::GuideDev guide;                   // learned proposal at diffuse vertices (mode 0: off)
 };
 
 namespace rth {
@@ -157,6 +161,30 @@ void launch_accumulate(const float* scratch, uint32_t nsamp, uint32_t npix, floa
                        const uint8_t* conv, float clamp, uint32_t min_samples, float floor_, cudaStream_t st);
 int gpu_build_binary(const float* boxes_h, int32_t n, int32_t* idx_h, int32_t* bl_h, int32_t* br_h, float* bbox_h,
                      int32_t* root_h, int sms, cudaStream_t st);
+// guide mixture of every path in the diffuse queue (before its shading kernel)
+void launch_guide_infer(const rtd::DevScene& S, const PathState& A, const RenderLaunch& R, const uint32_t* queue,
+                        const uint32_t* count, int sms, cudaStream_t st);
 void launch_develop(const float* lin, const float* sum, const uint32_t* cnt, uint32_t w, uint32_t h, float exposure,
                     int tm, float vignette, float distortion, uint8_t* out, int sms, cudaStream_t st);
 }  // namespace rth
+
+// host state of the path-guiding network (rt_guide.cu)
+#include <string>
+namespace rtgh {
+struct Guide;
+Guide* create(const RtGuideParams& p, const float scene_lo[3], const float scene_hi[3], std::string* err);
+void destroy(Guide* g);
+void set_mode(Guide* g, int mode);
+int mode(const Guide* g);
+rtg::GuideDev view(const Guide* g);
+int ensure_paths(Guide* g, uint32_t cap);
+cudaError_t params_io(Guide* g, float* host, int write, cudaStream_t st);
+void eval(Guide* g, const float* q, uint32_t n, const float* dirs, const float* u, float* raw, float* out, int sms,
+          cudaStream_t st);
+cudaError_t train_explicit(Guide* g, const float4* samples, uint32_t n, int steps, float* loss_host, int sms,
+                           cudaStream_t st);
+cudaError_t grad_out(Guide* g, float* host, cudaStream_t st);
+cudaError_t begin_pass(Guide* g, cudaStream_t st);
+cudaError_t train_pass(Guide* g, int sms, cudaStream_t st, int64_t* launches);
+void stats(const Guide* g, int64_t* records, int64_t* samples, int64_t* steps, double* ms);
+}  // namespace rtgh

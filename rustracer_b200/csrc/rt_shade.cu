@@ -411,6 +411,7 @@ RT_D void init_path(const DevScene& S, const PathState& P, const RenderLaunch& R
     P.thr[pid] = make_float4(1.f, 1.f, 1.f, 1.f);
     P.wts[pid] = make_float4(1.f, H > 1 ? 1.f : 0.f, H > 2 ? 1.f : 0.f, H > 3 ? 1.f : 0.f);
     P.meta[pid] = make_uint4(i, k, PF_PREV_SPEC | (H > 1 ? PF_SEC_ALIVE : 0u), __float_as_uint(lam0));
+    if (R.guide.mode == 2) P.rec[pid] = rtg::REC_NONE;
 }
 
 __global__ void k_generate(DevScene S, PathState A, RenderLaunch R, uint32_t pool, uint32_t* count0) {
@@ -449,6 +450,17 @@ __global__ void __launch_bounds__(RETIRE_BLOCK) k_retire(DevScene S, PathState B
             uint4 meta = Rt.meta[j];
             float* out = R.scratch + ((size_t)meta.y * R.npix + meta.x) * 3;
             out[0] = L.x; out[1] = L.y; out[2] = L.z;
+            if (R.guide.mode == 2) {
+                // weights of the path's guide records: radiance gathered after
+                // each vertex over the throughput there
+                float sl = L.x + L.y + L.z;
+                uint32_t r = Rt.rec[j];
+                for (int k = 0; k < RT_MAX_DEPTH && r != rtg::REC_NONE; k++) {
+                    float base = R.guide.rec_b[r].w, ts = R.guide.rec_a[r].w;
+                    if (base >= 0.0f && ts > 0.0f) R.guide.rec_w[r] = fmaxf(sl - base, 0.0f) / ts;
+                    r = __float_as_uint(R.guide.rec_c[r].w);
+                }
+            }
         }
         // one claim of new samples per block: the tile's ended paths are
         // t0 .. t0 + min(n − t0, RETIRE_BLOCK) − 1, in thread order
@@ -490,14 +502,18 @@ __global__ void k_zero_converged(const uint8_t* __restrict__ conv, uint32_t npix
 // no divergence between materials and a much smaller instruction footprint.
 // Sun NEE at a diffuse vertex (renderer.rs:495-518): the parked contribution
 // with the occlusion test still to do.
+// `gp`: the guide mixture of a guided bounce (its density replaces the cosine
+// lobe's in the MIS weight), or null.
 RT_D bool sun_nee_diffuse(const DevScene& S, float3 p, float3 nrm, float3 T_att, float3 sf,
-                                             float r1, float r2, float3* dir, float3* c) {
+                                             float r1, float r2, float3* dir, float3* c, const float4* gp = nullptr) {
     float3 sun_s = sample_sun_cone(S.sun_dir, r1, r2);
-    float brdf = fmaxf(dot3(nrm, unit3(sun_s)) / PI_F, 0.0f);
+    float3 su = unit3(sun_s);
+    float brdf = fmaxf(dot3(nrm, su) / PI_F, 0.0f);
     if (!(brdf > 0.0f)) return false;
     float3 sun_color = preetham_sky(sun_s, S.sun_dir, S.turbidity) * sf;
     float area_pdf = S.n_lights > 0 ? lights_pdf_value(S, p, sun_s) : 0.0f;
-    float mis_d = SUN_PDF * SUN_PDF + brdf * brdf + area_pdf * area_pdf;
+    float pb = gp ? rtg::guide_pdf(gp, nrm.x, nrm.y, nrm.z, su.x, su.y, su.z) : brdf;
+    float mis_d = SUN_PDF * SUN_PDF + pb * pb + area_pdf * area_pdf;
     *c = T_att * brdf * SUN_PDF * sun_color / mis_d;
     *dir = sun_s;
     return true;
@@ -644,7 +660,8 @@ RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
 // SKY: the scene has a Physical sky (Preetham background, sun NEE); the other
 // instantiation leaves that code out so env-map and plain scenes keep their
 // registers.
-template <int CLS, bool SKY>
+// GUIDE (diffuse class only): bounces drawn from the guide mixture.
+template <int CLS, bool SKY, bool GUIDE>
 __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState A, PathState B, PathState Rt,
                                                           RenderLaunch R, const uint32_t* __restrict__ qin,
                                                           const uint32_t* cin, uint32_t* cout,
@@ -675,6 +692,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
         float4 np0 = zero4, np1 = zero4, npc = zero4;     // contributions parked this bounce
         float4 Lout = zero4, o_out = zero4, d_out = zero4, thr_out = zero4, w_out = zero4;
         uint4 meta = make_uint4(0u, 0u, 0u, 0u);
+        uint32_t head = rtg::REC_NONE;   // newest guide record of the path
         if (active) {
             meta = A.meta[pid];
             float4 thr = A.thr[pid], w = A.wts[pid], L = A.L[pid];
@@ -699,6 +717,15 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
             Rng rng = make_rng(R.seed, meta.x, R.sample_idx + meta.y);
             uint32_t b = D_BOUNCE0 + depth * D_PER_BOUNCE;
             float3 Lc = mk(L.x, L.y, L.z);
+            if (R.guide.mode == 2) {
+                // the previous guided vertex's own estimates are folded: what the
+                // path gathers from here on arrives along that vertex's bounce
+                head = A.rec[pid];
+                if (flags & PF_REC_OPEN) {
+                    reinterpret_cast<float*>(R.guide.rec_b + head)[3] = L.x + L.y + L.z;
+                    flags &= ~PF_REC_OPEN;
+                }
+            }
             if (CLS == CLS_MISS) {                                                  // renderer.rs:381-403
                 float env_pdf = 0.0f;
                 float3 bg;
@@ -898,6 +925,11 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         hint = att;
                     }
                     if (diffuse) {
+                        const float4* gp = GUIDE ? R.guide.gpar + (size_t)pid * rtg::GP_F4 : nullptr;
+                        // density of the bounce strategy at unit direction u, for the MIS weights
+                        auto bounce_pdf = [&](float3 u, float cos_pdf) {
+                            return GUIDE ? rtg::guide_pdf(gp, sn.x, sn.y, sn.z, u.x, u.y, u.z) : cos_pdf;
+                        };
                         if (R.photons) {
                             // caustic injection: the gather kernel turns T·tint·albedo into × irradiance
                             float3 f = T * sf * hint;
@@ -912,10 +944,12 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                             LRec lr;
                             if (lights_hit(S, p, ldir, &lr)) {
                                 float l_pdf = lights_pdf_value(S, p, ldir);
-                                float brdf = fmaxf(dot3(sn, unit3(ldir)) / PI_F, 0.0f);
+                                float3 lu = unit3(ldir);
+                                float brdf = fmaxf(dot3(sn, lu) / PI_F, 0.0f);
                                 float sun_p = SKY ? sun_pdf_value(S, ldir) : 0.0f;
                                 float env_p = env_dir_pdf(S, ldir);
-                                float mis_d = l_pdf * l_pdf + brdf * brdf + sun_p * sun_p + env_p * env_p;
+                                float pb = bounce_pdf(lu, brdf);
+                                float mis_d = l_pdf * l_pdf + pb * pb + sun_p * sun_p + env_p * env_p;
                                 if (mis_d > 0.0f && brdf > 0.0f) {
                                     float3 nee = emission(S, S.mats[lr.mat], tint, w, lam0, H);
                                     float3 c = T * att * brdf * l_pdf * nee / mis_d;
@@ -930,7 +964,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                             // the sun shares the env-NEE slot: a Physical sky has no env map
                             float3 sun_s, c;
                             if (sun_nee_diffuse(S, p, sn, T * att, sf, rnd(rng, b + B_SUN0), rnd(rng, b + B_SUN1),
-                                                &sun_s, &c)) {
+                                                &sun_s, &c, gp)) {
                                 np1 = make_float4(c.x, c.y, c.z, 0.f);
                                 sh1 = true;
                                 sh1a = make_float4(p.x, p.y, p.z, INFINITY);
@@ -942,11 +976,13 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                             float3 edir = env_sample_dir(S, rnd(rng, b + B_ENV_ROW), rnd(rng, b + B_ENV_COL),
                                                          rnd(rng, b + B_ENV_JU), rnd(rng, b + B_ENV_JV), &epdf);
                             if (epdf > 0.0f) {
-                                float brdf = fmaxf(dot3(sn, unit3(edir)) / PI_F, 0.0f);
+                                float3 eu = unit3(edir);
+                                float brdf = fmaxf(dot3(sn, eu) / PI_F, 0.0f);
                                 if (brdf > 0.0f) {
                                     float area_pdf = have_lights ? lights_pdf_value(S, p, edir) : 0.0f;
                                     float3 ec = env_lookup(S, edir) * sf;
-                                    float mis_d = epdf * epdf + brdf * brdf + area_pdf * area_pdf;
+                                    float pb = bounce_pdf(eu, brdf);
+                                    float mis_d = epdf * epdf + pb * pb + area_pdf * area_pdf;
                                     float3 c = T * att * brdf * epdf * ec / mis_d;
                                     np1 = make_float4(c.x, c.y, c.z, 0.f);
                                     sh1 = true;
@@ -965,12 +1001,34 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                         float3 vv = unit3(cross3(wn, hh));
                         float3 uu = cross3(wn, vv);
                         float3 idir = (cp_ * sq_) * uu + (sp_ * sq_) * vv + sqrtf(1.0f - r2) * wn;
+                        if (GUIDE && rnd(rng, b + B_LOBE0) < __ldg(gp + 10).x) {
+                            // one-sample MIS: a vMF lobe of the guide instead of the cosine lobe
+                            float gx, gy, gz;
+                            rtg::vmf_mix_sample(gp, rnd(rng, b + B_LOBE1), rnd(rng, b + B_SCATTER0),
+                                                rnd(rng, b + B_SCATTER1), &gx, &gy, &gz);
+                            idir = mk(gx, gy, gz);
+                        }
                         float3 iu = unit3(idir);
-                        float pdf_val = fmaxf(dot3(iu, wn) / PI_F, 0.0f);
+                        float pdf_val = GUIDE ? rtg::guide_pdf(gp, wn.x, wn.y, wn.z, iu.x, iu.y, iu.z)
+                                              : fmaxf(dot3(iu, wn) / PI_F, 0.0f);
                         float scat = fmaxf(dot3(sn, iu) / PI_F, 0.0f);
                         if (pdf_val <= 0.0f || scat <= 0.0f || dot3(idir, nrm) <= 0.0f) {
                             alive = false;
                         } else {
+                            if (GUIDE && R.guide.mode == 2) {
+                                // training record: the radiance this path gathers after
+                                // the vertex, over T·sf here, estimates f·L_i·cos / p
+                                uint32_t r = atomicAdd(R.guide.rec_count, 1u);
+                                if (r < R.guide.rec_cap) {
+                                    float ts = T.x * sf.x + T.y * sf.y + T.z * sf.z;
+                                    R.guide.rec_a[r] = make_float4(p.x, p.y, p.z, ts);
+                                    R.guide.rec_b[r] = make_float4(wn.x, wn.y, wn.z, -1.0f);
+                                    R.guide.rec_c[r] = make_float4(iu.x, iu.y, iu.z, __uint_as_float(head));
+                                    R.guide.rec_w[r] = 0.0f;
+                                    head = r;
+                                    flags |= PF_REC_OPEN;
+                                }
+                            }
                             float area = have_lights ? lights_pdf_value(S, p, idir) : 0.0f;
                             float sun = SKY ? sun_pdf_value(S, idir) : 0.0f;
                             float env = env_dir_pdf(S, idir);
@@ -1022,9 +1080,11 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
             B.ray_o[slot] = o_out; B.ray_d[slot] = d_out; B.thr[slot] = thr_out; B.wts[slot] = w_out;
             B.meta[slot] = meta; B.L[slot] = Lout; B.pend0[slot] = np0; B.pend1[slot] = np1;
             if (R.photons) B.pendC[slot] = npc;
+            if (R.guide.mode == 2) B.rec[slot] = head;
         } else if (ended) {
             Rt.meta[rs] = meta; Rt.L[rs] = Lout; Rt.pend0[rs] = np0; Rt.pend1[rs] = np1;
             if (R.photons) Rt.pendC[rs] = npc;
+            if (R.guide.mode == 2) Rt.rec[rs] = head;
         }
         if constexpr (NQ == 4) {
             uint32_t tag = cont ? slot << 2 : (rs << 2) | PT_RETIRED;
@@ -1068,7 +1128,64 @@ __global__ void k_accumulate(const float* __restrict__ scratch, uint32_t nsamp, 
     }
 }
 
+// ── guide inference: the mixture of every diffuse-class path of the bounce ──
+// One warp evaluates 32 paths: each lane encodes its hit (position and
+// face-forward normal, as the shading kernel computes them), then the warp
+// runs the network on two 16-row tiles and lanes 0..15 write the mixtures.
+#define GUIDE_WARPS 4
+#define GUIDE_LDO 52
+static size_t guide_infer_smem() {
+    return (size_t)rtg::W_SMEM * 2 + (size_t)GUIDE_WARPS * (32 * rtg::LDW * 2 + 16 * GUIDE_LDO * 4);
+}
+__global__ void __launch_bounds__(GUIDE_WARPS * 32) k_guide_infer(DevScene S, PathState A, RenderLaunch R,
+                                                                  const uint32_t* __restrict__ qin,
+                                                                  const uint32_t* cin) {
+    extern __shared__ __align__(16) unsigned char gsm[];
+    __nv_bfloat16* Ws = reinterpret_cast<__nv_bfloat16*>(gsm);
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __nv_bfloat16* S_in = Ws + rtg::W_SMEM + warp * 32 * rtg::LDW;
+    float* S_o = reinterpret_cast<float*>(Ws + rtg::W_SMEM + GUIDE_WARPS * 32 * rtg::LDW) + warp * 16 * GUIDE_LDO;
+    rtg::load_weights(R.guide.wbf, Ws);
+    __syncthreads();
+    uint32_t n = *cin;
+    for (uint32_t base = (blockIdx.x * GUIDE_WARPS + warp) * 32; base < n; base += gridDim.x * GUIDE_WARPS * 32) {
+        uint32_t qi = base + lane;
+        bool valid = qi < n;
+        uint32_t pid = valid ? qin[qi] : 0u;
+        if (valid) {
+            float4 hv = A.hit[pid], ro = A.ray_o[pid], rdv = A.ray_d[pid];
+            Surf sf = surface(S, hv, mk(ro.x, ro.y, ro.z), mk(rdv.x, rdv.y, rdv.z));
+            rtg::encode_row(R.guide, R.guide.table, sf.p, sf.nrm, S_in + lane * rtg::LDW);
+        } else {
+            for (int k = 0; k < rtg::NIN; k++) S_in[lane * rtg::LDW + k] = __float2bfloat16_rn(0.0f);
+        }
+        uint32_t pid0 = __shfl_sync(0xFFFFFFFFu, pid, lane & 15), pid1 = __shfl_sync(0xFFFFFFFFu, pid, 16 + (lane & 15));
+        __syncwarp();
+        for (int mt = 0; mt < 2; mt++) {
+            uint32_t x0[4][4], h1[4][4], h2[4][4], h3[4][4];
+            float o[6][4];
+            rtg::load_frags<4>(S_in + 16 * mt * rtg::LDW, rtg::LDW, x0);
+            rtg::mlp_forward(Ws, x0, h1, h2, h3, o);
+            rtg::store_out(o, S_o, GUIDE_LDO);
+            __syncwarp();
+            if (lane < 16 && base + 16 * mt + lane < n) {
+                float4 gp[rtg::GP_F4];
+                rtg::mixture_from_outputs(S_o + lane * GUIDE_LDO, gp);
+                float4* dst = R.guide.gpar + (size_t)(mt ? pid1 : pid0) * rtg::GP_F4;
+#pragma unroll
+                for (int k = 0; k < rtg::GP_F4; k++) dst[k] = gp[k];
+            }
+            __syncwarp();
+        }
+    }
+}
+
 namespace rth {
+void launch_guide_infer(const DevScene& S, const PathState& A, const RenderLaunch& R, const uint32_t* queue,
+                        const uint32_t* count, int sms, cudaStream_t st) {
+    cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)guide_infer_smem());
+    k_guide_infer<<<sms * 3, GUIDE_WARPS * 32, guide_infer_smem(), st>>>(S, A, R, queue, count);
+}
 void launch_generate(const DevScene& S, const PathState& A, const RenderLaunch& R, uint32_t pool, uint32_t* count0,
                      cudaStream_t st) {
     int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>((pool + 255) / 256, 148u * 16u));
@@ -1079,19 +1196,24 @@ void launch_shade(const DevScene& S, const PathState& A, const PathState& B, con
     // ctr: this iteration's counter block (see rt_internal.h for the slots)
     int grid = sms * RT_SHADE_BLOCKS_PER_SM;
     k_classify<<<sms * 4, CLS_BLOCK, 0, st>>>(A.hit, ctr + CTR_COUNT, Q, ctr + CTR_CLS_COUNT);
-#define RT_SHADE_CLASS(C)                                                                                   \
+    if (R.guide.mode != 0)
+        launch_guide_infer(S, A, R, Q.q[CLS_DIFFUSE], ctr + CTR_CLS_COUNT + CLS_DIFFUSE, sms, st);
+#define RT_SHADE_CLASS_G(C, G)                                                                              \
     if (S.bg_type == RT_BG_PHYSICAL)                                                                        \
-        k_shade<C, true><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr); \
+        k_shade<C, true, G><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr); \
     else                                                                                                    \
-        k_shade<C, false><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr)
+        k_shade<C, false, G><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr)
+#define RT_SHADE_CLASS(C) RT_SHADE_CLASS_G(C, false)
     RT_SHADE_CLASS(CLS_MISS);
     RT_SHADE_CLASS(CLS_EMIT);
-    RT_SHADE_CLASS(CLS_DIFFUSE);
+    if (R.guide.mode != 0) { RT_SHADE_CLASS_G(CLS_DIFFUSE, true); }
+    else { RT_SHADE_CLASS(CLS_DIFFUSE); }
     RT_SHADE_CLASS(CLS_METAL);
     RT_SHADE_CLASS(CLS_DIELEC);
     if (S.n_pbr > 0) { RT_SHADE_CLASS(CLS_PBR); }
     if (S.n_media > 0) { RT_SHADE_CLASS(CLS_MEDIUM); }
 #undef RT_SHADE_CLASS
+#undef RT_SHADE_CLASS_G
 }
 void launch_retire(const DevScene& S, const PathState& B, const PathState& Rt, const RenderLaunch& R, uint32_t* ctr,
                    uint32_t* hdr, uint32_t* clear_block, uint32_t* cout, int sms, cudaStream_t st) {

@@ -63,6 +63,15 @@ def lib():
         L.rt_kernel_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
         L.rt_capture_rays.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), u32, vp, i64,
                                       C.POINTER(i64)]
+        L.rt_guide_init.argtypes = [vp, C.POINTER(abi.RtGuideParams)]
+        L.rt_guide_mode.argtypes = [vp, i32]
+        L.rt_guide_params.argtypes = [vp, vp, i32]
+        L.rt_guide_eval.argtypes = [vp, vp, i64, vp, i32]
+        L.rt_guide_pdf.argtypes = [vp, vp, vp, i64, vp, i32]
+        L.rt_guide_sample.argtypes = [vp, vp, vp, i64, vp, i32]
+        L.rt_guide_loss_grad.argtypes = [vp, vp, i64, C.POINTER(f), vp]
+        L.rt_guide_train.argtypes = [vp, vp, i64, i32, C.POINTER(f)]
+        L.rt_guide_stats.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -115,6 +124,21 @@ def pass_params(width, height, sample_idx=0, n_samples=1, strata=None, max_depth
     if frame_time is not None:
         p.use_frame_time = 1
         p.t0, p.t1 = float(frame_time[0]), float(frame_time[1])
+    return p
+
+
+def guide_params(lr=1e-2, batch=65536, steps_per_pass=4, record_capacity=1 << 24, min_resolution=16,
+                 level_scale=1.447, seed=1, domain=None, beta1=0.9, beta2=0.99, epsilon=1e-8):
+    """RtGuideParams with the learned proposal's defaults (16 levels from 16 to
+    ≈4096 cells, Adam lr 1e-2); domain None: the scene bounds."""
+    p = abi.RtGuideParams()
+    if domain is not None:
+        lo, hi = domain
+        p.domain_min[:] = [float(x) for x in lo]
+        p.domain_max[:] = [float(x) for x in hi]
+    p.learning_rate, p.beta1, p.beta2, p.epsilon = lr, beta1, beta2, epsilon
+    p.batch, p.steps_per_pass, p.record_capacity = batch, steps_per_pass, record_capacity
+    p.min_resolution, p.level_scale, p.seed = min_resolution, level_scale, seed
     return p
 
 
@@ -327,6 +351,69 @@ class GpuScene:
         return idx, d2
 
     # ── diagnostics ──────────────────────────────────────────────────────
+    # ── path guiding (rt_guide_*) ─────────────────────────────────────────
+    def guide_init(self, params=None):
+        """Create the guide network with fresh parameters (mode off)."""
+        self._gp = params if params is not None else guide_params()
+        self._check(lib().rt_guide_init(self.h, C.byref(self._gp)))
+
+    def guide_mode(self, mode):
+        """0: plain cosine bounces, 1: guided (frozen), 2: guided + training after each render call."""
+        self._check(lib().rt_guide_mode(self.h, int(mode)))
+
+    def guide_get_params(self):
+        out = np.zeros(abi.RT_GUIDE_PARAMS, np.float32)
+        self._check(lib().rt_guide_params(self.h, C.c_void_p(out.ctypes.data), 0))
+        return out
+
+    def guide_set_params(self, params):
+        params = np.ascontiguousarray(params, np.float32)
+        assert params.size == abi.RT_GUIDE_PARAMS
+        self._check(lib().rt_guide_params(self.h, C.c_void_p(params.ctypes.data), 1))
+
+    def guide_eval(self, q):
+        q = np.ascontiguousarray(np.asarray(q, np.float32).reshape(-1, 6))
+        out = np.zeros((len(q), 41), np.float32)
+        self._check(lib().rt_guide_eval(self.h, C.c_void_p(q.ctypes.data), len(q), C.c_void_p(out.ctypes.data),
+                                        abi.RT_MEM_HOST))
+        return out
+
+    def guide_pdf(self, q, dirs):
+        q = np.ascontiguousarray(np.asarray(q, np.float32).reshape(-1, 6))
+        d = np.ascontiguousarray(np.asarray(dirs, np.float32).reshape(-1, 3))
+        out = np.zeros(len(q), np.float32)
+        self._check(lib().rt_guide_pdf(self.h, C.c_void_p(q.ctypes.data), C.c_void_p(d.ctypes.data), len(q),
+                                       C.c_void_p(out.ctypes.data), abi.RT_MEM_HOST))
+        return out
+
+    def guide_sample(self, q, u):
+        q = np.ascontiguousarray(np.asarray(q, np.float32).reshape(-1, 6))
+        u = np.ascontiguousarray(np.asarray(u, np.float32).reshape(-1, 4))
+        out = np.zeros((len(q), 4), np.float32)
+        self._check(lib().rt_guide_sample(self.h, C.c_void_p(q.ctypes.data), C.c_void_p(u.ctypes.data), len(q),
+                                          C.c_void_p(out.ctypes.data), abi.RT_MEM_HOST))
+        return out
+
+    def guide_loss_grad(self, samples):
+        """(loss, gradient) of samples n × 10 (position, normal, direction, weight)."""
+        s = np.ascontiguousarray(np.asarray(samples, np.float32).reshape(-1, 10))
+        g = np.zeros(abi.RT_GUIDE_PARAMS, np.float32)
+        loss = C.c_float()
+        self._check(lib().rt_guide_loss_grad(self.h, C.c_void_p(s.ctypes.data), len(s), C.byref(loss),
+                                             C.c_void_p(g.ctypes.data)))
+        return loss.value, g
+
+    def guide_train(self, samples, steps=1):
+        s = np.ascontiguousarray(np.asarray(samples, np.float32).reshape(-1, 10))
+        loss = C.c_float()
+        self._check(lib().rt_guide_train(self.h, C.c_void_p(s.ctypes.data), len(s), int(steps), C.byref(loss)))
+        return loss.value
+
+    def guide_stats(self):
+        r, n, st, ms = C.c_int64(), C.c_int64(), C.c_int64(), C.c_double()
+        self._check(lib().rt_guide_stats(self.h, C.byref(r), C.byref(n), C.byref(st), C.byref(ms)))
+        return dict(records=r.value, samples=n.value, steps=st.value, train_ms=ms.value)
+
     def set_profiling(self, enable=True):
         self._check(lib().rt_set_profiling(self.h, 1 if enable else 0))
 

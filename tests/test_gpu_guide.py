@@ -1,0 +1,148 @@
+"""The path-guiding network on the GPU against its CPU restatement
+(oracle/guide.py): network outputs, mixture densities and draws, the
+gradient of the loss over every parameter, one Adam step; then, on the
+slit-light room, that guided rendering stays unbiased and what the trained
+network gains over cosine bounces at equal samples."""
+import numpy as np
+import pytest
+
+from oracle import guide as OG
+from rustracer_b200 import configs
+from rustracer_b200.guiding import relmse, render_guided
+from rustracer_b200.renderer import GpuScene, guide_params, pass_params
+from tests.test_gpu_render import assert_tiles_agree
+
+pytestmark = pytest.mark.gpu
+
+RES = OG.resolutions()
+LO, INV = np.zeros(3, np.float32), np.ones(3, np.float32)
+
+
+def _scene():
+    sb, _ = configs.box_scene(width=32, height=32)
+    gs = GpuScene(sb)
+    gs.guide_init(guide_params(domain=((0, 0, 0), (1, 1, 1)), batch=1024))
+    return gs
+
+
+def _params(seed=11):
+    p = OG.init_params(seed)
+    rng = np.random.default_rng(seed + 1)
+    p[OG.N_MLP:] = rng.uniform(-0.5, 0.5, p.size - OG.N_MLP).astype(np.float32)   # features that matter
+    return p
+
+
+def _queries(n, seed=2):
+    rng = np.random.default_rng(seed)
+    P = rng.uniform(-0.05, 1.05, (n, 3)).astype(np.float32)       # a few outside the box: clamped
+    N = rng.normal(size=(n, 3))
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    return P, N.astype(np.float32)
+
+
+def test_guide_network_outputs_match_oracle():
+    gs = _scene()
+    p = _params()
+    gs.guide_set_params(p)
+    assert np.array_equal(gs.guide_get_params(), p)
+    P, N = _queries(4096)
+    gpu = gs.guide_eval(np.concatenate([P, N], 1))
+    X = OG.encode(p, RES, LO, INV, P, N)
+    cpu, _ = OG.forward(p, X)
+    cpu = cpu[:, :41]
+    scale = cpu.std()
+    err = np.abs(gpu - cpu)
+    assert np.isfinite(gpu).all()
+    assert np.quantile(err, 0.99) < 1e-3 * scale, np.quantile(err, 0.99) / scale
+    assert err.max() < 5e-2 * scale, err.max() / scale
+
+
+def test_guide_density_and_draws():
+    gs = _scene()
+    gs.guide_set_params(_params(21))
+    n = 1 << 18
+    P, N = _queries(n, 4)
+    q = np.concatenate([P, N], 1)
+    raw = gs.guide_eval(q)
+    rng = np.random.default_rng(9)
+    D = rng.normal(size=(n, 3))
+    D /= np.linalg.norm(D, axis=1, keepdims=True)
+    pdf = gs.guide_pdf(q, D)
+    ref = OG.guide_pdf(raw, N, D)
+    assert np.allclose(pdf, ref, rtol=2e-3, atol=1e-6)
+    u = rng.random((n, 4)).astype(np.float32)
+    out = gs.guide_sample(q, u)
+    d = out[:, :3]
+    assert np.allclose(np.linalg.norm(d, axis=1), 1.0, atol=1e-5)
+    assert np.allclose(out[:, 3], gs.guide_pdf(q, d), rtol=1e-6)
+    assert np.allclose(out[:, 3], OG.guide_pdf(raw, N, d), rtol=2e-3, atol=1e-6)
+    # E[cos⁺/p] over draws from p is ∫ cos⁺ = π for every row's mixture
+    est = np.maximum((d * N).sum(1), 0) / out[:, 3]
+    assert abs(est.mean() / np.pi - 1) < 1e-2, est.mean() / np.pi
+
+
+def _samples(n, seed=6):
+    rng = np.random.default_rng(seed)
+    P, N = _queries(n, seed)
+    D = rng.normal(size=(n, 3))
+    D /= np.linalg.norm(D, axis=1, keepdims=True)
+    D = np.where(((D * N).sum(1) < 0)[:, None] & (rng.random((n, 1)) < 0.8), -D, D)
+    w = rng.exponential(1.0, n)
+    w[rng.random(n) < 0.1] = 0.0
+    return np.concatenate([P, N, D, w[:, None]], 1).astype(np.float32)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a.astype(np.float64) - b) / max(np.linalg.norm(b.astype(np.float64)), 1e-30)
+
+
+def test_guide_gradient_matches_oracle():
+    gs = _scene()
+    p = _params(31)
+    gs.guide_set_params(p)
+    s = _samples(1500)
+    loss, g = gs.guide_loss_grad(s)
+    lref, gref = OG.loss_and_grad(p, RES, LO, INV, s)
+    assert abs(loss / lref - 1) < 1e-3
+    for name, sl in (("W0", slice(0, 4096)), ("W1", slice(4096, 8192)), ("W2", slice(8192, 12288)),
+                     ("W3", slice(12288, OG.N_MLP)), ("table", slice(OG.N_MLP, None))):
+        r = _rel(g[sl], gref[sl])
+        assert r < 2e-2, (name, r)
+    assert np.array_equal(g[12288 + 41 * 64:OG.N_MLP], np.zeros(7 * 64, np.float32))   # padded outputs
+
+
+def test_guide_adam_step_matches_oracle():
+    gs = _scene()
+    p = _params(41)
+    gs.guide_set_params(p)
+    s = _samples(1024, 8)
+    _, g = gs.guide_loss_grad(s)
+    gs.guide_train(s, steps=1)
+    p1 = gs.guide_get_params()
+    ref, _, _ = OG.adam(p, np.zeros_like(p), np.zeros_like(p), g, 1)
+    big = np.abs(g) > 1e-4 * np.abs(g).max()
+    assert big.sum() > 1000
+    assert np.allclose(p1[big], ref[big], rtol=0, atol=1e-6 + 1e-3 * 1e-2)
+    assert np.abs(p1 - ref).max() <= 2.0e-2 + 1e-6            # sign of a near-zero gradient at worst
+    assert np.array_equal(p1[g == 0], p[g == 0])
+
+
+def test_guided_render_is_unbiased_and_gains_over_plain():
+    w = h = 64
+    sb, st = configs.guided_box_scene(width=w, height=h, max_depth=24)
+    gs = GpuScene(sb)
+    cam, hero = st["camera"], st["hero"]
+    base = pass_params(w, h, 0, 1, 8, 24, hero, 1.0, 5)
+    _, _, stats = render_guided(gs, cam, base, 48, train_spp=48, guide=guide_params(batch=16384, seed=3))
+    assert stats["steps"] == 48 * 4 and stats["samples"] > 10_000
+    gs.guide_mode(1)
+    spp = 256
+    gi = gs.render_pass(cam, pass_params(w, h, 1000, spp, 16, 24, hero, 1.0, 7))
+    gs.guide_mode(0)
+    pi = gs.render_pass(cam, pass_params(w, h, 1000, spp, 16, 24, hero, 1.0, 8))
+    assert np.isfinite(gi).all()
+    assert_tiles_agree(gi, pi)                                   # guided bounces leave the mean alone
+    ref = gs.render_pass(cam, pass_params(w, h, 0, 4096, 64, 24, hero, 1.0, 9)).mean(0)
+    e_g, e_p = relmse(gi.mean(0), ref), relmse(pi.mean(0), ref)
+    print(f"relMSE at {spp} spp: guided {e_g:.4g}, plain {e_p:.4g}")
+    assert e_g < e_p
