@@ -493,63 +493,70 @@ def run_guided(args):
     """Learned proposal against cosine bounces at equal GPU time on the
     slit-light room (1280x720, depth 24): a plain render of --plain-spp is
     timed and scored against a plain --ref-spp reference; a fresh network is
-    trained during the guided render's first 64 spp (one call per sample pass,
-    4 Adam steps of 65,536 records after each) and then frozen, and the guided
-    render's relMSE is read at checkpoints.  `value` is the GPU time the
-    guided render needs to reach the plain render's relMSE over the plain
-    render's time (interpolated in log-log between checkpoints; training
-    included), lower is better."""
-    from rustracer_b200 import configs
+    trained during the guided render's first 64 spp (render calls of 4 spp,
+    16 Adam steps of 65,536 records after each) and then frozen, and the
+    guided render's relMSE is read at checkpoints.  `value` is the GPU time
+    the guided render needs to reach the plain render's relMSE over the plain
+    render's time (log-log interpolation between checkpoints; training
+    included), lower is better.  Times are the library's CUDA-event times of
+    the render calls; accumulators stay on the device."""
+    import torch
+    from rustracer_b200 import abi, configs
     from rustracer_b200.guiding import relmse
     from rustracer_b200.renderer import GpuScene, guide_params, pass_params
-    from rustracer_b200 import abi
     sb, st = configs.guided_box_scene()
     w, h, depth, hero = st["width"], st["height"], st["max_depth"], st["hero"]
     scene = GpuScene(sb, device=0)
     cam = st["camera"]
+    dev = torch.device("cuda", 0)
+    outs = (torch.zeros((h, w, 3), device=dev), torch.zeros((h, w, 3), device=dev),
+            torch.zeros((h, w), dtype=torch.int32, device=dev))
 
     def acc(sample_idx, n, seed, reset):
-        s, _, c = scene.render_accumulate(cam, pass_params(w, h, sample_idx, n, 16, depth, hero, 1.0, seed),
-                                          reset=reset)
-        return s / np.maximum(c, 1)[..., None], scene.last_stats()["ms"]
+        scene.render_accumulate(cam, pass_params(w, h, sample_idx, n, 16, depth, hero, 1.0, seed), reset=reset,
+                                outputs=outs)
+        return scene.last_stats()["ms"]
 
-    # reference: plain, --ref-spp in calls of 256
-    ref, ref_ms = None, 0.0
-    for k in range(0, args.ref_spp, 256):
-        ref, ms = acc(k, min(256, args.ref_spp - k), 101, k == 0)
-        ref_ms += ms
+    def image():
+        s, _, c = outs
+        return (s / c.clamp(min=1)[..., None].float()).cpu().numpy()
+
+    ref_ms = 0.0
+    for k in range(0, args.ref_spp, 512):
+        ref_ms += acc(k, min(512, args.ref_spp - k), 101, k == 0)
+    ref = image()
     scene.guide_mode(abi.RT_GUIDE_OFF)
     acc(0, 4, 7, True)                                    # warm-up
-    img_p, t_p = acc(0, args.plain_spp, 7, True)
-    e_p = relmse(img_p, ref)
-    # guided: train for 64 spp, then frozen; checkpoints of (GPU ms, relMSE)
-    scene.guide_init(guide_params(batch=65536, steps_per_pass=4, seed=3))
+    t_p = acc(0, args.plain_spp, 7, True)
+    e_p = relmse(image(), ref)
+    scene.guide_init(guide_params(batch=65536, steps_per_pass=16, seed=3))
     scene.guide_mode(abi.RT_GUIDE_TRAIN)
     t_g, done, pts = 0.0, 0, []
-    for _ in range(64):
-        img, ms = acc(done, 1, 9, done == 0)
-        t_g += ms
-        done += 1
-    pts.append((t_g, relmse(img, ref), done))
+    while done < 64:
+        t_g += acc(done, 4, 9, done == 0)
+        done += 4
+    pts.append((t_g, relmse(image(), ref), done))
     scene.guide_mode(abi.RT_GUIDE_SAMPLE)
     while done < 4 * args.plain_spp and (pts[-1][1] > e_p or t_g < t_p):
         n = max(16, done // 4)
-        img, ms = acc(done, n, 9, False)
-        t_g += ms
+        t_g += acc(done, n, 9, False)
         done += n
-        pts.append((t_g, relmse(img, ref), done))
+        pts.append((t_g, relmse(image(), ref), done))
     gstats = scene.guide_stats()
     scene.guide_mode(abi.RT_GUIDE_OFF)
+    t_plain_frozen = acc(0, 64, 13, True)
+    scene.guide_mode(abi.RT_GUIDE_SAMPLE)
+    t_guided_frozen = acc(0, 64, 13, True)
+    scene.guide_mode(abi.RT_GUIDE_OFF)
 
-    def interp(key_i, key_v, x):
-        # log-log interpolation of column key_v at key_i = x
-        for (a, b) in zip(pts, pts[1:]):
-            if (a[key_i] - x) * (b[key_i] - x) <= 0 and a[key_i] != b[key_i]:
-                f = (np.log(x) - np.log(a[key_i])) / (np.log(b[key_i]) - np.log(a[key_i]))
-                return float(np.exp(np.log(a[key_v]) + f * (np.log(b[key_v]) - np.log(a[key_v]))))
+    def interp(ki, kv, x):
+        # log-log interpolation of column kv where column ki = x
+        for a, b in zip(pts, pts[1:]):
+            if (a[ki] - x) * (b[ki] - x) <= 0 and a[ki] != b[ki]:
+                f = (np.log(x) - np.log(a[ki])) / (np.log(b[ki]) - np.log(a[ki]))
+                return float(np.exp(np.log(a[kv]) + f * (np.log(b[kv]) - np.log(a[kv]))))
         return None
     t_match = interp(1, 0, e_p) if pts[-1][1] <= e_p else None
-    e_eq = interp(0, 1, t_p)
     line = {
         "metric": "equal-time relMSE: guided GPU time to reach the plain render's relMSE / plain GPU time "
                   "(slit-light room)",
@@ -558,8 +565,9 @@ def run_guided(args):
         "data": "synthetic (box room, slit light, round brilliant, Perlin medium; random-init network trained online)",
         "config": {"workload": st["name"], "reference": f"plain {args.ref_spp} spp ({ref_ms / 1000:.1f} s)",
                    "plain": f"{args.plain_spp} spp, {t_p:.0f} ms, relMSE {e_p:.5g}",
-                   "guided_relmse_at_equal_time": e_eq,
+                   "guided_relmse_at_equal_time": interp(0, 1, t_p),
                    "guided_checkpoints": [{"ms": round(a, 1), "relmse": b, "spp": c} for a, b, c in pts],
+                   "cost_per_spp_ms": {"plain": round(t_plain_frozen / 64, 3), "guided": round(t_guided_frozen / 64, 3)},
                    "training": {"records": gstats["records"], "samples": gstats["samples"],
                                 "adam_steps": gstats["steps"], "train_ms": round(gstats["train_ms"], 1)},
                    "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)"},
@@ -608,10 +616,28 @@ def one_pass():
     print("pass ok", scene.last_stats(), flush=True)
 
 
+def one_pass_guided():
+    """Profiler driver for the learned proposal: the 1280×720 slit-light room,
+    16 spp of training (4 render calls of 4 spp, 16 Adam steps after each),
+    then one frozen guided call of 16 spp."""
+    from rustracer_b200 import abi, configs
+    from rustracer_b200.renderer import GpuScene, guide_params, pass_params
+    sb, st = configs.guided_box_scene()
+    w, h, depth, hero = st["width"], st["height"], st["max_depth"], st["hero"]
+    scene = GpuScene(sb, device=0)
+    scene.guide_init(guide_params(seed=3))
+    scene.guide_mode(abi.RT_GUIDE_TRAIN)
+    for k in range(4):
+        scene.render_accumulate(st["camera"], pass_params(w, h, 4 * k, 4, 16, depth, hero, 1.0, 9), reset=k == 0)
+    scene.guide_mode(abi.RT_GUIDE_SAMPLE)
+    scene.render_accumulate(st["camera"], pass_params(w, h, 16, 16, 16, depth, hero, 1.0, 9), reset=False)
+    print("pass ok", scene.last_stats(), scene.guide_stats(), flush=True)
+
+
 def main():
     args = parse()
     if args.mode == "pass":
-        one_pass()
+        one_pass_guided() if args.config == "guided" else one_pass()
         return
     if args.impl == "reference":
         run_reference(args)

@@ -487,13 +487,14 @@ int32_t rt_render_pass_noalloc(RtScene* scene, const RtCamera* cam, const RtPass
  * entries per level) and a one-blob encoding of the shading normal feed a
  * 64-64-64 ReLU MLP (BF16 weights and activations, FP32 accumulation) whose
  * 41 outputs are 8 von Mises–Fisher lobes (mean, log κ, mixture logit) and a
- * guide fraction α ≤ 0.9.  With guiding on, a Lambertian bounce is drawn with
+ * guide fraction α ≤ alpha_max.  With guiding on, a Lambertian bounce is drawn with
  * probability α from the lobes and otherwise from the cosine lobe, weighted
  * by the exact mixture density; NEE and bounce MIS use the same density, so
  * the estimator stays unbiased.  In training mode every render call records
  * (position, normal, direction, f·L·cos/p) at its guided vertices and, after
- * the call, takes `steps_per_pass` Adam steps on minibatches of them,
- * minimising −w·log p (the KL divergence to the product distribution).
+ * the call, takes `steps_per_pass` Adam steps on minibatches of them: the
+ * lobes minimise −w·log p_vmf (the KL divergence from the product
+ * distribution), α minimises −w·log p_mix with the lobes held fixed.
  * rt_render_pass_noalloc never guides. */
 typedef struct RtGuideParams {
     float    domain_min[3], domain_max[3]; /* hash-grid box in world space; min == max: the scene bounds */
@@ -502,8 +503,10 @@ typedef struct RtGuideParams {
     uint32_t batch;                        /* training minibatch rows, a multiple of 1024 (65536) */
     uint32_t steps_per_pass;               /* Adam steps after each training render call */
     uint32_t record_capacity;              /* training records kept per render call */
-    uint32_t min_resolution;               /* grid resolution of the coarsest level (16) */
-    float    level_scale;                  /* resolution growth per level (1.447: 16 → ≈4096) */
+    uint32_t min_resolution;               /* grid resolution of the coarsest level (4) */
+    float    level_scale;                  /* resolution growth per level (1.32: 4 → ≈257) */
+    float    alpha_max;                    /* cap of the guide fraction α, in (0, 1); the cosine lobe keeps the rest */
+    float    log_kappa_max;                /* cap of log κ of a lobe, in (−5, 20] */
     uint64_t seed;                         /* initial parameters and minibatch draws */
 } RtGuideParams;
 

@@ -18,7 +18,7 @@ the GPU network is built from, at the GPU's rounding points:
     (float64) and rounded to float32 — the GPU sums in float32 on the tensor
     cores, so outputs agree to float32 rounding and an occasional one-ulp
     BF16 flip;
-  * 8 von Mises–Fisher lobes and a guide fraction α = 0.9·sigmoid, mixed
+  * 8 von Mises–Fisher lobes and a guide fraction α = amax·sigmoid, mixed
     with the cosine lobe by one-sample MIS; loss −w·log p and its analytic
     gradient; Adam (Kingma & Ba 2015) with bias-corrected moments.
 Parity: this oracle has no reference counterpart to pin against; the GPU
@@ -29,7 +29,8 @@ import numpy as np
 LEVELS, TSIZE, NIN, NHID, NOUT, NOUTP, NLOBE = 16, 1 << 19, 64, 64, 41, 48, 8
 N_MLP = 3 * NHID * NIN + NOUTP * NHID
 N_PARAMS = N_MLP + LEVELS * TSIZE * 2
-ALPHA_MAX, LOGK_LO, LOGK_HI = 0.9, -5.0, 7.0
+LOGK_LO = -5.0
+AMAX, LKMAX = 0.9, 7.0            # caps of α and log κ used when a call names none
 f32 = np.float32
 
 
@@ -127,18 +128,18 @@ def forward(params, X):
     return _mm(H3, W[3].T), (X, H1, H2, H3)
 
 
-def mixture(o):
+def mixture(o, amax=AMAX, lkmax=LKMAX):
     """Per-row mixture: mu (n, 8, 3), kappa (n, 8), pi (n, 8), alpha (n,)."""
     o = np.asarray(o, np.float64)[:, :NOUT]
     lob = o[:, :40].reshape(-1, NLOBE, 5)
     v = lob[:, :, :3]
     ln = np.linalg.norm(v, axis=2)
     mu = np.where(ln[..., None] > 1e-12, v / np.maximum(ln, 1e-300)[..., None], np.array([0.0, 0.0, 1.0]))
-    k = np.exp(np.clip(lob[:, :, 3], LOGK_LO, LOGK_HI))
+    k = np.exp(np.clip(lob[:, :, 3], LOGK_LO, lkmax))
     lg = lob[:, :, 4]
     e = np.exp(lg - lg.max(1, keepdims=True))
     pi = e / e.sum(1, keepdims=True)
-    alpha = ALPHA_MAX / (1 + np.exp(-o[:, 40]))
+    alpha = amax / (1 + np.exp(-o[:, 40]))
     return mu, k, pi, alpha, ln
 
 
@@ -146,9 +147,9 @@ def vmf_norm(k):
     return k / (2 * np.pi * -np.expm1(-2 * k))
 
 
-def guide_pdf(o, N, D):
+def guide_pdf(o, N, D, amax=AMAX, lkmax=LKMAX):
     """Density of the one-sample mixture (guide and cosine lobe about N) at unit D."""
-    mu, k, pi, a, _ = mixture(o)
+    mu, k, pi, a, _ = mixture(o, amax, lkmax)
     D = np.asarray(D, np.float64)
     c = np.einsum("nlj,nj->nl", mu, D)
     pg = (pi * vmf_norm(k) * np.exp(k * (c - 1))).sum(1)
@@ -156,10 +157,13 @@ def guide_pdf(o, N, D):
     return a * pg + (1 - a) * pb
 
 
-def loss_grad(o, N, D, w, scale):
-    """−w·log p per row and ∂(scale·loss)/∂o (n, 41)."""
+def loss_grad(o, N, D, w, scale, amax=AMAX, lkmax=LKMAX):
+    """−w·log p_mix per row and the training gradient (n, 41), times scale:
+    the lobe outputs descend −w·log p_vmf (the vMF mixture alone), the α
+    output descends −w·log p_mix with the lobes fixed; densities floored at
+    1e-8."""
     o = np.asarray(o, np.float64)[:, :NOUT]
-    mu, k, pi, a, ln = mixture(o)
+    mu, k, pi, a, ln = mixture(o, amax, lkmax)
     D = np.asarray(D, np.float64)
     N = np.asarray(N, np.float64)
     w = np.asarray(w, np.float64)
@@ -168,29 +172,30 @@ def loss_grad(o, N, D, w, scale):
     pg = (pi * f).sum(1)
     pb = np.maximum((N * D).sum(1), 0) / np.pi
     sg = 1 / (1 + np.exp(-o[:, 40]))
-    p = np.maximum(a * pg + (1 - a) * pb, 1e-30)
+    p = np.maximum(a * pg + (1 - a) * pb, 1e-8)
     loss = -w * np.log(p)
     dp = -w / p * scale
     g = np.zeros((len(o), NOUT))
-    g[:, 40] = dp * (pg - pb) * ALPHA_MAX * sg * (1 - sg)
-    gpi = dp[:, None] * a[:, None] * f
+    g[:, 40] = dp * (pg - pb) * amax * sg * (1 - sg)
+    dq = -w / np.maximum(pg, 1e-8) * scale
+    gpi = dq[:, None] * f
     gs = (pi * gpi).sum(1, keepdims=True)
     lob = np.zeros((len(o), NLOBE, 5))
     lob[:, :, 4] = pi * (gpi - gs)
-    df = dp[:, None] * a[:, None] * pi * f
+    df = dq[:, None] * pi * f
     lk = o[:, :40].reshape(-1, NLOBE, 5)[:, :, 3]
     with np.errstate(over="ignore"):
         dlk = 1 / k - 2 / np.expm1(2 * k) + (c - 1)
-    lob[:, :, 3] = np.where((lk > LOGK_LO) & (lk < LOGK_HI), df * dlk * k, 0)
+    lob[:, :, 3] = np.where((lk > LOGK_LO) & (lk < lkmax), df * dlk * k, 0)
     cm = np.where(ln > 1e-12, df * k / np.maximum(ln, 1e-300), 0)
     lob[:, :, :3] = cm[..., None] * (D[:, None, :] - mu * c[..., None])
     g[:, :40] = lob.reshape(-1, 40)
     return loss, g
 
 
-def loss_and_grad(params, res, lo, inv, samples):
-    """Σ loss and the gradient of (Σ loss)/n over all parameters, following the
-    GPU's rounding points: dO, dZ in BF16, weight gradients summed exactly,
+def loss_and_grad(params, res, lo, inv, samples, amax=AMAX, lkmax=LKMAX):
+    """Σ loss (−w·log p_mix) and the training gradient over all parameters
+    (loss_grad's objectives over n), following the GPU's rounding points: dO, dZ in BF16, weight gradients summed exactly,
     hash-grid gradients as float32 products scattered per corner."""
     s = np.asarray(samples, f32).reshape(-1, 10)
     n = len(s)
@@ -199,7 +204,7 @@ def loss_and_grad(params, res, lo, inv, samples):
     O, (X, H1, H2, H3) = forward(params, X)
     W = weights(params)
     valid = w > 0
-    loss, g = loss_grad(O, N, D, w, 1.0 / n)
+    loss, g = loss_grad(O, N, D, w, 1.0 / n, amax, lkmax)
     g[~valid] = 0
     dO = np.zeros((n, NOUTP), f32)
     dO[:, :NOUT] = g.astype(f32)

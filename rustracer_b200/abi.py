@@ -237,6 +237,8 @@ class RtGuideParams(C.Structure):
         ("record_capacity", C.c_uint32),
         ("min_resolution", C.c_uint32),
         ("level_scale", C.c_float),
+        ("alpha_max", C.c_float),
+        ("log_kappa_max", C.c_float),
         ("seed", C.c_uint64),
     ]
 

@@ -396,29 +396,37 @@ def gem_room_scene(width=1200, height=800, spp=128, max_depth=50, photons=500_00
                     photons=photons, radius=gather_radius)
 
 
-def guided_box_scene(width=1280, height=720, spp=64, max_depth=24, hero=4, seed=9, density=4.0):
+def guided_box_scene(width=1280, height=720, spp=64, max_depth=24, hero=4, seed=9, density=4.0, gem=True,
+                     medium=True):
     """The hard-transport workload of the learned proposal: the box room with
     its light hidden above two occluding quads that leave a 0.05-wide slit, a
     round brilliant (the gem workload's, radius 0.12, diamond dispersion) and a
     Perlin-noise medium in the lower half (σ_t up to `density`, albedo 0.9,
     g = 0.3; the reference's noise medium, volume.rs, stands in for a 128³
-    density grid).  Most light reaches the room through the slit and by way of
-    the occluders' tops and the ceiling, which cosine bounces find rarely."""
+    density grid).  Light enters the room only through the slit, as a narrow
+    beam onto the floor and the medium; everything else is lit by that patch,
+    which cosine bounces find rarely and light sampling cannot reach."""
     sb, st = box_scene(width, height, spp, max_depth, hero, seed)
     sb.name = "guided box"
     sb.spheres.clear()
     white = sb.add_material(Material.lambertian((0.73, 0.73, 0.73)))
-    # occluders 0.05 below the light, covering x, z ∈ [0.2, 0.8] but the slit x ∈ [0.475, 0.525]
+    # occluders 0.05 below the light spanning the room but for a slit 0.05 wide and 0.1
+    # long (x ∈ [0.475, 0.525], z ∈ [0.45, 0.55]): the light reaches the room through
+    # the slit alone, as a small bright patch on the floor
     y = 1.0 - 0.05
-    sb.add_quad((0.2, y, 0.2), (0.275, 0.0, 0.0), (0.0, 0.0, 0.6), white)
-    sb.add_quad((0.525, y, 0.2), (0.275, 0.0, 0.0), (0.0, 0.0, 0.6), white)
+    sb.add_quad((0.0, y, 0.0), (0.475, 0.0, 0.0), (0.0, 0.0, 1.0), white)
+    sb.add_quad((0.525, y, 0.0), (0.475, 0.0, 0.0), (0.0, 0.0, 1.0), white)
+    sb.add_quad((0.475, y, 0.0), (0.05, 0.0, 0.0), (0.0, 0.0, 0.45), white)
+    sb.add_quad((0.475, y, 0.55), (0.05, 0.0, 0.0), (0.0, 0.0, 0.45), white)
     diffuse = sb.add_material(Material.lambertian((0.73, 0.73, 0.73)))
     sb.add_sphere((0.3, 0.18, 0.6), 0.18, diffuse)
-    V, Fc = round_brilliant(radius=0.12, center=(0.68, 0.62, 0.45))
-    diamond = sb.add_material(Material.spectral_dielectric_cauchy(2.351, 0.0230))
-    sb.add_mesh(V, Fc, diamond)
-    sb.add_medium("noise", "box", density, (0.9, 0.9, 0.9), g=0.3, noise_scale=4.0, threshold=0.05,
-                  p_min=(0.0, 0.0, 0.0), p_max=(1.0, 0.5, 1.0), seed=seed)
+    if gem:
+        V, Fc = round_brilliant(radius=0.12, center=(0.68, 0.62, 0.45))
+        diamond = sb.add_material(Material.spectral_dielectric_cauchy(2.351, 0.0230))
+        sb.add_mesh(V, Fc, diamond)
+    if medium:
+        sb.add_medium("noise", "box", density, (0.9, 0.9, 0.9), g=0.3, noise_scale=4.0, threshold=0.05,
+                      p_min=(0.0, 0.0, 0.0), p_max=(1.0, 0.5, 1.0), seed=seed)
     st["name"] = f"guided box (slit light, gem, medium) {width}x{height} {spp}spp depth{max_depth} hero{hero}"
     return sb, st
 

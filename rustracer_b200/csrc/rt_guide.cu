@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(GW * 32) k_guide_api(GuideDev G, const float* 
                 for (int k = 0; k < NOUT; k++) raw[(size_t)r * NOUT + k] = o[k];
             if (!out) return;
             float4 gp[GP_F4];
-            mixture_from_outputs(o, gp);
+            mixture_from_outputs(o, gp, G.amax, G.lkmax);
             float nx = q[r * 6 + 3], ny = q[r * 6 + 4], nz = q[r * 6 + 5];
             if (dirs) {
                 out[r] = guide_pdf(gp, nx, ny, nz, dirs[r * 3], dirs[r * 3 + 1], dirs[r * 3 + 2]);
@@ -252,7 +252,8 @@ __global__ void __launch_bounds__(GW * 32) k_train(GuideDev G, TrainArgs A) {
                 rv = train_row(A, row0 + lane, n, r) && r[0].w > 0.0f;
                 float g[NOUT];
                 if (rv) {
-                    lsum += loss_grad(S_o + lane * LDO, r[1].x, r[1].y, r[1].z, r[2].x, r[2].y, r[2].z, r[0].w, scale, g);
+                    lsum += loss_grad(S_o + lane * LDO, r[1].x, r[1].y, r[1].z, r[2].x, r[2].y, r[2].z, r[0].w, scale,
+                                      G.amax, G.lkmax, g);
                 } else {
                     for (int k = 0; k < NOUT; k++) g[k] = 0.0f;
                 }
@@ -509,6 +510,8 @@ GuideDev view(const Guide* g) {
     d.wbf = g->wbf;
     for (int a = 0; a < 3; a++) { d.lo[a] = g->lo[a]; d.inv[a] = g->inv[a]; }
     for (int l = 0; l < LEVELS; l++) d.res[l] = g->res[l];
+    d.amax = g->prm.alpha_max;
+    d.lkmax = g->prm.log_kappa_max;
     d.gpar = g->gpar;
     d.rec_a = g->rec_a; d.rec_b = g->rec_b; d.rec_c = g->rec_c; d.rec_w = g->rec_w;
     d.rec_count = g->counters;

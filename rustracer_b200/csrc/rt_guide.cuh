@@ -10,8 +10,8 @@
 // to 48), no biases.  Weights and activations are BF16, products accumulate in
 // FP32 on the tensor cores (mma.sync m16n8k16; one warp evaluates 16 rows).
 //
-// Outputs: 8 von Mises–Fisher lobes (unnormalised mean 3, log κ 1, mixture
-// logit 1) and the guide fraction α = 0.9·sigmoid(o40).  The bounce direction
+// Outputs: 8 von Mises–Fisher lobes (unnormalised mean 3, log κ 1 clamped to
+// [−5, lkmax], mixture logit 1) and the guide fraction α = amax·sigmoid(o40).  The bounce direction
 // is drawn by one-sample MIS: with probability α from the vMF mixture, else
 // from the cosine lobe; its density is α·p_vmf + (1 − α)·cos/π, which is > 0
 // wherever the Lambertian integrand is, so the estimator stays unbiased.
@@ -29,7 +29,7 @@ constexpr int N_MLP = OFF_W3 + NOUTP * NHID;                      // 15360 weigh
 constexpr size_t N_TABLE = (size_t)LEVELS * TSIZE * FEAT;         // 16,777,216 table entries
 constexpr size_t N_PARAMS = (size_t)N_MLP + N_TABLE;
 constexpr int GP_F4 = 11;            // per-path mixture: 8 × (μ, κ), π0..3, π4..7, (α, -, -, -)
-constexpr float ALPHA_MAX = 0.9f, LOGK_LO = -5.0f, LOGK_HI = 7.0f;
+constexpr float LOGK_LO = -5.0f;     // log κ floor; the cap and α's cap are parameters
 constexpr int LDW = NIN + 8;         // padded shared-memory row of a forward weight matrix (bf16)
 constexpr int LDT3 = NOUTP + 8;      // padded row of the transposed output layer
 constexpr int W_SMEM = (3 * NHID + NOUTP) * LDW;                  // forward weights, bf16 elements
@@ -44,6 +44,7 @@ struct GuideDev {
     const __nv_bfloat16* wbf;         // the four layers, [out][in] row-major, bf16
     float lo[3], inv[3];              // hash-grid domain: pn = (p − lo) · inv, clamped to [0, 1]
     uint32_t res[LEVELS];             // grid resolution of each level
+    float amax, lkmax;                // cap of α, cap of log κ
     float4* gpar;                     // GP_F4 float4 per path slot
     float4 *rec_a, *rec_b, *rec_c;    // records: (p, Σ T·sf), (n, base Σ L), (ω_i, prev record)
     float* rec_w;                     // weight of each record, set when its path retires
@@ -225,7 +226,7 @@ RTG_D void load_weights(const __nv_bfloat16* __restrict__ wbf, __nv_bfloat16* Ws
 RTG_HD float vmf_norm(float k) { return k / (6.2831853f * -expm1f(-2.0f * k)); }
 
 // 41 outputs → mixture parameters (GP_F4 float4).
-RTG_HD void mixture_from_outputs(const float* o, float4* gp) {
+RTG_HD void mixture_from_outputs(const float* o, float4* gp, float amax, float lkmax) {
     float mx = o[4];
     for (int i = 1; i < NLOBE; i++) mx = fmaxf(mx, o[5 * i + 4]);
     float e[NLOBE], s = 0.0f;
@@ -233,12 +234,12 @@ RTG_HD void mixture_from_outputs(const float* o, float4* gp) {
     for (int i = 0; i < NLOBE; i++) {
         float vx = o[5 * i], vy = o[5 * i + 1], vz = o[5 * i + 2];
         float len = sqrtf(vx * vx + vy * vy + vz * vz);
-        float k = expf(fminf(fmaxf(o[5 * i + 3], LOGK_LO), LOGK_HI));
+        float k = expf(fminf(fmaxf(o[5 * i + 3], LOGK_LO), lkmax));
         gp[i] = len > 1e-12f ? make_float4(vx / len, vy / len, vz / len, k) : make_float4(0.f, 0.f, 1.f, k);
     }
     gp[8] = make_float4(e[0] / s, e[1] / s, e[2] / s, e[3] / s);
     gp[9] = make_float4(e[4] / s, e[5] / s, e[6] / s, e[7] / s);
-    gp[10] = make_float4(ALPHA_MAX / (1.0f + expf(-o[40])), 0.f, 0.f, 0.f);
+    gp[10] = make_float4(amax / (1.0f + expf(-o[40])), 0.f, 0.f, 0.f);
 }
 
 RTG_HD float lobe_weight(const float4* gp, int i) {
@@ -294,11 +295,17 @@ RTG_HD void vmf_mix_sample(const float4* gp, float u0, float u1, float u2, float
     *dx = x * il; *dy = y * il; *dz = z * il;
 }
 
-// −w·log p(ω_i) of one training record and its gradient with respect to the
-// 41 outputs, times `scale` (1/batch): the KL divergence between the density
-// ∝ f·L_i·cos that the weights estimate and the sampling density.
+// The training objective of one record, times `scale` (1/batch), with respect
+// to the 41 outputs.  The lobes descend −w·log p_vmf(ω_i): the KL divergence
+// from the density ∝ f·L_i·cos that the weights estimate to the vMF mixture
+// alone, so they learn whatever α is.  α descends −w·log p_mix(ω_i) with the
+// lobes held fixed (the selection probability learned on its own, as in
+// Müller et al. 2019): minimising the mixture loss jointly collapses α to 0
+// while the untrained lobes explain the records worse than the cosine lobe,
+// and then every lobe gradient carries the factor α.  Densities are floored
+// at 1e-8.  Returns −w·log p_mix.
 RTG_HD float loss_grad(const float* o, float nx, float ny, float nz, float wx, float wy, float wz, float wt,
-                       float scale, float* g) {
+                       float scale, float amax, float lkmax, float* g) {
     float mx = o[4];
     for (int i = 1; i < NLOBE; i++) mx = fmaxf(mx, o[5 * i + 4]);
     float e[NLOBE], s = 0.0f;
@@ -311,26 +318,27 @@ RTG_HD float loss_grad(const float* o, float nx, float ny, float nz, float wx, f
         len[i] = sqrtf(vx * vx + vy * vy + vz * vz);
         if (len[i] > 1e-12f) { mu[i][0] = vx / len[i]; mu[i][1] = vy / len[i]; mu[i][2] = vz / len[i]; }
         else { mu[i][0] = 0.0f; mu[i][1] = 0.0f; mu[i][2] = 1.0f; }
-        k[i] = expf(fminf(fmaxf(o[5 * i + 3], LOGK_LO), LOGK_HI));
+        k[i] = expf(fminf(fmaxf(o[5 * i + 3], LOGK_LO), lkmax));
         c[i] = mu[i][0] * wx + mu[i][1] * wy + mu[i][2] * wz;
         f[i] = vmf_norm(k[i]) * expf(k[i] * (c[i] - 1.0f));
         pg += pi[i] * f[i];
     }
     float sg = 1.0f / (1.0f + expf(-o[40]));
-    float a = ALPHA_MAX * sg;
+    float a = amax * sg;
     float pb = fmaxf(nx * wx + ny * wy + nz * wz, 0.0f) * 0.318309886f;
-    float p = fmaxf(a * pg + (1.0f - a) * pb, 1e-30f);
+    float p = fmaxf(a * pg + (1.0f - a) * pb, 1e-8f);
     float loss = -wt * logf(p);
-    float dp = -wt / p * scale;
-    g[40] = dp * (pg - pb) * ALPHA_MAX * sg * (1.0f - sg);
+    float dp = -wt / p * scale;                              // mixture loss: α only
+    g[40] = dp * (pg - pb) * amax * sg * (1.0f - sg);
+    float dq = -wt / fmaxf(pg, 1e-8f) * scale;               // vMF loss: the lobes
     float gs = 0.0f;
-    for (int i = 0; i < NLOBE; i++) gs += pi[i] * (dp * a * f[i]);
+    for (int i = 0; i < NLOBE; i++) gs += pi[i] * (dq * f[i]);
     for (int i = 0; i < NLOBE; i++) {
-        g[5 * i + 4] = pi[i] * (dp * a * f[i] - gs);
-        float df = dp * a * pi[i] * f[i];                    // ∂loss/∂f_i · f_i
+        g[5 * i + 4] = pi[i] * (dq * f[i] - gs);
+        float df = dq * pi[i] * f[i];                        // ∂loss/∂f_i · f_i
         float lk = o[5 * i + 3];
         float dlk = 1.0f / k[i] - 2.0f / expm1f(2.0f * k[i]) + (c[i] - 1.0f);
-        g[5 * i + 3] = (lk > LOGK_LO && lk < LOGK_HI) ? df * dlk * k[i] : 0.0f;
+        g[5 * i + 3] = (lk > LOGK_LO && lk < lkmax) ? df * dlk * k[i] : 0.0f;
         float cm = len[i] > 1e-12f ? df * k[i] / len[i] : 0.0f;
         g[5 * i] = cm * (wx - mu[i][0] * c[i]);
         g[5 * i + 1] = cm * (wy - mu[i][1] * c[i]);

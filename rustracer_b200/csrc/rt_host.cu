@@ -2268,6 +2268,8 @@ extern "C" int32_t rt_guide_init(RtScene* s, const RtGuideParams* p) {
     if (!(p->learning_rate > 0.0f) || !(p->beta1 >= 0.0f && p->beta1 < 1.0f) || !(p->beta2 >= 0.0f && p->beta2 < 1.0f) ||
         !(p->epsilon > 0.0f))
         return fail(s, RT_ERR_INVALID, "guide Adam parameters");
+    if (!(p->alpha_max > 0.0f && p->alpha_max < 1.0f) || !(p->log_kappa_max > rtg::LOGK_LO && p->log_kappa_max <= 20.0f))
+        return fail(s, RT_ERR_INVALID, "guide caps: alpha_max in (0, 1), log_kappa_max in (-5, 20]");
     if (p->min_resolution < 2 || !(p->level_scale >= 1.0f) ||
         (double)p->min_resolution * std::pow((double)p->level_scale, rtg::LEVELS - 1) > (double)(1u << 20))
         return fail(s, RT_ERR_INVALID, "guide grid resolutions must be in 2..2^20");

@@ -1170,7 +1170,7 @@ __global__ void __launch_bounds__(GUIDE_WARPS * 32) k_guide_infer(DevScene S, Pa
             __syncwarp();
             if (lane < 16 && base + 16 * mt + lane < n) {
                 float4 gp[rtg::GP_F4];
-                rtg::mixture_from_outputs(S_o + lane * GUIDE_LDO, gp);
+                rtg::mixture_from_outputs(S_o + lane * GUIDE_LDO, gp, R.guide.amax, R.guide.lkmax);
                 float4* dst = R.guide.gpar + (size_t)(mt ? pid1 : pid0) * rtg::GP_F4;
 #pragma unroll
                 for (int k = 0; k < rtg::GP_F4; k++) dst[k] = gp[k];

@@ -127,10 +127,15 @@ def pass_params(width, height, sample_idx=0, n_samples=1, strata=None, max_depth
     return p
 
 
-def guide_params(lr=1e-2, batch=65536, steps_per_pass=4, record_capacity=1 << 24, min_resolution=16,
-                 level_scale=1.447, seed=1, domain=None, beta1=0.9, beta2=0.99, epsilon=1e-8):
-    """RtGuideParams with the learned proposal's defaults (16 levels from 16 to
-    ≈4096 cells, Adam lr 1e-2); domain None: the scene bounds."""
+def guide_params(lr=1e-3, batch=65536, steps_per_pass=16, record_capacity=1 << 24, min_resolution=4,
+                 level_scale=1.32, seed=1, domain=None, beta1=0.9, beta2=0.99, epsilon=1e-8, alpha_max=0.5,
+                 log_kappa_max=5.0):
+    """RtGuideParams with the learned proposal's defaults: 16 levels from 4 to
+    ≈257 cells across the scene (finer levels memorise single records: a
+    record's direction is one noisy draw, and at ~4096 cells each record gets
+    a cell of its own), Adam lr 1e-3 (1e-2 and 3e-3 sharpened the lobes on
+    noisy records), α ≤ 0.5 and κ ≤ e^5 (a defensive share for the cosine
+    lobe and no needle lobes); domain None: the scene bounds."""
     p = abi.RtGuideParams()
     if domain is not None:
         lo, hi = domain
@@ -139,6 +144,7 @@ def guide_params(lr=1e-2, batch=65536, steps_per_pass=4, record_capacity=1 << 24
     p.learning_rate, p.beta1, p.beta2, p.epsilon = lr, beta1, beta2, epsilon
     p.batch, p.steps_per_pass, p.record_capacity = batch, steps_per_pass, record_capacity
     p.min_resolution, p.level_scale, p.seed = min_resolution, level_scale, seed
+    p.alpha_max, p.log_kappa_max = alpha_max, log_kappa_max
     return p
 
 

@@ -39,6 +39,8 @@ def test_mixture_density_integrates_to_one():
 
 
 def test_output_gradient_matches_finite_differences():
+    """Lobe outputs: the derivative of −w·log p_vmf; the α output: of
+    −w·log p_mix."""
     rng = np.random.default_rng(5)
     n = 8
     o = rng.normal(0, 1, (n, 41))
@@ -49,14 +51,21 @@ def test_output_gradient_matches_finite_differences():
     D /= np.linalg.norm(D, axis=1, keepdims=True)
     w = rng.uniform(0.1, 2.0, n)
     _, g = G.loss_grad(o, N, D, w, 1.0)
+
+    def lobe_loss(oo):                      # −w·log p_vmf: the lobes' objective
+        mu, k, pi, _, _ = G.mixture(oo)
+        c = np.einsum("nlj,nj->nl", mu, D)
+        return -w * np.log((pi * G.vmf_norm(k) * np.exp(k * (c - 1))).sum(1))
+
+    def mix_loss(oo):                       # −w·log p_mix: α's objective
+        return G.loss_grad(oo, N, D, w, 1.0)[0]
     h = 1e-6
     for k in range(41):
         op, om = o.copy(), o.copy()
         op[:, k] += h
         om[:, k] -= h
-        lp, _ = G.loss_grad(op, N, D, w, 1.0)
-        lm, _ = G.loss_grad(om, N, D, w, 1.0)
-        fd = (lp - lm) / (2 * h)
+        f = mix_loss if k == 40 else lobe_loss
+        fd = (f(op) - f(om)) / (2 * h)
         assert np.allclose(g[:, k], fd, rtol=1e-4, atol=1e-6), k
 
 
