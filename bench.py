@@ -584,6 +584,7 @@ def run_batch(args):
     jobs = batch.make_jobs(seed=0, n=64)
     builders = {k: batch.build_scene(k) for k in batch.SCENES}
     conc = batch.run_batch(jobs, workers=4, builders=builders)
+    tuned = batch.run_batch(jobs, workers=4, builders=builders, tune=True)
     seq = batch.run_batch(jobs, workers=1, builders=builders)
     line = {
         "metric": "path samples/s (64-job batch)", "value": conc["rate"], "unit": UNIT, "n_gpus": 1, "steps": 1,
@@ -594,6 +595,8 @@ def run_batch(args):
                    "path_samples": conc["path_samples"], "workers": 4},
         "latency_s": {"p50": conc["p50_s"], "p99": conc["p99_s"]},
         "sequential": {"value": seq["rate"], "wall_s": seq["wall_s"], "p50": seq["p50_s"], "p99": seq["p99_s"]},
+        "autotuned": {"value": tuned["rate"], "wall_s": tuned["wall_s"], "p50": tuned["p50_s"], "p99": tuned["p99_s"],
+                      "tunings": tuned["tunings"]},
         "timing": "host wall clock around the whole batch (the frames run on several streams)",
     }
     print(json.dumps(line), flush=True)

@@ -479,6 +479,21 @@ int32_t rt_capture_rays(RtScene* scene, const RtCamera* cam, const RtPassParams*
 int32_t rt_render_pass_noalloc(RtScene* scene, const RtCamera* cam, const RtPassParams* params,
                                float* scratch_rgb);
 
+/* ── launch tuning (no counterpart in the reference) ─────────────────────────
+ * The path-pool capacity and the grids of the persistent traversal kernels and
+ * of the shading kernels.  Every path draws its random numbers from (pixel,
+ * sample), so a tuning changes speed and memory, never the image.  Zero fields
+ * select the built-in values (8,388,608 paths; the traversal's resident limit;
+ * 8 shading blocks per SM).  rustracer_b200/autotune.py times candidates on a
+ * short render and sets the fastest. */
+typedef struct RtTuning {
+    uint32_t max_paths;            /* 0 or 65536 .. 8388608 */
+    uint32_t trace_blocks_per_sm;  /* 0 or 1 .. 8 (capped at the kernels' resident blocks) */
+    uint32_t shade_blocks_per_sm;  /* 0 or 1 .. 32 */
+} RtTuning;
+int32_t rt_set_tuning(RtScene* scene, const RtTuning* tuning);
+int32_t rt_get_tuning(const RtScene* scene, RtTuning* tuning);
+
 /* ── path guiding: a learned proposal at diffuse vertices (no counterpart in
  * the reference, whose diffuse bounce is the cosine lobe of pdf.rs:12-41 and
  * renderer.rs:545-571).

@@ -223,6 +223,11 @@ class RtDevelopParams(C.Structure):
     ]
 
 
+class RtTuning(C.Structure):
+    """RtTuning (include/rt_api.h): path-pool capacity and launch grids (0 = built-in)."""
+    _fields_ = [("max_paths", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32), ("shade_blocks_per_sm", C.c_uint32)]
+
+
 class RtGuideParams(C.Structure):
     """RtGuideParams (include/rt_api.h): the path-guiding network's set-up."""
     _fields_ = [

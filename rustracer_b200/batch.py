@@ -68,13 +68,31 @@ def render_job(handles, job):
     return g.render_accumulate(job_camera(job), p)
 
 
-def run_batch(jobs, workers=4, device=0, builders=None, keep_outputs=False):
+def tune_kinds(handles, jobs):
+    """Autotune each scene kind on its largest job (autotune.py) and set the
+    result on every handle of that kind; returns {kind: tuning}."""
+    from . import autotune
+    out = {}
+    for k in sorted({j["scene"] for j in jobs}):
+        job = max((j for j in jobs if j["scene"] == k), key=lambda j: j["width"] * j["height"] * j["spp"])
+        p = pass_params(job["width"], job["height"], 0, job["spp"], int(math.sqrt(job["spp"])), _DEPTH[k], 4, 1.0,
+                        job["seed"])
+        best, _ = autotune.autotune(handles[0][k], job_camera(job), p)
+        for h in handles[1:]:
+            h[k].set_tuning(**best)
+        out[k] = best
+    return out
+
+
+def run_batch(jobs, workers=4, device=0, builders=None, keep_outputs=False, tune=False):
     """Render `jobs` with `workers` concurrent threads; returns dict with the
-    wall time, per-job latencies (s) and the outputs when asked."""
+    wall time, per-job latencies (s), the tunings when `tune` (autotuned per
+    scene kind before the clock starts) and the outputs when asked."""
     builders = builders or {}
     kinds = sorted({j["scene"] for j in jobs})
     descs = {k: builders[k] if k in builders else build_scene(k) for k in kinds}
     handles = [{k: GpuScene(descs[k], device=device) for k in kinds} for _ in range(workers)]
+    tunings = tune_kinds(handles, jobs) if tune else None
     for h in handles:                                    # warm the buffers of every handle
         for k in kinds:
             render_job(h, dict(scene=k, width=64, height=64, spp=1, azimuth=0.0, elevation=20.0, seed=0))
@@ -109,4 +127,4 @@ def run_batch(jobs, workers=4, device=0, builders=None, keep_outputs=False):
     samples = sum(j["width"] * j["height"] * j["spp"] for j in jobs)
     ls = np.array([lat[j["id"]] for j in jobs])
     return dict(wall_s=wall, path_samples=samples, rate=samples / wall, p50_s=float(np.percentile(ls, 50)),
-                p99_s=float(np.percentile(ls, 99)), latencies=lat, outputs=outs)
+                p99_s=float(np.percentile(ls, 99)), latencies=lat, outputs=outs, tunings=tunings)

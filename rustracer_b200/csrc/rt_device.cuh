@@ -121,6 +121,7 @@ struct DevScene {
     // (see shape_test)
     const float4* shape_par;
     int n_analytic;             // convex solids + shapes (the traversal compiles their tests in only if > 0)
+    int trace_per_sm, shade_per_sm;   // launch tuning (host side; 0 = the built-in grids)
     // textures; per triangle 2 float4 of (u, v) at the corners and 3 float4 of
     // corner tangents (NULL: the reference's default UVs and (1, 0, 0) tangents)
     const DevTexture* tex;

@@ -510,6 +510,7 @@ struct RtScene {
     PathState P2{};                   // set 1 (shares hit and gq with set 0)
     PathState Rt{};                   // retire records: L, pend0, pend1, pendC, meta
     rtgh::Guide* guide = nullptr;     // path-guiding network (rt_guide_init)
+    uint32_t max_paths = 1u << 23;    // path-pool capacity (rt_set_tuning)
     uint32_t* queue[2] = {nullptr, nullptr};   // photon tracer queues
     ClassQueues cq{};
     float4* sq = nullptr;
@@ -1486,7 +1487,8 @@ static WaveBufs scene_bufs(const RtScene* s) {
     WaveBufs W;
     W.guide = true;
     W.set[0] = s->P; W.set[1] = s->P2; W.Rt = s->Rt;
-    W.cq = s->cq; W.sq = s->sq; W.counters = s->counters; W.derr = s->d_err; W.cap = s->cap;
+    W.cq = s->cq; W.sq = s->sq; W.counters = s->counters; W.derr = s->d_err;
+    W.cap = std::min(s->cap, s->max_paths);
     return W;
 }
 
@@ -1631,7 +1633,7 @@ static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p,
     uint32_t npix = p->width * p->height;
     uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
     uint64_t total = (uint64_t)nsamp * npix;
-    int rc = ensure_paths(s, (uint32_t)std::min<uint64_t>(total, MAX_PATHS));
+    int rc = ensure_paths(s, (uint32_t)std::min<uint64_t>(total, s->max_paths));
     if (rc) return rc;
     if (ext_rays) *ext_rays = 0;
     if (sh_rays) *sh_rays = 0;
@@ -1863,6 +1865,28 @@ extern "C" int32_t rt_last_render_stats(const RtScene* s, double* ms, int64_t* e
     if (ext) *ext = s->last_ext;
     if (sh) *sh = s->last_shadow;
     if (launches) *launches = s->last_launches;
+    return RT_OK;
+}
+
+extern "C" int32_t rt_set_tuning(RtScene* s, const RtTuning* t) {
+    if (!s || !t) return RT_ERR_INVALID;
+    if (t->max_paths != 0 && (t->max_paths < (1u << 16) || t->max_paths > MAX_PATHS))
+        return fail(s, RT_ERR_INVALID, "max_paths must be 0 or in 65536..8388608");
+    if (t->trace_blocks_per_sm > RT_TRACE_BLOCKS_PER_SM || t->shade_blocks_per_sm > 32)
+        return fail(s, RT_ERR_INVALID, "trace_blocks_per_sm must be in 0..8, shade_blocks_per_sm in 0..32");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    s->max_paths = t->max_paths ? t->max_paths : MAX_PATHS;
+    s->S.trace_per_sm = (int)t->trace_blocks_per_sm;
+    s->S.shade_per_sm = (int)t->shade_blocks_per_sm;
+    return RT_OK;
+}
+
+extern "C" int32_t rt_get_tuning(const RtScene* s, RtTuning* t) {
+    if (!s || !t) return RT_ERR_INVALID;
+    t->max_paths = s->max_paths;
+    t->trace_blocks_per_sm = (uint32_t)s->S.trace_per_sm;
+    t->shade_blocks_per_sm = (uint32_t)s->S.shade_per_sm;
     return RT_OK;
 }
 

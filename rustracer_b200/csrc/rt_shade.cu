@@ -1194,7 +1194,7 @@ void launch_generate(const DevScene& S, const PathState& A, const RenderLaunch& 
 void launch_shade(const DevScene& S, const PathState& A, const PathState& B, const PathState& Rt, const RenderLaunch& R,
                   uint32_t* ctr, const ClassQueues& Q, uint32_t* cout, float4* sq, int sms, cudaStream_t st) {
     // ctr: this iteration's counter block (see rt_internal.h for the slots)
-    int grid = sms * RT_SHADE_BLOCKS_PER_SM;
+    int grid = sms * (S.shade_per_sm > 0 ? S.shade_per_sm : RT_SHADE_BLOCKS_PER_SM);
     k_classify<<<sms * 4, CLS_BLOCK, 0, st>>>(A.hit, ctr + CTR_COUNT, Q, ctr + CTR_CLS_COUNT);
     if (R.guide.mode != 0)
         launch_guide_infer(S, A, R, Q.q[CLS_DIFFUSE], ctr + CTR_CLS_COUNT + CLS_DIFFUSE, sms, st);

@@ -13,6 +13,8 @@
 // first-wins, ties → smaller canonical id), then sorts the hit inner children
 // by entry distance with a 19-comparator network on packed (t | slot) keys and
 // continues with the nearest while the others go on a per-thread stack.
+#include <algorithm>
+
 #include "rt_internal.h"
 #include "rt_media.cuh"
 
@@ -576,14 +578,17 @@ namespace rth {
 #ifndef RT_TRACE_GRID_PER_SM
 #define RT_TRACE_GRID_PER_SM RT_TRACE_MINB
 #endif
-// persistent kernels: one wave of resident blocks
-int trace_grid(int dev_sms) { return dev_sms * RT_TRACE_GRID_PER_SM; }
+// persistent kernels: one wave of resident blocks, or fewer when tuned
+int trace_grid(const DevScene& S, int dev_sms) {
+    int per = S.trace_per_sm > 0 ? std::min(S.trace_per_sm, RT_TRACE_MINB) : RT_TRACE_GRID_PER_SM;
+    return dev_sms * per;
+}
 
 // the traversal kernels with (ANA) or without analytic solids
 #define RT_TRACE_LAUNCH(K, MODE, ...)                                                                    \
     do {                                                                                                 \
-        if (S.n_analytic > 0) K<MODE, true><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);   \
-        else                  K<MODE, false><<<trace_grid(sms), RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);  \
+        if (S.n_analytic > 0) K<MODE, true><<<trace_grid(S, sms), RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);   \
+        else                  K<MODE, false><<<trace_grid(S, sms), RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);  \
     } while (0)
 void launch_trace_closest_api(const DevScene& S, const float* rays, uint32_t n, int4* out, uint32_t* next, int* err,
                               int sms, cudaStream_t st) {

@@ -63,6 +63,8 @@ def lib():
         L.rt_kernel_times.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64)]
         L.rt_capture_rays.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), u32, vp, i64,
                                       C.POINTER(i64)]
+        L.rt_set_tuning.argtypes = [vp, C.POINTER(abi.RtTuning)]
+        L.rt_get_tuning.argtypes = [vp, C.POINTER(abi.RtTuning)]
         L.rt_guide_init.argtypes = [vp, C.POINTER(abi.RtGuideParams)]
         L.rt_guide_mode.argtypes = [vp, i32]
         L.rt_guide_params.argtypes = [vp, vp, i32]
@@ -357,6 +359,17 @@ class GpuScene:
         return idx, d2
 
     # ── diagnostics ──────────────────────────────────────────────────────
+    # ── launch tuning (rt_set_tuning) ─────────────────────────────────────
+    def set_tuning(self, max_paths=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0):
+        t = abi.RtTuning(int(max_paths), int(trace_blocks_per_sm), int(shade_blocks_per_sm))
+        self._check(lib().rt_set_tuning(self.h, C.byref(t)))
+
+    def get_tuning(self):
+        t = abi.RtTuning()
+        self._check(lib().rt_get_tuning(self.h, C.byref(t)))
+        return dict(max_paths=t.max_paths, trace_blocks_per_sm=t.trace_blocks_per_sm,
+                    shade_blocks_per_sm=t.shade_blocks_per_sm)
+
     # ── path guiding (rt_guide_*) ─────────────────────────────────────────
     def guide_init(self, params=None):
         """Create the guide network with fresh parameters (mode off)."""

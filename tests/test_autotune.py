@@ -1,0 +1,44 @@
+"""The launch autotuner's selection logic without a GPU: every candidate is
+timed, the fastest is set on the scene and cached, and the probe render stays
+within its sample budget."""
+from rustracer_b200 import autotune
+from rustracer_b200.renderer import pass_params
+
+
+class FakeScene:
+    def __init__(self):
+        self.set = []
+
+    def set_tuning(self, **t):
+        self.set.append(t)
+
+
+def test_candidates_cover_the_space():
+    c = autotune.candidates({"max_paths": (1, 2), "trace_blocks_per_sm": (3,), "shade_blocks_per_sm": (4, 5, 6)})
+    assert len(c) == 6
+    assert {(t["max_paths"], t["shade_blocks_per_sm"]) for t in c} == {(a, b) for a in (1, 2) for b in (4, 5, 6)}
+
+
+def test_autotune_picks_the_fastest_and_caches_it():
+    autotune.clear_cache()
+    g = FakeScene()
+    calls = []
+
+    def timer(t):
+        calls.append(t)
+        # fastest at 2M paths, 6 traversal blocks, 8 shading blocks
+        return abs(t["max_paths"] - (1 << 22)) / 1e6 + abs(t["trace_blocks_per_sm"] - 6) + \
+            abs(t["shade_blocks_per_sm"] - 8) + 1.0
+    best, table = autotune.autotune(g, None, pass_params(64, 64), key="k", timer=timer, repeats=2)
+    assert best == {"max_paths": 1 << 22, "trace_blocks_per_sm": 6, "shade_blocks_per_sm": 8}
+    assert len(table) == len(autotune.candidates()) and len(calls) == 2 * len(table)
+    assert g.set[-1] == best
+    g2 = FakeScene()
+    best2, table2 = autotune.autotune(g2, None, pass_params(64, 64), key="k", timer=lambda t: 1 / 0)
+    assert best2 == best and table2 is None and g2.set == [best]
+
+
+def test_probe_stays_within_its_budget():
+    p = autotune.probe_params(pass_params(1920, 1080, 0, 256))
+    assert p.n_samples == 9 and p.width == 1920 and 1920 * 1080 * (p.n_samples - 1) < autotune.PROBE_SAMPLES
+    assert autotune.probe_params(pass_params(128, 128, 0, 4)).n_samples == 4

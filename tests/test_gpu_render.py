@@ -143,3 +143,21 @@ def test_polygonal_aperture_depth_of_field_matches_oracle():
     oi = o.render_pass(cam, p)
     assert np.isfinite(gi).all()
     assert_tiles_agree(gi, oi)
+
+
+def test_launch_tuning_leaves_the_image_unchanged():
+    """rt_set_tuning: pool capacities and grids change speed, not samples —
+    every path's random numbers come from (pixel, sample)."""
+    sb, st = configs.box_scene(width=96, height=96)
+    g = GpuScene(sb)
+    p = pass_params(96, 96, 0, 32, 4, 8, 4, 1.0, 3)
+    ref = g.render_pass(st["camera"], p)
+    for t in (dict(max_paths=1 << 16, trace_blocks_per_sm=2, shade_blocks_per_sm=1),
+              dict(max_paths=1 << 18, trace_blocks_per_sm=6, shade_blocks_per_sm=16)):
+        g.set_tuning(**t)
+        assert g.get_tuning() == t
+        assert np.array_equal(g.render_pass(st["camera"], p).view(np.uint32), ref.view(np.uint32))
+    g.set_tuning()
+    assert g.get_tuning()["max_paths"] == 1 << 23
+    with pytest.raises(Exception):
+        g.set_tuning(max_paths=100)
