@@ -65,6 +65,10 @@ def parse():
                          "workload)")
     ap.add_argument("--ref-spp", type=int, default=16384, help="guided: samples per pixel of the plain reference")
     ap.add_argument("--plain-spp", type=int, default=256, help="guided: samples per pixel of the plain render")
+    ap.add_argument("--guide-spp-per-call", type=int, default=8, help="guided: samples per training render call")
+    ap.add_argument("--guide-steps", type=int, default=8, help="guided: Adam steps after each training call")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="icosphere: keep the built-in launch grids instead of autotune.py's choice")
     return ap.parse_args()
 
 
@@ -205,6 +209,13 @@ def run_ours(args):
     def params(step):
         return pass_params(W, H, (rank * 100003 + step) * SPP, SPP, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2)
 
+    tuning = None
+    if not args.no_autotune:
+        # the library's launch autotuner on a probe of this frame, before any timing
+        # (every rank tunes its own GPU; the image does not depend on the choice)
+        from rustracer_b200 import autotune
+        tuning, _ = autotune.autotune(scene, cam, params(1000))
+
     outs = (torch.zeros((H, W, 3), device=dev), torch.zeros((H, W, 3), device=dev),
             torch.zeros((H, W), dtype=torch.int32, device=dev))
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)   # 256 MB > 126 MB L2
@@ -280,6 +291,7 @@ def run_ours(args):
         "config": {"workload": "icosphere8 1310720 tris, GGX conductor + diffuse floor, 2048x1024 env, "
                                "1920x1080, 64 spp, depth 12, hero 4",
                    "spp_per_step": SPP, "path_samples_per_step_per_gpu": per_step,
+                   "launch_tuning": tuning or "built-in",
                    "parallelism": f"weak: {ws} rank(s), each its own 64 spp"
                                   + (", accumulators all-reduced every frame (NCCL)" if ws > 1 else ""),
                    "l2": "256 MB buffer written between timed steps; scene (~230 MB) exceeds L2",
@@ -493,8 +505,8 @@ def run_guided(args):
     """Learned proposal against cosine bounces at equal GPU time on the
     slit-light room (1280x720, depth 24): a plain render of --plain-spp is
     timed and scored against a plain --ref-spp reference; a fresh network is
-    trained during the guided render's first 64 spp (render calls of 4 spp,
-    16 Adam steps of 65,536 records after each) and then frozen, and the
+    trained during the guided render's first 64 spp (render calls of 8 spp,
+    8 Adam steps of 65,536 records after each) and then frozen, and the
     guided render's relMSE is read at checkpoints.  `value` is the GPU time
     the guided render needs to reach the plain render's relMSE over the plain
     render's time (log-log interpolation between checkpoints; training
@@ -529,12 +541,12 @@ def run_guided(args):
     acc(0, 4, 7, True)                                    # warm-up
     t_p = acc(0, args.plain_spp, 7, True)
     e_p = relmse(image(), ref)
-    scene.guide_init(guide_params(batch=65536, steps_per_pass=16, seed=3))
+    scene.guide_init(guide_params(batch=65536, steps_per_pass=args.guide_steps, seed=3))
     scene.guide_mode(abi.RT_GUIDE_TRAIN)
     t_g, done, pts = 0.0, 0, []
     while done < 64:
-        t_g += acc(done, 4, 9, done == 0)
-        done += 4
+        t_g += acc(done, args.guide_spp_per_call, 9, done == 0)
+        done += args.guide_spp_per_call
     pts.append((t_g, relmse(image(), ref), done))
     scene.guide_mode(abi.RT_GUIDE_SAMPLE)
     while done < 4 * args.plain_spp and (pts[-1][1] > e_p or t_g < t_p):
@@ -568,7 +580,8 @@ def run_guided(args):
                    "guided_relmse_at_equal_time": interp(0, 1, t_p),
                    "guided_checkpoints": [{"ms": round(a, 1), "relmse": b, "spp": c} for a, b, c in pts],
                    "cost_per_spp_ms": {"plain": round(t_plain_frozen / 64, 3), "guided": round(t_guided_frozen / 64, 3)},
-                   "training": {"records": gstats["records"], "samples": gstats["samples"],
+                   "training": {"spp_per_call": args.guide_spp_per_call, "steps_per_call": args.guide_steps,
+                                "records": gstats["records"], "samples": gstats["samples"],
                                 "adam_steps": gstats["steps"], "train_ms": round(gstats["train_ms"], 1)},
                    "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)"},
     }
@@ -628,7 +641,7 @@ def one_pass_guided():
     sb, st = configs.guided_box_scene()
     w, h, depth, hero = st["width"], st["height"], st["max_depth"], st["hero"]
     scene = GpuScene(sb, device=0)
-    scene.guide_init(guide_params(seed=3))
+    scene.guide_init(guide_params(steps_per_pass=16, seed=3))
     scene.guide_mode(abi.RT_GUIDE_TRAIN)
     for k in range(4):
         scene.render_accumulate(st["camera"], pass_params(w, h, 4 * k, 4, 16, depth, hero, 1.0, 9), reset=k == 0)

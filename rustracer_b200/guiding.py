@@ -37,7 +37,7 @@ def render_plain(gs, cam, params, spp, sample_idx=0):
     return s / np.maximum(c, 1)[..., None], gs.last_stats()["ms"]
 
 
-def render_guided(gs, cam, params, spp, train_spp=64, train_per_call=4, guide=None, sample_idx=0):
+def render_guided(gs, cam, params, spp, train_spp=64, train_per_call=8, guide=None, sample_idx=0):
     """`spp` samples per pixel with a fresh guide network trained during the
     first `train_spp` of them.  Returns (mean image, GPU ms of every render
     call — training steps included —, guide statistics)."""

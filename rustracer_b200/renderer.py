@@ -129,7 +129,7 @@ def pass_params(width, height, sample_idx=0, n_samples=1, strata=None, max_depth
     return p
 
 
-def guide_params(lr=1e-3, batch=65536, steps_per_pass=16, record_capacity=1 << 24, min_resolution=4,
+def guide_params(lr=1e-3, batch=65536, steps_per_pass=8, record_capacity=1 << 24, min_resolution=4,
                  level_scale=1.32, seed=1, domain=None, beta1=0.9, beta2=0.99, epsilon=1e-8, alpha_max=0.5,
                  log_kappa_max=5.0):
     """RtGuideParams with the learned proposal's defaults: 16 levels from 4 to
