@@ -397,6 +397,7 @@ struct Guide {
     __nv_bfloat16* act = nullptr;
     uint32_t act_batch = 0;
     float4* gpar = nullptr;
+    uint4* enc = nullptr;            // encoded inputs of the diffuse queue (128 B per path slot)
     uint32_t gpar_cap = 0;
     float4 *rec_a = nullptr, *rec_b = nullptr, *rec_c = nullptr;
     float* rec_w = nullptr;
@@ -413,7 +414,7 @@ struct Guide {
 
 void destroy(Guide* g) {
     if (!g) return;
-    void* ptrs[] = {g->params, g->grad, g->m, g->v, g->wbf, g->act, g->gpar, g->rec_a, g->rec_b, g->rec_c,
+    void* ptrs[] = {g->params, g->grad, g->m, g->v, g->wbf, g->act, g->gpar, g->enc, g->rec_a, g->rec_b, g->rec_c,
                     g->rec_w, g->counters, g->train, g->loss};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -513,6 +514,7 @@ GuideDev view(const Guide* g) {
     d.amax = g->prm.alpha_max;
     d.lkmax = g->prm.log_kappa_max;
     d.gpar = g->gpar;
+    d.enc = g->enc;
     d.rec_a = g->rec_a; d.rec_b = g->rec_b; d.rec_c = g->rec_c; d.rec_w = g->rec_w;
     d.rec_count = g->counters;
     d.rec_cap = g->rec_cap;
@@ -522,9 +524,12 @@ GuideDev view(const Guide* g) {
 int ensure_paths(Guide* g, uint32_t cap) {
     if (g->gpar_cap >= cap) return 0;
     if (g->gpar) cudaFree(g->gpar);
+    if (g->enc) cudaFree(g->enc);
     g->gpar = nullptr;
+    g->enc = nullptr;
     g->gpar_cap = 0;
     if (cudaMalloc(&g->gpar, (size_t)cap * GP_F4 * sizeof(float4)) != cudaSuccess) return -1;
+    if (cudaMalloc(&g->enc, (size_t)cap * 8 * sizeof(uint4)) != cudaSuccess) return -1;
     g->gpar_cap = cap;
     return 0;
 }

@@ -46,6 +46,7 @@ struct GuideDev {
     uint32_t res[LEVELS];             // grid resolution of each level
     float amax, lkmax;                // cap of α, cap of log κ
     float4* gpar;                     // GP_F4 float4 per path slot
+    uint4* enc;                       // encoded inputs of the diffuse queue (8 uint4 per entry)
     float4 *rec_a, *rec_b, *rec_c;    // records: (p, Σ T·sf), (n, base Σ L), (ω_i, prev record)
     float* rec_w;                     // weight of each record, set when its path retires
     uint32_t* rec_count;
@@ -85,12 +86,14 @@ RTG_D float corner_weight(int c, const float f[3]) {
     return __fmul_rn(__fmul_rn(wx, wy), wz);
 }
 
-// The 64 network inputs of one point, rounded to bf16, into a shared-memory row.
-RTG_D void encode_row(const GuideDev& G, const float* __restrict__ table, float3 p, float3 n,
-                      __nv_bfloat16* row) {
+RTG_D uint32_t pack_bf2(float lo, float hi);
+
+// The 64 network inputs of one point, rounded to bf16, as 32 packed pairs.
+RTG_D void encode_packed(const GuideDev& G, const float* __restrict__ table, float3 p, float3 n,
+                         uint32_t (&out)[32]) {
     float pn[3];
     normalise_pos(G, p.x, p.y, p.z, pn);
-#pragma unroll 1
+#pragma unroll
     for (int l = 0; l < LEVELS; l++) {
         uint32_t res = G.res[l], ci[3];
         float f[3];
@@ -105,18 +108,28 @@ RTG_D void encode_row(const GuideDev& G, const float* __restrict__ table, float3
             a0 = __fadd_rn(a0, __fmul_rn(w, v.x));
             a1 = __fadd_rn(a1, __fmul_rn(w, v.y));
         }
-        row[2 * l] = __float2bfloat16_rn(a0);
-        row[2 * l + 1] = __float2bfloat16_rn(a1);
+        out[l] = pack_bf2(a0, a1);
     }
     float th = acosf(fminf(fmaxf(n.z, -1.0f), 1.0f)) * 0.318309886f;
     float ph = (atan2f(n.y, n.x) + 3.14159265f) * 0.159154943f;
 #pragma unroll
-    for (int k = 0; k < NBLOB; k++) {
+    for (int k = 0; k < NBLOB; k += 2) {
         float d0 = __fsub_rn(__fmul_rn(16.0f, th), (float)k + 0.5f);
-        float d1 = __fsub_rn(__fmul_rn(16.0f, ph), (float)k + 0.5f);
-        row[32 + k] = __float2bfloat16_rn(expf(-0.5f * d0 * d0));
-        row[48 + k] = __float2bfloat16_rn(expf(-0.5f * d1 * d1));
+        float d1 = __fsub_rn(__fmul_rn(16.0f, th), (float)k + 1.5f);
+        float e0 = __fsub_rn(__fmul_rn(16.0f, ph), (float)k + 0.5f);
+        float e1 = __fsub_rn(__fmul_rn(16.0f, ph), (float)k + 1.5f);
+        out[16 + k / 2] = pack_bf2(expf(-0.5f * d0 * d0), expf(-0.5f * d1 * d1));
+        out[24 + k / 2] = pack_bf2(expf(-0.5f * e0 * e0), expf(-0.5f * e1 * e1));
     }
+}
+
+// The same inputs into a row of bf16 (shared or global memory, 4-byte aligned).
+RTG_D void encode_row(const GuideDev& G, const float* __restrict__ table, float3 p, float3 n,
+                      __nv_bfloat16* row) {
+    uint32_t v[32];
+    encode_packed(G, table, p, n, v);
+#pragma unroll
+    for (int k = 0; k < 32; k++) reinterpret_cast<uint32_t*>(row)[k] = v[k];
 }
 
 // ── tensor-core tiles ────────────────────────────────────────────────────────

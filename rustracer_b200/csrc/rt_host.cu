@@ -1589,7 +1589,7 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         rth::launch_retire(s->S, B, W.Rt, R, c, hdr, blk(it + 2), cn + CTR_COUNT, s->sms, s->stream);
         // extend, classify, shadow, retire, the shading classes other than media
         // and PBR, and the PBR class when the scene has PBR materials
-        nl += 4 + (CLS_N - 2) + (s->S.n_pbr > 0 ? 1 : 0) + (R.guide.mode != 0 ? 1 : 0);
+        nl += 4 + (CLS_N - 2) + (s->S.n_pbr > 0 ? 1 : 0) + (R.guide.mode != 0 ? 2 : 0);
         uint32_t slot = (uint32_t)(it % STATUS_RING);
         CK(cudaMemcpyAsync(s->h_status + slot, cn + CTR_COUNT, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
         CK(cudaEventRecord(s->st_ev[slot], s->stream));

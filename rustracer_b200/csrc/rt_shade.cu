@@ -1129,49 +1129,66 @@ __global__ void k_accumulate(const float* __restrict__ scratch, uint32_t nsamp, 
 }
 
 // ── guide inference: the mixture of every diffuse-class path of the bounce ──
-// One warp evaluates 32 paths: each lane encodes its hit (position and
-// face-forward normal, as the shading kernel computes them), then the warp
-// runs the network on two 16-row tiles and lanes 0..15 write the mixtures.
-#define GUIDE_WARPS 4
+// Two kernels.  k_guide_encode, one thread per queue entry and no shared
+// memory (so the hash-table gathers run at full occupancy), recomputes the hit
+// as the shading kernel does (position, face-forward normal) and writes the 64
+// bf16 inputs in queue order.  k_guide_infer runs the network on those rows,
+// 32 per warp as two 16-row tensor-core tiles fed straight from global memory,
+// and lanes 0..15 write the mixtures of the tile's paths.
+#define GUIDE_WARPS 8
 #define GUIDE_LDO 52
 static size_t guide_infer_smem() {
-    return (size_t)rtg::W_SMEM * 2 + (size_t)GUIDE_WARPS * (32 * rtg::LDW * 2 + 16 * GUIDE_LDO * 4);
+    return (size_t)rtg::W_SMEM * 2 + (size_t)GUIDE_WARPS * 16 * GUIDE_LDO * 4;
 }
-__global__ void __launch_bounds__(GUIDE_WARPS * 32) k_guide_infer(DevScene S, PathState A, RenderLaunch R,
-                                                                  const uint32_t* __restrict__ qin,
+__global__ void __launch_bounds__(256) k_guide_encode(DevScene S, PathState A, RenderLaunch R,
+                                                      const uint32_t* __restrict__ qin, const uint32_t* cin) {
+    uint32_t n = *cin;
+    for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n; qi += gridDim.x * blockDim.x) {
+        uint32_t pid = qin[qi];
+        float4 hv = A.hit[pid], ro = A.ray_o[pid], rdv = A.ray_d[pid];
+        Surf sf = surface(S, hv, mk(ro.x, ro.y, ro.z), mk(rdv.x, rdv.y, rdv.z));
+        uint32_t v[32];
+        rtg::encode_packed(R.guide, R.guide.table, sf.p, sf.nrm, v);
+        uint4* dst = R.guide.enc + (size_t)qi * 8;
+#pragma unroll
+        for (int k = 0; k < 8; k++) dst[k] = make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    }
+}
+__global__ void __launch_bounds__(GUIDE_WARPS * 32) k_guide_infer(RenderLaunch R, const uint32_t* __restrict__ qin,
                                                                   const uint32_t* cin) {
     extern __shared__ __align__(16) unsigned char gsm[];
     __nv_bfloat16* Ws = reinterpret_cast<__nv_bfloat16*>(gsm);
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __nv_bfloat16* S_in = Ws + rtg::W_SMEM + warp * 32 * rtg::LDW;
-    float* S_o = reinterpret_cast<float*>(Ws + rtg::W_SMEM + GUIDE_WARPS * 32 * rtg::LDW) + warp * 16 * GUIDE_LDO;
+    float* S_o = reinterpret_cast<float*>(Ws + rtg::W_SMEM) + warp * 16 * GUIDE_LDO;
     rtg::load_weights(R.guide.wbf, Ws);
     __syncthreads();
     uint32_t n = *cin;
+    const __nv_bfloat16* enc = reinterpret_cast<const __nv_bfloat16*>(R.guide.enc);
+    int g = lane >> 2, t = lane & 3;
     for (uint32_t base = (blockIdx.x * GUIDE_WARPS + warp) * 32; base < n; base += gridDim.x * GUIDE_WARPS * 32) {
-        uint32_t qi = base + lane;
-        bool valid = qi < n;
-        uint32_t pid = valid ? qin[qi] : 0u;
-        if (valid) {
-            float4 hv = A.hit[pid], ro = A.ray_o[pid], rdv = A.ray_d[pid];
-            Surf sf = surface(S, hv, mk(ro.x, ro.y, ro.z), mk(rdv.x, rdv.y, rdv.z));
-            rtg::encode_row(R.guide, R.guide.table, sf.p, sf.nrm, S_in + lane * rtg::LDW);
-        } else {
-            for (int k = 0; k < rtg::NIN; k++) S_in[lane * rtg::LDW + k] = __float2bfloat16_rn(0.0f);
-        }
-        uint32_t pid0 = __shfl_sync(0xFFFFFFFFu, pid, lane & 15), pid1 = __shfl_sync(0xFFFFFFFFu, pid, 16 + (lane & 15));
-        __syncwarp();
         for (int mt = 0; mt < 2; mt++) {
+            uint32_t r0 = base + 16 * mt;
+            if (r0 >= n) break;                                   // uniform across the warp
+            // rows past n read as zeros (the queue holds at most the pool)
+            uint32_t ra = r0 + g, rb = r0 + g + 8;
             uint32_t x0[4][4], h1[4][4], h2[4][4], h3[4][4];
+#pragma unroll
+            for (int kb = 0; kb < 4; kb++) {
+                int c = 16 * kb + 2 * t;
+                x0[kb][0] = ra < n ? rtg::ld_u32(enc + (size_t)ra * rtg::NIN + c) : 0u;
+                x0[kb][1] = rb < n ? rtg::ld_u32(enc + (size_t)rb * rtg::NIN + c) : 0u;
+                x0[kb][2] = ra < n ? rtg::ld_u32(enc + (size_t)ra * rtg::NIN + c + 8) : 0u;
+                x0[kb][3] = rb < n ? rtg::ld_u32(enc + (size_t)rb * rtg::NIN + c + 8) : 0u;
+            }
             float o[6][4];
-            rtg::load_frags<4>(S_in + 16 * mt * rtg::LDW, rtg::LDW, x0);
             rtg::mlp_forward(Ws, x0, h1, h2, h3, o);
             rtg::store_out(o, S_o, GUIDE_LDO);
             __syncwarp();
-            if (lane < 16 && base + 16 * mt + lane < n) {
+            uint32_t qi = r0 + lane;
+            if (lane < 16 && qi < n) {
                 float4 gp[rtg::GP_F4];
                 rtg::mixture_from_outputs(S_o + lane * GUIDE_LDO, gp, R.guide.amax, R.guide.lkmax);
-                float4* dst = R.guide.gpar + (size_t)(mt ? pid1 : pid0) * rtg::GP_F4;
+                float4* dst = R.guide.gpar + (size_t)qin[qi] * rtg::GP_F4;
 #pragma unroll
                 for (int k = 0; k < rtg::GP_F4; k++) dst[k] = gp[k];
             }
@@ -1184,7 +1201,8 @@ namespace rth {
 void launch_guide_infer(const DevScene& S, const PathState& A, const RenderLaunch& R, const uint32_t* queue,
                         const uint32_t* count, int sms, cudaStream_t st) {
     cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)guide_infer_smem());
-    k_guide_infer<<<sms * 3, GUIDE_WARPS * 32, guide_infer_smem(), st>>>(S, A, R, queue, count);
+    k_guide_encode<<<sms * 8, 256, 0, st>>>(S, A, R, queue, count);
+    k_guide_infer<<<sms * 2, GUIDE_WARPS * 32, guide_infer_smem(), st>>>(R, queue, count);
 }
 void launch_generate(const DevScene& S, const PathState& A, const RenderLaunch& R, uint32_t pool, uint32_t* count0,
                      cudaStream_t st) {
