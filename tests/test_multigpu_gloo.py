@@ -77,3 +77,52 @@ def test_merge_matches_sequential_welford():
         np.testing.assert_allclose(ms[0], s, rtol=1e-5)
         np.testing.assert_allclose(mm[0], m2, rtol=1e-4, atol=1e-4)
         assert (mc[0] == n).all()
+
+
+class _GuideStandIn:
+    """The two guide calls broadcast_guide makes, on host arrays."""
+
+    def __init__(self, params):
+        self.params = params
+
+    def guide_get_params(self):
+        return self.params.copy()
+
+    def guide_set_params(self, p):
+        self.params = np.array(p, np.float32)
+
+
+def _guide_worker(rank, world, port, out):
+    import torch.distributed as dist
+    from rustracer_b200 import abi
+    from rustracer_b200.multigpu import broadcast_guide
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(rank)
+        g = _GuideStandIn(rng.standard_normal(abi.RT_GUIDE_PARAMS).astype(np.float32))
+        n = broadcast_guide(g, src=0)
+        out[rank] = (n, float(g.params[:1000].sum()), float(g.params[-1000:].sum()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_broadcast_guide_shares_rank0_parameters():
+    """The trained guide of rank 0 reaches every rank unchanged (gloo, 2 ranks)."""
+    from rustracer_b200 import abi
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_guide_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(180)
+        assert p.exitcode == 0
+    ref = np.random.default_rng(0).standard_normal(abi.RT_GUIDE_PARAMS).astype(np.float32)
+    for r in range(2):
+        n, a, b = out[r]
+        assert n == abi.RT_GUIDE_PARAMS
+        assert a == float(ref[:1000].sum()) and b == float(ref[-1000:].sum())
