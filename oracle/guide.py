@@ -8,7 +8,8 @@ The reference has no learned proposal: its diffuse bounce is the cosine lobe
 (renderer.rs:545-571, pdf.rs:12-41).  This file restates the published methods
 the GPU network is built from, at the GPU's rounding points:
   * hash-grid encoding: Müller et al. 2022 ("Instant neural graphics
-    primitives"): 16 levels × 2 features, 2^19 entries per level, dense
+    primitives"): 16 levels × 2 features, 2^19 entries per level (read as
+    BF16; the float32 master is what Adam updates), dense
     indexing where (res+1)^3 fits, else x ⊕ 2654435761·y ⊕ 805459861·z;
     trilinear weights and sums in float32, in corner order 0..7;
   * one-blob encoding of the normal (Müller et al. 2019, "Neural importance
@@ -76,8 +77,9 @@ def normalise(P, lo, inv):
 
 
 def encode(params, res, lo, inv, P, N):
-    """(n, 64) BF16-rounded inputs: hash-grid features of P, one-blob of N."""
-    table = params[N_MLP:].reshape(LEVELS, TSIZE, 2)
+    """(n, 64) BF16-rounded inputs: hash-grid features of P (from the BF16
+    copy of the table the GPU gathers from), one-blob of N."""
+    table = bf16(params[N_MLP:]).reshape(LEVELS, TSIZE, 2)
     pn = normalise(P, lo, inv)
     n = len(pn)
     enc = np.zeros((n, NIN), f32)

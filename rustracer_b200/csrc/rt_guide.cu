@@ -97,7 +97,7 @@ template <class Emit>
 RTG_D void warp_eval(const GuideDev& G, const __nv_bfloat16* Ws, __nv_bfloat16* S_in, float* S_o, bool valid,
                      float3 p, float3 n, Emit emit) {
     int lane = threadIdx.x & 31;
-    if (valid) encode_row(G, G.table, p, n, S_in + lane * LDW);
+    if (valid) encode_row(G, G.tbf, p, n, S_in + lane * LDW);
     else
         for (int k = 0; k < NIN; k++) S_in[lane * LDW + k] = __float2bfloat16_rn(0.0f);
     __syncwarp();
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(GW * 32) k_train(GuideDev G, TrainArgs A) {
     for (uint32_t base = (blockIdx.x * GW + warp) * 32; base < A.batch; base += gridDim.x * GW * 32) {
         float4 s[3];
         bool valid = train_row(A, base + lane, n, s);
-        if (valid) encode_row(G, G.table, make_float3(s[0].x, s[0].y, s[0].z), make_float3(s[1].x, s[1].y, s[1].z),
+        if (valid) encode_row(G, G.tbf, make_float3(s[0].x, s[0].y, s[0].z), make_float3(s[1].x, s[1].y, s[1].z),
                               S_in + lane * LDW);
         else
             for (int k = 0; k < NIN; k++) S_in[lane * LDW + k] = __float2bfloat16_rn(0.0f);
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(GW * 32) k_wgrad(const __nv_bfloat16* __restri
 // Adam (Kingma & Ba 2015) with bias-corrected moments; refreshes the bf16 weights
 __global__ void k_adam(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
                        const float* __restrict__ g, size_t n, float lr, float b1, float b2, float eps, float bc1,
-                       float bc2, __nv_bfloat16* __restrict__ wbf) {
+                       float bc2, __nv_bfloat16* __restrict__ wbf, __nv_bfloat16* __restrict__ tbf) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         float gi = g[i];
         float mi = __fadd_rn(__fmul_rn(b1, m[i]), __fmul_rn(1.0f - b1, gi));
@@ -364,12 +364,17 @@ __global__ void k_adam(float* __restrict__ p, float* __restrict__ m, float* __re
         float pi = __fsub_rn(p[i], step);
         p[i] = pi;
         if (i < (size_t)N_MLP) wbf[i] = __float2bfloat16_rn(pi);
+        else tbf[i - N_MLP] = __float2bfloat16_rn(pi);
     }
 }
 
-__global__ void k_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ wbf, int n) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        wbf[i] = __float2bfloat16_rn(p[i]);
+// bf16 copies of the weights and of the table from the fp32 parameters
+__global__ void k_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ wbf,
+                          __nv_bfloat16* __restrict__ tbf) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N_PARAMS; i += (size_t)gridDim.x * blockDim.x) {
+        if (i < (size_t)N_MLP) wbf[i] = __float2bfloat16_rn(p[i]);
+        else tbf[i - N_MLP] = __float2bfloat16_rn(p[i]);
+    }
 }
 
 size_t api_smem() { return (size_t)W_SMEM * 2 + (size_t)GW * (32 * LDW * 2 + 16 * LDO * 4); }
@@ -394,6 +399,7 @@ struct Guide {
     int mode = 0;
     float *params = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
     __nv_bfloat16* wbf = nullptr;
+    __nv_bfloat16* tbf = nullptr;     // bf16 copy of the table (the encodings read it)
     __nv_bfloat16* act = nullptr;
     uint32_t act_batch = 0;
     float4* gpar = nullptr;
@@ -414,7 +420,7 @@ struct Guide {
 
 void destroy(Guide* g) {
     if (!g) return;
-    void* ptrs[] = {g->params, g->grad, g->m, g->v, g->wbf, g->act, g->gpar, g->enc, g->rec_a, g->rec_b, g->rec_c,
+    void* ptrs[] = {g->params, g->grad, g->m, g->v, g->wbf, g->tbf, g->act, g->gpar, g->enc, g->rec_a, g->rec_b, g->rec_c,
                     g->rec_w, g->counters, g->train, g->loss};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -454,7 +460,8 @@ Guide* create(const RtGuideParams& p, const float scene_lo[3], const float scene
     g->rec_cap = p.record_capacity;
     bool ok = cudaMalloc(&g->params, N_PARAMS * 4) == cudaSuccess && cudaMalloc(&g->grad, N_PARAMS * 4) == cudaSuccess &&
               cudaMalloc(&g->m, N_PARAMS * 4) == cudaSuccess && cudaMalloc(&g->v, N_PARAMS * 4) == cudaSuccess &&
-              cudaMalloc(&g->wbf, N_MLP * 2) == cudaSuccess && cudaMalloc(&g->counters, 16) == cudaSuccess &&
+              cudaMalloc(&g->wbf, N_MLP * 2) == cudaSuccess && cudaMalloc(&g->tbf, N_TABLE * 2) == cudaSuccess &&
+              cudaMalloc(&g->counters, 16) == cudaSuccess &&
               cudaMalloc(&g->loss, 4) == cudaSuccess &&
               cudaMalloc(&g->rec_a, (size_t)g->rec_cap * 16) == cudaSuccess &&
               cudaMalloc(&g->rec_b, (size_t)g->rec_cap * 16) == cudaSuccess &&
@@ -485,7 +492,7 @@ Guide* create(const RtGuideParams& p, const float scene_lo[3], const float scene
         destroy(g);
         return nullptr;
     }
-    k_to_bf16<<<16, 256>>>(g->params, g->wbf, N_MLP);
+    k_to_bf16<<<1024, 256>>>(g->params, g->wbf, g->tbf);
     if (cudaDeviceSynchronize() != cudaSuccess) {
         *err = "guide initialisation";
         destroy(g);
@@ -508,6 +515,7 @@ GuideDev view(const Guide* g) {
     if (!g) return d;
     d.mode = g->mode;
     d.table = g->params + N_MLP;
+    d.tbf = reinterpret_cast<const __nv_bfloat162*>(g->tbf);
     d.wbf = g->wbf;
     for (int a = 0; a < 3; a++) { d.lo[a] = g->lo[a]; d.inv[a] = g->inv[a]; }
     for (int l = 0; l < LEVELS; l++) d.res[l] = g->res[l];
@@ -541,7 +549,7 @@ cudaError_t params_io(Guide* g, float* host, int write, cudaStream_t st) {
         if ((e = cudaMemsetAsync(g->m, 0, N_PARAMS * 4, st))) return e;
         if ((e = cudaMemsetAsync(g->v, 0, N_PARAMS * 4, st))) return e;
         g->steps = 0;
-        k_to_bf16<<<16, 256, 0, st>>>(g->params, g->wbf, N_MLP);
+        k_to_bf16<<<1024, 256, 0, st>>>(g->params, g->wbf, g->tbf);
         return cudaGetLastError();
     }
     if ((e = cudaMemcpyAsync(host, g->params, N_PARAMS * 4, cudaMemcpyDeviceToHost, st))) return e;
@@ -572,7 +580,7 @@ static cudaError_t step(Guide* g, const TrainArgs& a0, bool adam, int sms, cudaS
         float bc1 = (float)(1.0 - std::pow((double)b1, (double)g->steps));
         float bc2 = (float)(1.0 - std::pow((double)b2, (double)g->steps));
         k_adam<<<sms * 8, 256, 0, st>>>(g->params, g->m, g->v, g->grad, N_PARAMS, g->prm.learning_rate, b1, b2,
-                                        g->prm.epsilon, bc1, bc2, g->wbf);
+                                        g->prm.epsilon, bc1, bc2, g->wbf, g->tbf);
     }
     return cudaGetLastError();
 }

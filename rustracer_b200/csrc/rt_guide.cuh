@@ -40,7 +40,8 @@ constexpr uint32_t REC_NONE = 0xFFFFFFFFu;
 // 2: guided bounces plus training records.
 struct GuideDev {
     int mode;
-    const float* table;               // [LEVELS][TSIZE][FEAT] fp32
+    const float* table;               // [LEVELS][TSIZE][FEAT] fp32 master (Adam)
+    const __nv_bfloat162* tbf;        // its bf16 copy, read by every encoding
     const __nv_bfloat16* wbf;         // the four layers, [out][in] row-major, bf16
     float lo[3], inv[3];              // hash-grid domain: pn = (p − lo) · inv, clamped to [0, 1]
     uint32_t res[LEVELS];             // grid resolution of each level
@@ -87,9 +88,11 @@ RTG_D float corner_weight(int c, const float f[3]) {
 }
 
 RTG_D uint32_t pack_bf2(float lo, float hi);
+RTG_D float bf_lo(uint32_t u);
+RTG_D float bf_hi(uint32_t u);
 
 // The 64 network inputs of one point, rounded to bf16, as 32 packed pairs.
-RTG_D void encode_packed(const GuideDev& G, const float* __restrict__ table, float3 p, float3 n,
+RTG_D void encode_packed(const GuideDev& G, const __nv_bfloat162* __restrict__ table, float3 p, float3 n,
                          uint32_t (&out)[32]) {
     float pn[3];
     normalise_pos(G, p.x, p.y, p.z, pn);
@@ -98,15 +101,15 @@ RTG_D void encode_packed(const GuideDev& G, const float* __restrict__ table, flo
         uint32_t res = G.res[l], ci[3];
         float f[3];
         for (int a = 0; a < 3; a++) level_cell(res, pn[a], &ci[a], &f[a]);
-        const float2* tl = reinterpret_cast<const float2*>(table) + (size_t)l * TSIZE;
+        const __nv_bfloat162* tl = table + (size_t)l * TSIZE;
         float a0 = 0.0f, a1 = 0.0f;
 #pragma unroll
         for (int c = 0; c < 8; c++) {
             uint32_t idx = grid_index(res, ci[0] + (c & 1), ci[1] + ((c >> 1) & 1), ci[2] + (c >> 2));
-            float2 v = __ldg(tl + idx);
+            uint32_t u = __ldg(reinterpret_cast<const unsigned int*>(tl + idx));
             float w = corner_weight(c, f);
-            a0 = __fadd_rn(a0, __fmul_rn(w, v.x));
-            a1 = __fadd_rn(a1, __fmul_rn(w, v.y));
+            a0 = __fadd_rn(a0, __fmul_rn(w, bf_lo(u)));
+            a1 = __fadd_rn(a1, __fmul_rn(w, bf_hi(u)));
         }
         out[l] = pack_bf2(a0, a1);
     }
@@ -124,7 +127,7 @@ RTG_D void encode_packed(const GuideDev& G, const float* __restrict__ table, flo
 }
 
 // The same inputs into a row of bf16 (shared or global memory, 4-byte aligned).
-RTG_D void encode_row(const GuideDev& G, const float* __restrict__ table, float3 p, float3 n,
+RTG_D void encode_row(const GuideDev& G, const __nv_bfloat162* __restrict__ table, float3 p, float3 n,
                       __nv_bfloat16* row) {
     uint32_t v[32];
     encode_packed(G, table, p, n, v);

@@ -1148,7 +1148,7 @@ __global__ void __launch_bounds__(256) k_guide_encode(DevScene S, PathState A, R
         float4 hv = A.hit[pid], ro = A.ray_o[pid], rdv = A.ray_d[pid];
         Surf sf = surface(S, hv, mk(ro.x, ro.y, ro.z), mk(rdv.x, rdv.y, rdv.z));
         uint32_t v[32];
-        rtg::encode_packed(R.guide, R.guide.table, sf.p, sf.nrm, v);
+        rtg::encode_packed(R.guide, R.guide.tbf, sf.p, sf.nrm, v);
         uint4* dst = R.guide.enc + (size_t)qi * 8;
 #pragma unroll
         for (int k = 0; k < 8; k++) dst[k] = make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
