@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--plain-spp", type=int, default=256, help="guided: samples per pixel of the plain render")
     ap.add_argument("--guide-spp-per-call", type=int, default=8, help="guided: samples per training render call")
     ap.add_argument("--guide-steps", type=int, default=8, help="guided: Adam steps after each training call")
+    ap.add_argument("--guide-train-spp", type=int, default=64, help="guided: samples per pixel of training")
     ap.add_argument("--no-autotune", action="store_true",
                     help="icosphere: keep the built-in launch grids instead of autotune.py's choice")
     return ap.parse_args()
@@ -544,7 +545,7 @@ def run_guided(args):
     scene.guide_init(guide_params(batch=65536, steps_per_pass=args.guide_steps, seed=3))
     scene.guide_mode(abi.RT_GUIDE_TRAIN)
     t_g, done, pts = 0.0, 0, []
-    while done < 64:
+    while done < args.guide_train_spp:
         t_g += acc(done, args.guide_spp_per_call, 9, done == 0)
         done += args.guide_spp_per_call
     pts.append((t_g, relmse(image(), ref), done))
@@ -580,7 +581,8 @@ def run_guided(args):
                    "guided_relmse_at_equal_time": interp(0, 1, t_p),
                    "guided_checkpoints": [{"ms": round(a, 1), "relmse": b, "spp": c} for a, b, c in pts],
                    "cost_per_spp_ms": {"plain": round(t_plain_frozen / 64, 3), "guided": round(t_guided_frozen / 64, 3)},
-                   "training": {"spp_per_call": args.guide_spp_per_call, "steps_per_call": args.guide_steps,
+                   "training": {"spp": args.guide_train_spp, "spp_per_call": args.guide_spp_per_call,
+                                "steps_per_call": args.guide_steps,
                                 "records": gstats["records"], "samples": gstats["samples"],
                                 "adam_steps": gstats["steps"], "train_ms": round(gstats["train_ms"], 1)},
                    "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)"},

@@ -28,7 +28,8 @@ constexpr int OFF_W0 = 0, OFF_W1 = NHID * NIN, OFF_W2 = 2 * NHID * NIN, OFF_W3 =
 constexpr int N_MLP = OFF_W3 + NOUTP * NHID;                      // 15360 weights
 constexpr size_t N_TABLE = (size_t)LEVELS * TSIZE * FEAT;         // 16,777,216 table entries
 constexpr size_t N_PARAMS = (size_t)N_MLP + N_TABLE;
-constexpr int GP_F4 = 11;            // per-path mixture: 8 × (μ, κ), π0..3, π4..7, (α, -, -, -)
+constexpr int GP_F4 = 13;            // per-path mixture: 8 × (μ, κ), π0..3, π4..7, (α, -, -, -), β0..3, β4..7
+                                     // with β_i = log(π_i · c(κ_i)) − κ_i, c the vMF normaliser
 constexpr float LOGK_LO = -5.0f;     // log κ floor; the cap and α's cap are parameters
 constexpr int LDW = NIN + 8;         // padded shared-memory row of a forward weight matrix (bf16)
 constexpr int LDT3 = NOUTP + 8;      // padded row of the transposed output layer
@@ -256,6 +257,13 @@ RTG_HD void mixture_from_outputs(const float* o, float4* gp, float amax, float l
     gp[8] = make_float4(e[0] / s, e[1] / s, e[2] / s, e[3] / s);
     gp[9] = make_float4(e[4] / s, e[5] / s, e[6] / s, e[7] / s);
     gp[10] = make_float4(amax / (1.0f + expf(-o[40])), 0.f, 0.f, 0.f);
+    float beta[NLOBE], ls = logf(s);
+    for (int i = 0; i < NLOBE; i++) {
+        float k = gp[i].w;
+        beta[i] = (o[5 * i + 4] - mx - ls) + logf(k) - 1.83787707f - logf(-expm1f(-2.0f * k)) - k;
+    }
+    gp[11] = make_float4(beta[0], beta[1], beta[2], beta[3]);
+    gp[12] = make_float4(beta[4], beta[5], beta[6], beta[7]);
 }
 
 RTG_HD float lobe_weight(const float4* gp, int i) {
@@ -264,13 +272,16 @@ RTG_HD float lobe_weight(const float4* gp, int i) {
     return r == 0 ? q.x : r == 1 ? q.y : r == 2 ? q.z : q.w;
 }
 
-// Density of the vMF mixture alone at unit direction w.
+// Density of the vMF mixture alone at unit direction w:
+// Σ π_i c(κ_i) exp(κ_i (μ_i·w − 1)) = Σ exp(κ_i μ_i·w + β_i).
 RTG_HD float vmf_mix_pdf(const float4* gp, float wx, float wy, float wz) {
+    float4 b0 = gp[11], b1 = gp[12];
+    float beta[NLOBE] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
     float p = 0.0f;
+#pragma unroll
     for (int i = 0; i < NLOBE; i++) {
         float4 m = gp[i];
-        float c = m.x * wx + m.y * wy + m.z * wz;
-        p += lobe_weight(gp, i) * vmf_norm(m.w) * expf(m.w * (c - 1.0f));
+        p += expf(m.w * (m.x * wx + m.y * wy + m.z * wz) + beta[i]);
     }
     return p;
 }
