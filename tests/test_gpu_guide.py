@@ -241,3 +241,32 @@ def test_guided_gem_room_with_photons_stays_unbiased():
     pi = gs.render_pass(cam, pass_params(96, 64, 100, 96, 8, 16, 1, 1.0, 8))
     assert np.isfinite(gi).all()
     assert_tiles_agree(gi, pi)
+
+
+def test_guide_entry_points_take_device_buffers():
+    """rt_guide_eval / _pdf / _sample with RT_MEM_DEVICE pointers (CUDA
+    tensors) give what the host-memory calls give."""
+    import ctypes as C
+    import torch
+    from rustracer_b200 import abi
+    from rustracer_b200.renderer import lib
+    gs = _scene()
+    gs.guide_set_params(_params(51))
+    P, N = _queries(3000, 12)
+    q = np.concatenate([P, N], 1).astype(np.float32)
+    rng = np.random.default_rng(3)
+    D = rng.normal(size=(3000, 3)).astype(np.float32)
+    D /= np.linalg.norm(D, axis=1, keepdims=True)
+    u = rng.random((3000, 4)).astype(np.float32)
+    qd, dd, ud = (torch.from_numpy(x).cuda() for x in (q, D, u))
+    raw_d = torch.zeros((3000, 41), device="cuda")
+    pdf_d = torch.zeros(3000, device="cuda")
+    smp_d = torch.zeros((3000, 4), device="cuda")
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    assert lib().rt_guide_eval(gs.h, ptr(qd), 3000, ptr(raw_d), abi.RT_MEM_DEVICE) == 0
+    assert lib().rt_guide_pdf(gs.h, ptr(qd), ptr(dd), 3000, ptr(pdf_d), abi.RT_MEM_DEVICE) == 0
+    assert lib().rt_guide_sample(gs.h, ptr(qd), ptr(ud), 3000, ptr(smp_d), abi.RT_MEM_DEVICE) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(raw_d.cpu().numpy(), gs.guide_eval(q))
+    assert np.array_equal(pdf_d.cpu().numpy(), gs.guide_pdf(q, D))
+    assert np.array_equal(smp_d.cpu().numpy(), gs.guide_sample(q, u))
