@@ -1,4 +1,4 @@
-"""Rendering with the learned proposal, and the error metric it is judged by.
+"""Rendering with the learned proposal, and the relMSE metric that compares it with cosine bounces.
 
 The reference has no path guiding: every diffuse bounce samples the cosine
 lobe (renderer.rs:545-571).  Here a frame is rendered the same way, but the
