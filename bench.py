@@ -22,7 +22,15 @@ roofline : the closest-hit traversal kernel (extend).  Algorithmic bytes per
            scaled by the bounce's ray count); divided by the kernel's CUDA-event
            time; peak = measured HBM copy bandwidth.
 cpu_baseline: the CPU oracle (restatement of the reference's CPU path) on a
-           bounded sample of the same frame (bands of rows, 1 spp each).
+           bounded sample of the same frame (bands of 32 rows, 1 spp each,
+           ~12 s on all host cores).
+secondary: on one GPU the same line carries the box workload (256x256,
+           16 spp, depth 8) and the gem workload (57-facet brilliant, 2M-photon
+           caustic map rebuilt every step, 1280x720, 256 spp, depth 32), each
+           with its value, e2e, roofline and cpu_baseline.
+--impl reference: the CPU oracle on all host cores, each step 80 bands of
+           32 rows x 1920 px x 1 spp of the icosphere frame (the cpu_baseline
+           sampler), so the default run times ~10 s.
 """
 import argparse
 import json
@@ -44,6 +52,7 @@ DEPTH = 12
 HERO = 4
 METRIC = "path samples/s (1920x1080 icosphere workload)"
 UNIT = "path samples/s"
+REF_BANDS = 80          # bands of 32 rows per reference-arm step (~0.5 s on 16 cores)
 
 
 def parse():
@@ -54,6 +63,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-roofline", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="leave out the box and gem lines")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--mode", choices=["bench", "pass"], default="bench",
                     help="pass: one warm-up call + one measured 16-spp call of the workload, no JSON (profiler driver)")
@@ -162,11 +172,14 @@ def run_reference(args):
     from rustracer_b200.renderer import pass_params
     o = O.OracleScene(sb)
 
+    def band(k):
+        row0 = (k * 97) % (H - 32)
+        p = pass_params(W, H, k, 1, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 1000 + k)
+        o.render_pass(st["camera"], p, threads=threads, rows=(row0, row0 + 32))
+        return 32 * W
+
     def step(k):
-        row0 = (k * 131) % (H - 16)
-        p = pass_params(W, H, k, 1, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 77 + k)
-        o.render_pass(st["camera"], p, threads=threads, rows=(row0, row0 + 16))
-        return 16 * W
+        return sum(band(k * REF_BANDS + b) for b in range(REF_BANDS))
 
     for k in range(args.warmup):
         step(k)
@@ -174,7 +187,8 @@ def run_reference(args):
     n = sum(step(args.warmup + k) for k in range(args.steps))
     el = time.perf_counter() - t0
     v = n / el
-    sample = f"{args.steps} steps of 16 rows x {W} px x 1 spp of the {W}x{H} frame"
+    sample = (f"{args.steps} steps of {REF_BANDS} bands of 32 rows x {W} px x 1 spp of the {W}x{H} frame "
+              f"({n} path samples, {el:.1f} s)")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": el * 1000 / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -194,6 +208,10 @@ def run_ours(args):
     from rustracer_b200.renderer import GpuScene, pass_params
 
     ws, rank, local = dist_env()
+    if ws != args.gpus:
+        sys.exit(f"bench.py --gpus {args.gpus} runs one process per GPU: start it with "
+                 f"`python -m torch.distributed.run --nproc-per-node {args.gpus} ... bench.py --gpus {args.gpus}` "
+                 f"(WORLD_SIZE is {ws})")
     if ws > 1:
         import torch.distributed as dist
         from datetime import timedelta
@@ -311,6 +329,12 @@ def run_ours(args):
         threads = os.cpu_count() or 1
         v, sample = cpu_band_rate(sb, st, args.cpu_seconds, threads)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+    if rank == 0 and ws == 1 and not args.no_secondary:
+        # configs 1 and 3 beside the headline (one GPU; the scaling run measures the headline)
+        scene.close()
+        del outs, flush
+        torch.cuda.empty_cache()
+        line["secondary"] = [secondary(k, args) for k in ("box", "gem")]
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -319,14 +343,20 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
-def roofline(scene, sb, cam):
-    """Roofline of the extend (closest-hit) kernel; see the module docstring."""
+def roofline(scene, sb, cam, w=W, h=H, spp=SPP, depth=DEPTH, hero=HERO, seed=2, traffic_file="extend_icosphere_traffic.txt"):
+    """Roofline of the extend (closest-hit) kernel; see the module docstring.
+    The kernel is not HBM-bound: its node and primitive fetches are served
+    mostly by L1 and L2, so `frac` (algorithmic bytes per second over the HBM
+    copy peak) measures how fast the cache hierarchy delivers the reference
+    layout's bytes, and `dram_frac` beside it is the DRAM traffic ncu measured
+    for the kernel over the same time."""
     from oracle import oracle as O
     from rustracer_b200.renderer import pass_params
     peak, peak_kind = measured_peak()
-    p1 = pass_params(W, H, 5000, 1, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2)
+    strata = int(np.sqrt(np.float32(spp)))
+    p1 = pass_params(w, h, 5000, 1, strata, depth, hero, 1.0, seed)
     scene.set_profiling(True)
-    p = pass_params(W, H, 6000, SPP, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2)
+    p = pass_params(w, h, 6000, spp, strata, depth, hero, 1.0, seed)
     scene.render_accumulate(cam, p)
     kt = scene.kernel_times()
     ext_rays = scene.last_stats()["ext_rays"]
@@ -335,8 +365,8 @@ def roofline(scene, sb, cam):
     rng = np.random.default_rng(0)
     total_bytes_pass = 0.0
     per_depth = []
-    for d in range(DEPTH):
-        r = scene.capture_rays(cam, p1, d, W * H)
+    for d in range(depth):
+        r = scene.capture_rays(cam, p1, d, w * h)
         if len(r) == 0:
             break
         sub = r[rng.choice(len(r), size=min(len(r), 20000), replace=False)]
@@ -345,23 +375,130 @@ def roofline(scene, sb, cam):
         total_bytes_pass += bpr * len(r)
         per_depth.append((d, len(r), float(bpr), float(stt[:, 0].mean()), float(stt[:, 1].mean())))
     ext_ms, ext_launches = kt["extend"]
-    # total algorithmic bytes of all extend launches of the 64-spp render ÷ their total device time
-    achieved = total_bytes_pass * SPP / (ext_ms / 1000.0) / 1e9 if ext_ms > 0 else None
-    # DRAM traffic: ncu's bytes per extension ray on this kernel and scene (profiles/)
-    # times this render's extension rays per launch
+    # total algorithmic bytes of all extend launches of the render ÷ their total device time
+    achieved = total_bytes_pass * spp / (ext_ms / 1000.0) / 1e9 if ext_ms > 0 else None
+    # DRAM traffic: ncu's bytes per extension ray on this kernel and scene
+    # (a profile summary) times this render's extension rays per launch
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "extend_icosphere_traffic.txt")
-    if os.path.exists(tfile):
+    tfile = os.path.join(ROOT, "profiles", traffic_file) if traffic_file else None
+    if tfile and os.path.exists(tfile):
         for ln in open(tfile):
             if ln.startswith("traffic_bytes_per_ray:"):
                 traffic = float(ln.split(":")[1]) * ext_rays / max(1, ext_launches)
-    return {"kernel": "k_extend (8-wide BVH closest hit)", "bound": "hbm", "achieved": achieved, "peak": peak,
+    launch_s = ext_ms / 1000.0 / max(1, ext_launches)
+    dram_gbs = traffic / launch_s / 1e9 if (traffic and launch_s > 0) else None
+    return {"kernel": "k_extend (8-wide BVH closest hit)", "bound": "hbm",
+            "limiter": "L1/TEX throughput and load latency (node fetches hit L1/L2), not DRAM bandwidth",
+            "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
-            "traffic": traffic, "algorithmic_bytes_per_launch": total_bytes_pass * SPP / max(1, ext_launches),
+            "traffic": traffic, "dram_gbs": dram_gbs, "dram_frac": dram_gbs / peak if dram_gbs else None,
+            "algorithmic_bytes_per_launch": total_bytes_pass * spp / max(1, ext_launches),
             "launches": ext_launches, "kernel_ms": ext_ms,
             "stage_ms": {k: v[0] for k, v in kt.items()},
             "per_bounce": [{"depth": d, "rays": n, "bytes_per_ray": b, "nodes_per_ray": nn, "tris_per_ray": tt}
                            for d, n, b, nn, tt in per_depth]}
+
+
+def secondary(kind, args):
+    """One secondary workload of the headline line (one GPU): `value` from the
+    library's CUDA-event time of each step (plus the photon build's device
+    time for the gem), `e2e` through rt_render_accumulate with host output
+    buffers (and the photon build) timed by the host clock, the extend
+    kernel's roofline and the oracle's CPU rate on bands of the same frame."""
+    import torch
+    from oracle import oracle as O
+    from rustracer_b200 import configs
+    from rustracer_b200.renderer import GpuScene, pass_params
+    if kind == "box":
+        sb, st = configs.box_scene()
+        steps, warm = args.steps, args.warmup
+    else:
+        sb, st = configs.gem_scene()
+        steps, warm = max(1, min(args.steps, 3)), 1
+    w, h, spp, depth, hero = st["width"], st["height"], st["spp"], st["max_depth"], st["hero"]
+    strata = int(np.sqrt(np.float32(spp)))
+    cam = st["camera"]
+    scene = GpuScene(sb, device=0)
+    dev = torch.device("cuda", 0)
+    outs = (torch.zeros((h, w, 3), device=dev), torch.zeros((h, w, 3), device=dev),
+            torch.zeros((h, w), dtype=torch.int32, device=dev))
+    host = (torch.empty((h, w, 3), pin_memory=True), torch.empty((h, w, 3), pin_memory=True),
+            torch.empty((h, w), dtype=torch.int32, pin_memory=True))
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    photons = kind == "gem"
+    stored = []
+
+    def step(k, o):
+        ph_ms = 0.0
+        if photons:
+            stored.append(scene.photon_build(st["photon_params"](seed=k)))
+            ph_ms = sum(scene.photon_stage_ms())
+        scene.render_accumulate(cam, pass_params(w, h, k * spp, spp, strata, depth, hero, 1.0, 7), outputs=o)
+        stt = scene.last_stats()
+        return stt["ms"] + ph_ms, ph_ms, stt
+
+    for k in range(warm):
+        step(k, outs)
+    flush.fill_(1)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms, ph, ext, sh, launches = [], [], 0, 0, 0
+    for k in range(steps):
+        a, b, stt = step(warm + k, outs)
+        ms.append(a)
+        ph.append(b)
+        ext += stt["ext_rays"]
+        sh += stt["shadow_rays"]
+        launches += stt["launches"]
+        flush.fill_(k & 0xFF)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    per_step = w * h * spp
+    e2e_s = []
+    for k in range(max(2, min(steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step(1000 + k, host)
+        e2e_s.append(time.perf_counter() - t0)
+    line = {
+        "workload": st["name"], "metric": f"path samples/s ({w}x{h} {kind} workload)",
+        "value": per_step * steps / (sum(ms) / 1000.0), "unit": UNIT, "steps": steps, "warmup": warm,
+        "ms_per_step": sum(ms) / steps, "clocks": clk, "gpu_launches": int(launches),
+        "e2e": {"value": per_step * len(e2e_s) / sum(e2e_s), "unit": UNIT,
+                "h2d_bytes_per_step": 136, "d2h_bytes_per_step": h * w * (3 + 3) * 4 + h * w * 4},
+        "rays": {"extension": int(ext), "shadow": int(sh), "rays_per_s": (ext + sh) / (sum(ms) / 1000.0)},
+        "l2": "256 MB buffer written between timed steps",
+    }
+    if photons:
+        line["photon_map"] = {"emitted": st["photons"], "stored_mean": int(np.mean(stored)),
+                              "build_ms": float(np.mean(ph)),
+                              "stage_ms": dict(zip(("trace", "compact", "tree"), scene.photon_stage_ms())),
+                              "source": "the two light quads, aimed at the stone's bounding sphere (projection map)",
+                              "knn_k": st["knn_k"], "radius_max": st["radius_max"]}
+    if not args.no_roofline:
+        line["roofline"] = roofline(scene, sb, cam, w, h, min(spp, 16), depth, hero, 7,
+                                    traffic_file=f"extend_{kind}_traffic.txt")
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        o = O.OracleScene(sb)
+        if photons:
+            o.photon_build(st["photon_params"](seed=1))
+        n, k, t0 = 0, 0, time.perf_counter()
+        while time.perf_counter() - t0 < args.cpu_seconds:
+            row0 = (k * 61) % max(1, h - 32)
+            o.render_pass(cam, pass_params(w, h, k, 1, strata, depth, hero, 1.0, 900 + k), threads=threads,
+                          rows=(row0, min(h, row0 + 32)))
+            n += min(32, h) * w
+            k += 1
+        el = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": n / el, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{k} bands of 32 rows x {w} px x 1 spp ({n} path samples, {el:.1f} s)"
+                                          + ("; photon map built once before timing" if photons else "")}
+    scene.close()
+    del outs, host, flush
+    torch.cuda.empty_cache()
+    return line
 
 
 def run_gem(args):

@@ -19,7 +19,12 @@
  *  - The caller owns every buffer it passes; the library copies what it keeps.
  *  - Buffers flagged RT_MEM_DEVICE are CUDA device pointers on the scene's
  *    device; otherwise they are host pointers (pageable or pinned).
- *  - One handle per thread; calls on one handle are serialised on its stream.
+ *  - One handle per thread; calls on one handle are serialised on its own
+ *    (non-blocking) stream.  Every call first makes that stream wait for the
+ *    work already queued on the caller's stream (rt_set_caller_stream; the
+ *    legacy default stream unless set), so device buffers written by the
+ *    caller's kernels are complete before the library reads them, and every
+ *    call has finished its device work when it returns.
  *  - All arithmetic is IEEE-754 binary32 ("f32" in the reference).
  */
 #ifndef RT_API_H
@@ -398,6 +403,11 @@ int32_t rt_rgbe_decode(const uint8_t* scanlines, size_t n_bytes, int32_t width, 
 #define RT_EMIT_QUAD     1   /* cosine-weighted quad (PhotonMap::build_from_quad, photon.rs:97-135) */
 #define RT_EMIT_SUN      2   /* the Physical sky's sun: a disk facing sun_dir with the sky radiance at
                                 the sun direction nudged by 0.04, ×π (scene.rs:40-52); dir/color unused */
+#define RT_EMIT_LIGHT    3   /* a quad of the scene's NEE light list as a cosine-weighted quad source
+                                (build_from_quad) coloured by its material's emission: a diffuse light's
+                                colour, a blackbody's time-averaged RGB × intensity (material.rs:53-59);
+                                the reference's rebuild_caustics picks the env disk over the lights when
+                                both exist (scene.rs:52-73), this type lets a caller emit from the lights */
 #define RT_MAX_EMITTERS  8
 
 typedef struct RtPhotonEmitter {
@@ -407,6 +417,16 @@ typedef struct RtPhotonEmitter {
     float    corner[3];     /* QUAD corner, edges u and v */
     float    u[3], v[3];
     uint32_t n_photons;     /* photons emitted by this source */
+    int32_t  light;         /* LIGHT: index into the scene's light list (RtSceneDesc.light_prims), a quad */
+    /* QUAD / LIGHT: a sphere (centre xyz, radius) around the specular objects
+     * the caustics come from, or radius 0.  With a radius, every photon leaves
+     * toward the sphere (uniform in the cone it subtends) and its power is
+     * scaled by the cosine-density ratio 2·cosθ·(1 − cos θ_max), zero below the
+     * light's plane; photons whose first hit is diffuse are never stored
+     * (trace_photon, photon.rs:232-277), so the expected map is that of the
+     * full hemisphere while almost every photon reaches the stones (a
+     * projection map).  The reference emits over the whole hemisphere. */
+    float    target[4];
 } RtPhotonEmitter;
 
 typedef struct RtPhotonParams {
@@ -415,6 +435,14 @@ typedef struct RtPhotonParams {
     float    gather_radius; /* Epanechnikov radius (photon.rs:137-157), or the k-NN maximum radius */
     uint32_t knn_k;         /* 0: fixed-radius gather (the reference); k > 0: k nearest within the radius */
     uint64_t seed;
+    /* A shard of the emission: trace only the photons with emission index
+     * first_photon .. first_photon + shard_photons − 1 (indices run over the
+     * emitters in order; shard_photons 0: all of them).  Photon power stays
+     * normalised by each emitter's full n_photons, so the stored photons of
+     * all shards together are the photons of one unsharded build (ranks of
+     * a multi-GPU render each trace a shard and exchange what they store). */
+    uint32_t first_photon;
+    uint32_t shard_photons;
 } RtPhotonParams;
 
 /* Emit, trace and store photons on the device, then build the gather
@@ -423,6 +451,12 @@ typedef struct RtPhotonParams {
  * photon.rs:41-135, trace_photon :232-277, kd_build :165-191).  The map then
  * feeds every diffuse vertex of later render calls (renderer.rs:461-467). */
 int32_t rt_photon_build(RtScene* scene, const RtPhotonParams* params, int64_t* n_stored);
+
+/* Device time of the last rt_photon_build's stages (diagnostics, no reference
+ * counterpart), from CUDA events on the scene's stream: ms[0] emission and
+ * tracing, ms[1] compaction of the stored photons, ms[2] the gather
+ * structure (Morton sort and box heap). */
+int32_t rt_photon_build_times(const RtScene* scene, float* ms);
 /* Replace the map with caller-given photons (n × 3 positions, powers, normals;
  * indices = emission index used to break distance ties). */
 int32_t rt_photon_set(RtScene* scene, const float* pos, const float* power, const float* nor,
@@ -467,9 +501,14 @@ int32_t rt_capture_rays(RtScene* scene, const RtCamera* cam, const RtPassParams*
  * fixed device array inside the library (RT_NOALLOC_SCRATCH_BYTES, held on
  * every GPU that loads the library until exit) instead of cudaMalloc.
  *  - scratch_rgb must be DEVICE memory: n_samples × height × width × 3 floats.
- *  - width × height must not exceed RT_NOALLOC_MAX_PIXELS (RT_ERR_CAPACITY).
+ *  - The array holds a pool of 32,768 paths that is refilled with new samples
+ *    as paths end, so any frame fits it; but 32,768 paths fill a small part of
+ *    the GPU, so width × height is capped at RT_NOALLOC_MAX_PIXELS (a chosen
+ *    limit, RT_ERR_CAPACITY beyond it): larger frames belong on
+ *    rt_render_pass, whose pool grows to 8,388,608 paths.
  *  - The first call on a device looks up the array's device address
  *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - Like every call here, it waits for its device work before returning.
  *  - All calls share the one array: calls that overlap on the GPU (two
  *    streams, two threads, two scenes on one device) race and must be
  *    serialised by the caller.
@@ -490,8 +529,29 @@ typedef struct RtTuning {
     uint32_t max_paths;            /* 0 or 65536 .. 8388608 */
     uint32_t trace_blocks_per_sm;  /* 0 or 1 .. 8 (capped at the kernels' resident blocks) */
     uint32_t shade_blocks_per_sm;  /* 0 or 1 .. 32 */
+    /* Limits of the device loops (0: the built-in ones, which a render of the
+     * scene never reaches).  Lower values exist to exercise the error paths:
+     * a render call whose wavefront has not drained after max_iterations
+     * iterations returns RT_ERR_TIMEOUT; a traversal that needs more than
+     * stack_limit stack entries stops and the call returns RT_ERR_CAPACITY.
+     * rt_get_tuning reports the stack entries in force (7 per tree level). */
+    uint32_t max_iterations;       /* 0 or ≥ 1 */
+    uint32_t stack_limit;          /* 0 or 1 .. the built-in capacity */
+    /* Traversal stack entries kept in shared memory per thread before the
+     * rest spills to global memory (0: 16; else a power of two ≤ 16).  The
+     * results never depend on it; small rings make every traversal take the
+     * spill path. */
+    uint32_t stack_ring;
 } RtTuning;
 int32_t rt_set_tuning(RtScene* scene, const RtTuning* tuning);
+
+/* The stream the caller queues its own work on (a cudaStream_t; NULL = the
+ * legacy default stream, the initial setting).  No counterpart in the
+ * reference, whose render_tiles works on host memory only: a host that passes
+ * RT_MEM_DEVICE buffers written by its own kernels names the stream they were
+ * queued on, and every later call on this handle waits for that stream's work
+ * so far before its first kernel. */
+int32_t rt_set_caller_stream(RtScene* scene, void* cuda_stream);
 int32_t rt_get_tuning(const RtScene* scene, RtTuning* tuning);
 
 /* ── path guiding: a learned proposal at diffuse vertices (no counterpart in

@@ -1981,9 +1981,30 @@ static Aabb world_bounds(const Scene& s) {
 }
 
 // Emitter geometry for photon `i` of emitter `e` (photon.rs:41-94, 97-135).
-struct EmitterSetup { V3 t, b, center, dir, power, normal, corner, u, v, ta, ba; float radius, lum_clamp; int type; };
+struct EmitterSetup {
+    V3 t, b, center, dir, power, normal, corner, u, v, ta, ba;
+    float radius, lum_clamp;
+    int type;
+    V3 target;        // projection sphere of a quad source (target_r 0: the whole hemisphere)
+    float target_r;
+};
 static EmitterSetup setup_emitter(const Scene& s, const RtPhotonEmitter& e0) {
     RtPhotonEmitter e = e0;
+    if (e.type == RT_EMIT_LIGHT) {
+        // a quad of the light list as PhotonMap::build_from_quad's source
+        // (photon.rs:97-135), coloured by the emission of its material: a diffuse
+        // light's colour, a blackbody's time-averaged RGB × intensity (material.rs:53-59)
+        const Quad& q = s.quads[s.lights[e.light] - s.n_tris];
+        const RtMaterial& m = s.mats[q.mat];
+        V3 col = m.type == RT_MAT_BLACKBODY_LIGHT ? s.bb_avg[q.mat]
+               : m.type == RT_MAT_PBR ? v3(m.emission[0], m.emission[1], m.emission[2]) * m.emission_strength
+               : v3(m.albedo[0], m.albedo[1], m.albedo[2]);
+        e.type = RT_EMIT_QUAD;
+        e.corner[0] = q.q.x; e.corner[1] = q.q.y; e.corner[2] = q.q.z;
+        e.u[0] = q.u.x; e.u[1] = q.u.y; e.u[2] = q.u.z;
+        e.v[0] = q.v.x; e.v[1] = q.v.y; e.v[2] = q.v.z;
+        e.color[0] = col.x; e.color[1] = col.y; e.color[2] = col.z;
+    }
     if (e.type == RT_EMIT_SUN) {
         // rebuild_caustics with a Physical sky (scene.rs:40-52): the sun as a disk
         // emitter, coloured by the sky radiance 0.04 off the sun direction, ×π
@@ -2025,24 +2046,45 @@ static EmitterSetup setup_emitter(const Scene& s, const RtPhotonEmitter& e0) {
         onb_vec(E.normal, &E.ta, &E.ba);
         E.power = v3(e.color[0], e.color[1], e.color[2]) * (area * PI_F / (float)e.n_photons);
         E.lum_clamp = 15.0f;
+        E.target = v3(e.target[0], e.target[1], e.target[2]);
+        E.target_r = e.target[3] > 0.0f ? e.target[3] : 0.0f;
     }
     return E;
 }
 
-static void emit_photon(const EmitterSetup& E, const Rng& rng, V3* pos, V3* dir) {
+// One photon of an emitter; returns the factor on the emitter's photon power
+// (1, or for a quad aimed at its projection sphere the ratio of the cosine
+// density to the cone's uniform density, 0: not traced).
+static float emit_photon(const EmitterSetup& E, const Rng& rng, V3* pos, V3* dir) {
     if (E.type == RT_EMIT_DISK) {
         float r = E.radius * std::sqrt(rnd(rng, P_EMIT0));
         float phi = 2.0f * PI_F * rnd(rng, P_EMIT1);
         *pos = E.center + E.t * (r * std::cos(phi)) + E.b * (r * std::sin(phi));
         *dir = E.dir;
-    } else {
-        float ss = rnd(rng, P_EMIT0), tt = rnd(rng, P_EMIT1);
-        *pos = E.corner + E.u * ss + E.v * tt;
-        float ct = std::sqrt(rnd(rng, P_EMIT2));
-        float st = std::sqrt(1.0f - ct * ct);
-        float phi = 2.0f * PI_F * rnd(rng, P_EMIT3);
-        *dir = st * std::cos(phi) * E.ta + st * std::sin(phi) * E.ba + ct * E.normal;
+        return 1.0f;
     }
+    float ss = rnd(rng, P_EMIT0), tt = rnd(rng, P_EMIT1);
+    *pos = E.corner + E.u * ss + E.v * tt;
+    if (E.target_r > 0.0f) {
+        // uniform in the cone toward the projection sphere (the sphere-light
+        // sampling of sphere.rs:111-118)
+        V3 tc = E.target - *pos;
+        float d2 = len2(tc), rr = E.target_r * E.target_r;
+        if (d2 > rr) {
+            float ctm = std::sqrt(1.0f - rr / d2);
+            float phi = 2.0f * PI_F * rnd(rng, P_EMIT3);
+            float ct = 1.0f - rnd(rng, P_EMIT2) * (1.0f - ctm);
+            float st = std::sqrt(rmax(1.0f - ct * ct, 0.0f));
+            *dir = onb_local(onb_from_w(unit(tc)), v3(std::cos(phi) * st, std::sin(phi) * st, ct));
+            float cl = dot(*dir, E.normal);
+            return cl > 0.0f ? 2.0f * cl * (1.0f - ctm) : 0.0f;
+        }
+    }
+    float ct = std::sqrt(rnd(rng, P_EMIT2));
+    float st = std::sqrt(1.0f - ct * ct);
+    float phi = 2.0f * PI_F * rnd(rng, P_EMIT3);
+    *dir = st * std::cos(phi) * E.ta + st * std::sin(phi) * E.ba + ct * E.normal;
+    return 1.0f;
 }
 
 // ── hero-wavelength state ────────────────────────────────────────────────────
@@ -3079,9 +3121,16 @@ int32_t orc_photon_build(void* sp, const RtPhotonParams* p, int64_t* n_stored, i
     if (!p || p->n_emitters < 0 || p->n_emitters > RT_MAX_EMITTERS || !(p->gather_radius > 0.0f)) return RT_ERR_INVALID;
     uint32_t total = 0;
     for (int e = 0; e < p->n_emitters; e++) {
-        if (p->emitters[e].type == RT_EMIT_SUN && s->bg.type != RT_BG_PHYSICAL) return RT_ERR_INVALID;
-        total += p->emitters[e].n_photons;
+        const RtPhotonEmitter& em = p->emitters[e];
+        if (em.type == RT_EMIT_SUN && s->bg.type != RT_BG_PHYSICAL) return RT_ERR_INVALID;
+        if (em.type == RT_EMIT_LIGHT &&
+            (em.light < 0 || em.light >= (int32_t)s->lights.size() || prim_type(*s, s->lights[em.light]) != RT_PRIM_QUAD))
+            return RT_ERR_INVALID;
+        total += em.n_photons;
     }
+    // a shard of the emission order: photons first .. first + count − 1
+    uint32_t first = p->first_photon, count = p->shard_photons ? p->shard_photons : total - first;
+    if ((uint64_t)first + count > total) return RT_ERR_INVALID;
     std::vector<KdPhoton> slot(total);
     std::vector<uint8_t> ok(total, 0);
     uint32_t off = 0;
@@ -3094,11 +3143,13 @@ int32_t orc_photon_build(void* sp, const RtPhotonParams* p, int64_t* n_stored, i
         parallel_rows(nch, threads, [&](uint32_t c, int) {
             for (uint32_t i = c * chunk; i < std::min(n, (c + 1) * chunk); i++) {
                 uint32_t gid = base + i;
+                if (gid < first || gid - first >= count) continue;
                 Rng rng = photon_rng(p->seed, gid);
                 V3 pos, dir;
-                emit_photon(E, rng, &pos, &dir);
+                float wgt = emit_photon(E, rng, &pos, &dir);
+                if (!(wgt > 0.0f)) continue;
                 KdPhoton k;
-                if (trace_photon(*s, pos, dir, E.lum_clamp, E.power, rng, &k)) {
+                if (trace_photon(*s, pos, dir, E.lum_clamp, E.power * wgt, rng, &k)) {
                     k.idx = (int32_t)gid;
                     slot[gid] = k;
                     ok[gid] = 1;

@@ -224,8 +224,10 @@ class RtDevelopParams(C.Structure):
 
 
 class RtTuning(C.Structure):
-    """RtTuning (include/rt_api.h): path-pool capacity and launch grids (0 = built-in)."""
-    _fields_ = [("max_paths", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32), ("shade_blocks_per_sm", C.c_uint32)]
+    """RtTuning (include/rt_api.h): path-pool capacity, launch grids and the
+    device loops' limits (0 = built-in)."""
+    _fields_ = [("max_paths", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32), ("shade_blocks_per_sm", C.c_uint32),
+                ("max_iterations", C.c_uint32), ("stack_limit", C.c_uint32), ("stack_ring", C.c_uint32)]
 
 
 class RtGuideParams(C.Structure):
@@ -287,7 +289,7 @@ def iptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_int32))
 
 
-RT_EMIT_DISK, RT_EMIT_QUAD, RT_EMIT_SUN = 0, 1, 2
+RT_EMIT_DISK, RT_EMIT_QUAD, RT_EMIT_SUN, RT_EMIT_LIGHT = 0, 1, 2, 3
 RT_MAX_EMITTERS = 8
 
 
@@ -300,6 +302,8 @@ class RtPhotonEmitter(C.Structure):
         ("u", F3),
         ("v", F3),
         ("n_photons", C.c_uint32),
+        ("light", C.c_int32),
+        ("target", C.c_float * 4),
     ]
 
 
@@ -310,4 +314,6 @@ class RtPhotonParams(C.Structure):
         ("gather_radius", C.c_float),
         ("knn_k", C.c_uint32),
         ("seed", C.c_uint64),
+        ("first_photon", C.c_uint32),
+        ("shard_photons", C.c_uint32),
     ]

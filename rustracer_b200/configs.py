@@ -204,51 +204,129 @@ def media_box_scene(width=256, height=256, spp=16, max_depth=24, hero=4, seed=5,
     return sb, st
 
 
-def round_brilliant(radius=0.5, table_pct=57.0, crown_angle=34.5, pavilion_angle=40.75, girdle_pct=3.0,
-                    girdle_facets=16, band_facets=64, subdiv=1, center=(0.0, 0.0, 0.0)):
-    """A round brilliant as a triangle mesh: the half-spaces of Diamond::new
-    (diamond.rs:93-195 — table, N crown and N pavilion facets through the girdle
-    band edges, and a ground-round band of vertical planes), intersected with
-    scipy's half-space intersection and triangulated by the convex hull; each
-    triangle is split 4-way `subdiv` times (the solid is unchanged).  Returns
-    (vertices (n,3), faces (m,3))."""
-    from scipy.spatial import ConvexHull, HalfspaceIntersection
+def brilliant_planes(radius=0.5, table_pct=57.0, crown_angle=34.5, pavilion_angle=40.75, girdle_pct=3.0,
+                     star_angle=22.0, upper_girdle_angle=42.0, lower_girdle_angle=41.5, girdle_facets=32):
+    """Half-spaces of a 57-facet round brilliant: the table, 8 star, 8 bezel
+    and 16 upper-girdle facets of the crown, 16 lower-girdle facets and 8
+    pavilion mains, plus a girdle of `girdle_facets` vertical planes.  Bezels
+    and pavilion mains sit at azimuths k·45° and leave the girdle edge there at
+    the crown and pavilion angles; the table height is where a bezel reaches
+    the table radius (table_pct % of the girdle diameter); stars lie on the
+    table's octagon edges between the bezels; the girdle halves leave the
+    girdle at k·45° + 22.5° ± 11.25°, steeper than the mains.  Returns a list
+    of (unit outward normal, point on the plane, facet kind)."""
     r = radius
-    table_r = table_pct / 100.0 * r
-    crown_h = (r - table_r) * math.tan(math.radians(crown_angle))
-    pav_h = r * math.tan(math.radians(pavilion_angle))
-    girdle_h = min(max(girdle_pct / 100.0 * 2.0 * r, 0.0), 0.3 * r)
-    n = max(girdle_facets, 4) // 2 * 2
-    planes = [((0.0, 1.0, 0.0), (0.0, 0.5 * girdle_h + crown_h, 0.0))]
-    for k in range(n):
-        th = k * 2.0 * math.pi / n
-        sn, c = math.sin(th), math.cos(th)
-        planes.append(((c * crown_h, r - table_r, sn * crown_h), (c * r, 0.5 * girdle_h, sn * r)))
-    for k in range(n):
-        ph = k * 2.0 * math.pi / n
-        sn, c = math.sin(ph), math.cos(ph)
-        planes.append(((c * pav_h, -r, sn * pav_h), (c * r, -0.5 * girdle_h, sn * r)))
-    for j in range(band_facets):
-        a = j * 2.0 * math.pi / band_facets
-        planes.append(((math.cos(a), 0.0, math.sin(a)), (math.cos(a) * r, 0.0, math.sin(a) * r)))
+    ca, pa = math.radians(crown_angle), math.radians(pavilion_angle)
+    t_r = table_pct / 100.0 * r
+    gh = girdle_pct / 100.0 * 2.0 * r
+    y_gt, y_gb = 0.5 * gh, -0.5 * gh
+    y_tab = y_gt + (r - t_r) * math.tan(ca)
+
+    def tilted(phi, alpha, rho, y, up):
+        n = (math.sin(alpha) * math.cos(phi), math.cos(alpha) if up else -math.cos(alpha), math.sin(alpha) * math.sin(phi))
+        return n, (rho * math.cos(phi), y, rho * math.sin(phi))
+
+    P = [((0.0, 1.0, 0.0), (0.0, y_tab, 0.0), "table")]
+    half = math.pi / 8.0
+    for k in range(8):
+        th = k * math.pi / 4.0
+        P.append(tilted(th, ca, r, y_gt, True) + ("bezel",))
+        P.append(tilted(th, pa, r, y_gb, False) + ("pavilion",))
+        P.append(tilted(th + half, math.radians(star_angle), t_r * math.cos(half), y_tab, True) + ("star",))
+        for sgn in (-1.0, 1.0):
+            phi = th + half + sgn * half / 2.0
+            P.append(tilted(phi, math.radians(upper_girdle_angle), r, y_gt, True) + ("upper_girdle",))
+            P.append(tilted(phi, math.radians(lower_girdle_angle), r, y_gb, False) + ("lower_girdle",))
+    for j in range(girdle_facets):
+        a = (j + 0.5) * 2.0 * math.pi / girdle_facets
+        P.append(((math.cos(a), 0.0, math.sin(a)), (math.cos(a) * r, 0.0, math.sin(a) * r), "girdle"))
+    return P
+
+
+def round_brilliant(radius=0.5, table_pct=57.0, crown_angle=34.5, pavilion_angle=40.75, girdle_pct=3.0,
+                    split=3, center=(0.0, 0.0, 0.0), **facet_angles):
+    """The 57-facet round brilliant of brilliant_planes as a closed triangle
+    mesh: the half-spaces are intersected (scipy's half-space intersection),
+    the solid's hull triangulated with outward winding, and every triangle
+    split into split² (the solid is unchanged): 254 hull triangles, 2,286 at
+    the default split.  Returns (vertices (n,3), faces (m,3))."""
+    from scipy.spatial import ConvexHull, HalfspaceIntersection
+    P = brilliant_planes(radius, table_pct, crown_angle, pavilion_angle, girdle_pct, **facet_angles)
     hs = []
-    for nv, g in planes:
+    for nv, g, _ in P:
         nv = np.asarray(nv, np.float64)
         nv = nv / np.linalg.norm(nv)
         hs.append(list(nv) + [-float(nv @ np.asarray(g, np.float64))])      # n·x − d ≤ 0
     hi = HalfspaceIntersection(np.array(hs), np.zeros(3))
     V = hi.intersections
     hull = ConvexHull(V)
+    V = hull.points
     F = hull.simplices.copy()
-    # orient every triangle outward
     ctr = V.mean(axis=0)
     for i, (a, b, c) in enumerate(F):
         nrm = np.cross(V[b] - V[a], V[c] - V[a])
         if nrm @ (V[a] - ctr) < 0:
             F[i] = (a, c, b)
-    for _ in range(subdiv):
-        V, F = _split4(V, F)
+    used = np.unique(F)
+    remap = -np.ones(len(V), np.int64)
+    remap[used] = np.arange(len(used))
+    V, F = V[used], remap[F]
+    if split > 1:
+        V, F = _split_n(V, F, split)
     return V + np.asarray(center, np.float64), F
+
+
+def brilliant_facets(V, F, radius=0.5, **kw):
+    """Facet kind of every triangle of a round_brilliant mesh (centred at the
+    origin), by the plane it lies on."""
+    P = brilliant_planes(radius, **kw)
+    kinds = []
+    for a, b, c in F:
+        m = (V[a] + V[b] + V[c]) / 3.0
+        nrm = np.cross(V[b] - V[a], V[c] - V[a])
+        nrm = nrm / np.linalg.norm(nrm)
+        best = min(P, key=lambda p: np.abs(np.asarray(p[0]) / np.linalg.norm(p[0]) - nrm).sum()
+                   + abs(np.dot(np.asarray(p[0]) / np.linalg.norm(p[0]), m - np.asarray(p[1]))))
+        kinds.append(best[2])
+    return kinds
+
+
+def _split_n(V, F, k):
+    """Split each triangle into k² by a k-step barycentric grid (shared edge
+    points are merged, so the mesh stays closed)."""
+    V = [tuple(v) for v in V]
+    index = {}
+
+    def point(a, b, c, i, j):
+        # barycentric grid point (i, j, k − i − j) over corners a, b, c, keyed by
+        # its exact rational position on the shared edge or face
+        w = {a: k - i - j, b: i, c: j}
+        key = tuple(sorted((p, q) for p, q in w.items() if q))
+        if key not in index:
+            pos = sum(np.asarray(V[p]) * q for p, q in w.items()) / k
+            index[key] = len(V)
+            V.append(tuple(pos))
+        return index[key]
+
+    out = []
+    for a, b, c in F:
+        g = {}
+        for i in range(k + 1):
+            for j in range(k + 1 - i):
+                if i == 0 and j == 0:
+                    g[(i, j)] = a
+                elif i == k:
+                    g[(i, j)] = b
+                elif j == k:
+                    g[(i, j)] = c
+                else:
+                    g[(i, j)] = point(a, b, c, i, j)
+        for i in range(k):
+            for j in range(k - i):
+                out.append((g[(i, j)], g[(i + 1, j)], g[(i, j + 1)]))
+                if i + j < k - 1:
+                    out.append((g[(i + 1, j)], g[(i + 1, j + 1)], g[(i, j + 1)]))
+    return np.array(V, np.float64), np.array(out, np.int64)
 
 
 def _split4(V, F):
@@ -291,11 +369,16 @@ def env_caustic_dir(env, seed=0xC0FFEE, n=8):
 
 def gem_scene(width=1280, height=720, spp=256, max_depth=32, hero=4, seed=3, env_w=1024, env_h=512,
               photons=2_000_000, knn_k=64, radius_max=0.01):
-    """The gem workload: a round brilliant (girdle Ø1, table 57 %, crown 34.5°,
-    pavilion 40.75°, girdle 3 %) in the diamond preset's Cauchy dispersion
-    (B 2.351, C 0.0230: n_D 2.417, n_F − n_C 0.044; scene_file.rs:686) on an
-    albedo-0.8 plane, two 0.3² blackbody lights at 5500 K, the sky env at 0.1,
-    and a caustic photon map (2M photons, k-NN 64 within r ≤ 0.01)."""
+    """The gem workload: a 57-facet round brilliant (girdle Ø1, table 57 %,
+    crown 34.5°, pavilion 40.75°, girdle 3 %; 2,286 triangles) in the diamond
+    preset's Cauchy dispersion (B 2.351, C 0.0230: n_D 2.417, n_F − n_C 0.044;
+    scene_file.rs:686) on an albedo-0.8 plane, two 0.3² blackbody lights at
+    5500 K, the sky env at 0.1, and a caustic photon map of 2M photons emitted
+    from the two lights toward the stone's bounding sphere (a projection map;
+    k-NN 64 within r ≤ 0.01).  The reference's rebuild_caustics would emit
+    from the env map's disk here (scene.rs:52-73), which sends nearly every
+    photon past the stone; the lights are the workload's caustic source.  st["photon_params"](seed) gives the build's
+    RtPhotonParams; st["env_dir"] / st["env_color"] keep the env-disk source."""
     sb = SceneBuilder()
     sb.name = "gem"
     sb.spectral_range = 1 if hero > 1 else 0
@@ -312,9 +395,17 @@ def gem_scene(width=1280, height=720, spp=256, max_depth=32, hero=4, seed=3, env
     sb.set_env(env)
     cam = make_camera((0.0, 1.55, 2.2), (0.0, 0.35, 0.0), vfov=32.0, aspect=width / height)
     d, col = env_caustic_dir(env)
+    from . import photons as _ph
+
+    gem_sphere = _ph.bounding_sphere(V)
+
+    def photon_params(seed=1, n=photons, projection=True):
+        return _ph.light_params(sb, n, radius_max, knn_k=knn_k, seed=seed,
+                                target=gem_sphere if projection else None)
     st = dict(width=width, height=height, spp=spp, max_depth=max_depth, hero=hero, seed=seed, camera=cam,
               name=f"gem {len(Fc)} tris {width}x{height} {spp}spp depth{max_depth} hero{hero}",
-              n_tris=len(Fc), photons=photons, knn_k=knn_k, radius_max=radius_max, env_dir=d, env_color=col)
+              n_tris=len(Fc), photons=photons, knn_k=knn_k, radius_max=radius_max, env_dir=d, env_color=col,
+              photon_params=photon_params)
     return sb, st
 
 

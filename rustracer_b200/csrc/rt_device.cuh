@@ -34,7 +34,6 @@
 #define RT_HIT_MAX_INDEX  0x07FFFFFFu
 // the hit record of a leaf reference (type in 30:28, index in 27:0) and a class code
 #define RT_HIT_MAKE(leaf_ref, code) (((uint32_t)(code) << 29) | ((((leaf_ref) >> 28) & 3u) << 27) | ((leaf_ref) & 0x07FFFFFFu))
-#define RT_STACK      96
 
 namespace rtd {
 
@@ -122,6 +121,12 @@ struct DevScene {
     const float4* shape_par;
     int n_analytic;             // convex solids + shapes (the traversal compiles their tests in only if > 0)
     int trace_per_sm, shade_per_sm;   // launch tuning (host side; 0 = the built-in grids)
+    // traversal stack beyond the shared-memory ring: entry e ≥ RT_SHORT_STACK
+    // of global thread g at stack_spill[(e − RT_SHORT_STACK) · threads + g];
+    // stack_cap entries in all (7 per tree level; lowered only by rt_set_tuning)
+    uint32_t* stack_spill;
+    int stack_cap;
+    int stack_ring;             // shared-memory ring slots: RT_SHORT_STACK unless tuned (a power of two)
     // textures; per triangle 2 float4 of (u, v) at the corners and 3 float4 of
     // corner tangents (NULL: the reference's default UVs and (1, 0, 0) tangents)
     const DevTexture* tex;
@@ -183,6 +188,14 @@ RT_D float3 unit3(float3 a) { return a / sqrtf(len2(a)); }
 RT_HD float lum3(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 RT_HD float clampf_(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
 RT_D float3 reflect3(float3 v, float3 n) { return v - 2.0f * dot3(v, n) * n; }
+// a in the frame of Onb::from_w(n) (onb.rs:10-20)
+RT_D float3 onb_local_w(float3 n, float3 a) {
+    float3 w = unit3(n);
+    float3 h = fabsf(w.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
+    float3 v = unit3(cross3(w, h));
+    float3 u = cross3(w, v);
+    return a.x * u + a.y * v + a.z * w;
+}
 
 // ── counter-based RNG: pcg3d (Jarzynski & Olano, JCGT 2020) ──────────────────
 RT_HD uint32_t mix32(uint32_t x) {

@@ -494,11 +494,21 @@ struct DevBuf {
 struct RtScene {
     int device = 0, sms = 148;
     cudaStream_t stream = nullptr;
+    // the caller's stream (rt_set_caller_stream; default: the legacy default
+    // stream): every call first makes `stream` wait for the work already queued
+    // there, so device buffers the caller is still writing are complete
+    cudaStream_t caller = 0;
+    cudaEvent_t caller_ev = nullptr;
     std::string err;
     DevScene S{};
     std::vector<DevBuf> owned;
     int64_t n_nodes = 0, n_leaves = 0, n_prims = 0;
     int32_t max_depth = 0;
+    int stack_cap_built = 0;          // traversal stack entries the spill columns hold
+    std::vector<DevLight> h_lights;   // host copy of the NEE light list (photon emitters from lights)
+    std::vector<float> h_emission;    // per material: RGB emission of a light material (3 floats)
+    float photon_stage_ms[3] = {0, 0, 0};   // last photon build: trace, compaction, tree
+    uint64_t max_iterations = 0;      // wavefront iteration bound (rt_set_tuning; 0 = derived)
     double sah_cost = 0.0;
     double build_ms = 0.0;
     std::vector<RefNode> ref_nodes;   // reference-layout copy for rt_scene_bvh_export
@@ -585,6 +595,24 @@ static void free_dev(void*& p) {
     p = nullptr;
 }
 
+// Start of every call that launches work: make the scene's device current and
+// order its stream after the work already queued on the caller's stream (the
+// stream is non-blocking, so without this a caller kernel still writing an
+// input buffer, or a caching allocator's freed block still in use, would race
+// with the library's kernels).  Every call synchronises its own stream before
+// it returns, so work the caller queues afterwards needs no ordering.
+static int enter(RtScene* s) {
+    CK(cudaSetDevice(s->device));
+    CK(cudaEventRecord(s->caller_ev, s->caller));
+    CK(cudaStreamWaitEvent(s->stream, s->caller_ev, 0));
+    return RT_OK;
+}
+#define ENTER(s)                          \
+    do {                                  \
+        int rc_e_ = enter(s);             \
+        if (rc_e_) return rc_e_;          \
+    } while (0)
+
 extern "C" {
 
 int32_t rt_version(void) { return RT_API_VERSION; }
@@ -619,6 +647,7 @@ int32_t rt_scene_destroy(RtScene* s) {
     if (s->h_status) cudaFreeHost(s->h_status);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->caller_ev) cudaEventDestroy(s->caller_ev);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return RT_OK;
@@ -641,6 +670,8 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         return bail(fail(s, RT_ERR_CUDA, "cudaStreamCreate failed"));
     cudaEventCreate(&s->ev0);
     cudaEventCreate(&s->ev1);
+    if (cudaEventCreateWithFlags(&s->caller_ev, cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(s, RT_ERR_CUDA, "cudaEventCreate failed"));
     for (auto& e : s->st_ev)
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(s, RT_ERR_CUDA, "cudaEventCreate failed"));
@@ -833,8 +864,20 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         if (brc) return bail(fail(s, RT_ERR_CUDA, std::string("device BVH build: ") + cudaGetErrorString((cudaError_t)brc)));
         s->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
         s->max_depth = B.max_depth;
-        if ((int64_t)B.max_depth * 7 + 8 > RT_STACK)
-            return bail(fail(s, RT_ERR_CAPACITY, "BVH depth " + std::to_string(B.max_depth) + " exceeds the traversal stack"));
+        // traversal stack: a visit of a node at depth k leaves at most 7 entries
+        // per level above it, so 7 · (depth + 1) entries always suffice; the
+        // ones beyond the shared-memory ring spill to a column per persistent
+        // traversal thread (grid ≤ SMs × RT_TRACE_MINB blocks)
+        if (B.max_depth > 4096) return bail(fail(s, RT_ERR_CAPACITY, "BVH deeper than 4096 levels"));
+        s->stack_cap_built = 7 * (B.max_depth + 1) + 8;
+        s->S.stack_cap = s->stack_cap_built;
+        s->S.stack_ring = RT_SHORT_STACK;
+        size_t spill_entries = (size_t)s->stack_cap_built;   // also room for a ring shrunk by rt_set_tuning
+        size_t spill_threads = (size_t)s->sms * RT_TRACE_MINB * RT_TRACE_BLOCK;
+        void* sp_buf = nullptr;
+        if (int rc = dalloc(s, &sp_buf, std::max<size_t>(spill_entries, 1) * spill_threads * sizeof(uint32_t)))
+            return bail(rc);
+        s->S.stack_spill = (uint32_t*)sp_buf;
         // SAH cost of the tree: Σ_inner area(node)/area(root) + Σ_leaf area(leaf)/area(root)
         s->ref_nodes = std::move(B.nodes);
         s->leaf_gids = std::move(B.leaves);
@@ -1006,6 +1049,7 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         if ((rc = upload(s, gquad.data(), gquad.size(), &s->S.quad))) return bail(rc);
         if ((rc = upload(s, gsph.data(), gsph.size(), &s->S.sphere))) return bail(rc);
         if ((rc = upload(s, lights.data(), lights.size(), &s->S.lights))) return bail(rc);
+        s->h_lights = lights;
         s->S.n_lights = d->n_lights;
         s->empty = false;
     }
@@ -1097,6 +1141,15 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         }
     }
     if ((rc = upload(s, mats.data(), mats.size(), &s->S.mats))) return bail(rc);
+    // the emission colour of every material, for photon emitters built from lights
+    s->h_emission.assign(mats.size() * 3, 0.0f);
+    for (size_t i = 0; i < (size_t)d->n_mats; i++) {
+        const DevMaterial& g = mats[i];
+        for (int c = 0; c < 3; c++)
+            s->h_emission[i * 3 + c] = g.type == RT_MAT_DIFFUSE_LIGHT ? g.albedo[c]
+                                     : g.type == RT_MAT_BLACKBODY_LIGHT ? g.bb_avg[c]
+                                     : g.type == RT_MAT_PBR ? g.emission[c] : 0.0f;
+    }
     s->S.n_pbr = n_pbr;
     s->S.n_mats = d->n_mats;
     std::vector<uint8_t> codes(mats.size(), 1);
@@ -1336,7 +1389,7 @@ extern "C" int32_t rt_trace_closest(RtScene* s, const float* rays, int64_t n, Rt
     if (!s || (n > 0 && (!rays || !hits))) return RT_ERR_INVALID;
     if (n <= 0) return RT_OK;
     if (n > (1ll << 31)) return fail(s, RT_ERR_CAPACITY, "more than 2^31 rays per call");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     bool media = s->S.n_media > 0;
     if (s->empty && !media) {
         if (mem == RT_MEM_DEVICE) { CK(cudaMemsetAsync(hits, 0xFF, n * sizeof(RtHit), s->stream)); return RT_OK; }
@@ -1384,7 +1437,7 @@ extern "C" int32_t rt_trace_any(RtScene* s, const float* rays, int64_t n, uint8_
     if (!s || (n > 0 && (!rays || !occ))) return RT_ERR_INVALID;
     if (n <= 0) return RT_OK;
     if (n > (1ll << 31)) return fail(s, RT_ERR_CAPACITY, "more than 2^31 rays per call");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     const float* drays = rays;
     uint8_t* dout = occ;
     size_t rb = (size_t)n * 8 * sizeof(float);
@@ -1406,7 +1459,7 @@ extern "C" int32_t rt_trace_transmittance(RtScene* s, const float* rays, int64_t
     if (!s || (n > 0 && (!rays || !tr))) return RT_ERR_INVALID;
     if (n <= 0) return RT_OK;
     if (n > (1ll << 31)) return fail(s, RT_ERR_CAPACITY, "more than 2^31 rays per call");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     size_t rb = (size_t)n * 8 * sizeof(float), ob = (size_t)n * sizeof(float);
     size_t off_out = (rb + 255) & ~(size_t)255, off_occ = (off_out + ob + 255) & ~(size_t)255;
     int rc = ensure_stage(s, off_occ + n + 256);
@@ -1547,6 +1600,7 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
     // every iteration with samples left advances `pool` path segments, and a
     // sample has at most maxd segments; the drain takes at most maxd more
     uint64_t max_it = total * maxd / pool + maxd + 2;
+    if (s->max_iterations) max_it = std::min<uint64_t>(max_it, s->max_iterations);
     bool done = false;
     uint64_t it = 0;
     for (; it < max_it && !done; it++) {
@@ -1608,7 +1662,8 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         // the bound was reached: the last iterations' counts must be zero
         for (uint32_t k = 0; k < std::min<uint64_t>(it, STATUS_LAG); k++)
             if (s->h_status[(uint32_t)((it - 1 - k) % STATUS_RING)] != 0)
-                return fail(s, RT_ERR_CAPACITY, "wavefront did not drain within its iteration bound");
+                return fail(s, RT_ERR_TIMEOUT, "wavefront did not drain within its iteration bound (" +
+                                                   std::to_string(max_it) + " iterations)");
     }
     if (ext_rays) *ext_rays += (int64_t)tot[HDR_EXT / 2];
     if (sh_rays) *sh_rays += (int64_t)tot[HDR_SHADOW / 2];
@@ -1699,7 +1754,7 @@ extern "C" int32_t rt_render_pass(RtScene* s, const RtCamera* cam, const RtPassP
     int rc = validate_pass(s, cam, p);
     if (rc) return rc;
     if (!scratch) return fail(s, RT_ERR_INVALID, "null scratch");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     size_t npix = (size_t)p->width * p->height;
     uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
     size_t bytes = (size_t)nsamp * npix * 3 * sizeof(float);
@@ -1733,7 +1788,7 @@ extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const R
                                         float* out_m2, uint32_t* out_count, int32_t mem) {
     int rc = validate_pass(s, cam, p);
     if (rc) return rc;
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     uint32_t npix = p->width * p->height;
     if (s->acc_npix != npix) {
         free_dev((void*&)s->acc); free_dev((void*&)s->m2); free_dev((void*&)s->cnt);
@@ -1806,7 +1861,7 @@ extern "C" int32_t rt_develop(RtScene* s, const float* lin, const RtDevelopParam
         return fail(s, RT_ERR_INVALID, "develop: vignette and distortion in [0, 1], a finite exposure");
     uint32_t npix = p->width * p->height;
     if (!lin && s->acc_npix != npix) return fail(s, RT_ERR_INVALID, "develop: no accumulators of this size");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     size_t in_bytes = lin && mem == RT_MEM_HOST ? (size_t)npix * 12 : 0;
     size_t out_bytes = mem == RT_MEM_HOST ? ((size_t)npix * 3 + 15) / 16 * 16 : 0;
     int rc = ensure_stage(s, in_bytes + out_bytes);
@@ -1874,11 +1929,25 @@ extern "C" int32_t rt_set_tuning(RtScene* s, const RtTuning* t) {
         return fail(s, RT_ERR_INVALID, "max_paths must be 0 or in 65536..8388608");
     if (t->trace_blocks_per_sm > RT_TRACE_BLOCKS_PER_SM || t->shade_blocks_per_sm > 32)
         return fail(s, RT_ERR_INVALID, "trace_blocks_per_sm must be in 0..8, shade_blocks_per_sm in 0..32");
-    CK(cudaSetDevice(s->device));
+    if (t->stack_ring != 0 && (t->stack_ring > RT_SHORT_STACK || (t->stack_ring & (t->stack_ring - 1)) != 0))
+        return fail(s, RT_ERR_INVALID, "stack_ring must be 0 or a power of two up to " + std::to_string(RT_SHORT_STACK));
+    if (t->stack_limit != 0 && (int64_t)t->stack_limit > s->stack_cap_built)
+        return fail(s, RT_ERR_INVALID, "stack_limit must be 0 or at most " + std::to_string(s->stack_cap_built) +
+                                           " (the entries the scene's stack columns hold)");
+    ENTER(s);
     CK(cudaStreamSynchronize(s->stream));
     s->max_paths = t->max_paths ? t->max_paths : MAX_PATHS;
     s->S.trace_per_sm = (int)t->trace_blocks_per_sm;
     s->S.shade_per_sm = (int)t->shade_blocks_per_sm;
+    s->max_iterations = t->max_iterations;
+    s->S.stack_cap = t->stack_limit ? (int)t->stack_limit : s->stack_cap_built;
+    s->S.stack_ring = t->stack_ring ? (int)t->stack_ring : RT_SHORT_STACK;
+    return RT_OK;
+}
+
+extern "C" int32_t rt_set_caller_stream(RtScene* s, void* stream) {
+    if (!s) return RT_ERR_INVALID;
+    s->caller = (cudaStream_t)stream;
     return RT_OK;
 }
 
@@ -1887,6 +1956,9 @@ extern "C" int32_t rt_get_tuning(const RtScene* s, RtTuning* t) {
     t->max_paths = s->max_paths;
     t->trace_blocks_per_sm = (uint32_t)s->S.trace_per_sm;
     t->shade_blocks_per_sm = (uint32_t)s->S.shade_per_sm;
+    t->max_iterations = (uint32_t)s->max_iterations;
+    t->stack_limit = (uint32_t)s->S.stack_cap;
+    t->stack_ring = (uint32_t)s->S.stack_ring;
     return RT_OK;
 }
 
@@ -1910,7 +1982,7 @@ extern "C" int32_t rt_capture_rays(RtScene* s, const RtCamera* cam, const RtPass
     int rc = validate_pass(s, cam, p);
     if (rc) return rc;
     if (!rays || max_rays < 0) return fail(s, RT_ERR_INVALID, "null ray buffer");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     RtPassParams q = *p;
     q.n_samples = 1;
     size_t bytes = (size_t)q.width * q.height * 3 * sizeof(float);
@@ -1989,7 +2061,7 @@ extern "C" int32_t rt_render_pass_noalloc(RtScene* s, const RtCamera* cam, const
                                             std::to_string(RT_NOALLOC_MAX_PIXELS) + " pixels");
     if (s->photons.present && s->photons.n > 0)
         return fail(s, RT_ERR_INVALID, "rt_render_pass_noalloc does not render scenes with a photon map");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     void* base = nullptr;
     if ((rc = noalloc_base(s, &base))) return rc;
     unsigned char* b = (unsigned char*)base;
@@ -2030,6 +2102,17 @@ extern "C" int32_t rt_render_pass_noalloc(RtScene* s, const RtCamera* cam, const
 static void emitter_setup(const RtScene* s, const RtPhotonEmitter& e0, float* f) {
     const float PI = 3.14159265358979323846f;
     RtPhotonEmitter e = e0;
+    if (e.type == RT_EMIT_LIGHT) {
+        // a quad of the light list, coloured by its material's emission; the quad
+        // record is (normal, d) (Q.xyz, u.x) (u.yz, v.xy) (v.z, w.xyz) (gid, mat, area, -)
+        const DevLight& L = s->h_lights[e.light];
+        const float4* g = L.g;
+        e.type = RT_EMIT_QUAD;
+        e.corner[0] = g[1].x; e.corner[1] = g[1].y; e.corner[2] = g[1].z;
+        e.u[0] = g[1].w; e.u[1] = g[2].x; e.u[2] = g[2].y;
+        e.v[0] = g[2].z; e.v[1] = g[2].w; e.v[2] = g[3].x;
+        for (int c = 0; c < 3; c++) e.color[c] = s->h_emission[(size_t)L.mat * 3 + c];
+    }
     if (e.type == RT_EMIT_SUN) {
         // rebuild_caustics with a Physical sky (scene.rs:40-52): a disk facing the
         // sun, coloured by the sky radiance 0.04 off the sun direction, ×π
@@ -2077,6 +2160,8 @@ static void emitter_setup(const RtScene* s, const RtPhotonEmitter& e0, float* f)
         put(24, ta); put(27, ba);
         put(30, h3(e.color[0], e.color[1], e.color[2]) * (area * PI / (float)e.n_photons));
         f[34] = 15.0f;
+        put(35, h3(e.target[0], e.target[1], e.target[2]));
+        f[38] = e.target[3] > 0.0f ? e.target[3] : 0.0f;
     }
 }
 
@@ -2089,23 +2174,36 @@ extern "C" int32_t rt_photon_build(RtScene* s, const RtPhotonParams* p, int64_t*
     uint64_t total = 0;
     for (int i = 0; i < p->n_emitters; i++) {
         const RtPhotonEmitter& e = p->emitters[i];
-        if (e.type != RT_EMIT_DISK && e.type != RT_EMIT_QUAD && e.type != RT_EMIT_SUN)
+        if (e.type != RT_EMIT_DISK && e.type != RT_EMIT_QUAD && e.type != RT_EMIT_SUN && e.type != RT_EMIT_LIGHT)
             return fail(s, RT_ERR_INVALID, "unknown emitter type");
         if (e.type == RT_EMIT_SUN && s->S.bg_type != RT_BG_PHYSICAL)
             return fail(s, RT_ERR_INVALID, "a sun emitter needs a Physical sky background");
+        if (e.type == RT_EMIT_LIGHT &&
+            (e.light < 0 || e.light >= (int32_t)s->h_lights.size() || s->h_lights[e.light].type != RT_PRIM_QUAD))
+            return fail(s, RT_ERR_INVALID, "a light emitter must name a quad of the light list");
         if (e.n_photons == 0) return fail(s, RT_ERR_INVALID, "emitter with zero photons");
         total += e.n_photons;
     }
-    if (total > MAX_PATHS) return fail(s, RT_ERR_CAPACITY, "more than 8M photons per build");
-    CK(cudaSetDevice(s->device));
-    int rc = ensure_paths(s, (uint32_t)std::max<uint64_t>(total, s->cap));
+    if (total > 0xFFFFFFFFull) return fail(s, RT_ERR_CAPACITY, "more than 2^32 - 1 photons");
+    uint64_t first = p->first_photon, count = p->shard_photons ? p->shard_photons : total;
+    if (first + count > total) return fail(s, RT_ERR_INVALID, "photon shard beyond the emitters' photons");
+    if (count > MAX_PATHS) return fail(s, RT_ERR_CAPACITY, "more than 8M photons traced per build");
+    ENTER(s);
+    int rc = ensure_paths(s, (uint32_t)std::max<uint64_t>(count, s->cap));
     if (rc) return rc;
     std::vector<float> setup((size_t)p->n_emitters * 40);
     for (int i = 0; i < p->n_emitters; i++) emitter_setup(s, p->emitters[i], &setup[(size_t)i * 40]);
     cudaError_t e = rth::photon_build(s->S, s->photons, s->P, s->queue[0], s->queue[1], s->counters, *p, setup.data(),
-                                      s->sms, s->stream, n_stored);
+                                      (uint32_t)first, (uint32_t)count, s->sms, s->stream, n_stored,
+                                      s->photon_stage_ms);
     if (e != cudaSuccess) return fail(s, RT_ERR_CUDA, std::string("photon build: ") + cudaGetErrorString(e));
     return check_err(s);
+}
+
+extern "C" int32_t rt_photon_build_times(const RtScene* s, float* ms) {
+    if (!s || !ms) return RT_ERR_INVALID;
+    for (int k = 0; k < 3; k++) ms[k] = s->photon_stage_ms[k];
+    return RT_OK;
 }
 
 extern "C" int32_t rt_photon_set(RtScene* s, const float* pos, const float* power, const float* nor,
@@ -2113,7 +2211,7 @@ extern "C" int32_t rt_photon_set(RtScene* s, const float* pos, const float* powe
     if (!s || n < 0 || (n > 0 && (!pos || !power || !nor))) return RT_ERR_INVALID;
     if (!(radius > 0.0f)) return fail(s, RT_ERR_INVALID, "gather radius must be positive");
     if (n > (int64_t)MAX_PATHS) return fail(s, RT_ERR_CAPACITY, "more than 8M photons");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     std::vector<float4> a(n), b(n), c(n);
     for (int64_t i = 0; i < n; i++) {
         int32_t id = index ? index[i] : (int32_t)i;
@@ -2158,7 +2256,7 @@ extern "C" int32_t rt_photon_export(const RtScene* s, float* pos, float* power, 
 extern "C" int32_t rt_photon_gather(RtScene* s, const float* q, int64_t n, float* irr, int32_t mem) {
     if (!s || n < 0 || (n > 0 && (!q || !irr))) return RT_ERR_INVALID;
     if (n == 0) return RT_OK;
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     if (!s->photons.present || s->photons.n == 0) {
         if (mem == RT_MEM_DEVICE) { CK(cudaMemsetAsync(irr, 0, n * 12, s->stream)); return RT_OK; }
         memset(irr, 0, n * 12);
@@ -2185,7 +2283,7 @@ extern "C" int32_t rt_knn(RtScene* s, const float* q, int64_t n, int32_t k, floa
     if (!s || n < 0 || k <= 0 || (n > 0 && (!q || !idx || !d2))) return RT_ERR_INVALID;
     if (k > 256) return fail(s, RT_ERR_INVALID, "k must be ≤ 256");
     if (n == 0) return RT_OK;
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     if (!s->photons.present || s->photons.n == 0) {
         std::vector<int32_t> mi((size_t)n * k, -1);
         std::vector<float> md((size_t)n * k, INFINITY);
@@ -2248,7 +2346,7 @@ int guide_api(RtScene* s, const float* q, const float* dirs, const float* u, int
     if (rc) return rc;
     if (n < 0 || n > (1ll << 28) || (n > 0 && !q)) return fail(s, RT_ERR_INVALID, "guide query count or pointer");
     if (n == 0) return RT_OK;
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     Tmp tq, td, tu, tr, to;
     const void *dq = nullptr, *dd = nullptr, *du = nullptr;
     void *dr = nullptr, *dout = nullptr;
@@ -2300,7 +2398,7 @@ extern "C" int32_t rt_guide_init(RtScene* s, const RtGuideParams* p) {
     for (int a = 0; a < 3; a++)
         if (!std::isfinite(p->domain_min[a]) || !std::isfinite(p->domain_max[a]) || p->domain_max[a] < p->domain_min[a])
             return fail(s, RT_ERR_INVALID, "guide domain");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     CK(cudaStreamSynchronize(s->stream));
     rtgh::destroy(s->guide);
     s->guide = nullptr;
@@ -2322,7 +2420,7 @@ extern "C" int32_t rt_guide_params(RtScene* s, float* params, int32_t write) {
     int rc = guide_ready(s);
     if (rc) return rc;
     if (!params) return fail(s, RT_ERR_INVALID, "null parameter buffer");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     CK(cudaStreamSynchronize(s->stream));
     CK(rtgh::params_io(s->guide, params, write, s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -2348,7 +2446,7 @@ extern "C" int32_t rt_guide_loss_grad(RtScene* s, const float* samples, int64_t 
     int rc = guide_ready(s);
     if (rc) return rc;
     if (n <= 0 || n > (1ll << 22) || !samples) return fail(s, RT_ERR_INVALID, "guide samples: 1..2^22 rows");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     Tmp t;
     const float4* d = nullptr;
     if ((rc = stage_samples(s, samples, n, t, &d))) return rc;
@@ -2362,7 +2460,7 @@ extern "C" int32_t rt_guide_train(RtScene* s, const float* samples, int64_t n, i
     if (rc) return rc;
     if (n <= 0 || n > (1ll << 22) || !samples) return fail(s, RT_ERR_INVALID, "guide samples: 1..2^22 rows");
     if (steps < 1) return fail(s, RT_ERR_INVALID, "steps must be at least 1");
-    CK(cudaSetDevice(s->device));
+    ENTER(s);
     Tmp t;
     const float4* d = nullptr;
     if ((rc = stage_samples(s, samples, n, t, &d))) return rc;

@@ -10,6 +10,18 @@
 
 #define RT_TRACE_BLOCK 128
 #define RT_TRACE_BLOCKS_PER_SM 8
+// resident blocks per SM of the persistent traversal kernels (their launch
+// bound and the most blocks per SM a traversal grid has): 6 blocks of 128
+// threads cap the kernels at 80 registers (measured faster than 5 blocks at
+// 96 registers and than 8 blocks at 64)
+#ifndef RT_TRACE_MINB
+#define RT_TRACE_MINB 6
+#endif
+// traversal stack: RT_SHORT_STACK entries per thread in shared memory (a
+// ring), deeper entries spilled to a per-thread column of global memory
+// sized from the tree depth at scene creation (7 per level: a visit pushes
+// at most 7 of its 8 children), so a traversal never runs out of stack
+#define RT_SHORT_STACK 16
 #define RT_SHADE_BLOCK 128
 #define RT_SHADE_BLOCKS_PER_SM 8
 #define RT_MAX_DEPTH 256
@@ -81,15 +93,27 @@ struct PendTargets {
 
 namespace rtph { struct Map; }
 
-// Device photon map: Morton-ordered photons, box heap, and an emission-order copy.
+// Device photon map: Morton-ordered photons, box heap, and an emission-order
+// copy.  Its arrays and the build's work buffers grow on demand and are kept
+// across builds, so a rebuild of a map no larger than before allocates and
+// frees nothing (release() only drops the map).
 struct PhotonMapDev {
     float4 *pos = nullptr, *pow = nullptr, *nor = nullptr, *blo = nullptr, *bhi = nullptr;
     float4 *exp_pos = nullptr, *exp_pow = nullptr, *exp_nor = nullptr;
     uint32_t n = 0, nleaf_pow2 = 1, knn_k = 0;
     float r2 = 0.0f;
     bool present = false;
+    // capacities (elements) of the map arrays, the heap and the build's work buffers
+    size_t cap_map = 0, cap_heap = 0, cap_work = 0, cap_tmp = 0;
+    uint8_t* flags = nullptr;                                 // stored flag per traced photon
+    float4 *st_pos = nullptr, *st_pow = nullptr, *st_nor = nullptr;   // stored record per traced photon
+    uint32_t *fl32 = nullptr, *scan = nullptr;                // compaction
+    uint32_t *key = nullptr, *val = nullptr, *key2 = nullptr, *val2 = nullptr;   // Morton sort
+    float* bounds = nullptr;
+    void* tmp = nullptr;                                      // CUB temporary storage
     ~PhotonMapDev();
     void release();
+    void free_all();
     rtph::Map view() const;
 };
 
@@ -147,9 +171,11 @@ void launch_active_list(const uint8_t* conv, uint32_t width, uint32_t height, ui
                         cudaStream_t st);
 void launch_zero_converged(const uint8_t* conv, uint32_t npix, uint32_t nsamp, float* scratch, cudaStream_t st);
 
+// traces photons first .. first + count − 1 of the emission order (the emitters'
+// photons one after the other) and builds the map of those stored
 cudaError_t photon_build(const rtd::DevScene& S, PhotonMapDev& map, const PathState& P, uint32_t* qa, uint32_t* qb,
-                         uint32_t* counters, const RtPhotonParams& prm, const float* emit_setup, int sms,
-                         cudaStream_t st, int64_t* n_stored);
+                         uint32_t* counters, const RtPhotonParams& prm, const float* emit_setup, uint32_t first,
+                         uint32_t count, int sms, cudaStream_t st, int64_t* n_stored, float stage_ms[3]);
 cudaError_t photon_set(PhotonMapDev& map, const float4* pos, const float4* pow, const float4* nor, uint32_t n,
                        float radius, uint32_t k, cudaStream_t st);
 void launch_photon_gather_api(const PhotonMapDev& map, const float* q, uint32_t n, float* out, int sms, cudaStream_t st);

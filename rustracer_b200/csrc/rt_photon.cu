@@ -44,6 +44,8 @@ struct EmitSetup {
     float3 t, b, center, dir, normal, corner, u, v, ta, ba, power;
     float radius, lum_clamp;
     uint32_t first, count;
+    float3 target;       // projection sphere of a quad source (target_r 0: the whole hemisphere)
+    float target_r;
 };
 struct EmitSet { EmitSetup e[RT_MAX_EMITTERS]; int n; float lam_lo, lam_range; uint64_t seed; };
 
@@ -56,14 +58,18 @@ RT_D Rng photon_rng(uint64_t seed, uint32_t gid) {
 }
 enum { P_EMIT0 = 0, P_EMIT1 = 1, P_EMIT2 = 2, P_EMIT3 = 3, P_LAMBDA = 4, P_BOUNCE0 = 8, P_PER_BOUNCE = 4 };
 
-__global__ void k_photon_emit(PathState P, EmitSet E, uint32_t total, uint32_t* queue0, uint32_t* count0,
-                              uint8_t* flags) {
-    for (uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x; gid < total; gid += gridDim.x * blockDim.x) {
+// Photon slot i traces emission index first + i (its random stream and the
+// index stored with it); the emitter is the one whose range holds that index.
+__global__ void k_photon_emit(PathState P, EmitSet E, uint32_t first, uint32_t total, uint32_t* queue0,
+                              uint32_t* count0, uint8_t* flags) {
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < total; slot += gridDim.x * blockDim.x) {
+        uint32_t gid = first + slot;
         int ei = 0;
         for (int k = 1; k < E.n; k++) if (gid >= E.e[k].first) ei = k;
         const EmitSetup& em = E.e[ei];
         Rng rng = photon_rng(E.seed, gid);
         float3 o, d;
+        float wgt = 1.0f;
         if (em.type == RT_EMIT_DISK) {
             float r = em.radius * sqrtf(rnd(rng, P_EMIT0));
             float sp, cp;
@@ -73,20 +79,38 @@ __global__ void k_photon_emit(PathState P, EmitSet E, uint32_t total, uint32_t* 
         } else {
             float ss = rnd(rng, P_EMIT0), tt = rnd(rng, P_EMIT1);
             o = em.corner + em.u * ss + em.v * tt;
-            float ct = sqrtf(rnd(rng, P_EMIT2));
-            float st = sqrtf(1.0f - ct * ct);
-            float sp, cp;
-            sincosf(2.0f * PI_F * rnd(rng, P_EMIT3), &sp, &cp);
-            d = st * cp * em.ta + st * sp * em.ba + ct * em.normal;
+            float3 tc = em.target - o;
+            float d2 = len2(tc), rr = em.target_r * em.target_r;
+            if (em.target_r > 0.0f && d2 > rr) {
+                // projection map: uniform in the cone toward the target sphere,
+                // power × cosine density / cone density (0: below the light's plane)
+                float ctm = sqrtf(1.0f - rr / d2);
+                float sp, cp;
+                sincosf(2.0f * PI_F * rnd(rng, P_EMIT3), &sp, &cp);
+                float ct = 1.0f - rnd(rng, P_EMIT2) * (1.0f - ctm);
+                float st = sqrtf(fmaxf(1.0f - ct * ct, 0.0f));
+                d = onb_local_w(unit3(tc), mk(cp * st, sp * st, ct));
+                float cl = dot3(d, em.normal);
+                wgt = cl > 0.0f ? 2.0f * cl * (1.0f - ctm) : 0.0f;
+            } else {
+                float ct = sqrtf(rnd(rng, P_EMIT2));
+                float st = sqrtf(1.0f - ct * ct);
+                float sp, cp;
+                sincosf(2.0f * PI_F * rnd(rng, P_EMIT3), &sp, &cp);
+                d = st * cp * em.ta + st * sp * em.ba + ct * em.normal;
+            }
         }
+        // a photon with no power is not traced: a NaN origin makes the
+        // traversal report a miss, which ends it
+        if (!(wgt > 0.0f)) o = mk(__int_as_float(0x7fc00000), 0.0f, 0.0f);
         float lam = E.lam_lo + E.lam_range * rnd(rng, P_LAMBDA);
         if (lam >= E.lam_lo + E.lam_range) lam = nextafterf(E.lam_lo + E.lam_range, 0.0f);
-        P.ray_o[gid] = make_float4(o.x, o.y, o.z, em.lum_clamp);
-        P.ray_d[gid] = make_float4(d.x, d.y, d.z, lam);
-        P.thr[gid] = make_float4(em.power.x, em.power.y, em.power.z, 0.0f);
-        P.meta[gid] = make_uint4(gid, 0u, 0u, 0u);
-        flags[gid] = 0;
-        queue0[gid] = gid;
+        P.ray_o[slot] = make_float4(o.x, o.y, o.z, em.lum_clamp);
+        P.ray_d[slot] = make_float4(d.x, d.y, d.z, lam);
+        P.thr[slot] = make_float4(em.power.x * wgt, em.power.y * wgt, em.power.z * wgt, 0.0f);
+        P.meta[slot] = make_uint4(gid, 0u, 0u, 0u);
+        flags[slot] = 0;
+        queue0[slot] = slot;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *count0 = total;
 }
@@ -133,22 +157,23 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
     for (uint32_t qi0 = blockIdx.x * blockDim.x; qi0 < n; qi0 += gridDim.x * blockDim.x) {
         uint32_t qi = qi0 + threadIdx.x;
         bool cont = false;
-        uint32_t gid = 0;
+        uint32_t slot = 0;
         if (qi < n) {
-            gid = qin[qi];
-            float4 hv = P.hit[gid], ro = P.ray_o[gid], rdv = P.ray_d[gid], th = P.thr[gid];
+            slot = qin[qi];
+            const uint32_t eidx = P.meta[slot].x;      // emission index: the photon's random stream
+            float4 hv = P.hit[slot], ro = P.ray_o[slot], rdv = P.ray_d[slot], th = P.thr[slot];
             uint32_t ref = __float_as_uint(hv.x);
             if (hit_is_medium(ref)) {
                 // a medium scatter is a skip_pdf bounce of the caustic path (photon.rs:252-260)
                 float3 o = mk(ro.x, ro.y, ro.z), d = mk(rdv.x, rdv.y, rdv.z);
                 const DevMedium& M = S.media[RT_HIT_INDEX(ref)];
-                Rng rng = photon_rng(seed, gid);
+                Rng rng = photon_rng(seed, eidx);
                 uint32_t base = P_BOUNCE0 + bounce * P_PER_BOUNCE;
                 float3 p = ray_at(o, d, hv.y);
                 float3 nd = hg_sample(unit3(d), M.g, rnd(rng, base + 0), rnd(rng, base + 1));
-                P.ray_o[gid] = make_float4(p.x, p.y, p.z, ro.w);
-                P.ray_d[gid] = make_float4(nd.x, nd.y, nd.z, rdv.w);
-                P.thr[gid] = make_float4(th.x * M.color.x, th.y * M.color.y, th.z * M.color.z,
+                P.ray_o[slot] = make_float4(p.x, p.y, p.z, ro.w);
+                P.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, rdv.w);
+                P.thr[slot] = make_float4(th.x * M.color.x, th.y * M.color.y, th.z * M.color.z,
                                          __uint_as_float(__float_as_uint(th.w) + 1u));
                 cont = true;
             } else if (ref != RT_MISS_REF) {
@@ -208,7 +233,7 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                 }
                 const DevMaterial& m = S.mats[mat];
                 bool store = false;
-                Rng rng = photon_rng(seed, gid);
+                Rng rng = photon_rng(seed, eidx);
                 uint32_t base = P_BOUNCE0 + bounce * P_PER_BOUNCE;
                 float3 udir = unit3(d);
                 if (m.type == RT_MAT_DIELECTRIC || m.type == RT_MAT_SPECTRAL_DIELECTRIC) {
@@ -290,16 +315,16 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
                     if (spec_depth > 0) {
                         float lum = lum3(power);
                         if (lum > lum_clamp) power = power * (lum_clamp / lum);
-                        st_pos[gid] = make_float4(p.x, p.y, p.z, __uint_as_float(gid));
-                        st_pow[gid] = make_float4(power.x, power.y, power.z, 0.f);
-                        st_nor[gid] = make_float4(nrm.x, nrm.y, nrm.z, 0.f);
-                        flags[gid] = 1;
+                        st_pos[slot] = make_float4(p.x, p.y, p.z, __uint_as_float(eidx));
+                        st_pow[slot] = make_float4(power.x, power.y, power.z, 0.f);
+                        st_nor[slot] = make_float4(nrm.x, nrm.y, nrm.z, 0.f);
+                        flags[slot] = 1;
                     }
                 }
                 if (cont) {
-                    P.ray_o[gid] = make_float4(o.x, o.y, o.z, lum_clamp);
-                    P.ray_d[gid] = make_float4(d.x, d.y, d.z, lam);
-                    P.thr[gid] = make_float4(power.x, power.y, power.z, __uint_as_float(spec_depth));
+                    P.ray_o[slot] = make_float4(o.x, o.y, o.z, lum_clamp);
+                    P.ray_d[slot] = make_float4(d.x, d.y, d.z, lam);
+                    P.thr[slot] = make_float4(power.x, power.y, power.z, __uint_as_float(spec_depth));
                 }
             }
         }
@@ -310,7 +335,7 @@ __global__ void k_photon_shade(DevScene S, PathState P, uint32_t bounce, const u
             uint32_t b = 0;
             if ((int)lane == leader) b = atomicAdd(cout, __popc(m));
             b = __shfl_sync(__activemask(), b, leader);
-            if (cont) qout[b + __popc(m & ((1u << lane) - 1u))] = gid;
+            if (cont) qout[b + __popc(m & ((1u << lane) - 1u))] = slot;
         }
     }
 }
@@ -746,13 +771,22 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Ma
 }
 
 // ── host side ───────────────────────────────────────────────────────────────
-PhotonMapDev::~PhotonMapDev() { release(); }
+PhotonMapDev::~PhotonMapDev() { free_all(); }
 void PhotonMapDev::release() {
-    void* ps[] = {pos, pow, nor, blo, bhi, exp_pos, exp_pow, exp_nor};
-    for (void* p : ps) if (p) cudaFree(p);
-    pos = pow = nor = blo = bhi = exp_pos = exp_pow = exp_nor = nullptr;
     n = 0;
     present = false;
+}
+void PhotonMapDev::free_all() {
+    void* ps[] = {pos, pow, nor, blo, bhi, exp_pos, exp_pow, exp_nor, flags, st_pos, st_pow, st_nor,
+                  fl32, scan, key, val, key2, val2, bounds, tmp};
+    for (void* p : ps) if (p) cudaFree(p);
+    pos = pow = nor = blo = bhi = exp_pos = exp_pow = exp_nor = st_pos = st_pow = st_nor = nullptr;
+    flags = nullptr;
+    fl32 = scan = key = val = key2 = val2 = nullptr;
+    bounds = nullptr;
+    tmp = nullptr;
+    cap_map = cap_heap = cap_work = cap_tmp = 0;
+    release();
 }
 
 rtph::Map PhotonMapDev::view() const {
@@ -765,134 +799,163 @@ rtph::Map PhotonMapDev::view() const {
 
 namespace rth {
 
-static cudaError_t build_tree(PhotonMapDev& map, const float4* cp, const float4* cw, const float4* cn, uint32_t n,
-                              cudaStream_t st) {
+// grow a device array to at least `n` elements of `bytes` (contents not kept)
+template <class T>
+static cudaError_t grow(T*& p, size_t n, size_t bytes) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    return cudaMalloc((void**)&p, std::max<size_t>(n, 1) * bytes);
+}
+
+// map arrays (emission-order copy, Morton-ordered copy, sort keys) for n photons
+static cudaError_t ensure_map(PhotonMapDev& map, size_t n) {
+    if (n <= map.cap_map && map.pos) return cudaSuccess;
+    size_t c = std::max<size_t>(n, map.cap_map * 5 / 4);
+    cudaError_t e;
+    float4** f4[] = {&map.pos, &map.pow, &map.nor, &map.exp_pos, &map.exp_pow, &map.exp_nor};
+    for (float4** q : f4) if ((e = grow(*q, c, sizeof(float4)))) return e;
+    uint32_t** u4[] = {&map.key, &map.val, &map.key2, &map.val2};
+    for (uint32_t** q : u4) if ((e = grow(*q, c, sizeof(uint32_t)))) return e;
+    if (!map.bounds && (e = grow(map.bounds, 6, sizeof(float)))) return e;
+    map.cap_map = c;
+    return cudaSuccess;
+}
+
+static cudaError_t ensure_tmp(PhotonMapDev& map, size_t bytes) {
+    if (bytes <= map.cap_tmp && map.tmp) return cudaSuccess;
+    size_t c = std::max<size_t>(bytes, map.cap_tmp * 5 / 4);
+    cudaError_t e = grow(map.tmp, c, 1);
+    if (!e) map.cap_tmp = c;
+    return e;
+}
+
+// Morton sort of the emission-order photons (exp_*, n of them) into pos/pow/nor,
+// then the box heap over PH_LEAF-photon leaves
+static cudaError_t build_tree(PhotonMapDev& map, uint32_t n, cudaStream_t st) {
     // Morton sort (stable radix sort keeps emission order among equal codes)
     cudaError_t e;
-    float* bounds;
-    if ((e = cudaMalloc(&bounds, 6 * sizeof(float)))) return e;
     float init[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
-    cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st);
-    k_bounds<<<std::min<uint32_t>((n + 255) / 256, 2048), 256, 0, st>>>(cp, n, bounds, bounds + 3);
-    uint32_t *key, *val, *key2, *val2;
-    cudaMalloc(&key, (size_t)n * 4); cudaMalloc(&val, (size_t)n * 4);
-    cudaMalloc(&key2, (size_t)n * 4); cudaMalloc(&val2, (size_t)n * 4);
-    k_morton<<<std::min<uint32_t>((n + 255) / 256, 4096), 256, 0, st>>>(cp, n, bounds, bounds + 3, key, val);
+    if ((e = cudaMemcpyAsync(map.bounds, init, sizeof(init), cudaMemcpyHostToDevice, st))) return e;
+    k_bounds<<<std::min<uint32_t>((n + 255) / 256, 2048), 256, 0, st>>>(map.exp_pos, n, map.bounds, map.bounds + 3);
+    k_morton<<<std::min<uint32_t>((n + 255) / 256, 4096), 256, 0, st>>>(map.exp_pos, n, map.bounds, map.bounds + 3,
+                                                                        map.key, map.val);
     size_t tb = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb, key, key2, val, val2, (int)n, 0, 30, st);
-    void* tmp;
-    cudaMalloc(&tmp, std::max<size_t>(tb, 16));
-    cub::DeviceRadixSort::SortPairs(tmp, tb, key, key2, val, val2, (int)n, 0, 30, st);
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, map.key, map.key2, map.val, map.val2, (int)n, 0, 30, st);
+    if ((e = ensure_tmp(map, tb))) return e;
+    cub::DeviceRadixSort::SortPairs(map.tmp, tb, map.key, map.key2, map.val, map.val2, (int)n, 0, 30, st);
     uint32_t nleaf = (n + PH_LEAF - 1) / PH_LEAF, p2 = 1;
     while (p2 < nleaf) p2 <<= 1;
     map.nleaf_pow2 = p2;
-    cudaMalloc(&map.pos, (size_t)std::max(n, 1u) * 16);
-    cudaMalloc(&map.pow, (size_t)std::max(n, 1u) * 16);
-    cudaMalloc(&map.nor, (size_t)std::max(n, 1u) * 16);
-    cudaMalloc(&map.blo, (size_t)(2 * p2 - 1) * 16);
-    cudaMalloc(&map.bhi, (size_t)(2 * p2 - 1) * 16);
-    k_gather_sorted<<<std::min<uint32_t>((n + 255) / 256, 4096), 256, 0, st>>>(val2, n, cp, cw, cn, map.pos, map.pow,
-                                                                               map.nor);
+    if ((size_t)(2 * p2 - 1) > map.cap_heap || !map.blo) {
+        size_t c = 2 * (size_t)p2 - 1;
+        if ((e = grow(map.blo, c, sizeof(float4))) || (e = grow(map.bhi, c, sizeof(float4)))) return e;
+        map.cap_heap = c;
+    }
+    k_gather_sorted<<<std::min<uint32_t>((n + 255) / 256, 4096), 256, 0, st>>>(map.val2, n, map.exp_pos, map.exp_pow,
+                                                                               map.exp_nor, map.pos, map.pow, map.nor);
     k_leaf_boxes<<<std::min<uint32_t>((p2 + 255) / 256, 4096), 256, 0, st>>>(map.pos, n, p2, map.blo, map.bhi);
     for (uint32_t cnt = p2 / 2; cnt >= 1; cnt /= 2)
         k_level_boxes<<<std::min<uint32_t>((cnt + 255) / 256, 4096), 256, 0, st>>>(cnt - 1, cnt, map.blo, map.bhi);
-    e = cudaStreamSynchronize(st);
-    cudaFree(bounds); cudaFree(key); cudaFree(val); cudaFree(key2); cudaFree(val2); cudaFree(tmp);
-    return e ? e : cudaGetLastError();
+    return cudaGetLastError();
 }
 
 cudaError_t photon_build(const DevScene& S, PhotonMapDev& map, const PathState& P, uint32_t* qa, uint32_t* qb,
-                         uint32_t* counters, const RtPhotonParams& prm, const float* emit_setup, int sms,
-                         cudaStream_t st, int64_t* n_stored) {
+                         uint32_t* counters, const RtPhotonParams& prm, const float* emit_setup, uint32_t first,
+                         uint32_t count, int sms, cudaStream_t st, int64_t* n_stored, float stage_ms[3]) {
     map.release();
     EmitSet E{};
     E.n = prm.n_emitters;
     E.lam_lo = S.lam_lo;
     E.lam_range = S.lam_range;
     E.seed = prm.seed;
-    uint32_t total = 0;
+    uint32_t off = 0;
     for (int i = 0; i < prm.n_emitters; i++) {
         const float* f = emit_setup + i * 40;
         EmitSetup& x = E.e[i];
-        x.type = prm.emitters[i].type == RT_EMIT_QUAD ? RT_EMIT_QUAD : RT_EMIT_DISK;   // the sun is a disk source
+        int ty = prm.emitters[i].type;
+        x.type = (ty == RT_EMIT_QUAD || ty == RT_EMIT_LIGHT) ? RT_EMIT_QUAD : RT_EMIT_DISK;   // the sun is a disk source
         x.t = mk(f[0], f[1], f[2]); x.b = mk(f[3], f[4], f[5]); x.center = mk(f[6], f[7], f[8]);
         x.dir = mk(f[9], f[10], f[11]); x.normal = mk(f[12], f[13], f[14]); x.corner = mk(f[15], f[16], f[17]);
         x.u = mk(f[18], f[19], f[20]); x.v = mk(f[21], f[22], f[23]); x.ta = mk(f[24], f[25], f[26]);
         x.ba = mk(f[27], f[28], f[29]); x.power = mk(f[30], f[31], f[32]);
         x.radius = f[33]; x.lum_clamp = f[34];
-        x.first = total; x.count = prm.emitters[i].n_photons;
-        total += x.count;
+        x.target = mk(f[35], f[36], f[37]); x.target_r = f[38];
+        x.first = off; x.count = prm.emitters[i].n_photons;
+        off += x.count;
     }
+    const uint32_t total = count;          // photons traced by this build (slots 0 .. total − 1)
     cudaError_t e;
-    uint8_t* flags;
-    float4 *sp, *sw, *sn;
-    if ((e = cudaMalloc(&flags, std::max(total, 1u)))) return e;
-    cudaMalloc(&sp, (size_t)std::max(total, 1u) * 16);
-    cudaMalloc(&sw, (size_t)std::max(total, 1u) * 16);
-    cudaMalloc(&sn, (size_t)std::max(total, 1u) * 16);
+    if (total > map.cap_work || !map.flags) {
+        size_t c = std::max<size_t>(total, map.cap_work * 5 / 4);
+        if ((e = grow(map.flags, c, 1)) || (e = grow(map.st_pos, c, sizeof(float4))) ||
+            (e = grow(map.st_pow, c, sizeof(float4))) || (e = grow(map.st_nor, c, sizeof(float4))) ||
+            (e = grow(map.fl32, c, sizeof(uint32_t))) || (e = grow(map.scan, c, sizeof(uint32_t))))
+            return e;
+        map.cap_work = c;
+    }
+    cudaEvent_t ev[4];
+    for (auto& x : ev) cudaEventCreate(&x);
+    cudaEventRecord(ev[0], st);
     cudaMemsetAsync(counters, 0, sizeof(uint32_t) * 14 * RT_CTR_STRIDE, st);
     int grid = std::min<uint32_t>((total + 255) / 256, 148u * 16u);
-    k_photon_emit<<<std::max(grid, 1), 256, 0, st>>>(P, E, total, qa, counters, flags);
+    k_photon_emit<<<std::max(grid, 1), 256, 0, st>>>(P, E, first, total, qa, counters, map.flags);
     uint32_t* q[2] = {qa, qb};
     for (uint32_t b = 0; b < 12; b++) {
         uint32_t* c = counters + b * RT_CTR_STRIDE;
         uint32_t* cn = counters + (b + 1) * RT_CTR_STRIDE;
         launch_extend(S, P, q[b & 1], c + CTR_COUNT, c + CTR_EXTEND_NEXT, (int*)(counters + 13 * RT_CTR_STRIDE), sms, st);
         if (S.n_media > 0) launch_media(S, P, q[b & 1], c + CTR_COUNT, sms, st);
-        k_photon_shade<<<sms * 8, 128, 0, st>>>(S, P, b, q[b & 1], c + CTR_COUNT, q[(b + 1) & 1], cn + CTR_COUNT, sp, sw,
-                                                sn, flags, prm.seed);
+        k_photon_shade<<<sms * 8, 128, 0, st>>>(S, P, b, q[b & 1], c + CTR_COUNT, q[(b + 1) & 1], cn + CTR_COUNT,
+                                                map.st_pos, map.st_pow, map.st_nor, map.flags, prm.seed);
     }
+    cudaEventRecord(ev[1], st);
     // compact in emission order
-    uint32_t *fl32, *scan;
-    cudaMalloc(&fl32, (size_t)std::max(total, 1u) * 4);
-    cudaMalloc(&scan, (size_t)std::max(total, 1u) * 4);
-    k_flags_to_u32<<<std::max(grid, 1), 256, 0, st>>>(flags, fl32, total);
+    k_flags_to_u32<<<std::max(grid, 1), 256, 0, st>>>(map.flags, map.fl32, total);
     size_t tb = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, tb, fl32, scan, (int)total, st);
-    void* tmp;
-    cudaMalloc(&tmp, std::max<size_t>(tb, 16));
-    cub::DeviceScan::ExclusiveSum(tmp, tb, fl32, scan, (int)total, st);
-    uint32_t last_scan = 0, last_flag = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, map.fl32, map.scan, (int)total, st);
+    if ((e = ensure_tmp(map, tb))) return e;
+    cub::DeviceScan::ExclusiveSum(map.tmp, tb, map.fl32, map.scan, (int)total, st);
+    uint32_t last[2] = {0, 0};
     if (total) {
-        cudaMemcpyAsync(&last_scan, scan + total - 1, 4, cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(&last_flag, fl32 + total - 1, 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&last[0], map.scan + total - 1, 4, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(&last[1], map.fl32 + total - 1, 4, cudaMemcpyDeviceToHost, st);
     }
     if ((e = cudaStreamSynchronize(st))) return e;
-    uint32_t n = total ? last_scan + last_flag : 0;
-    float4 *cp, *cw, *cn;
-    cudaMalloc(&cp, (size_t)std::max(n, 1u) * 16);
-    cudaMalloc(&cw, (size_t)std::max(n, 1u) * 16);
-    cudaMalloc(&cn, (size_t)std::max(n, 1u) * 16);
-    k_compact<<<std::max(grid, 1), 256, 0, st>>>(flags, scan, total, sp, sw, sn, cp, cw, cn);
-    e = cudaStreamSynchronize(st);
-    cudaFree(flags); cudaFree(sp); cudaFree(sw); cudaFree(sn); cudaFree(fl32); cudaFree(scan); cudaFree(tmp);
-    if (e) return e;
-    map.exp_pos = cp; map.exp_pow = cw; map.exp_nor = cn;   // emission-order copy for export
+    uint32_t n = total ? last[0] + last[1] : 0;
+    if ((e = ensure_map(map, n))) return e;
+    k_compact<<<std::max(grid, 1), 256, 0, st>>>(map.flags, map.scan, total, map.st_pos, map.st_pow, map.st_nor,
+                                                 map.exp_pos, map.exp_pow, map.exp_nor);
+    cudaEventRecord(ev[2], st);
     map.n = n;
     map.r2 = prm.gather_radius * prm.gather_radius;
     map.knn_k = prm.knn_k;
     if (n_stored) *n_stored = n;
-    if (n == 0) { map.present = true; return cudaSuccess; }
-    e = build_tree(map, cp, cw, cn, n, st);
-    map.present = e == cudaSuccess;
-    return e;
+    e = n ? build_tree(map, n, st) : cudaSuccess;
+    cudaEventRecord(ev[3], st);
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    if (stage_ms)
+        for (int k = 0; k < 3; k++) cudaEventElapsedTime(&stage_ms[k], ev[k], ev[k + 1]);
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (e || e2) return e ? e : e2;
+    map.present = true;
+    return cudaSuccess;
 }
 
 cudaError_t photon_set(PhotonMapDev& map, const float4* cp, const float4* cw, const float4* cn, uint32_t n, float radius,
                        uint32_t k, cudaStream_t st) {
     map.release();
-    cudaMalloc(&map.exp_pos, (size_t)std::max(n, 1u) * 16);
-    cudaMalloc(&map.exp_pow, (size_t)std::max(n, 1u) * 16);
-    cudaMalloc(&map.exp_nor, (size_t)std::max(n, 1u) * 16);
+    cudaError_t e = ensure_map(map, n);
+    if (e) return e;
     cudaMemcpyAsync(map.exp_pos, cp, (size_t)n * 16, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(map.exp_pow, cw, (size_t)n * 16, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(map.exp_nor, cn, (size_t)n * 16, cudaMemcpyHostToDevice, st);
     map.n = n;
     map.r2 = radius * radius;
     map.knn_k = k;
-    cudaError_t e = n ? build_tree(map, map.exp_pos, map.exp_pow, map.exp_nor, n, st) : cudaStreamSynchronize(st);
-    map.present = e == cudaSuccess;
-    return e;
+    if (n && (e = build_tree(map, n, st))) return e;
+    if ((e = cudaStreamSynchronize(st))) return e;
+    map.present = true;
+    return cudaSuccess;
 }
 
 void launch_photon_gather_api(const PhotonMapDev& map, const float* q, uint32_t n, float* out, int sms, cudaStream_t st) {

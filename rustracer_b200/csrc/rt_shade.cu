@@ -210,13 +210,6 @@ RT_D float lights_pdf_value(const DevScene& S, float3 o, float3 d) {
     for (int i = 0; i < S.n_lights; i++) sum += w * light_pdf_value(S.lights[i], o, d);
     return sum;
 }
-RT_D float3 onb_local_w(float3 n, float3 a) {                                      // onb.rs:10-20
-    float3 w = unit3(n);
-    float3 h = fabsf(w.x) > 0.9f ? mk(0.f, 1.f, 0.f) : mk(1.f, 0.f, 0.f);
-    float3 v = unit3(cross3(w, h));
-    float3 u = cross3(w, v);
-    return a.x * u + a.y * v + a.z * w;
-}
 RT_D float3 light_generate(const DevLight& L, float3 o, float r1, float r2) {
     if (L.type == RT_PRIM_QUAD) {
         float3 Q = mk(L.g[1].x, L.g[1].y, L.g[1].z), u = mk(L.g[1].w, L.g[2].x, L.g[2].y);

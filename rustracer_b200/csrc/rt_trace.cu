@@ -236,13 +236,58 @@ __device__ __noinline__ uint32_t node_test_general(const DevScene& S, uint32_t n
 
 namespace rtk {
 
+// Per-thread traversal stack (the reference keeps 128 entries inline and
+// spills to a heap Vec, bvh.rs:229-239).  The newest RT_SHORT_STACK entries
+// live in a shared-memory ring laid out [entry][thread], so the lanes of a
+// warp always hit 32 different banks whatever their depths; entry e ≥
+// RT_SHORT_STACK of a deeper stack waits in the thread's global column
+// spill[(e − RT_SHORT_STACK) · stride] (rt_set_tuning can shrink the ring to
+// fewer slots, so the tests run every traversal through the spill path).  A push beyond the ring first moves the
+// ring slot's old entry to its column, a pop that uncovers a spilled entry
+// brings it back.  `cap` (7 per tree level, sized at scene creation) is never
+// reached by a traversal of the scene's own tree; a lower cap from
+// rt_set_tuning makes the traversal stop with RT_ERR_CAPACITY.
+struct TStack {
+    uint32_t* ring;          // &shared[threadIdx.x]; ring slot k at ring[k · RT_TRACE_BLOCK]
+    uint32_t* spill;         // &S.stack_spill[global thread]; entry e at spill[(e − ring_n) · stride]
+    uint32_t stride;
+    int sp, cap;
+    int ring_n;              // ring slots in use: RT_SHORT_STACK, or fewer (a power of two) when tuned
+
+    RT_D bool room(int k) const { return sp + k <= cap; }
+    RT_D void push(uint32_t v) {
+        int slot = sp & (ring_n - 1);
+        if (sp >= ring_n) spill[(size_t)(sp - ring_n) * stride] = ring[slot * RT_TRACE_BLOCK];
+        ring[slot * RT_TRACE_BLOCK] = v;
+        sp++;
+    }
+    RT_D uint32_t pop() {
+        sp--;
+        int slot = sp & (ring_n - 1);
+        uint32_t v = ring[slot * RT_TRACE_BLOCK];
+        if (sp >= ring_n) ring[slot * RT_TRACE_BLOCK] = spill[(size_t)(sp - ring_n) * stride];
+        return v;
+    }
+};
+
+RT_D TStack make_stack(const DevScene& S, uint32_t* shared_ring) {
+    TStack st;
+    st.ring = shared_ring + threadIdx.x;
+    st.stride = gridDim.x * blockDim.x;
+    st.spill = S.stack_spill + blockIdx.x * blockDim.x + threadIdx.x;
+    st.sp = 0;
+    st.cap = S.stack_cap;
+    st.ring_n = S.stack_ring;
+    return st;
+}
+
 // One node visit of the closest-hit traversal: tests the 8 children of `node`,
 // intersects hit leaves in slot order, then continues with the nearest hit inner
 // child (sorted by a 19-comparator network on packed (t | slot) keys) and pushes
 // the others far → near.  Returns false when the traversal is finished.
 template <bool ANA>
 RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, Best& best,
-                       uint32_t& node, int& sp, uint32_t* stack, bool& ok) {
+                       uint32_t& node, TStack& stk, bool& ok) {
     float tn[8];
     uint32_t ch[8];
     // the closest hit so far bounds the boxes; widened like every exit distance
@@ -271,8 +316,8 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
         n += inner ? 1 : 0;
     }
     if (n == 0) {
-        if (sp == 0) return false;
-        node = stack[--sp];
+        if (stk.sp == 0) return false;
+        node = stk.pop();
         return true;
     }
     if (n == 2) {
@@ -284,9 +329,9 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
             if (a == 0xFFFFFFFFu) a = k[c]; else b = k[c];
         }
         uint32_t lo = min(a, b), hi = max(a, b);
-        if (sp + 1 > RT_STACK) { ok = false; return false; }
+        if (!stk.room(1)) { ok = false; return false; }
         const uint32_t* refs = reinterpret_cast<const uint32_t*>(S.nodes + (size_t)node * 14 + 12);
-        stack[sp++] = __ldg(refs + (hi & 7u));
+        stk.push(__ldg(refs + (hi & 7u)));
         node = __ldg(refs + (lo & 7u));
     } else if (n > 2) {
         CAS(0, 1) CAS(2, 3) CAS(4, 5) CAS(6, 7)
@@ -296,11 +341,11 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
         CAS(1, 4) CAS(3, 6)
         CAS(2, 4) CAS(3, 5)
         CAS(3, 4)
-        if (sp + n - 1 > RT_STACK) { ok = false; return false; }
+        if (!stk.room(n - 1)) { ok = false; return false; }
         const uint32_t* refs = reinterpret_cast<const uint32_t*>(S.nodes + (size_t)node * 14 + 12);
 #pragma unroll
         for (int j = 7; j >= 1; j--)
-            if (j < n) stack[sp++] = __ldg(refs + (k[j] & 7u));
+            if (j < n) stk.push(__ldg(refs + (k[j] & 7u)));
         node = __ldg(refs + (k[0] & 7u));
     } else {
         uint32_t c = 0;
@@ -315,7 +360,7 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
 // finished; *hit is set when a primitive was hit.
 template <bool ANA>
 RT_D bool any_step(const DevScene& S, const RayC& R, float3 d, float tmin, float tmax,
-                   uint32_t& node, int& sp, uint32_t* stack, bool& hit, bool& ok) {
+                   uint32_t& node, TStack& stk, bool& hit, bool& ok) {
     float tn[8];
     uint32_t ch[8];
     float tw = tmax + fabsf(tmax) * SLAB_WIDEN;
@@ -339,16 +384,16 @@ RT_D bool any_step(const DevScene& S, const RayC& R, float3 d, float tmin, float
         }
     }
     if (inner == 0) {
-        if (sp == 0) return false;
-        node = stack[--sp];
+        if (stk.sp == 0) return false;
+        node = stk.pop();
         return true;
     }
     int first = __ffs(inner) - 1;
     uint32_t rest = inner & (inner - 1);
-    if (sp + __popc(rest) > RT_STACK) { ok = false; return false; }
+    if (!stk.room(__popc(rest))) { ok = false; return false; }
 #pragma unroll
     for (int c = 0; c < 8; c++)
-        if ((rest >> c) & 1u) stack[sp++] = ch[c];
+        if ((rest >> c) & 1u) stk.push(ch[c]);
     node = ch[first];
     return true;
 }
@@ -372,11 +417,6 @@ RT_D bool nan_ray(float3 o, float3 d, float tmin, float tmax) {
 
 // MODE 0: wavefront extend (queue of path ids, rays in PathState, hits to PathState)
 // MODE 1: API (rays n×8 in memory, hits as int4)
-// 6 resident blocks of 128 threads per SM: caps the kernels at 80 registers
-// (measured faster than 5 blocks at 96 registers and than 8 blocks at 64)
-#ifndef RT_TRACE_MINB
-#define RT_TRACE_MINB 6
-#endif
 
 template <int MODE, bool ANA>
 __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevScene S, PathState P, const uint32_t* __restrict__ queue,
@@ -385,10 +425,10 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
                                                             int4* __restrict__ out, int* err) {
     const uint32_t n = MODE == 0 ? *count : n_api;
     const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
-    uint32_t stack[RT_STACK];
+    __shared__ uint32_t ring[RT_SHORT_STACK * RT_TRACE_BLOCK];
+    rtk::TStack stk = rtk::make_stack(S, ring);
     bool active = false, exhausted = false, ok = true;
     uint32_t item = 0, node = 0, pid = 0;
-    int sp = 0;
     float3 o = mk(0.f, 0.f, 0.f), d = o;
     RayC R = make_rayc(o, mk(1.f, 1.f, 1.f), 0.0f);
     float tmin = 0.0f;
@@ -417,7 +457,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
                     }
                     R = make_rayc(o, d, tmin);
                     best = Best{tmax, 0.0f, 0.0f, RT_MISS_REF, 0xFFFFFFFFu, 0u};
-                    node = 0; sp = 0;
+                    node = 0; stk.sp = 0;
                     active = !rtk::nan_ray(o, d, tmin, tmax);
                     if (!active) {
                         if (MODE == 0) P.hit[pid] = make_float4(__uint_as_float(RT_MISS_REF), 0.f, 0.f, 0.f);
@@ -429,7 +469,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
         if (exhausted && __ballot_sync(FULLMASK, active) == 0) break;
         if (active) {
             bool lok = true;
-            bool more = rtk::closest_step<ANA>(S, R, d, tmin, best, node, sp, stack, lok);
+            bool more = rtk::closest_step<ANA>(S, R, d, tmin, best, node, stk, lok);
             if (!lok) ok = false;
             if (!more) {
                 active = false;
@@ -458,10 +498,10 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
                                                         uint8_t* __restrict__ out, int* err) {
     const uint32_t n = MODE != 1 ? *count : n_api;
     const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
-    uint32_t stack[RT_STACK];
+    __shared__ uint32_t ring[RT_SHORT_STACK * RT_TRACE_BLOCK];
+    rtk::TStack stk = rtk::make_stack(S, ring);
     bool active = false, exhausted = false, ok = true;
     uint32_t item = 0, node = 0, tag = 0;
-    int sp = 0;
     float3 o = mk(0.f, 0.f, 0.f), d = o;
     RayC R = make_rayc(o, mk(1.f, 1.f, 1.f), 0.0f);
     float tmin = 0.0f, tmax = 0.0f;
@@ -488,7 +528,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
                         tmin = r[6]; tmax = r[7];
                     }
                     R = make_rayc(o, d, tmin);
-                    node = 0; sp = 0; hit = false;
+                    node = 0; stk.sp = 0; hit = false;
                     active = !rtk::nan_ray(o, d, tmin, tmax);
                     if (!active && MODE == 1) out[i] = 0;
                 }
@@ -497,7 +537,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
         if (exhausted && __ballot_sync(FULLMASK, active) == 0) break;
         if (active) {
             bool lok = true;
-            bool more = rtk::any_step<ANA>(S, R, d, tmin, tmax, node, sp, stack, hit, lok);
+            bool more = rtk::any_step<ANA>(S, R, d, tmin, tmax, node, stk, hit, lok);
             if (!lok) ok = false;
             if (!more) {
                 active = false;

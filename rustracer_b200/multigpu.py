@@ -12,6 +12,14 @@ what Welford's update over the concatenated sample sequence gives (the firefly
 clamp, which depends on the running mean, is not shard-invariant: merge only
 unclamped accumulations).
 
+The caustic photon map is built once per frame across the ranks: each rank
+traces a contiguous share of the emission order (RtPhotonParams.first_photon /
+shard_photons, the reference parallelises the same photon loop over its
+threads, photon.rs:78,112), the ranks all-gather what they stored (position,
+power, normal, emission index; ≤ 2M × 40 B), and every rank builds the same
+gather structure from the union, ordered by emission index: the map one
+unsharded build gives.
+
 The learned proposal trains on one rank and is then shared: the source
 rank's frozen parameters (rt_guide_params, 16.8M float32) are broadcast and
 written into every other rank's guide, so all ranks sample from the same
@@ -45,12 +53,14 @@ def merge_accumulators(acc_sum, acc_m2, acc_count, group=None):
 
 
 def broadcast_guide(scene, src=0, group=None):
-    """Copy rank `src`'s guide parameters into every rank's guide (each rank's
-    scene must have called guide_init).  The broadcast is one float32 tensor
+    """Copy global rank `src`'s guide parameters into every rank of `group`
+    (each rank's scene must have called guide_init).  The broadcast is one float32 tensor
     of RT_GUIDE_PARAMS values; the receiving guides' Adam state is reset,
     as rt_guide_params does on a write."""
     import torch.distributed as dist
-    rank = dist.get_rank(group)
+    # `src` is a global rank (dist.broadcast reads it that way), so compare it
+    # with this process's global rank, also inside a subgroup
+    rank = dist.get_rank()
     t = torch.from_numpy(scene.guide_get_params()) if rank == src else None
     if t is None:
         from . import abi
@@ -61,3 +71,35 @@ def broadcast_guide(scene, src=0, group=None):
     if rank != src:
         scene.guide_set_params(t.cpu().numpy())
     return t.numel()
+
+
+def build_photon_map(scene, params, group=None):
+    """Sharded caustic photon map: every rank of `group` traces its share of
+    `params`' photons, the stored photons are all-gathered and each rank's
+    scene receives the whole map (rt_photon_set with emission indices).
+    Returns the number of stored photons in the map.  `scene` needs
+    photon_build / photon_export / photon_set (a GpuScene)."""
+    import numpy as np
+    import torch.distributed as dist
+    from . import photons
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    scene.photon_build(photons.shard_params(params, world, rank))
+    pos, power, nor, idx = scene.photon_export()
+    rec = np.concatenate([pos, power, nor, idx.view(np.float32)[:, None]], 1).astype(np.float32)   # n × 10
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    n = torch.tensor([len(rec)], dtype=torch.int64, device=dev)
+    counts = [torch.zeros_like(n) for _ in range(world)]
+    dist.all_gather(counts, n, group=group)
+    counts = [int(c.item()) for c in counts]
+    m = max(max(counts), 1)
+    mine = torch.zeros((m, 10), dtype=torch.float32, device=dev)
+    if len(rec):
+        mine[: len(rec)] = torch.from_numpy(rec).to(dev)
+    parts = [torch.empty_like(mine) for _ in range(world)]
+    dist.all_gather(parts, mine, group=group)
+    allrec = np.concatenate([p[:c].cpu().numpy() for p, c in zip(parts, counts)], 0)
+    order = np.argsort(allrec[:, 9].view(np.int32), kind="stable")
+    allrec = allrec[order]
+    scene.photon_set(allrec[:, 0:3], allrec[:, 3:6], allrec[:, 6:9], allrec[:, 9].view(np.int32).copy(),
+                     radius=params.gather_radius, knn_k=params.knn_k)
+    return len(allrec)

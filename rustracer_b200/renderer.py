@@ -56,6 +56,7 @@ def lib():
         L.rt_photon_build.argtypes = [vp, C.POINTER(abi.RtPhotonParams), C.POINTER(i64)]
         L.rt_photon_set.argtypes = [vp, vp, vp, vp, vp, i64, f, u32]
         L.rt_photon_clear.argtypes = [vp]
+        L.rt_photon_build_times.argtypes = [vp, C.POINTER(C.c_float)]
         L.rt_photon_export.argtypes = [vp, vp, vp, vp, vp, C.POINTER(i64)]
         L.rt_photon_gather.argtypes = [vp, vp, i64, vp, i32]
         L.rt_knn.argtypes = [vp, vp, i64, i32, f, vp, vp, i32]
@@ -65,6 +66,7 @@ def lib():
                                       C.POINTER(i64)]
         L.rt_set_tuning.argtypes = [vp, C.POINTER(abi.RtTuning)]
         L.rt_get_tuning.argtypes = [vp, C.POINTER(abi.RtTuning)]
+        L.rt_set_caller_stream.argtypes = [vp, vp]
         L.rt_guide_init.argtypes = [vp, C.POINTER(abi.RtGuideParams)]
         L.rt_guide_mode.argtypes = [vp, i32]
         L.rt_guide_params.argtypes = [vp, vp, i32]
@@ -97,6 +99,16 @@ def _ptr(a):
     except ImportError:
         pass
     raise TypeError("expected a numpy array or a torch tensor")
+
+
+def _torch_stream(*arrays):
+    """cudaStream_t of torch's current stream on the device of the first CUDA
+    tensor among `arrays` (None when none is a CUDA tensor)."""
+    for a in arrays:
+        if a is not None and not isinstance(a, np.ndarray) and getattr(a, "is_cuda", False):
+            import torch
+            return torch.cuda.current_stream(a.device).cuda_stream
+    return None
 
 
 def develop_params(width, height, exposure=1.0, tonemapper="agx", vignette=0.0, distortion=0.0):
@@ -174,6 +186,13 @@ class GpuScene:
         if rc != 0:
             raise RtError(rc, self.last_error())
 
+    def _order(self, *arrays):
+        """Make the library's calls wait for torch's current stream when CUDA
+        tensors are passed (their producers may still be queued there)."""
+        st = _torch_stream(*arrays)
+        if st is not None:
+            self._check(lib().rt_set_caller_stream(self.h, C.c_void_p(st)))
+
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
             lib().rt_scene_destroy(self.h)
@@ -220,6 +239,7 @@ class GpuScene:
             return hits
         rp, mem = _ptr(rays)
         op, _ = _ptr(out)
+        self._order(rays, out)
         self._check(lib().rt_trace_closest(self.h, rp, n, op, mem))
         return out
 
@@ -249,6 +269,7 @@ class GpuScene:
         cp = None
         if converged is not None:
             cp, _ = _ptr(converged)
+        self._order(out, converged)
         self._check(lib().rt_render_pass(self.h, C.byref(cam), C.byref(params), op, cp, mem))
         return out
 
@@ -259,6 +280,7 @@ class GpuScene:
         op, mem = _ptr(out)
         if mem != abi.RT_MEM_DEVICE:
             raise TypeError("render_pass_noalloc writes device memory: pass a CUDA tensor")
+        self._order(out)
         self._check(lib().rt_render_pass_noalloc(self.h, C.byref(cam), C.byref(params), op))
         return out
 
@@ -284,6 +306,7 @@ class GpuScene:
         sp, mem = _ptr(s)
         mp, _ = _ptr(m)
         cp, _ = _ptr(c)
+        self._order(s, m, c)
         self._check(lib().rt_render_accumulate(self.h, C.byref(cam), C.byref(params), float(firefly_clamp),
                                                int(firefly_min_samples), float(firefly_floor), 1 if reset else 0,
                                                sp, mp, cp, mem))
@@ -308,6 +331,7 @@ class GpuScene:
             lp, lmem = _ptr(linear)
             if lmem != mem:
                 raise ValueError("linear and out must both be host arrays or both device tensors")
+        self._order(linear, out)
         self._check(lib().rt_develop(self.h, lp, C.byref(p), op, mem))
         return out
 
@@ -330,6 +354,12 @@ class GpuScene:
                                         C.c_void_p(nor.ctypes.data),
                                         None if idx is None else C.c_void_p(idx.ctypes.data), len(pos), float(radius),
                                         int(knn_k)))
+
+    def photon_stage_ms(self):
+        """Device ms of the last photon build's stages: (trace, compaction, tree)."""
+        ms = (C.c_float * 3)()
+        self._check(lib().rt_photon_build_times(self.h, ms))
+        return tuple(ms)
 
     def photon_clear(self):
         self._check(lib().rt_photon_clear(self.h))
@@ -360,15 +390,18 @@ class GpuScene:
 
     # ── diagnostics ──────────────────────────────────────────────────────
     # ── launch tuning (rt_set_tuning) ─────────────────────────────────────
-    def set_tuning(self, max_paths=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0):
-        t = abi.RtTuning(int(max_paths), int(trace_blocks_per_sm), int(shade_blocks_per_sm))
+    def set_tuning(self, max_paths=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, max_iterations=0,
+                   stack_limit=0, stack_ring=0):
+        t = abi.RtTuning(int(max_paths), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(max_iterations),
+                         int(stack_limit), int(stack_ring))
         self._check(lib().rt_set_tuning(self.h, C.byref(t)))
 
     def get_tuning(self):
         t = abi.RtTuning()
         self._check(lib().rt_get_tuning(self.h, C.byref(t)))
         return dict(max_paths=t.max_paths, trace_blocks_per_sm=t.trace_blocks_per_sm,
-                    shade_blocks_per_sm=t.shade_blocks_per_sm)
+                    shade_blocks_per_sm=t.shade_blocks_per_sm, max_iterations=t.max_iterations,
+                    stack_limit=t.stack_limit, stack_ring=t.stack_ring)
 
     # ── path guiding (rt_guide_*) ─────────────────────────────────────────
     def guide_init(self, params=None):

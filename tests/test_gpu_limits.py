@@ -1,0 +1,97 @@
+"""Limits of the device loops and the traversal stack.
+
+The traversal stack keeps its newest entries in a shared-memory ring and
+spills deeper ones to global memory, so no scene's tree overflows it (the
+reference keeps 128 entries inline and spills to a heap Vec, bvh.rs:229-239).
+rt_set_tuning can shrink the ring, which sends every traversal through the
+spill path: the hits must not change.  It can also lower the stack capacity
+and the wavefront's iteration bound, which makes the library return
+RT_ERR_CAPACITY / RT_ERR_TIMEOUT from a render or trace call instead of
+faulting, and leaves the scene usable."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rustracer_b200 import configs
+from rustracer_b200.renderer import GpuScene, RtError, pass_params
+from tests.helpers import camera_rays, random_rays
+
+pytestmark = pytest.mark.gpu
+
+RT_ERR_CAPACITY, RT_ERR_TIMEOUT = 2, 3
+
+
+def _hits_equal(a, b):
+    assert np.array_equal(a["prim"], b["prim"]), np.flatnonzero(a["prim"] != b["prim"])[:10]
+    hit = a["prim"] >= 0
+    for f in ("t", "b1", "b2"):
+        assert np.array_equal(a[f][hit].view(np.uint32), b[f][hit].view(np.uint32)), f
+
+
+def test_spilled_stack_gives_the_same_hits_on_the_icosphere():
+    """1.31M-triangle icosphere: with a ring of 1 or 2 slots nearly every push
+    and pop goes through the global spill columns; hits, t and barycentrics
+    stay bit-identical to the 16-slot ring and to the oracle."""
+    sb, st = configs.icosphere_scene(env_w=64, env_h=32)
+    g, o = GpuScene(sb), O.OracleScene(sb)
+    r = np.concatenate([random_rays(30000, 31, spread=0.7), camera_rays(st["camera"], 200, 100, seed=4)])
+    assert g.get_tuning()["stack_ring"] == 16
+    base = g.trace_closest(r)
+    base_any = g.trace_any(r)
+    _hits_equal(base[:8000], o.trace_closest(r[:8000]))
+    for ring in (1, 2, 8):
+        g.set_tuning(stack_ring=ring)
+        _hits_equal(g.trace_closest(r), base)
+        assert np.array_equal(g.trace_any(r), base_any)
+    g.set_tuning()
+    assert g.get_tuning()["stack_ring"] == 16
+
+
+def test_spilled_stack_renders_the_same_image():
+    """A render pass (extend and shadow kernels of the wavefront) with a
+    one-slot ring is bit-identical to the default."""
+    sb, st = configs.box_scene(width=96, height=96)
+    g = GpuScene(sb)
+    p = pass_params(96, 96, 0, 4, 2, 8, 4, 1.0, 17)
+    a = g.render_pass(st["camera"], p)
+    g.set_tuning(stack_ring=1)
+    b = g.render_pass(st["camera"], p)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_stack_capacity_error_is_returned_and_the_scene_stays_usable():
+    sb, st = configs.icosphere_scene(env_w=64, env_h=32)
+    g = GpuScene(sb)
+    cap = g.get_tuning()["stack_limit"]
+    depth = g.bvh_stats()["max_depth"]
+    assert cap == 7 * (depth + 1) + 8
+    r = random_rays(4096, 5, spread=0.7)
+    ref = g.trace_closest(r)
+    g.set_tuning(stack_limit=1)
+    with pytest.raises(RtError) as e:
+        g.trace_closest(r)
+    assert e.value.code == RT_ERR_CAPACITY
+    with pytest.raises(RtError) as e:
+        g.render_pass(st["camera"], pass_params(64, 36, 0, 1, 1, 12, 4, 1.0, 2))
+    assert e.value.code == RT_ERR_CAPACITY
+    with pytest.raises(RtError) as e:
+        g.set_tuning(stack_limit=cap + 1)
+    assert e.value.code == 1
+    g.set_tuning()
+    _hits_equal(g.trace_closest(r), ref)
+
+
+def test_iteration_bound_returns_timeout_and_the_scene_stays_usable():
+    sb, st = configs.box_scene(width=64, height=64)
+    g = GpuScene(sb)
+    p = pass_params(64, 64, 0, 2, 1, 8, 4, 1.0, 9)
+    ref = g.render_pass(st["camera"], p)
+    g.set_tuning(max_iterations=2)
+    with pytest.raises(RtError) as e:
+        g.render_pass(st["camera"], p)
+    assert e.value.code == RT_ERR_TIMEOUT and "iteration bound" in str(e.value)
+    with pytest.raises(RtError) as e:
+        g.render_accumulate(st["camera"], p)
+    assert e.value.code == RT_ERR_TIMEOUT
+    g.set_tuning()
+    assert np.array_equal(g.render_pass(st["camera"], p).view(np.uint32), ref.view(np.uint32))

@@ -59,6 +59,17 @@ def test_box_scene_tiles_match_oracle():
     assert_tiles_agree(gi, oi)
 
 
+def test_box_config_at_its_stated_size():
+    """The plain box workload at its stated size: 256×256, 16 spp (strata 4),
+    depth 8, 4 hero wavelengths — all 256 tiles of the frame."""
+    sb, st = configs.box_scene()
+    assert (st["width"], st["height"], st["spp"], st["max_depth"], st["hero"]) == (256, 256, 16, 8, 4)
+    gi, oi, _ = render_both(sb, st, 256, 256, 16, 11, 12)
+    assert gi.shape == (16, 256, 256, 3) and np.isfinite(gi).all()
+    z = assert_tiles_agree(gi, oi)
+    assert z.size == 256
+
+
 def test_box_scene_same_seed_matches_pixelwise():
     sb, st = configs.box_scene(width=64, height=64)
     gi, oi, _ = render_both(sb, st, 64, 64, 16, 7, 7)

@@ -126,3 +126,86 @@ def test_broadcast_guide_shares_rank0_parameters():
         n, a, b = out[r]
         assert n == abi.RT_GUIDE_PARAMS
         assert a == float(ref[:1000].sum()) and b == float(ref[-1000:].sum())
+
+
+def _guide_subgroup_worker(rank, world, port, out):
+    import torch.distributed as dist
+    from rustracer_b200 import abi
+    from rustracer_b200.multigpu import broadcast_guide
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        grp = dist.new_group([1, 2])            # every rank takes part in creating it
+        rng = np.random.default_rng(rank)
+        g = _GuideStandIn(rng.standard_normal(abi.RT_GUIDE_PARAMS).astype(np.float32))
+        if rank in (1, 2):
+            broadcast_guide(g, src=2, group=grp)
+        out[rank] = float(g.params[:1000].sum())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_broadcast_guide_in_a_subgroup_uses_the_global_source_rank():
+    """In the subgroup {1, 2} the source is global rank 2: rank 1 receives
+    rank 2's parameters and rank 0 keeps its own (gloo, 3 ranks)."""
+    from rustracer_b200 import abi
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_guide_subgroup_worker, args=(r, 3, port, out)) for r in range(3)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(180)
+        assert p.exitcode == 0
+    own = [float(np.random.default_rng(r).standard_normal(abi.RT_GUIDE_PARAMS).astype(np.float32)[:1000].sum())
+           for r in range(3)]
+    assert out[0] == own[0]
+    assert out[1] == own[2] and out[2] == own[2]
+
+
+def _photon_worker(rank, world, port, out):
+    import torch.distributed as dist
+    from oracle import oracle as O
+    from rustracer_b200 import configs
+    from rustracer_b200.multigpu import build_photon_map
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sb, st = configs.gem_scene(width=32, height=18, env_w=64, env_h=32)
+        o = O.OracleScene(sb)                     # the CPU restatement stands in for a GPU scene
+        n = build_photon_map(o, st["photon_params"](5, 60000))
+        out[rank] = (n,) + tuple(o.photon_export())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_photon_map_equals_the_single_rank_map():
+    """Two ranks each trace half of the emission order and exchange what they
+    stored (gloo): both end with exactly the map of one unsharded build —
+    the same photons, powers, normals and emission indices."""
+    from oracle import oracle as O
+    from rustracer_b200 import configs
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_photon_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(300)
+        assert p.exitcode == 0
+    sb, st = configs.gem_scene(width=32, height=18, env_w=64, env_h=32)
+    o = O.OracleScene(sb)
+    n = o.photon_build(st["photon_params"](5, 60000))
+    ref = o.photon_export()
+    assert n > 1000
+    for r in range(2):
+        got = out[r]
+        assert got[0] == n
+        for a, b in zip(got[1:], ref):
+            assert np.array_equal(a, b)

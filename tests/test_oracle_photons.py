@@ -73,3 +73,42 @@ def test_knn_rule_sorted_with_index_ties():
         order = order[dd[order] <= np.float32(0.25)][:16]
         assert list(idx[i][: len(order)]) == list(order)
         assert (idx[i][len(order):] == -1).all()
+
+
+def test_projection_map_keeps_the_expected_caustic_power():
+    """Light-quad photons sent toward the stone's bounding sphere (power ×
+    2·cosθ·(1 − cos θ_max)) store ~20× more photons than the full hemisphere,
+    with the same expected total stored power (within 4 standard errors)."""
+    from rustracer_b200 import configs
+    sb, st = configs.gem_scene(width=32, height=18, env_w=64, env_h=32)
+    s = O.OracleScene(sb)
+    tot = {}
+    for proj, n in ((False, 2_000_000), (True, 200_000)):
+        cnt = s.photon_build(st["photon_params"](11, n, projection=proj))
+        _, pw, _, _ = s.photon_export()
+        lum = pw @ np.array([0.2126, 0.7152, 0.0722])
+        # the map's total power is a sum over n photons (stored or not), so its
+        # standard error is sqrt(n · Var) with the unstored photons at 0
+        per = np.zeros(n)
+        per[:cnt] = lum * n
+        tot[proj] = (lum.sum(), per.std() / np.sqrt(n), cnt)
+    (a, sa, na), (b, sb_, nb) = tot[False], tot[True]
+    assert (nb / 200_000) > 10 * (na / 2_000_000), (na, nb)   # far more stored per emitted photon
+    assert abs(a - b) < 4.0 * np.hypot(sa, sb_), (a, b, sa, sb_)
+
+
+def test_photon_shards_partition_the_emission_order():
+    """first_photon / shard_photons: the shards' stored photons are exactly
+    the unsharded build's, split by emission index."""
+    from rustracer_b200 import configs
+    sb, st = configs.gem_scene(width=32, height=18, env_w=64, env_h=32)
+    s = O.OracleScene(sb)
+    p = st["photon_params"](2, 50000)
+    s.photon_build(p)
+    ref = s.photon_export()
+    parts = []
+    for r in range(3):
+        s.photon_build(photons.shard_params(p, 3, r))
+        parts.append(s.photon_export())
+    for k in range(4):
+        assert np.array_equal(np.concatenate([q[k] for q in parts]), ref[k])

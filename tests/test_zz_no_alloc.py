@@ -31,6 +31,28 @@ def test_noalloc_matches_render_pass_on_consecutive_calls():
         assert b.sum() > 0
 
 
+@pytest.mark.parametrize("w,h,n", [(128, 128, 4), (256, 256, 1)])
+def test_noalloc_refills_its_path_pool(w, h, n):
+    """Frames of more samples than the fixed array's 32,768 path slots: the
+    retire kernel hands each freed slot the next sample, through the shared
+    array, until all w·h·n samples are drawn (two calls in a row)."""
+    import torch
+    assert w * h * n > 32768
+    sb, st = configs.box_scene(width=w, height=h)
+    g = GpuScene(sb)
+    for call, (first, seed) in enumerate([(0, 21), (n, 22)]):
+        p = pass_params(w, h, first, n, 2, 8, 4, 1.0, seed)
+        ref = torch.zeros((n, h, w, 3), device="cuda")
+        out = torch.full((n, h, w, 3), float("nan"), device="cuda")
+        g.render_pass(st["camera"], p, out=ref)
+        g.render_pass_noalloc(st["camera"], p, out)
+        torch.cuda.synchronize()
+        a, b = out.cpu().numpy(), ref.cpu().numpy()
+        assert np.isfinite(a).all(), f"call {call}: non-finite output"
+        np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-7, err_msg=f"call {call}")
+        assert b.sum() > 0
+
+
 def test_noalloc_rejects_frames_beyond_its_scratch():
     import torch
     sb, st = configs.box_scene(width=512, height=512)
