@@ -168,6 +168,10 @@ typedef struct RtBackground {
  * canonical ids; an exact tie goes to the surface). */
 #define RT_MEDIUM_CONSTANT 0   /* ConstantMedium: exponential free flight, Beer–Lambert shadows */
 #define RT_MEDIUM_NOISE    1   /* NoiseMedium: delta tracking against density·max, 16-point shadow quadrature */
+#define RT_MEDIUM_GRID     2   /* no counterpart in the reference: a voxel grid of σ_t in a box boundary,
+                                  trilinear between voxel centres; delta tracking and ratio-tracked
+                                  shadows against per-brick majorants (8³ voxels per brick) */
+#define RT_GRID_MAX_RES    1024
 #define RT_BOUND_SPHERE    0
 #define RT_BOUND_BOX       1   /* axis-aligned box of 6 quads (quad.rs:201-215) */
 
@@ -185,6 +189,11 @@ typedef struct RtMedium {
      * vectors and three permutations of 0..255 */
     float   perlin_vec[256 * 3];
     int32_t perlin_perm[3 * 256];
+    /* grid: grid_res[0] × grid_res[1] × grid_res[2] values (x fastest), each
+     * 1 .. RT_GRID_MAX_RES, over the box p_min..p_max (box boundary only);
+     * σ_t(x) = density × trilinear(grid) ≥ 0.  The library copies the grid. */
+    const float* grid;
+    int32_t grid_res[3];
 } RtMedium;
 
 /* ── analytic convex solids (diamond.rs:198-253) ─────────────────────────────
@@ -542,7 +551,14 @@ typedef struct RtTuning {
      * results never depend on it; small rings make every traversal take the
      * spill path. */
     uint32_t stack_ring;
+    /* Node layout the traversal reads: RT_NODES_QUANTISED (0, the default
+     * when the scene's extents allow it) — 128-byte nodes whose child boxes
+     * are 8-bit offsets rounded outward, so the hits are unchanged — or
+     * RT_NODES_FULL (1), the reference's 224-byte float layout (bvh.rs:25-32). */
+    uint32_t node_format;
 } RtTuning;
+#define RT_NODES_QUANTISED 0
+#define RT_NODES_FULL      1
 int32_t rt_set_tuning(RtScene* scene, const RtTuning* tuning);
 
 /* The stream the caller queues its own work on (a cudaStream_t; NULL = the

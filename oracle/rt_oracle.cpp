@@ -602,6 +602,9 @@ struct Scene {
     uint32_t knn_k = 0;
     // participating media (volume.rs:78-263); a box boundary is its 6 quads
     std::vector<RtMedium> media;
+    // grid media (no counterpart in the reference): voxels and per-brick majorants
+    struct GridMed { std::vector<float> grid, major; int res[3] = {1, 1, 1}, nb[3] = {1, 1, 1}; V3 lo, inv_vox, bw, inv_bw; };
+    std::vector<GridMed> media_grid;
     std::vector<std::vector<Quad>> media_quads;
 };
 
@@ -1204,6 +1207,131 @@ static bool bound_hit(const Scene& s, int mi, const Ray& r, float tmin, float tm
     return any;
 }
 
+// ── grid medium (no counterpart in the reference) ────────────────────────────
+// σ_t(x) = density × trilinear interpolation of the voxels between voxel
+// centres, clamped at the box faces; majorants per brick of 8³ voxels, each the
+// largest voxel its lookups read (one voxel of apron) enlarged by 2^-20.
+static const int GRID_BRICK = 8;
+static const uint32_t GRID_MAX_STEPS = 4096;
+static float grid_density_at(const RtMedium& m, const Scene::GridMed& G, V3 p) {
+    const float c[3] = {(p.x - G.lo.x) * G.inv_vox.x - 0.5f, (p.y - G.lo.y) * G.inv_vox.y - 0.5f,
+                        (p.z - G.lo.z) * G.inv_vox.z - 0.5f};
+    int i0[3], i1[3];
+    float f[3];
+    for (int a = 0; a < 3; a++) {
+        float u = rmin(rmax(c[a], 0.0f), (float)(G.res[a] - 1));
+        int i = std::min((int)u, std::max(G.res[a] - 2, 0));
+        i0[a] = i;
+        i1[a] = std::min(i + 1, G.res[a] - 1);
+        f[a] = u - (float)i;
+    }
+    auto at = [&](int i, int j, int k) { return G.grid[((size_t)k * G.res[1] + j) * G.res[0] + i]; };
+    float c00 = at(i0[0], i0[1], i0[2]) * (1.0f - f[0]) + at(i1[0], i0[1], i0[2]) * f[0];
+    float c10 = at(i0[0], i1[1], i0[2]) * (1.0f - f[0]) + at(i1[0], i1[1], i0[2]) * f[0];
+    float c01 = at(i0[0], i0[1], i1[2]) * (1.0f - f[0]) + at(i1[0], i0[1], i1[2]) * f[0];
+    float c11 = at(i0[0], i1[1], i1[2]) * (1.0f - f[0]) + at(i1[0], i1[1], i1[2]) * f[0];
+    float c0 = c00 * (1.0f - f[1]) + c10 * f[1], c1 = c01 * (1.0f - f[1]) + c11 * f[1];
+    return m.density * (c0 * (1.0f - f[2]) + c1 * f[2]);
+}
+
+// 3-D DDA over the majorant bricks (Amanatides & Woo 1987) from the point at t0
+struct BrickWalk { int b[3], step[3]; float tnext[3], dt[3]; };
+static void brick_walk_init(const Scene::GridMed& G, const Ray& r, float t0, BrickWalk& w) {
+    V3 p = r.o + t0 * r.d;
+    const float pc[3] = {p.x, p.y, p.z}, oc[3] = {r.o.x, r.o.y, r.o.z}, dc[3] = {r.d.x, r.d.y, r.d.z};
+    const float lo[3] = {G.lo.x, G.lo.y, G.lo.z}, bw[3] = {G.bw.x, G.bw.y, G.bw.z};
+    const float ib[3] = {G.inv_bw.x, G.inv_bw.y, G.inv_bw.z};
+    for (int a = 0; a < 3; a++) {
+        int b = (int)std::floor((pc[a] - lo[a]) * ib[a]);
+        b = std::min(std::max(b, 0), G.nb[a] - 1);
+        w.b[a] = b;
+        if (dc[a] > 0.0f) {
+            w.step[a] = 1;
+            w.tnext[a] = (lo[a] + (float)(b + 1) * bw[a] - oc[a]) / dc[a];
+            w.dt[a] = bw[a] / dc[a];
+        } else if (dc[a] < 0.0f) {
+            w.step[a] = -1;
+            w.tnext[a] = (lo[a] + (float)b * bw[a] - oc[a]) / dc[a];
+            w.dt[a] = -bw[a] / dc[a];
+        } else {
+            w.step[a] = 0;
+            w.tnext[a] = INFINITY;
+            w.dt[a] = INFINITY;
+        }
+    }
+}
+static bool brick_walk_next(const Scene::GridMed& G, BrickWalk& w) {
+    int a = w.tnext[0] <= w.tnext[1] ? (w.tnext[0] <= w.tnext[2] ? 0 : 2) : (w.tnext[1] <= w.tnext[2] ? 1 : 2);
+    w.b[a] += w.step[a];
+    w.tnext[a] += w.dt[a];
+    return w.b[a] >= 0 && w.b[a] < G.nb[a];
+}
+static float brick_major(const RtMedium& m, const Scene::GridMed& G, const BrickWalk& w) {
+    return m.density * G.major[((size_t)w.b[2] * G.nb[1] + w.b[1]) * G.nb[0] + w.b[0]];
+}
+static const int GRID_MAX_SEGMENTS = 3 * RT_GRID_MAX_RES / GRID_BRICK + 4;
+
+// delta tracking (Woodcock) in [t1, t2] against each brick's majorant
+static float grid_sample(const RtMedium& m, const Scene::GridMed& G, const Ray& r, float lam, float t1, float t2) {
+    MedRng g = medium_rng(r.o, r.d, lam);
+    float len = length(r.d);
+    BrickWalk w;
+    brick_walk_init(G, r, t1, w);
+    float t = t1;
+    uint32_t k = 0;
+    for (int seg = 0; seg < GRID_MAX_SEGMENTS; seg++) {
+        float tb = rmin(rmin(w.tnext[0], w.tnext[1]), rmin(w.tnext[2], t2));
+        float mu = brick_major(m, G, w);
+        if (mu > 0.0f) {
+            float inv = 1.0f / (mu * len);
+            while (k < GRID_MAX_STEPS) {
+                float tt = t - inv * std::log(rmax(medium_rnd(g, 2 * k), FLT_EPSILON));
+                float xi = medium_rnd(g, 2 * k + 1);
+                k++;
+                if (tt >= tb) break;
+                t = tt;
+                if (xi * mu < grid_density_at(m, G, r.o + t * r.d)) return t;
+            }
+            if (k >= GRID_MAX_STEPS) return INFINITY;
+        }
+        if (tb >= t2) return INFINITY;
+        t = rmax(t, tb);
+        if (!brick_walk_next(G, w)) return INFINITY;
+    }
+    return INFINITY;
+}
+
+// ratio tracking (Cramer 1978; Novák et al. 2014) over [a, b]: the product of
+// (1 − σ_t/μ) at tentative collisions, an unbiased estimate of exp(−∫σ_t)
+static float grid_transmittance(const RtMedium& m, const Scene::GridMed& G, const Ray& r, float a, float b, float tmax) {
+    MedRng g = medium_rng(r.o, r.d, tmax);
+    float len = length(r.d);
+    BrickWalk w;
+    brick_walk_init(G, r, a, w);
+    float t = a, T = 1.0f;
+    uint32_t k = 0;
+    for (int seg = 0; seg < GRID_MAX_SEGMENTS; seg++) {
+        float tb = rmin(rmin(w.tnext[0], w.tnext[1]), rmin(w.tnext[2], b));
+        float mu = brick_major(m, G, w);
+        if (mu > 0.0f) {
+            float inv = 1.0f / (mu * len);
+            while (k < GRID_MAX_STEPS) {
+                float tt = t - inv * std::log(rmax(medium_rnd(g, 0x40000u + k), FLT_EPSILON));
+                k++;
+                if (tt >= tb) break;
+                t = tt;
+                T *= rmax(1.0f - grid_density_at(m, G, r.o + t * r.d) / mu, 0.0f);
+                if (T <= 0.0f) return 0.0f;
+            }
+            if (k >= GRID_MAX_STEPS) return T;
+        }
+        if (tb >= b) return T;
+        t = rmax(t, tb);
+        if (!brick_walk_next(G, w)) return T;
+    }
+    return T;
+}
+
 // Scatter distance of ConstantMedium::hit (volume.rs:97-138) / NoiseMedium::hit
 // (:195-235) for t_max = ∞; INFINITY when the ray leaves the medium first.  The
 // candidate depends on the ray alone, so "nearest of surface and medium" gives
@@ -1217,6 +1345,7 @@ static float medium_sample(const Scene& s, int mi, const Ray& r, float lam, floa
     if (t1 < tmin) t1 = tmin;
     if (t1 >= t2) return INFINITY;
     if (t1 < 0.0f) t1 = 0.0f;
+    if (m.type == RT_MEDIUM_GRID) return grid_sample(m, s.media_grid[mi], r, lam, t1, t2);
     float len = length(r.d);
     MedRng g = medium_rng(r.o, r.d, lam);
     if (m.type == RT_MEDIUM_CONSTANT) {
@@ -1258,6 +1387,7 @@ static float medium_transmittance(const Scene& s, int mi, const Ray& r, float tm
     if (!bound_hit(s, mi, r, t1 + 0.0001f, INFINITY, &t2)) return 1.0f;
     float a = rmax(rmax(t1, 0.0f), tmin), b = rmin(t2, tmax);
     if (a >= b) return 1.0f;
+    if (m.type == RT_MEDIUM_GRID) return grid_transmittance(m, s.media_grid[mi], r, a, b, tmax);
     float len = length(r.d);
     float l = (b - a) * len;
     if (m.type == RT_MEDIUM_CONSTANT) return std::exp(-m.density * l);
@@ -2564,7 +2694,7 @@ static int scene_create(const RtSceneDesc* d, Scene** out) {
     if (d->n_media < 0 || (d->n_media > 0 && !d->media)) { delete s; g_err = "bad media list"; return RT_ERR_INVALID; }
     for (int32_t i = 0; i < d->n_media; i++) {
         RtMedium m = d->media[i];
-        bool ok = (m.type == RT_MEDIUM_CONSTANT || m.type == RT_MEDIUM_NOISE) &&
+        bool ok = (m.type == RT_MEDIUM_CONSTANT || m.type == RT_MEDIUM_NOISE || m.type == RT_MEDIUM_GRID) &&
                   (m.boundary == RT_BOUND_SPHERE || m.boundary == RT_BOUND_BOX) && std::isfinite(m.density) &&
                   m.density >= 0.0f;
         if (m.boundary == RT_BOUND_SPHERE) ok = ok && m.radius > 0.0f;
@@ -2594,8 +2724,46 @@ static int scene_create(const RtSceneDesc* d, Scene** out) {
                 qs.push_back(Q);
             }
         }
+        Scene::GridMed G;
+        if (m.type == RT_MEDIUM_GRID) {
+            bool gok = m.boundary == RT_BOUND_BOX && m.grid != nullptr;
+            for (int a = 0; a < 3; a++) gok = gok && m.grid_res[a] >= 1 && m.grid_res[a] <= RT_GRID_MAX_RES;
+            if (!gok) { delete s; g_err = "invalid grid medium " + std::to_string(i); return RT_ERR_INVALID; }
+            size_t nv = (size_t)m.grid_res[0] * m.grid_res[1] * m.grid_res[2];
+            G.grid.assign(m.grid, m.grid + nv);
+            for (float v : G.grid)
+                if (!(v >= 0.0f) || !std::isfinite(v)) { delete s; g_err = "grid voxel values must be finite and >= 0"; return RT_ERR_INVALID; }
+            for (int a = 0; a < 3; a++) { G.res[a] = m.grid_res[a]; G.nb[a] = (G.res[a] + GRID_BRICK - 1) / GRID_BRICK; }
+            G.major.assign((size_t)G.nb[0] * G.nb[1] * G.nb[2], 0.0f);
+            for (int bz = 0; bz < G.nb[2]; bz++)
+                for (int by = 0; by < G.nb[1]; by++)
+                    for (int bx = 0; bx < G.nb[0]; bx++) {
+                        const int b[3] = {bx, by, bz};
+                        int lo[3], hi[3];
+                        for (int a = 0; a < 3; a++) {
+                            lo[a] = std::max(b[a] * GRID_BRICK - 1, 0);
+                            hi[a] = std::min(b[a] * GRID_BRICK + GRID_BRICK, G.res[a] - 1);
+                        }
+                        float mx = 0.0f;
+                        for (int z = lo[2]; z <= hi[2]; z++)
+                            for (int y = lo[1]; y <= hi[1]; y++)
+                                for (int x = lo[0]; x <= hi[0]; x++)
+                                    mx = rmax(mx, G.grid[((size_t)z * G.res[1] + y) * G.res[0] + x]);
+                        G.major[((size_t)bz * G.nb[1] + by) * G.nb[0] + bx] = mx * 1.00000095367431640625f;
+                    }
+            V3 mn = v3(rmin(m.p_min[0], m.p_max[0]), rmin(m.p_min[1], m.p_max[1]), rmin(m.p_min[2], m.p_max[2]));
+            V3 mx = v3(rmax(m.p_min[0], m.p_max[0]), rmax(m.p_min[1], m.p_max[1]), rmax(m.p_min[2], m.p_max[2]));
+            V3 ext = mx - mn;
+            G.lo = mn;
+            G.inv_vox = v3((float)G.res[0] / ext.x, (float)G.res[1] / ext.y, (float)G.res[2] / ext.z);
+            G.bw = v3(ext.x / (float)G.res[0] * GRID_BRICK, ext.y / (float)G.res[1] * GRID_BRICK,
+                      ext.z / (float)G.res[2] * GRID_BRICK);
+            G.inv_bw = v3(1.0f / G.bw.x, 1.0f / G.bw.y, 1.0f / G.bw.z);
+            m.grid = nullptr;                 // the scene keeps its own copy
+        }
         s->media.push_back(m);
         s->media_quads.push_back(qs);
+        s->media_grid.push_back(std::move(G));
     }
     // analytic convex solids (diamond.rs:93-195)
     if (d->n_convex < 0 || (d->n_convex > 0 && (!d->convex || !d->convex_planes))) {

@@ -99,7 +99,7 @@ class RtBackground(C.Structure):
     ]
 
 
-RT_MEDIUM_CONSTANT, RT_MEDIUM_NOISE = 0, 1
+RT_MEDIUM_CONSTANT, RT_MEDIUM_NOISE, RT_MEDIUM_GRID = 0, 1, 2
 RT_BOUND_SPHERE, RT_BOUND_BOX = 0, 1
 
 
@@ -118,6 +118,8 @@ class RtMedium(C.Structure):
         ("threshold", C.c_float),
         ("perlin_vec", C.c_float * (256 * 3)),
         ("perlin_perm", C.c_int32 * (3 * 256)),
+        ("grid", C.c_void_p),
+        ("grid_res", C.c_int32 * 3),
     ]
 
 
@@ -227,7 +229,8 @@ class RtTuning(C.Structure):
     """RtTuning (include/rt_api.h): path-pool capacity, launch grids and the
     device loops' limits (0 = built-in)."""
     _fields_ = [("max_paths", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32), ("shade_blocks_per_sm", C.c_uint32),
-                ("max_iterations", C.c_uint32), ("stack_limit", C.c_uint32), ("stack_ring", C.c_uint32)]
+                ("max_iterations", C.c_uint32), ("stack_limit", C.c_uint32), ("stack_ring", C.c_uint32),
+                ("node_format", C.c_uint32)]
 
 
 class RtGuideParams(C.Structure):
@@ -290,6 +293,7 @@ def iptr(a):
 
 
 RT_EMIT_DISK, RT_EMIT_QUAD, RT_EMIT_SUN, RT_EMIT_LIGHT = 0, 1, 2, 3
+RT_NODES_QUANTISED, RT_NODES_FULL = 0, 1
 RT_MAX_EMITTERS = 8
 
 

@@ -2,8 +2,10 @@
 renderer runs a fixed rayon row loop, renderer.rs:684).
 
 The knobs are rt_set_tuning's: the path-pool capacity (how many paths are in
-flight; memory, and how long the final drain runs on a partial wavefront) and
-the grids of the persistent traversal kernels and of the shading kernels.
+flight; memory, and how long the final drain runs on a partial wavefront),
+the grids of the persistent traversal kernels and of the shading kernels, and
+the node layout the traversal reads (8-bit quantised 128-byte nodes or the
+reference's 224-byte float nodes).
 Every path draws its random numbers from (pixel, sample), so the knobs change
 speed and memory, never the image.  The tuner times each candidate on a short
 render of the frame it will serve (a probe of at most PROBE_SAMPLES path
@@ -17,7 +19,8 @@ import math
 
 from . import abi
 
-SPACE = {"max_paths": (1 << 21, 1 << 22, 1 << 23), "trace_blocks_per_sm": (4, 6), "shade_blocks_per_sm": (4, 8, 16)}
+SPACE = {"max_paths": (1 << 21, 1 << 22, 1 << 23), "trace_blocks_per_sm": (4, 6), "shade_blocks_per_sm": (4, 8, 16),
+         "node_format": (0, 1)}
 PROBE_SAMPLES = 1 << 24
 _cache = {}
 

@@ -16,6 +16,7 @@ The Perlin noise is the lattice-gradient noise of src/perlin.rs:21-92 (random
 unit gradients, three 256-entry permutations, Hermite-smoothed trilinear
 interpolation), seeded from numpy instead of thread_rng.
 """
+import functools
 import math
 
 import numpy as np
@@ -188,6 +189,36 @@ def icosphere_scene(width=1920, height=1080, spp=64, max_depth=12, hero=4, seed=
                     name=f"icosphere{levels} {len(Fc)} tris {width}x{height} {spp}spp depth{max_depth} hero{hero}",
                     n_tris=len(Fc), sun_dir=sun)
     return sb, settings
+
+
+def perlin_density_grid(res=128, seed=7, freq=4.0, octaves=4, empty=0.1):
+    """A res³ grid (z, y, x) of fractal Perlin noise at the voxel centres of the
+    unit cube, mapped to [0, 1]: the lowest `empty` fraction of the voxels is 0
+    (clear gaps), the 99.5th percentile and above is 1.  (Cached: a copy.)"""
+    return _density_grid(res, seed, freq, octaves, empty).copy()
+
+
+@functools.lru_cache(maxsize=4)
+def _density_grid(res, seed, freq, octaves, empty):
+    per = Perlin(seed)
+    c = (np.arange(res) + 0.5) / res
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    P = np.stack([x.ravel(), y.ravel(), z.ravel()], 1) * freq
+    n = per.fbm(P, octaves).reshape(res, res, res)
+    lo, hi = np.quantile(n, [empty, 0.995])
+    return np.clip((n - lo) / (hi - lo), 0.0, 1.0).astype(F32)
+
+
+def grid_box_scene(width=128, height=128, spp=16, max_depth=24, hero=4, seed=5, res=32, sigma_max=4.0):
+    """The box room with a voxel-grid medium in its lower half: a res³
+    fractal-noise grid scaled to σ_t ∈ [0, sigma_max], albedo 0.9, HG g = 0.3."""
+    sb, st = box_scene(width, height, spp, max_depth, hero, seed)
+    sb.name = "grid box"
+    sb.spheres.clear()
+    sb.add_medium("grid", "box", sigma_max, (0.9, 0.9, 0.9), g=0.3, p_min=(0.0, 0.0, 0.0), p_max=(1.0, 0.5, 1.0),
+                  grid=perlin_density_grid(res, seed=seed))
+    st["name"] = f"grid box {res}^3 {width}x{height} {spp}spp depth{max_depth} hero{hero}"
+    return sb, st
 
 
 def media_box_scene(width=256, height=256, spp=16, max_depth=24, hero=4, seed=5, density=4.0):
@@ -488,15 +519,17 @@ def gem_room_scene(width=1200, height=800, spp=128, max_depth=50, photons=500_00
 
 
 def guided_box_scene(width=1280, height=720, spp=64, max_depth=24, hero=4, seed=9, density=4.0, gem=True,
-                     medium=True):
+                     medium=True, grid_res=128):
     """The hard-transport workload of the learned proposal: the box room with
     its light hidden above two occluding quads that leave a 0.05-wide slit, a
-    round brilliant (the gem workload's, radius 0.12, diamond dispersion) and a
-    Perlin-noise medium in the lower half (σ_t up to `density`, albedo 0.9,
-    g = 0.3; the reference's noise medium, volume.rs, stands in for a 128³
-    density grid).  Light enters the room only through the slit, as a narrow
-    beam onto the floor and the medium; everything else is lit by that patch,
-    which cosine bounces find rarely and light sampling cannot reach."""
+    57-facet round brilliant (radius 0.12, diamond dispersion) and a 128³
+    fractal-Perlin density grid in the lower half (σ_t ∈ [0, density], albedo
+    0.9, g = 0.3; delta tracking against per-brick majorants, ratio-tracked
+    shadows).  grid_res = 0 puts the reference's procedural noise medium
+    (volume.rs) there instead.  Light enters the room only through the slit,
+    as a narrow beam onto the floor and the medium; everything else is lit by
+    that patch, which cosine bounces find rarely and light sampling cannot
+    reach."""
     sb, st = box_scene(width, height, spp, max_depth, hero, seed)
     sb.name = "guided box"
     sb.spheres.clear()
@@ -515,12 +548,17 @@ def guided_box_scene(width=1280, height=720, spp=64, max_depth=24, hero=4, seed=
         V, Fc = round_brilliant(radius=0.12, center=(0.68, 0.62, 0.45))
         diamond = sb.add_material(Material.spectral_dielectric_cauchy(2.351, 0.0230))
         sb.add_mesh(V, Fc, diamond)
-    if medium:
+    if medium and grid_res:
+        sb.add_medium("grid", "box", density, (0.9, 0.9, 0.9), g=0.3, p_min=(0.0, 0.0, 0.0), p_max=(1.0, 0.5, 1.0),
+                      grid=perlin_density_grid(grid_res, seed=seed))
+    elif medium:
         sb.add_medium("noise", "box", density, (0.9, 0.9, 0.9), g=0.3, noise_scale=4.0, threshold=0.05,
                       p_min=(0.0, 0.0, 0.0), p_max=(1.0, 0.5, 1.0), seed=seed)
-    st["name"] = f"guided box (slit light, gem, medium) {width}x{height} {spp}spp depth{max_depth} hero{hero}"
+    st["name"] = (f"guided box (slit light, gem, {grid_res}^3 grid medium) {width}x{height} {spp}spp "
+                  f"depth{max_depth} hero{hero}")
     return sb, st
 
 
-CONFIGS = {"box": box_scene, "icosphere": icosphere_scene, "media_box": media_box_scene, "gem": gem_scene,
+CONFIGS = {"box": box_scene, "icosphere": icosphere_scene, "media_box": media_box_scene, "grid_box": grid_box_scene,
+           "gem": gem_scene,
            "gem_room": gem_room_scene, "guided_box": guided_box_scene}

@@ -83,7 +83,15 @@ struct DevMedium {
     float3 color;
     const float4* vec;           // 256 Perlin vectors
     const int32_t* perm;         // 3 × 256 permutations
+    // grid medium: σ_t = density × trilinear(grid) over the box [lo, lo + 1/inv_vox·res];
+    // major holds per brick of RT_GRID_BRICK³ voxels the largest voxel value the
+    // brick's trilinear lookups read (one voxel of apron), slightly enlarged
+    const float* grid;
+    const float* major;
+    int res[3], nb[3];
+    float3 lo, inv_vox, bw, inv_bw;   // box corner, voxels per unit, brick width, bricks per unit
 };
+#define RT_GRID_BRICK 8
 
 // A texture (texture.rs): an 8-bit RGB image, or a Perlin mottle between two colours
 struct DevTexture {
@@ -97,6 +105,10 @@ struct DevTexture {
 
 struct DevScene {
     const float4* nodes;
+    // the same nodes with 8-bit child boxes, 8 float4 each (see encode_qnode),
+    // and which copy the traversal reads (RT_NODES_*)
+    const float4* qnodes;
+    int node_format;
     const float4* tri;
     const float4* tri_n;
     const float4* quad;

@@ -173,6 +173,82 @@ static inline float area(const Box& b) {
 // Reference-layout node (bvh.rs:25-32).
 struct RefNode { float mn[3][8], mx[3][8]; int32_t ch[8]; };
 
+// ── quantised node (128 B): the child boxes as 8-bit offsets from the node's
+// lower corner p in steps of s = 2^e per axis, rounded outward so that the
+// real planes p + q·s contain the exact child box (Ylitie et al. 2017 store
+// child boxes this way; the rounding here is made conservative so the hits
+// stay the brute-force ones).  Layout (float4 words):
+//   0: p.x, p.y, p.z, (e_x + 127) | (e_y + 127) << 8 | (e_z + 127) << 16 | valid-slot mask << 24
+//   1-3: per axis x, y, z: q_lo of slots 0-3, 4-7, then q_hi of slots 0-3, 4-7 (a byte each)
+//   4-5: the 8 child references (as in the full node); 6-7: unused
+// x − y rounded down / up, exactly (TwoSum gives the rounding error of x − y)
+static inline float sub_dir(float x, float y, bool up) {
+    float a = x, b = -y;
+    float sm = a + b, bb = sm - a;
+    float err = (a - (sm - bb)) + (b - bb);
+    if (up) return err > 0.0f ? std::nextafter(sm, INFINITY) : sm;
+    return err < 0.0f ? std::nextafter(sm, -INFINITY) : sm;
+}
+// quantise one node; false when an extent needs a step beyond 2^60 (steps are
+// kept in [2^-60, 2^60], so with |1/d| in [2^-60, 2^60] every s/d is a normal float)
+static bool encode_qnode(const RefNode& r, const float4* full, float4* out) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    uint32_t valid = 0;
+    for (int c = 0; c < 8; c++) {
+        if (r.ch[c] == INT32_MIN) continue;
+        valid |= 1u << c;
+        for (int a = 0; a < 3; a++) { lo[a] = std::fmin(lo[a], r.mn[a][c]); hi[a] = std::fmax(hi[a], r.mx[a][c]); }
+    }
+    if (!valid) for (int a = 0; a < 3; a++) lo[a] = hi[a] = 0.0f;
+    int e[3];
+    bool flat[3];
+    int e_any = -60;
+    for (int a = 0; a < 3; a++) {
+        float ext = sub_dir(hi[a], lo[a], true);
+        flat[a] = !(ext > 0.0f);
+        if (flat[a]) continue;
+        int ex;
+        std::frexp(ext / 255.0f, &ex);              // ext/255 < 2^ex
+        while (ex > -60 && std::ldexp(255.0f, ex - 1) >= ext) ex--;
+        while (std::ldexp(255.0f, ex) < ext) ex++;
+        e[a] = std::max(ex, -60);                    // steps of at least 2^-60
+        e_any = std::max(e_any, e[a]);
+    }
+    for (int a = 0; a < 3; a++) {
+        if (flat[a]) e[a] = e_any;
+        if (e[a] > 60) return false;
+    }
+    uint8_t qlo[3][8], qhi[3][8];
+    for (int a = 0; a < 3; a++) {
+        float sa = std::ldexp(1.0f, e[a]);
+        for (int c = 0; c < 8; c++) {
+            if (!((valid >> c) & 1u)) { qlo[a][c] = 255; qhi[a][c] = 0; continue; }
+            float dl = sub_dir(r.mn[a][c], lo[a], false), dh = sub_dir(r.mx[a][c], lo[a], true);
+            float ql = std::floor(dl / sa), qh = std::ceil(dh / sa);
+            qlo[a][c] = (uint8_t)std::min(std::max(ql, 0.0f), 255.0f);
+            qhi[a][c] = (uint8_t)std::min(std::max(qh, 0.0f), 255.0f);
+        }
+    }
+    uint32_t meta = (uint32_t)(e[0] + 127) | (uint32_t)(e[1] + 127) << 8 | (uint32_t)(e[2] + 127) << 16 | valid << 24;
+    float fm;
+    memcpy(&fm, &meta, 4);
+    out[0] = make_float4(lo[0], lo[1], lo[2], fm);
+    for (int a = 0; a < 3; a++) {
+        uint32_t w[4] = {0, 0, 0, 0};
+        for (int c = 0; c < 8; c++) {
+            w[c >> 2] |= (uint32_t)qlo[a][c] << (8 * (c & 3));
+            w[2 + (c >> 2)] |= (uint32_t)qhi[a][c] << (8 * (c & 3));
+        }
+        float f[4];
+        memcpy(f, w, 16);
+        out[1 + a] = make_float4(f[0], f[1], f[2], f[3]);
+    }
+    out[4] = full[12];
+    out[5] = full[13];
+    out[6] = out[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+    return true;
+}
+
 // ── binned-SAH 8-wide builder (cost model of bvh.rs:52-174) ─────────────────
 // In place on an index array: each partition reorders idx[lo, hi) by a stable
 // counting sort on bucket id, which is what the reference's stable
@@ -505,6 +581,7 @@ struct RtScene {
     int64_t n_nodes = 0, n_leaves = 0, n_prims = 0;
     int32_t max_depth = 0;
     int stack_cap_built = 0;          // traversal stack entries the spill columns hold
+    bool qnodes_ok = false;           // the quantised node copy exists (extents within 255·2^60)
     std::vector<DevLight> h_lights;   // host copy of the NEE light list (photon emitters from lights)
     std::vector<float> h_emission;    // per material: RGB emission of a light material (3 floats)
     float photon_stage_ms[3] = {0, 0, 0};   // last photon build: trace, compaction, tree
@@ -1040,6 +1117,17 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         if ((rc = upload(s, wpl.data(), wpl.size(), &s->S.cvx_planes))) return bail(rc);
         if ((rc = upload(s, wsh.data(), wsh.size(), &s->S.cvx_shade))) return bail(rc);
         if ((rc = upload(s, gnodes.data(), gnodes.size(), &s->S.nodes))) return bail(rc);
+        {   // the quantised copy of the nodes (rt_set_tuning node_format 0, the default)
+            std::vector<float4> qn((size_t)s->n_nodes * 8);
+            bool qok = true;
+            for (int64_t k = 0; k < s->n_nodes && qok; k++)
+                qok = encode_qnode(s->ref_nodes[k], &gnodes[(size_t)k * 14], &qn[(size_t)k * 8]);
+            if (qok) {
+                if ((rc = upload(s, qn.data(), qn.size(), &s->S.qnodes))) return bail(rc);
+                s->qnodes_ok = true;
+            }
+            s->S.node_format = qok ? RT_NODES_QUANTISED : RT_NODES_FULL;
+        }
         if ((rc = upload(s, gtri.data(), gtri.size(), &s->S.tri))) return bail(rc);
         if ((rc = upload(s, gtri_n.data(), gtri_n.size(), &s->S.tri_n))) return bail(rc);
         if (!gtri_uv.empty()) {
@@ -1168,10 +1256,17 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         std::vector<DevMedium> dm(d->n_media);
         for (int32_t i = 0; i < d->n_media; i++) {
             const RtMedium& m = d->media[i];
-            bool ok = (m.type == RT_MEDIUM_CONSTANT || m.type == RT_MEDIUM_NOISE) &&
+            bool ok = (m.type == RT_MEDIUM_CONSTANT || m.type == RT_MEDIUM_NOISE || m.type == RT_MEDIUM_GRID) &&
                       (m.boundary == RT_BOUND_SPHERE || m.boundary == RT_BOUND_BOX) && std::isfinite(m.density) &&
                       m.density >= 0.0f && (m.boundary != RT_BOUND_SPHERE || m.radius > 0.0f);
             if (!ok) return bail(fail(s, RT_ERR_INVALID, "invalid medium " + std::to_string(i)));
+            if (m.type == RT_MEDIUM_GRID) {
+                bool gok = m.boundary == RT_BOUND_BOX && m.grid != nullptr;
+                for (int a = 0; a < 3; a++) gok = gok && m.grid_res[a] >= 1 && m.grid_res[a] <= RT_GRID_MAX_RES;
+                if (!gok)
+                    return bail(fail(s, RT_ERR_INVALID, "grid medium " + std::to_string(i) +
+                                                            " needs a box boundary, a grid and 1 .. 1024 voxels per axis"));
+            }
             DevMedium& g = dm[i];
             memset(&g, 0, sizeof(g));
             g.type = m.type;
@@ -1217,6 +1312,47 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
             }
             if ((rc = upload(s, vec.data(), vec.size(), &g.vec))) return bail(rc);
             if ((rc = upload(s, perm.data(), perm.size(), &g.perm))) return bail(rc);
+            if (m.type == RT_MEDIUM_GRID) {
+                // voxels, and per brick of RT_GRID_BRICK³ voxels the largest value its
+                // trilinear lookups read: voxels 8b − 1 .. 8b + 8 on each axis
+                const int R[3] = {m.grid_res[0], m.grid_res[1], m.grid_res[2]};
+                size_t nv = (size_t)R[0] * R[1] * R[2];
+                for (size_t v = 0; v < nv; v++)
+                    if (!(m.grid[v] >= 0.0f) || !std::isfinite(m.grid[v]))
+                        return bail(fail(s, RT_ERR_INVALID, "grid medium " + std::to_string(i) +
+                                                                ": voxel values must be finite and ≥ 0"));
+                int NB[3];
+                for (int a = 0; a < 3; a++) NB[a] = (R[a] + RT_GRID_BRICK - 1) / RT_GRID_BRICK;
+                std::vector<float> major((size_t)NB[0] * NB[1] * NB[2], 0.0f);
+                for (int bz = 0; bz < NB[2]; bz++)
+                    for (int by = 0; by < NB[1]; by++)
+                        for (int bx = 0; bx < NB[0]; bx++) {
+                            const int b[3] = {bx, by, bz};
+                            int lo[3], hi[3];
+                            for (int a = 0; a < 3; a++) {
+                                lo[a] = std::max(b[a] * RT_GRID_BRICK - 1, 0);
+                                hi[a] = std::min(b[a] * RT_GRID_BRICK + RT_GRID_BRICK, R[a] - 1);
+                            }
+                            float mx = 0.0f;
+                            for (int z = lo[2]; z <= hi[2]; z++)
+                                for (int y = lo[1]; y <= hi[1]; y++)
+                                    for (int x = lo[0]; x <= hi[0]; x++)
+                                        mx = std::fmax(mx, m.grid[((size_t)z * R[1] + y) * R[0] + x]);
+                            // enlarged by 2^-20 so the interpolation's rounding stays below it
+                            major[((size_t)bz * NB[1] + by) * NB[0] + bx] = mx * 1.00000095367431640625f;
+                        }
+                if ((rc = upload(s, m.grid, nv, &g.grid))) return bail(rc);
+                if ((rc = upload(s, major.data(), major.size(), &g.major))) return bail(rc);
+                H3 mn = h3(std::fmin(m.p_min[0], m.p_max[0]), std::fmin(m.p_min[1], m.p_max[1]), std::fmin(m.p_min[2], m.p_max[2]));
+                H3 mx = h3(std::fmax(m.p_min[0], m.p_max[0]), std::fmax(m.p_min[1], m.p_max[1]), std::fmax(m.p_min[2], m.p_max[2]));
+                H3 ext = mx - mn;
+                for (int a = 0; a < 3; a++) { g.res[a] = R[a]; g.nb[a] = NB[a]; }
+                g.lo = make_float3(mn.x, mn.y, mn.z);
+                g.inv_vox = make_float3((float)R[0] / ext.x, (float)R[1] / ext.y, (float)R[2] / ext.z);
+                g.bw = make_float3(ext.x / (float)R[0] * RT_GRID_BRICK, ext.y / (float)R[1] * RT_GRID_BRICK,
+                                   ext.z / (float)R[2] * RT_GRID_BRICK);
+                g.inv_bw = make_float3(1.0f / g.bw.x, 1.0f / g.bw.y, 1.0f / g.bw.z);
+            }
             // media join the photon bounds (volume.rs:152-154)
             for (int a = 0; a < 3; a++) {
                 bool first = s->empty && i == 0;
@@ -1931,6 +2067,10 @@ extern "C" int32_t rt_set_tuning(RtScene* s, const RtTuning* t) {
         return fail(s, RT_ERR_INVALID, "trace_blocks_per_sm must be in 0..8, shade_blocks_per_sm in 0..32");
     if (t->stack_ring != 0 && (t->stack_ring > RT_SHORT_STACK || (t->stack_ring & (t->stack_ring - 1)) != 0))
         return fail(s, RT_ERR_INVALID, "stack_ring must be 0 or a power of two up to " + std::to_string(RT_SHORT_STACK));
+    if (t->node_format != RT_NODES_QUANTISED && t->node_format != RT_NODES_FULL)
+        return fail(s, RT_ERR_INVALID, "node_format must be RT_NODES_QUANTISED or RT_NODES_FULL");
+    if (t->node_format == RT_NODES_QUANTISED && !s->qnodes_ok && !s->empty)
+        return fail(s, RT_ERR_INVALID, "the scene's extents exceed the quantised node layout");
     if (t->stack_limit != 0 && (int64_t)t->stack_limit > s->stack_cap_built)
         return fail(s, RT_ERR_INVALID, "stack_limit must be 0 or at most " + std::to_string(s->stack_cap_built) +
                                            " (the entries the scene's stack columns hold)");
@@ -1942,6 +2082,7 @@ extern "C" int32_t rt_set_tuning(RtScene* s, const RtTuning* t) {
     s->max_iterations = t->max_iterations;
     s->S.stack_cap = t->stack_limit ? (int)t->stack_limit : s->stack_cap_built;
     s->S.stack_ring = t->stack_ring ? (int)t->stack_ring : RT_SHORT_STACK;
+    s->S.node_format = (s->qnodes_ok && t->node_format == RT_NODES_QUANTISED) ? RT_NODES_QUANTISED : RT_NODES_FULL;
     return RT_OK;
 }
 
@@ -1959,6 +2100,7 @@ extern "C" int32_t rt_get_tuning(const RtScene* s, RtTuning* t) {
     t->max_iterations = (uint32_t)s->max_iterations;
     t->stack_limit = (uint32_t)s->S.stack_cap;
     t->stack_ring = (uint32_t)s->S.stack_ring;
+    t->node_format = (uint32_t)s->S.node_format;
     return RT_OK;
 }
 

@@ -1,7 +1,8 @@
 // rt_media.cuh — participating media on the device (volume.rs:39-263,
 // perlin.rs:35-91): the ray-keyed random stream, Perlin turbulence, boundary
 // intervals, free-flight sampling (constant: exponential; noise: delta
-// tracking to the density scale), shadow transmittance and the HG phase
+// tracking to the density scale; grid: delta tracking against per-brick
+// majorants), shadow transmittance (grid: ratio tracking) and the HG phase
 // function.  The CPU oracle restates the same functions (oracle/rt_oracle.cpp).
 #pragma once
 #include "../../include/rt_api.h"
@@ -78,6 +79,133 @@ RT_D bool bound_hit(const DevMedium& m, float3 o, float3 d, float tmin, float tm
     return any;
 }
 
+// ── grid medium (no counterpart in the reference) ────────────────────────────
+// σ_t(x) = density × trilinear interpolation of the voxel values between voxel
+// centres, clamped at the box faces.
+RT_D float grid_density_at(const DevMedium& m, float3 p) {
+    const float c[3] = {(p.x - m.lo.x) * m.inv_vox.x - 0.5f, (p.y - m.lo.y) * m.inv_vox.y - 0.5f,
+                        (p.z - m.lo.z) * m.inv_vox.z - 0.5f};
+    int i0[3], i1[3];
+    float f[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        float u = fminf(fmaxf(c[a], 0.0f), (float)(m.res[a] - 1));
+        int i = min((int)u, max(m.res[a] - 2, 0));
+        i0[a] = i;
+        i1[a] = min(i + 1, m.res[a] - 1);
+        f[a] = u - (float)i;
+    }
+    auto at = [&](int i, int j, int k) { return __ldg(m.grid + ((size_t)k * m.res[1] + j) * m.res[0] + i); };
+    float c00 = at(i0[0], i0[1], i0[2]) * (1.0f - f[0]) + at(i1[0], i0[1], i0[2]) * f[0];
+    float c10 = at(i0[0], i1[1], i0[2]) * (1.0f - f[0]) + at(i1[0], i1[1], i0[2]) * f[0];
+    float c01 = at(i0[0], i0[1], i1[2]) * (1.0f - f[0]) + at(i1[0], i0[1], i1[2]) * f[0];
+    float c11 = at(i0[0], i1[1], i1[2]) * (1.0f - f[0]) + at(i1[0], i1[1], i1[2]) * f[0];
+    float c0 = c00 * (1.0f - f[1]) + c10 * f[1], c1 = c01 * (1.0f - f[1]) + c11 * f[1];
+    return m.density * (c0 * (1.0f - f[2]) + c1 * f[2]);
+}
+
+// 3-D DDA over the majorant bricks (Amanatides & Woo 1987) from the point at t0
+struct BrickWalk { int b[3], step[3]; float tnext[3], dt[3]; };
+RT_D void brick_walk_init(const DevMedium& m, float3 o, float3 d, float t0, BrickWalk& w) {
+    float3 p = ray_at(o, d, t0);
+    const float pc[3] = {p.x, p.y, p.z}, oc[3] = {o.x, o.y, o.z}, dc[3] = {d.x, d.y, d.z};
+    const float lo[3] = {m.lo.x, m.lo.y, m.lo.z}, bw[3] = {m.bw.x, m.bw.y, m.bw.z};
+    const float ib[3] = {m.inv_bw.x, m.inv_bw.y, m.inv_bw.z};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        int b = (int)floorf((pc[a] - lo[a]) * ib[a]);
+        b = min(max(b, 0), m.nb[a] - 1);
+        w.b[a] = b;
+        if (dc[a] > 0.0f) {
+            w.step[a] = 1;
+            w.tnext[a] = (lo[a] + (float)(b + 1) * bw[a] - oc[a]) / dc[a];
+            w.dt[a] = bw[a] / dc[a];
+        } else if (dc[a] < 0.0f) {
+            w.step[a] = -1;
+            w.tnext[a] = (lo[a] + (float)b * bw[a] - oc[a]) / dc[a];
+            w.dt[a] = -bw[a] / dc[a];
+        } else {
+            w.step[a] = 0;
+            w.tnext[a] = INFINITY;
+            w.dt[a] = INFINITY;
+        }
+    }
+}
+// end of the current brick's segment; false when the walk left the grid
+RT_D bool brick_walk_next(const DevMedium& m, BrickWalk& w) {
+    int a = w.tnext[0] <= w.tnext[1] ? (w.tnext[0] <= w.tnext[2] ? 0 : 2) : (w.tnext[1] <= w.tnext[2] ? 1 : 2);
+    w.b[a] += w.step[a];
+    w.tnext[a] += w.dt[a];
+    return w.b[a] >= 0 && w.b[a] < m.nb[a];
+}
+RT_D float brick_major(const DevMedium& m, const BrickWalk& w) {
+    return m.density * __ldg(m.major + ((size_t)w.b[2] * m.nb[1] + w.b[1]) * m.nb[0] + w.b[0]);
+}
+#define RT_GRID_MAX_STEPS 4096u   // tentative collisions per ray (bounded device loop)
+
+// Delta tracking (Woodcock) in [t1, t2] against each brick's majorant: the
+// scatter distance, or INFINITY when the ray leaves the box first.
+RT_D float grid_sample(const DevMedium& m, float3 o, float3 d, float lam, float t1, float t2) {
+    MedRng g = medium_rng(o, d, lam);
+    float len = sqrtf(dot3(d, d));
+    BrickWalk w;
+    brick_walk_init(m, o, d, t1, w);
+    float t = t1;
+    uint32_t k = 0;
+    for (int seg = 0; seg < 3 * RT_GRID_MAX_RES / RT_GRID_BRICK + 4; seg++) {
+        float tb = fminf(fminf(w.tnext[0], w.tnext[1]), fminf(w.tnext[2], t2));
+        float mu = brick_major(m, w);
+        if (mu > 0.0f) {
+            float inv = 1.0f / (mu * len);
+            while (k < RT_GRID_MAX_STEPS) {
+                float tt = t - inv * logf(fmaxf(medium_rnd(g, 2u * k), 1.1920928955078125e-07f));
+                float xi = medium_rnd(g, 2u * k + 1u);
+                k++;
+                if (tt >= tb) break;
+                t = tt;
+                if (xi * mu < grid_density_at(m, ray_at(o, d, t))) return t;
+            }
+            if (k >= RT_GRID_MAX_STEPS) return INFINITY;
+        }
+        if (tb >= t2) return INFINITY;
+        t = fmaxf(t, tb);
+        if (!brick_walk_next(m, w)) return INFINITY;
+    }
+    return INFINITY;
+}
+
+// Ratio tracking (Cramer 1978; Novák et al. 2014) over [a, b]: the product of
+// (1 − σ_t/μ) at tentative collisions, an unbiased estimate of exp(−∫σ_t).
+// Its random stream is keyed on the shadow ray's bits and t_max.
+RT_D float grid_transmittance(const DevMedium& m, float3 o, float3 d, float a, float b, float tmax) {
+    MedRng g = medium_rng(o, d, tmax);
+    float len = sqrtf(dot3(d, d));
+    BrickWalk w;
+    brick_walk_init(m, o, d, a, w);
+    float t = a, T = 1.0f;
+    uint32_t k = 0;
+    for (int seg = 0; seg < 3 * RT_GRID_MAX_RES / RT_GRID_BRICK + 4; seg++) {
+        float tb = fminf(fminf(w.tnext[0], w.tnext[1]), fminf(w.tnext[2], b));
+        float mu = brick_major(m, w);
+        if (mu > 0.0f) {
+            float inv = 1.0f / (mu * len);
+            while (k < RT_GRID_MAX_STEPS) {
+                float tt = t - inv * logf(fmaxf(medium_rnd(g, 0x40000u + k), 1.1920928955078125e-07f));
+                k++;
+                if (tt >= tb) break;
+                t = tt;
+                T *= fmaxf(1.0f - grid_density_at(m, ray_at(o, d, t)) / mu, 0.0f);
+                if (T <= 0.0f) return 0.0f;
+            }
+            if (k >= RT_GRID_MAX_STEPS) return T;
+        }
+        if (tb >= b) return T;
+        t = fmaxf(t, tb);
+        if (!brick_walk_next(m, w)) return T;
+    }
+    return T;
+}
+
 // scatter distance for t_max = ∞ (INFINITY when the ray leaves first);
 // delta tracking is bounded at 4096 steps
 RT_D float medium_sample(const DevMedium& m, float3 o, float3 d, float lam, float tmin) {
@@ -87,6 +215,7 @@ RT_D float medium_sample(const DevMedium& m, float3 o, float3 d, float lam, floa
     if (t1 < tmin) t1 = tmin;
     if (t1 >= t2) return INFINITY;
     if (t1 < 0.0f) t1 = 0.0f;
+    if (m.type == RT_MEDIUM_GRID) return grid_sample(m, o, d, lam, t1, t2);
     float len = sqrtf(dot3(d, d));
     MedRng g = medium_rng(o, d, lam);
     if (m.type == RT_MEDIUM_CONSTANT) {
@@ -124,6 +253,7 @@ RT_D float medium_transmittance(const DevMedium& m, float3 o, float3 d, float tm
     if (!bound_hit(m, o, d, t1 + 0.0001f, INFINITY, &t2)) return 1.0f;
     float a = fmaxf(fmaxf(t1, 0.0f), tmin), b = fminf(t2, tmax);
     if (a >= b) return 1.0f;
+    if (m.type == RT_MEDIUM_GRID) return grid_transmittance(m, o, d, a, b, tmax);
     float len = sqrtf(dot3(d, d));
     float l = (b - a) * len;
     if (m.type == RT_MEDIUM_CONSTANT) return expf(-m.density * l);

@@ -142,7 +142,13 @@ struct RayC {
     float3 o, inv, invf;
     int nx, ny, nz;          // float4 offsets of the near-plane arrays in a node
     bool general;
+    bool qgeneral;           // quantised nodes: also any |1/d| outside [2^-60, 2^60]
 };
+
+RT_D bool inv_in_range(float x) {
+    float a = fabsf(x);
+    return a >= 8.673617379884035e-19f && a <= 1.152921504606846976e18f;   // 2^-60 .. 2^60
+}
 
 RT_D RayC make_rayc(float3 o, float3 d, float tmin) {
     RayC r;
@@ -151,6 +157,7 @@ RT_D RayC make_rayc(float3 o, float3 d, float tmin) {
     const float W = 1.000030517578125f;   // 1 + 2^-15
     r.invf = mk(r.inv.x * W, r.inv.y * W, r.inv.z * W);
     r.general = isinf(r.inv.x) || isinf(r.inv.y) || isinf(r.inv.z) || !(tmin >= 0.0f);
+    r.qgeneral = r.general || !inv_in_range(r.inv.x) || !inv_in_range(r.inv.y) || !inv_in_range(r.inv.z);
     r.nx = signbit(r.inv.x) ? 6 : 0;
     r.ny = signbit(r.inv.y) ? 8 : 2;
     r.nz = signbit(r.inv.z) ? 10 : 4;
@@ -232,6 +239,130 @@ __device__ __noinline__ uint32_t node_test_general(const DevScene& S, uint32_t n
     return mask;
 }
 
+// ── quantised nodes (8 float4: see encode_qnode in rt_host.cu) ───────────────
+// Child planes are the real numbers p + q·s (s = 2^e per axis), which contain
+// the exact child boxes.  Per ray and node, S = s/d is exact and
+// A = (p − o)/d is computed with two roundings; q·S + A then differs from the
+// exact plane distance by at most u·(255|S| + 3.02|A|) (u = 2^-24), so with
+// err = 2^-20·(|A| + 256|S|) the near distance fma(2^23 + q, S, A − err − 2^23·S)
+// rounded down is below it and the far one rounded up is above it: the
+// culling stays conservative and the hits are the brute-force ones.  The
+// byte q enters as the float 2^23 + q (one byte permute), its 2^23 folded
+// into the per-node constant.
+RT_D float qbyte(uint32_t w, uint32_t sel) { return __uint_as_float(__byte_perm(w, 0x4B000000u, sel)); }
+
+__device__ __noinline__ uint32_t qnode_test_general(const DevScene& S, uint32_t ni, const RayC& R, float tmin,
+                                                    float tmax, float* tn);
+
+RT_D uint32_t qnode_test(const DevScene& S, uint32_t ni, const RayC& R, float tmin, float tmax, float tn[8],
+                         uint32_t ch[8]) {
+    const float4* N = S.qnodes + (size_t)ni * 8;
+    float4 h = __ldg(N);
+    uint4 bq[3] = {__ldg(reinterpret_cast<const uint4*>(N + 1)), __ldg(reinterpret_cast<const uint4*>(N + 2)),
+                   __ldg(reinterpret_cast<const uint4*>(N + 3))};
+    float4 c0 = __ldg(N + 4), c1 = __ldg(N + 5);
+    const uint32_t cc[8] = {__float_as_uint(c0.x), __float_as_uint(c0.y), __float_as_uint(c0.z), __float_as_uint(c0.w),
+                            __float_as_uint(c1.x), __float_as_uint(c1.y), __float_as_uint(c1.z), __float_as_uint(c1.w)};
+#pragma unroll
+    for (int c = 0; c < 8; c++) ch[c] = cc[c];
+    const uint32_t meta = __float_as_uint(h.w);
+    if (R.qgeneral) {
+        float tg[8];
+        uint32_t m = qnode_test_general(S, ni, R, tmin, tmax, tg);
+#pragma unroll
+        for (int c = 0; c < 8; c++) tn[c] = tg[c];
+        return m;
+    }
+    const float M = 8388608.0f;                        // 2^23
+    const float P[3] = {h.x, h.y, h.z}, O[3] = {R.o.x, R.o.y, R.o.z}, I[3] = {R.inv.x, R.inv.y, R.inv.z};
+    float Sa[3], An[3], Af[3];
+    uint32_t wn[3][2], wf[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        float sa = __uint_as_float(((meta >> (8 * a)) & 0xFFu) << 23);   // 2^e
+        float Sx = sa * I[a];
+        float Ax = (P[a] - O[a]) * I[a];
+        float err = __fmul_ru(__fmaf_ru(fabsf(Sx), 256.0f, fabsf(Ax)), 9.5367431640625e-07f);   // × 2^-20
+        An[a] = __fmaf_rd(-M, Sx, __fsub_rd(Ax, err));
+        Af[a] = __fmaf_ru(-M, Sx, __fadd_ru(Ax, err));
+        Sa[a] = Sx;
+        // the near planes are the lower ones for a positive direction
+        bool neg = I[a] < 0.0f;
+        wn[a][0] = neg ? bq[a].z : bq[a].x; wn[a][1] = neg ? bq[a].w : bq[a].y;
+        wf[a][0] = neg ? bq[a].x : bq[a].z; wf[a][1] = neg ? bq[a].y : bq[a].w;
+    }
+    uint32_t mask = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const uint32_t sel = 0x7540u + (uint32_t)(c & 3);
+        float nx = __fmaf_rd(qbyte(wn[0][c >> 2], sel), Sa[0], An[0]);
+        float ny = __fmaf_rd(qbyte(wn[1][c >> 2], sel), Sa[1], An[1]);
+        float nz = __fmaf_rd(qbyte(wn[2][c >> 2], sel), Sa[2], An[2]);
+        float fx = __fmaf_ru(qbyte(wf[0][c >> 2], sel), Sa[0], Af[0]);
+        float fy = __fmaf_ru(qbyte(wf[1][c >> 2], sel), Sa[1], Af[1]);
+        float fz = __fmaf_ru(qbyte(wf[2][c >> 2], sel), Sa[2], Af[2]);
+        float t0 = fmax3f(fmaxf(tmin, nx), ny, nz);
+        float t1 = fmin3f(fminf(tmax, fx), fy, fz);
+        tn[c] = t0;
+        if (t0 <= t1) mask |= 1u << c;
+    }
+    return mask & (meta >> 24);
+}
+
+// General rays (a zero, denormal or extreme direction component, or t_min < 0):
+// the planes decoded with outward rounding, then the general slab test.
+__device__ __noinline__ uint32_t qnode_test_general(const DevScene& S, uint32_t ni, const RayC& R, float tmin,
+                                                    float tmax, float* tn) {
+    const float4* N = S.qnodes + (size_t)ni * 8;
+    float4 h = __ldg(N);
+    const uint32_t meta = __float_as_uint(h.w);
+    const float P[3] = {h.x, h.y, h.z};
+    float lo[3][8], hi[3][8];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        uint4 b = __ldg(reinterpret_cast<const uint4*>(N + 1 + a));
+        float sa = __uint_as_float(((meta >> (8 * a)) & 0xFFu) << 23);
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            uint32_t wl = c < 4 ? b.x : b.y, wh = c < 4 ? b.z : b.w;
+            float ql = (float)((wl >> (8 * (c & 3))) & 0xFFu), qh = (float)((wh >> (8 * (c & 3))) & 0xFFu);
+            lo[a][c] = __fmaf_rd(ql, sa, P[a]);
+            hi[a][c] = __fmaf_ru(qh, sa, P[a]);
+        }
+    }
+    uint32_t mask = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        float dax = (lo[0][c] - R.o.x) * R.inv.x, dbx = (hi[0][c] - R.o.x) * R.inv.x;
+        float day = (lo[1][c] - R.o.y) * R.inv.y, dby = (hi[1][c] - R.o.y) * R.inv.y;
+        float daz = (lo[2][c] - R.o.z) * R.inv.z, dbz = (hi[2][c] - R.o.z) * R.inv.z;
+        float lx = fminf(dax, dbx), hx = fmaxf(dax, dbx);
+        float ly = fminf(day, dby), hy = fmaxf(day, dby);
+        float lz = fminf(daz, dbz), hz = fmaxf(daz, dbz);
+        if (isnan(dax) || isnan(dbx)) { lx = -INFINITY; hx = INFINITY; }
+        if (isnan(day) || isnan(dby)) { ly = -INFINITY; hy = INFINITY; }
+        if (isnan(daz) || isnan(dbz)) { lz = -INFINITY; hz = INFINITY; }
+        float t0 = fmaxf(fmaxf(fmaxf(tmin, lx), ly), lz);
+        float t1 = fminf(fminf(fminf(tmax, hx), hy), hz);
+        float t1w = t1 + fabsf(t1) * SLAB_WIDEN;
+        tn[c] = t0;
+        if (t0 <= t1w) mask |= 1u << c;
+    }
+    return mask & (meta >> 24);
+}
+
+// the node test and the child-reference words of node `ni` in either copy
+template <bool QN>
+RT_D uint32_t node_test_any(const DevScene& S, uint32_t ni, const RayC& R, float tmin, float tmax, float tn[8],
+                            uint32_t ch[8]) {
+    return QN ? qnode_test(S, ni, R, tmin, tmax, tn, ch) : node_test(S, ni, R, tmin, tmax, tn, ch);
+}
+template <bool QN>
+RT_D const uint32_t* node_refs(const DevScene& S, uint32_t ni) {
+    return QN ? reinterpret_cast<const uint32_t*>(S.qnodes + (size_t)ni * 8 + 4)
+              : reinterpret_cast<const uint32_t*>(S.nodes + (size_t)ni * 14 + 12);
+}
+
 }  // namespace
 
 namespace rtk {
@@ -285,20 +416,20 @@ RT_D TStack make_stack(const DevScene& S, uint32_t* shared_ring) {
 // intersects hit leaves in slot order, then continues with the nearest hit inner
 // child (sorted by a 19-comparator network on packed (t | slot) keys) and pushes
 // the others far → near.  Returns false when the traversal is finished.
-template <bool ANA>
+template <bool ANA, bool QN>
 RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, Best& best,
                        uint32_t& node, TStack& stk, bool& ok) {
     float tn[8];
     uint32_t ch[8];
     // the closest hit so far bounds the boxes; widened like every exit distance
     float cwin = best.t + fabsf(best.t) * SLAB_WIDEN;
-    uint32_t mask = node_test(S, node, R, tmin, R.general ? best.t : cwin, tn, ch);
+    uint32_t mask = node_test_any<QN>(S, node, R, tmin, R.general ? best.t : cwin, tn, ch);
     uint32_t leaves = 0;
 #pragma unroll
     for (int c = 0; c < 8; c++) leaves |= ((ch[c] & RT_LEAF_BIT) ? 1u : 0u) << c;
     leaves &= mask;
     if (leaves) {
-        const uint32_t* refs = reinterpret_cast<const uint32_t*>(S.nodes + (size_t)node * 14 + 12);
+        const uint32_t* refs = node_refs<QN>(S, node);
 #pragma unroll 1
         while (leaves) {
             int c = __ffs(leaves) - 1;
@@ -330,7 +461,7 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
         }
         uint32_t lo = min(a, b), hi = max(a, b);
         if (!stk.room(1)) { ok = false; return false; }
-        const uint32_t* refs = reinterpret_cast<const uint32_t*>(S.nodes + (size_t)node * 14 + 12);
+        const uint32_t* refs = node_refs<QN>(S, node);
         stk.push(__ldg(refs + (hi & 7u)));
         node = __ldg(refs + (lo & 7u));
     } else if (n > 2) {
@@ -342,7 +473,7 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
         CAS(2, 4) CAS(3, 5)
         CAS(3, 4)
         if (!stk.room(n - 1)) { ok = false; return false; }
-        const uint32_t* refs = reinterpret_cast<const uint32_t*>(S.nodes + (size_t)node * 14 + 12);
+        const uint32_t* refs = node_refs<QN>(S, node);
 #pragma unroll
         for (int j = 7; j >= 1; j--)
             if (j < n) stk.push(__ldg(refs + (k[j] & 7u)));
@@ -358,13 +489,13 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
 
 // One node visit of the any-hit traversal (bvh.rs:487-530).  Returns false when
 // finished; *hit is set when a primitive was hit.
-template <bool ANA>
+template <bool ANA, bool QN>
 RT_D bool any_step(const DevScene& S, const RayC& R, float3 d, float tmin, float tmax,
                    uint32_t& node, TStack& stk, bool& hit, bool& ok) {
     float tn[8];
     uint32_t ch[8];
     float tw = tmax + fabsf(tmax) * SLAB_WIDEN;
-    uint32_t mask = node_test(S, node, R, tmin, R.general ? tmax : tw, tn, ch);
+    uint32_t mask = node_test_any<QN>(S, node, R, tmin, R.general ? tmax : tw, tn, ch);
     uint32_t inner = 0, leaves = 0;
 #pragma unroll
     for (int c = 0; c < 8; c++) {
@@ -375,7 +506,7 @@ RT_D bool any_step(const DevScene& S, const RayC& R, float3 d, float tmin, float
     leaves &= mask;
     inner &= mask;
     if (leaves) {
-        const uint32_t* refs = reinterpret_cast<const uint32_t*>(S.nodes + (size_t)node * 14 + 12);
+        const uint32_t* refs = node_refs<QN>(S, node);
 #pragma unroll 1
         while (leaves) {
             int c = __ffs(leaves) - 1;
@@ -418,7 +549,7 @@ RT_D bool nan_ray(float3 o, float3 d, float tmin, float tmax) {
 // MODE 0: wavefront extend (queue of path ids, rays in PathState, hits to PathState)
 // MODE 1: API (rays n×8 in memory, hits as int4)
 
-template <int MODE, bool ANA>
+template <int MODE, bool ANA, bool QN>
 __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevScene S, PathState P, const uint32_t* __restrict__ queue,
                                                             const float* __restrict__ rays, uint32_t n_api,
                                                             const uint32_t* count, uint32_t* next,
@@ -469,7 +600,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
         if (exhausted && __ballot_sync(FULLMASK, active) == 0) break;
         if (active) {
             bool lok = true;
-            bool more = rtk::closest_step<ANA>(S, R, d, tmin, best, node, stk, lok);
+            bool more = rtk::closest_step<ANA, QN>(S, R, d, tmin, best, node, stk, lok);
             if (!lok) ok = false;
             if (!more) {
                 active = false;
@@ -491,7 +622,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
 // MODE 1: API any-hit (occluded flags)
 // MODE 2: wavefront shadow rays in a scene with media (an unoccluded ray scales
 //         its parked contribution by the media's transmittance)
-template <int MODE, bool ANA>
+template <int MODE, bool ANA, bool QN>
 __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene S, PendTargets T, const float4* __restrict__ sq,
                                                         const float* __restrict__ rays, uint32_t n_api,
                                                         const uint32_t* count, uint32_t* next,
@@ -537,7 +668,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
         if (exhausted && __ballot_sync(FULLMASK, active) == 0) break;
         if (active) {
             bool lok = true;
-            bool more = rtk::any_step<ANA>(S, R, d, tmin, tmax, node, stk, hit, lok);
+            bool more = rtk::any_step<ANA, QN>(S, R, d, tmin, tmax, node, stk, hit, lok);
             if (!lok) ok = false;
             if (!more) {
                 active = false;
@@ -625,10 +756,17 @@ int trace_grid(const DevScene& S, int dev_sms) {
 }
 
 // the traversal kernels with (ANA) or without analytic solids
-#define RT_TRACE_LAUNCH(K, MODE, ...)                                                                    \
-    do {                                                                                                 \
-        if (S.n_analytic > 0) K<MODE, true><<<trace_grid(S, sms), RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);   \
-        else                  K<MODE, false><<<trace_grid(S, sms), RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);  \
+#define RT_TRACE_LAUNCH(K, MODE, ...)                                                                         \
+    do {                                                                                                      \
+        const int g_ = trace_grid(S, sms);                                                                    \
+        const bool q_ = S.node_format == RT_NODES_QUANTISED;                                                  \
+        if (S.n_analytic > 0) {                                                                               \
+            if (q_) K<MODE, true, true><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);                           \
+            else    K<MODE, true, false><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);                          \
+        } else {                                                                                              \
+            if (q_) K<MODE, false, true><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);                          \
+            else    K<MODE, false, false><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);                         \
+        }                                                                                                     \
     } while (0)
 void launch_trace_closest_api(const DevScene& S, const float* rays, uint32_t n, int4* out, uint32_t* next, int* err,
                               int sms, cudaStream_t st) {

@@ -391,9 +391,9 @@ class GpuScene:
     # ── diagnostics ──────────────────────────────────────────────────────
     # ── launch tuning (rt_set_tuning) ─────────────────────────────────────
     def set_tuning(self, max_paths=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, max_iterations=0,
-                   stack_limit=0, stack_ring=0):
+                   stack_limit=0, stack_ring=0, node_format=0):
         t = abi.RtTuning(int(max_paths), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(max_iterations),
-                         int(stack_limit), int(stack_ring))
+                         int(stack_limit), int(stack_ring), int(node_format))
         self._check(lib().rt_set_tuning(self.h, C.byref(t)))
 
     def get_tuning(self):
@@ -401,7 +401,7 @@ class GpuScene:
         self._check(lib().rt_get_tuning(self.h, C.byref(t)))
         return dict(max_paths=t.max_paths, trace_blocks_per_sm=t.trace_blocks_per_sm,
                     shade_blocks_per_sm=t.shade_blocks_per_sm, max_iterations=t.max_iterations,
-                    stack_limit=t.stack_limit, stack_ring=t.stack_ring)
+                    stack_limit=t.stack_limit, stack_ring=t.stack_ring, node_format=t.node_format)
 
     # ── path guiding (rt_guide_*) ─────────────────────────────────────────
     def guide_init(self, params=None):

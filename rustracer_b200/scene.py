@@ -217,13 +217,24 @@ class SceneBuilder:
 
     # participating media (volume.rs:78-263, scene_file.rs:297-336) ------
     def add_medium(self, kind, boundary, density, color, g=0.0, noise_scale=1.0, threshold=0.0, center=None,
-                   radius=None, p_min=None, p_max=None, seed=0):
-        """A constant ("constant") or Perlin-noise ("noise") medium inside a
-        sphere (center, radius) or an axis-aligned box (p_min, p_max).  The
-        noise medium's Perlin tables are drawn from `seed` (the reference draws
-        them from the thread RNG, perlin.rs:22-33)."""
+                   radius=None, p_min=None, p_max=None, seed=0, grid=None):
+        """A constant ("constant"), Perlin-noise ("noise") or voxel-grid
+        ("grid") medium inside a sphere (center, radius) or an axis-aligned box
+        (p_min, p_max).  The noise medium's Perlin tables are drawn from `seed`
+        (the reference draws them from the thread RNG, perlin.rs:22-33).  A grid
+        medium (box only; no reference counterpart) takes `grid` as a (nz, ny,
+        nx) array: σ_t = density × the trilinear interpolation of its values."""
         m = abi.RtMedium()
-        m.type = {"constant": abi.RT_MEDIUM_CONSTANT, "noise": abi.RT_MEDIUM_NOISE}[kind]
+        m.type = {"constant": abi.RT_MEDIUM_CONSTANT, "noise": abi.RT_MEDIUM_NOISE, "grid": abi.RT_MEDIUM_GRID}[kind]
+        if kind == "grid":
+            if boundary != "box" or grid is None:
+                raise ValueError("a grid medium needs a box boundary and a grid")
+            gr = np.ascontiguousarray(np.asarray(grid, dtype=F32))
+            if gr.ndim != 3:
+                raise ValueError("grid must be a (nz, ny, nx) array")
+            self._tex_keep.append(gr)
+            m.grid = gr.ctypes.data
+            m.grid_res[:] = [gr.shape[2], gr.shape[1], gr.shape[0]]
         m.boundary = {"sphere": abi.RT_BOUND_SPHERE, "box": abi.RT_BOUND_BOX}[boundary]
         if boundary == "sphere":
             m.center = _f3(center)

@@ -26,11 +26,11 @@ def test_autotune_picks_the_fastest_and_caches_it():
 
     def timer(t):
         calls.append(t)
-        # fastest at 2M paths, 6 traversal blocks, 8 shading blocks
+        # fastest at 4M paths, 6 traversal blocks, 8 shading blocks, quantised nodes
         return abs(t["max_paths"] - (1 << 22)) / 1e6 + abs(t["trace_blocks_per_sm"] - 6) + \
-            abs(t["shade_blocks_per_sm"] - 8) + 1.0
+            abs(t["shade_blocks_per_sm"] - 8) + t["node_format"] + 1.0
     best, table = autotune.autotune(g, None, pass_params(64, 64), key="k", timer=timer, repeats=2)
-    assert best == {"max_paths": 1 << 22, "trace_blocks_per_sm": 6, "shade_blocks_per_sm": 8}
+    assert best == {"max_paths": 1 << 22, "trace_blocks_per_sm": 6, "shade_blocks_per_sm": 8, "node_format": 0}
     assert len(table) == len(autotune.candidates()) and len(calls) == 2 * len(table)
     assert g.set[-1] == best
     g2 = FakeScene()
