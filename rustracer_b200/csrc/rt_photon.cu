@@ -11,8 +11,10 @@
 //             Morton order (node i has children 2i+1, 2i+2)
 // Gather (warp per query; lane j of the warp tests photon j of a leaf):
 //   radius    Σ power·(1 − d²/r²) over d² < r², n_p·n > 0, × 2/(π²r²) (photon.rs:195-228)
-//   k-NN      the k-th smallest d² among those photons within the maximum radius,
-//             found by histogram refinement, then the radius gather at that distance
+//   k-NN      the k-th smallest d² among those photons within the maximum radius:
+//             one traversal collects them into shared memory, a radix select
+//             finds the k-th, the sum runs over the collected photons (more
+//             than PH_CAND_CAP of them: histogram refinement over re-traversals)
 //   rt_knn    exact k nearest (d² ≤ rmax²) sorted by (d², emission index)
 #include <cub/cub.cuh>
 
@@ -654,17 +656,115 @@ RT_D float3 warp_irradiance(const Map& M, float3 p, float3 n, uint32_t* hist, fl
     return mk(warp_sum(acc.x) * s, warp_sum(acc.y) * s, warp_sum(acc.z) * s);
 }
 
+// Shared-memory workspace of one warp for the single-pass k-NN gather.
+#define PH_CAND_CAP 512
+struct WarpScratch {
+    float d2[PH_CAND_CAP];
+    uint32_t id[PH_CAND_CAP];
+    uint32_t hist[256];
+};
+
+// k-th smallest (1-based) of the cnt ≥ k non-negative floats v[] by a 4-pass
+// radix select on their bits (non-negative floats order as unsigned integers),
+// one warp, exact.
+RT_D float warp_radix_select(const float* v, uint32_t cnt, uint32_t k, uint32_t* hist) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t prefix = 0, mask = 0, need = k;
+#pragma unroll 1
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int b = lane; b < 256; b += 32) hist[b] = 0;
+        __syncwarp();
+        for (uint32_t j = lane; j < cnt; j += 32) {
+            uint32_t key = __float_as_uint(v[j]);
+            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+        }
+        __syncwarp();
+        // lane l owns bins 8l .. 8l + 7; an exclusive scan over the lanes finds the
+        // bin holding the need-th key
+        uint32_t h[8], tot = 0;
+#pragma unroll
+        for (int b = 0; b < 8; b++) { h[b] = hist[lane * 8 + b]; tot += h[b]; }
+        uint32_t inc = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t x = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if (lane >= (uint32_t)o) inc += x;
+        }
+        uint32_t exc = inc - tot;
+        bool mine = exc < need && need <= inc;
+        uint32_t digit = 0, before = 0;
+        if (mine) {
+            uint32_t c = exc;
+#pragma unroll
+            for (int b = 0; b < 8; b++) {
+                if (c + h[b] >= need) { digit = lane * 8 + b; before = c; break; }
+                c += h[b];
+            }
+        }
+        uint32_t who = __ffs(__ballot_sync(0xFFFFFFFFu, mine)) - 1;
+        digit = __shfl_sync(0xFFFFFFFFu, digit, who);
+        before = __shfl_sync(0xFFFFFFFFu, before, who);
+        need -= before;
+        prefix |= digit << shift;
+        mask |= 255u << shift;
+        __syncwarp();
+    }
+    return __uint_as_float(prefix);
+}
+
+// Irradiance at (p, n) by one warp in one traversal: the photons within the
+// gather radius that face n are collected into shared memory, the k-th
+// smallest d² is selected there (k-NN mode), and the Epanechnikov sum runs
+// over the collected photons.  More candidates than PH_CAND_CAP: the
+// histogram-refinement path (warp_irradiance) instead.  Same estimate as
+// warp_irradiance; the terms are summed in another order.
+RT_D float3 warp_irradiance_1pass(const Map& M, float3 p, float3 n, WarpScratch& W, uint32_t* hist, float* sel) {
+    const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+    uint32_t cnt = 0;
+    for_leaves(M, p, M.r2, [&](int i) {
+        bool c = false;
+        float d2 = 0.0f;
+        if (i >= 0) {
+            d2 = pdist2(__ldg(M.pos + i), p);
+            c = d2 < M.r2 && pdot(__ldg(M.nor + i), n) > 0.0f;
+        }
+        uint32_t m = __ballot_sync(0xFFFFFFFFu, c);
+        uint32_t slot = cnt + __popc(m & lt);
+        if (c && slot < PH_CAND_CAP) { W.d2[slot] = d2; W.id[slot] = (uint32_t)i; }
+        cnt += __popc(m);
+    });
+    __syncwarp();
+    if (cnt > PH_CAND_CAP) return warp_irradiance(M, p, n, hist, sel);
+    float r2 = M.r2;
+    if (M.knn_k > 0 && cnt >= M.knn_k) {
+        r2 = warp_radix_select(W.d2, cnt, M.knn_k, W.hist);
+        if (!(r2 > 0.0f)) return mk(0.f, 0.f, 0.f);
+    }
+    float3 acc = mk(0.f, 0.f, 0.f);
+    for (uint32_t j = lane; j < cnt; j += 32) {
+        float d2 = W.d2[j];
+        if (d2 < r2) {
+            float4 pw = __ldg(M.pow + W.id[j]);
+            acc = acc + mk(pw.x, pw.y, pw.z) * (1.0f - d2 / r2);
+        }
+    }
+    __syncwarp();
+    float s = 2.0f / (PI_F * PI_F * r2);
+    return mk(warp_sum(acc.x) * s, warp_sum(acc.y) * s, warp_sum(acc.z) * s);
+}
+
 }  // namespace rtph
 
 // queries n × 6 → irradiance n × 3; one warp per query
 __global__ void k_photon_gather_api(rtph::Map M, const float* q, uint32_t n, float* out) {
     __shared__ uint32_t hist[RT_SHADE_BLOCK / 32][32];
     __shared__ float sel[RT_SHADE_BLOCK / 32][PH_SEL_CAP];
+    __shared__ rtph::WarpScratch ws[RT_SHADE_BLOCK / 32];
     uint32_t w = threadIdx.x >> 5, gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t i = gw; i < n; i += nw) {
         float3 p = mk(q[i * 6], q[i * 6 + 1], q[i * 6 + 2]), nn = mk(q[i * 6 + 3], q[i * 6 + 4], q[i * 6 + 5]);
-        float3 r = rtph::warp_irradiance(M, p, nn, hist[w], sel[w]);
+        float3 r = rtph::warp_irradiance_1pass(M, p, nn, ws[w], hist[w], sel[w]);
         if ((threadIdx.x & 31u) == 0) { out[i * 3] = r.x; out[i * 3 + 1] = r.y; out[i * 3 + 2] = r.z; }
     }
 }
@@ -725,6 +825,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Ma
                                                                         const uint32_t* count) {
     __shared__ uint32_t hist[RT_SHADE_BLOCK / 32][32];
     __shared__ float sel[RT_SHADE_BLOCK / 32][PH_SEL_CAP];
+    __shared__ rtph::WarpScratch ws[RT_SHADE_BLOCK / 32];
     uint32_t n = *count;
     uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
@@ -758,7 +859,7 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Ma
                                     __shfl_sync(0xFFFFFFFFu, a.z, src), __shfl_sync(0xFFFFFFFFu, a.w, src));
             float3 qn = mk(__shfl_sync(0xFFFFFFFFu, b.x, src), __shfl_sync(0xFFFFFFFFu, b.y, src),
                            __shfl_sync(0xFFFFFFFFu, b.z, src));
-            float3 r = rtph::warp_irradiance(M, mk(qa.x, qa.y, qa.z), qn, hist[w], sel[w]);
+            float3 r = rtph::warp_irradiance_1pass(M, mk(qa.x, qa.y, qa.z), qn, ws[w], hist[w], sel[w]);
             if (lane == 0) {
                 uint32_t tag = __float_as_uint(qa.w);
                 float4* pc = T.pendC[(tag >> 1) & 1u] + (tag >> 2);
