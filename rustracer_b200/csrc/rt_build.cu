@@ -1,4 +1,5 @@
-// rt_build.cu — the binary SAH tree of the BVH built on the device.
+// rt_build.cu — the BVH built on the device: the binary SAH tree, then its
+// collapse to 8-wide nodes (full and quantised copies).
 //
 // The same tree as the host builder (SahBuilder in rt_host.cu), which restates
 // BvhTree::sah_partition (bvh.rs:290-323): at every node the centroid bounds,
@@ -361,15 +362,316 @@ __global__ void k_small(const Seg* __restrict__ segs, int32_t nseg, const float*
     }
 }
 
+// ── the collapse to 8-wide nodes on the device ──────────────────────────────
+// The host collapse (SahBuilder::collapse) builds a wide node from binary node
+// b by opening the inner child of largest surface area (the first of equal
+// ones) until 8 children (or only leaves) remain, and numbers the wide nodes
+// in preorder, leaves in the order the preorder meets them.  Here: every
+// binary node's opening is computed in parallel; the wide nodes are found
+// level by level from the root; subtree node and leaf counts are summed
+// bottom-up and the preorder indices handed down; then one thread per wide
+// node writes it.
+
+// kids of the wide node rooted at binary node b (≥ 0 binary node, < 0 leaf)
+__global__ void k_wide_kids(const int32_t* __restrict__ bl, const int32_t* __restrict__ br,
+                            const float* __restrict__ bbox, int32_t nn, int32_t* kids, int32_t* nk) {
+    for (int32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nn; b += gridDim.x * blockDim.x) {
+        int32_t k[8];
+        int n = 2;
+        k[0] = bl[b]; k[1] = br[b];
+        for (int c = 2; c < 8; c++) k[c] = 0;
+        while (n < 8) {
+            int best = -1;
+            float ba = -1.0f;
+            for (int i = 0; i < n; i++)
+                if (k[i] >= 0) { float a = area6(bbox + (size_t)k[i] * 6); if (a > ba) { ba = a; best = i; } }
+            if (best < 0) break;
+            int32_t o = k[best];
+            k[best] = bl[o];
+            k[n++] = br[o];
+        }
+        for (int c = 0; c < 8; c++) kids[(size_t)b * 8 + c] = k[c];
+        nk[b] = n;
+    }
+}
+
+__global__ void k_count_inner(const int32_t* __restrict__ lvl, int32_t m, const int32_t* __restrict__ kids,
+                              const int32_t* __restrict__ nk, int32_t* cnt) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        int32_t b = lvl[i], c = 0;
+        for (int j = 0; j < nk[b]; j++) c += kids[(size_t)b * 8 + j] >= 0;
+        cnt[i] = c;
+    }
+}
+__global__ void k_next_level(const int32_t* __restrict__ lvl, int32_t m, const int32_t* __restrict__ kids,
+                             const int32_t* __restrict__ nk, const int32_t* __restrict__ pos, int32_t* next) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        int32_t b = lvl[i], o = pos[i];
+        for (int j = 0; j < nk[b]; j++) {
+            int32_t k = kids[(size_t)b * 8 + j];
+            if (k >= 0) next[o++] = k;
+        }
+    }
+}
+// wide nodes (S) and leaves (L) in the wide subtree of every node of a level
+__global__ void k_subtree_sizes(const int32_t* __restrict__ lvl, int32_t m, const int32_t* __restrict__ kids,
+                                const int32_t* __restrict__ nk, int32_t* S, int32_t* L) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        int32_t b = lvl[i], sn = 1, sl = 0;
+        for (int j = 0; j < nk[b]; j++) {
+            int32_t k = kids[(size_t)b * 8 + j];
+            if (k >= 0) { sn += S[k]; sl += L[k]; } else sl += 1;
+        }
+        S[b] = sn;
+        L[b] = sl;
+    }
+}
+// preorder index (P) and first leaf slot (LB) of every inner kid of a level's nodes
+__global__ void k_preorder(const int32_t* __restrict__ lvl, int32_t m, const int32_t* __restrict__ kids,
+                           const int32_t* __restrict__ nk, const int32_t* __restrict__ S,
+                           const int32_t* __restrict__ L, int32_t* P, int32_t* LB) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        int32_t b = lvl[i], on = P[b] + 1, ol = LB[b];
+        for (int j = 0; j < nk[b]; j++) {
+            int32_t k = kids[(size_t)b * 8 + j];
+            if (k >= 0) { P[k] = on; LB[k] = ol; on += S[k]; ol += L[k]; } else ol += 1;
+        }
+    }
+}
+// the node of every wide root: child boxes (empty slots inverted), inner
+// children by preorder index, leaves for now as RT_LEAF_BIT | leaf slot
+__global__ void k_write_nodes(const int32_t* __restrict__ order, int32_t m, const int32_t* __restrict__ kids,
+                              const int32_t* __restrict__ nk, const int32_t* __restrict__ P,
+                              const int32_t* __restrict__ LB, const float* __restrict__ bbox,
+                              const float* __restrict__ box, const int32_t* __restrict__ idx, float4* nodes,
+                              int32_t* export_ch, int32_t* leaf_gid) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        int32_t b = order[i], me = P[b], ol = LB[b];
+        float f[56];
+        for (int c = 0; c < 8; c++) {
+            int32_t k = c < nk[b] ? kids[(size_t)b * 8 + c] : INT32_MIN;
+            uint32_t ref;
+            int32_t ex;
+            const float* cb = nullptr;
+            if (c >= nk[b]) {
+                ref = RT_EMPTY_REF; ex = INT32_MIN;
+            } else if (k >= 0) {
+                ref = (uint32_t)P[k]; ex = P[k]; cb = bbox + (size_t)k * 6;
+            } else {
+                int32_t slot = ol++, prim = idx[-k - 1];
+                leaf_gid[slot] = prim;
+                ref = RT_LEAF_BIT | (uint32_t)slot; ex = -(slot + 1); cb = box + (size_t)prim * 6;
+            }
+            for (int a = 0; a < 3; a++) {
+                f[a * 8 + c] = cb ? cb[a] : INFINITY;
+                f[24 + a * 8 + c] = cb ? cb[3 + a] : -INFINITY;
+            }
+            f[48 + c] = __uint_as_float(ref);
+            export_ch[(size_t)me * 8 + c] = ex;
+        }
+        float4* out = nodes + (size_t)me * 14;
+        for (int q = 0; q < 14; q++) out[q] = make_float4(f[q * 4], f[q * 4 + 1], f[q * 4 + 2], f[q * 4 + 3]);
+    }
+}
+// leaf type of every slot: one flag array per type for the typed-slot scans
+__global__ void k_leaf_types(const int32_t* __restrict__ leaf_gid, int32_t n, int64_t e0, int64_t e1, int64_t e2,
+                             int32_t* flags) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int64_t g = leaf_gid[i];
+        int t = g < e0 ? RT_PRIM_TRI : g < e1 ? RT_PRIM_QUAD : g < e2 ? RT_PRIM_SPHERE : RT_PRIM_CONVEX;
+        for (int k = 0; k < 4; k++) flags[(size_t)k * n + i] = t == k;
+    }
+}
+// leaf references: type in bits 28-30, the slot among leaves of that type
+__global__ void k_fix_leaf_refs(float4* nodes, int64_t n_nodes, const int32_t* __restrict__ leaf_gid, int32_t n,
+                                int64_t e0, int64_t e1, int64_t e2, const int32_t* __restrict__ scans) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_nodes * 8; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t* ch = reinterpret_cast<uint32_t*>(nodes + (size_t)(i / 8) * 14 + 12) + (i % 8);
+        uint32_t v = *ch;
+        if (v == RT_EMPTY_REF || !(v & RT_LEAF_BIT)) continue;
+        int32_t slot = (int32_t)(v & ~RT_LEAF_BIT);
+        int64_t g = leaf_gid[slot];
+        uint32_t t = g < e0 ? RT_PRIM_TRI : g < e1 ? RT_PRIM_QUAD : g < e2 ? RT_PRIM_SPHERE : RT_PRIM_CONVEX;
+        *ch = RT_LEAF_BIT | (t << 28) | (uint32_t)scans[(size_t)t * n + slot];
+    }
+}
+// the quantised copy of every node, as encode_qnode does on the host: the
+// directed-rounding subtractions are the exact ones the host forms from
+// TwoSum; a node whose extent needs a step beyond 2^60 sets *fail
+__global__ void k_encode_qnodes(const float4* __restrict__ nodes, int64_t n_nodes, float4* qnodes, int* fail) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        const float4* N = nodes + (size_t)i * 14;
+        float f[56];
+        for (int q = 0; q < 14; q++) { float4 v = N[q]; f[q * 4] = v.x; f[q * 4 + 1] = v.y; f[q * 4 + 2] = v.z; f[q * 4 + 3] = v.w; }
+        uint32_t valid = 0;
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int c = 0; c < 8; c++) {
+            if (__float_as_uint(f[48 + c]) == RT_EMPTY_REF) continue;
+            valid |= 1u << c;
+            for (int a = 0; a < 3; a++) { lo[a] = fminf(lo[a], f[a * 8 + c]); hi[a] = fmaxf(hi[a], f[24 + a * 8 + c]); }
+        }
+        if (!valid) for (int a = 0; a < 3; a++) lo[a] = hi[a] = 0.0f;
+        int e[3];
+        bool flat[3];
+        int e_any = -60;
+        for (int a = 0; a < 3; a++) {
+            float ext = __fsub_ru(hi[a], lo[a]);
+            flat[a] = !(ext > 0.0f);
+            if (flat[a]) continue;
+            int ex;
+            frexpf(ext / 255.0f, &ex);
+            while (ex > -60 && ldexpf(255.0f, ex - 1) >= ext) ex--;
+            while (ldexpf(255.0f, ex) < ext) ex++;
+            e[a] = max(ex, -60);
+            e_any = max(e_any, e[a]);
+        }
+        bool ok = true;
+        for (int a = 0; a < 3; a++) {
+            if (flat[a]) e[a] = e_any;
+            if (e[a] > 60) ok = false;
+        }
+        if (!ok) { atomicExch(fail, 1); continue; }
+        uint32_t w[3][4] = {};
+        for (int a = 0; a < 3; a++) {
+            float sa = ldexpf(1.0f, e[a]);
+            for (int c = 0; c < 8; c++) {
+                uint32_t ql = 255, qh = 0;
+                if ((valid >> c) & 1u) {
+                    float dl = __fsub_rd(f[a * 8 + c], lo[a]), dh = __fsub_ru(f[24 + a * 8 + c], lo[a]);
+                    ql = (uint32_t)fminf(fmaxf(floorf(dl / sa), 0.0f), 255.0f);
+                    qh = (uint32_t)fminf(fmaxf(ceilf(dh / sa), 0.0f), 255.0f);
+                }
+                w[a][c >> 2] |= ql << (8 * (c & 3));
+                w[a][2 + (c >> 2)] |= qh << (8 * (c & 3));
+            }
+        }
+        uint32_t meta = (uint32_t)(e[0] + 127) | (uint32_t)(e[1] + 127) << 8 | (uint32_t)(e[2] + 127) << 16 | valid << 24;
+        float4* Q = qnodes + (size_t)i * 8;
+        Q[0] = make_float4(lo[0], lo[1], lo[2], __uint_as_float(meta));
+        for (int a = 0; a < 3; a++)
+            Q[1 + a] = make_float4(__uint_as_float(w[a][0]), __uint_as_float(w[a][1]), __uint_as_float(w[a][2]),
+                                   __uint_as_float(w[a][3]));
+        Q[4] = N[12];
+        Q[5] = N[13];
+        Q[6] = Q[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
 }  // namespace
 
 namespace rth {
+
+// the device collapse: bl / br / bbox / box / idx and root are the device
+// arrays of the binary tree
+static cudaError_t collapse_wide(const int32_t* bl, const int32_t* br, const float* bbox, const float* box,
+                                 const int32_t* idx, int32_t root, int32_t n, int sms, cudaStream_t st, WideOut* W) {
+    const int32_t nn = n - 1;
+    int32_t *kids = nullptr, *nk = nullptr, *order = nullptr, *cnt = nullptr, *pos = nullptr;
+    int32_t *S = nullptr, *L = nullptr, *P = nullptr, *LB = nullptr, *leaf_gid = nullptr, *flags = nullptr, *scans = nullptr;
+    int* fail = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t r) { if (e == cudaSuccess && r != cudaSuccess) e = r; return e == cudaSuccess; };
+    auto scan = [&](const int32_t* in, int32_t* out, int32_t m) {
+        size_t need = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, need, in, out, m, st);
+        if (need > tmp_bytes) {
+            if (tmp) cudaFree(tmp);
+            tmp = nullptr;
+            if (!ok(cudaMalloc(&tmp, need))) return;
+            tmp_bytes = need;
+        }
+        ok(cub::DeviceScan::ExclusiveSum(tmp, need, in, out, m, st));
+    };
+    ok(cudaMalloc(&kids, (size_t)nn * 8 * 4)); ok(cudaMalloc(&nk, (size_t)nn * 4));
+    ok(cudaMalloc(&order, ((size_t)nn + 1) * 4)); ok(cudaMalloc(&cnt, ((size_t)nn + 1) * 4));
+    ok(cudaMalloc(&pos, ((size_t)nn + 1) * 4));
+    ok(cudaMalloc(&S, (size_t)nn * 4)); ok(cudaMalloc(&L, (size_t)nn * 4));
+    ok(cudaMalloc(&P, (size_t)nn * 4)); ok(cudaMalloc(&LB, (size_t)nn * 4));
+    ok(cudaMalloc(&leaf_gid, (size_t)n * 4)); ok(cudaMalloc(&flags, (size_t)n * 16)); ok(cudaMalloc(&scans, (size_t)n * 16));
+    ok(cudaMalloc(&fail, 4));
+    int grid = sms * 8;
+    std::vector<int32_t> lvl_off{0, 1};
+    if (e == cudaSuccess) {
+        k_wide_kids<<<grid, 256, 0, st>>>(bl, br, bbox, nn, kids, nk);
+        ok(cudaMemcpyAsync(order, &root, 4, cudaMemcpyHostToDevice, st));
+        // the wide roots, level by level, in `order`
+        while (e == cudaSuccess) {
+            int32_t off = lvl_off[lvl_off.size() - 2], m = lvl_off.back() - off;
+            k_count_inner<<<std::max(1, std::min((m + 255) / 256, grid)), 256, 0, st>>>(order + off, m, kids, nk, cnt);
+            scan(cnt, pos, m);
+            int32_t tail[2] = {0, 0};
+            ok(cudaMemcpyAsync(&tail[0], pos + m - 1, 4, cudaMemcpyDeviceToHost, st));
+            ok(cudaMemcpyAsync(&tail[1], cnt + m - 1, 4, cudaMemcpyDeviceToHost, st));
+            ok(cudaStreamSynchronize(st));
+            int32_t nxt = tail[0] + tail[1];
+            if (nxt == 0 || e != cudaSuccess) break;
+            if (lvl_off.back() + nxt > nn) { e = cudaErrorUnknown; break; }
+            k_next_level<<<std::max(1, std::min((m + 255) / 256, grid)), 256, 0, st>>>(order + off, m, kids, nk, pos,
+                                                                                   order + lvl_off.back());
+            lvl_off.push_back(lvl_off.back() + nxt);
+        }
+    }
+    const int nlev = (int)lvl_off.size() - 1;
+    if (e == cudaSuccess) {
+        for (int l = nlev - 1; l >= 0; l--) {
+            int32_t m = lvl_off[l + 1] - lvl_off[l];
+            k_subtree_sizes<<<std::max(1, std::min((m + 255) / 256, grid)), 256, 0, st>>>(order + lvl_off[l], m, kids,
+                                                                                       nk, S, L);
+        }
+        ok(cudaMemsetAsync(P + root, 0, 4, st));
+        ok(cudaMemsetAsync(LB + root, 0, 4, st));
+        for (int l = 0; l < nlev; l++) {
+            int32_t m = lvl_off[l + 1] - lvl_off[l];
+            k_preorder<<<std::max(1, std::min((m + 255) / 256, grid)), 256, 0, st>>>(order + lvl_off[l], m, kids, nk,
+                                                                                  S, L, P, LB);
+        }
+        int32_t total = 0;
+        ok(cudaMemcpyAsync(&total, S + root, 4, cudaMemcpyDeviceToHost, st));
+        ok(cudaStreamSynchronize(st));
+        if (e == cudaSuccess && total != lvl_off.back()) e = cudaErrorUnknown;   // every wide root counted once
+        W->n_nodes = total;
+        W->max_depth = nlev - 1;
+    }
+    if (e == cudaSuccess) {
+        ok(cudaMalloc(&W->nodes, (size_t)W->n_nodes * 14 * 16));
+        ok(cudaMalloc(&W->qnodes, (size_t)W->n_nodes * 8 * 16));
+        ok(cudaMalloc(&W->export_ch, (size_t)W->n_nodes * 8 * 4));
+    }
+    if (e == cudaSuccess) {
+        int32_t m = lvl_off.back();
+        k_write_nodes<<<std::max(1, std::min((m + 127) / 128, grid)), 128, 0, st>>>(
+            order, m, kids, nk, P, LB, bbox, box, idx, W->nodes, W->export_ch, leaf_gid);
+        k_leaf_types<<<grid, 256, 0, st>>>(leaf_gid, n, W->type_end[0], W->type_end[1], W->type_end[2], flags);
+        for (int t = 0; t < 4; t++) scan(flags + (size_t)t * n, scans + (size_t)t * n, n);
+        k_fix_leaf_refs<<<grid, 256, 0, st>>>(W->nodes, W->n_nodes, leaf_gid, n, W->type_end[0], W->type_end[1],
+                                             W->type_end[2], scans);
+        ok(cudaMemsetAsync(fail, 0, 4, st));
+        k_encode_qnodes<<<grid, 128, 0, st>>>(W->nodes, W->n_nodes, W->qnodes, fail);
+        int hfail = 0;
+        ok(cudaMemcpyAsync(W->leaf_gids_h, leaf_gid, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
+        ok(cudaMemcpyAsync(&hfail, fail, 4, cudaMemcpyDeviceToHost, st));
+        ok(cudaStreamSynchronize(st));
+        ok(cudaGetLastError());
+        if (e == cudaSuccess && hfail) { cudaFree(W->qnodes); W->qnodes = nullptr; }
+    }
+    void* all[] = {kids, nk, order, cnt, pos, S, L, P, LB, leaf_gid, flags, scans, fail, tmp};
+    for (void* p : all) if (p) cudaFree(p);
+    if (e != cudaSuccess) {
+        void* outs[] = {W->nodes, W->qnodes, W->export_ch};
+        for (void* p : outs) if (p) cudaFree(p);
+        W->nodes = W->qnodes = nullptr;
+        W->export_ch = nullptr;
+    }
+    return e;
+}
 
 // Build the binary SAH tree of n primitive boxes (host, 6 floats each) on the
 // device; idx (n), bl / br (n − 1 child refs: ≥ 0 node, < 0 leaf −(pos + 1))
 // and bbox ((n − 1) × 6) are written on the host.  Returns 0 or a CUDA error.
 int gpu_build_binary(const float* boxes_h, int32_t n, int32_t* idx_h, int32_t* bl_h, int32_t* br_h, float* bbox_h,
-                     int32_t* root_h, int sms, cudaStream_t st) {
+                     int32_t* root_h, int sms, cudaStream_t st, WideOut* wide) {
     float *box = nullptr, *cen = nullptr, *bbox = nullptr;
     int32_t *idx = nullptr, *tmp = nullptr, *bl = nullptr, *br = nullptr, *root = nullptr, *cnt = nullptr;
     int32_t *stats = nullptr, *mids = nullptr, *axes = nullptr, *chunk_seg = nullptr, *chunk_lo = nullptr;
@@ -457,7 +759,17 @@ int gpu_build_binary(const float* boxes_h, int32_t n, int32_t* idx_h, int32_t* b
     if (e == cudaSuccess && n_small > 0)
         k_small<<<(n_small + 63) / 64, 64, 0, st>>>(small, n_small, box, cen, idx, tmp, keys, bl, br, root, bbox);
     ok(cudaGetLastError());
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess && wide) {
+        // the collapse on the device; the host gets the leaf order, not the tree
+        int32_t rt = 0;
+        ok(cudaMemcpyAsync(&rt, root, 4, cudaMemcpyDeviceToHost, st));
+        ok(cudaStreamSynchronize(st));
+        if (e == cudaSuccess) {
+            if (rt < 0 || n < 2) e = cudaErrorInvalidValue;       // one primitive: the host builds that node
+            else ok(collapse_wide(bl, br, bbox, box, idx, rt, n, sms, st, wide));
+        }
+        if (root_h) *root_h = rt;
+    } else if (e == cudaSuccess) {
         ok(cudaMemcpyAsync(idx_h, idx, (size_t)n * 4, cudaMemcpyDeviceToHost, st));
         if (n > 1) {
             ok(cudaMemcpyAsync(bl_h, bl, (size_t)(n - 1) * 4, cudaMemcpyDeviceToHost, st));

@@ -586,9 +586,13 @@ struct RtScene {
     std::vector<float> h_emission;    // per material: RGB emission of a light material (3 floats)
     float photon_stage_ms[3] = {0, 0, 0};   // last photon build: trace, compaction, tree
     uint64_t max_iterations = 0;      // wavefront iteration bound (rt_set_tuning; 0 = derived)
-    double sah_cost = 0.0;
+    mutable double sah_cost = 0.0;
     double build_ms = 0.0;
-    std::vector<RefNode> ref_nodes;   // reference-layout copy for rt_scene_bvh_export
+    // reference-layout copy for rt_scene_bvh_export and the SAH statistic; with
+    // the device collapse it is made from the device nodes on first use
+    mutable std::vector<RefNode> ref_nodes;
+    mutable bool ref_ready = false;
+    const int32_t* d_export_ch = nullptr;   // device collapse: children in export form, 8 per node
     std::vector<int32_t> leaf_gids;
     bool empty = true;
     // wavefront buffers (grown on demand)
@@ -684,6 +688,56 @@ static int enter(RtScene* s) {
     CK(cudaStreamWaitEvent(s->stream, s->caller_ev, 0));
     return RT_OK;
 }
+// SAH cost of a wide tree (statistics): Σ_inner area(node)/area(root) +
+// Σ_leaf area(leaf)/area(root), inner nodes costing 1 per traversal
+static double sah_cost_of(const std::vector<RefNode>& nodes) {
+    if (nodes.empty()) return 0.0;
+    Box rb{h3(INFINITY, INFINITY, INFINITY), h3(-INFINITY, -INFINITY, -INFINITY)};
+    const RefNode& r0 = nodes[0];
+    for (int c = 0; c < 8; c++) if (r0.ch[c] != INT32_MIN)
+        rb = unite(rb, Box{h3(r0.mn[0][c], r0.mn[1][c], r0.mn[2][c]), h3(r0.mx[0][c], r0.mx[1][c], r0.mx[2][c])});
+    double root_sa = area(rb), cost = 0.0;
+    for (const RefNode& r : nodes) {
+        Box nb{h3(INFINITY, INFINITY, INFINITY), h3(-INFINITY, -INFINITY, -INFINITY)};
+        for (int c = 0; c < 8; c++) if (r.ch[c] != INT32_MIN) {
+            Box cb{h3(r.mn[0][c], r.mn[1][c], r.mn[2][c]), h3(r.mx[0][c], r.mx[1][c], r.mx[2][c])};
+            nb = unite(nb, cb);
+            if (r.ch[c] < 0) cost += (double)area(cb) / root_sa;
+        }
+        cost += (double)area(nb) / root_sa;
+    }
+    return cost;
+}
+
+// the reference-layout nodes of a device-collapsed tree, downloaded on first use
+static int ensure_ref_nodes(const RtScene* s) {
+    if (s->ref_ready) return RT_OK;
+    if (s->d_export_ch && s->n_nodes > 0) {
+        std::vector<float4> nodes((size_t)s->n_nodes * 14);
+        std::vector<int32_t> ch((size_t)s->n_nodes * 8);
+        if (cudaSetDevice(s->device) != cudaSuccess ||
+            cudaMemcpy(nodes.data(), s->S.nodes, nodes.size() * 16, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(ch.data(), s->d_export_ch, ch.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return RT_ERR_CUDA;
+        s->ref_nodes.assign((size_t)s->n_nodes, RefNode{});
+        for (int64_t k = 0; k < s->n_nodes; k++) {
+            RefNode& r = s->ref_nodes[k];
+            const float* f = reinterpret_cast<const float*>(&nodes[(size_t)k * 14]);
+            for (int c = 0; c < 8; c++) {
+                r.ch[c] = ch[(size_t)k * 8 + c];
+                bool empty = r.ch[c] == INT32_MIN;     // empty slots keep the reference's zero box
+                for (int a = 0; a < 3; a++) {
+                    r.mn[a][c] = empty ? 0.0f : f[a * 8 + c];
+                    r.mx[a][c] = empty ? 0.0f : f[24 + a * 8 + c];
+                }
+            }
+        }
+    }
+    s->sah_cost = sah_cost_of(s->ref_nodes);
+    s->ref_ready = true;
+    return RT_OK;
+}
+
 #define ENTER(s)                          \
     do {                                  \
         int rc_e_ = enter(s);             \
@@ -935,10 +989,29 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     std::vector<float4> gtri, gtri_n, gquad, gsph, gtri_uv, gtri_tan;
     if (n > 0) {
         SahBuilder B(boxes);
-        // the binary SAH tree is built on the device unless the description asks for the host
+        // the tree is built on the device (the binary SAH tree and its collapse to
+        // 8-wide nodes) unless the description asks for the host builder
+        const bool dev_wide = d->bvh_builder != RT_BVH_HOST && n >= 2;
+        rth::WideOut W;
         auto tb = std::chrono::steady_clock::now();
-        int brc = B.build_wide(d->bvh_builder == RT_BVH_HOST ? 0 : s->sms, s->stream);
-        if (brc) return bail(fail(s, RT_ERR_CUDA, std::string("device BVH build: ") + cudaGetErrorString((cudaError_t)brc)));
+        if (dev_wide) {
+            std::vector<float> bx((size_t)n * 6);
+            for (int64_t i = 0; i < n; i++)
+                for (int a = 0; a < 3; a++) { bx[i * 6 + a] = hc(boxes[i].mn, a); bx[i * 6 + 3 + a] = hc(boxes[i].mx, a); }
+            B.leaves.resize((size_t)n);
+            W.type_end[0] = d->n_tris; W.type_end[1] = d->n_tris + d->n_quads; W.type_end[2] = n_sph_end;
+            W.leaf_gids_h = B.leaves.data();
+            int32_t root = 0;
+            int brc = rth::gpu_build_binary(bx.data(), (int32_t)n, nullptr, nullptr, nullptr, nullptr, &root, s->sms,
+                                            s->stream, &W);
+            if (brc) return bail(fail(s, RT_ERR_CUDA, std::string("device BVH build: ") + cudaGetErrorString((cudaError_t)brc)));
+            void* owned_ptrs[] = {W.nodes, W.qnodes, W.export_ch};
+            for (void* p : owned_ptrs) if (p) s->owned.push_back(DevBuf{p, 0});
+            B.max_depth = W.max_depth;
+        } else {
+            int brc = B.build_wide(d->bvh_builder == RT_BVH_HOST ? 0 : s->sms, s->stream);
+            if (brc) return bail(fail(s, RT_ERR_CUDA, std::string("device BVH build: ") + cudaGetErrorString((cudaError_t)brc)));
+        }
         s->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
         s->max_depth = B.max_depth;
         // traversal stack: a visit of a node at depth k leaves at most 7 entries
@@ -955,11 +1028,12 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         if (int rc = dalloc(s, &sp_buf, std::max<size_t>(spill_entries, 1) * spill_threads * sizeof(uint32_t)))
             return bail(rc);
         s->S.stack_spill = (uint32_t*)sp_buf;
-        // SAH cost of the tree: Σ_inner area(node)/area(root) + Σ_leaf area(leaf)/area(root)
         s->ref_nodes = std::move(B.nodes);
         s->leaf_gids = std::move(B.leaves);
-        s->n_nodes = (int64_t)s->ref_nodes.size();
+        s->n_nodes = dev_wide ? W.n_nodes : (int64_t)s->ref_nodes.size();
         s->n_leaves = (int64_t)s->leaf_gids.size();
+        s->d_export_ch = W.export_ch;
+        s->ref_ready = !dev_wide;
         // leaf order per type
         std::vector<int32_t> typed_slot(s->n_leaves);
         std::vector<int64_t> order_tri, order_quad, order_sph, order_cvx;
@@ -970,9 +1044,8 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
             else if (g < n_sph_end) { typed_slot[k] = (int32_t)order_sph.size(); order_sph.push_back(g - d->n_tris - d->n_quads); }
             else { typed_slot[k] = (int32_t)order_cvx.size(); order_cvx.push_back(g - n_sph_end); }
         }
-        double root_sa = 0.0;
-        gnodes.resize((size_t)s->n_nodes * 14);
-        for (int64_t k = 0; k < s->n_nodes; k++) {
+        if (!dev_wide) gnodes.resize((size_t)s->n_nodes * 14);
+        for (int64_t k = 0; k < (dev_wide ? 0 : s->n_nodes); k++) {
             const RefNode& r = s->ref_nodes[k];
             float* f = reinterpret_cast<float*>(&gnodes[(size_t)k * 14]);
             // an empty slot gets an inverted box (+inf, −inf): its slab test fails
@@ -997,25 +1070,7 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
                 }
             }
         }
-        {   // SAH cost (for statistics): inner nodes cost 1 per traversal, leaves 1 per test
-            Box rb{h3(INFINITY, INFINITY, INFINITY), h3(-INFINITY, -INFINITY, -INFINITY)};
-            const RefNode& r0 = s->ref_nodes[0];
-            for (int c = 0; c < 8; c++) if (r0.ch[c] != INT32_MIN)
-                rb = unite(rb, Box{h3(r0.mn[0][c], r0.mn[1][c], r0.mn[2][c]), h3(r0.mx[0][c], r0.mx[1][c], r0.mx[2][c])});
-            root_sa = area(rb);
-            double cost = 0.0;
-            for (int64_t k = 0; k < s->n_nodes; k++) {
-                const RefNode& r = s->ref_nodes[k];
-                Box nb{h3(INFINITY, INFINITY, INFINITY), h3(-INFINITY, -INFINITY, -INFINITY)};
-                for (int c = 0; c < 8; c++) if (r.ch[c] != INT32_MIN) {
-                    Box cb{h3(r.mn[0][c], r.mn[1][c], r.mn[2][c]), h3(r.mx[0][c], r.mx[1][c], r.mx[2][c])};
-                    nb = unite(nb, cb);
-                    if (r.ch[c] < 0) cost += (double)area(cb) / root_sa;
-                }
-                cost += (double)area(nb) / root_sa;
-            }
-            s->sah_cost = cost;
-        }
+        if (!dev_wide) s->sah_cost = sah_cost_of(s->ref_nodes);
         // primitive records in leaf order
         gtri.resize(order_tri.size() * 3);
         bool has_n = d->tri_n != nullptr;
@@ -1116,8 +1171,14 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         if ((rc = upload(s, gcvx.data(), gcvx.size(), &s->S.cvx))) return bail(rc);
         if ((rc = upload(s, wpl.data(), wpl.size(), &s->S.cvx_planes))) return bail(rc);
         if ((rc = upload(s, wsh.data(), wsh.size(), &s->S.cvx_shade))) return bail(rc);
-        if ((rc = upload(s, gnodes.data(), gnodes.size(), &s->S.nodes))) return bail(rc);
-        {   // the quantised copy of the nodes (rt_set_tuning node_format 0, the default)
+        if (dev_wide) {
+            s->S.nodes = W.nodes;
+            s->S.qnodes = W.qnodes;
+            s->qnodes_ok = W.qnodes != nullptr;
+            s->S.node_format = s->qnodes_ok ? RT_NODES_QUANTISED : RT_NODES_FULL;
+        } else if ((rc = upload(s, gnodes.data(), gnodes.size(), &s->S.nodes))) {
+            return bail(rc);
+        } else {   // the quantised copy of the nodes (rt_set_tuning node_format 0, the default)
             std::vector<float4> qn((size_t)s->n_nodes * 8);
             bool qok = true;
             for (int64_t k = 0; k < s->n_nodes && qok; k++)
@@ -1483,6 +1544,7 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
 
 int32_t rt_scene_bvh_stats(const RtScene* s, int64_t* n_nodes, int64_t* n_leaves, int32_t* max_depth, double* sah) {
     if (!s) return RT_ERR_INVALID;
+    if (sah) if (int rc = ensure_ref_nodes(s)) return rc;
     if (n_nodes) *n_nodes = s->n_nodes;
     if (n_leaves) *n_leaves = s->n_leaves;
     if (max_depth) *max_depth = s->max_depth;
@@ -1492,6 +1554,7 @@ int32_t rt_scene_bvh_stats(const RtScene* s, int64_t* n_nodes, int64_t* n_leaves
 
 int32_t rt_scene_bvh_export(const RtScene* s, float* nodes, int64_t* n_nodes, int32_t* leaf, int64_t* n_leaves) {
     if (!s) return RT_ERR_INVALID;
+    if (nodes) if (int rc = ensure_ref_nodes(s)) return rc;
     if (n_nodes) *n_nodes = s->n_nodes;
     if (n_leaves) *n_leaves = s->n_leaves;
     if (nodes) memcpy(nodes, s->ref_nodes.data(), s->ref_nodes.size() * sizeof(RefNode));

@@ -185,8 +185,24 @@ void launch_photon_gather_paths(const PhotonMapDev& map, const PendTargets& T, c
                                 int sms, cudaStream_t st);
 void launch_accumulate(const float* scratch, uint32_t nsamp, uint32_t npix, float* acc, float* m2, uint32_t* cnt,
                        const uint8_t* conv, float clamp, uint32_t min_samples, float floor_, cudaStream_t st);
+// The 8-wide tree collapsed on the device from the binary tree (the host
+// collapse's greedy rule and preorder numbering): full and quantised node
+// arrays in device memory (the caller owns them), the leaf order, the node
+// count and depth, and per node the children in the reference's export form
+// (≥ 0 node, −(leaf slot + 1), INT32_MIN empty) for rt_scene_bvh_export.
+struct WideOut {
+    int64_t type_end[3];          // canonical ids below [0] are triangles, below [1] quads, below [2] spheres
+    float4* nodes = nullptr;      // 14 float4 per node
+    float4* qnodes = nullptr;     // 8 float4 per node (null when an extent is beyond the quantised range)
+    int32_t* export_ch = nullptr; // 8 per node
+    int64_t n_nodes = 0;
+    int32_t max_depth = 0;
+    int32_t* leaf_gids_h = nullptr;   // host, n entries
+};
+// binary tree on the device, then (wide == null) its arrays copied to the host
+// or (wide != null) the device collapse into *wide
 int gpu_build_binary(const float* boxes_h, int32_t n, int32_t* idx_h, int32_t* bl_h, int32_t* br_h, float* bbox_h,
-                     int32_t* root_h, int sms, cudaStream_t st);
+                     int32_t* root_h, int sms, cudaStream_t st, WideOut* wide = nullptr);
 // guide mixture of every path in the diffuse queue (before its shading kernel)
 void launch_guide_infer(const rtd::DevScene& S, const PathState& A, const RenderLaunch& R, const uint32_t* queue,
                         const uint32_t* count, int sms, cudaStream_t st);

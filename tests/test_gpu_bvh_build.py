@@ -1,7 +1,9 @@
-"""The device BVH builder (rt_build.cu) against the host builder: the same
-binary SAH partition (bvh.rs:290-323), so after the collapse to 8-wide nodes
-the exported node boxes, children and leaf order are equal, for large
-triangle meshes, random soups, degenerate clusters and mixed scenes."""
+"""The device BVH builder (rt_build.cu: the binary SAH tree and its collapse
+to 8-wide nodes on the device) against the host builder: the same binary SAH
+partition (bvh.rs:290-323) and the same greedy collapse, so the exported node
+boxes, children, leaf order and tree statistics are equal, and both node
+layouts of both builds trace the same hits, for large triangle meshes, random
+soups, degenerate clusters and mixed scenes."""
 import numpy as np
 import pytest
 
@@ -43,6 +45,22 @@ def _same_bvh(sb):
     assert hn.shape == dn.shape and np.array_equal(hl, dl)
     assert (hn[:, :48] == dn[:, :48]).all()       # child boxes: equal values (a zero may differ in sign)
     assert np.array_equal(hn[:, 48:].view(np.uint32), dn[:, 48:].view(np.uint32))   # child references
+    hs, ds = host.bvh_stats(), dev.bvh_stats()
+    assert (hs["nodes"], hs["leaves"], hs["max_depth"]) == (ds["nodes"], ds["leaves"], ds["max_depth"])
+    assert abs(hs["sah_cost"] - ds["sah_cost"]) <= 1e-9 * hs["sah_cost"]
+    # both node layouts of both builds trace the same hits
+    lo, hi = hn[:, :24].min(), hn[:, 24:48].max()
+    rng = np.random.default_rng(5)
+    o = rng.uniform(lo, hi, (4096, 3))
+    d = rng.normal(size=(4096, 3))
+    r = np.concatenate([o, d, np.full((4096, 1), 0.001), np.full((4096, 1), np.inf)], 1).astype(np.float32)
+    ref = host.trace_closest(r)
+    for g in (host, dev):
+        for fmt in (0, 1):
+            g.set_tuning(node_format=fmt)
+            h = g.trace_closest(r)
+            assert np.array_equal(h["prim"], ref["prim"]) and np.array_equal(h["t"].view(np.uint32), ref["t"].view(np.uint32))
+        g.set_tuning()
     return host, dev
 
 
