@@ -482,6 +482,35 @@ int32_t rt_photon_gather(RtScene* scene, const float* queries, int64_t n, float*
 int32_t rt_knn(RtScene* scene, const float* queries, int64_t n, int32_t k, float rmax,
                int32_t* idx, float* d2, int32_t mem);
 
+/* ── packed batches of render requests (no counterpart in the reference,
+ * whose renderer serves one frame at a time, renderer.rs:655-730) ───────────
+ * Many requests on one scene — each with its own camera, size, samples per
+ * pixel, first sample and seed — render together: one wavefront pool draws
+ * samples from all of them (a cursor over the concatenated requests), so the
+ * GPU stays full however small each frame is.  Every request's samples are
+ * those of an rt_render_accumulate call with the same camera and
+ * RtPassParams (width, height, sample_idx, n_samples = spp, strata, seed;
+ * max_depth, hero_count and bg_scale from `shared`), accumulated in the same
+ * sample order, so the results are bit-identical to rendering the requests
+ * one at a time.  Samples are taken in passes of at most `window` samples
+ * per pixel of every unfinished request (0: as many as fit a 2 GiB sample
+ * buffer).  Outputs are packed request after request: out_sum / out_m2
+ * (Σ w·h·3 floats), out_count (Σ w·h), and done_ms[j], the device time from
+ * the start of the call to the end of the pass that finished request j.
+ * No converged masks, no guide. */
+typedef struct RtBatchJob {
+    RtCamera cam;
+    uint32_t width, height;
+    uint32_t spp;            /* samples per pixel of the request (≥ 1) */
+    uint32_t strata;         /* ⌊√spp⌋ unless the caller says otherwise */
+    uint32_t sample_idx;     /* first sample index */
+    uint32_t pad;
+    uint64_t seed;
+} RtBatchJob;
+int32_t rt_render_batch(RtScene* scene, const RtBatchJob* jobs, int32_t n_jobs, const RtPassParams* shared,
+                        uint32_t window, float* out_sum, float* out_m2, uint32_t* out_count, float* done_ms,
+                        int32_t mem);
+
 /* Device timing of the last render call: total milliseconds and ray counts. */
 int32_t rt_last_render_stats(const RtScene* scene, double* ms, int64_t* ext_rays,
                              int64_t* shadow_rays, int64_t* kernel_launches);

@@ -275,6 +275,12 @@ class RtPassParams(C.Structure):
     ]
 
 
+class RtBatchJob(C.Structure):
+    """RtBatchJob (include/rt_api.h): one request of a packed batch."""
+    _fields_ = [("cam", RtCamera), ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
+                ("strata", C.c_uint32), ("sample_idx", C.c_uint32), ("pad", C.c_uint32), ("seed", C.c_uint64)]
+
+
 class RtHit(C.Structure):
     _fields_ = [("prim", C.c_int32), ("t", C.c_float), ("b1", C.c_float), ("b2", C.c_float)]
 

@@ -1,11 +1,17 @@
 """Batched rendering: many independent frames of several scenes on one GPU.
 
-Each worker thread owns one scene handle per scene kind (each handle has its
-own CUDA stream and buffers); the library's calls release the GIL, so the
-workers' frames run concurrently and small frames fill the GPU together.  Jobs
-are taken in submission order from one queue.  `run_batch` reports, per job,
-the latency from the batch's start to the job's completion, and the aggregate
-path-sample rate; with one worker it is the sequential baseline.
+`run_packed` is the batch service: the requests of each scene kind go into
+one packed rt_render_batch call — one wavefront pool draws samples from all
+of them, passes of a few samples per pixel of every unfinished request — and
+the scene kinds' calls run concurrently, each on its handle's stream.  A
+request's latency is the start of its call plus the device time at which the
+pass that finished it ended.
+
+`run_batch` is the frame-at-a-time service it replaces: worker threads with
+their own handles take jobs from one queue and render each alone
+(rt_render_accumulate); with one worker it is the sequential baseline.  Both
+report the aggregate path-sample rate and the per-request latencies from the
+batch's start.
 """
 import math
 import queue
@@ -117,6 +123,52 @@ def run_batch(jobs, workers=4, device=0, builders=None, keep_outputs=False, tune
                 errors.append(e)
 
     threads = [threading.Thread(target=worker, args=(h,)) for h in handles]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    wall = time.perf_counter() - t0
+    if errors:
+        raise errors[0]
+    samples = sum(j["width"] * j["height"] * j["spp"] for j in jobs)
+    ls = np.array([lat[j["id"]] for j in jobs])
+    return dict(wall_s=wall, path_samples=samples, rate=samples / wall, p50_s=float(np.percentile(ls, 50)),
+                p99_s=float(np.percentile(ls, 99)), latencies=lat, outputs=outs, tunings=tunings)
+
+
+def batch_request(job):
+    """A job of make_jobs as an rt_render_batch request (the samples of render_job)."""
+    return dict(cam=job_camera(job), width=job["width"], height=job["height"], spp=job["spp"],
+                strata=int(math.sqrt(job["spp"])), sample_idx=0, seed=job["seed"])
+
+
+def run_packed(jobs, device=0, builders=None, keep_outputs=False, tune=False, window=0):
+    """Render `jobs` packed: one rt_render_batch call per scene kind, the
+    kinds on concurrent threads (each handle its own stream).  Returns the
+    same summary as run_batch."""
+    builders = builders or {}
+    kinds = sorted({j["scene"] for j in jobs})
+    handles = {k: GpuScene(builders[k] if k in builders else build_scene(k), device=device) for k in kinds}
+    tunings = tune_kinds([handles], jobs) if tune else None
+    for k in kinds:                                       # warm each handle's buffers
+        render_job(handles, dict(scene=k, width=64, height=64, spp=1, azimuth=0.0, elevation=20.0, seed=0))
+    lat, outs, errors = {}, {}, []
+    t0 = time.perf_counter()
+
+    def worker(k):
+        mine = [j for j in jobs if j["scene"] == k]
+        try:
+            start = time.perf_counter() - t0
+            res, done = handles[k].render_batch([batch_request(j) for j in mine],
+                                                pass_params(64, 64, 0, 1, 1, _DEPTH[k], 4, 1.0, 0), window=window)
+            for j, r, d in zip(mine, res, done):
+                lat[j["id"]] = start + float(d) / 1000.0
+                if keep_outputs:
+                    outs[j["id"]] = r
+        except Exception as e:   # surfaced after the batch
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in kinds]
     for t in threads:
         t.start()
     for t in threads:

@@ -620,6 +620,12 @@ struct RtScene {
     float *acc = nullptr, *m2 = nullptr;
     uint32_t* cnt = nullptr;
     uint32_t acc_npix = 0;
+    // packed batches: accumulators of all requests and the device request table
+    float *b_acc = nullptr, *b_m2 = nullptr;
+    uint32_t* b_cnt = nullptr;
+    uint64_t batch_pix = 0;
+    JobDev* d_jobs = nullptr;
+    uint32_t jobs_cap = 0;
     // api staging
     void* stage = nullptr;
     size_t stage_bytes = 0;
@@ -768,7 +774,8 @@ int32_t rt_scene_destroy(RtScene* s) {
     if (!s) return RT_OK;
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto& b : s->owned) cudaFree(b.p);
-    void* ps[] = {s->counters, s->d_err, s->scratch, s->d_conv, s->acc, s->m2, s->cnt, s->stage, s->d_active};
+    void* ps[] = {s->counters, s->d_err, s->scratch, s->d_conv, s->acc, s->m2, s->cnt, s->stage, s->d_active,
+                  s->b_acc, s->b_m2, s->b_cnt, s->d_jobs};
     free_paths(s);
     rtgh::destroy(s->guide);
     s->photons.release();
@@ -1760,8 +1767,9 @@ static const uint32_t STATUS_RING = 8, STATUS_LAG = 2;
 
 static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, const RtPassParams* p, uint32_t sample_idx,
                          uint32_t nsamp, float* dscratch, const uint32_t* active, uint32_t nactive, int64_t* ext_rays,
-                         int64_t* sh_rays, int64_t* launches) {
-    uint64_t total = (uint64_t)nsamp * nactive;
+                         int64_t* sh_rays, int64_t* launches, const JobDev* jobs = nullptr, uint32_t n_jobs = 0,
+                         uint64_t jobs_total = 0) {
+    uint64_t total = n_jobs ? jobs_total : (uint64_t)nsamp * nactive;
     if (total == 0) return RT_OK;
     uint32_t pool = (uint32_t)std::min<uint64_t>(total, W.cap);
     uint32_t maxd = std::min<uint32_t>(p->max_depth, RT_MAX_DEPTH);
@@ -1782,6 +1790,8 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
     R.scratch = dscratch;
     R.photons = s->photons.present && s->photons.n > 0;
     if (W.guide && s->guide && rtgh::mode(s->guide) != RT_GUIDE_OFF) R.guide = rtgh::view(s->guide);
+    R.jobs = jobs;
+    R.n_jobs = n_jobs;
     uint32_t* hdr = W.counters;
     auto blk = [&](uint64_t it) { return W.counters + CTR_HDR_WORDS + (it % RT_CTR_RING) * RT_CTR_STRIDE; };
     size_t ev_used = 0;
@@ -2039,6 +2049,143 @@ extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const R
     s->last_ext = ext;
     s->last_shadow = sh;
     s->last_launches = nl;
+    return check_err(s);
+}
+
+// ── packed batches ──────────────────────────────────────────────────────────
+extern "C" int32_t rt_render_batch(RtScene* s, const RtBatchJob* jobs, int32_t n_jobs, const RtPassParams* shared,
+                                   uint32_t window, float* out_sum, float* out_m2, uint32_t* out_count, float* done_ms,
+                                   int32_t mem) {
+    if (!s || !jobs || !shared || n_jobs < 1) return RT_ERR_INVALID;
+    if (n_jobs > 65535) return fail(s, RT_ERR_CAPACITY, "more than 65535 requests in one batch");
+    if (shared->max_depth == 0 || shared->max_depth > RT_MAX_DEPTH) return fail(s, RT_ERR_INVALID, "max_depth must be in 1..256");
+    if (s->empty) return fail(s, RT_ERR_INVALID, "scene has no primitives");
+    std::vector<uint64_t> pix_off((size_t)n_jobs + 1, 0);
+    for (int32_t j = 0; j < n_jobs; j++) {
+        const RtBatchJob& b = jobs[j];
+        if (b.width == 0 || b.height == 0 || b.spp == 0) return fail(s, RT_ERR_INVALID, "batch request with no pixels or samples");
+        if ((uint64_t)b.width * b.height > (1ull << 26)) return fail(s, RT_ERR_CAPACITY, "batch request larger than 2^26 pixels");
+        pix_off[j + 1] = pix_off[j] + (uint64_t)b.width * b.height;
+    }
+    const uint64_t tot_pix = pix_off[n_jobs];
+    ENTER(s);
+    // packed accumulators (sum, M2, count) of every request
+    if (s->batch_pix < tot_pix) {
+        free_dev((void*&)s->b_acc); free_dev((void*&)s->b_m2); free_dev((void*&)s->b_cnt); free_dev((void*&)s->d_jobs);
+        s->batch_pix = 0;
+        if (cudaMalloc(&s->b_acc, tot_pix * 12) != cudaSuccess || cudaMalloc(&s->b_m2, tot_pix * 12) != cudaSuccess ||
+            cudaMalloc(&s->b_cnt, tot_pix * 4) != cudaSuccess)
+            return fail(s, RT_ERR_NOMEM, "cudaMalloc batch accumulators");
+        s->batch_pix = tot_pix;
+    }
+    if (s->jobs_cap < (uint32_t)n_jobs) {
+        free_dev((void*&)s->d_jobs);
+        s->jobs_cap = 0;
+        if (cudaMalloc(&s->d_jobs, (size_t)n_jobs * sizeof(JobDev)) != cudaSuccess)
+            return fail(s, RT_ERR_NOMEM, "cudaMalloc batch table");
+        s->jobs_cap = (uint32_t)n_jobs;
+    }
+    CK(cudaMemsetAsync(s->b_acc, 0, tot_pix * 12, s->stream));
+    CK(cudaMemsetAsync(s->b_m2, 0, tot_pix * 12, s->stream));
+    CK(cudaMemsetAsync(s->b_cnt, 0, tot_pix * 4, s->stream));
+    // samples per pixel per pass: as many as keep the pass's samples within 2 GiB
+    const uint64_t budget = (2ull << 30) / 12;
+    uint32_t W = window;
+    if (W == 0) {
+        uint32_t mx = 0;
+        for (int32_t j = 0; j < n_jobs; j++) mx = std::max(mx, jobs[j].spp);
+        W = 1;
+        for (uint32_t c = 2; c <= mx; c++) {
+            uint64_t need = 0;
+            for (int32_t j = 0; j < n_jobs; j++) need += (uint64_t)std::min(jobs[j].spp, c) * (pix_off[j + 1] - pix_off[j]);
+            if (need > budget) break;
+            W = c;
+        }
+    }
+    std::vector<uint32_t> left((size_t)n_jobs);
+    for (int32_t j = 0; j < n_jobs; j++) left[j] = jobs[j].spp;
+    std::vector<int> pass_of((size_t)n_jobs, -1);
+    std::vector<cudaEvent_t> evs;
+    cudaEvent_t e0;
+    CK(cudaEventCreate(&e0));
+    evs.push_back(e0);
+    CK(cudaEventRecord(e0, s->stream));
+    for (int k = 0; k < 4; k++) { s->kms[k] = 0.0; s->kcount[k] = 0; }
+    int64_t ext = 0, sh = 0, nl = 0;
+    RtPassParams q = *shared;
+    int rc = RT_OK;
+    for (int pass = 0; rc == RT_OK; pass++) {
+        std::vector<JobDev> tab;
+        std::vector<int32_t> ids;
+        uint64_t cursor = 0, floats = 0;
+        for (int32_t j = 0; j < n_jobs; j++) {
+            if (!left[j]) continue;
+            const RtBatchJob& b = jobs[j];
+            JobDev J{};
+            J.cam = b.cam;
+            J.width = b.width; J.height = b.height; J.npix = b.width * b.height; J.strata = b.strata;
+            J.nsamp = std::min(left[j], W);
+            J.sample_idx = b.sample_idx + (b.spp - left[j]);
+            J.first = cursor;
+            J.seed = b.seed;
+            J.scratch = reinterpret_cast<float*>(floats);        // offset now, pointer below
+            cursor += (uint64_t)J.nsamp * J.npix;
+            floats += (uint64_t)J.nsamp * J.npix * 3;
+            tab.push_back(J);
+            ids.push_back(j);
+        }
+        if (tab.empty()) break;
+        if (s->scratch_bytes < floats * 4) {
+            free_dev((void*&)s->scratch);
+            s->scratch_bytes = 0;
+            if (cudaMalloc(&s->scratch, floats * 4) != cudaSuccess) { rc = fail(s, RT_ERR_NOMEM, "cudaMalloc scratch"); break; }
+            s->scratch_bytes = floats * 4;
+        }
+        for (JobDev& J : tab) J.scratch = s->scratch + reinterpret_cast<uint64_t>(J.scratch);
+        if ((rc = ensure_paths(s, (uint32_t)std::min<uint64_t>(cursor, s->max_paths)))) break;
+        if (cudaMemcpyAsync(s->d_jobs, tab.data(), tab.size() * sizeof(JobDev), cudaMemcpyHostToDevice, s->stream) !=
+            cudaSuccess) { rc = fail(s, RT_ERR_CUDA, "batch table upload"); break; }
+        WaveBufs Wb = scene_bufs(s);
+        Wb.guide = false;
+        q.width = tab[0].width; q.height = tab[0].height;
+        int64_t e1 = 0, s1 = 0, l1 = 0;
+        rc = run_wavefront(s, Wb, &tab[0].cam, &q, 0, 1, s->scratch, nullptr, 1, &e1, &s1, &l1, s->d_jobs,
+                           (uint32_t)tab.size(), cursor);
+        if (rc) break;
+        for (size_t t = 0; t < tab.size(); t++) {
+            int32_t j = ids[t];
+            const JobDev& J = tab[t];
+            rth::launch_accumulate(J.scratch, J.nsamp, J.npix, s->b_acc + pix_off[j] * 3, s->b_m2 + pix_off[j] * 3,
+                                   s->b_cnt + pix_off[j], nullptr, 0.0f, 4u, 5.0f, s->stream);
+            left[j] -= J.nsamp;
+            if (!left[j]) pass_of[j] = pass + 1;
+        }
+        ext += e1; sh += s1; nl += l1 + (int64_t)tab.size();
+        cudaEvent_t ev;
+        if (cudaEventCreate(&ev) != cudaSuccess) { rc = fail(s, RT_ERR_CUDA, "cudaEventCreate"); break; }
+        evs.push_back(ev);
+        cudaEventRecord(ev, s->stream);
+    }
+    if (rc == RT_OK) {
+        auto kind = mem == RT_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+        if (out_sum && cudaMemcpyAsync(out_sum, s->b_acc, tot_pix * 12, kind, s->stream) != cudaSuccess) rc = RT_ERR_CUDA;
+        if (out_m2 && cudaMemcpyAsync(out_m2, s->b_m2, tot_pix * 12, kind, s->stream) != cudaSuccess) rc = RT_ERR_CUDA;
+        if (out_count && cudaMemcpyAsync(out_count, s->b_cnt, tot_pix * 4, kind, s->stream) != cudaSuccess) rc = RT_ERR_CUDA;
+        if (rc) rc = fail(s, rc, "batch output copy");
+    }
+    cudaStreamSynchronize(s->stream);
+    if (rc == RT_OK) {
+        std::vector<float> pass_ms(evs.size(), 0.0f);
+        for (size_t e = 1; e < evs.size(); e++) cudaEventElapsedTime(&pass_ms[e], evs[0], evs[e]);
+        if (done_ms)
+            for (int32_t j = 0; j < n_jobs; j++) done_ms[j] = pass_of[j] > 0 ? pass_ms[pass_of[j]] : 0.0f;
+        s->last_ms = pass_ms.back();
+        s->last_ext = ext;
+        s->last_shadow = sh;
+        s->last_launches = nl;
+    }
+    for (auto e : evs) cudaEventDestroy(e);
+    if (rc) return rc;
     return check_err(s);
 }
 

@@ -117,6 +117,18 @@ struct PhotonMapDev {
     rtph::Map view() const;
 };
 
+// One request of a packed batch pass: its camera and frame, the samples of
+// this pass (sample_idx .. sample_idx + nsamp − 1 of every pixel), where they
+// start in the pass's sample cursor, and where they are written.
+struct JobDev {
+    RtCamera cam;
+    uint32_t width, height, npix, strata, sample_idx, nsamp;
+    uint64_t first;            // first cursor value of this request
+    uint64_t seed;
+    float*   scratch;          // nsamp × npix × 3, slot-major
+};
+#define PF_JOB_SHIFT 16        // meta.z bits 16-31: the request of a packed batch path
+
 // One sample group of a render call: samples sample_idx .. sample_idx+nsamp−1
 // of every active pixel, traced by a pool of paths that is refilled with new
 // samples as paths end (sample g ↦ slot k = g / nactive, pixel active[g % nactive]).
@@ -133,6 +145,10 @@ struct RenderLaunch {
     float*   scratch;                      // nsamp × npix × 3 (device), slot-major
     int      photons;                      // a photon map feeds the diffuse vertices
     rtg::GuideDev guide;                   // learned proposal at diffuse vertices (mode 0: off)
+    // packed batch (n_jobs > 0): the requests, ascending in `first`; the cursor
+    // runs over all of them and width / height / cam / scratch above are unused
+    const JobDev* jobs;
+    uint32_t n_jobs;
 };
 
 namespace rth {

@@ -347,18 +347,40 @@ RT_D uint32_t tile_order_pixel(uint32_t j, uint32_t W, uint32_t H) {
 #endif
 }
 
+// The request of a packed batch that cursor value g belongs to (the last
+// whose first ≤ g)
+RT_D uint32_t batch_job(const RenderLaunch& R, uint64_t g) {
+    uint32_t lo = 0, hi = R.n_jobs - 1;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi + 1) >> 1;
+        if (R.jobs[mid].first <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 RT_D void init_path(const DevScene& S, const PathState& P, const RenderLaunch& R, uint32_t pid, uint64_t g) {
-    uint32_t k = (uint32_t)(g / R.nactive), j = (uint32_t)(g - (uint64_t)k * R.nactive);
-    uint32_t i = R.active ? __ldg(R.active + j) : tile_order_pixel(j, R.width, R.height);
-    uint32_t row = i / R.width, col = i - row * R.width;
-    uint32_t sample = R.sample_idx + k;
+    uint32_t job = 0, width = R.width, height = R.height, nact = R.nactive, strata = R.strata;
+    uint32_t sample0 = R.sample_idx;
+    uint64_t seed = R.seed;
+    const RtCamera* cp = &R.cam;
+    if (R.n_jobs) {
+        job = batch_job(R, g);
+        const JobDev& J = R.jobs[job];
+        g -= J.first;
+        width = J.width; height = J.height; nact = J.npix; strata = J.strata;
+        sample0 = J.sample_idx; seed = J.seed; cp = &J.cam;
+    }
+    uint32_t k = (uint32_t)(g / nact), j = (uint32_t)(g - (uint64_t)k * nact);
+    uint32_t i = R.active ? __ldg(R.active + j) : tile_order_pixel(j, width, height);
+    uint32_t row = i / width, col = i - row * width;
+    uint32_t sample = sample0 + k;
     P.L[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
     P.pend0[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
     P.pend1[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (R.photons) P.pendC[pid] = make_float4(0.f, 0.f, 0.f, 0.f);
-    Rng rng = make_rng(R.seed, i, sample);
-    float wd = (float)max(R.width - 1u, 1u), hd = (float)max(R.height - 1u, 1u);
-    uint32_t strata = R.strata, s2 = strata * strata, ray_y = R.height - 1u - row;
+    Rng rng = make_rng(seed, i, sample);
+    float wd = (float)max(width - 1u, 1u), hd = (float)max(height - 1u, 1u);
+    uint32_t s2 = strata * strata, ray_y = height - 1u - row;
     float uj, vj;
     if (s2 > 0) {
         uint32_t off = (i * 0x9E3779B9u) % s2;
@@ -369,7 +391,7 @@ RT_D void init_path(const DevScene& S, const PathState& P, const RenderLaunch& R
         uj = rnd(rng, D_JIT_U); vj = rnd(rng, D_JIT_V);
     }
     float u = ((float)col + uj) / wd, v = ((float)ray_y + vj) / hd;
-    const RtCamera& c = R.cam;
+    const RtCamera& c = *cp;
     float3 cu = mk(c.u[0], c.u[1], c.u[2]), cv = mk(c.v[0], c.v[1], c.v[2]);
     float3 org = mk(c.origin[0], c.origin[1], c.origin[2]);
     float3 rd;
@@ -403,7 +425,8 @@ RT_D void init_path(const DevScene& S, const PathState& P, const RenderLaunch& R
     P.ray_d[pid] = make_float4(d.x, d.y, d.z, 0.f);
     P.thr[pid] = make_float4(1.f, 1.f, 1.f, 1.f);
     P.wts[pid] = make_float4(1.f, H > 1 ? 1.f : 0.f, H > 2 ? 1.f : 0.f, H > 3 ? 1.f : 0.f);
-    P.meta[pid] = make_uint4(i, k, PF_PREV_SPEC | (H > 1 ? PF_SEC_ALIVE : 0u), __float_as_uint(lam0));
+    P.meta[pid] = make_uint4(i, k, PF_PREV_SPEC | (H > 1 ? PF_SEC_ALIVE : 0u) | (job << PF_JOB_SHIFT),
+                             __float_as_uint(lam0));
     if (R.guide.mode == 2) P.rec[pid] = rtg::REC_NONE;
 }
 
@@ -441,7 +464,13 @@ __global__ void __launch_bounds__(RETIRE_BLOCK) k_retire(DevScene S, PathState B
             L.x += a.x; L.y += a.y; L.z += a.z;
             L.x += b.x; L.y += b.y; L.z += b.z;
             uint4 meta = Rt.meta[j];
-            float* out = R.scratch + ((size_t)meta.y * R.npix + meta.x) * 3;
+            float* out;
+            if (R.n_jobs) {
+                const JobDev& J = R.jobs[meta.z >> PF_JOB_SHIFT];
+                out = J.scratch + ((size_t)meta.y * J.npix + meta.x) * 3;
+            } else {
+                out = R.scratch + ((size_t)meta.y * R.npix + meta.x) * 3;
+            }
             out[0] = L.x; out[1] = L.y; out[2] = L.z;
             if (R.guide.mode == 2) {
                 // weights of the path's guide records: radiance gathered after
@@ -707,7 +736,9 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
             bool prev_spec = flags & PF_PREV_SPEC;
             int tint = (flags & PF_TINT_MASK) >> PF_TINT_SHIFT;
             float lam0 = __uint_as_float(meta.w);
-            Rng rng = make_rng(R.seed, meta.x, R.sample_idx + meta.y);
+            Rng rng = R.n_jobs ? make_rng(R.jobs[meta.z >> PF_JOB_SHIFT].seed, meta.x,
+                                          R.jobs[meta.z >> PF_JOB_SHIFT].sample_idx + meta.y)
+                               : make_rng(R.seed, meta.x, R.sample_idx + meta.y);
             uint32_t b = D_BOUNCE0 + depth * D_PER_BOUNCE;
             float3 Lc = mk(L.x, L.y, L.z);
             if (R.guide.mode == 2) {

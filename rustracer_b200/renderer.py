@@ -53,6 +53,8 @@ def lib():
         L.rt_rgbe_decode.argtypes = [C.POINTER(C.c_uint8), C.c_size_t, i32, i32, C.POINTER(C.c_float)]
         L.rt_last_render_stats.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
         L.rt_render_pass_noalloc.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), vp]
+        L.rt_render_batch.argtypes = [vp, C.POINTER(abi.RtBatchJob), i32, C.POINTER(abi.RtPassParams), u32, vp, vp,
+                                      vp, vp, i32]
         L.rt_photon_build.argtypes = [vp, C.POINTER(abi.RtPhotonParams), C.POINTER(i64)]
         L.rt_photon_set.argtypes = [vp, vp, vp, vp, vp, i64, f, u32]
         L.rt_photon_clear.argtypes = [vp]
@@ -311,6 +313,42 @@ class GpuScene:
                                                int(firefly_min_samples), float(firefly_floor), 1 if reset else 0,
                                                sp, mp, cp, mem))
         return s, m, c
+
+    def render_batch(self, jobs, shared, window=0, outputs=None):
+        """A packed batch of requests on this scene (rt_render_batch).  jobs:
+        dicts with cam, width, height, spp and optionally strata (⌊√spp⌋),
+        sample_idx (0) and seed (0); shared: RtPassParams for max_depth,
+        hero_count and bg_scale.  Returns a list of (sum (h,w,3), m2 (h,w,3),
+        count (h,w)) per request — views of the packed outputs, numpy or the
+        CUDA tensors given as outputs=(sum, m2, count), flat — and done_ms, the
+        device time at which each request's last pass ended."""
+        arr = (abi.RtBatchJob * len(jobs))()
+        sizes = []
+        for k, j in enumerate(jobs):
+            b = arr[k]
+            b.cam = j["cam"]
+            b.width, b.height, b.spp = int(j["width"]), int(j["height"]), int(j["spp"])
+            b.strata = int(j.get("strata", int(np.sqrt(np.float32(b.spp)))))
+            b.sample_idx = int(j.get("sample_idx", 0))
+            b.seed = int(j.get("seed", 0)) & 0xFFFFFFFFFFFFFFFF
+            sizes.append((b.height, b.width))
+        tot = sum(h * w for h, w in sizes)
+        if outputs is None:
+            outputs = (np.zeros(tot * 3, np.float32), np.zeros(tot * 3, np.float32), np.zeros(tot, np.uint32))
+        s, m, c = outputs
+        sp, mem = _ptr(s)
+        mp, _ = _ptr(m)
+        cp, _ = _ptr(c)
+        done = np.zeros(len(jobs), np.float32)
+        self._order(s, m, c)
+        self._check(lib().rt_render_batch(self.h, arr, len(jobs), C.byref(shared), int(window), sp, mp, cp,
+                                          C.c_void_p(done.ctypes.data), mem))
+        out, o = [], 0
+        for h, w in sizes:
+            out.append((s[o * 3:(o + h * w) * 3].reshape(h, w, 3), m[o * 3:(o + h * w) * 3].reshape(h, w, 3),
+                        c[o:o + h * w].reshape(h, w)))
+            o += h * w
+        return out, done
 
     def develop(self, width, height, linear=None, exposure=1.0, tonemapper="agx", vignette=0.0, distortion=0.0,
                 out=None):

@@ -52,7 +52,7 @@ def test_ctypes_layouts_match_the_c_compiler(tmp_path):
     structs = {n: getattr(abi, n) for n in ("RtMaterial", "RtConvex", "RtShape", "RtTexture", "RtMedium",
                                              "RtBackground", "RtSceneDesc", "RtDevelopParams", "RtGuideParams",
                                              "RtCamera", "RtPassParams", "RtHit", "RtTuning", "RtPhotonEmitter",
-                                             "RtPhotonParams")}
+                                             "RtPhotonParams", "RtBatchJob")}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "rt_api.h"', "int main(void) {"]
     for n, t in structs.items():
         lines.append(f'printf("{n} %zu\\n", sizeof({n}));')
