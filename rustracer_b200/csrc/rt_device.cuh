@@ -120,6 +120,7 @@ struct DevScene {
     const DevMedium* media;
     int n_media;
     int n_pbr;                  // PBR materials in the scene (their shading kernel runs only if > 0)
+    uint32_t class_mask;        // bit per shading class some material of the scene can produce (host side)
     // analytic convex solids in leaf order: 2 float4 each, (plane offset, count,
     // material, polish) (canonical id, -, -, -); their world-space planes
     // (n.xyz, d); per plane the world-space shading normals of a front-face and

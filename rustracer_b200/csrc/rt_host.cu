@@ -1317,6 +1317,11 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
                  : t == RT_MAT_PBR ? 4 : 1;
     }
     if ((rc = upload(s, codes.data(), codes.size(), &s->S.mat_code))) return bail(rc);
+    // shading classes the scene can produce: a miss always, a hit's class from
+    // its material's code (launches of the other classes' kernels are skipped)
+    s->S.class_mask = 1u << CLS_MISS;
+    for (int32_t i = 0; i < d->n_mats; i++) s->S.class_mask |= 1u << (CLS_EMIT + codes[i]);
+    if (d->n_media > 0) s->S.class_mask |= 1u << CLS_MEDIUM;
 
     // ── participating media (scene_file.rs:962-983, volume.rs:88-97, 170-186) ─
     if (d->n_media < 0 || (d->n_media > 0 && !d->media)) return bail(fail(s, RT_ERR_INVALID, "bad media list"));
@@ -1850,9 +1855,9 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         rth::launch_shadow(s->S, T, W.sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, W.derr, s->sms, s->stream);
         mark(0);
         rth::launch_retire(s->S, B, W.Rt, R, c, hdr, blk(it + 2), cn + CTR_COUNT, s->sms, s->stream);
-        // extend, classify, shadow, retire, the shading classes other than media
-        // and PBR, and the PBR class when the scene has PBR materials
-        nl += 4 + (CLS_N - 2) + (s->S.n_pbr > 0 ? 1 : 0) + (R.guide.mode != 0 ? 2 : 0);
+        // extend, classify, shadow, retire, and one shading kernel per class the
+        // scene's materials produce (the medium class is counted with media)
+        nl += 4 + __builtin_popcount(s->S.class_mask & ~(1u << CLS_MEDIUM)) + (R.guide.mode != 0 ? 2 : 0);
         uint32_t slot = (uint32_t)(it % STATUS_RING);
         CK(cudaMemcpyAsync(s->h_status + slot, cn + CTR_COUNT, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
         CK(cudaEventRecord(s->st_ev[slot], s->stream));

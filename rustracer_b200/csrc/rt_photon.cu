@@ -718,15 +718,52 @@ RT_D float warp_radix_select(const float* v, uint32_t cnt, uint32_t k, uint32_t*
 // over the collected photons.  More candidates than PH_CAND_CAP: the
 // histogram-refinement path (warp_irradiance) instead.  Same estimate as
 // warp_irradiance; the terms are summed in another order.
+// An upper bound of the k-NN search's k-th distance: descend the box heap
+// toward p (the nearer child at every level) to a subtree of PH_SEED_LEAVES
+// leaves, and take the k-th smallest d² of its facing photons within the
+// maximum radius (r2max when it holds fewer than k).  The true k nearest are
+// at least as near, so every one of them lies within the bound.
+#define PH_SEED_LEAVES 4
+RT_D float seed_bound(const Map& M, float3 p, float3 n, WarpScratch& W) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t node = 0, pos = 0, span = M.nleaf_pow2;
+    while (span > PH_SEED_LEAVES) {
+        uint32_t l = 2 * node + 1, r = l + 1;
+        float dl = box_d2(__ldg(M.blo + l), __ldg(M.bhi + l), p), dr = box_d2(__ldg(M.blo + r), __ldg(M.bhi + r), p);
+        bool right = dr < dl;
+        node = right ? r : l;
+        pos = 2 * pos + (right ? 1u : 0u);
+        span >>= 1;
+    }
+    uint32_t first = pos * span * PH_LEAF, last = min(first + span * PH_LEAF, M.n);
+    uint32_t c = 0;
+    for (uint32_t i = first + lane; i < first + span * PH_LEAF; i += 32) {
+        float d2 = INFINITY;
+        if (i < last) {
+            float v = pdist2(__ldg(M.pos + i), p);
+            if (v < M.r2 && pdot(__ldg(M.nor + i), n) > 0.0f) d2 = v;
+        }
+        W.d2[i - first] = d2;
+        c += d2 < INFINITY;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    __syncwarp();
+    if (c < M.knn_k) return M.r2;
+    return warp_radix_select(W.d2, span * PH_LEAF, M.knn_k, W.hist);
+}
+
 RT_D float3 warp_irradiance_1pass(const Map& M, float3 p, float3 n, WarpScratch& W, uint32_t* hist, float* sel) {
     const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+    // the ball to collect: within the maximum radius and, in k-NN mode, within
+    // the seed subtree's k-th distance (inclusive, so ties at it are kept)
+    float bound = M.knn_k > 0 && M.knn_k <= PH_SEED_LEAVES * PH_LEAF ? seed_bound(M, p, n, W) : M.r2;
     uint32_t cnt = 0;
-    for_leaves(M, p, M.r2, [&](int i) {
+    for_leaves(M, p, bound, [&](int i) {
         bool c = false;
         float d2 = 0.0f;
         if (i >= 0) {
             d2 = pdist2(__ldg(M.pos + i), p);
-            c = d2 < M.r2 && pdot(__ldg(M.nor + i), n) > 0.0f;
+            c = d2 < M.r2 && d2 <= bound && pdot(__ldg(M.nor + i), n) > 0.0f;
         }
         uint32_t m = __ballot_sync(0xFFFFFFFFu, c);
         uint32_t slot = cnt + __popc(m & lt);
@@ -840,7 +877,9 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Ma
             a = gq[(size_t)i * 2];
             b = gq[(size_t)i * 2 + 1];
             float3 r;
-            uint32_t limit = M.knn_k > 0 ? M.knn_k : 64u;
+            // a lane gives a query to the warp once 16 photons are in range
+            // (below k every photon in range is used at the maximum radius)
+            uint32_t limit = M.knn_k > 0 ? min(M.knn_k, 16u) : 64u;
             if (rtph::lane_gather(M, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), M.r2, limit, &r)) {
                 uint32_t tag = __float_as_uint(a.w);
                 float4* pc = T.pendC[(tag >> 1) & 1u] + (tag >> 2);

@@ -1241,7 +1241,8 @@ void launch_shade(const DevScene& S, const PathState& A, const PathState& B, con
     if (R.guide.mode != 0)
         launch_guide_infer(S, A, R, Q.q[CLS_DIFFUSE], ctr + CTR_CLS_COUNT + CLS_DIFFUSE, sms, st);
 #define RT_SHADE_CLASS_G(C, G)                                                                              \
-    if (S.bg_type == RT_BG_PHYSICAL)                                                                        \
+    if (!((S.class_mask >> (C)) & 1u)) {                                                                   \
+    } else if (S.bg_type == RT_BG_PHYSICAL)                                                                 \
         k_shade<C, true, G><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr); \
     else                                                                                                    \
         k_shade<C, false, G><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr)

@@ -378,8 +378,14 @@ namespace rtk {
 // brings it back.  `cap` (7 per tree level, sized at scene creation) is never
 // reached by a traversal of the scene's own tree; a lower cap from
 // rt_set_tuning makes the traversal stop with RT_ERR_CAPACITY.
+// RT_STACK_LOCAL: the ring in the thread's local memory instead (measured
+// against the shared-memory ring; see the traversal notes)
+#ifndef RT_STACK_LOCAL
+#define RT_STACK_LOCAL 0
+#endif
+constexpr int RING_STRIDE = RT_STACK_LOCAL ? 1 : RT_TRACE_BLOCK;
 struct TStack {
-    uint32_t* ring;          // &shared[threadIdx.x]; ring slot k at ring[k · RT_TRACE_BLOCK]
+    uint32_t* ring;          // &shared[threadIdx.x]; ring slot k at ring[k · RING_STRIDE]
     uint32_t* spill;         // &S.stack_spill[global thread]; entry e at spill[(e − ring_n) · stride]
     uint32_t stride;
     int sp, cap;
@@ -388,22 +394,22 @@ struct TStack {
     RT_D bool room(int k) const { return sp + k <= cap; }
     RT_D void push(uint32_t v) {
         int slot = sp & (ring_n - 1);
-        if (sp >= ring_n) spill[(size_t)(sp - ring_n) * stride] = ring[slot * RT_TRACE_BLOCK];
-        ring[slot * RT_TRACE_BLOCK] = v;
+        if (sp >= ring_n) spill[(size_t)(sp - ring_n) * stride] = ring[slot * RING_STRIDE];
+        ring[slot * RING_STRIDE] = v;
         sp++;
     }
     RT_D uint32_t pop() {
         sp--;
         int slot = sp & (ring_n - 1);
-        uint32_t v = ring[slot * RT_TRACE_BLOCK];
-        if (sp >= ring_n) ring[slot * RT_TRACE_BLOCK] = spill[(size_t)(sp - ring_n) * stride];
+        uint32_t v = ring[slot * RING_STRIDE];
+        if (sp >= ring_n) ring[slot * RING_STRIDE] = spill[(size_t)(sp - ring_n) * stride];
         return v;
     }
 };
 
-RT_D TStack make_stack(const DevScene& S, uint32_t* shared_ring) {
+RT_D TStack make_stack(const DevScene& S, uint32_t* ring_base) {
     TStack st;
-    st.ring = shared_ring + threadIdx.x;
+    st.ring = RT_STACK_LOCAL ? ring_base : ring_base + threadIdx.x;
     st.stride = gridDim.x * blockDim.x;
     st.spill = S.stack_spill + blockIdx.x * blockDim.x + threadIdx.x;
     st.sp = 0;
@@ -556,7 +562,11 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
                                                             int4* __restrict__ out, int* err) {
     const uint32_t n = MODE == 0 ? *count : n_api;
     const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+#if RT_STACK_LOCAL
+    uint32_t ring[RT_SHORT_STACK];
+#else
     __shared__ uint32_t ring[RT_SHORT_STACK * RT_TRACE_BLOCK];
+#endif
     rtk::TStack stk = rtk::make_stack(S, ring);
     bool active = false, exhausted = false, ok = true;
     uint32_t item = 0, node = 0, pid = 0;
@@ -629,7 +639,11 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
                                                         uint8_t* __restrict__ out, int* err) {
     const uint32_t n = MODE != 1 ? *count : n_api;
     const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+#if RT_STACK_LOCAL
+    uint32_t ring[RT_SHORT_STACK];
+#else
     __shared__ uint32_t ring[RT_SHORT_STACK * RT_TRACE_BLOCK];
+#endif
     rtk::TStack stk = rtk::make_stack(S, ring);
     bool active = false, exhausted = false, ok = true;
     uint32_t item = 0, node = 0, tag = 0;
