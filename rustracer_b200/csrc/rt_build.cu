@@ -442,7 +442,7 @@ __global__ void k_preorder(const int32_t* __restrict__ lvl, int32_t m, const int
 // children by preorder index, leaves for now as RT_LEAF_BIT | leaf slot
 __global__ void k_write_nodes(const int32_t* __restrict__ order, int32_t m, const int32_t* __restrict__ kids,
                               const int32_t* __restrict__ nk, const int32_t* __restrict__ P,
-                              const int32_t* __restrict__ LB, const float* __restrict__ bbox,
+                              const int32_t* __restrict__ LB, const int32_t* __restrict__ L, const float* __restrict__ bbox,
                               const float* __restrict__ box, const int32_t* __restrict__ idx, float4* nodes,
                               int32_t* export_ch, int32_t* leaf_gid) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
@@ -457,6 +457,7 @@ __global__ void k_write_nodes(const int32_t* __restrict__ order, int32_t m, cons
                 ref = RT_EMPTY_REF; ex = INT32_MIN;
             } else if (k >= 0) {
                 ref = (uint32_t)P[k]; ex = P[k]; cb = bbox + (size_t)k * 6;
+                ol += L[k];                                  // the inner kid's leaves come first
             } else {
                 int32_t slot = ol++, prim = idx[-k - 1];
                 leaf_gid[slot] = prim;
@@ -642,7 +643,7 @@ static cudaError_t collapse_wide(const int32_t* bl, const int32_t* br, const flo
     if (e == cudaSuccess) {
         int32_t m = lvl_off.back();
         k_write_nodes<<<std::max(1, std::min((m + 127) / 128, grid)), 128, 0, st>>>(
-            order, m, kids, nk, P, LB, bbox, box, idx, W->nodes, W->export_ch, leaf_gid);
+            order, m, kids, nk, P, LB, L, bbox, box, idx, W->nodes, W->export_ch, leaf_gid);
         k_leaf_types<<<grid, 256, 0, st>>>(leaf_gid, n, W->type_end[0], W->type_end[1], W->type_end[2], flags);
         for (int t = 0; t < 4; t++) scan(flags + (size_t)t * n, scans + (size_t)t * n, n);
         k_fix_leaf_refs<<<grid, 256, 0, st>>>(W->nodes, W->n_nodes, leaf_gid, n, W->type_end[0], W->type_end[1],

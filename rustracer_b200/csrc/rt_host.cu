@@ -1044,6 +1044,14 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         // leaf order per type
         std::vector<int32_t> typed_slot(s->n_leaves);
         std::vector<int64_t> order_tri, order_quad, order_sph, order_cvx;
+        if (dev_wide) {   // the device's leaf order must be a permutation of the primitives
+            std::vector<uint8_t> seen((size_t)n, 0);
+            for (int64_t k = 0; k < s->n_leaves; k++) {
+                int64_t g = s->leaf_gids[k];
+                if (g < 0 || g >= n || seen[g]) return bail(fail(s, RT_ERR_CUDA, "device BVH collapse: invalid leaf order"));
+                seen[g] = 1;
+            }
+        }
         for (int64_t k = 0; k < s->n_leaves; k++) {
             int64_t g = s->leaf_gids[k];
             if (g < d->n_tris) { typed_slot[k] = (int32_t)order_tri.size(); order_tri.push_back(g); }
