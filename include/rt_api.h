@@ -580,14 +580,14 @@ typedef struct RtTuning {
      * results never depend on it; small rings make every traversal take the
      * spill path. */
     uint32_t stack_ring;
-    /* Node layout the traversal reads: RT_NODES_QUANTISED (0, the default
-     * when the scene's extents allow it) — 128-byte nodes whose child boxes
-     * are 8-bit offsets rounded outward, so the hits are unchanged — or
-     * RT_NODES_FULL (1), the reference's 224-byte float layout (bvh.rs:25-32). */
+    /* Node layout the traversal reads: RT_NODES_FULL (0, the default), the
+     * reference's 224-byte float layout (bvh.rs:25-32), or RT_NODES_QUANTISED
+     * (1, when the scene's extents allow it), 128-byte nodes whose child boxes
+     * are 8-bit offsets rounded outward, so the hits are unchanged. */
     uint32_t node_format;
 } RtTuning;
-#define RT_NODES_QUANTISED 0
-#define RT_NODES_FULL      1
+#define RT_NODES_FULL      0
+#define RT_NODES_QUANTISED 1
 int32_t rt_set_tuning(RtScene* scene, const RtTuning* tuning);
 
 /* The stream the caller queues its own work on (a cudaStream_t; NULL = the

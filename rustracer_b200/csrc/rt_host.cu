@@ -1190,10 +1190,10 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
             s->S.nodes = W.nodes;
             s->S.qnodes = W.qnodes;
             s->qnodes_ok = W.qnodes != nullptr;
-            s->S.node_format = s->qnodes_ok ? RT_NODES_QUANTISED : RT_NODES_FULL;
+            s->S.node_format = RT_NODES_FULL;
         } else if ((rc = upload(s, gnodes.data(), gnodes.size(), &s->S.nodes))) {
             return bail(rc);
-        } else {   // the quantised copy of the nodes (rt_set_tuning node_format 0, the default)
+        } else {   // the quantised copy of the nodes (rt_set_tuning node_format RT_NODES_QUANTISED)
             std::vector<float4> qn((size_t)s->n_nodes * 8);
             bool qok = true;
             for (int64_t k = 0; k < s->n_nodes && qok; k++)
@@ -1202,7 +1202,7 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
                 if ((rc = upload(s, qn.data(), qn.size(), &s->S.qnodes))) return bail(rc);
                 s->qnodes_ok = true;
             }
-            s->S.node_format = qok ? RT_NODES_QUANTISED : RT_NODES_FULL;
+            s->S.node_format = RT_NODES_FULL;
         }
         if ((rc = upload(s, gtri.data(), gtri.size(), &s->S.tri))) return bail(rc);
         if ((rc = upload(s, gtri_n.data(), gtri_n.size(), &s->S.tri_n))) return bail(rc);

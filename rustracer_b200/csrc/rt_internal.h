@@ -17,8 +17,15 @@
 #ifndef RT_TRACE_MINB
 #define RT_TRACE_MINB 6
 #endif
-// traversal stack: RT_SHORT_STACK entries per thread in shared memory (a
-// ring), deeper entries spilled to a per-thread column of global memory
+// the traversal stack's ring in local memory (1) or shared memory (0): a
+// shared ring reserves 8 KB per block of the SM's L1 / shared storage, and the
+// node fetches lose more to the smaller L1 than the stack gains (measured on
+// the icosphere workload: extend 67.5 ms shared, 62.8 ms local)
+#ifndef RT_STACK_LOCAL
+#define RT_STACK_LOCAL 1
+#endif
+// traversal stack: RT_SHORT_STACK entries per thread in a ring (local or
+// shared memory), deeper entries spilled to a per-thread column of global memory
 // sized from the tree depth at scene creation (7 per level: a visit pushes
 // at most 7 of its 8 children), so a traversal never runs out of stack
 #define RT_SHORT_STACK 16

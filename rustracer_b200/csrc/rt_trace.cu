@@ -369,23 +369,19 @@ namespace rtk {
 
 // Per-thread traversal stack (the reference keeps 128 entries inline and
 // spills to a heap Vec, bvh.rs:229-239).  The newest RT_SHORT_STACK entries
-// live in a shared-memory ring laid out [entry][thread], so the lanes of a
-// warp always hit 32 different banks whatever their depths; entry e ≥
-// RT_SHORT_STACK of a deeper stack waits in the thread's global column
-// spill[(e − RT_SHORT_STACK) · stride] (rt_set_tuning can shrink the ring to
-// fewer slots, so the tests run every traversal through the spill path).  A push beyond the ring first moves the
-// ring slot's old entry to its column, a pop that uncovers a spilled entry
-// brings it back.  `cap` (7 per tree level, sized at scene creation) is never
-// reached by a traversal of the scene's own tree; a lower cap from
-// rt_set_tuning makes the traversal stop with RT_ERR_CAPACITY.
-// RT_STACK_LOCAL: the ring in the thread's local memory instead (measured
-// against the shared-memory ring; see the traversal notes)
-#ifndef RT_STACK_LOCAL
-#define RT_STACK_LOCAL 0
-#endif
+// live in a ring: the thread's local memory (RT_STACK_LOCAL, the default) or
+// shared memory laid out [entry][thread], so the lanes of a warp hit 32
+// different banks whatever their depths.  Entry e ≥ RT_SHORT_STACK of a
+// deeper stack waits in the thread's global column spill[(e − RT_SHORT_STACK)
+// · stride] (rt_set_tuning can shrink the ring to fewer slots, so the tests
+// run every traversal through the spill path).  A push beyond the ring first
+// moves the ring slot's old entry to its column, a pop that uncovers a
+// spilled entry brings it back.  `cap` (7 per tree level, sized at scene
+// creation) is never reached by a traversal of the scene's own tree; a lower
+// cap from rt_set_tuning makes the traversal stop with RT_ERR_CAPACITY.
 constexpr int RING_STRIDE = RT_STACK_LOCAL ? 1 : RT_TRACE_BLOCK;
 struct TStack {
-    uint32_t* ring;          // &shared[threadIdx.x]; ring slot k at ring[k · RING_STRIDE]
+    uint32_t* ring;          // ring slot k at ring[k · RING_STRIDE] (shared: &ring[threadIdx.x])
     uint32_t* spill;         // &S.stack_spill[global thread]; entry e at spill[(e − ring_n) · stride]
     uint32_t stride;
     int sp, cap;

@@ -26,7 +26,7 @@ def test_autotune_picks_the_fastest_and_caches_it():
 
     def timer(t):
         calls.append(t)
-        # fastest at 4M paths, 6 traversal blocks, 8 shading blocks, quantised nodes
+        # fastest at 4M paths, 6 traversal blocks, 8 shading blocks, full nodes
         return abs(t["max_paths"] - (1 << 22)) / 1e6 + abs(t["trace_blocks_per_sm"] - 6) + \
             abs(t["shade_blocks_per_sm"] - 8) + t["node_format"] + 1.0
     best, table = autotune.autotune(g, None, pass_params(64, 64), key="k", timer=timer, repeats=2)

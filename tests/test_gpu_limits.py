@@ -103,17 +103,17 @@ def test_node_layouts_give_identical_hits_and_images():
     same hits bit for bit, hence the same image; the oracle agrees."""
     sb, st = configs.icosphere_scene(env_w=64, env_h=32)
     g, o = GpuScene(sb), O.OracleScene(sb)
-    assert g.get_tuning()["node_format"] == 0
+    assert g.get_tuning()["node_format"] == 0          # the full layout is the default
     r = np.concatenate([random_rays(30000, 41, spread=0.7), camera_rays(st["camera"], 200, 100, seed=6)])
     q = g.trace_closest(r)
     qa = g.trace_any(r)
     _hits_equal(q[:8000], o.trace_closest(r[:8000]))
-    g.set_tuning(node_format=1)
+    g.set_tuning(node_format=1)                        # quantised
     _hits_equal(g.trace_closest(r), q)
     assert np.array_equal(g.trace_any(r), qa)
     p = pass_params(64, 36, 0, 2, 1, 12, 4, 1.0, 3)
     cam = configs.make_camera((0.0, 0.45, 3.6), (0.0, -0.15, 0.0), vfov=40.0, aspect=64 / 36)
-    full = g.render_pass(cam, p)
-    g.set_tuning(node_format=0)
     quant = g.render_pass(cam, p)
+    g.set_tuning(node_format=0)
+    full = g.render_pass(cam, p)
     assert np.array_equal(full.view(np.uint32), quant.view(np.uint32))
