@@ -604,7 +604,8 @@ int32_t rt_get_tuning(const RtScene* scene, RtTuning* tuning);
  * renderer.rs:545-571).
  *
  * A 16-level hash grid of the hit position (2 features per level, 2^19
- * entries per level) and a one-blob encoding of the shading normal feed a
+ * entries per level) and a one-blob encoding of the outgoing direction ω_o
+ * (toward the previous path vertex) feed a
  * 64-64-64 ReLU MLP (BF16 weights and activations, FP32 accumulation) whose
  * 41 outputs are 8 von Mises–Fisher lobes (mean, log κ, mixture logit) and a
  * guide fraction α ≤ alpha_max.  With guiding on, a Lambertian bounce is drawn with
@@ -641,14 +642,14 @@ int32_t rt_guide_mode(RtScene* scene, int32_t mode);
 /* Copy the RT_GUIDE_PARAMS fp32 parameters out (write = 0) or in (write = 1;
  * also clears the Adam moments and step count).  Host memory. */
 int32_t rt_guide_params(RtScene* scene, float* params, int32_t write);
-/* Network outputs at q (n × 6: position, unit normal) into raw (n × 41). */
+/* Network outputs at q (n × 9: position, unit normal, unit ω_o) into raw (n × 41). */
 int32_t rt_guide_eval(RtScene* scene, const float* q, int64_t n, float* raw, int32_t mem);
 /* Mixture density (guide and cosine lobe) at unit directions dirs (n × 3). */
 int32_t rt_guide_pdf(RtScene* scene, const float* q, const float* dirs, int64_t n, float* pdf, int32_t mem);
 /* One-sample draw with u (n × 4: strategy, lobe, two direction numbers) →
  * out (n × 4: direction, mixture density), the draw the shading kernel makes. */
 int32_t rt_guide_sample(RtScene* scene, const float* q, const float* u, int64_t n, float* out, int32_t mem);
-/* Loss Σ −w·log p over samples (n × 10: position, normal, direction, weight)
+/* Loss Σ −w·log p over samples (n × 13: position, normal, ω_o, direction, weight)
  * and its gradient (RT_GUIDE_PARAMS floats, the loss divided by n) — no
  * update.  Host memory. */
 int32_t rt_guide_loss_grad(RtScene* scene, const float* samples, int64_t n, float* loss, float* grad);

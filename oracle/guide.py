@@ -12,8 +12,9 @@ the GPU network is built from, at the GPU's rounding points:
     BF16; the float32 master is what Adam updates), dense
     indexing where (res+1)^3 fits, else x ⊕ 2654435761·y ⊕ 805459861·z;
     trilinear weights and sums in float32, in corner order 0..7;
-  * one-blob encoding of the normal (Müller et al. 2019, "Neural importance
-    sampling"), 16 bins for θ/π and 16 for φ/2π;
+  * one-blob encoding of the outgoing direction ω_o (Müller et al. 2019,
+    "Neural importance sampling"), 16 bins for θ/π and 16 for φ/2π; the
+    normal enters only the cosine lobe of the mixture;
   * a 64-64-64-64-48 ReLU MLP without biases, BF16 weights, inputs and
     activations (round to nearest even) with products summed exactly here
     (float64) and rounded to float32 — the GPU sums in float32 on the tensor
@@ -76,9 +77,10 @@ def normalise(P, lo, inv):
     return np.clip(((np.asarray(P, f32) - np.asarray(lo, f32)).astype(f32) * np.asarray(inv, f32)).astype(f32), 0, 1)
 
 
-def encode(params, res, lo, inv, P, N):
+def encode(params, res, lo, inv, P, WO):
     """(n, 64) BF16-rounded inputs: hash-grid features of P (from the BF16
-    copy of the table the GPU gathers from), one-blob of N."""
+    copy of the table the GPU gathers from), one-blob of the unit outgoing
+    directions WO."""
     table = bf16(params[N_MLP:]).reshape(LEVELS, TSIZE, 2)
     pn = normalise(P, lo, inv)
     n = len(pn)
@@ -98,15 +100,21 @@ def encode(params, res, lo, inv, P, N):
             a1 = (a1 + (w * v[:, 1]).astype(f32)).astype(f32)
         enc[:, 2 * l] = a0
         enc[:, 2 * l + 1] = a1
-    N = np.asarray(N, f32)
-    th = (np.arccos(np.clip(N[:, 2], -1, 1)).astype(f32) * f32(0.318309886)).astype(f32)
-    ph = ((np.arctan2(N[:, 1], N[:, 0]).astype(f32) + f32(3.14159265)) * f32(0.159154943)).astype(f32)
+    th, ph = blob_angles(WO)
     for k in range(16):
         d0 = (f32(16) * th - f32(k + 0.5)).astype(f32)
         d1 = (f32(16) * ph - f32(k + 0.5)).astype(f32)
         enc[:, 32 + k] = np.exp(f32(-0.5) * d0 * d0)
         enc[:, 48 + k] = np.exp(f32(-0.5) * d1 * d1)
     return bf16(enc)
+
+
+def blob_angles(D):
+    """θ/π and φ/2π of unit directions D (n, 3), float32 as the GPU forms them."""
+    D = np.asarray(D, f32)
+    th = (np.arccos(np.clip(D[:, 2], -1, 1)).astype(f32) * f32(0.318309886)).astype(f32)
+    ph = ((np.arctan2(D[:, 1], D[:, 0]).astype(f32) + f32(3.14159265)) * f32(0.159154943)).astype(f32)
+    return th, ph
 
 
 def weights(params):
@@ -196,13 +204,14 @@ def loss_grad(o, N, D, w, scale, amax=AMAX, lkmax=LKMAX):
 
 
 def loss_and_grad(params, res, lo, inv, samples, amax=AMAX, lkmax=LKMAX):
-    """Σ loss (−w·log p_mix) and the training gradient over all parameters
+    """Σ loss (−w·log p_mix) of samples (n × 13: position, normal, ω_o,
+    direction, weight) and the training gradient over all parameters
     (loss_grad's objectives over n), following the GPU's rounding points: dO, dZ in BF16, weight gradients summed exactly,
     hash-grid gradients as float32 products scattered per corner."""
-    s = np.asarray(samples, f32).reshape(-1, 10)
+    s = np.asarray(samples, f32).reshape(-1, 13)
     n = len(s)
-    P, N, D, w = s[:, 0:3], s[:, 3:6], s[:, 6:9], s[:, 9]
-    X = encode(params, res, lo, inv, P, N)
+    P, N, WO, D, w = s[:, 0:3], s[:, 3:6], s[:, 6:9], s[:, 9:12], s[:, 12]
+    X = encode(params, res, lo, inv, P, WO)
     O, (X, H1, H2, H3) = forward(params, X)
     W = weights(params)
     valid = w > 0

@@ -95,9 +95,11 @@ RTG_D void load_weights_t(const __nv_bfloat16* __restrict__ wbf, __nv_bfloat16* 
 // Evaluate 32 points per warp; emit(mt, outputs) runs on lanes 0..15 for row 16·mt + lane.
 template <class Emit>
 RTG_D void warp_eval(const GuideDev& G, const __nv_bfloat16* Ws, __nv_bfloat16* S_in, float* S_o, bool valid,
-                     float3 p, float3 n, Emit emit) {
+                     float3 p, float3 wo, Emit emit) {
     int lane = threadIdx.x & 31;
-    if (valid) encode_row(G, G.tbf, p, n, S_in + lane * LDW);
+    float th, ph;
+    blob_angles(wo, &th, &ph);
+    if (valid) encode_row(G, G.tbf, p, th, ph, S_in + lane * LDW);
     else
         for (int k = 0; k < NIN; k++) S_in[lane * LDW + k] = __float2bfloat16_rn(0.0f);
     __syncwarp();
@@ -113,7 +115,7 @@ RTG_D void warp_eval(const GuideDev& G, const __nv_bfloat16* Ws, __nv_bfloat16* 
     }
 }
 
-// rt_guide_eval / _pdf / _sample: q is n × 6 (position, unit normal)
+// rt_guide_eval / _pdf / _sample: q is n × 9 (position, unit normal, unit ω_o)
 __global__ void __launch_bounds__(GW * 32) k_guide_api(GuideDev G, const float* __restrict__ q, uint32_t n,
                                                         const float* __restrict__ dirs, const float* __restrict__ u,
                                                         float* __restrict__ raw, float* __restrict__ out) {
@@ -127,12 +129,12 @@ __global__ void __launch_bounds__(GW * 32) k_guide_api(GuideDev G, const float* 
     for (uint32_t base = (blockIdx.x * GW + warp) * 32; base < n; base += gridDim.x * GW * 32) {
         uint32_t i = base + lane;
         bool valid = i < n;
-        float3 p = make_float3(0.f, 0.f, 0.f), nn = make_float3(0.f, 0.f, 1.f);
+        float3 p = make_float3(0.f, 0.f, 0.f), wo = make_float3(0.f, 0.f, 1.f);
         if (valid) {
-            p = make_float3(q[i * 6], q[i * 6 + 1], q[i * 6 + 2]);
-            nn = make_float3(q[i * 6 + 3], q[i * 6 + 4], q[i * 6 + 5]);
+            p = make_float3(q[i * 9], q[i * 9 + 1], q[i * 9 + 2]);
+            wo = make_float3(q[i * 9 + 6], q[i * 9 + 7], q[i * 9 + 8]);
         }
-        warp_eval(G, Ws, S_in, S_o, valid, p, nn, [&](int mt, const float* o) {
+        warp_eval(G, Ws, S_in, S_o, valid, p, wo, [&](int mt, const float* o) {
             uint32_t r = base + 16 * mt + lane;
             if (r >= n) return;
             if (raw)
@@ -140,7 +142,7 @@ __global__ void __launch_bounds__(GW * 32) k_guide_api(GuideDev G, const float* 
             if (!out) return;
             float4 gp[GP_F4];
             mixture_from_outputs(o, gp, G.amax, G.lkmax);
-            float nx = q[r * 6 + 3], ny = q[r * 6 + 4], nz = q[r * 6 + 5];
+            float nx = q[r * 9 + 3], ny = q[r * 9 + 4], nz = q[r * 9 + 5];
             if (dirs) {
                 out[r] = guide_pdf(gp, nx, ny, nz, dirs[r * 3], dirs[r * 3 + 1], dirs[r * 3 + 2]);
             } else if (u) {
@@ -160,19 +162,21 @@ __global__ void __launch_bounds__(GW * 32) k_guide_api(GuideDev G, const float* 
     }
 }
 
-// records of a render call → training samples (3 float4 each: (p, w), (n, -), (ω_i, -))
+// records of a render call → training samples (3 float4 each: (p, w), (n, θ_o/π),
+// (ω_i, φ_o/2π), the angles being ω_o's one-blob coordinates)
 __global__ void k_compact(const float4* __restrict__ ra, const float4* __restrict__ rb, const float4* __restrict__ rc,
-                          const float* __restrict__ rw, const uint32_t* counters, uint32_t cap, float4* train,
-                          uint32_t* ntrain) {
+                          const float2* __restrict__ ro, const float* __restrict__ rw, const uint32_t* counters,
+                          uint32_t cap, float4* train, uint32_t* ntrain) {
     uint32_t n = min(counters[0], cap);
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         float w = rw[r];
         if (!(w > 0.0f) || !isfinite(w)) continue;
         uint32_t j = atomicAdd(ntrain, 1u);
         float4 a = ra[r], b = rb[r], c = rc[r];
+        float2 ang = ro[r];
         train[(size_t)j * 3] = make_float4(a.x, a.y, a.z, w);
-        train[(size_t)j * 3 + 1] = make_float4(b.x, b.y, b.z, 0.f);
-        train[(size_t)j * 3 + 2] = make_float4(c.x, c.y, c.z, 0.f);
+        train[(size_t)j * 3 + 1] = make_float4(b.x, b.y, b.z, ang.x);
+        train[(size_t)j * 3 + 2] = make_float4(c.x, c.y, c.z, ang.y);
     }
 }
 
@@ -224,8 +228,7 @@ __global__ void __launch_bounds__(GW * 32) k_train(GuideDev G, TrainArgs A) {
     for (uint32_t base = (blockIdx.x * GW + warp) * 32; base < A.batch; base += gridDim.x * GW * 32) {
         float4 s[3];
         bool valid = train_row(A, base + lane, n, s);
-        if (valid) encode_row(G, G.tbf, make_float3(s[0].x, s[0].y, s[0].z), make_float3(s[1].x, s[1].y, s[1].z),
-                              S_in + lane * LDW);
+        if (valid) encode_row(G, G.tbf, make_float3(s[0].x, s[0].y, s[0].z), s[1].w, s[2].w, S_in + lane * LDW);
         else
             for (int k = 0; k < NIN; k++) S_in[lane * LDW + k] = __float2bfloat16_rn(0.0f);
         __syncwarp();
@@ -406,6 +409,7 @@ struct Guide {
     uint4* enc = nullptr;            // encoded inputs of the diffuse queue (128 B per path slot)
     uint32_t gpar_cap = 0;
     float4 *rec_a = nullptr, *rec_b = nullptr, *rec_c = nullptr;
+    float2* rec_o = nullptr;
     float* rec_w = nullptr;
     uint32_t* counters = nullptr;   // records, training samples
     float4* train = nullptr;
@@ -420,7 +424,7 @@ struct Guide {
 
 void destroy(Guide* g) {
     if (!g) return;
-    void* ptrs[] = {g->params, g->grad, g->m, g->v, g->wbf, g->tbf, g->act, g->gpar, g->enc, g->rec_a, g->rec_b, g->rec_c,
+    void* ptrs[] = {g->params, g->grad, g->m, g->v, g->wbf, g->tbf, g->act, g->gpar, g->enc, g->rec_a, g->rec_b, g->rec_c, g->rec_o,
                     g->rec_w, g->counters, g->train, g->loss};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -466,6 +470,7 @@ Guide* create(const RtGuideParams& p, const float scene_lo[3], const float scene
               cudaMalloc(&g->rec_a, (size_t)g->rec_cap * 16) == cudaSuccess &&
               cudaMalloc(&g->rec_b, (size_t)g->rec_cap * 16) == cudaSuccess &&
               cudaMalloc(&g->rec_c, (size_t)g->rec_cap * 16) == cudaSuccess &&
+              cudaMalloc(&g->rec_o, (size_t)g->rec_cap * 8) == cudaSuccess &&
               cudaMalloc(&g->rec_w, (size_t)g->rec_cap * 4) == cudaSuccess &&
               cudaMalloc(&g->train, (size_t)g->rec_cap * 48) == cudaSuccess && alloc_act(g, p.batch) &&
               cudaEventCreate(&g->e0) == cudaSuccess && cudaEventCreate(&g->e1) == cudaSuccess;
@@ -523,7 +528,7 @@ GuideDev view(const Guide* g) {
     d.lkmax = g->prm.log_kappa_max;
     d.gpar = g->gpar;
     d.enc = g->enc;
-    d.rec_a = g->rec_a; d.rec_b = g->rec_b; d.rec_c = g->rec_c; d.rec_w = g->rec_w;
+    d.rec_a = g->rec_a; d.rec_b = g->rec_b; d.rec_c = g->rec_c; d.rec_o = g->rec_o; d.rec_w = g->rec_w;
     d.rec_count = g->counters;
     d.rec_cap = g->rec_cap;
     return d;
@@ -625,7 +630,7 @@ cudaError_t train_pass(Guide* g, int sms, cudaStream_t st, int64_t* launches) {
     if (g->mode != 2) return cudaSuccess;
     cudaError_t e;
     cudaEventRecord(g->e0, st);
-    k_compact<<<sms * 8, 256, 0, st>>>(g->rec_a, g->rec_b, g->rec_c, g->rec_w, g->counters, g->rec_cap, g->train,
+    k_compact<<<sms * 8, 256, 0, st>>>(g->rec_a, g->rec_b, g->rec_c, g->rec_o, g->rec_w, g->counters, g->rec_cap, g->train,
                                        g->counters + 1);
     uint32_t cnt[2];
     if ((e = cudaMemcpyAsync(cnt, g->counters, 8, cudaMemcpyDeviceToHost, st))) return e;

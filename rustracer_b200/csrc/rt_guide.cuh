@@ -4,8 +4,10 @@
 //
 // Network: position → 16-level hash grid (2 features per level, 2^19 entries
 // per level, trilinear, the hashing of Müller et al. 2022 "Instant neural
-// graphics primitives"), shading normal → one-blob encoding (16 bins for each
-// of θ/π and φ/2π, Müller et al. 2019 "Neural importance sampling"); the 64
+// graphics primitives"), the outgoing direction ω_o (toward the previous vertex)
+// → one-blob encoding (16 bins for each of θ/π and φ/2π, Müller et al. 2019
+// "Neural importance sampling"); the shading normal enters only the cosine
+// lobe of the mixture; the 64
 // inputs pass three ReLU layers of width 64 and an output layer of 41 (padded
 // to 48), no biases.  Weights and activations are BF16, products accumulate in
 // FP32 on the tensor cores (mma.sync m16n8k16; one warp evaluates 16 rows).
@@ -50,6 +52,7 @@ struct GuideDev {
     float4* gpar;                     // GP_F4 float4 per path slot
     uint4* enc;                       // encoded inputs of the diffuse queue (8 uint4 per entry)
     float4 *rec_a, *rec_b, *rec_c;    // records: (p, Σ T·sf), (n, base Σ L), (ω_i, prev record)
+    float2* rec_o;                    // records: one-blob angles (θ/π, φ/2π) of ω_o
     float* rec_w;                     // weight of each record, set when its path retires
     uint32_t* rec_count;
     uint32_t rec_cap;
@@ -92,8 +95,15 @@ RTG_D uint32_t pack_bf2(float lo, float hi);
 RTG_D float bf_lo(uint32_t u);
 RTG_D float bf_hi(uint32_t u);
 
-// The 64 network inputs of one point, rounded to bf16, as 32 packed pairs.
-RTG_D void encode_packed(const GuideDev& G, const __nv_bfloat162* __restrict__ table, float3 p, float3 n,
+// The one-blob coordinates of a unit direction: θ/π and φ/2π.
+RTG_D void blob_angles(float3 d, float* th, float* ph) {
+    *th = acosf(fminf(fmaxf(d.z, -1.0f), 1.0f)) * 0.318309886f;
+    *ph = (atan2f(d.y, d.x) + 3.14159265f) * 0.159154943f;
+}
+
+// The 64 network inputs of one point, rounded to bf16, as 32 packed pairs:
+// the hash grid at p, the one-blob of the direction with angles (th, ph).
+RTG_D void encode_packed(const GuideDev& G, const __nv_bfloat162* __restrict__ table, float3 p, float th, float ph,
                          uint32_t (&out)[32]) {
     float pn[3];
     normalise_pos(G, p.x, p.y, p.z, pn);
@@ -114,8 +124,6 @@ RTG_D void encode_packed(const GuideDev& G, const __nv_bfloat162* __restrict__ t
         }
         out[l] = pack_bf2(a0, a1);
     }
-    float th = acosf(fminf(fmaxf(n.z, -1.0f), 1.0f)) * 0.318309886f;
-    float ph = (atan2f(n.y, n.x) + 3.14159265f) * 0.159154943f;
 #pragma unroll
     for (int k = 0; k < NBLOB; k += 2) {
         float d0 = __fsub_rn(__fmul_rn(16.0f, th), (float)k + 0.5f);
@@ -128,10 +136,10 @@ RTG_D void encode_packed(const GuideDev& G, const __nv_bfloat162* __restrict__ t
 }
 
 // The same inputs into a row of bf16 (shared or global memory, 4-byte aligned).
-RTG_D void encode_row(const GuideDev& G, const __nv_bfloat162* __restrict__ table, float3 p, float3 n,
+RTG_D void encode_row(const GuideDev& G, const __nv_bfloat162* __restrict__ table, float3 p, float th, float ph,
                       __nv_bfloat16* row) {
     uint32_t v[32];
-    encode_packed(G, table, p, n, v);
+    encode_packed(G, table, p, th, ph, v);
 #pragma unroll
     for (int k = 0; k < 32; k++) reinterpret_cast<uint32_t*>(row)[k] = v[k];
 }

@@ -2715,7 +2715,7 @@ int guide_api(RtScene* s, const float* q, const float* dirs, const float* u, int
     Tmp tq, td, tu, tr, to;
     const void *dq = nullptr, *dd = nullptr, *du = nullptr;
     void *dr = nullptr, *dout = nullptr;
-    if ((rc = stage_in(s, q, (size_t)n * 24, mem, tq, &dq))) return rc;
+    if ((rc = stage_in(s, q, (size_t)n * 36, mem, tq, &dq))) return rc;
     if (dirs && (rc = stage_in(s, dirs, (size_t)n * 12, mem, td, &dd))) return rc;
     if (u && (rc = stage_in(s, u, (size_t)n * 16, mem, tu, &du))) return rc;
     if (raw && (rc = stage_out(s, raw, (size_t)n * rtg::NOUT * 4, mem, tr, &dr))) return rc;
@@ -2730,14 +2730,17 @@ int guide_api(RtScene* s, const float* q, const float* dirs, const float* u, int
     CK(cudaStreamSynchronize(s->stream));
     return check_err(s);
 }
-// host samples (n × 10) → device training samples (3 float4 each)
+// host samples (n × 13: position, normal, ω_o, ω_i, weight) → device training
+// samples (3 float4 each: (p, w), (n, θ_o/π), (ω_i, φ_o/2π))
 int stage_samples(RtScene* s, const float* smp, int64_t n, Tmp& t, const float4** d) {
     std::vector<float4> h((size_t)n * 3);
     for (int64_t i = 0; i < n; i++) {
-        const float* r = smp + i * 10;
-        h[i * 3] = make_float4(r[0], r[1], r[2], r[9]);
-        h[i * 3 + 1] = make_float4(r[3], r[4], r[5], 0.f);
-        h[i * 3 + 2] = make_float4(r[6], r[7], r[8], 0.f);
+        const float* r = smp + i * 13;
+        float th = std::acos(std::fmin(std::fmax(r[8], -1.0f), 1.0f)) * 0.318309886f;
+        float ph = (std::atan2(r[7], r[6]) + 3.14159265f) * 0.159154943f;
+        h[i * 3] = make_float4(r[0], r[1], r[2], r[12]);
+        h[i * 3 + 1] = make_float4(r[3], r[4], r[5], th);
+        h[i * 3 + 2] = make_float4(r[9], r[10], r[11], ph);
     }
     if (cudaMalloc(&t.p, h.size() * sizeof(float4)) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc samples");
     CK(cudaMemcpy(t.p, h.data(), h.size() * sizeof(float4), cudaMemcpyHostToDevice));

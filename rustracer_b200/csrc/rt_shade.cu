@@ -1048,6 +1048,9 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState 
                                     R.guide.rec_a[r] = make_float4(p.x, p.y, p.z, ts);
                                     R.guide.rec_b[r] = make_float4(wn.x, wn.y, wn.z, -1.0f);
                                     R.guide.rec_c[r] = make_float4(iu.x, iu.y, iu.z, __uint_as_float(head));
+                                    float th_o, ph_o;
+                                    rtg::blob_angles(unit3(mk(-d.x, -d.y, -d.z)), &th_o, &ph_o);
+                                    R.guide.rec_o[r] = make_float2(th_o, ph_o);
                                     R.guide.rec_w[r] = 0.0f;
                                     head = r;
                                     flags |= PF_REC_OPEN;
@@ -1155,8 +1158,8 @@ __global__ void k_accumulate(const float* __restrict__ scratch, uint32_t nsamp, 
 // ── guide inference: the mixture of every diffuse-class path of the bounce ──
 // Two kernels.  k_guide_encode, one thread per queue entry and no shared
 // memory (so the hash-table gathers run at full occupancy), recomputes the hit
-// as the shading kernel does (position, face-forward normal) and writes the 64
-// bf16 inputs in queue order.  k_guide_infer runs the network on those rows,
+// as the shading kernel does and writes the 64 bf16 inputs (hash grid at the
+// hit, one-blob of the outgoing direction) in queue order.  k_guide_infer runs the network on those rows,
 // 32 per warp as two 16-row tensor-core tiles fed straight from global memory,
 // and lanes 0..15 write the mixtures of the tile's paths.
 #define GUIDE_WARPS 8
@@ -1172,7 +1175,9 @@ __global__ void __launch_bounds__(256) k_guide_encode(DevScene S, PathState A, R
         float4 hv = A.hit[pid], ro = A.ray_o[pid], rdv = A.ray_d[pid];
         Surf sf = surface(S, hv, mk(ro.x, ro.y, ro.z), mk(rdv.x, rdv.y, rdv.z));
         uint32_t v[32];
-        rtg::encode_packed(R.guide, R.guide.tbf, sf.p, sf.nrm, v);
+        float th, ph;
+        rtg::blob_angles(unit3(mk(-rdv.x, -rdv.y, -rdv.z)), &th, &ph);      // ω_o
+        rtg::encode_packed(R.guide, R.guide.tbf, sf.p, th, ph, v);
         uint4* dst = R.guide.enc + (size_t)qi * 8;
 #pragma unroll
         for (int k = 0; k < 8; k++) dst[k] = make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);

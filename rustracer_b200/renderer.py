@@ -462,14 +462,15 @@ class GpuScene:
         self._check(lib().rt_guide_params(self.h, C.c_void_p(params.ctypes.data), 1))
 
     def guide_eval(self, q):
-        q = np.ascontiguousarray(np.asarray(q, np.float32).reshape(-1, 6))
+        """Network outputs (n × 41) at q (n × 9: position, unit normal, unit ω_o)."""
+        q = np.ascontiguousarray(np.asarray(q, np.float32).reshape(-1, 9))
         out = np.zeros((len(q), 41), np.float32)
         self._check(lib().rt_guide_eval(self.h, C.c_void_p(q.ctypes.data), len(q), C.c_void_p(out.ctypes.data),
                                         abi.RT_MEM_HOST))
         return out
 
     def guide_pdf(self, q, dirs):
-        q = np.ascontiguousarray(np.asarray(q, np.float32).reshape(-1, 6))
+        q = np.ascontiguousarray(np.asarray(q, np.float32).reshape(-1, 9))
         d = np.ascontiguousarray(np.asarray(dirs, np.float32).reshape(-1, 3))
         out = np.zeros(len(q), np.float32)
         self._check(lib().rt_guide_pdf(self.h, C.c_void_p(q.ctypes.data), C.c_void_p(d.ctypes.data), len(q),
@@ -477,7 +478,7 @@ class GpuScene:
         return out
 
     def guide_sample(self, q, u):
-        q = np.ascontiguousarray(np.asarray(q, np.float32).reshape(-1, 6))
+        q = np.ascontiguousarray(np.asarray(q, np.float32).reshape(-1, 9))
         u = np.ascontiguousarray(np.asarray(u, np.float32).reshape(-1, 4))
         out = np.zeros((len(q), 4), np.float32)
         self._check(lib().rt_guide_sample(self.h, C.c_void_p(q.ctypes.data), C.c_void_p(u.ctypes.data), len(q),
@@ -485,8 +486,8 @@ class GpuScene:
         return out
 
     def guide_loss_grad(self, samples):
-        """(loss, gradient) of samples n × 10 (position, normal, direction, weight)."""
-        s = np.ascontiguousarray(np.asarray(samples, np.float32).reshape(-1, 10))
+        """(loss, gradient) of samples n × 13 (position, normal, ω_o, direction, weight)."""
+        s = np.ascontiguousarray(np.asarray(samples, np.float32).reshape(-1, 13))
         g = np.zeros(abi.RT_GUIDE_PARAMS, np.float32)
         loss = C.c_float()
         self._check(lib().rt_guide_loss_grad(self.h, C.c_void_p(s.ctypes.data), len(s), C.byref(loss),
@@ -494,7 +495,7 @@ class GpuScene:
         return loss.value, g
 
     def guide_train(self, samples, steps=1):
-        s = np.ascontiguousarray(np.asarray(samples, np.float32).reshape(-1, 10))
+        s = np.ascontiguousarray(np.asarray(samples, np.float32).reshape(-1, 13))
         loss = C.c_float()
         self._check(lib().rt_guide_train(self.h, C.c_void_p(s.ctypes.data), len(s), int(steps), C.byref(loss)))
         return loss.value

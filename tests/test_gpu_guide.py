@@ -34,11 +34,15 @@ def _params(seed=11):
 
 
 def _queries(n, seed=2):
+    """Positions (a few outside the box: clamped), unit normals and unit
+    outgoing directions ω_o (the one-blob input)."""
     rng = np.random.default_rng(seed)
-    P = rng.uniform(-0.05, 1.05, (n, 3)).astype(np.float32)       # a few outside the box: clamped
+    P = rng.uniform(-0.05, 1.05, (n, 3)).astype(np.float32)
     N = rng.normal(size=(n, 3))
     N /= np.linalg.norm(N, axis=1, keepdims=True)
-    return P, N.astype(np.float32)
+    WO = rng.normal(size=(n, 3))
+    WO /= np.linalg.norm(WO, axis=1, keepdims=True)
+    return P, N.astype(np.float32), WO.astype(np.float32)
 
 
 def test_guide_network_outputs_match_oracle():
@@ -46,9 +50,9 @@ def test_guide_network_outputs_match_oracle():
     p = _params()
     gs.guide_set_params(p)
     assert np.array_equal(gs.guide_get_params(), p)
-    P, N = _queries(4096)
-    gpu = gs.guide_eval(np.concatenate([P, N], 1))
-    X = OG.encode(p, RES, LO, INV, P, N)
+    P, N, WO = _queries(4096)
+    gpu = gs.guide_eval(np.concatenate([P, N, WO], 1))
+    X = OG.encode(p, RES, LO, INV, P, WO)
     cpu, _ = OG.forward(p, X)
     cpu = cpu[:, :41]
     scale = cpu.std()
@@ -62,8 +66,8 @@ def test_guide_density_and_draws():
     gs = _scene()
     gs.guide_set_params(_params(21))
     n = 1 << 18
-    P, N = _queries(n, 4)
-    q = np.concatenate([P, N], 1)
+    P, N, WO = _queries(n, 4)
+    q = np.concatenate([P, N, WO], 1)
     raw = gs.guide_eval(q)
     rng = np.random.default_rng(9)
     D = rng.normal(size=(n, 3))
@@ -84,13 +88,13 @@ def test_guide_density_and_draws():
 
 def _samples(n, seed=6):
     rng = np.random.default_rng(seed)
-    P, N = _queries(n, seed)
+    P, N, WO = _queries(n, seed)
     D = rng.normal(size=(n, 3))
     D /= np.linalg.norm(D, axis=1, keepdims=True)
     D = np.where(((D * N).sum(1) < 0)[:, None] & (rng.random((n, 1)) < 0.8), -D, D)
     w = rng.exponential(1.0, n)
     w[rng.random(n) < 0.1] = 0.0
-    return np.concatenate([P, N, D, w[:, None]], 1).astype(np.float32)
+    return np.concatenate([P, N, WO, D, w[:, None]], 1).astype(np.float32)
 
 
 def _rel(a, b):
@@ -153,8 +157,9 @@ def test_guide_training_learns_a_known_distribution():
     for mu, pt in zip(mus, pts):
         P = np.tile(pt, (n, 1))
         N = np.tile([0.0, 0.0, 1.0], (n, 1))
-        rows.append(np.concatenate([P, N, _vmf_draw(mu, 40.0, n, rng), np.ones((n, 1))], 1))
-        q.append(np.concatenate([P[:2048], N[:2048]], 1))
+        WO = np.tile([0.0, 0.6, 0.8], (n, 1))
+        rows.append(np.concatenate([P, N, WO, _vmf_draw(mu, 40.0, n, rng), np.ones((n, 1))], 1))
+        q.append(np.concatenate([P[:2048], N[:2048], WO[:2048]], 1))
         fresh.append(_vmf_draw(mu, 40.0, 2048, rng))
     s = np.concatenate(rows).astype(np.float32)
     before = [np.log(gs.guide_pdf(q[i], fresh[i])).mean() for i in range(2)]
@@ -252,8 +257,8 @@ def test_guide_entry_points_take_device_buffers():
     from rustracer_b200.renderer import lib
     gs = _scene()
     gs.guide_set_params(_params(51))
-    P, N = _queries(3000, 12)
-    q = np.concatenate([P, N], 1).astype(np.float32)
+    P, N, WO = _queries(3000, 12)
+    q = np.concatenate([P, N, WO], 1).astype(np.float32)
     rng = np.random.default_rng(3)
     D = rng.normal(size=(3000, 3)).astype(np.float32)
     D /= np.linalg.norm(D, axis=1, keepdims=True)
