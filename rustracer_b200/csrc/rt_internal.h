@@ -100,22 +100,38 @@ struct PendTargets {
 
 namespace rtph { struct Map; }
 
-// Device photon map: Morton-ordered photons, box heap, and an emission-order
-// copy.  Its arrays and the build's work buffers grow on demand and are kept
-// across builds, so a rebuild of a map no larger than before allocates and
-// frees nothing (release() only drops the map).
+// Uniform cell grid over the photons' box: cubic cells of at least twice the
+// gather radius (so a gather ball meets at most 2 cells per axis), at most
+// 1024 per axis and RT_PH_GRID_MAX_CELLS in all.
+#define RT_PH_GRID_MAX_CELLS (1u << 22)
+struct PhotonGrid {
+    float lo[3];
+    float inv;           // 1 / cell size
+    int n[3];            // cells per axis (1 × 1 × 1 when the map has no grid)
+    float r2;            // the squared radius the grid serves (< 0: none)
+};
+
+// Device photon map: photons sorted by (grid cell, Morton code) — every cell a
+// contiguous run — with the [start, end) table of the cells, a box heap over
+// 32-photon leaves of the same order, and an emission-order copy.  Its arrays
+// and the build's work buffers grow on demand and are kept across builds, so a
+// rebuild of a map no larger than before allocates and frees nothing
+// (release() only drops the map).
 struct PhotonMapDev {
     float4 *pos = nullptr, *pow = nullptr, *nor = nullptr, *blo = nullptr, *bhi = nullptr;
     float4 *exp_pos = nullptr, *exp_pow = nullptr, *exp_nor = nullptr;
     uint32_t n = 0, nleaf_pow2 = 1, knn_k = 0;
     float r2 = 0.0f;
     bool present = false;
-    // capacities (elements) of the map arrays, the heap and the build's work buffers
-    size_t cap_map = 0, cap_heap = 0, cap_work = 0, cap_tmp = 0;
+    PhotonGrid grid{{0.f, 0.f, 0.f}, 0.f, {1, 1, 1}, -1.f};
+    uint2* cells = nullptr;                                   // [start, end) per grid cell
+    // capacities (elements) of the map arrays, the heap, the cell table and the build's work buffers
+    size_t cap_map = 0, cap_heap = 0, cap_cells = 0, cap_work = 0, cap_tmp = 0;
     uint8_t* flags = nullptr;                                 // stored flag per traced photon
     float4 *st_pos = nullptr, *st_pow = nullptr, *st_nor = nullptr;   // stored record per traced photon
     uint32_t *fl32 = nullptr, *scan = nullptr;                // compaction
-    uint32_t *key = nullptr, *val = nullptr, *key2 = nullptr, *val2 = nullptr;   // Morton sort
+    uint64_t *key = nullptr, *key2 = nullptr;                 // sort keys: cell code << 30 | Morton code
+    uint32_t *val = nullptr, *val2 = nullptr;
     float* bounds = nullptr;
     void* tmp = nullptr;                                      // CUB temporary storage
     ~PhotonMapDev();

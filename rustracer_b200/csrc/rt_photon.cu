@@ -6,10 +6,15 @@
 //             continues specular photons and stores the first diffuse hit after a
 //             specular bounce (trace_photon, photon.rs:232-277) into its emission slot
 //   compact   stored photons in emission order (exclusive scan of the flags)
-//   sort      30-bit Morton codes of the positions, stable radix sort
+//   sort      key = grid cell (Morton code of its 10-bit coordinates) above the
+//             30-bit Morton code of the position; stable radix sort
+//   grid      [start, end) of every cell of a uniform grid (cells ≥ 2 × radius)
 //   tree      implicit complete binary tree of boxes over 32-photon leaves of the
-//             Morton order (node i has children 2i+1, 2i+2)
-// Gather (warp per query; lane j of the warp tests photon j of a leaf):
+//             same order (node i has children 2i+1, 2i+2)
+// Gather: the photons of the ≤ 2 × 2 × 2 cells that a ball of the map's radius
+// meets (the box heap for a larger radius, or when those cells hold very many):
+//   sparse    one lane per query while fewer photons than k (or 64) are in range
+//   dense     one warp per query; lane j tests photon j of a 32-photon chunk
 //   radius    Σ power·(1 − d²/r²) over d² < r², n_p·n > 0, × 2/(π²r²) (photon.rs:195-228)
 //   k-NN      the k-th smallest d² among those photons within the maximum radius:
 //             one traversal collects them into shared memory, a radix select
@@ -385,16 +390,45 @@ RT_D uint32_t expand10(uint32_t v) {
     v = (v | (v << 2)) & 0x09249249u;
     return v;
 }
-__global__ void k_morton(const float4* p, uint32_t n, const float* lo, const float* hi, uint32_t* key, uint32_t* val) {
+// One cubic cell size for all three axes: caustic photons often lie on one
+// plane, and stretching that plane's near-zero extent to 1024 cells would put
+// rounding noise into every third bit of the code (leaves of 32 photons
+// scattered across the whole map).
+// Cell of coordinate x along one axis: the same float arithmetic for photons
+// and for query bounds, clamped into the grid — monotone in x, so a photon
+// between two bounds lies in a cell between theirs.
+RT_D int grid_cell(float x, float lo, float inv, int n) {
+    float f = floorf((x - lo) * inv);
+    return (int)fminf(fmaxf(f, 0.0f), (float)(n - 1));
+}
+RT_D uint32_t cell_linear(const PhotonGrid& G, float4 q) {
+    uint32_t x = grid_cell(q.x, G.lo[0], G.inv, G.n[0]), y = grid_cell(q.y, G.lo[1], G.inv, G.n[1]);
+    uint32_t z = grid_cell(q.z, G.lo[2], G.inv, G.n[2]);
+    return x + (uint32_t)G.n[0] * (y + (uint32_t)G.n[1] * z);
+}
+__global__ void k_morton(const float4* p, uint32_t n, const float* lo, const float* hi, PhotonGrid G, uint64_t* key,
+                         uint32_t* val) {
     float3 l = mk(lo[0], lo[1], lo[2]);
-    float3 e = mk(fmaxf(hi[0] - lo[0], 1e-30f), fmaxf(hi[1] - lo[1], 1e-30f), fmaxf(hi[2] - lo[2], 1e-30f));
+    float ext = fmaxf(fmaxf(fmaxf(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]), 1e-30f);
+    float3 e = mk(ext, ext, ext);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 q = p[i];
         uint32_t x = (uint32_t)fminf(fmaxf((q.x - l.x) / e.x * 1024.0f, 0.0f), 1023.0f);
         uint32_t y = (uint32_t)fminf(fmaxf((q.y - l.y) / e.y * 1024.0f, 0.0f), 1023.0f);
         uint32_t z = (uint32_t)fminf(fmaxf((q.z - l.z) / e.z * 1024.0f, 0.0f), 1023.0f);
-        key[i] = (expand10(x) << 2) | (expand10(y) << 1) | expand10(z);
+        uint32_t cx = grid_cell(q.x, G.lo[0], G.inv, G.n[0]), cy = grid_cell(q.y, G.lo[1], G.inv, G.n[1]);
+        uint32_t cz = grid_cell(q.z, G.lo[2], G.inv, G.n[2]);
+        uint64_t cell = (expand10(cx) << 2) | (expand10(cy) << 1) | expand10(cz);
+        key[i] = cell << 30 | ((expand10(x) << 2) | (expand10(y) << 1) | expand10(z));
         val[i] = i;
+    }
+}
+// [start, end) of every non-empty cell (the table is zeroed first: empty = [0, 0))
+__global__ void k_cell_ranges(const float4* p, uint32_t n, PhotonGrid G, uint2* cells) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t c = cell_linear(G, p[i]);
+        if (i == 0 || cell_linear(G, p[i - 1]) != c) cells[c].x = i;
+        if (i + 1 == n || cell_linear(G, p[i + 1]) != c) cells[c].y = i + 1;
     }
 }
 __global__ void k_gather_sorted(const uint32_t* order, uint32_t n, const float4* sp, const float4* sw, const float4* sn,
@@ -433,12 +467,50 @@ __global__ void k_level_boxes(uint32_t first, uint32_t count, float4* blo, float
 namespace rtph {
 
 struct Map {
-    const float4 *pos, *pow, *nor;   // Morton order; pos.w = emission index bits
+    const float4 *pos, *pow, *nor;   // (cell, Morton) order; pos.w = emission index bits
     const float4 *blo, *bhi;         // heap of boxes
+    const uint2* cells;              // [start, end) per grid cell
+    PhotonGrid G;
     uint32_t n, nleaf_pow2;
     float r2;                        // radius (or k-NN maximum radius) squared
     uint32_t knn_k;
 };
+
+// Cells a ball of squared radius r2 around p may reach.  The bounds are
+// widened by 2^-10 of the radius plus 2^-20 of the coordinates' magnitude —
+// far more than the rounding of p ± r and of the photons' float distances —
+// so every photon with d² < r2 lies in one of the cells.
+struct CellSpan { int i0[3], i1[3]; };
+RT_D CellSpan cell_span(const Map& M, float3 p, float r2) {
+    float r = sqrtf(r2);
+    float q[3] = {p.x, p.y, p.z};
+    CellSpan s;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        float m = r * (1.0f + 0x1p-10f) + (fabsf(q[a]) + r) * 0x1p-20f;
+        s.i0[a] = grid_cell(q[a] - m, M.G.lo[a], M.G.inv, M.G.n[a]);
+        s.i1[a] = grid_cell(q[a] + m, M.G.lo[a], M.G.inv, M.G.n[a]);
+    }
+    return s;
+}
+RT_D uint2 cell_run(const Map& M, int x, int y, int z) {
+    return __ldg(M.cells + x + M.G.n[0] * (y + M.G.n[1] * z));
+}
+// photons in the cells of a span (an upper bound of the work of enumerating them)
+RT_D uint32_t span_photons(const Map& M, const CellSpan& s) {
+    uint32_t t = 0;
+    for (int z = s.i0[2]; z <= s.i1[2]; z++)
+        for (int y = s.i0[1]; y <= s.i1[1]; y++)
+            for (int x = s.i0[0]; x <= s.i1[0]; x++) {
+                uint2 r = cell_run(M, x, y, z);
+                t += r.y - r.x;
+            }
+    return t;
+}
+// the grid serves balls no larger than the map's radius, while the cells hold
+// at most this many photons (else the box heap prunes better)
+#define PH_GRID_WARP_MAX 4096u
+#define PH_GRID_LANE_MAX 1024u
 
 // Visit every leaf whose box is within r2 of p; for each, lane j gets photon j
 // of the leaf (or nothing).  `f(lane_photon_index_or_-1)` is called warp-wide.
@@ -464,6 +536,30 @@ RT_D void for_leaves(const Map& M, float3 p, float r2, F f) {
         if (sp == 0) break;
         node = stack[--sp];
     }
+}
+
+// Every photon within r2 of p (and others), each once, warp-wide: from the grid
+// cells the ball meets when the grid serves r2 and they hold at most
+// PH_GRID_WARP_MAX photons, else from the heap's leaves.
+template <class F>
+RT_D void for_near(const Map& M, float3 p, float r2, F f) {
+    if (r2 <= M.G.r2) {
+        CellSpan s = cell_span(M, p, r2);
+        if (span_photons(M, s) <= PH_GRID_WARP_MAX) {
+            uint32_t lane = threadIdx.x & 31u;
+            for (int z = s.i0[2]; z <= s.i1[2]; z++)
+                for (int y = s.i0[1]; y <= s.i1[1]; y++)
+                    for (int x = s.i0[0]; x <= s.i1[0]; x++) {
+                        uint2 r = cell_run(M, x, y, z);
+                        for (uint32_t b = r.x; b < r.y; b += 32) {
+                            uint32_t k = b + lane;
+                            f(k < r.y ? (int)k : -1);
+                        }
+                    }
+            return;
+        }
+    }
+    for_leaves(M, p, r2, f);
 }
 
 RT_D float warp_sum(float v) {
@@ -517,7 +613,7 @@ RT_D float warp_kth_d2(const Map& M, float3 p, const float3* nrm, float r2max, u
         // edge j = lo + w·j for j < 32, edge 32 = hi; bin = last edge ≤ d2
         float my_edge = R.lo + w * (float)lane;
         uint32_t total = 0;
-        for_leaves(M, p, R.hi, [&](int i) {
+        for_near(M, p, R.hi, [&](int i) {
             float d2 = 0.0f;
             bool c = kth_candidate(M, i, p, nrm, R, d2);
             if (c) {
@@ -533,7 +629,7 @@ RT_D float warp_kth_d2(const Map& M, float3 p, const float3* nrm, float r2max, u
         if (total <= PH_SEL_CAP) {
             // exact select: collect the candidates of the range and rank them
             uint32_t cnt = 0;
-            for_leaves(M, p, R.hi, [&](int i) {
+            for_near(M, p, R.hi, [&](int i) {
                 float d2 = 0.0f;
                 bool c = kth_candidate(M, i, p, nrm, R, d2);
                 uint32_t m = __ballot_sync(0xFFFFFFFFu, c);
@@ -577,14 +673,14 @@ RT_D float warp_kth_d2(const Map& M, float3 p, const float3* nrm, float r2max, u
     // peel distinct values, smallest first (bounded)
     for (int it = 0; it < 64; it++) {
         float mn = INFINITY;
-        for_leaves(M, p, R.hi, [&](int i) {
+        for_near(M, p, R.hi, [&](int i) {
             float d2 = 0.0f;
             if (kth_candidate(M, i, p, nrm, R, d2)) mn = fminf(mn, d2);
         });
         for (int o = 16; o > 0; o >>= 1) mn = fminf(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
         if (!(mn < INFINITY)) return R.hi;
         uint32_t eq = 0;
-        for_leaves(M, p, R.hi, [&](int i) {
+        for_near(M, p, R.hi, [&](int i) {
             float d2 = 0.0f;
             bool c = kth_candidate(M, i, p, nrm, R, d2) && d2 == mn;
             eq += __popc(__ballot_sync(0xFFFFFFFFu, c));
@@ -603,24 +699,43 @@ RT_D float warp_kth_d2(const Map& M, float3 p, const float3* nrm, float r2max, u
 // warp-cooperative gather is needed.  With fewer than k photons in range the
 // k-NN estimate is exactly this radius-r2 estimate.
 RT_D bool lane_gather(const Map& M, float3 p, float3 n, float r2, uint32_t limit, float3* out) {
+    uint32_t count = 0;
+    float3 acc = mk(0.f, 0.f, 0.f);
+    auto take = [&](uint32_t k) {
+        float d2 = pdist2(__ldg(M.pos + k), p);
+        if (d2 < r2 && pdot(__ldg(M.nor + k), n) > 0.0f) {
+            if (++count >= limit) return false;
+            float4 pw = __ldg(M.pow + k);
+            acc = acc + mk(pw.x, pw.y, pw.z) * (1.0f - d2 / r2);
+        }
+        return true;
+    };
+    if (r2 <= M.G.r2) {
+        // the grid's cells: a lane gives the query up when they hold too many
+        CellSpan s = cell_span(M, p, r2);
+        if (span_photons(M, s) > PH_GRID_LANE_MAX) return false;
+        for (int z = s.i0[2]; z <= s.i1[2]; z++)
+            for (int y = s.i0[1]; y <= s.i1[1]; y++)
+                for (int x = s.i0[0]; x <= s.i1[0]; x++) {
+                    uint2 r = cell_run(M, x, y, z);
+                    for (uint32_t k = r.x; k < r.y; k++)
+                        if (!take(k)) return false;
+                }
+        float s2 = 2.0f / (PI_F * PI_F * r2);
+        *out = count ? acc * s2 : mk(0.f, 0.f, 0.f);
+        return true;
+    }
     uint32_t stack[PH_STACK];
     int sp = 0;
-    uint32_t node = 0, count = 0;
+    uint32_t node = 0;
     uint32_t first_leaf = M.nleaf_pow2 - 1;
-    float3 acc = mk(0.f, 0.f, 0.f);
     while (true) {
         float4 lo = __ldg(M.blo + node), hi = __ldg(M.bhi + node);
         if (lo.x <= hi.x && box_d2(lo, hi, p) <= r2) {
             if (node >= first_leaf) {
                 uint32_t k0 = (node - first_leaf) * PH_LEAF, k1 = min(k0 + PH_LEAF, M.n);
-                for (uint32_t k = k0; k < k1; k++) {
-                    float d2 = pdist2(__ldg(M.pos + k), p);
-                    if (d2 < r2 && pdot(__ldg(M.nor + k), n) > 0.0f) {
-                        if (++count >= limit) return false;
-                        float4 pw = __ldg(M.pow + k);
-                        acc = acc + mk(pw.x, pw.y, pw.z) * (1.0f - d2 / r2);
-                    }
-                }
+                for (uint32_t k = k0; k < k1; k++)
+                    if (!take(k)) return false;
             } else if (sp + 2 <= PH_STACK) {
                 stack[sp++] = 2 * node + 2;
                 stack[sp++] = 2 * node + 1;
@@ -641,7 +756,7 @@ RT_D float3 warp_irradiance(const Map& M, float3 p, float3 n, uint32_t* hist, fl
         if (!(r2 > 0.0f)) return mk(0.f, 0.f, 0.f);
     }
     float3 acc = mk(0.f, 0.f, 0.f);
-    for_leaves(M, p, r2, [&](int i) {
+    for_near(M, p, r2, [&](int i) {
         if (i < 0) return;
         float d2 = pdist2(__ldg(M.pos + i), p);
         if (d2 < r2) {
@@ -720,9 +835,9 @@ RT_D float warp_radix_select(const float* v, uint32_t cnt, uint32_t k, uint32_t*
 // warp_irradiance; the terms are summed in another order.
 // An upper bound of the k-NN search's k-th distance: descend the box heap
 // toward p (the nearer child at every level) to a subtree of PH_SEED_LEAVES
-// leaves, and take the k-th smallest d² of its facing photons within the
-// maximum radius (r2max when it holds fewer than k).  The true k nearest are
-// at least as near, so every one of them lies within the bound.
+// leaves, and take the k-th smallest d² of its facing photons (the maximum
+// radius's r2 when it holds fewer than k or that is nearer).  The true k
+// nearest are at least as near, so every one of them lies within the bound.
 #define PH_SEED_LEAVES 4
 RT_D float seed_bound(const Map& M, float3 p, float3 n, WarpScratch& W) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -741,7 +856,7 @@ RT_D float seed_bound(const Map& M, float3 p, float3 n, WarpScratch& W) {
         float d2 = INFINITY;
         if (i < last) {
             float v = pdist2(__ldg(M.pos + i), p);
-            if (v < M.r2 && pdot(__ldg(M.nor + i), n) > 0.0f) d2 = v;
+            if (pdot(__ldg(M.nor + i), n) > 0.0f) d2 = v;
         }
         W.d2[i - first] = d2;
         c += d2 < INFINITY;
@@ -749,16 +864,18 @@ RT_D float seed_bound(const Map& M, float3 p, float3 n, WarpScratch& W) {
     for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
     __syncwarp();
     if (c < M.knn_k) return M.r2;
-    return warp_radix_select(W.d2, span * PH_LEAF, M.knn_k, W.hist);
+    return fminf(warp_radix_select(W.d2, span * PH_LEAF, M.knn_k, W.hist), M.r2);
 }
 
 RT_D float3 warp_irradiance_1pass(const Map& M, float3 p, float3 n, WarpScratch& W, uint32_t* hist, float* sel) {
     const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
     // the ball to collect: within the maximum radius and, in k-NN mode, within
     // the seed subtree's k-th distance (inclusive, so ties at it are kept)
-    float bound = M.knn_k > 0 && M.knn_k <= PH_SEED_LEAVES * PH_LEAF ? seed_bound(M, p, n, W) : M.r2;
+    // (the grid's cells hold a few times the photons in range: no seed there)
+    bool grid = M.r2 <= M.G.r2 && span_photons(M, cell_span(M, p, M.r2)) <= PH_GRID_WARP_MAX;
+    float bound = !grid && M.knn_k > 0 && M.knn_k <= PH_SEED_LEAVES * PH_LEAF ? seed_bound(M, p, n, W) : M.r2;
     uint32_t cnt = 0;
-    for_leaves(M, p, bound, [&](int i) {
+    for_near(M, p, bound, [&](int i) {
         bool c = false;
         float d2 = 0.0f;
         if (i >= 0) {
@@ -820,7 +937,7 @@ __global__ void k_knn_api(rtph::Map M, const float* q, uint32_t n, int k, float 
         float rk = rtph::warp_kth_d2(M, p, nullptr, rmax2, (uint32_t)k, false, hist[w], sel[w]);
         // every photon with d² ≤ r_k² (k plus ties at r_k)
         uint32_t cnt = 0;
-        rtph::for_leaves(M, p, rk, [&](int j) {
+        rtph::for_near(M, p, rk, [&](int j) {
             bool c = false;
             float d2 = 0.0f;
             uint32_t id = 0;
@@ -915,23 +1032,27 @@ PhotonMapDev::~PhotonMapDev() { free_all(); }
 void PhotonMapDev::release() {
     n = 0;
     present = false;
+    grid = PhotonGrid{{0.f, 0.f, 0.f}, 0.f, {1, 1, 1}, -1.f};
 }
 void PhotonMapDev::free_all() {
     void* ps[] = {pos, pow, nor, blo, bhi, exp_pos, exp_pow, exp_nor, flags, st_pos, st_pow, st_nor,
-                  fl32, scan, key, val, key2, val2, bounds, tmp};
+                  fl32, scan, key, val, key2, val2, bounds, tmp, cells};
     for (void* p : ps) if (p) cudaFree(p);
     pos = pow = nor = blo = bhi = exp_pos = exp_pow = exp_nor = st_pos = st_pow = st_nor = nullptr;
     flags = nullptr;
-    fl32 = scan = key = val = key2 = val2 = nullptr;
+    fl32 = scan = val = val2 = nullptr;
+    key = key2 = nullptr;
     bounds = nullptr;
     tmp = nullptr;
-    cap_map = cap_heap = cap_work = cap_tmp = 0;
+    cells = nullptr;
+    cap_map = cap_heap = cap_cells = cap_work = cap_tmp = 0;
     release();
 }
 
 rtph::Map PhotonMapDev::view() const {
     rtph::Map M;
     M.pos = pos; M.pow = pow; M.nor = nor; M.blo = blo; M.bhi = bhi;
+    M.cells = cells; M.G = grid;
     M.n = n; M.nleaf_pow2 = nleaf_pow2; M.r2 = r2; M.knn_k = knn_k;
     return M;
 }
@@ -954,8 +1075,9 @@ static cudaError_t ensure_map(PhotonMapDev& map, size_t n) {
     cudaError_t e;
     float4** f4[] = {&map.pos, &map.pow, &map.nor, &map.exp_pos, &map.exp_pow, &map.exp_nor};
     for (float4** q : f4) if ((e = grow(*q, c, sizeof(float4)))) return e;
-    uint32_t** u4[] = {&map.key, &map.val, &map.key2, &map.val2};
+    uint32_t** u4[] = {&map.val, &map.val2};
     for (uint32_t** q : u4) if ((e = grow(*q, c, sizeof(uint32_t)))) return e;
+    if ((e = grow(map.key, c, sizeof(uint64_t))) || (e = grow(map.key2, c, sizeof(uint64_t)))) return e;
     if (!map.bounds && (e = grow(map.bounds, 6, sizeof(float)))) return e;
     map.cap_map = c;
     return cudaSuccess;
@@ -969,20 +1091,58 @@ static cudaError_t ensure_tmp(PhotonMapDev& map, size_t bytes) {
     return e;
 }
 
-// Morton sort of the emission-order photons (exp_*, n of them) into pos/pow/nor,
-// then the box heap over PH_LEAF-photon leaves
+// The cell grid for photons in the box [lo, hi] and gather radius² r2: cubic
+// cells of 2r·(1 + 2^-9) — a ball of radius r (widened as cell_span widens it)
+// meets at most 2 cells per axis — or larger, to keep ≤ 1000 cells per axis
+// and ≤ RT_PH_GRID_MAX_CELLS cells in all.  No grid (one cell, r2 < 0) for a
+// zero radius.
+static PhotonGrid make_grid(const float lo[3], const float hi[3], float r2) {
+    PhotonGrid G{{lo[0], lo[1], lo[2]}, 0.0f, {1, 1, 1}, -1.0f};
+    if (!(r2 > 0.0f) || !std::isfinite(r2)) return G;
+    double ext = 0.0;
+    for (int a = 0; a < 3; a++) ext = std::max(ext, (double)hi[a] - (double)lo[a]);
+    double c = std::max(2.0 * std::sqrt((double)r2) * (1.0 + 1.0 / 512.0), ext / 1000.0);
+    if (!(c > 0.0)) return G;
+    for (;;) {
+        double cells = 1.0;
+        for (int a = 0; a < 3; a++) {
+            double na = std::floor(((double)hi[a] - (double)lo[a]) / c) + 1.0;
+            G.n[a] = (int)std::min(na, 1024.0);
+            cells *= G.n[a];
+        }
+        if (cells <= RT_PH_GRID_MAX_CELLS) break;
+        c *= 1.25;
+    }
+    G.inv = (float)(1.0 / c);
+    G.r2 = r2;
+    return G;
+}
+
+// Sort the emission-order photons (exp_*, n of them) by (grid cell, Morton
+// code) into pos/pow/nor, then the cell table and the box heap over
+// PH_LEAF-photon leaves
 static cudaError_t build_tree(PhotonMapDev& map, uint32_t n, cudaStream_t st) {
-    // Morton sort (stable radix sort keeps emission order among equal codes)
     cudaError_t e;
     float init[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
     if ((e = cudaMemcpyAsync(map.bounds, init, sizeof(init), cudaMemcpyHostToDevice, st))) return e;
     k_bounds<<<std::min<uint32_t>((n + 255) / 256, 2048), 256, 0, st>>>(map.exp_pos, n, map.bounds, map.bounds + 3);
+    float b[6];
+    if ((e = cudaMemcpyAsync(b, map.bounds, sizeof(b), cudaMemcpyDeviceToHost, st))) return e;
+    if ((e = cudaStreamSynchronize(st))) return e;
+    map.grid = make_grid(b, b + 3, map.r2);
+    size_t ncell = (size_t)map.grid.n[0] * map.grid.n[1] * map.grid.n[2];
+    if (ncell > map.cap_cells || !map.cells) {
+        if ((e = grow(map.cells, ncell, sizeof(uint2)))) return e;
+        map.cap_cells = ncell;
+    }
+    if ((e = cudaMemsetAsync(map.cells, 0, ncell * sizeof(uint2), st))) return e;
     k_morton<<<std::min<uint32_t>((n + 255) / 256, 4096), 256, 0, st>>>(map.exp_pos, n, map.bounds, map.bounds + 3,
-                                                                        map.key, map.val);
+                                                                        map.grid, map.key, map.val);
+    // stable radix sort: emission order among equal keys
     size_t tb = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb, map.key, map.key2, map.val, map.val2, (int)n, 0, 30, st);
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, map.key, map.key2, map.val, map.val2, (int)n, 0, 60, st);
     if ((e = ensure_tmp(map, tb))) return e;
-    cub::DeviceRadixSort::SortPairs(map.tmp, tb, map.key, map.key2, map.val, map.val2, (int)n, 0, 30, st);
+    cub::DeviceRadixSort::SortPairs(map.tmp, tb, map.key, map.key2, map.val, map.val2, (int)n, 0, 60, st);
     uint32_t nleaf = (n + PH_LEAF - 1) / PH_LEAF, p2 = 1;
     while (p2 < nleaf) p2 <<= 1;
     map.nleaf_pow2 = p2;
@@ -993,6 +1153,7 @@ static cudaError_t build_tree(PhotonMapDev& map, uint32_t n, cudaStream_t st) {
     }
     k_gather_sorted<<<std::min<uint32_t>((n + 255) / 256, 4096), 256, 0, st>>>(map.val2, n, map.exp_pos, map.exp_pow,
                                                                                map.exp_nor, map.pos, map.pow, map.nor);
+    k_cell_ranges<<<std::min<uint32_t>((n + 255) / 256, 4096), 256, 0, st>>>(map.pos, n, map.grid, map.cells);
     k_leaf_boxes<<<std::min<uint32_t>((p2 + 255) / 256, 4096), 256, 0, st>>>(map.pos, n, p2, map.blo, map.bhi);
     for (uint32_t cnt = p2 / 2; cnt >= 1; cnt /= 2)
         k_level_boxes<<<std::min<uint32_t>((cnt + 255) / 256, 4096), 256, 0, st>>>(cnt - 1, cnt, map.blo, map.bhi);

@@ -55,6 +55,32 @@ def test_gpu_gather_matches_oracle(knn_k):
     assert (b.sum(1) > 0).mean() > 0.9
 
 
+@pytest.mark.parametrize("knn_k", [0, 8])
+def test_gpu_gather_on_a_coarsened_grid(knn_k):
+    """Photons filling a cube with a small radius: cells of 2r would number
+    over 10^8, so the grid takes larger cells (fewer than 2^22 of them); the
+    estimates still match the oracle's, photon for photon."""
+    rng = np.random.default_rng(11)
+    n = 60000
+    pos = rng.uniform(-1, 1, size=(n, 3)).astype(np.float32)
+    power = rng.uniform(0, 1, size=(n, 3)).astype(np.float32)
+    nor = rng.normal(size=(n, 3)).astype(np.float32)
+    nor /= np.linalg.norm(nor, axis=1, keepdims=True)
+    sb = glass_over_floor()
+    g, o = GpuScene(sb), O.OracleScene(sb)
+    g.photon_set(pos, power, nor, np.arange(n), radius=0.004, knn_k=knn_k)
+    o.photon_set(pos, power, nor, np.arange(n), radius=0.004, knn_k=knn_k)
+    q = np.zeros((4000, 6), np.float32)
+    q[:, :3] = pos[:4000] + rng.uniform(-0.001, 0.001, size=(4000, 3))
+    q[:, 3:] = nor[:4000]
+    a, b = g.photon_gather(q), o.photon_gather(q)
+    np.testing.assert_allclose(a, b, rtol=2e-4, atol=1e-5)
+    assert (b.sum(1) > 0).mean() > 0.9
+    i1, d1 = g.knn(q[:, :3], 8, 0.004)
+    i2, d2 = o.knn(q[:, :3], 8, 0.004)
+    assert np.array_equal(i1, i2)
+
+
 def test_gpu_knn_sets_are_exact():
     pos, power, nor = _random_photons(40000, 7)
     pos = (np.round(pos * 64) / 64).astype(np.float32)          # exact distance ties
@@ -65,7 +91,8 @@ def test_gpu_knn_sets_are_exact():
     rng = np.random.default_rng(8)
     q = rng.uniform(-1, 1, size=(2000, 3)).astype(np.float32)
     q[:, 1] *= 0.05
-    for k, rmax in [(64, 0.01), (16, 0.05), (64, 0.05)]:
+    # radii up to the map's (0.1) use its cell grid, 0.2 the box heap
+    for k, rmax in [(64, 0.01), (16, 0.05), (64, 0.05), (64, 0.1), (16, 0.2)]:
         gi, gd = g.knn(q, k, rmax)
         oi, od = o.knn(q, k, rmax)
         assert np.array_equal(gi, oi), (k, rmax)
