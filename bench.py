@@ -67,8 +67,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--mode", choices=["bench", "pass"], default="bench",
                     help="pass: one warm-up call + one measured 16-spp call of the workload, no JSON (profiler driver)")
-    ap.add_argument("--config", choices=["icosphere", "gem", "room", "batch", "guided"], default="icosphere",
-                    help="gem: the 1280x720 gem workload with its caustic photon map; room: the reference's "
+    ap.add_argument("--config", choices=["icosphere", "gem", "box", "room", "batch", "guided"], default="icosphere",
+                    help="gem: the 1280x720 gem workload with its caustic photon map; box: the 256x256 box "
+                         "workload (the secondary line's, alone); room: the reference's "
                          "--bench room (1200x800, 128 spp); batch: 64 jobs of the box/icosphere/gem scenes on 4 "
                          "concurrent handles vs one; guided: equal-time relMSE of the learned proposal against "
                          "cosine bounces on the slit-light room (secondary lines; the headline is the icosphere "
@@ -414,7 +415,7 @@ def secondary(kind, args):
         steps, warm = args.steps, args.warmup
     else:
         sb, st = configs.gem_scene()
-        steps, warm = max(1, min(args.steps, 3)), 1
+        steps, warm = max(1, min(args.steps, 3)), args.warmup
     w, h, spp, depth, hero = st["width"], st["height"], st["spp"], st["max_depth"], st["hero"]
     strata = int(np.sqrt(np.float32(spp)))
     cam = st["camera"]
@@ -776,6 +777,23 @@ def one_pass():
     print("pass ok", scene.last_stats(), flush=True)
 
 
+def one_pass_scene(kind):
+    """Profiler driver for the box and gem workloads at their stated frames:
+    the gem builds its 2M-photon map, then one 1-spp warm-up call and one
+    measured 4-spp call (gem) or 16-spp call (box) of rt_render_accumulate."""
+    from rustracer_b200 import configs
+    from rustracer_b200.renderer import GpuScene, pass_params
+    sb, st = configs.gem_scene() if kind == "gem" else configs.box_scene()
+    w, h, depth, hero = st["width"], st["height"], st["max_depth"], st["hero"]
+    scene = GpuScene(sb, device=0)
+    if kind == "gem":
+        scene.photon_build(st["photon_params"](seed=1))
+    spp = 4 if kind == "gem" else st["spp"]
+    scene.render_accumulate(st["camera"], pass_params(w, h, 0, 1, 1, depth, hero, 1.0, 3))
+    scene.render_accumulate(st["camera"], pass_params(w, h, 1, spp, int(np.sqrt(spp)), depth, hero, 1.0, 3))
+    print("pass ok", scene.last_stats(), flush=True)
+
+
 def one_pass_guided():
     """Profiler driver for the learned proposal: the 1280×720 slit-light room,
     16 spp of training (4 render calls of 4 spp, 16 Adam steps after each),
@@ -797,12 +815,19 @@ def one_pass_guided():
 def main():
     args = parse()
     if args.mode == "pass":
-        one_pass_guided() if args.config == "guided" else one_pass()
+        if args.config == "guided":
+            one_pass_guided()
+        elif args.config in ("gem", "box"):
+            one_pass_scene(args.config)
+        else:
+            one_pass()
         return
     if args.impl == "reference":
         run_reference(args)
     elif args.config == "gem":
         run_gem(args)
+    elif args.config == "box":
+        print(json.dumps(secondary("box", args)), flush=True)
     elif args.config == "room":
         run_room(args)
     elif args.config == "batch":

@@ -11,10 +11,9 @@
 //   grid      [start, end) of every cell of a uniform grid (cells ≥ 2 × radius)
 //   tree      implicit complete binary tree of boxes over 32-photon leaves of the
 //             same order (node i has children 2i+1, 2i+2)
-// Gather: the photons of the ≤ 2 × 2 × 2 cells that a ball of the map's radius
-// meets (the box heap for a larger radius, or when those cells hold very many):
-//   sparse    one lane per query while fewer photons than k (or 64) are in range
-//   dense     one warp per query; lane j tests photon j of a 32-photon chunk
+// Gather (one warp per query): the photons of the ≤ 2 × 2 × 2 cells that a ball
+// of the map's radius meets, joined into one list that the lanes read 32 at a
+// time (the box heap for a larger radius, or when those cells hold very many):
 //   radius    Σ power·(1 − d²/r²) over d² < r², n_p·n > 0, × 2/(π²r²) (photon.rs:195-228)
 //   k-NN      the k-th smallest d² among those photons within the maximum radius:
 //             one traversal collects them into shared memory, a radix select
@@ -510,7 +509,6 @@ RT_D uint32_t span_photons(const Map& M, const CellSpan& s) {
 // the grid serves balls no larger than the map's radius, while the cells hold
 // at most this many photons (else the box heap prunes better)
 #define PH_GRID_WARP_MAX 4096u
-#define PH_GRID_LANE_MAX 1024u
 
 // Visit every leaf whose box is within r2 of p; for each, lane j gets photon j
 // of the leaf (or nothing).  `f(lane_photon_index_or_-1)` is called warp-wide.
@@ -693,62 +691,6 @@ RT_D float warp_kth_d2(const Map& M, float3 p, const float3* nrm, float r2max, u
 }
 
 // Irradiance estimate at (p, n) by one warp (all lanes call with the same query).
-// Lane-level gather for sparse neighbourhoods: the radius-r2 estimate of one
-// query by one lane, counting the photons it takes.  Gives up (returns false)
-// once `limit` photons are in range — then the k-th-distance search or the
-// warp-cooperative gather is needed.  With fewer than k photons in range the
-// k-NN estimate is exactly this radius-r2 estimate.
-RT_D bool lane_gather(const Map& M, float3 p, float3 n, float r2, uint32_t limit, float3* out) {
-    uint32_t count = 0;
-    float3 acc = mk(0.f, 0.f, 0.f);
-    auto take = [&](uint32_t k) {
-        float d2 = pdist2(__ldg(M.pos + k), p);
-        if (d2 < r2 && pdot(__ldg(M.nor + k), n) > 0.0f) {
-            if (++count >= limit) return false;
-            float4 pw = __ldg(M.pow + k);
-            acc = acc + mk(pw.x, pw.y, pw.z) * (1.0f - d2 / r2);
-        }
-        return true;
-    };
-    if (r2 <= M.G.r2) {
-        // the grid's cells: a lane gives the query up when they hold too many
-        CellSpan s = cell_span(M, p, r2);
-        if (span_photons(M, s) > PH_GRID_LANE_MAX) return false;
-        for (int z = s.i0[2]; z <= s.i1[2]; z++)
-            for (int y = s.i0[1]; y <= s.i1[1]; y++)
-                for (int x = s.i0[0]; x <= s.i1[0]; x++) {
-                    uint2 r = cell_run(M, x, y, z);
-                    for (uint32_t k = r.x; k < r.y; k++)
-                        if (!take(k)) return false;
-                }
-        float s2 = 2.0f / (PI_F * PI_F * r2);
-        *out = count ? acc * s2 : mk(0.f, 0.f, 0.f);
-        return true;
-    }
-    uint32_t stack[PH_STACK];
-    int sp = 0;
-    uint32_t node = 0;
-    uint32_t first_leaf = M.nleaf_pow2 - 1;
-    while (true) {
-        float4 lo = __ldg(M.blo + node), hi = __ldg(M.bhi + node);
-        if (lo.x <= hi.x && box_d2(lo, hi, p) <= r2) {
-            if (node >= first_leaf) {
-                uint32_t k0 = (node - first_leaf) * PH_LEAF, k1 = min(k0 + PH_LEAF, M.n);
-                for (uint32_t k = k0; k < k1; k++)
-                    if (!take(k)) return false;
-            } else if (sp + 2 <= PH_STACK) {
-                stack[sp++] = 2 * node + 2;
-                stack[sp++] = 2 * node + 1;
-            }
-        }
-        if (sp == 0) break;
-        node = stack[--sp];
-    }
-    float s = 2.0f / (PI_F * PI_F * r2);
-    *out = count ? acc * s : mk(0.f, 0.f, 0.f);
-    return true;
-}
-
 RT_D float3 warp_irradiance(const Map& M, float3 p, float3 n, uint32_t* hist, float* sel) {
     float r2 = M.r2;
     if (M.knn_k > 0) {
@@ -907,6 +849,86 @@ RT_D float3 warp_irradiance_1pass(const Map& M, float3 p, float3 n, WarpScratch&
     return mk(warp_sum(acc.x) * s, warp_sum(acc.y) * s, warp_sum(acc.z) * s);
 }
 
+// Irradiance at (p, n) by one warp from the grid: the ≤ 2 × 2 × 2 cells the
+// ball of the map's radius meets are read by lanes 0-7, their runs are joined
+// into one list (an inclusive scan of the lengths), and lane j tests entries
+// j, j + 32, … of the list — every load coalesced, no lane idle while another
+// works through a longer cell.  The facing photons within the radius go to
+// shared memory; in k-NN mode with more than k of them the k-th d² is selected
+// there.  Spans of more cells, crowded cells and maps without a grid take
+// warp_irradiance_1pass.  Same estimate as warp_irradiance; the terms are
+// summed in another order.
+RT_D float3 warp_gather(const Map& M, float3 p, float3 n, WarpScratch& W, uint32_t* hist, float* sel) {
+    const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+    if (!(M.r2 <= M.G.r2)) return warp_irradiance_1pass(M, p, n, W, hist, sel);
+    CellSpan s = cell_span(M, p, M.r2);
+    if (s.i1[0] - s.i0[0] > 1 || s.i1[1] - s.i0[1] > 1 || s.i1[2] - s.i0[2] > 1)
+        return warp_irradiance_1pass(M, p, n, W, hist, sel);
+    uint32_t st = 0, len = 0;
+    if (lane < 8) {
+        int x = s.i0[0] + (int)(lane & 1u), y = s.i0[1] + (int)((lane >> 1) & 1u), z = s.i0[2] + (int)(lane >> 2);
+        if (x <= s.i1[0] && y <= s.i1[1] && z <= s.i1[2]) {
+            uint2 r = cell_run(M, x, y, z);
+            st = r.x;
+            len = r.y - r.x;
+        }
+    }
+    uint32_t inc = len;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+        uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= (uint32_t)o) inc += v;
+    }
+    const uint32_t T = __shfl_sync(0xFFFFFFFFu, inc, 7);
+    if (T > PH_GRID_WARP_MAX) return warp_irradiance_1pass(M, p, n, W, hist, sel);
+    uint32_t ex[8], sv[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        ex[r] = __shfl_sync(0xFFFFFFFFu, inc - len, r);
+        sv[r] = __shfl_sync(0xFFFFFFFFu, st, r);
+    }
+    uint32_t cnt = 0;
+    for (uint32_t base = 0; base < T; base += 32) {
+        uint32_t f = base + lane;
+        bool c = false;
+        float d2 = 0.0f;
+        uint32_t k = 0;
+        if (f < T) {
+            // the run holding entry f: the last one starting at or before it
+            // (an empty run starts where the next begins and is passed over)
+            uint32_t e0 = ex[0], s0 = sv[0];
+#pragma unroll
+            for (int r = 1; r < 8; r++)
+                if (ex[r] <= f) { e0 = ex[r]; s0 = sv[r]; }
+            k = s0 + (f - e0);
+            d2 = pdist2(__ldg(M.pos + k), p);
+            c = d2 < M.r2 && pdot(__ldg(M.nor + k), n) > 0.0f;
+        }
+        uint32_t m = __ballot_sync(0xFFFFFFFFu, c);
+        uint32_t slot = cnt + __popc(m & lt);
+        if (c && slot < PH_CAND_CAP) { W.d2[slot] = d2; W.id[slot] = k; }
+        cnt += __popc(m);
+    }
+    __syncwarp();
+    if (cnt > PH_CAND_CAP) return warp_irradiance(M, p, n, hist, sel);
+    float r2 = M.r2;
+    if (M.knn_k > 0 && cnt >= M.knn_k) {
+        r2 = warp_radix_select(W.d2, cnt, M.knn_k, W.hist);
+        if (!(r2 > 0.0f)) return mk(0.f, 0.f, 0.f);
+    }
+    float3 acc = mk(0.f, 0.f, 0.f);
+    for (uint32_t j = lane; j < cnt; j += 32) {
+        float d2 = W.d2[j];
+        if (d2 < r2) {
+            float4 pw = __ldg(M.pow + W.id[j]);
+            acc = acc + mk(pw.x, pw.y, pw.z) * (1.0f - d2 / r2);
+        }
+    }
+    __syncwarp();
+    float sc = 2.0f / (PI_F * PI_F * r2);
+    return mk(warp_sum(acc.x) * sc, warp_sum(acc.y) * sc, warp_sum(acc.z) * sc);
+}
+
 }  // namespace rtph
 
 // queries n × 6 → irradiance n × 3; one warp per query
@@ -918,7 +940,7 @@ __global__ void k_photon_gather_api(rtph::Map M, const float* q, uint32_t n, flo
     uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t i = gw; i < n; i += nw) {
         float3 p = mk(q[i * 6], q[i * 6 + 1], q[i * 6 + 2]), nn = mk(q[i * 6 + 3], q[i * 6 + 4], q[i * 6 + 5]);
-        float3 r = rtph::warp_irradiance_1pass(M, p, nn, ws[w], hist[w], sel[w]);
+        float3 r = rtph::warp_gather(M, p, nn, ws[w], hist[w], sel[w]);
         if ((threadIdx.x & 31u) == 0) { out[i * 3] = r.x; out[i * 3 + 1] = r.y; out[i * 3 + 2] = r.z; }
     }
 }
@@ -983,46 +1005,16 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Ma
     uint32_t n = *count;
     uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    // each lane gathers one request on its own while the neighbourhood is sparse
-    // (fewer photons in range than k, or than 64 for the radius estimate); the
-    // warp then gathers the dense remaining requests together, one at a time
-    for (uint32_t base = gw * 32u; base < n; base += nw * 32u) {
-        uint32_t i = base + lane;
-        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-        bool cand = false;
-        if (i < n) {
-            a = gq[(size_t)i * 2];
-            b = gq[(size_t)i * 2 + 1];
-            float3 r;
-            // a lane gives a query to the warp once 16 photons are in range
-            // (below k every photon in range is used at the maximum radius)
-            uint32_t limit = M.knn_k > 0 ? min(M.knn_k, 16u) : 64u;
-            if (rtph::lane_gather(M, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), M.r2, limit, &r)) {
-                uint32_t tag = __float_as_uint(a.w);
-                float4* pc = T.pendC[(tag >> 1) & 1u] + (tag >> 2);
-                float4 f = *pc;
-                bool any = r.x > 0.0f || r.y > 0.0f || r.z > 0.0f;
-                *pc = any ? make_float4(f.x * r.x, f.y * r.y, f.z * r.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
-            } else {
-                cand = true;
-            }
-        }
-        uint32_t m = __ballot_sync(0xFFFFFFFFu, cand);
-        while (m) {
-            int src = __ffs(m) - 1;
-            m &= m - 1;
-            float4 qa = make_float4(__shfl_sync(0xFFFFFFFFu, a.x, src), __shfl_sync(0xFFFFFFFFu, a.y, src),
-                                    __shfl_sync(0xFFFFFFFFu, a.z, src), __shfl_sync(0xFFFFFFFFu, a.w, src));
-            float3 qn = mk(__shfl_sync(0xFFFFFFFFu, b.x, src), __shfl_sync(0xFFFFFFFFu, b.y, src),
-                           __shfl_sync(0xFFFFFFFFu, b.z, src));
-            float3 r = rtph::warp_irradiance_1pass(M, mk(qa.x, qa.y, qa.z), qn, ws[w], hist[w], sel[w]);
-            if (lane == 0) {
-                uint32_t tag = __float_as_uint(qa.w);
-                float4* pc = T.pendC[(tag >> 1) & 1u] + (tag >> 2);
-                float4 f = *pc;
-                bool any = r.x > 0.0f || r.y > 0.0f || r.z > 0.0f;
-                *pc = any ? make_float4(f.x * r.x, f.y * r.y, f.z * r.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+    // one warp per request (its cells' photons are few, and coalesced)
+    for (uint32_t i = gw; i < n; i += nw) {
+        float4 qa = gq[(size_t)i * 2], qb = gq[(size_t)i * 2 + 1];
+        float3 r = rtph::warp_gather(M, mk(qa.x, qa.y, qa.z), mk(qb.x, qb.y, qb.z), ws[w], hist[w], sel[w]);
+        if (lane == 0) {
+            uint32_t tag = __float_as_uint(qa.w);
+            float4* pc = T.pendC[(tag >> 1) & 1u] + (tag >> 2);
+            float4 f = *pc;
+            bool any = r.x > 0.0f || r.y > 0.0f || r.z > 0.0f;
+            *pc = any ? make_float4(f.x * r.x, f.y * r.y, f.z * r.z, 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
     }
 }
