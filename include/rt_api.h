@@ -379,6 +379,26 @@ int32_t rt_render_accumulate(RtScene* scene, const RtCamera* cam, const RtPassPa
                              float firefly_floor, int32_t reset,
                              float* out_sum, float* out_m2, uint32_t* out_count, int32_t mem);
 
+/* Asynchronous form of rt_render_accumulate, with the explicit stream of the
+ * replacement contract's threading rule (the reference's render_tiles,
+ * src/renderer.rs:655-669, is synchronous): the work is queued on the scene's
+ * stream after the work already on `cuda_stream` (a cudaStream_t; NULL = the
+ * legacy default stream), `cuda_stream` is made to wait for its end, and the
+ * call returns without waiting.  The wavefront runs as one CUDA graph (see
+ * RtTuning.graph).  Outputs are RT_MEM_DEVICE buffers (or NULL) that must
+ * stay valid until the work is done; at most one 2 GiB sample buffer of
+ * samples per call (W·H·n_samples·12 bytes), no guide training.  Errors of
+ * the device work (RT_ERR_TIMEOUT, RT_ERR_CAPACITY) and the statistics of
+ * rt_last_render_stats come from the next rt_sync on the handle. */
+int32_t rt_render_accumulate_async(RtScene* scene, const RtCamera* cam, const RtPassParams* params,
+                                   float firefly_clamp, uint32_t firefly_min_samples,
+                                   float firefly_floor, int32_t reset,
+                                   float* out_sum, float* out_m2, uint32_t* out_count, void* cuda_stream);
+/* Waits for the handle's queued work; returns the device status of the last
+ * asynchronous call (RT_OK, RT_ERR_TIMEOUT, RT_ERR_CAPACITY) and makes its
+ * statistics those of rt_last_render_stats. */
+int32_t rt_sync(RtScene* scene);
+
 /* ── output (src/output.rs, src/main.rs:571-583) ─────────────────────────── */
 #define RT_TONEMAP_AGX   0   /* Blender AgX with the "Punchy" look (output.rs:34-80), the default */
 #define RT_TONEMAP_ACES  1   /* Narkowicz ACES fit in AP1 (output.rs:7-31) */
@@ -585,6 +605,13 @@ typedef struct RtTuning {
      * (1, when the scene's extents allow it), 128-byte nodes whose child boxes
      * are 8-bit offsets rounded outward, so the hits are unchanged. */
     uint32_t node_format;
+    /* 1: every render call runs its wavefront as one CUDA graph — the path
+     * pool's first fill, then one conditional node per iteration up to the
+     * call's bound, each run only while rays remain — captured on the first
+     * call and replayed while the scene state, buffers and pool stay the
+     * same; 0 (the default): the host queues each iteration's launches and
+     * stops two iterations after the pool drains.  The images are the same. */
+    uint32_t graph;
 } RtTuning;
 #define RT_NODES_FULL      0
 #define RT_NODES_QUANTISED 1

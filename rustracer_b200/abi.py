@@ -230,7 +230,7 @@ class RtTuning(C.Structure):
     device loops' limits (0 = built-in)."""
     _fields_ = [("max_paths", C.c_uint32), ("trace_blocks_per_sm", C.c_uint32), ("shade_blocks_per_sm", C.c_uint32),
                 ("max_iterations", C.c_uint32), ("stack_limit", C.c_uint32), ("stack_ring", C.c_uint32),
-                ("node_format", C.c_uint32)]
+                ("node_format", C.c_uint32), ("graph", C.c_uint32)]
 
 
 class RtGuideParams(C.Structure):

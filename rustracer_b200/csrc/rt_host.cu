@@ -607,6 +607,21 @@ struct RtScene {
     float4* sq = nullptr;
     uint32_t* counters = nullptr;     // RT_CTR_WORDS (header + ring of iteration blocks)
     int* d_err = nullptr;
+    RenderLaunch* d_R = nullptr;      // device copy of the current call's RenderLaunch
+    // the wavefront as one captured graph (rt_set_tuning graph = 1, and the
+    // asynchronous entry point): kept while its key (buffers, scene state,
+    // pool, flags) matches and its iteration capacity K covers the call's bound
+    struct WaveGraph {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        std::vector<uint8_t> key;
+        uint64_t K = 0;
+    } wg;
+    bool graph_mode = false;
+    uint32_t* d_gstat = nullptr;      // next-iteration ray count and iterations run, left by the graph
+    uint64_t* h_tot = nullptr;        // pinned: ray totals of an asynchronous call
+    bool async_pending = false;       // an asynchronous call's statistics wait for rt_sync
+    int64_t async_per_it = 0;
     uint32_t* d_active = nullptr;     // active-pixel list of a converged mask
     uint32_t active_cap = 0;
     // lagged end-of-work check: next-iteration ray counts copied to pinned memory
@@ -775,7 +790,10 @@ int32_t rt_scene_destroy(RtScene* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto& b : s->owned) cudaFree(b.p);
     void* ps[] = {s->counters, s->d_err, s->scratch, s->d_conv, s->acc, s->m2, s->cnt, s->stage, s->d_active,
-                  s->b_acc, s->b_m2, s->b_cnt, s->d_jobs};
+                  s->b_acc, s->b_m2, s->b_cnt, s->d_jobs, s->d_R, s->d_gstat};
+    if (s->wg.exec) cudaGraphExecDestroy(s->wg.exec);
+    if (s->wg.graph) cudaGraphDestroy(s->wg.graph);
+    if (s->h_tot) cudaFreeHost(s->h_tot);
     free_paths(s);
     rtgh::destroy(s->guide);
     s->photons.release();
@@ -1558,6 +1576,9 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     }
     if (cudaMalloc(&s->d_err, sizeof(int)) != cudaSuccess) return bail(fail(s, RT_ERR_NOMEM, "cudaMalloc"));
     cudaMemset(s->d_err, 0, sizeof(int));
+    if (cudaMalloc(&s->d_R, sizeof(RenderLaunch)) != cudaSuccess || cudaMalloc(&s->d_gstat, 2 * sizeof(uint32_t)) != cudaSuccess ||
+        cudaHostAlloc((void**)&s->h_tot, 4 * sizeof(uint64_t), cudaHostAllocDefault) != cudaSuccess)
+        return bail(fail(s, RT_ERR_NOMEM, "cudaMalloc"));
     *out = s;
     return RT_OK;
 }
@@ -1599,7 +1620,9 @@ static int check_err(RtScene* s) {
     CK(cudaStreamSynchronize(s->stream));
     if (h) {
         cudaMemsetAsync(s->d_err, 0, sizeof(int), s->stream);
-        return fail(s, h, h == RT_ERR_CAPACITY ? "traversal stack overflow" : "device error");
+        return fail(s, h, h == RT_ERR_CAPACITY ? "traversal stack overflow"
+                          : h == RT_ERR_TIMEOUT ? "wavefront did not drain within its iteration bound"
+                                                : "device error");
     }
     return RT_OK;
 }
@@ -1778,10 +1801,110 @@ static WaveBufs scene_bufs(const RtScene* s) {
 // after it find empty queues.
 static const uint32_t STATUS_RING = 8, STATUS_LAG = 2;
 
+// End of iteration k in a graph: records the next iteration's ray count and
+// the iterations run, arms the next iteration's conditional node while rays
+// remain and the bound allows, and reports a bound reached with rays left.
+__global__ void k_wave_next(const uint32_t* __restrict__ cnt_next, const RenderLaunch* __restrict__ R, uint64_t k,
+                            cudaGraphConditionalHandle next, int has_next, uint32_t* gstat, int* derr) {
+    uint32_t c = *cnt_next;
+    gstat[0] = c;
+    gstat[1] = (uint32_t)(k + 1);
+    bool more = c > 0 && k + 1 < R->max_it;
+    if (has_next) cudaGraphSetConditional(next, more ? 1u : 0u);
+    if (c > 0 && !more) atomicCAS(derr, 0, RT_ERR_TIMEOUT);
+}
+
+static void wave_graph_free(RtScene* s) {
+    if (s->wg.exec) cudaGraphExecDestroy(s->wg.exec);
+    if (s->wg.graph) cudaGraphDestroy(s->wg.graph);
+    s->wg = RtScene::WaveGraph{};
+}
+
+// What a captured wavefront graph depends on besides the device RenderLaunch:
+// the scene state and buffers its launches were given, the pool and the flags
+// that choose its kernels.
+static std::vector<uint8_t> wave_key(const RtScene* s, const WaveBufs& W, const RenderLaunch& R, uint32_t pool) {
+    std::vector<uint8_t> k;
+    auto put = [&](const void* p, size_t n) { const uint8_t* b = (const uint8_t*)p; k.insert(k.end(), b, b + n); };
+    put(&s->S, sizeof(s->S));
+    put(&W.set[0], sizeof(PathState));
+    put(&W.set[1], sizeof(PathState));
+    put(&W.Rt, sizeof(PathState));
+    put(&W.cq, sizeof(W.cq));
+    const void* ptrs[3] = {W.sq, W.counters, W.derr};
+    put(ptrs, sizeof(ptrs));
+    int64_t v[5] = {pool, R.photons, R.guide.mode, s->sms, R.photons ? (int64_t)s->photons.generation : -1};
+    put(v, sizeof(v));
+    return k;
+}
+
+// Capture (or keep) the graph of a wavefront call: the prologue as a child
+// graph, then K ≥ max_it conditional IF nodes in a chain, node k holding
+// iteration k's launches and k_wave_next.  Node 0 always runs; node k + 1
+// runs when iteration k left rays and the call's bound allows — a chain of
+// IF nodes cannot run past K, whatever the device state.
+template <class Pro, class It>
+static int wave_graph_ensure(RtScene* s, const WaveBufs& W, const RenderLaunch& R, uint32_t pool, uint64_t max_it,
+                             Pro&& prologue, It&& iteration) {
+    std::vector<uint8_t> key = wave_key(s, W, R, pool);
+    if (s->wg.exec && s->wg.K >= max_it && key == s->wg.key) return RT_OK;
+    wave_graph_free(s);
+    const uint64_t K = (max_it + 31) / 32 * 32;
+    cudaGraph_t G = nullptr;
+    cudaError_t e = cudaGraphCreate(&G, 0);
+    auto ok = [&](cudaError_t r) { if (e == cudaSuccess && r != cudaSuccess) e = r; return e == cudaSuccess; };
+    cudaGraphNode_t prev = nullptr;
+    if (ok(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal))) {
+        int rc = prologue();
+        cudaGraph_t gp = nullptr;
+        ok(cudaStreamEndCapture(s->stream, &gp));
+        if (rc && e == cudaSuccess) e = cudaErrorUnknown;
+        if (gp) {
+            ok(cudaGraphAddChildGraphNode(&prev, G, nullptr, 0, gp));
+            cudaGraphDestroy(gp);
+        }
+    }
+    std::vector<cudaGraphConditionalHandle> h(K);
+    for (uint64_t k = 0; k < K && e == cudaSuccess; k++)
+        ok(cudaGraphConditionalHandleCreate(&h[k], G, k == 0 ? 1u : 0u, cudaGraphCondAssignDefault));
+    for (uint64_t k = 0; k < K && e == cudaSuccess; k++) {
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h[k];
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        if (!ok(cudaGraphAddNode(&node, G, &prev, 1, &cp))) break;
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        if (!ok(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)))
+            break;
+        int rc = iteration(k);
+        const uint32_t* cnt_next = W.counters + CTR_HDR_WORDS + ((k + 1) % RT_CTR_RING) * RT_CTR_STRIDE + CTR_COUNT;
+        k_wave_next<<<1, 1, 0, s->stream>>>(cnt_next, s->d_R, k, k + 1 < K ? h[k + 1] : 0, k + 1 < K ? 1 : 0,
+                                            s->d_gstat, W.derr);
+        ok(cudaGetLastError());
+        ok(cudaStreamEndCapture(s->stream, &body));
+        if (rc && e == cudaSuccess) e = cudaErrorUnknown;
+        prev = node;
+    }
+    if (e == cudaSuccess) ok(cudaGraphInstantiate(&s->wg.exec, G, 0));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (s->wg.exec) cudaGraphExecDestroy(s->wg.exec);
+        s->wg.exec = nullptr;
+        if (G) cudaGraphDestroy(G);
+        return fail(s, RT_ERR_CUDA, std::string("wavefront graph: ") + cudaGetErrorString(e));
+    }
+    s->wg.graph = G;
+    s->wg.key = std::move(key);
+    s->wg.K = K;
+    return RT_OK;
+}
+
 static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, const RtPassParams* p, uint32_t sample_idx,
                          uint32_t nsamp, float* dscratch, const uint32_t* active, uint32_t nactive, int64_t* ext_rays,
                          int64_t* sh_rays, int64_t* launches, const JobDev* jobs = nullptr, uint32_t n_jobs = 0,
-                         uint64_t jobs_total = 0) {
+                         uint64_t jobs_total = 0, bool async = false) {
     uint64_t total = n_jobs ? jobs_total : (uint64_t)nsamp * nactive;
     if (total == 0) return RT_OK;
     uint32_t pool = (uint32_t)std::min<uint64_t>(total, W.cap);
@@ -1805,27 +1928,37 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
     if (W.guide && s->guide && rtgh::mode(s->guide) != RT_GUIDE_OFF) R.guide = rtgh::view(s->guide);
     R.jobs = jobs;
     R.n_jobs = n_jobs;
-    uint32_t* hdr = W.counters;
-    auto blk = [&](uint64_t it) { return W.counters + CTR_HDR_WORDS + (it % RT_CTR_RING) * RT_CTR_STRIDE; };
-    size_t ev_used = 0;
-    auto mark = [&](int kind) {
-        if (!s->profiling) return;
-        if (ev_used >= s->pev.size()) { cudaEvent_t e; cudaEventCreate(&e); s->pev.push_back(e); s->pkind.push_back(0); }
-        s->pkind[ev_used] = kind;
-        cudaEventRecord(s->pev[ev_used++], s->stream);
-    };
-    int64_t nl = 0;
-    CK(cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * RT_CTR_WORDS, s->stream));
-    mark(0);
-    rth::launch_generate(s->S, W.set[0], R, pool, blk(0) + CTR_COUNT, s->stream);
-    nl++;
+    R.dev = s->d_R;
     // every iteration with samples left advances `pool` path segments, and a
     // sample has at most maxd segments; the drain takes at most maxd more
     uint64_t max_it = total * maxd / pool + maxd + 2;
     if (s->max_iterations) max_it = std::min<uint64_t>(max_it, s->max_iterations);
-    bool done = false;
-    uint64_t it = 0;
-    for (; it < max_it && !done; it++) {
+    R.max_it = max_it;
+    // stream-ordered: the previous call's kernels have read the old copy
+    CK(cudaMemcpyAsync(s->d_R, &R, sizeof(R), cudaMemcpyHostToDevice, s->stream));
+    uint32_t* hdr = W.counters;
+    auto blk = [&](uint64_t it) { return W.counters + CTR_HDR_WORDS + (it % RT_CTR_RING) * RT_CTR_STRIDE; };
+    size_t ev_used = 0;
+    const bool graph = (s->graph_mode || async) && !s->profiling && !(s->cap_out && s->cap_depth >= 0) && W.guide;
+    auto mark = [&](int kind) {
+        if (!s->profiling || graph) return;
+        if (ev_used >= s->pev.size()) { cudaEvent_t e; cudaEventCreate(&e); s->pev.push_back(e); s->pkind.push_back(0); }
+        s->pkind[ev_used] = kind;
+        cudaEventRecord(s->pev[ev_used++], s->stream);
+    };
+    // launches per iteration: extend, classify, shadow, retire, one shading
+    // kernel per class the scene's materials produce (the medium class counted
+    // with the media pair), the guide pair and the photon gather
+    const int64_t per_it = 4 + __builtin_popcount(s->S.class_mask & ~(1u << CLS_MEDIUM)) +
+                           (R.guide.mode != 0 ? 2 : 0) + (s->S.n_media > 0 ? 2 : 0) + (R.photons ? 1 : 0);
+    auto prologue = [&]() {
+        CK(cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * RT_CTR_WORDS, s->stream));
+        mark(0);
+        rth::launch_generate(s->S, W.set[0], R, pool, blk(0) + CTR_COUNT, s->stream);
+        return RT_OK;
+    };
+    // the launches of iteration `it`
+    auto iteration = [&](uint64_t it) {
         uint32_t* c = blk(it);
         uint32_t* cn = blk(it + 1);
         const PathState& A = W.set[it & 1];
@@ -1833,11 +1966,8 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         PendTargets T{{B.pend0, B.pend1, W.Rt.pend0, W.Rt.pend1}, {B.pendC, W.Rt.pendC}};
         mark(1);
         rth::launch_extend(s->S, A, nullptr, c + CTR_COUNT, c + CTR_EXTEND_NEXT, W.derr, s->sms, s->stream);
-        if (s->S.n_media > 0) {
-            rth::launch_media(s->S, A, nullptr, c + CTR_COUNT, s->sms, s->stream);
-            nl += 2;   // media events, medium shading
-        }
-        if ((int64_t)it == s->cap_depth && s->cap_out) {
+        if (s->S.n_media > 0) rth::launch_media(s->S, A, nullptr, c + CTR_COUNT, s->sms, s->stream);
+        if (!graph && (int64_t)it == s->cap_depth && s->cap_out) {
             // diagnostics: copy this iteration's rays out (origin, direction)
             CK(cudaStreamSynchronize(s->stream));
             uint32_t cnt = 0;
@@ -1855,37 +1985,62 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         }
         mark(2);
         rth::launch_shade(s->S, A, B, W.Rt, R, c, W.cq, cn + CTR_COUNT, W.sq, s->sms, s->stream);
-        if (R.photons) {
-            rth::launch_photon_gather_paths(s->photons, T, A.gq, c + CTR_GATHER_COUNT, s->sms, s->stream);
-            nl++;
-        }
+        if (R.photons) rth::launch_photon_gather_paths(s->photons, T, A.gq, c + CTR_GATHER_COUNT, s->sms, s->stream);
         mark(3);
         rth::launch_shadow(s->S, T, W.sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, W.derr, s->sms, s->stream);
         mark(0);
         rth::launch_retire(s->S, B, W.Rt, R, c, hdr, blk(it + 2), cn + CTR_COUNT, s->sms, s->stream);
-        // extend, classify, shadow, retire, and one shading kernel per class the
-        // scene's materials produce (the medium class is counted with media)
-        nl += 4 + __builtin_popcount(s->S.class_mask & ~(1u << CLS_MEDIUM)) + (R.guide.mode != 0 ? 2 : 0);
-        uint32_t slot = (uint32_t)(it % STATUS_RING);
-        CK(cudaMemcpyAsync(s->h_status + slot, cn + CTR_COUNT, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
-        CK(cudaEventRecord(s->st_ev[slot], s->stream));
-        if (it >= STATUS_LAG) {
-            uint32_t js = (uint32_t)((it - STATUS_LAG) % STATUS_RING);
-            CK(cudaEventSynchronize(s->st_ev[js]));
-            if (((volatile uint32_t*)s->h_status)[js] == 0) done = true;
-        }
-    }
-    mark(0);
-    CK(cudaGetLastError());
+        return RT_OK;
+    };
+    int64_t nl = 0;
     uint64_t tot[3] = {0, 0, 0};
-    CK(cudaMemcpyAsync(tot, W.counters, sizeof(tot), cudaMemcpyDeviceToHost, s->stream));
-    CK(cudaStreamSynchronize(s->stream));
-    if (!done) {
-        // the bound was reached: the last iterations' counts must be zero
-        for (uint32_t k = 0; k < std::min<uint64_t>(it, STATUS_LAG); k++)
-            if (s->h_status[(uint32_t)((it - 1 - k) % STATUS_RING)] != 0)
-                return fail(s, RT_ERR_TIMEOUT, "wavefront did not drain within its iteration bound (" +
-                                                   std::to_string(max_it) + " iterations)");
+    if (graph) {
+        // the call as one graph launch: the prologue, then one conditional node
+        // per iteration up to the bound, each run only while rays remain (the
+        // graph is captured once and kept while the buffers, scene state and
+        // bound it was made for stay the same)
+        if (int rc = wave_graph_ensure(s, W, R, pool, max_it, prologue, iteration)) return rc;
+        CK(cudaGraphLaunch(s->wg.exec, s->stream));
+        CK(cudaMemcpyAsync(s->h_status, s->d_gstat, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
+        if (async) {
+            CK(cudaMemcpyAsync(s->h_tot, W.counters, sizeof(tot), cudaMemcpyDeviceToHost, s->stream));
+            s->async_pending = true;
+            s->async_per_it = per_it;
+            return RT_OK;
+        }
+        CK(cudaMemcpyAsync(tot, W.counters, sizeof(tot), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        nl = 1 + (int64_t)s->h_status[1] * (per_it + 1);
+        // a bound reached with rays left sets RT_ERR_TIMEOUT in the error word
+    } else {
+        prologue();
+        nl++;
+        bool done = false;
+        uint64_t it = 0;
+        for (; it < max_it && !done; it++) {
+            iteration(it);
+            nl += per_it;
+            uint32_t slot = (uint32_t)(it % STATUS_RING);
+            CK(cudaMemcpyAsync(s->h_status + slot, blk(it + 1) + CTR_COUNT, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                               s->stream));
+            CK(cudaEventRecord(s->st_ev[slot], s->stream));
+            if (it >= STATUS_LAG) {
+                uint32_t js = (uint32_t)((it - STATUS_LAG) % STATUS_RING);
+                CK(cudaEventSynchronize(s->st_ev[js]));
+                if (((volatile uint32_t*)s->h_status)[js] == 0) done = true;
+            }
+        }
+        mark(0);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(tot, W.counters, sizeof(tot), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        if (!done) {
+            // the bound was reached: the last iterations' counts must be zero
+            for (uint32_t k = 0; k < std::min<uint64_t>(it, STATUS_LAG); k++)
+                if (s->h_status[(uint32_t)((it - 1 - k) % STATUS_RING)] != 0)
+                    return fail(s, RT_ERR_TIMEOUT, "wavefront did not drain within its iteration bound (" +
+                                                       std::to_string(max_it) + " iterations)");
+        }
     }
     if (ext_rays) *ext_rays += (int64_t)tot[HDR_EXT / 2];
     if (sh_rays) *sh_rays += (int64_t)tot[HDR_SHADOW / 2];
@@ -1906,7 +2061,7 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
 // `dscratch` (n_samples × npix × 3).  Pixels set in the converged mask are
 // not traced and get zero.
 static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p, float* dscratch, const uint8_t* dconv,
-                         int64_t* ext_rays, int64_t* sh_rays, int64_t* launches) {
+                         int64_t* ext_rays, int64_t* sh_rays, int64_t* launches, bool async = false) {
     uint32_t npix = p->width * p->height;
     uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
     uint64_t total = (uint64_t)nsamp * npix;
@@ -1940,7 +2095,7 @@ static int render_device(RtScene* s, const RtCamera* cam, const RtPassParams* p,
         CK(rtgh::begin_pass(s->guide, s->stream));
     }
     rc = run_wavefront(s, scene_bufs(s), cam, p, p->sample_idx, nsamp, dscratch, active, nactive, ext_rays, sh_rays,
-                       launches);
+                       launches, nullptr, 0, 0, async);
     if (rc || !guided) return rc;
     int64_t tl = 0;
     CK(rtgh::train_pass(s->guide, s->sms, s->stream, &tl));
@@ -2005,14 +2160,37 @@ extern "C" int32_t rt_render_pass(RtScene* s, const RtCamera* cam, const RtPassP
     return check_err(s);
 }
 
-extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const RtPassParams* p, float clamp,
-                                        uint32_t min_samples, float floor_, int32_t reset, float* out_sum,
-                                        float* out_m2, uint32_t* out_count, int32_t mem) {
+// rt_render_accumulate and its asynchronous form: `async` queues the work
+// after `caller` (device outputs only), signals `caller` when it is done and
+// leaves the error word, the statistics and the timing to rt_sync.
+static int accumulate_impl(RtScene* s, const RtCamera* cam, const RtPassParams* p, float clamp, uint32_t min_samples,
+                           float floor_, int32_t reset, float* out_sum, float* out_m2, uint32_t* out_count, int32_t mem,
+                           bool async, cudaStream_t caller) {
     int rc = validate_pass(s, cam, p);
     if (rc) return rc;
-    ENTER(s);
     uint32_t npix = p->width * p->height;
+    uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
+    // samples per wavefront run: as many as fit a 2 GiB sample buffer
+    uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nsamp, (2ull << 30) / ((uint64_t)npix * 12)));
+    if (async) {
+        if (mem != RT_MEM_DEVICE) return fail(s, RT_ERR_INVALID, "asynchronous calls take device buffers only");
+        if (per < nsamp)
+            return fail(s, RT_ERR_INVALID, "asynchronous calls take at most " + std::to_string(per) +
+                                               " samples per pixel at this size (one 2 GiB sample buffer)");
+        if (s->guide && rtgh::mode(s->guide) == RT_GUIDE_TRAIN)
+            return fail(s, RT_ERR_INVALID, "asynchronous calls do not train the guide");
+        if (s->async_pending) {
+            // the previous asynchronous call's statistics are folded first
+            if (int r2 = rt_sync(s)) return r2;
+        }
+        CK(cudaSetDevice(s->device));
+        CK(cudaEventRecord(s->caller_ev, caller));
+        CK(cudaStreamWaitEvent(s->stream, s->caller_ev, 0));
+    } else {
+        ENTER(s);
+    }
     if (s->acc_npix != npix) {
+        if (async) CK(cudaStreamSynchronize(s->stream));
         free_dev((void*&)s->acc); free_dev((void*&)s->m2); free_dev((void*&)s->cnt);
         if (cudaMalloc(&s->acc, (size_t)npix * 12) != cudaSuccess || cudaMalloc(&s->m2, (size_t)npix * 12) != cudaSuccess ||
             cudaMalloc(&s->cnt, (size_t)npix * 4) != cudaSuccess)
@@ -2025,11 +2203,9 @@ extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const R
         CK(cudaMemsetAsync(s->m2, 0, (size_t)npix * 12, s->stream));
         CK(cudaMemsetAsync(s->cnt, 0, (size_t)npix * 4, s->stream));
     }
-    uint32_t nsamp = std::max<uint32_t>(p->n_samples, 1);
-    // samples per wavefront run: as many as fit a 2 GiB sample buffer
-    uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(nsamp, (2ull << 30) / ((uint64_t)npix * 12)));
     size_t bytes = (size_t)per * npix * 3 * sizeof(float);
     if (s->scratch_bytes < bytes) {
+        CK(cudaStreamSynchronize(s->stream));
         free_dev((void*&)s->scratch);
         s->scratch_bytes = 0;
         if (cudaMalloc(&s->scratch, bytes) != cudaSuccess) return fail(s, RT_ERR_NOMEM, "cudaMalloc scratch");
@@ -2043,7 +2219,7 @@ extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const R
         q.sample_idx = p->sample_idx + k0;
         q.n_samples = std::min(per, nsamp - k0);
         int64_t e1, s1, l1;
-        rc = render_device(s, cam, &q, s->scratch, nullptr, &e1, &s1, &l1);
+        rc = render_device(s, cam, &q, s->scratch, nullptr, &e1, &s1, &l1, async);
         if (rc) return rc;
         rth::launch_accumulate(s->scratch, q.n_samples, npix, s->acc, s->m2, s->cnt, nullptr, clamp, min_samples, floor_,
                                s->stream);
@@ -2055,6 +2231,13 @@ extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const R
     if (out_sum) CK(cudaMemcpyAsync(out_sum, s->acc, (size_t)npix * 12, kind, s->stream));
     if (out_m2) CK(cudaMemcpyAsync(out_m2, s->m2, (size_t)npix * 12, kind, s->stream));
     if (out_count) CK(cudaMemcpyAsync(out_count, s->cnt, (size_t)npix * 4, kind, s->stream));
+    if (async) {
+        // the caller's stream waits for the outputs; statistics at rt_sync
+        CK(cudaEventRecord(s->caller_ev, s->stream));
+        CK(cudaStreamWaitEvent(caller, s->caller_ev, 0));
+        s->last_launches = nl;                        // without the iterations, known at rt_sync
+        return RT_OK;
+    }
     CK(cudaStreamSynchronize(s->stream));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, s->ev0, s->ev1);
@@ -2062,6 +2245,36 @@ extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const R
     s->last_ext = ext;
     s->last_shadow = sh;
     s->last_launches = nl;
+    return check_err(s);
+}
+
+extern "C" int32_t rt_render_accumulate(RtScene* s, const RtCamera* cam, const RtPassParams* p, float clamp,
+                                        uint32_t min_samples, float floor_, int32_t reset, float* out_sum,
+                                        float* out_m2, uint32_t* out_count, int32_t mem) {
+    return accumulate_impl(s, cam, p, clamp, min_samples, floor_, reset, out_sum, out_m2, out_count, mem, false, 0);
+}
+
+extern "C" int32_t rt_render_accumulate_async(RtScene* s, const RtCamera* cam, const RtPassParams* p, float clamp,
+                                              uint32_t min_samples, float floor_, int32_t reset, float* out_sum,
+                                              float* out_m2, uint32_t* out_count, void* cuda_stream) {
+    if (!s) return RT_ERR_INVALID;
+    return accumulate_impl(s, cam, p, clamp, min_samples, floor_, reset, out_sum, out_m2, out_count, RT_MEM_DEVICE,
+                           true, (cudaStream_t)cuda_stream);
+}
+
+extern "C" int32_t rt_sync(RtScene* s) {
+    if (!s) return RT_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    if (s->async_pending) {
+        s->async_pending = false;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+        s->last_ms = ms;
+        s->last_ext = (int64_t)s->h_tot[HDR_EXT / 2];
+        s->last_shadow = (int64_t)s->h_tot[HDR_SHADOW / 2];
+        s->last_launches += (int64_t)s->h_status[1] * (s->async_per_it + 1);
+    }
     return check_err(s);
 }
 
@@ -2297,6 +2510,7 @@ extern "C" int32_t rt_set_tuning(RtScene* s, const RtTuning* t) {
     if (t->stack_limit != 0 && (int64_t)t->stack_limit > s->stack_cap_built)
         return fail(s, RT_ERR_INVALID, "stack_limit must be 0 or at most " + std::to_string(s->stack_cap_built) +
                                            " (the entries the scene's stack columns hold)");
+    if (t->graph > 1) return fail(s, RT_ERR_INVALID, "graph must be 0 or 1");
     ENTER(s);
     CK(cudaStreamSynchronize(s->stream));
     s->max_paths = t->max_paths ? t->max_paths : MAX_PATHS;
@@ -2306,6 +2520,7 @@ extern "C" int32_t rt_set_tuning(RtScene* s, const RtTuning* t) {
     s->S.stack_cap = t->stack_limit ? (int)t->stack_limit : s->stack_cap_built;
     s->S.stack_ring = t->stack_ring ? (int)t->stack_ring : RT_SHORT_STACK;
     s->S.node_format = (s->qnodes_ok && t->node_format == RT_NODES_QUANTISED) ? RT_NODES_QUANTISED : RT_NODES_FULL;
+    s->graph_mode = t->graph != 0;
     return RT_OK;
 }
 
@@ -2324,6 +2539,7 @@ extern "C" int32_t rt_get_tuning(const RtScene* s, RtTuning* t) {
     t->stack_limit = (uint32_t)s->S.stack_cap;
     t->stack_ring = (uint32_t)s->S.stack_ring;
     t->node_format = (uint32_t)s->S.node_format;
+    t->graph = s->graph_mode ? 1u : 0u;
     return RT_OK;
 }
 

@@ -123,6 +123,7 @@ struct PhotonMapDev {
     uint32_t n = 0, nleaf_pow2 = 1, knn_k = 0;
     float r2 = 0.0f;
     bool present = false;
+    uint64_t generation = 0;                                  // bumped by every build, set and release
     PhotonGrid grid{{0.f, 0.f, 0.f}, 0.f, {1, 1, 1}, -1.f};
     uint2* cells = nullptr;                                   // [start, end) per grid cell
     // capacities (elements) of the map arrays, the heap, the cell table and the build's work buffers
@@ -172,6 +173,10 @@ struct RenderLaunch {
     // runs over all of them and width / height / cam / scratch above are unused
     const JobDev* jobs;
     uint32_t n_jobs;
+    // the device copy of this struct, which the kernels read (uploaded once per
+    // call, so a captured graph of the call's launches serves every call)
+    const RenderLaunch* dev;
+    uint64_t max_it;                       // the call's wavefront iteration bound
 };
 
 namespace rth {

@@ -1024,6 +1024,7 @@ PhotonMapDev::~PhotonMapDev() { free_all(); }
 void PhotonMapDev::release() {
     n = 0;
     present = false;
+    generation++;
     grid = PhotonGrid{{0.f, 0.f, 0.f}, 0.f, {1, 1, 1}, -1.f};
 }
 void PhotonMapDev::free_all() {

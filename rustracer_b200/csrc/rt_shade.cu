@@ -430,7 +430,9 @@ RT_D void init_path(const DevScene& S, const PathState& P, const RenderLaunch& R
     if (R.guide.mode == 2) P.rec[pid] = rtg::REC_NONE;
 }
 
-__global__ void k_generate(DevScene S, PathState A, RenderLaunch R, uint32_t pool, uint32_t* count0) {
+__global__ void k_generate(DevScene S, PathState A, const RenderLaunch* __restrict__ Rp, uint32_t pool,
+                           uint32_t* count0) {
+    const RenderLaunch& R = *Rp;
     if (blockIdx.x == 0 && threadIdx.x == 0) { *R.gen_next = pool; *count0 = pool; }
     for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < pool; pid += gridDim.x * blockDim.x)
         init_path(S, A, R, pid, pid);
@@ -441,9 +443,10 @@ __global__ void k_generate(DevScene S, PathState A, RenderLaunch R, uint32_t poo
 // env NEE — the order of renderer.rs:461-540) and writes its sample; for each
 // ended path the next ungenerated sample, if any, is appended to the next set.
 #define RETIRE_BLOCK 256
-__global__ void __launch_bounds__(RETIRE_BLOCK) k_retire(DevScene S, PathState B, PathState Rt, RenderLaunch R,
-                                                         uint32_t* ctr, uint32_t* hdr, uint32_t* clear_block,
-                                                         uint32_t* cout) {
+__global__ void __launch_bounds__(RETIRE_BLOCK) k_retire(DevScene S, PathState B, PathState Rt,
+                                                         const RenderLaunch* __restrict__ Rp, uint32_t* ctr,
+                                                         uint32_t* hdr, uint32_t* clear_block, uint32_t* cout) {
+    const RenderLaunch& R = *Rp;
     __shared__ BlockQ<1, RETIRE_BLOCK / 32> shq;
     __shared__ unsigned long long gbase;
     uint32_t n = ctr[CTR_RETIRE_COUNT];
@@ -685,9 +688,10 @@ RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
 // GUIDE (diffuse class only): bounces drawn from the guide mixture.
 template <int CLS, bool SKY, bool GUIDE>
 __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_shade(DevScene S, PathState A, PathState B, PathState Rt,
-                                                          RenderLaunch R, const uint32_t* __restrict__ qin,
-                                                          const uint32_t* cin, uint32_t* cout,
-                                                          float4* __restrict__ sq, uint32_t* ctr) {
+                                                          const RenderLaunch* __restrict__ Rp,
+                                                          const uint32_t* __restrict__ qin, const uint32_t* cin,
+                                                          uint32_t* cout, float4* __restrict__ sq, uint32_t* ctr) {
+    const RenderLaunch& R = *Rp;
     // queues appended to: [next set, retire records, gather requests, shadow rays]
     constexpr int NQ = (CLS == CLS_DIFFUSE || CLS == CLS_METAL || CLS == CLS_PBR) ? 4
                      : (CLS == CLS_MISS || CLS == CLS_EMIT) ? 1 : 2;
@@ -1167,8 +1171,9 @@ __global__ void k_accumulate(const float* __restrict__ scratch, uint32_t nsamp, 
 static size_t guide_infer_smem() {
     return (size_t)rtg::W_SMEM * 2 + (size_t)GUIDE_WARPS * 16 * GUIDE_LDO * 4;
 }
-__global__ void __launch_bounds__(256) k_guide_encode(DevScene S, PathState A, RenderLaunch R,
+__global__ void __launch_bounds__(256) k_guide_encode(DevScene S, PathState A, const RenderLaunch* __restrict__ Rp,
                                                       const uint32_t* __restrict__ qin, const uint32_t* cin) {
+    const RenderLaunch& R = *Rp;
     uint32_t n = *cin;
     for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n; qi += gridDim.x * blockDim.x) {
         uint32_t pid = qin[qi];
@@ -1183,8 +1188,10 @@ __global__ void __launch_bounds__(256) k_guide_encode(DevScene S, PathState A, R
         for (int k = 0; k < 8; k++) dst[k] = make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
     }
 }
-__global__ void __launch_bounds__(GUIDE_WARPS * 32) k_guide_infer(RenderLaunch R, const uint32_t* __restrict__ qin,
+__global__ void __launch_bounds__(GUIDE_WARPS * 32) k_guide_infer(const RenderLaunch* __restrict__ Rp,
+                                                                  const uint32_t* __restrict__ qin,
                                                                   const uint32_t* cin) {
+    const RenderLaunch& R = *Rp;
     extern __shared__ __align__(16) unsigned char gsm[];
     __nv_bfloat16* Ws = reinterpret_cast<__nv_bfloat16*>(gsm);
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1230,13 +1237,13 @@ namespace rth {
 void launch_guide_infer(const DevScene& S, const PathState& A, const RenderLaunch& R, const uint32_t* queue,
                         const uint32_t* count, int sms, cudaStream_t st) {
     cudaFuncSetAttribute(k_guide_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)guide_infer_smem());
-    k_guide_encode<<<sms * 8, 256, 0, st>>>(S, A, R, queue, count);
-    k_guide_infer<<<sms * 2, GUIDE_WARPS * 32, guide_infer_smem(), st>>>(R, queue, count);
+    k_guide_encode<<<sms * 8, 256, 0, st>>>(S, A, R.dev, queue, count);
+    k_guide_infer<<<sms * 2, GUIDE_WARPS * 32, guide_infer_smem(), st>>>(R.dev, queue, count);
 }
 void launch_generate(const DevScene& S, const PathState& A, const RenderLaunch& R, uint32_t pool, uint32_t* count0,
                      cudaStream_t st) {
     int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>((pool + 255) / 256, 148u * 16u));
-    k_generate<<<grid, 256, 0, st>>>(S, A, R, pool, count0);
+    k_generate<<<grid, 256, 0, st>>>(S, A, R.dev, pool, count0);
 }
 void launch_shade(const DevScene& S, const PathState& A, const PathState& B, const PathState& Rt, const RenderLaunch& R,
                   uint32_t* ctr, const ClassQueues& Q, uint32_t* cout, float4* sq, int sms, cudaStream_t st) {
@@ -1248,9 +1255,9 @@ void launch_shade(const DevScene& S, const PathState& A, const PathState& B, con
 #define RT_SHADE_CLASS_G(C, G)                                                                              \
     if (!((S.class_mask >> (C)) & 1u)) {                                                                   \
     } else if (S.bg_type == RT_BG_PHYSICAL)                                                                 \
-        k_shade<C, true, G><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr); \
+        k_shade<C, true, G><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R.dev, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr); \
     else                                                                                                    \
-        k_shade<C, false, G><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr)
+        k_shade<C, false, G><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R.dev, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr)
 #define RT_SHADE_CLASS(C) RT_SHADE_CLASS_G(C, false)
     RT_SHADE_CLASS(CLS_MISS);
     RT_SHADE_CLASS(CLS_EMIT);
@@ -1265,7 +1272,7 @@ void launch_shade(const DevScene& S, const PathState& A, const PathState& B, con
 }
 void launch_retire(const DevScene& S, const PathState& B, const PathState& Rt, const RenderLaunch& R, uint32_t* ctr,
                    uint32_t* hdr, uint32_t* clear_block, uint32_t* cout, int sms, cudaStream_t st) {
-    k_retire<<<sms * 8, RETIRE_BLOCK, 0, st>>>(S, B, Rt, R, ctr, hdr, clear_block, cout);
+    k_retire<<<sms * 8, RETIRE_BLOCK, 0, st>>>(S, B, Rt, R.dev, ctr, hdr, clear_block, cout);
 }
 void launch_active_list(const uint8_t* conv, uint32_t width, uint32_t height, uint32_t* list, uint32_t* count,
                         cudaStream_t st) {

@@ -67,6 +67,9 @@ def lib():
         L.rt_capture_rays.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), u32, vp, i64,
                                       C.POINTER(i64)]
         L.rt_set_tuning.argtypes = [vp, C.POINTER(abi.RtTuning)]
+        L.rt_render_accumulate_async.argtypes = [vp, C.POINTER(abi.RtCamera), C.POINTER(abi.RtPassParams), f, u32, f,
+                                                 i32, vp, vp, vp, vp]
+        L.rt_sync.argtypes = [vp]
         L.rt_get_tuning.argtypes = [vp, C.POINTER(abi.RtTuning)]
         L.rt_set_caller_stream.argtypes = [vp, vp]
         L.rt_guide_init.argtypes = [vp, C.POINTER(abi.RtGuideParams)]
@@ -314,6 +317,27 @@ class GpuScene:
                                                sp, mp, cp, mem))
         return s, m, c
 
+    def render_accumulate_async(self, cam, params, outputs, firefly_clamp=0.0, firefly_min_samples=4,
+                                firefly_floor=5.0, reset=True, stream=None):
+        """rt_render_accumulate_async: queue the render on the scene's stream
+        after torch's current stream (or `stream`, a torch.cuda.Stream), which
+        then waits for it; returns at once.  outputs: CUDA tensors (sum, m2,
+        count) that must stay alive until the work is done.  sync() reports
+        the device status and the statistics."""
+        import torch
+        s, m, c = outputs
+        st = stream if stream is not None else torch.cuda.current_stream(s.device)
+        self._check(lib().rt_render_accumulate_async(self.h, C.byref(cam), C.byref(params), float(firefly_clamp),
+                                                     int(firefly_min_samples), float(firefly_floor),
+                                                     1 if reset else 0, C.c_void_p(s.data_ptr()),
+                                                     C.c_void_p(m.data_ptr()), C.c_void_p(c.data_ptr()),
+                                                     C.c_void_p(st.cuda_stream)))
+
+    def sync(self):
+        """rt_sync: wait for the handle's queued work; raises on a device error of
+        the last asynchronous call."""
+        self._check(lib().rt_sync(self.h))
+
     def render_batch(self, jobs, shared, window=0, outputs=None):
         """A packed batch of requests on this scene (rt_render_batch).  jobs:
         dicts with cam, width, height, spp and optionally strata (⌊√spp⌋),
@@ -429,9 +453,9 @@ class GpuScene:
     # ── diagnostics ──────────────────────────────────────────────────────
     # ── launch tuning (rt_set_tuning) ─────────────────────────────────────
     def set_tuning(self, max_paths=0, trace_blocks_per_sm=0, shade_blocks_per_sm=0, max_iterations=0,
-                   stack_limit=0, stack_ring=0, node_format=0):
+                   stack_limit=0, stack_ring=0, node_format=0, graph=0):
         t = abi.RtTuning(int(max_paths), int(trace_blocks_per_sm), int(shade_blocks_per_sm), int(max_iterations),
-                         int(stack_limit), int(stack_ring), int(node_format))
+                         int(stack_limit), int(stack_ring), int(node_format), int(graph))
         self._check(lib().rt_set_tuning(self.h, C.byref(t)))
 
     def get_tuning(self):
@@ -439,7 +463,7 @@ class GpuScene:
         self._check(lib().rt_get_tuning(self.h, C.byref(t)))
         return dict(max_paths=t.max_paths, trace_blocks_per_sm=t.trace_blocks_per_sm,
                     shade_blocks_per_sm=t.shade_blocks_per_sm, max_iterations=t.max_iterations,
-                    stack_limit=t.stack_limit, stack_ring=t.stack_ring, node_format=t.node_format)
+                    stack_limit=t.stack_limit, stack_ring=t.stack_ring, node_format=t.node_format, graph=t.graph)
 
     # ── path guiding (rt_guide_*) ─────────────────────────────────────────
     def guide_init(self, params=None):
