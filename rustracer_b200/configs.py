@@ -519,29 +519,43 @@ def gem_room_scene(width=1200, height=800, spp=128, max_depth=50, photons=500_00
 
 
 def guided_box_scene(width=1280, height=720, spp=64, max_depth=24, hero=4, seed=9, density=4.0, gem=True,
-                     medium=True, grid_res=128):
-    """The hard-transport workload of the learned proposal: the box room with
-    its light hidden above two occluding quads that leave a 0.05-wide slit, a
-    57-facet round brilliant (radius 0.12, diamond dispersion) and a 128³
-    fractal-Perlin density grid in the lower half (σ_t ∈ [0, density], albedo
-    0.9, g = 0.3; delta tracking against per-brick majorants, ratio-tracked
-    shadows).  grid_res = 0 puts the reference's procedural noise medium
-    (volume.rs) there instead.  Light enters the room only through the slit,
-    as a narrow beam onto the floor and the medium; everything else is lit by
-    that patch, which cosine bounces find rarely and light sampling cannot
-    reach."""
-    sb, st = box_scene(width, height, spp, max_depth, hero, seed)
+                     medium=True, grid_res=128, emission=600.0):
+    """The hard-transport workload of the learned proposal: the box room whose
+    ceiling has only a 0.05 × 0.1 slit (x ∈ [0.475, 0.525], z ∈ [0.45, 0.55]),
+    with a 0.1² blackbody light (6500 K × `emission`) in a closed light box
+    0.5 above it, a 57-facet round brilliant (radius 0.12, diamond
+    dispersion) and a 128³ fractal-Perlin density grid in the lower half
+    (σ_t ∈ [0, density], albedo 0.9, g = 0.3; delta tracking against
+    per-brick majorants, ratio-tracked shadows).  grid_res = 0 puts the
+    reference's procedural noise medium (volume.rs) there instead.  The light
+    reaches the room only as the beam through the slit (a patch about 0.3
+    across on the floor, and the medium along it); every other surface is lit
+    from that patch, which cosine bounces find rarely and light sampling
+    cannot reach."""
+    sb = SceneBuilder()
     sb.name = "guided box"
-    sb.spheres.clear()
+    sb.spectral_range = 1 if hero > 1 else 0
     white = sb.add_material(Material.lambertian((0.73, 0.73, 0.73)))
-    # occluders 0.05 below the light spanning the room but for a slit 0.05 wide and 0.1
-    # long (x ∈ [0.475, 0.525], z ∈ [0.45, 0.55]): the light reaches the room through
-    # the slit alone, as a small bright patch on the floor
-    y = 1.0 - 0.05
-    sb.add_quad((0.0, y, 0.0), (0.475, 0.0, 0.0), (0.0, 0.0, 1.0), white)
-    sb.add_quad((0.525, y, 0.0), (0.475, 0.0, 0.0), (0.0, 0.0, 1.0), white)
-    sb.add_quad((0.475, y, 0.0), (0.05, 0.0, 0.0), (0.0, 0.0, 0.45), white)
-    sb.add_quad((0.475, y, 0.55), (0.05, 0.0, 0.0), (0.0, 0.0, 0.45), white)
+    red = sb.add_material(Material.lambertian((0.65, 0.05, 0.05)))
+    green = sb.add_material(Material.lambertian((0.12, 0.45, 0.15)))
+    sb.add_quad((0, 0, 0), (1, 0, 0), (0, 0, 1), white)      # floor
+    sb.add_quad((0, 0, 1), (1, 0, 0), (0, 1, 0), white)      # back wall
+    sb.add_quad((1, 0, 0), (0, 0, 1), (0, 1, 0), red)        # left wall (image left)
+    sb.add_quad((0, 0, 0), (0, 0, 1), (0, 1, 0), green)      # right wall
+    # the ceiling at y = 1 around the slit
+    sb.add_quad((0.0, 1.0, 0.0), (0.475, 0.0, 0.0), (0.0, 0.0, 1.0), white)
+    sb.add_quad((0.525, 1.0, 0.0), (0.475, 0.0, 0.0), (0.0, 0.0, 1.0), white)
+    sb.add_quad((0.475, 1.0, 0.0), (0.05, 0.0, 0.0), (0.0, 0.0, 0.45), white)
+    sb.add_quad((0.475, 1.0, 0.55), (0.05, 0.0, 0.0), (0.0, 0.0, 0.45), white)
+    # the light box above the slit: four walls and a lid, the light just below the lid
+    lo, hi, top = 0.35, 0.65, 1.5
+    sb.add_quad((lo, 1.0, lo), (hi - lo, 0.0, 0.0), (0.0, top - 1.0, 0.0), white)
+    sb.add_quad((lo, 1.0, hi), (hi - lo, 0.0, 0.0), (0.0, top - 1.0, 0.0), white)
+    sb.add_quad((lo, 1.0, lo), (0.0, 0.0, hi - lo), (0.0, top - 1.0, 0.0), white)
+    sb.add_quad((hi, 1.0, lo), (0.0, 0.0, hi - lo), (0.0, top - 1.0, 0.0), white)
+    sb.add_quad((lo, top, lo), (hi - lo, 0.0, 0.0), (0.0, 0.0, hi - lo), white)
+    light = sb.add_material(Material.blackbody(6500.0, emission))
+    sb.add_light_quad((0.45, top - 1e-3, 0.45), (0.1, 0, 0), (0, 0, 0.1), light)
     diffuse = sb.add_material(Material.lambertian((0.73, 0.73, 0.73)))
     sb.add_sphere((0.3, 0.18, 0.6), 0.18, diffuse)
     if gem:
@@ -554,8 +568,11 @@ def guided_box_scene(width=1280, height=720, spp=64, max_depth=24, hero=4, seed=
     elif medium:
         sb.add_medium("noise", "box", density, (0.9, 0.9, 0.9), g=0.3, noise_scale=4.0, threshold=0.05,
                       p_min=(0.0, 0.0, 0.0), p_max=(1.0, 0.5, 1.0), seed=seed)
-    st["name"] = (f"guided box (slit light, gem, {grid_res}^3 grid medium) {width}x{height} {spp}spp "
-                  f"depth{max_depth} hero{hero}")
+    sb.set_solid((0.0, 0.0, 0.0))
+    cam = make_camera((0.5, 0.5, -1.4), (0.5, 0.5, 0.5), vfov=40.0, aspect=width / height)
+    st = dict(width=width, height=height, spp=spp, max_depth=max_depth, hero=hero, seed=seed, camera=cam)
+    st["name"] = (f"guided box (ceiling slit under a light box, gem, {grid_res}^3 grid medium) {width}x{height} "
+                  f"{spp}spp depth{max_depth} hero{hero}")
     return sb, st
 
 

@@ -181,7 +181,7 @@ def test_guided_render_is_unbiased_and_measures_its_gain():
     base = pass_params(w, h, 0, 1, 8, 24, hero, 1.0, 5)
     _, _, stats = render_guided(gs, cam, base, 48, train_spp=48, train_per_call=4,
                                 guide=guide_params(batch=16384, steps_per_pass=16, seed=3))
-    assert stats["steps"] == 12 * 16 and stats["samples"] > 10_000
+    assert stats["steps"] == 12 * 16 and stats["samples"] > 2_000     # records that gathered light
     gs.guide_mode(1)
     spp = 256
     gi = gs.render_pass(cam, pass_params(w, h, 1000, spp, 16, 24, hero, 1.0, 7))
