@@ -79,6 +79,8 @@ def parse():
     ap.add_argument("--guide-spp-per-call", type=int, default=8, help="guided: samples per training render call")
     ap.add_argument("--guide-steps", type=int, default=8, help="guided: Adam steps after each training call")
     ap.add_argument("--guide-train-spp", type=int, default=64, help="guided: samples per pixel of training")
+    ap.add_argument("--pass-size", default=None, help="pass mode: frame WxH (default: the workload's)")
+    ap.add_argument("--pass-spp", type=int, default=None, help="pass mode: samples per pixel of the measured call")
     ap.add_argument("--no-autotune", action="store_true",
                     help="icosphere: keep the built-in launch grids instead of autotune.py's choice")
     return ap.parse_args()
@@ -380,19 +382,22 @@ def roofline(scene, sb, cam, w=W, h=H, spp=SPP, depth=DEPTH, hero=HERO, seed=2, 
     achieved = total_bytes_pass * spp / (ext_ms / 1000.0) / 1e9 if ext_ms > 0 else None
     # DRAM traffic: ncu's bytes per extension ray on this kernel and scene
     # (a profile summary) times this render's extension rays per launch
-    traffic = None
+    traffic, traffic_source = None, None
     tfile = os.path.join(ROOT, "profiles", traffic_file) if traffic_file else None
     if tfile and os.path.exists(tfile):
         for ln in open(tfile):
             if ln.startswith("traffic_bytes_per_ray:"):
                 traffic = float(ln.split(":")[1]) * ext_rays / max(1, ext_launches)
+            elif ln.startswith("source:"):
+                traffic_source = f"profiles/{traffic_file}: ncu on {ln.split(':', 1)[1].strip()}, per extension ray"
     launch_s = ext_ms / 1000.0 / max(1, ext_launches)
     dram_gbs = traffic / launch_s / 1e9 if (traffic and launch_s > 0) else None
     return {"kernel": "k_extend (8-wide BVH closest hit)", "bound": "hbm",
             "limiter": "L1/TEX throughput and load latency (node fetches hit L1/L2), not DRAM bandwidth",
             "achieved": achieved, "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
-            "traffic": traffic, "dram_gbs": dram_gbs, "dram_frac": dram_gbs / peak if dram_gbs else None,
+            "traffic": traffic, "traffic_source": traffic_source, "dram_gbs": dram_gbs,
+            "dram_frac": dram_gbs / peak if dram_gbs else None,
             "algorithmic_bytes_per_launch": total_bytes_pass * spp / max(1, ext_launches),
             "launches": ext_launches, "kernel_ms": ext_ms,
             "stage_ms": {k: v[0] for k, v in kt.items()},
@@ -760,38 +765,50 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
-def one_pass():
+def one_pass(args):
     """Profiler driver: one warm-up call and one measured call of the 1920×1080
-    icosphere workload, 16 samples per pixel per call: 33.2M path samples
-    through the 8.4M-path pool, so most launches run on a full, refilled pool
-    as in the timed 64-spp render."""
+    icosphere workload (or --pass-size / --pass-spp), 16 samples per pixel per
+    call: 33.2M path samples through the 8.4M-path pool, so most launches run
+    on a full, refilled pool as in the timed 64-spp render."""
     import torch
     from rustracer_b200 import configs
     from rustracer_b200.renderer import GpuScene, pass_params
     sb, st = configs.icosphere_scene(seed=2)
     scene = GpuScene(sb, device=0)
-    out = torch.zeros((16, H, W, 3), device="cuda")
+    w, h, spp = pass_frame(args, W, H, 16)
+    out = torch.zeros((spp, h, w, 3), device="cuda")
     for k in range(2):
-        scene.render_pass(st["camera"], pass_params(W, H, 16 * k, 16, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2), out=out)
+        scene.render_pass(st["camera"], pass_params(w, h, spp * k, spp, int(np.sqrt(SPP)), DEPTH, HERO, 1.0, 2), out=out)
+        print(f"call {k + 1}", scene.last_stats(), flush=True)
     torch.cuda.synchronize()
-    print("pass ok", scene.last_stats(), flush=True)
+    print("pass ok", flush=True)
 
 
-def one_pass_scene(kind):
-    """Profiler driver for the box and gem workloads at their stated frames:
-    the gem builds its 2M-photon map, then one 1-spp warm-up call and one
-    measured 4-spp call (gem) or 16-spp call (box) of rt_render_accumulate."""
+def pass_frame(args, w, h, spp):
+    """The pass mode's frame and samples: the workload's unless --pass-size / --pass-spp."""
+    if args.pass_size:
+        w, h = (int(x) for x in args.pass_size.lower().split("x"))
+    return w, h, args.pass_spp or spp
+
+
+def one_pass_scene(kind, args):
+    """Profiler driver for the box and gem workloads (at their stated frames
+    unless --pass-size / --pass-spp): the gem builds its 2M-photon map, then
+    one 1-spp warm-up call and one measured 4-spp call (gem) or 16-spp call
+    (box) of rt_render_accumulate."""
     from rustracer_b200 import configs
     from rustracer_b200.renderer import GpuScene, pass_params
     sb, st = configs.gem_scene() if kind == "gem" else configs.box_scene()
-    w, h, depth, hero = st["width"], st["height"], st["max_depth"], st["hero"]
+    depth, hero = st["max_depth"], st["hero"]
+    w, h, spp = pass_frame(args, st["width"], st["height"], 4 if kind == "gem" else st["spp"])
     scene = GpuScene(sb, device=0)
     if kind == "gem":
         scene.photon_build(st["photon_params"](seed=1))
-    spp = 4 if kind == "gem" else st["spp"]
     scene.render_accumulate(st["camera"], pass_params(w, h, 0, 1, 1, depth, hero, 1.0, 3))
+    print("call 1", scene.last_stats(), flush=True)
     scene.render_accumulate(st["camera"], pass_params(w, h, 1, spp, int(np.sqrt(spp)), depth, hero, 1.0, 3))
-    print("pass ok", scene.last_stats(), flush=True)
+    print("call 2", scene.last_stats(), flush=True)
+    print("pass ok", flush=True)
 
 
 def one_pass_guided():
@@ -818,9 +835,9 @@ def main():
         if args.config == "guided":
             one_pass_guided()
         elif args.config in ("gem", "box"):
-            one_pass_scene(args.config)
+            one_pass_scene(args.config, args)
         else:
-            one_pass()
+            one_pass(args)
         return
     if args.impl == "reference":
         run_reference(args)
