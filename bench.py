@@ -28,9 +28,9 @@ secondary: on one GPU the same line carries the box workload (256x256,
            16 spp, depth 8) and the gem workload (57-facet brilliant, 2M-photon
            caustic map rebuilt every step, 1280x720, 256 spp, depth 32), each
            with its value, e2e, roofline and cpu_baseline.
---impl reference: the CPU oracle on all host cores, each step 80 bands of
+--impl reference: the CPU oracle on all host cores, each step 320 bands of
            32 rows x 1920 px x 1 spp of the icosphere frame (the cpu_baseline
-           sampler), so the default run times ~10 s.
+           sampler, ~2.5 s per step), so the default 5 steps time ≥ 10 s.
 """
 import argparse
 import json
@@ -52,7 +52,7 @@ DEPTH = 12
 HERO = 4
 METRIC = "path samples/s (1920x1080 icosphere workload)"
 UNIT = "path samples/s"
-REF_BANDS = 80          # bands of 32 rows per reference-arm step (~0.5 s on 16 cores)
+REF_BANDS = 320         # bands of 32 rows per reference-arm step (~2.5 s on 16 cores: 5 steps ≥ 10 s)
 
 
 def parse():
@@ -181,11 +181,11 @@ def run_reference(args):
         o.render_pass(st["camera"], p, threads=threads, rows=(row0, row0 + 32))
         return 32 * W
 
-    def step(k):
-        return sum(band(k * REF_BANDS + b) for b in range(REF_BANDS))
+    def step(k, bands=REF_BANDS):
+        return sum(band(k * REF_BANDS + b) for b in range(bands))
 
     for k in range(args.warmup):
-        step(k)
+        step(k, REF_BANDS // 8)                 # warm-up steps at an eighth of the size
     t0 = time.perf_counter()
     n = sum(step(args.warmup + k) for k in range(args.steps))
     el = time.perf_counter() - t0
