@@ -601,9 +601,12 @@ typedef struct RtTuning {
      * spill path. */
     uint32_t stack_ring;
     /* Node layout the traversal reads: RT_NODES_FULL (0, the default), the
-     * reference's 224-byte float layout (bvh.rs:25-32), or RT_NODES_QUANTISED
+     * reference's 224-byte float layout (bvh.rs:25-32); RT_NODES_QUANTISED
      * (1, when the scene's extents allow it), 128-byte nodes whose child boxes
-     * are 8-bit offsets rounded outward, so the hits are unchanged. */
+     * are 8-bit offsets rounded outward; RT_NODES_WIDE4 (2, scenes whose tree
+     * was built on the device), 4-wide nodes of 112 bytes over the same binary
+     * SAH tree — the reference's BVH width choice (bvh.rs:10-14).  The hits do
+     * not depend on it. */
     uint32_t node_format;
     /* 1: every render call runs its wavefront as one CUDA graph — the path
      * pool's first fill, then one conditional node per iteration up to the
@@ -615,6 +618,7 @@ typedef struct RtTuning {
 } RtTuning;
 #define RT_NODES_FULL      0
 #define RT_NODES_QUANTISED 1
+#define RT_NODES_WIDE4     2
 int32_t rt_set_tuning(RtScene* scene, const RtTuning* tuning);
 
 /* The stream the caller queues its own work on (a cudaStream_t; NULL = the

@@ -299,7 +299,7 @@ def iptr(a):
 
 
 RT_EMIT_DISK, RT_EMIT_QUAD, RT_EMIT_SUN, RT_EMIT_LIGHT = 0, 1, 2, 3
-RT_NODES_FULL, RT_NODES_QUANTISED = 0, 1
+RT_NODES_FULL, RT_NODES_QUANTISED, RT_NODES_WIDE4 = 0, 1, 2
 RT_MAX_EMITTERS = 8
 
 

@@ -4,14 +4,16 @@ renderer runs a fixed rayon row loop, renderer.rs:684).
 The knobs are rt_set_tuning's: the path-pool capacity (how many paths are in
 flight; memory, and how long the final drain runs on a partial wavefront),
 the grids of the persistent traversal kernels and of the shading kernels, and
-the node layout the traversal reads (8-bit quantised 128-byte nodes or the
-reference's 224-byte float nodes).
+the node layout the traversal reads: the reference's 224-byte 8-wide float
+nodes, their 8-bit quantised 128-byte copy, or 4-wide 112-byte nodes over the
+same binary tree — the BVH width the reference picks by target
+(bvh.rs:10-14).
 Every path draws its random numbers from (pixel, sample), so the knobs change
 speed and memory, never the image.  The tuner times each candidate on a short
 render of the frame it will serve (a probe of at most PROBE_SAMPLES path
 samples), keeps the fastest, sets it on the scene and caches it under the
-caller's key; BVH width is not a knob (the node layout is the 8-wide one
-built at scene creation).
+caller's key.  A layout the scene lacks (a quantised copy beyond its range,
+4-wide nodes of a tree built on the host) is skipped.
 """
 import ctypes as C
 import itertools
@@ -20,7 +22,7 @@ import math
 from . import abi
 
 SPACE = {"max_paths": (1 << 21, 1 << 22, 1 << 23), "trace_blocks_per_sm": (4, 6), "shade_blocks_per_sm": (4, 8, 16),
-         "node_format": (0, 1)}
+         "node_format": (abi.RT_NODES_FULL, abi.RT_NODES_QUANTISED, abi.RT_NODES_WIDE4)}
 PROBE_SAMPLES = 1 << 24
 _cache = {}
 
@@ -57,9 +59,13 @@ def autotune(gs, cam, params, key=None, space=None, repeats=2, timer=None):
             gs.set_tuning(**t)
             gs.render_accumulate(cam, probe)
             return gs.last_stats()["ms"]
+    from .renderer import RtError
     table = []
     for t in candidates(space):
-        table.append((min(timer(t) for _ in range(max(1, repeats))), t))
+        try:
+            table.append((min(timer(t) for _ in range(max(1, repeats))), t))
+        except RtError:
+            continue                    # a layout this scene does not have
     best = min(table, key=lambda x: x[0])[1]
     gs.set_tuning(**best)
     if key is not None:

@@ -374,13 +374,13 @@ __global__ void k_small(const Seg* __restrict__ segs, int32_t nseg, const float*
 
 // kids of the wide node rooted at binary node b (≥ 0 binary node, < 0 leaf)
 __global__ void k_wide_kids(const int32_t* __restrict__ bl, const int32_t* __restrict__ br,
-                            const float* __restrict__ bbox, int32_t nn, int32_t* kids, int32_t* nk) {
+                            const float* __restrict__ bbox, int32_t nn, int32_t* kids, int32_t* nk, int width) {
     for (int32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < nn; b += gridDim.x * blockDim.x) {
         int32_t k[8];
         int n = 2;
         k[0] = bl[b]; k[1] = br[b];
         for (int c = 2; c < 8; c++) k[c] = 0;
-        while (n < 8) {
+        while (n < width) {
             int best = -1;
             float ba = -1.0f;
             for (int i = 0; i < n; i++)
@@ -473,6 +473,46 @@ __global__ void k_write_nodes(const int32_t* __restrict__ order, int32_t m, cons
         float4* out = nodes + (size_t)me * 14;
         for (int q = 0; q < 14; q++) out[q] = make_float4(f[q * 4], f[q * 4 + 1], f[q * 4 + 2], f[q * 4 + 3]);
     }
+}
+// 4-wide nodes (7 float4: lower x, y, z and upper x, y, z planes of the 4
+// children, then their references).  The leaves keep the 8-wide tree's leaf
+// order, in which the primitive records are stored: a leaf kid's reference is
+// its primitive's typed slot there (inv8: primitive → 8-wide leaf slot).
+__global__ void k_write_nodes4(const int32_t* __restrict__ order, int32_t m, const int32_t* __restrict__ kids,
+                               const int32_t* __restrict__ nk, const int32_t* __restrict__ P,
+                               const float* __restrict__ bbox, const float* __restrict__ box,
+                               const int32_t* __restrict__ idx, const int32_t* __restrict__ inv8,
+                               const int32_t* __restrict__ scans, int32_t n, int64_t e0, int64_t e1, int64_t e2,
+                               float4* nodes4) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        int32_t b = order[i], me = P[b];
+        float f[28];
+        for (int c = 0; c < 4; c++) {
+            int32_t k = c < nk[b] ? kids[(size_t)b * 8 + c] : INT32_MIN;
+            uint32_t ref;
+            const float* cb = nullptr;
+            if (c >= nk[b]) {
+                ref = RT_EMPTY_REF;
+            } else if (k >= 0) {
+                ref = (uint32_t)P[k]; cb = bbox + (size_t)k * 6;
+            } else {
+                int32_t prim = idx[-k - 1], slot = inv8[prim];
+                uint32_t t = prim < e0 ? RT_PRIM_TRI : prim < e1 ? RT_PRIM_QUAD : prim < e2 ? RT_PRIM_SPHERE : RT_PRIM_CONVEX;
+                ref = RT_LEAF_BIT | (t << 28) | (uint32_t)scans[(size_t)t * n + slot];
+                cb = box + (size_t)prim * 6;
+            }
+            for (int a = 0; a < 3; a++) {
+                f[a * 4 + c] = cb ? cb[a] : INFINITY;
+                f[12 + a * 4 + c] = cb ? cb[3 + a] : -INFINITY;
+            }
+            f[24 + c] = __uint_as_float(ref);
+        }
+        float4* out = nodes4 + (size_t)me * 7;
+        for (int q = 0; q < 7; q++) out[q] = make_float4(f[q * 4], f[q * 4 + 1], f[q * 4 + 2], f[q * 4 + 3]);
+    }
+}
+__global__ void k_invert(const int32_t* __restrict__ leaf_gid, int32_t n, int32_t* inv) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) inv[leaf_gid[i]] = i;
 }
 // leaf type of every slot: one flag array per type for the typed-slot scans
 __global__ void k_leaf_types(const int32_t* __restrict__ leaf_gid, int32_t n, int64_t e0, int64_t e1, int64_t e2,
@@ -593,11 +633,15 @@ static cudaError_t collapse_wide(const int32_t* bl, const int32_t* br, const flo
     ok(cudaMalloc(&leaf_gid, (size_t)n * 4)); ok(cudaMalloc(&flags, (size_t)n * 16)); ok(cudaMalloc(&scans, (size_t)n * 16));
     ok(cudaMalloc(&fail, 4));
     int grid = sms * 8;
-    std::vector<int32_t> lvl_off{0, 1};
-    if (e == cudaSuccess) {
-        k_wide_kids<<<grid, 256, 0, st>>>(bl, br, bbox, nn, kids, nk);
+    std::vector<int32_t> lvl_off;
+    // the wide nodes of one width: each binary node's opening, the wide roots
+    // level by level (in `order`), subtree sizes bottom-up and preorder indices
+    // top-down; returns the node count (0 on an error) and the depth in *depth
+    auto plan = [&](int width, int32_t* depth) -> int32_t {
+        lvl_off.assign({0, 1});
+        if (e != cudaSuccess) return 0;
+        k_wide_kids<<<grid, 256, 0, st>>>(bl, br, bbox, nn, kids, nk, width);
         ok(cudaMemcpyAsync(order, &root, 4, cudaMemcpyHostToDevice, st));
-        // the wide roots, level by level, in `order`
         while (e == cudaSuccess) {
             int32_t off = lvl_off[lvl_off.size() - 2], m = lvl_off.back() - off;
             k_count_inner<<<std::max(1, std::min((m + 255) / 256, grid)), 256, 0, st>>>(order + off, m, kids, nk, cnt);
@@ -613,9 +657,8 @@ static cudaError_t collapse_wide(const int32_t* bl, const int32_t* br, const flo
                                                                                    order + lvl_off.back());
             lvl_off.push_back(lvl_off.back() + nxt);
         }
-    }
-    const int nlev = (int)lvl_off.size() - 1;
-    if (e == cudaSuccess) {
+        const int nlev = (int)lvl_off.size() - 1;
+        if (e != cudaSuccess) return 0;
         for (int l = nlev - 1; l >= 0; l--) {
             int32_t m = lvl_off[l + 1] - lvl_off[l];
             k_subtree_sizes<<<std::max(1, std::min((m + 255) / 256, grid)), 256, 0, st>>>(order + lvl_off[l], m, kids,
@@ -632,9 +675,10 @@ static cudaError_t collapse_wide(const int32_t* bl, const int32_t* br, const flo
         ok(cudaMemcpyAsync(&total, S + root, 4, cudaMemcpyDeviceToHost, st));
         ok(cudaStreamSynchronize(st));
         if (e == cudaSuccess && total != lvl_off.back()) e = cudaErrorUnknown;   // every wide root counted once
-        W->n_nodes = total;
-        W->max_depth = nlev - 1;
-    }
+        *depth = nlev - 1;
+        return e == cudaSuccess ? total : 0;
+    };
+    if (e == cudaSuccess) W->n_nodes = plan(8, &W->max_depth);
     if (e == cudaSuccess) {
         ok(cudaMalloc(&W->nodes, (size_t)W->n_nodes * 14 * 16));
         ok(cudaMalloc(&W->qnodes, (size_t)W->n_nodes * 8 * 16));
@@ -657,12 +701,28 @@ static cudaError_t collapse_wide(const int32_t* bl, const int32_t* br, const flo
         ok(cudaGetLastError());
         if (e == cudaSuccess && hfail) { cudaFree(W->qnodes); W->qnodes = nullptr; }
     }
+    // the 4-wide tree over the same binary tree (RT_NODES_WIDE4), its leaves
+    // referring to the primitive records in the 8-wide leaf order
+    if (e == cudaSuccess) {
+        int32_t* inv8 = cnt;                         // n + 1 ≥ n entries, free now
+        W->n_nodes4 = plan(4, &W->max_depth4);
+        if (e == cudaSuccess) ok(cudaMalloc(&W->nodes4, (size_t)W->n_nodes4 * 7 * 16));
+        if (e == cudaSuccess) {
+            k_invert<<<grid, 256, 0, st>>>(leaf_gid, n, inv8);
+            int32_t m = lvl_off.back();
+            k_write_nodes4<<<std::max(1, std::min((m + 127) / 128, grid)), 128, 0, st>>>(
+                order, m, kids, nk, P, bbox, box, idx, inv8, scans, n, W->type_end[0], W->type_end[1], W->type_end[2],
+                W->nodes4);
+            ok(cudaStreamSynchronize(st));
+            ok(cudaGetLastError());
+        }
+    }
     void* all[] = {kids, nk, order, cnt, pos, S, L, P, LB, leaf_gid, flags, scans, fail, tmp};
     for (void* p : all) if (p) cudaFree(p);
     if (e != cudaSuccess) {
-        void* outs[] = {W->nodes, W->qnodes, W->export_ch};
+        void* outs[] = {W->nodes, W->qnodes, W->export_ch, W->nodes4};
         for (void* p : outs) if (p) cudaFree(p);
-        W->nodes = W->qnodes = nullptr;
+        W->nodes = W->qnodes = W->nodes4 = nullptr;
         W->export_ch = nullptr;
     }
     return e;

@@ -108,6 +108,9 @@ struct DevScene {
     // the same nodes with 8-bit child boxes, 8 float4 each (see encode_qnode),
     // and which copy the traversal reads (RT_NODES_*)
     const float4* qnodes;
+    // 4-wide nodes of the same binary tree, 7 float4 each (lower x, y, z and
+    // upper x, y, z planes of 4 children, then their references)
+    const float4* nodes4;
     int node_format;
     const float4* tri;
     const float4* tri_n;

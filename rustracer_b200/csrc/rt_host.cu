@@ -582,6 +582,7 @@ struct RtScene {
     int32_t max_depth = 0;
     int stack_cap_built = 0;          // traversal stack entries the spill columns hold
     bool qnodes_ok = false;           // the quantised node copy exists (extents within 255·2^60)
+    bool wide4_ok = false;            // the 4-wide node copy exists (trees built on the device)
     std::vector<DevLight> h_lights;   // host copy of the NEE light list (photon emitters from lights)
     std::vector<float> h_emission;    // per material: RGB emission of a light material (3 floats)
     float photon_stage_ms[3] = {0, 0, 0};   // last photon build: trace, compaction, tree
@@ -1030,7 +1031,7 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
             int brc = rth::gpu_build_binary(bx.data(), (int32_t)n, nullptr, nullptr, nullptr, nullptr, &root, s->sms,
                                             s->stream, &W);
             if (brc) return bail(fail(s, RT_ERR_CUDA, std::string("device BVH build: ") + cudaGetErrorString((cudaError_t)brc)));
-            void* owned_ptrs[] = {W.nodes, W.qnodes, W.export_ch};
+            void* owned_ptrs[] = {W.nodes, W.qnodes, W.export_ch, W.nodes4};
             for (void* p : owned_ptrs) if (p) s->owned.push_back(DevBuf{p, 0});
             B.max_depth = W.max_depth;
         } else {
@@ -1045,6 +1046,8 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
         // traversal thread (grid ≤ SMs × RT_TRACE_MINB blocks)
         if (B.max_depth > 4096) return bail(fail(s, RT_ERR_CAPACITY, "BVH deeper than 4096 levels"));
         s->stack_cap_built = 7 * (B.max_depth + 1) + 8;
+        // the 4-wide tree is deeper; a visit there pushes at most 3 entries
+        if (dev_wide) s->stack_cap_built = std::max(s->stack_cap_built, 3 * (W.max_depth4 + 1) + 8);
         s->S.stack_cap = s->stack_cap_built;
         s->S.stack_ring = RT_SHORT_STACK;
         size_t spill_entries = (size_t)s->stack_cap_built;   // also room for a ring shrunk by rt_set_tuning
@@ -1208,6 +1211,8 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
             s->S.nodes = W.nodes;
             s->S.qnodes = W.qnodes;
             s->qnodes_ok = W.qnodes != nullptr;
+            s->S.nodes4 = W.nodes4;
+            s->wide4_ok = W.nodes4 != nullptr;
             s->S.node_format = RT_NODES_FULL;
         } else if ((rc = upload(s, gnodes.data(), gnodes.size(), &s->S.nodes))) {
             return bail(rc);
@@ -2503,10 +2508,12 @@ extern "C" int32_t rt_set_tuning(RtScene* s, const RtTuning* t) {
         return fail(s, RT_ERR_INVALID, "trace_blocks_per_sm must be in 0..8, shade_blocks_per_sm in 0..32");
     if (t->stack_ring != 0 && (t->stack_ring > RT_SHORT_STACK || (t->stack_ring & (t->stack_ring - 1)) != 0))
         return fail(s, RT_ERR_INVALID, "stack_ring must be 0 or a power of two up to " + std::to_string(RT_SHORT_STACK));
-    if (t->node_format != RT_NODES_QUANTISED && t->node_format != RT_NODES_FULL)
-        return fail(s, RT_ERR_INVALID, "node_format must be RT_NODES_QUANTISED or RT_NODES_FULL");
+    if (t->node_format != RT_NODES_QUANTISED && t->node_format != RT_NODES_FULL && t->node_format != RT_NODES_WIDE4)
+        return fail(s, RT_ERR_INVALID, "node_format must be RT_NODES_FULL, RT_NODES_QUANTISED or RT_NODES_WIDE4");
     if (t->node_format == RT_NODES_QUANTISED && !s->qnodes_ok && !s->empty)
         return fail(s, RT_ERR_INVALID, "the scene's extents exceed the quantised node layout");
+    if (t->node_format == RT_NODES_WIDE4 && !s->wide4_ok && !s->empty)
+        return fail(s, RT_ERR_INVALID, "4-wide nodes exist for trees built on the device only");
     if (t->stack_limit != 0 && (int64_t)t->stack_limit > s->stack_cap_built)
         return fail(s, RT_ERR_INVALID, "stack_limit must be 0 or at most " + std::to_string(s->stack_cap_built) +
                                            " (the entries the scene's stack columns hold)");
@@ -2519,7 +2526,9 @@ extern "C" int32_t rt_set_tuning(RtScene* s, const RtTuning* t) {
     s->max_iterations = t->max_iterations;
     s->S.stack_cap = t->stack_limit ? (int)t->stack_limit : s->stack_cap_built;
     s->S.stack_ring = t->stack_ring ? (int)t->stack_ring : RT_SHORT_STACK;
-    s->S.node_format = (s->qnodes_ok && t->node_format == RT_NODES_QUANTISED) ? RT_NODES_QUANTISED : RT_NODES_FULL;
+    s->S.node_format = (s->qnodes_ok && t->node_format == RT_NODES_QUANTISED) ? RT_NODES_QUANTISED
+                     : (s->wide4_ok && t->node_format == RT_NODES_WIDE4)    ? RT_NODES_WIDE4
+                                                                            : RT_NODES_FULL;
     s->graph_mode = t->graph != 0;
     return RT_OK;
 }

@@ -242,6 +242,9 @@ struct WideOut {
     int64_t n_nodes = 0;
     int32_t max_depth = 0;
     int32_t* leaf_gids_h = nullptr;   // host, n entries
+    float4* nodes4 = nullptr;     // 4-wide nodes of the same binary tree, 7 float4 per node
+    int64_t n_nodes4 = 0;
+    int32_t max_depth4 = 0;
 };
 // binary tree on the device, then (wide == null) its arrays copied to the host
 // or (wide != null) the device collapse into *wide

@@ -351,17 +351,88 @@ __device__ __noinline__ uint32_t qnode_test_general(const DevScene& S, uint32_t 
     return mask & (meta >> 24);
 }
 
-// the node test and the child-reference words of node `ni` in either copy
-template <bool QN>
+// ── 4-wide nodes (7 float4: lower x, y, z, upper x, y, z, references) ──────
+__device__ __noinline__ uint32_t node4_test_general(const DevScene& S, uint32_t ni, const RayC& R, float tmin,
+                                                    float tmax, float* tn);
+
+RT_D uint32_t node4_test(const DevScene& S, uint32_t ni, const RayC& R, float tmin, float tmax, float tn[8],
+                         uint32_t ch[8]) {
+    const float4* N = S.nodes4 + (size_t)ni * 7;
+    float4 c0 = __ldg(N + 6);
+    ch[0] = __float_as_uint(c0.x); ch[1] = __float_as_uint(c0.y);
+    ch[2] = __float_as_uint(c0.z); ch[3] = __float_as_uint(c0.w);
+    if (!R.general) {
+        // the near planes of an axis are the lower ones for a positive direction
+        // (R.nx / 2 is 0 or 3, R.ny / 2 is 1 or 4, R.nz / 2 is 2 or 5)
+        float4 q[6];
+        q[0] = __ldg(N + R.nx / 2); q[1] = __ldg(N + R.ny / 2); q[2] = __ldg(N + R.nz / 2);
+        q[3] = __ldg(N + 3 - R.nx / 2); q[4] = __ldg(N + 5 - R.ny / 2); q[5] = __ldg(N + 7 - R.nz / 2);
+        const float* f = reinterpret_cast<const float*>(q);
+        uint32_t mask = 0;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            float nx = (f[0 + c] - R.o.x) * R.inv.x, fx = (f[12 + c] - R.o.x) * R.invf.x;
+            float ny = (f[4 + c] - R.o.y) * R.inv.y, fy = (f[16 + c] - R.o.y) * R.invf.y;
+            float nz = (f[8 + c] - R.o.z) * R.inv.z, fz = (f[20 + c] - R.o.z) * R.invf.z;
+            float t0 = fmax3f(fmaxf(tmin, nx), ny, nz);
+            float t1 = fmin3f(fminf(tmax, fx), fy, fz);
+            tn[c] = t0;
+            if (t0 <= t1) mask |= 1u << c;     // empty slots hold inverted boxes
+        }
+        return mask;
+    }
+    float tg[4];
+    uint32_t mask = node4_test_general(S, ni, R, tmin, tmax, tg);
+#pragma unroll
+    for (int c = 0; c < 4; c++) tn[c] = tg[c];
+    return mask;
+}
+
+__device__ __noinline__ uint32_t node4_test_general(const DevScene& S, uint32_t ni, const RayC& R, float tmin,
+                                                    float tmax, float* tn) {
+    const float4* N = S.nodes4 + (size_t)ni * 7;
+    float4 q[7];
+#pragma unroll
+    for (int i = 0; i < 7; i++) q[i] = __ldg(N + i);
+    const float* f = reinterpret_cast<const float*>(q);
+    const uint32_t* ch = reinterpret_cast<const uint32_t*>(f + 24);
+    uint32_t mask = 0;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        float dax = (f[0 + c] - R.o.x) * R.inv.x, dbx = (f[12 + c] - R.o.x) * R.inv.x;
+        float day = (f[4 + c] - R.o.y) * R.inv.y, dby = (f[16 + c] - R.o.y) * R.inv.y;
+        float daz = (f[8 + c] - R.o.z) * R.inv.z, dbz = (f[20 + c] - R.o.z) * R.inv.z;
+        float lx = fminf(dax, dbx), hx = fmaxf(dax, dbx);
+        float ly = fminf(day, dby), hy = fmaxf(day, dby);
+        float lz = fminf(daz, dbz), hz = fmaxf(daz, dbz);
+        if (isnan(dax) || isnan(dbx)) { lx = -INFINITY; hx = INFINITY; }
+        if (isnan(day) || isnan(dby)) { ly = -INFINITY; hy = INFINITY; }
+        if (isnan(daz) || isnan(dbz)) { lz = -INFINITY; hz = INFINITY; }
+        float t0 = fmaxf(fmaxf(fmaxf(tmin, lx), ly), lz);
+        float t1 = fminf(fminf(fminf(tmax, hx), hy), hz);
+        float t1w = t1 + fabsf(t1) * SLAB_WIDEN;
+        tn[c] = t0;
+        if (t0 <= t1w && ch[c] != RT_EMPTY_REF) mask |= 1u << c;
+    }
+    return mask;
+}
+
+// the node test and the child-reference words of node `ni` in the layout NF
+// (RT_NODES_FULL, RT_NODES_QUANTISED, RT_NODES_WIDE4), and its width
+template <int NF>
 RT_D uint32_t node_test_any(const DevScene& S, uint32_t ni, const RayC& R, float tmin, float tmax, float tn[8],
                             uint32_t ch[8]) {
-    return QN ? qnode_test(S, ni, R, tmin, tmax, tn, ch) : node_test(S, ni, R, tmin, tmax, tn, ch);
+    if constexpr (NF == RT_NODES_QUANTISED) return qnode_test(S, ni, R, tmin, tmax, tn, ch);
+    else if constexpr (NF == RT_NODES_WIDE4) return node4_test(S, ni, R, tmin, tmax, tn, ch);
+    else return node_test(S, ni, R, tmin, tmax, tn, ch);
 }
-template <bool QN>
+template <int NF>
 RT_D const uint32_t* node_refs(const DevScene& S, uint32_t ni) {
-    return QN ? reinterpret_cast<const uint32_t*>(S.qnodes + (size_t)ni * 8 + 4)
-              : reinterpret_cast<const uint32_t*>(S.nodes + (size_t)ni * 14 + 12);
+    if constexpr (NF == RT_NODES_QUANTISED) return reinterpret_cast<const uint32_t*>(S.qnodes + (size_t)ni * 8 + 4);
+    else if constexpr (NF == RT_NODES_WIDE4) return reinterpret_cast<const uint32_t*>(S.nodes4 + (size_t)ni * 7 + 6);
+    else return reinterpret_cast<const uint32_t*>(S.nodes + (size_t)ni * 14 + 12);
 }
+template <int NF> constexpr int node_width() { return NF == RT_NODES_WIDE4 ? 4 : 8; }
 
 }  // namespace
 
@@ -418,20 +489,21 @@ RT_D TStack make_stack(const DevScene& S, uint32_t* ring_base) {
 // intersects hit leaves in slot order, then continues with the nearest hit inner
 // child (sorted by a 19-comparator network on packed (t | slot) keys) and pushes
 // the others far → near.  Returns false when the traversal is finished.
-template <bool ANA, bool QN>
+template <bool ANA, int NF>
 RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, Best& best,
                        uint32_t& node, TStack& stk, bool& ok) {
+    constexpr int WN = node_width<NF>();
     float tn[8];
     uint32_t ch[8];
     // the closest hit so far bounds the boxes; widened like every exit distance
     float cwin = best.t + fabsf(best.t) * SLAB_WIDEN;
-    uint32_t mask = node_test_any<QN>(S, node, R, tmin, R.general ? best.t : cwin, tn, ch);
+    uint32_t mask = node_test_any<NF>(S, node, R, tmin, R.general ? best.t : cwin, tn, ch);
     uint32_t leaves = 0;
 #pragma unroll
-    for (int c = 0; c < 8; c++) leaves |= ((ch[c] & RT_LEAF_BIT) ? 1u : 0u) << c;
+    for (int c = 0; c < WN; c++) leaves |= ((ch[c] & RT_LEAF_BIT) ? 1u : 0u) << c;
     leaves &= mask;
     if (leaves) {
-        const uint32_t* refs = node_refs<QN>(S, node);
+        const uint32_t* refs = node_refs<NF>(S, node);
 #pragma unroll 1
         while (leaves) {
             int c = __ffs(leaves) - 1;
@@ -443,7 +515,7 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
     uint32_t k[8];
     int n = 0;
 #pragma unroll
-    for (int c = 0; c < 8; c++) {
+    for (int c = 0; c < WN; c++) {
         bool inner = ((mask >> c) & 1u) && !(ch[c] & RT_LEAF_BIT) && tn[c] <= cw;
         k[c] = inner ? ((__float_as_uint(fmaxf(tn[c], 0.0f)) & ~7u) | (uint32_t)c) : 0xFFFFFFFFu;
         n += inner ? 1 : 0;
@@ -457,33 +529,39 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
         // two inner children: continue with the nearer, push the farther
         uint32_t a = 0xFFFFFFFFu, b = 0xFFFFFFFFu;
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
+        for (int c = 0; c < WN; c++) {
             if (k[c] == 0xFFFFFFFFu) continue;
             if (a == 0xFFFFFFFFu) a = k[c]; else b = k[c];
         }
         uint32_t lo = min(a, b), hi = max(a, b);
         if (!stk.room(1)) { ok = false; return false; }
-        const uint32_t* refs = node_refs<QN>(S, node);
+        const uint32_t* refs = node_refs<NF>(S, node);
         stk.push(__ldg(refs + (hi & 7u)));
         node = __ldg(refs + (lo & 7u));
     } else if (n > 2) {
-        CAS(0, 1) CAS(2, 3) CAS(4, 5) CAS(6, 7)
-        CAS(0, 2) CAS(1, 3) CAS(4, 6) CAS(5, 7)
-        CAS(1, 2) CAS(5, 6) CAS(0, 4) CAS(3, 7)
-        CAS(1, 5) CAS(2, 6)
-        CAS(1, 4) CAS(3, 6)
-        CAS(2, 4) CAS(3, 5)
-        CAS(3, 4)
+        if constexpr (WN == 4) {
+            CAS(0, 1) CAS(2, 3)
+            CAS(0, 2) CAS(1, 3)
+            CAS(1, 2)
+        } else {
+            CAS(0, 1) CAS(2, 3) CAS(4, 5) CAS(6, 7)
+            CAS(0, 2) CAS(1, 3) CAS(4, 6) CAS(5, 7)
+            CAS(1, 2) CAS(5, 6) CAS(0, 4) CAS(3, 7)
+            CAS(1, 5) CAS(2, 6)
+            CAS(1, 4) CAS(3, 6)
+            CAS(2, 4) CAS(3, 5)
+            CAS(3, 4)
+        }
         if (!stk.room(n - 1)) { ok = false; return false; }
-        const uint32_t* refs = node_refs<QN>(S, node);
+        const uint32_t* refs = node_refs<NF>(S, node);
 #pragma unroll
-        for (int j = 7; j >= 1; j--)
+        for (int j = WN - 1; j >= 1; j--)
             if (j < n) stk.push(__ldg(refs + (k[j] & 7u)));
         node = __ldg(refs + (k[0] & 7u));
     } else {
         uint32_t c = 0;
 #pragma unroll
-        for (int j = 0; j < 8; j++) if (k[j] != 0xFFFFFFFFu) c = j;
+        for (int j = 0; j < WN; j++) if (k[j] != 0xFFFFFFFFu) c = j;
         node = ch[c];
     }
     return true;
@@ -491,16 +569,17 @@ RT_D bool closest_step(const DevScene& S, const RayC& R, float3 d, float tmin, B
 
 // One node visit of the any-hit traversal (bvh.rs:487-530).  Returns false when
 // finished; *hit is set when a primitive was hit.
-template <bool ANA, bool QN>
+template <bool ANA, int NF>
 RT_D bool any_step(const DevScene& S, const RayC& R, float3 d, float tmin, float tmax,
                    uint32_t& node, TStack& stk, bool& hit, bool& ok) {
+    constexpr int WN = node_width<NF>();
     float tn[8];
     uint32_t ch[8];
     float tw = tmax + fabsf(tmax) * SLAB_WIDEN;
-    uint32_t mask = node_test_any<QN>(S, node, R, tmin, R.general ? tmax : tw, tn, ch);
+    uint32_t mask = node_test_any<NF>(S, node, R, tmin, R.general ? tmax : tw, tn, ch);
     uint32_t inner = 0, leaves = 0;
 #pragma unroll
-    for (int c = 0; c < 8; c++) {
+    for (int c = 0; c < WN; c++) {
         bool lf = ch[c] & RT_LEAF_BIT;
         leaves |= (lf ? 1u : 0u) << c;
         inner |= (lf ? 0u : 1u) << c;
@@ -508,7 +587,7 @@ RT_D bool any_step(const DevScene& S, const RayC& R, float3 d, float tmin, float
     leaves &= mask;
     inner &= mask;
     if (leaves) {
-        const uint32_t* refs = node_refs<QN>(S, node);
+        const uint32_t* refs = node_refs<NF>(S, node);
 #pragma unroll 1
         while (leaves) {
             int c = __ffs(leaves) - 1;
@@ -525,7 +604,7 @@ RT_D bool any_step(const DevScene& S, const RayC& R, float3 d, float tmin, float
     uint32_t rest = inner & (inner - 1);
     if (!stk.room(__popc(rest))) { ok = false; return false; }
 #pragma unroll
-    for (int c = 0; c < 8; c++)
+    for (int c = 0; c < WN; c++)
         if ((rest >> c) & 1u) stk.push(ch[c]);
     node = ch[first];
     return true;
@@ -557,7 +636,7 @@ RT_D bool nan_ray(float3 o, float3 d, float tmin, float tmax) {
 // MODE 0: wavefront extend (queue of path ids, rays in PathState, hits to PathState)
 // MODE 1: API (rays n×8 in memory, hits as int4)
 
-template <int MODE, bool ANA, bool QN>
+template <int MODE, bool ANA, int NF>
 __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevScene S, PathState P, const uint32_t* __restrict__ queue,
                                                             const float* __restrict__ rays, uint32_t n_api,
                                                             const uint32_t* count, uint32_t* next,
@@ -612,7 +691,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
         if (exhausted && __ballot_sync(FULLMASK, active) == 0) break;
         if (active) {
             bool lok = true;
-            bool more = rtk::closest_step<ANA, QN>(S, R, d, tmin, best, node, stk, lok);
+            bool more = rtk::closest_step<ANA, NF>(S, R, d, tmin, best, node, stk, lok);
             if (!lok) ok = false;
             if (!more) {
                 active = false;
@@ -634,7 +713,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_closest(DevSc
 // MODE 1: API any-hit (occluded flags)
 // MODE 2: wavefront shadow rays in a scene with media (an unoccluded ray scales
 //         its parked contribution by the media's transmittance)
-template <int MODE, bool ANA, bool QN>
+template <int MODE, bool ANA, int NF>
 __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene S, PendTargets T, const float4* __restrict__ sq,
                                                         const float* __restrict__ rays, uint32_t n_api,
                                                         const uint32_t* count, uint32_t* next,
@@ -684,7 +763,7 @@ __global__ void __launch_bounds__(RT_TRACE_BLOCK, RT_TRACE_MINB) k_any(DevScene 
         if (exhausted && __ballot_sync(FULLMASK, active) == 0) break;
         if (active) {
             bool lok = true;
-            bool more = rtk::any_step<ANA, QN>(S, R, d, tmin, tmax, node, stk, hit, lok);
+            bool more = rtk::any_step<ANA, NF>(S, R, d, tmin, tmax, node, stk, hit, lok);
             if (!lok) ok = false;
             if (!more) {
                 active = false;
@@ -775,13 +854,15 @@ int trace_grid(const DevScene& S, int dev_sms) {
 #define RT_TRACE_LAUNCH(K, MODE, ...)                                                                         \
     do {                                                                                                      \
         const int g_ = trace_grid(S, sms);                                                                    \
-        const bool q_ = S.node_format == RT_NODES_QUANTISED;                                                  \
+        const int f_ = S.node_format;                                                                        \
         if (S.n_analytic > 0) {                                                                               \
-            if (q_) K<MODE, true, true><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);                           \
-            else    K<MODE, true, false><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);                          \
+            if (f_ == RT_NODES_QUANTISED)  K<MODE, true, RT_NODES_QUANTISED><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__); \
+            else if (f_ == RT_NODES_WIDE4) K<MODE, true, RT_NODES_WIDE4><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);     \
+            else                           K<MODE, true, RT_NODES_FULL><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);      \
         } else {                                                                                              \
-            if (q_) K<MODE, false, true><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);                          \
-            else    K<MODE, false, false><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);                         \
+            if (f_ == RT_NODES_QUANTISED)  K<MODE, false, RT_NODES_QUANTISED><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__); \
+            else if (f_ == RT_NODES_WIDE4) K<MODE, false, RT_NODES_WIDE4><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);     \
+            else                           K<MODE, false, RT_NODES_FULL><<<g_, RT_TRACE_BLOCK, 0, st>>>(__VA_ARGS__);      \
         }                                                                                                     \
     } while (0)
 void launch_trace_closest_api(const DevScene& S, const float* rays, uint32_t n, int4* out, uint32_t* next, int* err,

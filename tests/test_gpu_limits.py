@@ -99,8 +99,9 @@ def test_iteration_bound_returns_timeout_and_the_scene_stays_usable():
 
 def test_node_layouts_give_identical_hits_and_images():
     """The quantised 128-byte nodes (8-bit child boxes rounded outward, a
-    conservative slab test) and the reference's 224-byte float nodes give the
-    same hits bit for bit, hence the same image; the oracle agrees."""
+    conservative slab test), the 4-wide 112-byte nodes over the same binary
+    tree (bvh.rs:10-14's other width) and the reference's 224-byte float nodes
+    give the same hits bit for bit, hence the same image; the oracle agrees."""
     sb, st = configs.icosphere_scene(env_w=64, env_h=32)
     g, o = GpuScene(sb), O.OracleScene(sb)
     assert g.get_tuning()["node_format"] == 0          # the full layout is the default
@@ -108,12 +109,26 @@ def test_node_layouts_give_identical_hits_and_images():
     q = g.trace_closest(r)
     qa = g.trace_any(r)
     _hits_equal(q[:8000], o.trace_closest(r[:8000]))
-    g.set_tuning(node_format=1)                        # quantised
-    _hits_equal(g.trace_closest(r), q)
-    assert np.array_equal(g.trace_any(r), qa)
     p = pass_params(64, 36, 0, 2, 1, 12, 4, 1.0, 3)
     cam = configs.make_camera((0.0, 0.45, 3.6), (0.0, -0.15, 0.0), vfov=40.0, aspect=64 / 36)
-    quant = g.render_pass(cam, p)
-    g.set_tuning(node_format=0)
     full = g.render_pass(cam, p)
-    assert np.array_equal(full.view(np.uint32), quant.view(np.uint32))
+    for fmt in (1, 2):                                 # quantised, 4-wide
+        g.set_tuning(node_format=fmt)
+        assert g.get_tuning()["node_format"] == fmt
+        _hits_equal(g.trace_closest(r), q)
+        assert np.array_equal(g.trace_any(r), qa)
+        assert np.array_equal(g.render_pass(cam, p).view(np.uint32), full.view(np.uint32))
+    # the 4-wide tree through a two-slot stack ring (every traversal spills)
+    g.set_tuning(node_format=2, stack_ring=2)
+    _hits_equal(g.trace_closest(r), q)
+    g.set_tuning()
+
+
+def test_wide4_nodes_need_a_device_built_tree():
+    from rustracer_b200 import abi
+    sb, _ = configs.box_scene(width=32, height=32)
+    sb.bvh_builder = abi.RT_BVH_HOST
+    g = GpuScene(sb)
+    with pytest.raises(RtError):
+        g.set_tuning(node_format=2)
+    assert g.get_tuning()["node_format"] == 0
