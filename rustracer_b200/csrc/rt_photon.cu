@@ -888,6 +888,9 @@ RT_D float3 warp_gather(const Map& M, float3 p, float3 n, WarpScratch& W, uint32
         sv[r] = __shfl_sync(0xFFFFFFFFu, st, r);
     }
     uint32_t cnt = 0;
+    // the radius-r_max sum, gathered in the same pass: the estimate whenever
+    // fewer than k photons are in range (and always in radius mode)
+    float3 acc0 = mk(0.f, 0.f, 0.f);
     for (uint32_t base = 0; base < T; base += 32) {
         uint32_t f = base + lane;
         bool c = false;
@@ -901,8 +904,11 @@ RT_D float3 warp_gather(const Map& M, float3 p, float3 n, WarpScratch& W, uint32
             for (int r = 1; r < 8; r++)
                 if (ex[r] <= f) { e0 = ex[r]; s0 = sv[r]; }
             k = s0 + (f - e0);
-            d2 = pdist2(__ldg(M.pos + k), p);
-            c = d2 < M.r2 && pdot(__ldg(M.nor + k), n) > 0.0f;
+            // position, normal and power in one round trip (the map is L2-resident)
+            float4 q = __ldg(M.pos + k), nv = __ldg(M.nor + k), pw = __ldg(M.pow + k);
+            d2 = pdist2(q, p);
+            c = d2 < M.r2 && pdot(nv, n) > 0.0f;
+            if (c) acc0 = acc0 + mk(pw.x, pw.y, pw.z) * (1.0f - d2 / M.r2);
         }
         uint32_t m = __ballot_sync(0xFFFFFFFFu, c);
         uint32_t slot = cnt + __popc(m & lt);
@@ -912,10 +918,12 @@ RT_D float3 warp_gather(const Map& M, float3 p, float3 n, WarpScratch& W, uint32
     __syncwarp();
     if (cnt > PH_CAND_CAP) return warp_irradiance(M, p, n, hist, sel);
     float r2 = M.r2;
-    if (M.knn_k > 0 && cnt >= M.knn_k) {
-        r2 = warp_radix_select(W.d2, cnt, M.knn_k, W.hist);
-        if (!(r2 > 0.0f)) return mk(0.f, 0.f, 0.f);
+    if (!(M.knn_k > 0 && cnt >= M.knn_k)) {
+        float sc = 2.0f / (PI_F * PI_F * r2);
+        return mk(warp_sum(acc0.x) * sc, warp_sum(acc0.y) * sc, warp_sum(acc0.z) * sc);
     }
+    r2 = warp_radix_select(W.d2, cnt, M.knn_k, W.hist);
+    if (!(r2 > 0.0f)) return mk(0.f, 0.f, 0.f);
     float3 acc = mk(0.f, 0.f, 0.f);
     for (uint32_t j = lane; j < cnt; j += 32) {
         float d2 = W.d2[j];
@@ -1005,9 +1013,13 @@ __global__ void __launch_bounds__(RT_SHADE_BLOCK) k_photon_gather_paths(rtph::Ma
     uint32_t n = *count;
     uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    // one warp per request (its cells' photons are few, and coalesced)
+    // one warp per request (its cells' photons are few, and coalesced); the
+    // next request is loaded while this one is gathered
+    float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
+    if (gw < n) { na = gq[(size_t)gw * 2]; nb = gq[(size_t)gw * 2 + 1]; }
     for (uint32_t i = gw; i < n; i += nw) {
-        float4 qa = gq[(size_t)i * 2], qb = gq[(size_t)i * 2 + 1];
+        float4 qa = na, qb = nb;
+        if (i + nw < n) { na = gq[(size_t)(i + nw) * 2]; nb = gq[(size_t)(i + nw) * 2 + 1]; }
         float3 r = rtph::warp_gather(M, mk(qa.x, qa.y, qa.z), mk(qb.x, qb.y, qb.z), ws[w], hist[w], sel[w]);
         if (lane == 0) {
             uint32_t tag = __float_as_uint(qa.w);
