@@ -686,20 +686,22 @@ RT_D Surf surface(const DevScene& S, float4 hv, float3 o, float3 d) {
 // instantiation leaves that code out so env-map and plain scenes keep their
 // registers.
 // GUIDE (diffuse class only): bounces drawn from the guide mixture.
-// Resident blocks per SM the shading kernels are compiled for.  Diffuse
-// shading (the busiest class) at 8 blocks = 64 registers, with some spilling,
-// measured fastest: icosphere shade 26.3 ms against 26.4 at 127 registers and
-// 26.5 at 80, box frame 1.285 ms against 1.30 and 1.33.  The other classes at
-// 4 (≤ 128 registers): an explicit bound of 1 lets ptxas take more registers
-// than the plain heuristic and cost 15 % of the shading time.
-#ifndef RT_SHADE_DIFFUSE_MINB
-#define RT_SHADE_DIFFUSE_MINB 8
-#endif
+// Resident blocks per SM the shading kernels are compiled for: 8 (64
+// registers).  Diffuse shading, the busiest class, spills some there and still
+// measured fastest (icosphere shade 26.3 ms against 26.4 at 127 registers and
+// 26.5 at 80; box frame 1.285 ms against 1.30 and 1.33); the conductor and
+// miss classes fit without spilling (icosphere shade 24.5 ms against 26.1 at
+// 4 blocks).  PBR, which would spill half a kilobyte per thread at 64, stays at
+// 4 (≤ 128 registers).  An explicit bound of 1 lets ptxas take more registers
+// than its plain heuristic and cost 15 % of the shading time.
 #ifndef RT_SHADE_MINB
-#define RT_SHADE_MINB 4
+#define RT_SHADE_MINB 8
+#endif
+#ifndef RT_SHADE_PBR_MINB
+#define RT_SHADE_PBR_MINB 4
 #endif
 template <int CLS, bool SKY, bool GUIDE>
-__global__ void __launch_bounds__(RT_SHADE_BLOCK, CLS == CLS_DIFFUSE ? RT_SHADE_DIFFUSE_MINB : RT_SHADE_MINB)
+__global__ void __launch_bounds__(RT_SHADE_BLOCK, CLS == CLS_PBR ? RT_SHADE_PBR_MINB : RT_SHADE_MINB)
 k_shade(DevScene S, PathState A, PathState B, PathState Rt,
                                                           const RenderLaunch* __restrict__ Rp,
                                                           const uint32_t* __restrict__ qin, const uint32_t* cin,
