@@ -417,7 +417,9 @@ def secondary(kind, args):
     from rustracer_b200.renderer import GpuScene, pass_params
     if kind == "box":
         sb, st = configs.box_scene()
-        steps, warm = args.steps, args.warmup
+        # a frame is ~1.3 ms: at least 400 timed frames (~0.5 s), so the clock
+        # sampler (every 200 ms) sees the timed region
+        steps, warm = max(args.steps, 400), args.warmup
     else:
         sb, st = configs.gem_scene()
         steps, warm = max(1, min(args.steps, 3)), args.warmup
@@ -462,7 +464,7 @@ def secondary(kind, args):
     clk = clocks.stop()
     per_step = w * h * spp
     e2e_s = []
-    for k in range(max(2, min(steps, 3))):
+    for k in range(50 if kind == "box" else max(2, min(steps, 3))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         step(1000 + k, host)
