@@ -595,7 +595,7 @@ typedef struct RtTuning {
      * rt_get_tuning reports the stack entries in force (7 per tree level). */
     uint32_t max_iterations;       /* 0 or ≥ 1 */
     uint32_t stack_limit;          /* 0 or 1 .. the built-in capacity */
-    /* Traversal stack entries kept in shared memory per thread before the
+    /* Traversal stack entries kept in a per-thread ring (local memory) before the
      * rest spills to global memory (0: 16; else a power of two ≤ 16).  The
      * results never depend on it; small rings make every traversal take the
      * spill path. */

@@ -1,6 +1,6 @@
 """Limits of the device loops and the traversal stack, and the node layouts.
 
-The traversal stack keeps its newest entries in a shared-memory ring and
+The traversal stack keeps its newest entries in a per-thread ring and
 spills deeper ones to global memory, so no scene's tree overflows it (the
 reference keeps 128 entries inline and spills to a heap Vec, bvh.rs:229-239).
 rt_set_tuning can shrink the ring, which sends every traversal through the
