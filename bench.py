@@ -445,6 +445,13 @@ def secondary(kind, args):
         stt = scene.last_stats()
         return stt["ms"] + ph_ms, ph_ms, stt
 
+    tuning = None
+    if not args.no_autotune:
+        # the library's launch autotuner on a probe of this frame, as for the headline
+        from rustracer_b200 import autotune
+        if photons:
+            scene.photon_build(st["photon_params"](seed=0))
+        tuning, _ = autotune.autotune(scene, cam, pass_params(w, h, 0, spp, strata, depth, hero, 1.0, 7))
     for k in range(warm):
         step(k, outs)
     flush.fill_(1)
@@ -477,6 +484,7 @@ def secondary(kind, args):
                 "h2d_bytes_per_step": 136, "d2h_bytes_per_step": h * w * (3 + 3) * 4 + h * w * 4},
         "rays": {"extension": int(ext), "shadow": int(sh), "rays_per_s": (ext + sh) / (sum(ms) / 1000.0)},
         "l2": "256 MB buffer written between timed steps",
+        "launch_tuning": tuning or "built-in",
     }
     if photons:
         line["photon_map"] = {"emitted": st["photons"], "stored_mean": int(np.mean(stored)),
