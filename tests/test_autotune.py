@@ -42,3 +42,24 @@ def test_probe_stays_within_its_budget():
     p = autotune.probe_params(pass_params(1920, 1080, 0, 256))
     assert p.n_samples == 9 and p.width == 1920 and 1920 * 1080 * (p.n_samples - 1) < autotune.PROBE_SAMPLES
     assert autotune.probe_params(pass_params(128, 128, 0, 4)).n_samples == 4
+
+
+def test_autotune_skips_layouts_the_scene_lacks():
+    """A scene whose tree was built on the host has no 4-wide nodes:
+    rt_set_tuning refuses RT_NODES_WIDE4 and the tuner passes those
+    candidates over instead of failing."""
+    from rustracer_b200 import abi
+    from rustracer_b200.renderer import RtError
+
+    autotune.clear_cache()
+    g = FakeScene()
+
+    def timer(t):
+        if t["node_format"] == abi.RT_NODES_WIDE4:
+            raise RtError(1, "4-wide nodes exist for trees built on the device only")
+        g.set_tuning(**t)
+        return 10.0 - t["node_format"] - t["shade_blocks_per_sm"] / 100.0
+    best, table = autotune.autotune(g, None, pass_params(64, 64), timer=timer, repeats=1)
+    assert best["node_format"] == abi.RT_NODES_QUANTISED and best["shade_blocks_per_sm"] == 16
+    assert all(t["node_format"] != abi.RT_NODES_WIDE4 for _, t in table)
+    assert len(table) == len(autotune.candidates()) * 2 // 3
