@@ -132,3 +132,24 @@ def test_wide4_nodes_need_a_device_built_tree():
     with pytest.raises(RtError):
         g.set_tuning(node_format=2)
     assert g.get_tuning()["node_format"] == 0
+
+
+@pytest.mark.parametrize("name", ["media_box", "gem_room"])
+def test_node_layouts_render_identically_with_media_and_solids(name):
+    """The traversal instantiations with analytic solids (the gem room's
+    [[gems]] stones and shapes) and the media shadow mode read every layout
+    the same way: renders are bit-identical."""
+    if name == "media_box":
+        sb, st = configs.media_box_scene(width=48, height=48)
+    else:
+        sb, st = configs.gem_room_scene(48, 32)
+    g = GpuScene(sb)
+    p = pass_params(48, 48 if name == "media_box" else 32, 0, 4, 2, 12, 4, 1.0, 17)
+    ref = g.render_pass(st["camera"], p)
+    for fmt in (1, 2):
+        try:
+            g.set_tuning(node_format=fmt)
+        except RtError:
+            continue                                   # a layout this scene lacks
+        assert np.array_equal(g.render_pass(st["camera"], p).view(np.uint32), ref.view(np.uint32)), fmt
+    g.set_tuning()
