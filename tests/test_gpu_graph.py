@@ -122,3 +122,22 @@ def test_async_errors():
     g.render_accumulate_async(st["camera"], pass_params(64, 64, 0, 2, 1, 8, 4, 1.0, 9), outs)
     g.sync()
     assert int(outs[2].sum()) == 64 * 64 * 2
+
+
+def test_graph_with_the_frozen_guide_is_bit_identical():
+    """The guide's encode and inference kernels inside the captured iterations:
+    with the network frozen (RT_GUIDE_SAMPLE) a render is deterministic, and
+    the graph form gives the host-driven loop's image bit for bit."""
+    from rustracer_b200 import abi
+    from rustracer_b200.renderer import guide_params
+    sb, st = configs.guided_box_scene(width=64, height=48, gem=False)
+    g = GpuScene(sb)
+    g.guide_init(guide_params(batch=4096, steps_per_pass=2, seed=5))
+    g.guide_mode(abi.RT_GUIDE_TRAIN)
+    g.render_accumulate(st["camera"], pass_params(64, 48, 0, 4, 2, 12, 4, 1.0, 3))
+    g.guide_mode(abi.RT_GUIDE_SAMPLE)
+    p = pass_params(64, 48, 100, 8, 2, 12, 4, 1.0, 9)
+    ref = g.render_pass(st["camera"], p)
+    g.set_tuning(graph=1)
+    _same(g.render_pass(st["camera"], p), ref)
+    _same(g.render_pass(st["camera"], p), ref)      # replayed
