@@ -72,3 +72,22 @@ def test_gpu_gem_scene_matches_oracle():
     oi = o.render_pass(st["camera"], pp)
     assert np.isfinite(gi).all()
     assert_tiles_agree(gi, oi)
+
+
+def test_gem_config_band_at_its_stated_size():
+    """The gem workload at its stated frame, 1280×720, depth 32, hero 4, with
+    its 2M-photon caustic map (each side builds its own from the same seed):
+    a 32-row band through the stone and its caustic, tiles within 3 SE."""
+    sb, st = configs.gem_scene()
+    assert (st["width"], st["height"], st["max_depth"], st["hero"]) == (1280, 720, 32, 4)
+    g, o = GpuScene(sb), O.OracleScene(sb)
+    p = st["photon_params"](seed=1)
+    ng, no = g.photon_build(p), o.photon_build(p)
+    assert abs(ng - no) <= no // 100
+    pp = pass_params(1280, 720, 0, 32, 4, 32, 4, 1.0, 51)
+    gi = g.render_pass(st["camera"], pp)
+    pp.seed = 52
+    oi = o.render_pass(st["camera"], pp, rows=(384, 416))
+    assert gi.shape == (32, 720, 1280, 3) and np.isfinite(gi).all()
+    z = assert_tiles_agree(gi[:, 384:416], oi[:, 384:416])
+    assert z.size == 2 * 80
