@@ -388,8 +388,10 @@ int32_t rt_render_accumulate(RtScene* scene, const RtCamera* cam, const RtPassPa
  * RtTuning.graph).  Outputs are RT_MEM_DEVICE buffers (or NULL) that must
  * stay valid until the work is done; at most one 2 GiB sample buffer of
  * samples per call (W·H·n_samples·12 bytes), no guide training.  Errors of
- * the device work (RT_ERR_TIMEOUT, RT_ERR_CAPACITY) and the statistics of
- * rt_last_render_stats come from the next rt_sync on the handle. */
+ * the device work (RT_ERR_TIMEOUT, RT_ERR_CAPACITY) come from the next
+ * rt_sync, or from the next call on the handle that checks the device's
+ * status, whichever comes first; the statistics of rt_last_render_stats from
+ * rt_sync (a later call on the handle first waits for the queued work). */
 int32_t rt_render_accumulate_async(RtScene* scene, const RtCamera* cam, const RtPassParams* params,
                                    float firefly_clamp, uint32_t firefly_min_samples,
                                    float firefly_floor, int32_t reset,

@@ -704,8 +704,15 @@ static void free_dev(void*& p) {
 // input buffer, or a caching allocator's freed block still in use, would race
 // with the library's kernels).  Every call synchronises its own stream before
 // it returns, so work the caller queues afterwards needs no ordering.
+static int fold_async(RtScene* s);
 static int enter(RtScene* s) {
     CK(cudaSetDevice(s->device));
+    if (s->async_pending) {
+        // a queued asynchronous call's statistics are folded before its
+        // pinned status words are reused (its device status stays in the
+        // error word for the next check)
+        if (int rc = fold_async(s)) return rc;
+    }
     CK(cudaEventRecord(s->caller_ev, s->caller));
     CK(cudaStreamWaitEvent(s->stream, s->caller_ev, 0));
     return RT_OK;
@@ -2184,11 +2191,11 @@ static int accumulate_impl(RtScene* s, const RtCamera* cam, const RtPassParams* 
                                                " samples per pixel at this size (one 2 GiB sample buffer)");
         if (s->guide && rtgh::mode(s->guide) == RT_GUIDE_TRAIN)
             return fail(s, RT_ERR_INVALID, "asynchronous calls do not train the guide");
+        CK(cudaSetDevice(s->device));
         if (s->async_pending) {
             // the previous asynchronous call's statistics are folded first
-            if (int r2 = rt_sync(s)) return r2;
+            if (int r2 = fold_async(s)) return r2;
         }
-        CK(cudaSetDevice(s->device));
         CK(cudaEventRecord(s->caller_ev, caller));
         CK(cudaStreamWaitEvent(s->stream, s->caller_ev, 0));
     } else {
@@ -2267,9 +2274,7 @@ extern "C" int32_t rt_render_accumulate_async(RtScene* s, const RtCamera* cam, c
                            true, (cudaStream_t)cuda_stream);
 }
 
-extern "C" int32_t rt_sync(RtScene* s) {
-    if (!s) return RT_ERR_INVALID;
-    CK(cudaSetDevice(s->device));
+static int fold_async(RtScene* s) {
     CK(cudaStreamSynchronize(s->stream));
     if (s->async_pending) {
         s->async_pending = false;
@@ -2280,6 +2285,13 @@ extern "C" int32_t rt_sync(RtScene* s) {
         s->last_shadow = (int64_t)s->h_tot[HDR_SHADOW / 2];
         s->last_launches += (int64_t)s->h_status[1] * (s->async_per_it + 1);
     }
+    return RT_OK;
+}
+
+extern "C" int32_t rt_sync(RtScene* s) {
+    if (!s) return RT_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    if (int rc = fold_async(s)) return rc;
     return check_err(s);
 }
 
