@@ -628,6 +628,8 @@ struct RtScene {
     // lagged end-of-work check: next-iteration ray counts copied to pinned memory
     uint32_t* h_status = nullptr;
     cudaEvent_t st_ev[8] = {};
+    // side streams of the per-class shading kernels (rth::launch_shade)
+    ShadeFork fk{};
     float* scratch = nullptr;
     size_t scratch_bytes = 0;
     uint8_t* d_conv = nullptr;
@@ -812,6 +814,9 @@ int32_t rt_scene_destroy(RtScene* s) {
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->caller_ev) cudaEventDestroy(s->caller_ev);
+    for (auto e : s->fk.join) if (e) cudaEventDestroy(e);
+    if (s->fk.fork) cudaEventDestroy(s->fk.fork);
+    for (auto q : s->fk.side) if (q) cudaStreamDestroy(q);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return RT_OK;
@@ -837,6 +842,14 @@ int32_t rt_scene_create(const RtSceneDesc* d, int32_t device, RtScene** out) {
     if (cudaEventCreateWithFlags(&s->caller_ev, cudaEventDisableTiming) != cudaSuccess)
         return bail(fail(s, RT_ERR_CUDA, "cudaEventCreate failed"));
     for (auto& e : s->st_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(s, RT_ERR_CUDA, "cudaEventCreate failed"));
+    for (auto& q : s->fk.side)
+        if (cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) != cudaSuccess)
+            return bail(fail(s, RT_ERR_CUDA, "cudaStreamCreate failed"));
+    if (cudaEventCreateWithFlags(&s->fk.fork, cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(s, RT_ERR_CUDA, "cudaEventCreate failed"));
+    for (auto& e : s->fk.join)
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
             return bail(fail(s, RT_ERR_CUDA, "cudaEventCreate failed"));
     if (cudaHostAlloc((void**)&s->h_status, 8 * sizeof(uint32_t), cudaHostAllocDefault) != cudaSuccess)
@@ -1996,7 +2009,7 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
             s->cap_n = m;
         }
         mark(2);
-        rth::launch_shade(s->S, A, B, W.Rt, R, c, W.cq, cn + CTR_COUNT, W.sq, s->sms, s->stream);
+        rth::launch_shade(s->S, A, B, W.Rt, R, c, W.cq, cn + CTR_COUNT, W.sq, s->sms, s->stream, &s->fk);
         if (R.photons) rth::launch_photon_gather_paths(s->photons, T, A.gq, c + CTR_GATHER_COUNT, s->sms, s->stream);
         mark(3);
         rth::launch_shadow(s->S, T, W.sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, W.derr, s->sms, s->stream);

@@ -62,6 +62,19 @@ enum { CLS_MISS = 0, CLS_EMIT = 1, CLS_DIFFUSE = 2, CLS_METAL = 3, CLS_DIELEC = 
 struct ClassQueues { uint32_t* q[CLS_N]; };
 static_assert(CTR_CLS_COUNT + CLS_N <= CTR_GATHER_COUNT, "counter slots");
 
+// Streams the shading kernels of one iteration fan out to.  The class kernels
+// read disjoint class queues and append to the shared queues (next set, retire
+// records, shadow and gather requests) by atomic reservation, so they may run
+// at the same time: `fork` is recorded after classification and every class
+// but the diffuse one waits on it from a side stream of its own; each `join`
+// orders the launching stream after its class before the shadow rays.
+struct ShadeFork {
+    static constexpr int N = CLS_N - 1;
+    cudaStream_t side[N];
+    cudaEvent_t fork;
+    cudaEvent_t join[N];
+};
+
 // Per-path wavefront state, structure of arrays.  The render loop keeps two
 // dense sets (iteration it reads set it&1 at positions 0..count−1 and writes
 // the paths that go on, compacted, into the other set), plus a set of
@@ -202,9 +215,10 @@ void launch_generate(const rtd::DevScene& S, const PathState& A, const RenderLau
                      uint32_t* count0, cudaStream_t st);
 // classify + one shading kernel per material class: paths that go on are
 // compacted into B (count `cout`), ended paths into the retire records Rt
+// (side by side on the streams of `fk` when it is given, else in turn on `st`)
 void launch_shade(const rtd::DevScene& S, const PathState& A, const PathState& B, const PathState& Rt,
                   const RenderLaunch& R, uint32_t* ctr, const ClassQueues& Q, uint32_t* cout, float4* sq, int sms,
-                  cudaStream_t st);
+                  cudaStream_t st, const ShadeFork* fk = nullptr);
 // write the ended paths' samples and append new samples, one per ended path
 // while samples remain, to B; add the iteration's ray counts to the header;
 // clear the counter block of iteration it + 2

@@ -1261,18 +1261,33 @@ void launch_generate(const DevScene& S, const PathState& A, const RenderLaunch& 
     k_generate<<<grid, 256, 0, st>>>(S, A, R.dev, pool, count0);
 }
 void launch_shade(const DevScene& S, const PathState& A, const PathState& B, const PathState& Rt, const RenderLaunch& R,
-                  uint32_t* ctr, const ClassQueues& Q, uint32_t* cout, float4* sq, int sms, cudaStream_t st) {
+                  uint32_t* ctr, const ClassQueues& Q, uint32_t* cout, float4* sq, int sms, cudaStream_t st,
+                  const ShadeFork* fk) {
     // ctr: this iteration's counter block (see rt_internal.h for the slots)
     int grid = sms * (S.shade_per_sm > 0 ? S.shade_per_sm : RT_SHADE_BLOCKS_PER_SM);
     k_classify<<<sms * 4, CLS_BLOCK, 0, st>>>(A.hit, ctr + CTR_COUNT, Q, ctr + CTR_CLS_COUNT);
+    // the classes but diffuse go to side streams, ordered after classification
+    // only (not after the guide's inference, which only the diffuse class reads)
+    int nside = 0;
+    if (fk) cudaEventRecord(fk->fork, st);
+    auto stream_of = [&](int C) -> cudaStream_t {
+        if (!fk || C == CLS_DIFFUSE) return st;
+        cudaStream_t s2 = fk->side[nside];
+        cudaStreamWaitEvent(s2, fk->fork, 0);
+        return s2;
+    };
     if (R.guide.mode != 0)
         launch_guide_infer(S, A, R, Q.q[CLS_DIFFUSE], ctr + CTR_CLS_COUNT + CLS_DIFFUSE, sms, st);
 #define RT_SHADE_CLASS_G(C, G)                                                                              \
-    if (!((S.class_mask >> (C)) & 1u)) {                                                                   \
-    } else if (S.bg_type == RT_BG_PHYSICAL)                                                                 \
-        k_shade<C, true, G><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R.dev, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr); \
-    else                                                                                                    \
-        k_shade<C, false, G><<<grid, RT_SHADE_BLOCK, 0, st>>>(S, A, B, Rt, R.dev, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr)
+    do {                                                                                                    \
+        if (!((S.class_mask >> (C)) & 1u)) break;                                                           \
+        cudaStream_t cs = stream_of(C);                                                                     \
+        if (S.bg_type == RT_BG_PHYSICAL)                                                                    \
+            k_shade<C, true, G><<<grid, RT_SHADE_BLOCK, 0, cs>>>(S, A, B, Rt, R.dev, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr); \
+        else                                                                                                \
+            k_shade<C, false, G><<<grid, RT_SHADE_BLOCK, 0, cs>>>(S, A, B, Rt, R.dev, Q.q[C], ctr + CTR_CLS_COUNT + C, cout, sq, ctr); \
+        if (cs != st) cudaEventRecord(fk->join[nside++], cs);                                              \
+    } while (0)
 #define RT_SHADE_CLASS(C) RT_SHADE_CLASS_G(C, false)
     RT_SHADE_CLASS(CLS_MISS);
     RT_SHADE_CLASS(CLS_EMIT);
@@ -1284,6 +1299,7 @@ void launch_shade(const DevScene& S, const PathState& A, const PathState& B, con
     if (S.n_media > 0) { RT_SHADE_CLASS(CLS_MEDIUM); }
 #undef RT_SHADE_CLASS
 #undef RT_SHADE_CLASS_G
+    for (int i = 0; i < nside; i++) cudaStreamWaitEvent(st, fk->join[i], 0);
 }
 void launch_retire(const DevScene& S, const PathState& B, const PathState& Rt, const RenderLaunch& R, uint32_t* ctr,
                    uint32_t* hdr, uint32_t* clear_block, uint32_t* cout, int sms, cudaStream_t st) {
