@@ -2010,9 +2010,18 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         }
         mark(2);
         rth::launch_shade(s->S, A, B, W.Rt, R, c, W.cq, cn + CTR_COUNT, W.sq, s->sms, s->stream, &s->fk);
-        if (R.photons) rth::launch_photon_gather_paths(s->photons, T, A.gq, c + CTR_GATHER_COUNT, s->sms, s->stream);
+        if (R.photons) {
+            // the caustic lookup scales the parked pendC terms and the shadow
+            // rays cancel pend0 / pend1: disjoint writes, so the lookup runs
+            // on a side stream beside the shadow rays (joined before retire)
+            CK(cudaEventRecord(s->fk.fork, s->stream));
+            CK(cudaStreamWaitEvent(s->fk.side[0], s->fk.fork, 0));
+            rth::launch_photon_gather_paths(s->photons, T, A.gq, c + CTR_GATHER_COUNT, s->sms, s->fk.side[0]);
+            CK(cudaEventRecord(s->fk.join[0], s->fk.side[0]));
+        }
         mark(3);
         rth::launch_shadow(s->S, T, W.sq, c + CTR_SHADOW_COUNT, c + CTR_SHADOW_NEXT, W.derr, s->sms, s->stream);
+        if (R.photons) CK(cudaStreamWaitEvent(s->stream, s->fk.join[0], 0));
         mark(0);
         rth::launch_retire(s->S, B, W.Rt, R, c, hdr, blk(it + 2), cn + CTR_COUNT, s->sms, s->stream);
         return RT_OK;
