@@ -614,8 +614,11 @@ typedef struct RtTuning {
      * pool's first fill, then one conditional node per iteration up to the
      * call's bound, each run only while rays remain — captured on the first
      * call and replayed while the scene state, buffers and pool stay the
-     * same; 0 (the default): the host queues each iteration's launches and
-     * stops two iterations after the pool drains.  The images are the same. */
+     * same (every pass of an rt_render_batch call included: its job table
+     * is read from device memory); 0 (the default): the host queues each
+     * iteration's launches and stops two iterations after the pool drains.
+     * rt_render_pass_noalloc always runs the host-driven loop.  The images
+     * are the same. */
     uint32_t graph;
 } RtTuning;
 #define RT_NODES_FULL      0

@@ -142,16 +142,29 @@ def batch_request(job):
                 strata=int(math.sqrt(job["spp"])), sample_idx=0, seed=job["seed"])
 
 
-def run_packed(jobs, device=0, builders=None, keep_outputs=False, tune=False, window=0):
+def run_packed(jobs, device=0, builders=None, keep_outputs=False, tune=False, window=0, graph=True):
     """Render `jobs` packed: one rt_render_batch call per scene kind, the
-    kinds on concurrent threads (each handle its own stream).  Returns the
-    same summary as run_batch."""
+    kinds on concurrent threads (each handle its own stream).  With `graph`,
+    every pass of a call replays the handle's captured wavefront graph (the
+    job table and launch parameters are read from device memory, so one
+    capture serves every pass of the same pool size).  Returns the same
+    summary as run_batch."""
     builders = builders or {}
     kinds = sorted({j["scene"] for j in jobs})
     handles = {k: GpuScene(builders[k] if k in builders else build_scene(k), device=device) for k in kinds}
     tunings = tune_kinds([handles], jobs) if tune else None
-    for k in kinds:                                       # warm each handle's buffers
-        render_job(handles, dict(scene=k, width=64, height=64, spp=1, azimuth=0.0, elevation=20.0, seed=0))
+    if graph:
+        for h in handles.values():
+            h.set_tuning(**{**h.get_tuning(), "graph": 1})
+    for k in kinds:
+        # warm each handle: a packed request of one pool's worth of samples
+        # grows the path buffers to the pool and, with `graph`, captures the
+        # wavefront graph the timed passes replay
+        side = 1024
+        spp = max(1, -(-handles[k].get_tuning()["max_paths"] // (side * side)))
+        warm = dict(scene=k, width=side, height=side, azimuth=0.0, elevation=20.0)
+        handles[k].render_batch([dict(cam=job_camera(warm), width=side, height=side, spp=spp, seed=0)],
+                                pass_params(64, 64, 0, 1, 1, _DEPTH[k], 4, 1.0, 0))
     lat, outs, errors = {}, {}, []
     t0 = time.perf_counter()
 

@@ -1801,11 +1801,13 @@ struct WaveBufs {
     int* derr = nullptr;
     uint32_t cap = 0;
     bool guide = false;               // the scene's guide may run (not the no-alloc array)
+    bool graphable = false;           // the scene's own buffers: the call may run as the captured graph
 };
 
 static WaveBufs scene_bufs(const RtScene* s) {
     WaveBufs W;
     W.guide = true;
+    W.graphable = true;
     W.set[0] = s->P; W.set[1] = s->P2; W.Rt = s->Rt;
     W.cq = s->cq; W.sq = s->sq; W.counters = s->counters; W.derr = s->d_err;
     W.cap = std::min(s->cap, s->max_paths);
@@ -1845,10 +1847,11 @@ static void wave_graph_free(RtScene* s) {
     s->wg = RtScene::WaveGraph{};
 }
 
-// What a captured wavefront graph depends on besides the device RenderLaunch:
-// the scene state and buffers its launches were given, the pool and the flags
-// that choose its kernels.
-static std::vector<uint8_t> wave_key(const RtScene* s, const WaveBufs& W, const RenderLaunch& R, uint32_t pool) {
+// What a captured wavefront graph depends on besides the device RenderLaunch
+// (which carries the pool size, the bound and the batch table): the scene
+// state and buffers its launches were given, the pool's capacity and the
+// flags that choose its kernels.
+static std::vector<uint8_t> wave_key(const RtScene* s, const WaveBufs& W, const RenderLaunch& R) {
     std::vector<uint8_t> k;
     auto put = [&](const void* p, size_t n) { const uint8_t* b = (const uint8_t*)p; k.insert(k.end(), b, b + n); };
     put(&s->S, sizeof(s->S));
@@ -1858,7 +1861,7 @@ static std::vector<uint8_t> wave_key(const RtScene* s, const WaveBufs& W, const 
     put(&W.cq, sizeof(W.cq));
     const void* ptrs[3] = {W.sq, W.counters, W.derr};
     put(ptrs, sizeof(ptrs));
-    int64_t v[5] = {pool, R.photons, R.guide.mode, s->sms, R.photons ? (int64_t)s->photons.generation : -1};
+    int64_t v[5] = {W.cap, R.photons, R.guide.mode, s->sms, R.photons ? (int64_t)s->photons.generation : -1};
     put(v, sizeof(v));
     return k;
 }
@@ -1869,12 +1872,12 @@ static std::vector<uint8_t> wave_key(const RtScene* s, const WaveBufs& W, const 
 // runs when iteration k left rays and the call's bound allows — a chain of
 // IF nodes cannot run past K, whatever the device state.
 template <class Pro, class It>
-static int wave_graph_ensure(RtScene* s, const WaveBufs& W, const RenderLaunch& R, uint32_t pool, uint64_t max_it,
+static int wave_graph_ensure(RtScene* s, const WaveBufs& W, const RenderLaunch& R, uint64_t max_it, uint64_t kmin,
                              Pro&& prologue, It&& iteration) {
-    std::vector<uint8_t> key = wave_key(s, W, R, pool);
+    std::vector<uint8_t> key = wave_key(s, W, R);
     if (s->wg.exec && s->wg.K >= max_it && key == s->wg.key) return RT_OK;
     wave_graph_free(s);
-    const uint64_t K = (max_it + 31) / 32 * 32;
+    const uint64_t K = (std::max(max_it, kmin) + 31) / 32 * 32;
     cudaGraph_t G = nullptr;
     cudaError_t e = cudaGraphCreate(&G, 0);
     auto ok = [&](cudaError_t r) { if (e == cudaSuccess && r != cudaSuccess) e = r; return e == cudaSuccess; };
@@ -1929,7 +1932,7 @@ static int wave_graph_ensure(RtScene* s, const WaveBufs& W, const RenderLaunch& 
 static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, const RtPassParams* p, uint32_t sample_idx,
                          uint32_t nsamp, float* dscratch, const uint32_t* active, uint32_t nactive, int64_t* ext_rays,
                          int64_t* sh_rays, int64_t* launches, const JobDev* jobs = nullptr, uint32_t n_jobs = 0,
-                         uint64_t jobs_total = 0, bool async = false) {
+                         uint64_t jobs_total = 0, bool async = false, uint64_t graph_kmin = 0) {
     uint64_t total = n_jobs ? jobs_total : (uint64_t)nsamp * nactive;
     if (total == 0) return RT_OK;
     uint32_t pool = (uint32_t)std::min<uint64_t>(total, W.cap);
@@ -1959,12 +1962,13 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
     uint64_t max_it = total * maxd / pool + maxd + 2;
     if (s->max_iterations) max_it = std::min<uint64_t>(max_it, s->max_iterations);
     R.max_it = max_it;
+    R.pool = pool;
     // stream-ordered: the previous call's kernels have read the old copy
     CK(cudaMemcpyAsync(s->d_R, &R, sizeof(R), cudaMemcpyHostToDevice, s->stream));
     uint32_t* hdr = W.counters;
     auto blk = [&](uint64_t it) { return W.counters + CTR_HDR_WORDS + (it % RT_CTR_RING) * RT_CTR_STRIDE; };
     size_t ev_used = 0;
-    const bool graph = (s->graph_mode || async) && !s->profiling && !(s->cap_out && s->cap_depth >= 0) && W.guide;
+    const bool graph = (s->graph_mode || async) && !s->profiling && !(s->cap_out && s->cap_depth >= 0) && W.graphable;
     auto mark = [&](int kind) {
         if (!s->profiling || graph) return;
         if (ev_used >= s->pev.size()) { cudaEvent_t e; cudaEventCreate(&e); s->pev.push_back(e); s->pkind.push_back(0); }
@@ -1979,7 +1983,8 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
     auto prologue = [&]() {
         CK(cudaMemsetAsync(W.counters, 0, sizeof(uint32_t) * RT_CTR_WORDS, s->stream));
         mark(0);
-        rth::launch_generate(s->S, W.set[0], R, pool, blk(0) + CTR_COUNT, s->stream);
+        // a captured first fill serves every pool size up to the capacity
+        rth::launch_generate(s->S, W.set[0], R, graph ? W.cap : pool, blk(0) + CTR_COUNT, s->stream);
         return RT_OK;
     };
     // the launches of iteration `it`
@@ -2033,7 +2038,7 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         // per iteration up to the bound, each run only while rays remain (the
         // graph is captured once and kept while the buffers, scene state and
         // bound it was made for stay the same)
-        if (int rc = wave_graph_ensure(s, W, R, pool, max_it, prologue, iteration)) return rc;
+        if (int rc = wave_graph_ensure(s, W, R, max_it, graph_kmin, prologue, iteration)) return rc;
         CK(cudaGraphLaunch(s->wg.exec, s->stream));
         CK(cudaMemcpyAsync(s->h_status, s->d_gstat, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream));
         if (async) {
@@ -2354,7 +2359,14 @@ extern "C" int32_t rt_render_batch(RtScene* s, const RtBatchJob* jobs, int32_t n
     CK(cudaMemsetAsync(s->b_m2, 0, tot_pix * 12, s->stream));
     CK(cudaMemsetAsync(s->b_cnt, 0, tot_pix * 4, s->stream));
     // samples per pixel per pass: as many as keep the pass's samples within 2 GiB
-    const uint64_t budget = (2ull << 30) / 12;
+    // and, when the passes replay the captured wavefront graph, within
+    // RT_GRAPH_PASS_POOLS pools, so that one chain of (RT_GRAPH_PASS_POOLS + 1)
+    // × depth + 2 iterations bounds every pass and the graph captured for the
+    // first pass serves the others
+    const uint32_t maxd_b = std::min<uint32_t>(shared->max_depth, RT_MAX_DEPTH);
+    const uint64_t budget = s->graph_mode ? std::min<uint64_t>((2ull << 30) / 12,
+                                                               (uint64_t)RT_GRAPH_PASS_POOLS * s->max_paths)
+                                          : (2ull << 30) / 12;
     uint32_t W = window;
     if (W == 0) {
         uint32_t mx = 0;
@@ -2415,7 +2427,7 @@ extern "C" int32_t rt_render_batch(RtScene* s, const RtBatchJob* jobs, int32_t n
         q.width = tab[0].width; q.height = tab[0].height;
         int64_t e1 = 0, s1 = 0, l1 = 0;
         rc = run_wavefront(s, Wb, &tab[0].cam, &q, 0, 1, s->scratch, nullptr, 1, &e1, &s1, &l1, s->d_jobs,
-                           (uint32_t)tab.size(), cursor);
+                           (uint32_t)tab.size(), cursor, false, (RT_GRAPH_PASS_POOLS + 1ull) * maxd_b + 2);
         if (rc) break;
         for (size_t t = 0; t < tab.size(); t++) {
             int32_t j = ids[t];

@@ -32,6 +32,11 @@
 #define RT_SHADE_BLOCK 128
 #define RT_SHADE_BLOCKS_PER_SM 8
 #define RT_MAX_DEPTH 256
+// samples of one rt_render_batch pass, in path pools, when the passes replay
+// the captured wavefront graph (the chain it captures grows with it)
+#ifndef RT_GRAPH_PASS_POOLS
+#define RT_GRAPH_PASS_POOLS 32
+#endif
 
 // Counter block of one wavefront iteration (RT_CTR_STRIDE uint32): ray count,
 // fetch cursors of the persistent kernels, shadow-ray count, per-material-class
@@ -190,6 +195,8 @@ struct RenderLaunch {
     // call, so a captured graph of the call's launches serves every call)
     const RenderLaunch* dev;
     uint64_t max_it;                       // the call's wavefront iteration bound
+    uint32_t pool;                         // paths of the pool's first fill (read on the device, so a
+                                           // captured graph serves calls of any pool size)
 };
 
 namespace rth {
@@ -210,8 +217,9 @@ void launch_extend(const rtd::DevScene& S, const PathState& P, const uint32_t* q
 void launch_shadow(const rtd::DevScene& S, const PendTargets& T, const float4* sq, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st);
 
-// first fill of the path pool: samples 0 .. pool−1 into positions 0 .. pool−1 of set A
-void launch_generate(const rtd::DevScene& S, const PathState& A, const RenderLaunch& R, uint32_t pool,
+// first fill of the path pool: samples 0 .. R.pool−1 into positions 0 .. R.pool−1 of set A
+// (R.pool read on the device; `capacity` ≥ R.pool only sizes the grid)
+void launch_generate(const rtd::DevScene& S, const PathState& A, const RenderLaunch& R, uint32_t capacity,
                      uint32_t* count0, cudaStream_t st);
 // classify + one shading kernel per material class: paths that go on are
 // compacted into B (count `cout`), ended paths into the retire records Rt

@@ -430,9 +430,9 @@ RT_D void init_path(const DevScene& S, const PathState& P, const RenderLaunch& R
     if (R.guide.mode == 2) P.rec[pid] = rtg::REC_NONE;
 }
 
-__global__ void k_generate(DevScene S, PathState A, const RenderLaunch* __restrict__ Rp, uint32_t pool,
-                           uint32_t* count0) {
+__global__ void k_generate(DevScene S, PathState A, const RenderLaunch* __restrict__ Rp, uint32_t* count0) {
     const RenderLaunch& R = *Rp;
+    const uint32_t pool = R.pool;
     if (blockIdx.x == 0 && threadIdx.x == 0) { *R.gen_next = pool; *count0 = pool; }
     for (uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x; pid < pool; pid += gridDim.x * blockDim.x)
         init_path(S, A, R, pid, pid);
@@ -1255,10 +1255,10 @@ void launch_guide_infer(const DevScene& S, const PathState& A, const RenderLaunc
     k_guide_encode<<<sms * 8, 256, 0, st>>>(S, A, R.dev, queue, count);
     k_guide_infer<<<sms * 2, GUIDE_WARPS * 32, guide_infer_smem(), st>>>(R.dev, queue, count);
 }
-void launch_generate(const DevScene& S, const PathState& A, const RenderLaunch& R, uint32_t pool, uint32_t* count0,
-                     cudaStream_t st) {
-    int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>((pool + 255) / 256, 148u * 16u));
-    k_generate<<<grid, 256, 0, st>>>(S, A, R.dev, pool, count0);
+void launch_generate(const DevScene& S, const PathState& A, const RenderLaunch& R, uint32_t capacity,
+                     uint32_t* count0, cudaStream_t st) {
+    int grid = (int)std::max<uint32_t>(1u, std::min<uint32_t>((capacity + 255) / 256, 148u * 16u));
+    k_generate<<<grid, 256, 0, st>>>(S, A, R.dev, count0);
 }
 void launch_shade(const DevScene& S, const PathState& A, const PathState& B, const PathState& Rt, const RenderLaunch& R,
                   uint32_t* ctr, const ClassQueues& Q, uint32_t* cout, float4* sq, int sms, cudaStream_t st,

@@ -24,14 +24,16 @@ def _bits(a):
     return np.ascontiguousarray(a).view(np.uint32)
 
 
-def test_packed_batch_frames_are_bit_identical_to_single_renders():
+@pytest.mark.parametrize("graph", [False, True])
+def test_packed_batch_frames_are_bit_identical_to_single_renders(graph):
     """Requests of different size, spp, camera and seed packed into one
     wavefront pool (rt_render_batch, in passes of 3 samples per pixel so most
     requests span several passes) give every request exactly the sum, M2 and
-    count of rendering it alone with rt_render_accumulate."""
+    count of rendering it alone with rt_render_accumulate, whether the passes
+    run the host-driven loop or replay the captured wavefront graph."""
     jobs = batch.make_jobs(seed=7, n=10, scenes=("box", "icosphere"), min_width=24, max_width=80, min_spp=1, max_spp=9)
     builders = {"box": configs.box_scene()[0], "icosphere": configs.icosphere_scene(levels=4, env_w=64, env_h=32)[0]}
-    packed = batch.run_packed(jobs, builders=builders, keep_outputs=True, window=3)
+    packed = batch.run_packed(jobs, builders=builders, keep_outputs=True, window=3, graph=graph)
     seq = batch.run_batch(jobs, workers=1, builders=builders, keep_outputs=True)
     for j in jobs:
         a, b = packed["outputs"][j["id"]], seq["outputs"][j["id"]]
