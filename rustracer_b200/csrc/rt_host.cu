@@ -608,6 +608,7 @@ struct RtScene {
     float4* sq = nullptr;
     uint32_t* counters = nullptr;     // RT_CTR_WORDS (header + ring of iteration blocks)
     int* d_err = nullptr;
+    uint32_t* d_bins = nullptr;       // ray binning histogram and cursors
     RenderLaunch* d_R = nullptr;      // device copy of the current call's RenderLaunch
     // the wavefront as one captured graph (rt_set_tuning graph = 1, and the
     // asynchronous entry point): kept while its key (buffers, scene state,
@@ -800,7 +801,7 @@ int32_t rt_scene_destroy(RtScene* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto& b : s->owned) cudaFree(b.p);
     void* ps[] = {s->counters, s->d_err, s->scratch, s->d_conv, s->acc, s->m2, s->cnt, s->stage, s->d_active,
-                  s->b_acc, s->b_m2, s->b_cnt, s->d_jobs, s->d_R, s->d_gstat};
+                  s->b_acc, s->b_m2, s->b_cnt, s->d_jobs, s->d_R, s->d_gstat, s->d_bins};
     if (s->wg.exec) cudaGraphExecDestroy(s->wg.exec);
     if (s->wg.graph) cudaGraphDestroy(s->wg.graph);
     if (s->h_tot) cudaFreeHost(s->h_tot);
@@ -1786,6 +1787,8 @@ static int ensure_paths(RtScene* s, uint32_t cap) {
     s->P2.gq = s->P.gq;
     if (!s->counters && cudaMalloc(&s->counters, sizeof(uint32_t) * RT_CTR_WORDS) != cudaSuccess)
         return fail(s, RT_ERR_NOMEM, "cudaMalloc counters");
+    if (!s->d_bins && cudaMalloc(&s->d_bins, sizeof(uint32_t) * 2 * RT_NBINS) != cudaSuccess)
+        return fail(s, RT_ERR_NOMEM, "cudaMalloc ray bins");
     s->cap = cap;
     return RT_OK;
 }
@@ -1802,6 +1805,8 @@ struct WaveBufs {
     uint32_t cap = 0;
     bool guide = false;               // the scene's guide may run (not the no-alloc array)
     bool graphable = false;           // the scene's own buffers: the call may run as the captured graph
+    uint32_t* binq = nullptr;         // extend order after ray binning (RT_RAY_BINS), or null
+    uint32_t* bins = nullptr;         // its histogram and cursors
 };
 
 static WaveBufs scene_bufs(const RtScene* s) {
@@ -1811,6 +1816,9 @@ static WaveBufs scene_bufs(const RtScene* s) {
     W.set[0] = s->P; W.set[1] = s->P2; W.Rt = s->Rt;
     W.cq = s->cq; W.sq = s->sq; W.counters = s->counters; W.derr = s->d_err;
     W.cap = std::min(s->cap, s->max_paths);
+    // the photon tracer's queue is free while a render runs
+    W.binq = s->queue[0];
+    W.bins = s->d_bins;
     return W;
 }
 
@@ -1995,7 +2003,17 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         const PathState& B = W.set[(it + 1) & 1];
         PendTargets T{{B.pend0, B.pend1, W.Rt.pend0, W.Rt.pend1}, {B.pendC, W.Rt.pendC}};
         mark(1);
-        rth::launch_extend(s->S, A, nullptr, c + CTR_COUNT, c + CTR_EXTEND_NEXT, W.derr, s->sms, s->stream);
+        const uint32_t* xq = nullptr;
+#if RT_RAY_BINS
+        if (W.binq && W.bins) {
+            float3 lo = make_float3(s->world_lo[0], s->world_lo[1], s->world_lo[2]);
+            auto sc = [&](int a) { return (float)RT_BIN_CELLS / std::max(s->world_hi[a] - s->world_lo[a], 1e-6f); };
+            rth::launch_bin_rays(A, c + CTR_COUNT, W.cap, lo, make_float3(sc(0), sc(1), sc(2)), W.bins, W.binq,
+                                 s->stream);
+            xq = W.binq;
+        }
+#endif
+        rth::launch_extend(s->S, A, xq, c + CTR_COUNT, c + CTR_EXTEND_NEXT, W.derr, s->sms, s->stream);
         if (s->S.n_media > 0) rth::launch_media(s->S, A, nullptr, c + CTR_COUNT, s->sms, s->stream);
         if (!graph && (int64_t)it == s->cap_depth && s->cap_out) {
             // diagnostics: copy this iteration's rays out (origin, direction)

@@ -34,6 +34,11 @@
 #define RT_MAX_DEPTH 256
 // samples of one rt_render_batch pass, in path pools, when the passes replay
 // the captured wavefront graph (the chain it captures grows with it)
+#ifndef RT_RAY_BINS
+#define RT_RAY_BINS 0
+#endif
+#define RT_BIN_CELLS 4
+#define RT_NBINS (8 * RT_BIN_CELLS * RT_BIN_CELLS * RT_BIN_CELLS)
 #ifndef RT_GRAPH_PASS_POOLS
 #define RT_GRAPH_PASS_POOLS 32
 #endif
@@ -217,6 +222,12 @@ void launch_extend(const rtd::DevScene& S, const PathState& P, const uint32_t* q
 void launch_shadow(const rtd::DevScene& S, const PendTargets& T, const float4* sq, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st);
 
+// ray binning before extend (RT_RAY_BINS): a counting sort of set A's rays
+// by direction octant and an RT_BIN_CELLS³ cell of the origin in the box
+// (lo, lo + RT_BIN_CELLS / scale); `out` receives the path positions in bin
+// order, `bins` holds 2 × RT_NBINS words of scratch (cleared here)
+void launch_bin_rays(const PathState& A, const uint32_t* count, uint32_t capacity, float3 lo, float3 scale,
+                     uint32_t* bins, uint32_t* out, cudaStream_t st);
 // first fill of the path pool: samples 0 .. R.pool−1 into positions 0 .. R.pool−1 of set A
 // (R.pool read on the device; `capacity` ≥ R.pool only sizes the grid)
 void launch_generate(const rtd::DevScene& S, const PathState& A, const RenderLaunch& R, uint32_t capacity,

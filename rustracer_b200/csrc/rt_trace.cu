@@ -15,6 +15,8 @@
 // continues with the nearest while the others go on a per-thread stack.
 #include <algorithm>
 
+#include <cub/block/block_scan.cuh>
+
 #include "rt_internal.h"
 #include "rt_media.cuh"
 
@@ -840,6 +842,69 @@ __global__ void k_transmittance_api(DevScene S, const float* __restrict__ rays, 
 }
 
 // ── host launchers ──────────────────────────────────────────────────────────
+// ── ray binning before extend (RT_RAY_BINS) ────────────────────────────────
+// A counting sort of the set's rays by direction octant and a coarse cell of
+// the origin: the extend kernel then takes its rays in bin order, so the lanes
+// of a warp start rays that visit similar nodes in a similar order.  Each
+// block sorts a contiguous chunk, so neighbours in the set stay neighbours
+// within a bin.  The hits do not depend on the order.
+#define BIN_BLOCK 256
+#define BIN_ITEMS 8
+#define BIN_CHUNK (BIN_BLOCK * BIN_ITEMS)
+__device__ __forceinline__ uint32_t ray_bin(float4 ro, float4 rd, float3 lo, float3 sc) {
+    uint32_t oct = (rd.x < 0.f ? 1u : 0u) | (rd.y < 0.f ? 2u : 0u) | (rd.z < 0.f ? 4u : 0u);
+    int cx = min(max(__float2int_rz((ro.x - lo.x) * sc.x), 0), RT_BIN_CELLS - 1);
+    int cy = min(max(__float2int_rz((ro.y - lo.y) * sc.y), 0), RT_BIN_CELLS - 1);
+    int cz = min(max(__float2int_rz((ro.z - lo.z) * sc.z), 0), RT_BIN_CELLS - 1);
+    return ((oct * RT_BIN_CELLS + (uint32_t)cx) * RT_BIN_CELLS + (uint32_t)cy) * RT_BIN_CELLS + (uint32_t)cz;
+}
+__global__ void __launch_bounds__(BIN_BLOCK) k_bin_count(PathState A, const uint32_t* __restrict__ count, float3 lo,
+                                                         float3 sc, uint32_t* hist) {
+    __shared__ uint32_t h[RT_NBINS];
+    const uint32_t n = *count, base = blockIdx.x * BIN_CHUNK;
+    if (base >= n) return;                       // uniform in the block
+    for (int b = threadIdx.x; b < RT_NBINS; b += BIN_BLOCK) h[b] = 0;
+    __syncthreads();
+    for (int k = 0; k < BIN_ITEMS; k++) {
+        uint32_t i = base + k * BIN_BLOCK + threadIdx.x;
+        if (i < n) atomicAdd(&h[ray_bin(A.ray_o[i], A.ray_d[i], lo, sc)], 1u);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < RT_NBINS; b += BIN_BLOCK)
+        if (h[b]) atomicAdd(hist + b, h[b]);
+}
+__global__ void __launch_bounds__(BIN_BLOCK) k_bin_scatter(PathState A, const uint32_t* __restrict__ count, float3 lo,
+                                                           float3 sc, const uint32_t* __restrict__ hist,
+                                                           uint32_t* cursor, uint32_t* out) {
+    static_assert(RT_NBINS == 2 * BIN_BLOCK, "two bins per thread in the scan");
+    typedef cub::BlockScan<uint32_t, BIN_BLOCK> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ uint32_t h[RT_NBINS], start[RT_NBINS];
+    const uint32_t n = *count, base = blockIdx.x * BIN_CHUNK;
+    if (base >= n) return;                       // uniform in the block
+    // the bins' starts: exclusive prefix of the histogram
+    uint32_t v[2] = {hist[2 * threadIdx.x], hist[2 * threadIdx.x + 1]};
+    Scan(tmp).ExclusiveSum(v, v);
+    start[2 * threadIdx.x] = v[0];
+    start[2 * threadIdx.x + 1] = v[1];
+    h[2 * threadIdx.x] = 0;
+    h[2 * threadIdx.x + 1] = 0;
+    __syncthreads();
+    uint32_t key[BIN_ITEMS], rank[BIN_ITEMS];
+    for (int k = 0; k < BIN_ITEMS; k++) {
+        uint32_t i = base + k * BIN_BLOCK + threadIdx.x;
+        key[k] = i < n ? ray_bin(A.ray_o[i], A.ray_d[i], lo, sc) : RT_NBINS;
+        rank[k] = key[k] < RT_NBINS ? atomicAdd(&h[key[k]], 1u) : 0u;
+    }
+    __syncthreads();
+    // this block's run in each bin
+    for (int b = threadIdx.x; b < RT_NBINS; b += BIN_BLOCK)
+        if (h[b]) h[b] = start[b] + atomicAdd(cursor + b, h[b]);
+    __syncthreads();
+    for (int k = 0; k < BIN_ITEMS; k++)
+        if (key[k] < RT_NBINS) out[h[key[k]] + rank[k]] = base + k * BIN_BLOCK + threadIdx.x;
+}
+
 namespace rth {
 #ifndef RT_TRACE_GRID_PER_SM
 #define RT_TRACE_GRID_PER_SM RT_TRACE_MINB
@@ -872,6 +937,13 @@ void launch_trace_closest_api(const DevScene& S, const float* rays, uint32_t n, 
 void launch_trace_any_api(const DevScene& S, const float* rays, uint32_t n, uint8_t* out, uint32_t* next, int* err,
                           int sms, cudaStream_t st) {
     RT_TRACE_LAUNCH(k_any, 1, S, PendTargets{}, nullptr, rays, n, nullptr, next, out, err);
+}
+void launch_bin_rays(const PathState& A, const uint32_t* count, uint32_t capacity, float3 lo, float3 scale,
+                     uint32_t* bins, uint32_t* out, cudaStream_t st) {
+    uint32_t grid = std::max<uint32_t>(1u, (capacity + BIN_CHUNK - 1) / BIN_CHUNK);
+    cudaMemsetAsync(bins, 0, 2 * RT_NBINS * sizeof(uint32_t), st);
+    k_bin_count<<<grid, BIN_BLOCK, 0, st>>>(A, count, lo, scale, bins);
+    k_bin_scatter<<<grid, BIN_BLOCK, 0, st>>>(A, count, lo, scale, bins, bins + RT_NBINS, out);
 }
 void launch_extend(const DevScene& S, const PathState& P, const uint32_t* queue, const uint32_t* count,
                    uint32_t* next, int* err, int sms, cudaStream_t st) {
