@@ -1966,8 +1966,11 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
     R.n_jobs = n_jobs;
     R.dev = s->d_R;
     // every iteration with samples left advances `pool` path segments, and a
-    // sample has at most maxd segments; the drain takes at most maxd more
-    uint64_t max_it = total * maxd / pool + maxd + 2;
+    // sample has at most maxd segments; the drain takes at most maxd more.  A
+    // call whose samples all fit in the pool is never refilled: its paths all
+    // start at depth 0 and none goes on past depth maxd − 1, so maxd
+    // iterations (at least one) drain it, and the host queues no empty ones
+    uint64_t max_it = total <= pool ? std::max<uint64_t>(maxd, 1) : total * maxd / pool + maxd + 2;
     if (s->max_iterations) max_it = std::min<uint64_t>(max_it, s->max_iterations);
     R.max_it = max_it;
     R.pool = pool;
@@ -2092,11 +2095,12 @@ static int run_wavefront(RtScene* s, const WaveBufs& W, const RtCamera* cam, con
         CK(cudaMemcpyAsync(tot, W.counters, sizeof(tot), cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
         if (!done) {
-            // the bound was reached: the last iterations' counts must be zero
-            for (uint32_t k = 0; k < std::min<uint64_t>(it, STATUS_LAG); k++)
-                if (s->h_status[(uint32_t)((it - 1 - k) % STATUS_RING)] != 0)
-                    return fail(s, RT_ERR_TIMEOUT, "wavefront did not drain within its iteration bound (" +
-                                                       std::to_string(max_it) + " iterations)");
+            // the bound was reached: the last iteration must have left no rays
+            // (a count that reaches zero stays zero: no path is left to retire
+            // and hand its slot a new sample)
+            if (it > 0 && s->h_status[(uint32_t)((it - 1) % STATUS_RING)] != 0)
+                return fail(s, RT_ERR_TIMEOUT, "wavefront did not drain within its iteration bound (" +
+                                                   std::to_string(max_it) + " iterations)");
         }
     }
     if (ext_rays) *ext_rays += (int64_t)tot[HDR_EXT / 2];
